@@ -1,0 +1,403 @@
+"""Host-side scene description shared by the XML loader, the synthetic scene
+generators and the C-ABI upload path.
+
+A :class:`SceneDesc` is the flattened result of Hikari's XML parse
+(src/core/Parser.cpp:9): meshes in XML order with their BSDF and optional
+area emitter, one optional environment emitter, the perspective camera, the
+reconstruction filter and the pathMIS ``depth``.  Emitter order follows
+Scene::AddChild (src/core/Scene.cpp:167): mesh emitters in XML order, the
+environment emitter at the position where it is parsed.
+"""
+from __future__ import annotations
+
+import math
+import os
+import xml.etree.ElementTree as ET
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+# BSDF kinds, matching hk_bsdf_type in include/hikari_b200.h
+BSDF_DIFFUSE, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_PLASTIC, BSDF_ROUGH_COATING = range(5)
+BECKMANN, GGX = 0, 1
+BSDF_TYPE_NAMES = {
+    "diffuse": BSDF_DIFFUSE,
+    "roughConductor": BSDF_ROUGH_CONDUCTOR,
+    "roughDielectric": BSDF_ROUGH_DIELECTRIC,
+    "roughPlastic": BSDF_ROUGH_PLASTIC,
+    "roughCoating": BSDF_ROUGH_COATING,
+}
+FILTER_KINDS = {"box": 0, "tent": 1, "gaussian": 2, "mitchell": 3}
+
+AIR_IOR = 1.000277  # DEFAULT_*_EXT_IOR, include/core/Common.hpp:333
+
+
+class SceneError(RuntimeError):
+    """Raised for malformed scenes (the reference throws HikariException)."""
+
+
+@dataclass
+class BSDFDesc:
+    """Properties of one BSDF; defaults are the reference's
+    (include/core/Common.hpp:331-392)."""
+
+    type: int = BSDF_DIFFUSE
+    distribution: int = BECKMANN
+    anisotropic: bool = False
+    nonlinear: bool = False
+    alpha_u: float = 0.1
+    alpha_v: float = 0.1
+    int_ior: float = 1.5046
+    ext_ior: float = AIR_IOR
+    eta: Optional[List[float]] = None  # per-channel conductor eta; None -> int_ior/ext_ior
+    k: List[float] = field(default_factory=lambda: [1.0, 1.0, 1.0])
+    ks: List[float] = field(default_factory=lambda: [1.0, 1.0, 1.0])
+    ks_refract: List[float] = field(default_factory=lambda: [1.0, 1.0, 1.0])
+    kd: List[float] = field(default_factory=lambda: [0.5, 0.5, 0.5])
+    sigma_a: List[float] = field(default_factory=lambda: [0.0, 0.0, 0.0])
+    thickness: float = 1.0
+    nested: Optional["BSDFDesc"] = None
+
+    def conductor_eta(self) -> List[float]:
+        if self.eta is not None:
+            return list(self.eta)
+        e = np.float32(self.int_ior) / np.float32(self.ext_ior)
+        return [float(e)] * 3
+
+
+@dataclass
+class MeshDesc:
+    positions: np.ndarray  # (nv, 3) float32, world space
+    indices: np.ndarray  # (nt, 3) uint32
+    bsdf: BSDFDesc
+    normals: Optional[np.ndarray] = None  # (nv, 3) float32
+    radiance: Optional[List[float]] = None  # area emitter
+    bbox: Optional[np.ndarray] = None  # (2,3): includes unreferenced vertices
+
+
+@dataclass
+class EnvDesc:
+    rgb: np.ndarray  # (H, W, 3) float32
+    to_world: np.ndarray  # (4,4) float32
+    scale: float = 1.0
+
+
+@dataclass
+class CameraDesc:
+    width: int = 1280
+    height: int = 720
+    to_world: np.ndarray = field(default_factory=lambda: np.eye(4, dtype=np.float32))
+    fov: float = 30.0
+    near_clip: float = 1e-4
+    far_clip: float = 1e4
+
+
+@dataclass
+class FilterDesc:
+    kind: int = 2
+    radius: float = 2.0
+    p0: float = 0.5  # gaussian stddev / mitchell B
+    p1: float = 0.0  # mitchell C
+
+
+@dataclass
+class SceneDesc:
+    meshes: List[MeshDesc] = field(default_factory=list)
+    env: Optional[EnvDesc] = None
+    env_emitter_index: int = -1  # position of the env emitter in the emitter list
+    camera: CameraDesc = field(default_factory=CameraDesc)
+    filter: FilterDesc = field(default_factory=FilterDesc)
+    depth: int = 32
+    spp: int = 1
+    background: List[float] = field(default_factory=lambda: [0.0, 0.0, 0.0])
+    force_background: bool = False
+    integrator: str = "pathMIS"
+
+    @property
+    def n_triangles(self) -> int:
+        return int(sum(m.indices.shape[0] for m in self.meshes))
+
+    def emitter_order(self) -> List[int]:
+        """Mesh index per emitter, -1 for the environment (Scene::AddChild order)."""
+        order = []
+        for i, m in enumerate(self.meshes):
+            if m.radiance is not None:
+                order.append(i)
+        if self.env is not None:
+            pos = self.env_emitter_index if self.env_emitter_index >= 0 else len(order)
+            order.insert(min(pos, len(order)), -1)
+        return order
+
+
+# ----------------------------------------------------------------- transforms
+def _vec3(s: str) -> np.ndarray:
+    """ToVector3f  src/core/Common.cpp:108 (exactly 3 comma/space separated values)."""
+    toks = [t for t in s.replace(",", " ").split() if t]
+    if len(toks) != 3:
+        raise SceneError(f"Expected 3 values, got {s!r}")
+    return np.array([float(np.float32(t)) for t in toks], dtype=np.float32)
+
+
+def _angle_axis(angle_rad: float, axis: np.ndarray) -> np.ndarray:
+    """Eigen::AngleAxis matrix (the axis is used as given, not re-normalised)."""
+    x, y, z = (float(a) for a in axis)
+    c, s = math.cos(angle_rad), math.sin(angle_rad)
+    C = 1 - c
+    R = np.array(
+        [
+            [x * x * C + c, x * y * C - z * s, x * z * C + y * s],
+            [y * x * C + z * s, y * y * C + c, y * z * C - x * s],
+            [z * x * C - y * s, z * y * C + x * s, z * z * C + c],
+        ],
+        dtype=np.float64,
+    )
+    M = np.eye(4)
+    M[:3, :3] = R
+    return M
+
+
+def parse_transform(node: ET.Element) -> np.ndarray:
+    """<transform> children composed as Trans = Op * Trans (src/core/Parser.cpp:311-372)."""
+    T = np.eye(4, dtype=np.float64)
+    for ch in node:
+        tag = ch.tag
+        if tag == "translate":
+            v = _vec3(ch.attrib["value"])
+            M = np.eye(4)
+            M[:3, 3] = v
+        elif tag == "scale":
+            v = _vec3(ch.attrib["value"])
+            M = np.diag([v[0], v[1], v[2], 1.0])
+        elif tag == "rotate":
+            ang = math.radians(float(ch.attrib["angle"]))
+            M = _angle_axis(ang, _vec3(ch.attrib["axis"]))
+        elif tag == "matrix":
+            vals = [float(t) for t in ch.attrib["value"].replace(",", " ").split() if t]
+            if len(vals) != 16:
+                raise SceneError("Expected 16 values")
+            M = np.array(vals, dtype=np.float64).reshape(4, 4)
+        elif tag == "lookat":
+            o = _vec3(ch.attrib["origin"]).astype(np.float64)
+            t = _vec3(ch.attrib["target"]).astype(np.float64)
+            up = _vec3(ch.attrib["up"]).astype(np.float64)
+            d = t - o
+            d /= np.linalg.norm(d)
+            left = np.cross(up / np.linalg.norm(up), d)
+            left /= np.linalg.norm(left)
+            nup = np.cross(d, left)
+            nup /= np.linalg.norm(nup)
+            M = np.eye(4)
+            M[:3, 0], M[:3, 1], M[:3, 2], M[:3, 3] = left, nup, d, o
+        else:
+            raise SceneError(f"Unhandled element {tag!r}")
+        T = M @ T
+    return T.astype(np.float32)
+
+
+# ----------------------------------------------------------------------- OBJ
+def load_obj(path: str, to_world: Optional[np.ndarray] = None):
+    """WavefrontObjMesh ctor (src/mesh/WavefrontObjMesh.cpp:10-152): positions are
+    transformed as points, normals by the inverse transpose and normalised,
+    vertices are de-duplicated on their (p, uv, n) index triple in first-use
+    order, and quads split into (v1,v2,v3), (v4,v1,v3)."""
+    M = np.eye(4, dtype=np.float64) if to_world is None else np.asarray(to_world, dtype=np.float64)
+    Minv_t = np.linalg.inv(M)[:3, :3].T
+    P, N, UV, F = [], [], [], []
+    vmap: Dict[tuple, int] = {}
+    verts: List[tuple] = []
+    with open(path, "r") as fh:
+        for line in fh:
+            toks = line.split()
+            if not toks:
+                continue
+            pre = toks[0]
+            if pre == "v":
+                p = np.array([float(toks[1]), float(toks[2]), float(toks[3]), 1.0])
+                q = M @ p
+                P.append(q[:3] / q[3])
+            elif pre == "vt":
+                UV.append((float(toks[1]), float(toks[2])))
+            elif pre == "vn":
+                n = Minv_t @ np.array([float(toks[1]), float(toks[2]), float(toks[3])])
+                N.append(n / np.linalg.norm(n))
+            elif pre == "f":
+                fv = toks[1:5]
+                keys = []
+                for s in fv:
+                    parts = s.split("/")
+                    if len(parts) < 1 or len(parts) > 3:
+                        raise SceneError(f"Invalid OBJ vertex {s!r}")
+                    pi = int(parts[0])
+                    ti = int(parts[1]) if len(parts) > 1 and parts[1] else 0
+                    ni = int(parts[2]) if len(parts) > 2 and parts[2] else 0
+                    keys.append((pi, ti, ni))
+                tri = keys[:3] + ([keys[3], keys[0], keys[2]] if len(keys) == 4 else [])
+                for k in tri:
+                    if k not in vmap:
+                        vmap[k] = len(verts)
+                        verts.append(k)
+                    F.append(vmap[k])
+    Parr = np.asarray(P, dtype=np.float32).reshape(-1, 3)
+    positions = np.array([Parr[k[0] - 1] for k in verts], dtype=np.float32).reshape(-1, 3)
+    normals = None
+    if N:
+        Narr = np.asarray(N, dtype=np.float32)
+        normals = np.array([Narr[k[2] - 1] for k in verts], dtype=np.float32).reshape(-1, 3)
+    indices = np.asarray(F, dtype=np.uint32).reshape(-1, 3)
+    bbox = np.stack([Parr.min(0), Parr.max(0)]) if len(Parr) else None
+    return positions, indices, normals, bbox
+
+
+# ----------------------------------------------------------------------- XML
+def _props(node: ET.Element) -> Dict[str, object]:
+    out: Dict[str, object] = {}
+    for ch in node:
+        name = ch.attrib.get("name")
+        if ch.tag == "float":
+            out[name] = float(np.float32(ch.attrib["value"]))
+        elif ch.tag == "integer":
+            out[name] = int(ch.attrib["value"])
+        elif ch.tag == "boolean":
+            out[name] = ch.attrib["value"].strip().lower() == "true"
+        elif ch.tag == "string":
+            out[name] = ch.attrib["value"]
+        elif ch.tag in ("color", "point", "vector"):
+            out[name] = [float(x) for x in _vec3(ch.attrib["value"])]
+        elif ch.tag == "transform":
+            out[name] = parse_transform(ch)
+    return out
+
+
+def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
+    t = node.attrib["type"]
+    if t not in BSDF_TYPE_NAMES:
+        raise SceneError(f"BSDF type {t!r} is not supported by the CUDA pathMIS core")
+    p = _props(node)
+    d = BSDFDesc(type=BSDF_TYPE_NAMES[t])
+    dist = p.get("type", "beckmann")
+    if dist not in ("beckmann", "ggx"):
+        raise SceneError(f"Unexpected distribution type : {dist}")
+    d.distribution = GGX if dist == "ggx" else BECKMANN
+    if d.type == BSDF_DIFFUSE:
+        d.kd = p.get("albedo", [0.5, 0.5, 0.5])
+    elif d.type == BSDF_ROUGH_CONDUCTOR:
+        d.int_ior = p.get("intIOR", 1.5046)
+        d.ext_ior = p.get("extIOR", AIR_IOR)
+        d.k = p.get("k", [1.0, 1.0, 1.0])
+        d.ks = p.get("ks", [1.0, 1.0, 1.0])
+    elif d.type == BSDF_ROUGH_DIELECTRIC:
+        d.int_ior = p.get("intIOR", 1.5046)
+        d.ext_ior = p.get("extIOR", AIR_IOR)
+        d.ks = p.get("ksReflect", [1.0, 1.0, 1.0])
+        d.ks_refract = p.get("ksRefract", [1.0, 1.0, 1.0])
+    elif d.type == BSDF_ROUGH_PLASTIC:
+        d.int_ior = p.get("intIOR", 1.49)
+        d.ext_ior = p.get("extIOR", AIR_IOR)
+        d.ks = p.get("ks", [1.0, 1.0, 1.0])
+        d.kd = p.get("kd", [0.5, 0.5, 0.5])
+        d.nonlinear = bool(p.get("nonlinear", False))
+    elif d.type == BSDF_ROUGH_COATING:
+        d.int_ior = p.get("intIOR", 1.49)
+        d.ext_ior = p.get("extIOR", AIR_IOR)
+        d.ks = p.get("ks", [1.0, 1.0, 1.0])
+        d.sigma_a = p.get("sigmaA", [0.0, 0.0, 0.0])
+        d.thickness = p.get("thickness", 1.0)
+        nested = [c for c in node if c.tag == "bsdf"]
+        if len(nested) != 1:
+            raise SceneError("RoughCoatingBSDF needs a nested BSDF!")
+        d.nested = _bsdf_from_xml(nested[0])
+    if d.type in (BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC):
+        d.anisotropic = bool(p.get("as", False))
+    if d.anisotropic:
+        d.alpha_u = p.get("alphaU", 0.1)
+        d.alpha_v = p.get("alphaV", 0.1)
+    else:
+        d.alpha_u = d.alpha_v = p.get("alpha", 0.1)
+    return d
+
+
+def parse_scene_node(node: ET.Element, base_dir: str, env_loader=None) -> SceneDesc:
+    sd = SceneDesc()
+    p = _props(node)
+    sd.background = p.get("background", [0.0, 0.0, 0.0])
+    sd.force_background = bool(p.get("forceBackground", False))
+    n_emit = 0
+    for ch in node:
+        if ch.tag == "integrator":
+            sd.integrator = ch.attrib["type"]
+            ip = _props(ch)
+            if "depth" not in ip:
+                raise SceneError("Property 'depth' is missing")
+            sd.depth = int(ip["depth"])
+        elif ch.tag == "camera":
+            cp = _props(ch)
+            cam = CameraDesc()
+            cam.width = int(cp.get("width", 1280))
+            cam.height = int(cp.get("height", 720))
+            cam.fov = float(cp.get("fov", 30.0))
+            cam.near_clip = float(cp.get("nearClip", 1e-4))
+            cam.far_clip = float(cp.get("farClip", 1e4))
+            if "toWorld" in cp:
+                cam.to_world = cp["toWorld"]
+            for f in ch:
+                if f.tag == "rfilter":
+                    fp = _props(f)
+                    kind = FILTER_KINDS[f.attrib["type"]]
+                    if kind == 0:
+                        sd.filter = FilterDesc(0, 0.5)
+                    elif kind == 1:
+                        sd.filter = FilterDesc(1, 1.0)
+                    elif kind == 2:
+                        sd.filter = FilterDesc(2, fp.get("radius", 2.0), fp.get("stddev", 0.5))
+                    else:
+                        sd.filter = FilterDesc(3, fp.get("radius", 2.0), fp.get("B", 1 / 3), fp.get("C", 1 / 3))
+            sd.camera = cam
+        elif ch.tag == "sampler":
+            sd.spp = int(_props(ch).get("sampleCount", 1))
+        elif ch.tag == "mesh":
+            mp = _props(ch)
+            fn = os.path.join(base_dir, mp["filename"])
+            pos, idx, nrm, bbox = load_obj(fn, mp.get("toWorld"))
+            bs = [c for c in ch if c.tag == "bsdf"]
+            bsdf = _bsdf_from_xml(bs[0]) if bs else BSDFDesc()
+            em = [c for c in ch if c.tag == "emitter"]
+            rad = None
+            if em:
+                if em[0].attrib["type"] != "area":
+                    raise SceneError("only area emitters attach to meshes")
+                rad = _props(em[0])["radiance"]
+                n_emit += 1
+            sd.meshes.append(MeshDesc(pos, idx, bsdf, nrm, rad, bbox))
+        elif ch.tag == "emitter":
+            et = ch.attrib["type"]
+            if et != "env":
+                raise SceneError(f"emitter type {et!r} is not supported by the CUDA pathMIS core")
+            if sd.env is not None:
+                raise SceneError("Only one environment emiiter is allowed for the entire scene")
+            ep = _props(ch)
+            if env_loader is None:
+                raise SceneError("no environment-map loader given")
+            rgb = env_loader(os.path.join(base_dir, ep["filename"]))
+            sd.env = EnvDesc(rgb, ep.get("toWorld", np.eye(4, dtype=np.float32)), ep.get("scale", 1.0))
+            sd.env_emitter_index = n_emit
+            n_emit += 1
+        elif ch.tag == "accelerator" or ch.tag == "acceleration":
+            pass
+    return sd
+
+
+def parse_xml(path: str, env_loader=None) -> List[SceneDesc]:
+    """Parse a scene file: one <scene>, or a <test> holding several scenes.
+    Returns the list of scenes and, for tests, attaches ``references``."""
+    root = ET.parse(path).getroot()
+    base = os.path.dirname(os.path.abspath(path))
+    if root.tag == "scene":
+        return [parse_scene_node(root, base, env_loader)]
+    scenes = [parse_scene_node(n, base, env_loader) for n in root if n.tag == "scene"]
+    refs = [c for c in root if c.tag == "string" and c.attrib.get("name") == "references"]
+    if refs:
+        vals = [float(v) for v in refs[0].attrib["value"].replace(",", " ").split() if v]
+        for s, r in zip(scenes, vals):
+            s.reference = r  # type: ignore[attr-defined]
+    return scenes

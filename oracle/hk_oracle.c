@@ -1,0 +1,1580 @@
+/*
+ * hk_oracle.c -- CPU restatement of Hikari's pathMIS hot path (checker only).
+ *
+ * TEST INFRASTRUCTURE: loaded by tests/, __graft_entry__.smoke() and the
+ * cpu_baseline leg of bench.py, never by the product.  Citations are
+ * reference-project paths (file:line).  Arithmetic is float in the
+ * reference's evaluation order; film accumulation is double.
+ *
+ * Build: oracle/build.py (gcc -O2 -fopenmp -ffp-contract=off).
+ */
+#define _GNU_SOURCE
+#include "hk_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define PI_F 3.14159265358979323846f
+#define INV_PI_D 0.31830988618379067154
+#define EPS_RAY 1e-4f
+
+static __thread char g_err[512];
+const char *ho_last_error(void) { return g_err; }
+static int fail(const char *m) { snprintf(g_err, sizeof g_err, "%s", m); return -1; }
+
+/* ------------------------------------------------------------------ vec */
+typedef struct { float x, y, z; } v3;
+static inline v3 V(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static inline v3 add(v3 a, v3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub(v3 a, v3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 mul(v3 a, v3 b) { return V(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline v3 scl(v3 a, float s) { return V(a.x * s, a.y * s, a.z * s); }
+static inline v3 divs(v3 a, float s) { return V(a.x / s, a.y / s, a.z / s); }
+/* Eigen 3.3 fixed-size dot/squaredNorm reduce as a binary tree: x + (y + z)
+ * (redux_novec_unroller, ext/eigen/Eigen/src/Core/Redux.h:91) */
+static inline float dot(v3 a, v3 b) { return a.x * b.x + (a.y * b.y + a.z * b.z); }
+static inline v3 cross(v3 a, v3 b) {
+    return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline float norm(v3 a) { return sqrtf(dot(a, a)); }
+/* Eigen MatrixBase::normalized(): divide by sqrt(squaredNorm) if > 0 */
+static inline v3 normalize(v3 a) {
+    float z = dot(a, a);
+    return z > 0.0f ? divs(a, sqrtf(z)) : a;
+}
+static inline v3 vload(const float *p) { return V(p[0], p[1], p[2]); }
+static inline void vstore(float *p, v3 a) { p[0] = a.x; p[1] = a.y; p[2] = a.z; }
+/* Eigen DenseBase::isZero(): every |c| <= 1e-5f (dummy_precision<float>) */
+static inline int is_zero(v3 a) {
+    return fabsf(a.x) <= 1e-5f && fabsf(a.y) <= 1e-5f && fabsf(a.z) <= 1e-5f;
+}
+/* Color3f::IsValid  src/core/Color.cpp:44 */
+static inline int is_valid(v3 a) {
+    return !(a.x < 0.0f || !isfinite(a.x) || a.y < 0.0f || !isfinite(a.y) || a.z < 0.0f ||
+             !isfinite(a.z));
+}
+/* Color3f::GetLuminance  src/core/Color.cpp:95 */
+static inline float lum(v3 c) { return c.x * 0.212671f + c.y * 0.715160f + c.z * 0.072169f; }
+static inline float clampf(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+/* Signum  include/core/Common.hpp:901 */
+static inline float signum(float v) { return copysignf(1.0f, v); }
+/* Hypot2  include/core/Common.hpp:829 */
+static float hypot2(float a, float b) {
+    float r;
+    if (fabsf(a) > fabsf(b)) { r = b / a; r = fabsf(a) * sqrtf(1.0f + r * r); }
+    else if (b != 0.0f) { r = a / b; r = fabsf(b) * sqrtf(1.0f + r * r); }
+    else r = 0.0f;
+    return r;
+}
+
+/* ------------------------------------------------------------------ pcg32 */
+/* O'Neill's PCG-XSH-RR 64/32 as packaged in ext/pcg32/pcg32.h:29-110 */
+#define PCG_MULT 0x5851f42d4c957f2dULL
+uint32_t ho_pcg32_next(ho_pcg32 *r) {
+    uint64_t old = r->state;
+    r->state = old * PCG_MULT + r->inc;
+    uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((~rot + 1u) & 31));
+}
+void ho_pcg32_seed(ho_pcg32 *r, uint64_t initstate, uint64_t initseq) {
+    r->state = 0u;
+    r->inc = (initseq << 1u) | 1u;
+    ho_pcg32_next(r);
+    r->state += initstate;
+    ho_pcg32_next(r);
+}
+float ho_pcg32_nextf(ho_pcg32 *r) {
+    union { uint32_t u; float f; } x;
+    x.u = (ho_pcg32_next(r) >> 9) | 0x3f800000u;
+    return x.f - 1.0f;
+}
+static void pcg_default(ho_pcg32 *r) { r->state = 0x853c49e6748fea9bULL; r->inc = 0xda3e39cb94b95bdbULL; }
+
+/* ------------------------------------------------------------------ frame */
+typedef struct { v3 s, t, n; } frame;
+/* CoordinateSystem  src/core/Common.cpp:591 ; Frame(N)  src/core/Frame.cpp:18 */
+static frame frame_from_n(v3 n) {
+    frame f; f.n = n;
+    if (fabsf(n.x) > fabsf(n.y)) {
+        float inv = 1.0f / sqrtf(n.x * n.x + n.z * n.z);
+        f.t = V(n.z * inv, 0.0f, -n.x * inv);
+    } else {
+        float inv = 1.0f / sqrtf(n.y * n.y + n.z * n.z);
+        f.t = V(0.0f, n.z * inv, -n.y * inv);
+    }
+    f.s = cross(f.t, f.n);
+    return f;
+}
+static inline v3 to_local(const frame *f, v3 v) { return V(dot(v, f->s), dot(v, f->t), dot(v, f->n)); }
+static inline v3 to_world(const frame *f, v3 v) {
+    return add(add(scl(f->s, v.x), scl(f->t, v.y)), scl(f->n, v.z));
+}
+/* Frame::TanTheta / SinTheta2  src/core/Frame.cpp:47,57 */
+static inline float tan_theta(v3 v) {
+    float t = 1.0f - v.z * v.z;
+    if (t <= 0.0f) return 0.0f;
+    return sqrtf(t) / v.z;
+}
+static inline float sin_theta2(v3 v) { return 1.0f - v.z * v.z; }
+
+/* --------------------------------------------------------------- sampling */
+/* Sampling::SquareToUniformDisk  src/core/Sampling.cpp:29 (concentric map) */
+static void square_to_disk(float ux, float uy, float *dx, float *dy) {
+    float ox = 2.0f * ux - 1.0f, oy = 2.0f * uy - 1.0f;
+    if (ox == 0.0f && oy == 0.0f) { *dx = 0.0f; *dy = 0.0f; return; }
+    float th, r;
+    if (fabsf(ox) > fabsf(oy)) { r = ox; th = PI_F * 0.25f * (oy / ox); }
+    else { r = oy; th = PI_F * 0.5f - PI_F * 0.25f * (ox / oy); }
+    *dx = r * cosf(th);
+    *dy = r * sinf(th);
+}
+/* Sampling::SquareToCosineHemisphere  src/core/Sampling.cpp:97 */
+static v3 square_to_cos_hemi(float ux, float uy) {
+    float dx, dy;
+    square_to_disk(ux, uy, &dx, &dy);
+    float z = sqrtf(1.0f - dx * dx - dy * dy);
+    if (isnan(z)) z = 0.0f;
+    return V(dx, dy, z);
+}
+/* Sampling::SquareToCosineHemispherePdf  src/core/Sampling.cpp:110 */
+static float cos_hemi_pdf(v3 v) {
+    return (norm(v) - 1.0f <= 1e-6f && v.z >= 0.0f) ? v.z / PI_F : 0.0f;
+}
+
+/* ----------------------------------------------------------- microfacet */
+/* src/core/MicrofacetDistribution.cpp */
+typedef struct { int type; float au, av; } mfd;
+static mfd mfd_make(int type, float au, float av) {   /* :10-26 */
+    mfd d; d.type = type;
+    d.au = clampf(au, 5e-4f, 1.0f);
+    d.av = clampf(av, 5e-4f, 1.0f);
+    return d;
+}
+static inline int mfd_iso(const mfd *d) { return d->au == d->av; }
+static float mfd_eval(const mfd *d, v3 m) {   /* :34 */
+    if (m.z <= 0.0f) return 0.0f;
+    float c2 = m.z * m.z;
+    float be = ((m.x * m.x) / (d->au * d->au) + (m.y * m.y) / (d->av * d->av)) / c2;
+    float r;
+    if (d->type == HO_BECKMANN) {
+        r = expf(-be) / (PI_F * d->au * d->av * c2 * c2);
+    } else {
+        float root = (1.0f + be) * c2;
+        r = 1.0f / (PI_F * d->au * d->av * root * root);
+    }
+    if (r * m.z < 1e-20f) r = 0.0f;
+    return r;
+}
+static float mfd_project_roughness(const mfd *d, v3 v) {   /* :238 */
+    float inv = 1.0f / sin_theta2(v);
+    if (mfd_iso(d) || inv <= 0.0f) return d->au;
+    float c2 = v.x * v.x * inv, s2 = v.y * v.y * inv;
+    return sqrtf(c2 * d->au * d->au + s2 * d->av * d->av);
+}
+static float mfd_g1(const mfd *d, v3 v, v3 m) {   /* :82 */
+    if (dot(v, m) * v.z <= 0.0f) return 0.0f;
+    float tt = fabsf(tan_theta(v));
+    if (tt == 0.0f) return 1.0f;
+    float a = mfd_project_roughness(d, v);
+    if (d->type == HO_BECKMANN) {
+        float x = 1.0f / (a * tt);
+        if (x >= 1.6f) return 1.0f;
+        float x2 = x * x;
+        return (3.535f * x + 2.181f * x2) / (1.0f + 2.276f * x + 2.577f * x2);
+    }
+    float root = a * tt;
+    return 2.0f / (1.0f + hypot2(1.0f, root));
+}
+static inline float mfd_g(const mfd *d, v3 wi, v3 wo, v3 m) { return mfd_g1(d, wi, m) * mfd_g1(d, wo, m); }
+static v3 mfd_sample(const mfd *d, float ux, float uy, float *pdf) {   /* SampleAll :148 */
+    float cm = 0.0f, sp, cp, a2;
+    if (mfd_iso(d)) {
+        float ph = (2.0f * PI_F) * uy;
+        sp = sinf(ph); cp = cosf(ph);
+        a2 = d->au * d->au;
+    } else {
+        float ph = atanf(d->av / d->au * tanf(PI_F + 2.0f * PI_F * uy)) + PI_F * floorf(2.0f * uy + 0.5f);
+        sp = sinf(ph); cp = cosf(ph);
+        float cs = cp / d->au, ss = sp / d->av;
+        a2 = 1.0f / (cs * cs + ss * ss);
+    }
+    if (d->type == HO_BECKMANN) {
+        float t2 = a2 * -logf(1.0f - ux);
+        cm = 1.0f / sqrtf(1.0f + t2);
+        *pdf = (1.0f - ux) / (PI_F * d->au * d->av * cm * cm * cm);
+    } else {
+        float t2 = a2 * ux / (1.0f - ux);
+        cm = 1.0f / sqrtf(1.0f + t2);
+        float tmp = 1.0f + t2 / a2;
+        *pdf = (float)INV_PI_D / (d->au * d->av * cm * cm * cm * tmp * tmp);
+    }
+    if (*pdf < 1e-20f) *pdf = 0.0f;
+    float sm = sqrtf(fmaxf(0.0f, 1.0f - cm * cm));
+    return V(sm * cp, sm * sp, cm);
+}
+static inline float mfd_pdf(const mfd *d, v3 m) { return mfd_eval(d, m) * m.z; }   /* PdfAll :231 */
+
+/* ---------------------------------------------------------------- fresnel */
+/* FresnelDielectric  src/core/Common.cpp:494 */
+static float fresnel_dielectric(float ci, float eta, float inv_eta, float *ct) {
+    if (eta == 1.0f) { *ct = -ci; return 0.0f; }
+    float sc = (ci > 0.0f) ? inv_eta : eta;
+    float ct2 = 1.0f - (1.0f - ci * ci) * (sc * sc);
+    if (ct2 <= 0.0f) { *ct = 0.0f; return 1.0f; }
+    float cii = fabsf(ci), ctt = sqrtf(ct2);
+    float rs = (cii - eta * ctt) / (cii + eta * ctt);
+    float rp = (eta * cii - ctt) / (eta * cii + ctt);
+    *ct = (ci > 0.0f) ? -ctt : ctt;
+    return 0.5f * (rs * rs + rp * rp);
+}
+/* FresnelConductor  src/core/Common.cpp:529 (per channel) */
+static float fresnel_conductor1(float ci, float eta, float k) {
+    float ci2 = ci * ci, si2 = 1.0f - ci2;
+    float e2 = eta * eta, k2 = k * k;
+    float t0 = e2 - k2 - si2;
+    float a2b2 = sqrtf(t0 * t0 + 4.0f * e2 * k2);
+    float t1 = a2b2 + ci2;
+    float a = sqrtf(0.5f * (a2b2 + t0));
+    float t2 = 2.0f * ci * a;
+    float rs = (t1 - t2) / (t1 + t2);
+    float t3 = ci2 * a2b2 + si2 * si2;
+    float t4 = t2 * si2;
+    float rp = rs * ((t3 - t4) / (t3 + t4));
+    return 0.5f * (rp + rs);
+}
+static v3 fresnel_conductor(float ci, const float *eta, const float *k) {
+    return V(fresnel_conductor1(ci, eta[0], k[0]), fresnel_conductor1(ci, eta[1], k[1]),
+             fresnel_conductor1(ci, eta[2], k[2]));
+}
+/* Reflect / Refract in global coordinates  src/core/Common.cpp:616-626 */
+static inline v3 reflect_m(v3 wi, v3 m) { return sub(scl(m, 2.0f * dot(wi, m)), wi); }
+static inline v3 refract_m(v3 wi, v3 m, float ct, float eta, float inv_eta) {
+    float e = (ct < 0.0f ? inv_eta : eta);
+    return sub(scl(m, dot(wi, m) * e + ct), scl(wi, e));
+}
+
+/* ------------------------------------------------------- cubic / RFT */
+/* EvalCubicInterpolate1D  src/core/Common.cpp:230 */
+static float cubic1d(float x, const float *val, int size, float mn, float mx) {
+    if (!(x >= mn && x <= mx)) return 0.0f;
+    float t = ((x - mn) * (size - 1)) / (mx - mn);
+    int k = (int)t; if (k > size - 2) k = size - 2; if (k < 0) k = 0;
+    float f0 = val[k], f1 = val[k + 1], d0, d1;
+    d0 = (k > 0) ? 0.5f * (val[k + 1] - val[k - 1]) : val[k + 1] - val[k];
+    d1 = (k + 2 < size) ? 0.5f * (val[k + 2] - val[k]) : val[k + 1] - val[k];
+    t = t - (float)k;
+    float t2 = t * t, t3 = t2 * t;
+    return (2.0f * t3 - 3.0f * t2 + 1) * f0 + (-2.0f * t3 + 3.0f * t2) * f1 + (t3 - 2.0f * t2 + t) * d0 +
+           (t3 - t2) * d1;
+}
+/* knot weights shared by EvalCubicInterpolate2D/3D  src/core/Common.cpp:299-336 */
+static int cubic_weights(float p, int size, float *w, int *knot) {
+    if (!(p >= 0.0f && p <= 1.0f)) return 0;
+    float t = ((p - 0.0f) * (float)(size - 1)) / (1.0f - 0.0f);
+    int k = (int)t; if (k > size - 2) k = size - 2;
+    *knot = k;
+    t = t - (float)k;
+    float t2 = t * t, t3 = t2 * t;
+    w[0] = 0.0f; w[1] = 2.0f * t3 - 3.0f * t2 + 1; w[2] = -2.0f * t3 + 3.0f * t2; w[3] = 0.0f;
+    float d0 = t3 - 2.0f * t2 + t, d1 = t3 - t2;
+    if (k > 0) { w[2] += 0.5f * d0; w[0] -= 0.5f * d0; }
+    else { w[2] += d0; w[1] -= d0; }
+    if (k + 2 < size) { w[3] += 0.5f * d1; w[1] -= 0.5f * d1; }
+    else { w[2] += d1; w[1] -= d1; }
+    return 1;
+}
+/* EvalCubicInterpolate2D on [0,1]^2  src/core/Common.cpp:285 */
+static float cubic2d(float px, float py, const float *val, int sx, int sy) {
+    float w[2][4]; int kn[2];
+    if (!cubic_weights(px, sx, w[0], &kn[0])) return 0.0f;
+    if (!cubic_weights(py, sy, w[1], &kn[1])) return 0.0f;
+    float r = 0.0f;
+    for (int y = -1; y <= 2; y++) {
+        float wy = w[1][y + 1];
+        for (int x = -1; x <= 2; x++) {
+            float wxy = w[0][x + 1] * wy;
+            if (wxy == 0) continue;
+            r += val[(kn[1] + y) * sx + kn[0] + x] * wxy;
+        }
+    }
+    return r;
+}
+/* EvalCubicInterpolate3D on [0,1]^3  src/core/Common.cpp:373 */
+static float cubic3d(float px, float py, float pz, const float *val, int sx, int sy, int sz) {
+    float w[3][4]; int kn[3];
+    if (!cubic_weights(px, sx, w[0], &kn[0])) return 0.0f;
+    if (!cubic_weights(py, sy, w[1], &kn[1])) return 0.0f;
+    if (!cubic_weights(pz, sz, w[2], &kn[2])) return 0.0f;
+    float r = 0.0f;
+    for (int z = -1; z <= 2; z++) {
+        float wz = w[2][z + 1];
+        for (int y = -1; y <= 2; y++) {
+            float wyz = w[1][y + 1] * wz;
+            for (int x = -1; x <= 2; x++) {
+                float wxyz = w[0][x + 1] * wyz;
+                if (wxyz == 0) continue;
+                r += val[((kn[2] + z) * sy + (kn[1] + y)) * sx + kn[0] + x] * wxyz;
+            }
+        }
+    }
+    return r;
+}
+
+typedef struct {
+    uint64_t eta_n, alpha_n, theta_n, t_size, d_size;
+    float eta_min, eta_max, alpha_min, alpha_max;
+    const float *trans;   /* eta_n*alpha_n*theta_n*2 */
+    const float *diff;    /* eta_n*alpha_n*2 */
+    float *owned;
+} rft_table;
+
+/* RoughTransmittance ctor  src/core/RoughTransmitance.cpp:9 (file layout) */
+static int rft_parse(rft_table *t, const void *bytes, uint64_t n) {
+    const unsigned char *b = (const unsigned char *)bytes;
+    if (n < 56) return fail("rft: short header");
+    uint64_t h[5]; float f[4];
+    memcpy(h, b, 40); memcpy(f, b + 40, 16);
+    t->eta_n = h[0]; t->alpha_n = h[1]; t->theta_n = h[2]; t->t_size = h[3]; t->d_size = h[4];
+    t->eta_min = f[0]; t->eta_max = f[1]; t->alpha_min = f[2]; t->alpha_max = f[3];
+    if (56 + 4 * (t->t_size + t->d_size) > n) return fail("rft: short body");
+    t->owned = (float *)malloc(4 * (t->t_size + t->d_size));
+    memcpy(t->owned, b + 56, 4 * (t->t_size + t->d_size));
+    t->trans = t->owned; t->diff = t->owned + t->t_size;
+    return 0;
+}
+/* SetEta  src/core/RoughTransmitance.cpp:170 -> 2D [alpha][theta] + diffuse[alpha] */
+static void rft_set_eta(const rft_table *t, float eta, float *t2d, float *d1d) {
+    const float *pt = t->trans, *pd = t->diff;
+    int E = (int)t->eta_n, A = (int)t->alpha_n, T = (int)t->theta_n;
+    if (eta < 1.0f) { pt += (uint64_t)E * A * T; pd += (uint64_t)E * A; eta = 1.0f / eta; }
+    if (eta < t->eta_min) eta = t->eta_min;
+    float we = powf((eta - t->eta_min) / (t->eta_max - t->eta_min), 0.25f);
+    float da = 1.0f / (A - 1.0f), dt = 1.0f / (T - 1.0f);
+    for (int i = 0; i < A; i++) {
+        for (int j = 0; j < T; j++)
+            t2d[i * T + j] = cubic3d(j * dt, i * da, we, pt, T, A, E);
+        d1d[i] = cubic2d(i * da, we, pd, A, E);
+    }
+}
+/* SetAlpha  src/core/RoughTransmitance.cpp:237 -> 1D [theta] + diffuse scalar */
+static void rft_set_alpha(const rft_table *t, const float *t2d, const float *d1d, float alpha,
+                          float *t1d, float *dscalar) {
+    int A = (int)t->alpha_n, T = (int)t->theta_n;
+    float wa = powf((alpha - t->alpha_min) / (t->alpha_max - t->alpha_min), 0.25f);
+    float dt = 1.0f / (T - 1.0f);
+    for (int i = 0; i < T; i++) t1d[i] = cubic2d(i * dt, wa, t2d, T, A);
+    *dscalar = cubic1d(wa, d1d, A, 0.0f, 1.0f);
+}
+/* Eval with eta and alpha fixed  src/core/RoughTransmitance.cpp:48-70 */
+static float rft_eval1d(const float *t1d, int T, float c) {
+    float wc = powf(fabsf(c), 0.25f);
+    if (c < 0.0f) return 0.0f;
+    return clampf(cubic1d(wc, t1d, T, 0.0f, 1.0f), 0.0f, 1.0f);
+}
+
+/* ------------------------------------------------------------------ BSDF */
+#define RFT_MAX_THETA 128
+typedef struct {
+    ho_bsdf_desc d;
+    float eta, inv_eta, inv_eta2;      /* dielectric-type relative IOR */
+    float eta_c[3], k_c[3];            /* conductor eta and k/extIOR */
+    float spec_w;                      /* m_SpecularSamplingWeight */
+    float rft[RFT_MAX_THETA];          /* activated 1D transmittance table */
+    int rft_n;
+    float fdr_int;                     /* plastic: 1 - IntData.EvalDiffuse(alpha) */
+} bsdf_t;
+
+typedef struct { v3 wi, wo; float eta; int measure; } brec;
+
+struct ho_scene;
+static v3 bsdf_eval(const struct ho_scene *s, int id, const brec *r);
+static float bsdf_pdf(const struct ho_scene *s, int id, const brec *r);
+static v3 bsdf_sample(const struct ho_scene *s, int id, brec *r, float ux, float uy, ho_pcg32 *rng,
+                      const float *u1fixed);
+
+/* ------------------------------------------------------------------ scene */
+typedef struct {
+    uint32_t v0, nv, t0, nt;
+    int32_t bsdf, emitter;
+    int has_n;
+    float *cdf;        /* nt+1 area CDF (DiscretePDF1D) */
+    float *func;       /* nt areas */
+    float func_int;    /* m_FuncIntegral */
+    float inv_area;    /* Mesh::m_InvMeshArea */
+    v3 radiance;
+} mesh_t;
+
+typedef struct { int n; float *func; float *cdf; float integral; } pdf1d;
+
+typedef struct { float bmin[3], bmax[3]; int32_t left_or_first, count, axis, right; } bnode;
+
+struct ho_scene {
+    int nb, cap_b; bsdf_t *bsdfs;
+    int nm, cap_m; mesh_t *meshes;
+    float *P; float *N; uint32_t nv, cap_v;          /* global vertices (world space) */
+    uint32_t *F; int32_t *tri_mesh; uint32_t nt, cap_t;
+    rft_table rft[2]; int has_rft[2];
+    /* emitters in Scene::AddChild order: meshes (XML order), env appended */
+    int n_emit; int32_t emit_mesh[64]; int env_index;
+    /* env */
+    int has_env; uint32_t ew, eh; float *env; float env_scale; float to_world[9], to_local[9];
+    pdf1d *env_rows; pdf1d env_marg;
+    /* camera */
+    uint32_t W, H; float cam[16]; float fov, near_c, far_c;
+    float cot, aspect;
+    /* filter */
+    int filt_kind; float filt_r, filt_p0, filt_p1; float ftab[33]; float lookup; int border;
+    v3 background; int force_bg;
+    /* bvh */
+    bnode *nodes; int nnodes; uint32_t *order;
+    float bbox[6];
+    int finalized;
+};
+
+ho_scene *ho_scene_create(void) {
+    ho_scene *s = (ho_scene *)calloc(1, sizeof(ho_scene));
+    s->filt_kind = 2; s->filt_r = 2.0f; s->filt_p0 = 0.5f;    /* DEFAULT_CAMERA_RFILTER gaussian */
+    s->env_index = -1;
+    return s;
+}
+void ho_scene_destroy(ho_scene *s) {
+    if (!s) return;
+    for (int i = 0; i < s->nm; i++) { free(s->meshes[i].cdf); free(s->meshes[i].func); }
+    free(s->meshes); free(s->bsdfs); free(s->P); free(s->N); free(s->F); free(s->tri_mesh);
+    for (int i = 0; i < 2; i++) free(s->rft[i].owned);
+    free(s->env);
+    if (s->env_rows) { for (uint32_t i = 0; i < s->eh; i++) { free(s->env_rows[i].func); free(s->env_rows[i].cdf); } }
+    free(s->env_rows); free(s->env_marg.func); free(s->env_marg.cdf);
+    free(s->nodes); free(s->order);
+    free(s);
+}
+int ho_scene_set_rft(ho_scene *s, int dist, const void *bytes, uint64_t n) {
+    if (dist < 0 || dist > 1) return fail("bad distribution");
+    if (rft_parse(&s->rft[dist], bytes, n)) return -1;
+    if (s->rft[dist].theta_n > RFT_MAX_THETA) return fail("rft theta too large");
+    s->has_rft[dist] = 1;
+    return 0;
+}
+int ho_scene_add_bsdf(ho_scene *s, const ho_bsdf_desc *d) {
+    if (s->nb == s->cap_b) { s->cap_b = s->cap_b ? 2 * s->cap_b : 8; s->bsdfs = realloc(s->bsdfs, s->cap_b * sizeof(bsdf_t)); }
+    bsdf_t *b = &s->bsdfs[s->nb]; memset(b, 0, sizeof *b);
+    b->d = *d;
+    return s->nb++;
+}
+int ho_scene_add_mesh(ho_scene *s, const float *pos, uint32_t nv, const uint32_t *idx, uint32_t nt,
+                      const float *nrm, int32_t bsdf, const float *rad) {
+    if (s->nm == s->cap_m) { s->cap_m = s->cap_m ? 2 * s->cap_m : 8; s->meshes = realloc(s->meshes, s->cap_m * sizeof(mesh_t)); }
+    if (s->nv + nv > s->cap_v) {
+        while (s->nv + nv > s->cap_v) s->cap_v = s->cap_v ? 2 * s->cap_v : 1024;
+        s->P = realloc(s->P, 3ull * s->cap_v * 4); s->N = realloc(s->N, 3ull * s->cap_v * 4);
+    }
+    if (s->nt + nt > s->cap_t) {
+        while (s->nt + nt > s->cap_t) s->cap_t = s->cap_t ? 2 * s->cap_t : 1024;
+        s->F = realloc(s->F, 3ull * s->cap_t * 4); s->tri_mesh = realloc(s->tri_mesh, 4ull * s->cap_t);
+    }
+    mesh_t *m = &s->meshes[s->nm]; memset(m, 0, sizeof *m);
+    m->v0 = s->nv; m->nv = nv; m->t0 = s->nt; m->nt = nt; m->bsdf = bsdf; m->emitter = -1;
+    m->has_n = nrm != NULL;
+    memcpy(s->P + 3ull * s->nv, pos, 12ull * nv);
+    if (nrm) memcpy(s->N + 3ull * s->nv, nrm, 12ull * nv);
+    for (uint64_t i = 0; i < 3ull * nt; i++) {
+        if (idx[i] >= nv) return fail("mesh index out of range");
+        s->F[3ull * s->nt + i] = idx[i] + s->nv;
+    }
+    for (uint32_t i = 0; i < nt; i++) s->tri_mesh[s->nt + i] = s->nm;
+    if (rad) {
+        if (s->n_emit >= 64) return fail("too many emitters");
+        m->radiance = vload(rad);
+        m->emitter = s->n_emit;
+        s->emit_mesh[s->n_emit++] = s->nm;
+    }
+    s->nv += nv; s->nt += nt;
+    return s->nm++;
+}
+static void mat3_inverse(const float *m, float *o) {
+    double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5], g = m[6], h = m[7], i = m[8];
+    double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+    o[0] = (float)((e * i - f * h) / det); o[1] = (float)((c * h - b * i) / det); o[2] = (float)((b * f - c * e) / det);
+    o[3] = (float)((f * g - d * i) / det); o[4] = (float)((a * i - c * g) / det); o[5] = (float)((c * d - a * f) / det);
+    o[6] = (float)((d * h - e * g) / det); o[7] = (float)((b * g - a * h) / det); o[8] = (float)((a * e - b * d) / det);
+}
+static inline v3 mat3_mul(const float *m, v3 v) {
+    return V(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
+             m[6] * v.x + m[7] * v.y + m[8] * v.z);
+}
+/* DiscretePDF1D ctor  src/core/DiscretePDF.cpp:5 */
+static void pdf1d_build(pdf1d *p, const float *f, int n) {
+    p->n = n; p->func = malloc(4ull * n); p->cdf = malloc(4ull * (n + 1));
+    memcpy(p->func, f, 4ull * n);
+    p->cdf[0] = 0.0f;
+    for (int i = 1; i < n + 1; i++) p->cdf[i] = p->cdf[i - 1] + p->func[i - 1] / n;
+    p->integral = p->cdf[n];
+    if (p->integral == 0.0f) for (int i = 1; i < n + 1; i++) p->cdf[i] = (float)i / (float)n;
+    else for (int i = 1; i < n + 1; i++) p->cdf[i] /= p->integral;
+}
+/* std::lower_bound then clamp to [0, n-1]  src/core/DiscretePDF.cpp:41-46 */
+static int cdf_find(const float *cdf, int n, float u) {
+    int lo = 0, hi = n + 1;            /* first index with cdf[i] >= u */
+    while (lo < hi) { int mid = (lo + hi) >> 1; if (cdf[mid] < u) lo = mid + 1; else hi = mid; }
+    int idx = lo - 1; if (idx < 0) idx = 0; if (idx > n - 1) idx = n - 1;
+    return idx;
+}
+/* DiscretePDF1D::SampleContinuous  src/core/DiscretePDF.cpp:39 */
+static float pdf1d_sample_cont(const pdf1d *p, float u, float *pdf, int *pidx) {
+    int idx = cdf_find(p->cdf, p->n, u);
+    *pidx = idx;
+    float du = u - p->cdf[idx];
+    if (p->cdf[idx + 1] - p->cdf[idx] > 0.0f) du /= (p->cdf[idx + 1] - p->cdf[idx]);
+    *pdf = p->func[idx] / p->integral;
+    return ((float)idx + du) / (float)p->n;
+}
+int ho_scene_set_envmap(ho_scene *s, const float *rgb, uint32_t w, uint32_t h, const float *tw16, float scale) {
+    if (s->has_env) return fail("only one environment emitter");   /* Scene.cpp:198 */
+    s->has_env = 1; s->ew = w; s->eh = h; s->env_scale = scale;
+    s->env = malloc(12ull * w * h); memcpy(s->env, rgb, 12ull * w * h);
+    for (int r = 0; r < 3; r++) for (int c = 0; c < 3; c++) s->to_world[3 * r + c] = tw16[4 * r + c];
+    mat3_inverse(s->to_world, s->to_local);
+    /* EnvironmentLight ctor  src/emitter/EnvironmentLight.cpp:8-31 */
+    float *L = malloc(4ull * w * h);
+    for (uint32_t y = 0; y < h; y++) {
+        float th = (float)(y + 0.5f) / h * PI_F;
+        float st = sinf(th);
+        for (uint32_t x = 0; x < w; x++) L[(uint64_t)y * w + x] = lum(vload(rgb + 3ull * ((uint64_t)y * w + x))) * st;
+    }
+    s->env_rows = calloc(h, sizeof(pdf1d));
+    float *marg = malloc(4ull * h);
+    for (uint32_t y = 0; y < h; y++) { pdf1d_build(&s->env_rows[y], L + (uint64_t)y * w, (int)w); marg[y] = s->env_rows[y].integral; }
+    pdf1d_build(&s->env_marg, marg, (int)h);
+    free(marg); free(L);
+    if (s->n_emit >= 64) return fail("too many emitters");
+    s->env_index = s->n_emit;
+    s->emit_mesh[s->n_emit++] = -1;
+    return 0;
+}
+int ho_scene_set_camera(ho_scene *s, uint32_t w, uint32_t h, const float *tw16, float fov, float n, float f) {
+    s->W = w; s->H = h; memcpy(s->cam, tw16, 64); s->fov = fov; s->near_c = n; s->far_c = f;
+    return 0;
+}
+int ho_scene_set_filter(ho_scene *s, int kind, float r, float p0, float p1) {
+    s->filt_kind = kind; s->filt_r = r; s->filt_p0 = p0; s->filt_p1 = p1; return 0;
+}
+int ho_scene_set_background(ho_scene *s, const float *rgb, int force) { s->background = vload(rgb); s->force_bg = force; return 0; }
+
+/* filters  src/filter/{Box,Tent,Gaussian,MitchellNetraval}Filter.cpp */
+static float filter_eval(const ho_scene *s, float x) {
+    switch (s->filt_kind) {
+    case 0: return 1.0f;
+    case 1: return fmaxf(0.0f, 1.0f - fabsf(x));
+    case 2: {
+        float a = -1.0f / (2.0f * s->filt_p0 * s->filt_p0);
+        return fmaxf(0.0f, expf(a * x * x) - expf(a * s->filt_r * s->filt_r));
+    }
+    default: {
+        float B = s->filt_p0, C = s->filt_p1;
+        x = fabsf(2.0f * x / s->filt_r);
+        float x2 = x * x, x3 = x2 * x;
+        if (x < 1.0f) return 1.0f / 6.0f * ((12.0f - 9.0f * B - 6.0f * C) * x3 + (-18.0f + 12.0f * B + 6.0f * C) * x2 + (6.0f - 2.0f * B));
+        if (x < 2.0f) return 1.0f / 6.0f * ((-B - 6 * C) * x3 + (6.0f * B + 30.0f * C) * x2 + (-12.0f * B - 48.0f * C) * x + (8.0f * B + 24.0f * C));
+        return 0.0f;
+    }
+    }
+}
+
+static int bvh_build(ho_scene *s);
+
+/* BSDF activation: RoughPlasticBSDF::Activate :261, RoughCoatingBSDF::Activate :315 */
+static int activate_bsdf(ho_scene *s, bsdf_t *b) {
+    const ho_bsdf_desc *d = &b->d;
+    b->eta = d->int_ior / d->ext_ior;
+    b->inv_eta = 1.0f / b->eta;
+    b->inv_eta2 = b->inv_eta * b->inv_eta;
+    for (int c = 0; c < 3; c++) { b->eta_c[c] = d->eta[c]; b->k_c[c] = d->k[c] / d->ext_ior; }
+    if (d->type == HO_BSDF_ROUGH_PLASTIC || d->type == HO_BSDF_ROUGH_COATING) {
+        int dist = d->distribution;
+        if (!s->has_rft[dist]) return fail("missing RFT table");
+        const rft_table *t = &s->rft[dist];
+        float alpha = clampf(d->alpha_u, 5e-4f, 1.0f);
+        float e = b->eta < 1.0f ? 1.0f / b->eta : b->eta;        /* CheckEta :315 */
+        if (e < t->eta_min || e > t->eta_max) return fail("eta outside RFT range");
+        if (alpha < t->alpha_min || alpha > t->alpha_max) return fail("alpha outside RFT range");
+        int A = (int)t->alpha_n, T = (int)t->theta_n;
+        float *t2d = malloc(4ull * A * T), *d1d = malloc(4ull * A);
+        float dsc;
+        rft_set_eta(t, b->eta, t2d, d1d);
+        rft_set_alpha(t, t2d, d1d, alpha, b->rft, &dsc);
+        b->rft_n = T;
+        if (d->type == HO_BSDF_ROUGH_PLASTIC) {
+            float ksa = lum(vload(d->ks)), kda = lum(vload(d->kd));
+            b->spec_w = ksa / (kda + ksa);
+            /* m_pIntData: SetEta(1/eta) only; EvalDiffuse(alpha) is the 1D cubic over alpha */
+            rft_set_eta(t, b->inv_eta, t2d, d1d);
+            float wa = powf((alpha - t->alpha_min) / (t->alpha_max - t->alpha_min), 0.25f);
+            float ed = clampf(cubic1d(wa, d1d, A, 0.0f, 1.0f), 0.0f, 1.0f);
+            b->fdr_int = 1.0f - ed;
+        } else {
+            float th = d->thickness;
+            float a0 = expf(d->sigma_a[0] * (-2.0f * th)), a1 = expf(d->sigma_a[1] * (-2.0f * th)),
+                  a2 = expf(d->sigma_a[2] * (-2.0f * th));
+            float avg = (a0 + a1 + a2) / 3.0f;
+            b->spec_w = 1.0f / (avg + 1.0f);
+            if (d->nested < 0 || d->nested >= s->nb) return fail("roughCoating needs a nested BSDF");
+        }
+        free(t2d); free(d1d);
+    }
+    return 0;
+}
+
+int ho_scene_finalize(ho_scene *s) {
+    for (int i = 0; i < s->nb; i++) if (activate_bsdf(s, &s->bsdfs[i])) return -1;
+    /* Mesh::Activate  src/core/Mesh.cpp:233 (area CDF) */
+    for (int i = 0; i < s->nm; i++) {
+        mesh_t *m = &s->meshes[i];
+        float *areas = malloc(4ull * (m->nt ? m->nt : 1));
+        float total = 0.0f;
+        for (uint32_t t = 0; t < m->nt; t++) {
+            const uint32_t *f = s->F + 3ull * (m->t0 + t);
+            v3 p0 = vload(s->P + 3ull * f[0]), p1 = vload(s->P + 3ull * f[1]), p2 = vload(s->P + 3ull * f[2]);
+            float a = 0.5f * norm(cross(sub(p1, p0), sub(p2, p0)));
+            areas[t] = a; total += a;
+        }
+        m->inv_area = 1.0f / total;
+        pdf1d p; pdf1d_build(&p, areas, (int)m->nt);
+        m->cdf = p.cdf; m->func = p.func; m->func_int = p.integral;
+        free(areas);
+    }
+    /* camera  src/camera/PerspectiveCamera.cpp:32 */
+    s->aspect = (float)s->W / (float)s->H;
+    s->cot = 1.0f / tanf((s->fov / 2.0f) * (PI_F / 180.0f));
+    /* ImageBlock ctor  src/core/Block.cpp:9 */
+    s->border = (int)ceilf(s->filt_r - 0.5f);
+    for (int i = 0; i < 32; i++) s->ftab[i] = filter_eval(s, (s->filt_r * i) / 32);
+    s->ftab[32] = 0.0f;
+    s->lookup = 32 / s->filt_r;
+    if (bvh_build(s)) return -1;
+    s->finalized = 1;
+    return 0;
+}
+void ho_scene_bbox(const ho_scene *s, float *o) { memcpy(o, s->bbox, 24); }
+int ho_scene_num_emitters(const ho_scene *s) { return s->n_emit; }
+int ho_film_border(const ho_scene *s) { return s->border; }
+
+/* ------------------------------------------------------------ BSDF impl */
+static inline float alpha_u_of(const bsdf_t *b) { return clampf(b->d.alpha_u, 5e-4f, 1.0f); }
+static inline float alpha_v_of(const bsdf_t *b) {
+    return b->d.anisotropic ? clampf(b->d.alpha_v, 5e-4f, 1.0f) : alpha_u_of(b);
+}
+
+/* DiffuseBSDF  src/bsdf/DiffuseBSDF.cpp:20-67 */
+static v3 diffuse_sample(const bsdf_t *b, brec *r, float ux, float uy) {
+    if (r->wi.z <= 0) return V(0, 0, 0);
+    r->measure = HO_MEASURE_SOLID_ANGLE;
+    r->wo = square_to_cos_hemi(ux, uy);
+    r->eta = 1.0f;
+    return vload(b->d.kd);
+}
+static v3 diffuse_eval(const bsdf_t *b, const brec *r) {
+    if (r->measure != HO_MEASURE_SOLID_ANGLE || r->wi.z <= 0 || r->wo.z <= 0) return V(0, 0, 0);
+    return scl(vload(b->d.kd), (float)INV_PI_D);
+}
+static float diffuse_pdf(const brec *r) {
+    if (r->measure != HO_MEASURE_SOLID_ANGLE || r->wi.z <= 0 || r->wo.z <= 0) return 0.0f;
+    return (float)INV_PI_D * r->wo.z;
+}
+
+/* RoughConductorBSDF  src/bsdf/RoughConductorBSDF.cpp:54-154 */
+static v3 conductor_sample(const bsdf_t *b, brec *r, float ux, float uy) {
+    r->measure = HO_MEASURE_SOLID_ANGLE;
+    float ci = r->wi.z;
+    if (ci <= 0.0f) return V(0, 0, 0);
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    float pdf;
+    v3 m = mfd_sample(&d, ux, uy, &pdf);
+    if (pdf == 0.0f) return V(0, 0, 0);
+    r->wo = reflect_m(r->wi, m);
+    r->eta = 1.0f;
+    if (r->wo.z < 0.0f) return V(0, 0, 0);
+    float mdw = dot(m, r->wi);
+    v3 F = fresnel_conductor(mdw, b->eta_c, b->k_c);
+    float G = mfd_g(&d, r->wi, r->wo, m);
+    float D = mfd_eval(&d, m);
+    v3 ks = vload(b->d.ks);
+    float den = pdf * r->wi.z;
+    return V((((ks.x * F.x) * D) * G) * mdw / den, (((ks.y * F.y) * D) * G) * mdw / den,
+             (((ks.z * F.z) * D) * G) * mdw / den);
+}
+static v3 conductor_eval(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (r->measure != HO_MEASURE_SOLID_ANGLE || ci <= 0.0f || co <= 0.0f) return V(0, 0, 0);
+    v3 h = normalize(add(r->wi, r->wo));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    float D = mfd_eval(&d, h);
+    if (D == 0.0f) return V(0, 0, 0);
+    v3 F = mul(fresnel_conductor(dot(h, r->wi), b->eta_c, b->k_c), vload(b->d.ks));
+    float G = mfd_g(&d, r->wi, r->wo, h);
+    float dg = D * G, den = 4.0f * ci;
+    return V(dg * F.x / den, dg * F.y / den, dg * F.z / den);
+}
+static float conductor_pdf(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (r->measure != HO_MEASURE_SOLID_ANGLE || ci <= 0.0f || co <= 0.0f) return 0.0f;
+    v3 h = normalize(add(r->wi, r->wo));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    return mfd_pdf(&d, h) / (4.0f * fabsf(dot(h, r->wo)));
+}
+
+/* RoughDielectricBSDF  src/bsdf/RoughDielectricBSDF.cpp:57-281 */
+static v3 dielectric_sample(const bsdf_t *b, brec *r, float ux, float uy, ho_pcg32 *rng, const float *u1f) {
+    r->measure = HO_MEASURE_SOLID_ANGLE;
+    float ci = r->wi.z;
+    if (ci == 0.0f) return V(0, 0, 0);
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    mfd sd = d;
+    float s = 1.2f - 0.2f * sqrtf(fabsf(ci));
+    sd.au *= s; sd.av *= s;                                    /* ScaleAlpha */
+    float pdf;
+    v3 m = mfd_sample(&sd, ux, uy, &pdf);
+    if (pdf == 0.0f) return V(0, 0, 0);
+    float ct;
+    float F = fresnel_dielectric(dot(r->wi, m), b->eta, b->inv_eta, &ct);
+    float u1;
+    if (u1f) u1 = *u1f;
+    else if (rng) u1 = ho_pcg32_nextf(rng);
+    else { ho_pcg32 t; pcg_default(&t); u1 = ho_pcg32_nextf(&t); }   /* :96-100 null sampler */
+    int refl = !(u1 > F);
+    v3 W = V(1, 1, 1);
+    if (refl) {
+        r->wo = reflect_m(r->wi, m);
+        r->eta = 1.0f;
+        float co = r->wo.z;
+        if (co * ci <= 0.0f) return V(0, 0, 0);
+        W = mul(W, vload(b->d.ks));
+    } else {
+        if (ct == 0.0f) return V(0, 0, 0);
+        r->wo = refract_m(r->wi, m, ct, b->eta, b->inv_eta);
+        r->eta = (ct < 0.0f ? b->eta : b->inv_eta);
+        float co = r->wo.z;
+        if (co * ci >= 0.0f) return V(0, 0, 0);
+        float fac = (ct < 0.0f ? b->inv_eta : b->eta);
+        W = mul(W, scl(vload(b->d.ks_refract), fac * fac));
+    }
+    float v = fabsf(mfd_eval(&d, m) * mfd_g(&d, r->wi, r->wo, m) * dot(r->wi, m) / (pdf * ci));
+    return scl(W, v);
+}
+static v3 dielectric_eval(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (r->measure != HO_MEASURE_SOLID_ANGLE || ci == 0.0f) return V(0, 0, 0);
+    int refl = ci * co > 0.0f;
+    v3 h;
+    if (refl) h = normalize(add(r->wi, r->wo));
+    else { float e = ci > 0.0f ? b->eta : b->inv_eta; h = normalize(add(r->wi, scl(r->wo, e))); }
+    h = scl(h, signum(h.z));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    float D = mfd_eval(&d, h);
+    if (D == 0.0f) return V(0, 0, 0);
+    float ct;
+    float F = fresnel_dielectric(dot(r->wi, h), b->eta, b->inv_eta, &ct);
+    float G = mfd_g(&d, r->wi, r->wo, h);
+    if (refl) return scl(vload(b->d.ks), F * D * G / (4.0f * fabsf(ci)));
+    float e = ci > 0.0f ? b->eta : b->inv_eta;
+    float sd = dot(r->wi, h) + e * dot(r->wo, h);
+    float val = ((1.0f - F) * D * G * e * e * dot(r->wi, h) * dot(r->wo, h)) / (ci * sd * sd);
+    float fac = (ci < 0.0f ? b->inv_eta : b->eta);
+    return scl(vload(b->d.ks_refract), fabsf(val * fac * fac));
+}
+static float dielectric_pdf(const bsdf_t *b, const brec *r) {
+    if (r->measure != HO_MEASURE_SOLID_ANGLE) return 0.0f;
+    float ci = r->wi.z, co = r->wo.z;
+    if (ci == 0.0f || co == 0.0f) return 0.0f;
+    int refl = ci * co > 0.0f;
+    v3 h; float J;
+    if (refl) { h = normalize(add(r->wi, r->wo)); J = 1.0f / (4.0f * dot(r->wo, h)); }
+    else {
+        float e = ci > 0.0f ? b->eta : b->inv_eta;
+        h = normalize(add(r->wi, scl(r->wo, e)));
+        float sd = dot(r->wi, h) + e * dot(r->wo, h);
+        J = (e * e * dot(r->wo, h)) / (sd * sd);
+    }
+    h = scl(h, signum(h.z));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    float s = 1.2f - 0.2f * sqrtf(fabsf(ci));
+    d.au *= s; d.av *= s;
+    float ct;
+    float F = fresnel_dielectric(dot(r->wi, h), b->eta, b->inv_eta, &ct);
+    float pdf = mfd_pdf(&d, h) * (refl ? F : (1.0f - F));
+    return fabsf(pdf * J);
+}
+
+/* RoughPlasticBSDF  src/bsdf/RoughPlasticBSDF.cpp:66-192 */
+static v3 plastic_eval(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (r->measure == HO_MEASURE_UNKNOWN || ci <= 0.0f || co <= 0.0f) return V(0, 0, 0);
+    float a = alpha_u_of(b);
+    mfd d = mfd_make(b->d.distribution, a, a);
+    float ct;
+    v3 h = normalize(add(r->wi, r->wo));
+    float D = mfd_eval(&d, h);
+    float F = fresnel_dielectric(dot(r->wi, h), b->eta, b->inv_eta, &ct);
+    float G = mfd_g(&d, r->wi, r->wi, h);                     /* G(Wi, Wi, H) as in :146 */
+    float val = F * D * G / (4.0f * ci);
+    v3 res = scl(vload(b->d.ks), val);
+    v3 dif = vload(b->d.kd);
+    float t12 = rft_eval1d(b->rft, b->rft_n, ci);
+    float t21 = rft_eval1d(b->rft, b->rft_n, co);
+    float fdr = b->fdr_int;
+    if (b->d.nonlinear) dif = V(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
+    else dif = divs(dif, 1.0f - fdr);
+    float k = (float)(INV_PI_D * co * t12 * t21 * b->inv_eta2);
+    return add(res, scl(dif, k));
+}
+static float plastic_spec_pdf(const bsdf_t *b, float ci) {
+    float sp = 1.0f - rft_eval1d(b->rft, b->rft_n, ci);
+    return (sp * b->spec_w) / (sp * b->spec_w + (1.0f - sp) * (1.0f - b->spec_w));
+}
+static float plastic_pdf(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (r->measure == HO_MEASURE_UNKNOWN || ci <= 0.0f || co <= 0.0f) return 0.0f;
+    float a = alpha_u_of(b);
+    mfd d = mfd_make(b->d.distribution, a, a);
+    v3 h = normalize(add(r->wi, r->wo));
+    float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
+    float J = 1.0f / (4.0f * dot(r->wo, h));
+    float res = mfd_pdf(&d, h) * J * sp;
+    res += dp * cos_hemi_pdf(r->wo);
+    return res;
+}
+static v3 plastic_sample(const bsdf_t *b, brec *r, float ux, float uy) {
+    float ci = r->wi.z;
+    if (ci <= 0.0f) return V(0, 0, 0);
+    float a = alpha_u_of(b);
+    mfd d = mfd_make(b->d.distribution, a, a);
+    float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
+    int spec;
+    if (uy < sp) { uy /= sp; spec = 1; }
+    else { uy = (uy - sp) / (1.0f - sp); spec = 0; }
+    if (spec) {
+        float pdf;
+        v3 m = mfd_sample(&d, ux, uy, &pdf);
+        r->wo = reflect_m(r->wi, m);
+        r->measure = HO_MEASURE_DISCRETE;
+    } else {
+        r->wo = square_to_cos_hemi(ux, uy);
+        r->measure = HO_MEASURE_SOLID_ANGLE;
+    }
+    r->eta = 1.0f;
+    v3 h = normalize(add(r->wi, r->wo));
+    float J = 1.0f / (4.0f * dot(r->wo, h));
+    float P = mfd_pdf(&d, h) * J * sp + dp * cos_hemi_pdf(r->wo);
+    if (P == 0.0f) return V(0, 0, 0);
+    return divs(plastic_eval(b, r), P);
+}
+
+/* RoughCoatingBSDF  src/bsdf/RoughCoatingBSDF.cpp:62-385 */
+static v3 coat_refract(v3 wi, float inv_eta) {   /* RefractIn :347 (RefractOut :367 with eta) */
+    float ci = wi.z;
+    int entering = ci > 0.0f;
+    float st2 = inv_eta * inv_eta * sin_theta2(wi);
+    if (st2 >= 1.0f) return V(0, 0, 0);
+    float ct = sqrtf(1.0f - st2);
+    return V(inv_eta * wi.x, inv_eta * wi.y, entering ? ct : -ct);
+}
+static v3 coating_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (ci * co <= 0.0f) return V(0, 0, 0);
+    float a = alpha_u_of(b);
+    mfd d = mfd_make(b->d.distribution, a, a);
+    v3 h = scl(normalize(add(r->wi, r->wo)), signum(r->wo.z));
+    float ct;
+    float D = mfd_eval(&d, h);
+    float F = fresnel_dielectric(fabsf(dot(r->wi, h)), b->eta, b->inv_eta, &ct);
+    float G = mfd_g(&d, r->wi, r->wo, h);
+    v3 ks = vload(b->d.ks);
+    float den = 4.0f * fabsf(ci);
+    v3 res = V((((ks.x * F) * D) * G) / den, (((ks.y * F) * D) * G) / den, (((ks.z * F) * D) * G) / den);
+    brec ri = *r;
+    ri.wi = coat_refract(r->wi, b->inv_eta);
+    ri.wo = coat_refract(r->wo, b->inv_eta);
+    v3 nv = bsdf_eval(s, b->d.nested, &ri);
+    float ti = rft_eval1d(b->rft, b->rft_n, fabsf(ci)), to = rft_eval1d(b->rft, b->rft_n, fabsf(co));
+    nv = V(nv.x * ti * to, nv.y * ti * to, nv.z * ti * to);
+    v3 sa = scl(vload(b->d.sigma_a), b->d.thickness);
+    if (!is_zero(sa)) {
+        float q = 1.0f / fabsf(ri.wi.z) + 1.0f / fabsf(ri.wo.z);
+        nv = mul(nv, V(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q)));
+    }
+    if (r->measure == HO_MEASURE_SOLID_ANGLE) nv = scl(nv, b->inv_eta * b->inv_eta * r->wo.z / ri.wo.z);
+    return add(res, nv);
+}
+static float coating_pdf(const ho_scene *s, const bsdf_t *b, const brec *r) {
+    v3 h = scl(normalize(add(r->wi, r->wo)), signum(r->wo.z));
+    float a = alpha_u_of(b);
+    mfd d = mfd_make(b->d.distribution, a, a);
+    float ci = r->wi.z, co = r->wo.z;
+    float r12 = 1.0f - rft_eval1d(b->rft, b->rft_n, fabsf(ci));
+    float sp = (r12 * b->spec_w) / (r12 * b->spec_w + (1.0f - r12) * (1.0f - b->spec_w));
+    float np = 1.0f - sp;
+    float res = 0.0f;
+    if (ci * co > 0.0f) {
+        float J = 1.0f / (4.0f * fabsf(dot(r->wo, h)));
+        res = mfd_pdf(&d, h) * J * sp;
+    }
+    brec ri = *r;
+    ri.wi = coat_refract(r->wi, b->inv_eta);
+    ri.wo = coat_refract(r->wo, b->inv_eta);
+    float p = bsdf_pdf(s, b->d.nested, &ri);
+    if (ri.measure == HO_MEASURE_SOLID_ANGLE) p *= b->inv_eta * b->inv_eta * co / ri.wo.z;
+    return res + p * np;
+}
+static v3 coating_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux, float uy, ho_pcg32 *rng,
+                         const float *u1f) {
+    float a = alpha_u_of(b);
+    mfd d = mfd_make(b->d.distribution, a, a);
+    float aci = fabsf(r->wi.z);
+    float r12 = 1.0f - rft_eval1d(b->rft, b->rft_n, aci);
+    float sp = (r12 * b->spec_w) / (r12 * b->spec_w + (1.0f - r12) * (1.0f - b->spec_w));
+    int spec;
+    if (ux < sp) { spec = 1; ux /= sp; }
+    else { spec = 0; ux = (ux - sp) / (1.0f - sp); }
+    if (spec) {
+        float pdf;
+        v3 m = mfd_sample(&d, ux, uy, &pdf);
+        r->wo = reflect_m(r->wi, m);
+        r->measure = HO_MEASURE_DISCRETE;
+        r->eta = 1.0f;
+        if (r->wo.z * r->wo.z <= 0.0f) return V(0, 0, 0);
+    } else {
+        v3 wib = r->wi;
+        r->wi = coat_refract(r->wi, b->inv_eta);
+        v3 res = bsdf_sample(s, b->d.nested, r, ux, uy, rng, u1f);
+        r->wi = wib;
+        if (is_zero(res)) return V(0, 0, 0);
+        r->wo = coat_refract(r->wo, b->eta);
+        if (is_zero(r->wo)) return V(0, 0, 0);
+    }
+    float P = coating_pdf(s, b, r);
+    if (P == 0.0f) return V(0, 0, 0);
+    return divs(coating_eval(s, b, r), P);
+}
+
+static v3 bsdf_eval(const ho_scene *s, int id, const brec *r) {
+    const bsdf_t *b = &s->bsdfs[id];
+    switch (b->d.type) {
+    case HO_BSDF_DIFFUSE: return diffuse_eval(b, r);
+    case HO_BSDF_ROUGH_CONDUCTOR: return conductor_eval(b, r);
+    case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_eval(b, r);
+    case HO_BSDF_ROUGH_PLASTIC: return plastic_eval(b, r);
+    default: return coating_eval(s, b, r);
+    }
+}
+static float bsdf_pdf(const ho_scene *s, int id, const brec *r) {
+    const bsdf_t *b = &s->bsdfs[id];
+    switch (b->d.type) {
+    case HO_BSDF_DIFFUSE: return diffuse_pdf(r);
+    case HO_BSDF_ROUGH_CONDUCTOR: return conductor_pdf(b, r);
+    case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_pdf(b, r);
+    case HO_BSDF_ROUGH_PLASTIC: return plastic_pdf(b, r);
+    default: return coating_pdf(s, b, r);
+    }
+}
+static v3 bsdf_sample(const ho_scene *s, int id, brec *r, float ux, float uy, ho_pcg32 *rng, const float *u1f) {
+    const bsdf_t *b = &s->bsdfs[id];
+    switch (b->d.type) {
+    case HO_BSDF_DIFFUSE: return diffuse_sample(b, r, ux, uy);
+    case HO_BSDF_ROUGH_CONDUCTOR: return conductor_sample(b, r, ux, uy);
+    case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_sample(b, r, ux, uy, rng, u1f);
+    case HO_BSDF_ROUGH_PLASTIC: return plastic_sample(b, r, ux, uy);
+    default: return coating_sample(s, b, r, ux, uy, rng, u1f);
+    }
+}
+
+void ho_bsdf_sample(const ho_scene *s, int id, const float *wi, const float *u2, float u1, float *owo,
+                    float *ow, int *om, float *oeta) {
+    brec r; memset(&r, 0, sizeof r);
+    r.wi = vload(wi); r.measure = HO_MEASURE_UNKNOWN; r.eta = 0.0f;
+    v3 w = bsdf_sample(s, id, &r, u2[0], u2[1], NULL, &u1);
+    vstore(owo, r.wo); vstore(ow, w); *om = r.measure; *oeta = r.eta;
+}
+void ho_bsdf_eval(const ho_scene *s, int id, const float *wi, const float *wo, int measure, float *o) {
+    brec r; r.wi = vload(wi); r.wo = vload(wo); r.measure = measure; r.eta = 0.0f;
+    vstore(o, bsdf_eval(s, id, &r));
+}
+float ho_bsdf_pdf(const ho_scene *s, int id, const float *wi, const float *wo, int measure) {
+    brec r; r.wi = vload(wi); r.wo = vload(wo); r.measure = measure; r.eta = 0.0f;
+    return bsdf_pdf(s, id, &r);
+}
+float ho_bsdf_rft_eval(const ho_scene *s, int id, float c) {
+    const bsdf_t *b = &s->bsdfs[id];
+    return rft_eval1d(b->rft, b->rft_n, c);
+}
+void ho_bsdf_batch(const ho_scene *s, int id, uint64_t n, const float *wi, const float *u2, const float *u1,
+                   const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
+                   float *p_pdf, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(static)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        brec r; memset(&r, 0, sizeof r);
+        r.wi = vload(wi + 3 * i); r.measure = HO_MEASURE_UNKNOWN;
+        float uu = u1 ? u1[i] : 0.0f;
+        v3 w = bsdf_sample(s, id, &r, u2[2 * i], u2[2 * i + 1], NULL, &uu);
+        if (s_wo) vstore(s_wo + 3 * i, r.wo);
+        if (s_w) vstore(s_w + 3 * i, w);
+        if (s_m) s_m[i] = r.measure;
+        if (s_pdf) s_pdf[i] = is_zero(w) && w.x == 0 && w.y == 0 && w.z == 0 ? 0.0f : bsdf_pdf(s, id, &r);
+        brec q; q.wi = vload(wi + 3 * i); q.wo = vload(wo + 3 * i); q.measure = HO_MEASURE_SOLID_ANGLE; q.eta = 0;
+        if (e_rgb) vstore(e_rgb + 3 * i, bsdf_eval(s, id, &q));
+        if (p_pdf) p_pdf[i] = bsdf_pdf(s, id, &q);
+    }
+}
+
+/* ------------------------------------------------------------ geometry */
+/* Mesh::RayIntersect  src/core/Mesh.cpp:340 (Moller-Trumbore) */
+static int tri_intersect(const ho_scene *s, uint32_t t, v3 o, v3 d, float mint, float maxt, float *ou,
+                         float *ov, float *ot) {
+    const uint32_t *f = s->F + 3ull * t;
+    v3 p0 = vload(s->P + 3ull * f[0]), p1 = vload(s->P + 3ull * f[1]), p2 = vload(s->P + 3ull * f[2]);
+    v3 e1 = sub(p1, p0), e2 = sub(p2, p0);
+    v3 pv = cross(d, e2);
+    float det = dot(e1, pv);
+    if (det > -1e-8f && det < 1e-8f) return 0;
+    float inv = 1.0f / det;
+    v3 tv = sub(o, p0);
+    float u = dot(tv, pv) * inv;
+    if (u < 0.0 || u > 1.0) return 0;
+    v3 qv = cross(tv, e1);
+    float v = dot(d, qv) * inv;
+    if (v < 0.0 || u + v > 1.0) return 0;
+    float tt = dot(e2, qv) * inv;
+    *ou = u; *ov = v; *ot = tt;
+    return tt >= mint && tt <= maxt;
+}
+/* BoundingBox::RayIntersect  include/core/BoundingBox.hpp:371 */
+static int box_hit(const float *mn, const float *mx, const float *o, const float *d, const float *rd,
+                   float mint, float maxt) {
+    float nt = -INFINITY, ft = INFINITY;
+    for (int i = 0; i < 3; i++) {
+        if (d[i] == 0) { if (o[i] < mn[i] || o[i] > mx[i]) return 0; }
+        else {
+            float t1 = (mn[i] - o[i]) * rd[i], t2 = (mx[i] - o[i]) * rd[i];
+            if (t1 > t2) { float tmp = t1; t1 = t2; t2 = tmp; }
+            nt = fmaxf(t1, nt); ft = fminf(t2, ft);
+            if (!(nt <= ft)) return 0;
+        }
+    }
+    return mint <= ft && nt <= maxt;
+}
+
+typedef struct { float mn[3], mx[3]; } aabb;
+static inline void aabb_empty(aabb *b) { for (int i = 0; i < 3; i++) { b->mn[i] = INFINITY; b->mx[i] = -INFINITY; } }
+static inline void aabb_grow(aabb *b, const aabb *o) { for (int i = 0; i < 3; i++) { b->mn[i] = fminf(b->mn[i], o->mn[i]); b->mx[i] = fmaxf(b->mx[i], o->mx[i]); } }
+static inline float aabb_area(const aabb *b) {
+    float dx = b->mx[0] - b->mn[0], dy = b->mx[1] - b->mn[1], dz = b->mx[2] - b->mn[2];
+    if (dx < 0) return 0;
+    return 2.0f * (dx * dy + dy * dz + dz * dx);
+}
+
+typedef struct { aabb *tb; float *cent; uint32_t *ord; bnode *nodes; int nn, cap; } bctx;
+
+static int bvh_rec(bctx *c, uint32_t b, uint32_t e) {
+    if (c->nn == c->cap) { c->cap *= 2; c->nodes = realloc(c->nodes, c->cap * sizeof(bnode)); }
+    int me = c->nn++;
+    aabb bb, cb; aabb_empty(&bb); aabb_empty(&cb);
+    for (uint32_t i = b; i < e; i++) {
+        aabb_grow(&bb, &c->tb[c->ord[i]]);
+        aabb pc; for (int k = 0; k < 3; k++) pc.mn[k] = pc.mx[k] = c->cent[3 * c->ord[i] + k];
+        aabb_grow(&cb, &pc);
+    }
+    for (int k = 0; k < 3; k++) { c->nodes[me].bmin[k] = bb.mn[k]; c->nodes[me].bmax[k] = bb.mx[k]; }
+    uint32_t n = e - b;
+    int axis = 0; float ext = cb.mx[0] - cb.mn[0];
+    for (int k = 1; k < 3; k++) if (cb.mx[k] - cb.mn[k] > ext) { ext = cb.mx[k] - cb.mn[k]; axis = k; }
+    if (n <= 4 || ext <= 0.0f) {
+        c->nodes[me].left_or_first = (int32_t)b; c->nodes[me].count = (int32_t)n; c->nodes[me].axis = axis; c->nodes[me].right = -1;
+        return me;
+    }
+    /* 12-bucket binned SAH (the scheme of src/acceleration/BVHAcceleration.cpp:150) */
+    enum { NB = 12 };
+    aabb bk[NB]; uint32_t cnt[NB] = {0};
+    for (int i = 0; i < NB; i++) aabb_empty(&bk[i]);
+    float inv = 1.0f / ext;
+    for (uint32_t i = b; i < e; i++) {
+        int bi = (int)((NB - 1) * (c->cent[3 * c->ord[i] + axis] - cb.mn[axis]) * inv);
+        bi = clampi(bi, 0, NB - 1);
+        cnt[bi]++; aabb_grow(&bk[bi], &c->tb[c->ord[i]]);
+    }
+    float best = INFINITY; int bs = -1;
+    for (int i = 0; i < NB - 1; i++) {
+        aabb l, r; aabb_empty(&l); aabb_empty(&r); uint32_t nl = 0, nr = 0;
+        for (int j = 0; j <= i; j++) { aabb_grow(&l, &bk[j]); nl += cnt[j]; }
+        for (int j = i + 1; j < NB; j++) { aabb_grow(&r, &bk[j]); nr += cnt[j]; }
+        if (!nl || !nr) continue;
+        float cost = aabb_area(&l) * nl + aabb_area(&r) * nr;
+        if (cost < best) { best = cost; bs = i; }
+    }
+    uint32_t mid = b;
+    if (bs >= 0) {
+        for (uint32_t i = b; i < e; i++) {
+            int bi = (int)((NB - 1) * (c->cent[3 * c->ord[i] + axis] - cb.mn[axis]) * inv);
+            bi = clampi(bi, 0, NB - 1);
+            if (bi <= bs) { uint32_t t = c->ord[i]; c->ord[i] = c->ord[mid]; c->ord[mid] = t; mid++; }
+        }
+    }
+    if (mid == b || mid == e) mid = b + n / 2;
+    c->nodes[me].axis = axis; c->nodes[me].count = 0;
+    int l = bvh_rec(c, b, mid);
+    int r = bvh_rec(c, mid, e);
+    c->nodes[me].left_or_first = l; c->nodes[me].right = r;
+    return me;
+}
+static int bvh_build(ho_scene *s) {
+    free(s->nodes); free(s->order); s->nodes = NULL; s->order = NULL; s->nnodes = 0;
+    aabb all; aabb_empty(&all);
+    for (uint64_t i = 0; i < s->nv; i++) {
+        aabb p; for (int k = 0; k < 3; k++) p.mn[k] = p.mx[k] = s->P[3 * i + k];
+        aabb_grow(&all, &p);
+    }
+    for (int k = 0; k < 3; k++) { s->bbox[k] = all.mn[k]; s->bbox[3 + k] = all.mx[k]; }
+    if (s->nt == 0) return 0;
+    bctx c; c.tb = malloc(sizeof(aabb) * s->nt); c.cent = malloc(12ull * s->nt); c.ord = malloc(4ull * s->nt);
+    for (uint32_t t = 0; t < s->nt; t++) {
+        const uint32_t *f = s->F + 3ull * t;
+        aabb_empty(&c.tb[t]);
+        for (int j = 0; j < 3; j++) { aabb p; for (int k = 0; k < 3; k++) p.mn[k] = p.mx[k] = s->P[3ull * f[j] + k]; aabb_grow(&c.tb[t], &p); }
+        for (int k = 0; k < 3; k++) c.cent[3 * t + k] = (1.0f / 3.0f) * (s->P[3ull * f[0] + k] + s->P[3ull * f[1] + k] + s->P[3ull * f[2] + k]);
+        c.ord[t] = t;
+    }
+    c.cap = 1024; c.nn = 0; c.nodes = malloc(c.cap * sizeof(bnode));
+    bvh_rec(&c, 0, s->nt);
+    s->nodes = c.nodes; s->nnodes = c.nn; s->order = c.ord;
+    free(c.tb); free(c.cent);
+    return 0;
+}
+
+typedef struct { float t, u, v; int32_t tri; } hit_t;
+/* Closest/any hit.  Reference tie rule: accept T <= MaxT, so later-visited wins
+ * (src/core/Acceleration.cpp:59-69, src/acceleration/HLBVHAcceleration.cpp:229-240). */
+static int trace(const ho_scene *s, v3 o, v3 d, float mint, float maxt, int any, int use_bvh, hit_t *h) {
+    int found = 0;
+    h->tri = -1;
+    if (!use_bvh || !s->nodes) {
+        for (uint32_t t = 0; t < s->nt; t++) {
+            float u, v, tt;
+            if (tri_intersect(s, t, o, d, mint, maxt, &u, &v, &tt)) {
+                if (any) { h->tri = (int32_t)t; return 1; }
+                maxt = tt; h->t = tt; h->u = u; h->v = v; h->tri = (int32_t)t; found = 1;
+            }
+        }
+        return found;
+    }
+    float of[3] = {o.x, o.y, o.z}, df[3] = {d.x, d.y, d.z}, rd[3] = {1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    int neg[3] = {rd[0] < 0, rd[1] < 0, rd[2] < 0};
+    int stack[128]; int sp = 0; int cur = 0;
+    for (;;) {
+        const bnode *nd = &s->nodes[cur];
+        if (box_hit(nd->bmin, nd->bmax, of, df, rd, mint, maxt)) {
+            if (nd->count > 0) {
+                for (int i = 0; i < nd->count; i++) {
+                    uint32_t t = s->order[nd->left_or_first + i];
+                    float u, v, tt;
+                    if (tri_intersect(s, t, o, d, mint, maxt, &u, &v, &tt)) {
+                        if (any) { h->tri = (int32_t)t; return 1; }
+                        maxt = tt; h->t = tt; h->u = u; h->v = v; h->tri = (int32_t)t; found = 1;
+                    }
+                }
+                if (sp == 0) break;
+                cur = stack[--sp];
+            } else {
+                if (neg[nd->axis]) { stack[sp++] = nd->left_or_first; cur = nd->right; }
+                else { stack[sp++] = nd->right; cur = nd->left_or_first; }
+            }
+        } else {
+            if (sp == 0) break;
+            cur = stack[--sp];
+        }
+    }
+    return found;
+}
+
+void ho_trace(const ho_scene *s, uint64_t n, const float *rays, float *th, float *uh, float *vh, int32_t *tri,
+              int any, int use_bvh, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 256)
+#endif
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        const float *r = rays + 8 * i;
+        hit_t h; h.t = h.u = h.v = 0.0f;
+        int f = trace(s, V(r[0], r[1], r[2]), V(r[3], r[4], r[5]), r[6], r[7], any, use_bvh, &h);
+        if (any) { tri[i] = f; continue; }
+        tri[i] = f ? h.tri : -1;
+        if (th) th[i] = f ? h.t : 0.0f;
+        if (uh) uh[i] = f ? h.u : 0.0f;
+        if (vh) vh[i] = f ? h.v : 0.0f;
+    }
+}
+
+/* Triangle::PostIntersect  src/core/Mesh.cpp:67 (no UV partials: meshes here carry no vt) */
+typedef struct { v3 p; frame sh, geo; int mesh; float t; } isect_t;
+static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
+    const uint32_t *f = s->F + 3ull * h->tri;
+    v3 p0 = vload(s->P + 3ull * f[0]), p1 = vload(s->P + 3ull * f[1]), p2 = vload(s->P + 3ull * f[2]);
+    float b0 = 1 - (h->u + h->v), b1 = h->u, b2 = h->v;
+    it->p = add(add(scl(p0, b0), scl(p1, b1)), scl(p2, b2));
+    it->geo = frame_from_n(normalize(cross(sub(p1, p0), sub(p2, p0))));
+    it->mesh = s->tri_mesh[h->tri];
+    it->t = h->t;
+    if (s->meshes[it->mesh].has_n) {
+        v3 n0 = vload(s->N + 3ull * f[0]), n1 = vload(s->N + 3ull * f[1]), n2 = vload(s->N + 3ull * f[2]);
+        it->sh = frame_from_n(normalize(add(add(scl(n0, b0), scl(n1, b1)), scl(n2, b2))));
+    } else {
+        it->sh = it->geo;
+    }
+}
+
+/* ------------------------------------------------------------ emitters */
+typedef struct { v3 ref, p, n, wi; float pdf, dist; } erec;
+
+/* Mesh::SamplePosition  src/core/Mesh.cpp:273 */
+static void mesh_sample(const ho_scene *s, const mesh_t *m, float u1, float ux, float uy, v3 *P, v3 *N) {
+    int ti = cdf_find(m->cdf, (int)m->nt, u1);    /* DiscretePDF1D::SampleDiscrete :65 */
+    float sq = sqrtf(1.0f - ux);
+    float al = 1.0f - sq, be = uy * sq, ga = 1.0f - al - be;
+    const uint32_t *f = s->F + 3ull * (m->t0 + ti);
+    v3 p0 = vload(s->P + 3ull * f[0]), p1 = vload(s->P + 3ull * f[1]), p2 = vload(s->P + 3ull * f[2]);
+    *P = add(add(scl(p0, ga), scl(p1, al)), scl(p2, be));
+    if (m->has_n) {
+        v3 n0 = vload(s->N + 3ull * f[0]), n1 = vload(s->N + 3ull * f[1]), n2 = vload(s->N + 3ull * f[2]);
+        *N = add(add(scl(n0, ga), scl(n1, al)), scl(n2, be));
+    } else {
+        *N = normalize(cross(sub(p1, p0), sub(p2, p0)));
+    }
+}
+/* AreaLight::Pdf / Eval  src/emitter/AreaLight.cpp:38,59 */
+static float area_pdf(const mesh_t *m, const erec *r) {
+    float gd = fabsf(dot(scl(r->wi, -1.0f), r->n));
+    if (gd == 0.0f) return 0.0f;
+    float gn = r->dist * r->dist;
+    return m->inv_area * (gn / gd);
+}
+static v3 area_eval(const mesh_t *m, const erec *r) { return dot(r->n, r->wi) < 0.0f ? m->radiance : V(0, 0, 0); }
+/* AreaLight::Sample  src/emitter/AreaLight.cpp:14 */
+static v3 area_sample(const ho_scene *s, const mesh_t *m, erec *r, float ux, float uy, float u1) {
+    mesh_sample(s, m, u1, ux, uy, &r->p, &r->n);
+    v3 wi = sub(r->p, r->ref);
+    r->dist = norm(wi);
+    r->wi = normalize(wi);
+    r->pdf = area_pdf(m, r);
+    if (r->pdf == 0.0f || isinf(r->pdf)) return V(0, 0, 0);
+    return divs(area_eval(m, r), r->pdf);
+}
+static inline v3 env_texel(const ho_scene *s, int y, int x) { return vload(s->env + 3ull * ((uint64_t)y * s->ew + x)); }
+/* SphericalCoordinates  src/core/Common.cpp:481 */
+static void spherical_coords(v3 d, float *th, float *ph) {
+    *th = acosf(d.z); *ph = atan2f(d.y, d.x);
+    if (*ph < 0) *ph += 2.0f * PI_F;
+}
+/* EnvironmentLight::Sample  src/emitter/EnvironmentLight.cpp:41 */
+static v3 env_sample(const ho_scene *s, erec *r, float ux, float uy) {
+    float py, px; int iy, ix;
+    float dy = pdf1d_sample_cont(&s->env_marg, uy, &py, &iy);
+    float dx = pdf1d_sample_cont(&s->env_rows[iy], ux, &px, &ix);
+    float mp = px * py;
+    float th = dy * PI_F, st = sinf(th);
+    if (mp == 0.0f) return V(0, 0, 0);
+    if (st != 0.0f) r->pdf = mp / (2.0f * (float)(M_PI * M_PI) * st);
+    else return V(0, 0, 0);
+    float ph = dx * (float)(2.0 * M_PI);
+    float sp = sinf(ph), cp = cosf(ph), ct = cosf(th);
+    v3 dir = V(st * cp, st * sp, ct);                 /* SphericalDirection :467 */
+    r->wi = mat3_mul(s->to_world, dir);
+    r->n = scl(r->wi, -1.0f);
+    r->p = add(r->ref, scl(scl(r->wi, r->dist), 2.0f));
+    v3 rad = env_texel(s, iy, ix);
+    if (!is_valid(rad)) return V(0, 0, 0);
+    return divs(scl(rad, s->env_scale), r->pdf);
+}
+/* EnvironmentLight::Pdf :78 and DiscretePDF2D::Pdf  src/core/DiscretePDF.cpp:127 */
+static float env_pdf(const ho_scene *s, const erec *r) {
+    float th, ph;
+    spherical_coords(mat3_mul(s->to_local, r->wi), &th, &ph);
+    float st = sinf(th);
+    if (st == 0.0f) return 0.0f;
+    float u = ph / (float)(2.0 * M_PI), v = th / (float)M_PI;
+    int X = clampi((int)(u * s->ew), 0, (int)s->ew - 1), Y = clampi((int)(v * s->eh), 0, (int)s->eh - 1);
+    float p = s->env_rows[Y].func[X] / s->env_marg.integral;
+    return p / (2.0f * (float)(M_PI * M_PI) * st);
+}
+/* EnvironmentLight::Eval :92 */
+static v3 env_eval(const ho_scene *s, v3 wi) {
+    float th, ph;
+    spherical_coords(mat3_mul(s->to_local, wi), &th, &ph);
+    if (isnan(th) || isnan(ph)) return V(0, 0, 0);
+    float X = clampf(ph / (float)(2.0 * M_PI) * (float)s->ew, 0.0f, (float)(s->ew - 1.0f));
+    float Y = clampf(th / (float)M_PI * (float)s->eh, 0.0f, (float)(s->eh - 1.0f));
+    v3 rad = env_texel(s, (int)Y, (int)X);
+    if (!is_valid(rad)) return V(0, 0, 0);
+    return scl(rad, s->env_scale);
+}
+
+/* ------------------------------------------------------------ camera */
+/* PerspectiveCamera::SampleRay  src/camera/PerspectiveCamera.cpp:77.  The
+ * sample->camera map inverted in closed form: near-plane point
+ * (near(1-2u)/cot, near(1-2v)/(aspect cot), near). */
+static void camera_ray(const ho_scene *s, float px, float py, v3 *o, v3 *d, float *mint, float *maxt) {
+    float u = px * (1.0f / (float)s->W), v = py * (1.0f / (float)s->H);
+    v3 np = V(s->near_c * (1.0f - 2.0f * u) / s->cot, s->near_c * (1.0f - 2.0f * v) / (s->aspect * s->cot), s->near_c);
+    v3 dir = normalize(np);
+    float invz = 1.0f / dir.z;
+    const float *M = s->cam;
+    float w = M[15];
+    *o = V(M[3] / w, M[7] / w, M[11] / w);
+    *d = V(M[0] * dir.x + M[1] * dir.y + M[2] * dir.z, M[4] * dir.x + M[5] * dir.y + M[6] * dir.z,
+           M[8] * dir.x + M[9] * dir.y + M[10] * dir.z);
+    *mint = s->near_c * invz;
+    *maxt = s->far_c * invz;
+}
+
+/* ------------------------------------------------------------ integrator */
+typedef struct { uint64_t rays, shadow; } ctr_t;
+static inline v3 emitter_sample_any(const ho_scene *s, int e, erec *r, float ux, float uy, float u1) {
+    int mi = s->emit_mesh[e];
+    if (mi < 0) return env_sample(s, r, ux, uy);
+    return area_sample(s, &s->meshes[mi], r, ux, uy, u1);
+}
+
+/* PathMISIntegrator::Li  src/integrator/PathMISIntegrator.cpp:16-157 */
+static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 rdir, float rmint, float rmaxt,
+                     ctr_t *ctr) {
+    hit_t hn; int found_next = 0;
+    isect_t it, itn;
+    v3 L = V(0, 0, 0), beta = V(1, 1, 1);
+    uint32_t depth = 0;
+    float w_ems = 1.0f, w_mats = 1.0f;
+    int has_env = s->has_env;
+    float radius = 0.5f * norm(V(s->bbox[3] - s->bbox[0], s->bbox[4] - s->bbox[1], s->bbox[5] - s->bbox[2]));
+    while (depth < (uint32_t)depth_max) {
+        if (depth == 0) {
+            hit_t h;
+            ctr->rays++;
+            if (!trace(s, ro, rdir, rmint, rmaxt, 0, 1, &h)) {
+                if (has_env && !s->force_bg) { L = add(L, mul(beta, env_eval(s, rdir))); break; }
+                return s->background;
+            }
+            post_intersect(s, &h, &it);
+        } else {
+            if (found_next) it = itn;
+            else {
+                if (has_env) L = add(L, mul(beta, env_eval(s, rdir)));
+                break;
+            }
+        }
+        const mesh_t *m = &s->meshes[it.mesh];
+        int bsdf = m->bsdf;
+        if (m->emitter >= 0) {
+            erec er; er.ref = ro; er.p = it.p; er.n = it.sh.n;
+            v3 wi = sub(er.p, er.ref); er.dist = norm(wi); er.wi = divs(wi, er.dist);
+            v3 le = area_eval(m, &er);
+            L = add(L, mul(scl(beta, w_mats), le));
+        }
+        for (int e = 0; e < s->n_emit; e++) {
+            erec er; memset(&er, 0, sizeof er); er.ref = it.p;
+            if (s->emit_mesh[e] < 0) er.dist = radius;
+            float u1 = ho_pcg32_nextf(rng);
+            float ux = ho_pcg32_nextf(rng), uy = ho_pcg32_nextf(rng);
+            v3 ld = emitter_sample_any(s, e, &er, ux, uy, u1);
+            float pl = er.pdf;
+            if (!is_zero(ld)) {
+                v3 sd = sub(er.p, it.p);
+                ctr->shadow++;
+                hit_t sh;
+                if (!trace(s, it.p, sd, EPS_RAY, 1.0f - EPS_RAY, 1, 1, &sh)) {
+                    brec br; br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.wo = to_local(&it.sh, er.wi);
+                    br.measure = HO_MEASURE_SOLID_ANGLE; br.eta = 0;
+                    float pb = bsdf_pdf(s, bsdf, &br);
+                    if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
+                    v3 f = bsdf_eval(s, bsdf, &br);
+                    float c = fabsf(br.wo.z);
+                    L = add(L, V((((beta.x * f.x) * c) * ld.x) * w_ems, (((beta.y * f.y) * c) * ld.y) * w_ems,
+                                 (((beta.z * f.z) * c) * ld.z) * w_ems));
+                }
+            }
+        }
+        brec br; memset(&br, 0, sizeof br);
+        br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.measure = HO_MEASURE_UNKNOWN;
+        float sx = ho_pcg32_nextf(rng), sy = ho_pcg32_nextf(rng);
+        v3 F = bsdf_sample(s, bsdf, &br, sx, sy, rng, NULL);
+        ro = it.p; rdir = to_world(&it.sh, br.wo);
+        beta = mul(beta, F);
+        if (is_zero(beta)) break;
+        ctr->rays++;
+        found_next = trace(s, ro, rdir, EPS_RAY, INFINITY, 0, 1, &hn);
+        if (found_next) {
+            post_intersect(s, &hn, &itn);
+            const mesh_t *mn = &s->meshes[itn.mesh];
+            if (mn->emitter >= 0) {
+                erec er; er.ref = it.p; er.p = itn.p; er.n = itn.sh.n;
+                v3 wi = sub(er.p, er.ref); er.dist = norm(wi); er.wi = divs(wi, er.dist);
+                float plm = area_pdf(mn, &er);
+                float pbm = bsdf_pdf(s, bsdf, &br);
+                if (pbm + plm != 0.0f) w_mats = pbm / (pbm + plm);
+            }
+        }
+        if (br.measure == HO_MEASURE_DISCRETE) { w_ems = 0.0f; w_mats = 1.0f; }
+        if (ho_pcg32_nextf(rng) < 0.95f) beta = scl(beta, 1.0f / 0.95f);
+        else break;
+        depth++;
+    }
+    return L;
+}
+
+/* ImageBlock::Put(Point2f, Color3f)  src/core/Block.cpp:95 (whole image, double accum) */
+static int film_put(const ho_scene *s, double *film, float px, float py, v3 val) {
+    if (!is_valid(val)) return 1;
+    int B = s->border, FW = (int)s->W + 2 * B, FH = (int)s->H + 2 * B;
+    float cx = px - 0.5f - (0 - B), cy = py - 0.5f - (0 - B);
+    int x0 = (int)ceilf(cx - s->filt_r), y0 = (int)ceilf(cy - s->filt_r);
+    int x1 = (int)floorf(cx + s->filt_r), y1 = (int)floorf(cy + s->filt_r);
+    x0 = x0 < 0 ? 0 : x0; y0 = y0 < 0 ? 0 : y0; x1 = x1 > FW - 1 ? FW - 1 : x1; y1 = y1 > FH - 1 ? FH - 1 : y1;
+    float wx[16], wy[16];
+    for (int x = x0, i = 0; x <= x1; ++x) wx[i++] = s->ftab[(int)(fabsf((float)x - cx) * s->lookup)];
+    for (int y = y0, i = 0; y <= y1; ++y) wy[i++] = s->ftab[(int)(fabsf((float)y - cy) * s->lookup)];
+    for (int y = y0, yr = 0; y <= y1; ++y, ++yr)
+        for (int x = x0, xr = 0; x <= x1; ++x, ++xr) {
+            float w = wx[xr] * wy[yr];
+            double *p = film + 4ull * ((uint64_t)y * FW + x);
+            p[0] += (double)(val.x * w); p[1] += (double)(val.y * w); p[2] += (double)(val.z * w); p[3] += (double)w;
+        }
+    return 0;
+}
+
+/* Render / RenderBlock  src/Main.cpp:11-44, 46-147 */
+int64_t ho_render(const ho_scene *s, int depth, int spp, const int32_t *blist, int nblk, double *film, int nthreads,
+                  uint64_t *counters) {
+    int BS = 32;
+    int nbx = ((int)s->W + BS - 1) / BS, nby = ((int)s->H + BS - 1) / BS;
+    int total = blist ? nblk : nbx * nby;
+    int B = s->border;
+    uint64_t FW = s->W + 2 * B, FH = s->H + 2 * B;
+    int64_t dropped = 0; uint64_t rays = 0, shadow = 0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel reduction(+ : dropped, rays, shadow)
+#endif
+    {
+        double *loc = calloc(FW * FH * 4, sizeof(double));
+        ctr_t c = {0, 0};
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 1)
+#endif
+        for (int bi = 0; bi < total; bi++) {
+            int b = blist ? blist[bi] : bi;
+            int ox = (b % nbx) * BS, oy = (b / nbx) * BS;
+            ho_pcg32 rng; ho_pcg32_seed(&rng, (uint64_t)ox, (uint64_t)oy);   /* IndependentSampler::Prepare */
+            int sx = ((int)s->W - ox) < BS ? ((int)s->W - ox) : BS, sy = ((int)s->H - oy) < BS ? ((int)s->H - oy) : BS;
+            for (int y = 0; y < sy; ++y)
+                for (int x = 0; x < sx; ++x)
+                    for (int i = 0; i < spp; ++i) {
+                        float jx = ho_pcg32_nextf(&rng), jy = ho_pcg32_nextf(&rng);
+                        float px = (float)(x + ox) + jx, py = (float)(y + oy) + jy;
+                        (void)ho_pcg32_nextf(&rng); (void)ho_pcg32_nextf(&rng);   /* aperture sample */
+                        v3 o, d; float mn, mx;
+                        camera_ray(s, px, py, &o, &d, &mn, &mx);
+                        v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, &c);
+                        dropped += film_put(s, loc, px, py, L);
+                    }
+        }
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+        for (uint64_t i = 0; i < FW * FH * 4; i++) film[i] += loc[i];
+        free(loc);
+        rays += c.rays; shadow += c.shadow;
+    }
+    if (counters) { counters[0] = (uint64_t)total; counters[1] = rays; counters[2] = shadow; counters[3] = 0; }
+    return dropped;
+}
+
+void ho_pixel_stats(const ho_scene *s, int depth, int spp, uint64_t seed, int npix, const int32_t *pix, double *out,
+                    int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+    for (int k = 0; k < npix; k++) {
+        int x = pix[2 * k], y = pix[2 * k + 1];
+        ho_pcg32 rng; ho_pcg32_seed(&rng, seed, (uint64_t)y * s->W + x);
+        double m[3] = {0, 0, 0}, v[3] = {0, 0, 0};
+        ctr_t c = {0, 0};
+        for (int i = 0; i < spp; i++) {
+            float px = (float)x + ho_pcg32_nextf(&rng), py = (float)y + ho_pcg32_nextf(&rng);
+            v3 o, d; float mn, mx;
+            camera_ray(s, px, py, &o, &d, &mn, &mx);
+            v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, &c);
+            double r[3] = {L.x, L.y, L.z};
+            for (int ch = 0; ch < 3; ch++) { double dl = r[ch] - m[ch]; m[ch] += dl / (i + 1); v[ch] += dl * (r[ch] - m[ch]); }
+        }
+        for (int ch = 0; ch < 3; ch++) { out[6 * k + ch] = m[ch]; out[6 * k + 3 + ch] = spp > 1 ? v[ch] / (spp - 1) : 0; }
+    }
+}
+
+void ho_ttest_scene(const ho_scene *s, int depth, int n, double *mean, double *var) {
+    ho_pcg32 rng; pcg_default(&rng);
+    double m = 0, v = 0;
+    ctr_t c = {0, 0};
+    for (int k = 0; k < n; k++) {
+        float a = ho_pcg32_nextf(&rng), b = ho_pcg32_nextf(&rng);
+        float px = a * (float)s->W, py = b * (float)s->H;
+        (void)ho_pcg32_nextf(&rng); (void)ho_pcg32_nextf(&rng);
+        v3 o, d; float mn, mx;
+        camera_ray(s, px, py, &o, &d, &mn, &mx);
+        v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, &c);
+        double r = lum(L);
+        double dl = r - m; m += dl / (double)(k + 1); v += dl * (r - m);
+    }
+    *mean = m; *var = v / (n - 1);
+}
+
+void ho_film_resolve(const ho_scene *s, const double *film, float *out) {
+    int B = s->border; uint64_t FW = s->W + 2 * B;
+    for (uint32_t y = 0; y < s->H; y++)
+        for (uint32_t x = 0; x < s->W; x++) {
+            const double *p = film + 4 * ((uint64_t)(y + B) * FW + (x + B));
+            float *o = out + 3ull * ((uint64_t)y * s->W + x);
+            if (p[3] != 0.0) { o[0] = (float)(p[0] / p[3]); o[1] = (float)(p[1] / p[3]); o[2] = (float)(p[2] / p[3]); }
+            else { o[0] = o[1] = o[2] = 0.0f; }
+        }
+}
+
+/* ------------------------------------------------ emitter record queries */
+/* Emitter::Sample for emitter e (Scene order) at reference point ref. out: p(3) n(3) wi(3) pdf dist value(3) */
+void ho_emitter_sample(const ho_scene *s, int e, const float *ref, float ux, float uy, float u1, float *out) {
+    erec r; memset(&r, 0, sizeof r); r.ref = vload(ref);
+    float radius = 0.5f * norm(V(s->bbox[3] - s->bbox[0], s->bbox[4] - s->bbox[1], s->bbox[5] - s->bbox[2]));
+    if (s->emit_mesh[e] < 0) r.dist = radius;
+    v3 val = emitter_sample_any(s, e, &r, ux, uy, u1);
+    vstore(out, r.p); vstore(out + 3, r.n); vstore(out + 6, r.wi); out[9] = r.pdf; out[10] = r.dist; vstore(out + 11, val);
+}
+/* Emitter::Pdf for a record built as EmitterQueryRecord(emitter, ref, p, n)  src/core/Emitter.cpp:16 */
+float ho_emitter_pdf(const ho_scene *s, int e, const float *ref, const float *p, const float *n) {
+    erec r; r.ref = vload(ref); r.p = vload(p); r.n = vload(n);
+    v3 wi = sub(r.p, r.ref); r.dist = norm(wi); r.wi = divs(wi, r.dist);
+    int mi = s->emit_mesh[e];
+    if (mi < 0) { r.wi = vload(p); return env_pdf(s, &r); }   /* env: p carries the direction */
+    return area_pdf(&s->meshes[mi], &r);
+}
+/* Environment Eval for a world direction. */
+void ho_env_eval(const ho_scene *s, const float *wi, float *out) { vstore(out, env_eval(s, vload(wi))); }
+/* Camera ray for a film position (px, py): out o(3) d(3) mint maxt */
+void ho_camera_ray(const ho_scene *s, float px, float py, float *out) {
+    v3 o, d; float mn, mx; camera_ray(s, px, py, &o, &d, &mn, &mx);
+    vstore(out, o); vstore(out + 3, d); out[6] = mn; out[7] = mx;
+}
+/* Activated filter table (33 floats) and lookup factor. */
+void ho_filter_table(const ho_scene *s, float *out33, float *lookup) { memcpy(out33, s->ftab, 33 * 4); *lookup = s->lookup; }

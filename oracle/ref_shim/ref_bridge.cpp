@@ -1,0 +1,101 @@
+/* C entry points over the reference's own BSDF classes, compiled from the
+ * reference sources by oracle/ref_build.py.  Used by tests only, to pin the
+ * oracle restatement (oracle/hk_oracle.c) record by record. */
+#include <core\Common.hpp>
+#include <core\Object.hpp>
+#include <core\PropertyList.hpp>
+#include <core\BSDF.hpp>
+#include <core\Sampler.hpp>
+#include <core\Intersection.hpp>
+#include <core\Color.hpp>
+#include <core\Vector.hpp>
+
+using namespace Hikari;
+
+namespace {
+/* Sampler whose Next1D returns a value set per query (roughDielectric draws
+ * its reflect/refract choice from the record's sampler). */
+class FixedSampler : public Sampler {
+public:
+    float u1 = 0.0f;
+    std::unique_ptr<Sampler> Clone() const override { return std::unique_ptr<Sampler>(new FixedSampler(*this)); }
+    void Prepare(const ImageBlock &) override {}
+    void Generate() override {}
+    void Advance() override {}
+    float Next1D() override { return u1; }
+    Point2f Next2D() override { return Point2f(u1, u1); }
+    std::string ToString() const override { return "FixedSampler"; }
+};
+thread_local FixedSampler g_sampler;
+const Intersection &null_isect() { static const Intersection I; return I; }
+}
+
+extern "C" {
+
+void hr_init(const char *search_dir) { GetFileResolver()->prepend(filesystem::path(search_dir)); }
+
+/* type: 0 diffuse, 1 roughConductor, 2 roughDielectric, 3 roughPlastic, 4 roughCoating */
+void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_ior, const float *k,
+                     const float *ks, const float *kd, const float *sigma_a, float thickness, void *nested) {
+    static const char *names[] = {"diffuse", "roughConductor", "roughDielectric", "roughPlastic", "roughCoating"};
+    try {
+        PropertyList pl;
+        if (type == 0) {
+            pl.SetColor("albedo", Color3f(kd[0], kd[1], kd[2]));
+        } else {
+            pl.SetString("type", ggx ? "ggx" : "beckmann");
+            pl.SetFloat("alpha", alpha);
+            pl.SetFloat("intIOR", int_ior);
+            pl.SetFloat("extIOR", ext_ior);
+            if (type == 1) { pl.SetColor("k", Color3f(k[0], k[1], k[2])); pl.SetColor("ks", Color3f(ks[0], ks[1], ks[2])); }
+            if (type == 2) pl.SetColor("ksReflect", Color3f(ks[0], ks[1], ks[2]));
+            if (type == 3) { pl.SetColor("ks", Color3f(ks[0], ks[1], ks[2])); pl.SetColor("kd", Color3f(kd[0], kd[1], kd[2])); }
+            if (type == 4) { pl.SetColor("ks", Color3f(ks[0], ks[1], ks[2])); pl.SetColor("sigmaA", Color3f(sigma_a[0], sigma_a[1], sigma_a[2])); pl.SetFloat("thickness", thickness); }
+        }
+        BSDF *b = (BSDF *)ObjectFactory::CreateInstance(names[type], pl);
+        if (nested) b->AddChild((Object *)nested, "");
+        b->Activate();
+        return b;
+    } catch (const std::exception &e) {
+        fprintf(stderr, "hr_bsdf_create: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+void hr_bsdf_sample(void *h, const float *wi, const float *u2, float u1, float *wo, float *w, int *measure, float *eta) {
+    g_sampler.u1 = u1;
+    BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), ETransportMode::ERadiance, &g_sampler, null_isect());
+    r.Wo = Vector3f(0.0f); r.Eta = 0.0f;
+    Color3f c = ((BSDF *)h)->Sample(r, Point2f(u2[0], u2[1]));
+    wo[0] = r.Wo.x(); wo[1] = r.Wo.y(); wo[2] = r.Wo.z();
+    w[0] = c[0]; w[1] = c[1]; w[2] = c[2];
+    *measure = int(r.Measure); *eta = r.Eta;
+}
+
+void hr_bsdf_eval(void *h, const float *wi, const float *wo, int measure, float *out) {
+    BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), Vector3f(wo[0], wo[1], wo[2]), EMeasure(measure),
+                      ETransportMode::ERadiance, &g_sampler, null_isect());
+    Color3f c = ((BSDF *)h)->Eval(r);
+    out[0] = c[0]; out[1] = c[1]; out[2] = c[2];
+}
+
+float hr_bsdf_pdf(void *h, const float *wi, const float *wo, int measure) {
+    BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), Vector3f(wo[0], wo[1], wo[2]), EMeasure(measure),
+                      ETransportMode::ERadiance, &g_sampler, null_isect());
+    return ((BSDF *)h)->Pdf(r);
+}
+
+/* batched over n AoS records (same layout as ho_bsdf_batch) */
+void hr_bsdf_batch(void *h, uint64_t n, const float *wi, const float *u2, const float *u1, const float *wo,
+                   float *s_wo, float *s_w, float *s_pdf, int *s_m, float *e_rgb, float *p_pdf) {
+    for (uint64_t i = 0; i < n; i++) {
+        float eta; int m;
+        hr_bsdf_sample(h, wi + 3 * i, u2 + 2 * i, u1 ? u1[i] : 0.0f, s_wo + 3 * i, s_w + 3 * i, &m, &eta);
+        s_m[i] = m;
+        bool zero = s_w[3 * i] == 0.0f && s_w[3 * i + 1] == 0.0f && s_w[3 * i + 2] == 0.0f;
+        s_pdf[i] = zero ? 0.0f : hr_bsdf_pdf(h, wi + 3 * i, s_wo + 3 * i, m);
+        hr_bsdf_eval(h, wi + 3 * i, wo + 3 * i, 1, e_rgb + 3 * i);
+        p_pdf[i] = hr_bsdf_pdf(h, wi + 3 * i, wo + 3 * i, 1);
+    }
+}
+}

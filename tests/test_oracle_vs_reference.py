@@ -1,0 +1,103 @@
+"""Record-wise pin of the oracle BSDFs against the reference's own BSDF classes
+compiled from its sources (oracle/ref_build.py -> oracle/_ref).  Bit-exact
+equality is required: the oracle follows the reference's float evaluation
+order, including Eigen's x + (y + z) reduction of 3-vectors."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from hikari_b200.scenedesc import (BECKMANN, BSDF_DIFFUSE, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR,
+                                   BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_PLASTIC, GGX, BSDFDesc, SceneDesc)
+from oracle import oracle as O
+
+REF_LIB = os.path.join(os.path.dirname(O.HERE), "oracle", "_ref", "libhikari_ref_bsdf.so")
+
+
+def _ref_lib():
+    if not os.path.exists(REF_LIB):
+        try:
+            from oracle import ref_build
+            ref_build.build()
+        except Exception as e:  # reference checkout absent (e.g. on the GPU box)
+            pytest.skip(f"reference BSDF library unavailable: {e}")
+    R = C.CDLL(REF_LIB)
+    R.hr_init.argtypes = [C.c_char_p]
+    R.hr_bsdf_create.restype = C.c_void_p
+    R.hr_bsdf_create.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_float] + [C.c_void_p] * 4 + [
+        C.c_float, C.c_void_p]
+    R.hr_bsdf_batch.argtypes = [C.c_void_p, C.c_uint64] + [C.c_void_p] * 10
+    R.hr_init(os.path.dirname(REF_LIB).encode())
+    return R
+
+
+CU_K = [3.9, 2.4, 2.2]
+
+
+def _cases():
+    nested = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=0.2,
+                      ext_ior=1.0, k=CU_K)
+    return {
+        "diffuse": BSDFDesc(type=BSDF_DIFFUSE, kd=[0.3, 0.5, 0.7]),
+        "conductor_beckmann": BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=BECKMANN, alpha_u=0.2,
+                                       alpha_v=0.2, int_ior=0.2, ext_ior=1.0, k=CU_K),
+        "conductor_ggx": BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.05, alpha_v=0.05,
+                                  int_ior=0.2, ext_ior=1.0, k=CU_K),
+        "dielectric_ggx": BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=0.1, alpha_v=0.1,
+                                   int_ior=1.5, ext_ior=1.0),
+        "dielectric_beckmann": BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=BECKMANN, alpha_u=0.3,
+                                        alpha_v=0.3, int_ior=1.5),
+        "plastic_ggx": BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=0.15, alpha_v=0.15),
+        "plastic_beckmann": BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=BECKMANN, alpha_u=0.3, alpha_v=0.3),
+        "coating": BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2, nested=nested),
+    }
+
+
+def records(n, seed):
+    rng = np.random.default_rng(seed)
+    z = rng.uniform(-0.2, 1, n)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    s = np.sqrt(1 - z * z)
+    wi = np.stack([s * np.cos(ph), s * np.sin(ph), z], 1).astype(np.float32)
+    u2 = rng.random((n, 2), dtype=np.float32)
+    u1 = rng.random(n, dtype=np.float32)
+    z2 = np.sqrt(rng.random(n))
+    ph2 = rng.uniform(0, 2 * np.pi, n)
+    s2 = np.sqrt(1 - z2 * z2)
+    sign = np.where(rng.random(n) < 0.8, 1, -1)
+    wo = np.stack([s2 * np.cos(ph2), s2 * np.sin(ph2), z2 * sign], 1).astype(np.float32)
+    return wi, u2, u1, wo
+
+
+@pytest.mark.parametrize("name", list(_cases()))
+def test_oracle_bsdf_bit_exact_vs_reference(name):
+    R = _ref_lib()
+    d = _cases()[name]
+    n = 50000
+    wi, u2, u1, wo = records(n, 7)
+    sd = SceneDesc()
+    o = O.OracleScene(sd)
+    bid = o.add_bsdf(d)
+    assert O.lib().ho_scene_finalize(o.h) == 0
+
+    def mk(b, nested=None):
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        k, ks, kd, sa = f(b.k), f(b.ks), f(b.kd), f(b.sigma_a)
+        h = R.hr_bsdf_create(b.type, b.distribution, b.alpha_u, b.int_ior, b.ext_ior, O._p(k), O._p(ks), O._p(kd),
+                             O._p(sa), b.thickness, nested)
+        assert h
+        return h
+
+    h = mk(d, mk(d.nested) if d.nested is not None else None)
+    a = o.bsdf_batch(bid, wi, u2, u1, wo)
+    b = {k: np.zeros_like(v) for k, v in a.items()}
+    R.hr_bsdf_batch(h, n, O._p(wi), O._p(u2), O._p(u1), O._p(wo), O._p(b["s_wo"]), O._p(b["s_w"]),
+                    O._p(b["s_pdf"]), O._p(b["s_measure"]), O._p(b["e_rgb"]), O._p(b["p_pdf"]))
+    valid = np.any(a["s_w"] != 0, axis=1)
+    np.testing.assert_array_equal(a["s_w"], b["s_w"])
+    np.testing.assert_array_equal(a["s_wo"][valid], b["s_wo"][valid])
+    np.testing.assert_array_equal(a["s_measure"], b["s_measure"])
+    np.testing.assert_array_equal(a["s_pdf"], b["s_pdf"])
+    np.testing.assert_array_equal(a["e_rgb"], b["e_rgb"])
+    np.testing.assert_array_equal(a["p_pdf"], b["p_pdf"])
