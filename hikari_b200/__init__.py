@@ -1,0 +1,359 @@
+"""hikari_b200: a B200-native core for Hikari's pathMIS path-tracing hot path.
+
+The product is the sm_100a CUDA library ``_build/libhikari_b200.so`` behind
+the C ABI of ``include/hikari_b200.h``.  This module binds that ABI with
+ctypes; torch is used only to hold device buffers and streams.  There is no
+CPU fallback: every entry point raises if the CUDA library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import scenedesc
+from .scenedesc import BSDFDesc, SceneDesc
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libhikari_b200.so")
+DATA_DIR = os.path.join(HERE, "data")
+
+HK_OK = 0
+
+
+class HikariError(RuntimeError):
+    """A non-zero status from the C ABI (the reference raises HikariException)."""
+
+
+class BsdfDesc(C.Structure):
+    _fields_ = [
+        ("type", C.c_int32), ("distribution", C.c_int32), ("anisotropic", C.c_int32), ("nonlinear", C.c_int32),
+        ("alpha_u", C.c_float), ("alpha_v", C.c_float), ("int_ior", C.c_float), ("ext_ior", C.c_float),
+        ("eta", C.c_float * 3), ("k", C.c_float * 3), ("ks", C.c_float * 3), ("ks_refract", C.c_float * 3),
+        ("kd", C.c_float * 3), ("sigma_a", C.c_float * 3), ("thickness", C.c_float), ("nested", C.c_int32),
+    ]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [
+        ("n_meshes", C.c_uint32), ("n_triangles", C.c_uint32), ("n_bsdfs", C.c_uint32), ("n_emitters", C.c_uint32),
+        ("n_bvh_nodes", C.c_uint32), ("bvh_depth", C.c_uint32), ("env_index", C.c_int32), ("film_border", C.c_int32),
+        ("bbox", C.c_float * 6), ("device_bytes", C.c_uint64),
+    ]
+
+
+class RenderDesc(C.Structure):
+    _fields_ = [
+        ("spp", C.c_int32), ("depth", C.c_int32), ("rr_start", C.c_int32), ("sample_offset", C.c_int32),
+        ("seed", C.c_uint64), ("image_index", C.c_int32), ("spp_per_item", C.c_int32),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load the CUDA library (raises HikariError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise HikariError(f"CUDA library not built: {LIB_PATH} (run hikari_b200.build.build())")
+    L = C.CDLL(LIB_PATH)
+    P, U64, I32, F = C.c_void_p, C.c_uint64, C.c_int32, C.c_float
+    sig = {
+        "hk_last_error": ([], C.c_char_p),
+        "hk_version": ([], C.c_int),
+        "hk_scene_create": ([C.POINTER(P)], C.c_int),
+        "hk_scene_destroy": ([P], C.c_int),
+        "hk_scene_set_rft": ([P, C.c_int, C.c_char_p, U64], C.c_int),
+        "hk_scene_add_bsdf": ([P, C.POINTER(BsdfDesc), C.POINTER(I32)], C.c_int),
+        "hk_scene_add_mesh": ([P, P, C.c_uint32, P, C.c_uint32, P, I32, P, C.POINTER(I32)], C.c_int),
+        "hk_scene_set_envmap": ([P, P, C.c_uint32, C.c_uint32, P, F], C.c_int),
+        "hk_scene_set_camera": ([P, C.c_uint32, C.c_uint32, P, F, F, F], C.c_int),
+        "hk_scene_set_filter": ([P, C.c_int, F, F, F], C.c_int),
+        "hk_scene_set_background": ([P, P, C.c_int], C.c_int),
+        "hk_scene_build": ([P], C.c_int),
+        "hk_scene_get_info": ([P, C.POINTER(SceneInfo)], C.c_int),
+        "hk_scene_load_xml": ([C.c_char_p, C.c_char_p, C.POINTER(P), C.POINTER(I32), C.POINTER(I32)], C.c_int),
+        "hk_scene_parse_xml": ([C.c_char_p, C.c_char_p, C.POINTER(P), C.POINTER(I32), C.POINTER(I32)], C.c_int),
+        "hk_exr_read": ([C.c_char_p, C.POINTER(I32), C.POINTER(I32), P, U64], C.c_int),
+        "hk_exr_write": ([C.c_char_p, I32, I32, P], C.c_int),
+        "hk_render": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
+        "hk_film_resolve": ([P, P, P, P], C.c_int),
+        "hk_render_image": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
+        "hk_trace": ([P, U64, P, P, P, P, P, C.c_int, P, P], C.c_int),
+        "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
+        "hk_emitter_sample": ([P, I32, U64, P, P, P], C.c_int),
+        "hk_camera_rays": ([P, U64, P, P, P], C.c_int),
+        "hk_env_eval": ([P, U64, P, P, P, P], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        if not hasattr(L, name):
+            raise HikariError(f"{LIB_PATH} does not export {name}; rebuild the library")
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != HK_OK:
+        raise HikariError(f"hikari_b200 error {rc}: {lib().hk_last_error().decode()}")
+
+
+def _p(a) -> Optional[int]:
+    """Raw pointer of a numpy array or a torch tensor (None passes NULL)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        import torch
+
+        return torch.cuda.current_stream().cuda_stream
+    return getattr(stream, "cuda_stream", stream)
+
+
+def bsdf_desc_c(d: BSDFDesc, nested_id: int = -1) -> BsdfDesc:
+    c = BsdfDesc()
+    c.type, c.distribution = d.type, d.distribution
+    c.anisotropic, c.nonlinear = int(d.anisotropic), int(d.nonlinear)
+    c.alpha_u, c.alpha_v, c.int_ior, c.ext_ior = d.alpha_u, d.alpha_v, d.int_ior, d.ext_ior
+    c.eta[:] = d.conductor_eta()
+    c.k[:], c.ks[:], c.ks_refract[:], c.kd[:], c.sigma_a[:] = d.k, d.ks, d.ks_refract, d.kd, d.sigma_a
+    c.thickness, c.nested = d.thickness, nested_id
+    return c
+
+
+def read_rft(distribution: int) -> bytes:
+    name = "GGXRFTData.bin" if distribution == scenedesc.GGX else "BeckmannRFTData.bin"
+    with open(os.path.join(DATA_DIR, name), "rb") as f:
+        return f.read()
+
+
+class Scene:
+    """A device-resident scene (hk_scene handle)."""
+
+    def __init__(self, handle, desc: Optional[SceneDesc] = None, bsdf_ids=None):
+        self.h = handle
+        self.desc = desc
+        self.bsdf_ids = bsdf_ids or {}
+        info = SceneInfo()
+        check(lib().hk_scene_get_info(self.h, C.byref(info)))
+        self.info = info
+        self._film = None
+
+    # ------------------------------------------------------------ construction
+    @classmethod
+    def from_desc(cls, desc: SceneDesc) -> "Scene":
+        L = lib()
+        h = C.c_void_p()
+        check(L.hk_scene_create(C.byref(h)))
+        try:
+            for dist in (0, 1):
+                b = read_rft(dist)
+                check(L.hk_scene_set_rft(h, dist, b, len(b)))
+            ids = {}
+
+            def add_bsdf(d: BSDFDesc) -> int:
+                if id(d) in ids:
+                    return ids[id(d)]
+                nested = add_bsdf(d.nested) if d.nested is not None else -1
+                c = bsdf_desc_c(d, nested)
+                out = C.c_int32()
+                check(L.hk_scene_add_bsdf(h, C.byref(c), C.byref(out)))
+                ids[id(d)] = out.value
+                return out.value
+
+            mesh_bsdf = [add_bsdf(m.bsdf) for m in desc.meshes]
+            order = desc.emitter_order()
+            env_pos = order.index(-1) if -1 in order else -1
+            n_emit = 0
+            env_done = False
+
+            def set_env():
+                e = desc.env
+                rgb, tw = _f32(e.rgb), _f32(e.to_world)
+                check(L.hk_scene_set_envmap(h, rgb.ctypes.data, rgb.shape[1], rgb.shape[0], tw.ctypes.data, e.scale))
+
+            for i, m in enumerate(desc.meshes):
+                if desc.env is not None and not env_done and n_emit == env_pos:
+                    set_env()
+                    env_done = True
+                    n_emit += 1
+                pos = _f32(m.positions)
+                idx = np.ascontiguousarray(m.indices, dtype=np.uint32)
+                nrm = _f32(m.normals) if m.normals is not None else None
+                rad = _f32(m.radiance) if m.radiance is not None else None
+                check(L.hk_scene_add_mesh(h, _p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm), mesh_bsdf[i],
+                                          _p(rad), None))
+                if m.radiance is not None:
+                    n_emit += 1
+            if desc.env is not None and not env_done:
+                set_env()
+            cam = desc.camera
+            tw = _f32(cam.to_world)
+            check(L.hk_scene_set_camera(h, cam.width, cam.height, tw.ctypes.data, cam.fov, cam.near_clip, cam.far_clip))
+            f = desc.filter
+            check(L.hk_scene_set_filter(h, f.kind, f.radius, f.p0, f.p1))
+            bg = _f32(desc.background)
+            check(L.hk_scene_set_background(h, bg.ctypes.data, int(desc.force_background)))
+            check(L.hk_scene_build(h))
+        except Exception:
+            L.hk_scene_destroy(h)
+            raise
+        return cls(h, desc, ids)
+
+    @classmethod
+    def from_xml(cls, path: str) -> "Scene":
+        """Load through the C++ plugin layer (LoadFromXML mirror)."""
+        L = lib()
+        h = C.c_void_p()
+        depth, spp = C.c_int32(), C.c_int32()
+        check(L.hk_scene_load_xml(path.encode(), DATA_DIR.encode(), C.byref(h), C.byref(depth), C.byref(spp)))
+        s = cls(h)
+        s.xml_depth, s.xml_spp = depth.value, spp.value
+        return s
+
+    def close(self):
+        if self.h:
+            lib().hk_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ rendering
+    @property
+    def width(self):
+        return self.desc.camera.width if self.desc else None
+
+    def film_shape(self):
+        import torch  # noqa: F401
+
+        B = self.info.film_border
+        cam = self.desc.camera
+        return (cam.height + 2 * B, cam.width + 2 * B, 4)
+
+    def render(self, film, spp: int, depth: int, seed: int = 0, sample_offset: int = 0, rr_start: int = 0,
+               image_index: int = 0, counters=None, spp_per_item: int = 0, stream=None) -> None:
+        """Accumulate into a device film tensor ((H+2B, W+2B, 4) float32)."""
+        d = RenderDesc(spp, depth, rr_start, sample_offset, seed, image_index, spp_per_item)
+        check(lib().hk_render(self.h, C.byref(d), _p(film), _p(counters), _stream(stream)))
+
+    def resolve(self, film, rgb, stream=None) -> None:
+        check(lib().hk_film_resolve(self.h, _p(film), _p(rgb), _stream(stream)))
+
+    def render_image(self, spp: int, depth: int, seed: int = 0, rr_start: int = 0, out: Optional[np.ndarray] = None,
+                     stream=None):
+        """End-to-end: render, resolve and return the H x W x 3 float32 image on the host."""
+        cam = self.desc.camera
+        if out is None:
+            out = np.empty((cam.height, cam.width, 3), np.float32)
+        ctr = np.zeros(3, np.uint64)
+        d = RenderDesc(spp, depth, rr_start, 0, seed, 0, 0)
+        check(lib().hk_render_image(self.h, C.byref(d), out.ctypes.data, ctr.ctypes.data, _stream(stream)))
+        return out, ctr
+
+    # ------------------------------------------------------------ record queries
+    def trace(self, rays, any_hit: bool = False, stream=None):
+        import torch
+
+        n = rays.shape[0]
+        dev = rays.device
+        tri = torch.empty(n, dtype=torch.int32, device=dev)
+        t = torch.empty(n, dtype=torch.float32, device=dev)
+        u = torch.empty_like(t)
+        v = torch.empty_like(t)
+        visits = torch.zeros(1, dtype=torch.int64, device=dev)
+        check(lib().hk_trace(self.h, n, _p(rays), _p(tri), _p(t), _p(u), _p(v), int(any_hit), _p(visits),
+                             _stream(stream)))
+        return tri, t, u, v, visits
+
+    def bsdf_batch(self, bsdf_id: int, wi, u2, u1, wo, stream=None):
+        import torch
+
+        n = wi.shape[0]
+        dev = wi.device
+        out = dict(
+            s_wo=torch.empty((n, 3), dtype=torch.float32, device=dev),
+            s_w=torch.empty((n, 3), dtype=torch.float32, device=dev),
+            s_pdf=torch.empty(n, dtype=torch.float32, device=dev),
+            s_measure=torch.empty(n, dtype=torch.int32, device=dev),
+            e_rgb=torch.empty((n, 3), dtype=torch.float32, device=dev),
+            p_pdf=torch.empty(n, dtype=torch.float32, device=dev),
+        )
+        check(lib().hk_bsdf_batch(self.h, bsdf_id, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(out["s_wo"]),
+                                  _p(out["s_w"]), _p(out["s_pdf"]), _p(out["s_measure"]), _p(out["e_rgb"]),
+                                  _p(out["p_pdf"]), _stream(stream)))
+        return out
+
+    def emitter_sample(self, e: int, inp, stream=None):
+        import torch
+
+        out = torch.empty((inp.shape[0], 16), dtype=torch.float32, device=inp.device)
+        check(lib().hk_emitter_sample(self.h, e, inp.shape[0], _p(inp), _p(out), _stream(stream)))
+        return out
+
+    def camera_rays(self, pos, stream=None):
+        import torch
+
+        out = torch.empty((pos.shape[0], 8), dtype=torch.float32, device=pos.device)
+        check(lib().hk_camera_rays(self.h, pos.shape[0], _p(pos), _p(out), _stream(stream)))
+        return out
+
+    def env_eval(self, wi, stream=None):
+        import torch
+
+        rgb = torch.empty((wi.shape[0], 3), dtype=torch.float32, device=wi.device)
+        pdf = torch.empty(wi.shape[0], dtype=torch.float32, device=wi.device)
+        check(lib().hk_env_eval(self.h, wi.shape[0], _p(wi), _p(rgb), _p(pdf), _stream(stream)))
+        return rgb, pdf
+
+
+def exr_read(path: str) -> np.ndarray:
+    """Read an RGB OpenEXR image (H x W x 3 float32) through the library."""
+    L = lib()
+    w, h = C.c_int32(), C.c_int32()
+    check(L.hk_exr_read(path.encode(), C.byref(w), C.byref(h), None, 0))
+    out = np.empty((h.value, w.value, 3), np.float32)
+    check(L.hk_exr_read(path.encode(), C.byref(w), C.byref(h), out.ctypes.data, out.size))
+    return out
+
+
+def exr_write(path: str, rgb: np.ndarray) -> None:
+    """Write an H x W x 3 float image as an uncompressed FLOAT RGB OpenEXR."""
+    a = np.ascontiguousarray(rgb, np.float32)
+    check(lib().hk_exr_write(path.encode(), a.shape[1], a.shape[0], a.ctypes.data))
+
+
+def parse_xml_info(path: str):
+    """Parse a scene through the C++ plugin layer without building it (no GPU needed)."""
+    L = lib()
+    h = C.c_void_p()
+    depth, spp = C.c_int32(), C.c_int32()
+    check(L.hk_scene_parse_xml(path.encode(), DATA_DIR.encode(), C.byref(h), C.byref(depth), C.byref(spp)))
+    info = SceneInfo()
+    try:
+        check(L.hk_scene_get_info(h, C.byref(info)))
+    finally:
+        L.hk_scene_destroy(h)
+    return info, depth.value, spp.value
+
+
+__all__ = ["Scene", "SceneDesc", "BSDFDesc", "HikariError", "lib", "scenedesc"]

@@ -1,0 +1,64 @@
+"""Compile the sm_100a CUDA library in-tree (hikari_b200/_build/libhikari_b200.so).
+
+nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo -fmad=false:
+-fmad=false keeps products and sums rounded like the reference's x86 build
+(no FMA contraction); box tests use explicit __fmaf_rn where rounding cannot
+change a result.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_build")
+LIB = os.path.join(OUT_DIR, "libhikari_b200.so")
+SOURCES = ["hk_kernels.cu", "hk_host.cpp", "hk_bvh.cpp", "hk_xml.cpp"]
+HEADERS = ["hk_device.h", "hk_math.cuh", "hk_bsdf.cuh", "hk_traverse.cuh", "hk_shading.cuh", "hk_kernels.h",
+           "hk_bvh.h", "hk_xml.h"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-pthread",
+                     "--expt-relaxed-constexpr"]
+
+
+def _nvcc() -> str:
+    for p in ("/usr/local/cuda/bin/nvcc",):
+        if os.path.exists(p):
+            return p
+    return "nvcc"
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [
+        os.path.join(os.path.dirname(HERE), "include", "hikari_b200.h")]
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if not force and not needs_build():
+        return LIB
+    os.makedirs(OUT_DIR, exist_ok=True)
+    objs = []
+    for src in SOURCES:
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(OUT_DIR, src + ".o")
+        cmd = [_nvcc()] + NVCC_FLAGS + ["-c", path, "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = [_nvcc()] + NVCC_FLAGS + ["-x", "cu", "-c", path, "-o", obj]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.check_call(cmd)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    subprocess.check_call([_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lpthread", "-lz"])
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

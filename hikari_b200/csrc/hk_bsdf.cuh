@@ -1,0 +1,493 @@
+// Device BSDFs of the pathMIS core: diffuse, roughConductor, roughDielectric,
+// roughPlastic and roughCoating (one nesting level), with the Beckmann/GGX
+// microfacet distribution and the 1D rough-transmittance lookups.
+//
+// Each function follows the reference method cited beside it, in the same
+// float evaluation order, so results agree with the reference to the ulp
+// differences of CUDA's expf/logf/sinf/cosf/powf against the host libm.
+#pragma once
+#include "hk_device.h"
+#include "hk_math.cuh"
+
+namespace hk {
+
+struct BRec {
+    V3 wi, wo;
+    float eta;
+    int measure;
+};
+
+// ------------------------------------------------------------ microfacet
+// src/core/MicrofacetDistribution.cpp
+struct Mfd {
+    int type;
+    float au, av;
+};
+__device__ __forceinline__ Mfd mfd_make(int type, float au, float av) {   // ctor :10-26
+    return Mfd{type, clampf(au, 5e-4f, 1.0f), clampf(av, 5e-4f, 1.0f)};
+}
+__device__ __forceinline__ float mfd_eval(const Mfd &d, V3 m) {   // Eval :34
+    if (m.z <= 0.0f) return 0.0f;
+    float c2 = m.z * m.z;
+    float be = ((m.x * m.x) / (d.au * d.au) + (m.y * m.y) / (d.av * d.av)) / c2;
+    float r;
+    if (d.type == kBeckmann) {
+        r = expf(-be) / (kPi * d.au * d.av * c2 * c2);
+    } else {
+        float root = (1.0f + be) * c2;
+        r = 1.0f / (kPi * d.au * d.av * root * root);
+    }
+    if (r * m.z < 1e-20f) r = 0.0f;
+    return r;
+}
+__device__ __forceinline__ float mfd_project_roughness(const Mfd &d, V3 v) {   // :238
+    float inv = 1.0f / sin_theta2(v);
+    if (d.au == d.av || inv <= 0.0f) return d.au;
+    float c2 = v.x * v.x * inv, s2 = v.y * v.y * inv;
+    return sqrtf(c2 * d.au * d.au + s2 * d.av * d.av);
+}
+__device__ __forceinline__ float mfd_g1(const Mfd &d, V3 v, V3 m) {   // SmithG1 :82
+    if (dot(v, m) * v.z <= 0.0f) return 0.0f;
+    float tt = fabsf(tan_theta(v));
+    if (tt == 0.0f) return 1.0f;
+    float a = mfd_project_roughness(d, v);
+    if (d.type == kBeckmann) {
+        float x = 1.0f / (a * tt);
+        if (x >= 1.6f) return 1.0f;
+        float x2 = x * x;
+        return (3.535f * x + 2.181f * x2) / (1.0f + 2.276f * x + 2.577f * x2);
+    }
+    float root = a * tt;
+    return 2.0f / (1.0f + hypot2(1.0f, root));
+}
+__device__ __forceinline__ float mfd_g(const Mfd &d, V3 wi, V3 wo, V3 m) { return mfd_g1(d, wi, m) * mfd_g1(d, wo, m); }
+__device__ __forceinline__ V3 mfd_sample(const Mfd &d, float ux, float uy, float &pdf) {   // SampleAll :148
+    float sp, cp, a2;
+    if (d.au == d.av) {
+        float ph = (2.0f * kPi) * uy;
+        sincosf(ph, &sp, &cp);
+        a2 = d.au * d.au;
+    } else {
+        float ph = atanf(d.av / d.au * tanf(kPi + 2.0f * kPi * uy)) + kPi * floorf(2.0f * uy + 0.5f);
+        sincosf(ph, &sp, &cp);
+        float cs = cp / d.au, ss = sp / d.av;
+        a2 = 1.0f / (cs * cs + ss * ss);
+    }
+    float cm;
+    if (d.type == kBeckmann) {
+        float t2 = a2 * -logf(1.0f - ux);
+        cm = 1.0f / sqrtf(1.0f + t2);
+        pdf = (1.0f - ux) / (kPi * d.au * d.av * cm * cm * cm);
+    } else {
+        float t2 = a2 * ux / (1.0f - ux);
+        cm = 1.0f / sqrtf(1.0f + t2);
+        float tmp = 1.0f + t2 / a2;
+        pdf = (float)kInvPiD / (d.au * d.av * cm * cm * cm * tmp * tmp);
+    }
+    if (pdf < 1e-20f) pdf = 0.0f;
+    float sm = sqrtf(fmaxf(0.0f, 1.0f - cm * cm));
+    return v3(sm * cp, sm * sp, cm);
+}
+__device__ __forceinline__ float mfd_pdf(const Mfd &d, V3 m) { return mfd_eval(d, m) * m.z; }   // PdfAll :231
+
+// ------------------------------------------------------------ fresnel
+// FresnelDielectric (src/core/Common.cpp:494)
+__device__ __forceinline__ float fresnel_dielectric(float ci, float eta, float inv_eta, float &ct) {
+    if (eta == 1.0f) { ct = -ci; return 0.0f; }
+    float sc = (ci > 0.0f) ? inv_eta : eta;
+    float ct2 = 1.0f - (1.0f - ci * ci) * (sc * sc);
+    if (ct2 <= 0.0f) { ct = 0.0f; return 1.0f; }
+    float cii = fabsf(ci), ctt = sqrtf(ct2);
+    float rs = (cii - eta * ctt) / (cii + eta * ctt);
+    float rp = (eta * cii - ctt) / (eta * cii + ctt);
+    ct = (ci > 0.0f) ? -ctt : ctt;
+    return 0.5f * (rs * rs + rp * rp);
+}
+// FresnelConductor (src/core/Common.cpp:529), one channel
+__device__ __forceinline__ float fresnel_conductor1(float ci, float eta, float k) {
+    float ci2 = ci * ci, si2 = 1.0f - ci2;
+    float e2 = eta * eta, k2 = k * k;
+    float t0 = e2 - k2 - si2;
+    float a2b2 = sqrtf(t0 * t0 + 4.0f * e2 * k2);
+    float t1 = a2b2 + ci2;
+    float a = sqrtf(0.5f * (a2b2 + t0));
+    float t2 = 2.0f * ci * a;
+    float rs = (t1 - t2) / (t1 + t2);
+    float t3 = ci2 * a2b2 + si2 * si2;
+    float t4 = t2 * si2;
+    float rp = rs * ((t3 - t4) / (t3 + t4));
+    return 0.5f * (rp + rs);
+}
+__device__ __forceinline__ V3 reflect_m(V3 wi, V3 m) { return m * (2.0f * dot(wi, m)) - wi; }   // :616
+__device__ __forceinline__ V3 refract_m(V3 wi, V3 m, float ct, float eta, float inv_eta) {   // :622
+    float e = (ct < 0.0f ? inv_eta : eta);
+    return m * (dot(wi, m) * e + ct) - wi * e;
+}
+
+// ------------------------------------------------------------ RFT
+// EvalCubicInterpolate1D over [0,1] (src/core/Common.cpp:230) on the activated table
+__device__ __forceinline__ float cubic1d01(float x, const float *val, int size) {
+    if (!(x >= 0.0f && x <= 1.0f)) return 0.0f;
+    float t = ((x - 0.0f) * (size - 1)) / (1.0f - 0.0f);
+    int k = (int)t;
+    k = k > size - 2 ? size - 2 : k;
+    k = k < 0 ? 0 : k;
+    float f0 = __ldg(val + k), f1 = __ldg(val + k + 1), d0, d1;
+    d0 = (k > 0) ? 0.5f * (f1 - __ldg(val + k - 1)) : f1 - f0;
+    d1 = (k + 2 < size) ? 0.5f * (__ldg(val + k + 2) - f0) : f1 - f0;
+    t = t - (float)k;
+    float t2 = t * t, t3 = t2 * t;
+    return (2.0f * t3 - 3.0f * t2 + 1) * f0 + (-2.0f * t3 + 3.0f * t2) * f1 + (t3 - 2.0f * t2 + t) * d0 +
+           (t3 - t2) * d1;
+}
+// RoughTransmittance::Eval with eta and alpha fixed (src/core/RoughTransmitance.cpp:48-70)
+__device__ __forceinline__ float rft_eval(const DevBsdf &b, float c) {
+    float wc = powf(fabsf(c), 0.25f);
+    if (c < 0.0f) return 0.0f;
+    return clampf(cubic1d01(wc, b.rft, b.rft_n), 0.0f, 1.0f);
+}
+
+__device__ __forceinline__ V3 ld_rgb(const float *p) { return v3(p[0], p[1], p[2]); }
+
+// ------------------------------------------------------------ diffuse
+// src/bsdf/DiffuseBSDF.cpp:20-67
+__device__ __forceinline__ V3 diffuse_sample(const DevBsdf &b, BRec &r, float ux, float uy) {
+    if (r.wi.z <= 0) return v3(0, 0, 0);
+    r.measure = kMeasureSolidAngle;
+    r.wo = square_to_cos_hemi(ux, uy);
+    r.eta = 1.0f;
+    return ld_rgb(b.kd);
+}
+__device__ __forceinline__ V3 diffuse_eval(const DevBsdf &b, const BRec &r) {
+    if (r.measure != kMeasureSolidAngle || r.wi.z <= 0 || r.wo.z <= 0) return v3(0, 0, 0);
+    return ld_rgb(b.kd) * (float)kInvPiD;
+}
+__device__ __forceinline__ float diffuse_pdf(const BRec &r) {
+    if (r.measure != kMeasureSolidAngle || r.wi.z <= 0 || r.wo.z <= 0) return 0.0f;
+    return (float)kInvPiD * r.wo.z;
+}
+
+// ------------------------------------------------------------ roughConductor
+// src/bsdf/RoughConductorBSDF.cpp:54-154
+__device__ __forceinline__ Mfd bsdf_mfd(const DevBsdf &b) {
+    return mfd_make(b.distribution, b.alpha_u, b.anisotropic ? b.alpha_v : b.alpha_u);
+}
+__device__ __forceinline__ V3 conductor_fresnel(const DevBsdf &b, float c) {
+    return v3(fresnel_conductor1(c, b.eta_c[0], b.k_c[0]), fresnel_conductor1(c, b.eta_c[1], b.k_c[1]),
+              fresnel_conductor1(c, b.eta_c[2], b.k_c[2]));
+}
+__device__ __forceinline__ V3 conductor_sample(const DevBsdf &b, BRec &r, float ux, float uy) {
+    r.measure = kMeasureSolidAngle;
+    float ci = r.wi.z;
+    if (ci <= 0.0f) return v3(0, 0, 0);
+    Mfd d = bsdf_mfd(b);
+    float pdf;
+    V3 m = mfd_sample(d, ux, uy, pdf);
+    if (pdf == 0.0f) return v3(0, 0, 0);
+    r.wo = reflect_m(r.wi, m);
+    r.eta = 1.0f;
+    if (r.wo.z < 0.0f) return v3(0, 0, 0);
+    float mdw = dot(m, r.wi);
+    V3 F = conductor_fresnel(b, mdw);
+    float G = mfd_g(d, r.wi, r.wo, m);
+    float D = mfd_eval(d, m);
+    float den = pdf * r.wi.z;
+    return v3((((b.ks[0] * F.x) * D) * G) * mdw / den, (((b.ks[1] * F.y) * D) * G) * mdw / den,
+              (((b.ks[2] * F.z) * D) * G) * mdw / den);
+}
+__device__ __forceinline__ V3 conductor_eval(const DevBsdf &b, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (r.measure != kMeasureSolidAngle || ci <= 0.0f || co <= 0.0f) return v3(0, 0, 0);
+    V3 h = normalize(r.wi + r.wo);
+    Mfd d = bsdf_mfd(b);
+    float D = mfd_eval(d, h);
+    if (D == 0.0f) return v3(0, 0, 0);
+    V3 F = conductor_fresnel(b, dot(h, r.wi)) * ld_rgb(b.ks);
+    float G = mfd_g(d, r.wi, r.wo, h);
+    float dg = D * G, den = 4.0f * ci;
+    return v3(dg * F.x / den, dg * F.y / den, dg * F.z / den);
+}
+__device__ __forceinline__ float conductor_pdf(const DevBsdf &b, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (r.measure != kMeasureSolidAngle || ci <= 0.0f || co <= 0.0f) return 0.0f;
+    V3 h = normalize(r.wi + r.wo);
+    Mfd d = bsdf_mfd(b);
+    return mfd_pdf(d, h) / (4.0f * fabsf(dot(h, r.wo)));
+}
+
+// ------------------------------------------------------------ roughDielectric
+// src/bsdf/RoughDielectricBSDF.cpp:57-281.  u1 is the Next1D draw the
+// reference takes from the record's sampler inside Sample (:92).
+__device__ __forceinline__ V3 dielectric_sample(const DevBsdf &b, BRec &r, float ux, float uy, float u1) {
+    r.measure = kMeasureSolidAngle;
+    float ci = r.wi.z;
+    if (ci == 0.0f) return v3(0, 0, 0);
+    Mfd d = bsdf_mfd(b);
+    Mfd sd = d;
+    float s = 1.2f - 0.2f * sqrtf(fabsf(ci));
+    sd.au *= s;
+    sd.av *= s;
+    float pdf;
+    V3 m = mfd_sample(sd, ux, uy, pdf);
+    if (pdf == 0.0f) return v3(0, 0, 0);
+    float ct;
+    float F = fresnel_dielectric(dot(r.wi, m), b.eta, b.inv_eta, ct);
+    bool refl = !(u1 > F);
+    V3 W;
+    if (refl) {
+        r.wo = reflect_m(r.wi, m);
+        r.eta = 1.0f;
+        if (r.wo.z * ci <= 0.0f) return v3(0, 0, 0);
+        W = ld_rgb(b.ks);
+    } else {
+        if (ct == 0.0f) return v3(0, 0, 0);
+        r.wo = refract_m(r.wi, m, ct, b.eta, b.inv_eta);
+        r.eta = (ct < 0.0f ? b.eta : b.inv_eta);
+        if (r.wo.z * ci >= 0.0f) return v3(0, 0, 0);
+        float fac = (ct < 0.0f ? b.inv_eta : b.eta);
+        W = ld_rgb(b.ks_refract) * (fac * fac);
+    }
+    float v = fabsf(mfd_eval(d, m) * mfd_g(d, r.wi, r.wo, m) * dot(r.wi, m) / (pdf * ci));
+    return W * v;
+}
+__device__ __forceinline__ V3 dielectric_eval(const DevBsdf &b, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (r.measure != kMeasureSolidAngle || ci == 0.0f) return v3(0, 0, 0);
+    bool refl = ci * co > 0.0f;
+    float e = ci > 0.0f ? b.eta : b.inv_eta;
+    V3 h = refl ? normalize(r.wi + r.wo) : normalize(r.wi + r.wo * e);
+    h = h * signum(h.z);
+    Mfd d = bsdf_mfd(b);
+    float D = mfd_eval(d, h);
+    if (D == 0.0f) return v3(0, 0, 0);
+    float ct;
+    float F = fresnel_dielectric(dot(r.wi, h), b.eta, b.inv_eta, ct);
+    float G = mfd_g(d, r.wi, r.wo, h);
+    if (refl) return ld_rgb(b.ks) * (F * D * G / (4.0f * fabsf(ci)));
+    float sd = dot(r.wi, h) + e * dot(r.wo, h);
+    float val = ((1.0f - F) * D * G * e * e * dot(r.wi, h) * dot(r.wo, h)) / (ci * sd * sd);
+    float fac = (ci < 0.0f ? b.inv_eta : b.eta);
+    return ld_rgb(b.ks_refract) * fabsf(val * fac * fac);
+}
+__device__ __forceinline__ float dielectric_pdf(const DevBsdf &b, const BRec &r) {
+    if (r.measure != kMeasureSolidAngle) return 0.0f;
+    float ci = r.wi.z, co = r.wo.z;
+    if (ci == 0.0f || co == 0.0f) return 0.0f;
+    bool refl = ci * co > 0.0f;
+    V3 h;
+    float J;
+    if (refl) {
+        h = normalize(r.wi + r.wo);
+        J = 1.0f / (4.0f * dot(r.wo, h));
+    } else {
+        float e = ci > 0.0f ? b.eta : b.inv_eta;
+        h = normalize(r.wi + r.wo * e);
+        float sd = dot(r.wi, h) + e * dot(r.wo, h);
+        J = (e * e * dot(r.wo, h)) / (sd * sd);
+    }
+    h = h * signum(h.z);
+    Mfd d = bsdf_mfd(b);
+    float s = 1.2f - 0.2f * sqrtf(fabsf(ci));
+    d.au *= s;
+    d.av *= s;
+    float ct;
+    float F = fresnel_dielectric(dot(r.wi, h), b.eta, b.inv_eta, ct);
+    float pdf = mfd_pdf(d, h) * (refl ? F : (1.0f - F));
+    return fabsf(pdf * J);
+}
+
+// ------------------------------------------------------------ roughPlastic
+// src/bsdf/RoughPlasticBSDF.cpp:66-192
+__device__ __forceinline__ V3 plastic_eval(const DevBsdf &b, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (r.measure == kMeasureUnknown || ci <= 0.0f || co <= 0.0f) return v3(0, 0, 0);
+    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    float ct;
+    V3 h = normalize(r.wi + r.wo);
+    float D = mfd_eval(d, h);
+    float F = fresnel_dielectric(dot(r.wi, h), b.eta, b.inv_eta, ct);
+    float G = mfd_g(d, r.wi, r.wi, h);   // G(Wi, Wi, H) as the reference does (:146)
+    float val = F * D * G / (4.0f * ci);
+    V3 res = ld_rgb(b.ks) * val;
+    V3 dif = ld_rgb(b.kd);
+    float t12 = rft_eval(b, ci), t21 = rft_eval(b, co);
+    float fdr = b.fdr_int;
+    if (b.nonlinear) dif = v3(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
+    else dif = dif / (1.0f - fdr);
+    // INV_PI is a double literal in the reference: the scalar is formed in double
+    float k = (float)(kInvPiD * co * t12 * t21 * b.inv_eta2);
+    return res + dif * k;
+}
+__device__ __forceinline__ float plastic_spec_pdf(const DevBsdf &b, float ci) {
+    float sp = 1.0f - rft_eval(b, ci);
+    return (sp * b.spec_w) / (sp * b.spec_w + (1.0f - sp) * (1.0f - b.spec_w));
+}
+__device__ __forceinline__ float plastic_pdf(const DevBsdf &b, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (r.measure == kMeasureUnknown || ci <= 0.0f || co <= 0.0f) return 0.0f;
+    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    V3 h = normalize(r.wi + r.wo);
+    float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
+    float J = 1.0f / (4.0f * dot(r.wo, h));
+    float res = mfd_pdf(d, h) * J * sp;
+    res += dp * cos_hemi_pdf(r.wo);
+    return res;
+}
+__device__ __forceinline__ V3 plastic_sample(const DevBsdf &b, BRec &r, float ux, float uy) {
+    float ci = r.wi.z;
+    if (ci <= 0.0f) return v3(0, 0, 0);
+    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
+    bool spec;
+    if (uy < sp) { uy /= sp; spec = true; }
+    else { uy = (uy - sp) / (1.0f - sp); spec = false; }
+    if (spec) {
+        float pdf;
+        V3 m = mfd_sample(d, ux, uy, pdf);
+        r.wo = reflect_m(r.wi, m);
+        r.measure = kMeasureDiscrete;
+    } else {
+        r.wo = square_to_cos_hemi(ux, uy);
+        r.measure = kMeasureSolidAngle;
+    }
+    r.eta = 1.0f;
+    V3 h = normalize(r.wi + r.wo);
+    float J = 1.0f / (4.0f * dot(r.wo, h));
+    float P = mfd_pdf(d, h) * J * sp + dp * cos_hemi_pdf(r.wo);
+    if (P == 0.0f) return v3(0, 0, 0);
+    return plastic_eval(b, r) / P;
+}
+
+// ------------------------------------------------------------ dispatch (leaf BSDFs)
+__device__ __forceinline__ V3 leaf_eval(const DevBsdf &b, const BRec &r) {
+    switch (b.type) {
+    case kDiffuse: return diffuse_eval(b, r);
+    case kRoughConductor: return conductor_eval(b, r);
+    case kRoughDielectric: return dielectric_eval(b, r);
+    default: return plastic_eval(b, r);
+    }
+}
+__device__ __forceinline__ float leaf_pdf(const DevBsdf &b, const BRec &r) {
+    switch (b.type) {
+    case kDiffuse: return diffuse_pdf(r);
+    case kRoughConductor: return conductor_pdf(b, r);
+    case kRoughDielectric: return dielectric_pdf(b, r);
+    default: return plastic_pdf(b, r);
+    }
+}
+__device__ __forceinline__ V3 leaf_sample(const DevBsdf &b, BRec &r, float ux, float uy, float u1) {
+    switch (b.type) {
+    case kDiffuse: return diffuse_sample(b, r, ux, uy);
+    case kRoughConductor: return conductor_sample(b, r, ux, uy);
+    case kRoughDielectric: return dielectric_sample(b, r, ux, uy, u1);
+    default: return plastic_sample(b, r, ux, uy);
+    }
+}
+
+// ------------------------------------------------------------ roughCoating
+// src/bsdf/RoughCoatingBSDF.cpp:62-385 over one nested leaf BSDF
+__device__ __forceinline__ V3 coat_refract(V3 wi, float inv_eta) {   // RefractIn :347 / RefractOut :367
+    bool entering = wi.z > 0.0f;
+    float st2 = inv_eta * inv_eta * sin_theta2(wi);
+    if (st2 >= 1.0f) return v3(0, 0, 0);
+    float ct = sqrtf(1.0f - st2);
+    return v3(inv_eta * wi.x, inv_eta * wi.y, entering ? ct : -ct);
+}
+__device__ __forceinline__ V3 coating_eval(const DevBsdf &b, const DevBsdf &nb, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (ci * co <= 0.0f) return v3(0, 0, 0);
+    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    V3 h = normalize(r.wi + r.wo) * signum(r.wo.z);
+    float ct;
+    float D = mfd_eval(d, h);
+    float F = fresnel_dielectric(fabsf(dot(r.wi, h)), b.eta, b.inv_eta, ct);
+    float G = mfd_g(d, r.wi, r.wo, h);
+    float den = 4.0f * fabsf(ci);
+    V3 res = v3((((b.ks[0] * F) * D) * G) / den, (((b.ks[1] * F) * D) * G) / den, (((b.ks[2] * F) * D) * G) / den);
+    BRec ri = r;
+    ri.wi = coat_refract(r.wi, b.inv_eta);
+    ri.wo = coat_refract(r.wo, b.inv_eta);
+    V3 nv = leaf_eval(nb, ri);
+    float ti = rft_eval(b, fabsf(ci)), to = rft_eval(b, fabsf(co));
+    nv = v3(nv.x * ti * to, nv.y * ti * to, nv.z * ti * to);
+    V3 sa = ld_rgb(b.sigma_a) * b.thickness;
+    if (!is_zero(sa)) {
+        float q = 1.0f / fabsf(ri.wi.z) + 1.0f / fabsf(ri.wo.z);
+        nv = nv * v3(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q));
+    }
+    if (r.measure == kMeasureSolidAngle) nv = nv * (b.inv_eta * b.inv_eta * r.wo.z / ri.wo.z);
+    return res + nv;
+}
+__device__ __forceinline__ float coating_pdf(const DevBsdf &b, const DevBsdf &nb, const BRec &r) {
+    V3 h = normalize(r.wi + r.wo) * signum(r.wo.z);
+    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    float ci = r.wi.z, co = r.wo.z;
+    float r12 = 1.0f - rft_eval(b, fabsf(ci));
+    float sp = (r12 * b.spec_w) / (r12 * b.spec_w + (1.0f - r12) * (1.0f - b.spec_w));
+    float np = 1.0f - sp;
+    float res = 0.0f;
+    if (ci * co > 0.0f) {
+        float J = 1.0f / (4.0f * fabsf(dot(r.wo, h)));
+        res = mfd_pdf(d, h) * J * sp;
+    }
+    BRec ri = r;
+    ri.wi = coat_refract(r.wi, b.inv_eta);
+    ri.wo = coat_refract(r.wo, b.inv_eta);
+    float p = leaf_pdf(nb, ri);
+    if (ri.measure == kMeasureSolidAngle) p *= b.inv_eta * b.inv_eta * co / ri.wo.z;
+    return res + p * np;
+}
+__device__ __forceinline__ V3 coating_sample(const DevBsdf &b, const DevBsdf &nb, BRec &r, float ux, float uy, float u1) {
+    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    float aci = fabsf(r.wi.z);
+    float r12 = 1.0f - rft_eval(b, aci);
+    float sp = (r12 * b.spec_w) / (r12 * b.spec_w + (1.0f - r12) * (1.0f - b.spec_w));
+    bool spec;
+    if (ux < sp) { spec = true; ux /= sp; }
+    else { spec = false; ux = (ux - sp) / (1.0f - sp); }
+    if (spec) {
+        float pdf;
+        V3 m = mfd_sample(d, ux, uy, pdf);
+        r.wo = reflect_m(r.wi, m);
+        r.measure = kMeasureDiscrete;
+        r.eta = 1.0f;
+        if (r.wo.z * r.wo.z <= 0.0f) return v3(0, 0, 0);
+    } else {
+        V3 wib = r.wi;
+        r.wi = coat_refract(r.wi, b.inv_eta);
+        V3 res = leaf_sample(nb, r, ux, uy, u1);
+        r.wi = wib;
+        if (is_zero(res)) return v3(0, 0, 0);
+        r.wo = coat_refract(r.wo, b.eta);
+        if (is_zero(r.wo)) return v3(0, 0, 0);
+    }
+    float P = coating_pdf(b, nb, r);
+    if (P == 0.0f) return v3(0, 0, 0);
+    return coating_eval(b, nb, r) / P;
+}
+
+// ------------------------------------------------------------ full dispatch
+__device__ __forceinline__ V3 bsdf_eval(const DevBsdf *bs, int id, const BRec &r) {
+    const DevBsdf &b = bs[id];
+    if (b.type == kRoughCoating) return coating_eval(b, bs[b.nested], r);
+    return leaf_eval(b, r);
+}
+__device__ __forceinline__ float bsdf_pdf(const DevBsdf *bs, int id, const BRec &r) {
+    const DevBsdf &b = bs[id];
+    if (b.type == kRoughCoating) return coating_pdf(b, bs[b.nested], r);
+    return leaf_pdf(b, r);
+}
+// u1 is consumed only by a roughDielectric (top-level or nested); the caller
+// draws it lazily through needs_u1().
+__device__ __forceinline__ bool needs_u1(const DevBsdf *bs, int id) {
+    const DevBsdf &b = bs[id];
+    if (b.type == kRoughDielectric) return true;
+    return b.type == kRoughCoating && bs[b.nested].type == kRoughDielectric;
+}
+__device__ __forceinline__ V3 bsdf_sample(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1) {
+    const DevBsdf &b = bs[id];
+    if (b.type == kRoughCoating) return coating_sample(b, bs[b.nested], r, ux, uy, u1);
+    return leaf_sample(b, r, ux, uy, u1);
+}
+
+}  // namespace hk

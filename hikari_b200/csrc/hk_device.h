@@ -1,0 +1,107 @@
+// Device-resident scene layout shared by the host builder (hk_host.cpp) and the
+// sm_100a kernels.  Everything here lives in HBM and is read through the
+// read-only path; record sizes are multiples of 16 bytes so every fetch is a
+// 128-bit load.
+#pragma once
+#include <cstdint>
+#include <vector_types.h>
+
+namespace hk {
+
+enum BsdfType : int32_t { kDiffuse = 0, kRoughConductor = 1, kRoughDielectric = 2, kRoughPlastic = 3, kRoughCoating = 4 };
+enum Distribution : int32_t { kBeckmann = 0, kGGX = 1 };
+enum Measure : int32_t { kMeasureUnknown = 0, kMeasureSolidAngle = 1, kMeasureDiscrete = 2 };
+
+constexpr int kRftThetaMax = 100;   // data/*RFTData.bin hold 100 theta samples
+
+// One activated BSDF: constant-texture parameters plus the 1D rough
+// transmittance table reduced at activation (RoughTransmittance::SetEta then
+// SetAlpha, src/core/RoughTransmitance.cpp:170,237).
+struct alignas(16) DevBsdf {
+    int32_t type, distribution, anisotropic, nonlinear;
+    float alpha_u, alpha_v;          // clamped to [MIN_ALPHA, MAX_ALPHA]
+    float eta, inv_eta;              // intIOR / extIOR and its inverse
+    float inv_eta2;
+    float spec_w;                    // m_SpecularSamplingWeight
+    float fdr_int;                   // roughPlastic: 1 - IntData.EvalDiffuse(alpha)
+    float thickness;
+    float eta_c[3], k_c[3];          // conductor eta and k/extIOR per channel
+    float ks[3], ks_refract[3], kd[3], sigma_a[3];
+    int32_t nested;                  // roughCoating nested BSDF index, -1 otherwise
+    int32_t rft_n;                   // theta samples in rft[]
+    int32_t pad0, pad1;
+    float rft[kRftThetaMax];
+};
+
+// Per-mesh shading data.
+struct alignas(16) DevMesh {
+    int32_t bsdf;          // DevBsdf index
+    int32_t emitter;       // emitter index or -1
+    int32_t has_normals;   // vertex normals present -> interpolated shading frame
+    int32_t pad;
+    float radiance[3];     // area emitter radiance
+    float pad1;
+};
+
+// Area emitter: triangles of its mesh in mesh order with the area CDF
+// (DiscretePDF1D over triangle areas, src/core/Mesh.cpp:233).
+struct alignas(16) DevAreaLight {
+    uint32_t tri0;         // first record in DevScene::light_tris (3 float4 per triangle)
+    uint32_t ntri;
+    uint32_t cdf0;         // first entry in DevScene::light_cdf (ntri+1 floats)
+    int32_t mesh;
+    float inv_area;
+    float radiance[3];
+};
+
+// BVH2 node: both children's boxes, 64 bytes = 4 x 128-bit loads.
+//   a = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   d = (child0, child1, -, -) as int; child < 0 -> leaf ~(start | count << 27)
+constexpr int kLeafCountShift = 27;
+constexpr uint32_t kLeafStartMask = (1u << kLeafCountShift) - 1u;
+
+struct DevScene {
+    // geometry: triangle records in BVH leaf order, 3 float4 each:
+    //   v0.xyz, bits(original triangle index); v1.xyz, bits(mesh); v2.xyz, 0
+    const float4 *tris;
+    const float4 *nodes;          // 4 float4 per BVH2 node
+    const float4 *tri_normals;    // 3 float4 per ORIGINAL triangle (only if any mesh has normals)
+    uint32_t ntris, nnodes;
+    const DevMesh *meshes;
+    const DevBsdf *bsdfs;
+    int32_t nmeshes, nbsdfs;
+    // emitters in Scene order; env is the one with area index -1
+    int32_t nemitters;
+    int32_t env_index;            // position of the environment emitter, -1 if none
+    const int32_t *emitter_area;  // per emitter: index into area_lights or -1 (env)
+    const DevAreaLight *area_lights;
+    const float4 *light_tris;     // emitter triangles, 3 float4 each (v0, v1, v2)
+    const float4 *light_normals;  // matching vertex normals (w = has normals)
+    const float *light_cdf;
+    // environment map
+    const float4 *env_rgb;        // H*W texels (rgb, 0)
+    const float *env_marg_cdf;    // H+1
+    const float *env_marg_func;   // H
+    const float *env_cond_cdf;    // H*(W+1)
+    const float *env_cond_func;   // H*W
+    const float *env_cond_int;    // H row integrals
+    float env_marg_int;
+    uint32_t env_w, env_h;
+    float env_scale;
+    float env_to_world[9], env_to_local[9];
+    float scene_radius;           // BoundingBox::GetRadius of the accel bbox
+    // camera (PerspectiveCamera, src/camera/PerspectiveCamera.cpp:32-100)
+    float cam[12];                // row-major 3x4 camera-to-world (rows of the 4x4 divided by w)
+    float cam_cot, cam_aspect, cam_near, cam_far;
+    uint32_t width, height;
+    // reconstruction filter table (ImageBlock ctor, src/core/Block.cpp:9)
+    const float *ftab;            // 33 entries in HBM (dynamic index)
+    float filt_radius, filt_lookup;
+    int32_t border;
+    float background[3];
+    int32_t force_background;
+};
+
+}  // namespace hk

@@ -1,0 +1,917 @@
+// Host side of the B200 pathMIS core: scene assembly, object activation
+// (BSDF tables, light CDFs, camera, filter), the BVH build and the C ABI of
+// include/hikari_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/hikari_b200.h"
+#include "hk_bvh.h"
+#include "hk_device.h"
+#include "hk_kernels.h"
+
+extern "C" int hk_scene_load_xml_impl(const char *path, const char *data_dir, hk_scene **out, int32_t *depth,
+                                      int32_t *spp, int build, std::string *err);
+extern "C" int hk_exr_read_impl(const char *path, int *w, int *h, std::vector<float> *rgb, std::string *err);
+extern "C" int hk_exr_write_impl(const char *path, int w, int h, const float *rgb, std::string *err);
+
+namespace {
+
+thread_local std::string g_error;
+
+int set_error(int code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+struct HkError {
+    int code;
+    std::string msg;
+};
+#define HK_CUDA(call)                                                                                   \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess)                                                                          \
+            throw HkError{e_ == cudaErrorMemoryAllocation ? HK_ERR_NOMEM : HK_ERR_CUDA,                 \
+                          std::string(#call) + ": " + cudaGetErrorString(e_)};                          \
+    } while (0)
+
+template <class F>
+int guarded(F &&f) {
+    try {
+        return f();
+    } catch (const HkError &e) {
+        return set_error(e.code, e.msg);
+    } catch (const std::bad_alloc &) {
+        return set_error(HK_ERR_NOMEM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return set_error(HK_ERR_INVALID, e.what());
+    }
+}
+
+// ------------------------------------------------------------ float helpers
+// Host 3-vectors in the reference's Eigen evaluation order: x + (y + z).
+struct F3 {
+    float x, y, z;
+};
+inline F3 f3sub(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline F3 f3cross(F3 a, F3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline float f3dot(F3 a, F3 b) { return a.x * b.x + (a.y * b.y + a.z * b.z); }
+inline float f3norm(F3 a) { return std::sqrt(f3dot(a, a)); }
+inline float lum(const float *c) { return c[0] * 0.212671f + c[1] * 0.715160f + c[2] * 0.072169f; }
+inline float clampf(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// DiscretePDF1D ctor (src/core/DiscretePDF.cpp:5): cdf in float, normalised.
+struct Pdf1D {
+    std::vector<float> func, cdf;
+    float integral = 0.0f;
+    void build(const float *f, int n) {
+        func.assign(f, f + n);
+        cdf.assign(n + 1, 0.0f);
+        for (int i = 1; i < n + 1; i++) cdf[i] = cdf[i - 1] + func[i - 1] / n;
+        integral = cdf[n];
+        if (integral == 0.0f) {
+            for (int i = 1; i < n + 1; i++) cdf[i] = float(i) / float(n);
+        } else {
+            for (int i = 1; i < n + 1; i++) cdf[i] /= integral;
+        }
+    }
+};
+
+// ------------------------------------------------------------ RFT activation
+// EvalCubicInterpolate1D/2D/3D (src/core/Common.cpp:230-464) restricted to
+// the [0,1] domains the rough transmittance tables use.
+float cubic1d(float x, const float *val, int size, float mn, float mx) {
+    if (!(x >= mn && x <= mx)) return 0.0f;
+    float t = ((x - mn) * (size - 1)) / (mx - mn);
+    int k = std::max(0, std::min(int(t), size - 2));
+    float f0 = val[k], f1 = val[k + 1];
+    float d0 = (k > 0) ? 0.5f * (val[k + 1] - val[k - 1]) : val[k + 1] - val[k];
+    float d1 = (k + 2 < size) ? 0.5f * (val[k + 2] - val[k]) : val[k + 1] - val[k];
+    t = t - float(k);
+    float t2 = t * t, t3 = t2 * t;
+    return (2.0f * t3 - 3.0f * t2 + 1) * f0 + (-2.0f * t3 + 3.0f * t2) * f1 + (t3 - 2.0f * t2 + t) * d0 + (t3 - t2) * d1;
+}
+bool knot_weights(float p, int size, float *w, int &knot) {
+    if (!(p >= 0.0f && p <= 1.0f)) return false;
+    float t = ((p - 0.0f) * float(size - 1)) / (1.0f - 0.0f);
+    knot = std::min(int(t), size - 2);
+    t = t - float(knot);
+    float t2 = t * t, t3 = t2 * t;
+    w[0] = 0.0f;
+    w[1] = 2.0f * t3 - 3.0f * t2 + 1;
+    w[2] = -2.0f * t3 + 3.0f * t2;
+    w[3] = 0.0f;
+    float d0 = t3 - 2.0f * t2 + t, d1 = t3 - t2;
+    if (knot > 0) { w[2] += 0.5f * d0; w[0] -= 0.5f * d0; }
+    else { w[2] += d0; w[1] -= d0; }
+    if (knot + 2 < size) { w[3] += 0.5f * d1; w[1] -= 0.5f * d1; }
+    else { w[2] += d1; w[1] -= d1; }
+    return true;
+}
+float cubic2d(float px, float py, const float *val, int sx, int sy) {
+    float w[2][4];
+    int k[2];
+    if (!knot_weights(px, sx, w[0], k[0]) || !knot_weights(py, sy, w[1], k[1])) return 0.0f;
+    float r = 0.0f;
+    for (int y = -1; y <= 2; y++) {
+        float wy = w[1][y + 1];
+        for (int x = -1; x <= 2; x++) {
+            float wxy = w[0][x + 1] * wy;
+            if (wxy == 0) continue;
+            r += val[(k[1] + y) * sx + k[0] + x] * wxy;
+        }
+    }
+    return r;
+}
+float cubic3d(float px, float py, float pz, const float *val, int sx, int sy, int sz) {
+    float w[3][4];
+    int k[3];
+    if (!knot_weights(px, sx, w[0], k[0]) || !knot_weights(py, sy, w[1], k[1]) || !knot_weights(pz, sz, w[2], k[2]))
+        return 0.0f;
+    float r = 0.0f;
+    for (int z = -1; z <= 2; z++) {
+        float wz = w[2][z + 1];
+        for (int y = -1; y <= 2; y++) {
+            float wyz = w[1][y + 1] * wz;
+            for (int x = -1; x <= 2; x++) {
+                float wxyz = w[0][x + 1] * wyz;
+                if (wxyz == 0) continue;
+                r += val[((k[2] + z) * sy + (k[1] + y)) * sx + k[0] + x] * wxyz;
+            }
+        }
+    }
+    return r;
+}
+
+struct RftTable {
+    uint64_t eta_n = 0, alpha_n = 0, theta_n = 0, t_size = 0, d_size = 0;
+    float eta_min = 0, eta_max = 0, alpha_min = 0, alpha_max = 0;
+    std::vector<float> trans, diff;
+    bool loaded = false;
+
+    // RoughTransmittance ctor (src/core/RoughTransmitance.cpp:9): header then data
+    void parse(const void *bytes, uint64_t n) {
+        const unsigned char *b = (const unsigned char *)bytes;
+        if (n < 56) throw HkError{HK_ERR_IO, "RFT table: short header"};
+        uint64_t h[5];
+        float f[4];
+        std::memcpy(h, b, 40);
+        std::memcpy(f, b + 40, 16);
+        eta_n = h[0]; alpha_n = h[1]; theta_n = h[2]; t_size = h[3]; d_size = h[4];
+        eta_min = f[0]; eta_max = f[1]; alpha_min = f[2]; alpha_max = f[3];
+        if (theta_n > (uint64_t)hk::kRftThetaMax || theta_n < 2 || alpha_n < 2 || eta_n < 2)
+            throw HkError{HK_ERR_IO, "RFT table: unsupported dimensions"};
+        if (t_size != eta_n * alpha_n * theta_n * 2 || d_size != eta_n * alpha_n * 2)
+            throw HkError{HK_ERR_IO, "RFT table: inconsistent sizes"};
+        if (56 + 4 * (t_size + d_size) > n) throw HkError{HK_ERR_IO, "RFT table: short body"};
+        trans.resize(t_size);
+        diff.resize(d_size);
+        std::memcpy(trans.data(), b + 56, 4 * t_size);
+        std::memcpy(diff.data(), b + 56 + 4 * t_size, 4 * d_size);
+        loaded = true;
+    }
+    // SetEta (src/core/RoughTransmitance.cpp:170)
+    void set_eta(float eta, std::vector<float> &t2d, std::vector<float> &d1d) const {
+        const float *pt = trans.data(), *pd = diff.data();
+        int E = (int)eta_n, A = (int)alpha_n, T = (int)theta_n;
+        if (eta < 1.0f) { pt += (uint64_t)E * A * T; pd += (uint64_t)E * A; eta = 1.0f / eta; }
+        if (eta < eta_min) eta = eta_min;
+        float we = std::pow((eta - eta_min) / (eta_max - eta_min), 0.25f);
+        float da = 1.0f / (A - 1.0f), dt = 1.0f / (T - 1.0f);
+        t2d.assign((size_t)A * T, 0.0f);
+        d1d.assign(A, 0.0f);
+        for (int i = 0; i < A; i++) {
+            for (int j = 0; j < T; j++) t2d[i * T + j] = cubic3d(j * dt, i * da, we, pt, T, A, E);
+            d1d[i] = cubic2d(i * da, we, pd, A, E);
+        }
+    }
+    // SetAlpha (src/core/RoughTransmitance.cpp:237)
+    void set_alpha(const std::vector<float> &t2d, const std::vector<float> &d1d, float alpha, float *t1d,
+                   float &dscalar) const {
+        int A = (int)alpha_n, T = (int)theta_n;
+        float wa = std::pow((alpha - alpha_min) / (alpha_max - alpha_min), 0.25f);
+        float dt = 1.0f / (T - 1.0f);
+        for (int i = 0; i < T; i++) t1d[i] = cubic2d(i * dt, wa, t2d.data(), T, A);
+        dscalar = cubic1d(wa, d1d.data(), A, 0.0f, 1.0f);
+    }
+};
+
+// ------------------------------------------------------------ device buffers
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void alloc(size_t n) {
+        release();
+        if (n == 0) n = 16;
+        HK_CUDA(cudaMalloc(&p, n));
+        bytes = n;
+    }
+    template <class T>
+    void upload(const std::vector<T> &v) {
+        alloc(v.size() * sizeof(T));
+        if (!v.empty()) HK_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+    template <class T>
+    T *as() const { return (T *)p; }
+};
+
+struct MeshIn {
+    std::vector<float> pos, nrm;
+    std::vector<uint32_t> idx;
+    int32_t bsdf;
+    bool emitter;
+    float radiance[3];
+};
+
+}  // namespace
+
+struct hk_scene {
+    // inputs
+    std::vector<hk_bsdf_desc> bsdfs;
+    std::vector<MeshIn> meshes;
+    std::vector<int> emitter_mesh;   // Scene order; -1 = environment
+    RftTable rft[2];
+    bool has_env = false;
+    uint32_t env_w = 0, env_h = 0;
+    std::vector<float> env_rgb;
+    float env_to_world[16];
+    float env_scale = 1.0f;
+    uint32_t width = 1280, height = 720;
+    float cam_to_world[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    float fov = 30.0f, near_clip = 1e-4f, far_clip = 1e4f;
+    int filt_kind = 2;
+    float filt_r = 2.0f, filt_p0 = 0.5f, filt_p1 = 0.0f;
+    float background[3] = {0, 0, 0};
+    int force_background = 0;
+    // built state
+    bool built = false;
+    hk::DevScene dev{};
+    DevBuf b_tris, b_nodes, b_tri_normals, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
+        b_light_cdf, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
+    DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
+    hk_scene_info info{};
+    int margin_lo = 0, margin_hi = 0;
+    int sm_count = 148;
+    int occupancy = 1;
+};
+
+namespace {
+
+float filter_eval(const hk_scene *s, float x) {   // src/filter/*.cpp Eval
+    switch (s->filt_kind) {
+    case 0: return 1.0f;
+    case 1: return std::max(0.0f, 1.0f - std::abs(x));
+    case 2: {
+        float a = -1.0f / (2.0f * s->filt_p0 * s->filt_p0);
+        return std::max(0.0f, std::exp(a * x * x) - std::exp(a * s->filt_r * s->filt_r));
+    }
+    default: {
+        float B = s->filt_p0, C = s->filt_p1;
+        x = std::abs(2.0f * x / s->filt_r);
+        float x2 = x * x, x3 = x2 * x;
+        if (x < 1.0f)
+            return 1.0f / 6.0f * ((12.0f - 9.0f * B - 6.0f * C) * x3 + (-18.0f + 12.0f * B + 6.0f * C) * x2 + (6.0f - 2.0f * B));
+        if (x < 2.0f)
+            return 1.0f / 6.0f * ((-B - 6 * C) * x3 + (6.0f * B + 30.0f * C) * x2 + (-12.0f * B - 48.0f * C) * x + (8.0f * B + 24.0f * C));
+        return 0.0f;
+    }
+    }
+}
+
+void mat3_inverse(const float *m, float *o) {
+    double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5], g = m[6], h = m[7], i = m[8];
+    double det = a * (e * i - f * h) - b * (d * i - f * g) + c * (d * h - e * g);
+    if (det == 0.0) throw HkError{HK_ERR_INVALID, "environment toWorld is singular"};
+    o[0] = float((e * i - f * h) / det); o[1] = float((c * h - b * i) / det); o[2] = float((b * f - c * e) / det);
+    o[3] = float((f * g - d * i) / det); o[4] = float((a * i - c * g) / det); o[5] = float((c * d - a * f) / det);
+    o[6] = float((d * h - e * g) / det); o[7] = float((b * g - a * h) / det); o[8] = float((a * e - b * d) / det);
+}
+
+// Activation of one BSDF (RoughPlasticBSDF::Activate :261, RoughCoatingBSDF::Activate :315)
+hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs) {
+    hk::DevBsdf b;
+    std::memset(&b, 0, sizeof b);
+    if (d.type < 0 || d.type > 4) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+    if (d.distribution != 0 && d.distribution != 1) throw HkError{HK_ERR_INVALID, "Unexpected distribution type"};
+    b.type = d.type;
+    b.distribution = d.distribution;
+    b.anisotropic = d.anisotropic;
+    b.nonlinear = d.nonlinear;
+    b.alpha_u = clampf(d.alpha_u, 5e-4f, 1.0f);
+    b.alpha_v = clampf(d.alpha_v, 5e-4f, 1.0f);
+    b.eta = d.int_ior / d.ext_ior;
+    b.inv_eta = 1.0f / b.eta;
+    b.inv_eta2 = b.inv_eta * b.inv_eta;
+    b.thickness = d.thickness;
+    for (int c = 0; c < 3; c++) {
+        b.eta_c[c] = d.eta[c];
+        b.k_c[c] = d.k[c] / d.ext_ior;
+        b.ks[c] = d.ks[c];
+        b.ks_refract[c] = d.ks_refract[c];
+        b.kd[c] = d.kd[c];
+        b.sigma_a[c] = d.sigma_a[c];
+    }
+    b.nested = d.nested;
+    if (d.type == hk::kRoughPlastic || d.type == hk::kRoughCoating) {
+        const RftTable &t = s->rft[d.distribution];
+        if (!t.loaded) throw HkError{HK_ERR_INVALID, "RFT table for the BSDF's distribution was not set"};
+        float alpha = b.alpha_u;
+        float e = b.eta < 1.0f ? 1.0f / b.eta : b.eta;   // CheckEta / CheckAlpha (:315-345)
+        if (e < t.eta_min || e > t.eta_max) throw HkError{HK_ERR_INVALID, "relative IOR outside the RFT table range"};
+        if (alpha < t.alpha_min || alpha > t.alpha_max) throw HkError{HK_ERR_INVALID, "alpha outside the RFT range"};
+        std::vector<float> t2d, d1d;
+        float dsc;
+        t.set_eta(b.eta, t2d, d1d);
+        t.set_alpha(t2d, d1d, alpha, b.rft, dsc);
+        b.rft_n = (int)t.theta_n;
+        if (d.type == hk::kRoughPlastic) {
+            float ksa = lum(d.ks), kda = lum(d.kd);
+            b.spec_w = ksa / (kda + ksa);
+            t.set_eta(b.inv_eta, t2d, d1d);   // m_pIntData: SetEta(1/eta) only
+            float wa = std::pow((alpha - t.alpha_min) / (t.alpha_max - t.alpha_min), 0.25f);
+            b.fdr_int = 1.0f - clampf(cubic1d(wa, d1d.data(), (int)t.alpha_n, 0.0f, 1.0f), 0.0f, 1.0f);
+        } else {
+            float th = d.thickness;
+            float a0 = std::exp(d.sigma_a[0] * (-2.0f * th)), a1 = std::exp(d.sigma_a[1] * (-2.0f * th)),
+                  a2 = std::exp(d.sigma_a[2] * (-2.0f * th));
+            b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
+            if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
+            if (s->bsdfs[d.nested].type == hk::kRoughCoating)
+                throw HkError{HK_ERR_INVALID, "roughCoating nested in roughCoating is not supported"};
+        }
+    }
+    return b;
+}
+
+void build_scene(hk_scene *s) {
+    if (s->meshes.empty()) throw HkError{HK_ERR_INVALID, "scene has no meshes"};
+    if (s->width == 0 || s->height == 0) throw HkError{HK_ERR_INVALID, "camera has an empty film"};
+    hk::DevScene &D = s->dev;
+    std::memset(&D, 0, sizeof D);
+    size_t dev_bytes = 0;
+    auto track = [&](DevBuf &b) { dev_bytes += b.bytes; };
+
+    // BSDFs
+    std::vector<hk::DevBsdf> bs;
+    for (auto &d : s->bsdfs) bs.push_back(activate_bsdf(s, d, (int)s->bsdfs.size()));
+    s->b_bsdfs.upload(bs); track(s->b_bsdfs);
+    D.bsdfs = s->b_bsdfs.as<hk::DevBsdf>();
+    D.nbsdfs = (int)bs.size();
+
+    // meshes, global triangles
+    std::vector<hk::DevMesh> dm;
+    uint64_t ntris = 0;
+    bool any_normals = false;
+    for (auto &m : s->meshes) ntris += m.idx.size() / 3;
+    if (ntris >= (1ull << hk::kLeafCountShift)) throw HkError{HK_ERR_INVALID, "too many triangles"};
+    std::vector<float> P;       // 9 floats per triangle (original order)
+    std::vector<int32_t> tmesh;
+    P.reserve(ntris * 9);
+    tmesh.reserve(ntris);
+    std::vector<float> tri_normals;   // 12 floats per triangle (3 float4) if any normals
+    for (auto &m : s->meshes) any_normals |= !m.nrm.empty();
+    if (any_normals) tri_normals.resize(ntris * 12, 0.0f);
+    float bb[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    std::vector<int> mesh_emitter(s->meshes.size(), -1);
+    for (size_t e = 0; e < s->emitter_mesh.size(); ++e)
+        if (s->emitter_mesh[e] >= 0) mesh_emitter[s->emitter_mesh[e]] = (int)e;
+    uint64_t t = 0;
+    for (size_t mi = 0; mi < s->meshes.size(); ++mi) {
+        auto &m = s->meshes[mi];
+        hk::DevMesh d;
+        std::memset(&d, 0, sizeof d);
+        if (m.bsdf < 0 || m.bsdf >= (int)bs.size()) throw HkError{HK_ERR_INVALID, "mesh has an invalid BSDF id"};
+        d.bsdf = m.bsdf;
+        d.emitter = mesh_emitter[mi];
+        d.has_normals = !m.nrm.empty();
+        for (int c = 0; c < 3; c++) d.radiance[c] = m.radiance[c];
+        dm.push_back(d);
+        size_t nv = m.pos.size() / 3;
+        for (size_t v = 0; v < nv; ++v)
+            for (int c = 0; c < 3; c++) {
+                bb[c] = std::min(bb[c], m.pos[3 * v + c]);
+                bb[3 + c] = std::max(bb[3 + c], m.pos[3 * v + c]);
+            }
+        for (size_t f = 0; f < m.idx.size() / 3; ++f, ++t) {
+            for (int k = 0; k < 3; k++) {
+                uint32_t vi = m.idx[3 * f + k];
+                for (int c = 0; c < 3; c++) P.push_back(m.pos[3 * vi + c]);
+                if (any_normals && !m.nrm.empty())
+                    for (int c = 0; c < 3; c++) tri_normals[t * 12 + 4 * k + c] = m.nrm[3 * vi + c];
+            }
+            tmesh.push_back((int32_t)mi);
+        }
+    }
+    s->b_meshes.upload(dm); track(s->b_meshes);
+    D.meshes = s->b_meshes.as<hk::DevMesh>();
+    D.nmeshes = (int)dm.size();
+    if (any_normals) { s->b_tri_normals.upload(tri_normals); track(s->b_tri_normals); }
+    D.tri_normals = s->b_tri_normals.as<float4>();
+
+    // BVH
+    hk::Bvh2 bvh = hk::build_bvh2(P.data(), (uint32_t)ntris);
+    std::vector<float> recs(bvh.tri_order.size() * 12);
+    for (size_t i = 0; i < bvh.tri_order.size(); ++i) {
+        uint32_t o = bvh.tri_order[i];
+        float *r = &recs[i * 12];
+        for (int k = 0; k < 3; k++)
+            for (int c = 0; c < 3; c++) r[4 * k + c] = P[9 * o + 3 * k + c];
+        int32_t oi = (int32_t)o, mm = tmesh[o];
+        std::memcpy(&r[3], &oi, 4);
+        std::memcpy(&r[7], &mm, 4);
+        r[11] = 0.0f;
+    }
+    s->b_tris.upload(recs); track(s->b_tris);
+    s->b_nodes.upload(bvh.nodes); track(s->b_nodes);
+    D.tris = s->b_tris.as<float4>();
+    D.nodes = s->b_nodes.as<float4>();
+    D.ntris = (uint32_t)ntris;
+    D.nnodes = (uint32_t)(bvh.nodes.size() / 16);
+
+    // emitters (Scene order)
+    std::vector<int32_t> emitter_area;
+    std::vector<hk::DevAreaLight> area;
+    std::vector<float> ltris, lnorms, lcdf;
+    D.env_index = -1;
+    for (size_t e = 0; e < s->emitter_mesh.size(); ++e) {
+        int mi = s->emitter_mesh[e];
+        if (mi < 0) { emitter_area.push_back(-1); D.env_index = (int)e; continue; }
+        auto &m = s->meshes[mi];
+        hk::DevAreaLight L;
+        std::memset(&L, 0, sizeof L);
+        L.tri0 = (uint32_t)(ltris.size() / 12);
+        L.ntri = (uint32_t)(m.idx.size() / 3);
+        L.cdf0 = (uint32_t)lcdf.size();
+        L.mesh = mi;
+        std::vector<float> areas(L.ntri);
+        float total = 0.0f;
+        for (uint32_t f = 0; f < L.ntri; ++f) {   // Mesh::Activate / SurfaceArea (src/core/Mesh.cpp:233,311)
+            F3 p[3];
+            for (int k = 0; k < 3; k++) {
+                uint32_t vi = m.idx[3 * f + k];
+                p[k] = {m.pos[3 * vi], m.pos[3 * vi + 1], m.pos[3 * vi + 2]};
+                for (int c = 0; c < 3; c++) ltris.push_back(c == 0 ? p[k].x : (c == 1 ? p[k].y : p[k].z));
+                ltris.push_back(0.0f);
+                if (!m.nrm.empty()) {
+                    for (int c = 0; c < 3; c++) lnorms.push_back(m.nrm[3 * vi + c]);
+                    lnorms.push_back(1.0f);
+                } else {
+                    for (int c = 0; c < 4; c++) lnorms.push_back(0.0f);
+                }
+            }
+            float a = 0.5f * f3norm(f3cross(f3sub(p[1], p[0]), f3sub(p[2], p[0])));
+            areas[f] = a;
+            total += a;
+        }
+        L.inv_area = 1.0f / total;
+        Pdf1D pdf;
+        pdf.build(areas.data(), (int)L.ntri);
+        lcdf.insert(lcdf.end(), pdf.cdf.begin(), pdf.cdf.end());
+        for (int c = 0; c < 3; c++) L.radiance[c] = m.radiance[c];
+        emitter_area.push_back((int32_t)area.size());
+        area.push_back(L);
+    }
+    s->b_emitter_area.upload(emitter_area); track(s->b_emitter_area);
+    s->b_area.upload(area); track(s->b_area);
+    s->b_light_tris.upload(ltris); track(s->b_light_tris);
+    s->b_light_normals.upload(lnorms); track(s->b_light_normals);
+    s->b_light_cdf.upload(lcdf); track(s->b_light_cdf);
+    D.nemitters = (int)emitter_area.size();
+    D.emitter_area = s->b_emitter_area.as<int32_t>();
+    D.area_lights = s->b_area.as<hk::DevAreaLight>();
+    D.light_tris = s->b_light_tris.as<float4>();
+    D.light_normals = s->b_light_normals.as<float4>();
+    D.light_cdf = s->b_light_cdf.as<float>();
+
+    // environment (EnvironmentLight ctor, src/emitter/EnvironmentLight.cpp:8-31)
+    if (s->has_env) {
+        uint32_t W = s->env_w, H = s->env_h;
+        std::vector<float> rgb4((size_t)W * H * 4), lumv((size_t)W * H);
+        for (uint32_t y = 0; y < H; y++) {
+            float th = float(y + 0.5f) / H * float(M_PI);
+            float st = std::sin(th);
+            for (uint32_t x = 0; x < W; x++) {
+                const float *c = &s->env_rgb[3 * ((size_t)y * W + x)];
+                float *o = &rgb4[4 * ((size_t)y * W + x)];
+                o[0] = c[0]; o[1] = c[1]; o[2] = c[2]; o[3] = 0.0f;
+                lumv[(size_t)y * W + x] = lum(c) * st;
+            }
+        }
+        std::vector<float> ccdf((size_t)H * (W + 1)), cfunc((size_t)H * W), cint(H), marg(H);
+        for (uint32_t y = 0; y < H; y++) {
+            Pdf1D r;
+            r.build(&lumv[(size_t)y * W], (int)W);
+            std::copy(r.cdf.begin(), r.cdf.end(), ccdf.begin() + (size_t)y * (W + 1));
+            std::copy(r.func.begin(), r.func.end(), cfunc.begin() + (size_t)y * W);
+            cint[y] = r.integral;
+            marg[y] = r.integral;
+        }
+        Pdf1D mp;
+        mp.build(marg.data(), (int)H);
+        s->b_env_rgb.upload(rgb4); track(s->b_env_rgb);
+        s->b_env_marg_cdf.upload(mp.cdf); track(s->b_env_marg_cdf);
+        s->b_env_marg_func.upload(mp.func); track(s->b_env_marg_func);
+        s->b_env_cond_cdf.upload(ccdf); track(s->b_env_cond_cdf);
+        s->b_env_cond_func.upload(cfunc); track(s->b_env_cond_func);
+        s->b_env_cond_int.upload(cint); track(s->b_env_cond_int);
+        D.env_rgb = s->b_env_rgb.as<float4>();
+        D.env_marg_cdf = s->b_env_marg_cdf.as<float>();
+        D.env_marg_func = s->b_env_marg_func.as<float>();
+        D.env_cond_cdf = s->b_env_cond_cdf.as<float>();
+        D.env_cond_func = s->b_env_cond_func.as<float>();
+        D.env_cond_int = s->b_env_cond_int.as<float>();
+        D.env_marg_int = mp.integral;
+        D.env_w = W;
+        D.env_h = H;
+        D.env_scale = s->env_scale;
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) D.env_to_world[3 * r + c] = s->env_to_world[4 * r + c];
+        mat3_inverse(D.env_to_world, D.env_to_local);
+    }
+    // BoundingBox::GetRadius of the accel bbox (include/core/BoundingBox.hpp:453)
+    D.scene_radius = f3norm(F3{bb[3] - bb[0], bb[4] - bb[1], bb[5] - bb[2]}) * 0.5f;
+
+    // camera (PerspectiveCamera::Activate, src/camera/PerspectiveCamera.cpp:32)
+    D.width = s->width;
+    D.height = s->height;
+    D.cam_aspect = float(s->width) / float(s->height);
+    D.cam_cot = 1.0f / std::tan((s->fov / 2.0f) * (float(M_PI) / 180.0f));
+    D.cam_near = s->near_clip;
+    D.cam_far = s->far_clip;
+    const float *M = s->cam_to_world;
+    float w = M[15];
+    for (int r = 0; r < 3; r++) {
+        for (int c = 0; c < 3; c++) D.cam[4 * r + c] = M[4 * r + c];
+        D.cam[4 * r + 3] = M[4 * r + 3] / w;
+    }
+    // filter table (ImageBlock ctor, src/core/Block.cpp:9-30)
+    std::vector<float> ftab(33);
+    for (int i = 0; i < 32; i++) ftab[i] = filter_eval(s, (s->filt_r * i) / 32);
+    ftab[32] = 0.0f;
+    s->b_ftab.upload(ftab); track(s->b_ftab);
+    D.ftab = s->b_ftab.as<float>();
+    D.filt_radius = s->filt_r;
+    D.filt_lookup = 32 / s->filt_r;
+    D.border = (int)std::ceil(s->filt_r - 0.5f);
+    if (D.border > 8) throw HkError{HK_ERR_INVALID, "reconstruction filter radius too large (max 8.5)"};
+    for (int c = 0; c < 3; c++) D.background[c] = s->background[c];
+    D.force_background = s->force_background;
+    s->margin_lo = (int)std::ceil(D.border - 0.5f - s->filt_r);
+    s->margin_hi = (int)std::floor(D.border + 0.5f + s->filt_r);
+
+    // scratch: [0] work counter (u32 in a u64 slot), [1..3] counters
+    s->b_scratch.alloc(8 * sizeof(unsigned long long));
+    HK_CUDA(cudaMemset(s->b_scratch.p, 0, s->b_scratch.bytes));
+    track(s->b_scratch);
+
+    int dev = 0;
+    HK_CUDA(cudaGetDevice(&dev));
+    HK_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, dev));
+    s->occupancy = std::max(1, hk::render_occupancy(s->margin_lo, s->margin_hi));
+    HK_CUDA(cudaGetLastError());
+
+    hk_scene_info &I = s->info;
+    I.n_meshes = (uint32_t)s->meshes.size();
+    I.n_triangles = (uint32_t)ntris;
+    I.n_bsdfs = (uint32_t)bs.size();
+    I.n_emitters = (uint32_t)emitter_area.size();
+    I.n_bvh_nodes = D.nnodes;
+    I.bvh_depth = bvh.depth;
+    I.env_index = D.env_index;
+    I.film_border = D.border;
+    std::memcpy(I.bbox, bb, sizeof bb);
+    I.device_bytes = dev_bytes;
+    s->built = true;
+}
+
+void require_built(const hk_scene *s) {
+    if (!s) throw HkError{HK_ERR_INVALID, "null scene"};
+    if (!s->built) throw HkError{HK_ERR_INVALID, "scene is not built (call hk_scene_build)"};
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *hk_last_error(void) { return g_error.c_str(); }
+int hk_version(void) { return 1; }
+
+int hk_scene_create(hk_scene **out) {
+    return guarded([&] {
+        if (!out) throw HkError{HK_ERR_INVALID, "null output pointer"};
+        *out = new hk_scene();
+        return HK_OK;
+    });
+}
+int hk_scene_destroy(hk_scene *s) {
+    return guarded([&] {
+        delete s;
+        return HK_OK;
+    });
+}
+int hk_scene_set_rft(hk_scene *s, int distribution, const void *bytes, uint64_t nbytes) {
+    return guarded([&] {
+        if (!s || !bytes || (distribution != 0 && distribution != 1)) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        s->rft[distribution].parse(bytes, nbytes);
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_add_bsdf(hk_scene *s, const hk_bsdf_desc *d, int32_t *out_id) {
+    return guarded([&] {
+        if (!s || !d) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (d->type < 0 || d->type > 4) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+        if (d->type == HK_BSDF_ROUGH_COATING && (d->nested < 0 || d->nested >= (int)s->bsdfs.size()))
+            throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
+        s->bsdfs.push_back(*d);
+        if (out_id) *out_id = (int32_t)s->bsdfs.size() - 1;
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_add_mesh(hk_scene *s, const float *pos, uint32_t nv, const uint32_t *idx, uint32_t nt, const float *nrm,
+                      int32_t bsdf, const float *rad, int32_t *out_id) {
+    return guarded([&] {
+        if (!s || !pos || !idx || nv == 0 || nt == 0) throw HkError{HK_ERR_INVALID, "mesh needs vertices and faces"};
+        MeshIn m;
+        m.pos.assign(pos, pos + 3 * (size_t)nv);
+        m.idx.assign(idx, idx + 3 * (size_t)nt);
+        for (uint32_t v : m.idx)
+            if (v >= nv) throw HkError{HK_ERR_INVALID, "mesh index out of range"};
+        if (nrm) m.nrm.assign(nrm, nrm + 3 * (size_t)nv);
+        m.bsdf = bsdf;
+        m.emitter = rad != nullptr;
+        for (int c = 0; c < 3; c++) m.radiance[c] = rad ? rad[c] : 0.0f;
+        s->meshes.push_back(std::move(m));
+        if (rad) s->emitter_mesh.push_back((int)s->meshes.size() - 1);
+        if (out_id) *out_id = (int32_t)s->meshes.size() - 1;
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_set_envmap(hk_scene *s, const float *rgb, uint32_t w, uint32_t h, const float *tw16, float scale) {
+    return guarded([&] {
+        if (!s || !rgb || !tw16 || w == 0 || h == 0) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (s->has_env) throw HkError{HK_ERR_INVALID, "Only one environment emitter is allowed for the entire scene"};
+        s->has_env = true;
+        s->env_w = w;
+        s->env_h = h;
+        s->env_rgb.assign(rgb, rgb + 3 * (size_t)w * h);
+        std::memcpy(s->env_to_world, tw16, 64);
+        s->env_scale = scale;
+        s->emitter_mesh.push_back(-1);
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_set_camera(hk_scene *s, uint32_t w, uint32_t h, const float *tw16, float fov, float n, float f) {
+    return guarded([&] {
+        if (!s || w == 0 || h == 0) throw HkError{HK_ERR_INVALID, "bad camera"};
+        s->width = w;
+        s->height = h;
+        if (tw16) std::memcpy(s->cam_to_world, tw16, 64);
+        s->fov = fov;
+        s->near_clip = n;
+        s->far_clip = f;
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_set_filter(hk_scene *s, int kind, float r, float p0, float p1) {
+    return guarded([&] {
+        if (!s || kind < 0 || kind > 3 || !(r > 0.0f)) throw HkError{HK_ERR_INVALID, "bad filter"};
+        s->filt_kind = kind;
+        s->filt_r = r;
+        s->filt_p0 = p0;
+        s->filt_p1 = p1;
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_set_background(hk_scene *s, const float *rgb, int force) {
+    return guarded([&] {
+        if (!s || !rgb) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        std::memcpy(s->background, rgb, 12);
+        s->force_background = force;
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_build(hk_scene *s) {
+    return guarded([&] {
+        if (!s) throw HkError{HK_ERR_INVALID, "null scene"};
+        build_scene(s);
+        return HK_OK;
+    });
+}
+int hk_scene_get_info(const hk_scene *s, hk_scene_info *info) {
+    return guarded([&] {
+        if (!s || !info) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (s->built) {
+            *info = s->info;
+            return HK_OK;
+        }
+        // host-side view of an unbuilt scene (no BVH / device fields yet)
+        hk_scene_info I{};
+        I.n_meshes = (uint32_t)s->meshes.size();
+        float bb[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+        for (auto &m : s->meshes) {
+            I.n_triangles += (uint32_t)(m.idx.size() / 3);
+            for (size_t v = 0; v < m.pos.size() / 3; ++v)
+                for (int c = 0; c < 3; c++) {
+                    bb[c] = std::min(bb[c], m.pos[3 * v + c]);
+                    bb[3 + c] = std::max(bb[3 + c], m.pos[3 * v + c]);
+                }
+        }
+        I.n_bsdfs = (uint32_t)s->bsdfs.size();
+        I.n_emitters = (uint32_t)s->emitter_mesh.size();
+        I.env_index = -1;
+        for (size_t e = 0; e < s->emitter_mesh.size(); ++e)
+            if (s->emitter_mesh[e] < 0) I.env_index = (int32_t)e;
+        I.film_border = (int32_t)std::ceil(s->filt_r - 0.5f);
+        std::memcpy(I.bbox, bb, sizeof bb);
+        *info = I;
+        return HK_OK;
+    });
+}
+
+int hk_render(hk_scene *s, const hk_render_desc *d, float *film, unsigned long long *counters, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (!d || !film) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (d->spp <= 0 || d->depth < 0) throw HkError{HK_ERR_INVALID, "spp must be > 0 and depth >= 0"};
+        cudaStream_t st = (cudaStream_t)stream;
+        hk::RenderLaunch P;
+        std::memset(&P, 0, sizeof P);
+        P.film = film;
+        P.work_counter = (unsigned int *)s->b_scratch.p;
+        P.counters = counters;
+        P.seed = d->seed;
+        P.spp = d->spp;
+        P.sample_offset = d->sample_offset;
+        P.depth = d->depth;
+        P.rr_start = d->rr_start;
+        P.image_index = d->image_index;
+        P.tiles_x = ((int)s->width + hk::kTile - 1) / hk::kTile;
+        P.tiles_y = ((int)s->height + hk::kTile - 1) / hk::kTile;
+        const int tiles = P.tiles_x * P.tiles_y;
+        const int resident = s->sm_count * s->occupancy;
+        int per_item = d->spp_per_item;
+        if (per_item <= 0) {
+            int chunks = std::max(1, std::min(d->spp, (4 * resident + tiles - 1) / tiles));
+            per_item = (d->spp + chunks - 1) / chunks;
+        }
+        P.spp_per_item = per_item;
+        P.n_chunks = (d->spp + per_item - 1) / per_item;
+        P.n_items = tiles * P.n_chunks;
+        P.margin_lo = s->margin_lo;
+        P.margin_hi = s->margin_hi;
+        HK_CUDA(cudaMemsetAsync(s->b_scratch.p, 0, sizeof(unsigned long long), st));
+        int grid = std::min(P.n_items, resident);
+        HK_CUDA(hk::launch_render(s->dev, P, grid, st));
+        return HK_OK;
+    });
+}
+int hk_film_resolve(hk_scene *s, const float *film, float *rgb, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (!film || !rgb) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        HK_CUDA(hk::launch_resolve(film, rgb, (int)s->width, (int)s->height, s->dev.border, (cudaStream_t)stream));
+        return HK_OK;
+    });
+}
+int hk_render_image(hk_scene *s, const hk_render_desc *d, float *rgb_host, unsigned long long *counters, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (!rgb_host) throw HkError{HK_ERR_INVALID, "null output"};
+        cudaStream_t st = (cudaStream_t)stream;
+        size_t FW = s->width + 2 * s->dev.border, FH = s->height + 2 * s->dev.border;
+        size_t film_bytes = FW * FH * 4 * sizeof(float), rgb_bytes = (size_t)s->width * s->height * 3 * sizeof(float);
+        if (s->b_film.bytes < film_bytes) s->b_film.alloc(film_bytes);
+        if (s->b_rgb.bytes < rgb_bytes) s->b_rgb.alloc(rgb_bytes);
+        unsigned long long *ctr = (unsigned long long *)s->b_scratch.p + 1;
+        HK_CUDA(cudaMemsetAsync(s->b_film.p, 0, film_bytes, st));
+        HK_CUDA(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), st));
+        int rc = hk_render(s, d, s->b_film.as<float>(), ctr, stream);
+        if (rc != HK_OK) return rc;
+        HK_CUDA(hk::launch_resolve(s->b_film.as<float>(), s->b_rgb.as<float>(), (int)s->width, (int)s->height,
+                                   s->dev.border, st));
+        HK_CUDA(cudaMemcpyAsync(rgb_host, s->b_rgb.p, rgb_bytes, cudaMemcpyDeviceToHost, st));
+        if (counters) HK_CUDA(cudaMemcpyAsync(counters, ctr, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        HK_CUDA(cudaStreamSynchronize(st));
+        return HK_OK;
+    });
+}
+int hk_trace(hk_scene *s, uint64_t n, const float *rays, int32_t *tri, float *t, float *u, float *v, int any_hit,
+             unsigned long long *visits, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (n == 0) return HK_OK;
+        if (!rays || !tri) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        HK_CUDA(hk::launch_trace(s->dev, n, rays, tri, t, u, v, any_hit, visits, (cudaStream_t)stream));
+        return HK_OK;
+    });
+}
+int hk_bsdf_batch(hk_scene *s, int32_t bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
+                  const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb, float *p_pdf,
+                  void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (bsdf < 0 || bsdf >= s->dev.nbsdfs) throw HkError{HK_ERR_INVALID, "invalid BSDF id"};
+        if (n == 0) return HK_OK;
+        if (!wi || !u2 || !wo) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf,
+                                      (cudaStream_t)stream));
+        return HK_OK;
+    });
+}
+int hk_emitter_sample(hk_scene *s, int32_t e, uint64_t n, const float *in, float *out, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (e < 0 || e >= s->dev.nemitters) throw HkError{HK_ERR_INVALID, "invalid emitter index"};
+        if (n == 0) return HK_OK;
+        HK_CUDA(hk::launch_emitter_sample(s->dev, e, n, in, out, (cudaStream_t)stream));
+        return HK_OK;
+    });
+}
+int hk_camera_rays(hk_scene *s, uint64_t n, const float *pos, float *rays, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (n == 0) return HK_OK;
+        HK_CUDA(hk::launch_camera_rays(s->dev, n, pos, rays, (cudaStream_t)stream));
+        return HK_OK;
+    });
+}
+int hk_env_eval(hk_scene *s, uint64_t n, const float *wi, float *rgb, float *pdf, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (s->dev.env_index < 0) throw HkError{HK_ERR_INVALID, "scene has no environment emitter"};
+        if (n == 0) return HK_OK;
+        HK_CUDA(hk::launch_env_eval(s->dev, n, wi, rgb, pdf, (cudaStream_t)stream));
+        return HK_OK;
+    });
+}
+
+int hk_scene_load_xml(const char *path, const char *data_dir, hk_scene **out, int32_t *depth, int32_t *spp) {
+    return guarded([&] {
+        if (!path || !out) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        std::string err;
+        int rc = hk_scene_load_xml_impl(path, data_dir, out, depth, spp, 1, &err);
+        if (rc != HK_OK && !err.empty()) return set_error(rc, err);
+        return rc;
+    });
+}
+int hk_scene_parse_xml(const char *path, const char *data_dir, hk_scene **out, int32_t *depth, int32_t *spp) {
+    return guarded([&] {
+        if (!path || !out) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        std::string err;
+        int rc = hk_scene_load_xml_impl(path, data_dir, out, depth, spp, 0, &err);
+        if (rc != HK_OK && !err.empty()) return set_error(rc, err);
+        return rc;
+    });
+}
+int hk_exr_read(const char *path, int32_t *w, int32_t *h, float *rgb, uint64_t capacity) {
+    return guarded([&] {
+        if (!path || !w || !h) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        std::vector<float> buf;
+        std::string err;
+        int W = 0, H = 0;
+        int rc = hk_exr_read_impl(path, &W, &H, &buf, &err);
+        if (rc != HK_OK) return set_error(rc, err);
+        *w = W;
+        *h = H;
+        if (rgb) {
+            if (capacity < buf.size()) throw HkError{HK_ERR_INVALID, "output buffer too small"};
+            std::memcpy(rgb, buf.data(), buf.size() * sizeof(float));
+        }
+        return HK_OK;
+    });
+}
+int hk_exr_write(const char *path, int32_t w, int32_t h, const float *rgb) {
+    return guarded([&] {
+        if (!path || !rgb || w <= 0 || h <= 0) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        std::string err;
+        int rc = hk_exr_write_impl(path, w, h, rgb, &err);
+        if (rc != HK_OK) return set_error(rc, err);
+        return HK_OK;
+    });
+}
+
+}  // extern "C"

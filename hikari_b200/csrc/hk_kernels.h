@@ -1,0 +1,39 @@
+// Launch interface between the host library (hk_host.cpp) and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "hk_device.h"
+
+namespace hk {
+
+constexpr int kTile = 16;                  // render tile: 16 x 16 pixels
+constexpr int kTileThreads = kTile * kTile;
+
+struct RenderLaunch {
+    float *film;                          // (H+2B) x (W+2B) x 4 floats, accumulated
+    unsigned int *work_counter;           // zeroed before launch
+    unsigned long long *counters;         // [rays, shadow rays, dropped samples]
+    uint64_t seed;
+    int spp;                              // samples per pixel in this launch
+    int sample_offset;                    // first sample index (progressive rendering)
+    int spp_per_item;                     // samples per thread per work item
+    int n_chunks;                         // work items per tile
+    int tiles_x, tiles_y, n_items;
+    int depth, rr_start;
+    int image_index;
+    int margin_lo, margin_hi;             // film footprint offsets of a tile pixel
+};
+
+cudaError_t launch_render(const DevScene &S, const RenderLaunch &P, int grid, cudaStream_t st);
+cudaError_t launch_resolve(const float *film, float *rgb, int W, int H, int B, cudaStream_t st);
+cudaError_t launch_trace(const DevScene &S, uint64_t n, const float *rays, int32_t *tri, float *t, float *u, float *v,
+                         int any_hit, unsigned long long *visits, cudaStream_t st);
+cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
+                              const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
+                              float *p_pdf, cudaStream_t st);
+cudaError_t launch_emitter_sample(const DevScene &S, int e, uint64_t n, const float *in, float *out, cudaStream_t st);
+cudaError_t launch_camera_rays(const DevScene &S, uint64_t n, const float *pos, float *out, cudaStream_t st);
+cudaError_t launch_env_eval(const DevScene &S, uint64_t n, const float *wi, float *out, float *pdf, cudaStream_t st);
+int render_occupancy(int margin_lo, int margin_hi);
+
+}  // namespace hk

@@ -1,0 +1,175 @@
+// Emitters, camera, intersection post-processing and film splatting of the
+// pathMIS core (device side).
+#pragma once
+#include "hk_bsdf.cuh"
+#include "hk_device.h"
+#include "hk_math.cuh"
+#include "hk_traverse.cuh"
+
+namespace hk {
+
+// ------------------------------------------------------------ intersection
+struct Isect {
+    V3 p;
+    Frame sh;
+    int mesh;
+};
+
+// Triangle::PostIntersect (src/core/Mesh.cpp:67): position from barycentrics,
+// geometric frame from the face normal, shading frame from interpolated
+// vertex normals when the mesh has them.
+__device__ __forceinline__ void post_intersect(const DevScene &S, const Hit &h, Isect &it) {
+    const float4 *tp = S.tris + 3 * h.tri;
+    float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
+    V3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2);
+    float b0 = 1 - (h.u + h.v), b1 = h.u, b2 = h.v;
+    it.p = (p0 * b0 + p1 * b1) + p2 * b2;
+    it.mesh = __float_as_int(q1.w);
+    const DevMesh &m = S.meshes[it.mesh];
+    if (m.has_normals) {
+        const float4 *np = S.tri_normals + 3 * (uint32_t)__float_as_int(q0.w);
+        V3 n0 = xyz(__ldg(np)), n1 = xyz(__ldg(np + 1)), n2 = xyz(__ldg(np + 2));
+        it.sh = frame_from_n(normalize((n0 * b0 + n1 * b1) + n2 * b2));
+    } else {
+        it.sh = frame_from_n(normalize(cross(p1 - p0, p2 - p0)));
+    }
+}
+
+// ------------------------------------------------------------ emitters
+struct ERec {
+    V3 ref, p, n, wi;
+    float pdf, dist;
+};
+
+// std::lower_bound over cdf[0..n] then clamp to [0, n-1] (src/core/DiscretePDF.cpp:41-46)
+__device__ __forceinline__ int cdf_find(const float *cdf, int n, float u) {
+    int lo = 0, hi = n + 1;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) < u) lo = mid + 1; else hi = mid;
+    }
+    return clampi(lo - 1, 0, n - 1);
+}
+
+// AreaLight::Pdf / Eval (src/emitter/AreaLight.cpp:38,59)
+__device__ __forceinline__ float area_pdf(const DevAreaLight &L, const ERec &r) {
+    float gd = fabsf(dot(r.wi * -1.0f, r.n));
+    if (gd == 0.0f) return 0.0f;
+    float gn = r.dist * r.dist;
+    return L.inv_area * (gn / gd);
+}
+__device__ __forceinline__ V3 area_eval(const DevAreaLight &L, const ERec &r) {
+    return dot(r.n, r.wi) < 0.0f ? ld3(L.radiance) : v3(0, 0, 0);
+}
+// AreaLight::Sample (src/emitter/AreaLight.cpp:14) with Mesh::SamplePosition (src/core/Mesh.cpp:273)
+__device__ __forceinline__ V3 area_sample(const DevScene &S, const DevAreaLight &L, ERec &r, float ux, float uy, float u1) {
+    int ti = cdf_find(S.light_cdf + L.cdf0, (int)L.ntri, u1);
+    float sq = sqrtf(1.0f - ux);
+    float al = 1.0f - sq, be = uy * sq, ga = 1.0f - al - be;
+    const float4 *tp = S.light_tris + 3 * (L.tri0 + ti);
+    V3 p0 = xyz(__ldg(tp)), p1 = xyz(__ldg(tp + 1)), p2 = xyz(__ldg(tp + 2));
+    r.p = (p0 * ga + p1 * al) + p2 * be;
+    const float4 *np = S.light_normals + 3 * (L.tri0 + ti);
+    float4 n0 = __ldg(np);
+    if (n0.w != 0.0f) {
+        V3 n1 = xyz(__ldg(np + 1)), n2 = xyz(__ldg(np + 2));
+        r.n = (xyz(n0) * ga + n1 * al) + n2 * be;
+    } else {
+        r.n = normalize(cross(p1 - p0, p2 - p0));
+    }
+    V3 wi = r.p - r.ref;
+    r.dist = norm(wi);
+    r.wi = normalize(wi);
+    r.pdf = area_pdf(L, r);
+    if (r.pdf == 0.0f || isinf(r.pdf)) return v3(0, 0, 0);
+    return area_eval(L, r) / r.pdf;
+}
+
+__device__ __forceinline__ V3 mat3(const float *m, V3 v) {
+    return v3(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
+              m[6] * v.x + m[7] * v.y + m[8] * v.z);
+}
+// SphericalCoordinates (src/core/Common.cpp:481)
+__device__ __forceinline__ void spherical_coords(V3 d, float &th, float &ph) {
+    th = acosf(d.z);
+    ph = atan2f(d.y, d.x);
+    if (ph < 0) ph += 2.0f * kPi;
+}
+__device__ __forceinline__ V3 env_texel(const DevScene &S, int y, int x) {
+    return xyz(__ldg(S.env_rgb + (uint64_t)y * S.env_w + x));
+}
+// DiscretePDF1D::SampleContinuous (src/core/DiscretePDF.cpp:39)
+__device__ __forceinline__ float sample_cont(const float *cdf, const float *func, float integral, int n, float u,
+                                             float &pdf, int &idx) {
+    idx = cdf_find(cdf, n, u);
+    float c0 = __ldg(cdf + idx), c1 = __ldg(cdf + idx + 1);
+    float du = u - c0;
+    if (c1 - c0 > 0.0f) du /= (c1 - c0);
+    pdf = __ldg(func + idx) / integral;
+    return ((float)idx + du) / (float)n;
+}
+// EnvironmentLight::Sample (src/emitter/EnvironmentLight.cpp:41)
+__device__ __forceinline__ V3 env_sample(const DevScene &S, ERec &r, float ux, float uy) {
+    float py, px;
+    int iy, ix;
+    float dy = sample_cont(S.env_marg_cdf, S.env_marg_func, S.env_marg_int, (int)S.env_h, uy, py, iy);
+    float dx = sample_cont(S.env_cond_cdf + (uint64_t)iy * (S.env_w + 1), S.env_cond_func + (uint64_t)iy * S.env_w,
+                           __ldg(S.env_cond_int + iy), (int)S.env_w, ux, px, ix);
+    float mp = px * py;
+    float th = dy * kPi, st = sinf(th);
+    if (mp == 0.0f) return v3(0, 0, 0);
+    if (st != 0.0f) r.pdf = mp / (2.0f * (float)(3.14159265358979323846 * 3.14159265358979323846) * st);
+    else return v3(0, 0, 0);
+    float ph = dx * (float)(2.0 * 3.14159265358979323846);
+    float sp = sinf(ph), cp = cosf(ph), ct = cosf(th);
+    V3 dir = v3(st * cp, st * sp, ct);   // SphericalDirection (src/core/Common.cpp:467)
+    r.wi = mat3(S.env_to_world, dir);
+    r.n = r.wi * -1.0f;
+    r.p = r.ref + (r.wi * r.dist) * 2.0f;
+    V3 rad = env_texel(S, iy, ix);
+    if (!is_valid(rad)) return v3(0, 0, 0);
+    return (rad * S.env_scale) / r.pdf;
+}
+// EnvironmentLight::Pdf (:78) with DiscretePDF2D::Pdf (src/core/DiscretePDF.cpp:127)
+__device__ __forceinline__ float env_pdf(const DevScene &S, V3 wi) {
+    float th, ph;
+    spherical_coords(mat3(S.env_to_local, wi), th, ph);
+    float st = sinf(th);
+    if (st == 0.0f) return 0.0f;
+    float u = ph / (float)(2.0 * 3.14159265358979323846), v = th / (float)3.14159265358979323846;
+    int X = clampi((int)(u * S.env_w), 0, (int)S.env_w - 1), Y = clampi((int)(v * S.env_h), 0, (int)S.env_h - 1);
+    float p = __ldg(S.env_cond_func + (uint64_t)Y * S.env_w + X) / S.env_marg_int;
+    return p / (2.0f * (float)(3.14159265358979323846 * 3.14159265358979323846) * st);
+}
+// EnvironmentLight::Eval (:92): nearest texel
+__device__ __forceinline__ V3 env_eval(const DevScene &S, V3 wi) {
+    float th, ph;
+    spherical_coords(mat3(S.env_to_local, wi), th, ph);
+    if (isnan(th) || isnan(ph)) return v3(0, 0, 0);
+    float X = clampf(ph / (float)(2.0 * 3.14159265358979323846) * (float)S.env_w, 0.0f, (float)(S.env_w - 1.0f));
+    float Y = clampf(th / (float)3.14159265358979323846 * (float)S.env_h, 0.0f, (float)(S.env_h - 1.0f));
+    V3 rad = env_texel(S, (int)Y, (int)X);
+    if (!is_valid(rad)) return v3(0, 0, 0);
+    return rad * S.env_scale;
+}
+
+// ------------------------------------------------------------ camera
+// PerspectiveCamera::SampleRay (src/camera/PerspectiveCamera.cpp:77) with the
+// sample->camera projective map inverted in closed form.
+__device__ __forceinline__ Ray camera_ray(const DevScene &S, float px, float py) {
+    float u = px * (1.0f / (float)S.width), v = py * (1.0f / (float)S.height);
+    V3 np = v3(S.cam_near * (1.0f - 2.0f * u) / S.cam_cot, S.cam_near * (1.0f - 2.0f * v) / (S.cam_aspect * S.cam_cot),
+               S.cam_near);
+    V3 dir = normalize(np);
+    float invz = 1.0f / dir.z;
+    const float *M = S.cam;
+    Ray r;
+    r.o = v3(M[3], M[7], M[11]);
+    r.d = v3(M[0] * dir.x + M[1] * dir.y + M[2] * dir.z, M[4] * dir.x + M[5] * dir.y + M[6] * dir.z,
+             M[8] * dir.x + M[9] * dir.y + M[10] * dir.z);
+    r.tmin = S.cam_near * invz;
+    r.tmax = S.cam_far * invz;
+    return r;
+}
+
+}  // namespace hk

@@ -1,0 +1,176 @@
+// Software BVH traversal for sm_100a (B200 has no RT cores).
+//
+// Nodes are 64-byte BVH2 records (both child boxes in one node, fetched with
+// four 128-bit read-only loads); triangles are pre-gathered 48-byte records
+// in leaf order.  The ray-triangle test is the watertight test of Woop,
+// Benthin and Wald (JCGT 2013), accepting both windings like the reference's
+// Moller-Trumbore (src/core/Mesh.cpp:340) and the reference's closest-hit
+// rule: a hit with t in [tmin, tmax] replaces the current one, tmax shrinks
+// to its t (src/acceleration/HLBVHAcceleration.cpp:229-240).
+#pragma once
+#include "hk_device.h"
+#include "hk_math.cuh"
+
+namespace hk {
+
+constexpr int kStackSize = 64;
+
+struct Ray {
+    V3 o, d;
+    float tmin, tmax;
+};
+
+struct Hit {
+    float t, u, v;    // u, v: weights of the 2nd and 3rd vertex (reference UV)
+    int tri;          // index in leaf order, -1 = miss
+};
+
+// Per-ray constants of the watertight test.
+struct WatertightRay {
+    int kx, ky, kz;
+    float sx, sy, sz;
+};
+__device__ __forceinline__ float comp(V3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+__device__ __forceinline__ WatertightRay watertight_setup(V3 d) {
+    WatertightRay w;
+    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+    w.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    w.kx = w.kz + 1 == 3 ? 0 : w.kz + 1;
+    w.ky = w.kx + 1 == 3 ? 0 : w.kx + 1;
+    float dz = comp(d, w.kz);
+    if (dz < 0.0f) { int t = w.kx; w.kx = w.ky; w.ky = t; }   // keep winding
+    w.sx = comp(d, w.kx) / dz;
+    w.sy = comp(d, w.ky) / dz;
+    w.sz = 1.0f / dz;
+    return w;
+}
+
+// Returns true and t, u, v when the ray hits triangle (a, b, c) with t in [tmin, tmax].
+__device__ __forceinline__ bool intersect_watertight(const WatertightRay &w, V3 o, V3 a, V3 b, V3 c, float tmin,
+                                                     float tmax, float &t, float &u, float &v) {
+    V3 A = a - o, B = b - o, C = c - o;
+    float Az = comp(A, w.kz), Bz = comp(B, w.kz), Cz = comp(C, w.kz);
+    float Ax = comp(A, w.kx) - w.sx * Az, Ay = comp(A, w.ky) - w.sy * Az;
+    float Bx = comp(B, w.kx) - w.sx * Bz, By = comp(B, w.ky) - w.sy * Bz;
+    float Cx = comp(C, w.kx) - w.sx * Cz, Cy = comp(C, w.ky) - w.sy * Cz;
+    float U = Cx * By - Cy * Bx;
+    float Vv = Ax * Cy - Ay * Cx;
+    float W = Bx * Ay - By * Ax;
+    if (U == 0.0f || Vv == 0.0f || W == 0.0f) {   // edge: redo in double (watertight fallback)
+        double CxBy = (double)Cx * (double)By, CyBx = (double)Cy * (double)Bx;
+        U = (float)(CxBy - CyBx);
+        double AxCy = (double)Ax * (double)Cy, AyCx = (double)Ay * (double)Cx;
+        Vv = (float)(AxCy - AyCx);
+        double BxAy = (double)Bx * (double)Ay, ByAx = (double)By * (double)Ax;
+        W = (float)(BxAy - ByAx);
+    }
+    if ((U < 0.0f || Vv < 0.0f || W < 0.0f) && (U > 0.0f || Vv > 0.0f || W > 0.0f)) return false;
+    float det = U + Vv + W;
+    if (det == 0.0f) return false;
+    Az *= w.sz; Bz *= w.sz; Cz *= w.sz;
+    float T = U * Az + Vv * Bz + W * Cz;
+    float rcp = 1.0f / det;
+    float tt = T * rcp;
+    if (!(tt >= tmin && tt <= tmax)) return false;
+    t = tt;
+    u = Vv * rcp;
+    v = W * rcp;
+    return true;
+}
+
+__device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
+
+// Slab test of two child boxes against the ray interval; explicit FMAs (the
+// result only prunes, it never changes which triangle is reported).
+__device__ __forceinline__ void box2(const float4 a, const float4 b, const float4 c, V3 idir, V3 ood, float tmin,
+                                     float tmax, bool &hit0, bool &hit1, float &t0, float &t1) {
+    float c0lox = __fmaf_rn(a.x, idir.x, -ood.x), c0hix = __fmaf_rn(a.y, idir.x, -ood.x);
+    float c0loy = __fmaf_rn(a.z, idir.y, -ood.y), c0hiy = __fmaf_rn(a.w, idir.y, -ood.y);
+    float c1lox = __fmaf_rn(b.x, idir.x, -ood.x), c1hix = __fmaf_rn(b.y, idir.x, -ood.x);
+    float c1loy = __fmaf_rn(b.z, idir.y, -ood.y), c1hiy = __fmaf_rn(b.w, idir.y, -ood.y);
+    float c0loz = __fmaf_rn(c.x, idir.z, -ood.z), c0hiz = __fmaf_rn(c.y, idir.z, -ood.z);
+    float c1loz = __fmaf_rn(c.z, idir.z, -ood.z), c1hiz = __fmaf_rn(c.w, idir.z, -ood.z);
+    float n0 = fmaxf(fmaxf(fminf(c0lox, c0hix), fminf(c0loy, c0hiy)), fmaxf(fminf(c0loz, c0hiz), tmin));
+    float f0 = fminf(fminf(fmaxf(c0lox, c0hix), fmaxf(c0loy, c0hiy)), fminf(fmaxf(c0loz, c0hiz), tmax));
+    float n1 = fmaxf(fmaxf(fminf(c1lox, c1hix), fminf(c1loy, c1hiy)), fmaxf(fminf(c1loz, c1hiz), tmin));
+    float f1 = fminf(fminf(fmaxf(c1lox, c1hix), fmaxf(c1loy, c1hiy)), fminf(fmaxf(c1loz, c1hiz), tmax));
+    // slack of a few ulps keeps boxes of axis-aligned, zero-thickness geometry
+    hit0 = n0 <= f0 * 1.00000024f + 1e-30f;
+    hit1 = n1 <= f1 * 1.00000024f + 1e-30f;
+    t0 = n0;
+    t1 = n1;
+}
+
+// Closest hit (any_hit = false) or first hit (any_hit = true).  Returns the
+// number of nodes visited in *visits when non-null (for traffic accounting).
+template <bool kAnyHit>
+__device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hit &hit, uint32_t *visits = nullptr) {
+    hit.tri = -1;
+    if (S.nnodes == 0) return false;
+    V3 d = ray.d;
+    // zero components -> tiny signed values: inverse stays finite, no 0*inf NaN
+    const float tiny = 1e-30f;
+    V3 dd = v3(fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x, fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y,
+               fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z);
+    V3 idir = v3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    V3 ood = v3(ray.o.x * idir.x, ray.o.y * idir.y, ray.o.z * idir.z);
+    WatertightRay w = watertight_setup(d);
+    float tmax = ray.tmax;
+    int stack[kStackSize];
+    int sp = 0;
+    int node = 0;
+    uint32_t nvis = 0;
+    bool found = false;
+    // root: test the root's own children; a single-leaf tree is stored as a
+    // root whose child0 is the leaf and child1 an empty box.
+    for (;;) {
+        const float4 *np = S.nodes + 4 * node;
+        float4 a = ldg4(np), b = ldg4(np + 1), c = ldg4(np + 2), e = ldg4(np + 3);
+        int c0 = __float_as_int(e.x), c1 = __float_as_int(e.y);
+        ++nvis;
+        bool h0, h1;
+        float t0, t1;
+        box2(a, b, c, idir, ood, ray.tmin, tmax, h0, h1, t0, t1);
+        int next = -0x7fffffff;   // sentinel: pop
+        // visit leaves immediately; push/choose internal children near-first
+        int leafs[2];
+        int nleaf = 0;
+        int inner[2];
+        float tin[2];
+        int ninner = 0;
+        if (h0) { if (c0 < 0) leafs[nleaf++] = c0; else { inner[ninner] = c0; tin[ninner++] = t0; } }
+        if (h1) { if (c1 < 0) leafs[nleaf++] = c1; else { inner[ninner] = c1; tin[ninner++] = t1; } }
+        for (int l = 0; l < nleaf; ++l) {
+            uint32_t enc = ~(uint32_t)leafs[l];
+            uint32_t start = enc & kLeafStartMask, cnt = enc >> kLeafCountShift;
+            for (uint32_t i = 0; i < cnt; ++i) {
+                const float4 *tp = S.tris + 3 * (start + i);
+                float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
+                float tt, uu, vv;
+                if (intersect_watertight(w, ray.o, xyz(p0), xyz(p1), xyz(p2), ray.tmin, tmax, tt, uu, vv)) {
+                    found = true;
+                    hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)(start + i);
+                    if (kAnyHit) { if (visits) *visits += nvis; return true; }
+                    tmax = tt;
+                }
+            }
+        }
+        if (ninner == 2) {
+            bool swap = tin[1] < tin[0];
+            int nearc = swap ? inner[1] : inner[0], farc = swap ? inner[0] : inner[1];
+            if (sp < kStackSize) stack[sp++] = farc;
+            next = nearc;
+        } else if (ninner == 1) {
+            next = inner[0];
+        }
+        if (next == -0x7fffffff) {
+            if (sp == 0) break;
+            next = stack[--sp];
+        }
+        node = next;
+    }
+    if (visits) *visits += nvis;
+    return found;
+}
+
+}  // namespace hk

@@ -1,0 +1,344 @@
+"""Seeded synthetic scenes of the benchmark configurations.
+
+* ``cornell_box``      -- plain-method small case: a Cornell box of OBJ quads
+* ``icosphere``        -- subdivided icosahedron, optionally displaced by value noise
+* ``sky_envmap``       -- procedural lat-long sky (sun disk of radiance 2e4 + gradient)
+* ``mesh_heavy``       -- displaced level-8 icosphere on a ground quad under the sky
+* ``heterogeneous``    -- 64 displaced icospheres with random materials, 4 area lights + sky
+
+All geometry is generated in world space with the winding the reference's
+one-sided BSDFs need (src/bsdf/DiffuseBSDF.cpp:45): the geometric normal
+cross(p1 - p0, p2 - p0) points towards the viewer side.
+"""
+from __future__ import annotations
+
+import math
+from typing import List, Optional
+
+import numpy as np
+
+from .scenedesc import (BECKMANN, BSDF_DIFFUSE, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
+                        BSDF_ROUGH_PLASTIC, GGX, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, MeshDesc, SceneDesc)
+
+# Per-channel complex IOR (n, k) of copper and gold at R, G, B ~ (650, 550, 450) nm,
+# rounded from Johnson & Christy (1972) optical constants.
+CU_ETA = [0.27, 0.98, 1.16]
+CU_K = [3.41, 2.58, 2.40]
+AU_ETA = [0.17, 0.42, 1.37]
+AU_K = [3.57, 2.39, 1.79]
+
+
+def look_at(origin, target, up) -> np.ndarray:
+    """The <lookat> transform of src/core/Parser.cpp:353 (columns left, up, dir, origin)."""
+    o, t, u = (np.asarray(v, np.float64) for v in (origin, target, up))
+    d = t - o
+    d /= np.linalg.norm(d)
+    left = np.cross(u / np.linalg.norm(u), d)
+    left /= np.linalg.norm(left)
+    nup = np.cross(d, left)
+    M = np.eye(4)
+    M[:3, 0], M[:3, 1], M[:3, 2], M[:3, 3] = left, nup, d, o
+    return M.astype(np.float32)
+
+
+def quad(p0, p1, p2, p3):
+    """Quad p0..p3 split like the OBJ loader: (v1,v2,v3), (v4,v1,v3)."""
+    pos = np.array([p0, p1, p2, p3], np.float32)
+    idx = np.array([[0, 1, 2], [3, 0, 2]], np.uint32)
+    return pos, idx
+
+
+def box_mesh(center, size, angle_deg):
+    """Axis box rotated about +y, faces wound outwards (12 triangles)."""
+    cx, cy, cz = center
+    sx, sy, sz = size
+    a = math.radians(angle_deg)
+    ca, sa = math.cos(a), math.sin(a)
+    corners = []
+    for x in (-0.5, 0.5):
+        for y in (0.0, 1.0):
+            for z in (-0.5, 0.5):
+                px, pz = x * sx, z * sz
+                corners.append((cx + ca * px + sa * pz, cy + y * sy, cz - sa * px + ca * pz))
+    C = np.array(corners, np.float32)
+    # corner index = 4*xi + 2*yi + zi
+    faces = [
+        (0, 1, 3, 2),  # -x
+        (4, 6, 7, 5),  # +x
+        (0, 4, 5, 1),  # -z... reorder below by normal check
+        (2, 3, 7, 6),
+        (0, 2, 6, 4),  # bottom
+        (1, 5, 7, 3),  # top
+    ]
+    pos, idx = [], []
+    cen = C.mean(0)
+    for f in faces:
+        q = [C[i] for i in f]
+        n = np.cross(q[1] - q[0], q[2] - q[0])
+        fc = np.mean(q, 0)
+        if np.dot(n, fc - cen) < 0:
+            q = q[::-1]
+        base = len(pos)
+        pos += q
+        idx += [[base, base + 1, base + 2], [base + 3, base, base + 2]]
+    return np.array(pos, np.float32), np.array(idx, np.uint32)
+
+
+def cornell_box(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64, depth: int = 64) -> SceneDesc:
+    """Five 2x2 diffuse walls (white 0.725, red (0.63,0.065,0.05), green
+    (0.14,0.45,0.09)), two 12-triangle boxes rotated about y by U[0,45] deg
+    (seeded), a 0.5x0.5 area light of radiance (17,12,4); perspective fov 40,
+    independent sampler, Gaussian filter radius 2."""
+    rng = np.random.default_rng(seed)
+    white = BSDFDesc(type=BSDF_DIFFUSE, kd=[0.725, 0.725, 0.725])
+    red = BSDFDesc(type=BSDF_DIFFUSE, kd=[0.63, 0.065, 0.05])
+    green = BSDFDesc(type=BSDF_DIFFUSE, kd=[0.14, 0.45, 0.09])
+    sd = SceneDesc()
+    # interior of [-1,1] x [0,2] x [-1,1]; normals point inwards
+    walls = [
+        (quad((-1, 0, -1), (-1, 0, 1), (1, 0, 1), (1, 0, -1)), white),   # floor  (+y)
+        (quad((-1, 2, -1), (1, 2, -1), (1, 2, 1), (-1, 2, 1)), white),   # ceiling (-y)
+        (quad((-1, 0, -1), (1, 0, -1), (1, 2, -1), (-1, 2, -1)), white),  # back (+z)
+        (quad((-1, 0, -1), (-1, 2, -1), (-1, 2, 1), (-1, 0, 1)), red),    # left (+x)
+        (quad((1, 0, -1), (1, 0, 1), (1, 2, 1), (1, 2, -1)), green),      # right (-x)
+    ]
+    for (pos, idx), b in walls:
+        n = np.cross(pos[1] - pos[0], pos[2] - pos[0])
+        sd.meshes.append(MeshDesc(pos, idx, b))
+    a1, a2 = rng.uniform(0, 45, 2)
+    for (c, s, a) in [((-0.35, 0.0, -0.3), (0.55, 1.2, 0.55), a1), ((0.4, 0.0, 0.35), (0.55, 0.6, 0.55), -a2)]:
+        pos, idx = box_mesh(c, s, a)
+        sd.meshes.append(MeshDesc(pos, idx, white))
+    lp, li = quad((-0.25, 1.98, -0.25), (0.25, 1.98, -0.25), (0.25, 1.98, 0.25), (-0.25, 1.98, 0.25))
+    sd.meshes.append(MeshDesc(lp, li, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.0, 0.0, 0.0]), radiance=[17.0, 12.0, 4.0]))
+    sd.camera = CameraDesc(width, height, look_at((0, 1, 3.8), (0, 1, 0), (0, 1, 0)), 40.0, 1e-4, 1e4)
+    sd.filter = FilterDesc(2, 2.0, 0.5)
+    sd.depth = depth
+    sd.spp = spp
+    return sd
+
+
+# ------------------------------------------------------------ icosphere
+def icosphere(level: int):
+    """Unit icosahedron subdivided `level` times (20 * 4^level triangles), outward winding."""
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    V = np.array([(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+                  (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)], np.float64)
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    F = np.array([(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+                  (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+                  (6, 2, 10), (8, 6, 7), (9, 8, 1)], np.int64)
+    for _ in range(level):
+        e = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]], 0)
+        e.sort(axis=1)
+        key = e[:, 0] * (len(V) + 1) + e[:, 1]
+        uk, inv = np.unique(key, return_inverse=True)
+        a, b = uk // (len(V) + 1), uk % (len(V) + 1)
+        mid = V[a] + V[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        m = inv.reshape(3, -1).T + len(V)
+        V = np.concatenate([V, mid], 0)
+        v0, v1, v2 = F[:, 0], F[:, 1], F[:, 2]
+        m01, m12, m20 = m[:, 0], m[:, 1], m[:, 2]
+        F = np.concatenate([np.stack([v0, m01, m20], 1), np.stack([v1, m12, m01], 1), np.stack([v2, m20, m12], 1),
+                            np.stack([m01, m12, m20], 1)], 0)
+    # make the winding outward
+    n = np.cross(V[F[:, 1]] - V[F[:, 0]], V[F[:, 2]] - V[F[:, 0]])
+    flip = np.einsum("ij,ij->i", n, V[F[:, 0]]) < 0
+    F[flip] = F[flip][:, [0, 2, 1]]
+    return V, F
+
+
+def value_noise_3d(p: np.ndarray, seed: int, octaves: int = 4) -> np.ndarray:
+    """Seeded fractal value noise in [-1, 1] (trilinear lattice noise, smoothstep
+    fade, octave frequency x2, amplitude x0.5)."""
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(256)
+    vals = rng.uniform(-1.0, 1.0, 256)
+
+    def lattice(ix, iy, iz):
+        h = perm[(perm[(perm[ix & 255] + iy) & 255] + iz) & 255]
+        return vals[h]
+
+    out = np.zeros(len(p))
+    amp, freq, norm = 1.0, 2.0, 0.0
+    for _ in range(octaves):
+        q = p * freq + 17.0
+        i0 = np.floor(q).astype(np.int64)
+        f = q - i0
+        w = f * f * (3 - 2 * f)
+        acc = 0.0
+        for dx in (0, 1):
+            for dy in (0, 1):
+                for dz in (0, 1):
+                    wt = (w[:, 0] if dx else 1 - w[:, 0]) * (w[:, 1] if dy else 1 - w[:, 1]) * (w[:, 2] if dz else 1 - w[:, 2])
+                    acc = acc + wt * lattice(i0[:, 0] + dx, i0[:, 1] + dy, i0[:, 2] + dz)
+        out += amp * acc
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return out / norm
+
+
+def displaced_icosphere(level: int, radius: float, center, amplitude: float, seed: int):
+    V, F = icosphere(level)
+    d = value_noise_3d(V, seed) if amplitude != 0.0 else 0.0
+    P = V * (radius * (1.0 + amplitude * np.asarray(d))[:, None]) + np.asarray(center, np.float64)
+    return P.astype(np.float32), F.astype(np.uint32)
+
+
+# ------------------------------------------------------------ sky
+def sky_envmap(width: int = 2048, height: int = 1024, sun_dir=(0.3, 0.8, 0.5), sun_radiance: float = 2e4,
+               sun_deg: float = 0.5):
+    """Lat-long sky in the reference's SphericalCoordinates convention
+    (theta from +z of the map frame, row 0 at theta = 0): a gradient sky
+    brighter at the zenith and a sun disk of angular diameter sun_deg.  The
+    map's +z is the world up axis through the returned to_world."""
+    # map frame: z = world y (up); x = world x; y = world -z  -> to_world maps map->world
+    to_world = np.array([[1, 0, 0, 0], [0, 0, 1, 0], [0, -1, 0, 0], [0, 0, 0, 1]], np.float32)
+    th = (np.arange(height) + 0.5) / height * math.pi
+    ph = (np.arange(width) + 0.5) / width * 2 * math.pi
+    T, Ph = np.meshgrid(th, ph, indexing="ij")
+    d_map = np.stack([np.sin(T) * np.cos(Ph), np.sin(T) * np.sin(Ph), np.cos(T)], -1)
+    up = np.clip(np.cos(T), -1, 1)
+    zen = np.array([0.25, 0.45, 1.0])
+    hor = np.array([0.9, 0.95, 1.0])
+    gnd = np.array([0.15, 0.13, 0.12])
+    s = np.clip(up, 0, 1)[..., None]
+    rgb = np.where(up[..., None] >= 0, hor * (1 - s) + zen * s, gnd)
+    sd = np.asarray(sun_dir, np.float64)
+    sd = sd / np.linalg.norm(sd)
+    sd_map = np.linalg.inv(to_world[:3, :3].astype(np.float64)) @ sd
+    cosang = np.einsum("ijk,k->ij", d_map, sd_map)
+    rgb = rgb.astype(np.float32)
+    rgb[cosang >= math.cos(math.radians(sun_deg / 2))] = sun_radiance
+    return rgb.astype(np.float32), to_world
+
+
+def mesh_heavy(material: str = "conductor", width: int = 1024, height: int = 1024, spp: int = 256, depth: int = 16,
+               level: int = 8, env_res=(2048, 1024), seed: int = 0) -> SceneDesc:
+    """Displaced level-`level` icosphere (20*4^level triangles, 4-octave value
+    noise of amplitude 0.08) on a 20x20 diffuse ground quad under the sky.
+    material: 'conductor' (GGX alpha 0.2, Cu), 'dielectric' (IOR 1.5, alpha
+    0.1), 'plastic' (alpha 0.15)."""
+    sd = SceneDesc()
+    if material == "conductor":
+        b = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=1.0, ext_ior=1.0,
+                     eta=CU_ETA, k=CU_K)
+    elif material == "dielectric":
+        b = BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=0.1, alpha_v=0.1, int_ior=1.5, ext_ior=1.0)
+    elif material == "plastic":
+        b = BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=0.15, alpha_v=0.15, kd=[0.5, 0.5, 0.5])
+    else:
+        raise ValueError(material)
+    P, F = displaced_icosphere(level, 1.0, (0.0, 1.0, 0.0), 0.08, seed)
+    sd.meshes.append(MeshDesc(P, F, b))
+    gp, gi = quad((-10, 0, -10), (-10, 0, 10), (10, 0, 10), (10, 0, -10))
+    sd.meshes.append(MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5])))
+    rgb, tw = sky_envmap(*env_res)
+    sd.env = EnvDesc(rgb, tw, 1.0)
+    sd.env_emitter_index = 0
+    sd.camera = CameraDesc(width, height, look_at((0, 1.6, 4.2), (0, 0.9, 0), (0, 1, 0)), 40.0, 1e-4, 1e4)
+    sd.filter = FilterDesc(2, 2.0, 0.5)
+    sd.depth = depth
+    sd.spp = spp
+    return sd
+
+
+def random_material(rng, kind: Optional[str] = None) -> BSDFDesc:
+    kinds = ["diffuse", "ggx_conductor", "beckmann_conductor", "dielectric", "plastic", "coated"]
+    kind = kind or kinds[rng.integers(len(kinds))]
+    a = float(rng.uniform(0.05, 0.5))
+    col = [float(x) for x in rng.uniform(0.2, 0.9, 3)]
+    if kind == "diffuse":
+        return BSDFDesc(type=BSDF_DIFFUSE, kd=col)
+    if kind in ("ggx_conductor", "beckmann_conductor"):
+        cu = rng.random() < 0.5
+        return BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX if kind == "ggx_conductor" else BECKMANN,
+                        alpha_u=a, alpha_v=a, int_ior=1.0, ext_ior=1.0, eta=CU_ETA if cu else AU_ETA,
+                        k=CU_K if cu else AU_K)
+    if kind == "dielectric":
+        return BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=a, alpha_v=a, int_ior=1.5, ext_ior=1.0)
+    if kind == "plastic":
+        return BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=a, alpha_v=a, kd=col)
+    nested = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=a, alpha_v=a, int_ior=1.0, ext_ior=1.0,
+                      eta=AU_ETA, k=AU_K)
+    return BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2, nested=nested)
+
+
+def heterogeneous(width: int = 1024, height: int = 1024, spp: int = 128, depth: int = 16, n_spheres: int = 64,
+                  levels=(5, 6, 7), level_p=(0.55, 0.30, 0.15), env_res=(2048, 1024), seed: int = 0) -> SceneDesc:
+    """64 displaced icospheres (levels 5-7) at seeded positions in a 40x40x10
+    box, each with a material drawn uniformly from {diffuse, GGX conductor,
+    Beckmann conductor, rough dielectric, rough plastic, coated}, roughness
+    U[0.05, 0.5]; a ground plane, 4 area lights and the sky."""
+    rng = np.random.default_rng(seed)
+    sd = SceneDesc()
+    for i in range(n_spheres):
+        lvl = int(rng.choice(levels, p=level_p))
+        c = (float(rng.uniform(-20, 20)), float(rng.uniform(1.0, 10.0)), float(rng.uniform(-20, 20)))
+        r = float(rng.uniform(0.8, 2.0))
+        P, F = displaced_icosphere(lvl, r, c, 0.08, seed * 1000 + i)
+        sd.meshes.append(MeshDesc(P, F, random_material(rng)))
+    gp, gi = quad((-40, 0, -40), (-40, 0, 40), (40, 0, 40), (40, 0, -40))
+    sd.meshes.append(MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5])))
+    for k in range(4):
+        cx, cz = (-10 if k % 2 else 10), (-10 if k // 2 else 10)
+        lp, li = quad((cx - 2, 14, cz - 2), (cx + 2, 14, cz - 2), (cx + 2, 14, cz + 2), (cx - 2, 14, cz + 2))
+        sd.meshes.append(MeshDesc(lp, li, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.0, 0.0, 0.0]),
+                                  radiance=[float(x) for x in rng.uniform(20, 40, 3)]))
+    rgb, tw = sky_envmap(*env_res)
+    sd.env = EnvDesc(rgb, tw, 1.0)
+    sd.env_emitter_index = 4
+    sd.camera = CameraDesc(width, height, look_at((0, 18, 42), (0, 3, 0), (0, 1, 0)), 45.0, 1e-4, 1e4)
+    sd.filter = FilterDesc(2, 2.0, 0.5)
+    sd.depth = depth
+    sd.spp = spp
+    return sd
+
+
+def heterogeneous_cameras(n: int = 8) -> List[np.ndarray]:
+    """Camera-to-world transforms of the 8 views of the heterogeneous scene."""
+    out = []
+    for k in range(n):
+        a = 2 * math.pi * k / n
+        out.append(look_at((42 * math.sin(a), 18, 42 * math.cos(a)), (0, 3, 0), (0, 1, 0)))
+    return out
+
+
+def config2_materials():
+    """The BSDF-batch material set: Beckmann and GGX rough conductors (alpha in
+    {0.05, 0.1, 0.2, 0.3, 0.5}, Cu and Au), rough dielectric IOR 1.5 on the
+    same alpha grid, rough plastic alpha 0.15 / 0.3 with kd 0.5, and a rough
+    coating (alpha 0.2) over a GGX rough conductor."""
+    out = []
+    alphas = [0.05, 0.1, 0.2, 0.3, 0.5]
+    for dist, dn in ((BECKMANN, "beckmann"), (GGX, "ggx")):
+        for metal, eta, k in (("cu", CU_ETA, CU_K), ("au", AU_ETA, AU_K)):
+            for a in alphas:
+                out.append((f"conductor_{dn}_{metal}_a{a}",
+                            BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=dist, alpha_u=a, alpha_v=a, int_ior=1.0,
+                                     ext_ior=1.0, eta=eta, k=k)))
+    for dist, dn in ((BECKMANN, "beckmann"), (GGX, "ggx")):
+        for a in alphas:
+            out.append((f"dielectric_{dn}_a{a}", BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=dist, alpha_u=a,
+                                                          alpha_v=a, int_ior=1.5, ext_ior=1.0)))
+    for a in (0.15, 0.3):
+        out.append((f"plastic_a{a}", BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=a, alpha_v=a,
+                                             kd=[0.5, 0.5, 0.5])))
+    nested = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=1.0, ext_ior=1.0,
+                      eta=CU_ETA, k=CU_K)
+    out.append(("coated_a0.2", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2,
+                                        nested=nested)))
+    return out
+
+
+def bsdf_scene(materials) -> SceneDesc:
+    """A minimal scene holding the given BSDFs (one tiny mesh each) so the BSDF
+    batch entry point can address them by id."""
+    sd = SceneDesc()
+    for i, (_, b) in enumerate(materials):
+        p, idx = quad((i, 0, 0), (i + 0.5, 0, 0), (i + 0.5, 0, 0.5), (i, 0, 0.5))
+        sd.meshes.append(MeshDesc(p, idx, b))
+    sd.camera = CameraDesc(8, 8, np.eye(4, dtype=np.float32), 40.0, 1e-4, 1e4)
+    return sd

@@ -1,0 +1,163 @@
+/*
+ * hikari_b200.h -- C ABI of the B200 pathMIS renderer core.
+ *
+ * The drop-in boundary for Hikari's path-tracing hot path.  In the reference
+ * the per-sample virtual call Integrator::Li (include/core/Integrator.hpp:35)
+ * is driven by RenderBlock (src/Main.cpp:11-44) over TBB blocks
+ * (src/Main.cpp:46-147); here a scene is uploaded once (the Preprocess hook,
+ * include/core/Integrator.hpp:21) and whole images are rendered by one call.
+ *
+ * Conventions: every function returns an int status (HK_OK = 0, negative on
+ * error) and never throws; hk_last_error() returns a thread-local message.
+ * Pointers named *_dev are device (HBM) pointers; all others are host
+ * pointers.  `stream` is a cudaStream_t (NULL = legacy default stream).
+ * Handles are owned by the library and are not thread-safe per handle.
+ */
+#ifndef HIKARI_B200_H
+#define HIKARI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HK_OK 0
+#define HK_ERR_INVALID (-1)   /* bad argument / scene state (HikariException) */
+#define HK_ERR_CUDA (-2)      /* CUDA runtime error */
+#define HK_ERR_NOMEM (-3)     /* device allocation failed */
+#define HK_ERR_IO (-4)        /* file could not be read or parsed */
+
+typedef struct hk_scene hk_scene;
+
+/* BSDF kinds: XML type names of the reference (include/core/Common.hpp:229-272) */
+#define HK_BSDF_DIFFUSE 0          /* "diffuse"         src/bsdf/DiffuseBSDF.cpp        */
+#define HK_BSDF_ROUGH_CONDUCTOR 1  /* "roughConductor"  src/bsdf/RoughConductorBSDF.cpp */
+#define HK_BSDF_ROUGH_DIELECTRIC 2 /* "roughDielectric" src/bsdf/RoughDielectricBSDF.cpp*/
+#define HK_BSDF_ROUGH_PLASTIC 3    /* "roughPlastic"    src/bsdf/RoughPlasticBSDF.cpp   */
+#define HK_BSDF_ROUGH_COATING 4    /* "roughCoating"    src/bsdf/RoughCoatingBSDF.cpp   */
+#define HK_BECKMANN 0
+#define HK_GGX 1
+
+/* XML properties of one BSDF (the reference's PropertyList for that type).
+ * Replaces the BSDF plugin constructors, e.g. RoughConductorBSDF ctor
+ * (src/bsdf/RoughConductorBSDF.cpp:11). */
+typedef struct {
+    int32_t type;          /* HK_BSDF_* */
+    int32_t distribution;  /* HK_BECKMANN / HK_GGX ("type" property) */
+    int32_t anisotropic;   /* "as" */
+    int32_t nonlinear;     /* roughPlastic "nonlinear" */
+    float alpha_u, alpha_v;/* "alpha" (or "alphaU", "alphaV") */
+    float int_ior, ext_ior;
+    float eta[3];          /* roughConductor relative IOR per channel (intIOR/extIOR) */
+    float k[3];            /* roughConductor "k" */
+    float ks[3];           /* "ks" / "ksReflect" */
+    float ks_refract[3];   /* roughDielectric "ksRefract" */
+    float kd[3];           /* roughPlastic "kd", diffuse "albedo" */
+    float sigma_a[3];      /* roughCoating "sigmaA" */
+    float thickness;       /* roughCoating "thickness" */
+    int32_t nested;        /* roughCoating: id of the nested BSDF (added first), else -1 */
+} hk_bsdf_desc;
+
+typedef struct {
+    uint32_t n_meshes, n_triangles, n_bsdfs, n_emitters;
+    uint32_t n_bvh_nodes, bvh_depth;
+    int32_t env_index;
+    int32_t film_border;
+    float bbox[6];
+    uint64_t device_bytes;
+} hk_scene_info;
+
+const char *hk_last_error(void);
+int hk_version(void);
+
+/* ---- scene construction (Scene::AddChild src/core/Scene.cpp:167 order) ---- */
+int hk_scene_create(hk_scene **out);
+int hk_scene_destroy(hk_scene *s);
+/* Raw bytes of data/BeckmannRFTData.bin (distribution 0) or GGXRFTData.bin (1),
+ * the RoughTransmittance table file (src/core/RoughTransmitance.cpp:9). */
+int hk_scene_set_rft(hk_scene *s, int distribution, const void *bytes, uint64_t nbytes);
+int hk_scene_add_bsdf(hk_scene *s, const hk_bsdf_desc *desc, int32_t *out_id);
+/* Mesh (WavefrontObjMesh, src/mesh/WavefrontObjMesh.cpp:10) in world space:
+ * positions 3*nv floats, indices 3*nt, normals 3*nv or NULL, radiance 3 floats
+ * for an attached area emitter (src/emitter/AreaLight.cpp:8) or NULL. */
+int hk_scene_add_mesh(hk_scene *s, const float *positions, uint32_t nv, const uint32_t *indices, uint32_t nt,
+                      const float *normals, int32_t bsdf, const float *radiance, int32_t *out_id);
+/* Environment emitter (EnvironmentLight ctor, src/emitter/EnvironmentLight.cpp:8):
+ * rgb is H*W*3 floats, row 0 at theta = 0; to_world row-major 4x4. */
+int hk_scene_set_envmap(hk_scene *s, const float *rgb, uint32_t width, uint32_t height, const float *to_world16,
+                        float scale);
+/* PerspectiveCamera (src/camera/PerspectiveCamera.cpp:13): to_world row-major 4x4. */
+int hk_scene_set_camera(hk_scene *s, uint32_t width, uint32_t height, const float *to_world16, float fov_deg,
+                        float near_clip, float far_clip);
+/* Reconstruction filter (src/filter/*.cpp): kind 0 box, 1 tent, 2 gaussian
+ * (p0 = stddev), 3 mitchell (p0 = B, p1 = C). */
+int hk_scene_set_filter(hk_scene *s, int kind, float radius, float p0, float p1);
+int hk_scene_set_background(hk_scene *s, const float *rgb3, int force_background);
+/* Activate every object and upload (Scene::Activate src/core/Scene.cpp:128 +
+ * Integrator::Preprocess): BSDF tables, light CDFs, the BVH, device buffers. */
+int hk_scene_build(hk_scene *s);
+/* Counts and bbox; before hk_scene_build the BVH and device fields are 0. */
+int hk_scene_get_info(const hk_scene *s, hk_scene_info *info);
+/* Parse a Hikari scene XML file through the C++ plugin layer (LoadFromXML,
+ * src/core/Parser.cpp:9) and build it.  data_dir holds the RFT tables.
+ * Returns the pathMIS depth and sampler sampleCount in *depth / *spp. */
+int hk_scene_load_xml(const char *path, const char *data_dir, hk_scene **out, int32_t *depth, int32_t *spp);
+/* Same parse without the build/upload step (host only; hk_scene_build later). */
+int hk_scene_parse_xml(const char *path, const char *data_dir, hk_scene **out, int32_t *depth, int32_t *spp);
+
+/* OpenEXR I/O of the output path (Bitmap, src/core/Bitmap.cpp:14,76): read an
+ * RGB(A) scanline EXR (NONE/ZIPS/ZIP, HALF/FLOAT) -- call with rgb = NULL to
+ * get the size, then with a buffer of capacity >= w*h*3 floats; write an
+ * uncompressed FLOAT RGB EXR from h*w*3 floats. */
+int hk_exr_read(const char *path, int32_t *width, int32_t *height, float *rgb, uint64_t capacity);
+int hk_exr_write(const char *path, int32_t width, int32_t height, const float *rgb);
+
+/* ---- rendering (replaces the Render / RenderBlock loop, src/Main.cpp:11-147) ---- */
+typedef struct {
+    int32_t spp;            /* samples per pixel of this call */
+    int32_t depth;          /* pathMIS "depth" (src/integrator/PathMISIntegrator.cpp:13) */
+    int32_t rr_start;       /* first depth with Russian roulette; 0 = reference behaviour */
+    int32_t sample_offset;  /* index of the first sample (progressive accumulation) */
+    uint64_t seed;
+    int32_t image_index;    /* decorrelates streams of several images of one scene */
+    int32_t spp_per_item;   /* 0 = automatic work split */
+} hk_render_desc;
+
+/* Accumulate spp samples per pixel into film_dev ((H+2B)*(W+2B)*4 floats of
+ * RGB*w and w, B = ceil(radius - 0.5)); counters_dev (optional, 3 x u64) gets
+ * closest-hit rays, shadow rays and dropped (invalid) samples added. */
+int hk_render(hk_scene *s, const hk_render_desc *desc, float *film_dev, unsigned long long *counters_dev,
+              void *stream);
+/* film -> H*W*3 RGB (ImageBlock::ToBitmap, src/core/Block.cpp:61) */
+int hk_film_resolve(hk_scene *s, const float *film_dev, float *rgb_dev, void *stream);
+/* End-to-end call: render into the scene's own film, resolve and copy the
+ * H*W*3 float image to host memory rgb_host.  counters (host, 3) optional. */
+int hk_render_image(hk_scene *s, const hk_render_desc *desc, float *rgb_host, unsigned long long *counters,
+                    void *stream);
+
+/* ---- record-level entry points (parity tests and the BSDF batch) ---- */
+/* Ray queries against the scene accel (Acceleration::RayIntersect,
+ * include/core/Acceleration.hpp:57).  rays_dev: n x 8 floats (o, d, mint,
+ * maxt).  tri_dev: original triangle index or -1 (any_hit: 1/0). */
+int hk_trace(hk_scene *s, uint64_t n, const float *rays_dev, int32_t *tri_dev, float *t_dev, float *u_dev, float *v_dev,
+             int any_hit, unsigned long long *node_visits_dev, void *stream);
+/* BSDF::Sample/Eval/Pdf (include/core/BSDF.hpp:67,78,94) over n records in
+ * the local frame: inputs wi (n x 3), u2 (n x 2), u1 (n, roughDielectric's
+ * Next1D draw, may be NULL), wo (n x 3); outputs (any may be NULL): sampled
+ * wo, weight, pdf of the sample, measure; Eval and Pdf at wo (ESolidAngle). */
+int hk_bsdf_batch(hk_scene *s, int32_t bsdf, uint64_t n, const float *wi_dev, const float *u2_dev, const float *u1_dev,
+                  const float *wo_dev, float *s_wo_dev, float *s_w_dev, float *s_pdf_dev, int32_t *s_measure_dev,
+                  float *e_rgb_dev, float *p_pdf_dev, void *stream);
+/* Emitter::Sample (include/core/Emitter.hpp:77) for emitter e: in n x 8
+ * (ref xyz, u2, u1, -, -), out n x 16 (p, n, wi, pdf, distance, value, -). */
+int hk_emitter_sample(hk_scene *s, int32_t e, uint64_t n, const float *in_dev, float *out_dev, void *stream);
+/* Camera::SampleRay (include/core/Camera.hpp:38): pos n x 2 -> rays n x 8 */
+int hk_camera_rays(hk_scene *s, uint64_t n, const float *pos_dev, float *rays_dev, void *stream);
+/* EnvironmentLight::Eval/Pdf for world directions: n x 3 -> n x 3, n */
+int hk_env_eval(hk_scene *s, uint64_t n, const float *wi_dev, float *rgb_dev, float *pdf_dev, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -62,8 +62,9 @@ def build(ref: str = "/root/reference") -> str:
         _forward(os.path.join(ref, "ext", "eigen", "Eigen", real), os.path.join(shim, f"Eigen\\{name}"))
     _forward(os.path.join(HERE, "ref_shim", "glog_logging.h"), os.path.join(shim, "glog\\logging.h"))
     _forward(os.path.join(ref, "ext", "filesystem", "filesystem", "resolver.h"), os.path.join(shim, "filesystem\\resolver.h"))
+    data = os.path.join(os.path.dirname(HERE), "hikari_b200", "data")   # identical copies of ref data/
     for f in ("BeckmannRFTData.bin", "GGXRFTData.bin"):
-        _link(os.path.join(ref, "data", f), os.path.join(OUT, f"data\\{f}"))
+        _link(os.path.join(data, f), os.path.join(OUT, f"data\\{f}"))
     flags = ["g++", "-std=c++14", "-O2", "-ffp-contract=off", "-fPIC", "-w", "-DWIN32", "-DNDEBUG",
              "-include", os.path.join(HERE, "ref_shim", "prelude.h"),
              "-I", shim, "-I", os.path.join(HERE, "ref_shim"), "-I", os.path.join(ref, "include"),

@@ -1,0 +1,201 @@
+"""Parity of the CUDA core (through the C ABI) with the CPU oracle.
+
+Tolerances: integer outputs (measure, triangle ids) must match exactly;
+float outputs agree within 1e-5 relative -- the ulp differences between
+CUDA's expf/logf/sinf/cosf/powf/atan2f and the host libm are the only source
+of disagreement, the arithmetic order is the reference's.  Rendered images
+are compared statistically (per-pixel z-scores against the oracle's means
+and variances).
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import hikari_b200 as hk  # noqa: E402
+from hikari_b200 import scenes  # noqa: E402
+from hikari_b200.scenedesc import FilterDesc, parse_xml  # noqa: E402
+from oracle.oracle import OracleScene, students_t_test  # noqa: E402
+from tests.gpu_helpers import bsdf_records, rel_close  # noqa: E402
+
+DEV = "cuda:0"
+RTOL = 1e-5
+
+
+@pytest.fixture(scope="module")
+def bsdf_pair():
+    mats = scenes.config2_materials()
+    sd = scenes.bsdf_scene(mats)
+    return mats, hk.Scene.from_desc(sd), OracleScene(sd)
+
+
+def _t(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def test_bsdf_batch_parity(bsdf_pair):
+    mats, gs, os_ = bsdf_pair
+    n = 1 << 17
+    wi, u2, u1, wo = bsdf_records(n, 11)
+    twi, tu2, tu1, two = _t(wi), _t(u2), _t(u1), _t(wo)
+    report = []
+    for i, (name, d) in enumerate(mats):
+        gid = gs.bsdf_ids[id(d)]
+        oid = os_.bsdf_ids[id(d)]
+        g = {k: v.cpu().numpy() for k, v in gs.bsdf_batch(gid, twi, tu2, tu1, two).items()}
+        o = os_.bsdf_batch(oid, wi, u2, u1, wo)
+        np.testing.assert_array_equal(g["s_measure"], o["s_measure"], err_msg=name)
+        for key in ("s_w", "s_pdf", "e_rgb", "p_pdf", "s_wo"):
+            a, b = g[key], o[key]
+            if key == "s_wo":
+                valid = np.any(o["s_w"] != 0, axis=1)
+                a, b = a[valid], b[valid]
+            scale = np.percentile(np.abs(b[np.isfinite(b)]), 99.9) if b.size else 1.0
+            ok = rel_close(a, b, RTOL, atol=1e-6 * scale)
+            frac = ok.mean()
+            report.append((name, key, frac))
+            assert frac >= 0.9999, f"{name} {key}: only {frac:.6f} within {RTOL} relative"
+    worst = min(report, key=lambda r: r[2])
+    print("worst BSDF agreement:", worst)
+
+
+def test_camera_rays_parity():
+    sd = scenes.cornell_box(width=64, height=48)
+    gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    rng = np.random.default_rng(3)
+    pos = np.stack([rng.uniform(0, 64, 4096), rng.uniform(0, 48, 4096)], 1).astype(np.float32)
+    g = gs.camera_rays(_t(pos)).cpu().numpy()
+    o = np.stack([os_.camera_ray(float(p[0]), float(p[1])) for p in pos])
+    assert rel_close(g, o, 1e-6, atol=1e-7).all()
+
+
+def _camera_rays(sd, os_, n, seed):
+    rng = np.random.default_rng(seed)
+    W, H = sd.camera.width, sd.camera.height
+    return np.stack([os_.camera_ray(float(x), float(y)) for x, y in
+                     zip(rng.uniform(0, W, n), rng.uniform(0, H, n))]).astype(np.float32)
+
+
+def test_trace_parity_cornell():
+    sd = scenes.cornell_box(width=64, height=64)
+    gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    rays = _camera_rays(sd, os_, 20000, 5)
+    # add random interior rays (origins inside the box, random directions)
+    rng = np.random.default_rng(9)
+    o = np.stack([rng.uniform(-0.9, 0.9, 20000), rng.uniform(0.1, 1.9, 20000), rng.uniform(-0.9, 0.9, 20000)], 1)
+    d = rng.normal(size=(20000, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    extra = np.concatenate([o, d, np.full((20000, 1), 1e-4), np.full((20000, 1), np.inf)], 1).astype(np.float32)
+    rays = np.concatenate([rays, extra], 0)
+    tri_g, t_g, u_g, v_g, _ = gs.trace(_t(rays))
+    tri_g, t_g = tri_g.cpu().numpy(), t_g.cpu().numpy()
+    tri_o, t_o, u_o, v_o = os_.trace(rays, use_bvh=False)
+    same = tri_g == tri_o
+    # mismatches must be edge/tie cases: the oracle's barycentrics lie within 1e-5 of an edge
+    bad = ~same
+    edge = (np.minimum(np.minimum(u_o, v_o), 1 - u_o - v_o) < 1e-5) | (tri_o < 0) | (tri_g < 0)
+    assert same.mean() > 0.999, f"triangle ids agree on {same.mean():.5f}"
+    assert np.all(edge[bad] | np.isclose(t_g[bad], t_o[bad], rtol=1e-6)), "non-edge triangle mismatch"
+    both = same & (tri_o >= 0)
+    assert rel_close(t_g[both], t_o[both], 1e-6).mean() > 0.999
+    # any-hit agrees on the hit/miss decision
+    any_g = gs.trace(_t(rays), any_hit=True)[0].cpu().numpy()
+    any_o = os_.trace(rays, any_hit=True, use_bvh=False)[0]
+    assert (any_g == any_o).mean() > 0.999
+
+
+def test_area_emitter_sample_parity():
+    sd = scenes.cornell_box(width=16, height=16)
+    gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    rng = np.random.default_rng(4)
+    n = 4096
+    inp = np.zeros((n, 8), np.float32)
+    inp[:, 0] = rng.uniform(-0.9, 0.9, n)
+    inp[:, 1] = rng.uniform(0.1, 1.5, n)
+    inp[:, 2] = rng.uniform(-0.9, 0.9, n)
+    inp[:, 3:6] = rng.random((n, 3))
+    g = gs.emitter_sample(0, _t(inp)).cpu().numpy()
+    o = np.stack([os_.emitter_sample(0, r[:3], (r[3], r[4], r[5])) for r in inp])
+    assert rel_close(g[:, :14], o[:, :14], 1e-5, atol=1e-6).mean() > 0.9999
+
+
+def test_env_emitter_parity():
+    sd = scenes.mesh_heavy("conductor", width=32, height=32, level=2, env_res=(256, 128))
+    gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    e = sd.emitter_order().index(-1)
+    rng = np.random.default_rng(8)
+    n = 4096
+    inp = np.zeros((n, 8), np.float32)
+    inp[:, 0:3] = rng.uniform(-1, 1, (n, 3))
+    inp[:, 3:6] = rng.random((n, 3))
+    g = gs.emitter_sample(e, _t(inp)).cpu().numpy()
+    o = np.stack([os_.emitter_sample(e, r[:3], (r[3], r[4], r[5])) for r in inp])
+    assert rel_close(g[:, :14], o[:, :14], 1e-5, atol=1e-5).mean() > 0.999
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rgb_g, _ = gs.env_eval(_t(d))
+    rgb_o = np.stack([os_.env_eval(x) for x in d])
+    assert rel_close(rgb_g.cpu().numpy(), rgb_o, 1e-6).mean() > 0.999
+
+
+def _render_mean_over_seeds(gs, depth, spp, k, film_shape):
+    means = []
+    for s in range(k):
+        film = torch.zeros(film_shape, dtype=torch.float32, device=DEV)
+        gs.render(film, spp=spp, depth=depth, seed=1000 + s)
+        rgb = torch.empty((gs.desc.camera.height, gs.desc.camera.width, 3), dtype=torch.float32, device=DEV)
+        gs.resolve(film, rgb)
+        c = rgb.cpu().numpy().reshape(-1, 3).mean(0)
+        means.append(c[0] * 0.212671 + c[1] * 0.715160 + c[2] * 0.072169)
+    return np.array(means)
+
+
+@pytest.mark.parametrize("fname", ["test-direct.xml", "test-furnace.xml"])
+def test_render_golden_ttest(golden_dir, fname):
+    """The reference's pathMIS known answers, rendered by the CUDA megakernel:
+    K independent renders of N spp each; t-test of their mean against the
+    reference value (Sidak-corrected like hypothesis::students_t_test)."""
+    import os
+
+    all_scenes = parse_xml(os.path.join(golden_dir, "pa5", fname))
+    mis = [s for s in all_scenes if s.integrator == "pathMIS"]
+    for sd in mis:
+        gs = hk.Scene.from_desc(sd)
+        shape = gs.film_shape()
+        m = _render_mean_over_seeds(gs, sd.depth, 2000, 64, shape)
+        ok, p = students_t_test(m.mean(), m.var(ddof=1), sd.reference, len(m), 0.01, len(all_scenes))
+        assert ok, f"{fname}: GPU mean {m.mean()} vs reference {sd.reference} (p={p})"
+
+
+def test_render_cornell_matches_oracle():
+    """Per-pixel means of the GPU image (box filter) against the oracle's
+    per-pixel means and variances."""
+    sd = scenes.cornell_box(width=48, height=48)
+    sd.filter = FilterDesc(0, 0.5)
+    gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    spp_g, spp_o = 4096, 512
+    img, ctr = gs.render_image(spp_g, sd.depth, seed=7)
+    pix = np.stack(np.meshgrid(np.arange(48), np.arange(48), indexing="xy"), -1).reshape(-1, 2)
+    mean_o, var_o = os_.pixel_stats(pix, spp_o, seed=3)
+    g = img.reshape(-1, 3).astype(np.float64)
+    se = np.sqrt(var_o / spp_g + var_o / spp_o) + 1e-6
+    z = (g - mean_o) / se
+    frac3 = np.mean(np.abs(z) > 3)
+    print("z mean", z.mean(), "frac |z|>3", frac3, "max", np.abs(z).max(), "counters", ctr)
+    assert abs(g.mean() / mean_o.mean() - 1) < 0.01
+    assert frac3 < 0.02
+    assert ctr[0] >= 48 * 48 * spp_g
+
+
+def test_render_rmse_scales_with_spp():
+    """RMSE against a high-spp GPU reference falls like 1/sqrt(spp)."""
+    sd = scenes.cornell_box(width=32, height=32)
+    gs = hk.Scene.from_desc(sd)
+    ref, _ = gs.render_image(16384, sd.depth, seed=99)
+    errs = []
+    for spp in (16, 64, 256):
+        img, _ = gs.render_image(spp, sd.depth, seed=spp)
+        errs.append(np.sqrt(np.mean((img - ref) ** 2)))
+    r1, r2 = errs[0] / errs[1], errs[1] / errs[2]
+    assert 1.5 < r1 < 2.7 and 1.5 < r2 < 2.7, errs
