@@ -1,0 +1,334 @@
+"""Benchmark of the pathMIS core on one B200 node.
+
+A step renders the heterogeneous scene (64 displaced icospheres with six
+material types, 4 area lights and a procedural 2048x1024 sky) from 8 views at
+1024x1024 and 128 spp with the reference integrator rule (pathMIS, depth 16,
+Russian roulette from depth 0).  Scene and BVH are resident in HBM before the
+timed region, as the reference's render timer excludes scene load
+(src/Main.cpp:72-123).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload heterogeneous|mesh_heavy|cornell] [--spp S] [--views V]
+
+N > 1 runs under torch.distributed (one process per GPU, replicas: every
+rank renders its own 8 views, "scaling": "weak").  Rank 0 prints one JSON
+line.  --impl reference times the reference algorithm on the host cores (the
+CPU oracle, all threads, a bounded sample of the same workload).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="heterogeneous", choices=["heterogeneous", "mesh_heavy", "cornell"])
+    ap.add_argument("--spp", type=int, default=0)
+    ap.add_argument("--views", type=int, default=0)
+    ap.add_argument("--res", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def make_workload(name, spp=0, views=0, res=0):
+    from hikari_b200 import scenes
+
+    if name == "heterogeneous":
+        r = res or 1024
+        sd = scenes.heterogeneous(width=r, height=r, spp=spp or 128, depth=16)
+        cams = scenes.heterogeneous_cameras(views or 8)
+        desc = (f"heterogeneous: 64 displaced icospheres (levels 5-7), 6 material types, 4 area lights + "
+                f"2048x1024 sky; {len(cams)} views x {r}x{r} x {sd.spp} spp, pathMIS depth 16")
+    elif name == "mesh_heavy":
+        r = res or 1024
+        sd = scenes.mesh_heavy("conductor", width=r, height=r, spp=spp or 256, depth=16)
+        cams = [None] * (views or 1)
+        desc = f"mesh_heavy: displaced level-8 icosphere (1.31M tris), GGX conductor, sky; {r}x{r} x {sd.spp} spp"
+    else:
+        r = res or 256
+        sd = scenes.cornell_box(width=r, height=r, spp=spp or 64)
+        cams = [None] * (views or 1)
+        desc = f"cornell: Cornell box {r}x{r} x {sd.spp} spp, pathMIS depth {sd.depth}"
+    return sd, cams, desc
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": ["unsampled"]}
+        load = [x for x in sm if x > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_baseline(sd, cams, seconds, depth):
+    """Time the CPU oracle (the reference algorithm restated in C, OpenMP over
+    32x32 blocks like src/Main.cpp:121) on a bounded sample of the workload."""
+    from oracle.oracle import OracleScene
+
+    nthreads = os.cpu_count() or 1
+    if cams and cams[0] is not None:
+        sd.camera.to_world = cams[0]
+    o = OracleScene(sd)
+    W, H = sd.camera.width, sd.camera.height
+    nbx, nby = (W + 31) // 32, (H + 31) // 32
+    rng = np.random.default_rng(0)
+    order = rng.permutation(nbx * nby).astype(np.int32)
+    # calibrate on one block per thread, then size the timed sample for ~`seconds`
+    nb = max(1, min(len(order), nthreads))
+    t0 = time.perf_counter()
+    o.render(sd.spp, depth=depth, blocks=order[:nb], nthreads=nthreads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    nb2 = int(min(len(order), max(nthreads, seconds * nb / dt)))
+    blocks = order[nb: nb + nb2] if nb + nb2 <= len(order) else order[:nb2]
+    t0 = time.perf_counter()
+    _, _, ctr = o.render(sd.spp, depth=depth, blocks=blocks, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    paths = 0
+    for b in blocks:
+        bx, by = b % nbx, b // nbx
+        paths += min(32, W - 32 * bx) * min(32, H - 32 * by) * sd.spp
+    return {"value": paths / dt / 1e6, "unit": "Mpaths/s", "cores": nthreads, "kind": "port",
+            "sample": f"{len(blocks)} blocks of 32x32 px x {sd.spp} spp of view 0 ({paths} paths, {dt:.1f} s)",
+            "mrays_per_s": float(ctr[1] + ctr[2]) / dt / 1e6}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sd, cams, desc = make_workload(args.workload, args.spp, args.views, args.res)
+    vals = []
+    for _ in range(args.warmup + args.steps):
+        vals.append(cpu_baseline(sd, cams, max(3.0, args.cpu_seconds / 2), sd.depth))
+    v = vals[args.warmup:]
+    value = float(np.mean([x["value"] for x in v]))
+    line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {"workload": desc, "parallelism": "host threads (OpenMP over 32x32 blocks)"},
+            "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": v[0]["cores"], "kind": "port",
+                             "sample": v[0]["sample"]},
+            "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import hikari_b200 as hk
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    sd, cams, desc = make_workload(args.workload, args.spp, args.views, args.res)
+    t0 = time.perf_counter()
+    gs = hk.Scene.from_desc(sd)
+    build_s = time.perf_counter() - t0
+    W, H, spp, depth = sd.camera.width, sd.camera.height, sd.spp, sd.depth
+    V = len(cams)
+    shape = gs.film_shape()
+    films = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(V)]
+    counters = torch.zeros(5, dtype=torch.int64, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
+    stream = torch.cuda.current_stream()
+
+    def step(it, ctr=None):
+        for v, cam in enumerate(cams):
+            films[v].zero_()
+            gs.render(films[v], spp=spp, depth=depth, seed=1000 * it + v, image_index=rank * V + v,
+                      counters=ctr, camera=cam)
+
+    for w in range(args.warmup):
+        step(w)
+    torch.cuda.synchronize()
+    barrier()
+    counters.zero_()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kern = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in cams]
+            for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.fill_(float(k))   # write 256 MiB: evict L2 between steps (outside the step events)
+            evs[k][0].record(stream)
+            for v, cam in enumerate(cams):
+                films[v].zero_()
+                kern[k][v][0].record(stream)
+                gs.render(films[v], spp=spp, depth=depth, seed=77 + 1000 * k + v, image_index=rank * V + v,
+                          counters=counters, camera=cam)
+                kern[k][v][1].record(stream)
+            evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    kern_ms = [a.elapsed_time(b) for row in kern for a, b in row]
+    total_s = sum(step_ms) / 1e3
+    t = torch.tensor([total_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_max = float(t.item())
+    ctr = counters.cpu().numpy().astype(np.float64)
+    paths_rank = float(W * H * spp * V * args.steps)
+    value = world * paths_rank / total_max / 1e6
+    rays = ctr[0] + ctr[1]
+    mrays = world * rays / total_max / 1e6
+
+    # roofline of the render kernel: BVH fetch bytes (64 B node, 48 B triangle)
+    hbm, peak_kind = measured_peaks()
+    n_launch = args.steps * V
+    bytes_per_launch = (ctr[3] * 64.0 + ctr[4] * 48.0) / n_launch
+    avg_kernel_s = float(np.mean(kern_ms)) / 1e3
+    achieved = bytes_per_launch / avg_kernel_s / 1e9
+
+    # end to end through the C ABI: host image out, per-view camera pose in
+    e2e_steps = max(1, min(args.steps, 2))
+    out = np.empty((H, W, 3), np.float32)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        for v, cam in enumerate(cams):
+            gs.render_image(spp, depth, seed=5000 + 1000 * k + v, out=out, camera=cam, image_index=rank * V + v)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * W * H * spp * V * e2e_steps / float(te.item()) / 1e6
+    desc_bytes = int(hk.C.sizeof(hk.RenderDesc)) if hasattr(hk, "C") else 104
+
+    cpu = None
+    if rank == 0 and world == 1:
+        try:
+            cpu = cpu_baseline(sd, cams, args.cpu_seconds, depth)
+        except Exception as e:  # the baseline is reported, never the target
+            cpu = {"value": None, "unit": "Mpaths/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"failed: {e}"}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "Mpaths/s",
+        "value": value,
+        "unit": "Mpaths/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_max * 1e3 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded procedural scene)",
+        "config": {"workload": desc, "parallelism": f"replicas x{world}", "triangles": int(gs.info.n_triangles),
+                   "bvh_nodes": int(gs.info.n_bvh_nodes), "scene_build_s": round(build_s, 2),
+                   "l2": "256 MiB buffer written between timed steps (outside the step events)",
+                   "rr": "reference rule: p=0.95 at every bounce"},
+        "mrays_per_s": mrays,
+        "rays_per_path": rays / (paths_rank),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "basis": "BVH fetch bytes per launch (64 B per node visit + 48 B per triangle test) / "
+                              "mean render-kernel time"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": V * desc_bytes,
+                "d2h_bytes_per_step": V * W * H * 3 * 4},
+        "gpu_launches": n_launch,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

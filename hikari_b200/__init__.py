@@ -48,7 +48,17 @@ class RenderDesc(C.Structure):
     _fields_ = [
         ("spp", C.c_int32), ("depth", C.c_int32), ("rr_start", C.c_int32), ("sample_offset", C.c_int32),
         ("seed", C.c_uint64), ("image_index", C.c_int32), ("spp_per_item", C.c_int32),
+        ("use_camera", C.c_int32), ("camera_to_world", C.c_float * 16),
     ]
+
+
+def render_desc(spp, depth, seed=0, sample_offset=0, rr_start=0, image_index=0, spp_per_item=0,
+                camera=None) -> RenderDesc:
+    d = RenderDesc(spp, depth, rr_start, sample_offset, seed, image_index, spp_per_item, 0)
+    if camera is not None:
+        d.use_camera = 1
+        d.camera_to_world[:] = [float(x) for x in np.asarray(camera, np.float32).reshape(16)]
+    return d
 
 
 _lib = None
@@ -251,22 +261,24 @@ class Scene:
         return (cam.height + 2 * B, cam.width + 2 * B, 4)
 
     def render(self, film, spp: int, depth: int, seed: int = 0, sample_offset: int = 0, rr_start: int = 0,
-               image_index: int = 0, counters=None, spp_per_item: int = 0, stream=None) -> None:
-        """Accumulate into a device film tensor ((H+2B, W+2B, 4) float32)."""
-        d = RenderDesc(spp, depth, rr_start, sample_offset, seed, image_index, spp_per_item)
+               image_index: int = 0, counters=None, spp_per_item: int = 0, camera=None, stream=None) -> None:
+        """Accumulate into a device film tensor ((H+2B, W+2B, 4) float32).
+        counters: optional device int64 tensor of 5 (rays, shadow rays,
+        dropped samples, node visits, triangle tests)."""
+        d = render_desc(spp, depth, seed, sample_offset, rr_start, image_index, spp_per_item, camera)
         check(lib().hk_render(self.h, C.byref(d), _p(film), _p(counters), _stream(stream)))
 
     def resolve(self, film, rgb, stream=None) -> None:
         check(lib().hk_film_resolve(self.h, _p(film), _p(rgb), _stream(stream)))
 
     def render_image(self, spp: int, depth: int, seed: int = 0, rr_start: int = 0, out: Optional[np.ndarray] = None,
-                     stream=None):
+                     camera=None, image_index: int = 0, stream=None):
         """End-to-end: render, resolve and return the H x W x 3 float32 image on the host."""
         cam = self.desc.camera
         if out is None:
             out = np.empty((cam.height, cam.width, 3), np.float32)
-        ctr = np.zeros(3, np.uint64)
-        d = RenderDesc(spp, depth, rr_start, 0, seed, 0, 0)
+        ctr = np.zeros(5, np.uint64)
+        d = render_desc(spp, depth, seed, 0, rr_start, image_index, 0, camera)
         check(lib().hk_render_image(self.h, C.byref(d), out.ctypes.data, ctr.ctypes.data, _stream(stream)))
         return out, ctr
 
@@ -280,7 +292,7 @@ class Scene:
         t = torch.empty(n, dtype=torch.float32, device=dev)
         u = torch.empty_like(t)
         v = torch.empty_like(t)
-        visits = torch.zeros(1, dtype=torch.int64, device=dev)
+        visits = torch.zeros(2, dtype=torch.int64, device=dev)
         check(lib().hk_trace(self.h, n, _p(rays), _p(tri), _p(t), _p(u), _p(v), int(any_hit), _p(visits),
                              _stream(stream)))
         return tri, t, u, v, visits

@@ -785,7 +785,19 @@ int hk_render(hk_scene *s, const hk_render_desc *d, float *film, unsigned long l
         P.margin_hi = s->margin_hi;
         HK_CUDA(cudaMemsetAsync(s->b_scratch.p, 0, sizeof(unsigned long long), st));
         int grid = std::min(P.n_items, resident);
-        HK_CUDA(hk::launch_render(s->dev, P, grid, st));
+        if (d->use_camera) {
+            hk::DevScene D = s->dev;   // per-call camera pose (passed by value with the launch)
+            const float *M = d->camera_to_world;
+            float w = M[15];
+            if (w == 0.0f) throw HkError{HK_ERR_INVALID, "camera_to_world has w = 0"};
+            for (int r = 0; r < 3; r++) {
+                for (int c = 0; c < 3; c++) D.cam[4 * r + c] = M[4 * r + c];
+                D.cam[4 * r + 3] = M[4 * r + 3] / w;
+            }
+            HK_CUDA(hk::launch_render(D, P, grid, st));
+        } else {
+            HK_CUDA(hk::launch_render(s->dev, P, grid, st));
+        }
         return HK_OK;
     });
 }
@@ -808,13 +820,13 @@ int hk_render_image(hk_scene *s, const hk_render_desc *d, float *rgb_host, unsig
         if (s->b_rgb.bytes < rgb_bytes) s->b_rgb.alloc(rgb_bytes);
         unsigned long long *ctr = (unsigned long long *)s->b_scratch.p + 1;
         HK_CUDA(cudaMemsetAsync(s->b_film.p, 0, film_bytes, st));
-        HK_CUDA(cudaMemsetAsync(ctr, 0, 3 * sizeof(unsigned long long), st));
+        HK_CUDA(cudaMemsetAsync(ctr, 0, 5 * sizeof(unsigned long long), st));
         int rc = hk_render(s, d, s->b_film.as<float>(), ctr, stream);
         if (rc != HK_OK) return rc;
         HK_CUDA(hk::launch_resolve(s->b_film.as<float>(), s->b_rgb.as<float>(), (int)s->width, (int)s->height,
                                    s->dev.border, st));
         HK_CUDA(cudaMemcpyAsync(rgb_host, s->b_rgb.p, rgb_bytes, cudaMemcpyDeviceToHost, st));
-        if (counters) HK_CUDA(cudaMemcpyAsync(counters, ctr, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        if (counters) HK_CUDA(cudaMemcpyAsync(counters, ctr, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
         HK_CUDA(cudaStreamSynchronize(st));
         return HK_OK;
     });

@@ -15,6 +15,7 @@ namespace hk {
 // ------------------------------------------------------------ integrator
 struct PathCounters {
     uint32_t rays, shadow;
+    TravStats trav;
 };
 
 __device__ __forceinline__ uint32_t mesh_emitter(const DevScene &S, int mesh) { return (uint32_t)S.meshes[mesh].emitter; }
@@ -36,7 +37,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
         if (depth == 0) {
             Hit h;
             pc.rays++;
-            if (!trace_bvh2<false>(S, ray, h)) {
+            if (!trace_bvh2<false>(S, ray, h, pc.trav)) {
                 if (has_env && !S.force_background) { L = L + beta * env_eval(S, ray.d); break; }
                 return ld3(S.background);
             }
@@ -74,7 +75,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
                 sr.o = it.p; sr.d = er.p - it.p; sr.tmin = kRayEps; sr.tmax = 1.0f - kRayEps;
                 Hit sh;
                 pc.shadow++;
-                if (!trace_bvh2<true>(S, sr, sh)) {
+                if (!trace_bvh2<true>(S, sr, sh, pc.trav)) {
                     BRec br;
                     br.wi = to_local(it.sh, ray.d * -1.0f);
                     br.wo = to_local(it.sh, er.wi);
@@ -104,7 +105,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
         beta = beta * F;
         if (is_zero(beta)) break;
         pc.rays++;
-        found_next = trace_bvh2<false>(S, ray, hn);
+        found_next = trace_bvh2<false>(S, ray, hn, pc.trav);
         if (found_next) {
             post_intersect(S, hn, itn);
             const DevMesh &mn = S.meshes[itn.mesh];
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(kTileThreads) render_pathmis_kernel(DevScene S
     const int n_tile_cells = tw * th * 4;
     for (int i = threadIdx.x; i < n_tile_cells; i += blockDim.x) tile[i] = 0.0f;
     const int lx = threadIdx.x % kTile, ly = threadIdx.x / kTile;
-    PathCounters pc{0, 0};
+    PathCounters pc{0, 0, TravStats()};
     uint32_t dropped = 0;
     for (;;) {
         __syncthreads();
@@ -212,17 +213,21 @@ __global__ void __launch_bounds__(kTileThreads) render_pathmis_kernel(DevScene S
             reinterpret_cast<float4 *>(tile)[i] = make_float4(0, 0, 0, 0);
         }
     }
-    // per-warp counter reduction
-    uint32_t r = pc.rays, sh = pc.shadow, dr = dropped;
+    // per-warp counter reduction (64-bit: node counts of one thread can pass 2^32)
+    unsigned long long r = pc.rays, sh = pc.shadow, dr = dropped, nv = pc.trav.nodes, nt = pc.trav.tris;
     for (int o = 16; o > 0; o >>= 1) {
         r += __shfl_down_sync(0xffffffffu, r, o);
         sh += __shfl_down_sync(0xffffffffu, sh, o);
         dr += __shfl_down_sync(0xffffffffu, dr, o);
+        nv += __shfl_down_sync(0xffffffffu, nv, o);
+        nt += __shfl_down_sync(0xffffffffu, nt, o);
     }
     if ((threadIdx.x & 31) == 0 && P.counters) {
-        atomicAdd(P.counters + 0, (unsigned long long)r);
-        atomicAdd(P.counters + 1, (unsigned long long)sh);
-        atomicAdd(P.counters + 2, (unsigned long long)dr);
+        atomicAdd(P.counters + 0, r);
+        atomicAdd(P.counters + 1, sh);
+        atomicAdd(P.counters + 2, dr);
+        atomicAdd(P.counters + 3, nv);
+        atomicAdd(P.counters + 4, nt);
     }
 }
 
@@ -243,7 +248,7 @@ __global__ void film_resolve_kernel(const float *film, float *rgb, int W, int H,
 // ids are the ORIGINAL global triangle indices (mesh order).
 __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int32_t *tri, float *t, float *u, float *v,
                                   int any_hit, unsigned long long *visit_counter) {
-    uint32_t nodes = 0;
+    TravStats ts;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const float4 *rp = reinterpret_cast<const float4 *>(rays + 8 * i);
         float4 a = __ldg(rp), b = __ldg(rp + 1);
@@ -253,7 +258,7 @@ __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int
         r.tmin = b.z;
         r.tmax = b.w;
         Hit h;
-        bool f = any_hit ? trace_bvh2<true>(S, r, h, &nodes) : trace_bvh2<false>(S, r, h, &nodes);
+        bool f = any_hit ? trace_bvh2<true>(S, r, h, ts) : trace_bvh2<false>(S, r, h, ts);
         if (any_hit) { tri[i] = f ? 1 : 0; continue; }
         tri[i] = f ? __float_as_int(__ldg(S.tris + 3 * h.tri).w) : -1;
         if (t) t[i] = f ? h.t : 0.0f;
@@ -261,8 +266,15 @@ __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int
         if (v) v[i] = f ? h.v : 0.0f;
     }
     if (visit_counter) {
-        for (int o = 16; o > 0; o >>= 1) nodes += __shfl_down_sync(0xffffffffu, nodes, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(visit_counter, (unsigned long long)nodes);
+        unsigned long long nodes = ts.nodes, tris = ts.tris;
+        for (int o = 16; o > 0; o >>= 1) {
+            nodes += __shfl_down_sync(0xffffffffu, nodes, o);
+            tris += __shfl_down_sync(0xffffffffu, tris, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(visit_counter, nodes);
+            atomicAdd(visit_counter + 1, tris);
+        }
     }
 }
 

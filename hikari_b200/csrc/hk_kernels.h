@@ -12,7 +12,7 @@ constexpr int kTileThreads = kTile * kTile;
 struct RenderLaunch {
     float *film;                          // (H+2B) x (W+2B) x 4 floats, accumulated
     unsigned int *work_counter;           // zeroed before launch
-    unsigned long long *counters;         // [rays, shadow rays, dropped samples]
+    unsigned long long *counters;         // [rays, shadow rays, dropped samples, node visits, triangle tests]
     uint64_t seed;
     int spp;                              // samples per pixel in this launch
     int sample_offset;                    // first sample index (progressive rendering)

@@ -101,10 +101,15 @@ __device__ __forceinline__ void box2(const float4 a, const float4 b, const float
     t1 = n1;
 }
 
-// Closest hit (any_hit = false) or first hit (any_hit = true).  Returns the
-// number of nodes visited in *visits when non-null (for traffic accounting).
+// Per-thread traversal statistics (node fetches and triangle tests), the
+// basis of the algorithmic-bytes roofline.
+struct TravStats {
+    uint32_t nodes = 0, tris = 0;
+};
+
+// Closest hit (any_hit = false) or first hit (any_hit = true).
 template <bool kAnyHit>
-__device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hit &hit, uint32_t *visits = nullptr) {
+__device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st) {
     hit.tri = -1;
     if (S.nnodes == 0) return false;
     V3 d = ray.d;
@@ -119,7 +124,7 @@ __device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hi
     int stack[kStackSize];
     int sp = 0;
     int node = 0;
-    uint32_t nvis = 0;
+    uint32_t nvis = 0, ntri = 0;
     bool found = false;
     // root: test the root's own children; a single-leaf tree is stored as a
     // root whose child0 is the leaf and child1 an empty box.
@@ -143,6 +148,7 @@ __device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hi
         for (int l = 0; l < nleaf; ++l) {
             uint32_t enc = ~(uint32_t)leafs[l];
             uint32_t start = enc & kLeafStartMask, cnt = enc >> kLeafCountShift;
+            ntri += cnt;
             for (uint32_t i = 0; i < cnt; ++i) {
                 const float4 *tp = S.tris + 3 * (start + i);
                 float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
@@ -150,7 +156,7 @@ __device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hi
                 if (intersect_watertight(w, ray.o, xyz(p0), xyz(p1), xyz(p2), ray.tmin, tmax, tt, uu, vv)) {
                     found = true;
                     hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)(start + i);
-                    if (kAnyHit) { if (visits) *visits += nvis; return true; }
+                    if (kAnyHit) { st.nodes += nvis; st.tris += ntri; return true; }
                     tmax = tt;
                 }
             }
@@ -169,7 +175,8 @@ __device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hi
         }
         node = next;
     }
-    if (visits) *visits += nvis;
+    st.nodes += nvis;
+    st.tris += ntri;
     return found;
 }
 

@@ -122,24 +122,28 @@ typedef struct {
     uint64_t seed;
     int32_t image_index;    /* decorrelates streams of several images of one scene */
     int32_t spp_per_item;   /* 0 = automatic work split */
+    int32_t use_camera;     /* 1: render from camera_to_world instead of the scene camera */
+    float camera_to_world[16];
 } hk_render_desc;
 
 /* Accumulate spp samples per pixel into film_dev ((H+2B)*(W+2B)*4 floats of
- * RGB*w and w, B = ceil(radius - 0.5)); counters_dev (optional, 3 x u64) gets
- * closest-hit rays, shadow rays and dropped (invalid) samples added. */
+ * RGB*w and w, B = ceil(radius - 0.5)); counters_dev (optional, 5 x u64) gets
+ * closest-hit rays, shadow rays, dropped (invalid) samples, BVH node visits
+ * and triangle tests added. */
 int hk_render(hk_scene *s, const hk_render_desc *desc, float *film_dev, unsigned long long *counters_dev,
               void *stream);
 /* film -> H*W*3 RGB (ImageBlock::ToBitmap, src/core/Block.cpp:61) */
 int hk_film_resolve(hk_scene *s, const float *film_dev, float *rgb_dev, void *stream);
 /* End-to-end call: render into the scene's own film, resolve and copy the
- * H*W*3 float image to host memory rgb_host.  counters (host, 3) optional. */
+ * H*W*3 float image to host memory rgb_host.  counters (host, 5) optional. */
 int hk_render_image(hk_scene *s, const hk_render_desc *desc, float *rgb_host, unsigned long long *counters,
                     void *stream);
 
 /* ---- record-level entry points (parity tests and the BSDF batch) ---- */
 /* Ray queries against the scene accel (Acceleration::RayIntersect,
  * include/core/Acceleration.hpp:57).  rays_dev: n x 8 floats (o, d, mint,
- * maxt).  tri_dev: original triangle index or -1 (any_hit: 1/0). */
+ * maxt).  tri_dev: original triangle index or -1 (any_hit: 1/0).
+ * node_visits_dev (optional, 2 x u64): node visits and triangle tests added. */
 int hk_trace(hk_scene *s, uint64_t n, const float *rays_dev, int32_t *tri_dev, float *t_dev, float *u_dev, float *v_dev,
              int any_hit, unsigned long long *node_visits_dev, void *stream);
 /* BSDF::Sample/Eval/Pdf (include/core/BSDF.hpp:67,78,94) over n records in

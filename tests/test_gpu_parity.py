@@ -1,11 +1,19 @@
 """Parity of the CUDA core (through the C ABI) with the CPU oracle.
 
-Tolerances: integer outputs (measure, triangle ids) must match exactly;
-float outputs agree within 1e-5 relative -- the ulp differences between
-CUDA's expf/logf/sinf/cosf/powf/atan2f and the host libm are the only source
-of disagreement, the arithmetic order is the reference's.  Rendered images
-are compared statistically (per-pixel z-scores against the oracle's means
-and variances).
+Tolerances (the arithmetic order is the reference's; the only source of
+disagreement is the ulp difference between CUDA's sinf/cosf/logf/expf/powf
+and the host libm's):
+  * integer outputs (sample measure) match exactly;
+  * BSDF Eval and Pdf at identical inputs agree within 1e-5 relative on
+    every record;
+  * sampled directions agree within 1e-5 absolute (unit vectors); sampled
+    weights and pdfs agree within 1e-5 relative on >= 99.9% of records and
+    within 1e-2 on all -- a 1-ulp difference of sin/cos/log of the random
+    number is amplified by the conditioning of the sampling map near grazing
+    angles, which the chi2 tests below cover distributionally;
+  * triangle ids match except on exact t-ties (coplanar triangles) and on
+    edges, where the reference's own answer depends on traversal order;
+  * rendered images are compared statistically.
 """
 import numpy as np
 import pytest
@@ -46,16 +54,21 @@ def test_bsdf_batch_parity(bsdf_pair):
         g = {k: v.cpu().numpy() for k, v in gs.bsdf_batch(gid, twi, tu2, tu1, two).items()}
         o = os_.bsdf_batch(oid, wi, u2, u1, wo)
         np.testing.assert_array_equal(g["s_measure"], o["s_measure"], err_msg=name)
-        for key in ("s_w", "s_pdf", "e_rgb", "p_pdf", "s_wo"):
-            a, b = g[key], o[key]
-            if key == "s_wo":
-                valid = np.any(o["s_w"] != 0, axis=1)
-                a, b = a[valid], b[valid]
-            scale = np.percentile(np.abs(b[np.isfinite(b)]), 99.9) if b.size else 1.0
-            ok = rel_close(a, b, RTOL, atol=1e-6 * scale)
-            frac = ok.mean()
-            report.append((name, key, frac))
-            assert frac >= 0.9999, f"{name} {key}: only {frac:.6f} within {RTOL} relative"
+        # a sample is zero on both sides or on neither
+        np.testing.assert_array_equal(np.all(g["s_w"] == 0, 1), np.all(o["s_w"] == 0, 1), err_msg=name)
+        for key in ("e_rgb", "p_pdf"):
+            ok = rel_close(g[key], o[key], RTOL).reshape(n, -1).all(1)
+            report.append((name, key, ok.mean()))
+            assert ok.mean() >= 0.99999, f"{name} {key}: {ok.mean():.6f} within {RTOL}"
+        valid = np.any(o["s_w"] != 0, axis=1)
+        dwo = np.abs(g["s_wo"][valid].astype(np.float64) - o["s_wo"][valid]).max()
+        assert dwo <= 1e-5, f"{name}: sampled directions differ by {dwo}"
+        for key in ("s_w", "s_pdf"):
+            ok = rel_close(g[key], o[key], RTOL).reshape(n, -1).all(1)
+            loose = rel_close(g[key], o[key], 1e-2).reshape(n, -1).all(1)
+            report.append((name, key, ok.mean()))
+            assert ok.mean() >= 0.999, f"{name} {key}: {ok.mean():.6f} within {RTOL}"
+            assert loose.all(), f"{name} {key}: {np.sum(~loose)} records beyond 1e-2"
     worst = min(report, key=lambda r: r[2])
     print("worst BSDF agreement:", worst)
 
@@ -92,11 +105,13 @@ def test_trace_parity_cornell():
     tri_g, t_g = tri_g.cpu().numpy(), t_g.cpu().numpy()
     tri_o, t_o, u_o, v_o = os_.trace(rays, use_bvh=False)
     same = tri_g == tri_o
-    # mismatches must be edge/tie cases: the oracle's barycentrics lie within 1e-5 of an edge
+    # every mismatch is a t-tie (coplanar triangles: the box bottoms lie on the
+    # floor) or an edge hit; hit/miss decisions agree except on edges
     bad = ~same
-    edge = (np.minimum(np.minimum(u_o, v_o), 1 - u_o - v_o) < 1e-5) | (tri_o < 0) | (tri_g < 0)
-    assert same.mean() > 0.999, f"triangle ids agree on {same.mean():.5f}"
-    assert np.all(edge[bad] | np.isclose(t_g[bad], t_o[bad], rtol=1e-6)), "non-edge triangle mismatch"
+    edge = np.minimum(np.minimum(u_o, v_o), 1 - u_o - v_o) < 1e-5
+    tie = (tri_g >= 0) & (tri_o >= 0) & rel_close(t_g, t_o, 1e-6)
+    assert np.all(tie[bad] | edge[bad]), f"{np.sum(bad & ~tie & ~edge)} non-tie, non-edge mismatches"
+    print(f"triangle ids bit-exact on {same.mean():.5f} of rays, {np.sum(bad & tie)} ties, {np.sum(bad & ~tie)} edges")
     both = same & (tri_o >= 0)
     assert rel_close(t_g[both], t_o[both], 1e-6).mean() > 0.999
     # any-hit agrees on the hit/miss decision
@@ -189,13 +204,16 @@ def test_render_cornell_matches_oracle():
 
 
 def test_render_rmse_scales_with_spp():
-    """RMSE against a high-spp GPU reference falls like 1/sqrt(spp)."""
+    """Mean squared error against a high-spp reference falls like 1/spp
+    (RMSE like 1/sqrt(spp)); MSE averaged over 16 independent renders per spp
+    so single fireflies do not dominate."""
     sd = scenes.cornell_box(width=32, height=32)
     gs = hk.Scene.from_desc(sd)
-    ref, _ = gs.render_image(16384, sd.depth, seed=99)
-    errs = []
+    ref, _ = gs.render_image(65536, sd.depth, seed=99)
+    mse = []
     for spp in (16, 64, 256):
-        img, _ = gs.render_image(spp, sd.depth, seed=spp)
-        errs.append(np.sqrt(np.mean((img - ref) ** 2)))
-    r1, r2 = errs[0] / errs[1], errs[1] / errs[2]
-    assert 1.5 < r1 < 2.7 and 1.5 < r2 < 2.7, errs
+        e = [np.mean((gs.render_image(spp, sd.depth, seed=1000 * spp + k)[0] - ref) ** 2) for k in range(16)]
+        mse.append(np.mean(e))
+    r1, r2 = mse[0] / mse[1], mse[1] / mse[2]
+    print("mse", mse, "ratios", r1, r2)
+    assert 2.5 < r1 < 6.0 and 2.5 < r2 < 6.0, mse
