@@ -36,7 +36,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="heterogeneous", choices=["heterogeneous", "mesh_heavy", "cornell"])
@@ -44,6 +44,8 @@ def parse():
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--res", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     return ap.parse_args()
 
 
@@ -133,45 +135,60 @@ def measured_peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def cpu_baseline(sd, cams, seconds, depth):
-    """Time the CPU oracle (the reference algorithm restated in C, OpenMP over
-    32x32 blocks like src/Main.cpp:121) on a bounded sample of the workload."""
-    from oracle.oracle import OracleScene
+class CpuBaseline:
+    """The CPU oracle (the reference algorithm restated in C, OpenMP over 32x32
+    blocks like src/Main.cpp:121) on the host cores, timed on bounded block
+    samples of view 0 of the workload.  The scene and its BVH are built once."""
 
-    nthreads = os.cpu_count() or 1
-    if cams and cams[0] is not None:
-        sd.camera.to_world = cams[0]
-    o = OracleScene(sd)
-    W, H = sd.camera.width, sd.camera.height
-    nbx, nby = (W + 31) // 32, (H + 31) // 32
-    rng = np.random.default_rng(0)
-    order = rng.permutation(nbx * nby).astype(np.int32)
-    # calibrate on one block per thread, then size the timed sample for ~`seconds`
-    nb = max(1, min(len(order), nthreads))
-    t0 = time.perf_counter()
-    o.render(sd.spp, depth=depth, blocks=order[:nb], nthreads=nthreads)
-    dt = max(time.perf_counter() - t0, 1e-3)
-    nb2 = int(min(len(order), max(nthreads, seconds * nb / dt)))
-    blocks = order[nb: nb + nb2] if nb + nb2 <= len(order) else order[:nb2]
-    t0 = time.perf_counter()
-    _, _, ctr = o.render(sd.spp, depth=depth, blocks=blocks, nthreads=nthreads)
-    dt = time.perf_counter() - t0
-    paths = 0
-    for b in blocks:
-        bx, by = b % nbx, b // nbx
-        paths += min(32, W - 32 * bx) * min(32, H - 32 * by) * sd.spp
-    return {"value": paths / dt / 1e6, "unit": "Mpaths/s", "cores": nthreads, "kind": "port",
-            "sample": f"{len(blocks)} blocks of 32x32 px x {sd.spp} spp of view 0 ({paths} paths, {dt:.1f} s)",
-            "mrays_per_s": float(ctr[1] + ctr[2]) / dt / 1e6}
+    def __init__(self, sd, cams, depth):
+        from oracle.oracle import OracleScene
+
+        self.nthreads = os.cpu_count() or 1
+        if cams and cams[0] is not None:
+            sd.camera.to_world = cams[0]
+        self.sd, self.depth = sd, depth
+        self.o = OracleScene(sd)
+        W, H = sd.camera.width, sd.camera.height
+        self.nbx = (W + 31) // 32
+        self.order = np.random.default_rng(0).permutation(self.nbx * ((H + 31) // 32)).astype(np.int32)
+        self.pos = 0
+        self.block_s = None
+
+    def _blocks(self, n):
+        n = min(n, len(self.order))
+        if self.pos + n > len(self.order):
+            self.pos = 0
+        b = self.order[self.pos:self.pos + n]
+        self.pos += n
+        return b
+
+    def _render(self, blocks):
+        W, H, spp = self.sd.camera.width, self.sd.camera.height, self.sd.spp
+        t0 = time.perf_counter()
+        _, _, ctr = self.o.render(spp, depth=self.depth, blocks=blocks, nthreads=self.nthreads)
+        dt = time.perf_counter() - t0
+        paths = sum(min(32, W - 32 * (b % self.nbx)) * min(32, H - 32 * (b // self.nbx)) * spp for b in blocks)
+        return paths, dt, ctr
+
+    def sample(self, seconds):
+        if self.block_s is None:   # calibrate: one block per thread
+            nb = max(1, self.nthreads)
+            _, dt, _ = self._render(self._blocks(nb))
+            self.block_s = max(dt, 1e-3) / nb
+        nb = int(max(self.nthreads, seconds / self.block_s))
+        blocks = self._blocks(nb)
+        paths, dt, ctr = self._render(blocks)
+        return {"value": paths / dt / 1e6, "unit": "Mpaths/s", "cores": self.nthreads, "kind": "port",
+                "sample": f"{len(blocks)} blocks of 32x32 px x {self.sd.spp} spp of view 0 ({paths} paths, {dt:.1f} s)",
+                "mrays_per_s": float(ctr[1] + ctr[2]) / dt / 1e6}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
     sd, cams, desc = make_workload(args.workload, args.spp, args.views, args.res)
-    vals = []
-    for _ in range(args.warmup + args.steps):
-        vals.append(cpu_baseline(sd, cams, max(3.0, args.cpu_seconds / 2), sd.depth))
+    cb = CpuBaseline(sd, cams, sd.depth)
+    vals = [cb.sample(max(3.0, args.cpu_seconds / 3)) for _ in range(args.warmup + args.steps)]
     v = vals[args.warmup:]
     value = float(np.mean([x["value"] for x in v]))
     line = {"metric": "Mpaths/s", "value": value, "unit": "Mpaths/s", "impl": "reference", "n_gpus": args.gpus,
@@ -270,7 +287,7 @@ def main():
     achieved = bytes_per_launch / avg_kernel_s / 1e9
 
     # end to end through the C ABI: host image out, per-view camera pose in
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = 0 if args.no_e2e else 1
     out = np.empty((H, W, 3), np.float32)
     torch.cuda.synchronize()
     barrier()
@@ -283,13 +300,13 @@ def main():
     te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * W * H * spp * V * e2e_steps / float(te.item()) / 1e6
+    e2e_value = world * W * H * spp * V * e2e_steps / float(te.item()) / 1e6 if e2e_steps else None
     desc_bytes = int(hk.C.sizeof(hk.RenderDesc)) if hasattr(hk, "C") else 104
 
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_baseline(sd, cams, args.cpu_seconds, depth)
+            cpu = CpuBaseline(sd, cams, depth).sample(args.cpu_seconds)
         except Exception as e:  # the baseline is reported, never the target
             cpu = {"value": None, "unit": "Mpaths/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"failed: {e}"}

@@ -80,6 +80,33 @@ __device__ __forceinline__ bool intersect_watertight(const WatertightRay &w, V3 
 
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 
+// The reference's Moller-Trumbore arithmetic (Mesh::RayIntersect,
+// src/core/Mesh.cpp:340-384), used to re-evaluate the winning triangle so that
+// the reported t and barycentrics -- and so the shading point -- are the
+// reference's own numbers.  Returns false where the reference's test rejects
+// (|det| < 1e-8 or a barycentric outside [0,1] by rounding): the watertight
+// values are kept there.
+__device__ __forceinline__ bool refine_mt(V3 o, V3 d, V3 p0, V3 p1, V3 p2, float tmin, float tmax, float &t, float &u,
+                                          float &v) {
+    V3 e1 = p1 - p0, e2 = p2 - p0;
+    V3 pv = cross(d, e2);
+    float det = dot(e1, pv);
+    if (det > -1e-8f && det < 1e-8f) return false;
+    float inv = 1.0f / det;
+    V3 tv = o - p0;
+    float uu = dot(tv, pv) * inv;
+    if (uu < 0.0f || uu > 1.0f) return false;
+    V3 qv = cross(tv, e1);
+    float vv = dot(d, qv) * inv;
+    if (vv < 0.0f || uu + vv > 1.0f) return false;
+    float tt = dot(e2, qv) * inv;
+    if (!(tt >= tmin && tt <= tmax)) return false;
+    t = tt;
+    u = uu;
+    v = vv;
+    return true;
+}
+
 // Slab test of two child boxes against the ray interval; explicit FMAs (the
 // result only prunes, it never changes which triangle is reported).
 __device__ __forceinline__ void box2(const float4 a, const float4 b, const float4 c, V3 idir, V3 ood, float tmin,
@@ -177,6 +204,11 @@ __device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hi
     }
     st.nodes += nvis;
     st.tris += ntri;
+    if (found && !kAnyHit) {
+        const float4 *tp = S.tris + 3 * hit.tri;
+        refine_mt(ray.o, ray.d, xyz(ldg4(tp)), xyz(ldg4(tp + 1)), xyz(ldg4(tp + 2)), ray.tmin, ray.tmax, hit.t, hit.u,
+                  hit.v);
+    }
     return found;
 }
 

@@ -5,7 +5,16 @@ frequencies from integrating Pdf over each cell, cells with expected
 frequency below 5 pooled, Sidak-corrected significance 0.01.  Unlike the
 reference test harness (which passes a null sampler, freezing the rough
 dielectric's reflect/refract choice), the dielectric's Next1D draw is a real
-uniform, so both lobes are tested."""
+uniform, so both lobes are tested.
+
+The reference's GGX rough dielectric is not self-consistent:
+RoughDielectricBSDF::Pdf (src/bsdf/RoughDielectricBSDF.cpp:221-281) has no
+orientation check, so it gives density to grazing refraction configurations
+that Sample never produces (GGX's heavy tails make this visible; the Beckmann
+variant passes).  The CPU oracle -- bit-exact with the reference's BSDF code --
+fails that case the same way, so GGX rough dielectrics are checked by the
+two-sample test against the oracle's own sampling instead, which every
+material must pass."""
 import numpy as np
 import pytest
 
@@ -21,9 +30,9 @@ SUB = 24                      # Simpson intervals per cell and axis (even)
 N_SAMPLES = 10_000_000
 
 
-def simpson_weights(n_cells, sub):
-    n = n_cells * sub
-    w = np.ones(n + 1)
+def simpson_weights(sub):
+    """Composite Simpson weights of one cell: [1, 4, 2, 4, ..., 2, 4, 1] / 3."""
+    w = np.ones(sub + 1)
     w[1:-1:2] = 4
     w[2:-1:2] = 2
     return w / 3.0
@@ -48,13 +57,13 @@ def expected_frequencies(gs, bid, wi):
     zeros2 = torch.zeros((n, 2), dtype=torch.float32, device=dev)
     out = gs.bsdf_batch(bid, twi, zeros2, None, torch.from_numpy(wo).to(dev))
     pdf = out["p_pdf"].cpu().numpy().astype(np.float64).reshape(nt + 1, npd + 1)
-    wt = simpson_weights(RES_T, SUB) * (2.0 / nt)
-    wp = simpson_weights(RES_P, SUB) * (2 * np.pi / npd)
+    wt = simpson_weights(SUB) * (2.0 / nt)
+    wp = simpson_weights(SUB) * (2 * np.pi / npd)
     exp = np.zeros((RES_T, RES_P))
     for i in range(RES_T):
         for j in range(RES_P):
             blk = pdf[i * SUB:(i + 1) * SUB + 1, j * SUB:(j + 1) * SUB + 1]
-            exp[i, j] = wt[: SUB + 1] @ blk @ wp[: SUB + 1]
+            exp[i, j] = wt @ blk @ wp
     return exp * N_SAMPLES
 
 
@@ -77,15 +86,29 @@ def observed_frequencies(gs, bid, wi, seed):
     return hist.cpu().numpy().astype(np.float64).reshape(RES_T, RES_P)
 
 
-def test_bsdf_sampling_chi2(bsdf_scene):
-    mats, gs = bsdf_scene
+def _wi_list(n):
     rng = np.random.default_rng(2024)
-    failures = []
-    for k, (name, d) in enumerate(mats):
+    out = []
+    for _ in range(n):
         ct = rng.random()
         phi = 2 * np.pi * rng.random()
         st = np.sqrt(max(0.0, 1 - ct * ct))
-        wi = np.array([np.cos(phi) * st, np.sin(phi) * st, ct], np.float32)
+        out.append(np.array([np.cos(phi) * st, np.sin(phi) * st, ct], np.float32))
+    return out
+
+
+def _self_consistent(name):
+    return not name.startswith("dielectric_ggx")
+
+
+def test_bsdf_sampling_chi2(bsdf_scene):
+    mats, gs = bsdf_scene
+    wis = _wi_list(len(mats))
+    failures = []
+    for k, (name, d) in enumerate(mats):
+        if not _self_consistent(name):
+            continue
+        wi = wis[k]
         bid = gs.bsdf_ids[id(d)]
         obs = observed_frequencies(gs, bid, wi, seed=k)
         exp = expected_frequencies(gs, bid, wi)
@@ -93,4 +116,59 @@ def test_bsdf_sampling_chi2(bsdf_scene):
         print(f"{name:30s} p={p:.4f} {msg}")
         if not ok:
             failures.append((name, p, msg))
+    assert not failures, failures
+
+
+def _histogram(wo):
+    tb = np.clip(np.floor((wo[:, 2] * 0.5 + 0.5) * RES_T).astype(np.int64), 0, RES_T - 1)
+    sp = np.arctan2(wo[:, 1], wo[:, 0]) / (2 * np.pi)
+    sp = np.where(sp < 0, sp + 1, sp)
+    pb = np.clip(np.floor(sp * RES_P).astype(np.int64), 0, RES_P - 1)
+    return np.bincount(tb * RES_P + pb, minlength=RES_T * RES_P).astype(np.float64)
+
+
+def two_sample_chi2(x, y, min_count=10):
+    """Chi-square homogeneity test of two histograms with different totals
+    (cells with fewer than min_count combined samples pooled)."""
+    from scipy import stats
+
+    n1, n2 = x.sum(), y.sum()
+    k1, k2 = np.sqrt(n2 / n1), np.sqrt(n1 / n2)
+    big = (x + y) >= min_count
+    xs, ys = list(x[big]), list(y[big])
+    if (~big).any() and (x[~big] + y[~big]).sum() > 0:
+        xs.append(x[~big].sum())
+        ys.append(y[~big].sum())
+    xs, ys = np.array(xs), np.array(ys)
+    chsq = np.sum((k1 * xs - k2 * ys) ** 2 / (xs + ys))
+    dof = len(xs) - 1
+    return 1 - stats.chi2.cdf(chsq, dof), chsq, dof
+
+
+def test_bsdf_sampling_matches_oracle(bsdf_scene):
+    """The GPU samples and the oracle's samples (the reference's sampling
+    restated bit-exactly) come from the same distribution: two-sample chi2 on
+    the same 20 x 40 grid, Sidak-corrected over all materials."""
+    from oracle.oracle import OracleScene
+
+    mats, gs = bsdf_scene
+    os_ = OracleScene(scenes.bsdf_scene(mats))
+    wis = _wi_list(len(mats))
+    n_o = 2_000_000
+    alpha = 1.0 - (1.0 - 0.01) ** (1.0 / len(mats))
+    failures = []
+    for k, (name, d) in enumerate(mats):
+        wi = wis[k]
+        obs_g = observed_frequencies(gs, gs.bsdf_ids[id(d)], wi, seed=100 + k).ravel()
+        r = np.random.default_rng(500 + k)
+        u2 = r.random((n_o, 2), dtype=np.float32)
+        u1 = r.random(n_o, dtype=np.float32)
+        W = np.ascontiguousarray(np.repeat(wi[None, :], n_o, 0))
+        out = os_.bsdf_batch(os_.bsdf_ids[id(d)], W, u2, u1, W)
+        ok = np.any(out["s_w"] != 0, 1)
+        obs_o = _histogram(out["s_wo"][ok])
+        p, chsq, dof = two_sample_chi2(obs_g, obs_o)
+        print(f"{name:30s} two-sample p={p:.4f} chi2={chsq:.1f} dof={dof}")
+        if p < alpha:
+            failures.append((name, p))
     assert not failures, failures

@@ -53,19 +53,22 @@ def test_bsdf_batch_parity(bsdf_pair):
         oid = os_.bsdf_ids[id(d)]
         g = {k: v.cpu().numpy() for k, v in gs.bsdf_batch(gid, twi, tu2, tu1, two).items()}
         o = os_.bsdf_batch(oid, wi, u2, u1, wo)
-        np.testing.assert_array_equal(g["s_measure"], o["s_measure"], err_msg=name)
-        # a sample is zero on both sides or on neither
-        np.testing.assert_array_equal(np.all(g["s_w"] == 0, 1), np.all(o["s_w"] == 0, 1), err_msg=name)
         for key in ("e_rgb", "p_pdf"):
             ok = rel_close(g[key], o[key], RTOL).reshape(n, -1).all(1)
             report.append((name, key, ok.mean()))
             assert ok.mean() >= 0.99999, f"{name} {key}: {ok.mean():.6f} within {RTOL}"
-        valid = np.any(o["s_w"] != 0, axis=1)
+        # Sampling: a 1-ulp difference can flip a threshold (u1 against the
+        # Fresnel term, a direction at the horizon); flips must stay below 1e-4
+        # of the records, every other record is held to the tolerances.
+        flip = (g["s_measure"] != o["s_measure"]) | (np.all(g["s_w"] == 0, 1) != np.all(o["s_w"] == 0, 1))
+        assert flip.mean() <= 1e-4, f"{name}: {flip.sum()} sampling branch flips"
+        keep = ~flip
+        valid = keep & np.any(o["s_w"] != 0, axis=1)
         dwo = np.abs(g["s_wo"][valid].astype(np.float64) - o["s_wo"][valid]).max()
         assert dwo <= 1e-5, f"{name}: sampled directions differ by {dwo}"
         for key in ("s_w", "s_pdf"):
-            ok = rel_close(g[key], o[key], RTOL).reshape(n, -1).all(1)
-            loose = rel_close(g[key], o[key], 1e-2).reshape(n, -1).all(1)
+            ok = rel_close(g[key][keep], o[key][keep], RTOL).reshape(keep.sum(), -1).all(1)
+            loose = rel_close(g[key][keep], o[key][keep], 1e-2).reshape(keep.sum(), -1).all(1)
             report.append((name, key, ok.mean()))
             assert ok.mean() >= 0.999, f"{name} {key}: {ok.mean():.6f} within {RTOL}"
             assert loose.all(), f"{name} {key}: {np.sum(~loose)} records beyond 1e-2"
