@@ -94,6 +94,7 @@ def lib():
         "hk_render": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
         "hk_film_resolve": ([P, P, P, P], C.c_int),
         "hk_render_image": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
+        "hk_render_image_static": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
         "hk_trace": ([P, U64, P, P, P, P, P, C.c_int, P, P], C.c_int),
         "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
         "hk_emitter_sample": ([P, I32, U64, P, P, P], C.c_int),
@@ -281,6 +282,14 @@ class Scene:
         d = render_desc(spp, depth, seed, 0, rr_start, image_index, 0, camera)
         check(lib().hk_render_image(self.h, C.byref(d), out.ctypes.data, ctr.ctypes.data, _stream(stream)))
         return out, ctr
+
+    def render_image_static(self, out, spp: int, depth: int, seed: int = 0, rr_start: int = 0, counters=None,
+                            camera=None, image_index: int = 0, stream=None) -> None:
+        """Render into the device tensor `out` (H x W x 3 float32) through the
+        entry point that allocates no device memory (static scratch; films up
+        to 520 x 520 including the filter border)."""
+        d = render_desc(spp, depth, seed, 0, rr_start, image_index, 0, camera)
+        check(lib().hk_render_image_static(self.h, C.byref(d), _p(out), _p(counters), _stream(stream)))
 
     # ------------------------------------------------------------ record queries
     def trace(self, rays, any_hit: bool = False, stream=None):

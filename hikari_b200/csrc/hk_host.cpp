@@ -831,6 +831,73 @@ int hk_render_image(hk_scene *s, const hk_render_desc *d, float *rgb_host, unsig
         return HK_OK;
     });
 }
+// Render without any device allocation: the work counter, the counters and the
+// film accumulator live in the library's static scratch (hk_kernels.cu); the
+// caller supplies the output image.  Asynchronous on `stream`.
+int hk_render_image_static(hk_scene *s, const hk_render_desc *d, float *rgb_dev, unsigned long long *counters_dev,
+                           void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (!d || !rgb_dev) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (d->spp <= 0 || d->depth < 0) throw HkError{HK_ERR_INVALID, "spp must be > 0 and depth >= 0"};
+        const size_t FW = s->width + 2 * s->dev.border, FH = s->height + 2 * s->dev.border;
+        const size_t film_floats = FW * FH * 4;
+        if (film_floats > hk::kStaticFilmFloats)
+            throw HkError{HK_ERR_INVALID, "image of " + std::to_string(s->width) + "x" + std::to_string(s->height) +
+                                              " with filter border " + std::to_string(s->dev.border) + " needs " +
+                                              std::to_string(film_floats) + " film floats; the static scratch holds " +
+                                              std::to_string(hk::kStaticFilmFloats) +
+                                              " (up to 512x512 pixels at border 4); use hk_render"};
+        void *scratch = nullptr;
+        HK_CUDA(hk::static_render_scratch(&scratch));
+        cudaStream_t st = (cudaStream_t)stream;
+        unsigned long long *hdr = (unsigned long long *)scratch;
+        float *film = (float *)(hdr + hk::kStaticHeaderWords);
+        // the array keeps the previous call's contents: clear what must start at zero
+        HK_CUDA(cudaMemsetAsync(hdr, 0, hk::kStaticHeaderWords * sizeof(unsigned long long), st));
+        HK_CUDA(cudaMemsetAsync(film, 0, film_floats * sizeof(float), st));
+        hk::RenderLaunch P;
+        std::memset(&P, 0, sizeof P);
+        P.film = film;
+        P.work_counter = (unsigned int *)hdr;
+        P.counters = hdr + 1;
+        P.seed = d->seed;
+        P.spp = d->spp;
+        P.sample_offset = d->sample_offset;
+        P.depth = d->depth;
+        P.rr_start = d->rr_start;
+        P.image_index = d->image_index;
+        P.tiles_x = ((int)s->width + hk::kTile - 1) / hk::kTile;
+        P.tiles_y = ((int)s->height + hk::kTile - 1) / hk::kTile;
+        const int tiles = P.tiles_x * P.tiles_y;
+        const int resident = s->sm_count * s->occupancy;
+        int per_item = d->spp_per_item;
+        if (per_item <= 0) {
+            int chunks = std::max(1, std::min(d->spp, (4 * resident + tiles - 1) / tiles));
+            per_item = (d->spp + chunks - 1) / chunks;
+        }
+        P.spp_per_item = per_item;
+        P.n_chunks = (d->spp + per_item - 1) / per_item;
+        P.n_items = tiles * P.n_chunks;
+        P.margin_lo = s->margin_lo;
+        P.margin_hi = s->margin_hi;
+        const int grid = std::min(P.n_items, resident);
+        hk::DevScene D = s->dev;
+        if (d->use_camera) {
+            const float *M = d->camera_to_world;
+            if (M[15] == 0.0f) throw HkError{HK_ERR_INVALID, "camera_to_world has w = 0"};
+            for (int r = 0; r < 3; r++) {
+                for (int c = 0; c < 3; c++) D.cam[4 * r + c] = M[4 * r + c];
+                D.cam[4 * r + 3] = M[4 * r + 3] / M[15];
+            }
+        }
+        HK_CUDA(hk::launch_render(D, P, grid, st));
+        HK_CUDA(hk::launch_resolve(film, rgb_dev, (int)s->width, (int)s->height, s->dev.border, st));
+        if (counters_dev)
+            HK_CUDA(cudaMemcpyAsync(counters_dev, hdr + 1, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st));
+        return HK_OK;
+    });
+}
 int hk_trace(hk_scene *s, uint64_t n, const float *rays, int32_t *tri, float *t, float *u, float *v, int any_hit,
              unsigned long long *visits, void *stream) {
     return guarded([&] {

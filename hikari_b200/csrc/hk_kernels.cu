@@ -6,6 +6,7 @@
 //   * film_resolve, trace_rays, bsdf_batch and record-query kernels used by
 //     the C-ABI and its parity tests.
 #include <cstdio>
+#include <mutex>
 
 #include "hk_kernels.h"
 #include "hk_shading.cuh"
@@ -345,6 +346,31 @@ __global__ void env_eval_kernel(DevScene S, uint64_t n, const float *wi, float *
         out[3 * i] = c.x; out[3 * i + 1] = c.y; out[3 * i + 2] = c.z;
         if (pdf) pdf[i] = env_pdf(S, d);
     }
+}
+
+// ------------------------------------------------------------ static scratch
+// Scratch for hk_render_image_static, the entry point for callers that cannot
+// allocate device memory.  Every GPU that loads the library holds this array
+// (about 4.3 MB) until the process exits; all calls share it.
+static __device__ __align__(256) unsigned long long g_render_scratch[kStaticScratchWords];
+
+cudaError_t static_render_scratch(void **out) {
+    static std::mutex mu;
+    static void *ptrs[kStaticMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kStaticMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[dev]) {
+        // the host-side name of the array is not a device address: ask the runtime
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_render_scratch);
+        if (e != cudaSuccess) return e;
+        ptrs[dev] = p;
+    }
+    *out = ptrs[dev];
+    return cudaSuccess;
 }
 
 // ------------------------------------------------------------ launchers

@@ -24,6 +24,17 @@ struct RenderLaunch {
     int margin_lo, margin_hi;             // film footprint offsets of a tile pixel
 };
 
+// Static scratch of hk_render_image_static: a 256-byte header ([0] work
+// counter, [1..5] ray/sample counters) followed by the film accumulator, sized
+// for films of up to 512 x 512 pixels with a filter border of up to 4.
+constexpr size_t kStaticHeaderWords = 32;
+constexpr size_t kStaticFilmFloats = 4ull * 520 * 520;
+constexpr size_t kStaticScratchWords = kStaticHeaderWords + kStaticFilmFloats / 2;
+constexpr int kStaticMaxDevices = 64;
+// Device address of the static scratch on the current device (looked up once
+// per device with cudaGetSymbolAddress, then cached).
+cudaError_t static_render_scratch(void **out);
+
 cudaError_t launch_render(const DevScene &S, const RenderLaunch &P, int grid, cudaStream_t st);
 cudaError_t launch_resolve(const float *film, float *rgb, int W, int H, int B, cudaStream_t st);
 cudaError_t launch_trace(const DevScene &S, uint64_t n, const float *rays, int32_t *tri, float *t, float *u, float *v,

@@ -139,6 +139,24 @@ int hk_film_resolve(hk_scene *s, const float *film_dev, float *rgb_dev, void *st
 int hk_render_image(hk_scene *s, const hk_render_desc *desc, float *rgb_host, unsigned long long *counters,
                     void *stream);
 
+/* Render into a caller-provided device image without allocating any device
+ * memory.  This entry point has no counterpart in the reference.  It is for
+ * callers that cannot call cudaMalloc while rendering -- a host application
+ * whose device memory is owned by its own allocator or held to a fixed
+ * budget, or a plugin that may not grow the process's footprint after
+ * start-up.  The scene must already be built (hk_scene_build allocates the
+ * scene itself).  Scratch (work counter, counters, film accumulator) lives in
+ * one static device array of about 4.3 MB that every GPU loading the library
+ * holds until exit; films are limited to (W+2B)*(H+2B) <= 520*520 pixels
+ * (512x512 at a filter border of 4) and larger images are rejected with
+ * HK_ERR_INVALID.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and caches it; make that first call before
+ * any stream capture.  All calls share the array and each call clears it:
+ * calls that overlap on the GPU (other streams, other threads) race.
+ * rgb_dev: H*W*3 floats; counters_dev (optional): 5 x u64 as hk_render. */
+int hk_render_image_static(hk_scene *s, const hk_render_desc *desc, float *rgb_dev, unsigned long long *counters_dev,
+                           void *stream);
+
 /* ---- record-level entry points (parity tests and the BSDF batch) ---- */
 /* Ray queries against the scene accel (Acceleration::RayIntersect,
  * include/core/Acceleration.hpp:57).  rays_dev: n x 8 floats (o, d, mint,
