@@ -26,7 +26,7 @@ from hikari_b200 import scenes  # noqa: E402
 from oracle.oracle import chi2_test  # noqa: E402
 
 RES_T, RES_P = 20, 40
-SUB = 24                      # Simpson intervals per cell and axis (even)
+SUB = 160                     # Simpson intervals per cell and axis (even)
 N_SAMPLES = 10_000_000
 
 
@@ -44,27 +44,40 @@ def bsdf_scene():
     return mats, hk.Scene.from_desc(scenes.bsdf_scene(mats))
 
 
+def _cell_weights(n_cells, h):
+    """(n_cells x n_cells*SUB+1) matrix of per-cell composite Simpson weights."""
+    w = simpson_weights(SUB) * h
+    M = np.zeros((n_cells, n_cells * SUB + 1))
+    for i in range(n_cells):
+        M[i, i * SUB:(i + 1) * SUB + 1] = w
+    return M
+
+
 def expected_frequencies(gs, bid, wi):
-    nt, npd = RES_T * SUB, RES_P * SUB
-    ct = np.linspace(-1.0, 1.0, nt + 1)
-    ph = np.linspace(0.0, 2 * np.pi, npd + 1)
-    C, P = np.meshgrid(ct, ph, indexing="ij")
-    S = np.sqrt(np.maximum(0.0, 1.0 - C * C))
-    wo = np.stack([S * np.cos(P), S * np.sin(P), C], -1).reshape(-1, 3).astype(np.float32)
-    n = wo.shape[0]
+    """Integrate Pdf over each cos(theta) x phi cell with composite Simpson on
+    a SUB x SUB grid per cell (evaluated on the GPU in row chunks)."""
     dev = "cuda"
-    twi = torch.from_numpy(np.repeat(wi[None, :], n, 0)).to(dev)
-    zeros2 = torch.zeros((n, 2), dtype=torch.float32, device=dev)
-    out = gs.bsdf_batch(bid, twi, zeros2, None, torch.from_numpy(wo).to(dev))
-    pdf = out["p_pdf"].cpu().numpy().astype(np.float64).reshape(nt + 1, npd + 1)
-    wt = simpson_weights(SUB) * (2.0 / nt)
-    wp = simpson_weights(SUB) * (2 * np.pi / npd)
-    exp = np.zeros((RES_T, RES_P))
-    for i in range(RES_T):
-        for j in range(RES_P):
-            blk = pdf[i * SUB:(i + 1) * SUB + 1, j * SUB:(j + 1) * SUB + 1]
-            exp[i, j] = wt @ blk @ wp
-    return exp * N_SAMPLES
+    nt, npd = RES_T * SUB, RES_P * SUB
+    ct = torch.linspace(-1.0, 1.0, nt + 1, dtype=torch.float64, device=dev)
+    ph = torch.linspace(0.0, 2 * np.pi, npd + 1, dtype=torch.float64, device=dev)
+    cph, sph = torch.cos(ph), torch.sin(ph)
+    pdf = torch.empty((nt + 1, npd + 1), dtype=torch.float64, device=dev)
+    rows = 256
+    twi = torch.from_numpy(np.ascontiguousarray(np.repeat(wi[None, :], rows * (npd + 1), 0))).to(dev)
+    u2 = torch.zeros((rows * (npd + 1), 2), dtype=torch.float32, device=dev)
+    for r0 in range(0, nt + 1, rows):
+        r1 = min(nt + 1, r0 + rows)
+        c = ct[r0:r1, None]
+        st = torch.sqrt(torch.clamp(1 - c * c, min=0.0))
+        wo = torch.stack([st * cph[None, :], st * sph[None, :], c.expand(-1, npd + 1)], -1).reshape(-1, 3)
+        wo = wo.to(torch.float32).contiguous()
+        n = wo.shape[0]
+        out = gs.bsdf_batch(bid, twi[:n], u2[:n], None, wo)
+        pdf[r0:r1] = out["p_pdf"].reshape(r1 - r0, npd + 1).to(torch.float64)
+    Wt = torch.from_numpy(_cell_weights(RES_T, 2.0 / nt)).to(dev)
+    Wp = torch.from_numpy(_cell_weights(RES_P, 2 * np.pi / npd)).to(dev)
+    exp = Wt @ pdf @ Wp.T
+    return exp.cpu().numpy() * N_SAMPLES
 
 
 def observed_frequencies(gs, bid, wi, seed):

@@ -6,7 +6,8 @@ and the host libm's):
   * integer outputs (sample measure) match exactly;
   * BSDF Eval and Pdf at identical inputs agree within 1e-5 relative on
     every record;
-  * sampled directions agree within 1e-5 absolute (unit vectors); sampled
+  * sampled directions agree within 1e-5 absolute (unit vectors) on >= 99.99%
+    of records and within 1e-3 on all; sampled
     weights and pdfs agree within 1e-5 relative on >= 99.9% of records and
     within 1e-2 on all -- a 1-ulp difference of sin/cos/log of the random
     number is amplified by the conditioning of the sampling map near grazing
@@ -64,8 +65,10 @@ def test_bsdf_batch_parity(bsdf_pair):
         assert flip.mean() <= 1e-4, f"{name}: {flip.sum()} sampling branch flips"
         keep = ~flip
         valid = keep & np.any(o["s_w"] != 0, axis=1)
-        dwo = np.abs(g["s_wo"][valid].astype(np.float64) - o["s_wo"][valid]).max()
-        assert dwo <= 1e-5, f"{name}: sampled directions differ by {dwo}"
+        dwo = np.abs(g["s_wo"][valid].astype(np.float64) - o["s_wo"][valid]).max(1)
+        # the cosine warp's z = sqrt(1 - r^2) is ill-conditioned at the horizon
+        assert np.mean(dwo <= 1e-5) >= 0.9999, f"{name}: sampled directions differ by > 1e-5 on {np.sum(dwo > 1e-5)}"
+        assert dwo.max() <= 1e-3, f"{name}: sampled directions differ by {dwo.max()}"
         for key in ("s_w", "s_pdf"):
             ok = rel_close(g[key][keep], o[key][keep], RTOL).reshape(keep.sum(), -1).all(1)
             loose = rel_close(g[key][keep], o[key][keep], 1e-2).reshape(keep.sum(), -1).all(1)
