@@ -52,6 +52,15 @@ class RenderDesc(C.Structure):
     ]
 
 
+class RenderJob(C.Structure):
+    _fields_ = [("film_dev", C.c_void_p), ("desc", RenderDesc)]
+
+
+class WavefrontConfig(C.Structure):
+    _fields_ = [("capacity", C.c_int32), ("threads_extend", C.c_int32), ("threads_shade", C.c_int32),
+                ("iterations_per_check", C.c_int32), ("no_graph", C.c_int32)]
+
+
 def render_desc(spp, depth, seed=0, sample_offset=0, rr_start=0, image_index=0, spp_per_item=0,
                 camera=None) -> RenderDesc:
     d = RenderDesc(spp, depth, rr_start, sample_offset, seed, image_index, spp_per_item, 0)
@@ -95,6 +104,7 @@ def lib():
         "hk_film_resolve": ([P, P, P, P], C.c_int),
         "hk_render_image": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
         "hk_render_image_static": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
+        "hk_render_batch": ([P, C.POINTER(RenderJob), C.c_int, C.POINTER(WavefrontConfig), P, P], C.c_int),
         "hk_trace": ([P, U64, P, P, P, P, P, C.c_int, P, P], C.c_int),
         "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
         "hk_emitter_sample": ([P, I32, U64, P, P, P], C.c_int),
@@ -282,6 +292,23 @@ class Scene:
         d = render_desc(spp, depth, seed, 0, rr_start, image_index, 0, camera)
         check(lib().hk_render_image(self.h, C.byref(d), out.ctypes.data, ctr.ctypes.data, _stream(stream)))
         return out, ctr
+
+    def render_batch(self, films, spp: int, depth: int, seeds=None, cameras=None, image_indices=None,
+                     sample_offset: int = 0, rr_start: int = 0, counters=None, capacity: int = 0,
+                     threads_extend: int = 0, threads_shade: int = 0, iterations_per_check: int = 0,
+                     no_graph: bool = False, stream=None) -> None:
+        """Wavefront render of several images at once: films[i] (device
+        tensors of film_shape()) accumulate spp samples of view cameras[i]."""
+        n = len(films)
+        jobs = (RenderJob * n)()
+        for i, f in enumerate(films):
+            cam = cameras[i] if cameras is not None else None
+            seed = seeds[i] if seeds is not None else i
+            idx = image_indices[i] if image_indices is not None else i
+            jobs[i].film_dev = _p(f)
+            jobs[i].desc = render_desc(spp, depth, seed, sample_offset, rr_start, idx, 0, cam)
+        cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, int(no_graph))
+        check(lib().hk_render_batch(self.h, jobs, n, C.byref(cfg), _p(counters), _stream(stream)))
 
     def render_image_static(self, out, spp: int, depth: int, seed: int = 0, rr_start: int = 0, counters=None,
                             camera=None, image_index: int = 0, stream=None) -> None:

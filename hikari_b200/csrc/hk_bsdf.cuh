@@ -491,3 +491,35 @@ __device__ __forceinline__ V3 bsdf_sample(const DevBsdf *bs, int id, BRec &r, fl
 }
 
 }  // namespace hk
+
+namespace hk {
+// Dispatch with the top-level BSDF type known at compile time (the wavefront
+// shades one material type per kernel, so each kernel carries one BSDF).
+template <int BT>
+__device__ __forceinline__ V3 bsdf_eval_t(const DevBsdf *bs, int id, const BRec &r) {
+    const DevBsdf &b = bs[id];
+    if constexpr (BT == kDiffuse) return diffuse_eval(b, r);
+    else if constexpr (BT == kRoughConductor) return conductor_eval(b, r);
+    else if constexpr (BT == kRoughDielectric) return dielectric_eval(b, r);
+    else if constexpr (BT == kRoughPlastic) return plastic_eval(b, r);
+    else return coating_eval(b, bs[b.nested], r);
+}
+template <int BT>
+__device__ __forceinline__ float bsdf_pdf_t(const DevBsdf *bs, int id, const BRec &r) {
+    const DevBsdf &b = bs[id];
+    if constexpr (BT == kDiffuse) return diffuse_pdf(r);
+    else if constexpr (BT == kRoughConductor) return conductor_pdf(b, r);
+    else if constexpr (BT == kRoughDielectric) return dielectric_pdf(b, r);
+    else if constexpr (BT == kRoughPlastic) return plastic_pdf(b, r);
+    else return coating_pdf(b, bs[b.nested], r);
+}
+template <int BT>
+__device__ __forceinline__ V3 bsdf_sample_t(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1) {
+    const DevBsdf &b = bs[id];
+    if constexpr (BT == kDiffuse) return diffuse_sample(b, r, ux, uy);
+    else if constexpr (BT == kRoughConductor) return conductor_sample(b, r, ux, uy);
+    else if constexpr (BT == kRoughDielectric) return dielectric_sample(b, r, ux, uy, u1);
+    else if constexpr (BT == kRoughPlastic) return plastic_sample(b, r, ux, uy);
+    else return coating_sample(b, bs[b.nested], r, ux, uy, u1);
+}
+}  // namespace hk

@@ -16,6 +16,7 @@
 #include "hk_bvh.h"
 #include "hk_device.h"
 #include "hk_kernels.h"
+#include "hk_wavefront.h"
 
 extern "C" int hk_scene_load_xml_impl(const char *path, const char *data_dir, hk_scene **out, int32_t *depth,
                                       int32_t *spp, int build, std::string *err);
@@ -270,6 +271,21 @@ struct hk_scene {
     int margin_lo = 0, margin_hi = 0;
     int sm_count = 148;
     int occupancy = 1;
+    // wavefront engine (allocated on first use)
+    struct Wavefront {
+        int capacity = 0, max_shadow = 0;
+        DevBuf state, queues, shadow, counters, jobs, finished;
+        hk::WfState W{};
+        hk::WfCounters *host_ctr = nullptr;   // pinned mirror for termination checks
+        cudaStream_t stream = nullptr;
+        cudaEvent_t ev = nullptr;
+        ~Wavefront() {
+            if (host_ctr) cudaFreeHost(host_ctr);
+            if (stream) cudaStreamDestroy(stream);
+            if (ev) cudaEventDestroy(ev);
+        }
+    };
+    std::unique_ptr<Wavefront> wf;
 };
 
 namespace {
@@ -606,6 +622,40 @@ void require_built(const hk_scene *s) {
     if (!s->built) throw HkError{HK_ERR_INVALID, "scene is not built (call hk_scene_build)"};
 }
 
+// ------------------------------------------------------------ wavefront engine
+void wf_ensure(hk_scene *s, int capacity) {
+    if (s->wf && s->wf->capacity == capacity) return;
+    s->wf.reset(new hk_scene::Wavefront());
+    auto &E = *s->wf;
+    E.capacity = capacity;
+    E.max_shadow = capacity * std::max(1, s->dev.nemitters);
+    const size_t N = (size_t)capacity;
+    // state: 9 float4-sized arrays per slot
+    E.state.alloc(N * 16 * 9);
+    E.queues.alloc(N * sizeof(int) * (2 + hk::kWfTypes + 1));
+    E.shadow.alloc((size_t)E.max_shadow * 16 * 3);
+    E.counters.alloc(sizeof(hk::WfCounters));
+    E.jobs.alloc(sizeof(hk::WfJob) * hk::kWfMaxJobs);
+    E.finished.alloc(sizeof(unsigned long long) * hk::kWfMaxJobs);
+    hk::WfState &W = E.W;
+    W.capacity = capacity;
+    W.max_shadow = E.max_shadow;
+    float4 *st = E.state.as<float4>();
+    W.ray_o = st; W.ray_d = st + N; W.beta = st + 2 * N; W.lacc = st + 3 * N; W.pix = st + 4 * N;
+    W.rng = (uint4 *)(st + 5 * N); W.prev_wi = st + 6 * N; W.prev_wo = st + 7 * N; W.hit = st + 8 * N;
+    int *q = E.queues.as<int>();
+    W.eq[0] = q; W.eq[1] = q + N;
+    for (int t = 0; t < hk::kWfTypes; ++t) W.sq[t] = q + (2 + t) * N;
+    W.fq = q + (2 + hk::kWfTypes) * N;
+    float4 *sh = E.shadow.as<float4>();
+    W.sh_o = sh; W.sh_d = sh + E.max_shadow; W.sh_c = sh + 2 * (size_t)E.max_shadow;
+    W.ctr = E.counters.as<hk::WfCounters>();
+    W.jobs = E.jobs.as<hk::WfJob>();
+    HK_CUDA(cudaMallocHost((void **)&E.host_ctr, sizeof(hk::WfCounters)));
+    HK_CUDA(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
+    HK_CUDA(cudaEventCreateWithFlags(&E.ev, cudaEventDisableTiming));
+}
+
 }  // namespace
 
 extern "C" {
@@ -895,6 +945,122 @@ int hk_render_image_static(hk_scene *s, const hk_render_desc *d, float *rgb_dev,
         HK_CUDA(hk::launch_resolve(film, rgb_dev, (int)s->width, (int)s->height, s->dev.border, st));
         if (counters_dev)
             HK_CUDA(cudaMemcpyAsync(counters_dev, hdr + 1, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st));
+        return HK_OK;
+    });
+}
+int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_wavefront_config *cfg,
+                    unsigned long long *counters_dev, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (!jobs || njobs <= 0 || njobs > hk::kWfMaxJobs) throw HkError{HK_ERR_INVALID, "need 1..1024 jobs"};
+        hk_wavefront_config c{};
+        if (cfg) c = *cfg;
+        int capacity = c.capacity > 0 ? c.capacity : (1 << 21);
+        capacity = std::max(1024, std::min(capacity, 1 << 26));
+        wf_ensure(s, capacity);
+        auto &E = *s->wf;
+        hk::WfState W = E.W;
+        W.njobs = njobs;
+        // job table
+        std::vector<hk::WfJob> J(njobs);
+        const int tiles_x = ((int)s->width + hk::kWfTileSide - 1) / hk::kWfTileSide;
+        const int tiles_y = ((int)s->height + hk::kWfTileSide - 1) / hk::kWfTileSide;
+        uint64_t total = 0;
+        for (int j = 0; j < njobs; ++j) {
+            const hk_render_job &in = jobs[j];
+            const hk_render_desc &d = in.desc;
+            if (!in.film_dev || d.spp <= 0 || d.depth < 0) throw HkError{HK_ERR_INVALID, "bad job"};
+            hk::WfJob &o = J[j];
+            std::memset(&o, 0, sizeof o);
+            o.film = in.film_dev;
+            std::memcpy(o.cam, s->dev.cam, sizeof o.cam);
+            if (d.use_camera) {
+                const float *M = d.camera_to_world;
+                if (M[15] == 0.0f) throw HkError{HK_ERR_INVALID, "camera_to_world has w = 0"};
+                for (int r = 0; r < 3; r++) {
+                    for (int cc = 0; cc < 3; cc++) o.cam[4 * r + cc] = M[4 * r + cc];
+                    o.cam[4 * r + 3] = M[4 * r + 3] / M[15];
+                }
+            }
+            o.finished = E.finished.as<unsigned long long>() + j;
+            o.seed = d.seed;
+            o.spp = (uint32_t)d.spp;
+            o.sample_offset = (uint32_t)d.sample_offset;
+            o.image_index = (uint32_t)d.image_index;
+            o.tiles_x = (uint32_t)tiles_x;
+            o.depth = d.depth;
+            o.rr_start = d.rr_start;
+            o.work_begin = total;
+            o.work_count = (uint64_t)tiles_x * tiles_y * d.spp * hk::kWfTilePixels;
+            total += o.work_count;
+        }
+        cudaStream_t user = (cudaStream_t)stream, st = E.stream;
+        // order after the caller's stream
+        HK_CUDA(cudaEventRecord(E.ev, user));
+        HK_CUDA(cudaStreamWaitEvent(st, E.ev, 0));
+        HK_CUDA(cudaMemcpyAsync(E.jobs.p, J.data(), sizeof(hk::WfJob) * njobs, cudaMemcpyHostToDevice, st));
+        HK_CUDA(cudaMemsetAsync(E.finished.p, 0, sizeof(unsigned long long) * njobs, st));
+        hk::WfCounters init{};
+        init.total_work = total;
+        HK_CUDA(cudaMemcpyAsync(E.counters.p, &init, sizeof init, cudaMemcpyHostToDevice, st));
+        // launch configuration: persistent grids, one wave of resident blocks
+        hk::WfLaunchConfig L;
+        L.threads_extend = c.threads_extend > 0 ? c.threads_extend : 128;
+        L.threads_shade = c.threads_shade > 0 ? c.threads_shade : 128;
+        L.threads_shadow = L.threads_extend;
+        L.threads_regen = 256;
+        auto grid = [&](int which, int threads, int mult) {
+            int occ = std::max(1, hk::wf_occupancy(which, threads));
+            return std::max(1, s->sm_count * occ * mult);
+        };
+        L.blocks_extend = grid(0, L.threads_extend, 1);
+        L.blocks_shade = grid(1, L.threads_shade, 1);
+        L.blocks_shadow = grid(2, L.threads_shadow, 1);
+        L.blocks_regen = grid(3, L.threads_regen, 1);
+        HK_CUDA(hk::wf_launch_init(s->dev, W, L, st));
+        // capture two iterations (extend queue 0, then 1) in a graph and replay it
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        const bool use_graph = c.no_graph == 0;
+        if (use_graph) {
+            HK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e0 = hk::wf_launch_iteration(s->dev, W, L, 0, st);
+            cudaError_t e1 = hk::wf_launch_iteration(s->dev, W, L, 1, st);
+            cudaError_t ec = cudaStreamEndCapture(st, &graph);
+            if (e0 != cudaSuccess || e1 != cudaSuccess || ec != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                throw HkError{HK_ERR_CUDA, "wavefront graph capture failed"};
+            }
+            HK_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        }
+        const int per_check = c.iterations_per_check > 0 ? c.iterations_per_check : 16;
+        uint64_t iters = 0;
+        const uint64_t max_iters = 1ull << 40;
+        for (;;) {
+            for (int k = 0; k < per_check; k += 2) {
+                if (use_graph) HK_CUDA(cudaGraphLaunch(exec, st));
+                else {
+                    HK_CUDA(hk::wf_launch_iteration(s->dev, W, L, 0, st));
+                    HK_CUDA(hk::wf_launch_iteration(s->dev, W, L, 1, st));
+                }
+            }
+            iters += per_check;
+            HK_CUDA(cudaMemcpyAsync(E.host_ctr, E.counters.p, sizeof(hk::WfCounters), cudaMemcpyDeviceToHost, st));
+            HK_CUDA(cudaStreamSynchronize(st));
+            if (E.host_ctr->active == 0 && E.host_ctr->next_work >= E.host_ctr->total_work) break;
+            if (iters > max_iters) throw HkError{HK_ERR_CUDA, "wavefront did not terminate"};
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (counters_dev) {
+            unsigned long long out[5] = {E.host_ctr->rays, E.host_ctr->shadow_rays, E.host_ctr->dropped,
+                                         E.host_ctr->node_visits, E.host_ctr->tri_tests};
+            HK_CUDA(cudaMemcpyAsync(counters_dev, out, sizeof out, cudaMemcpyHostToDevice, st));
+            HK_CUDA(cudaStreamSynchronize(st));
+        }
+        // the caller's stream continues after the engine's work
+        HK_CUDA(cudaEventRecord(E.ev, st));
+        HK_CUDA(cudaStreamWaitEvent(user, E.ev, 0));
         return HK_OK;
     });
 }

@@ -1,0 +1,410 @@
+// Wavefront pathMIS on sm_100a: the integrator of
+// src/integrator/PathMISIntegrator.cpp:16-157 split at its ray casts so that
+// every kernel runs one kind of work over a compacted queue.
+//
+//   regen   finished paths are splatted (ImageBlock::Put, src/core/Block.cpp:95)
+//           into their job's film with 128-bit vector reductions; slots claim
+//           new (job, tile, sample, pixel) work and start camera rays
+//   extend  closest hit of every queued ray; the hit's material type picks
+//           the shade queue
+//   shade<T> one kernel per top-level BSDF type (and one for misses): emitter
+//           hit with its MIS weight, next-event estimation over every emitter
+//           (shadow rays queued with their contribution), BSDF sampling,
+//           Russian roulette
+//   shadow  any-hit of every queued shadow ray; unoccluded contributions are
+//           added to their path's radiance
+//
+// The estimator is the reference's: the next-event MIS weight of an
+// unoccluded emitter is its own pl / (pl + pb) (the reference updates its
+// carried weight exactly when the shadow ray is unoccluded, and uses it right
+// away); the emitter-hit weight is computed from the previous vertex's BSDF
+// record and forced to 1 after an EDiscrete sample; Russian roulette runs
+// before the continuation ray is traced (the reference traces first and
+// discards the hit of a terminated path, which changes nothing).
+#include "hk_shading.cuh"
+#include "hk_wavefront.h"
+
+namespace hk {
+
+// ------------------------------------------------------------ helpers
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated append to a queue counter: one atomic per warp.
+__device__ __forceinline__ unsigned warp_append(unsigned *counter) {
+    unsigned mask = __activemask();
+    int leader = __ffs(mask) - 1;
+    unsigned rank = __popc(mask & ((1u << lane_id()) - 1u));
+    unsigned base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(counter, (unsigned)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + rank;
+}
+// Append grouped by key (lanes with equal keys share one atomic).
+__device__ __forceinline__ unsigned warp_append_keyed(unsigned *counters, int key) {
+    unsigned mask = __activemask();
+    unsigned peers = __match_any_sync(mask, key);
+    int leader = __ffs(peers) - 1;
+    unsigned rank = __popc(peers & ((1u << lane_id()) - 1u));
+    unsigned base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(counters + key, (unsigned)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    return base + rank;
+}
+__device__ __forceinline__ void red_add_v4(float4 *addr, float a, float b, float c, float d) {
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
+                 : "memory");
+}
+__device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
+
+__device__ __forceinline__ Ray camera_ray_cam(const DevScene &S, const float *M, float px, float py) {
+    float u = px * (1.0f / (float)S.width), v = py * (1.0f / (float)S.height);
+    V3 np = v3(S.cam_near * (1.0f - 2.0f * u) / S.cam_cot, S.cam_near * (1.0f - 2.0f * v) / (S.cam_aspect * S.cam_cot),
+               S.cam_near);
+    V3 dir = normalize(np);
+    float invz = 1.0f / dir.z;
+    Ray r;
+    r.o = v3(M[3], M[7], M[11]);
+    r.d = v3(M[0] * dir.x + M[1] * dir.y + M[2] * dir.z, M[4] * dir.x + M[5] * dir.y + M[6] * dir.z,
+             M[8] * dir.x + M[9] * dir.y + M[10] * dir.z);
+    r.tmin = S.cam_near * invz;
+    r.tmax = S.cam_far * invz;
+    return r;
+}
+
+__device__ __forceinline__ uint64_t wf_mix_seed(uint64_t seed, uint64_t s) {
+    uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (s + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ int find_job(const WfState &W, uint64_t w) {
+    int lo = 0, hi = W.njobs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (W.jobs[mid].work_begin <= w) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ImageBlock::Put into the job's global film with vector reductions.
+__device__ __forceinline__ void splat_global(const DevScene &S, float *film, float px, float py, V3 val) {
+    const int B = S.border, FW = (int)S.width + 2 * B, FH = (int)S.height + 2 * B;
+    float cx = px - 0.5f - (0 - B), cy = py - 0.5f - (0 - B);
+    int x0 = max((int)ceilf(cx - S.filt_radius), 0), y0 = max((int)ceilf(cy - S.filt_radius), 0);
+    int x1 = min((int)floorf(cx + S.filt_radius), FW - 1), y1 = min((int)floorf(cy + S.filt_radius), FH - 1);
+    float4 *F = reinterpret_cast<float4 *>(film);
+    for (int y = y0; y <= y1; ++y) {
+        float wy = __ldg(S.ftab + (int)(fabsf((float)y - cy) * S.filt_lookup));
+        for (int x = x0; x <= x1; ++x) {
+            float wx = __ldg(S.ftab + (int)(fabsf((float)x - cx) * S.filt_lookup));
+            float w = wx * wy;
+            if (w == 0.0f) continue;
+            red_add_v4(F + (size_t)y * FW + x, (val.x * wx) * wy, (val.y * wx) * wy, (val.z * wx) * wy, w);
+        }
+    }
+}
+
+// ------------------------------------------------------------ regen
+// Finish the paths of the finished queue (or, with init, every slot) and
+// start new ones from the work dispenser.
+__global__ void wf_regen_kernel(DevScene S, WfState W, int cur, int init) {
+    const int n = init ? W.capacity : (int)W.ctr->fq_count;
+    unsigned long long dropped = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = init ? i : W.fq[i];
+        if (!init) {
+            float4 p = W.pix[slot];
+            float4 L = W.lacc[slot];
+            const WfJob &J = W.jobs[__float_as_int(p.z)];
+            V3 val = v3(L.x, L.y, L.z);
+            if (is_valid(val)) splat_global(S, J.film, p.x, p.y, val);
+            else ++dropped;
+            atomicAdd(J.finished, 1ull);
+            atomicSub(&W.ctr->active, 1u);
+        }
+        // claim work until a pixel inside the image or the dispenser runs dry
+        for (;;) {
+            unsigned mask = __activemask();
+            int leader = __ffs(mask) - 1;
+            unsigned rank = __popc(mask & ((1u << lane_id()) - 1u));
+            unsigned long long base = 0;
+            if ((int)lane_id() == leader) base = atomicAdd(&W.ctr->next_work, (unsigned long long)__popc(mask));
+            base = __shfl_sync(mask, base, leader);
+            const uint64_t w = base + rank;
+            if (w >= W.ctr->total_work) break;
+            const int j = find_job(W, w);
+            const WfJob &J = W.jobs[j];
+            const uint64_t l = w - J.work_begin;
+            const uint32_t p = (uint32_t)(l % kWfTilePixels);
+            const uint64_t ts = l / kWfTilePixels;
+            const uint32_t s = (uint32_t)(ts % J.spp);
+            const uint32_t t = (uint32_t)(ts / J.spp);
+            const uint32_t x = (t % J.tiles_x) * kWfTileSide + p % kWfTileSide;
+            const uint32_t y = (t / J.tiles_x) * kWfTileSide + p / kWfTileSide;
+            if (x >= S.width || y >= S.height) {
+                atomicAdd(J.finished, 1ull);   // counted as work done: no path
+                continue;
+            }
+            Pcg32 rng;
+            rng.seed(wf_mix_seed(J.seed, (uint64_t)J.sample_offset + s),
+                     (uint64_t)y * S.width + x + (uint64_t)J.image_index * S.width * S.height);
+            float px = (float)x + rng.nextf(), py = (float)y + rng.nextf();
+            Ray r = camera_ray_cam(S, J.cam, px, py);
+            W.ray_o[slot] = f4(r.o, r.tmin);
+            W.ray_d[slot] = f4(r.d, r.tmax);
+            W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+            W.lacc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            W.pix[slot] = make_float4(px, py, __int_as_float(j), __int_as_float(0));
+            W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
+                                     (uint32_t)(rng.inc >> 32));
+            W.eq[cur][warp_append(&W.ctr->eq_count[cur])] = slot;
+            atomicAdd(&W.ctr->active, 1u);
+            break;
+        }
+    }
+    if (dropped) atomicAdd(&W.ctr->dropped, dropped);
+}
+
+// Reset the counters of the queues the next phases fill.
+__global__ void wf_reset_kernel(WfState W, int cur) {
+    if (threadIdx.x == 0) {
+        W.ctr->fq_count = 0;
+        W.ctr->eq_count[cur ^ 1] = 0;
+        W.ctr->shadow_count = 0;
+    }
+    if (threadIdx.x < kWfTypes) W.ctr->sq_count[threadIdx.x] = 0;
+}
+
+// ------------------------------------------------------------ extend
+__global__ void __launch_bounds__(128) wf_extend_kernel(DevScene S, WfState W, int cur) {
+    const int n = (int)W.ctr->eq_count[cur];
+    TravStats ts;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = W.eq[cur][i];
+        float4 o = W.ray_o[slot], d = W.ray_d[slot];
+        Ray r;
+        r.o = v3(o.x, o.y, o.z);
+        r.d = v3(d.x, d.y, d.z);
+        r.tmin = o.w;
+        r.tmax = d.w;
+        Hit h;
+        int type = 0;
+        if (trace_bvh2<false>(S, r, h, ts)) {
+            int mesh = __float_as_int(__ldg(S.tris + 3 * h.tri + 1).w);
+            type = S.bsdfs[S.meshes[mesh].bsdf].type + 1;
+        }
+        W.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
+        W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
+    }
+    unsigned long long nv = ts.nodes, nt = ts.tris;
+    for (int o = 16; o > 0; o >>= 1) {
+        nv += __shfl_down_sync(0xffffffffu, nv, o);
+        nt += __shfl_down_sync(0xffffffffu, nt, o);
+    }
+    if (lane_id() == 0 && (nv || nt)) {
+        atomicAdd(&W.ctr->node_visits, nv);
+        atomicAdd(&W.ctr->tri_tests, nt);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&W.ctr->rays, (unsigned long long)n);
+}
+
+// ------------------------------------------------------------ shade
+__device__ __forceinline__ void finish(const WfState &W, int slot) { W.fq[warp_append(&W.ctr->fq_count)] = slot; }
+
+template <int kType>
+__global__ void __launch_bounds__(128) wf_shade_kernel(DevScene S, WfState W, int nxt) {
+    const int n = (int)W.ctr->sq_count[kType];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = W.sq[kType][i];
+        const float4 o4 = W.ray_o[slot], d4 = W.ray_d[slot];
+        const V3 ro = v3(o4.x, o4.y, o4.z), rd = v3(d4.x, d4.y, d4.z);
+        float4 b4 = W.beta[slot];
+        V3 beta = v3(b4.x, b4.y, b4.z);
+        float w_mats = b4.w;
+        float4 p4 = W.pix[slot];
+        const uint32_t dflags = (uint32_t)__float_as_int(p4.w);
+        int depth = (int)(dflags & 0xffffu);
+        uint32_t flags = dflags >> 16;
+        const WfJob &J = W.jobs[__float_as_int(p4.z)];
+        float4 L4 = W.lacc[slot];
+        V3 L = v3(L4.x, L4.y, L4.z);
+        if constexpr (kType == 0) {
+            // miss (PathMISIntegrator.cpp:35-66)
+            if (S.env_index >= 0 && (depth > 0 || !S.force_background)) L = L + beta * env_eval(S, rd);
+            else if (depth == 0) L = ld3(S.background);
+            W.lacc[slot] = f4(L, 0.0f);
+            finish(W, slot);
+            continue;
+        } else {
+            constexpr int BT = kType - 1;
+            uint4 rs = W.rng[slot];
+            Pcg32 rng;
+            rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
+            rng.inc = (uint64_t)rs.z | ((uint64_t)rs.w << 32);
+            float4 h4 = W.hit[slot];
+            Hit h;
+            h.t = h4.x; h.u = h4.y; h.v = h4.z; h.tri = __float_as_int(h4.w);
+            Isect it;
+            post_intersect(S, h, it);
+            const DevMesh &m = S.meshes[it.mesh];
+            const int bsdf = m.bsdf;
+            if (m.emitter >= 0) {
+                const DevAreaLight &AL = S.area_lights[__ldg(S.emitter_area + m.emitter)];
+                ERec er;
+                er.ref = ro; er.p = it.p; er.n = it.sh.n;
+                V3 wi = er.p - er.ref; er.dist = norm(wi); er.wi = wi / er.dist;
+                if (depth > 0) {
+                    // MIS weight of the BSDF-sampled hit (PathMISIntegrator.cpp:122-140)
+                    if (flags & kWfFlagForceMats) {
+                        w_mats = 1.0f;
+                    } else {
+                        float4 pwi = W.prev_wi[slot], pwo = W.prev_wo[slot];
+                        BRec pb;
+                        pb.wi = v3(pwi.x, pwi.y, pwi.z);
+                        pb.wo = v3(pwo.x, pwo.y, pwo.z);
+                        pb.measure = __float_as_int(pwo.w);
+                        pb.eta = 0.0f;
+                        float plm = area_pdf(AL, er);
+                        float pbm = bsdf_pdf(S.bsdfs, __float_as_int(pwi.w), pb);
+                        if (pbm + plm != 0.0f) w_mats = pbm / (pbm + plm);
+                    }
+                }
+                L = L + (beta * w_mats) * area_eval(AL, er);
+            }
+            // next-event estimation over every emitter (PathMISIntegrator.cpp:83-109)
+            const V3 wi_local = to_local(it.sh, rd * -1.0f);
+            for (int e = 0; e < S.nemitters; ++e) {
+                ERec er;
+                er.ref = it.p;
+                er.dist = 0.0f;
+                er.pdf = 0.0f;
+                float u1 = rng.nextf();
+                float ux = rng.nextf(), uy = rng.nextf();
+                int ai = __ldg(S.emitter_area + e);
+                V3 ld;
+                if (ai < 0) { er.dist = S.scene_radius; ld = env_sample(S, er, ux, uy); }
+                else ld = area_sample(S, S.area_lights[ai], er, ux, uy, u1);
+                if (is_zero(ld)) continue;
+                BRec br;
+                br.wi = wi_local;
+                br.wo = to_local(it.sh, er.wi);
+                br.measure = kMeasureSolidAngle;
+                br.eta = 0.0f;
+                float pl = er.pdf;
+                float pb = bsdf_pdf_t<BT>(S.bsdfs, bsdf, br);
+                float w = (pl + pb != 0.0f) ? pl / (pl + pb) : 1.0f;
+                V3 f = bsdf_eval_t<BT>(S.bsdfs, bsdf, br);
+                float c = fabsf(br.wo.z);
+                V3 contrib = v3((((beta.x * f.x) * c) * ld.x) * w, (((beta.y * f.y) * c) * ld.y) * w,
+                                (((beta.z * f.z) * c) * ld.z) * w);
+                if (all_zero(contrib)) continue;   // adds nothing whether occluded or not
+                unsigned q = warp_append(&W.ctr->shadow_count);
+                if (q < (unsigned)W.max_shadow) {
+                    W.sh_o[q] = f4(it.p, __int_as_float(slot));
+                    W.sh_d[q] = f4(er.p - it.p, 0.0f);
+                    W.sh_c[q] = f4(contrib, 0.0f);
+                }
+            }
+            // BSDF sampling (PathMISIntegrator.cpp:111-120)
+            BRec br;
+            br.wi = wi_local;
+            br.wo = v3(0, 0, 0);
+            br.measure = kMeasureUnknown;
+            br.eta = 0.0f;
+            float sx = rng.nextf(), sy = rng.nextf();
+            float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
+            V3 F = bsdf_sample_t<BT>(S.bsdfs, bsdf, br, sx, sy, u1);
+            beta = beta * F;
+            bool alive = !is_zero(beta);
+            if (alive) {
+                flags = (br.measure == kMeasureDiscrete) ? kWfFlagForceMats : 0u;
+                if (flags) w_mats = 1.0f;
+                // Russian roulette (PathMISIntegrator.cpp:142-151)
+                if (depth >= J.rr_start) {
+                    if (rng.nextf() < 0.95f) beta = beta * (1.0f / 0.95f);
+                    else alive = false;
+                }
+                ++depth;
+                if (depth >= J.depth) alive = false;   // the next hit would not be shaded
+            }
+            W.lacc[slot] = f4(L, 0.0f);
+            if (!alive) {
+                finish(W, slot);
+                continue;
+            }
+            W.ray_o[slot] = f4(it.p, kRayEps);
+            W.ray_d[slot] = f4(to_world(it.sh, br.wo), __int_as_float(0x7f800000));
+            W.beta[slot] = f4(beta, w_mats);
+            W.pix[slot] = make_float4(p4.x, p4.y, p4.z, __int_as_float((int)((flags << 16) | (uint32_t)depth)));
+            W.prev_wi[slot] = f4(br.wi, __int_as_float(bsdf));
+            W.prev_wo[slot] = f4(br.wo, __int_as_float(br.measure));
+            W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
+                                     (uint32_t)(rng.inc >> 32));
+            W.eq[nxt][warp_append(&W.ctr->eq_count[nxt])] = slot;
+        }
+    }
+}
+
+// ------------------------------------------------------------ shadow
+__global__ void __launch_bounds__(128) wf_shadow_kernel(DevScene S, WfState W) {
+    const int n = min((int)W.ctr->shadow_count, W.max_shadow);
+    TravStats ts;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 o = W.sh_o[i], d = W.sh_d[i];
+        Ray r;
+        r.o = v3(o.x, o.y, o.z);
+        r.d = v3(d.x, d.y, d.z);
+        r.tmin = kRayEps;
+        r.tmax = 1.0f - kRayEps;
+        Hit h;
+        if (!trace_bvh2<true>(S, r, h, ts)) {
+            float4 c = W.sh_c[i];
+            red_add_v4(W.lacc + __float_as_int(o.w), c.x, c.y, c.z, 0.0f);
+        }
+    }
+    unsigned long long nv = ts.nodes, nt = ts.tris;
+    for (int o = 16; o > 0; o >>= 1) {
+        nv += __shfl_down_sync(0xffffffffu, nv, o);
+        nt += __shfl_down_sync(0xffffffffu, nt, o);
+    }
+    if (lane_id() == 0 && (nv || nt)) {
+        atomicAdd(&W.ctr->node_visits, nv);
+        atomicAdd(&W.ctr->tri_tests, nt);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&W.ctr->shadow_rays, (unsigned long long)n);
+}
+
+// ------------------------------------------------------------ launchers
+cudaError_t wf_launch_init(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
+    wf_regen_kernel<<<(W.capacity + C.threads_regen - 1) / C.threads_regen, C.threads_regen, 0, st>>>(S, W, 0, 1);
+    return cudaGetLastError();
+}
+
+cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
+    const int nxt = cur ^ 1;
+    wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur, 0);
+    wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
+    wf_extend_kernel<<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur);
+    wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+    wf_shade_kernel<1><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+    wf_shade_kernel<2><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+    wf_shade_kernel<3><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+    wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+    wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+    wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W);
+    return cudaGetLastError();
+}
+
+int wf_occupancy(int which, int threads) {
+    int n = 0;
+    switch (which) {
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel, threads, 0); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade_kernel<5>, threads, 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel, threads, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_regen_kernel, threads, 0); break;
+    }
+    return n;
+}
+
+}  // namespace hk

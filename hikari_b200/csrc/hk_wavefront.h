@@ -1,0 +1,89 @@
+// Wavefront pathMIS: device-side structures shared by hk_wavefront.cu and the
+// host driver in hk_host.cpp.
+//
+// A pool of `capacity` path slots lives in HBM as structure-of-arrays.  One
+// iteration runs: regen (splat finished paths, claim new work, generate camera
+// rays) -> extend (closest hit of every queued ray, classify by material) ->
+// shade<material> (emission, MIS, next-event shadow rays, BSDF sampling,
+// Russian roulette) -> shadow (any-hit, add unoccluded next-event terms).
+// Kernels use fixed persistent grids and read queue sizes from HBM, so an
+// iteration can be captured once in a CUDA graph and replayed.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hk_device.h"
+
+namespace hk {
+
+constexpr int kWfTypes = 6;        // 0: miss, 1..5: BSDF type + 1 of the hit
+constexpr int kWfMaxJobs = 1024;
+constexpr int kWfTileSide = 16;
+constexpr int kWfTilePixels = kWfTileSide * kWfTileSide;
+
+// One image being rendered (a job): a view of the scene with its own film.
+struct WfJob {
+    float *film;                    // (H+2B) x (W+2B) x 4, 16-byte aligned
+    float cam[12];                  // camera-to-world rows (translation divided by w)
+    unsigned long long *finished;   // paths of this job finished (device counter)
+    uint64_t seed;
+    uint64_t work_begin, work_count;   // global work range: tiles * spp * 256
+    uint32_t spp, sample_offset, image_index, tiles_x;
+    int32_t depth, rr_start;
+};
+
+// Device-wide counters of the engine (one struct in HBM).
+struct WfCounters {
+    unsigned long long next_work;      // global work dispenser
+    unsigned long long total_work;     // end of the dispensed range
+    unsigned int eq_count[2];          // extend queues (ping-pong)
+    unsigned int sq_count[kWfTypes];   // shade queues per material type
+    unsigned int fq_count;             // finished paths awaiting splat + regeneration
+    unsigned int shadow_count;         // next-event shadow rays
+    unsigned int active;               // paths in flight
+    unsigned int pad;
+    unsigned long long rays, shadow_rays, dropped, node_visits, tri_tests, paths;
+};
+
+struct WfState {
+    int capacity;
+    int max_shadow;                    // shadow queue capacity
+    // per-slot path state
+    float4 *ray_o;      // o.xyz, tmin
+    float4 *ray_d;      // d.xyz, tmax
+    float4 *beta;       // throughput.xyz, w_mats
+    float4 *lacc;       // radiance.xyz (next-event terms added atomically), -
+    float4 *pix;        // film x, film y, bits(job), bits(depth | flags << 16)
+    uint4 *rng;         // pcg32 state, increment
+    float4 *prev_wi;    // previous vertex: BSDF record wi.xyz, bits(bsdf id)
+    float4 *prev_wo;    // previous vertex: BSDF record wo.xyz, bits(measure)
+    float4 *hit;        // t, u, v, bits(tri in leaf order or -1)
+    // queues
+    int *eq[2];
+    int *sq[kWfTypes];
+    int *fq;
+    float4 *sh_o;       // shadow origin.xyz, bits(slot)
+    float4 *sh_d;       // shadow direction.xyz (unnormalised), -
+    float4 *sh_c;       // contribution.xyz, -
+    WfCounters *ctr;
+    const WfJob *jobs;
+    int njobs;
+};
+
+// flags in the high half of pix.w
+constexpr uint32_t kWfFlagForceMats = 1u;   // previous BSDF sample was EDiscrete
+
+struct WfLaunchConfig {
+    int blocks_extend, threads_extend;
+    int blocks_shade, threads_shade;
+    int blocks_shadow, threads_shadow;
+    int blocks_regen, threads_regen;
+};
+
+cudaError_t wf_launch_init(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st);
+// one iteration with extend queue `cur` (0/1)
+cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st);
+int wf_occupancy(int which, int threads);
+
+}  // namespace hk

@@ -139,6 +139,31 @@ int hk_film_resolve(hk_scene *s, const float *film_dev, float *rgb_dev, void *st
 int hk_render_image(hk_scene *s, const hk_render_desc *desc, float *rgb_host, unsigned long long *counters,
                     void *stream);
 
+/* ---- wavefront rendering (the batched form) ---- */
+/* One image of a batch: accumulate desc.spp samples into film_dev (film layout
+ * of hk_render).  desc.use_camera selects a per-image camera pose. */
+typedef struct {
+    float *film_dev;
+    hk_render_desc desc;
+} hk_render_job;
+
+typedef struct {
+    int32_t capacity;              /* path slots in flight (0 = 2^21) */
+    int32_t threads_extend;        /* block size of the extend/shadow kernels (0 = 128) */
+    int32_t threads_shade;         /* block size of the shade kernels (0 = 128) */
+    int32_t iterations_per_check;  /* iterations between host termination checks (0 = 16) */
+    int32_t no_graph;              /* 1: launch kernels directly instead of replaying a CUDA graph */
+} hk_wavefront_config;
+
+/* Render every job of the batch with the wavefront integrator: a pool of path
+ * slots shared by all images, compacted ray queues, one shading kernel per
+ * material type, and iterations replayed from a CUDA graph.  Same estimator
+ * as hk_render (PathMISIntegrator::Li, src/integrator/PathMISIntegrator.cpp:16).
+ * Returns when every job is done; counters_dev (optional, 5 x u64): rays,
+ * shadow rays, dropped samples, node visits, triangle tests. */
+int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_wavefront_config *cfg,
+                    unsigned long long *counters_dev, void *stream);
+
 /* Render into a caller-provided device image without allocating any device
  * memory.  This entry point has no counterpart in the reference.  It is for
  * callers that cannot call cudaMalloc while rendering -- a host application

@@ -1,0 +1,100 @@
+"""The wavefront integrator against the megakernel and the reference's known
+answers.  Both run the reference estimator; their sample streams differ, so
+images are compared statistically."""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import hikari_b200 as hk  # noqa: E402
+from hikari_b200 import scenes  # noqa: E402
+from hikari_b200.scenedesc import FilterDesc, parse_xml  # noqa: E402
+from oracle.oracle import OracleScene, students_t_test  # noqa: E402
+
+DEV = "cuda:0"
+
+
+def _resolve(gs, film):
+    cam = gs.desc.camera
+    rgb = torch.empty((cam.height, cam.width, 3), dtype=torch.float32, device=DEV)
+    gs.resolve(film, rgb)
+    return rgb.cpu().numpy()
+
+
+@pytest.mark.parametrize("fname", ["test-direct.xml", "test-furnace.xml"])
+def test_wavefront_golden_ttest(golden_dir, fname):
+    all_scenes = parse_xml(os.path.join(golden_dir, "pa5", fname))
+    for sd in [s for s in all_scenes if s.integrator == "pathMIS"]:
+        gs = hk.Scene.from_desc(sd)
+        k = 64
+        films = [torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV) for _ in range(k)]
+        gs.render_batch(films, spp=2000, depth=sd.depth, seeds=list(range(100, 100 + k)), capacity=1 << 16)
+        means = []
+        for f in films:
+            c = _resolve(gs, f).reshape(-1, 3).mean(0)
+            means.append(c[0] * 0.212671 + c[1] * 0.715160 + c[2] * 0.072169)
+        m = np.array(means)
+        ok, p = students_t_test(m.mean(), m.var(ddof=1), sd.reference, len(m), 0.01, len(all_scenes))
+        assert ok, f"{fname}: wavefront mean {m.mean()} vs reference {sd.reference} (p={p})"
+
+
+def test_wavefront_cornell_matches_oracle():
+    sd = scenes.cornell_box(width=48, height=48)
+    sd.filter = FilterDesc(0, 0.5)
+    gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    film = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
+    ctr = torch.zeros(5, dtype=torch.int64, device=DEV)
+    gs.render_batch([film], spp=4096, depth=sd.depth, seeds=[7], counters=ctr, capacity=1 << 18)
+    g = _resolve(gs, film).reshape(-1, 3).astype(np.float64)
+    pix = np.stack(np.meshgrid(np.arange(48), np.arange(48), indexing="xy"), -1).reshape(-1, 2)
+    mean_o, var_o = os_.pixel_stats(pix, 512, seed=3)
+    z = (g - mean_o) / (np.sqrt(var_o / 4096 + var_o / 512) + 1e-6)
+    frac3 = np.mean(np.abs(z) > 3)
+    c = ctr.cpu().numpy()
+    print("z mean", z.mean(), "frac |z|>3", frac3, "max", np.abs(z).max(), "counters", c)
+    assert abs(g.mean() / mean_o.mean() - 1) < 0.01
+    assert frac3 < 0.02
+    assert c[0] >= 48 * 48 * 4096
+
+
+def test_wavefront_matches_megakernel_heterogeneous():
+    """Same scene, same views: the two integrators agree on the image mean per
+    view and per channel within their statistical error."""
+    sd = scenes.heterogeneous(width=96, height=96, spp=64)
+    cams = scenes.heterogeneous_cameras(2)
+    gs = hk.Scene.from_desc(sd)
+    mk, wf = [], []
+    for v, cam in enumerate(cams):
+        means_m, means_w = [], []
+        for rep in range(6):
+            f = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
+            gs.render(f, spp=64, depth=sd.depth, seed=10 * rep + v, camera=cam)
+            means_m.append(_resolve(gs, f).mean((0, 1)))
+            f2 = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
+            gs.render_batch([f2], spp=64, depth=sd.depth, seeds=[1000 + 10 * rep + v], cameras=[cam],
+                            capacity=1 << 18)
+            means_w.append(_resolve(gs, f2).mean((0, 1)))
+        mm, mw = np.array(means_m), np.array(means_w)
+        se = np.sqrt(mm.var(0, ddof=1) / len(mm) + mw.var(0, ddof=1) / len(mw)) + 1e-6
+        z = (mm.mean(0) - mw.mean(0)) / se
+        print("view", v, "megakernel", mm.mean(0), "wavefront", mw.mean(0), "z", z)
+        assert np.all(np.abs(z) < 4.5), (v, z)
+
+
+def test_wavefront_batch_of_images_equals_separate_images():
+    """Every image of a batch is the image rendered alone (same seeds): the
+    sample streams depend on (seed, sample, pixel) only."""
+    sd = scenes.cornell_box(width=40, height=32)
+    gs = hk.Scene.from_desc(sd)
+    cams = [scenes.look_at((0.3 * i, 1, 3.8), (0, 1, 0), (0, 1, 0)) for i in range(3)]
+    batch = [torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV) for _ in cams]
+    gs.render_batch(batch, spp=32, depth=sd.depth, seeds=[5, 6, 7], cameras=cams, capacity=1 << 14)
+    for i, cam in enumerate(cams):
+        alone = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
+        gs.render_batch([alone], spp=32, depth=sd.depth, seeds=[5 + i], cameras=[cam], image_indices=[i],
+                        capacity=1 << 12)
+        a, b = _resolve(gs, batch[i]), _resolve(gs, alone)
+        assert np.allclose(a, b, rtol=1e-5, atol=1e-6), np.abs(a - b).max()
