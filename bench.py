@@ -1,6 +1,7 @@
 """Benchmark of the pathMIS core on one B200 node.
 
-A step renders the heterogeneous scene (64 displaced icospheres with six
+A step renders, with the wavefront integrator (--form megakernel: the plain
+one-thread-per-path kernel), the heterogeneous scene (64 displaced icospheres with six
 material types, 4 area lights and a procedural 2048x1024 sky) from 8 views at
 1024x1024 and 128 spp with the reference integrator rule (pathMIS, depth 16,
 Russian roulette from depth 0).  Scene and BVH are resident in HBM before the
@@ -36,7 +37,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="heterogeneous", choices=["heterogeneous", "mesh_heavy", "cornell"])
@@ -46,6 +47,9 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-megakernel comparison sample")
+    ap.add_argument("--form", default="wavefront", choices=["wavefront", "megakernel"],
+                    help="wavefront (the batched form) or the plain one-thread-per-path megakernel")
     return ap.parse_args()
 
 
@@ -233,41 +237,44 @@ def main():
     V = len(cams)
     shape = gs.film_shape()
     films = [torch.zeros(shape, dtype=torch.float32, device="cuda") for _ in range(V)]
-    counters = torch.zeros(5, dtype=torch.int64, device="cuda")
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")   # 256 MiB > 126 MB L2
     stream = torch.cuda.current_stream()
+    wave = args.form == "wavefront"
+    n_ctr = 7 if wave else 5
+    counters = torch.zeros(n_ctr, dtype=torch.int64, device="cuda")
+    cam_list = [c for c in cams] if cams[0] is not None else None
+    tuned, tune_ms = {}, None
+    if wave:
+        tuned, tune_ms = gs.autotune(min(16, spp), depth, camera=cams[0])   # untimed set-up
 
-    def step(it, ctr=None):
-        for v, cam in enumerate(cams):
-            films[v].zero_()
-            gs.render(films[v], spp=spp, depth=depth, seed=1000 * it + v, image_index=rank * V + v,
-                      counters=ctr, camera=cam)
+    def step(it, ctr=None, **extra):
+        for f in films:
+            f.zero_()
+        if wave:
+            gs.render_batch(films, spp=spp, depth=depth, seeds=[77 + 1000 * it + v for v in range(V)], cameras=cam_list,
+                            image_indices=[rank * V + v for v in range(V)], counters=ctr, **tuned, **extra)
+        else:
+            for v, cam in enumerate(cams):
+                gs.render(films[v], spp=spp, depth=depth, seed=77 + 1000 * it + v, image_index=rank * V + v,
+                          counters=ctr, camera=cam)
 
     for w in range(args.warmup):
-        step(w)
+        step(10_000 + w)
     torch.cuda.synchronize()
     barrier()
     counters.zero_()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    kern = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in cams]
-            for _ in range(args.steps)]
     with ClockSampler(local) as clk:
         barrier()
         torch.cuda.synchronize()
         for k in range(args.steps):
             flush.fill_(float(k))   # write 256 MiB: evict L2 between steps (outside the step events)
             evs[k][0].record(stream)
-            for v, cam in enumerate(cams):
-                films[v].zero_()
-                kern[k][v][0].record(stream)
-                gs.render(films[v], spp=spp, depth=depth, seed=77 + 1000 * k + v, image_index=rank * V + v,
-                          counters=counters, camera=cam)
-                kern[k][v][1].record(stream)
+            step(k, counters)
             evs[k][1].record(stream)
         torch.cuda.synchronize()
         barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    kern_ms = [a.elapsed_time(b) for row in kern for a, b in row]
     total_s = sum(step_ms) / 1e3
     t = torch.tensor([total_s], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -278,30 +285,75 @@ def main():
     value = world * paths_rank / total_max / 1e6
     rays = ctr[0] + ctr[1]
     mrays = world * rays / total_max / 1e6
-
-    # roofline of the render kernel: BVH fetch bytes (64 B node, 48 B triangle)
     hbm, peak_kind = measured_peaks()
-    n_launch = args.steps * V
-    bytes_per_launch = (ctr[3] * 64.0 + ctr[4] * 48.0) / n_launch
-    avg_kernel_s = float(np.mean(kern_ms)) / 1e3
-    achieved = bytes_per_launch / avg_kernel_s / 1e9
 
-    # end to end through the C ABI: host image out, per-view camera pose in
-    e2e_steps = 0 if args.no_e2e else 1
-    out = np.empty((H, W, 3), np.float32)
-    torch.cuda.synchronize()
-    barrier()
-    t0 = time.perf_counter()
-    for k in range(e2e_steps):
-        for v, cam in enumerate(cams):
-            gs.render_image(spp, depth, seed=5000 + 1000 * k + v, out=out, camera=cam, image_index=rank * V + v)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * W * H * spp * V * e2e_steps / float(te.item()) / 1e6 if e2e_steps else None
-    desc_bytes = int(hk.C.sizeof(hk.RenderDesc)) if hasattr(hk, "C") else 104
+    # roofline of the dominant kernel, timed live with CUDA events on the launching stream
+    if wave:
+        kms = np.zeros(4, np.float32)
+        kl = np.zeros(4, np.int32)
+        pc = torch.zeros(7, dtype=torch.int64, device="cuda")
+        step(99_999, pc, kernel_ms=kms, kernel_launches=kl)
+        torch.cuda.synchronize()
+        pcn = pc.cpu().numpy().astype(np.float64)
+        phases = ["regen", "extend", "shade", "shadow"]
+        dom = int(np.argmax(kms))
+        trav_bytes = {1: pcn[3] * 64.0 + pcn[4] * 48.0, 3: pcn[5] * 64.0 + pcn[6] * 48.0}
+        if dom in trav_bytes:
+            bytes_per_launch = trav_bytes[dom] / max(1, kl[dom])
+            avg_s = float(kms[dom]) / max(1, kl[dom]) / 1e3
+            basis = (f"{phases[dom]} kernel: BVH fetch bytes (64 B per node visit + 48 B per triangle test, counted "
+                     f"in the kernel) per launch / mean launch time over {int(kl[dom])} launches of a profiled step")
+        else:
+            # shading: path-state bytes read + written per path vertex (~144 B) as the algorithmic unit
+            bytes_per_launch = (pcn[0] * 144.0) / max(1, kl[dom])
+            avg_s = float(kms[dom]) / max(1, kl[dom]) / 1e3
+            basis = f"{phases[dom]} kernels: path-state bytes (144 B per shaded vertex) per launch"
+        achieved = bytes_per_launch / max(avg_s, 1e-12) / 1e9
+        launches_per_step = int(kl.sum()) + 1
+        phase_share = {p: round(float(kms[i] / kms.sum()), 4) for i, p in enumerate(phases)}
+    else:
+        n_launch = args.steps * V
+        bytes_per_launch = (ctr[3] * 64.0 + ctr[4] * 48.0) / n_launch
+        achieved = bytes_per_launch / (total_max / n_launch) / 1e9
+        basis = "render megakernel: BVH fetch bytes (64 B per node visit + 48 B per triangle test) / mean kernel time"
+        launches_per_step = V
+        phase_share = None
+
+    # end to end through the C ABI: host images out, per-view camera pose in
+    e2e_value = None
+    if not args.no_e2e:
+        outs = [np.empty((H, W, 3), np.float32) for _ in range(V)]
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        if wave:
+            gs.render_batch_host(outs, spp, depth, seeds=[5000 + v for v in range(V)], cameras=cam_list,
+                                 image_indices=[rank * V + v for v in range(V)], **tuned)
+        else:
+            for v, cam in enumerate(cams):
+                gs.render_image(spp, depth, seed=5000 + v, out=outs[v], camera=cam, image_index=rank * V + v)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_value = world * W * H * spp * V / float(te.item()) / 1e6
+
+    # the plain megakernel on a short sample of the same scene, for comparison
+    plain = None
+    if wave and not args.no_plain and rank == 0:
+        ps = max(1, min(16, spp))
+        f = films[0]
+        f.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        gs.render(f, spp=ps, depth=depth, seed=3, camera=cams[0])
+        torch.cuda.synchronize()
+        e0.record(stream)
+        gs.render(f, spp=ps, depth=depth, seed=4, camera=cams[0])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain = {"mpaths_per_s": W * H * ps / (e0.elapsed_time(e1) / 1e3) / 1e6,
+                 "sample": f"view 0, {W}x{H} x {ps} spp, render_pathmis_kernel"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -328,20 +380,22 @@ def main():
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded procedural scene)",
-        "config": {"workload": desc, "parallelism": f"replicas x{world}", "triangles": int(gs.info.n_triangles),
-                   "bvh_nodes": int(gs.info.n_bvh_nodes), "scene_build_s": round(build_s, 2),
+        "config": {"workload": desc, "form": args.form, "parallelism": f"replicas x{world}",
+                   "triangles": int(gs.info.n_triangles), "bvh_nodes": int(gs.info.n_bvh_nodes),
+                   "scene_build_s": round(build_s, 2), "wavefront": tuned or None,
+                   "autotune_probe_ms": tune_ms,
                    "l2": "256 MiB buffer written between timed steps (outside the step events)",
                    "rr": "reference rule: p=0.95 at every bounce"},
         "mrays_per_s": mrays,
-        "rays_per_path": rays / (paths_rank),
+        "rays_per_path": rays / paths_rank,
+        "phase_share": phase_share,
+        "plain_megakernel": plain,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "peak_kind": peak_kind,
-                     "basis": "BVH fetch bytes per launch (64 B per node visit + 48 B per triangle test) / "
-                              "mean render-kernel time"},
+                     "traffic": None, "peak_kind": peak_kind, "basis": basis},
         "cpu_baseline": cpu,
-        "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": V * desc_bytes,
+        "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": V * int(hk.C.sizeof(hk.RenderDesc)),
                 "d2h_bytes_per_step": V * W * H * 3 * 4},
-        "gpu_launches": n_launch,
+        "gpu_launches": launches_per_step * args.steps,
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)

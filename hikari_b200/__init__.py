@@ -58,7 +58,8 @@ class RenderJob(C.Structure):
 
 class WavefrontConfig(C.Structure):
     _fields_ = [("capacity", C.c_int32), ("threads_extend", C.c_int32), ("threads_shade", C.c_int32),
-                ("iterations_per_check", C.c_int32), ("no_graph", C.c_int32)]
+                ("iterations_per_check", C.c_int32), ("no_graph", C.c_int32), ("kernel_ms", C.c_void_p),
+                ("kernel_launches", C.c_void_p)]
 
 
 def render_desc(spp, depth, seed=0, sample_offset=0, rr_start=0, image_index=0, spp_per_item=0,
@@ -105,6 +106,10 @@ def lib():
         "hk_render_image": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
         "hk_render_image_static": ([P, C.POINTER(RenderDesc), P, P, P], C.c_int),
         "hk_render_batch": ([P, C.POINTER(RenderJob), C.c_int, C.POINTER(WavefrontConfig), P, P], C.c_int),
+        "hk_render_batch_host": ([P, C.POINTER(RenderDesc), C.c_int, C.POINTER(WavefrontConfig),
+                                  C.POINTER(C.c_void_p), P, P], C.c_int),
+        "hk_wavefront_autotune": ([P, C.POINTER(RenderDesc), C.POINTER(WavefrontConfig), C.POINTER(C.c_float)],
+                                  C.c_int),
         "hk_trace": ([P, U64, P, P, P, P, P, C.c_int, P, P], C.c_int),
         "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
         "hk_emitter_sample": ([P, I32, U64, P, P, P], C.c_int),
@@ -296,9 +301,12 @@ class Scene:
     def render_batch(self, films, spp: int, depth: int, seeds=None, cameras=None, image_indices=None,
                      sample_offset: int = 0, rr_start: int = 0, counters=None, capacity: int = 0,
                      threads_extend: int = 0, threads_shade: int = 0, iterations_per_check: int = 0,
-                     no_graph: bool = False, stream=None) -> None:
+                     no_graph: bool = False, kernel_ms=None, kernel_launches=None, stream=None) -> None:
         """Wavefront render of several images at once: films[i] (device
-        tensors of film_shape()) accumulate spp samples of view cameras[i]."""
+        tensors of film_shape()) accumulate spp samples of view cameras[i].
+        counters: device int64 tensor of 7 (see hk_render_batch).  kernel_ms /
+        kernel_launches: host float32[4] / int32[4] arrays that receive the
+        per-phase device time and launch counts (profiling; no graph)."""
         n = len(films)
         jobs = (RenderJob * n)()
         for i, f in enumerate(films):
@@ -307,8 +315,36 @@ class Scene:
             idx = image_indices[i] if image_indices is not None else i
             jobs[i].film_dev = _p(f)
             jobs[i].desc = render_desc(spp, depth, seed, sample_offset, rr_start, idx, 0, cam)
-        cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, int(no_graph))
+        cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, int(no_graph),
+                              _p(kernel_ms), _p(kernel_launches))
         check(lib().hk_render_batch(self.h, jobs, n, C.byref(cfg), _p(counters), _stream(stream)))
+
+    def render_batch_host(self, outs, spp: int, depth: int, seeds=None, cameras=None, image_indices=None,
+                          rr_start: int = 0, capacity: int = 0, threads_extend: int = 0, threads_shade: int = 0,
+                          iterations_per_check: int = 0, stream=None):
+        """End-to-end wavefront batch into host images outs[i] (H x W x 3 float32)."""
+        n = len(outs)
+        descs = (RenderDesc * n)()
+        for i in range(n):
+            cam = cameras[i] if cameras is not None else None
+            seed = seeds[i] if seeds is not None else i
+            idx = image_indices[i] if image_indices is not None else i
+            descs[i] = render_desc(spp, depth, seed, 0, rr_start, idx, 0, cam)
+        ptrs = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        ctr = np.zeros(7, np.uint64)
+        cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, 0, None, None)
+        check(lib().hk_render_batch_host(self.h, descs, n, C.byref(cfg), ptrs, ctr.ctypes.data, _stream(stream)))
+        return ctr
+
+    def autotune(self, spp: int, depth: int, camera=None):
+        """Pick the wavefront configuration (slot capacity, block sizes, check
+        interval) that renders one probe image fastest; returns (config dict, ms)."""
+        d = render_desc(spp, depth, 1, 0, 0, 0, 0, camera)
+        cfg = WavefrontConfig()
+        ms = C.c_float()
+        check(lib().hk_wavefront_autotune(self.h, C.byref(d), C.byref(cfg), C.byref(ms)))
+        return dict(capacity=cfg.capacity, threads_extend=cfg.threads_extend, threads_shade=cfg.threads_shade,
+                    iterations_per_check=cfg.iterations_per_check), ms.value
 
     def render_image_static(self, out, spp: int, depth: int, seed: int = 0, rr_start: int = 0, counters=None,
                             camera=None, image_index: int = 0, stream=None) -> None:

@@ -267,6 +267,7 @@ struct hk_scene {
     DevBuf b_tris, b_nodes, b_tri_normals, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
         b_light_cdf, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
     DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
+    std::vector<std::unique_ptr<DevBuf>> batch_films;   // films of hk_render_batch_host
     hk_scene_info info{};
     int margin_lo = 0, margin_hi = 0;
     int sm_count = 148;
@@ -593,7 +594,7 @@ void build_scene(hk_scene *s) {
     s->margin_hi = (int)std::floor(D.border + 0.5f + s->filt_r);
 
     // scratch: [0] work counter (u32 in a u64 slot), [1..3] counters
-    s->b_scratch.alloc(8 * sizeof(unsigned long long));
+    s->b_scratch.alloc(16 * sizeof(unsigned long long));
     HK_CUDA(cudaMemset(s->b_scratch.p, 0, s->b_scratch.bytes));
     track(s->b_scratch);
 
@@ -1007,6 +1008,8 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         hk::WfLaunchConfig L;
         L.threads_extend = c.threads_extend > 0 ? c.threads_extend : 128;
         L.threads_shade = c.threads_shade > 0 ? c.threads_shade : 128;
+        for (int t : {L.threads_extend, L.threads_shade})
+            if (t % 32 != 0 || t > 256) throw HkError{HK_ERR_INVALID, "wavefront block sizes must be multiples of 32 up to 256"};
         L.threads_shadow = L.threads_extend;
         L.threads_regen = 256;
         auto grid = [&](int which, int threads, int mult) {
@@ -1021,7 +1024,30 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         // capture two iterations (extend queue 0, then 1) in a graph and replay it
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
-        const bool use_graph = c.no_graph == 0;
+        const bool profile = c.kernel_ms != nullptr;
+        const bool use_graph = c.no_graph == 0 && !profile;
+        cudaEvent_t pe[2] = {nullptr, nullptr};
+        if (profile) {
+            HK_CUDA(cudaEventCreate(&pe[0]));
+            HK_CUDA(cudaEventCreate(&pe[1]));
+        }
+        const int phase_launches[4] = {2, 1, hk::kWfTypes, 1};
+        auto run_iteration = [&](int cur) {
+            if (!profile) {
+                HK_CUDA(hk::wf_launch_iteration(s->dev, W, L, cur, st));
+                return;
+            }
+            for (int ph = 0; ph < 4; ++ph) {
+                HK_CUDA(cudaEventRecord(pe[0], st));
+                HK_CUDA(hk::wf_launch_phase(s->dev, W, L, cur, ph, st));
+                HK_CUDA(cudaEventRecord(pe[1], st));
+                HK_CUDA(cudaEventSynchronize(pe[1]));
+                float ms = 0;
+                HK_CUDA(cudaEventElapsedTime(&ms, pe[0], pe[1]));
+                c.kernel_ms[ph] += ms;
+                if (c.kernel_launches) c.kernel_launches[ph] += phase_launches[ph];
+            }
+        };
         if (use_graph) {
             HK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             cudaError_t e0 = hk::wf_launch_iteration(s->dev, W, L, 0, st);
@@ -1040,8 +1066,8 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
             for (int k = 0; k < per_check; k += 2) {
                 if (use_graph) HK_CUDA(cudaGraphLaunch(exec, st));
                 else {
-                    HK_CUDA(hk::wf_launch_iteration(s->dev, W, L, 0, st));
-                    HK_CUDA(hk::wf_launch_iteration(s->dev, W, L, 1, st));
+                    run_iteration(0);
+                    run_iteration(1);
                 }
             }
             iters += per_check;
@@ -1052,15 +1078,112 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         }
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        for (cudaEvent_t e : pe)
+            if (e) cudaEventDestroy(e);
         if (counters_dev) {
-            unsigned long long out[5] = {E.host_ctr->rays, E.host_ctr->shadow_rays, E.host_ctr->dropped,
-                                         E.host_ctr->node_visits, E.host_ctr->tri_tests};
+            unsigned long long out[7] = {E.host_ctr->rays, E.host_ctr->shadow_rays, E.host_ctr->dropped,
+                                         E.host_ctr->node_visits, E.host_ctr->tri_tests,
+                                         E.host_ctr->node_visits_shadow, E.host_ctr->tri_tests_shadow};
             HK_CUDA(cudaMemcpyAsync(counters_dev, out, sizeof out, cudaMemcpyHostToDevice, st));
             HK_CUDA(cudaStreamSynchronize(st));
         }
         // the caller's stream continues after the engine's work
         HK_CUDA(cudaEventRecord(E.ev, st));
         HK_CUDA(cudaStreamWaitEvent(user, E.ev, 0));
+        return HK_OK;
+    });
+}
+int hk_render_batch_host(hk_scene *s, const hk_render_desc *descs, int n, const hk_wavefront_config *cfg,
+                         float *const *rgb_host, unsigned long long *counters_host, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (!descs || !rgb_host || n <= 0 || n > hk::kWfMaxJobs) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        cudaStream_t st = (cudaStream_t)stream;
+        size_t FW = s->width + 2 * s->dev.border, FH = s->height + 2 * s->dev.border;
+        size_t film_bytes = FW * FH * 4 * sizeof(float), rgb_bytes = (size_t)s->width * s->height * 3 * sizeof(float);
+        while ((int)s->batch_films.size() < n) {
+            s->batch_films.emplace_back(new DevBuf());
+            s->batch_films.back()->alloc(film_bytes);
+        }
+        if (s->b_rgb.bytes < rgb_bytes) s->b_rgb.alloc(rgb_bytes);
+        unsigned long long *ctr = (unsigned long long *)s->b_scratch.p + 1;   // 7 slots
+        std::vector<hk_render_job> jobs(n);
+        for (int j = 0; j < n; ++j) {
+            if (s->batch_films[j]->bytes < film_bytes) s->batch_films[j]->alloc(film_bytes);
+            HK_CUDA(cudaMemsetAsync(s->batch_films[j]->p, 0, film_bytes, st));
+            jobs[j].film_dev = s->batch_films[j]->as<float>();
+            jobs[j].desc = descs[j];
+        }
+        int rc = hk_render_batch(s, jobs.data(), n, cfg, ctr, stream);
+        if (rc != HK_OK) return rc;
+        for (int j = 0; j < n; ++j) {
+            HK_CUDA(hk::launch_resolve(jobs[j].film_dev, s->b_rgb.as<float>(), (int)s->width, (int)s->height,
+                                       s->dev.border, st));
+            HK_CUDA(cudaMemcpyAsync(rgb_host[j], s->b_rgb.p, rgb_bytes, cudaMemcpyDeviceToHost, st));
+        }
+        if (counters_host)
+            HK_CUDA(cudaMemcpyAsync(counters_host, ctr, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        HK_CUDA(cudaStreamSynchronize(st));
+        return HK_OK;
+    });
+}
+int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront_config *best, float *best_ms) {
+    return guarded([&] {
+        require_built(s);
+        if (!probe || !best) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        // probe film (the tuner allocates; rendering afterwards does not need it)
+        size_t FW = s->width + 2 * s->dev.border, FH = s->height + 2 * s->dev.border;
+        DevBuf film;
+        film.alloc(FW * FH * 4 * sizeof(float));
+        hk_render_job job;
+        job.film_dev = film.as<float>();
+        job.desc = *probe;
+        cudaEvent_t e0, e1;
+        HK_CUDA(cudaEventCreate(&e0));
+        HK_CUDA(cudaEventCreate(&e1));
+        float best_t = INFINITY;
+        hk_wavefront_config bc{};
+        const int caps[] = {1 << 20, 1 << 21, 1 << 22};
+        const int threads[] = {64, 128, 256};
+        const int checks[] = {16, 64};
+        auto run = [&](const hk_wavefront_config &c) {
+            HK_CUDA(cudaMemset(film.p, 0, film.bytes));
+            int rc = hk_render_batch(s, &job, 1, &c, nullptr, nullptr);   // warm (allocation, graph)
+            if (rc != HK_OK) throw HkError{rc, hk_last_error()};
+            HK_CUDA(cudaEventRecord(e0, nullptr));
+            rc = hk_render_batch(s, &job, 1, &c, nullptr, nullptr);
+            if (rc != HK_OK) throw HkError{rc, hk_last_error()};
+            HK_CUDA(cudaEventRecord(e1, nullptr));
+            HK_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            HK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            return ms;
+        };
+        // coordinate descent: capacity, then block sizes, then the check interval
+        hk_wavefront_config c{};
+        c.threads_extend = 128; c.threads_shade = 128; c.iterations_per_check = 16;
+        for (int cap : caps) {
+            c.capacity = cap;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        c = bc;
+        for (int te : threads)
+            for (int ts : threads) {
+                c.threads_extend = te; c.threads_shade = ts;
+                float ms = run(c);
+                if (ms < best_t) { best_t = ms; bc = c; }
+            }
+        c = bc;
+        for (int k : checks) {
+            c.iterations_per_check = k;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        *best = bc;
+        if (best_ms) *best_ms = best_t;
         return HK_OK;
     });
 }

@@ -177,7 +177,7 @@ __global__ void wf_reset_kernel(WfState W, int cur) {
 }
 
 // ------------------------------------------------------------ extend
-__global__ void __launch_bounds__(128) wf_extend_kernel(DevScene S, WfState W, int cur) {
+__global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, int cur) {
     const int n = (int)W.ctr->eq_count[cur];
     TravStats ts;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(128) wf_extend_kernel(DevScene S, WfState W, i
 __device__ __forceinline__ void finish(const WfState &W, int slot) { W.fq[warp_append(&W.ctr->fq_count)] = slot; }
 
 template <int kType>
-__global__ void __launch_bounds__(128) wf_shade_kernel(DevScene S, WfState W, int nxt) {
+__global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, int nxt) {
     const int n = (int)W.ctr->sq_count[kType];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = W.sq[kType][i];
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(DevScene S, WfState W, in
 }
 
 // ------------------------------------------------------------ shadow
-__global__ void __launch_bounds__(128) wf_shadow_kernel(DevScene S, WfState W) {
+__global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
     const int n = min((int)W.ctr->shadow_count, W.max_shadow);
     TravStats ts;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -369,8 +369,8 @@ __global__ void __launch_bounds__(128) wf_shadow_kernel(DevScene S, WfState W) {
         nt += __shfl_down_sync(0xffffffffu, nt, o);
     }
     if (lane_id() == 0 && (nv || nt)) {
-        atomicAdd(&W.ctr->node_visits, nv);
-        atomicAdd(&W.ctr->tri_tests, nt);
+        atomicAdd(&W.ctr->node_visits_shadow, nv);
+        atomicAdd(&W.ctr->tri_tests_shadow, nt);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&W.ctr->shadow_rays, (unsigned long long)n);
 }
@@ -393,6 +393,28 @@ cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLau
     wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W);
+    return cudaGetLastError();
+}
+
+cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, int phase,
+                            cudaStream_t st) {
+    const int nxt = cur ^ 1;
+    switch (phase) {
+    case 0:
+        wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur, 0);
+        wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
+        break;
+    case 1: wf_extend_kernel<<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur); break;
+    case 2:
+        wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+        wf_shade_kernel<1><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+        wf_shade_kernel<2><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+        wf_shade_kernel<3><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+        wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+        wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+        break;
+    default: wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W); break;
+    }
     return cudaGetLastError();
 }
 

@@ -43,7 +43,9 @@ struct WfCounters {
     unsigned int shadow_count;         // next-event shadow rays
     unsigned int active;               // paths in flight
     unsigned int pad;
-    unsigned long long rays, shadow_rays, dropped, node_visits, tri_tests, paths;
+    unsigned long long rays, shadow_rays, dropped;
+    unsigned long long node_visits, tri_tests;                 // closest-hit traversal (extend)
+    unsigned long long node_visits_shadow, tri_tests_shadow;   // any-hit traversal (shadow)
 };
 
 struct WfState {
@@ -84,6 +86,9 @@ struct WfLaunchConfig {
 cudaError_t wf_launch_init(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st);
 // one iteration with extend queue `cur` (0/1)
 cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st);
+// one phase of an iteration: 0 regen + reset, 1 extend, 2 shade (all materials), 3 shadow
+cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, int phase,
+                            cudaStream_t st);
 int wf_occupancy(int which, int threads);
 
 }  // namespace hk

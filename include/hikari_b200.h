@@ -153,16 +153,31 @@ typedef struct {
     int32_t threads_shade;         /* block size of the shade kernels (0 = 128) */
     int32_t iterations_per_check;  /* iterations between host termination checks (0 = 16) */
     int32_t no_graph;              /* 1: launch kernels directly instead of replaying a CUDA graph */
+    float *kernel_ms;              /* optional host float[4]: adds the device time of the regen, extend,
+                                      shade and shadow phases (timed with events, no graph) */
+    int32_t *kernel_launches;      /* optional host int32[4]: adds the kernel launches per phase */
 } hk_wavefront_config;
 
 /* Render every job of the batch with the wavefront integrator: a pool of path
  * slots shared by all images, compacted ray queues, one shading kernel per
  * material type, and iterations replayed from a CUDA graph.  Same estimator
  * as hk_render (PathMISIntegrator::Li, src/integrator/PathMISIntegrator.cpp:16).
- * Returns when every job is done; counters_dev (optional, 5 x u64): rays,
- * shadow rays, dropped samples, node visits, triangle tests. */
+ * Returns when every job is done; counters_dev (optional, 7 x u64): rays,
+ * shadow rays, dropped samples, node visits and triangle tests of the
+ * closest-hit traversal, node visits and triangle tests of the shadow rays. */
 int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_wavefront_config *cfg,
                     unsigned long long *counters_dev, void *stream);
+
+/* End-to-end batch: render n images with the wavefront into films owned by the
+ * scene, resolve them and copy each H*W*3 float image to host memory
+ * rgb_host[i].  counters_host (optional, 7 x u64) as hk_render_batch. */
+int hk_render_batch_host(hk_scene *s, const hk_render_desc *descs, int n, const hk_wavefront_config *cfg,
+                         float *const *rgb_host, unsigned long long *counters_host, void *stream);
+
+/* Autotuner: render `probe` (one image) under candidate configurations --
+ * slot capacity 2^20..2^22, block sizes 64/128/256, termination-check
+ * interval 16/64 -- by coordinate descent and return the fastest. */
+int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront_config *best, float *best_ms);
 
 /* Render into a caller-provided device image without allocating any device
  * memory.  This entry point has no counterpart in the reference.  It is for

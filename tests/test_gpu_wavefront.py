@@ -46,7 +46,7 @@ def test_wavefront_cornell_matches_oracle():
     sd.filter = FilterDesc(0, 0.5)
     gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
     film = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
-    ctr = torch.zeros(5, dtype=torch.int64, device=DEV)
+    ctr = torch.zeros(7, dtype=torch.int64, device=DEV)
     gs.render_batch([film], spp=4096, depth=sd.depth, seeds=[7], counters=ctr, capacity=1 << 18)
     g = _resolve(gs, film).reshape(-1, 3).astype(np.float64)
     pix = np.stack(np.meshgrid(np.arange(48), np.arange(48), indexing="xy"), -1).reshape(-1, 2)
