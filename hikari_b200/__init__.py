@@ -304,7 +304,8 @@ class Scene:
                      no_graph: bool = False, kernel_ms=None, kernel_launches=None, stream=None) -> None:
         """Wavefront render of several images at once: films[i] (device
         tensors of film_shape()) accumulate spp samples of view cameras[i].
-        counters: device int64 tensor of 7 (see hk_render_batch).  kernel_ms /
+        counters: device int64 tensor of 7 that the statistics are added to
+        (see hk_render_batch).  kernel_ms /
         kernel_launches: host float32[4] / int32[4] arrays that receive the
         per-phase device time and launch counts (profiling; no graph)."""
         n = len(films)

@@ -1080,13 +1080,7 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         if (graph) cudaGraphDestroy(graph);
         for (cudaEvent_t e : pe)
             if (e) cudaEventDestroy(e);
-        if (counters_dev) {
-            unsigned long long out[7] = {E.host_ctr->rays, E.host_ctr->shadow_rays, E.host_ctr->dropped,
-                                         E.host_ctr->node_visits, E.host_ctr->tri_tests,
-                                         E.host_ctr->node_visits_shadow, E.host_ctr->tri_tests_shadow};
-            HK_CUDA(cudaMemcpyAsync(counters_dev, out, sizeof out, cudaMemcpyHostToDevice, st));
-            HK_CUDA(cudaStreamSynchronize(st));
-        }
+        if (counters_dev) HK_CUDA(hk::wf_launch_counters_add(W, counters_dev, st));
         // the caller's stream continues after the engine's work
         HK_CUDA(cudaEventRecord(E.ev, st));
         HK_CUDA(cudaStreamWaitEvent(user, E.ev, 0));
@@ -1107,6 +1101,7 @@ int hk_render_batch_host(hk_scene *s, const hk_render_desc *descs, int n, const 
         }
         if (s->b_rgb.bytes < rgb_bytes) s->b_rgb.alloc(rgb_bytes);
         unsigned long long *ctr = (unsigned long long *)s->b_scratch.p + 1;   // 7 slots
+        HK_CUDA(cudaMemsetAsync(ctr, 0, 7 * sizeof(unsigned long long), st));
         std::vector<hk_render_job> jobs(n);
         for (int j = 0; j < n; ++j) {
             if (s->batch_films[j]->bytes < film_bytes) s->batch_films[j]->alloc(film_bytes);

@@ -375,7 +375,24 @@ __global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&W.ctr->shadow_rays, (unsigned long long)n);
 }
 
+// Add the engine's statistics to a caller's 7-slot u64 array.
+__global__ void wf_counters_add_kernel(const WfCounters *c, unsigned long long *out) {
+    if (threadIdx.x != 0) return;
+    out[0] += c->rays;
+    out[1] += c->shadow_rays;
+    out[2] += c->dropped;
+    out[3] += c->node_visits;
+    out[4] += c->tri_tests;
+    out[5] += c->node_visits_shadow;
+    out[6] += c->tri_tests_shadow;
+}
+
 // ------------------------------------------------------------ launchers
+cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st) {
+    wf_counters_add_kernel<<<1, 32, 0, st>>>(W.ctr, out);
+    return cudaGetLastError();
+}
+
 cudaError_t wf_launch_init(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
     wf_regen_kernel<<<(W.capacity + C.threads_regen - 1) / C.threads_regen, C.threads_regen, 0, st>>>(S, W, 0, 1);
     return cudaGetLastError();

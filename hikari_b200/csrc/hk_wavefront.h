@@ -89,6 +89,8 @@ cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLau
 // one phase of an iteration: 0 regen + reset, 1 extend, 2 shade (all materials), 3 shadow
 cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, int phase,
                             cudaStream_t st);
+// out[0..6] += rays, shadow rays, dropped, node visits, triangle tests, shadow node visits, shadow tests
+cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st);
 int wf_occupancy(int which, int threads);
 
 }  // namespace hk

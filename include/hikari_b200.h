@@ -162,9 +162,10 @@ typedef struct {
  * slots shared by all images, compacted ray queues, one shading kernel per
  * material type, and iterations replayed from a CUDA graph.  Same estimator
  * as hk_render (PathMISIntegrator::Li, src/integrator/PathMISIntegrator.cpp:16).
- * Returns when every job is done; counters_dev (optional, 7 x u64): rays,
+ * Returns when every job is done; counters_dev (optional, 7 x u64) gets rays,
  * shadow rays, dropped samples, node visits and triangle tests of the
- * closest-hit traversal, node visits and triangle tests of the shadow rays. */
+ * closest-hit traversal, node visits and triangle tests of the shadow rays
+ * added (as hk_render adds its 5). */
 int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_wavefront_config *cfg,
                     unsigned long long *counters_dev, void *stream);
 
