@@ -40,7 +40,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="heterogeneous", choices=["heterogeneous", "mesh_heavy", "cornell"])
+    ap.add_argument("--workload", default="heterogeneous",
+                    choices=["heterogeneous", "mesh_heavy", "cornell", "serving"])
+    ap.add_argument("--jobs", type=int, default=40, help="serving: jobs of the Poisson run")
+    ap.add_argument("--load", type=float, default=0.8, help="serving: arrival rate as a fraction of the peak")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--res", type=int, default=0)
@@ -205,8 +208,91 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def serving_scenes():
+    """The serving set: Cornell box, the mesh-heavy icosphere, the heterogeneous
+    scene and five seeded variants of it from about 20k to 3M triangles."""
+    from hikari_b200 import scenes
+
+    sds = [scenes.cornell_box(width=256, height=256, spp=64),
+           scenes.mesh_heavy("conductor", width=1024, height=1024, spp=256, depth=16),
+           scenes.heterogeneous(width=1024, height=1024, spp=128, depth=16)]
+    for k, n in enumerate((1, 4, 12, 24, 40)):
+        sds.append(scenes.heterogeneous(width=1024, height=1024, spp=128, depth=16, n_spheres=n, seed=k + 1))
+    return sds
+
+
+def run_serving(args):
+    """Serving: a Poisson stream of jobs over 8 resident scenes, each job a
+    square image of 256, 512 or 1024 pixels at 16, 64 or 256 spp.  Measures
+    the peak sustainable throughput (all jobs submitted at once), each job's
+    latency alone on the idle server, and the latencies of a Poisson run at
+    --load x the peak arrival rate."""
+    import torch
+
+    import hikari_b200 as hk
+    from hikari_b200 import serving
+
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    sds = serving_scenes()
+    gss = [hk.Scene.from_desc(sd) for sd in sds]
+    build_s = time.perf_counter() - t0
+    tris = [int(g.info.n_triangles) for g in gss]
+    rng = np.random.default_rng(7)
+    depths = [sd.depth for sd in sds]
+    with serving.Server(capacity=1 << 20, iterations_per_poll=4) as srv:
+        for g in gss:
+            srv.add_scene(g)
+        for k in range(len(gss)):   # engines and graphs of every scene (untimed)
+            srv.wait(srv.submit(k, 4, depths[k], 1, 64, 64)[0])
+        # peak: a burst of jobs submitted at once
+        burst = serving.job_mix(max(16, args.jobs // 2), len(gss), rng, depths)
+        t = time.perf_counter()
+        ids = [srv.submit(j.scene, j.spp, j.depth, j.seed, j.width, j.height)[0] for j in burst]
+        for i in ids:
+            srv.wait(i)
+        makespan = time.perf_counter() - t
+        peak_mpaths = sum(j.paths for j in burst) / makespan / 1e6
+        jobs = serving.job_mix(args.jobs, len(gss), rng, depths)
+        mean_paths = float(np.mean([j.paths for j in jobs]))
+        peak_rate = peak_mpaths * 1e6 / mean_paths
+        iso = serving.isolated_latencies(srv, jobs)
+        rate = args.load * peak_rate
+        res = serving.run_poisson(srv, jobs, rate, seed=11, isolated=iso)
+        summ = res.summary()
+        st = srv.stats()
+    line = {
+        "metric": "Mpaths/s", "value": summ["mpaths_per_s"], "unit": "Mpaths/s", "n_gpus": 1, "steps": 1,
+        "warmup": 1, "ms_per_step": summ["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scenes)",
+        "config": {"workload": "serving: Poisson arrivals over 8 resident scenes (Cornell box, mesh-heavy 1.31M tris, "
+                               "heterogeneous 4.75M tris, 5 heterogeneous variants); jobs of 256/512/1024 px "
+                               "square at 16/64/256 spp",
+                   "form": "wavefront serving loop (continuous batching, SRPT dispatch)", "triangles": tris,
+                   "scene_build_s": round(build_s, 2), "capacity": 1 << 20, "jobs": args.jobs,
+                   "load": args.load},
+        "serving": {
+            "peak_mpaths_per_s": peak_mpaths, "peak_rate_hz": peak_rate, "arrival_rate_hz": rate,
+            "mean_job_paths": mean_paths,
+            "latency_s": {"p50": summ["p50_s"], "p95": summ["p95_s"], "p99": summ["p99_s"]},
+            "isolated_latency_s": {"p50": float(np.percentile(iso, 50)), "p95": float(np.percentile(iso, 95)),
+                                   "p99": float(np.percentile(iso, 99))},
+            "p99_over_isolated_p99": summ["p99_s"] / float(np.percentile(iso, 99)),
+            "slowdown": {"p50": summ["slowdown_p50"], "p95": summ["slowdown_p95"], "p99": summ["slowdown_p99"]},
+            "rays": int(st["rays"]), "shadow_rays": int(st["shadow_rays"]),
+        },
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "serving":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop"}), flush=True)
+        elif int(os.environ.get("RANK", "0")) == 0:
+            run_serving(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -48,7 +48,7 @@ class RenderDesc(C.Structure):
     _fields_ = [
         ("spp", C.c_int32), ("depth", C.c_int32), ("rr_start", C.c_int32), ("sample_offset", C.c_int32),
         ("seed", C.c_uint64), ("image_index", C.c_int32), ("spp_per_item", C.c_int32),
-        ("use_camera", C.c_int32), ("camera_to_world", C.c_float * 16),
+        ("use_camera", C.c_int32), ("camera_to_world", C.c_float * 16), ("width", C.c_int32), ("height", C.c_int32),
     ]
 
 
@@ -62,9 +62,29 @@ class WavefrontConfig(C.Structure):
                 ("kernel_launches", C.c_void_p)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("capacity", C.c_int32), ("threads_extend", C.c_int32), ("threads_shade", C.c_int32),
+                ("iterations_per_poll", C.c_int32), ("policy", C.c_int32), ("max_jobs", C.c_int32),
+                ("hbm_budget", C.c_uint64)]
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("state", C.c_int32), ("scene", C.c_int32), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("paths", C.c_uint64), ("device_bytes", C.c_uint64), ("submit_s", C.c_double),
+                ("admit_s", C.c_double), ("done_s", C.c_double), ("latency_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("jobs_submitted", C.c_uint64), ("jobs_done", C.c_uint64), ("jobs_cancelled", C.c_uint64),
+                ("jobs_queued", C.c_uint64), ("jobs_running", C.c_uint64), ("paths_done", C.c_uint64),
+                ("rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("bytes_in_use", C.c_uint64),
+                ("hbm_budget", C.c_uint64), ("busy_s", C.c_double), ("now_s", C.c_double)]
+
+
 def render_desc(spp, depth, seed=0, sample_offset=0, rr_start=0, image_index=0, spp_per_item=0,
-                camera=None) -> RenderDesc:
+                camera=None, width=0, height=0) -> RenderDesc:
     d = RenderDesc(spp, depth, rr_start, sample_offset, seed, image_index, spp_per_item, 0)
+    d.width, d.height = int(width), int(height)
     if camera is not None:
         d.use_camera = 1
         d.camera_to_world[:] = [float(x) for x in np.asarray(camera, np.float32).reshape(16)]
@@ -110,6 +130,14 @@ def lib():
                                   C.POINTER(C.c_void_p), P, P], C.c_int),
         "hk_wavefront_autotune": ([P, C.POINTER(RenderDesc), C.POINTER(WavefrontConfig), C.POINTER(C.c_float)],
                                   C.c_int),
+        "hk_server_create": ([C.POINTER(ServerConfig), C.POINTER(P)], C.c_int),
+        "hk_server_destroy": ([P], C.c_int),
+        "hk_server_add_scene": ([P, P, C.POINTER(I32)], C.c_int),
+        "hk_job_submit": ([P, I32, C.POINTER(RenderDesc), P, C.POINTER(U64)], C.c_int),
+        "hk_job_poll": ([P, U64, C.POINTER(JobStatus)], C.c_int),
+        "hk_job_wait": ([P, U64, C.c_double, C.POINTER(JobStatus)], C.c_int),
+        "hk_job_cancel": ([P, U64], C.c_int),
+        "hk_server_get_stats": ([P, C.POINTER(ServerStats)], C.c_int),
         "hk_trace": ([P, U64, P, P, P, P, P, C.c_int, P, P], C.c_int),
         "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
         "hk_emitter_sample": ([P, I32, U64, P, P, P], C.c_int),
@@ -269,12 +297,12 @@ class Scene:
     def width(self):
         return self.desc.camera.width if self.desc else None
 
-    def film_shape(self):
-        import torch  # noqa: F401
-
+    def film_shape(self, width: int = 0, height: int = 0):
+        """Film (RGBW accumulator) shape at the scene camera's size or at width x height."""
         B = self.info.film_border
         cam = self.desc.camera
-        return (cam.height + 2 * B, cam.width + 2 * B, 4)
+        w, h = (width or cam.width), (height or cam.height)
+        return (h + 2 * B, w + 2 * B, 4)
 
     def render(self, film, spp: int, depth: int, seed: int = 0, sample_offset: int = 0, rr_start: int = 0,
                image_index: int = 0, counters=None, spp_per_item: int = 0, camera=None, stream=None) -> None:
@@ -301,9 +329,11 @@ class Scene:
     def render_batch(self, films, spp: int, depth: int, seeds=None, cameras=None, image_indices=None,
                      sample_offset: int = 0, rr_start: int = 0, counters=None, capacity: int = 0,
                      threads_extend: int = 0, threads_shade: int = 0, iterations_per_check: int = 0,
-                     no_graph: bool = False, kernel_ms=None, kernel_launches=None, stream=None) -> None:
+                     no_graph: bool = False, kernel_ms=None, kernel_launches=None, sizes=None,
+                     stream=None) -> None:
         """Wavefront render of several images at once: films[i] (device
-        tensors of film_shape()) accumulate spp samples of view cameras[i].
+        tensors of film_shape(), or of film_shape(*sizes[i]) with per-image
+        sizes (width, height)) accumulate spp samples of view cameras[i].
         counters: device int64 tensor of 7 that the statistics are added to
         (see hk_render_batch).  kernel_ms /
         kernel_launches: host float32[4] / int32[4] arrays that receive the
@@ -315,7 +345,8 @@ class Scene:
             seed = seeds[i] if seeds is not None else i
             idx = image_indices[i] if image_indices is not None else i
             jobs[i].film_dev = _p(f)
-            jobs[i].desc = render_desc(spp, depth, seed, sample_offset, rr_start, idx, 0, cam)
+            w, h = sizes[i] if sizes is not None else (0, 0)
+            jobs[i].desc = render_desc(spp, depth, seed, sample_offset, rr_start, idx, 0, cam, w, h)
         cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, int(no_graph),
                               _p(kernel_ms), _p(kernel_launches))
         check(lib().hk_render_batch(self.h, jobs, n, C.byref(cfg), _p(counters), _stream(stream)))

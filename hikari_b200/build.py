@@ -7,6 +7,7 @@ change a result.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -15,9 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libhikari_b200.so")
-SOURCES = ["hk_kernels.cu", "hk_wavefront.cu", "hk_host.cpp", "hk_bvh.cpp", "hk_xml.cpp"]
+SOURCES = ["hk_kernels.cu", "hk_wavefront.cu", "hk_host.cpp", "hk_engine.cpp", "hk_server.cpp", "hk_bvh.cpp", "hk_xml.cpp"]
 HEADERS = ["hk_device.h", "hk_math.cuh", "hk_bsdf.cuh", "hk_traverse.cuh", "hk_shading.cuh", "hk_kernels.h",
-           "hk_bvh.h", "hk_xml.h", "hk_wavefront.h"]
+           "hk_bvh.h", "hk_xml.h", "hk_wavefront.h", "hk_engine.h", "hk_hostutil.h", "hk_internal.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-pthread",
                      "--expt-relaxed-constexpr"]
@@ -43,7 +44,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
+    cmds, objs = [], []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(OUT_DIR, src + ".o")
@@ -52,8 +53,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
             cmd = [_nvcc()] + NVCC_FLAGS + ["-x", "cu", "-c", path, "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        subprocess.check_call(cmd)
+        cmds.append(cmd)
         objs.append(obj)
+    # translation units compile in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     subprocess.check_call([_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lpthread", "-lz"])
     os.replace(tmp, LIB)

@@ -1,0 +1,77 @@
+// Host driver of one wavefront engine: the path-slot pool of one scene in HBM,
+// its job table and dispatch plan, its own stream and the CUDA graph of its
+// iterations.  hk_render_batch runs one engine per scene over a fixed batch;
+// the serving loop keeps one engine per resident scene and adds jobs to it
+// while it runs.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "hk_device.h"
+#include "hk_hostutil.h"
+#include "hk_wavefront.h"
+
+namespace hk {
+
+struct WfEngineConfig {
+    int capacity = 1 << 21;   // path slots
+    int threads_extend = 128;
+    int threads_shade = 128;
+};
+
+class WfEngine {
+public:
+    // S must stay valid (its device buffers alive) for the engine's lifetime.
+    WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg);
+    ~WfEngine();
+    WfEngine(const WfEngine &) = delete;
+    WfEngine &operator=(const WfEngine &) = delete;
+
+    // Device bytes an engine of this capacity holds for a scene with nemitters emitters.
+    static size_t bytes_for(int capacity, int nemitters);
+    size_t device_bytes() const { return bytes_; }
+    const WfEngineConfig &config() const { return cfg_; }
+    cudaStream_t stream() const { return stream_; }
+
+    // Empty pool (every slot idle), zero statistics, empty plan.  Async on stream().
+    void reset();
+    // Job-table entry `slot`: its finished counter is zeroed and J.finished set.  Async;
+    // the slot must not be in use by paths in flight.
+    void set_job(int slot, WfJob J);
+    // Dispatch plan: pieces sorted by plan_begin, `total` items.  Async.
+    void set_plan(const std::vector<WfSeg> &segs, uint64_t total);
+    // `iterations` (even) wavefront iterations, from the graph or as plain launches.
+    // With kernel_ms (host float[4]) each phase is timed with events and added.
+    void run(int iterations, bool use_graph, float *kernel_ms = nullptr, int32_t *kernel_launches = nullptr);
+    // Copy the counters and the job table's finished counters to the host mirrors
+    // and record done_event(); read them after the event completed.
+    void fetch_status();
+    cudaEvent_t done_event() const { return ev_done_; }
+    const WfCounters &status() const { return *h_ctr_.p; }
+    const unsigned long long *finished() const { return h_fin_.p; }
+    // Add the statistics to a caller's 7-slot device array.  Async.
+    void add_counters(unsigned long long *out_dev);
+    const WfState &state() const { return W_; }
+
+private:
+    void capture();
+    DevScene S_;
+    WfEngineConfig cfg_;
+    WfLaunchConfig L_{};
+    WfState W_{};
+    size_t bytes_ = 0;
+    DevBuf state_, queues_, shadow_, counters_, jobs_, finished_, segs_;
+    PinnedBuf<WfCounters> h_ctr_;
+    PinnedBuf<unsigned long long> h_fin_;
+    PinnedBuf<WfJob> h_jobs_;
+    PinnedBuf<WfSeg> h_segs_;
+    PinnedBuf<WfCounters> h_head_;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev_done_ = nullptr, ev_plan_ = nullptr, pe_[2] = {nullptr, nullptr};
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+};
+
+}  // namespace hk

@@ -14,7 +14,10 @@
 
 #include "../../include/hikari_b200.h"
 #include "hk_bvh.h"
+#include "hk_hostutil.h"
 #include "hk_device.h"
+#include "hk_engine.h"
+#include "hk_internal.h"
 #include "hk_kernels.h"
 #include "hk_wavefront.h"
 
@@ -23,39 +26,20 @@ extern "C" int hk_scene_load_xml_impl(const char *path, const char *data_dir, hk
 extern "C" int hk_exr_read_impl(const char *path, int *w, int *h, std::vector<float> *rgb, std::string *err);
 extern "C" int hk_exr_write_impl(const char *path, int w, int h, const float *rgb, std::string *err);
 
-namespace {
-
+namespace hk {
 thread_local std::string g_error;
-
 int set_error(int code, const std::string &msg) {
     g_error = msg;
     return code;
 }
+}  // namespace hk
 
-struct HkError {
-    int code;
-    std::string msg;
-};
-#define HK_CUDA(call)                                                                                   \
-    do {                                                                                                \
-        cudaError_t e_ = (call);                                                                        \
-        if (e_ != cudaSuccess)                                                                          \
-            throw HkError{e_ == cudaErrorMemoryAllocation ? HK_ERR_NOMEM : HK_ERR_CUDA,                 \
-                          std::string(#call) + ": " + cudaGetErrorString(e_)};                          \
-    } while (0)
+using hk::DevBuf;
+using hk::guarded;
+using hk::HkError;
+using hk::set_error;
 
-template <class F>
-int guarded(F &&f) {
-    try {
-        return f();
-    } catch (const HkError &e) {
-        return set_error(e.code, e.msg);
-    } catch (const std::bad_alloc &) {
-        return set_error(HK_ERR_NOMEM, "host allocation failed");
-    } catch (const std::exception &e) {
-        return set_error(HK_ERR_INVALID, e.what());
-    }
-}
+namespace {
 
 // ------------------------------------------------------------ float helpers
 // Host 3-vectors in the reference's Eigen evaluation order: x + (y + z).
@@ -205,34 +189,6 @@ struct RftTable {
     }
 };
 
-// ------------------------------------------------------------ device buffers
-struct DevBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf &) = delete;
-    DevBuf &operator=(const DevBuf &) = delete;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        bytes = 0;
-    }
-    void alloc(size_t n) {
-        release();
-        if (n == 0) n = 16;
-        HK_CUDA(cudaMalloc(&p, n));
-        bytes = n;
-    }
-    template <class T>
-    void upload(const std::vector<T> &v) {
-        alloc(v.size() * sizeof(T));
-        if (!v.empty()) HK_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
-    }
-    template <class T>
-    T *as() const { return (T *)p; }
-};
-
 struct MeshIn {
     std::vector<float> pos, nrm;
     std::vector<uint32_t> idx;
@@ -272,21 +228,7 @@ struct hk_scene {
     int margin_lo = 0, margin_hi = 0;
     int sm_count = 148;
     int occupancy = 1;
-    // wavefront engine (allocated on first use)
-    struct Wavefront {
-        int capacity = 0, max_shadow = 0;
-        DevBuf state, queues, shadow, counters, jobs, finished;
-        hk::WfState W{};
-        hk::WfCounters *host_ctr = nullptr;   // pinned mirror for termination checks
-        cudaStream_t stream = nullptr;
-        cudaEvent_t ev = nullptr;
-        ~Wavefront() {
-            if (host_ctr) cudaFreeHost(host_ctr);
-            if (stream) cudaStreamDestroy(stream);
-            if (ev) cudaEventDestroy(ev);
-        }
-    };
-    std::unique_ptr<Wavefront> wf;
+    std::unique_ptr<hk::WfEngine> wf;   // wavefront engine (allocated on first use)
 };
 
 namespace {
@@ -380,6 +322,7 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
 void build_scene(hk_scene *s) {
     if (s->meshes.empty()) throw HkError{HK_ERR_INVALID, "scene has no meshes"};
     if (s->width == 0 || s->height == 0) throw HkError{HK_ERR_INVALID, "camera has an empty film"};
+    s->wf.reset();   // the engine holds a copy of the device description that is rebuilt here
     hk::DevScene &D = s->dev;
     std::memset(&D, 0, sizeof D);
     size_t dev_bytes = 0;
@@ -622,46 +565,85 @@ void require_built(const hk_scene *s) {
     if (!s) throw HkError{HK_ERR_INVALID, "null scene"};
     if (!s->built) throw HkError{HK_ERR_INVALID, "scene is not built (call hk_scene_build)"};
 }
+// The megakernel entry points render at the scene camera's size only.
+void require_scene_size(const hk_scene *s, const hk_render_desc &d) {
+    if ((d.width != 0 && (uint32_t)d.width != s->width) || (d.height != 0 && (uint32_t)d.height != s->height))
+        throw HkError{HK_ERR_INVALID, "this entry point renders at the scene camera's resolution only"};
+}
 
 // ------------------------------------------------------------ wavefront engine
-void wf_ensure(hk_scene *s, int capacity) {
-    if (s->wf && s->wf->capacity == capacity) return;
-    s->wf.reset(new hk_scene::Wavefront());
-    auto &E = *s->wf;
-    E.capacity = capacity;
-    E.max_shadow = capacity * std::max(1, s->dev.nemitters);
-    const size_t N = (size_t)capacity;
-    // state: 9 float4-sized arrays per slot
-    E.state.alloc(N * 16 * 9);
-    E.queues.alloc(N * sizeof(int) * (2 + hk::kWfTypes + 1));
-    E.shadow.alloc((size_t)E.max_shadow * 16 * 3);
-    E.counters.alloc(sizeof(hk::WfCounters));
-    E.jobs.alloc(sizeof(hk::WfJob) * hk::kWfMaxJobs);
-    E.finished.alloc(sizeof(unsigned long long) * hk::kWfMaxJobs);
-    hk::WfState &W = E.W;
-    W.capacity = capacity;
-    W.max_shadow = E.max_shadow;
-    float4 *st = E.state.as<float4>();
-    W.ray_o = st; W.ray_d = st + N; W.beta = st + 2 * N; W.lacc = st + 3 * N; W.pix = st + 4 * N;
-    W.rng = (uint4 *)(st + 5 * N); W.prev_wi = st + 6 * N; W.prev_wo = st + 7 * N; W.hit = st + 8 * N;
-    int *q = E.queues.as<int>();
-    W.eq[0] = q; W.eq[1] = q + N;
-    for (int t = 0; t < hk::kWfTypes; ++t) W.sq[t] = q + (2 + t) * N;
-    W.fq = q + (2 + hk::kWfTypes) * N;
-    float4 *sh = E.shadow.as<float4>();
-    W.sh_o = sh; W.sh_d = sh + E.max_shadow; W.sh_c = sh + 2 * (size_t)E.max_shadow;
-    W.ctr = E.counters.as<hk::WfCounters>();
-    W.jobs = E.jobs.as<hk::WfJob>();
-    HK_CUDA(cudaMallocHost((void **)&E.host_ctr, sizeof(hk::WfCounters)));
-    HK_CUDA(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
-    HK_CUDA(cudaEventCreateWithFlags(&E.ev, cudaEventDisableTiming));
+hk::WfEngine &wf_ensure(hk_scene *s, const hk::WfEngineConfig &c) {
+    if (s->wf) {
+        const hk::WfEngineConfig &o = s->wf->config();
+        if (o.capacity == c.capacity && o.threads_extend == c.threads_extend && o.threads_shade == c.threads_shade)
+            return *s->wf;
+        s->wf.reset();
+    }
+    s->wf.reset(new hk::WfEngine(s->dev, s->sm_count, c));
+    return *s->wf;
 }
 
 }  // namespace
 
+namespace hk {
+
+SceneView scene_view(hk_scene *s) {
+    require_built(s);
+    SceneView v;
+    v.dev = &s->dev;
+    v.sm_count = s->sm_count;
+    v.width = s->width;
+    v.height = s->height;
+    return v;
+}
+
+JobSize job_size(const hk_scene *s, const hk_render_desc &d) {
+    if (d.width < 0 || d.height < 0) throw HkError{HK_ERR_INVALID, "negative image size"};
+    JobSize z;
+    z.width = d.width > 0 ? (uint32_t)d.width : s->width;
+    z.height = d.height > 0 ? (uint32_t)d.height : s->height;
+    if (z.width > 16384 || z.height > 16384) throw HkError{HK_ERR_INVALID, "image larger than 16384 x 16384"};
+    const size_t FW = z.width + 2 * (size_t)s->dev.border, FH = z.height + 2 * (size_t)s->dev.border;
+    z.film_bytes = FW * FH * 4 * sizeof(float);
+    z.rgb_bytes = (size_t)z.width * z.height * 3 * sizeof(float);
+    return z;
+}
+
+WfJob make_wf_job(const hk_scene *s, const hk_render_desc &d) {
+    if (d.spp <= 0 || d.depth < 0) throw HkError{HK_ERR_INVALID, "bad job: spp must be > 0 and depth >= 0"};
+    const JobSize z = job_size(s, d);
+    WfJob o;
+    std::memset(&o, 0, sizeof o);
+    std::memcpy(o.cam, s->dev.cam, sizeof o.cam);
+    if (d.use_camera) {
+        const float *M = d.camera_to_world;
+        if (M[15] == 0.0f) throw HkError{HK_ERR_INVALID, "camera_to_world has w = 0"};
+        for (int r = 0; r < 3; r++) {
+            for (int c = 0; c < 3; c++) o.cam[4 * r + c] = M[4 * r + c];
+            o.cam[4 * r + 3] = M[4 * r + 3] / M[15];
+        }
+    }
+    const uint32_t tiles_x = (z.width + kWfTileSide - 1) / kWfTileSide;
+    const uint32_t tiles_y = (z.height + kWfTileSide - 1) / kWfTileSide;
+    o.seed = d.seed;
+    o.spp = (uint32_t)d.spp;
+    o.sample_offset = (uint32_t)d.sample_offset;
+    o.image_index = (uint32_t)d.image_index;
+    o.tiles_x = tiles_x;
+    o.width = z.width;
+    o.height = z.height;
+    o.cam_aspect = float(z.width) / float(z.height);   // PerspectiveCamera::Activate aspect
+    o.depth = d.depth;
+    o.rr_start = d.rr_start;
+    o.work_count = (uint64_t)tiles_x * tiles_y * (uint64_t)d.spp * kWfTilePixels;
+    return o;
+}
+
+}  // namespace hk
+
 extern "C" {
 
-const char *hk_last_error(void) { return g_error.c_str(); }
+const char *hk_last_error(void) { return hk::g_error.c_str(); }
 int hk_version(void) { return 1; }
 
 int hk_scene_create(hk_scene **out) {
@@ -808,6 +790,7 @@ int hk_render(hk_scene *s, const hk_render_desc *d, float *film, unsigned long l
         require_built(s);
         if (!d || !film) throw HkError{HK_ERR_INVALID, "bad arguments"};
         if (d->spp <= 0 || d->depth < 0) throw HkError{HK_ERR_INVALID, "spp must be > 0 and depth >= 0"};
+        require_scene_size(s, *d);
         cudaStream_t st = (cudaStream_t)stream;
         hk::RenderLaunch P;
         std::memset(&P, 0, sizeof P);
@@ -891,6 +874,7 @@ int hk_render_image_static(hk_scene *s, const hk_render_desc *d, float *rgb_dev,
         require_built(s);
         if (!d || !rgb_dev) throw HkError{HK_ERR_INVALID, "bad arguments"};
         if (d->spp <= 0 || d->depth < 0) throw HkError{HK_ERR_INVALID, "spp must be > 0 and depth >= 0"};
+        require_scene_size(s, *d);
         const size_t FW = s->width + 2 * s->dev.border, FH = s->height + 2 * s->dev.border;
         const size_t film_floats = FW * FH * 4;
         if (film_floats > hk::kStaticFilmFloats)
@@ -956,134 +940,51 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         if (!jobs || njobs <= 0 || njobs > hk::kWfMaxJobs) throw HkError{HK_ERR_INVALID, "need 1..1024 jobs"};
         hk_wavefront_config c{};
         if (cfg) c = *cfg;
-        int capacity = c.capacity > 0 ? c.capacity : (1 << 21);
-        capacity = std::max(1024, std::min(capacity, 1 << 26));
-        wf_ensure(s, capacity);
-        auto &E = *s->wf;
-        hk::WfState W = E.W;
-        W.njobs = njobs;
-        // job table
-        std::vector<hk::WfJob> J(njobs);
-        const int tiles_x = ((int)s->width + hk::kWfTileSide - 1) / hk::kWfTileSide;
-        const int tiles_y = ((int)s->height + hk::kWfTileSide - 1) / hk::kWfTileSide;
+        hk::WfEngineConfig ec;
+        ec.capacity = std::max(1024, std::min(c.capacity > 0 ? c.capacity : (1 << 21), 1 << 26));
+        ec.threads_extend = c.threads_extend > 0 ? c.threads_extend : 128;
+        ec.threads_shade = c.threads_shade > 0 ? c.threads_shade : 128;
+        hk::WfEngine &E = wf_ensure(s, ec);
+        cudaStream_t user = (cudaStream_t)stream, st = E.stream();
+        // order after the caller's stream (the films may have been cleared there)
+        cudaEvent_t ev;
+        HK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        struct EvGuard {
+            cudaEvent_t e;
+            ~EvGuard() { cudaEventDestroy(e); }
+        } guard{ev};
+        HK_CUDA(cudaEventRecord(ev, user));
+        HK_CUDA(cudaStreamWaitEvent(st, ev, 0));
+        std::vector<hk::WfSeg> plan(njobs);
         uint64_t total = 0;
+        E.reset();
         for (int j = 0; j < njobs; ++j) {
-            const hk_render_job &in = jobs[j];
-            const hk_render_desc &d = in.desc;
-            if (!in.film_dev || d.spp <= 0 || d.depth < 0) throw HkError{HK_ERR_INVALID, "bad job"};
-            hk::WfJob &o = J[j];
-            std::memset(&o, 0, sizeof o);
-            o.film = in.film_dev;
-            std::memcpy(o.cam, s->dev.cam, sizeof o.cam);
-            if (d.use_camera) {
-                const float *M = d.camera_to_world;
-                if (M[15] == 0.0f) throw HkError{HK_ERR_INVALID, "camera_to_world has w = 0"};
-                for (int r = 0; r < 3; r++) {
-                    for (int cc = 0; cc < 3; cc++) o.cam[4 * r + cc] = M[4 * r + cc];
-                    o.cam[4 * r + 3] = M[4 * r + 3] / M[15];
-                }
-            }
-            o.finished = E.finished.as<unsigned long long>() + j;
-            o.seed = d.seed;
-            o.spp = (uint32_t)d.spp;
-            o.sample_offset = (uint32_t)d.sample_offset;
-            o.image_index = (uint32_t)d.image_index;
-            o.tiles_x = (uint32_t)tiles_x;
-            o.depth = d.depth;
-            o.rr_start = d.rr_start;
-            o.work_begin = total;
-            o.work_count = (uint64_t)tiles_x * tiles_y * d.spp * hk::kWfTilePixels;
-            total += o.work_count;
+            if (!jobs[j].film_dev) throw HkError{HK_ERR_INVALID, "bad job: null film"};
+            hk::WfJob J = hk::make_wf_job(s, jobs[j].desc);
+            J.film = jobs[j].film_dev;
+            E.set_job(j, J);
+            plan[j] = hk::WfSeg{total, 0, j, 0};
+            total += J.work_count;
         }
-        cudaStream_t user = (cudaStream_t)stream, st = E.stream;
-        // order after the caller's stream
-        HK_CUDA(cudaEventRecord(E.ev, user));
-        HK_CUDA(cudaStreamWaitEvent(st, E.ev, 0));
-        HK_CUDA(cudaMemcpyAsync(E.jobs.p, J.data(), sizeof(hk::WfJob) * njobs, cudaMemcpyHostToDevice, st));
-        HK_CUDA(cudaMemsetAsync(E.finished.p, 0, sizeof(unsigned long long) * njobs, st));
-        hk::WfCounters init{};
-        init.total_work = total;
-        HK_CUDA(cudaMemcpyAsync(E.counters.p, &init, sizeof init, cudaMemcpyHostToDevice, st));
-        // launch configuration: persistent grids, one wave of resident blocks
-        hk::WfLaunchConfig L;
-        L.threads_extend = c.threads_extend > 0 ? c.threads_extend : 128;
-        L.threads_shade = c.threads_shade > 0 ? c.threads_shade : 128;
-        for (int t : {L.threads_extend, L.threads_shade})
-            if (t % 32 != 0 || t > 256) throw HkError{HK_ERR_INVALID, "wavefront block sizes must be multiples of 32 up to 256"};
-        L.threads_shadow = L.threads_extend;
-        L.threads_regen = 256;
-        auto grid = [&](int which, int threads, int mult) {
-            int occ = std::max(1, hk::wf_occupancy(which, threads));
-            return std::max(1, s->sm_count * occ * mult);
-        };
-        L.blocks_extend = grid(0, L.threads_extend, 1);
-        L.blocks_shade = grid(1, L.threads_shade, 1);
-        L.blocks_shadow = grid(2, L.threads_shadow, 1);
-        L.blocks_regen = grid(3, L.threads_regen, 1);
-        HK_CUDA(hk::wf_launch_init(s->dev, W, L, st));
-        // capture two iterations (extend queue 0, then 1) in a graph and replay it
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
+        E.set_plan(plan, total);
         const bool profile = c.kernel_ms != nullptr;
         const bool use_graph = c.no_graph == 0 && !profile;
-        cudaEvent_t pe[2] = {nullptr, nullptr};
-        if (profile) {
-            HK_CUDA(cudaEventCreate(&pe[0]));
-            HK_CUDA(cudaEventCreate(&pe[1]));
-        }
-        const int phase_launches[4] = {2, 1, hk::kWfTypes, 1};
-        auto run_iteration = [&](int cur) {
-            if (!profile) {
-                HK_CUDA(hk::wf_launch_iteration(s->dev, W, L, cur, st));
-                return;
-            }
-            for (int ph = 0; ph < 4; ++ph) {
-                HK_CUDA(cudaEventRecord(pe[0], st));
-                HK_CUDA(hk::wf_launch_phase(s->dev, W, L, cur, ph, st));
-                HK_CUDA(cudaEventRecord(pe[1], st));
-                HK_CUDA(cudaEventSynchronize(pe[1]));
-                float ms = 0;
-                HK_CUDA(cudaEventElapsedTime(&ms, pe[0], pe[1]));
-                c.kernel_ms[ph] += ms;
-                if (c.kernel_launches) c.kernel_launches[ph] += phase_launches[ph];
-            }
-        };
-        if (use_graph) {
-            HK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            cudaError_t e0 = hk::wf_launch_iteration(s->dev, W, L, 0, st);
-            cudaError_t e1 = hk::wf_launch_iteration(s->dev, W, L, 1, st);
-            cudaError_t ec = cudaStreamEndCapture(st, &graph);
-            if (e0 != cudaSuccess || e1 != cudaSuccess || ec != cudaSuccess) {
-                if (graph) cudaGraphDestroy(graph);
-                throw HkError{HK_ERR_CUDA, "wavefront graph capture failed"};
-            }
-            HK_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        }
         const int per_check = c.iterations_per_check > 0 ? c.iterations_per_check : 16;
         uint64_t iters = 0;
         const uint64_t max_iters = 1ull << 40;
         for (;;) {
-            for (int k = 0; k < per_check; k += 2) {
-                if (use_graph) HK_CUDA(cudaGraphLaunch(exec, st));
-                else {
-                    run_iteration(0);
-                    run_iteration(1);
-                }
-            }
+            E.run(per_check, use_graph, c.kernel_ms, c.kernel_launches);
             iters += per_check;
-            HK_CUDA(cudaMemcpyAsync(E.host_ctr, E.counters.p, sizeof(hk::WfCounters), cudaMemcpyDeviceToHost, st));
-            HK_CUDA(cudaStreamSynchronize(st));
-            if (E.host_ctr->active == 0 && E.host_ctr->next_work >= E.host_ctr->total_work) break;
+            E.fetch_status();
+            HK_CUDA(cudaEventSynchronize(E.done_event()));
+            const hk::WfCounters &h = E.status();
+            if (h.active == 0 && h.next_work >= h.total_work) break;
             if (iters > max_iters) throw HkError{HK_ERR_CUDA, "wavefront did not terminate"};
         }
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        for (cudaEvent_t e : pe)
-            if (e) cudaEventDestroy(e);
-        if (counters_dev) HK_CUDA(hk::wf_launch_counters_add(W, counters_dev, st));
+        if (counters_dev) E.add_counters(counters_dev);
         // the caller's stream continues after the engine's work
-        HK_CUDA(cudaEventRecord(E.ev, st));
-        HK_CUDA(cudaStreamWaitEvent(user, E.ev, 0));
+        HK_CUDA(cudaEventRecord(ev, st));
+        HK_CUDA(cudaStreamWaitEvent(user, ev, 0));
         return HK_OK;
     });
 }
@@ -1093,28 +994,29 @@ int hk_render_batch_host(hk_scene *s, const hk_render_desc *descs, int n, const 
         require_built(s);
         if (!descs || !rgb_host || n <= 0 || n > hk::kWfMaxJobs) throw HkError{HK_ERR_INVALID, "bad arguments"};
         cudaStream_t st = (cudaStream_t)stream;
-        size_t FW = s->width + 2 * s->dev.border, FH = s->height + 2 * s->dev.border;
-        size_t film_bytes = FW * FH * 4 * sizeof(float), rgb_bytes = (size_t)s->width * s->height * 3 * sizeof(float);
-        while ((int)s->batch_films.size() < n) {
-            s->batch_films.emplace_back(new DevBuf());
-            s->batch_films.back()->alloc(film_bytes);
+        std::vector<hk::JobSize> sz(n);
+        size_t rgb_max = 0;
+        for (int j = 0; j < n; ++j) {
+            sz[j] = hk::job_size(s, descs[j]);
+            rgb_max = std::max(rgb_max, sz[j].rgb_bytes);
         }
-        if (s->b_rgb.bytes < rgb_bytes) s->b_rgb.alloc(rgb_bytes);
+        while ((int)s->batch_films.size() < n) s->batch_films.emplace_back(new DevBuf());
+        if (s->b_rgb.bytes < rgb_max) s->b_rgb.alloc(rgb_max);
         unsigned long long *ctr = (unsigned long long *)s->b_scratch.p + 1;   // 7 slots
         HK_CUDA(cudaMemsetAsync(ctr, 0, 7 * sizeof(unsigned long long), st));
         std::vector<hk_render_job> jobs(n);
         for (int j = 0; j < n; ++j) {
-            if (s->batch_films[j]->bytes < film_bytes) s->batch_films[j]->alloc(film_bytes);
-            HK_CUDA(cudaMemsetAsync(s->batch_films[j]->p, 0, film_bytes, st));
+            if (s->batch_films[j]->bytes < sz[j].film_bytes) s->batch_films[j]->alloc(sz[j].film_bytes);
+            HK_CUDA(cudaMemsetAsync(s->batch_films[j]->p, 0, sz[j].film_bytes, st));
             jobs[j].film_dev = s->batch_films[j]->as<float>();
             jobs[j].desc = descs[j];
         }
         int rc = hk_render_batch(s, jobs.data(), n, cfg, ctr, stream);
         if (rc != HK_OK) return rc;
         for (int j = 0; j < n; ++j) {
-            HK_CUDA(hk::launch_resolve(jobs[j].film_dev, s->b_rgb.as<float>(), (int)s->width, (int)s->height,
+            HK_CUDA(hk::launch_resolve(jobs[j].film_dev, s->b_rgb.as<float>(), (int)sz[j].width, (int)sz[j].height,
                                        s->dev.border, st));
-            HK_CUDA(cudaMemcpyAsync(rgb_host[j], s->b_rgb.p, rgb_bytes, cudaMemcpyDeviceToHost, st));
+            HK_CUDA(cudaMemcpyAsync(rgb_host[j], s->b_rgb.p, sz[j].rgb_bytes, cudaMemcpyDeviceToHost, st));
         }
         if (counters_host)
             HK_CUDA(cudaMemcpyAsync(counters_host, ctr, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));

@@ -56,9 +56,12 @@ __device__ __forceinline__ void red_add_v4(float4 *addr, float a, float b, float
 }
 __device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
 
-__device__ __forceinline__ Ray camera_ray_cam(const DevScene &S, const float *M, float px, float py) {
-    float u = px * (1.0f / (float)S.width), v = py * (1.0f / (float)S.height);
-    V3 np = v3(S.cam_near * (1.0f - 2.0f * u) / S.cam_cot, S.cam_near * (1.0f - 2.0f * v) / (S.cam_aspect * S.cam_cot),
+// PerspectiveCamera::SampleRay (src/camera/PerspectiveCamera.cpp:71) at the
+// job's resolution and pose; field of view and clip planes are the scene's.
+__device__ __forceinline__ Ray camera_ray_job(const DevScene &S, const WfJob &J, float px, float py) {
+    const float *M = J.cam;
+    float u = px * (1.0f / (float)J.width), v = py * (1.0f / (float)J.height);
+    V3 np = v3(S.cam_near * (1.0f - 2.0f * u) / S.cam_cot, S.cam_near * (1.0f - 2.0f * v) / (J.cam_aspect * S.cam_cot),
                S.cam_near);
     V3 dir = normalize(np);
     float invz = 1.0f / dir.z;
@@ -78,18 +81,20 @@ __device__ __forceinline__ uint64_t wf_mix_seed(uint64_t seed, uint64_t s) {
     return z ^ (z >> 31);
 }
 
-__device__ __forceinline__ int find_job(const WfState &W, uint64_t w) {
-    int lo = 0, hi = W.njobs - 1;
+// Piece of the current plan that holds plan item w (pieces are sorted by plan_begin).
+__device__ __forceinline__ int find_seg(const WfState &W, uint64_t w, int nseg) {
+    int lo = 0, hi = nseg - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (W.jobs[mid].work_begin <= w) lo = mid; else hi = mid - 1;
+        if (W.segs[mid].plan_begin <= w) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
 
 // ImageBlock::Put into the job's global film with vector reductions.
-__device__ __forceinline__ void splat_global(const DevScene &S, float *film, float px, float py, V3 val) {
-    const int B = S.border, FW = (int)S.width + 2 * B, FH = (int)S.height + 2 * B;
+__device__ __forceinline__ void splat_global(const DevScene &S, const WfJob &J, float px, float py, V3 val) {
+    const int B = S.border, FW = (int)J.width + 2 * B, FH = (int)J.height + 2 * B;
+    float *film = J.film;
     float cx = px - 0.5f - (0 - B), cy = py - 0.5f - (0 - B);
     int x0 = max((int)ceilf(cx - S.filt_radius), 0), y0 = max((int)ceilf(cy - S.filt_radius), 0);
     int x1 = min((int)floorf(cx + S.filt_radius), FW - 1), y1 = min((int)floorf(cy + S.filt_radius), FH - 1);
@@ -106,25 +111,33 @@ __device__ __forceinline__ void splat_global(const DevScene &S, float *film, flo
 }
 
 // ------------------------------------------------------------ regen
-// Finish the paths of the finished queue (or, with init, every slot) and
-// start new ones from the work dispenser.
-__global__ void wf_regen_kernel(DevScene S, WfState W, int cur, int init) {
-    const int n = init ? W.capacity : (int)W.ctr->fq_count;
+// Splat and retire the finished paths, then give every finished or idle slot
+// new work from the dispatch plan; slots that find none wait in the next idle
+// list.  Queues read here: fq, idle[cur]; written: eq[cur], idle[cur ^ 1].
+__global__ void wf_regen_kernel(DevScene S, WfState W, int cur) {
+    const int nf = (int)W.ctr->fq_count;
+    const int n = nf + (int)W.ctr->idle_count[cur];
+    const uint64_t total = W.ctr->total_work;
+    const int nseg = (int)W.ctr->seg_count;
     unsigned long long dropped = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = init ? i : W.fq[i];
-        if (!init) {
+        int slot;
+        if (i < nf) {
+            slot = W.fq[i];
             float4 p = W.pix[slot];
             float4 L = W.lacc[slot];
             const WfJob &J = W.jobs[__float_as_int(p.z)];
             V3 val = v3(L.x, L.y, L.z);
-            if (is_valid(val)) splat_global(S, J.film, p.x, p.y, val);
+            if (is_valid(val)) splat_global(S, J, p.x, p.y, val);
             else ++dropped;
             atomicAdd(J.finished, 1ull);
             atomicSub(&W.ctr->active, 1u);
+        } else {
+            slot = W.idle[cur][i - nf];
         }
-        // claim work until a pixel inside the image or the dispenser runs dry
-        for (;;) {
+        // claim plan items until a pixel inside its image or the plan runs dry
+        bool started = false;
+        while (W.ctr->next_work < total) {
             unsigned mask = __activemask();
             int leader = __ffs(mask) - 1;
             unsigned rank = __popc(mask & ((1u << lane_id()) - 1u));
@@ -132,25 +145,26 @@ __global__ void wf_regen_kernel(DevScene S, WfState W, int cur, int init) {
             if ((int)lane_id() == leader) base = atomicAdd(&W.ctr->next_work, (unsigned long long)__popc(mask));
             base = __shfl_sync(mask, base, leader);
             const uint64_t w = base + rank;
-            if (w >= W.ctr->total_work) break;
-            const int j = find_job(W, w);
+            if (w >= total) break;
+            const WfSeg &G = W.segs[find_seg(W, w, nseg)];
+            const int j = G.job;
             const WfJob &J = W.jobs[j];
-            const uint64_t l = w - J.work_begin;
+            const uint64_t l = G.job_begin + (w - G.plan_begin);
             const uint32_t p = (uint32_t)(l % kWfTilePixels);
             const uint64_t ts = l / kWfTilePixels;
             const uint32_t s = (uint32_t)(ts % J.spp);
             const uint32_t t = (uint32_t)(ts / J.spp);
             const uint32_t x = (t % J.tiles_x) * kWfTileSide + p % kWfTileSide;
             const uint32_t y = (t / J.tiles_x) * kWfTileSide + p / kWfTileSide;
-            if (x >= S.width || y >= S.height) {
+            if (x >= J.width || y >= J.height) {
                 atomicAdd(J.finished, 1ull);   // counted as work done: no path
                 continue;
             }
             Pcg32 rng;
             rng.seed(wf_mix_seed(J.seed, (uint64_t)J.sample_offset + s),
-                     (uint64_t)y * S.width + x + (uint64_t)J.image_index * S.width * S.height);
+                     (uint64_t)y * J.width + x + (uint64_t)J.image_index * J.width * J.height);
             float px = (float)x + rng.nextf(), py = (float)y + rng.nextf();
-            Ray r = camera_ray_cam(S, J.cam, px, py);
+            Ray r = camera_ray_job(S, J, px, py);
             W.ray_o[slot] = f4(r.o, r.tmin);
             W.ray_d[slot] = f4(r.d, r.tmax);
             W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
@@ -160,20 +174,39 @@ __global__ void wf_regen_kernel(DevScene S, WfState W, int cur, int init) {
                                      (uint32_t)(rng.inc >> 32));
             W.eq[cur][warp_append(&W.ctr->eq_count[cur])] = slot;
             atomicAdd(&W.ctr->active, 1u);
+            started = true;
             break;
         }
+        if (!started) W.idle[cur ^ 1][warp_append(&W.ctr->idle_count[cur ^ 1])] = slot;
     }
     if (dropped) atomicAdd(&W.ctr->dropped, dropped);
 }
 
-// Reset the counters of the queues the next phases fill.
+// Reset the counters of the queues consumed by regen and of those the next
+// phases fill.
 __global__ void wf_reset_kernel(WfState W, int cur) {
     if (threadIdx.x == 0) {
         W.ctr->fq_count = 0;
+        W.ctr->idle_count[cur] = 0;
         W.ctr->eq_count[cur ^ 1] = 0;
         W.ctr->shadow_count = 0;
     }
     if (threadIdx.x < kWfTypes) W.ctr->sq_count[threadIdx.x] = 0;
+}
+
+// Empty pool: every slot in idle list 0, all queues and statistics zero.
+__global__ void wf_init_kernel(WfState W) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < W.capacity; i += gridDim.x * blockDim.x) W.idle[0][i] = i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        WfCounters *c = W.ctr;
+        c->eq_count[0] = c->eq_count[1] = 0;
+        c->idle_count[0] = (unsigned)W.capacity;
+        c->idle_count[1] = 0;
+        for (int t = 0; t < kWfTypes; ++t) c->sq_count[t] = 0;
+        c->fq_count = c->shadow_count = c->active = 0;
+        c->rays = c->shadow_rays = c->dropped = 0;
+        c->node_visits = c->tri_tests = c->node_visits_shadow = c->tri_tests_shadow = 0;
+    }
 }
 
 // ------------------------------------------------------------ extend
@@ -393,14 +426,14 @@ cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cu
     return cudaGetLastError();
 }
 
-cudaError_t wf_launch_init(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
-    wf_regen_kernel<<<(W.capacity + C.threads_regen - 1) / C.threads_regen, C.threads_regen, 0, st>>>(S, W, 0, 1);
+cudaError_t wf_launch_init(const WfState &W, cudaStream_t st) {
+    wf_init_kernel<<<(W.capacity + 255) / 256, 256, 0, st>>>(W);
     return cudaGetLastError();
 }
 
 cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
     const int nxt = cur ^ 1;
-    wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur, 0);
+    wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur);
     wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
     wf_extend_kernel<<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur);
     wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
@@ -418,7 +451,7 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
     const int nxt = cur ^ 1;
     switch (phase) {
     case 0:
-        wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur, 0);
+        wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur);
         wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
         break;
     case 1: wf_extend_kernel<<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur); break;

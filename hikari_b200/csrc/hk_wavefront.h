@@ -2,12 +2,13 @@
 // host driver in hk_host.cpp.
 //
 // A pool of `capacity` path slots lives in HBM as structure-of-arrays.  One
-// iteration runs: regen (splat finished paths, claim new work, generate camera
-// rays) -> extend (closest hit of every queued ray, classify by material) ->
-// shade<material> (emission, MIS, next-event shadow rays, BSDF sampling,
-// Russian roulette) -> shadow (any-hit, add unoccluded next-event terms).
-// Kernels use fixed persistent grids and read queue sizes from HBM, so an
-// iteration can be captured once in a CUDA graph and replayed.
+// iteration runs: regen (splat finished paths, claim new work for finished and
+// idle slots, generate camera rays) -> extend (closest hit of every queued ray,
+// classify by material) -> shade<material> (emission, MIS, next-event shadow
+// rays, BSDF sampling, Russian roulette) -> shadow (any-hit, add unoccluded
+// next-event terms).  Kernels use fixed persistent grids and read queue sizes
+// and the dispatch plan from HBM, so iterations are captured once in a CUDA
+// graph and replayed; jobs and plans change between replays.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -18,31 +19,51 @@
 namespace hk {
 
 constexpr int kWfTypes = 6;        // 0: miss, 1..5: BSDF type + 1 of the hit
-constexpr int kWfMaxJobs = 1024;
+constexpr int kWfMaxJobs = 1024;   // job table entries of one engine
+constexpr int kWfMaxSegs = 4096;   // pieces of one dispatch plan
 constexpr int kWfTileSide = 16;
 constexpr int kWfTilePixels = kWfTileSide * kWfTileSide;
 
-// One image being rendered (a job): a view of the scene with its own film.
+// One image being rendered (a job): a view of the scene with its own film and
+// resolution.  Jobs live in a table of kWfMaxJobs entries; a path records the
+// index of its job.
 struct WfJob {
-    float *film;                    // (H+2B) x (W+2B) x 4, 16-byte aligned
+    float *film;                    // (height+2B) x (width+2B) x 4, 16-byte aligned
     float cam[12];                  // camera-to-world rows (translation divided by w)
-    unsigned long long *finished;   // paths of this job finished (device counter)
+    unsigned long long *finished;   // work items of this job finished (device counter)
     uint64_t seed;
-    uint64_t work_begin, work_count;   // global work range: tiles * spp * 256
+    uint64_t work_count;            // tiles * spp * 256 work items
     uint32_t spp, sample_offset, image_index, tiles_x;
+    uint32_t width, height;
+    float cam_aspect;               // width / height (PerspectiveCamera::Activate)
     int32_t depth, rr_start;
+    int32_t pad;
 };
 
-// Device-wide counters of the engine (one struct in HBM).
+// One piece of the dispatch plan: work items [plan_begin, next piece's
+// plan_begin) of the plan are the job's items starting at job_begin.  The host
+// writes a plan between chunks of iterations; slots claim plan items in order.
+struct WfSeg {
+    uint64_t plan_begin;
+    uint64_t job_begin;
+    int32_t job;
+    int32_t pad;
+};
+
+// Device-wide counters of the engine (one struct in HBM).  The first three
+// fields are the dispatch head, rewritten by the host with each plan.
 struct WfCounters {
-    unsigned long long next_work;      // global work dispenser
-    unsigned long long total_work;     // end of the dispensed range
+    unsigned long long next_work;      // next plan item to hand out
+    unsigned long long total_work;     // plan items in the current plan
+    unsigned int seg_count;            // pieces in the current plan
+    unsigned int pad0;
     unsigned int eq_count[2];          // extend queues (ping-pong)
+    unsigned int idle_count[2];        // slots without a path (ping-pong)
     unsigned int sq_count[kWfTypes];   // shade queues per material type
     unsigned int fq_count;             // finished paths awaiting splat + regeneration
     unsigned int shadow_count;         // next-event shadow rays
     unsigned int active;               // paths in flight
-    unsigned int pad;
+    unsigned int pad1;
     unsigned long long rays, shadow_rays, dropped;
     unsigned long long node_visits, tri_tests;                 // closest-hit traversal (extend)
     unsigned long long node_visits_shadow, tri_tests_shadow;   // any-hit traversal (shadow)
@@ -63,6 +84,7 @@ struct WfState {
     float4 *hit;        // t, u, v, bits(tri in leaf order or -1)
     // queues
     int *eq[2];
+    int *idle[2];
     int *sq[kWfTypes];
     int *fq;
     float4 *sh_o;       // shadow origin.xyz, bits(slot)
@@ -70,7 +92,7 @@ struct WfState {
     float4 *sh_c;       // contribution.xyz, -
     WfCounters *ctr;
     const WfJob *jobs;
-    int njobs;
+    const WfSeg *segs;
 };
 
 // flags in the high half of pix.w
@@ -83,7 +105,8 @@ struct WfLaunchConfig {
     int blocks_regen, threads_regen;
 };
 
-cudaError_t wf_launch_init(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st);
+// empty pool: every slot idle, queues and statistics zero (the dispatch head is the host's)
+cudaError_t wf_launch_init(const WfState &W, cudaStream_t st);
 // one iteration with extend queue `cur` (0/1)
 cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st);
 // one phase of an iteration: 0 regen + reset, 1 extend, 2 shade (all materials), 3 shadow

@@ -124,6 +124,8 @@ typedef struct {
     int32_t spp_per_item;   /* 0 = automatic work split */
     int32_t use_camera;     /* 1: render from camera_to_world instead of the scene camera */
     float camera_to_world[16];
+    int32_t width, height;  /* image size; 0 = the scene camera's (wavefront and serving only:
+                               hk_render rejects any other size) */
 } hk_render_desc;
 
 /* Accumulate spp samples per pixel into film_dev ((H+2B)*(W+2B)*4 floats of
@@ -197,6 +199,78 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
  * rgb_dev: H*W*3 floats; counters_dev (optional): 5 x u64 as hk_render. */
 int hk_render_image_static(hk_scene *s, const hk_render_desc *desc, float *rgb_dev, unsigned long long *counters_dev,
                            void *stream);
+
+/* ---- serving: continuous batching of render jobs ---- */
+/* No counterpart in the reference (its renderer runs one scene file per
+ * process, src/Main.cpp:150).  A server keeps registered scenes resident and
+ * renders jobs -- (scene, image size, spp, camera) -- as they arrive: a job
+ * is admitted when its film and image fit the device-memory budget (the
+ * first job of a scene also charges the scene's path-slot pool), its paths
+ * join the scene's wavefront pool between iterations, and its image is
+ * copied to the caller's host buffer when its last path is done.  Jobs of
+ * one scene share one pool; scenes run on separate streams.  A job's image
+ * is the same whether it runs alone or among others: each path's random
+ * stream depends only on (seed, sample, pixel, image_index), so results
+ * differ only in the order of the film's float additions.  One host thread
+ * per server drives the device; the functions below are thread-safe. */
+typedef struct hk_server hk_server;
+
+#define HK_ERR_TIMEOUT (-5)   /* hk_job_wait: the job did not finish in time */
+
+#define HK_SERVE_SRPT 0   /* dispatch the job with the least undispensed work first */
+#define HK_SERVE_FIFO 1   /* dispatch jobs in arrival order */
+
+#define HK_JOB_QUEUED 0
+#define HK_JOB_RUNNING 1
+#define HK_JOB_DONE 2
+#define HK_JOB_CANCELLED 3
+#define HK_JOB_FAILED 4      /* the server hit a device error; hk_job_wait returns it */
+
+typedef struct {
+    int32_t capacity;             /* path slots of each scene's pool (0 = 2^20) */
+    int32_t threads_extend;       /* 0 = 128 */
+    int32_t threads_shade;        /* 0 = 128 */
+    int32_t iterations_per_poll;  /* wavefront iterations between host polls (0 = 4) */
+    int32_t policy;               /* HK_SERVE_SRPT or HK_SERVE_FIFO */
+    int32_t max_jobs;             /* jobs admitted at once per scene (0 = 256, max 1024) */
+    uint64_t hbm_budget;          /* device bytes for pools, films and images (0 = 90% of free at create) */
+} hk_server_config;
+
+typedef struct {
+    int32_t state;                /* HK_JOB_* */
+    int32_t scene;
+    uint32_t width, height;
+    uint64_t paths;               /* width * height * spp */
+    uint64_t device_bytes;        /* film + image charged while admitted */
+    double submit_s, admit_s, done_s;   /* server clock (seconds since hk_server_create) */
+    double latency_s;             /* done_s - submit_s (0 until done) */
+} hk_job_status;
+
+typedef struct {
+    uint64_t jobs_submitted, jobs_done, jobs_cancelled, jobs_queued, jobs_running;
+    uint64_t paths_done;          /* paths of finished jobs */
+    uint64_t rays, shadow_rays;   /* traced by all pools */
+    uint64_t bytes_in_use, hbm_budget;
+    double busy_s;                /* time with at least one job admitted */
+    double now_s;
+} hk_server_stats;
+
+int hk_server_create(const hk_server_config *cfg, hk_server **out);
+/* Cancels queued jobs, finishes the running ones and frees everything. */
+int hk_server_destroy(hk_server *srv);
+/* Register a built scene (not owned; keep it alive and unchanged while the server lives). */
+int hk_server_add_scene(hk_server *srv, hk_scene *scene, int32_t *scene_id);
+/* Queue a job.  rgb_host receives height*width*3 floats (pinned memory is
+ * copied into directly, other memory through a pinned staging buffer); it
+ * must stay valid until the job is done or cancelled. */
+int hk_job_submit(hk_server *srv, int32_t scene_id, const hk_render_desc *desc, float *rgb_host, uint64_t *job_id);
+int hk_job_poll(hk_server *srv, uint64_t job_id, hk_job_status *status);
+/* Block until the job is done or cancelled, or timeout_s passes (HK_ERR_TIMEOUT). */
+int hk_job_wait(hk_server *srv, uint64_t job_id, double timeout_s, hk_job_status *status);
+/* A queued job is dropped; a running job stops dispatching and ends when its
+ * paths in flight are done (its image is not written). */
+int hk_job_cancel(hk_server *srv, uint64_t job_id);
+int hk_server_get_stats(hk_server *srv, hk_server_stats *stats);
 
 /* ---- record-level entry points (parity tests and the BSDF batch) ---- */
 /* Ray queries against the scene accel (Acceleration::RayIntersect,

@@ -1,0 +1,131 @@
+"""The C-ABI library on a machine without a GPU: it builds for sm_100a, loads,
+exports every function include/hikari_b200.h declares, and its host-only
+parts (the XML plugin layer, EXR I/O, argument checks) work without a device."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import hikari_b200 as hk
+from hikari_b200 import build as hkbuild
+from hikari_b200.scenedesc import parse_xml
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "hikari_b200.h")
+
+
+@pytest.fixture(scope="module")
+def L():
+    hkbuild.build()
+    return hk.lib()
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(hk_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_header_declares_the_boundary():
+    names = declared_functions()
+    for must in ["hk_scene_create", "hk_scene_build", "hk_render", "hk_render_batch", "hk_render_image_static",
+                 "hk_trace", "hk_bsdf_batch", "hk_server_create", "hk_job_submit", "hk_job_poll", "hk_job_cancel",
+                 "hk_wavefront_autotune", "hk_scene_load_xml", "hk_exr_read"]:
+        assert must in names
+    assert len(names) >= 35
+
+
+def test_library_exports_every_declared_function(L):
+    so = C.CDLL(hkbuild.LIB)
+    missing = [n for n in declared_functions() if not hasattr(so, n)]
+    assert not missing, f"not exported: {missing}"
+
+
+def test_build_targets_sm100a():
+    assert "arch=compute_100a,code=sm_100a" in " ".join(hkbuild.ARCH)
+    assert "-fmad=false" in hkbuild.NVCC_FLAGS
+
+
+SCENE_XML = """<?xml version="1.0"?>
+<scene>
+  <integrator type="pathMIS"><integer name="depth" value="12"/></integrator>
+  <sampler type="independent"><integer name="sampleCount" value="9"/></sampler>
+  <camera type="perspective">
+    <transform name="toWorld"><lookat origin="0, 1, 4" target="0, 0.5, 0" up="0, 1, 0"/></transform>
+    <float name="fov" value="35"/>
+    <integer name="width" value="40"/><integer name="height" value="30"/>
+  </camera>
+  <mesh type="obj">
+    <string name="filename" value="quad.obj"/>
+    <bsdf type="roughPlastic"><float name="alpha" value="0.2"/><color name="kd" value="0.4, 0.5, 0.6"/></bsdf>
+  </mesh>
+  <mesh type="obj">
+    <string name="filename" value="quad.obj"/>
+    <transform name="toWorld"><translate value="0, 3, 0"/></transform>
+    <bsdf type="diffuse"/>
+    <emitter type="area"><color name="radiance" value="5, 5, 5"/></emitter>
+  </mesh>
+  <mesh type="obj">
+    <string name="filename" value="quad.obj"/>
+    <transform name="toWorld"><translate value="0, -1, 0"/></transform>
+    <bsdf type="roughCoating">
+      <float name="alpha" value="0.2"/>
+      <bsdf type="roughConductor"><float name="alpha" value="0.3"/></bsdf>
+    </bsdf>
+  </mesh>
+</scene>
+"""
+QUAD_OBJ = "v -1 0 -1\nv 1 0 -1\nv 1 0 1\nv -1 0 1\nf 1 4 3 2\n"
+
+
+def test_xml_plugin_layer_matches_python_parser(L, tmp_path):
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "scene.xml")
+    open(path, "w").write(SCENE_XML)
+    info, depth, spp = hk.parse_xml_info(path)
+    sd = parse_xml(path)[0]
+    assert (depth, spp) == (12, 9) == (sd.depth, sd.spp)
+    assert info.n_meshes == len(sd.meshes) == 3
+    assert info.n_triangles == sum(len(m.indices) for m in sd.meshes) == 6
+    assert info.n_emitters == 1
+    assert info.n_bsdfs == 4          # plastic, diffuse, coating + its nested conductor
+
+
+def test_xml_errors_are_reported(L, tmp_path):
+    bad = tmp_path / "bad.xml"
+    bad.write_text('<scene><bsdf type="noSuchBSDF"/></scene>')
+    with pytest.raises(hk.HikariError):
+        hk.parse_xml_info(str(bad))
+    with pytest.raises(hk.HikariError):
+        hk.parse_xml_info(str(tmp_path / "missing.xml"))
+
+
+def test_exr_roundtrip(L, tmp_path):
+    rng = np.random.default_rng(0)
+    img = rng.uniform(0, 100, (7, 13, 3)).astype(np.float32)
+    img[0, 0] = [0.0, 1e-30, 3.4e38]
+    p = str(tmp_path / "x.exr")
+    hk.exr_write(p, img)
+    back = hk.exr_read(p)
+    assert back.shape == img.shape
+    assert np.array_equal(back, img)
+
+
+def test_argument_checks_without_device(L):
+    h = C.c_void_p()
+    assert L.hk_scene_create(C.byref(h)) == 0
+    try:
+        assert L.hk_scene_build(h) == -1                       # no meshes
+        assert b"no meshes" in L.hk_last_error()
+        d = hk.BsdfDesc()
+        d.type = 7
+        assert L.hk_scene_add_bsdf(h, C.byref(d), None) == -1  # unknown BSDF type
+        d.type = 4
+        d.nested = 3
+        assert L.hk_scene_add_bsdf(h, C.byref(d), None) == -1  # coating without a nested BSDF
+        assert b"nested" in L.hk_last_error()
+        assert L.hk_render(h, None, None, None, None) == -1    # not built
+    finally:
+        L.hk_scene_destroy(h)
