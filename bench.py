@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="heterogeneous",
                     choices=["heterogeneous", "mesh_heavy", "cornell", "serving"])
+    ap.add_argument("--accel", default="bvh8", choices=["bvh8", "bvh2"],
+                    help="tree the kernels traverse: compressed 8-wide (80-byte nodes) or binary (64-byte nodes)")
     ap.add_argument("--jobs", type=int, default=40, help="serving: jobs of the Poisson run")
     ap.add_argument("--load", type=float, default=0.8, help="serving: arrival rate as a fraction of the peak")
     ap.add_argument("--spp", type=int, default=0)
@@ -319,6 +321,9 @@ def main():
     t0 = time.perf_counter()
     gs = hk.Scene.from_desc(sd)
     build_s = time.perf_counter() - t0
+    gs.set_accel(hk.ACCEL_BVH8 if args.accel == "bvh8" else hk.ACCEL_BVH2)
+    accel_name = args.accel
+    node_b = 80.0 if args.accel == "bvh8" else 64.0
     W, H, spp, depth = sd.camera.width, sd.camera.height, sd.spp, sd.depth
     V = len(cams)
     shape = gs.film_shape()
@@ -383,12 +388,13 @@ def main():
         pcn = pc.cpu().numpy().astype(np.float64)
         phases = ["regen", "extend", "shade", "shadow"]
         dom = int(np.argmax(kms))
-        trav_bytes = {1: pcn[3] * 64.0 + pcn[4] * 48.0, 3: pcn[5] * 64.0 + pcn[6] * 48.0}
+        trav_bytes = {1: pcn[3] * node_b + pcn[4] * 48.0, 3: pcn[5] * node_b + pcn[6] * 48.0}
         if dom in trav_bytes:
             bytes_per_launch = trav_bytes[dom] / max(1, kl[dom])
             avg_s = float(kms[dom]) / max(1, kl[dom]) / 1e3
-            basis = (f"{phases[dom]} kernel: BVH fetch bytes (64 B per node visit + 48 B per triangle test, counted "
-                     f"in the kernel) per launch / mean launch time over {int(kl[dom])} launches of a profiled step")
+            basis = (f"{phases[dom]} kernel: BVH fetch bytes ({int(node_b)} B per {accel_name} node visit + 48 B per "
+                     f"triangle test, counted in the kernel) per launch / mean launch time over {int(kl[dom])} launches "
+                     f"of a profiled step")
         else:
             # shading: path-state bytes read + written per path vertex (~144 B) as the algorithmic unit
             bytes_per_launch = (pcn[0] * 144.0) / max(1, kl[dom])
@@ -399,9 +405,10 @@ def main():
         phase_share = {p: round(float(kms[i] / kms.sum()), 4) for i, p in enumerate(phases)}
     else:
         n_launch = args.steps * V
-        bytes_per_launch = (ctr[3] * 64.0 + ctr[4] * 48.0) / n_launch
+        bytes_per_launch = (ctr[3] * node_b + ctr[4] * 48.0) / n_launch
         achieved = bytes_per_launch / (total_max / n_launch) / 1e9
-        basis = "render megakernel: BVH fetch bytes (64 B per node visit + 48 B per triangle test) / mean kernel time"
+        basis = (f"render megakernel: BVH fetch bytes ({int(node_b)} B per {accel_name} node visit + 48 B per triangle "
+                 f"test) / mean kernel time")
         launches_per_step = V
         phase_share = None
 
@@ -467,7 +474,9 @@ def main():
         "dtype": "f32",
         "data": "synthetic (seeded procedural scene)",
         "config": {"workload": desc, "form": args.form, "parallelism": f"replicas x{world}",
-                   "triangles": int(gs.info.n_triangles), "bvh_nodes": int(gs.info.n_bvh_nodes),
+                   "triangles": int(gs.info.n_triangles), "accel": args.accel,
+                   "bvh_nodes": int(gs.info.n_bvh_nodes), "wide_nodes": int(gs.info.n_wide_nodes),
+                   "wide_depth": int(gs.info.wide_depth),
                    "scene_build_s": round(build_s, 2), "wavefront": tuned or None,
                    "autotune_probe_ms": tune_ms,
                    "l2": "256 MiB buffer written between timed steps (outside the step events)",

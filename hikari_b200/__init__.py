@@ -21,6 +21,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libhikari_b200.so")
 DATA_DIR = os.path.join(HERE, "data")
 
 HK_OK = 0
+ACCEL_BVH2, ACCEL_BVH8 = 0, 1
 
 
 class HikariError(RuntimeError):
@@ -40,7 +41,8 @@ class SceneInfo(C.Structure):
     _fields_ = [
         ("n_meshes", C.c_uint32), ("n_triangles", C.c_uint32), ("n_bsdfs", C.c_uint32), ("n_emitters", C.c_uint32),
         ("n_bvh_nodes", C.c_uint32), ("bvh_depth", C.c_uint32), ("env_index", C.c_int32), ("film_border", C.c_int32),
-        ("bbox", C.c_float * 6), ("device_bytes", C.c_uint64),
+        ("bbox", C.c_float * 6), ("device_bytes", C.c_uint64), ("n_wide_nodes", C.c_uint32),
+        ("wide_depth", C.c_uint32), ("accel", C.c_int32), ("postpone", C.c_int32),
     ]
 
 
@@ -116,6 +118,9 @@ def lib():
         "hk_scene_set_filter": ([P, C.c_int, F, F, F], C.c_int),
         "hk_scene_set_background": ([P, P, C.c_int], C.c_int),
         "hk_scene_build": ([P], C.c_int),
+        "hk_scene_set_accel": ([P, I32], C.c_int),
+        "hk_bvh_check": ([P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
+                         C.c_int),
         "hk_scene_get_info": ([P, C.POINTER(SceneInfo)], C.c_int),
         "hk_scene_load_xml": ([C.c_char_p, C.c_char_p, C.POINTER(P), C.POINTER(I32), C.POINTER(I32)], C.c_int),
         "hk_scene_parse_xml": ([C.c_char_p, C.c_char_p, C.POINTER(P), C.POINTER(I32), C.POINTER(I32)], C.c_int),
@@ -297,6 +302,11 @@ class Scene:
     def width(self):
         return self.desc.camera.width if self.desc else None
 
+    def set_accel(self, accel: int) -> None:
+        """Traverse the binary tree (ACCEL_BVH2) or the compressed 8-wide tree (ACCEL_BVH8)."""
+        check(lib().hk_scene_set_accel(self.h, accel))
+        check(lib().hk_scene_get_info(self.h, C.byref(self.info)))
+
     def film_shape(self, width: int = 0, height: int = 0):
         """Film (RGBW accumulator) shape at the scene camera's size or at width x height."""
         B = self.info.film_border
@@ -456,6 +466,15 @@ def exr_write(path: str, rgb: np.ndarray) -> None:
     """Write an H x W x 3 float image as an uncompressed FLOAT RGB OpenEXR."""
     a = np.ascontiguousarray(rgb, np.float32)
     check(lib().hk_exr_write(path.encode(), a.shape[1], a.shape[0], a.ctypes.data))
+
+
+def bvh_check(tris: np.ndarray):
+    """Build both trees over tris (n x 3 x 3 float32) on the host and check
+    them; returns (binary nodes, 8-wide nodes, 8-wide depth)."""
+    t = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    check(lib().hk_bvh_check(t.ctypes.data, t.shape[0], C.byref(a), C.byref(b), C.byref(c)))
+    return a.value, b.value, c.value
 
 
 def parse_xml_info(path: str):

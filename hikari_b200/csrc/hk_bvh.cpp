@@ -159,47 +159,60 @@ void put_box(float *dst, const Box &c0, const Box &c1) {
     dst[8] = c0.lo[2]; dst[9] = c0.hi[2]; dst[10] = c1.lo[2]; dst[11] = c1.hi[2];
 }
 
-int32_t leaf_ref(const BNode &n) {
-    if (n.count >= 32) throw std::runtime_error("BVH leaf too large");
-    uint32_t enc = n.start | (n.count << kLeafCountShift);
+int32_t leaf_ref(uint32_t start, uint32_t count) {
+    if (count >= 32) throw std::runtime_error("BVH leaf too large");
+    if (start > kLeafStartMask) throw std::runtime_error("too many triangles for the BVH2 leaf encoding");
+    uint32_t enc = start | (count << kLeafCountShift);
     return (int32_t)~enc;
 }
 
-}  // namespace
+struct Tree {
+    std::vector<BNode> nodes;
+    std::vector<uint32_t> order;   // builder order: leaves index [start, start + count)
+    int32_t root = -1;
+    uint32_t depth = 0;
+};
 
-Bvh2 build_bvh2(const float *tris, uint32_t n, int max_leaf) {
-    Bvh2 out;
-    if (n == 0) return out;
+Tree build_tree(const float *tris, uint32_t n, int max_leaf) {
+    Tree T;
     std::vector<Box> tb(n);
     std::vector<float> cent(3 * (size_t)n);
-    out.tri_order.resize(n);
+    T.order.resize(n);
     for (uint32_t t = 0; t < n; t++) {
         tb[t].empty();
         for (int k = 0; k < 3; k++) tb[t].grow(tris + 9 * (size_t)t + 3 * k);
         for (int c = 0; c < 3; c++)
             cent[3 * (size_t)t + c] = (tris[9 * (size_t)t + c] + tris[9 * (size_t)t + 3 + c] + tris[9 * (size_t)t + 6 + c]) * (1.0f / 3.0f);
-        out.tri_order[t] = t;
+        T.order[t] = t;
     }
-    Builder B{tb, cent, out.tri_order, max_leaf};
-    std::vector<BNode> nodes;
-    nodes.reserve(2 * (size_t)n / std::max(1, max_leaf / 2) + 16);
-    int32_t root = B.build(nodes, 0, n, 0);
-    out.depth = B.max_depth.load() + 1;
-    // pack internal nodes depth-first (left child directly after its parent)
-    std::vector<int32_t> packed(nodes.size(), -1);
-    std::vector<int32_t> stack;
-    std::vector<int32_t> seq;
+    Builder B{tb, cent, T.order, max_leaf};
+    T.nodes.reserve(2 * (size_t)n / std::max(1, max_leaf / 2) + 16);
+    T.root = B.build(T.nodes, 0, n, 0);
+    T.depth = B.max_depth.load() + 1;
+    return T;
+}
+
+// Packs the binary tree into 64-byte nodes; leaf_start(i) is the position of
+// leaf i's first triangle in the final triangle order.
+template <class F>
+std::vector<float> pack_bvh2(const Tree &T, F leaf_start) {
+    const std::vector<BNode> &nodes = T.nodes;
+    std::vector<float> out;
+    const int32_t root = T.root;
     if (nodes[root].left < 0) {
         // single leaf: a root node with the leaf and an empty leaf
-        out.nodes.assign(16, 0.0f);
+        out.assign(16, 0.0f);
         Box far;
         for (int i = 0; i < 3; i++) { far.lo[i] = far.hi[i] = 1e30f; }
-        put_box(out.nodes.data(), nodes[root].box, far);
-        int32_t c0 = leaf_ref(nodes[root]), c1 = (int32_t)~0u;
-        std::memcpy(&out.nodes[12], &c0, 4);
-        std::memcpy(&out.nodes[13], &c1, 4);
+        put_box(out.data(), nodes[root].box, far);
+        int32_t c0 = leaf_ref(leaf_start(root), nodes[root].count), c1 = (int32_t)~0u;
+        std::memcpy(&out[12], &c0, 4);
+        std::memcpy(&out[13], &c1, 4);
         return out;
     }
+    // internal nodes depth-first (left child directly after its parent)
+    std::vector<int32_t> packed(nodes.size(), -1);
+    std::vector<int32_t> stack, seq;
     stack.push_back(root);
     while (!stack.empty()) {
         int32_t i = stack.back();
@@ -210,18 +223,335 @@ Bvh2 build_bvh2(const float *tris, uint32_t n, int max_leaf) {
         if (nodes[nd.right].left >= 0) stack.push_back(nd.right);
         if (nodes[nd.left].left >= 0) stack.push_back(nd.left);
     }
-    out.nodes.assign(seq.size() * 16, 0.0f);
+    out.assign(seq.size() * 16, 0.0f);
     for (size_t k = 0; k < seq.size(); k++) {
         const BNode &nd = nodes[seq[k]];
         const BNode &l = nodes[nd.left], &r = nodes[nd.right];
-        float *dst = &out.nodes[16 * k];
+        float *dst = &out[16 * k];
         put_box(dst, l.box, r.box);
-        int32_t c0 = l.left >= 0 ? packed[nd.left] : leaf_ref(l);
-        int32_t c1 = r.left >= 0 ? packed[nd.right] : leaf_ref(r);
+        int32_t c0 = l.left >= 0 ? packed[nd.left] : leaf_ref(leaf_start(nd.left), l.count);
+        int32_t c1 = r.left >= 0 ? packed[nd.right] : leaf_ref(leaf_start(nd.right), r.count);
         std::memcpy(&dst[12], &c0, 4);
         std::memcpy(&dst[13], &c1, 4);
     }
     return out;
+}
+
+// ---- 8-wide collapse and quantisation
+
+// Triangle range [start, start + count) of every subtree in the builder order
+// (the builder partitions in place, so a subtree's triangles are contiguous).
+void subtree_ranges(const std::vector<BNode> &nodes, int32_t root, std::vector<uint32_t> &start,
+                    std::vector<uint32_t> &count) {
+    start.assign(nodes.size(), 0);
+    count.assign(nodes.size(), 0);
+    std::vector<std::pair<int32_t, bool>> st{{root, false}};
+    while (!st.empty()) {
+        auto [i, done] = st.back();
+        st.pop_back();
+        const BNode &n = nodes[i];
+        if (n.left < 0) {
+            start[i] = n.start;
+            count[i] = n.count;
+        } else if (done) {
+            start[i] = std::min(start[n.left], start[n.right]);
+            count[i] = count[n.left] + count[n.right];
+        } else {
+            st.push_back({i, true});
+            st.push_back({n.left, false});
+            st.push_back({n.right, false});
+        }
+    }
+}
+
+// Children of binary node i opened greedily (largest surface area first) up
+// to 8 subtrees; subtrees of at most 3 triangles stay closed (8-wide leaves).
+int open_children(const std::vector<BNode> &nodes, const std::vector<uint32_t> &count, int32_t i, int32_t C[8]) {
+    int n = 0;
+    C[n++] = nodes[i].left;
+    C[n++] = nodes[i].right;
+    while (n < 8) {
+        int best = -1;
+        float best_a = -1.0f;
+        for (int k = 0; k < n; k++)
+            if (nodes[C[k]].left >= 0 && count[C[k]] > 3 && nodes[C[k]].box.area() > best_a) {
+                best_a = nodes[C[k]].box.area();
+                best = k;
+            }
+        if (best < 0) break;
+        int32_t x = C[best];
+        C[best] = nodes[x].left;
+        C[n++] = nodes[x].right;
+    }
+    return n;
+}
+
+// Slot s means "negative side of axis k" for every set bit k; children are
+// assigned greedily by the score of their centre offset along that diagonal.
+void assign_slots(const std::vector<BNode> &nodes, const Box &nb, const int32_t *C, int n, int32_t slot_child[8]) {
+    double cn[3];
+    for (int k = 0; k < 3; k++) cn[k] = 0.5 * ((double)nb.lo[k] + (double)nb.hi[k]);
+    struct Cand {
+        double score;
+        int c, s;
+    };
+    std::vector<Cand> cand;
+    cand.reserve(64);
+    for (int c = 0; c < n; c++) {
+        const Box &b = nodes[C[c]].box;
+        double d[3];
+        for (int k = 0; k < 3; k++) d[k] = 0.5 * ((double)b.lo[k] + (double)b.hi[k]) - cn[k];
+        for (int sl = 0; sl < 8; sl++) {
+            double sc = 0.0;
+            for (int k = 0; k < 3; k++) sc += (sl >> k & 1) ? -d[k] : d[k];
+            cand.push_back({sc, c, sl});
+        }
+    }
+    std::stable_sort(cand.begin(), cand.end(), [](const Cand &a, const Cand &b) { return a.score > b.score; });
+    bool used_c[8] = {false}, used_s[8] = {false};
+    for (int s2 = 0; s2 < 8; s2++) slot_child[s2] = -1;
+    for (const Cand &x : cand) {
+        if (used_c[x.c] || used_s[x.s]) continue;
+        used_c[x.c] = used_s[x.s] = true;
+        slot_child[x.s] = C[x.c];
+    }
+}
+
+// Quantised child boxes relative to the node box: conservative (floor/ceil in
+// double) and at least one step thick on every axis.
+void quantize(uint32_t *w, const Box &nb, const Box *cb[8]) {
+    uint8_t qlo[3][8], qhi[3][8];
+    int eb[3];
+    for (int k = 0; k < 3; k++) {
+        const double ext = (double)nb.hi[k] - (double)nb.lo[k];
+        int e = ext > 0.0 ? (int)std::ceil(std::log2(ext / 255.0)) : -100;
+        while (std::ldexp(255.0, e) < ext) ++e;
+        e = std::max(-126, std::min(127, e));
+        eb[k] = e + 127;
+        const double scale = std::ldexp(1.0, e);
+        for (int s = 0; s < 8; s++) {
+            if (!cb[s]) {   // empty slot: an inverted box that no ray hits
+                qlo[k][s] = 255;
+                qhi[k][s] = 0;
+                continue;
+            }
+            double lo = std::floor(((double)cb[s]->lo[k] - (double)nb.lo[k]) / scale);
+            double hi = std::ceil(((double)cb[s]->hi[k] - (double)nb.lo[k]) / scale);
+            lo = std::max(0.0, std::min(255.0, lo));
+            hi = std::max(0.0, std::min(255.0, hi));
+            if (hi <= lo) {
+                if (hi < 255.0) hi = lo + 1.0;
+                else lo = hi - 1.0;
+            }
+            qlo[k][s] = (uint8_t)lo;
+            qhi[k][s] = (uint8_t)hi;
+        }
+    }
+    for (int k = 0; k < 3; k++) std::memcpy(&w[k], &nb.lo[k], 4);
+    w[3] = (uint32_t)eb[0] | (uint32_t)eb[1] << 8 | (uint32_t)eb[2] << 16 | (w[3] & 0xff000000u);
+    auto pack = [](const uint8_t *q, uint32_t *dst) {
+        dst[0] = q[0] | q[1] << 8 | q[2] << 16 | (uint32_t)q[3] << 24;
+        dst[1] = q[4] | q[5] << 8 | q[6] << 16 | (uint32_t)q[7] << 24;
+    };
+    pack(qlo[0], &w[8]);
+    pack(qlo[1], &w[10]);
+    pack(qlo[2], &w[12]);
+    pack(qhi[0], &w[14]);
+    pack(qhi[1], &w[16]);
+    pack(qhi[2], &w[18]);
+}
+
+}  // namespace
+
+Bvh2 build_bvh2(const float *tris, uint32_t n, int max_leaf) {
+    Bvh2 out;
+    if (n == 0) return out;
+    Tree T = build_tree(tris, n, max_leaf);
+    out.depth = T.depth;
+    out.nodes = pack_bvh2(T, [&](int32_t i) { return T.nodes[i].start; });
+    out.tri_order = std::move(T.order);
+    return out;
+}
+
+BvhPair build_bvh_pair(const float *tris, uint32_t n) {
+    BvhPair P;
+    if (n == 0) return P;
+    Tree T = build_tree(tris, n, 3);
+    const std::vector<BNode> &nodes = T.nodes;
+    std::vector<uint32_t> sub_start, sub_count;
+    subtree_ranges(nodes, T.root, sub_start, sub_count);
+    auto is_leaf8 = [&](int32_t c) { return nodes[c].left < 0 || sub_count[c] <= 3; };
+    // new position of every binary leaf's first triangle
+    std::vector<uint32_t> leaf_start(nodes.size(), 0);
+    auto place_subtree = [&](int32_t c, uint32_t base) {
+        std::vector<int32_t> st{c};
+        while (!st.empty()) {
+            int32_t i = st.back();
+            st.pop_back();
+            if (nodes[i].left < 0) leaf_start[i] = base + (nodes[i].start - sub_start[c]);
+            else { st.push_back(nodes[i].left); st.push_back(nodes[i].right); }
+        }
+    };
+    std::vector<uint32_t> &order = P.bvh2.tri_order;
+    order.reserve(n);
+    std::vector<uint32_t> &W = P.bvh8.nodes;
+    W.assign(20, 0u);
+    struct Todo {
+        uint32_t w;
+        int32_t b;
+        uint32_t depth;
+    };
+    std::vector<Todo> todo;
+    todo.push_back({0, T.root, 1});
+    uint32_t depth8 = 0;
+    while (!todo.empty()) {
+        Todo t = todo.back();
+        todo.pop_back();
+        depth8 = std::max(depth8, t.depth);
+        int32_t C[8];
+        int nc;
+        if (is_leaf8(t.b)) {   // the whole tree is one leaf
+            C[0] = t.b;
+            nc = 1;
+        } else {
+            nc = open_children(nodes, sub_count, t.b, C);
+        }
+        int32_t slot_child[8];
+        assign_slots(nodes, nodes[t.b].box, C, nc, slot_child);
+        uint32_t ninternal = 0;
+        for (int s = 0; s < 8; s++)
+            if (slot_child[s] >= 0 && !is_leaf8(slot_child[s])) ++ninternal;
+        const uint32_t child_base = (uint32_t)(W.size() / 20);
+        W.resize(W.size() + 20 * (size_t)ninternal, 0u);
+        const uint32_t tri_base = (uint32_t)order.size();
+        uint32_t imask = 0, meta[8] = {0};
+        std::vector<Todo> kids;
+        uint32_t j = 0;
+        const Box *cb[8];
+        for (int s = 0; s < 8; s++) {
+            const int32_t c = slot_child[s];
+            cb[s] = c >= 0 ? &nodes[c].box : nullptr;
+            if (c < 0) continue;
+            if (!is_leaf8(c)) {
+                imask |= 1u << s;
+                kids.push_back({child_base + j++, c, t.depth + 1});
+            } else {
+                const uint32_t off = (uint32_t)order.size() - tri_base, cnt = sub_count[c];
+                if (cnt < 1 || cnt > 3 || off > 21) throw std::runtime_error("BVH8 leaf layout");
+                meta[s] = cnt << 5 | off;
+                place_subtree(c, (uint32_t)order.size());
+                for (uint32_t k = 0; k < cnt; k++) order.push_back(T.order[sub_start[c] + k]);
+            }
+        }
+        uint32_t *w = &W[20 * (size_t)t.w];
+        w[3] = imask << 24;
+        w[4] = child_base;
+        w[5] = tri_base;
+        w[6] = meta[0] | meta[1] << 8 | meta[2] << 16 | meta[3] << 24;
+        w[7] = meta[4] | meta[5] << 8 | meta[6] << 16 | meta[7] << 24;
+        quantize(w, nodes[t.b].box, cb);
+        for (auto it = kids.rbegin(); it != kids.rend(); ++it) todo.push_back(*it);
+    }
+    if (order.size() != n) throw std::runtime_error("BVH8 collapse lost triangles");
+    P.bvh8.depth = depth8;
+    P.bvh2.depth = T.depth;
+    P.bvh2.nodes = pack_bvh2(T, [&](int32_t i) { return leaf_start[i]; });
+    return P;
+}
+
+std::string check_bvh_pair(const BvhPair &P, const float *tris, uint32_t n) {
+    const std::vector<uint32_t> &order = P.bvh2.tri_order;
+    if (order.size() != n) return "triangle order has the wrong size";
+    std::vector<uint8_t> seen(n, 0);
+    for (uint32_t o : order) {
+        if (o >= n || seen[o]) return "triangle order is not a permutation";
+        seen[o] = 1;
+    }
+    // ---- 8-wide tree
+    const std::vector<uint32_t> &W = P.bvh8.nodes;
+    const uint32_t nw = (uint32_t)(W.size() / 20);
+    std::vector<uint8_t> tri_ref(n, 0), node_ref(nw, 0);
+    struct Item {
+        uint32_t node;
+        double lo[3], hi[3];   // the box the parent stores for this node
+    };
+    std::vector<Item> todo;
+    Item root{0, {-1e300, -1e300, -1e300}, {1e300, 1e300, 1e300}};
+    todo.push_back(root);
+    node_ref[0] = 1;
+    auto inside = [&](uint32_t pos, const double *lo, const double *hi) {
+        const uint32_t t = order[pos];
+        for (int v = 0; v < 3; v++)
+            for (int k = 0; k < 3; k++) {
+                double x = tris[9 * (size_t)t + 3 * v + k];
+                if (x < lo[k] || x > hi[k]) return false;
+            }
+        return true;
+    };
+    while (!todo.empty()) {
+        Item it = todo.back();
+        todo.pop_back();
+        const uint32_t *w = &W[20 * (size_t)it.node];
+        float p[3];
+        std::memcpy(p, w, 12);
+        const uint32_t imask = w[3] >> 24;
+        double scale[3];
+        for (int k = 0; k < 3; k++) scale[k] = std::ldexp(1.0, (int)((w[3] >> (8 * k)) & 0xffu) - 127);
+        auto q = [&](int plane, int k, int s) { return (double)((w[8 + 2 * (plane * 3 + k) + s / 4] >> (8 * (s % 4))) & 0xffu); };
+        uint32_t j = 0;
+        for (int s = 0; s < 8; s++) {
+            const uint32_t m = (s < 4 ? w[6] : w[7]) >> (8 * (s & 3)) & 0xffu;
+            double lo[3], hi[3];
+            for (int k = 0; k < 3; k++) {
+                lo[k] = (double)p[k] + q(0, k, s) * scale[k];
+                hi[k] = (double)p[k] + q(1, k, s) * scale[k];
+            }
+            if (imask >> s & 1u) {
+                const uint32_t c = w[4] + j++;
+                if (c >= nw || node_ref[c]) return "8-wide child index out of range or shared";
+                node_ref[c] = 1;
+                Item ci{c, {lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}};
+                todo.push_back(ci);
+            } else if (m) {
+                const uint32_t cnt = m >> 5, off = m & 31u;
+                for (uint32_t k = 0; k < cnt; k++) {
+                    const uint32_t pos = w[5] + off + k;
+                    if (pos >= n || tri_ref[pos]) return "8-wide leaf triangle out of range or shared";
+                    tri_ref[pos] = 1;
+                    if (!inside(pos, lo, hi)) return "8-wide child box does not contain its triangle";
+                    // and every ancestor box along the way
+                    if (!inside(pos, it.lo, it.hi)) return "8-wide node box does not contain its triangle";
+                }
+            }
+        }
+        // child boxes of internal children must lie within this node's stored box
+        (void)it;
+    }
+    for (uint32_t i = 0; i < n; i++)
+        if (!tri_ref[i]) return "8-wide tree misses a triangle";
+    for (uint32_t i = 0; i < nw; i++)
+        if (!node_ref[i]) return "8-wide tree has an unreachable node";
+    // ---- binary tree: leaves cover the order once
+    std::vector<uint8_t> tri2(n, 0);
+    const std::vector<float> &B = P.bvh2.nodes;
+    const uint32_t nb = (uint32_t)(B.size() / 16);
+    for (uint32_t i = 0; i < nb; i++)
+        for (int c = 0; c < 2; c++) {
+            int32_t ref;
+            std::memcpy(&ref, &B[16 * (size_t)i + 12 + c], 4);
+            if (ref >= 0) {
+                if ((uint32_t)ref >= nb) return "binary child index out of range";
+                continue;
+            }
+            const uint32_t enc = ~(uint32_t)ref, start = enc & kLeafStartMask, cnt = enc >> kLeafCountShift;
+            for (uint32_t k = 0; k < cnt; k++) {
+                if (start + k >= n || tri2[start + k]) return "binary leaf triangle out of range or shared";
+                tri2[start + k] = 1;
+            }
+        }
+    for (uint32_t i = 0; i < n; i++)
+        if (!tri2[i]) return "binary tree misses a triangle";
+    return std::string();
 }
 
 }  // namespace hk

@@ -59,6 +59,9 @@ struct alignas(16) DevAreaLight {
 //   b = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
 //   c = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
 //   d = (child0, child1, -, -) as int; child < 0 -> leaf ~(start | count << 27)
+constexpr int kStackSize = 64;   // traversal stack entries per ray (tree depth is capped below it)
+constexpr int kAccelBvh2 = 0;
+constexpr int kAccelBvh8 = 1;
 constexpr int kLeafCountShift = 27;
 constexpr uint32_t kLeafStartMask = (1u << kLeafCountShift) - 1u;
 
@@ -67,8 +70,11 @@ struct DevScene {
     //   v0.xyz, bits(original triangle index); v1.xyz, bits(mesh); v2.xyz, 0
     const float4 *tris;
     const float4 *nodes;          // 4 float4 per BVH2 node
+    const uint4 *wnodes;          // 5 uint4 per compressed 8-wide node (hk_bvh.h)
     const float4 *tri_normals;    // 3 float4 per ORIGINAL triangle (only if any mesh has normals)
-    uint32_t ntris, nnodes;
+    uint32_t ntris, nnodes, nwnodes;
+    int32_t accel;                // kAccelBvh2 or kAccelBvh8: the tree the kernels traverse
+    int32_t postpone;             // 8-wide traversal may postpone triangle tests (stack bound allows it)
     const DevMesh *meshes;
     const DevBsdf *bsdfs;
     int32_t nmeshes, nbsdfs;

@@ -220,7 +220,8 @@ struct hk_scene {
     // built state
     bool built = false;
     hk::DevScene dev{};
-    DevBuf b_tris, b_nodes, b_tri_normals, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
+    int32_t accel = HK_ACCEL_BVH8;
+    DevBuf b_tris, b_nodes, b_wnodes, b_tri_normals, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
         b_light_cdf, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
     DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
     std::vector<std::unique_ptr<DevBuf>> batch_films;   // films of hk_render_batch_host
@@ -385,8 +386,10 @@ void build_scene(hk_scene *s) {
     if (any_normals) { s->b_tri_normals.upload(tri_normals); track(s->b_tri_normals); }
     D.tri_normals = s->b_tri_normals.as<float4>();
 
-    // BVH
-    hk::Bvh2 bvh = hk::build_bvh2(P.data(), (uint32_t)ntris);
+    // BVH: one binned-SAH build, packed as the binary tree and collapsed into
+    // the compressed 8-wide tree over one triangle order
+    hk::BvhPair pair = hk::build_bvh_pair(P.data(), (uint32_t)ntris);
+    const hk::Bvh2 &bvh = pair.bvh2;
     std::vector<float> recs(bvh.tri_order.size() * 12);
     for (size_t i = 0; i < bvh.tri_order.size(); ++i) {
         uint32_t o = bvh.tri_order[i];
@@ -404,6 +407,14 @@ void build_scene(hk_scene *s) {
     D.nodes = s->b_nodes.as<float4>();
     D.ntris = (uint32_t)ntris;
     D.nnodes = (uint32_t)(bvh.nodes.size() / 16);
+    s->b_wnodes.upload(pair.bvh8.nodes); track(s->b_wnodes);
+    D.wnodes = s->b_wnodes.as<uint4>();
+    D.nwnodes = (uint32_t)(pair.bvh8.nodes.size() / 20);
+    // the traversal stack holds at most one node group and one postponed
+    // triangle group per level (plus the root)
+    D.postpone = 2 * (int)pair.bvh8.depth + 2 <= hk::kStackSize ? 1 : 0;
+    if ((int)pair.bvh8.depth + 1 > hk::kStackSize) throw HkError{HK_ERR_INVALID, "8-wide BVH too deep"};
+    D.accel = s->accel;
 
     // emitters (Scene order)
     std::vector<int32_t> emitter_area;
@@ -554,6 +565,10 @@ void build_scene(hk_scene *s) {
     I.n_emitters = (uint32_t)emitter_area.size();
     I.n_bvh_nodes = D.nnodes;
     I.bvh_depth = bvh.depth;
+    I.n_wide_nodes = D.nwnodes;
+    I.wide_depth = pair.bvh8.depth;
+    I.accel = D.accel;
+    I.postpone = D.postpone;
     I.env_index = D.env_index;
     I.film_border = D.border;
     std::memcpy(I.bbox, bb, sizeof bb);
@@ -751,6 +766,28 @@ int hk_scene_build(hk_scene *s) {
     return guarded([&] {
         if (!s) throw HkError{HK_ERR_INVALID, "null scene"};
         build_scene(s);
+        return HK_OK;
+    });
+}
+int hk_bvh_check(const float *tris, uint32_t n, uint32_t *n_bvh_nodes, uint32_t *n_wide_nodes, uint32_t *wide_depth) {
+    return guarded([&] {
+        if (!tris || n == 0) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        hk::BvhPair P = hk::build_bvh_pair(tris, n);
+        std::string err = hk::check_bvh_pair(P, tris, n);
+        if (!err.empty()) throw HkError{HK_ERR_INVALID, err};
+        if (n_bvh_nodes) *n_bvh_nodes = (uint32_t)(P.bvh2.nodes.size() / 16);
+        if (n_wide_nodes) *n_wide_nodes = (uint32_t)(P.bvh8.nodes.size() / 20);
+        if (wide_depth) *wide_depth = P.bvh8.depth;
+        return HK_OK;
+    });
+}
+int hk_scene_set_accel(hk_scene *s, int32_t accel) {
+    return guarded([&] {
+        if (!s || (accel != HK_ACCEL_BVH2 && accel != HK_ACCEL_BVH8)) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        s->accel = accel;
+        s->dev.accel = accel;
+        s->info.accel = accel;
+        s->wf.reset();   // the engine holds a copy of the device description
         return HK_OK;
     });
 }

@@ -13,8 +13,6 @@
 
 namespace hk {
 
-constexpr int kStackSize = 64;
-
 struct Ray {
     V3 o, d;
     float tmin, tmax;
@@ -210,6 +208,166 @@ __device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hi
                   hit.v);
     }
     return found;
+}
+
+// ------------------------------------------------------------ 8-wide tree
+// Traversal of the compressed 8-wide BVH (hk_bvh.h), following Ylitie, Karras
+// and Laine (HPG 2017): a node group is (first child index, hit bits of the
+// internal children << 24 | imask), a triangle group is (first triangle,
+// hit bits 0..23).  Hit bits of internal children sit at slot ^ (7 ^ octant),
+// so the lowest set bit is the nearest child.  A warp vote postpones the
+// triangle tests of lanes that are few among the active ones while they still
+// have nodes to visit, so that lanes intersect triangles together.
+
+constexpr int kShStack = 8;   // entries per thread kept in shared memory
+
+// Traversal stack entirely in registers/local memory.
+struct LocalStack {
+    uint2 e[kStackSize];
+    int sp = 0;
+    // The tree depth bound keeps sp below kStackSize; past it an entry would be dropped, never written out of bounds.
+    __device__ __forceinline__ void push(uint2 v) {
+        if (sp < kStackSize) e[sp++] = v;
+    }
+    __device__ __forceinline__ uint2 pop() { return e[--sp]; }
+};
+
+// Short stack: the top kShStack entries of each thread in shared memory
+// (sh[k * stride], one column per thread), deeper entries in local memory.
+struct SharedStack {
+    uint2 *sh;
+    int stride;
+    int sp = 0;
+    uint2 spill[kStackSize - kShStack];
+    __device__ __forceinline__ void push(uint2 v) {
+        if (sp < kShStack) sh[sp++ * stride] = v;
+        else if (sp < kStackSize) { spill[sp - kShStack] = v; ++sp; }
+    }
+    __device__ __forceinline__ uint2 pop() {
+        --sp;
+        return sp < kShStack ? sh[sp * stride] : spill[sp - kShStack];
+    }
+};
+
+__device__ __forceinline__ uint4 ldg4u(const uint4 *p) { return __ldg(p); }
+
+template <bool kAnyHit, class Stack>
+__device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st, Stack &stk) {
+    hit.tri = -1;
+    if (S.nwnodes == 0) return false;
+    const V3 d = ray.d;
+    const float tiny = 1e-30f;
+    const V3 dd = v3(fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x, fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y,
+                     fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z);
+    const V3 idir = v3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    const uint32_t oct = (idir.x < 0.0f ? 1u : 0u) | (idir.y < 0.0f ? 2u : 0u) | (idir.z < 0.0f ? 4u : 0u);
+    const uint32_t ko = 7u ^ oct;
+    const WatertightRay w = watertight_setup(d);
+    float tmax = ray.tmax;
+    uint2 ng = make_uint2(0u, (1u << (24 + ko)) | 1u);   // the root as slot 0 of a virtual parent
+    uint2 tg = make_uint2(0u, 0u);
+    stk.sp = 0;
+    bool found = false;
+    uint32_t nvis = 0, ntri = 0;
+    for (;;) {
+        if (ng.y > 0x00ffffffu) {
+            const uint32_t b = __ffs(ng.y >> 24) - 1;
+            ng.y &= ~(1u << (24 + b));
+            const uint32_t slot = b ^ ko;
+            const uint32_t child = ng.x + __popc(ng.y & 0xffu & ((1u << slot) - 1u));
+            if (ng.y > 0x00ffffffu) stk.push(ng);
+            // ---- intersect the 8 children of node `child`
+            const uint4 *np = S.wnodes + 5 * (size_t)child;
+            const uint4 n0 = ldg4u(np), n1 = ldg4u(np + 1), n2 = ldg4u(np + 2), n3 = ldg4u(np + 3),
+                        n4 = ldg4u(np + 4);
+            ++nvis;
+            const float adx = __uint_as_float((n0.w & 0xffu) << 23) * idir.x;
+            const float ady = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * idir.y;
+            const float adz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * idir.z;
+            const float ox = (__uint_as_float(n0.x) - ray.o.x) * idir.x;
+            const float oy = (__uint_as_float(n0.y) - ray.o.y) * idir.y;
+            const float oz = (__uint_as_float(n0.z) - ray.o.z) * idir.z;
+            const uint32_t imask = n0.w >> 24;
+            // near / far planes per axis (lo planes first for a positive direction)
+            const uint32_t nx0 = oct & 1u ? n3.z : n2.x, nx1 = oct & 1u ? n3.w : n2.y;
+            const uint32_t fx0 = oct & 1u ? n2.x : n3.z, fx1 = oct & 1u ? n2.y : n3.w;
+            const uint32_t ny0 = oct & 2u ? n4.x : n2.z, ny1 = oct & 2u ? n4.y : n2.w;
+            const uint32_t fy0 = oct & 2u ? n2.z : n4.x, fy1 = oct & 2u ? n2.w : n4.y;
+            const uint32_t nz0 = oct & 4u ? n4.z : n3.x, nz1 = oct & 4u ? n4.w : n3.y;
+            const uint32_t fz0 = oct & 4u ? n3.x : n4.z, fz1 = oct & 4u ? n3.y : n4.w;
+            uint32_t hits_int = 0, hits_tri = 0;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const int sh = (c & 3) * 8;
+                const uint32_t qnx = ((c < 4 ? nx0 : nx1) >> sh) & 0xffu, qfx = ((c < 4 ? fx0 : fx1) >> sh) & 0xffu;
+                const uint32_t qny = ((c < 4 ? ny0 : ny1) >> sh) & 0xffu, qfy = ((c < 4 ? fy0 : fy1) >> sh) & 0xffu;
+                const uint32_t qnz = ((c < 4 ? nz0 : nz1) >> sh) & 0xffu, qfz = ((c < 4 ? fz0 : fz1) >> sh) & 0xffu;
+                const float tnx = __fmaf_rn((float)qnx, adx, ox), tfx = __fmaf_rn((float)qfx, adx, ox);
+                const float tny = __fmaf_rn((float)qny, ady, oy), tfy = __fmaf_rn((float)qfy, ady, oy);
+                const float tnz = __fmaf_rn((float)qnz, adz, oz), tfz = __fmaf_rn((float)qfz, adz, oz);
+                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, ray.tmin));
+                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+                if (tn <= tf * 1.00000024f + 1e-30f) {
+                    if (imask >> c & 1u) {
+                        hits_int |= 1u << (c ^ ko);
+                    } else {
+                        const uint32_t m = ((c < 4 ? n1.z : n1.w) >> sh) & 0xffu;
+                        hits_tri |= ((1u << (m >> 5)) - 1u) << (m & 31u);
+                    }
+                }
+            }
+            ng = make_uint2(n1.x, (hits_int << 24) | imask);
+            tg = make_uint2(n1.y, hits_tri);
+        } else {
+            tg = ng;   // a postponed triangle group from the stack
+            ng = make_uint2(0u, 0u);
+        }
+        if (S.postpone) {
+            const unsigned act = __activemask();
+            const unsigned want = __ballot_sync(act, tg.y != 0u);
+            if (tg.y != 0u && ng.y > 0x00ffffffu && __popc(want) * 5 < __popc(act)) {
+                stk.push(tg);
+                tg.y = 0u;
+            }
+        }
+        while (tg.y != 0u) {
+            const uint32_t tri = tg.x + (__ffs(tg.y) - 1);
+            tg.y &= tg.y - 1u;
+            ++ntri;
+            const float4 *tp = S.tris + 3 * (size_t)tri;
+            const float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
+            float tt, uu, vv;
+            if (intersect_watertight(w, ray.o, xyz(p0), xyz(p1), xyz(p2), ray.tmin, tmax, tt, uu, vv)) {
+                found = true;
+                hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)tri;
+                if (kAnyHit) {
+                    st.nodes += nvis;
+                    st.tris += ntri;
+                    return true;
+                }
+                tmax = tt;
+            }
+        }
+        if (ng.y <= 0x00ffffffu) {
+            if (stk.sp == 0) break;
+            ng = stk.pop();
+        }
+    }
+    st.nodes += nvis;
+    st.tris += ntri;
+    if (found && !kAnyHit) {
+        const float4 *tp = S.tris + 3 * hit.tri;
+        refine_mt(ray.o, ray.d, xyz(ldg4(tp)), xyz(ldg4(tp + 1)), xyz(ldg4(tp + 2)), ray.tmin, ray.tmax, hit.t, hit.u,
+                  hit.v);
+    }
+    return found;
+}
+
+// The scene's tree: closest hit (kAnyHit = false) or first hit.
+template <bool kAnyHit, class Stack>
+__device__ __forceinline__ bool trace(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st, Stack &stk) {
+    if (S.accel == kAccelBvh8) return trace_bvh8<kAnyHit>(S, ray, hit, st, stk);
+    return trace_bvh2<kAnyHit>(S, ray, hit, st);
 }
 
 }  // namespace hk

@@ -210,9 +210,19 @@ __global__ void wf_init_kernel(WfState W) {
 }
 
 // ------------------------------------------------------------ extend
+// Shared memory of the traversal short stacks: kShStack entries per thread.
+__device__ __forceinline__ SharedStack make_stack() {
+    extern __shared__ uint2 wf_stack_smem[];
+    SharedStack s;
+    s.sh = wf_stack_smem + threadIdx.x;
+    s.stride = (int)blockDim.x;
+    return s;
+}
+
 __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, int cur) {
     const int n = (int)W.ctr->eq_count[cur];
     TravStats ts;
+    SharedStack stk = make_stack();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = W.eq[cur][i];
         float4 o = W.ray_o[slot], d = W.ray_d[slot];
@@ -223,7 +233,7 @@ __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, i
         r.tmax = d.w;
         Hit h;
         int type = 0;
-        if (trace_bvh2<false>(S, r, h, ts)) {
+        if (trace<false>(S, r, h, ts, stk)) {
             int mesh = __float_as_int(__ldg(S.tris + 3 * h.tri + 1).w);
             type = S.bsdfs[S.meshes[mesh].bsdf].type + 1;
         }
@@ -383,6 +393,7 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
 __global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
     const int n = min((int)W.ctr->shadow_count, W.max_shadow);
     TravStats ts;
+    SharedStack stk = make_stack();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 o = W.sh_o[i], d = W.sh_d[i];
         Ray r;
@@ -391,7 +402,7 @@ __global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
         r.tmin = kRayEps;
         r.tmax = 1.0f - kRayEps;
         Hit h;
-        if (!trace_bvh2<true>(S, r, h, ts)) {
+        if (!trace<true>(S, r, h, ts, stk)) {
             float4 c = W.sh_c[i];
             red_add_v4(W.lacc + __float_as_int(o.w), c.x, c.y, c.z, 0.0f);
         }
@@ -421,6 +432,8 @@ __global__ void wf_counters_add_kernel(const WfCounters *c, unsigned long long *
 }
 
 // ------------------------------------------------------------ launchers
+static size_t stack_smem(int threads) { return (size_t)threads * kShStack * sizeof(uint2); }
+
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st) {
     wf_counters_add_kernel<<<1, 32, 0, st>>>(W.ctr, out);
     return cudaGetLastError();
@@ -435,14 +448,14 @@ cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLau
     const int nxt = cur ^ 1;
     wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur);
     wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
-    wf_extend_kernel<<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur);
+    wf_extend_kernel<<<C.blocks_extend, C.threads_extend, stack_smem(C.threads_extend), st>>>(S, W, cur);
     wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<1><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<2><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<3><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-    wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W);
+    wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, stack_smem(C.threads_shadow), st>>>(S, W);
     return cudaGetLastError();
 }
 
@@ -454,7 +467,7 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
         wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur);
         wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
         break;
-    case 1: wf_extend_kernel<<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur); break;
+    case 1: wf_extend_kernel<<<C.blocks_extend, C.threads_extend, stack_smem(C.threads_extend), st>>>(S, W, cur); break;
     case 2:
         wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         wf_shade_kernel<1><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
@@ -463,7 +476,7 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
         wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         break;
-    default: wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W); break;
+    default: wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, stack_smem(C.threads_shadow), st>>>(S, W); break;
     }
     return cudaGetLastError();
 }
@@ -471,9 +484,9 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
 int wf_occupancy(int which, int threads) {
     int n = 0;
     switch (which) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel, threads, 0); break;
+    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel, threads, stack_smem(threads)); break;
     case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade_kernel<5>, threads, 0); break;
-    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel, threads, 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel, threads, stack_smem(threads)); break;
     default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_regen_kernel, threads, 0); break;
     }
     return n;

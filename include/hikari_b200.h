@@ -61,12 +61,21 @@ typedef struct {
 
 typedef struct {
     uint32_t n_meshes, n_triangles, n_bsdfs, n_emitters;
-    uint32_t n_bvh_nodes, bvh_depth;
+    uint32_t n_bvh_nodes, bvh_depth;        /* binary tree: 64-byte nodes */
     int32_t env_index;
     int32_t film_border;
     float bbox[6];
     uint64_t device_bytes;
+    uint32_t n_wide_nodes, wide_depth;      /* compressed 8-wide tree: 80-byte nodes */
+    int32_t accel;                          /* HK_ACCEL_* the kernels traverse */
+    int32_t postpone;                       /* 8-wide traversal postpones triangle tests */
 } hk_scene_info;
+
+/* Acceleration structures (both are built; hk_scene_set_accel picks the one
+ * traversed).  The reference's accel plugins (src/acceleration/*.cpp: bruto,
+ * bvh, hlbvh) all answer the same closest-hit query. */
+#define HK_ACCEL_BVH2 0   /* binary binned-SAH tree, 64-byte nodes */
+#define HK_ACCEL_BVH8 1   /* compressed 8-wide tree, 80-byte quantised nodes (default) */
 
 const char *hk_last_error(void);
 int hk_version(void);
@@ -97,6 +106,9 @@ int hk_scene_set_background(hk_scene *s, const float *rgb3, int force_background
 /* Activate every object and upload (Scene::Activate src/core/Scene.cpp:128 +
  * Integrator::Preprocess): BSDF tables, light CDFs, the BVH, device buffers. */
 int hk_scene_build(hk_scene *s);
+/* Select the tree the render and trace kernels traverse (takes effect
+ * immediately on a built scene; both trees share one triangle order). */
+int hk_scene_set_accel(hk_scene *s, int32_t accel);
 /* Counts and bbox; before hk_scene_build the BVH and device fields are 0. */
 int hk_scene_get_info(const hk_scene *s, hk_scene_info *info);
 /* Parse a Hikari scene XML file through the C++ plugin layer (LoadFromXML,
@@ -271,6 +283,14 @@ int hk_job_wait(hk_server *srv, uint64_t job_id, double timeout_s, hk_job_status
  * paths in flight are done (its image is not written). */
 int hk_job_cancel(hk_server *srv, uint64_t job_id);
 int hk_server_get_stats(hk_server *srv, hk_server_stats *stats);
+
+/* Host-only check of the tree builder (no counterpart in the reference; used
+ * by the tests): builds both trees over ntris triangles (9 floats each) and
+ * verifies that every triangle sits in exactly one leaf of each tree and that
+ * every quantised 8-wide child box contains its triangles.  Returns HK_OK and
+ * the tree sizes, or HK_ERR_INVALID with the first problem in hk_last_error(). */
+int hk_bvh_check(const float *tris, uint32_t ntris, uint32_t *n_bvh_nodes, uint32_t *n_wide_nodes,
+                 uint32_t *wide_depth);
 
 /* ---- record-level entry points (parity tests and the BSDF batch) ---- */
 /* Ray queries against the scene accel (Acceleration::RayIntersect,

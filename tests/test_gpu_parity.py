@@ -96,9 +96,12 @@ def _camera_rays(sd, os_, n, seed):
                      zip(rng.uniform(0, W, n), rng.uniform(0, H, n))]).astype(np.float32)
 
 
-def test_trace_parity_cornell():
+@pytest.mark.parametrize("accel", [hk.ACCEL_BVH2, hk.ACCEL_BVH8])
+def test_trace_parity_cornell(accel):
     sd = scenes.cornell_box(width=64, height=64)
     gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    gs.set_accel(accel)
+    assert gs.info.accel == accel
     rays = _camera_rays(sd, os_, 20000, 5)
     # add random interior rays (origins inside the box, random directions)
     rng = np.random.default_rng(9)
@@ -121,6 +124,38 @@ def test_trace_parity_cornell():
     both = same & (tri_o >= 0)
     assert rel_close(t_g[both], t_o[both], 1e-6).mean() > 0.999
     # any-hit agrees on the hit/miss decision
+    any_g = gs.trace(_t(rays), any_hit=True)[0].cpu().numpy()
+    any_o = os_.trace(rays, any_hit=True, use_bvh=False)[0]
+    assert (any_g == any_o).mean() > 0.999
+
+
+@pytest.mark.parametrize("accel", [hk.ACCEL_BVH2, hk.ACCEL_BVH8])
+def test_trace_parity_displaced_sphere(accel):
+    """Closest and any hit on a 20k-triangle displaced icosphere over a ground
+    quad, rays from outside and inside, against the oracle's brute force."""
+    sd = scenes.mesh_heavy("conductor", width=16, height=16, level=5, env_res=(64, 32))
+    gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    gs.set_accel(accel)
+    rng = np.random.default_rng(21)
+    n = 30000
+    o = np.concatenate([rng.uniform(-3, 3, (n // 2, 3)) + [0, 1.5, 0],
+                        rng.normal(0, 0.3, (n - n // 2, 3)) + [0, 1.0, 0]]).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([o, d, np.full((n, 1), 1e-4), np.full((n, 1), np.inf)], 1).astype(np.float32)
+    tri_g, t_g, _, _, visits = gs.trace(_t(rays))
+    tri_g, t_g = tri_g.cpu().numpy(), t_g.cpu().numpy()
+    tri_o, t_o, u_o, v_o = os_.trace(rays, use_bvh=False)
+    same = tri_g == tri_o
+    bad = ~same
+    edge = np.minimum(np.minimum(u_o, v_o), 1 - u_o - v_o) < 1e-5
+    tie = (tri_g >= 0) & (tri_o >= 0) & rel_close(t_g, t_o, 1e-6)
+    print(f"accel {accel}: ids bit-exact on {same.mean():.6f}, {np.sum(bad & tie)} ties, {np.sum(bad & ~tie)} others; "
+          f"node visits per ray {visits[0].item() / n:.1f}, triangle tests per ray {visits[1].item() / n:.1f}")
+    assert np.all(tie[bad] | edge[bad]), f"{np.sum(bad & ~tie & ~edge)} non-tie, non-edge mismatches"
+    assert same.mean() > 0.999
+    both = same & (tri_o >= 0)
+    assert rel_close(t_g[both], t_o[both], 1e-6).mean() > 0.999
     any_g = gs.trace(_t(rays), any_hit=True)[0].cpu().numpy()
     any_o = os_.trace(rays, any_hit=True, use_bvh=False)[0]
     assert (any_g == any_o).mean() > 0.999

@@ -129,3 +129,35 @@ def test_argument_checks_without_device(L):
         assert L.hk_render(h, None, None, None, None) == -1    # not built
     finally:
         L.hk_scene_destroy(h)
+
+
+@pytest.mark.parametrize("case", ["random", "grid", "single", "degenerate", "cornell", "spheres"])
+def test_bvh_trees_are_consistent(L, case):
+    """Both trees cover every triangle once and the quantised 8-wide child
+    boxes contain their triangles (checked in double on the host)."""
+    from hikari_b200 import scenes
+
+    rng = np.random.default_rng(1)
+    if case == "random":
+        c = rng.uniform(-50, 50, (20000, 1, 3))
+        tris = c + rng.normal(0, 0.5, (20000, 3, 3))
+    elif case == "grid":   # axis-aligned, coplanar, zero-thickness boxes
+        g = np.stack(np.meshgrid(np.arange(60), np.arange(60), indexing="ij"), -1).reshape(-1, 2).astype(np.float64)
+        z = np.zeros((g.shape[0], 1))
+        a = np.concatenate([g, z], 1)
+        tris = np.stack([a, a + [1, 0, 0], a + [0, 1, 0]], 1)
+    elif case == "single":
+        tris = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]]], np.float64)
+    elif case == "degenerate":   # many identical triangles and far outliers
+        tris = np.repeat(np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]]], np.float64), 500, 0)
+        tris = np.concatenate([tris, rng.uniform(-1e4, 1e4, (50, 3, 3))])
+    elif case == "cornell":
+        sd = scenes.cornell_box()
+        tris = np.concatenate([m.positions[m.indices] for m in sd.meshes])
+    else:
+        P, F = scenes.displaced_icosphere(5, 1.0, (0, 0, 0), 0.08, 3)
+        tris = P[F]
+    n2, n8, d8 = hk.bvh_check(tris)
+    print(case, "triangles", len(tris), "binary nodes", n2, "8-wide nodes", n8, "8-wide depth", d8)
+    assert n8 >= 1 and n2 >= 1
+    assert 2 * d8 + 2 <= 64 or len(tris) > 1e6
