@@ -317,37 +317,44 @@ void assign_slots(const std::vector<BNode> &nodes, const Box &nb, const int32_t 
     }
 }
 
-// Quantised child boxes relative to the node box: conservative (floor/ceil in
-// double) and at least one step thick on every axis.
+// Quantised child boxes: conservative (floor/ceil in double) and padded by
+// one step on every side, which absorbs the rounding of the traversal's
+// folded slab arithmetic (at most half a step).  The step s = 2^e covers the
+// node extent in 252 steps and the origin sits at least one step below the
+// node box (float rounding of p is below a quarter step because s is at least
+// 2^-20 of the coordinates' magnitude), so padded planes stay within 0..255.
 void quantize(uint32_t *w, const Box &nb, const Box *cb[8]) {
     uint8_t qlo[3][8], qhi[3][8];
     int eb[3];
+    float p[3];
     for (int k = 0; k < 3; k++) {
-        const double ext = (double)nb.hi[k] - (double)nb.lo[k];
-        int e = ext > 0.0 ? (int)std::ceil(std::log2(ext / 255.0)) : -100;
-        while (std::ldexp(255.0, e) < ext) ++e;
-        e = std::max(-126, std::min(127, e));
+        const double lo_n = nb.lo[k], hi_n = nb.hi[k];
+        const double ext = hi_n - lo_n;
+        const double mag = std::max(std::max(std::fabs(lo_n), std::fabs(hi_n)), 1e-30);
+        int e = (int)std::floor(std::log2(mag)) - 20;
+        if (ext > 0.0) e = std::max(e, (int)std::ceil(std::log2(ext / 252.0)));
+        while (std::ldexp(252.0, e) < ext) ++e;
+        if (e > 38) throw std::runtime_error("scene extent too large for the 8-wide node quantisation");
+        e = std::max(-126, e);
         eb[k] = e + 127;
         const double scale = std::ldexp(1.0, e);
+        // origin at least one step below the node box (rounded toward -inf)
+        p[k] = (float)(lo_n - scale);
+        if ((double)p[k] > lo_n - scale) p[k] = std::nextafter(p[k], -INFINITY);
         for (int s = 0; s < 8; s++) {
             if (!cb[s]) {   // empty slot: an inverted box that no ray hits
                 qlo[k][s] = 255;
                 qhi[k][s] = 0;
                 continue;
             }
-            double lo = std::floor(((double)cb[s]->lo[k] - (double)nb.lo[k]) / scale);
-            double hi = std::ceil(((double)cb[s]->hi[k] - (double)nb.lo[k]) / scale);
-            lo = std::max(0.0, std::min(255.0, lo));
-            hi = std::max(0.0, std::min(255.0, hi));
-            if (hi <= lo) {
-                if (hi < 255.0) hi = lo + 1.0;
-                else lo = hi - 1.0;
-            }
+            const double lo = std::floor(((double)cb[s]->lo[k] - (double)p[k]) / scale) - 1.0;
+            const double hi = std::ceil(((double)cb[s]->hi[k] - (double)p[k]) / scale) + 1.0;
+            if (lo < 0.0 || hi > 255.0) throw std::runtime_error("8-wide child box outside its node's range");
             qlo[k][s] = (uint8_t)lo;
             qhi[k][s] = (uint8_t)hi;
         }
     }
-    for (int k = 0; k < 3; k++) std::memcpy(&w[k], &nb.lo[k], 4);
+    for (int k = 0; k < 3; k++) std::memcpy(&w[k], &p[k], 4);
     w[3] = (uint32_t)eb[0] | (uint32_t)eb[1] << 8 | (uint32_t)eb[2] << 16 | (w[3] & 0xff000000u);
     auto pack = [](const uint8_t *q, uint32_t *dst) {
         dst[0] = q[0] | q[1] << 8 | q[2] << 16 | (uint32_t)q[3] << 24;
@@ -434,11 +441,12 @@ BvhPair build_bvh_pair(const float *tris, uint32_t n) {
             if (c < 0) continue;
             if (!is_leaf8(c)) {
                 imask |= 1u << s;
+                meta[s] = 1u << 5 | (24u + (uint32_t)s);   // one hit bit at 24 + slot
                 kids.push_back({child_base + j++, c, t.depth + 1});
             } else {
                 const uint32_t off = (uint32_t)order.size() - tri_base, cnt = sub_count[c];
                 if (cnt < 1 || cnt > 3 || off > 21) throw std::runtime_error("BVH8 leaf layout");
-                meta[s] = cnt << 5 | off;
+                meta[s] = ((1u << cnt) - 1u) << 5 | off;   // cnt hit bits from off
                 place_subtree(c, (uint32_t)order.size());
                 for (uint32_t k = 0; k < cnt; k++) order.push_back(T.order[sub_start[c] + k]);
             }
@@ -507,13 +515,15 @@ std::string check_bvh_pair(const BvhPair &P, const float *tris, uint32_t n) {
                 hi[k] = (double)p[k] + q(1, k, s) * scale[k];
             }
             if (imask >> s & 1u) {
+                if (m != (0x38u | (uint32_t)s)) return "8-wide internal child meta";
                 const uint32_t c = w[4] + j++;
                 if (c >= nw || node_ref[c]) return "8-wide child index out of range or shared";
                 node_ref[c] = 1;
                 Item ci{c, {lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}};
                 todo.push_back(ci);
             } else if (m) {
-                const uint32_t cnt = m >> 5, off = m & 31u;
+                const uint32_t cnt = (uint32_t)__builtin_popcount(m >> 5), off = m & 31u;
+                if ((m >> 5) != (1u << cnt) - 1u) return "8-wide leaf meta is not a unary count";
                 for (uint32_t k = 0; k < cnt; k++) {
                     const uint32_t pos = w[5] + off + k;
                     if (pos >= n || tri_ref[pos]) return "8-wide leaf triangle out of range or shared";

@@ -21,11 +21,14 @@ Bvh2 build_bvh2(const float *tris, uint32_t ntris, int max_leaf = 4);
 // "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs",
 // HPG 2017): 80 bytes = 20 words per node.
 //   w0..2  origin p (float bits), w3 = e.x | e.y << 8 | e.z << 16 | imask << 24
-//          (child boxes are p + q * 2^(e - 127) per axis, q in 0..255)
+//          (child boxes are p + q * 2^(e - 127) per axis, q in 0..255, padded
+//          by one step on every side)
 //   w4     index of the first internal child node (children are consecutive)
 //   w5     index of the node's first triangle (leaf children's triangles are consecutive)
-//   w6, w7 meta byte per child slot: leaf = count << 5 | offset (count 1..3,
-//          offset 0..23 from w5), 0 = internal or empty
+//   w6, w7 meta byte per child slot, bits << 5 | position: a hit sets `bits`
+//          at `position` of the node's hit word -- leaf: count ones at its
+//          first triangle's offset 0..21 from w5; internal: one bit at 24 +
+//          slot (the traversal XORs the slot with the ray octant); 0 = empty
 //   w8..19 q_lo.x[8], q_lo.y[8], q_lo.z[8], q_hi.x[8], q_hi.y[8], q_hi.z[8]
 // A child in slot s lies on the negative side of axis k when bit k of s is
 // set, so a ray visits children in the order s ^ (7 ^ octant) near first.

@@ -64,7 +64,9 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     L_.threads_shade = cfg_.threads_shade;
     L_.threads_shadow = cfg_.threads_extend;
     L_.threads_regen = 256;
-    auto grid = [&](int which, int threads) { return std::max(1, sm_count * std::max(1, wf_occupancy(which, threads))); };
+    auto grid = [&](int which, int threads) {
+        return std::max(1, sm_count * std::max(1, wf_occupancy(which, threads, S.accel)));
+    };
     L_.blocks_extend = grid(0, L_.threads_extend);
     L_.blocks_shade = grid(1, L_.threads_shade);
     L_.blocks_shadow = grid(2, L_.threads_shadow);

@@ -228,7 +228,8 @@ struct hk_scene {
     hk_scene_info info{};
     int margin_lo = 0, margin_hi = 0;
     int sm_count = 148;
-    int occupancy = 1;
+    int occupancy = 1;        // resident megakernel CTAs per SM for the traversed tree
+    int occupancy_of[2] = {1, 1};
     std::unique_ptr<hk::WfEngine> wf;   // wavefront engine (allocated on first use)
 };
 
@@ -555,7 +556,8 @@ void build_scene(hk_scene *s) {
     int dev = 0;
     HK_CUDA(cudaGetDevice(&dev));
     HK_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, dev));
-    s->occupancy = std::max(1, hk::render_occupancy(s->margin_lo, s->margin_hi));
+    for (int a = 0; a < 2; ++a) s->occupancy_of[a] = std::max(1, hk::render_occupancy(s->margin_lo, s->margin_hi, a));
+    s->occupancy = s->occupancy_of[D.accel];
     HK_CUDA(cudaGetLastError());
 
     hk_scene_info &I = s->info;
@@ -787,6 +789,7 @@ int hk_scene_set_accel(hk_scene *s, int32_t accel) {
         s->accel = accel;
         s->dev.accel = accel;
         s->info.accel = accel;
+        s->occupancy = s->occupancy_of[accel];
         s->wf.reset();   // the engine holds a copy of the device description
         return HK_OK;
     });

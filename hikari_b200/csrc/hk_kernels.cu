@@ -26,6 +26,7 @@ __device__ __forceinline__ uint32_t mesh_emitter(const DevScene &S, int mesh) { 
 // (reference: every bounce), NEE over all emitters, MIS state carried across
 // bounces, unweighted environment on BSDF-sampled misses, the EDiscrete
 // override and Eigen's |c| <= 1e-5 zero test on throughput and NEE values.
+template <int kAccel>
 __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, int rr_start, PathCounters &pc) {
     Hit hn;
     bool found_next = false;
@@ -34,12 +35,12 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
     int depth = 0;
     float w_ems = 1.0f, w_mats = 1.0f;
     const bool has_env = S.env_index >= 0;
-    LocalStack stk;
+    std::conditional_t<kAccel == kAccelBvh8, LocalStack, NoStack> stk;
     while (depth < depth_max) {
         if (depth == 0) {
             Hit h;
             pc.rays++;
-            if (!trace<false>(S, ray, h, pc.trav, stk)) {
+            if (!trace<kAccel, false>(S, ray, h, pc.trav, stk)) {
                 if (has_env && !S.force_background) { L = L + beta * env_eval(S, ray.d); break; }
                 return ld3(S.background);
             }
@@ -77,7 +78,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
                 sr.o = it.p; sr.d = er.p - it.p; sr.tmin = kRayEps; sr.tmax = 1.0f - kRayEps;
                 Hit sh;
                 pc.shadow++;
-                if (!trace<true>(S, sr, sh, pc.trav, stk)) {
+                if (!trace<kAccel, true>(S, sr, sh, pc.trav, stk)) {
                     BRec br;
                     br.wi = to_local(it.sh, ray.d * -1.0f);
                     br.wo = to_local(it.sh, er.wi);
@@ -107,7 +108,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
         beta = beta * F;
         if (is_zero(beta)) break;
         pc.rays++;
-        found_next = trace<false>(S, ray, hn, pc.trav, stk);
+        found_next = trace<kAccel, false>(S, ray, hn, pc.trav, stk);
         if (found_next) {
             post_intersect(S, hn, itn);
             const DevMesh &mn = S.meshes[itn.mesh];
@@ -164,6 +165,7 @@ __device__ __forceinline__ uint64_t mix_seed(uint64_t seed, uint64_t s0) {
     return z ^ (z >> 31);
 }
 
+template <int kAccel>
 __global__ void __launch_bounds__(kTileThreads) render_pathmis_kernel(DevScene S, RenderLaunch P) {
     extern __shared__ float tile[];
     __shared__ int s_item;
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(kTileThreads) render_pathmis_kernel(DevScene S
             for (int s = s0; s < s1; ++s) {
                 float px = (float)x + rng.nextf(), py = (float)y + rng.nextf();
                 Ray r = camera_ray(S, px, py);
-                V3 L = li_pathmis(S, rng, r, P.depth, P.rr_start, pc);
+                V3 L = li_pathmis<kAccel>(S, rng, r, P.depth, P.rr_start, pc);
                 if (!is_valid(L)) { ++dropped; continue; }
                 splat_shared(S, tile, tw, th, fx0, fy0, FW, FH, px, py, L);
             }
@@ -248,6 +250,7 @@ __global__ void film_resolve_kernel(const float *film, float *rgb, int W, int H,
 
 // Ray queries: rays are n x 8 floats (o, d, tmin, tmax).  Reported triangle
 // ids are the ORIGINAL global triangle indices (mesh order).
+template <int kAccel>
 __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int32_t *tri, float *t, float *u, float *v,
                                   int any_hit, unsigned long long *visit_counter) {
     TravStats ts;
@@ -260,8 +263,8 @@ __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int
         r.tmin = b.z;
         r.tmax = b.w;
         Hit h;
-        LocalStack stk;
-        bool f = any_hit ? trace<true>(S, r, h, ts, stk) : trace<false>(S, r, h, ts, stk);
+        std::conditional_t<kAccel == kAccelBvh8, LocalStack, NoStack> stk;
+        bool f = any_hit ? trace<kAccel, true>(S, r, h, ts, stk) : trace<kAccel, false>(S, r, h, ts, stk);
         if (any_hit) { tri[i] = f ? 1 : 0; continue; }
         tri[i] = f ? __float_as_int(__ldg(S.tris + 3 * h.tri).w) : -1;
         if (t) t[i] = f ? h.t : 0.0f;
@@ -385,7 +388,8 @@ static int grid_for(uint64_t n, int threads) {
 cudaError_t launch_render(const DevScene &S, const RenderLaunch &P, int grid, cudaStream_t st) {
     const int tw = kTile + P.margin_hi - P.margin_lo;
     size_t smem = (size_t)tw * tw * 4 * sizeof(float);
-    render_pathmis_kernel<<<grid, kTileThreads, smem, st>>>(S, P);
+    if (S.accel == kAccelBvh8) render_pathmis_kernel<kAccelBvh8><<<grid, kTileThreads, smem, st>>>(S, P);
+    else render_pathmis_kernel<kAccelBvh2><<<grid, kTileThreads, smem, st>>>(S, P);
     return cudaGetLastError();
 }
 cudaError_t launch_resolve(const float *film, float *rgb, int W, int H, int B, cudaStream_t st) {
@@ -395,7 +399,10 @@ cudaError_t launch_resolve(const float *film, float *rgb, int W, int H, int B, c
 }
 cudaError_t launch_trace(const DevScene &S, uint64_t n, const float *rays, int32_t *tri, float *t, float *u, float *v,
                          int any_hit, unsigned long long *visits, cudaStream_t st) {
-    trace_rays_kernel<<<grid_for(n, 128), 128, 0, st>>>(S, n, rays, tri, t, u, v, any_hit, visits);
+    if (S.accel == kAccelBvh8)
+        trace_rays_kernel<kAccelBvh8><<<grid_for(n, 128), 128, 0, st>>>(S, n, rays, tri, t, u, v, any_hit, visits);
+    else
+        trace_rays_kernel<kAccelBvh2><<<grid_for(n, 128), 128, 0, st>>>(S, n, rays, tri, t, u, v, any_hit, visits);
     return cudaGetLastError();
 }
 cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
@@ -416,10 +423,13 @@ cudaError_t launch_env_eval(const DevScene &S, uint64_t n, const float *wi, floa
     env_eval_kernel<<<grid_for(n, 128), 128, 0, st>>>(S, n, wi, out, pdf);
     return cudaGetLastError();
 }
-int render_occupancy(int margin_lo, int margin_hi) {
+int render_occupancy(int margin_lo, int margin_hi, int accel) {
     int n = 0;
     const int tw = kTile + margin_hi - margin_lo;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel, kTileThreads, (size_t)tw * tw * 16);
+    if (accel == kAccelBvh8)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel<kAccelBvh8>, kTileThreads, (size_t)tw * tw * 16);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel<kAccelBvh2>, kTileThreads, (size_t)tw * tw * 16);
     return n;
 }
 

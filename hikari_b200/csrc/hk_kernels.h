@@ -45,6 +45,6 @@ cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, uint64_t n, const flo
 cudaError_t launch_emitter_sample(const DevScene &S, int e, uint64_t n, const float *in, float *out, cudaStream_t st);
 cudaError_t launch_camera_rays(const DevScene &S, uint64_t n, const float *pos, float *out, cudaStream_t st);
 cudaError_t launch_env_eval(const DevScene &S, uint64_t n, const float *wi, float *out, float *pdf, cudaStream_t st);
-int render_occupancy(int margin_lo, int margin_hi);
+int render_occupancy(int margin_lo, int margin_hi, int accel);
 
 }  // namespace hk

@@ -11,6 +11,8 @@
 #include "hk_device.h"
 #include "hk_math.cuh"
 
+#include <type_traits>
+
 namespace hk {
 
 struct Ray {
@@ -251,12 +253,29 @@ struct SharedStack {
 
 __device__ __forceinline__ uint4 ldg4u(const uint4 *p) { return __ldg(p); }
 
+// Byte k of x as a float in [0, 255]: a byte permute builds the float
+// 2^23 + q (exponent byte 0x4B, q in the low mantissa byte), and subtracting
+// 2^23 is exact -- two full-rate instructions instead of an integer-to-float
+// conversion.
+template <int k>
+__device__ __forceinline__ float qbyte(uint32_t x) {
+    return __uint_as_float(__byte_perm(x, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
+}
+// The float 2^23 + q without the subtraction: the slab offsets of a node are
+// shifted by -2^23 steps instead (one rounding of at most half a step, which
+// the one-step padding of the quantised boxes absorbs).
+template <int k>
+__device__ __forceinline__ float qbyte_biased(uint32_t x) {
+    return __uint_as_float(__byte_perm(x, 0x4B000000u, 0x7440u | k));
+}
+
 template <bool kAnyHit, class Stack>
 __device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st, Stack &stk) {
     hit.tri = -1;
     if (S.nwnodes == 0) return false;
     const V3 d = ray.d;
-    const float tiny = 1e-30f;
+    // |1/d| <= 1e20 keeps 2^23 steps of up to 2^38 (the largest step the build emits) finite
+    const float tiny = 1e-20f;
     const V3 dd = v3(fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x, fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y,
                      fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z);
     const V3 idir = v3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
@@ -284,10 +303,14 @@ __device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hi
             const float adx = __uint_as_float((n0.w & 0xffu) << 23) * idir.x;
             const float ady = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * idir.y;
             const float adz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * idir.z;
-            const float ox = (__uint_as_float(n0.x) - ray.o.x) * idir.x;
-            const float oy = (__uint_as_float(n0.y) - ray.o.y) * idir.y;
-            const float oz = (__uint_as_float(n0.z) - ray.o.z) * idir.z;
+            const float ox = __fmaf_rn(-8388608.0f, adx, (__uint_as_float(n0.x) - ray.o.x) * idir.x);
+            const float oy = __fmaf_rn(-8388608.0f, ady, (__uint_as_float(n0.y) - ray.o.y) * idir.y);
+            const float oz = __fmaf_rn(-8388608.0f, adz, (__uint_as_float(n0.z) - ray.o.z) * idir.z);
             const uint32_t imask = n0.w >> 24;
+            // meta of internal children: slot ^ (7 ^ octant) in the position bits
+            const uint32_t in0 = ((imask & 0xfu) * 0x00204081u) & 0x01010101u;
+            const uint32_t in1 = ((imask >> 4) * 0x00204081u) & 0x01010101u;
+            const uint32_t meta0 = n1.z ^ (in0 * ko), meta1 = n1.w ^ (in1 * ko);
             // near / far planes per axis (lo planes first for a positive direction)
             const uint32_t nx0 = oct & 1u ? n3.z : n2.x, nx1 = oct & 1u ? n3.w : n2.y;
             const uint32_t fx0 = oct & 1u ? n2.x : n3.z, fx1 = oct & 1u ? n2.y : n3.w;
@@ -295,34 +318,33 @@ __device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hi
             const uint32_t fy0 = oct & 2u ? n2.z : n4.x, fy1 = oct & 2u ? n2.w : n4.y;
             const uint32_t nz0 = oct & 4u ? n4.z : n3.x, nz1 = oct & 4u ? n4.w : n3.y;
             const uint32_t fz0 = oct & 4u ? n3.x : n4.z, fz1 = oct & 4u ? n3.y : n4.w;
-            uint32_t hits_int = 0, hits_tri = 0;
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                const int sh = (c & 3) * 8;
-                const uint32_t qnx = ((c < 4 ? nx0 : nx1) >> sh) & 0xffu, qfx = ((c < 4 ? fx0 : fx1) >> sh) & 0xffu;
-                const uint32_t qny = ((c < 4 ? ny0 : ny1) >> sh) & 0xffu, qfy = ((c < 4 ? fy0 : fy1) >> sh) & 0xffu;
-                const uint32_t qnz = ((c < 4 ? nz0 : nz1) >> sh) & 0xffu, qfz = ((c < 4 ? fz0 : fz1) >> sh) & 0xffu;
-                const float tnx = __fmaf_rn((float)qnx, adx, ox), tfx = __fmaf_rn((float)qfx, adx, ox);
-                const float tny = __fmaf_rn((float)qny, ady, oy), tfy = __fmaf_rn((float)qfy, ady, oy);
-                const float tnz = __fmaf_rn((float)qnz, adz, oz), tfz = __fmaf_rn((float)qfz, adz, oz);
+            uint32_t hits = 0;
+            auto test_child = [&](auto kk, uint32_t xn, uint32_t xf, uint32_t yn, uint32_t yf, uint32_t zn, uint32_t zf,
+                                  uint32_t meta) {
+                constexpr int k = decltype(kk)::value;
+                const float tnx = __fmaf_rn(qbyte_biased<k>(xn), adx, ox), tfx = __fmaf_rn(qbyte_biased<k>(xf), adx, ox);
+                const float tny = __fmaf_rn(qbyte_biased<k>(yn), ady, oy), tfy = __fmaf_rn(qbyte_biased<k>(yf), ady, oy);
+                const float tnz = __fmaf_rn(qbyte_biased<k>(zn), adz, oz), tfz = __fmaf_rn(qbyte_biased<k>(zf), adz, oz);
                 const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, ray.tmin));
                 const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
-                if (tn <= tf * 1.00000024f + 1e-30f) {
-                    if (imask >> c & 1u) {
-                        hits_int |= 1u << (c ^ ko);
-                    } else {
-                        const uint32_t m = ((c < 4 ? n1.z : n1.w) >> sh) & 0xffu;
-                        hits_tri |= ((1u << (m >> 5)) - 1u) << (m & 31u);
-                    }
-                }
-            }
-            ng = make_uint2(n1.x, (hits_int << 24) | imask);
-            tg = make_uint2(n1.y, hits_tri);
+                const uint32_t m = __byte_perm(meta, 0u, 0x4440u | k);
+                if (tn <= tf * 1.00000024f + 1e-30f) hits |= (m >> 5) << (m & 31u);
+            };
+            test_child(std::integral_constant<int, 0>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
+            test_child(std::integral_constant<int, 1>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
+            test_child(std::integral_constant<int, 2>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
+            test_child(std::integral_constant<int, 3>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
+            test_child(std::integral_constant<int, 0>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
+            test_child(std::integral_constant<int, 1>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
+            test_child(std::integral_constant<int, 2>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
+            test_child(std::integral_constant<int, 3>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
+            ng = make_uint2(n1.x, (hits & 0xff000000u) | imask);
+            tg = make_uint2(n1.y, hits & 0x00ffffffu);
         } else {
             tg = ng;   // a postponed triangle group from the stack
             ng = make_uint2(0u, 0u);
         }
-        if (S.postpone) {
+        if (!kAnyHit && S.postpone) {   // a shadow ray wants any hit soon: it never postpones
             const unsigned act = __activemask();
             const unsigned want = __ballot_sync(act, tg.y != 0u);
             if (tg.y != 0u && ng.y > 0x00ffffffu && __popc(want) * 5 < __popc(act)) {
@@ -363,11 +385,17 @@ __device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hi
     return found;
 }
 
-// The scene's tree: closest hit (kAnyHit = false) or first hit.
-template <bool kAnyHit, class Stack>
+// Closest hit (kAnyHit = false) or first hit in the tree kAccel; kernels are
+// instantiated per tree and the host launches the scene's one.
+template <int kAccel, bool kAnyHit, class Stack>
 __device__ __forceinline__ bool trace(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st, Stack &stk) {
-    if (S.accel == kAccelBvh8) return trace_bvh8<kAnyHit>(S, ray, hit, st, stk);
-    return trace_bvh2<kAnyHit>(S, ray, hit, st);
+    if constexpr (kAccel == kAccelBvh8) return trace_bvh8<kAnyHit>(S, ray, hit, st, stk);
+    else return trace_bvh2<kAnyHit>(S, ray, hit, st);
 }
+
+// Stack type of a tree's traversal (the binary traversal keeps its own).
+struct NoStack {
+    int sp = 0;
+};
 
 }  // namespace hk

@@ -219,10 +219,12 @@ __device__ __forceinline__ SharedStack make_stack() {
     return s;
 }
 
+template <int kAccel>
 __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, int cur) {
     const int n = (int)W.ctr->eq_count[cur];
     TravStats ts;
-    SharedStack stk = make_stack();
+    std::conditional_t<kAccel == kAccelBvh8, SharedStack, NoStack> stk;
+    if constexpr (kAccel == kAccelBvh8) stk = make_stack();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = W.eq[cur][i];
         float4 o = W.ray_o[slot], d = W.ray_d[slot];
@@ -233,7 +235,7 @@ __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, i
         r.tmax = d.w;
         Hit h;
         int type = 0;
-        if (trace<false>(S, r, h, ts, stk)) {
+        if (trace<kAccel, false>(S, r, h, ts, stk)) {
             int mesh = __float_as_int(__ldg(S.tris + 3 * h.tri + 1).w);
             type = S.bsdfs[S.meshes[mesh].bsdf].type + 1;
         }
@@ -390,10 +392,12 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
 }
 
 // ------------------------------------------------------------ shadow
+template <int kAccel>
 __global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
     const int n = min((int)W.ctr->shadow_count, W.max_shadow);
     TravStats ts;
-    SharedStack stk = make_stack();
+    std::conditional_t<kAccel == kAccelBvh8, SharedStack, NoStack> stk;
+    if constexpr (kAccel == kAccelBvh8) stk = make_stack();
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 o = W.sh_o[i], d = W.sh_d[i];
         Ray r;
@@ -402,7 +406,7 @@ __global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
         r.tmin = kRayEps;
         r.tmax = 1.0f - kRayEps;
         Hit h;
-        if (!trace<true>(S, r, h, ts, stk)) {
+        if (!trace<kAccel, true>(S, r, h, ts, stk)) {
             float4 c = W.sh_c[i];
             red_add_v4(W.lacc + __float_as_int(o.w), c.x, c.y, c.z, 0.0f);
         }
@@ -434,6 +438,19 @@ __global__ void wf_counters_add_kernel(const WfCounters *c, unsigned long long *
 // ------------------------------------------------------------ launchers
 static size_t stack_smem(int threads) { return (size_t)threads * kShStack * sizeof(uint2); }
 
+static void launch_extend(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
+    if (S.accel == kAccelBvh8)
+        wf_extend_kernel<kAccelBvh8><<<C.blocks_extend, C.threads_extend, stack_smem(C.threads_extend), st>>>(S, W, cur);
+    else
+        wf_extend_kernel<kAccelBvh2><<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur);
+}
+static void launch_shadow(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
+    if (S.accel == kAccelBvh8)
+        wf_shadow_kernel<kAccelBvh8><<<C.blocks_shadow, C.threads_shadow, stack_smem(C.threads_shadow), st>>>(S, W);
+    else
+        wf_shadow_kernel<kAccelBvh2><<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W);
+}
+
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st) {
     wf_counters_add_kernel<<<1, 32, 0, st>>>(W.ctr, out);
     return cudaGetLastError();
@@ -448,14 +465,14 @@ cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLau
     const int nxt = cur ^ 1;
     wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur);
     wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
-    wf_extend_kernel<<<C.blocks_extend, C.threads_extend, stack_smem(C.threads_extend), st>>>(S, W, cur);
+    launch_extend(S, W, C, cur, st);
     wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<1><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<2><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<3><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-    wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, stack_smem(C.threads_shadow), st>>>(S, W);
+    launch_shadow(S, W, C, st);
     return cudaGetLastError();
 }
 
@@ -467,7 +484,7 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
         wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur);
         wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
         break;
-    case 1: wf_extend_kernel<<<C.blocks_extend, C.threads_extend, stack_smem(C.threads_extend), st>>>(S, W, cur); break;
+    case 1: launch_extend(S, W, C, cur, st); break;
     case 2:
         wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         wf_shade_kernel<1><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
@@ -476,17 +493,24 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
         wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         break;
-    default: wf_shadow_kernel<<<C.blocks_shadow, C.threads_shadow, stack_smem(C.threads_shadow), st>>>(S, W); break;
+    default: launch_shadow(S, W, C, st); break;
     }
     return cudaGetLastError();
 }
 
-int wf_occupancy(int which, int threads) {
+int wf_occupancy(int which, int threads, int accel) {
     int n = 0;
+    const bool w8 = accel == kAccelBvh8;
     switch (which) {
-    case 0: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel, threads, stack_smem(threads)); break;
+    case 0:
+        if (w8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccelBvh8>, threads, stack_smem(threads));
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccelBvh2>, threads, 0);
+        break;
     case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade_kernel<5>, threads, 0); break;
-    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel, threads, stack_smem(threads)); break;
+    case 2:
+        if (w8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccelBvh8>, threads, stack_smem(threads));
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccelBvh2>, threads, 0);
+        break;
     default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_regen_kernel, threads, 0); break;
     }
     return n;

@@ -114,6 +114,6 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
                             cudaStream_t st);
 // out[0..6] += rays, shadow rays, dropped, node visits, triangle tests, shadow node visits, shadow tests
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st);
-int wf_occupancy(int which, int threads);
+int wf_occupancy(int which, int threads, int accel);
 
 }  // namespace hk
