@@ -402,6 +402,12 @@ def main():
             basis = f"{phases[dom]} kernels: path-state bytes (144 B per shaded vertex) per launch"
         achieved = bytes_per_launch / max(avg_s, 1e-12) / 1e9
         launches_per_step = int(kl.sum()) + 1
+        rays_c, rays_s = max(pcn[0], 1.0), max(pcn[1], 1.0)
+        traversal = {"closest": {"node_visits_per_ray": pcn[3] / rays_c, "tri_tests_per_ray": pcn[4] / rays_c,
+                                 "ns_per_ray": float(kms[1]) * 1e6 / rays_c},
+                     "shadow": {"node_visits_per_ray": pcn[5] / rays_s, "tri_tests_per_ray": pcn[6] / rays_s,
+                                "ns_per_ray": float(kms[3]) * 1e6 / rays_s},
+                     "node_bytes": node_b, "tri_bytes": 48}
         phase_share = {p: round(float(kms[i] / kms.sum()), 4) for i, p in enumerate(phases)}
     else:
         n_launch = args.steps * V
@@ -411,6 +417,7 @@ def main():
                  f"test) / mean kernel time")
         launches_per_step = V
         phase_share = None
+        traversal = None
 
     # end to end through the C ABI: host images out, per-view camera pose in
     e2e_value = None
@@ -484,6 +491,7 @@ def main():
         "mrays_per_s": mrays,
         "rays_per_path": rays / paths_rank,
         "phase_share": phase_share,
+        "traversal": traversal,
         "plain_megakernel": plain,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None, "peak_kind": peak_kind, "basis": basis},

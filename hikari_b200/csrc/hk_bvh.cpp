@@ -264,27 +264,73 @@ void subtree_ranges(const std::vector<BNode> &nodes, int32_t root, std::vector<u
     }
 }
 
-// Children of binary node i opened greedily (largest surface area first) up
-// to 8 subtrees; subtrees of at most 3 triangles stay closed (8-wide leaves).
-int open_children(const std::vector<BNode> &nodes, const std::vector<uint32_t> &count, int32_t i, int32_t C[8]) {
-    int n = 0;
-    C[n++] = nodes[i].left;
-    C[n++] = nodes[i].right;
-    while (n < 8) {
-        int best = -1;
-        float best_a = -1.0f;
-        for (int k = 0; k < n; k++)
-            if (nodes[C[k]].left >= 0 && count[C[k]] > 3 && nodes[C[k]].box.area() > best_a) {
-                best_a = nodes[C[k]].box.area();
-                best = k;
+// Collapse by dynamic programming over the binary tree (Ylitie, Karras and
+// Laine, HPG 2017, section 3.1): cost(n, i) is the least SAH cost of the
+// subtree n when it may occupy at most i child slots of its parent -- as one
+// leaf (at most 3 triangles, area * c_prim * count), as one 8-wide node (area
+// * c_node + the best split of its two children over 8 slots), or, for i >= 2,
+// split between its children.  The tree's nodes are numbered parents first,
+// so a reverse sweep visits children before parents.
+struct Collapse {
+    static constexpr float kNode = 1.0f, kPrim = 0.3f;
+    std::vector<float> cost;         // 8 per node: cost(n, 1..8)
+    std::vector<int8_t> split;       // 8 per node: 0 = one child, k = k slots to the left subtree
+    std::vector<uint8_t> as_leaf;    // cost(n, 1) is the leaf option
+    std::vector<int8_t> node_split;  // slots to the left child when n is an 8-wide node
+
+    Collapse(const std::vector<BNode> &nodes, const std::vector<uint32_t> &count) {
+        const size_t N = nodes.size();
+        cost.assign(8 * N, 0.0f);
+        split.assign(8 * N, 0);
+        as_leaf.assign(N, 0);
+        node_split.assign(N, 0);
+        for (size_t q = N; q-- > 0;) {
+            const BNode &nd = nodes[q];
+            const float area = std::max(nd.box.area(), 0.0f);
+            const float leaf = count[q] <= 3 ? area * kPrim * (float)count[q] : INFINITY;
+            float *C = &cost[8 * q];
+            if (nd.left < 0) {
+                for (int i = 0; i < 8; i++) C[i] = leaf;
+                as_leaf[q] = 1;
+                continue;
             }
-        if (best < 0) break;
-        int32_t x = C[best];
-        C[best] = nodes[x].left;
-        C[n++] = nodes[x].right;
+            const float *L = &cost[8 * (size_t)nd.left], *R = &cost[8 * (size_t)nd.right];
+            float dist[9];
+            int arg[9];
+            for (int j = 2; j <= 8; j++) {
+                dist[j] = INFINITY;
+                arg[j] = 1;
+                for (int k = 1; k < j; k++) {
+                    const float c = L[k - 1] + R[j - k - 1];
+                    if (c < dist[j]) { dist[j] = c; arg[j] = k; }
+                }
+            }
+            const float node = area * kNode + dist[8];
+            node_split[q] = (int8_t)arg[8];
+            C[0] = std::min(leaf, node);
+            as_leaf[q] = leaf <= node ? 1 : 0;
+            for (int i = 2; i <= 8; i++) {
+                if (dist[i] < C[0]) { C[i - 1] = dist[i]; split[8 * q + i - 1] = (int8_t)arg[i]; }
+                else C[i - 1] = C[0];
+            }
+        }
     }
-    return n;
-}
+    // Subtrees that fill at most i slots for subtree q.
+    void collect(const std::vector<BNode> &nodes, int32_t q, int i, int32_t *out, int &n) const {
+        const int k = split[8 * (size_t)q + i - 1];
+        if (k == 0) { out[n++] = q; return; }
+        collect(nodes, nodes[q].left, k, out, n);
+        collect(nodes, nodes[q].right, i - k, out, n);
+    }
+    // Children of the 8-wide node made from binary node q.
+    int children(const std::vector<BNode> &nodes, int32_t q, int32_t C[8]) const {
+        int n = 0;
+        const int k = node_split[q];
+        collect(nodes, nodes[q].left, k, C, n);
+        collect(nodes, nodes[q].right, 8 - k, C, n);
+        return n;
+    }
+};
 
 // Slot s means "negative side of axis k" for every set bit k; children are
 // assigned greedily by the score of their centre offset along that diagonal.
@@ -387,7 +433,8 @@ BvhPair build_bvh_pair(const float *tris, uint32_t n) {
     const std::vector<BNode> &nodes = T.nodes;
     std::vector<uint32_t> sub_start, sub_count;
     subtree_ranges(nodes, T.root, sub_start, sub_count);
-    auto is_leaf8 = [&](int32_t c) { return nodes[c].left < 0 || sub_count[c] <= 3; };
+    const Collapse dp(nodes, sub_count);
+    auto is_leaf8 = [&](int32_t c) { return dp.as_leaf[c] != 0; };
     // new position of every binary leaf's first triangle
     std::vector<uint32_t> leaf_start(nodes.size(), 0);
     auto place_subtree = [&](int32_t c, uint32_t base) {
@@ -421,7 +468,7 @@ BvhPair build_bvh_pair(const float *tris, uint32_t n) {
             C[0] = t.b;
             nc = 1;
         } else {
-            nc = open_children(nodes, sub_count, t.b, C);
+            nc = dp.children(nodes, t.b, C);
         }
         int32_t slot_child[8];
         assign_slots(nodes, nodes[t.b].box, C, nc, slot_child);

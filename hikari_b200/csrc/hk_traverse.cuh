@@ -107,6 +107,18 @@ __device__ __forceinline__ bool refine_mt(V3 o, V3 d, V3 p0, V3 p1, V3 p2, float
     return true;
 }
 
+// Three-input min / max (PTX min.f32 / max.f32 with three sources, sm_100a).
+__device__ __forceinline__ float fmax3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float fmin3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Slab test of two child boxes against the ray interval; explicit FMAs (the
 // result only prunes, it never changes which triangle is reported).
 __device__ __forceinline__ void box2(const float4 a, const float4 b, const float4 c, V3 idir, V3 ood, float tmin,
@@ -117,10 +129,10 @@ __device__ __forceinline__ void box2(const float4 a, const float4 b, const float
     float c1loy = __fmaf_rn(b.z, idir.y, -ood.y), c1hiy = __fmaf_rn(b.w, idir.y, -ood.y);
     float c0loz = __fmaf_rn(c.x, idir.z, -ood.z), c0hiz = __fmaf_rn(c.y, idir.z, -ood.z);
     float c1loz = __fmaf_rn(c.z, idir.z, -ood.z), c1hiz = __fmaf_rn(c.w, idir.z, -ood.z);
-    float n0 = fmaxf(fmaxf(fminf(c0lox, c0hix), fminf(c0loy, c0hiy)), fmaxf(fminf(c0loz, c0hiz), tmin));
-    float f0 = fminf(fminf(fmaxf(c0lox, c0hix), fmaxf(c0loy, c0hiy)), fminf(fmaxf(c0loz, c0hiz), tmax));
-    float n1 = fmaxf(fmaxf(fminf(c1lox, c1hix), fminf(c1loy, c1hiy)), fmaxf(fminf(c1loz, c1hiz), tmin));
-    float f1 = fminf(fminf(fmaxf(c1lox, c1hix), fmaxf(c1loy, c1hiy)), fminf(fmaxf(c1loz, c1hiz), tmax));
+    float n0 = fmax3f(fminf(c0lox, c0hix), fminf(c0loy, c0hiy), fmaxf(fminf(c0loz, c0hiz), tmin));
+    float f0 = fmin3f(fmaxf(c0lox, c0hix), fmaxf(c0loy, c0hiy), fminf(fmaxf(c0loz, c0hiz), tmax));
+    float n1 = fmax3f(fminf(c1lox, c1hix), fminf(c1loy, c1hiy), fmaxf(fminf(c1loz, c1hiz), tmin));
+    float f1 = fmin3f(fmaxf(c1lox, c1hix), fmaxf(c1loy, c1hiy), fminf(fmaxf(c1loz, c1hiz), tmax));
     // slack of a few ulps keeps boxes of axis-aligned, zero-thickness geometry
     hit0 = n0 <= f0 * 1.00000024f + 1e-30f;
     hit1 = n1 <= f1 * 1.00000024f + 1e-30f;
@@ -325,8 +337,8 @@ __device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hi
                 const float tnx = __fmaf_rn(qbyte_biased<k>(xn), adx, ox), tfx = __fmaf_rn(qbyte_biased<k>(xf), adx, ox);
                 const float tny = __fmaf_rn(qbyte_biased<k>(yn), ady, oy), tfy = __fmaf_rn(qbyte_biased<k>(yf), ady, oy);
                 const float tnz = __fmaf_rn(qbyte_biased<k>(zn), adz, oz), tfz = __fmaf_rn(qbyte_biased<k>(zf), adz, oz);
-                const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, ray.tmin));
-                const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+                const float tn = fmax3f(tnx, tny, fmaxf(tnz, ray.tmin));
+                const float tf = fmin3f(tfx, tfy, fminf(tfz, tmax));
                 const uint32_t m = __byte_perm(meta, 0u, 0x4440u | k);
                 if (tn <= tf * 1.00000024f + 1e-30f) hits |= (m >> 5) << (m & 31u);
             };
