@@ -35,12 +35,11 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
     int depth = 0;
     float w_ems = 1.0f, w_mats = 1.0f;
     const bool has_env = S.env_index >= 0;
-    std::conditional_t<kAccel == kAccelBvh8, LocalStack, NoStack> stk;
     while (depth < depth_max) {
         if (depth == 0) {
             Hit h;
             pc.rays++;
-            if (!trace<kAccel, false>(S, ray, h, pc.trav, stk)) {
+            if (!trace<kAccel, false>(S, ray, h, pc.trav)) {
                 if (has_env && !S.force_background) { L = L + beta * env_eval(S, ray.d); break; }
                 return ld3(S.background);
             }
@@ -78,7 +77,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
                 sr.o = it.p; sr.d = er.p - it.p; sr.tmin = kRayEps; sr.tmax = 1.0f - kRayEps;
                 Hit sh;
                 pc.shadow++;
-                if (!trace<kAccel, true>(S, sr, sh, pc.trav, stk)) {
+                if (!trace<kAccel, true>(S, sr, sh, pc.trav)) {
                     BRec br;
                     br.wi = to_local(it.sh, ray.d * -1.0f);
                     br.wo = to_local(it.sh, er.wi);
@@ -108,7 +107,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
         beta = beta * F;
         if (is_zero(beta)) break;
         pc.rays++;
-        found_next = trace<kAccel, false>(S, ray, hn, pc.trav, stk);
+        found_next = trace<kAccel, false>(S, ray, hn, pc.trav);
         if (found_next) {
             post_intersect(S, hn, itn);
             const DevMesh &mn = S.meshes[itn.mesh];
@@ -263,8 +262,7 @@ __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int
         r.tmin = b.z;
         r.tmax = b.w;
         Hit h;
-        std::conditional_t<kAccel == kAccelBvh8, LocalStack, NoStack> stk;
-        bool f = any_hit ? trace<kAccel, true>(S, r, h, ts, stk) : trace<kAccel, false>(S, r, h, ts, stk);
+        bool f = any_hit ? trace<kAccel, true>(S, r, h, ts) : trace<kAccel, false>(S, r, h, ts);
         if (any_hit) { tri[i] = f ? 1 : 0; continue; }
         tri[i] = f ? __float_as_int(__ldg(S.tris + 3 * h.tri).w) : -1;
         if (t) t[i] = f ? h.t : 0.0f;

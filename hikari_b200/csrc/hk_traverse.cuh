@@ -146,37 +146,52 @@ struct TravStats {
     uint32_t nodes = 0, tris = 0;
 };
 
-// Closest hit (any_hit = false) or first hit (any_hit = true).
-template <bool kAnyHit>
-__device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st) {
-    hit.tri = -1;
-    if (S.nnodes == 0) return false;
-    V3 d = ray.d;
-    // zero components -> tiny signed values: inverse stays finite, no 0*inf NaN
-    const float tiny = 1e-30f;
-    V3 dd = v3(fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x, fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y,
-               fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z);
-    V3 idir = v3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
-    V3 ood = v3(ray.o.x * idir.x, ray.o.y * idir.y, ray.o.z * idir.z);
-    WatertightRay w = watertight_setup(d);
-    float tmax = ray.tmax;
-    int stack[kStackSize];
-    int sp = 0;
-    int node = 0;
-    uint32_t nvis = 0, ntri = 0;
-    bool found = false;
-    // root: test the root's own children; a single-leaf tree is stored as a
-    // root whose child0 is the leaf and child1 an empty box.
-    for (;;) {
+// Binary-tree traversal as a resumable walker: begin() sets a ray up, each
+// step() visits one node (box test of both children, leaf triangles tested
+// at once, near child next, far child pushed) and returns true when the ray
+// is done; end() adds the statistics and re-evaluates the closest hit with the
+// reference's arithmetic.  A single-leaf tree is stored as a root whose child0
+// is the leaf and child1 an empty box.
+struct Bvh2Walker {
+    V3 o, d, idir, ood;
+    float tmin, tmax, tmax0;
+    WatertightRay w;
+    int node, sp;
+    bool found;
+    Hit hit;
+    uint32_t nvis, ntri;
+    int *stack;   // kStackSize entries owned by the caller (kept out of the walker so it stays in registers)
+
+    __device__ __forceinline__ void begin(const DevScene &S, const Ray &ray) {
+        o = ray.o;
+        d = ray.d;
+        // zero components -> tiny signed values: inverse stays finite, no 0*inf NaN
+        const float tiny = 1e-30f;
+        const V3 dd = v3(fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x, fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y,
+                         fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z);
+        idir = v3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+        ood = v3(o.x * idir.x, o.y * idir.y, o.z * idir.z);
+        w = watertight_setup(d);
+        tmin = ray.tmin;
+        tmax = tmax0 = ray.tmax;
+        node = S.nnodes == 0 ? -1 : 0;
+        sp = 0;
+        found = false;
+        hit.tri = -1;
+        nvis = ntri = 0;
+    }
+
+    template <bool kAnyHit>
+    __device__ __forceinline__ bool step(const DevScene &S) {
+        if (node < 0) return true;
         const float4 *np = S.nodes + 4 * node;
-        float4 a = ldg4(np), b = ldg4(np + 1), c = ldg4(np + 2), e = ldg4(np + 3);
-        int c0 = __float_as_int(e.x), c1 = __float_as_int(e.y);
+        const float4 a = ldg4(np), b = ldg4(np + 1), c = ldg4(np + 2), e = ldg4(np + 3);
+        const int c0 = __float_as_int(e.x), c1 = __float_as_int(e.y);
         ++nvis;
         bool h0, h1;
         float t0, t1;
-        box2(a, b, c, idir, ood, ray.tmin, tmax, h0, h1, t0, t1);
+        box2(a, b, c, idir, ood, tmin, tmax, h0, h1, t0, t1);
         int next = -0x7fffffff;   // sentinel: pop
-        // visit leaves immediately; push/choose internal children near-first
         int leafs[2];
         int nleaf = 0;
         int inner[2];
@@ -185,43 +200,59 @@ __device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hi
         if (h0) { if (c0 < 0) leafs[nleaf++] = c0; else { inner[ninner] = c0; tin[ninner++] = t0; } }
         if (h1) { if (c1 < 0) leafs[nleaf++] = c1; else { inner[ninner] = c1; tin[ninner++] = t1; } }
         for (int l = 0; l < nleaf; ++l) {
-            uint32_t enc = ~(uint32_t)leafs[l];
-            uint32_t start = enc & kLeafStartMask, cnt = enc >> kLeafCountShift;
+            const uint32_t enc = ~(uint32_t)leafs[l];
+            const uint32_t start = enc & kLeafStartMask, cnt = enc >> kLeafCountShift;
             ntri += cnt;
             for (uint32_t i = 0; i < cnt; ++i) {
                 const float4 *tp = S.tris + 3 * (start + i);
-                float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
+                const float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
                 float tt, uu, vv;
-                if (intersect_watertight(w, ray.o, xyz(p0), xyz(p1), xyz(p2), ray.tmin, tmax, tt, uu, vv)) {
+                if (intersect_watertight(w, o, xyz(p0), xyz(p1), xyz(p2), tmin, tmax, tt, uu, vv)) {
                     found = true;
                     hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)(start + i);
-                    if (kAnyHit) { st.nodes += nvis; st.tris += ntri; return true; }
+                    if (kAnyHit) return true;
                     tmax = tt;
                 }
             }
         }
         if (ninner == 2) {
-            bool swap = tin[1] < tin[0];
-            int nearc = swap ? inner[1] : inner[0], farc = swap ? inner[0] : inner[1];
+            const bool swap = tin[1] < tin[0];
+            const int nearc = swap ? inner[1] : inner[0], farc = swap ? inner[0] : inner[1];
             if (sp < kStackSize) stack[sp++] = farc;
             next = nearc;
         } else if (ninner == 1) {
             next = inner[0];
         }
         if (next == -0x7fffffff) {
-            if (sp == 0) break;
+            if (sp == 0) return true;
             next = stack[--sp];
         }
         node = next;
+        return false;
     }
-    st.nodes += nvis;
-    st.tris += ntri;
-    if (found && !kAnyHit) {
-        const float4 *tp = S.tris + 3 * hit.tri;
-        refine_mt(ray.o, ray.d, xyz(ldg4(tp)), xyz(ldg4(tp + 1)), xyz(ldg4(tp + 2)), ray.tmin, ray.tmax, hit.t, hit.u,
-                  hit.v);
+
+    template <bool kAnyHit>
+    __device__ __forceinline__ void end(const DevScene &S, TravStats &st) {
+        st.nodes += nvis;
+        st.tris += ntri;
+        if (found && !kAnyHit) {
+            const float4 *tp = S.tris + 3 * hit.tri;
+            refine_mt(o, d, xyz(ldg4(tp)), xyz(ldg4(tp + 1)), xyz(ldg4(tp + 2)), tmin, tmax0, hit.t, hit.u, hit.v);
+        }
     }
-    return found;
+};
+
+// Closest hit (any_hit = false) or first hit (any_hit = true).
+template <bool kAnyHit>
+__device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st) {
+    int stack[kStackSize];
+    Bvh2Walker wk;
+    wk.stack = stack;
+    wk.begin(S, ray);
+    while (!wk.template step<kAnyHit>(S)) {}
+    wk.template end<kAnyHit>(S, st);
+    hit = wk.hit;
+    return wk.found;
 }
 
 // ------------------------------------------------------------ 8-wide tree
@@ -235,9 +266,9 @@ __device__ __forceinline__ bool trace_bvh2(const DevScene &S, const Ray &ray, Hi
 
 constexpr int kShStack = 8;   // entries per thread kept in shared memory
 
-// Traversal stack entirely in registers/local memory.
+// Traversal stack in local memory (e: kStackSize entries owned by the caller).
 struct LocalStack {
-    uint2 e[kStackSize];
+    uint2 *e;
     int sp = 0;
     // The tree depth bound keeps sp below kStackSize; past it an entry would be dropped, never written out of bounds.
     __device__ __forceinline__ void push(uint2 v) {
@@ -252,7 +283,7 @@ struct SharedStack {
     uint2 *sh;
     int stride;
     int sp = 0;
-    uint2 spill[kStackSize - kShStack];
+    uint2 *spill;   // kStackSize - kShStack entries in local memory, owned by the caller
     __device__ __forceinline__ void push(uint2 v) {
         if (sp < kShStack) sh[sp++ * stride] = v;
         else if (sp < kStackSize) { spill[sp - kShStack] = v; ++sp; }
@@ -281,79 +312,52 @@ __device__ __forceinline__ float qbyte_biased(uint32_t x) {
     return __uint_as_float(__byte_perm(x, 0x4B000000u, 0x7440u | k));
 }
 
-template <bool kAnyHit, class Stack>
-__device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st, Stack &stk) {
-    hit.tri = -1;
-    if (S.nwnodes == 0) return false;
-    const V3 d = ray.d;
-    // |1/d| <= 1e20 keeps 2^23 steps of up to 2^38 (the largest step the build emits) finite
-    const float tiny = 1e-20f;
-    const V3 dd = v3(fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x, fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y,
-                     fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z);
-    const V3 idir = v3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
-    const uint32_t oct = (idir.x < 0.0f ? 1u : 0u) | (idir.y < 0.0f ? 2u : 0u) | (idir.z < 0.0f ? 4u : 0u);
-    const uint32_t ko = 7u ^ oct;
-    const WatertightRay w = watertight_setup(d);
-    float tmax = ray.tmax;
-    uint2 ng = make_uint2(0u, (1u << (24 + ko)) | 1u);   // the root as slot 0 of a virtual parent
-    uint2 tg = make_uint2(0u, 0u);
-    stk.sp = 0;
-    bool found = false;
-    uint32_t nvis = 0, ntri = 0;
-    for (;;) {
+template <class Stack>
+struct Bvh8Walker {
+    V3 o, d, idir;
+    float tmin, tmax, tmax0;
+    WatertightRay w;
+    uint32_t oct, ko;
+    uint2 ng, tg;
+    bool found;
+    Hit hit;
+    uint32_t nvis, ntri;
+    Stack stk;
+
+    __device__ __forceinline__ void begin(const DevScene &S, const Ray &ray) {
+        o = ray.o;
+        d = ray.d;
+        // |1/d| <= 1e20 keeps 2^23 steps of up to 2^38 (the largest step the build emits) finite
+        const float tiny = 1e-20f;
+        const V3 dd = v3(fabsf(d.x) < tiny ? copysignf(tiny, d.x) : d.x, fabsf(d.y) < tiny ? copysignf(tiny, d.y) : d.y,
+                         fabsf(d.z) < tiny ? copysignf(tiny, d.z) : d.z);
+        idir = v3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+        oct = (idir.x < 0.0f ? 1u : 0u) | (idir.y < 0.0f ? 2u : 0u) | (idir.z < 0.0f ? 4u : 0u);
+        ko = 7u ^ oct;
+        w = watertight_setup(d);
+        tmin = ray.tmin;
+        tmax = tmax0 = ray.tmax;
+        // the root as slot 0 of a virtual parent (nothing for an empty tree)
+        ng = make_uint2(0u, S.nwnodes == 0 ? 0u : ((1u << (24 + ko)) | 1u));
+        tg = make_uint2(0u, 0u);
+        stk.sp = 0;
+        found = false;
+        hit.tri = -1;
+        nvis = ntri = 0;
+    }
+
+    // One node visit (or one popped triangle group) and its triangle tests.
+    template <bool kAnyHit>
+    __device__ __forceinline__ bool step(const DevScene &S) {
         if (ng.y > 0x00ffffffu) {
             const uint32_t b = __ffs(ng.y >> 24) - 1;
             ng.y &= ~(1u << (24 + b));
             const uint32_t slot = b ^ ko;
             const uint32_t child = ng.x + __popc(ng.y & 0xffu & ((1u << slot) - 1u));
             if (ng.y > 0x00ffffffu) stk.push(ng);
-            // ---- intersect the 8 children of node `child`
-            const uint4 *np = S.wnodes + 5 * (size_t)child;
-            const uint4 n0 = ldg4u(np), n1 = ldg4u(np + 1), n2 = ldg4u(np + 2), n3 = ldg4u(np + 3),
-                        n4 = ldg4u(np + 4);
-            ++nvis;
-            const float adx = __uint_as_float((n0.w & 0xffu) << 23) * idir.x;
-            const float ady = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * idir.y;
-            const float adz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * idir.z;
-            const float ox = __fmaf_rn(-8388608.0f, adx, (__uint_as_float(n0.x) - ray.o.x) * idir.x);
-            const float oy = __fmaf_rn(-8388608.0f, ady, (__uint_as_float(n0.y) - ray.o.y) * idir.y);
-            const float oz = __fmaf_rn(-8388608.0f, adz, (__uint_as_float(n0.z) - ray.o.z) * idir.z);
-            const uint32_t imask = n0.w >> 24;
-            // meta of internal children: slot ^ (7 ^ octant) in the position bits
-            const uint32_t in0 = ((imask & 0xfu) * 0x00204081u) & 0x01010101u;
-            const uint32_t in1 = ((imask >> 4) * 0x00204081u) & 0x01010101u;
-            const uint32_t meta0 = n1.z ^ (in0 * ko), meta1 = n1.w ^ (in1 * ko);
-            // near / far planes per axis (lo planes first for a positive direction)
-            const uint32_t nx0 = oct & 1u ? n3.z : n2.x, nx1 = oct & 1u ? n3.w : n2.y;
-            const uint32_t fx0 = oct & 1u ? n2.x : n3.z, fx1 = oct & 1u ? n2.y : n3.w;
-            const uint32_t ny0 = oct & 2u ? n4.x : n2.z, ny1 = oct & 2u ? n4.y : n2.w;
-            const uint32_t fy0 = oct & 2u ? n2.z : n4.x, fy1 = oct & 2u ? n2.w : n4.y;
-            const uint32_t nz0 = oct & 4u ? n4.z : n3.x, nz1 = oct & 4u ? n4.w : n3.y;
-            const uint32_t fz0 = oct & 4u ? n3.x : n4.z, fz1 = oct & 4u ? n3.y : n4.w;
-            uint32_t hits = 0;
-            auto test_child = [&](auto kk, uint32_t xn, uint32_t xf, uint32_t yn, uint32_t yf, uint32_t zn, uint32_t zf,
-                                  uint32_t meta) {
-                constexpr int k = decltype(kk)::value;
-                const float tnx = __fmaf_rn(qbyte_biased<k>(xn), adx, ox), tfx = __fmaf_rn(qbyte_biased<k>(xf), adx, ox);
-                const float tny = __fmaf_rn(qbyte_biased<k>(yn), ady, oy), tfy = __fmaf_rn(qbyte_biased<k>(yf), ady, oy);
-                const float tnz = __fmaf_rn(qbyte_biased<k>(zn), adz, oz), tfz = __fmaf_rn(qbyte_biased<k>(zf), adz, oz);
-                const float tn = fmax3f(tnx, tny, fmaxf(tnz, ray.tmin));
-                const float tf = fmin3f(tfx, tfy, fminf(tfz, tmax));
-                const uint32_t m = __byte_perm(meta, 0u, 0x4440u | k);
-                if (tn <= tf * 1.00000024f + 1e-30f) hits |= (m >> 5) << (m & 31u);
-            };
-            test_child(std::integral_constant<int, 0>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
-            test_child(std::integral_constant<int, 1>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
-            test_child(std::integral_constant<int, 2>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
-            test_child(std::integral_constant<int, 3>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
-            test_child(std::integral_constant<int, 0>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
-            test_child(std::integral_constant<int, 1>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
-            test_child(std::integral_constant<int, 2>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
-            test_child(std::integral_constant<int, 3>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
-            ng = make_uint2(n1.x, (hits & 0xff000000u) | imask);
-            tg = make_uint2(n1.y, hits & 0x00ffffffu);
+            visit(S, child);
         } else {
-            tg = ng;   // a postponed triangle group from the stack
+            tg = ng;   // a postponed triangle group from the stack (or nothing)
             ng = make_uint2(0u, 0u);
         }
         if (!kAnyHit && S.postpone) {   // a shadow ray wants any hit soon: it never postpones
@@ -371,43 +375,145 @@ __device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hi
             const float4 *tp = S.tris + 3 * (size_t)tri;
             const float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
             float tt, uu, vv;
-            if (intersect_watertight(w, ray.o, xyz(p0), xyz(p1), xyz(p2), ray.tmin, tmax, tt, uu, vv)) {
+            if (intersect_watertight(w, o, xyz(p0), xyz(p1), xyz(p2), tmin, tmax, tt, uu, vv)) {
                 found = true;
                 hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)tri;
-                if (kAnyHit) {
-                    st.nodes += nvis;
-                    st.tris += ntri;
-                    return true;
-                }
+                if (kAnyHit) return true;
                 tmax = tt;
             }
         }
         if (ng.y <= 0x00ffffffu) {
-            if (stk.sp == 0) break;
+            if (stk.sp == 0) return true;
             ng = stk.pop();
         }
+        return false;
     }
-    st.nodes += nvis;
-    st.tris += ntri;
-    if (found && !kAnyHit) {
-        const float4 *tp = S.tris + 3 * hit.tri;
-        refine_mt(ray.o, ray.d, xyz(ldg4(tp)), xyz(ldg4(tp + 1)), xyz(ldg4(tp + 2)), ray.tmin, ray.tmax, hit.t, hit.u,
-                  hit.v);
+
+    // Intersect the 8 children of node `child`: ng / tg become its groups.
+    __device__ __forceinline__ void visit(const DevScene &S, uint32_t child) {
+        const uint4 *np = S.wnodes + 5 * (size_t)child;
+        const uint4 n0 = ldg4u(np), n1 = ldg4u(np + 1), n2 = ldg4u(np + 2), n3 = ldg4u(np + 3), n4 = ldg4u(np + 4);
+        ++nvis;
+        const float adx = __uint_as_float((n0.w & 0xffu) << 23) * idir.x;
+        const float ady = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * idir.y;
+        const float adz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * idir.z;
+        const float ox = __fmaf_rn(-8388608.0f, adx, (__uint_as_float(n0.x) - o.x) * idir.x);
+        const float oy = __fmaf_rn(-8388608.0f, ady, (__uint_as_float(n0.y) - o.y) * idir.y);
+        const float oz = __fmaf_rn(-8388608.0f, adz, (__uint_as_float(n0.z) - o.z) * idir.z);
+        const uint32_t imask = n0.w >> 24;
+        // meta of internal children: slot ^ (7 ^ octant) in the position bits
+        const uint32_t in0 = ((imask & 0xfu) * 0x00204081u) & 0x01010101u;
+        const uint32_t in1 = ((imask >> 4) * 0x00204081u) & 0x01010101u;
+        const uint32_t meta0 = n1.z ^ (in0 * ko), meta1 = n1.w ^ (in1 * ko);
+        // near / far planes per axis (lo planes first for a positive direction)
+        const uint32_t nx0 = oct & 1u ? n3.z : n2.x, nx1 = oct & 1u ? n3.w : n2.y;
+        const uint32_t fx0 = oct & 1u ? n2.x : n3.z, fx1 = oct & 1u ? n2.y : n3.w;
+        const uint32_t ny0 = oct & 2u ? n4.x : n2.z, ny1 = oct & 2u ? n4.y : n2.w;
+        const uint32_t fy0 = oct & 2u ? n2.z : n4.x, fy1 = oct & 2u ? n2.w : n4.y;
+        const uint32_t nz0 = oct & 4u ? n4.z : n3.x, nz1 = oct & 4u ? n4.w : n3.y;
+        const uint32_t fz0 = oct & 4u ? n3.x : n4.z, fz1 = oct & 4u ? n3.y : n4.w;
+        uint32_t hits = 0;
+        const float t0 = tmin, t1 = tmax;
+        auto test_child = [&](auto kk, uint32_t xn, uint32_t xf, uint32_t yn, uint32_t yf, uint32_t zn, uint32_t zf,
+                              uint32_t meta) {
+            constexpr int k = decltype(kk)::value;
+            const float tnx = __fmaf_rn(qbyte_biased<k>(xn), adx, ox), tfx = __fmaf_rn(qbyte_biased<k>(xf), adx, ox);
+            const float tny = __fmaf_rn(qbyte_biased<k>(yn), ady, oy), tfy = __fmaf_rn(qbyte_biased<k>(yf), ady, oy);
+            const float tnz = __fmaf_rn(qbyte_biased<k>(zn), adz, oz), tfz = __fmaf_rn(qbyte_biased<k>(zf), adz, oz);
+            const float tn = fmax3f(tnx, tny, fmaxf(tnz, t0));
+            const float tf = fmin3f(tfx, tfy, fminf(tfz, t1));
+            const uint32_t m = __byte_perm(meta, 0u, 0x4440u | k);
+            if (tn <= tf * 1.00000024f + 1e-30f) hits |= (m >> 5) << (m & 31u);
+        };
+        test_child(std::integral_constant<int, 0>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
+        test_child(std::integral_constant<int, 1>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
+        test_child(std::integral_constant<int, 2>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
+        test_child(std::integral_constant<int, 3>{}, nx0, fx0, ny0, fy0, nz0, fz0, meta0);
+        test_child(std::integral_constant<int, 0>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
+        test_child(std::integral_constant<int, 1>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
+        test_child(std::integral_constant<int, 2>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
+        test_child(std::integral_constant<int, 3>{}, nx1, fx1, ny1, fy1, nz1, fz1, meta1);
+        ng = make_uint2(n1.x, (hits & 0xff000000u) | imask);
+        tg = make_uint2(n1.y, hits & 0x00ffffffu);
     }
-    return found;
+
+    template <bool kAnyHit>
+    __device__ __forceinline__ void end(const DevScene &S, TravStats &st) {
+        st.nodes += nvis;
+        st.tris += ntri;
+        if (found && !kAnyHit) {
+            const float4 *tp = S.tris + 3 * hit.tri;
+            refine_mt(o, d, xyz(ldg4(tp)), xyz(ldg4(tp + 1)), xyz(ldg4(tp + 2)), tmin, tmax0, hit.t, hit.u, hit.v);
+        }
+    }
+};
+
+template <bool kAnyHit>
+__device__ __forceinline__ bool trace_bvh8(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st) {
+    uint2 stack[kStackSize];
+    Bvh8Walker<LocalStack> wk;
+    wk.stk.e = stack;
+    wk.begin(S, ray);
+    while (!wk.template step<kAnyHit>(S)) {}
+    wk.template end<kAnyHit>(S, st);
+    hit = wk.hit;
+    return wk.found;
 }
 
 // Closest hit (kAnyHit = false) or first hit in the tree kAccel; kernels are
 // instantiated per tree and the host launches the scene's one.
-template <int kAccel, bool kAnyHit, class Stack>
-__device__ __forceinline__ bool trace(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st, Stack &stk) {
-    if constexpr (kAccel == kAccelBvh8) return trace_bvh8<kAnyHit>(S, ray, hit, st, stk);
+template <int kAccel, bool kAnyHit>
+__device__ __forceinline__ bool trace(const DevScene &S, const Ray &ray, Hit &hit, TravStats &st) {
+    if constexpr (kAccel == kAccelBvh8) return trace_bvh8<kAnyHit>(S, ray, hit, st);
     else return trace_bvh2<kAnyHit>(S, ray, hit, st);
 }
 
-// Stack type of a tree's traversal (the binary traversal keeps its own).
-struct NoStack {
-    int sp = 0;
-};
+// Walker type of a tree.
+template <int kAccel, class Stack>
+using WalkerOf = std::conditional_t<kAccel == kAccelBvh8, Bvh8Walker<Stack>, Bvh2Walker>;
+
+// Traverses n rays of a queue with dynamic fetching: a lane whose ray is done
+// takes the next unclaimed ray (one warp-aggregated atomic on *fetch per
+// refill) after at most kSteps node visits, so lanes do not idle until the
+// warp's longest ray ends (persistent while-while traversal with ray
+// replacement, Aila and Laine, "Understanding the Efficiency of Ray Traversal
+// on GPUs", HPG 2009).  load(i) returns ray i; store(i, walker) consumes the
+// result.  Every lane of the warp must call this (full-warp votes).
+template <bool kAnyHit, int kSteps, class Walker, class Load, class Store>
+__device__ __forceinline__ void trace_queue(const DevScene &S, Walker &wk, unsigned *fetch, unsigned n, Load load,
+                                            Store store, TravStats &st) {
+    const unsigned lane = threadIdx.x & 31u;
+    int item = -1;
+    bool exhausted = false;
+    for (;;) {
+        const unsigned want = __ballot_sync(0xffffffffu, item < 0 && !exhausted);
+        if (want) {
+            const int leader = __ffs(want) - 1;
+            unsigned base = 0;
+            if ((int)lane == leader) base = atomicAdd(fetch, (unsigned)__popc(want));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (want >> lane & 1u) {
+                const unsigned idx = base + __popc(want & ((1u << lane) - 1u));
+                if (idx < n) {
+                    item = (int)idx;
+                    wk.begin(S, load(item));
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, item >= 0)) break;
+        if (item >= 0) {
+            for (int k = 0; k < kSteps; ++k) {
+                if (wk.template step<kAnyHit>(S)) {
+                    wk.template end<kAnyHit>(S, st);
+                    store(item, wk);
+                    item = -1;
+                    break;
+                }
+            }
+        }
+    }
+}
 
 }  // namespace hk

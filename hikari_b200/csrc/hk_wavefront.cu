@@ -190,6 +190,8 @@ __global__ void wf_reset_kernel(WfState W, int cur) {
         W.ctr->idle_count[cur] = 0;
         W.ctr->eq_count[cur ^ 1] = 0;
         W.ctr->shadow_count = 0;
+        W.ctr->ext_fetch = 0;
+        W.ctr->sh_fetch = 0;
     }
     if (threadIdx.x < kWfTypes) W.ctr->sq_count[threadIdx.x] = 0;
 }
@@ -204,6 +206,7 @@ __global__ void wf_init_kernel(WfState W) {
         c->idle_count[1] = 0;
         for (int t = 0; t < kWfTypes; ++t) c->sq_count[t] = 0;
         c->fq_count = c->shadow_count = c->active = 0;
+        c->ext_fetch = c->sh_fetch = 0;
         c->rays = c->shadow_rays = c->dropped = 0;
         c->node_visits = c->tri_tests = c->node_visits_shadow = c->tri_tests_shadow = 0;
     }
@@ -216,32 +219,50 @@ __device__ __forceinline__ SharedStack make_stack() {
     SharedStack s;
     s.sh = wf_stack_smem + threadIdx.x;
     s.stride = (int)blockDim.x;
+    s.spill = nullptr;
     return s;
 }
 
+// Node visits between refills of the dynamic ray fetch, per tree (a binary
+// node visit is a few times cheaper than an 8-wide one).
+template <int kAccel>
+constexpr int kFetchSteps = kAccel == kAccelBvh8 ? 3 : 8;
+
 template <int kAccel>
 __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, int cur) {
-    const int n = (int)W.ctr->eq_count[cur];
+    const unsigned n = W.ctr->eq_count[cur];
     TravStats ts;
-    std::conditional_t<kAccel == kAccelBvh8, SharedStack, NoStack> stk;
-    if constexpr (kAccel == kAccelBvh8) stk = make_stack();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = W.eq[cur][i];
-        float4 o = W.ray_o[slot], d = W.ray_d[slot];
-        Ray r;
-        r.o = v3(o.x, o.y, o.z);
-        r.d = v3(d.x, d.y, d.z);
-        r.tmin = o.w;
-        r.tmax = d.w;
-        Hit h;
-        int type = 0;
-        if (trace<kAccel, false>(S, r, h, ts, stk)) {
-            int mesh = __float_as_int(__ldg(S.tris + 3 * h.tri + 1).w);
-            type = S.bsdfs[S.meshes[mesh].bsdf].type + 1;
-        }
-        W.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(h.tri));
-        W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
+    WalkerOf<kAccel, SharedStack> wk;
+    std::conditional_t<kAccel == kAccelBvh8, uint2, int> stack_mem[kAccel == kAccelBvh8 ? kStackSize - kShStack : kStackSize];
+    if constexpr (kAccel == kAccelBvh8) {
+        wk.stk = make_stack();
+        wk.stk.spill = stack_mem;
+    } else {
+        wk.stack = stack_mem;
     }
+    int slot = -1;
+    trace_queue<false, kFetchSteps<kAccel>>(
+        S, wk, &W.ctr->ext_fetch, n,
+        [&](int i) {
+            slot = W.eq[cur][i];
+            const float4 o = W.ray_o[slot], d = W.ray_d[slot];
+            Ray r;
+            r.o = v3(o.x, o.y, o.z);
+            r.d = v3(d.x, d.y, d.z);
+            r.tmin = o.w;
+            r.tmax = d.w;
+            return r;
+        },
+        [&](int, const auto &w) {
+            int type = 0;
+            if (w.found) {
+                const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
+                type = S.bsdfs[S.meshes[mesh].bsdf].type + 1;
+            }
+            W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
+            W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
+        },
+        ts);
     unsigned long long nv = ts.nodes, nt = ts.tris;
     for (int o = 16; o > 0; o >>= 1) {
         nv += __shfl_down_sync(0xffffffffu, nv, o);
@@ -394,23 +415,36 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
 // ------------------------------------------------------------ shadow
 template <int kAccel>
 __global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
-    const int n = min((int)W.ctr->shadow_count, W.max_shadow);
+    const unsigned n = min(W.ctr->shadow_count, (unsigned)W.max_shadow);
     TravStats ts;
-    std::conditional_t<kAccel == kAccelBvh8, SharedStack, NoStack> stk;
-    if constexpr (kAccel == kAccelBvh8) stk = make_stack();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 o = W.sh_o[i], d = W.sh_d[i];
-        Ray r;
-        r.o = v3(o.x, o.y, o.z);
-        r.d = v3(d.x, d.y, d.z);
-        r.tmin = kRayEps;
-        r.tmax = 1.0f - kRayEps;
-        Hit h;
-        if (!trace<kAccel, true>(S, r, h, ts, stk)) {
-            float4 c = W.sh_c[i];
-            red_add_v4(W.lacc + __float_as_int(o.w), c.x, c.y, c.z, 0.0f);
-        }
+    WalkerOf<kAccel, SharedStack> wk;
+    std::conditional_t<kAccel == kAccelBvh8, uint2, int> stack_mem[kAccel == kAccelBvh8 ? kStackSize - kShStack : kStackSize];
+    if constexpr (kAccel == kAccelBvh8) {
+        wk.stk = make_stack();
+        wk.stk.spill = stack_mem;
+    } else {
+        wk.stack = stack_mem;
     }
+    int slot = -1;
+    trace_queue<true, kFetchSteps<kAccel>>(
+        S, wk, &W.ctr->sh_fetch, n,
+        [&](int i) {
+            const float4 o = W.sh_o[i], d = W.sh_d[i];
+            slot = __float_as_int(o.w);
+            Ray r;
+            r.o = v3(o.x, o.y, o.z);
+            r.d = v3(d.x, d.y, d.z);
+            r.tmin = kRayEps;
+            r.tmax = 1.0f - kRayEps;
+            return r;
+        },
+        [&](int i, const auto &w) {
+            if (!w.found) {
+                const float4 c = W.sh_c[i];
+                red_add_v4(W.lacc + slot, c.x, c.y, c.z, 0.0f);
+            }
+        },
+        ts);
     unsigned long long nv = ts.nodes, nt = ts.tris;
     for (int o = 16; o > 0; o >>= 1) {
         nv += __shfl_down_sync(0xffffffffu, nv, o);

@@ -63,6 +63,7 @@ struct WfCounters {
     unsigned int fq_count;             // finished paths awaiting splat + regeneration
     unsigned int shadow_count;         // next-event shadow rays
     unsigned int active;               // paths in flight
+    unsigned int ext_fetch, sh_fetch;  // rays claimed by the extend / shadow kernels (dynamic fetch)
     unsigned int pad1;
     unsigned long long rays, shadow_rays, dropped;
     unsigned long long node_visits, tri_tests;                 // closest-hit traversal (extend)
