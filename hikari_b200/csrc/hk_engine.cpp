@@ -71,6 +71,8 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     L_.blocks_shade = grid(1, L_.threads_shade);
     L_.blocks_shadow = grid(2, L_.threads_shadow);
     L_.blocks_regen = grid(3, L_.threads_regen);
+    L_.fetch_steps = cfg_.fetch_steps > 0 ? cfg_.fetch_steps : (S.accel == kAccelBvh8 ? 3 : 8);
+    L_.fetch_min_idle = std::max(1, std::min(32, cfg_.fetch_min_idle));
     HK_CUDA(cudaGetLastError());
     reset();
 }

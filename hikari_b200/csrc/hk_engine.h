@@ -19,6 +19,8 @@ struct WfEngineConfig {
     int capacity = 1 << 21;   // path slots
     int threads_extend = 128;
     int threads_shade = 128;
+    int fetch_steps = 0;      // node visits between traversal refills (0: per-tree default)
+    int fetch_min_idle = 1;   // idle lanes before a warp refills while others traverse
 };
 
 class WfEngine {

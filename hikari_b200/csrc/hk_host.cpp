@@ -592,7 +592,8 @@ void require_scene_size(const hk_scene *s, const hk_render_desc &d) {
 hk::WfEngine &wf_ensure(hk_scene *s, const hk::WfEngineConfig &c) {
     if (s->wf) {
         const hk::WfEngineConfig &o = s->wf->config();
-        if (o.capacity == c.capacity && o.threads_extend == c.threads_extend && o.threads_shade == c.threads_shade)
+        if (o.capacity == c.capacity && o.threads_extend == c.threads_extend && o.threads_shade == c.threads_shade &&
+            o.fetch_steps == c.fetch_steps && o.fetch_min_idle == c.fetch_min_idle)
             return *s->wf;
         s->wf.reset();
     }
@@ -984,6 +985,8 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         ec.capacity = std::max(1024, std::min(c.capacity > 0 ? c.capacity : (1 << 21), 1 << 26));
         ec.threads_extend = c.threads_extend > 0 ? c.threads_extend : 128;
         ec.threads_shade = c.threads_shade > 0 ? c.threads_shade : 128;
+        ec.fetch_steps = std::max(0, std::min(1024, c.fetch_steps));
+        ec.fetch_min_idle = c.fetch_min_idle > 0 ? std::min(32, c.fetch_min_idle) : 1;
         hk::WfEngine &E = wf_ensure(s, ec);
         cudaStream_t user = (cudaStream_t)stream, st = E.stream();
         // order after the caller's stream (the films may have been cleared there)
@@ -1083,6 +1086,8 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
         const int caps[] = {1 << 20, 1 << 21, 1 << 22};
         const int threads[] = {64, 128, 256};
         const int checks[] = {16, 64};
+        const int steps8[] = {2, 3, 6}, steps2[] = {4, 8, 16};
+        const int min_idle[] = {1, 8, 16};
         auto run = [&](const hk_wavefront_config &c) {
             HK_CUDA(cudaMemset(film.p, 0, film.bytes));
             int rc = hk_render_batch(s, &job, 1, &c, nullptr, nullptr);   // warm (allocation, graph)
@@ -1114,6 +1119,19 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
         c = bc;
         for (int k : checks) {
             c.iterations_per_check = k;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        // dynamic ray fetch: node visits between refills, idle lanes before a refill
+        c = bc;
+        for (int k : (s->dev.accel == hk::kAccelBvh8 ? steps8 : steps2)) {
+            c.fetch_steps = k;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        c = bc;
+        for (int k : min_idle) {
+            c.fetch_min_idle = k;
             float ms = run(c);
             if (ms < best_t) { best_t = ms; bc = c; }
         }

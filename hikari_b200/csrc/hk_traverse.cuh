@@ -474,20 +474,24 @@ using WalkerOf = std::conditional_t<kAccel == kAccelBvh8, Bvh8Walker<Stack>, Bvh
 
 // Traverses n rays of a queue with dynamic fetching: a lane whose ray is done
 // takes the next unclaimed ray (one warp-aggregated atomic on *fetch per
-// refill) after at most kSteps node visits, so lanes do not idle until the
-// warp's longest ray ends (persistent while-while traversal with ray
-// replacement, Aila and Laine, "Understanding the Efficiency of Ray Traversal
-// on GPUs", HPG 2009).  load(i) returns ray i; store(i, walker) consumes the
-// result.  Every lane of the warp must call this (full-warp votes).
-template <bool kAnyHit, int kSteps, class Walker, class Load, class Store>
-__device__ __forceinline__ void trace_queue(const DevScene &S, Walker &wk, unsigned *fetch, unsigned n, Load load,
-                                            Store store, TravStats &st) {
+// refill), so lanes do not idle until the warp's longest ray ends (persistent
+// while-while traversal with ray replacement, Aila and Laine, "Understanding
+// the Efficiency of Ray Traversal on GPUs", HPG 2009).  Lanes check for a
+// refill every `steps` node visits; while other lanes still traverse, a warp
+// refills only once at least `min_idle` lanes are idle (larger batches of
+// consecutive queue entries keep neighbouring rays together).  load(i)
+// returns ray i; store(i, walker) consumes the result.  Every lane of the
+// warp must call this (full-warp votes).
+template <bool kAnyHit, class Walker, class Load, class Store>
+__device__ __forceinline__ void trace_queue(const DevScene &S, Walker &wk, unsigned *fetch, unsigned n, int steps,
+                                            int min_idle, Load load, Store store, TravStats &st) {
     const unsigned lane = threadIdx.x & 31u;
     int item = -1;
     bool exhausted = false;
     for (;;) {
         const unsigned want = __ballot_sync(0xffffffffu, item < 0 && !exhausted);
-        if (want) {
+        const unsigned busy = __ballot_sync(0xffffffffu, item >= 0);
+        if (want && (busy == 0u || __popc(want) >= min_idle)) {
             const int leader = __ffs(want) - 1;
             unsigned base = 0;
             if ((int)lane == leader) base = atomicAdd(fetch, (unsigned)__popc(want));
@@ -504,7 +508,7 @@ __device__ __forceinline__ void trace_queue(const DevScene &S, Walker &wk, unsig
         }
         if (!__any_sync(0xffffffffu, item >= 0)) break;
         if (item >= 0) {
-            for (int k = 0; k < kSteps; ++k) {
+            for (int k = 0; k < steps; ++k) {
                 if (wk.template step<kAnyHit>(S)) {
                     wk.template end<kAnyHit>(S, st);
                     store(item, wk);

@@ -223,13 +223,8 @@ __device__ __forceinline__ SharedStack make_stack() {
     return s;
 }
 
-// Node visits between refills of the dynamic ray fetch, per tree (a binary
-// node visit is a few times cheaper than an 8-wide one).
 template <int kAccel>
-constexpr int kFetchSteps = kAccel == kAccelBvh8 ? 3 : 8;
-
-template <int kAccel>
-__global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, int cur) {
+__global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, int cur, int steps, int min_idle) {
     const unsigned n = W.ctr->eq_count[cur];
     TravStats ts;
     WalkerOf<kAccel, SharedStack> wk;
@@ -241,8 +236,8 @@ __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, i
         wk.stack = stack_mem;
     }
     int slot = -1;
-    trace_queue<false, kFetchSteps<kAccel>>(
-        S, wk, &W.ctr->ext_fetch, n,
+    trace_queue<false>(
+        S, wk, &W.ctr->ext_fetch, n, steps, min_idle,
         [&](int i) {
             slot = W.eq[cur][i];
             const float4 o = W.ray_o[slot], d = W.ray_d[slot];
@@ -414,7 +409,7 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
 
 // ------------------------------------------------------------ shadow
 template <int kAccel>
-__global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
+__global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W, int steps, int min_idle) {
     const unsigned n = min(W.ctr->shadow_count, (unsigned)W.max_shadow);
     TravStats ts;
     WalkerOf<kAccel, SharedStack> wk;
@@ -426,8 +421,8 @@ __global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W) {
         wk.stack = stack_mem;
     }
     int slot = -1;
-    trace_queue<true, kFetchSteps<kAccel>>(
-        S, wk, &W.ctr->sh_fetch, n,
+    trace_queue<true>(
+        S, wk, &W.ctr->sh_fetch, n, steps, min_idle,
         [&](int i) {
             const float4 o = W.sh_o[i], d = W.sh_d[i];
             slot = __float_as_int(o.w);
@@ -474,15 +469,19 @@ static size_t stack_smem(int threads) { return (size_t)threads * kShStack * size
 
 static void launch_extend(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
     if (S.accel == kAccelBvh8)
-        wf_extend_kernel<kAccelBvh8><<<C.blocks_extend, C.threads_extend, stack_smem(C.threads_extend), st>>>(S, W, cur);
+        wf_extend_kernel<kAccelBvh8><<<C.blocks_extend, C.threads_extend, stack_smem(C.threads_extend), st>>>(
+            S, W, cur, C.fetch_steps, C.fetch_min_idle);
     else
-        wf_extend_kernel<kAccelBvh2><<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur);
+        wf_extend_kernel<kAccelBvh2><<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur, C.fetch_steps,
+                                                                               C.fetch_min_idle);
 }
 static void launch_shadow(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
     if (S.accel == kAccelBvh8)
-        wf_shadow_kernel<kAccelBvh8><<<C.blocks_shadow, C.threads_shadow, stack_smem(C.threads_shadow), st>>>(S, W);
+        wf_shadow_kernel<kAccelBvh8><<<C.blocks_shadow, C.threads_shadow, stack_smem(C.threads_shadow), st>>>(
+            S, W, C.fetch_steps, C.fetch_min_idle);
     else
-        wf_shadow_kernel<kAccelBvh2><<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W);
+        wf_shadow_kernel<kAccelBvh2><<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W, C.fetch_steps,
+                                                                              C.fetch_min_idle);
 }
 
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st) {

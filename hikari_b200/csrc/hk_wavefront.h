@@ -104,6 +104,7 @@ struct WfLaunchConfig {
     int blocks_shade, threads_shade;
     int blocks_shadow, threads_shadow;
     int blocks_regen, threads_regen;
+    int fetch_steps, fetch_min_idle;   // dynamic ray fetch of the extend and shadow kernels
 };
 
 // empty pool: every slot idle, queues and statistics zero (the dispatch head is the host's)

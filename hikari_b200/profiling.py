@@ -4,6 +4,15 @@ selected raw metrics of a `--set full` report (`ncu -i X --page raw --csv`).
 
 usage: python -m hikari_b200.profiling launches <launches.csv>
        python -m hikari_b200.profiling raw <report.ncu-rep> [regex]
+       python -m hikari_b200.profiling render [--views V] [--spp S] [--accel bvh2|bvh8] [--out F]
+       python -m hikari_b200.profiling traffic <dram.csv> <render.json>
+
+`render` renders the heterogeneous scene once with the wavefront integrator
+(no autotuning, no other launches of the traversal kernels) and writes its
+counters as JSON; run under `ncu --metrics dram__bytes_read.sum,
+dram__bytes_write.sum,gpu__time_duration.sum -k regex:"wf_(extend|shadow)"
+--cache-control none`, `traffic` turns the per-launch DRAM bytes of that
+capture into DRAM bytes per closest-hit and per shadow ray.
 """
 import csv
 import io
@@ -66,8 +75,77 @@ def raw(report, regex=None):
     return "\n".join(out)
 
 
+def _metric_rows(path):
+    text = open(path).read()
+    lines = [ln for ln in text.splitlines() if ln.startswith('"')]
+    rows = list(csv.reader(io.StringIO("\n".join(lines))))
+    hdr, data = rows[0], rows[1:]
+    ki, ni, vi, ui = hdr.index("Kernel Name"), hdr.index("Metric Name"), hdr.index("Metric Value"), hdr.index("Metric Unit")
+    ii = hdr.index("ID")
+    return [(r[ii], r[ki].split("(")[0], r[ni], float(r[vi].replace(",", "")), r[ui]) for r in data]
+
+
+BYTE_UNIT = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+
+
+def traffic(csv_path, render_json):
+    import json
+
+    ctr = json.load(open(render_json))["counters"]
+    agg = {}
+    for _, kern, metric, val, unit in _metric_rows(csv_path):
+        a = agg.setdefault(kern, {"launches": set(), "bytes": 0.0, "ms": 0.0})
+        if metric.startswith("dram__bytes"):
+            a["bytes"] += val * BYTE_UNIT[unit]
+        elif metric == "gpu__time_duration.sum":
+            a["ms"] += val * UNIT_MS[unit]
+    rows = ["| kernel | DRAM bytes | rays | DRAM bytes per ray | device ms (ncu) |", "|---|---|---|---|---|"]
+    for kern, a in sorted(agg.items()):
+        rays = ctr["shadow_rays"] if "shadow" in kern else ctr["rays"]
+        rows.append(f"| {kern} | {a['bytes']:.4g} | {rays} | {a['bytes'] / max(rays, 1):.2f} | {a['ms']:.2f} |")
+    return "\n".join(rows)
+
+
+def render(argv):
+    import argparse
+    import json
+
+    import torch
+
+    import hikari_b200 as hk
+    from hikari_b200 import scenes
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--views", type=int, default=1)
+    ap.add_argument("--spp", type=int, default=16)
+    ap.add_argument("--accel", default="bvh2", choices=["bvh2", "bvh8"])
+    ap.add_argument("--capacity", type=int, default=1 << 22)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args(argv)
+    sd = scenes.heterogeneous(width=1024, height=1024, spp=a.spp, depth=16)
+    cams = scenes.heterogeneous_cameras(a.views)
+    gs = hk.Scene.from_desc(sd)
+    gs.set_accel(hk.ACCEL_BVH8 if a.accel == "bvh8" else hk.ACCEL_BVH2)
+    films = [torch.zeros(gs.film_shape(), device="cuda") for _ in range(a.views)]
+    ctr = torch.zeros(7, dtype=torch.int64, device="cuda")
+    gs.render_batch(films, spp=a.spp, depth=sd.depth, cameras=cams, counters=ctr, capacity=a.capacity)
+    torch.cuda.synchronize()
+    c = [int(x) for x in ctr.cpu().tolist()]
+    names = ["rays", "shadow_rays", "dropped", "node_visits", "tri_tests", "node_visits_shadow", "tri_tests_shadow"]
+    out = {"workload": f"heterogeneous {a.views} x 1024^2 x {a.spp} spp", "accel": a.accel,
+           "counters": dict(zip(names, c))}
+    text = json.dumps(out)
+    if a.out:
+        open(a.out, "w").write(text + "\n")
+    print(text)
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "launches":
         print(launches(sys.argv[2]))
+    elif sys.argv[1] == "render":
+        render(sys.argv[2:])
+    elif sys.argv[1] == "traffic":
+        print(traffic(sys.argv[2], sys.argv[3]))
     else:
         print(raw(sys.argv[2], sys.argv[3] if len(sys.argv) > 3 else None))

@@ -170,6 +170,10 @@ typedef struct {
     float *kernel_ms;              /* optional host float[4]: adds the device time of the regen, extend,
                                       shade and shadow phases (timed with events, no graph) */
     int32_t *kernel_launches;      /* optional host int32[4]: adds the kernel launches per phase */
+    int32_t fetch_steps;           /* node visits of a ray between refills of the traversal lanes
+                                      (0 = 8 for the binary tree, 3 for the 8-wide tree) */
+    int32_t fetch_min_idle;        /* idle lanes of a warp before it refills while others still
+                                      traverse (0 = 1: refill at once) */
 } hk_wavefront_config;
 
 /* Render every job of the batch with the wavefront integrator: a pool of path
@@ -191,7 +195,8 @@ int hk_render_batch_host(hk_scene *s, const hk_render_desc *descs, int n, const 
 
 /* Autotuner: render `probe` (one image) under candidate configurations --
  * slot capacity 2^20..2^22, block sizes 64/128/256, termination-check
- * interval 16/64 -- by coordinate descent and return the fastest. */
+ * interval 16/64, traversal refill interval and idle-lane threshold -- by
+ * coordinate descent and return the fastest. */
 int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront_config *best, float *best_ms);
 
 /* Render into a caller-provided device image without allocating any device
