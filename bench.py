@@ -135,6 +135,19 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def slowest_rank_seconds(seconds, device="cuda"):
+    """The longest time of any rank (all ranks call this; max all-reduce when
+    torch.distributed runs with more than one rank).  Whole-job throughput of
+    independent replicas is the units all ranks processed over this time."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -367,10 +380,7 @@ def main():
         barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_s = sum(step_ms) / 1e3
-    t = torch.tensor([total_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_max = float(t.item())
+    total_max = slowest_rank_seconds(total_s)
     ctr = counters.cpu().numpy().astype(np.float64)
     paths_rank = float(W * H * spp * V * args.steps)
     value = world * paths_rank / total_max / 1e6
@@ -425,19 +435,21 @@ def main():
         outs = [np.empty((H, W, 3), np.float32) for _ in range(V)]
         torch.cuda.synchronize()
         barrier()
-        t0 = time.perf_counter()
+        # device time on the calling stream: the host-to-device pose/desc
+        # upload, the render, the resolve and the device-to-host image copies
+        # of every view are all ordered on it
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
         if wave:
             gs.render_batch_host(outs, spp, depth, seeds=[5000 + v for v in range(V)], cameras=cam_list,
                                  image_indices=[rank * V + v for v in range(V)], **tuned)
         else:
             for v, cam in enumerate(cams):
                 gs.render_image(spp, depth, seed=5000 + v, out=outs[v], camera=cam, image_index=rank * V + v)
+        e1.record(stream)
         torch.cuda.synchronize()
-        e2e_s = time.perf_counter() - t0
-        te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_value = world * W * H * spp * V / float(te.item()) / 1e6
+        e2e_s = e0.elapsed_time(e1) / 1e3
+        e2e_value = world * W * H * spp * V / slowest_rank_seconds(e2e_s) / 1e6
 
     # the plain megakernel on a short sample of the same scene, for comparison
     plain = None

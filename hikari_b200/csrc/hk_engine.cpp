@@ -56,7 +56,12 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     h_head_.alloc(1);
     std::memset(h_ctr_.p, 0, sizeof(WfCounters));
     std::memset(h_fin_.p, 0, sizeof(unsigned long long) * kWfMaxJobs);
-    HK_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    int least = 0, greatest = 0;
+    HK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    HK_CUDA(cudaStreamCreateWithPriority(&streams_[0], cudaStreamNonBlocking, least));
+    HK_CUDA(cudaStreamCreateWithPriority(&streams_[1], cudaStreamNonBlocking, greatest));
+    stream_ = streams_[0];
+    HK_CUDA(cudaEventCreateWithFlags(&ev_switch_, cudaEventDisableTiming));
     HK_CUDA(cudaEventCreateWithFlags(&ev_done_, cudaEventDisableTiming));
     HK_CUDA(cudaEventCreateWithFlags(&ev_plan_, cudaEventDisableTiming));
     // launch configuration: persistent grids of one wave of resident blocks
@@ -78,12 +83,22 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
 }
 
 WfEngine::~WfEngine() {
-    if (stream_) cudaStreamSynchronize(stream_);
+    for (cudaStream_t s : streams_)
+        if (s) cudaStreamSynchronize(s);
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
-    for (cudaEvent_t e : {ev_done_, ev_plan_, pe_[0], pe_[1]})
+    for (cudaEvent_t e : {ev_done_, ev_plan_, ev_switch_, pe_[0], pe_[1]})
         if (e) cudaEventDestroy(e);
-    if (stream_) cudaStreamDestroy(stream_);
+    for (cudaStream_t s : streams_)
+        if (s) cudaStreamDestroy(s);
+}
+
+void WfEngine::set_priority(bool high) {
+    cudaStream_t target = streams_[high ? 1 : 0];
+    if (target == stream_) return;
+    HK_CUDA(cudaEventRecord(ev_switch_, stream_));
+    HK_CUDA(cudaStreamWaitEvent(target, ev_switch_, 0));
+    stream_ = target;
 }
 
 void WfEngine::reset() {

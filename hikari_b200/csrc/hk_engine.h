@@ -35,7 +35,12 @@ public:
     static size_t bytes_for(int capacity, int nemitters);
     size_t device_bytes() const { return bytes_; }
     const WfEngineConfig &config() const { return cfg_; }
+    // The stream the engine's work goes to next (one of two of different priority).
     cudaStream_t stream() const { return stream_; }
+    // Move later work to the high- or low-priority stream, ordered after all
+    // earlier work: pending kernels of a high-priority engine are scheduled
+    // before those of low-priority engines sharing the GPU.
+    void set_priority(bool high);
 
     // Empty pool (every slot idle), zero statistics, empty plan.  Async on stream().
     void reset();
@@ -70,7 +75,9 @@ private:
     PinnedBuf<WfJob> h_jobs_;
     PinnedBuf<WfSeg> h_segs_;
     PinnedBuf<WfCounters> h_head_;
-    cudaStream_t stream_ = nullptr;
+    cudaStream_t stream_ = nullptr;             // current: streams_[0] or streams_[1]
+    cudaStream_t streams_[2] = {nullptr, nullptr};   // low, high priority
+    cudaEvent_t ev_switch_ = nullptr;
     cudaEvent_t ev_done_ = nullptr, ev_plan_ = nullptr, pe_[2] = {nullptr, nullptr};
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;

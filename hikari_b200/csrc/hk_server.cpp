@@ -9,7 +9,8 @@
 //   launch  for every idle engine with work: a dispatch plan over its jobs'
 //           undispensed work (least remaining first, or arrival order), then
 //           `iterations_per_poll` wavefront iterations from the CUDA graph and
-//           an async copy of the counters
+//           an async copy of the counters; when several scenes render, the one
+//           with the least remaining job goes to its high-priority stream
 //   poll    engines whose copy completed: the plan items consumed are credited
 //           to their jobs; a job whose every item is dispensed and finished
 //           is resolved and copied to its host buffer; a finished copy ends it
@@ -229,6 +230,21 @@ void hk_server::admit(const std::vector<SceneEntry *> &sc) {
 }
 
 void hk_server::launch(const std::vector<SceneEntry *> &sc) {
+    // the scene holding the job with the least undispensed work (fully
+    // dispensed jobs still rendering count as zero) runs at high priority
+    const SceneEntry *urgent = nullptr;
+    uint64_t least = UINT64_MAX;
+    int busy = 0;
+    for (SceneEntry *ep : sc) {
+        bool any = false;
+        for (Job *j : ep->jobs)
+            if (j->phase == 1) {
+                any = true;
+                const uint64_t rem = j->work - j->dispensed;
+                if (rem < least) { least = rem; urgent = ep; }
+            }
+        busy += any ? 1 : 0;
+    }
     for (SceneEntry *ep : sc) {
         SceneEntry &e = *ep;
         if (!e.eng || e.inflight) continue;
@@ -260,6 +276,7 @@ void hk_server::launch(const std::vector<SceneEntry *> &sc) {
             total += j->work - j->dispensed;
         }
         e.plan_total = total;
+        e.eng->set_priority(busy > 1 && &e == urgent);
         e.eng->set_plan(e.plan, total);
         e.eng->run(cfg.iterations_per_poll, true);
         e.eng->fetch_status();
