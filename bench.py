@@ -32,6 +32,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per ray of the
+# 8-wide traversal kernels, from one ncu capture of every extend / shadow launch
+# of `python -m hikari_b200.profiling render --views 1 --spp 4 --accel bvh8`
+# (the heterogeneous scene, pool of 2^22 slots) divided by the rays the render
+# traced; the bench scales them by the rays of its own launches.
+DRAM_BYTES_PER_RAY = {"bvh8": {"extend": 178.0, "shadow": 117.7}}
 
 
 def parse():
@@ -399,6 +405,12 @@ def main():
         phases = ["regen", "extend", "shade", "shadow"]
         dom = int(np.argmax(kms))
         trav_bytes = {1: pcn[3] * node_b + pcn[4] * 48.0, 3: pcn[5] * node_b + pcn[6] * 48.0}
+        traffic = None
+        per_ray = DRAM_BYTES_PER_RAY.get(args.accel, {})
+        if dom == 1 and "extend" in per_ray:
+            traffic = per_ray["extend"] * pcn[0] / max(1, kl[dom])
+        elif dom == 3 and "shadow" in per_ray:
+            traffic = per_ray["shadow"] * pcn[1] / max(1, kl[dom])
         if dom in trav_bytes:
             bytes_per_launch = trav_bytes[dom] / max(1, kl[dom])
             avg_s = float(kms[dom]) / max(1, kl[dom]) / 1e3
@@ -428,11 +440,21 @@ def main():
         launches_per_step = V
         phase_share = None
         traversal = None
+        traffic = None
 
     # end to end through the C ABI: host images out, per-view camera pose in
     e2e_value = None
     if not args.no_e2e:
         outs = [np.empty((H, W, 3), np.float32) for _ in range(V)]
+        def e2e_call():
+            if wave:
+                gs.render_batch_host(outs, spp, depth, seeds=[5000 + v for v in range(V)], cameras=cam_list,
+                                     image_indices=[rank * V + v for v in range(V)], **tuned)
+            else:
+                for v, cam in enumerate(cams):
+                    gs.render_image(spp, depth, seed=5000 + v, out=outs[v], camera=cam, image_index=rank * V + v)
+
+        e2e_call()   # untimed: the first call allocates the library's host-output films
         torch.cuda.synchronize()
         barrier()
         # device time on the calling stream: the host-to-device pose/desc
@@ -440,12 +462,7 @@ def main():
         # of every view are all ordered on it
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        if wave:
-            gs.render_batch_host(outs, spp, depth, seeds=[5000 + v for v in range(V)], cameras=cam_list,
-                                 image_indices=[rank * V + v for v in range(V)], **tuned)
-        else:
-            for v, cam in enumerate(cams):
-                gs.render_image(spp, depth, seed=5000 + v, out=outs[v], camera=cam, image_index=rank * V + v)
+        e2e_call()
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_s = e0.elapsed_time(e1) / 1e3
@@ -506,7 +523,9 @@ def main():
         "traversal": traversal,
         "plain_megakernel": plain,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "peak_kind": peak_kind, "basis": basis},
+                     "traffic": traffic, "peak_kind": peak_kind, "basis": basis,
+                     "traffic_basis": ("DRAM bytes per ray from one ncu capture of the 1-view 4-spp case, scaled by "
+                                       "the rays per launch" if traffic is not None else None)},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": V * int(hk.C.sizeof(hk.RenderDesc)),
                 "d2h_bytes_per_step": V * W * H * 3 * 4},

@@ -473,31 +473,43 @@ template <int kAccel, class Stack>
 using WalkerOf = std::conditional_t<kAccel == kAccelBvh8, Bvh8Walker<Stack>, Bvh2Walker>;
 
 // Traverses n rays of a queue with dynamic fetching: a lane whose ray is done
-// takes the next unclaimed ray (one warp-aggregated atomic on *fetch per
-// refill), so lanes do not idle until the warp's longest ray ends (persistent
-// while-while traversal with ray replacement, Aila and Laine, "Understanding
-// the Efficiency of Ray Traversal on GPUs", HPG 2009).  Lanes check for a
-// refill every `steps` node visits; while other lanes still traverse, a warp
-// refills only once at least `min_idle` lanes are idle (larger batches of
-// consecutive queue entries keep neighbouring rays together).  load(i)
-// returns ray i; store(i, walker) consumes the result.  Every lane of the
-// warp must call this (full-warp votes).
+// takes the next unclaimed ray, so lanes do not idle until the warp's longest
+// ray ends (persistent while-while traversal with ray replacement, Aila and
+// Laine, "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009).
+// A warp claims kFetchChunk consecutive queue entries with one atomic on
+// *fetch and hands them to its lanes itself (one atomic per refill would
+// serialise at the L2 on that one address).  Lanes check for a refill every
+// `steps` node visits; while other lanes still traverse, a warp refills only
+// once at least `min_idle` lanes are idle.  load(i) returns ray i;
+// store(i, walker) consumes the result.  Every lane of the warp must call
+// this (full-warp votes).
+constexpr unsigned kFetchChunk = 128;
+
 template <bool kAnyHit, class Walker, class Load, class Store>
 __device__ __forceinline__ void trace_queue(const DevScene &S, Walker &wk, unsigned *fetch, unsigned n, int steps,
                                             int min_idle, Load load, Store store, TravStats &st) {
     const unsigned lane = threadIdx.x & 31u;
     int item = -1;
     bool exhausted = false;
+    unsigned chunk_next = 0, chunk_end = 0;   // warp-uniform: unhanded entries of the claimed chunk
     for (;;) {
         const unsigned want = __ballot_sync(0xffffffffu, item < 0 && !exhausted);
         const unsigned busy = __ballot_sync(0xffffffffu, item >= 0);
         if (want && (busy == 0u || __popc(want) >= min_idle)) {
-            const int leader = __ffs(want) - 1;
-            unsigned base = 0;
-            if ((int)lane == leader) base = atomicAdd(fetch, (unsigned)__popc(want));
-            base = __shfl_sync(0xffffffffu, base, leader);
+            const unsigned k = __popc(want), rank = __popc(want & ((1u << lane) - 1u));
+            const unsigned avail = chunk_end - chunk_next;
+            unsigned idx = chunk_next + rank;
+            if (k > avail) {   // warp-uniform: claim the next chunk for the lanes past the old one
+                unsigned base = 0;
+                if ((int)lane == __ffs(want) - 1) base = atomicAdd(fetch, kFetchChunk);
+                base = __shfl_sync(0xffffffffu, base, __ffs(want) - 1);
+                if (rank >= avail) idx = base + (rank - avail);
+                chunk_next = base + (k - avail);
+                chunk_end = base + kFetchChunk;
+            } else {
+                chunk_next += k;
+            }
             if (want >> lane & 1u) {
-                const unsigned idx = base + __popc(want & ((1u << lane) - 1u));
                 if (idx < n) {
                     item = (int)idx;
                     wk.begin(S, load(item));

@@ -114,24 +114,34 @@ __device__ __forceinline__ void splat_global(const DevScene &S, const WfJob &J, 
 // Splat and retire the finished paths, then give every finished or idle slot
 // new work from the dispatch plan; slots that find none wait in the next idle
 // list.  Queues read here: fq, idle[cur]; written: eq[cur], idle[cur ^ 1].
+// The per-job finished counts and the change of the in-flight count are
+// gathered per block in shared memory and added once per block: a global
+// atomic per path on a handful of addresses would serialise at the L2.
 __global__ void wf_regen_kernel(DevScene S, WfState W, int cur) {
+    __shared__ unsigned s_finished[kWfMaxJobs];
+    __shared__ int s_active;
+    for (int k = threadIdx.x; k < kWfMaxJobs; k += blockDim.x) s_finished[k] = 0u;
+    if (threadIdx.x == 0) s_active = 0;
+    __syncthreads();
     const int nf = (int)W.ctr->fq_count;
     const int n = nf + (int)W.ctr->idle_count[cur];
     const uint64_t total = W.ctr->total_work;
     const int nseg = (int)W.ctr->seg_count;
     unsigned long long dropped = 0;
+    int active_delta = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int slot;
         if (i < nf) {
             slot = W.fq[i];
             float4 p = W.pix[slot];
             float4 L = W.lacc[slot];
-            const WfJob &J = W.jobs[__float_as_int(p.z)];
+            const int pj = __float_as_int(p.z);
+            const WfJob &J = W.jobs[pj];
             V3 val = v3(L.x, L.y, L.z);
             if (is_valid(val)) splat_global(S, J, p.x, p.y, val);
             else ++dropped;
-            atomicAdd(J.finished, 1ull);
-            atomicSub(&W.ctr->active, 1u);
+            atomicAdd(&s_finished[pj], 1u);
+            --active_delta;
         } else {
             slot = W.idle[cur][i - nf];
         }
@@ -157,7 +167,7 @@ __global__ void wf_regen_kernel(DevScene S, WfState W, int cur) {
             const uint32_t x = (t % J.tiles_x) * kWfTileSide + p % kWfTileSide;
             const uint32_t y = (t / J.tiles_x) * kWfTileSide + p / kWfTileSide;
             if (x >= J.width || y >= J.height) {
-                atomicAdd(J.finished, 1ull);   // counted as work done: no path
+                atomicAdd(&s_finished[j], 1u);   // counted as work done: no path
                 continue;
             }
             Pcg32 rng;
@@ -173,13 +183,20 @@ __global__ void wf_regen_kernel(DevScene S, WfState W, int cur) {
             W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
                                      (uint32_t)(rng.inc >> 32));
             W.eq[cur][warp_append(&W.ctr->eq_count[cur])] = slot;
-            atomicAdd(&W.ctr->active, 1u);
+            ++active_delta;
             started = true;
             break;
         }
         if (!started) W.idle[cur ^ 1][warp_append(&W.ctr->idle_count[cur ^ 1])] = slot;
     }
     if (dropped) atomicAdd(&W.ctr->dropped, dropped);
+    // one atomic per warp into the block, one per block and job into HBM
+    for (int o = 16; o > 0; o >>= 1) active_delta += __shfl_down_sync(0xffffffffu, active_delta, o);
+    if (lane_id() == 0 && active_delta) atomicAdd(&s_active, active_delta);
+    __syncthreads();
+    for (int k = threadIdx.x; k < kWfMaxJobs; k += blockDim.x)
+        if (s_finished[k]) atomicAdd(W.jobs[k].finished, (unsigned long long)s_finished[k]);
+    if (threadIdx.x == 0 && s_active) atomicAdd(&W.ctr->active, (unsigned)s_active);
 }
 
 // Reset the counters of the queues consumed by regen and of those the next
