@@ -52,6 +52,7 @@ def parse():
                     help="tree the kernels traverse: compressed 8-wide (80-byte nodes) or binary (64-byte nodes)")
     ap.add_argument("--jobs", type=int, default=40, help="serving: jobs of the Poisson run")
     ap.add_argument("--load", type=float, default=0.8, help="serving: arrival rate as a fraction of the peak")
+    ap.add_argument("--capacity", type=int, default=1 << 19, help="serving: path slots of each scene's pool")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--res", type=int, default=0)
@@ -261,7 +262,7 @@ def run_serving(args):
     tris = [int(g.info.n_triangles) for g in gss]
     rng = np.random.default_rng(7)
     depths = [sd.depth for sd in sds]
-    with serving.Server(capacity=1 << 20, iterations_per_poll=4) as srv:
+    with serving.Server(capacity=args.capacity, iterations_per_poll=4) as srv:
         for g in gss:
             srv.add_scene(g)
         for k in range(len(gss)):   # engines and graphs of every scene (untimed)
@@ -290,7 +291,7 @@ def run_serving(args):
                                "heterogeneous 4.75M tris, 5 heterogeneous variants); jobs of 256/512/1024 px "
                                "square at 16/64/256 spp",
                    "form": "wavefront serving loop (continuous batching, SRPT dispatch)", "triangles": tris,
-                   "scene_build_s": round(build_s, 2), "capacity": 1 << 20, "jobs": args.jobs,
+                   "scene_build_s": round(build_s, 2), "capacity": args.capacity, "jobs": args.jobs,
                    "load": args.load},
         "serving": {
             "peak_mpaths_per_s": peak_mpaths, "peak_rate_hz": peak_rate, "arrival_rate_hz": rate,

@@ -438,7 +438,7 @@ int hk_server_create(const hk_server_config *cfg, hk_server **out) {
         std::unique_ptr<hk_server> s(new hk_server());
         if (cfg) s->cfg = *cfg;
         hk_server_config &c = s->cfg;
-        if (c.capacity <= 0) c.capacity = 1 << 20;
+        if (c.capacity <= 0) c.capacity = 1 << 19;   // small pools keep iterations short for newly admitted jobs
         if (c.threads_extend <= 0) c.threads_extend = 128;
         if (c.threads_shade <= 0) c.threads_shade = 128;
         if (c.iterations_per_poll <= 0) c.iterations_per_poll = 4;

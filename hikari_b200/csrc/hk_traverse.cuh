@@ -304,6 +304,18 @@ template <int k>
 __device__ __forceinline__ float qbyte(uint32_t x) {
     return __uint_as_float(__byte_perm(x, 0x4B000000u, 0x7440u | k)) - 8388608.0f;
 }
+// Two FMAs in one instruction (PTX fma.rn.f32x2, sm_100a): each lane is an
+// IEEE round-to-nearest FMA, the same result as two __fmaf_rn.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+    float2 r;
+    asm("{\n\t.reg .b64 pa, pb, pc, pr;\n\t"
+        "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\tmov.b64 pc, {%6, %7};\n\t"
+        "fma.rn.f32x2 pr, pa, pb, pc;\n\tmov.b64 {%0, %1}, pr;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return r;
+}
+
 // The float 2^23 + q without the subtraction: the slab offsets of a node are
 // shifted by -2^23 steps instead (one rounding of at most half a step, which
 // the one-step padding of the quantised boxes absorbs).
@@ -414,14 +426,17 @@ struct Bvh8Walker {
         const uint32_t fz0 = oct & 4u ? n3.x : n4.z, fz1 = oct & 4u ? n3.y : n4.w;
         uint32_t hits = 0;
         const float t0 = tmin, t1 = tmax;
+        const float2 adx2 = make_float2(adx, adx), ady2 = make_float2(ady, ady), adz2 = make_float2(adz, adz);
+        const float2 ox2 = make_float2(ox, ox), oy2 = make_float2(oy, oy), oz2 = make_float2(oz, oz);
         auto test_child = [&](auto kk, uint32_t xn, uint32_t xf, uint32_t yn, uint32_t yf, uint32_t zn, uint32_t zf,
                               uint32_t meta) {
             constexpr int k = decltype(kk)::value;
-            const float tnx = __fmaf_rn(qbyte_biased<k>(xn), adx, ox), tfx = __fmaf_rn(qbyte_biased<k>(xf), adx, ox);
-            const float tny = __fmaf_rn(qbyte_biased<k>(yn), ady, oy), tfy = __fmaf_rn(qbyte_biased<k>(yf), ady, oy);
-            const float tnz = __fmaf_rn(qbyte_biased<k>(zn), adz, oz), tfz = __fmaf_rn(qbyte_biased<k>(zf), adz, oz);
-            const float tn = fmax3f(tnx, tny, fmaxf(tnz, t0));
-            const float tf = fmin3f(tfx, tfy, fminf(tfz, t1));
+            // near and far plane of an axis in one packed FMA
+            const float2 tx = fma2(make_float2(qbyte_biased<k>(xn), qbyte_biased<k>(xf)), adx2, ox2);
+            const float2 ty = fma2(make_float2(qbyte_biased<k>(yn), qbyte_biased<k>(yf)), ady2, oy2);
+            const float2 tz = fma2(make_float2(qbyte_biased<k>(zn), qbyte_biased<k>(zf)), adz2, oz2);
+            const float tn = fmax3f(tx.x, ty.x, fmaxf(tz.x, t0));
+            const float tf = fmin3f(tx.y, ty.y, fminf(tz.y, t1));
             const uint32_t m = __byte_perm(meta, 0u, 0x4440u | k);
             if (tn <= tf * 1.00000024f + 1e-30f) hits |= (m >> 5) << (m & 31u);
         };

@@ -244,7 +244,7 @@ typedef struct hk_server hk_server;
 #define HK_JOB_FAILED 4      /* the server hit a device error; hk_job_wait returns it */
 
 typedef struct {
-    int32_t capacity;             /* path slots of each scene's pool (0 = 2^20) */
+    int32_t capacity;             /* path slots of each scene's pool (0 = 2^19) */
     int32_t threads_extend;       /* 0 = 128 */
     int32_t threads_shade;        /* 0 = 128 */
     int32_t iterations_per_poll;  /* wavefront iterations between host polls (0 = 4) */

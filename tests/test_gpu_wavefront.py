@@ -98,3 +98,35 @@ def test_wavefront_batch_of_images_equals_separate_images():
                         capacity=1 << 12)
         a, b = _resolve(gs, batch[i]), _resolve(gs, alone)
         assert np.allclose(a, b, rtol=1e-5, atol=1e-6), np.abs(a - b).max()
+
+
+@pytest.mark.parametrize("accel", [hk.ACCEL_BVH8, hk.ACCEL_BVH2])
+def test_equal_rmse_wavefront_and_megakernel(accel):
+    """At equal spp the wavefront and the megakernel have equal RMSE against a
+    high-spp reference (they run the same estimator), and both halve their MSE
+    when spp doubles.  The reference is a 65536-spp image of the Cornell box
+    whose per-pixel means match the CPU oracle (test_wavefront_cornell_matches_oracle)."""
+    sd = scenes.cornell_box(width=48, height=48)
+    sd.filter = FilterDesc(0, 0.5)
+    gs = hk.Scene.from_desc(sd)
+    gs.set_accel(accel)
+    ref_film = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
+    gs.render(ref_film, spp=65536, depth=sd.depth, seed=424242)
+    ref = _resolve(gs, ref_film).astype(np.float64)
+
+    def mse(form, spp, k):
+        out = []
+        for s in range(k):
+            f = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
+            if form == "mega":
+                gs.render(f, spp=spp, depth=sd.depth, seed=9000 + s)
+            else:
+                gs.render_batch([f], spp=spp, depth=sd.depth, seeds=[7000 + s], capacity=1 << 16)
+            out.append(np.mean((_resolve(gs, f).astype(np.float64) - ref) ** 2))
+        return float(np.mean(out))
+
+    m64, w64 = mse("mega", 64, 16), mse("wave", 64, 16)
+    w256 = mse("wave", 256, 16)
+    print(f"accel {accel}: MSE at 64 spp megakernel {m64:.3e} wavefront {w64:.3e}; wavefront 256 spp {w256:.3e}")
+    assert 0.75 < w64 / m64 < 1.33           # equal RMSE at equal spp (16 images each; fireflies add spread)
+    assert 2.8 < w64 / w256 < 5.5            # MSE ~ 1/spp (4x spp -> 1/4 MSE)
