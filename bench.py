@@ -204,7 +204,7 @@ class CpuBaseline:
             nb = max(1, self.nthreads)
             _, dt, _ = self._render(self._blocks(nb))
             self.block_s = max(dt, 1e-3) / nb
-        nb = int(max(self.nthreads, seconds / self.block_s))
+        nb = int(max(4 * self.nthreads, seconds / self.block_s))   # >= 4 blocks per thread: balanced threads
         blocks = self._blocks(nb)
         paths, dt, ctr = self._render(blocks)
         return {"value": paths / dt / 1e6, "unit": "Mpaths/s", "cores": self.nthreads, "kind": "port",
