@@ -305,13 +305,15 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
         int depth = (int)(dflags & 0xffffu);
         uint32_t flags = dflags >> 16;
         const WfJob &J = W.jobs[__float_as_int(p4.z)];
-        float4 L4 = W.lacc[slot];
-        V3 L = v3(L4.x, L4.y, L4.z);
+        // radiance terms go to the path's accumulator with vector reductions
+        // (as the unoccluded next-event terms do): shade neither reads nor
+        // rewrites it
         if constexpr (kType == 0) {
-            // miss (PathMISIntegrator.cpp:35-66)
-            if (S.env_index >= 0 && (depth > 0 || !S.force_background)) L = L + beta * env_eval(S, rd);
-            else if (depth == 0) L = ld3(S.background);
-            W.lacc[slot] = f4(L, 0.0f);
+            // miss (PathMISIntegrator.cpp:35-66); a new path's accumulator is zero
+            V3 Le = v3(0, 0, 0);
+            if (S.env_index >= 0 && (depth > 0 || !S.force_background)) Le = beta * env_eval(S, rd);
+            else if (depth == 0) Le = ld3(S.background);
+            if (!all_zero(Le)) red_add_v4(W.lacc + slot, Le.x, Le.y, Le.z, 0.0f);
             finish(W, slot);
             continue;
         } else {
@@ -348,7 +350,8 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                         if (pbm + plm != 0.0f) w_mats = pbm / (pbm + plm);
                     }
                 }
-                L = L + (beta * w_mats) * area_eval(AL, er);
+                const V3 Le = (beta * w_mats) * area_eval(AL, er);
+                if (!all_zero(Le)) red_add_v4(W.lacc + slot, Le.x, Le.y, Le.z, 0.0f);
             }
             // next-event estimation over every emitter (PathMISIntegrator.cpp:83-109)
             const V3 wi_local = to_local(it.sh, rd * -1.0f);
@@ -406,7 +409,6 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                 ++depth;
                 if (depth >= J.depth) alive = false;   // the next hit would not be shaded
             }
-            W.lacc[slot] = f4(L, 0.0f);
             if (!alive) {
                 finish(W, slot);
                 continue;
