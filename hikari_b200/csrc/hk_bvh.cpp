@@ -8,6 +8,8 @@
 #include <cstring>
 #include <future>
 #include <stdexcept>
+#include <thread>
+#include <utility>
 
 #include "hk_device.h"
 
@@ -42,12 +44,59 @@ constexpr int kBins = 32;
 constexpr int kMaxDepth = 60;         // traversal stack holds 64 entries
 constexpr uint32_t kParallelMin = 1u << 16;
 
+// Centroid bins of the three axes: box and triangle count per bin.
+struct Bins {
+    Box box[3][kBins];
+    uint32_t cnt[3][kBins];
+    Bins() {
+        for (int a = 0; a < 3; a++)
+            for (int k = 0; k < kBins; k++) {
+                box[a][k].empty();
+                cnt[a][k] = 0;
+            }
+    }
+    void merge(const Bins &o) {
+        for (int a = 0; a < 3; a++)
+            for (int k = 0; k < kBins; k++) {
+                box[a][k].grow(o.box[a][k]);
+                cnt[a][k] += o.cnt[a][k];
+            }
+    }
+};
+
+constexpr uint32_t kParallelScan = 1u << 20;   // ranges this long are scanned in parallel chunks
+
 struct Builder {
     const std::vector<Box> &tb;
     const std::vector<float> &cent;
     std::vector<uint32_t> &order;
     int max_leaf;
     std::atomic<uint32_t> max_depth{0};
+
+    static uint32_t chunks_for(uint32_t n) {
+        if (n < kParallelScan) return 1;
+        const uint32_t hw = std::max(1u, std::thread::hardware_concurrency());
+        return std::min(std::min(hw, 16u), n / (kParallelScan / 4));
+    }
+
+    Bins bin_range(uint32_t i0, uint32_t i1, const Box &cb) const {
+        Bins B;
+        float scale[3];
+        for (int ax = 0; ax < 3; ax++) {
+            const float ext = cb.hi[ax] - cb.lo[ax];
+            scale[ax] = ext > 0.0f ? kBins / ext : 0.0f;
+        }
+        for (uint32_t i = i0; i < i1; i++) {
+            const uint32_t t = order[i];
+            for (int ax = 0; ax < 3; ax++) {
+                if (scale[ax] == 0.0f) continue;
+                const int k = std::min(kBins - 1, (int)((cent[3 * t + ax] - cb.lo[ax]) * scale[ax]));
+                B.cnt[ax][k]++;
+                B.box[ax][k].grow(tb[t]);
+            }
+        }
+        return B;
+    }
 
     // Builds [b, e) into its own node vector; returns the local root index.
     int32_t build(std::vector<BNode> &nodes, uint32_t b, uint32_t e, uint32_t depth) {
@@ -58,9 +107,31 @@ struct Builder {
         Box bb, cb;
         bb.empty();
         cb.empty();
-        for (uint32_t i = b; i < e; i++) {
-            bb.grow(tb[order[i]]);
-            cb.grow(&cent[3 * order[i]]);
+        const uint32_t nchunks = chunks_for(e - b);
+        if (nchunks > 1) {   // large ranges: bounds in parallel chunks (min / max reduce exactly)
+            std::vector<std::future<std::pair<Box, Box>>> f;
+            for (uint32_t q = 0; q < nchunks; ++q)
+                f.push_back(std::async(std::launch::async, [&, q] {
+                    Box x, y;
+                    x.empty();
+                    y.empty();
+                    const uint32_t i0 = b + (uint64_t)(e - b) * q / nchunks, i1 = b + (uint64_t)(e - b) * (q + 1) / nchunks;
+                    for (uint32_t i = i0; i < i1; i++) {
+                        x.grow(tb[order[i]]);
+                        y.grow(&cent[3 * order[i]]);
+                    }
+                    return std::make_pair(x, y);
+                }));
+            for (auto &x : f) {
+                auto r = x.get();
+                bb.grow(r.first);
+                cb.grow(r.second);
+            }
+        } else {
+            for (uint32_t i = b; i < e; i++) {
+                bb.grow(tb[order[i]]);
+                cb.grow(&cent[3 * order[i]]);
+            }
         }
         nodes[me].box = bb;
         uint32_t n = e - b;
@@ -72,18 +143,24 @@ struct Builder {
         if (n <= 1) return make_leaf();
         int best_axis = -1, best_split = -1;
         float best_cost = INFINITY;
+        // bins of all three axes in one pass over the range (in parallel chunks when large)
+        Bins all;
+        if (nchunks > 1) {
+            std::vector<std::future<Bins>> f;
+            for (uint32_t q = 0; q < nchunks; ++q)
+                f.push_back(std::async(std::launch::async, [&, q] {
+                    const uint32_t i0 = b + (uint64_t)(e - b) * q / nchunks, i1 = b + (uint64_t)(e - b) * (q + 1) / nchunks;
+                    return bin_range(i0, i1, cb);
+                }));
+            for (auto &x : f) all.merge(x.get());
+        } else {
+            all = bin_range(b, e, cb);
+        }
         for (int ax = 0; ax < 3; ax++) {
             float ext = cb.hi[ax] - cb.lo[ax];
             if (!(ext > 0.0f)) continue;
-            Box bins[kBins];
-            uint32_t cnt[kBins] = {0};
-            for (int k = 0; k < kBins; k++) bins[k].empty();
-            float scale = kBins / ext;
-            for (uint32_t i = b; i < e; i++) {
-                int k = std::min(kBins - 1, (int)((cent[3 * order[i] + ax] - cb.lo[ax]) * scale));
-                cnt[k]++;
-                bins[k].grow(tb[order[i]]);
-            }
+            const Box *bins = all.box[ax];
+            const uint32_t *cnt = all.cnt[ax];
             float rarea[kBins];
             uint32_t rcnt[kBins];
             Box acc;
@@ -341,8 +418,8 @@ void assign_slots(const std::vector<BNode> &nodes, const Box &nb, const int32_t 
         double score;
         int c, s;
     };
-    std::vector<Cand> cand;
-    cand.reserve(64);
+    Cand cand[64];
+    int nc = 0;
     for (int c = 0; c < n; c++) {
         const Box &b = nodes[C[c]].box;
         double d[3];
@@ -350,14 +427,17 @@ void assign_slots(const std::vector<BNode> &nodes, const Box &nb, const int32_t 
         for (int sl = 0; sl < 8; sl++) {
             double sc = 0.0;
             for (int k = 0; k < 3; k++) sc += (sl >> k & 1) ? -d[k] : d[k];
-            cand.push_back({sc, c, sl});
+            cand[nc++] = {sc, c, sl};
         }
     }
-    std::stable_sort(cand.begin(), cand.end(), [](const Cand &a, const Cand &b) { return a.score > b.score; });
+    // repeatedly take the best remaining (child, slot) pair (the first one on ties)
     bool used_c[8] = {false}, used_s[8] = {false};
     for (int s2 = 0; s2 < 8; s2++) slot_child[s2] = -1;
-    for (const Cand &x : cand) {
-        if (used_c[x.c] || used_s[x.s]) continue;
+    for (int done = 0; done < n; ++done) {
+        int best = -1;
+        for (int q = 0; q < nc; q++)
+            if (!used_c[cand[q].c] && !used_s[cand[q].s] && (best < 0 || cand[q].score > cand[best].score)) best = q;
+        const Cand &x = cand[best];
         used_c[x.c] = used_s[x.s] = true;
         slot_child[x.s] = C[x.c];
     }
@@ -437,13 +517,14 @@ BvhPair build_bvh_pair(const float *tris, uint32_t n) {
     auto is_leaf8 = [&](int32_t c) { return dp.as_leaf[c] != 0; };
     // new position of every binary leaf's first triangle
     std::vector<uint32_t> leaf_start(nodes.size(), 0);
-    auto place_subtree = [&](int32_t c, uint32_t base) {
-        std::vector<int32_t> st{c};
-        while (!st.empty()) {
-            int32_t i = st.back();
-            st.pop_back();
+    auto place_subtree = [&](int32_t c, uint32_t base) {   // c holds at most 3 triangles: at most 5 nodes
+        int32_t st[8];
+        int sp = 0;
+        st[sp++] = c;
+        while (sp > 0) {
+            const int32_t i = st[--sp];
             if (nodes[i].left < 0) leaf_start[i] = base + (nodes[i].start - sub_start[c]);
-            else { st.push_back(nodes[i].left); st.push_back(nodes[i].right); }
+            else { st[sp++] = nodes[i].left; st[sp++] = nodes[i].right; }
         }
     };
     std::vector<uint32_t> &order = P.bvh2.tri_order;
@@ -479,7 +560,8 @@ BvhPair build_bvh_pair(const float *tris, uint32_t n) {
         W.resize(W.size() + 20 * (size_t)ninternal, 0u);
         const uint32_t tri_base = (uint32_t)order.size();
         uint32_t imask = 0, meta[8] = {0};
-        std::vector<Todo> kids;
+        Todo kids[8];
+        int nkids = 0;
         uint32_t j = 0;
         const Box *cb[8];
         for (int s = 0; s < 8; s++) {
@@ -489,7 +571,7 @@ BvhPair build_bvh_pair(const float *tris, uint32_t n) {
             if (!is_leaf8(c)) {
                 imask |= 1u << s;
                 meta[s] = 1u << 5 | (24u + (uint32_t)s);   // one hit bit at 24 + slot
-                kids.push_back({child_base + j++, c, t.depth + 1});
+                kids[nkids++] = {child_base + j++, c, t.depth + 1};
             } else {
                 const uint32_t off = (uint32_t)order.size() - tri_base, cnt = sub_count[c];
                 if (cnt < 1 || cnt > 3 || off > 21) throw std::runtime_error("BVH8 leaf layout");
@@ -505,7 +587,7 @@ BvhPair build_bvh_pair(const float *tris, uint32_t n) {
         w[6] = meta[0] | meta[1] << 8 | meta[2] << 16 | meta[3] << 24;
         w[7] = meta[4] | meta[5] << 8 | meta[6] << 16 | meta[7] << 24;
         quantize(w, nodes[t.b].box, cb);
-        for (auto it = kids.rbegin(); it != kids.rend(); ++it) todo.push_back(*it);
+        for (int q = nkids - 1; q >= 0; --q) todo.push_back(kids[q]);
     }
     if (order.size() != n) throw std::runtime_error("BVH8 collapse lost triangles");
     P.bvh8.depth = depth8;
