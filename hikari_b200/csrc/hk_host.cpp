@@ -1160,7 +1160,7 @@ int hk_bsdf_batch(hk_scene *s, int32_t bsdf, uint64_t n, const float *wi, const 
         if (bsdf < 0 || bsdf >= s->dev.nbsdfs) throw HkError{HK_ERR_INVALID, "invalid BSDF id"};
         if (n == 0) return HK_OK;
         if (!wi || !u2 || !wo) throw HkError{HK_ERR_INVALID, "bad arguments"};
-        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf,
+        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, s->bsdfs[bsdf].type, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf,
                                       (cudaStream_t)stream));
         return HK_OK;
     });

@@ -284,6 +284,9 @@ __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int
 
 // Config-2 BSDF batch: per record Sample (wo, weight, pdf of the sampled
 // direction, measure), Eval and Pdf at the given wo with ESolidAngle.
+// One instantiation per top-level BSDF type (the host picks the id's type),
+// so a launch carries only that BSDF's code.
+template <int BT>
 __global__ void bsdf_batch_kernel(DevScene S, int bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
                                   const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
                                   float *p_pdf) {
@@ -293,21 +296,21 @@ __global__ void bsdf_batch_kernel(DevScene S, int bsdf, uint64_t n, const float 
         r.wo = v3(0, 0, 0);
         r.measure = kMeasureUnknown;
         r.eta = 0.0f;
-        V3 w = bsdf_sample(S.bsdfs, bsdf, r, u2[2 * i], u2[2 * i + 1], u1 ? u1[i] : 0.0f);
+        V3 w = bsdf_sample_t<BT>(S.bsdfs, bsdf, r, u2[2 * i], u2[2 * i + 1], u1 ? u1[i] : 0.0f);
         if (s_wo) { s_wo[3 * i] = r.wo.x; s_wo[3 * i + 1] = r.wo.y; s_wo[3 * i + 2] = r.wo.z; }
         if (s_w) { s_w[3 * i] = w.x; s_w[3 * i + 1] = w.y; s_w[3 * i + 2] = w.z; }
         if (s_m) s_m[i] = r.measure;
-        if (s_pdf) s_pdf[i] = all_zero(w) ? 0.0f : bsdf_pdf(S.bsdfs, bsdf, r);
+        if (s_pdf) s_pdf[i] = all_zero(w) ? 0.0f : bsdf_pdf_t<BT>(S.bsdfs, bsdf, r);
         BRec q;
         q.wi = r.wi;
         q.wo = v3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
         q.measure = kMeasureSolidAngle;
         q.eta = 0.0f;
         if (e_rgb) {
-            V3 e = bsdf_eval(S.bsdfs, bsdf, q);
+            V3 e = bsdf_eval_t<BT>(S.bsdfs, bsdf, q);
             e_rgb[3 * i] = e.x; e_rgb[3 * i + 1] = e.y; e_rgb[3 * i + 2] = e.z;
         }
-        if (p_pdf) p_pdf[i] = bsdf_pdf(S.bsdfs, bsdf, q);
+        if (p_pdf) p_pdf[i] = bsdf_pdf_t<BT>(S.bsdfs, bsdf, q);
     }
 }
 
@@ -403,10 +406,17 @@ cudaError_t launch_trace(const DevScene &S, uint64_t n, const float *rays, int32
         trace_rays_kernel<kAccelBvh2><<<grid_for(n, 128), 128, 0, st>>>(S, n, rays, tri, t, u, v, any_hit, visits);
     return cudaGetLastError();
 }
-cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
+cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, int type, uint64_t n, const float *wi, const float *u2, const float *u1,
                               const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
                               float *p_pdf, cudaStream_t st) {
-    bsdf_batch_kernel<<<grid_for(n, 256), 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf);
+    const int g = grid_for(n, 256);
+    switch (type) {
+    case 0: bsdf_batch_kernel<0><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
+    case 1: bsdf_batch_kernel<1><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
+    case 2: bsdf_batch_kernel<2><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
+    case 3: bsdf_batch_kernel<3><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
+    default: bsdf_batch_kernel<4><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_emitter_sample(const DevScene &S, int e, uint64_t n, const float *in, float *out, cudaStream_t st) {
