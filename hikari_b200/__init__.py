@@ -34,6 +34,7 @@ class BsdfDesc(C.Structure):
         ("alpha_u", C.c_float), ("alpha_v", C.c_float), ("int_ior", C.c_float), ("ext_ior", C.c_float),
         ("eta", C.c_float * 3), ("k", C.c_float * 3), ("ks", C.c_float * 3), ("ks_refract", C.c_float * 3),
         ("kd", C.c_float * 3), ("sigma_a", C.c_float * 3), ("thickness", C.c_float), ("nested", C.c_int32),
+        ("nested2", C.c_int32),
     ]
 
 
@@ -185,14 +186,14 @@ def _stream(stream) -> Optional[int]:
     return getattr(stream, "cuda_stream", stream)
 
 
-def bsdf_desc_c(d: BSDFDesc, nested_id: int = -1) -> BsdfDesc:
+def bsdf_desc_c(d: BSDFDesc, nested_id: int = -1, nested2_id: int = -1) -> BsdfDesc:
     c = BsdfDesc()
     c.type, c.distribution = d.type, d.distribution
     c.anisotropic, c.nonlinear = int(d.anisotropic), int(d.nonlinear)
     c.alpha_u, c.alpha_v, c.int_ior, c.ext_ior = d.alpha_u, d.alpha_v, d.int_ior, d.ext_ior
     c.eta[:] = d.conductor_eta()
     c.k[:], c.ks[:], c.ks_refract[:], c.kd[:], c.sigma_a[:] = d.k, d.ks, d.ks_refract, d.kd, d.sigma_a
-    c.thickness, c.nested = d.thickness, nested_id
+    c.thickness, c.nested, c.nested2 = d.thickness, nested_id, nested2_id
     return c
 
 
@@ -230,7 +231,8 @@ class Scene:
                 if id(d) in ids:
                     return ids[id(d)]
                 nested = add_bsdf(d.nested) if d.nested is not None else -1
-                c = bsdf_desc_c(d, nested)
+                nested2 = add_bsdf(d.nested2) if d.nested2 is not None else -1
+                c = bsdf_desc_c(d, nested, nested2)
                 out = C.c_int32()
                 check(L.hk_scene_add_bsdf(h, C.byref(c), C.byref(out)))
                 ids[id(d)] = out.value

@@ -20,6 +20,7 @@ import numpy as np
 
 # BSDF kinds, matching hk_bsdf_type in include/hikari_b200.h
 BSDF_DIFFUSE, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_PLASTIC, BSDF_ROUGH_COATING = range(5)
+BSDF_MIRROR, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_PLASTIC, BSDF_TWO_SIDED = range(5, 10)
 BECKMANN, GGX = 0, 1
 BSDF_TYPE_NAMES = {
     "diffuse": BSDF_DIFFUSE,
@@ -27,7 +28,14 @@ BSDF_TYPE_NAMES = {
     "roughDielectric": BSDF_ROUGH_DIELECTRIC,
     "roughPlastic": BSDF_ROUGH_PLASTIC,
     "roughCoating": BSDF_ROUGH_COATING,
+    "mirror": BSDF_MIRROR,
+    "conductor": BSDF_CONDUCTOR,
+    "dielectric": BSDF_DIELECTRIC,
+    "plastic": BSDF_PLASTIC,
+    "twoSided": BSDF_TWO_SIDED,
 }
+# BSDFs with a delta (specular) lobe and no microfacet distribution
+SMOOTH_BSDFS = (BSDF_MIRROR, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_PLASTIC)
 FILTER_KINDS = {"box": 0, "tent": 1, "gaussian": 2, "mitchell": 3}
 
 AIR_IOR = 1.000277  # DEFAULT_*_EXT_IOR, include/core/Common.hpp:333
@@ -57,7 +65,8 @@ class BSDFDesc:
     kd: List[float] = field(default_factory=lambda: [0.5, 0.5, 0.5])
     sigma_a: List[float] = field(default_factory=lambda: [0.0, 0.0, 0.0])
     thickness: float = 1.0
-    nested: Optional["BSDFDesc"] = None
+    nested: Optional["BSDFDesc"] = None    # roughCoating's BSDF, twoSided's front BSDF
+    nested2: Optional["BSDFDesc"] = None   # twoSided's back BSDF (None: the front one)
 
     def conductor_eta(self) -> List[float]:
         if self.eta is not None:
@@ -297,6 +306,33 @@ def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
         d.ks = p.get("ks", [1.0, 1.0, 1.0])
         d.kd = p.get("kd", [0.5, 0.5, 0.5])
         d.nonlinear = bool(p.get("nonlinear", False))
+    elif d.type == BSDF_CONDUCTOR:   # src/bsdf/ConductorBSDF.cpp:11
+        d.int_ior = p.get("intIOR", 1.5046)
+        d.ext_ior = p.get("extIOR", AIR_IOR)
+        d.k = p.get("k", [1.0, 1.0, 1.0])
+        d.ks = p.get("ks", [1.0, 1.0, 1.0])
+    elif d.type == BSDF_DIELECTRIC:   # src/bsdf/DielectricBSDF.cpp:9
+        d.int_ior = p.get("intIOR", 1.5046)
+        d.ext_ior = p.get("extIOR", AIR_IOR)
+        d.ks = p.get("ksReflect", [1.0, 1.0, 1.0])
+        d.ks_refract = p.get("ksRefract", [1.0, 1.0, 1.0])
+    elif d.type == BSDF_PLASTIC:   # src/bsdf/PlasticBSDF.cpp:10
+        d.int_ior = p.get("intIOR", 1.5046)
+        d.ext_ior = p.get("extIOR", AIR_IOR)
+        d.ks = p.get("ks", [1.0, 1.0, 1.0])
+        d.kd = p.get("kd", [0.5, 0.5, 0.5])
+        d.nonlinear = bool(p.get("nonlinear", False))
+    elif d.type == BSDF_TWO_SIDED:   # src/bsdf/TwoSidedBSDF.cpp:86-125
+        nested = [c for c in node if c.tag == "bsdf"]
+        if not nested:
+            raise SceneError("TwoSidedBSDF needs at least one nested BSDF!")
+        if len(nested) > 2:
+            raise SceneError("TwoSidedBSDF: tried to specify the third nested BSDF")
+        d.nested = _bsdf_from_xml(nested[0])
+        d.nested2 = _bsdf_from_xml(nested[1]) if len(nested) == 2 else None
+        for b in (d.nested, d.nested2 or d.nested):
+            if b.type in (BSDF_DIELECTRIC, BSDF_ROUGH_DIELECTRIC):
+                raise SceneError("TwoSidedBSDF: nested BSDFs should not have transmission")
     elif d.type == BSDF_ROUGH_COATING:
         d.int_ior = p.get("intIOR", 1.49)
         d.ext_ior = p.get("extIOR", AIR_IOR)

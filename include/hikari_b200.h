@@ -36,6 +36,11 @@ typedef struct hk_scene hk_scene;
 #define HK_BSDF_ROUGH_DIELECTRIC 2 /* "roughDielectric" src/bsdf/RoughDielectricBSDF.cpp*/
 #define HK_BSDF_ROUGH_PLASTIC 3    /* "roughPlastic"    src/bsdf/RoughPlasticBSDF.cpp   */
 #define HK_BSDF_ROUGH_COATING 4    /* "roughCoating"    src/bsdf/RoughCoatingBSDF.cpp   */
+#define HK_BSDF_MIRROR 5           /* "mirror"          src/bsdf/MirrorBSDF.cpp         */
+#define HK_BSDF_CONDUCTOR 6        /* "conductor"       src/bsdf/ConductorBSDF.cpp      */
+#define HK_BSDF_DIELECTRIC 7       /* "dielectric"      src/bsdf/DielectricBSDF.cpp     */
+#define HK_BSDF_PLASTIC 8          /* "plastic"         src/bsdf/PlasticBSDF.cpp        */
+#define HK_BSDF_TWO_SIDED 9        /* "twoSided"        src/bsdf/TwoSidedBSDF.cpp       */
 #define HK_BECKMANN 0
 #define HK_GGX 1
 
@@ -56,7 +61,8 @@ typedef struct {
     float kd[3];           /* roughPlastic "kd", diffuse "albedo" */
     float sigma_a[3];      /* roughCoating "sigmaA" */
     float thickness;       /* roughCoating "thickness" */
-    int32_t nested;        /* roughCoating: id of the nested BSDF (added first), else -1 */
+    int32_t nested;        /* roughCoating / twoSided front: id of the nested BSDF (added first), else -1 */
+    int32_t nested2;       /* twoSided back: id of the second nested BSDF, -1 = the front one */
 } hk_bsdf_desc;
 
 typedef struct {

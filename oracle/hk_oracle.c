@@ -589,6 +589,21 @@ static float filter_eval(const ho_scene *s, float x) {
 
 static int bvh_build(ho_scene *s);
 
+static float approx_fresnel_diffuse(float e);
+/* Whether a BSDF has a transmission lobe (EDeltaTransmission / EGlossyTransmission;
+ * coatings inherit their nested BSDF's types, RoughCoatingBSDF.cpp:317). */
+static int bsdf_transmits(const ho_scene *s, int id, int depth) {
+    if (id < 0 || id >= s->nb || depth > 8) return 0;
+    const ho_bsdf_desc *d = &s->bsdfs[id].d;
+    switch (d->type) {
+    case HO_BSDF_ROUGH_DIELECTRIC: case HO_BSDF_DIELECTRIC: return 1;
+    case HO_BSDF_ROUGH_COATING: return bsdf_transmits(s, d->nested, depth + 1);
+    case HO_BSDF_TWO_SIDED:
+        return bsdf_transmits(s, d->nested, depth + 1) || bsdf_transmits(s, d->nested2, depth + 1);
+    default: return 0;
+    }
+}
+
 /* BSDF activation: RoughPlasticBSDF::Activate :261, RoughCoatingBSDF::Activate :315 */
 static int activate_bsdf(ho_scene *s, bsdf_t *b) {
     const ho_bsdf_desc *d = &b->d;
@@ -628,6 +643,21 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
         }
         free(t2d); free(d1d);
     }
+    if (d->type == HO_BSDF_CONDUCTOR)   /* ConductorBSDF ctor :17: m_Eta = Color3f(intIOR / extIOR) */
+        for (int c = 0; c < 3; c++) b->eta_c[c] = b->eta;
+    if (d->type == HO_BSDF_PLASTIC) {   /* PlasticBSDF ctor :25 and Activate :170 */
+        float ksa = lum(vload(d->ks)), kda = lum(vload(d->kd));
+        b->spec_w = ksa / (kda + ksa);
+        b->fdr_int = approx_fresnel_diffuse(b->inv_eta);
+    }
+    if (d->type == HO_BSDF_TWO_SIDED) {   /* TwoSidedBSDF::Activate :98 */
+        if (d->nested < 0 || d->nested >= s->nb) return fail("TwoSidedBSDF needs at least one nested BSDF!");
+        if (d->nested2 >= s->nb) return fail("twoSided: invalid second nested BSDF");
+        if (d->nested2 < 0) b->d.nested2 = d->nested;
+        if (bsdf_transmits(s, d->nested, 0) || bsdf_transmits(s, b->d.nested2, 0))
+            return fail("Only BSDF without transmission can be nested!");
+    }
+    if (d->type < HO_BSDF_DIFFUSE || d->type > HO_BSDF_TWO_SIDED) return fail("unknown BSDF type");
     return 0;
 }
 
@@ -962,6 +992,166 @@ static v3 coating_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux, 
     return divs(coating_eval(s, b, r), P);
 }
 
+/* ------------------------------------------------------- smooth BSDFs */
+/* Delta-direction match |d . wo - 1| <= DeltaEpsilon (include/core/Common.hpp:46).
+ * DeltaEpsilon is the double literal 1e-3: the comparison is made in double. */
+static inline int delta_match(v3 d, v3 wo) { return (double)fabsf(dot(d, wo) - 1.0f) <= 1e-3; }
+/* Reflect / Refract about the local normal  src/core/Common.cpp:606-615 */
+static inline v3 reflect_n(v3 wi) { return V(-wi.x, -wi.y, wi.z); }
+static inline v3 refract_n(v3 wi, float ct, float eta, float inv_eta) {
+    float sc = -(ct < 0.0f ? inv_eta : eta);
+    return V(sc * wi.x, sc * wi.y, ct);
+}
+/* ApproxFresnelDiffuseReflectance  src/core/Common.cpp:550: the published fits of
+ * Egan & Hilgeman (1973) for eta < 1 and d'Eon & Irving (2011) otherwise. */
+static float approx_fresnel_diffuse(float e) {
+    if (e < 1.0f) return -1.4399f * (e * e) + 0.7099f * e + 0.6681f + 0.0636f / e;
+    float i1 = 1.0f / e, i2 = i1 * i1, i3 = i2 * i1, i4 = i3 * i1, i5 = i4 * i1;
+    return 0.919317f - 3.4793f * i1 + 6.75335f * i2 - 7.80989f * i3 + 4.98554f * i4 - 1.36881f * i5;
+}
+
+/* MirrorBSDF  src/bsdf/MirrorBSDF.cpp:15-55 (the measure is set only past the cosine test) */
+static int mirror_match(const brec *r) {
+    return r->wi.z > 0.0f && r->wo.z > 0.0f && r->measure == HO_MEASURE_DISCRETE && delta_match(reflect_n(r->wi), r->wo);
+}
+static v3 mirror_sample(brec *r) {
+    if (r->wi.z <= 0) return V(0, 0, 0);
+    r->wo = reflect_n(r->wi);
+    r->measure = HO_MEASURE_DISCRETE;
+    r->eta = 1.0f;
+    return V(1, 1, 1);
+}
+static v3 mirror_eval(const brec *r) { return mirror_match(r) ? V(1, 1, 1) : V(0, 0, 0); }
+static float mirror_pdf(const brec *r) { return mirror_match(r) ? 1.0f : 0.0f; }
+
+/* ConductorBSDF  src/bsdf/ConductorBSDF.cpp:32-70 (eta = intIOR/extIOR on every channel) */
+static v3 sconductor_sample(const bsdf_t *b, brec *r) {
+    r->measure = HO_MEASURE_DISCRETE;
+    float ci = r->wi.z;
+    if (ci <= 0.0f) return V(0, 0, 0);
+    v3 F = fresnel_conductor(ci, b->eta_c, b->k_c);
+    r->wo = reflect_n(r->wi);
+    r->eta = 1.0f;
+    return mul(vload(b->d.ks), F);
+}
+static v3 sconductor_eval(const bsdf_t *b, const brec *r) {
+    if (!mirror_match(r)) return V(0, 0, 0);
+    return mul(vload(b->d.ks), fresnel_conductor(r->wi.z, b->eta_c, b->k_c));
+}
+static float sconductor_pdf(const brec *r) { return mirror_match(r) ? 1.0f : 0.0f; }
+
+/* DielectricBSDF  src/bsdf/DielectricBSDF.cpp:33-110 (Eval and Pdf test no measure) */
+static v3 sdielectric_sample(const bsdf_t *b, brec *r, float ux) {
+    r->measure = HO_MEASURE_DISCRETE;
+    float ct;
+    float F = fresnel_dielectric(r->wi.z, b->eta, b->inv_eta, &ct);
+    if (ux < F) {
+        r->wo = reflect_n(r->wi);
+        r->eta = 1.0f;
+        return vload(b->d.ks);
+    }
+    r->wo = refract_n(r->wi, ct, b->eta, b->inv_eta);
+    r->eta = ct < 0.0f ? b->eta : b->inv_eta;
+    float f = ct < 0.0f ? b->inv_eta : b->eta;   /* radiance transport */
+    return scl(vload(b->d.ks_refract), f * f);
+}
+static v3 sdielectric_eval(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z, ct;
+    float F = fresnel_dielectric(ci, b->eta, b->inv_eta, &ct);
+    if (ci * co >= 0.0f) {
+        if (delta_match(reflect_n(r->wi), r->wo)) return scl(vload(b->d.ks), F);
+    } else if (delta_match(refract_n(r->wi, ct, b->eta, b->inv_eta), r->wo)) {
+        float f = ct < 0.0f ? b->inv_eta : b->eta;
+        return scl(scl(vload(b->d.ks_refract), f * f), 1.0f - F);
+    }
+    return V(0, 0, 0);
+}
+static float sdielectric_pdf(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z, ct;
+    float F = fresnel_dielectric(ci, b->eta, b->inv_eta, &ct);
+    if (ci * co >= 0.0f) {
+        if (delta_match(reflect_n(r->wi), r->wo)) return F;
+    } else if (delta_match(refract_n(r->wi, ct, b->eta, b->inv_eta), r->wo)) {
+        return 1.0f - F;
+    }
+    return 0.0f;
+}
+
+/* PlasticBSDF  src/bsdf/PlasticBSDF.cpp:33-142 */
+static float splastic_spec_pdf(const bsdf_t *b, float Fi) {
+    return (Fi * b->spec_w) / (Fi * b->spec_w + (1.0f - Fi) * (1.0f - b->spec_w));
+}
+static v3 splastic_diffuse(const bsdf_t *b) {
+    v3 dif = vload(b->d.kd);
+    float fdr = b->fdr_int;
+    if (b->d.nonlinear) return V(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
+    return divs(dif, 1.0f - fdr);
+}
+static v3 splastic_sample(const bsdf_t *b, brec *r, float ux, float uy) {
+    float ci = r->wi.z;
+    if (ci <= 0.0f) return V(0, 0, 0);
+    float ct;
+    float Fi = fresnel_dielectric(ci, b->eta, b->inv_eta, &ct);
+    float sp = splastic_spec_pdf(b, Fi);
+    r->eta = 1.0f;
+    if (ux < sp) {
+        r->measure = HO_MEASURE_DISCRETE;
+        r->wo = reflect_n(r->wi);
+        return divs(scl(vload(b->d.ks), Fi), sp);
+    }
+    r->measure = HO_MEASURE_SOLID_ANGLE;
+    r->wo = square_to_cos_hemi((ux - sp) / (1.0f - sp), uy);
+    float Fo = fresnel_dielectric(r->wo.z, b->eta, b->inv_eta, &ct);
+    return scl(splastic_diffuse(b), b->inv_eta2 * (1.0f - Fi) * (1.0f - Fo) / (1.0f - sp));
+}
+static v3 splastic_eval(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (r->measure == HO_MEASURE_UNKNOWN || ci <= 0.0f || co <= 0.0f) return V(0, 0, 0);
+    float ct;
+    float Fi = fresnel_dielectric(ci, b->eta, b->inv_eta, &ct);
+    if (r->measure == HO_MEASURE_DISCRETE)
+        return delta_match(reflect_n(r->wi), r->wo) ? scl(vload(b->d.ks), Fi) : V(0, 0, 0);
+    float Fo = fresnel_dielectric(co, b->eta, b->inv_eta, &ct);
+    return scl(splastic_diffuse(b), cos_hemi_pdf(r->wo) * b->inv_eta2 * (1.0f - Fi) * (1.0f - Fo));
+}
+static float splastic_pdf(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (r->measure == HO_MEASURE_UNKNOWN || ci <= 0.0f || co <= 0.0f) return 0.0f;
+    float ct;
+    float Fi = fresnel_dielectric(ci, b->eta, b->inv_eta, &ct);
+    float sp = splastic_spec_pdf(b, Fi);
+    if (r->measure == HO_MEASURE_DISCRETE)
+        return delta_match(reflect_n(r->wi), r->wo) ? 1.0f - sp : 0.0f;   /* 1 - SpecularPDF, as :118 */
+    return cos_hemi_pdf(r->wo) * (1.0f - sp);
+}
+
+/* TwoSidedBSDF  src/bsdf/TwoSidedBSDF.cpp:19-67: the back side mirrors z into the second BSDF */
+static v3 twosided_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux, float uy, ho_pcg32 *rng,
+                          const float *u1f) {
+    int flip = r->wi.z < 0.0f;
+    if (flip) r->wi.z *= -1.0f;
+    v3 res = bsdf_sample(s, flip ? b->d.nested2 : b->d.nested, r, ux, uy, rng, u1f);
+    if (flip) {
+        r->wi.z *= -1.0f;
+        if (!is_zero(res)) r->wo.z *= -1.0f;
+    }
+    return res;
+}
+static v3 twosided_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
+    brec c = *r;
+    if (c.wi.z > 0.0f) return bsdf_eval(s, b->d.nested, &c);
+    c.wi.z *= -1.0f;
+    c.wo.z *= -1.0f;
+    return bsdf_eval(s, b->d.nested2, &c);
+}
+static float twosided_pdf(const ho_scene *s, const bsdf_t *b, const brec *r) {
+    brec c = *r;
+    if (c.wi.z > 0.0f) return bsdf_pdf(s, b->d.nested, &c);
+    c.wi.z *= -1.0f;
+    c.wo.z *= -1.0f;
+    return bsdf_pdf(s, b->d.nested2, &c);
+}
+
 static v3 bsdf_eval(const ho_scene *s, int id, const brec *r) {
     const bsdf_t *b = &s->bsdfs[id];
     switch (b->d.type) {
@@ -969,7 +1159,12 @@ static v3 bsdf_eval(const ho_scene *s, int id, const brec *r) {
     case HO_BSDF_ROUGH_CONDUCTOR: return conductor_eval(b, r);
     case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_eval(b, r);
     case HO_BSDF_ROUGH_PLASTIC: return plastic_eval(b, r);
-    default: return coating_eval(s, b, r);
+    case HO_BSDF_ROUGH_COATING: return coating_eval(s, b, r);
+    case HO_BSDF_MIRROR: return mirror_eval(r);
+    case HO_BSDF_CONDUCTOR: return sconductor_eval(b, r);
+    case HO_BSDF_DIELECTRIC: return sdielectric_eval(b, r);
+    case HO_BSDF_PLASTIC: return splastic_eval(b, r);
+    default: return twosided_eval(s, b, r);
     }
 }
 static float bsdf_pdf(const ho_scene *s, int id, const brec *r) {
@@ -979,7 +1174,12 @@ static float bsdf_pdf(const ho_scene *s, int id, const brec *r) {
     case HO_BSDF_ROUGH_CONDUCTOR: return conductor_pdf(b, r);
     case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_pdf(b, r);
     case HO_BSDF_ROUGH_PLASTIC: return plastic_pdf(b, r);
-    default: return coating_pdf(s, b, r);
+    case HO_BSDF_ROUGH_COATING: return coating_pdf(s, b, r);
+    case HO_BSDF_MIRROR: return mirror_pdf(r);
+    case HO_BSDF_CONDUCTOR: return sconductor_pdf(r);
+    case HO_BSDF_DIELECTRIC: return sdielectric_pdf(b, r);
+    case HO_BSDF_PLASTIC: return splastic_pdf(b, r);
+    default: return twosided_pdf(s, b, r);
     }
 }
 static v3 bsdf_sample(const ho_scene *s, int id, brec *r, float ux, float uy, ho_pcg32 *rng, const float *u1f) {
@@ -989,7 +1189,12 @@ static v3 bsdf_sample(const ho_scene *s, int id, brec *r, float ux, float uy, ho
     case HO_BSDF_ROUGH_CONDUCTOR: return conductor_sample(b, r, ux, uy);
     case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_sample(b, r, ux, uy, rng, u1f);
     case HO_BSDF_ROUGH_PLASTIC: return plastic_sample(b, r, ux, uy);
-    default: return coating_sample(s, b, r, ux, uy, rng, u1f);
+    case HO_BSDF_ROUGH_COATING: return coating_sample(s, b, r, ux, uy, rng, u1f);
+    case HO_BSDF_MIRROR: return mirror_sample(r);
+    case HO_BSDF_CONDUCTOR: return sconductor_sample(b, r);
+    case HO_BSDF_DIELECTRIC: return sdielectric_sample(b, r, ux);
+    case HO_BSDF_PLASTIC: return splastic_sample(b, r, ux, uy);
+    default: return twosided_sample(s, b, r, ux, uy, rng, u1f);
     }
 }
 

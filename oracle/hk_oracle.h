@@ -28,7 +28,12 @@ enum {
     HO_BSDF_ROUGH_CONDUCTOR = 1,  /* "roughConductor"   src/bsdf/RoughConductorBSDF.cpp */
     HO_BSDF_ROUGH_DIELECTRIC = 2, /* "roughDielectric"  src/bsdf/RoughDielectricBSDF.cpp*/
     HO_BSDF_ROUGH_PLASTIC = 3,    /* "roughPlastic"     src/bsdf/RoughPlasticBSDF.cpp   */
-    HO_BSDF_ROUGH_COATING = 4     /* "roughCoating"     src/bsdf/RoughCoatingBSDF.cpp   */
+    HO_BSDF_ROUGH_COATING = 4,    /* "roughCoating"     src/bsdf/RoughCoatingBSDF.cpp   */
+    HO_BSDF_MIRROR = 5,           /* "mirror"           src/bsdf/MirrorBSDF.cpp         */
+    HO_BSDF_CONDUCTOR = 6,        /* "conductor"        src/bsdf/ConductorBSDF.cpp      */
+    HO_BSDF_DIELECTRIC = 7,       /* "dielectric"       src/bsdf/DielectricBSDF.cpp     */
+    HO_BSDF_PLASTIC = 8,          /* "plastic"          src/bsdf/PlasticBSDF.cpp        */
+    HO_BSDF_TWO_SIDED = 9         /* "twoSided"         src/bsdf/TwoSidedBSDF.cpp       */
 };
 enum { HO_BECKMANN = 0, HO_GGX = 1 };
 enum { HO_MEASURE_UNKNOWN = 0, HO_MEASURE_SOLID_ANGLE = 1, HO_MEASURE_DISCRETE = 2 };
@@ -48,7 +53,8 @@ typedef struct {
     float kd[3];           /* roughPlastic kd, diffuse albedo */
     float sigma_a[3];      /* roughCoating sigmaA */
     float thickness;       /* roughCoating thickness */
-    int32_t nested;        /* roughCoating: index of the nested BSDF, else -1 */
+    int32_t nested;        /* roughCoating / twoSided (front): index of the nested BSDF, else -1 */
+    int32_t nested2;       /* twoSided (back): index of the second nested BSDF, -1 = the front one */
 } ho_bsdf_desc;
 
 typedef struct ho_scene ho_scene;

@@ -35,6 +35,7 @@ class BsdfDescC(C.Structure):
         ("alpha_u", C.c_float), ("alpha_v", C.c_float), ("int_ior", C.c_float), ("ext_ior", C.c_float),
         ("eta", C.c_float * 3), ("k", C.c_float * 3), ("ks", C.c_float * 3), ("ks_refract", C.c_float * 3),
         ("kd", C.c_float * 3), ("sigma_a", C.c_float * 3), ("thickness", C.c_float), ("nested", C.c_int32),
+        ("nested2", C.c_int32),
     ]
 
 
@@ -90,14 +91,14 @@ def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
-def bsdf_desc_c(d, nested_index=-1) -> BsdfDescC:
+def bsdf_desc_c(d, nested_index=-1, nested2_index=-1) -> BsdfDescC:
     c = BsdfDescC()
     c.type, c.distribution = d.type, d.distribution
     c.anisotropic, c.nonlinear = int(d.anisotropic), int(d.nonlinear)
     c.alpha_u, c.alpha_v, c.int_ior, c.ext_ior = d.alpha_u, d.alpha_v, d.int_ior, d.ext_ior
     c.eta[:] = d.conductor_eta()
     c.k[:], c.ks[:], c.ks_refract[:], c.kd[:], c.sigma_a[:] = d.k, d.ks, d.ks_refract, d.kd, d.sigma_a
-    c.thickness, c.nested = d.thickness, nested_index
+    c.thickness, c.nested, c.nested2 = d.thickness, nested_index, nested2_index
     return c
 
 
@@ -165,7 +166,8 @@ class OracleScene:
         if key in self.bsdf_ids:
             return self.bsdf_ids[key]
         nested = self.add_bsdf(d.nested) if d.nested is not None else -1
-        c = bsdf_desc_c(d, nested)
+        nested2 = self.add_bsdf(d.nested2) if getattr(d, "nested2", None) is not None else -1
+        c = bsdf_desc_c(d, nested, nested2)
         self._keep.append(c)
         i = lib().ho_scene_add_bsdf(self.h, C.byref(c))
         self.bsdf_ids[key] = i

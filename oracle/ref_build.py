@@ -30,7 +30,8 @@ LIB = os.path.join(OUT, "libhikari_ref_bsdf.so")
 CORE = ["Object", "PropertyList", "BSDF", "Texture", "MicrofacetDistribution", "RoughTransmitance", "Frame",
         "Sampling", "Color", "Vector", "Transform", "Sampler", "Intersection", "Timer", "MemoryArena", "Shape",
         "Mesh", "Emitter", "DiscretePDF", "BoundingBox", "Ray"]
-BSDFS = ["DiffuseBSDF", "RoughConductorBSDF", "RoughDielectricBSDF", "RoughPlasticBSDF", "RoughCoatingBSDF"]
+BSDFS = ["DiffuseBSDF", "RoughConductorBSDF", "RoughDielectricBSDF", "RoughPlasticBSDF", "RoughCoatingBSDF",
+         "MirrorBSDF", "ConductorBSDF", "DielectricBSDF", "PlasticBSDF", "TwoSidedBSDF"]
 
 
 def _link(src, dst):
@@ -58,6 +59,9 @@ def build(ref: str = "/root/reference") -> str:
     for hdr in glob.glob(os.path.join(ref, "include", "*", "*.hpp")):
         sub = os.path.basename(os.path.dirname(hdr))
         _forward(hdr, os.path.join(shim, f"{sub}\\{os.path.basename(hdr)}"))
+    # TwoSidedBSDF.cpp includes its header by the relative Windows path "..\\..\\include\\bsdf\\..."
+    _forward(os.path.join(ref, "include", "bsdf", "TwoSidedBSDF.hpp"),
+             os.path.join(shim, "..\\..\\include\\bsdf\\TwoSidedBSDF.hpp"))
     for name, real in [("Core", "Core"), ("Geometry", "Geometry"), ("Lu", "LU")]:
         _forward(os.path.join(ref, "ext", "eigen", "Eigen", real), os.path.join(shim, f"Eigen\\{name}"))
     _forward(os.path.join(HERE, "ref_shim", "glog_logging.h"), os.path.join(shim, "glog\\logging.h"))

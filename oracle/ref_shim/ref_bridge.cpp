@@ -34,26 +34,37 @@ extern "C" {
 
 void hr_init(const char *search_dir) { GetFileResolver()->prepend(filesystem::path(search_dir)); }
 
-/* type: 0 diffuse, 1 roughConductor, 2 roughDielectric, 3 roughPlastic, 4 roughCoating */
+/* type: 0 diffuse, 1 roughConductor, 2 roughDielectric, 3 roughPlastic, 4 roughCoating,
+ * 5 mirror, 6 conductor, 7 dielectric, 8 plastic, 9 twoSided (nested, then nested2 if given) */
 void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_ior, const float *k,
-                     const float *ks, const float *kd, const float *sigma_a, float thickness, void *nested) {
-    static const char *names[] = {"diffuse", "roughConductor", "roughDielectric", "roughPlastic", "roughCoating"};
+                     const float *ks, const float *kd, const float *sigma_a, float thickness, void *nested,
+                     void *nested2, const float *ks_refract, int nonlinear) {
+    static const char *names[] = {"diffuse", "roughConductor", "roughDielectric", "roughPlastic", "roughCoating",
+                                  "mirror", "conductor", "dielectric", "plastic", "twoSided"};
+    auto col = [](const float *c) { return Color3f(c[0], c[1], c[2]); };
     try {
         PropertyList pl;
         if (type == 0) {
-            pl.SetColor("albedo", Color3f(kd[0], kd[1], kd[2]));
-        } else {
+            pl.SetColor("albedo", col(kd));
+        } else if (type <= 4) {
             pl.SetString("type", ggx ? "ggx" : "beckmann");
             pl.SetFloat("alpha", alpha);
             pl.SetFloat("intIOR", int_ior);
             pl.SetFloat("extIOR", ext_ior);
-            if (type == 1) { pl.SetColor("k", Color3f(k[0], k[1], k[2])); pl.SetColor("ks", Color3f(ks[0], ks[1], ks[2])); }
-            if (type == 2) pl.SetColor("ksReflect", Color3f(ks[0], ks[1], ks[2]));
-            if (type == 3) { pl.SetColor("ks", Color3f(ks[0], ks[1], ks[2])); pl.SetColor("kd", Color3f(kd[0], kd[1], kd[2])); }
-            if (type == 4) { pl.SetColor("ks", Color3f(ks[0], ks[1], ks[2])); pl.SetColor("sigmaA", Color3f(sigma_a[0], sigma_a[1], sigma_a[2])); pl.SetFloat("thickness", thickness); }
+            if (type == 1) { pl.SetColor("k", col(k)); pl.SetColor("ks", col(ks)); }
+            if (type == 2) { pl.SetColor("ksReflect", col(ks)); pl.SetColor("ksRefract", col(ks_refract)); }
+            if (type == 3) { pl.SetColor("ks", col(ks)); pl.SetColor("kd", col(kd)); pl.SetBoolean("nonlinear", nonlinear != 0); }
+            if (type == 4) { pl.SetColor("ks", col(ks)); pl.SetColor("sigmaA", col(sigma_a)); pl.SetFloat("thickness", thickness); }
+        } else if (type >= 6 && type <= 8) {
+            pl.SetFloat("intIOR", int_ior);
+            pl.SetFloat("extIOR", ext_ior);
+            if (type == 6) { pl.SetColor("k", col(k)); pl.SetColor("ks", col(ks)); }
+            if (type == 7) { pl.SetColor("ksReflect", col(ks)); pl.SetColor("ksRefract", col(ks_refract)); }
+            if (type == 8) { pl.SetColor("ks", col(ks)); pl.SetColor("kd", col(kd)); pl.SetBoolean("nonlinear", nonlinear != 0); }
         }
         BSDF *b = (BSDF *)ObjectFactory::CreateInstance(names[type], pl);
         if (nested) b->AddChild((Object *)nested, "");
+        if (nested2) b->AddChild((Object *)nested2, "");
         b->Activate();
         return b;
     } catch (const std::exception &e) {

@@ -8,8 +8,9 @@ import os
 import numpy as np
 import pytest
 
-from hikari_b200.scenedesc import (BECKMANN, BSDF_DIFFUSE, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR,
-                                   BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_PLASTIC, GGX, BSDFDesc, SceneDesc)
+from hikari_b200.scenedesc import (BECKMANN, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR,
+                                   BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
+                                   BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX, SMOOTH_BSDFS, BSDFDesc, SceneDesc)
 from oracle import oracle as O
 
 REF_LIB = os.path.join(os.path.dirname(O.HERE), "oracle", "_ref", "libhikari_ref_bsdf.so")
@@ -26,7 +27,10 @@ def _ref_lib():
     R.hr_init.argtypes = [C.c_char_p]
     R.hr_bsdf_create.restype = C.c_void_p
     R.hr_bsdf_create.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_float] + [C.c_void_p] * 4 + [
-        C.c_float, C.c_void_p]
+        C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    R.hr_bsdf_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    R.hr_bsdf_pdf.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    R.hr_bsdf_pdf.restype = C.c_float
     R.hr_bsdf_batch.argtypes = [C.c_void_p, C.c_uint64] + [C.c_void_p] * 10
     R.hr_init(os.path.dirname(REF_LIB).encode())
     return R
@@ -51,6 +55,26 @@ def _cases():
         "plastic_ggx": BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=0.15, alpha_v=0.15),
         "plastic_beckmann": BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=BECKMANN, alpha_u=0.3, alpha_v=0.3),
         "coating": BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2, nested=nested),
+        "plastic_nonlinear": BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=0.15, alpha_v=0.15,
+                                      kd=[0.8, 0.4, 0.1], nonlinear=True),
+        "smooth_mirror": BSDFDesc(type=BSDF_MIRROR),
+        "smooth_conductor": BSDFDesc(type=BSDF_CONDUCTOR, int_ior=0.2, ext_ior=1.0, k=CU_K, ks=[0.9, 0.8, 0.7]),
+        "smooth_dielectric": BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.5046, ext_ior=1.000277, ks=[0.9, 0.95, 1.0],
+                                      ks_refract=[1.0, 0.9, 0.8]),
+        "smooth_dielectric_inv": BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.0, ext_ior=1.33),
+        "smooth_plastic": BSDFDesc(type=BSDF_PLASTIC, int_ior=1.5046, ext_ior=1.000277, kd=[0.6, 0.3, 0.1]),
+        "smooth_plastic_nonlinear": BSDFDesc(type=BSDF_PLASTIC, int_ior=1.9, ext_ior=1.0, kd=[0.9, 0.5, 0.2],
+                                             nonlinear=True),
+        "smooth_plastic_low_ior": BSDFDesc(type=BSDF_PLASTIC, int_ior=1.0, ext_ior=1.4, kd=[0.5, 0.5, 0.5]),
+        "twosided_one": BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.7, 0.2, 0.3])),
+        "twosided_two": BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_PLASTIC, kd=[0.2, 0.6, 0.3]),
+                                 nested2=BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=BECKMANN, alpha_u=0.3,
+                                                  alpha_v=0.3, int_ior=0.2, ext_ior=1.0, k=CU_K)),
+        "twosided_coating": BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX,
+                                                                           alpha_u=0.2, alpha_v=0.2, nested=nested),
+                                     nested2=BSDFDesc(type=BSDF_MIRROR)),
+        "coating_over_smooth": BSDFDesc(type=BSDF_ROUGH_COATING, distribution=BECKMANN, alpha_u=0.3, alpha_v=0.3,
+                                        nested=BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.3, ext_ior=1.0)),
     }
 
 
@@ -81,15 +105,26 @@ def test_oracle_bsdf_bit_exact_vs_reference(name):
     bid = o.add_bsdf(d)
     assert O.lib().ho_scene_finalize(o.h) == 0
 
-    def mk(b, nested=None):
+    def mk(b):
+        if b is None:
+            return None
         f = lambda a: np.ascontiguousarray(a, np.float32)
-        k, ks, kd, sa = f(b.k), f(b.ks), f(b.kd), f(b.sigma_a)
+        arrs = [f(b.k), f(b.ks), f(b.kd), f(b.sigma_a), f(b.ks_refract)]
+        keep.append(arrs)
+        k, ks, kd, sa, kr = arrs
         h = R.hr_bsdf_create(b.type, b.distribution, b.alpha_u, b.int_ior, b.ext_ior, O._p(k), O._p(ks), O._p(kd),
-                             O._p(sa), b.thickness, nested)
+                             O._p(sa), b.thickness, mk(b.nested), mk(b.nested2), O._p(kr), int(b.nonlinear))
         assert h
         return h
 
-    h = mk(d, mk(d.nested) if d.nested is not None else None)
+    keep = []
+    h = mk(d)
+    if _has_delta(d):
+        # a tenth of the evaluation directions on the mirror direction, a tenth on the refracted one
+        wo[0::10] = wi[0::10] * [-1, -1, 1]
+        t = wi[5::10] * [-0.6, -0.6, 1]
+        t[:, 2] = -np.sign(t[:, 2]) * np.sqrt(np.maximum(0, 1 - t[:, 0] ** 2 - t[:, 1] ** 2))
+        wo[5::10] = t.astype(np.float32)
     a = o.bsdf_batch(bid, wi, u2, u1, wo)
     b = {k: np.zeros_like(v) for k, v in a.items()}
     R.hr_bsdf_batch(h, n, O._p(wi), O._p(u2), O._p(u1), O._p(wo), O._p(b["s_wo"]), O._p(b["s_w"]),
@@ -101,3 +136,16 @@ def test_oracle_bsdf_bit_exact_vs_reference(name):
     np.testing.assert_array_equal(a["s_pdf"], b["s_pdf"])
     np.testing.assert_array_equal(a["e_rgb"], b["e_rgb"])
     np.testing.assert_array_equal(a["p_pdf"], b["p_pdf"])
+    if _has_delta(d):
+        # Eval / Pdf on the sampled direction with the sampled measure (the delta lobes)
+        for i in range(0, 3000):
+            m = int(a["s_measure"][i])
+            wi_i, wo_i = np.ascontiguousarray(wi[i]), np.ascontiguousarray(a["s_wo"][i])
+            er = np.zeros(3, np.float32)
+            R.hr_bsdf_eval(h, O._p(wi_i), O._p(wo_i), m, O._p(er))
+            np.testing.assert_array_equal(o.bsdf_eval(bid, wi_i, wo_i, m), er)
+            assert o.bsdf_pdf(bid, wi_i, wo_i, m) == R.hr_bsdf_pdf(h, O._p(wi_i), O._p(wo_i), m)
+
+
+def _has_delta(d):
+    return d is not None and (d.type in SMOOTH_BSDFS or _has_delta(d.nested) or _has_delta(d.nested2))
