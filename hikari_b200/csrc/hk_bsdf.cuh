@@ -1,6 +1,8 @@
 // Device BSDFs of the pathMIS core: diffuse, roughConductor, roughDielectric,
-// roughPlastic and roughCoating (one nesting level), with the Beckmann/GGX
-// microfacet distribution and the 1D rough-transmittance lookups.
+// roughPlastic, roughCoating (over one leaf BSDF), the smooth mirror,
+// conductor, dielectric and plastic, and twoSided (over one layer per side),
+// with the Beckmann/GGX microfacet distribution and the 1D rough-transmittance
+// lookups.
 //
 // Each function follows the reference method cited beside it, in the same
 // float evaluation order, so results agree with the reference to the ulp
@@ -358,13 +360,146 @@ __device__ __forceinline__ V3 plastic_sample(const DevBsdf &b, BRec &r, float ux
     return plastic_eval(b, r) / P;
 }
 
+// ------------------------------------------------------------ smooth BSDFs
+// Delta-direction match |d . wo - 1| <= DeltaEpsilon (include/core/Common.hpp:46);
+// DeltaEpsilon is the double literal 1e-3, so the comparison is made in double.
+__device__ __forceinline__ bool delta_match(V3 d, V3 wo) { return (double)fabsf(dot(d, wo) - 1.0f) <= 1e-3; }
+// Reflect / Refract about the local normal (src/core/Common.cpp:606-615)
+__device__ __forceinline__ V3 reflect_n(V3 wi) { return v3(-wi.x, -wi.y, wi.z); }
+__device__ __forceinline__ V3 refract_n(V3 wi, float ct, float eta, float inv_eta) {
+    float sc = -(ct < 0.0f ? inv_eta : eta);
+    return v3(sc * wi.x, sc * wi.y, ct);
+}
+
+// src/bsdf/MirrorBSDF.cpp:15-55 (the measure is set only past the cosine test);
+// ConductorBSDF's Eval / Pdf use the same match (src/bsdf/ConductorBSDF.cpp:46-70)
+__device__ __forceinline__ bool mirror_match(const BRec &r) {
+    return r.wi.z > 0.0f && r.wo.z > 0.0f && r.measure == kMeasureDiscrete && delta_match(reflect_n(r.wi), r.wo);
+}
+__device__ __forceinline__ V3 mirror_sample(BRec &r) {
+    if (r.wi.z <= 0) return v3(0, 0, 0);
+    r.wo = reflect_n(r.wi);
+    r.measure = kMeasureDiscrete;
+    r.eta = 1.0f;
+    return v3(1, 1, 1);
+}
+__device__ __forceinline__ V3 mirror_eval(const BRec &r) { return mirror_match(r) ? v3(1, 1, 1) : v3(0, 0, 0); }
+__device__ __forceinline__ float mirror_pdf(const BRec &r) { return mirror_match(r) ? 1.0f : 0.0f; }
+
+// src/bsdf/ConductorBSDF.cpp:32-70 (eta_c = intIOR / extIOR on every channel)
+__device__ __forceinline__ V3 sconductor_sample(const DevBsdf &b, BRec &r) {
+    r.measure = kMeasureDiscrete;
+    float ci = r.wi.z;
+    if (ci <= 0.0f) return v3(0, 0, 0);
+    V3 F = conductor_fresnel(b, ci);
+    r.wo = reflect_n(r.wi);
+    r.eta = 1.0f;
+    return ld_rgb(b.ks) * F;
+}
+__device__ __forceinline__ V3 sconductor_eval(const DevBsdf &b, const BRec &r) {
+    if (!mirror_match(r)) return v3(0, 0, 0);
+    return ld_rgb(b.ks) * conductor_fresnel(b, r.wi.z);
+}
+
+// src/bsdf/DielectricBSDF.cpp:33-110 (Eval and Pdf test no measure)
+__device__ __forceinline__ V3 sdielectric_sample(const DevBsdf &b, BRec &r, float ux) {
+    r.measure = kMeasureDiscrete;
+    float ct;
+    float F = fresnel_dielectric(r.wi.z, b.eta, b.inv_eta, ct);
+    if (ux < F) {
+        r.wo = reflect_n(r.wi);
+        r.eta = 1.0f;
+        return ld_rgb(b.ks);
+    }
+    r.wo = refract_n(r.wi, ct, b.eta, b.inv_eta);
+    r.eta = ct < 0.0f ? b.eta : b.inv_eta;
+    float f = ct < 0.0f ? b.inv_eta : b.eta;   // radiance transport
+    return ld_rgb(b.ks_refract) * (f * f);
+}
+// Eval and Pdf share the lobe test: 0 none, 1 reflection, 2 refraction with
+// cos(theta_t) < 0 (entering), 3 refraction leaving
+__device__ __forceinline__ float sdielectric_lobe(const DevBsdf &b, const BRec &r, int &lobe) {
+    float ci = r.wi.z, co = r.wo.z, ct;
+    float F = fresnel_dielectric(ci, b.eta, b.inv_eta, ct);
+    lobe = 0;
+    if (ci * co >= 0.0f) {
+        if (delta_match(reflect_n(r.wi), r.wo)) lobe = 1;
+    } else if (delta_match(refract_n(r.wi, ct, b.eta, b.inv_eta), r.wo)) {
+        lobe = ct < 0.0f ? 2 : 3;
+    }
+    return F;
+}
+__device__ __forceinline__ V3 sdielectric_eval(const DevBsdf &b, const BRec &r) {
+    int lobe;
+    float F = sdielectric_lobe(b, r, lobe);
+    if (lobe == 1) return ld_rgb(b.ks) * F;
+    if (lobe == 0) return v3(0, 0, 0);
+    float f = lobe == 2 ? b.inv_eta : b.eta;
+    return (ld_rgb(b.ks_refract) * (f * f)) * (1.0f - F);
+}
+__device__ __forceinline__ float sdielectric_pdf(const DevBsdf &b, const BRec &r) {
+    int lobe;
+    float F = sdielectric_lobe(b, r, lobe);
+    return lobe == 0 ? 0.0f : (lobe == 1 ? F : 1.0f - F);
+}
+
+// src/bsdf/PlasticBSDF.cpp:33-142 (fdr_int = ApproxFresnelDiffuseReflectance(1 / eta))
+__device__ __forceinline__ float splastic_spec_pdf(const DevBsdf &b, float Fi) {
+    return (Fi * b.spec_w) / (Fi * b.spec_w + (1.0f - Fi) * (1.0f - b.spec_w));
+}
+__device__ __forceinline__ V3 splastic_diffuse(const DevBsdf &b) {
+    V3 dif = ld_rgb(b.kd);
+    float fdr = b.fdr_int;
+    if (b.nonlinear) return v3(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
+    return dif / (1.0f - fdr);
+}
+__device__ __forceinline__ V3 splastic_sample(const DevBsdf &b, BRec &r, float ux, float uy) {
+    float ci = r.wi.z;
+    if (ci <= 0.0f) return v3(0, 0, 0);
+    float ct;
+    float Fi = fresnel_dielectric(ci, b.eta, b.inv_eta, ct);
+    float sp = splastic_spec_pdf(b, Fi);
+    r.eta = 1.0f;
+    if (ux < sp) {
+        r.measure = kMeasureDiscrete;
+        r.wo = reflect_n(r.wi);
+        return (ld_rgb(b.ks) * Fi) / sp;
+    }
+    r.measure = kMeasureSolidAngle;
+    r.wo = square_to_cos_hemi((ux - sp) / (1.0f - sp), uy);
+    float Fo = fresnel_dielectric(r.wo.z, b.eta, b.inv_eta, ct);
+    return splastic_diffuse(b) * (b.inv_eta2 * (1.0f - Fi) * (1.0f - Fo) / (1.0f - sp));
+}
+__device__ __forceinline__ V3 splastic_eval(const DevBsdf &b, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (r.measure == kMeasureUnknown || ci <= 0.0f || co <= 0.0f) return v3(0, 0, 0);
+    float ct;
+    float Fi = fresnel_dielectric(ci, b.eta, b.inv_eta, ct);
+    if (r.measure == kMeasureDiscrete) return delta_match(reflect_n(r.wi), r.wo) ? ld_rgb(b.ks) * Fi : v3(0, 0, 0);
+    float Fo = fresnel_dielectric(co, b.eta, b.inv_eta, ct);
+    return splastic_diffuse(b) * (cos_hemi_pdf(r.wo) * b.inv_eta2 * (1.0f - Fi) * (1.0f - Fo));
+}
+__device__ __forceinline__ float splastic_pdf(const DevBsdf &b, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (r.measure == kMeasureUnknown || ci <= 0.0f || co <= 0.0f) return 0.0f;
+    float ct;
+    float Fi = fresnel_dielectric(ci, b.eta, b.inv_eta, ct);
+    float sp = splastic_spec_pdf(b, Fi);
+    if (r.measure == kMeasureDiscrete) return delta_match(reflect_n(r.wi), r.wo) ? 1.0f - sp : 0.0f;   // as :118
+    return cos_hemi_pdf(r.wo) * (1.0f - sp);
+}
+
 // ------------------------------------------------------------ dispatch (leaf BSDFs)
 __device__ __forceinline__ V3 leaf_eval(const DevBsdf &b, const BRec &r) {
     switch (b.type) {
     case kDiffuse: return diffuse_eval(b, r);
     case kRoughConductor: return conductor_eval(b, r);
     case kRoughDielectric: return dielectric_eval(b, r);
-    default: return plastic_eval(b, r);
+    case kRoughPlastic: return plastic_eval(b, r);
+    case kMirror: return mirror_eval(r);
+    case kConductor: return sconductor_eval(b, r);
+    case kDielectric: return sdielectric_eval(b, r);
+    default: return splastic_eval(b, r);
     }
 }
 __device__ __forceinline__ float leaf_pdf(const DevBsdf &b, const BRec &r) {
@@ -372,7 +507,11 @@ __device__ __forceinline__ float leaf_pdf(const DevBsdf &b, const BRec &r) {
     case kDiffuse: return diffuse_pdf(r);
     case kRoughConductor: return conductor_pdf(b, r);
     case kRoughDielectric: return dielectric_pdf(b, r);
-    default: return plastic_pdf(b, r);
+    case kRoughPlastic: return plastic_pdf(b, r);
+    case kMirror:
+    case kConductor: return mirror_pdf(r);
+    case kDielectric: return sdielectric_pdf(b, r);
+    default: return splastic_pdf(b, r);
     }
 }
 __device__ __forceinline__ V3 leaf_sample(const DevBsdf &b, BRec &r, float ux, float uy, float u1) {
@@ -380,7 +519,11 @@ __device__ __forceinline__ V3 leaf_sample(const DevBsdf &b, BRec &r, float ux, f
     case kDiffuse: return diffuse_sample(b, r, ux, uy);
     case kRoughConductor: return conductor_sample(b, r, ux, uy);
     case kRoughDielectric: return dielectric_sample(b, r, ux, uy, u1);
-    default: return plastic_sample(b, r, ux, uy);
+    case kRoughPlastic: return plastic_sample(b, r, ux, uy);
+    case kMirror: return mirror_sample(r);
+    case kConductor: return sconductor_sample(b, r);
+    case kDielectric: return sdielectric_sample(b, r, ux);
+    default: return splastic_sample(b, r, ux, uy);
     }
 }
 
@@ -467,18 +610,58 @@ __device__ __forceinline__ V3 coating_sample(const DevBsdf &b, const DevBsdf &nb
 }
 
 // ------------------------------------------------------------ full dispatch
-__device__ __forceinline__ V3 bsdf_eval(const DevBsdf *bs, int id, const BRec &r) {
-    const DevBsdf &b = bs[id];
+// A layer is a leaf BSDF or a roughCoating over a leaf; a twoSided BSDF picks
+// one layer per side (src/bsdf/TwoSidedBSDF.cpp:19-67), mirroring z for the
+// back side.  The host rejects deeper nestings.
+__device__ __forceinline__ V3 layer_eval(const DevBsdf *bs, const DevBsdf &b, const BRec &r) {
     if (b.type == kRoughCoating) return coating_eval(b, bs[b.nested], r);
     return leaf_eval(b, r);
 }
-__device__ __forceinline__ float bsdf_pdf(const DevBsdf *bs, int id, const BRec &r) {
-    const DevBsdf &b = bs[id];
+__device__ __forceinline__ float layer_pdf(const DevBsdf *bs, const DevBsdf &b, const BRec &r) {
     if (b.type == kRoughCoating) return coating_pdf(b, bs[b.nested], r);
     return leaf_pdf(b, r);
 }
-// u1 is consumed only by a roughDielectric (top-level or nested); the caller
-// draws it lazily through needs_u1().
+__device__ __forceinline__ V3 layer_sample(const DevBsdf *bs, const DevBsdf &b, BRec &r, float ux, float uy, float u1) {
+    if (b.type == kRoughCoating) return coating_sample(b, bs[b.nested], r, ux, uy, u1);
+    return leaf_sample(b, r, ux, uy, u1);
+}
+__device__ __forceinline__ V3 twosided_eval(const DevBsdf *bs, const DevBsdf &b, const BRec &r) {
+    BRec c = r;
+    if (c.wi.z > 0.0f) return layer_eval(bs, bs[b.nested], c);
+    c.wi.z *= -1.0f;
+    c.wo.z *= -1.0f;
+    return layer_eval(bs, bs[b.nested2], c);
+}
+__device__ __forceinline__ float twosided_pdf(const DevBsdf *bs, const DevBsdf &b, const BRec &r) {
+    BRec c = r;
+    if (c.wi.z > 0.0f) return layer_pdf(bs, bs[b.nested], c);
+    c.wi.z *= -1.0f;
+    c.wo.z *= -1.0f;
+    return layer_pdf(bs, bs[b.nested2], c);
+}
+__device__ __forceinline__ V3 twosided_sample(const DevBsdf *bs, const DevBsdf &b, BRec &r, float ux, float uy, float u1) {
+    const bool flip = r.wi.z < 0.0f;
+    if (flip) r.wi.z *= -1.0f;
+    V3 res = layer_sample(bs, bs[flip ? b.nested2 : b.nested], r, ux, uy, u1);
+    if (flip) {
+        r.wi.z *= -1.0f;
+        if (!is_zero(res)) r.wo.z *= -1.0f;
+    }
+    return res;
+}
+__device__ __forceinline__ V3 bsdf_eval(const DevBsdf *bs, int id, const BRec &r) {
+    const DevBsdf &b = bs[id];
+    if (b.type == kTwoSided) return twosided_eval(bs, b, r);
+    return layer_eval(bs, b, r);
+}
+__device__ __forceinline__ float bsdf_pdf(const DevBsdf *bs, int id, const BRec &r) {
+    const DevBsdf &b = bs[id];
+    if (b.type == kTwoSided) return twosided_pdf(bs, b, r);
+    return layer_pdf(bs, b, r);
+}
+// u1 is consumed only by a roughDielectric (top-level or under a coating); the
+// caller draws it lazily through needs_u1().  A twoSided BSDF nests no
+// transmission, so it never draws one.
 __device__ __forceinline__ bool needs_u1(const DevBsdf *bs, int id) {
     const DevBsdf &b = bs[id];
     if (b.type == kRoughDielectric) return true;
@@ -486,40 +669,58 @@ __device__ __forceinline__ bool needs_u1(const DevBsdf *bs, int id) {
 }
 __device__ __forceinline__ V3 bsdf_sample(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1) {
     const DevBsdf &b = bs[id];
-    if (b.type == kRoughCoating) return coating_sample(b, bs[b.nested], r, ux, uy, u1);
-    return leaf_sample(b, r, ux, uy, u1);
+    if (b.type == kTwoSided) return twosided_sample(bs, b, r, ux, uy, u1);
+    return layer_sample(bs, b, r, ux, uy, u1);
 }
 
 }  // namespace hk
 
 namespace hk {
 // Dispatch with the top-level BSDF type known at compile time (the wavefront
-// shades one material type per kernel, so each kernel carries one BSDF).
+// shades one material type per kernel, so each kernel carries one BSDF);
+// BT < 0 dispatches at run time.
 template <int BT>
 __device__ __forceinline__ V3 bsdf_eval_t(const DevBsdf *bs, int id, const BRec &r) {
     const DevBsdf &b = bs[id];
-    if constexpr (BT == kDiffuse) return diffuse_eval(b, r);
+    if constexpr (BT < 0) return bsdf_eval(bs, id, r);
+    else if constexpr (BT == kDiffuse) return diffuse_eval(b, r);
     else if constexpr (BT == kRoughConductor) return conductor_eval(b, r);
     else if constexpr (BT == kRoughDielectric) return dielectric_eval(b, r);
     else if constexpr (BT == kRoughPlastic) return plastic_eval(b, r);
-    else return coating_eval(b, bs[b.nested], r);
+    else if constexpr (BT == kRoughCoating) return coating_eval(b, bs[b.nested], r);
+    else if constexpr (BT == kMirror) return mirror_eval(r);
+    else if constexpr (BT == kConductor) return sconductor_eval(b, r);
+    else if constexpr (BT == kDielectric) return sdielectric_eval(b, r);
+    else if constexpr (BT == kPlastic) return splastic_eval(b, r);
+    else return twosided_eval(bs, b, r);
 }
 template <int BT>
 __device__ __forceinline__ float bsdf_pdf_t(const DevBsdf *bs, int id, const BRec &r) {
     const DevBsdf &b = bs[id];
-    if constexpr (BT == kDiffuse) return diffuse_pdf(r);
+    if constexpr (BT < 0) return bsdf_pdf(bs, id, r);
+    else if constexpr (BT == kDiffuse) return diffuse_pdf(r);
     else if constexpr (BT == kRoughConductor) return conductor_pdf(b, r);
     else if constexpr (BT == kRoughDielectric) return dielectric_pdf(b, r);
     else if constexpr (BT == kRoughPlastic) return plastic_pdf(b, r);
-    else return coating_pdf(b, bs[b.nested], r);
+    else if constexpr (BT == kRoughCoating) return coating_pdf(b, bs[b.nested], r);
+    else if constexpr (BT == kMirror || BT == kConductor) return mirror_pdf(r);
+    else if constexpr (BT == kDielectric) return sdielectric_pdf(b, r);
+    else if constexpr (BT == kPlastic) return splastic_pdf(b, r);
+    else return twosided_pdf(bs, b, r);
 }
 template <int BT>
 __device__ __forceinline__ V3 bsdf_sample_t(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1) {
     const DevBsdf &b = bs[id];
-    if constexpr (BT == kDiffuse) return diffuse_sample(b, r, ux, uy);
+    if constexpr (BT < 0) return bsdf_sample(bs, id, r, ux, uy, u1);
+    else if constexpr (BT == kDiffuse) return diffuse_sample(b, r, ux, uy);
     else if constexpr (BT == kRoughConductor) return conductor_sample(b, r, ux, uy);
     else if constexpr (BT == kRoughDielectric) return dielectric_sample(b, r, ux, uy, u1);
     else if constexpr (BT == kRoughPlastic) return plastic_sample(b, r, ux, uy);
-    else return coating_sample(b, bs[b.nested], r, ux, uy, u1);
+    else if constexpr (BT == kRoughCoating) return coating_sample(b, bs[b.nested], r, ux, uy, u1);
+    else if constexpr (BT == kMirror) return mirror_sample(r);
+    else if constexpr (BT == kConductor) return sconductor_sample(b, r);
+    else if constexpr (BT == kDielectric) return sdielectric_sample(b, r, ux);
+    else if constexpr (BT == kPlastic) return splastic_sample(b, r, ux, uy);
+    else return twosided_sample(bs, b, r, ux, uy, u1);
 }
 }  // namespace hk

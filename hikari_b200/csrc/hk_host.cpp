@@ -266,10 +266,32 @@ void mat3_inverse(const float *m, float *o) {
 }
 
 // Activation of one BSDF (RoughPlasticBSDF::Activate :261, RoughCoatingBSDF::Activate :315)
+// ApproxFresnelDiffuseReflectance (src/core/Common.cpp:550): the published fits
+// of Egan & Hilgeman (1973) for eta < 1 and of d'Eon & Irving (2011) otherwise.
+float approx_fresnel_diffuse(float e) {
+    if (e < 1.0f) return -1.4399f * (e * e) + 0.7099f * e + 0.6681f + 0.0636f / e;
+    float i1 = 1.0f / e, i2 = i1 * i1, i3 = i2 * i1, i4 = i3 * i1, i5 = i4 * i1;
+    return 0.919317f - 3.4793f * i1 + 6.75335f * i2 - 7.80989f * i3 + 4.98554f * i4 - 1.36881f * i5;
+}
+
+// Whether a BSDF has a transmission lobe; coatings inherit the nested BSDF's
+// lobes (RoughCoatingBSDF.cpp:317).
+bool bsdf_transmits(const hk_scene *s, int id, int depth) {
+    if (id < 0 || id >= (int)s->bsdfs.size() || depth > 8) return false;
+    const hk_bsdf_desc &d = s->bsdfs[id];
+    switch (d.type) {
+    case hk::kRoughDielectric:
+    case hk::kDielectric: return true;
+    case hk::kRoughCoating: return bsdf_transmits(s, d.nested, depth + 1);
+    case hk::kTwoSided: return bsdf_transmits(s, d.nested, depth + 1) || bsdf_transmits(s, d.nested2, depth + 1);
+    default: return false;
+    }
+}
+
 hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs) {
     hk::DevBsdf b;
     std::memset(&b, 0, sizeof b);
-    if (d.type < 0 || d.type > 4) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+    if (d.type < hk::kDiffuse || d.type > hk::kTwoSided) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
     if (d.distribution != 0 && d.distribution != 1) throw HkError{HK_ERR_INVALID, "Unexpected distribution type"};
     b.type = d.type;
     b.distribution = d.distribution;
@@ -290,6 +312,7 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
         b.sigma_a[c] = d.sigma_a[c];
     }
     b.nested = d.nested;
+    b.nested2 = d.nested2;
     if (d.type == hk::kRoughPlastic || d.type == hk::kRoughCoating) {
         const RftTable &t = s->rft[d.distribution];
         if (!t.loaded) throw HkError{HK_ERR_INVALID, "RFT table for the BSDF's distribution was not set"};
@@ -314,8 +337,26 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
                   a2 = std::exp(d.sigma_a[2] * (-2.0f * th));
             b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
             if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
-            if (s->bsdfs[d.nested].type == hk::kRoughCoating)
-                throw HkError{HK_ERR_INVALID, "roughCoating nested in roughCoating is not supported"};
+            const int nt = s->bsdfs[d.nested].type;
+            if (nt == hk::kRoughCoating || nt == hk::kTwoSided)
+                throw HkError{HK_ERR_INVALID, "roughCoating over a roughCoating or twoSided BSDF is not supported"};
+        }
+    }
+    if (d.type == hk::kConductor)   // ConductorBSDF ctor (:17): m_Eta = Color3f(intIOR / extIOR)
+        for (int c = 0; c < 3; c++) b.eta_c[c] = b.eta;
+    if (d.type == hk::kPlastic) {   // PlasticBSDF ctor (:25) and Activate (:170)
+        float ksa = lum(d.ks), kda = lum(d.kd);
+        b.spec_w = ksa / (kda + ksa);
+        b.fdr_int = approx_fresnel_diffuse(b.inv_eta);
+    }
+    if (d.type == hk::kTwoSided) {   // TwoSidedBSDF::Activate (:98)
+        if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "TwoSidedBSDF needs at least one nested BSDF!"};
+        if (d.nested2 >= n_bsdfs) throw HkError{HK_ERR_INVALID, "twoSided: invalid second nested BSDF"};
+        if (d.nested2 < 0) b.nested2 = d.nested;
+        for (int side : {b.nested, b.nested2}) {
+            if (s->bsdfs[side].type == hk::kTwoSided)
+                throw HkError{HK_ERR_INVALID, "twoSided nested in twoSided is not supported"};
+            if (bsdf_transmits(s, side, 0)) throw HkError{HK_ERR_INVALID, "Only BSDF without transmission can be nested!"};
         }
     }
     return b;
@@ -688,9 +729,12 @@ int hk_scene_set_rft(hk_scene *s, int distribution, const void *bytes, uint64_t 
 int hk_scene_add_bsdf(hk_scene *s, const hk_bsdf_desc *d, int32_t *out_id) {
     return guarded([&] {
         if (!s || !d) throw HkError{HK_ERR_INVALID, "bad arguments"};
-        if (d->type < 0 || d->type > 4) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
-        if (d->type == HK_BSDF_ROUGH_COATING && (d->nested < 0 || d->nested >= (int)s->bsdfs.size()))
+        const int nb = (int)s->bsdfs.size();
+        if (d->type < HK_BSDF_DIFFUSE || d->type > HK_BSDF_TWO_SIDED) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+        if (d->type == HK_BSDF_ROUGH_COATING && (d->nested < 0 || d->nested >= nb))
             throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
+        if (d->type == HK_BSDF_TWO_SIDED && (d->nested < 0 || d->nested >= nb || d->nested2 >= nb))
+            throw HkError{HK_ERR_INVALID, "TwoSidedBSDF needs at least one nested BSDF!"};
         s->bsdfs.push_back(*d);
         if (out_id) *out_id = (int32_t)s->bsdfs.size() - 1;
         s->built = false;

@@ -410,13 +410,22 @@ cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, int type, uint64_t n,
                               const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
                               float *p_pdf, cudaStream_t st) {
     const int g = grid_for(n, 256);
+#define HK_BSDF_BATCH(T) \
+    case T: bsdf_batch_kernel<T><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break
     switch (type) {
-    case 0: bsdf_batch_kernel<0><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
-    case 1: bsdf_batch_kernel<1><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
-    case 2: bsdf_batch_kernel<2><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
-    case 3: bsdf_batch_kernel<3><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
-    default: bsdf_batch_kernel<4><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break;
+        HK_BSDF_BATCH(kDiffuse);
+        HK_BSDF_BATCH(kRoughConductor);
+        HK_BSDF_BATCH(kRoughDielectric);
+        HK_BSDF_BATCH(kRoughPlastic);
+        HK_BSDF_BATCH(kRoughCoating);
+        HK_BSDF_BATCH(kMirror);
+        HK_BSDF_BATCH(kConductor);
+        HK_BSDF_BATCH(kDielectric);
+        HK_BSDF_BATCH(kPlastic);
+        HK_BSDF_BATCH(kTwoSided);
+    default: return cudaErrorInvalidValue;
     }
+#undef HK_BSDF_BATCH
     return cudaGetLastError();
 }
 cudaError_t launch_emitter_sample(const DevScene &S, int e, uint64_t n, const float *in, float *out, cudaStream_t st) {

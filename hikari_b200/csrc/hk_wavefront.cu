@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, i
             int type = 0;
             if (w.found) {
                 const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
-                type = S.bsdfs[S.meshes[mesh].bsdf].type + 1;
+                type = wf_queue_of(S.bsdfs[S.meshes[mesh].bsdf].type);
             }
             W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
             W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
@@ -317,7 +317,7 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             finish(W, slot);
             continue;
         } else {
-            constexpr int BT = kType - 1;
+            constexpr int BT = kType == kWfGenericQueue ? -1 : kType - 1;
             uint4 rs = W.rng[slot];
             Pcg32 rng;
             rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
@@ -524,6 +524,7 @@ cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLau
     wf_shade_kernel<3><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+    wf_shade_kernel<6><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     launch_shadow(S, W, C, st);
     return cudaGetLastError();
 }
@@ -544,6 +545,7 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
         wf_shade_kernel<3><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+        wf_shade_kernel<6><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
         break;
     default: launch_shadow(S, W, C, st); break;
     }

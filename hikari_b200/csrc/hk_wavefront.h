@@ -18,7 +18,14 @@
 
 namespace hk {
 
-constexpr int kWfTypes = 6;        // 0: miss, 1..5: BSDF type + 1 of the hit
+// Shade queues: 0 miss, 1..5 the rough BSDF types (type + 1), each shaded by a
+// kernel compiled for that type; 6 the smooth and twoSided BSDFs, shaded by one
+// kernel that dispatches at run time.
+constexpr int kWfTypes = 7;
+constexpr int kWfGenericQueue = kWfTypes - 1;
+__host__ __device__ constexpr int wf_queue_of(int bsdf_type) {
+    return bsdf_type <= kRoughCoating ? bsdf_type + 1 : kWfGenericQueue;
+}
 constexpr int kWfMaxJobs = 1024;   // job table entries of one engine
 constexpr int kWfMaxSegs = 4096;   // pieces of one dispatch plan
 constexpr int kWfTileSide = 16;

@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <sstream>
 #include <unordered_map>
 
@@ -605,14 +606,16 @@ std::string resolve(const std::string &f) {
 class BSDFPlugin : public Object {
 public:
     hk_bsdf_desc d{};
-    std::unique_ptr<BSDFPlugin> nested;
+    std::unique_ptr<BSDFPlugin> nested;    // roughCoating's BSDF, twoSided's front BSDF
+    std::unique_ptr<BSDFPlugin> nested2;   // twoSided's back BSDF
     BSDFPlugin(const PropertyList &p, int type) {
         std::memset(&d, 0, sizeof d);
         d.type = type;
         d.nested = -1;
+        d.nested2 = -1;
         const float air = 1.000277f;
         std::string dist = p.GetString("type", "beckmann");
-        if (type != HK_BSDF_DIFFUSE) {
+        if (type >= HK_BSDF_ROUGH_CONDUCTOR && type <= HK_BSDF_ROUGH_COATING) {
             if (dist == "beckmann") d.distribution = HK_BECKMANN;
             else if (dist == "ggx") d.distribution = HK_GGX;
             else throw HikariException("Unexpected distribution type : " + dist);
@@ -643,12 +646,34 @@ public:
             setc(d.kd, p.GetColor("kd", half));
             d.nonlinear = p.GetBoolean("nonlinear", false);
             break;
-        default:
+        case HK_BSDF_ROUGH_COATING:
             d.int_ior = p.GetFloat("intIOR", 1.49f);
             d.ext_ior = p.GetFloat("extIOR", air);
             setc(d.ks, p.GetColor("ks", one));
             setc(d.sigma_a, p.GetColor("sigmaA", zero));
             d.thickness = p.GetFloat("thickness", 1.0f);
+            break;
+        case HK_BSDF_CONDUCTOR:   // src/bsdf/ConductorBSDF.cpp:9-19
+            d.int_ior = p.GetFloat("intIOR", 1.5046f);
+            d.ext_ior = p.GetFloat("extIOR", air);
+            setc(d.k, p.GetColor("k", one));
+            setc(d.ks, p.GetColor("ks", one));
+            break;
+        case HK_BSDF_DIELECTRIC:   // src/bsdf/DielectricBSDF.cpp:9-20
+            d.int_ior = p.GetFloat("intIOR", 1.5046f);
+            d.ext_ior = p.GetFloat("extIOR", air);
+            setc(d.ks, p.GetColor("ksReflect", one));
+            setc(d.ks_refract, p.GetColor("ksRefract", one));
+            break;
+        case HK_BSDF_PLASTIC:   // src/bsdf/PlasticBSDF.cpp:10-28
+            d.int_ior = p.GetFloat("intIOR", 1.5046f);
+            d.ext_ior = p.GetFloat("extIOR", air);
+            setc(d.ks, p.GetColor("ks", one));
+            setc(d.kd, p.GetColor("kd", half));
+            d.nonlinear = p.GetBoolean("nonlinear", false);
+            break;
+        default:   // mirror, twoSided: no properties
+            d.int_ior = d.ext_ior = 1.0f;
             break;
         }
         if (type == HK_BSDF_ROUGH_CONDUCTOR || type == HK_BSDF_ROUGH_DIELECTRIC) d.anisotropic = p.GetBoolean("as", false);
@@ -669,12 +694,30 @@ public:
             nested.reset((BSDFPlugin *)c);
             return;
         }
+        if (d.type == HK_BSDF_TWO_SIDED && c->GetClassType() == EClassType::EBSDF) {   // TwoSidedBSDF.cpp:75
+            if (!nested) nested.reset((BSDFPlugin *)c);
+            else if (!nested2) nested2.reset((BSDFPlugin *)c);
+            else {
+                delete c;
+                throw HikariException("TwoSidedBSDF: tried to specify the third nested BSDF");
+            }
+            return;
+        }
         delete c;
         throw HikariException(type_name + "::AddChild(<" + class_name(c->GetClassType()) + ">, <" + name +
                               ">) is not supported!");
     }
     void Activate() override {
         if (d.type == HK_BSDF_ROUGH_COATING && !nested) throw HikariException("RoughCoatingBSDF needs a nested BSDF!");
+        if (d.type == HK_BSDF_TWO_SIDED) {   // TwoSidedBSDF::Activate :98
+            if (!nested) throw HikariException("TwoSidedBSDF needs at least one nested BSDF!");
+            if (nested->transmits() || (nested2 && nested2->transmits()))
+                throw HikariException("Only BSDF without transmission can be nested!");
+        }
+    }
+    bool transmits() const {
+        if (d.type == HK_BSDF_ROUGH_DIELECTRIC || d.type == HK_BSDF_DIELECTRIC) return true;
+        return (nested && nested->transmits()) || (nested2 && nested2->transmits());
     }
 };
 struct DiffuseBSDF : BSDFPlugin { DiffuseBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_DIFFUSE) {} };
@@ -687,6 +730,16 @@ HK_REGISTER_CLASS(RoughConductorBSDF, "roughConductor")
 HK_REGISTER_CLASS(RoughDielectricBSDF, "roughDielectric")
 HK_REGISTER_CLASS(RoughPlasticBSDF, "roughPlastic")
 HK_REGISTER_CLASS(RoughCoatingBSDF, "roughCoating")
+struct MirrorBSDF : BSDFPlugin { MirrorBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_MIRROR) {} };
+struct ConductorBSDF : BSDFPlugin { ConductorBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_CONDUCTOR) {} };
+struct DielectricBSDF : BSDFPlugin { DielectricBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_DIELECTRIC) {} };
+struct PlasticBSDF : BSDFPlugin { PlasticBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_PLASTIC) {} };
+struct TwoSidedBSDF : BSDFPlugin { TwoSidedBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_TWO_SIDED) {} };
+HK_REGISTER_CLASS(MirrorBSDF, "mirror")
+HK_REGISTER_CLASS(ConductorBSDF, "conductor")
+HK_REGISTER_CLASS(DielectricBSDF, "dielectric")
+HK_REGISTER_CLASS(PlasticBSDF, "plastic")
+HK_REGISTER_CLASS(TwoSidedBSDF, "twoSided")
 
 class Mesh;
 // Emitters: AreaLight (src/emitter/AreaLight.cpp:8), EnvironmentLight (src/emitter/EnvironmentLight.cpp:8)
@@ -1011,14 +1064,11 @@ int upload_scene(const Scene &sc, const std::string &data_dir, hk_scene *h) {
         std::vector<char> bytes((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
         if ((rc = hk_scene_set_rft(h, dist, bytes.data(), bytes.size())) != HK_OK) return rc;
     }
-    auto add_bsdf = [&](const BSDFPlugin &b) -> int32_t {
+    // nested BSDFs first, so that the parent can name their ids
+    std::function<int32_t(const BSDFPlugin &)> add_bsdf = [&](const BSDFPlugin &b) -> int32_t {
         hk_bsdf_desc d = b.d;
-        int32_t nid = -1;
-        if (b.nested) {
-            hk_bsdf_desc nd = b.nested->d;
-            if ((rc = hk_scene_add_bsdf(h, &nd, &nid)) != HK_OK) throw HikariException(hk_last_error());
-            d.nested = nid;
-        }
+        if (b.nested) d.nested = add_bsdf(*b.nested);
+        if (b.nested2) d.nested2 = add_bsdf(*b.nested2);
         int32_t id;
         if ((rc = hk_scene_add_bsdf(h, &d, &id)) != HK_OK) throw HikariException(hk_last_error());
         return id;

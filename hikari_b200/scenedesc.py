@@ -278,6 +278,16 @@ def _props(node: ET.Element) -> Dict[str, object]:
     return out
 
 
+def _transmits(d: Optional[BSDFDesc]) -> bool:
+    """Whether a BSDF has a transmission lobe; coatings inherit their nested
+    BSDF's lobes (src/bsdf/RoughCoatingBSDF.cpp:317)."""
+    if d is None:
+        return False
+    if d.type in (BSDF_DIELECTRIC, BSDF_ROUGH_DIELECTRIC):
+        return True
+    return _transmits(d.nested) or _transmits(d.nested2)
+
+
 def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
     t = node.attrib["type"]
     if t not in BSDF_TYPE_NAMES:
@@ -330,9 +340,8 @@ def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
             raise SceneError("TwoSidedBSDF: tried to specify the third nested BSDF")
         d.nested = _bsdf_from_xml(nested[0])
         d.nested2 = _bsdf_from_xml(nested[1]) if len(nested) == 2 else None
-        for b in (d.nested, d.nested2 or d.nested):
-            if b.type in (BSDF_DIELECTRIC, BSDF_ROUGH_DIELECTRIC):
-                raise SceneError("TwoSidedBSDF: nested BSDFs should not have transmission")
+        if _transmits(d.nested) or _transmits(d.nested2):
+            raise SceneError("Only BSDF without transmission can be nested!")
     elif d.type == BSDF_ROUGH_COATING:
         d.int_ior = p.get("intIOR", 1.49)
         d.ext_ior = p.get("extIOR", AIR_IOR)

@@ -1,6 +1,7 @@
 """Seeded synthetic scenes of the benchmark configurations.
 
 * ``cornell_box``      -- plain-method small case: a Cornell box of OBJ quads
+* ``cornell_smooth``   -- the Cornell box with smooth (delta) and two-sided materials
 * ``icosphere``        -- subdivided icosahedron, optionally displaced by value noise
 * ``sky_envmap``       -- procedural lat-long sky (sun disk of radiance 2e4 + gradient)
 * ``mesh_heavy``       -- displaced level-8 icosphere on a ground quad under the sky
@@ -17,8 +18,9 @@ from typing import List, Optional
 
 import numpy as np
 
-from .scenedesc import (BECKMANN, BSDF_DIFFUSE, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
-                        BSDF_ROUGH_PLASTIC, GGX, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, MeshDesc, SceneDesc)
+from .scenedesc import (AIR_IOR, BECKMANN, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR, BSDF_PLASTIC,
+                        BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_PLASTIC,
+                        BSDF_TWO_SIDED, GGX, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, MeshDesc, SceneDesc)
 
 # Per-channel complex IOR (n, k) of copper and gold at R, G, B ~ (650, 550, 450) nm,
 # rounded from Johnson & Christy (1972) optical constants.
@@ -115,6 +117,29 @@ def cornell_box(seed: int = 0, width: int = 256, height: int = 256, spp: int = 6
     sd.filter = FilterDesc(2, 2.0, 0.5)
     sd.depth = depth
     sd.spp = spp
+    return sd
+
+
+def cornell_smooth(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64, depth: int = 64) -> SceneDesc:
+    """The Cornell box with the smooth BSDFs: a smooth-plastic floor, a
+    two-sided diffuse back wall, a smooth gold-like conductor for the tall box,
+    a glass box (dielectric 1.5046 in air), a mirror panel on the left wall and
+    a two-sided panel (smooth plastic in front, Beckmann rough conductor behind)
+    whose back faces the camera."""
+    sd = cornell_box(seed, width, height, spp, depth)
+    floor, ceil, back, left, right, tall, short, light = sd.meshes
+    floor.bsdf = BSDFDesc(type=BSDF_PLASTIC, int_ior=1.5046, ext_ior=AIR_IOR, kd=[0.725, 0.725, 0.725])
+    back.bsdf = BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.725, 0.725, 0.725]))
+    tall.bsdf = BSDFDesc(type=BSDF_CONDUCTOR, int_ior=0.4, ext_ior=1.0, k=[3.5, 2.5, 1.5], ks=[1.0, 0.85, 0.6])
+    short.bsdf = BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.5046, ext_ior=AIR_IOR)
+    mp, mi = quad((-0.98, 0.3, -0.7), (-0.98, 1.3, -0.7), (-0.98, 1.3, 0.1), (-0.98, 0.3, 0.1))   # faces +x
+    sd.meshes.insert(5, MeshDesc(mp, mi, BSDFDesc(type=BSDF_MIRROR)))
+    two = BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_PLASTIC, kd=[0.2, 0.3, 0.7]),
+                   nested2=BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=BECKMANN, alpha_u=0.3, alpha_v=0.3,
+                                    int_ior=1.0, ext_ior=1.0, eta=CU_ETA, k=CU_K))
+    # front face towards -z (away from the camera at z = 3.8): the camera sees the back side
+    pp, pi = quad((0.55, 1.1, 0.0), (0.55, 1.7, 0.0), (0.95, 1.7, -0.3), (0.95, 1.1, -0.3))
+    sd.meshes.insert(6, MeshDesc(pp, pi, two))
     return sd
 
 
@@ -331,6 +356,41 @@ def config2_materials():
     out.append(("coated_a0.2", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2,
                                         nested=nested)))
     return out
+
+
+def smooth_materials():
+    """The smooth (delta) BSDFs and two-sided compositions: mirror, smooth
+    conductors (Cu-like k), dielectrics entering and leaving denser media,
+    smooth plastics (linear, nonlinear, IOR below 1), two-sided diffuse,
+    plastic / rough conductor and coating / mirror pairs, and rough coatings
+    over a smooth dielectric and a smooth plastic."""
+    rc = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=1.0, ext_ior=1.0,
+                  eta=CU_ETA, k=CU_K)
+    return [
+        ("mirror", BSDFDesc(type=BSDF_MIRROR)),
+        ("conductor_cu", BSDFDesc(type=BSDF_CONDUCTOR, int_ior=0.27, ext_ior=1.0, k=CU_K)),
+        ("conductor_tinted", BSDFDesc(type=BSDF_CONDUCTOR, int_ior=1.5046, ext_ior=AIR_IOR, k=[1, 1, 1],
+                                      ks=[0.9, 0.7, 0.4])),
+        ("dielectric_glass", BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.5046, ext_ior=AIR_IOR)),
+        ("dielectric_tinted", BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.33, ext_ior=1.0, ks=[0.9, 0.95, 1.0],
+                                       ks_refract=[1.0, 0.8, 0.6])),
+        ("dielectric_bubble", BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.0, ext_ior=1.33)),
+        ("plastic", BSDFDesc(type=BSDF_PLASTIC, int_ior=1.5046, ext_ior=AIR_IOR, kd=[0.6, 0.3, 0.1])),
+        ("plastic_nonlinear", BSDFDesc(type=BSDF_PLASTIC, int_ior=1.9, ext_ior=1.0, kd=[0.9, 0.5, 0.2],
+                                       nonlinear=True)),
+        ("plastic_low_ior", BSDFDesc(type=BSDF_PLASTIC, int_ior=1.0, ext_ior=1.4, kd=[0.5, 0.5, 0.5])),
+        ("twosided_diffuse", BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.7, 0.2, 0.3]))),
+        ("twosided_plastic_conductor", BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_PLASTIC),
+                                                nested2=rc)),
+        ("twosided_coating_mirror", BSDFDesc(type=BSDF_TWO_SIDED,
+                                             nested=BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2,
+                                                             alpha_v=0.2, nested=rc),
+                                             nested2=BSDFDesc(type=BSDF_MIRROR))),
+        ("coated_dielectric", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=BECKMANN, alpha_u=0.3, alpha_v=0.3,
+                                       nested=BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.3, ext_ior=1.0))),
+        ("coated_plastic", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.1, alpha_v=0.1,
+                                    nested=BSDFDesc(type=BSDF_PLASTIC, kd=[0.3, 0.6, 0.2]))),
+    ]
 
 
 def bsdf_scene(materials) -> SceneDesc:

@@ -32,11 +32,13 @@ DEV = "cuda:0"
 RTOL = 1e-5
 
 
-@pytest.fixture(scope="module")
-def bsdf_pair():
-    mats = scenes.config2_materials()
+@pytest.fixture(scope="module", params=["rough", "smooth"])
+def bsdf_pair(request):
+    """The BSDF-batch material set (rough BSDFs and a coating) or the smooth
+    and two-sided set."""
+    mats = scenes.config2_materials() if request.param == "rough" else scenes.smooth_materials()
     sd = scenes.bsdf_scene(mats)
-    return mats, hk.Scene.from_desc(sd), OracleScene(sd)
+    return mats, hk.Scene.from_desc(sd), OracleScene(sd), request.param
 
 
 def _t(a):
@@ -44,9 +46,11 @@ def _t(a):
 
 
 def test_bsdf_batch_parity(bsdf_pair):
-    mats, gs, os_ = bsdf_pair
+    mats, gs, os_, kind = bsdf_pair
     n = 1 << 17
     wi, u2, u1, wo = bsdf_records(n, 11)
+    if kind == "smooth":   # a tenth of the evaluation directions on the mirror direction
+        wo[0::10] = wi[0::10] * np.float32([-1, -1, 1])
     twi, tu2, tu1, two = _t(wi), _t(u2), _t(u1), _t(wo)
     report = []
     for i, (name, d) in enumerate(mats):

@@ -120,12 +120,16 @@ def test_argument_checks_without_device(L):
         assert L.hk_scene_build(h) == -1                       # no meshes
         assert b"no meshes" in L.hk_last_error()
         d = hk.BsdfDesc()
-        d.type = 7
+        d.type = 12
         assert L.hk_scene_add_bsdf(h, C.byref(d), None) == -1  # unknown BSDF type
         d.type = 4
         d.nested = 3
         assert L.hk_scene_add_bsdf(h, C.byref(d), None) == -1  # coating without a nested BSDF
         assert b"nested" in L.hk_last_error()
+        d.type = 9
+        d.nested = -1
+        assert L.hk_scene_add_bsdf(h, C.byref(d), None) == -1  # twoSided without a nested BSDF
+        assert b"TwoSidedBSDF" in L.hk_last_error()
         assert L.hk_render(h, None, None, None, None) == -1    # not built
     finally:
         L.hk_scene_destroy(h)
@@ -161,3 +165,60 @@ def test_bvh_trees_are_consistent(L, case):
     print(case, "triangles", len(tris), "binary nodes", n2, "8-wide nodes", n8, "8-wide depth", d8)
     assert n8 >= 1 and n2 >= 1
     assert 2 * d8 + 2 <= 64 or len(tris) > 1e6
+
+
+SMOOTH_XML = """<?xml version="1.0"?>
+<scene>
+  <integrator type="pathMIS"><integer name="depth" value="8"/></integrator>
+  <camera type="perspective">
+    <transform name="toWorld"><lookat origin="0, 1, 4" target="0, 0.5, 0" up="0, 1, 0"/></transform>
+    <integer name="width" value="16"/><integer name="height" value="16"/>
+  </camera>
+  <mesh type="obj"><string name="filename" value="quad.obj"/><bsdf type="mirror"/></mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="conductor"><float name="intIOR" value="0.3"/><color name="k" value="3, 2.5, 2"/></bsdf></mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/><bsdf type="dielectric"/></mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="plastic"><color name="kd" value="0.2, 0.4, 0.6"/><boolean name="nonlinear" value="true"/></bsdf></mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="twoSided">
+      <bsdf type="roughCoating"><bsdf type="plastic"/></bsdf>
+      <bsdf type="diffuse"/>
+    </bsdf>
+    <emitter type="area"><color name="radiance" value="1, 1, 1"/></emitter>
+  </mesh>
+</scene>
+"""
+
+
+def test_xml_smooth_and_two_sided_plugins(L, tmp_path):
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "smooth.xml")
+    open(path, "w").write(SMOOTH_XML)
+    info, depth, spp = hk.parse_xml_info(path)
+    sd = parse_xml(path)[0]
+    assert info.n_meshes == len(sd.meshes) == 5
+    assert info.n_bsdfs == 8          # 4 smooth + twoSided, its coating, the coating's plastic, diffuse
+    types = [m.bsdf.type for m in sd.meshes]
+    assert types == [5, 6, 7, 8, 9]
+    two = sd.meshes[4].bsdf
+    assert two.nested.type == 4 and two.nested.nested.type == 8 and two.nested2.type == 0
+    assert sd.meshes[3].bsdf.nonlinear and sd.meshes[3].bsdf.int_ior == pytest.approx(1.5046)
+
+
+@pytest.mark.parametrize("body,needle", [
+    ('<bsdf type="twoSided"/>', "at least one nested"),
+    ('<bsdf type="twoSided"><bsdf type="dielectric"/></bsdf>', "transmission"),
+    ('<bsdf type="twoSided"><bsdf type="roughCoating"><bsdf type="roughDielectric"/></bsdf></bsdf>', "transmission"),
+    ('<bsdf type="twoSided"><bsdf type="diffuse"/><bsdf type="diffuse"/><bsdf type="diffuse"/></bsdf>', "third"),
+])
+def test_xml_two_sided_errors(L, tmp_path, body, needle):
+    from hikari_b200.scenedesc import SceneError
+
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "bad.xml")
+    open(path, "w").write(f'<scene><mesh type="obj"><string name="filename" value="quad.obj"/>{body}</mesh></scene>')
+    with pytest.raises(hk.HikariError, match=needle):
+        hk.parse_xml_info(path)
+    with pytest.raises(SceneError, match=needle):
+        parse_xml(path)
