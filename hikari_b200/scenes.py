@@ -125,7 +125,7 @@ def cornell_smooth(seed: int = 0, width: int = 256, height: int = 256, spp: int 
     two-sided diffuse back wall, a smooth gold-like conductor for the tall box,
     a glass box (dielectric 1.5046 in air), a mirror panel on the left wall and
     a two-sided panel (smooth plastic in front, Beckmann rough conductor behind)
-    whose back faces the camera."""
+    whose back faces the camera, under a 1 x 1 light of radiance (4.25, 3, 1)."""
     sd = cornell_box(seed, width, height, spp, depth)
     floor, ceil, back, left, right, tall, short, light = sd.meshes
     floor.bsdf = BSDFDesc(type=BSDF_PLASTIC, int_ior=1.5046, ext_ior=AIR_IOR, kd=[0.725, 0.725, 0.725])
@@ -140,6 +140,10 @@ def cornell_smooth(seed: int = 0, width: int = 256, height: int = 256, spp: int 
     # front face towards -z (away from the camera at z = 3.8): the camera sees the back side
     pp, pi = quad((0.55, 1.1, 0.0), (0.55, 1.7, 0.0), (0.95, 1.7, -0.3), (0.95, 1.1, -0.3))
     sd.meshes.insert(6, MeshDesc(pp, pi, two))
+    # a 1 x 1 light of a quarter of the radiance (same power): caustics reached
+    # by BSDF sampling alone are found four times as often
+    lp, li = quad((-0.5, 1.98, -0.5), (0.5, 1.98, -0.5), (0.5, 1.98, 0.5), (-0.5, 1.98, 0.5))
+    light.positions, light.indices, light.radiance = lp, li, [4.25, 3.0, 1.0]
     return sd
 
 

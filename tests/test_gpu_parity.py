@@ -70,8 +70,14 @@ def test_bsdf_batch_parity(bsdf_pair):
         keep = ~flip
         valid = keep & np.any(o["s_w"] != 0, axis=1)
         dwo = np.abs(g["s_wo"][valid].astype(np.float64) - o["s_wo"][valid]).max(1)
-        # the cosine warp's z = sqrt(1 - r^2) is ill-conditioned at the horizon
-        assert np.mean(dwo <= 1e-5) >= 0.9999, f"{name}: sampled directions differ by > 1e-5 on {np.sum(dwo > 1e-5)}"
+        # z = sqrt(1 - r^2) is ill-conditioned at the horizon: the cosine warp's
+        # output, and a coating's refraction out of the layer near the critical
+        # angle (dz_out / dz_in ~ eta^2 z_in / z_out); grazing records
+        # (|z| < 0.05, where a few-ulp difference of sin/cos can exceed 1e-5)
+        # are held to the looser bound only
+        steep = np.abs(o["s_wo"][valid][:, 2]) >= 0.05
+        bad = (dwo > 1e-5) & steep
+        assert np.mean(~bad) >= 0.9999, f"{name}: sampled directions differ by > 1e-5 on {bad.sum()} steep records"
         assert dwo.max() <= 1e-3, f"{name}: sampled directions differ by {dwo.max()}"
         for key in ("s_w", "s_pdf"):
             ok = rel_close(g[key][keep], o[key][keep], RTOL).reshape(keep.sum(), -1).all(1)
