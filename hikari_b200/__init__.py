@@ -34,7 +34,7 @@ class BsdfDesc(C.Structure):
         ("alpha_u", C.c_float), ("alpha_v", C.c_float), ("int_ior", C.c_float), ("ext_ior", C.c_float),
         ("eta", C.c_float * 3), ("k", C.c_float * 3), ("ks", C.c_float * 3), ("ks_refract", C.c_float * 3),
         ("kd", C.c_float * 3), ("sigma_a", C.c_float * 3), ("thickness", C.c_float), ("nested", C.c_int32),
-        ("nested2", C.c_int32),
+        ("nested2", C.c_int32), ("fast_approx", C.c_int32),
     ]
 
 
@@ -194,6 +194,7 @@ def bsdf_desc_c(d: BSDFDesc, nested_id: int = -1, nested2_id: int = -1) -> BsdfD
     c.eta[:] = d.conductor_eta()
     c.k[:], c.ks[:], c.ks_refract[:], c.kd[:], c.sigma_a[:] = d.k, d.ks, d.ks_refract, d.kd, d.sigma_a
     c.thickness, c.nested, c.nested2 = d.thickness, nested_id, nested2_id
+    c.fast_approx = int(getattr(d, "fast_approx", False))
     return c
 
 

@@ -1,6 +1,7 @@
 // Device BSDFs of the pathMIS core: diffuse, roughConductor, roughDielectric,
-// roughPlastic, roughCoating (over one leaf BSDF), the smooth mirror,
-// conductor, dielectric and plastic, and twoSided (over one layer per side),
+// roughPlastic, roughCoating and coating (over one leaf BSDF), roughDiffuse,
+// the smooth mirror, conductor, dielectric and plastic, and twoSided (over one
+// layer per side),
 // with the Beckmann/GGX microfacet distribution and the 1D rough-transmittance
 // lookups.
 //
@@ -489,6 +490,82 @@ __device__ __forceinline__ float splastic_pdf(const DevBsdf &b, const BRec &r) {
     return cos_hemi_pdf(r.wo) * (1.0f - sp);
 }
 
+// ------------------------------------------------------------ roughDiffuse
+// src/bsdf/RoughDiffuseBSDF.cpp:19-140 (Oren-Nayar: the full model or the fast
+// approximation); std::max / std::min / SafeAcos / SafeSqrt as the reference
+// spells them (include/core/Common.hpp:818-839)
+__device__ __forceinline__ float max_f(float a, float b) { return (a < b) ? b : a; }
+__device__ __forceinline__ float min_f(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float safe_acos(float v) { return acosf(min_f(1.0f, max_f(-1.0f, v))); }
+__device__ __forceinline__ float safe_sqrt(float v) { return sqrtf(max_f(0.0f, v)); }
+__device__ __forceinline__ float frame_sin_theta(V3 v) {   // Frame::SinTheta (src/core/Frame.cpp:38)
+    float t = sin_theta2(v);
+    return t <= 0.0f ? 0.0f : sqrtf(t);
+}
+__device__ __forceinline__ float frame_sin_phi(V3 v) {   // :68
+    float t = frame_sin_theta(v);
+    return t == 0.0f ? 1.0f : clampf(v.y / t, -1.0f, 1.0f);
+}
+__device__ __forceinline__ float frame_cos_phi(V3 v) {   // :78
+    float t = frame_sin_theta(v);
+    return t == 0.0f ? 1.0f : clampf(v.x / t, -1.0f, 1.0f);
+}
+__device__ __forceinline__ V3 roughdiffuse_eval(const DevBsdf &b, const BRec &r) {
+    float ci = r.wi.z, co = r.wo.z;
+    if (ci <= 0.0f || co <= 0.0f || r.measure != kMeasureSolidAngle) return v3(0, 0, 0);
+    float sigma = clampf(b.alpha_u, 5e-4f, 1.0f) * 0.70710678118655f;
+    float s2 = sigma * sigma;
+    float sti = frame_sin_theta(r.wi), sto = frame_sin_theta(r.wo);
+    float cpd = 0.0f;
+    if (sti > 1e-4f && sto > 1e-4f) {
+        float spi = frame_sin_phi(r.wi), cpi = frame_cos_phi(r.wi);
+        float spo = frame_sin_phi(r.wo), cpo = frame_cos_phi(r.wo);
+        cpd = cpi * cpo + spi * spo;
+    }
+    const float inv_pi = (float)kInvPiD;
+    if (b.fast_approx) {
+        float A = 1.0f - 0.5f * s2 / (s2 + 0.33f);
+        float B = 0.45f * s2 / (s2 + 0.09f);
+        float sa, tb;
+        if (ci > co) { sa = sto; tb = sti / ci; }
+        else { sa = sti; tb = sto / co; }
+        return ld_rgb(b.kd) * (inv_pi * co * (A + B * max_f(cpd, 0.0f) * sa * tb));
+    }
+    float thi = safe_acos(ci), tho = safe_acos(co);
+    float al = max_f(thi, tho), be = min_f(thi, tho);
+    float sa, sb, tb;
+    if (ci > co) { sa = sto; sb = sti; tb = sti / ci; }
+    else { sa = sti; sb = sto; tb = sto / co; }
+    float t1 = s2 / (s2 + 0.09f);
+    float t2 = (4.0f * (float)(kInvPiD * kInvPiD)) * al * be;
+    float t3 = 2.0f * be * inv_pi;
+    float C1 = 1.0f - 0.5f * s2 / (s2 + 0.33f);
+    float C2 = 0.45f * t1;
+    float C3 = 0.125f * t1 * t2 * t2;
+    float C4 = 0.17f * s2 / (s2 + 0.13f);
+    if (cpd > 0.0f) C2 *= sa;
+    else C2 *= sa - t3 * t3 * t3;
+    float th = (sa + sb) / (safe_sqrt(1.0f - sa * sa) + safe_sqrt(1.0f - sb * sb));
+    if (isinf(th) || isnan(th)) return v3(0, 0, 0);
+    V3 rho = ld_rgb(b.kd);
+    V3 lr1 = rho * (C1 + cpd * C2 * tb + (1.0f - fabsf(cpd)) * C3 * th);
+    V3 lr2 = (rho * rho) * (C4 * (1.0f - cpd * t3 * t3));
+    return (lr1 + lr2) * (inv_pi * co);
+}
+__device__ __forceinline__ float roughdiffuse_pdf(const BRec &r) {
+    if (r.wi.z <= 0.0f || r.wo.z <= 0.0f || r.measure != kMeasureSolidAngle) return 0.0f;
+    return cos_hemi_pdf(r.wo);
+}
+__device__ __forceinline__ V3 roughdiffuse_sample(const DevBsdf &b, BRec &r, float ux, float uy) {
+    r.measure = kMeasureSolidAngle;
+    if (r.wi.z <= 0.0f) return v3(0, 0, 0);
+    r.wo = square_to_cos_hemi(ux, uy);
+    r.eta = 1.0f;
+    float pdf = cos_hemi_pdf(r.wo);
+    if (pdf == 0.0f) return v3(0, 0, 0);
+    return roughdiffuse_eval(b, r) / pdf;
+}
+
 // ------------------------------------------------------------ dispatch (leaf BSDFs)
 __device__ __forceinline__ V3 leaf_eval(const DevBsdf &b, const BRec &r) {
     switch (b.type) {
@@ -499,6 +576,7 @@ __device__ __forceinline__ V3 leaf_eval(const DevBsdf &b, const BRec &r) {
     case kMirror: return mirror_eval(r);
     case kConductor: return sconductor_eval(b, r);
     case kDielectric: return sdielectric_eval(b, r);
+    case kRoughDiffuse: return roughdiffuse_eval(b, r);
     default: return splastic_eval(b, r);
     }
 }
@@ -511,6 +589,7 @@ __device__ __forceinline__ float leaf_pdf(const DevBsdf &b, const BRec &r) {
     case kMirror:
     case kConductor: return mirror_pdf(r);
     case kDielectric: return sdielectric_pdf(b, r);
+    case kRoughDiffuse: return roughdiffuse_pdf(r);
     default: return splastic_pdf(b, r);
     }
 }
@@ -523,6 +602,7 @@ __device__ __forceinline__ V3 leaf_sample(const DevBsdf &b, BRec &r, float ux, f
     case kMirror: return mirror_sample(r);
     case kConductor: return sconductor_sample(b, r);
     case kDielectric: return sdielectric_sample(b, r, ux);
+    case kRoughDiffuse: return roughdiffuse_sample(b, r, ux, uy);
     default: return splastic_sample(b, r, ux, uy);
     }
 }
@@ -609,20 +689,100 @@ __device__ __forceinline__ V3 coating_sample(const DevBsdf &b, const DevBsdf &nb
     return coating_eval(b, nb, r) / P;
 }
 
+// ------------------------------------------------------------ coating
+// src/bsdf/CoatingBSDF.cpp:28-302: a smooth dielectric layer over one leaf BSDF
+__device__ __forceinline__ V3 scoat_refract_in(const DevBsdf &b, V3 wi, float &R) {   // RefractIn :290
+    float ct;
+    R = fresnel_dielectric(fabsf(wi.z), b.eta, b.inv_eta, ct);
+    return v3(b.inv_eta * wi.x, b.inv_eta * wi.y, -signum(wi.z) * ct);
+}
+__device__ __forceinline__ V3 scoat_refract_out(const DevBsdf &b, V3 wi, float &R) {   // RefractOut :297
+    float ct;
+    R = fresnel_dielectric(fabsf(wi.z), b.inv_eta, b.eta, ct);
+    return v3(b.eta * wi.x, b.eta * wi.y, -signum(wi.z) * ct);
+}
+__device__ __forceinline__ V3 scoat_absorb(const DevBsdf &b, V3 res, V3 wi_int, V3 wo_int) {
+    V3 sa = ld_rgb(b.sigma_a) * b.thickness;
+    if (is_zero(sa)) return res;
+    float q = 1.0f / fabsf(wi_int.z) + 1.0f / fabsf(wo_int.z);
+    return res * v3(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q));
+}
+__device__ __forceinline__ float scoat_spec_pdf(const DevBsdf &b, float R12) {
+    return (R12 * b.spec_w) / (R12 * b.spec_w + (1.0f - R12) * (1.0f - b.spec_w));
+}
+__device__ __forceinline__ V3 scoating_sample(const DevBsdf &b, const DevBsdf &nb, BRec &r, float ux, float uy, float u1) {
+    float R12;
+    V3 wip = scoat_refract_in(b, r.wi, R12);
+    float sp = scoat_spec_pdf(b, R12);
+    if (ux < sp) {
+        r.wo = reflect_n(r.wi);
+        r.eta = 1.0f;
+        r.measure = kMeasureDiscrete;
+        return ld_rgb(b.ks) * (R12 / sp);
+    }
+    ux = (ux - sp) / (1.0f - sp);
+    if (R12 == 1.0f) return v3(0, 0, 0);
+    V3 wib = r.wi;
+    r.wi = wip;
+    V3 res = leaf_sample(nb, r, ux, uy, u1);
+    r.wi = wib;
+    if (is_zero(res)) return v3(0, 0, 0);
+    V3 wop = r.wo;
+    res = scoat_absorb(b, res, wip, wop);
+    float R21;
+    r.wo = scoat_refract_out(b, wop, R21);
+    if (R21 == 1.0f) return v3(0, 0, 0);
+    res = res / (1.0f - sp);
+    return res * ((1.0f - R12) * (1.0f - R21));
+}
+__device__ __forceinline__ V3 scoating_eval(const DevBsdf &b, const DevBsdf &nb, const BRec &r) {
+    if (r.measure == kMeasureDiscrete) {
+        if (!delta_match(reflect_n(r.wi), r.wo)) return v3(0, 0, 0);
+        float ct;
+        return ld_rgb(b.ks) * fresnel_dielectric(fabsf(r.wi.z), b.eta, b.inv_eta, ct);
+    }
+    float R12, R21;
+    BRec ri = r;
+    ri.wi = scoat_refract_in(b, r.wi, R12);
+    ri.wo = scoat_refract_in(b, r.wo, R21);
+    if (R12 == 1.0f || R21 == 1.0f) return v3(0, 0, 0);
+    V3 res = (leaf_eval(nb, ri) * (1.0f - R12)) * (1.0f - R21);
+    res = scoat_absorb(b, res, ri.wi, ri.wo);
+    if (r.measure == kMeasureSolidAngle) res = res * (b.inv_eta * b.inv_eta * r.wo.z / ri.wo.z);
+    return res;
+}
+__device__ __forceinline__ float scoating_pdf(const DevBsdf &b, const DevBsdf &nb, const BRec &r) {
+    float R12;
+    V3 wip = scoat_refract_in(b, r.wi, R12);
+    float sp = scoat_spec_pdf(b, R12);
+    if (r.measure == kMeasureDiscrete) return delta_match(reflect_n(r.wi), r.wo) ? sp : 0.0f;
+    float R21;
+    BRec ri = r;
+    ri.wi = wip;
+    ri.wo = scoat_refract_in(b, r.wo, R21);
+    if (R12 == 1.0f || R21 == 1.0f) return 0.0f;
+    float p = leaf_pdf(nb, ri);
+    if (r.measure == kMeasureSolidAngle) p *= b.inv_eta * b.inv_eta * r.wo.z / ri.wo.z;
+    return p * (1.0f - sp);
+}
+
 // ------------------------------------------------------------ full dispatch
-// A layer is a leaf BSDF or a roughCoating over a leaf; a twoSided BSDF picks
+// A layer is a leaf BSDF or a (rough) coating over a leaf; a twoSided BSDF picks
 // one layer per side (src/bsdf/TwoSidedBSDF.cpp:19-67), mirroring z for the
 // back side.  The host rejects deeper nestings.
 __device__ __forceinline__ V3 layer_eval(const DevBsdf *bs, const DevBsdf &b, const BRec &r) {
     if (b.type == kRoughCoating) return coating_eval(b, bs[b.nested], r);
+    if (b.type == kCoating) return scoating_eval(b, bs[b.nested], r);
     return leaf_eval(b, r);
 }
 __device__ __forceinline__ float layer_pdf(const DevBsdf *bs, const DevBsdf &b, const BRec &r) {
     if (b.type == kRoughCoating) return coating_pdf(b, bs[b.nested], r);
+    if (b.type == kCoating) return scoating_pdf(b, bs[b.nested], r);
     return leaf_pdf(b, r);
 }
 __device__ __forceinline__ V3 layer_sample(const DevBsdf *bs, const DevBsdf &b, BRec &r, float ux, float uy, float u1) {
     if (b.type == kRoughCoating) return coating_sample(b, bs[b.nested], r, ux, uy, u1);
+    if (b.type == kCoating) return scoating_sample(b, bs[b.nested], r, ux, uy, u1);
     return leaf_sample(b, r, ux, uy, u1);
 }
 __device__ __forceinline__ V3 twosided_eval(const DevBsdf *bs, const DevBsdf &b, const BRec &r) {
@@ -665,7 +825,7 @@ __device__ __forceinline__ float bsdf_pdf(const DevBsdf *bs, int id, const BRec 
 __device__ __forceinline__ bool needs_u1(const DevBsdf *bs, int id) {
     const DevBsdf &b = bs[id];
     if (b.type == kRoughDielectric) return true;
-    return b.type == kRoughCoating && bs[b.nested].type == kRoughDielectric;
+    return (b.type == kRoughCoating || b.type == kCoating) && bs[b.nested].type == kRoughDielectric;
 }
 __device__ __forceinline__ V3 bsdf_sample(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1) {
     const DevBsdf &b = bs[id];
@@ -692,6 +852,8 @@ __device__ __forceinline__ V3 bsdf_eval_t(const DevBsdf *bs, int id, const BRec 
     else if constexpr (BT == kConductor) return sconductor_eval(b, r);
     else if constexpr (BT == kDielectric) return sdielectric_eval(b, r);
     else if constexpr (BT == kPlastic) return splastic_eval(b, r);
+    else if constexpr (BT == kCoating) return scoating_eval(b, bs[b.nested], r);
+    else if constexpr (BT == kRoughDiffuse) return roughdiffuse_eval(b, r);
     else return twosided_eval(bs, b, r);
 }
 template <int BT>
@@ -706,6 +868,8 @@ __device__ __forceinline__ float bsdf_pdf_t(const DevBsdf *bs, int id, const BRe
     else if constexpr (BT == kMirror || BT == kConductor) return mirror_pdf(r);
     else if constexpr (BT == kDielectric) return sdielectric_pdf(b, r);
     else if constexpr (BT == kPlastic) return splastic_pdf(b, r);
+    else if constexpr (BT == kCoating) return scoating_pdf(b, bs[b.nested], r);
+    else if constexpr (BT == kRoughDiffuse) return roughdiffuse_pdf(r);
     else return twosided_pdf(bs, b, r);
 }
 template <int BT>
@@ -721,6 +885,8 @@ __device__ __forceinline__ V3 bsdf_sample_t(const DevBsdf *bs, int id, BRec &r, 
     else if constexpr (BT == kConductor) return sconductor_sample(b, r);
     else if constexpr (BT == kDielectric) return sdielectric_sample(b, r, ux);
     else if constexpr (BT == kPlastic) return splastic_sample(b, r, ux, uy);
+    else if constexpr (BT == kCoating) return scoating_sample(b, bs[b.nested], r, ux, uy, u1);
+    else if constexpr (BT == kRoughDiffuse) return roughdiffuse_sample(b, r, ux, uy);
     else return twosided_sample(bs, b, r, ux, uy, u1);
 }
 }  // namespace hk

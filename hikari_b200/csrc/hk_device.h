@@ -10,7 +10,7 @@ namespace hk {
 
 enum BsdfType : int32_t {
     kDiffuse = 0, kRoughConductor = 1, kRoughDielectric = 2, kRoughPlastic = 3, kRoughCoating = 4,
-    kMirror = 5, kConductor = 6, kDielectric = 7, kPlastic = 8, kTwoSided = 9
+    kMirror = 5, kConductor = 6, kDielectric = 7, kPlastic = 8, kTwoSided = 9, kCoating = 10, kRoughDiffuse = 11
 };
 enum Distribution : int32_t { kBeckmann = 0, kGGX = 1 };
 enum Measure : int32_t { kMeasureUnknown = 0, kMeasureSolidAngle = 1, kMeasureDiscrete = 2 };
@@ -30,10 +30,10 @@ struct alignas(16) DevBsdf {
     float thickness;
     float eta_c[3], k_c[3];          // conductor eta and k/extIOR per channel
     float ks[3], ks_refract[3], kd[3], sigma_a[3];
-    int32_t nested;                  // roughCoating nested BSDF / twoSided front BSDF index, -1 otherwise
+    int32_t nested;                  // (rough)coating nested BSDF / twoSided front BSDF index, -1 otherwise
     int32_t rft_n;                   // theta samples in rft[]
     int32_t nested2;                 // twoSided back BSDF index (the front one when only one is given)
-    int32_t pad1;
+    int32_t fast_approx;             // roughDiffuse: the fast Oren-Nayar approximation
     float rft[kRftThetaMax];
 };
 

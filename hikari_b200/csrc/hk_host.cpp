@@ -282,7 +282,8 @@ bool bsdf_transmits(const hk_scene *s, int id, int depth) {
     switch (d.type) {
     case hk::kRoughDielectric:
     case hk::kDielectric: return true;
-    case hk::kRoughCoating: return bsdf_transmits(s, d.nested, depth + 1);
+    case hk::kRoughCoating:
+    case hk::kCoating: return bsdf_transmits(s, d.nested, depth + 1);
     case hk::kTwoSided: return bsdf_transmits(s, d.nested, depth + 1) || bsdf_transmits(s, d.nested2, depth + 1);
     default: return false;
     }
@@ -291,7 +292,7 @@ bool bsdf_transmits(const hk_scene *s, int id, int depth) {
 hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs) {
     hk::DevBsdf b;
     std::memset(&b, 0, sizeof b);
-    if (d.type < hk::kDiffuse || d.type > hk::kTwoSided) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+    if (d.type < hk::kDiffuse || d.type > hk::kRoughDiffuse) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
     if (d.distribution != 0 && d.distribution != 1) throw HkError{HK_ERR_INVALID, "Unexpected distribution type"};
     b.type = d.type;
     b.distribution = d.distribution;
@@ -313,6 +314,7 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
     }
     b.nested = d.nested;
     b.nested2 = d.nested2;
+    b.fast_approx = d.fast_approx;
     if (d.type == hk::kRoughPlastic || d.type == hk::kRoughCoating) {
         const RftTable &t = s->rft[d.distribution];
         if (!t.loaded) throw HkError{HK_ERR_INVALID, "RFT table for the BSDF's distribution was not set"};
@@ -338,9 +340,19 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
             b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
             if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
             const int nt = s->bsdfs[d.nested].type;
-            if (nt == hk::kRoughCoating || nt == hk::kTwoSided)
-                throw HkError{HK_ERR_INVALID, "roughCoating over a roughCoating or twoSided BSDF is not supported"};
+            if (nt == hk::kRoughCoating || nt == hk::kCoating || nt == hk::kTwoSided)
+                throw HkError{HK_ERR_INVALID, "roughCoating over a coating or twoSided BSDF is not supported"};
         }
+    }
+    if (d.type == hk::kCoating) {   // CoatingBSDF::Activate (:255)
+        float th = d.thickness;
+        float a0 = std::exp(d.sigma_a[0] * (-2.0f * th)), a1 = std::exp(d.sigma_a[1] * (-2.0f * th)),
+              a2 = std::exp(d.sigma_a[2] * (-2.0f * th));
+        b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
+        if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "CoatingBSDF needs a nested BSDF!"};
+        const int nt = s->bsdfs[d.nested].type;
+        if (nt == hk::kRoughCoating || nt == hk::kCoating || nt == hk::kTwoSided)
+            throw HkError{HK_ERR_INVALID, "coating over a coating or twoSided BSDF is not supported"};
     }
     if (d.type == hk::kConductor)   // ConductorBSDF ctor (:17): m_Eta = Color3f(intIOR / extIOR)
         for (int c = 0; c < 3; c++) b.eta_c[c] = b.eta;
@@ -730,9 +742,11 @@ int hk_scene_add_bsdf(hk_scene *s, const hk_bsdf_desc *d, int32_t *out_id) {
     return guarded([&] {
         if (!s || !d) throw HkError{HK_ERR_INVALID, "bad arguments"};
         const int nb = (int)s->bsdfs.size();
-        if (d->type < HK_BSDF_DIFFUSE || d->type > HK_BSDF_TWO_SIDED) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+        if (d->type < HK_BSDF_DIFFUSE || d->type > HK_BSDF_ROUGH_DIFFUSE) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
         if (d->type == HK_BSDF_ROUGH_COATING && (d->nested < 0 || d->nested >= nb))
             throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
+        if (d->type == HK_BSDF_COATING && (d->nested < 0 || d->nested >= nb))
+            throw HkError{HK_ERR_INVALID, "CoatingBSDF needs a nested BSDF!"};
         if (d->type == HK_BSDF_TWO_SIDED && (d->nested < 0 || d->nested >= nb || d->nested2 >= nb))
             throw HkError{HK_ERR_INVALID, "TwoSidedBSDF needs at least one nested BSDF!"};
         s->bsdfs.push_back(*d);

@@ -423,6 +423,8 @@ cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, int type, uint64_t n,
         HK_BSDF_BATCH(kDielectric);
         HK_BSDF_BATCH(kPlastic);
         HK_BSDF_BATCH(kTwoSided);
+        HK_BSDF_BATCH(kCoating);
+        HK_BSDF_BATCH(kRoughDiffuse);
     default: return cudaErrorInvalidValue;
     }
 #undef HK_BSDF_BATCH

@@ -672,6 +672,17 @@ public:
             setc(d.kd, p.GetColor("kd", half));
             d.nonlinear = p.GetBoolean("nonlinear", false);
             break;
+        case HK_BSDF_COATING:   // src/bsdf/CoatingBSDF.cpp:9-23
+            d.int_ior = p.GetFloat("intIOR", 1.49f);
+            d.ext_ior = p.GetFloat("extIOR", air);
+            d.thickness = p.GetFloat("thickness", 1.0f);
+            setc(d.sigma_a, p.GetColor("sigmaA", zero));
+            setc(d.ks, p.GetColor("ks", one));
+            break;
+        case HK_BSDF_ROUGH_DIFFUSE:   // src/bsdf/RoughDiffuseBSDF.cpp:10-17
+            setc(d.kd, p.GetColor("albedo", half));
+            d.fast_approx = p.GetBoolean("fastApprox", false);
+            break;
         default:   // mirror, twoSided: no properties
             d.int_ior = d.ext_ior = 1.0f;
             break;
@@ -682,15 +693,19 @@ public:
             d.alpha_u = clampa(p.GetFloat("alphaU", 0.1f));
             d.alpha_v = clampa(p.GetFloat("alphaV", 0.1f));
         } else {
-            d.alpha_u = d.alpha_v = clampa(p.GetFloat("alpha", 0.1f));
+            d.alpha_u = d.alpha_v = clampa(p.GetFloat("alpha", type == HK_BSDF_ROUGH_DIFFUSE ? 0.2f : 0.1f));
         }
         float e = d.ext_ior != 0.0f ? d.int_ior / d.ext_ior : 0.0f;
         d.eta[0] = d.eta[1] = d.eta[2] = e;
     }
     EClassType GetClassType() const override { return EClassType::EBSDF; }
     void AddChild(Object *c, const std::string &name) override {
-        if (d.type == HK_BSDF_ROUGH_COATING && c->GetClassType() == EClassType::EBSDF) {
-            if (nested) throw HikariException("RoughCoatingBSDF: tried to specify multiple nested BSDF");
+        if ((d.type == HK_BSDF_ROUGH_COATING || d.type == HK_BSDF_COATING) && c->GetClassType() == EClassType::EBSDF) {
+            if (nested) {
+                delete c;
+                throw HikariException(std::string(d.type == HK_BSDF_COATING ? "CoatingBSDF" : "RoughCoatingBSDF") +
+                                      ": tried to specify multiple nested BSDF");
+            }
             nested.reset((BSDFPlugin *)c);
             return;
         }
@@ -709,6 +724,7 @@ public:
     }
     void Activate() override {
         if (d.type == HK_BSDF_ROUGH_COATING && !nested) throw HikariException("RoughCoatingBSDF needs a nested BSDF!");
+        if (d.type == HK_BSDF_COATING && !nested) throw HikariException("CoatingBSDF needs a nested BSDF!");
         if (d.type == HK_BSDF_TWO_SIDED) {   // TwoSidedBSDF::Activate :98
             if (!nested) throw HikariException("TwoSidedBSDF needs at least one nested BSDF!");
             if (nested->transmits() || (nested2 && nested2->transmits()))
@@ -740,6 +756,10 @@ HK_REGISTER_CLASS(ConductorBSDF, "conductor")
 HK_REGISTER_CLASS(DielectricBSDF, "dielectric")
 HK_REGISTER_CLASS(PlasticBSDF, "plastic")
 HK_REGISTER_CLASS(TwoSidedBSDF, "twoSided")
+struct CoatingBSDF : BSDFPlugin { CoatingBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_COATING) {} };
+struct RoughDiffuseBSDF : BSDFPlugin { RoughDiffuseBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_ROUGH_DIFFUSE) {} };
+HK_REGISTER_CLASS(CoatingBSDF, "coating")
+HK_REGISTER_CLASS(RoughDiffuseBSDF, "roughDiffuse")
 
 class Mesh;
 // Emitters: AreaLight (src/emitter/AreaLight.cpp:8), EnvironmentLight (src/emitter/EnvironmentLight.cpp:8)

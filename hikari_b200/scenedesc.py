@@ -20,7 +20,7 @@ import numpy as np
 
 # BSDF kinds, matching hk_bsdf_type in include/hikari_b200.h
 BSDF_DIFFUSE, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_PLASTIC, BSDF_ROUGH_COATING = range(5)
-BSDF_MIRROR, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_PLASTIC, BSDF_TWO_SIDED = range(5, 10)
+BSDF_MIRROR, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_PLASTIC, BSDF_TWO_SIDED, BSDF_COATING, BSDF_ROUGH_DIFFUSE = range(5, 12)
 BECKMANN, GGX = 0, 1
 BSDF_TYPE_NAMES = {
     "diffuse": BSDF_DIFFUSE,
@@ -33,9 +33,13 @@ BSDF_TYPE_NAMES = {
     "dielectric": BSDF_DIELECTRIC,
     "plastic": BSDF_PLASTIC,
     "twoSided": BSDF_TWO_SIDED,
+    "coating": BSDF_COATING,
+    "roughDiffuse": BSDF_ROUGH_DIFFUSE,
 }
 # BSDFs with a delta (specular) lobe and no microfacet distribution
-SMOOTH_BSDFS = (BSDF_MIRROR, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_PLASTIC)
+SMOOTH_BSDFS = (BSDF_MIRROR, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_PLASTIC, BSDF_COATING)
+# BSDFs that nest others: (roughCoating, coating) one, twoSided one or two
+LAYER_BSDFS = (BSDF_ROUGH_COATING, BSDF_COATING)
 FILTER_KINDS = {"box": 0, "tent": 1, "gaussian": 2, "mitchell": 3}
 
 AIR_IOR = 1.000277  # DEFAULT_*_EXT_IOR, include/core/Common.hpp:333
@@ -67,6 +71,7 @@ class BSDFDesc:
     thickness: float = 1.0
     nested: Optional["BSDFDesc"] = None    # roughCoating's BSDF, twoSided's front BSDF
     nested2: Optional["BSDFDesc"] = None   # twoSided's back BSDF (None: the front one)
+    fast_approx: bool = False              # roughDiffuse "fastApprox"
 
     def conductor_eta(self) -> List[float]:
         if self.eta is not None:
@@ -352,13 +357,30 @@ def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
         if len(nested) != 1:
             raise SceneError("RoughCoatingBSDF needs a nested BSDF!")
         d.nested = _bsdf_from_xml(nested[0])
+    elif d.type == BSDF_COATING:   # src/bsdf/CoatingBSDF.cpp:9-23, Activate :255
+        d.int_ior = p.get("intIOR", 1.49)
+        d.ext_ior = p.get("extIOR", AIR_IOR)
+        d.ks = p.get("ks", [1.0, 1.0, 1.0])
+        d.sigma_a = p.get("sigmaA", [0.0, 0.0, 0.0])
+        d.thickness = p.get("thickness", 1.0)
+        nested = [c for c in node if c.tag == "bsdf"]
+        if not nested:
+            raise SceneError("CoatingBSDF needs a nested BSDF!")
+        if len(nested) > 1:
+            raise SceneError("CoatingBSDF: tried to specify multiple nested BSDF")
+        d.nested = _bsdf_from_xml(nested[0])
+    elif d.type == BSDF_ROUGH_DIFFUSE:   # src/bsdf/RoughDiffuseBSDF.cpp:10-17
+        d.kd = p.get("albedo", [0.5, 0.5, 0.5])
+        d.fast_approx = bool(p.get("fastApprox", False))
     if d.type in (BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC):
         d.anisotropic = bool(p.get("as", False))
     if d.anisotropic:
         d.alpha_u = p.get("alphaU", 0.1)
         d.alpha_v = p.get("alphaV", 0.1)
     else:
-        d.alpha_u = d.alpha_v = p.get("alpha", 0.1)
+        d.alpha_u = d.alpha_v = p.get("alpha", 0.2 if d.type == BSDF_ROUGH_DIFFUSE else 0.1)
+    if d.type == BSDF_ROUGH_DIFFUSE:
+        d.alpha_u = d.alpha_v = min(max(d.alpha_u, 5e-4), 1.0)   # Clamp(alpha, MIN_ALPHA, MAX_ALPHA)
     return d
 
 

@@ -18,9 +18,10 @@ from typing import List, Optional
 
 import numpy as np
 
-from .scenedesc import (AIR_IOR, BECKMANN, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR, BSDF_PLASTIC,
-                        BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_PLASTIC,
-                        BSDF_TWO_SIDED, GGX, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, MeshDesc, SceneDesc)
+from .scenedesc import (AIR_IOR, BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR,
+                        BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
+                        BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX, BSDFDesc, CameraDesc, EnvDesc,
+                        FilterDesc, MeshDesc, SceneDesc)
 
 # Per-channel complex IOR (n, k) of copper and gold at R, G, B ~ (650, 550, 450) nm,
 # rounded from Johnson & Christy (1972) optical constants.
@@ -122,7 +123,9 @@ def cornell_box(seed: int = 0, width: int = 256, height: int = 256, spp: int = 6
 
 def cornell_smooth(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64, depth: int = 64) -> SceneDesc:
     """The Cornell box with the smooth BSDFs: a smooth-plastic floor, a
-    two-sided diffuse back wall, a smooth gold-like conductor for the tall box,
+    two-sided diffuse back wall, an Oren-Nayar (roughDiffuse, alpha 0.5) red
+    left wall, a smooth coating over the green diffuse right wall, a smooth
+    gold-like conductor for the tall box,
     a glass box (dielectric 1.5046 in air), a mirror panel on the left wall and
     a two-sided panel (smooth plastic in front, Beckmann rough conductor behind)
     whose back faces the camera, under a 1 x 1 light of radiance (4.25, 3, 1)."""
@@ -130,6 +133,9 @@ def cornell_smooth(seed: int = 0, width: int = 256, height: int = 256, spp: int 
     floor, ceil, back, left, right, tall, short, light = sd.meshes
     floor.bsdf = BSDFDesc(type=BSDF_PLASTIC, int_ior=1.5046, ext_ior=AIR_IOR, kd=[0.725, 0.725, 0.725])
     back.bsdf = BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.725, 0.725, 0.725]))
+    left.bsdf = BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.63, 0.065, 0.05], alpha_u=0.5, alpha_v=0.5)
+    right.bsdf = BSDFDesc(type=BSDF_COATING, int_ior=1.49, ext_ior=AIR_IOR, sigma_a=[0.2, 0.1, 0.3], thickness=0.5,
+                          nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.14, 0.45, 0.09]))
     tall.bsdf = BSDFDesc(type=BSDF_CONDUCTOR, int_ior=0.4, ext_ior=1.0, k=[3.5, 2.5, 1.5], ks=[1.0, 0.85, 0.6])
     short.bsdf = BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.5046, ext_ior=AIR_IOR)
     # lift the glass box off the floor: a bottom face coplanar with the floor
@@ -367,11 +373,13 @@ def config2_materials():
 
 
 def smooth_materials():
-    """The smooth (delta) BSDFs and two-sided compositions: mirror, smooth
-    conductors (Cu-like k), dielectrics entering and leaving denser media,
-    smooth plastics (linear, nonlinear, IOR below 1), two-sided diffuse,
-    plastic / rough conductor and coating / mirror pairs, and rough coatings
-    over a smooth dielectric and a smooth plastic."""
+    """The smooth (delta) BSDFs, two-sided compositions and Oren-Nayar: mirror,
+    smooth conductors (Cu-like k), dielectrics entering and leaving denser
+    media, smooth plastics (linear, nonlinear, IOR below 1), two-sided diffuse,
+    plastic / rough conductor and coating / mirror pairs, rough coatings over a
+    smooth dielectric and a smooth plastic, smooth coatings over a rough
+    conductor, an absorbing layer over diffuse and a rough dielectric, and
+    roughDiffuse (full model at two roughnesses, fast approximation)."""
     rc = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=1.0, ext_ior=1.0,
                   eta=CU_ETA, k=CU_K)
     return [
@@ -398,6 +406,19 @@ def smooth_materials():
                                        nested=BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.3, ext_ior=1.0))),
         ("coated_plastic", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.1, alpha_v=0.1,
                                     nested=BSDFDesc(type=BSDF_PLASTIC, kd=[0.3, 0.6, 0.2]))),
+        ("smooth_coated_conductor", BSDFDesc(type=BSDF_COATING, nested=rc)),
+        ("smooth_coated_absorbing", BSDFDesc(type=BSDF_COATING, int_ior=1.7, ext_ior=1.0, ks=[0.9, 0.9, 0.8],
+                                             sigma_a=[0.5, 1.0, 2.0], thickness=0.5,
+                                             nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.8, 0.6, 0.2]))),
+        ("smooth_coated_rough_dielectric", BSDFDesc(type=BSDF_COATING, int_ior=1.3, ext_ior=1.0,
+                                                    nested=BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX,
+                                                                    alpha_u=0.2, alpha_v=0.2, int_ior=1.5,
+                                                                    ext_ior=1.0))),
+        ("twosided_smooth_coating", BSDFDesc(type=BSDF_TWO_SIDED, nested=BSDFDesc(type=BSDF_COATING, nested=rc))),
+        ("rough_diffuse", BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.7, 0.5, 0.3], alpha_u=0.2, alpha_v=0.2)),
+        ("rough_diffuse_rough", BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.9, 0.9, 0.9], alpha_u=0.8, alpha_v=0.8)),
+        ("rough_diffuse_fast", BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.7, 0.5, 0.3], alpha_u=0.4, alpha_v=0.4,
+                                        fast_approx=True)),
     ]
 
 

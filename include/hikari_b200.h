@@ -41,6 +41,8 @@ typedef struct hk_scene hk_scene;
 #define HK_BSDF_DIELECTRIC 7       /* "dielectric"      src/bsdf/DielectricBSDF.cpp     */
 #define HK_BSDF_PLASTIC 8          /* "plastic"         src/bsdf/PlasticBSDF.cpp        */
 #define HK_BSDF_TWO_SIDED 9        /* "twoSided"        src/bsdf/TwoSidedBSDF.cpp       */
+#define HK_BSDF_COATING 10         /* "coating"         src/bsdf/CoatingBSDF.cpp        */
+#define HK_BSDF_ROUGH_DIFFUSE 11   /* "roughDiffuse"    src/bsdf/RoughDiffuseBSDF.cpp   */
 #define HK_BECKMANN 0
 #define HK_GGX 1
 
@@ -63,6 +65,7 @@ typedef struct {
     float thickness;       /* roughCoating "thickness" */
     int32_t nested;        /* roughCoating / twoSided front: id of the nested BSDF (added first), else -1 */
     int32_t nested2;       /* twoSided back: id of the second nested BSDF, -1 = the front one */
+    int32_t fast_approx;   /* roughDiffuse "fastApprox" */
 } hk_bsdf_desc;
 
 typedef struct {

@@ -597,7 +597,8 @@ static int bsdf_transmits(const ho_scene *s, int id, int depth) {
     const ho_bsdf_desc *d = &s->bsdfs[id].d;
     switch (d->type) {
     case HO_BSDF_ROUGH_DIELECTRIC: case HO_BSDF_DIELECTRIC: return 1;
-    case HO_BSDF_ROUGH_COATING: return bsdf_transmits(s, d->nested, depth + 1);
+    case HO_BSDF_ROUGH_COATING:
+    case HO_BSDF_COATING: return bsdf_transmits(s, d->nested, depth + 1);
     case HO_BSDF_TWO_SIDED:
         return bsdf_transmits(s, d->nested, depth + 1) || bsdf_transmits(s, d->nested2, depth + 1);
     default: return 0;
@@ -657,7 +658,14 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
         if (bsdf_transmits(s, d->nested, 0) || bsdf_transmits(s, b->d.nested2, 0))
             return fail("Only BSDF without transmission can be nested!");
     }
-    if (d->type < HO_BSDF_DIFFUSE || d->type > HO_BSDF_TWO_SIDED) return fail("unknown BSDF type");
+    if (d->type == HO_BSDF_COATING) {   /* CoatingBSDF::Activate :255 */
+        float th = d->thickness;
+        float a0 = expf(d->sigma_a[0] * (-2.0f * th)), a1 = expf(d->sigma_a[1] * (-2.0f * th)),
+              a2 = expf(d->sigma_a[2] * (-2.0f * th));
+        b->spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
+        if (d->nested < 0 || d->nested >= s->nb) return fail("CoatingBSDF needs a nested BSDF!");
+    }
+    if (d->type < HO_BSDF_DIFFUSE || d->type > HO_BSDF_ROUGH_DIFFUSE) return fail("unknown BSDF type");
     return 0;
 }
 
@@ -1125,6 +1133,156 @@ static float splastic_pdf(const bsdf_t *b, const brec *r) {
     return cos_hemi_pdf(r->wo) * (1.0f - sp);
 }
 
+/* CoatingBSDF  src/bsdf/CoatingBSDF.cpp:28-302: a smooth dielectric layer over a nested BSDF */
+static v3 scoat_refract_in(const bsdf_t *b, v3 wi, float *R) {   /* RefractIn :290 */
+    float ct;
+    *R = fresnel_dielectric(fabsf(wi.z), b->eta, b->inv_eta, &ct);
+    return V(b->inv_eta * wi.x, b->inv_eta * wi.y, -signum(wi.z) * ct);
+}
+static v3 scoat_refract_out(const bsdf_t *b, v3 wi, float *R) {   /* RefractOut :297 */
+    float ct;
+    *R = fresnel_dielectric(fabsf(wi.z), b->inv_eta, b->eta, &ct);
+    return V(b->eta * wi.x, b->eta * wi.y, -signum(wi.z) * ct);
+}
+static v3 scoat_absorb(const bsdf_t *b, v3 res, v3 wi_int, v3 wo_int) {
+    v3 sa = scl(vload(b->d.sigma_a), b->d.thickness);
+    if (is_zero(sa)) return res;
+    float q = 1.0f / fabsf(wi_int.z) + 1.0f / fabsf(wo_int.z);
+    return mul(res, V(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q)));
+}
+static float scoat_spec_pdf(const bsdf_t *b, float R12) {
+    return (R12 * b->spec_w) / (R12 * b->spec_w + (1.0f - R12) * (1.0f - b->spec_w));
+}
+static v3 scoating_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux, float uy, ho_pcg32 *rng,
+                          const float *u1f) {
+    float R12;
+    v3 wip = scoat_refract_in(b, r->wi, &R12);
+    float sp = scoat_spec_pdf(b, R12);
+    if (ux < sp) {
+        r->wo = reflect_n(r->wi);
+        r->eta = 1.0f;
+        r->measure = HO_MEASURE_DISCRETE;
+        return scl(vload(b->d.ks), R12 / sp);
+    }
+    ux = (ux - sp) / (1.0f - sp);
+    if (R12 == 1.0f) return V(0, 0, 0);
+    v3 wib = r->wi;
+    r->wi = wip;
+    v3 res = bsdf_sample(s, b->d.nested, r, ux, uy, rng, u1f);
+    r->wi = wib;
+    if (is_zero(res)) return V(0, 0, 0);
+    v3 wop = r->wo;
+    res = scoat_absorb(b, res, wip, wop);
+    float R21;
+    r->wo = scoat_refract_out(b, wop, &R21);
+    if (R21 == 1.0f) return V(0, 0, 0);
+    res = divs(res, 1.0f - sp);
+    return scl(res, (1.0f - R12) * (1.0f - R21));
+}
+static v3 scoating_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
+    if (r->measure == HO_MEASURE_DISCRETE) {
+        if (!delta_match(reflect_n(r->wi), r->wo)) return V(0, 0, 0);
+        float ct;
+        return scl(vload(b->d.ks), fresnel_dielectric(fabsf(r->wi.z), b->eta, b->inv_eta, &ct));
+    }
+    float R12, R21;
+    brec ri = *r;
+    ri.wi = scoat_refract_in(b, r->wi, &R12);
+    ri.wo = scoat_refract_in(b, r->wo, &R21);
+    if (R12 == 1.0f || R21 == 1.0f) return V(0, 0, 0);
+    v3 res = scl(scl(bsdf_eval(s, b->d.nested, &ri), 1.0f - R12), 1.0f - R21);
+    res = scoat_absorb(b, res, ri.wi, ri.wo);
+    if (r->measure == HO_MEASURE_SOLID_ANGLE) res = scl(res, b->inv_eta * b->inv_eta * r->wo.z / ri.wo.z);
+    return res;
+}
+static float scoating_pdf(const ho_scene *s, const bsdf_t *b, const brec *r) {
+    float R12;
+    v3 wip = scoat_refract_in(b, r->wi, &R12);
+    float sp = scoat_spec_pdf(b, R12);
+    if (r->measure == HO_MEASURE_DISCRETE) return delta_match(reflect_n(r->wi), r->wo) ? sp : 0.0f;
+    float R21;
+    brec ri = *r;
+    ri.wi = wip;
+    ri.wo = scoat_refract_in(b, r->wo, &R21);
+    if (R12 == 1.0f || R21 == 1.0f) return 0.0f;
+    float p = bsdf_pdf(s, b->d.nested, &ri);
+    if (r->measure == HO_MEASURE_SOLID_ANGLE) p *= b->inv_eta * b->inv_eta * r->wo.z / ri.wo.z;
+    return p * (1.0f - sp);
+}
+
+/* RoughDiffuseBSDF  src/bsdf/RoughDiffuseBSDF.cpp:19-140 (Oren-Nayar, full model or fast approximation) */
+static inline float max_f(float a, float b) { return (a < b) ? b : a; }   /* std::max */
+static inline float min_f(float a, float b) { return (b < a) ? b : a; }   /* std::min */
+static inline float safe_acos(float v) { return acosf(min_f(1.0f, max_f(-1.0f, v))); }
+static inline float safe_sqrt(float v) { return sqrtf(max_f(0.0f, v)); }
+static inline float frame_sin_theta(v3 v) {   /* Frame::SinTheta  src/core/Frame.cpp:38 */
+    float t = sin_theta2(v);
+    return t <= 0.0f ? 0.0f : sqrtf(t);
+}
+static inline float frame_sin_phi(v3 v) {   /* :68 */
+    float t = frame_sin_theta(v);
+    return t == 0.0f ? 1.0f : clampf(v.y / t, -1.0f, 1.0f);
+}
+static inline float frame_cos_phi(v3 v) {   /* :78 */
+    float t = frame_sin_theta(v);
+    return t == 0.0f ? 1.0f : clampf(v.x / t, -1.0f, 1.0f);
+}
+static v3 roughdiffuse_eval(const bsdf_t *b, const brec *r) {
+    float ci = r->wi.z, co = r->wo.z;
+    if (ci <= 0.0f || co <= 0.0f || r->measure != HO_MEASURE_SOLID_ANGLE) return V(0, 0, 0);
+    float sigma = clampf(b->d.alpha_u, 5e-4f, 1.0f) * 0.70710678118655f;
+    float s2 = sigma * sigma;
+    float sti = frame_sin_theta(r->wi), sto = frame_sin_theta(r->wo);
+    float cpd = 0.0f;
+    if (sti > 1e-4f && sto > 1e-4f) {
+        float spi = frame_sin_phi(r->wi), cpi = frame_cos_phi(r->wi);
+        float spo = frame_sin_phi(r->wo), cpo = frame_cos_phi(r->wo);
+        cpd = cpi * cpo + spi * spo;
+    }
+    const float inv_pi = (float)INV_PI_D;
+    if (b->d.fast_approx) {
+        float A = 1.0f - 0.5f * s2 / (s2 + 0.33f);
+        float B = 0.45f * s2 / (s2 + 0.09f);
+        float sa, tb;
+        if (ci > co) { sa = sto; tb = sti / ci; }
+        else { sa = sti; tb = sto / co; }
+        return scl(vload(b->d.kd), inv_pi * co * (A + B * max_f(cpd, 0.0f) * sa * tb));
+    }
+    float thi = safe_acos(ci), tho = safe_acos(co);
+    float al = max_f(thi, tho), be = min_f(thi, tho);
+    float sa, sb, tb;
+    if (ci > co) { sa = sto; sb = sti; tb = sti / ci; }
+    else { sa = sti; sb = sto; tb = sto / co; }
+    float t1 = s2 / (s2 + 0.09f);
+    float t2 = (4.0f * (float)(INV_PI_D * INV_PI_D)) * al * be;
+    float t3 = 2.0f * be * inv_pi;
+    float C1 = 1.0f - 0.5f * s2 / (s2 + 0.33f);
+    float C2 = 0.45f * t1;
+    float C3 = 0.125f * t1 * t2 * t2;
+    float C4 = 0.17f * s2 / (s2 + 0.13f);
+    if (cpd > 0.0f) C2 *= sa;
+    else C2 *= sa - t3 * t3 * t3;
+    float th = (sa + sb) / (safe_sqrt(1.0f - sa * sa) + safe_sqrt(1.0f - sb * sb));
+    if (isinf(th) || isnan(th)) return V(0, 0, 0);
+    v3 rho = vload(b->d.kd);
+    v3 lr1 = scl(rho, C1 + cpd * C2 * tb + (1.0f - fabsf(cpd)) * C3 * th);
+    v3 lr2 = scl(mul(rho, rho), C4 * (1.0f - cpd * t3 * t3));
+    return scl(add(lr1, lr2), inv_pi * co);
+}
+static float roughdiffuse_pdf(const brec *r) {
+    if (r->wi.z <= 0.0f || r->wo.z <= 0.0f || r->measure != HO_MEASURE_SOLID_ANGLE) return 0.0f;
+    return cos_hemi_pdf(r->wo);
+}
+static v3 roughdiffuse_sample(const bsdf_t *b, brec *r, float ux, float uy) {
+    r->measure = HO_MEASURE_SOLID_ANGLE;
+    if (r->wi.z <= 0.0f) return V(0, 0, 0);
+    r->wo = square_to_cos_hemi(ux, uy);
+    r->eta = 1.0f;
+    float pdf = cos_hemi_pdf(r->wo);
+    if (pdf == 0.0f) return V(0, 0, 0);
+    return divs(roughdiffuse_eval(b, r), pdf);
+}
+
 /* TwoSidedBSDF  src/bsdf/TwoSidedBSDF.cpp:19-67: the back side mirrors z into the second BSDF */
 static v3 twosided_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux, float uy, ho_pcg32 *rng,
                           const float *u1f) {
@@ -1164,6 +1322,8 @@ static v3 bsdf_eval(const ho_scene *s, int id, const brec *r) {
     case HO_BSDF_CONDUCTOR: return sconductor_eval(b, r);
     case HO_BSDF_DIELECTRIC: return sdielectric_eval(b, r);
     case HO_BSDF_PLASTIC: return splastic_eval(b, r);
+    case HO_BSDF_COATING: return scoating_eval(s, b, r);
+    case HO_BSDF_ROUGH_DIFFUSE: return roughdiffuse_eval(b, r);
     default: return twosided_eval(s, b, r);
     }
 }
@@ -1179,6 +1339,8 @@ static float bsdf_pdf(const ho_scene *s, int id, const brec *r) {
     case HO_BSDF_CONDUCTOR: return sconductor_pdf(r);
     case HO_BSDF_DIELECTRIC: return sdielectric_pdf(b, r);
     case HO_BSDF_PLASTIC: return splastic_pdf(b, r);
+    case HO_BSDF_COATING: return scoating_pdf(s, b, r);
+    case HO_BSDF_ROUGH_DIFFUSE: return roughdiffuse_pdf(r);
     default: return twosided_pdf(s, b, r);
     }
 }
@@ -1194,6 +1356,8 @@ static v3 bsdf_sample(const ho_scene *s, int id, brec *r, float ux, float uy, ho
     case HO_BSDF_CONDUCTOR: return sconductor_sample(b, r);
     case HO_BSDF_DIELECTRIC: return sdielectric_sample(b, r, ux);
     case HO_BSDF_PLASTIC: return splastic_sample(b, r, ux, uy);
+    case HO_BSDF_COATING: return scoating_sample(s, b, r, ux, uy, rng, u1f);
+    case HO_BSDF_ROUGH_DIFFUSE: return roughdiffuse_sample(b, r, ux, uy);
     default: return twosided_sample(s, b, r, ux, uy, rng, u1f);
     }
 }

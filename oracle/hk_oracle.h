@@ -33,12 +33,14 @@ enum {
     HO_BSDF_CONDUCTOR = 6,        /* "conductor"        src/bsdf/ConductorBSDF.cpp      */
     HO_BSDF_DIELECTRIC = 7,       /* "dielectric"       src/bsdf/DielectricBSDF.cpp     */
     HO_BSDF_PLASTIC = 8,          /* "plastic"          src/bsdf/PlasticBSDF.cpp        */
-    HO_BSDF_TWO_SIDED = 9         /* "twoSided"         src/bsdf/TwoSidedBSDF.cpp       */
+    HO_BSDF_TWO_SIDED = 9,        /* "twoSided"         src/bsdf/TwoSidedBSDF.cpp       */
+    HO_BSDF_COATING = 10,         /* "coating"          src/bsdf/CoatingBSDF.cpp        */
+    HO_BSDF_ROUGH_DIFFUSE = 11    /* "roughDiffuse"     src/bsdf/RoughDiffuseBSDF.cpp   */
 };
 enum { HO_BECKMANN = 0, HO_GGX = 1 };
 enum { HO_MEASURE_UNKNOWN = 0, HO_MEASURE_SOLID_ANGLE = 1, HO_MEASURE_DISCRETE = 2 };
 
-/* Flat BSDF description: the XML properties of the five in-scope BSDFs. */
+/* Flat BSDF description: the XML properties of the in-scope BSDFs. */
 typedef struct {
     int32_t type;          /* HO_BSDF_* */
     int32_t distribution;  /* HO_BECKMANN / HO_GGX */
@@ -55,6 +57,7 @@ typedef struct {
     float thickness;       /* roughCoating thickness */
     int32_t nested;        /* roughCoating / twoSided (front): index of the nested BSDF, else -1 */
     int32_t nested2;       /* twoSided (back): index of the second nested BSDF, -1 = the front one */
+    int32_t fast_approx;   /* roughDiffuse "fastApprox" */
 } ho_bsdf_desc;
 
 typedef struct ho_scene ho_scene;

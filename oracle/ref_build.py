@@ -31,7 +31,8 @@ CORE = ["Object", "PropertyList", "BSDF", "Texture", "MicrofacetDistribution", "
         "Sampling", "Color", "Vector", "Transform", "Sampler", "Intersection", "Timer", "MemoryArena", "Shape",
         "Mesh", "Emitter", "DiscretePDF", "BoundingBox", "Ray"]
 BSDFS = ["DiffuseBSDF", "RoughConductorBSDF", "RoughDielectricBSDF", "RoughPlasticBSDF", "RoughCoatingBSDF",
-         "MirrorBSDF", "ConductorBSDF", "DielectricBSDF", "PlasticBSDF", "TwoSidedBSDF"]
+         "MirrorBSDF", "ConductorBSDF", "DielectricBSDF", "PlasticBSDF", "TwoSidedBSDF", "CoatingBSDF",
+         "RoughDiffuseBSDF"]
 
 
 def _link(src, dst):

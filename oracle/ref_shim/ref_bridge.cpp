@@ -35,12 +35,14 @@ extern "C" {
 void hr_init(const char *search_dir) { GetFileResolver()->prepend(filesystem::path(search_dir)); }
 
 /* type: 0 diffuse, 1 roughConductor, 2 roughDielectric, 3 roughPlastic, 4 roughCoating,
- * 5 mirror, 6 conductor, 7 dielectric, 8 plastic, 9 twoSided (nested, then nested2 if given) */
+ * 5 mirror, 6 conductor, 7 dielectric, 8 plastic, 9 twoSided (nested, then nested2 if given),
+ * 10 coating, 11 roughDiffuse */
 void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_ior, const float *k,
                      const float *ks, const float *kd, const float *sigma_a, float thickness, void *nested,
-                     void *nested2, const float *ks_refract, int nonlinear) {
+                     void *nested2, const float *ks_refract, int nonlinear, int fast_approx) {
     static const char *names[] = {"diffuse", "roughConductor", "roughDielectric", "roughPlastic", "roughCoating",
-                                  "mirror", "conductor", "dielectric", "plastic", "twoSided"};
+                                  "mirror", "conductor", "dielectric", "plastic", "twoSided", "coating",
+                                  "roughDiffuse"};
     auto col = [](const float *c) { return Color3f(c[0], c[1], c[2]); };
     try {
         PropertyList pl;
@@ -61,6 +63,16 @@ void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_io
             if (type == 6) { pl.SetColor("k", col(k)); pl.SetColor("ks", col(ks)); }
             if (type == 7) { pl.SetColor("ksReflect", col(ks)); pl.SetColor("ksRefract", col(ks_refract)); }
             if (type == 8) { pl.SetColor("ks", col(ks)); pl.SetColor("kd", col(kd)); pl.SetBoolean("nonlinear", nonlinear != 0); }
+        } else if (type == 10) {
+            pl.SetFloat("intIOR", int_ior);
+            pl.SetFloat("extIOR", ext_ior);
+            pl.SetColor("ks", col(ks));
+            pl.SetColor("sigmaA", col(sigma_a));
+            pl.SetFloat("thickness", thickness);
+        } else if (type == 11) {
+            pl.SetColor("albedo", col(kd));
+            pl.SetFloat("alpha", alpha);
+            pl.SetBoolean("fastApprox", fast_approx != 0);
         }
         BSDF *b = (BSDF *)ObjectFactory::CreateInstance(names[type], pl);
         if (nested) b->AddChild((Object *)nested, "");

@@ -1,4 +1,4 @@
-"""The smooth (delta) BSDFs and two-sided compositions rendered end to end:
+"""The smooth (delta) BSDFs, two-sided compositions and roughDiffuse rendered end to end:
 the megakernel and the wavefront against the oracle on a Cornell box with a
 smooth-plastic floor, a glass box, a smooth conductor, a mirror and two-sided
 panels.  Caustics through the glass are reached by BSDF sampling alone, so
@@ -49,8 +49,10 @@ def _compare(imgs, mean_o, var_o, label):
           "block max |z|", np.abs(zb).max())
     assert abs(ratio - 1) < 0.01
     assert frac3 < 0.02
-    assert np.abs(zb).max() < 4.5
-    assert np.mean(np.abs(zb) > 3) <= 2 / zb.size
+    # heavy tails (caustics through glass and off the coated wall) put about one
+    # block of 192 beyond 3 sigma in oracle-against-oracle trials
+    assert np.abs(zb).max() < 5.0
+    assert np.sum(np.abs(zb) > 3) <= 3
 
 
 def test_megakernel_smooth_matches_oracle(smooth_scene):

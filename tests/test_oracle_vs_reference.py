@@ -8,9 +8,10 @@ import os
 import numpy as np
 import pytest
 
-from hikari_b200.scenedesc import (BECKMANN, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR,
-                                   BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
-                                   BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX, SMOOTH_BSDFS, BSDFDesc, SceneDesc)
+from hikari_b200.scenedesc import (BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE,
+                                   BSDF_MIRROR, BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR,
+                                   BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX,
+                                   SMOOTH_BSDFS, BSDFDesc, SceneDesc)
 from oracle import oracle as O
 
 REF_LIB = os.path.join(os.path.dirname(O.HERE), "oracle", "_ref", "libhikari_ref_bsdf.so")
@@ -27,7 +28,7 @@ def _ref_lib():
     R.hr_init.argtypes = [C.c_char_p]
     R.hr_bsdf_create.restype = C.c_void_p
     R.hr_bsdf_create.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_float] + [C.c_void_p] * 4 + [
-        C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+        C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
     R.hr_bsdf_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     R.hr_bsdf_pdf.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     R.hr_bsdf_pdf.restype = C.c_float
@@ -75,6 +76,17 @@ def _cases():
                                      nested2=BSDFDesc(type=BSDF_MIRROR)),
         "coating_over_smooth": BSDFDesc(type=BSDF_ROUGH_COATING, distribution=BECKMANN, alpha_u=0.3, alpha_v=0.3,
                                         nested=BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.3, ext_ior=1.0)),
+        "smooth_coating_conductor": BSDFDesc(type=BSDF_COATING, nested=nested),
+        "smooth_coating_absorbing": BSDFDesc(type=BSDF_COATING, int_ior=1.7, ext_ior=1.0, ks=[0.9, 0.9, 0.8],
+                                             sigma_a=[0.5, 1.0, 2.0], thickness=0.5,
+                                             nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.8, 0.6, 0.2])),
+        "smooth_coating_dielectric": BSDFDesc(type=BSDF_COATING, int_ior=1.3, ext_ior=1.0,
+                                              nested=BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX,
+                                                              alpha_u=0.2, alpha_v=0.2, int_ior=1.5, ext_ior=1.0)),
+        "rough_diffuse": BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.7, 0.5, 0.3], alpha_u=0.2, alpha_v=0.2),
+        "rough_diffuse_rough": BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.9, 0.9, 0.9], alpha_u=0.8, alpha_v=0.8),
+        "rough_diffuse_fast": BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.7, 0.5, 0.3], alpha_u=0.4, alpha_v=0.4,
+                                       fast_approx=True),
     }
 
 
@@ -113,7 +125,8 @@ def test_oracle_bsdf_bit_exact_vs_reference(name):
         keep.append(arrs)
         k, ks, kd, sa, kr = arrs
         h = R.hr_bsdf_create(b.type, b.distribution, b.alpha_u, b.int_ior, b.ext_ior, O._p(k), O._p(ks), O._p(kd),
-                             O._p(sa), b.thickness, mk(b.nested), mk(b.nested2), O._p(kr), int(b.nonlinear))
+                             O._p(sa), b.thickness, mk(b.nested), mk(b.nested2), O._p(kr), int(b.nonlinear),
+                             int(b.fast_approx))
         assert h
         return h
 
