@@ -115,6 +115,9 @@ def lib():
         "hk_scene_add_bsdf": ([P, C.POINTER(BsdfDesc), C.POINTER(I32)], C.c_int),
         "hk_scene_add_mesh": ([P, P, C.c_uint32, P, C.c_uint32, P, I32, P, C.POINTER(I32)], C.c_int),
         "hk_scene_set_envmap": ([P, P, C.c_uint32, C.c_uint32, P, F], C.c_int),
+        "hk_scene_set_constant_light": ([P, P], C.c_int),
+        "hk_scene_add_point_light": ([P, P, P], C.c_int),
+        "hk_scene_add_directional_light": ([P, P, P], C.c_int),
         "hk_scene_set_camera": ([P, C.c_uint32, C.c_uint32, P, F, F, F], C.c_int),
         "hk_scene_set_filter": ([P, C.c_int, F, F, F], C.c_int),
         "hk_scene_set_background": ([P, P, C.c_int], C.c_int),
@@ -240,31 +243,28 @@ class Scene:
                 return out.value
 
             mesh_bsdf = [add_bsdf(m.bsdf) for m in desc.meshes]
-            order = desc.emitter_order()
-            env_pos = order.index(-1) if -1 in order else -1
-            n_emit = 0
-            env_done = False
-
-            def set_env():
-                e = desc.env
-                rgb, tw = _f32(e.rgb), _f32(e.to_world)
-                check(L.hk_scene_set_envmap(h, rgb.ctypes.data, rgb.shape[1], rgb.shape[0], tw.ctypes.data, e.scale))
-
-            for i, m in enumerate(desc.meshes):
-                if desc.env is not None and not env_done and n_emit == env_pos:
-                    set_env()
-                    env_done = True
-                    n_emit += 1
-                pos = _f32(m.positions)
-                idx = np.ascontiguousarray(m.indices, dtype=np.uint32)
-                nrm = _f32(m.normals) if m.normals is not None else None
-                rad = _f32(m.radiance) if m.radiance is not None else None
-                check(L.hk_scene_add_mesh(h, _p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm), mesh_bsdf[i],
-                                          _p(rad), None))
-                if m.radiance is not None:
-                    n_emit += 1
-            if desc.env is not None and not env_done:
-                set_env()
+            for kind, i in desc.build_steps():   # emitters in Scene::AddChild order
+                if kind == "env" and desc.env_constant is not None:
+                    rad = _f32(desc.env_constant)
+                    check(L.hk_scene_set_constant_light(h, _p(rad)))
+                elif kind == "env":
+                    e = desc.env
+                    rgb, tw = _f32(e.rgb), _f32(e.to_world)
+                    check(L.hk_scene_set_envmap(h, rgb.ctypes.data, rgb.shape[1], rgb.shape[0], tw.ctypes.data,
+                                                e.scale))
+                elif kind == "light":
+                    l = desc.lights[i]
+                    add = L.hk_scene_add_point_light if l.kind == "point" else L.hk_scene_add_directional_light
+                    col, vec = _f32(l.color), _f32(l.vector)
+                    check(add(h, _p(col), _p(vec)))
+                else:
+                    m = desc.meshes[i]
+                    pos = _f32(m.positions)
+                    idx = np.ascontiguousarray(m.indices, dtype=np.uint32)
+                    nrm = _f32(m.normals) if m.normals is not None else None
+                    rad = _f32(m.radiance) if m.radiance is not None else None
+                    check(L.hk_scene_add_mesh(h, _p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm), mesh_bsdf[i],
+                                              _p(rad), None))
             cam = desc.camera
             tw = _f32(cam.to_world)
             check(L.hk_scene_set_camera(h, cam.width, cam.height, tw.ctypes.data, cam.fov, cam.near_clip, cam.far_clip))

@@ -15,6 +15,8 @@ enum BsdfType : int32_t {
 enum Distribution : int32_t { kBeckmann = 0, kGGX = 1 };
 enum Measure : int32_t { kMeasureUnknown = 0, kMeasureSolidAngle = 1, kMeasureDiscrete = 2 };
 
+enum EnvKind : int32_t { kEnvMap = 1, kEnvConstant = 2 };
+
 constexpr int kRftThetaMax = 100;   // data/*RFTData.bin hold 100 theta samples
 
 // One activated BSDF: constant-texture parameters plus the 1D rough
@@ -85,7 +87,11 @@ struct DevScene {
     // emitters in Scene order; env is the one with area index -1
     int32_t nemitters;
     int32_t env_index;            // position of the environment emitter, -1 if none
-    const int32_t *emitter_area;  // per emitter: index into area_lights or -1 (env)
+    // per emitter: index into area_lights, -1 the environment, -2 - k delta_lights[k]
+    const int32_t *emitter_area;
+    const float4 *delta_lights;   // point / directional: (position or direction, kind), (power or irradiance, 0)
+    int32_t env_kind;             // kEnvMap or kEnvConstant when env_index >= 0
+    float env_const[3];           // ConstantLight radiance
     const DevAreaLight *area_lights;
     const float4 *light_tris;     // emitter triangles, 3 float4 each (v0, v1, v2)
     const float4 *light_normals;  // matching vertex normals (w = has normals)

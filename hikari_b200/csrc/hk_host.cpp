@@ -203,9 +203,13 @@ struct hk_scene {
     // inputs
     std::vector<hk_bsdf_desc> bsdfs;
     std::vector<MeshIn> meshes;
-    std::vector<int> emitter_mesh;   // Scene order; -1 = environment
+    std::vector<int> emitter_mesh;   // Scene order: mesh id, -1 environment, -2 - k delta_lights[k]
+    struct DeltaLight { int directional; float color[3], vec[3]; };
+    std::vector<DeltaLight> delta_lights;   // point / directional lights
     RftTable rft[2];
     bool has_env = false;
+    bool env_constant = false;       // the environment is a ConstantLight
+    float env_const[3] = {0, 0, 0};
     uint32_t env_w = 0, env_h = 0;
     std::vector<float> env_rgb;
     float env_to_world[16];
@@ -222,7 +226,7 @@ struct hk_scene {
     hk::DevScene dev{};
     int32_t accel = HK_ACCEL_BVH8;
     DevBuf b_tris, b_nodes, b_wnodes, b_tri_normals, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
-        b_light_cdf, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
+        b_light_cdf, b_delta, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
     DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
     std::vector<std::unique_ptr<DevBuf>> batch_films;   // films of hk_render_batch_host
     hk_scene_info info{};
@@ -477,7 +481,8 @@ void build_scene(hk_scene *s) {
     D.env_index = -1;
     for (size_t e = 0; e < s->emitter_mesh.size(); ++e) {
         int mi = s->emitter_mesh[e];
-        if (mi < 0) { emitter_area.push_back(-1); D.env_index = (int)e; continue; }
+        if (mi == -1) { emitter_area.push_back(-1); D.env_index = (int)e; continue; }
+        if (mi < -1) { emitter_area.push_back(mi); continue; }   // point / directional light -2 - k
         auto &m = s->meshes[mi];
         hk::DevAreaLight L;
         std::memset(&L, 0, sizeof L);
@@ -525,8 +530,21 @@ void build_scene(hk_scene *s) {
     D.light_normals = s->b_light_normals.as<float4>();
     D.light_cdf = s->b_light_cdf.as<float>();
 
+    // point / directional lights: (position or direction, kind), (power or irradiance, 0)
+    std::vector<float> delta;
+    for (auto &l : s->delta_lights) {
+        for (int c = 0; c < 3; c++) delta.push_back(l.vec[c]);
+        delta.push_back((float)l.directional);
+        for (int c = 0; c < 3; c++) delta.push_back(l.color[c]);
+        delta.push_back(0.0f);
+    }
+    s->b_delta.upload(delta); track(s->b_delta);
+    D.delta_lights = s->b_delta.as<float4>();
+    D.env_kind = s->has_env ? (s->env_constant ? hk::kEnvConstant : hk::kEnvMap) : 0;
+    for (int c = 0; c < 3; c++) D.env_const[c] = s->env_const[c];
+
     // environment (EnvironmentLight ctor, src/emitter/EnvironmentLight.cpp:8-31)
-    if (s->has_env) {
+    if (s->has_env && !s->env_constant) {
         uint32_t W = s->env_w, H = s->env_h;
         std::vector<float> rgb4((size_t)W * H * 4), lumv((size_t)W * H);
         for (uint32_t y = 0; y < H; y++) {
@@ -790,6 +808,36 @@ int hk_scene_set_envmap(hk_scene *s, const float *rgb, uint32_t w, uint32_t h, c
         return HK_OK;
     });
 }
+int hk_scene_set_constant_light(hk_scene *s, const float *radiance) {
+    return guarded([&] {
+        if (!s || !radiance) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (s->has_env) throw HkError{HK_ERR_INVALID, "Only one environment emitter is allowed for the entire scene"};
+        s->has_env = true;
+        s->env_constant = true;
+        for (int c = 0; c < 3; c++) s->env_const[c] = radiance[c];
+        s->emitter_mesh.push_back(-1);
+        s->built = false;
+        return HK_OK;
+    });
+}
+static int add_delta_light(hk_scene *s, int directional, const float *color, const float *vec) {
+    return guarded([&] {
+        if (!s || !color || !vec) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        hk_scene::DeltaLight l;
+        l.directional = directional;
+        for (int c = 0; c < 3; c++) { l.color[c] = color[c]; l.vec[c] = vec[c]; }
+        s->emitter_mesh.push_back(-2 - (int)s->delta_lights.size());
+        s->delta_lights.push_back(l);
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_add_point_light(hk_scene *s, const float *power, const float *position) {
+    return add_delta_light(s, 0, power, position);
+}
+int hk_scene_add_directional_light(hk_scene *s, const float *irradiance, const float *direction) {
+    return add_delta_light(s, 1, irradiance, direction);
+}
 int hk_scene_set_camera(hk_scene *s, uint32_t w, uint32_t h, const float *tw16, float fov, float n, float f) {
     return guarded([&] {
         if (!s || w == 0 || h == 0) throw HkError{HK_ERR_INVALID, "bad camera"};
@@ -876,7 +924,7 @@ int hk_scene_get_info(const hk_scene *s, hk_scene_info *info) {
         I.n_emitters = (uint32_t)s->emitter_mesh.size();
         I.env_index = -1;
         for (size_t e = 0; e < s->emitter_mesh.size(); ++e)
-            if (s->emitter_mesh[e] < 0) I.env_index = (int32_t)e;
+            if (s->emitter_mesh[e] == -1) I.env_index = (int32_t)e;
         I.film_border = (int32_t)std::ceil(s->filt_r - 0.5f);
         std::memcpy(I.bbox, bb, sizeof bb);
         *info = I;

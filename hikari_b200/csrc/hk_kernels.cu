@@ -67,10 +67,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
             er.pdf = 0.0f;
             float u1 = rng.nextf();
             float ux = rng.nextf(), uy = rng.nextf();
-            int ai = __ldg(S.emitter_area + e);
-            V3 ld;
-            if (ai < 0) { er.dist = S.scene_radius; ld = env_sample(S, er, ux, uy); }
-            else ld = area_sample(S, S.area_lights[ai], er, ux, uy, u1);
+            V3 ld = emitter_sample(S, e, er, ux, uy, u1);
             float pl = er.pdf;
             if (!is_zero(ld)) {
                 Ray sr;
@@ -324,10 +321,7 @@ __global__ void emitter_sample_kernel(DevScene S, int e, uint64_t n, const float
         r.dist = 0.0f;
         r.pdf = 0.0f;
         r.p = r.n = r.wi = v3(0, 0, 0);
-        int ai = S.emitter_area[e];
-        V3 val;
-        if (ai < 0) { r.dist = S.scene_radius; val = env_sample(S, r, q[3], q[4]); }
-        else val = area_sample(S, S.area_lights[ai], r, q[3], q[4], q[5]);
+        V3 val = emitter_sample(S, e, r, q[3], q[4], q[5]);
         float *o = out + 16 * i;
         o[0] = r.p.x; o[1] = r.p.y; o[2] = r.p.z; o[3] = r.n.x; o[4] = r.n.y; o[5] = r.n.z;
         o[6] = r.wi.x; o[7] = r.wi.y; o[8] = r.wi.z; o[9] = r.pdf; o[10] = r.dist;

@@ -108,8 +108,40 @@ __device__ __forceinline__ float sample_cont(const float *cdf, const float *func
     pdf = __ldg(func + idx) / integral;
     return ((float)idx + du) / (float)n;
 }
+// ConstantLight::Sample (src/emitter/ConstantLight.cpp:15)
+__device__ __forceinline__ V3 const_sample(const DevScene &S, ERec &r, float ux, float uy) {
+    float th = uy * kPi;
+    float st = sinf(th);
+    if (st != 0.0f) r.pdf = 1.0f / (2.0f * (float)(3.14159265358979323846 * 3.14159265358979323846) * st);
+    else return v3(0, 0, 0);
+    float ph = ux * (float)(2.0 * 3.14159265358979323846);
+    float ct = cosf(th), sp = sinf(ph), cp = cosf(ph);
+    r.wi = v3(st * cp, st * sp, ct);   // SphericalDirection (src/core/Common.cpp:467)
+    r.n = r.wi * -1.0f;
+    r.p = r.ref + (r.wi * r.dist) * 2.0f;
+    return ld3(S.env_const) / r.pdf;
+}
+// PointLight::Sample (src/emitter/PointLight.cpp:15), DirectionalLight::Sample
+// (src/emitter/DirectionalLight.cpp:18); both report pdf 1
+__device__ __forceinline__ V3 delta_sample(const DevScene &S, int k, ERec &r) {
+    const float4 a = __ldg(S.delta_lights + 2 * k), c = __ldg(S.delta_lights + 2 * k + 1);
+    r.pdf = 1.0f;
+    if (a.w == 0.0f) {
+        r.p = v3(a.x, a.y, a.z);
+        V3 wi = r.p - r.ref;
+        r.dist = norm(wi);
+        r.wi = normalize(wi);
+        r.n = r.wi * -1.0f;
+        return v3(c.x, c.y, c.z) * (1.0f / ((4.0f * kPi) * (r.dist * r.dist)));
+    }
+    r.wi = normalize(v3(a.x, a.y, a.z)) * -1.0f;
+    r.p = r.ref + r.wi * (2.0f * r.dist);
+    r.n = r.wi * -1.0f;
+    return v3(c.x, c.y, c.z);
+}
 // EnvironmentLight::Sample (src/emitter/EnvironmentLight.cpp:41)
 __device__ __forceinline__ V3 env_sample(const DevScene &S, ERec &r, float ux, float uy) {
+    if (S.env_kind == kEnvConstant) return const_sample(S, r, ux, uy);
     float py, px;
     int iy, ix;
     float dy = sample_cont(S.env_marg_cdf, S.env_marg_func, S.env_marg_int, (int)S.env_h, uy, py, iy);
@@ -133,6 +165,12 @@ __device__ __forceinline__ V3 env_sample(const DevScene &S, ERec &r, float ux, f
 // EnvironmentLight::Pdf (:78) with DiscretePDF2D::Pdf (src/core/DiscretePDF.cpp:127)
 __device__ __forceinline__ float env_pdf(const DevScene &S, V3 wi) {
     float th, ph;
+    if (S.env_kind == kEnvConstant) {   // ConstantLight::Pdf (src/emitter/ConstantLight.cpp:36)
+        spherical_coords(wi, th, ph);
+        float st = sinf(th);
+        if (st == 0.0f) return 0.0f;
+        return 1.0f / (2.0f * (float)(3.14159265358979323846 * 3.14159265358979323846) * st);
+    }
     spherical_coords(mat3(S.env_to_local, wi), th, ph);
     float st = sinf(th);
     if (st == 0.0f) return 0.0f;
@@ -143,6 +181,7 @@ __device__ __forceinline__ float env_pdf(const DevScene &S, V3 wi) {
 }
 // EnvironmentLight::Eval (:92): nearest texel
 __device__ __forceinline__ V3 env_eval(const DevScene &S, V3 wi) {
+    if (S.env_kind == kEnvConstant) return ld3(S.env_const);   // ConstantLight::Eval (:47)
     float th, ph;
     spherical_coords(mat3(S.env_to_local, wi), th, ph);
     if (isnan(th) || isnan(ph)) return v3(0, 0, 0);
@@ -151,6 +190,17 @@ __device__ __forceinline__ V3 env_eval(const DevScene &S, V3 wi) {
     V3 rad = env_texel(S, (int)Y, (int)X);
     if (!is_valid(rad)) return v3(0, 0, 0);
     return rad * S.env_scale;
+}
+
+// Emitter::Sample of emitter e (Scene order) for next-event estimation: the
+// integrator gives environment and directional emitters the scene's
+// bounding-sphere radius as Distance (PathMISIntegrator.cpp:87-90)
+__device__ __forceinline__ V3 emitter_sample(const DevScene &S, int e, ERec &er, float ux, float uy, float u1) {
+    const int ai = __ldg(S.emitter_area + e);
+    if (ai >= 0) return area_sample(S, S.area_lights[ai], er, ux, uy, u1);
+    er.dist = S.scene_radius;
+    if (ai == -1) return env_sample(S, er, ux, uy);
+    return delta_sample(S, -2 - ai, er);
 }
 
 // ------------------------------------------------------------ camera

@@ -362,10 +362,7 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                 er.pdf = 0.0f;
                 float u1 = rng.nextf();
                 float ux = rng.nextf(), uy = rng.nextf();
-                int ai = __ldg(S.emitter_area + e);
-                V3 ld;
-                if (ai < 0) { er.dist = S.scene_radius; ld = env_sample(S, er, ux, uy); }
-                else ld = area_sample(S, S.area_lights[ai], er, ux, uy, u1);
+                V3 ld = emitter_sample(S, e, er, ux, uy, u1);
                 if (is_zero(ld)) continue;
                 BRec br;
                 br.wi = wi_local;

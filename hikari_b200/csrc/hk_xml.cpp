@@ -793,6 +793,30 @@ public:
 };
 HK_REGISTER_CLASS(EnvironmentLight, "env")
 
+// ConstantLight (src/emitter/ConstantLight.cpp:8): an environment emitter of one radiance
+class ConstantLight : public Object {
+public:
+    Color3f radiance;
+    explicit ConstantLight(const PropertyList &p) : radiance(p.GetColor("radiance")) {}
+    EClassType GetClassType() const override { return EClassType::EEmitter; }
+};
+HK_REGISTER_CLASS(ConstantLight, "constant")
+
+// PointLight (src/emitter/PointLight.cpp:8) and DirectionalLight (src/emitter/DirectionalLight.cpp:8)
+class DeltaLight : public Object {
+public:
+    bool directional;
+    Color3f color, vec;   // power and position, or irradiance and direction
+    DeltaLight(const PropertyList &p, bool dir)
+        : directional(dir), color(p.GetColor(dir ? "irradiance" : "power")),
+          vec(dir ? p.GetVector("direction") : p.GetPoint("position")) {}
+    EClassType GetClassType() const override { return EClassType::EEmitter; }
+};
+struct PointLight : DeltaLight { explicit PointLight(const PropertyList &p) : DeltaLight(p, false) {} };
+struct DirectionalLight : DeltaLight { explicit DirectionalLight(const PropertyList &p) : DeltaLight(p, true) {} };
+HK_REGISTER_CLASS(PointLight, "point")
+HK_REGISTER_CLASS(DirectionalLight, "directional")
+
 // WavefrontObjMesh (src/mesh/WavefrontObjMesh.cpp:10-152)
 class Mesh : public Object {
 public:
@@ -1000,7 +1024,9 @@ public:
     bool force_background;
     std::vector<std::unique_ptr<Mesh>> meshes;
     std::unique_ptr<EnvironmentLight> env;
-    int env_position = -1;   // emitter index of the environment
+    std::unique_ptr<ConstantLight> env_constant;
+    int env_position = -1;   // emitter index of the environment (map or constant)
+    std::vector<std::pair<int, std::unique_ptr<DeltaLight>>> delta_lights;   // (emitter index, light)
     int n_emitters = 0;
     std::unique_ptr<PerspectiveCamera> camera;
     std::unique_ptr<PathMISIntegrator> integrator;
@@ -1019,10 +1045,16 @@ public:
             if (meshes.back()->emitter) n_emitters++;
             break;
         case EClassType::EEmitter: {
+            if (DeltaLight *d = dynamic_cast<DeltaLight *>(c)) {   // Scene.cpp:186: point and directional
+                delta_lights.emplace_back(n_emitters++, std::unique_ptr<DeltaLight>(d));
+                break;
+            }
             EnvironmentLight *e = dynamic_cast<EnvironmentLight *>(c);
-            if (!e) { delete c; throw HikariException("Scene::AddChild(): You need to implement this for emitters"); }
-            if (env) { delete c; throw HikariException("Scene::AddChild(): Only one environment emiiter is allowed for the entire scene"); }
-            env.reset(e);
+            ConstantLight *k = dynamic_cast<ConstantLight *>(c);
+            if (!e && !k) { delete c; throw HikariException("Scene::AddChild(): You need to implement this for emitters"); }
+            if (env || env_constant) { delete c; throw HikariException("Scene::AddChild(): Only one environment emiiter is allowed for the entire scene"); }
+            if (e) env.reset(e);
+            else env_constant.reset(k);
             env_position = n_emitters++;
             break;
         }
@@ -1093,17 +1125,37 @@ int upload_scene(const Scene &sc, const std::string &data_dir, hk_scene *h) {
         if ((rc = hk_scene_add_bsdf(h, &d, &id)) != HK_OK) throw HikariException(hk_last_error());
         return id;
     };
+    // non-mesh emitters go in before the mesh emitter they precede (Scene::AddChild order)
     int emitted = 0;
     bool env_done = false;
-    auto set_env = [&]() {
-        const EnvironmentLight &e = *sc.env;
-        if ((rc = hk_scene_set_envmap(h, e.rgb.data(), (uint32_t)e.w, (uint32_t)e.h, e.to_world.data(), e.scale)) != HK_OK)
-            throw HikariException(hk_last_error());
-        env_done = true;
-        emitted++;
+    size_t next_delta = 0;
+    auto add_pending = [&](bool all) {
+        for (;;) {
+            if ((sc.env || sc.env_constant) && !env_done && (all || emitted == sc.env_position) &&
+                (next_delta == sc.delta_lights.size() || sc.env_position < sc.delta_lights[next_delta].first)) {
+                if (sc.env) {
+                    const EnvironmentLight &e = *sc.env;
+                    rc = hk_scene_set_envmap(h, e.rgb.data(), (uint32_t)e.w, (uint32_t)e.h, e.to_world.data(), e.scale);
+                } else {
+                    rc = hk_scene_set_constant_light(h, sc.env_constant->radiance.data());
+                }
+                if (rc != HK_OK) throw HikariException(hk_last_error());
+                env_done = true;
+                emitted++;
+            } else if (next_delta < sc.delta_lights.size() && (all || emitted == sc.delta_lights[next_delta].first)) {
+                const DeltaLight &l = *sc.delta_lights[next_delta].second;
+                rc = l.directional ? hk_scene_add_directional_light(h, l.color.data(), l.vec.data())
+                                   : hk_scene_add_point_light(h, l.color.data(), l.vec.data());
+                if (rc != HK_OK) throw HikariException(hk_last_error());
+                next_delta++;
+                emitted++;
+            } else {
+                break;
+            }
+        }
     };
     for (auto &m : sc.meshes) {
-        if (sc.env && !env_done && emitted == sc.env_position) set_env();
+        add_pending(false);
         int32_t bid = add_bsdf(*m->bsdf);
         const float *rad = m->emitter ? m->emitter->radiance.data() : nullptr;
         if ((rc = hk_scene_add_mesh(h, m->pos.data(), (uint32_t)(m->pos.size() / 3), m->idx.data(),
@@ -1112,7 +1164,7 @@ int upload_scene(const Scene &sc, const std::string &data_dir, hk_scene *h) {
             throw HikariException(hk_last_error());
         if (rad) emitted++;
     }
-    if (sc.env && !env_done) set_env();
+    add_pending(true);
     const PerspectiveCamera &c = *sc.camera;
     if ((rc = hk_scene_set_camera(h, (uint32_t)c.width, (uint32_t)c.height, c.to_world.data(), c.fov, c.near_clip,
                                   c.far_clip)) != HK_OK)

@@ -48,6 +48,8 @@ public:
     std::string GetString(const std::string &n, const std::string &d) const { return has(n) ? get(n, kString).s : d; }
     Color3f GetColor(const std::string &n) const { return get(n, kColor).c; }
     Color3f GetColor(const std::string &n, const Color3f &d) const { return has(n) ? get(n, kColor).c : d; }
+    Color3f GetPoint(const std::string &n) const { return get(n, kPoint).c; }
+    Color3f GetVector(const std::string &n) const { return get(n, kVector).c; }
     Matrix4f GetTransform(const std::string &n, const Matrix4f &d) const { return has(n) ? get(n, kTransform).m : d; }
     bool has(const std::string &n) const { return m_.count(n) != 0; }
 

@@ -98,6 +98,16 @@ class EnvDesc:
 
 
 @dataclass
+class LightDesc:
+    """A point or a directional light (src/emitter/PointLight.cpp:8,
+    src/emitter/DirectionalLight.cpp:8)."""
+    kind: str                # "point" or "directional"
+    color: List[float]       # power (point) or irradiance (directional)
+    vector: List[float]      # position (point) or direction of travel (directional)
+    emitter_index: int = -1  # position in the emitter list (Scene::AddChild order); -1: after the others
+
+
+@dataclass
 class CameraDesc:
     width: int = 1280
     height: int = 720
@@ -119,7 +129,9 @@ class FilterDesc:
 class SceneDesc:
     meshes: List[MeshDesc] = field(default_factory=list)
     env: Optional[EnvDesc] = None
+    env_constant: Optional[List[float]] = None  # ConstantLight radiance (instead of an environment map)
     env_emitter_index: int = -1  # position of the env emitter in the emitter list
+    lights: List[LightDesc] = field(default_factory=list)
     camera: CameraDesc = field(default_factory=CameraDesc)
     filter: FilterDesc = field(default_factory=FilterDesc)
     depth: int = 32
@@ -133,15 +145,33 @@ class SceneDesc:
         return int(sum(m.indices.shape[0] for m in self.meshes))
 
     def emitter_order(self) -> List[int]:
-        """Mesh index per emitter, -1 for the environment (Scene::AddChild order)."""
-        order = []
-        for i, m in enumerate(self.meshes):
-            if m.radiance is not None:
-                order.append(i)
-        if self.env is not None:
-            pos = self.env_emitter_index if self.env_emitter_index >= 0 else len(order)
-            order.insert(min(pos, len(order)), -1)
+        """The emitter list in Scene::AddChild order: a mesh index per area
+        emitter, -1 for the environment (map or constant), -2 - k for
+        lights[k].  Non-mesh emitters sit at the positions recorded when they
+        were parsed."""
+        order = [i for i, m in enumerate(self.meshes) if m.radiance is not None]
+        extra = []
+        if self.env is not None or self.env_constant is not None:
+            extra.append((self.env_emitter_index, -1))
+        extra += [(l.emitter_index, -2 - k) for k, l in enumerate(self.lights)]
+        for pos, code in sorted(extra, key=lambda t: (t[0] < 0, t[0])):
+            order.insert(pos if 0 <= pos <= len(order) else len(order), code)
         return order
+
+    def build_steps(self) -> List[tuple]:
+        """Scene construction steps that reproduce emitter_order(): ("mesh", i)
+        in mesh order, ("env", 0) and ("light", k) each just before the mesh
+        emitter it precedes."""
+        steps, mi = [], 0
+        for code in self.emitter_order():
+            if code >= 0:
+                while mi <= code:
+                    steps.append(("mesh", mi))
+                    mi += 1
+            else:
+                steps.append(("env", 0) if code == -1 else ("light", -2 - code))
+        steps += [("mesh", i) for i in range(mi, len(self.meshes))]
+        return steps
 
 
 # ----------------------------------------------------------------- transforms
@@ -438,15 +468,29 @@ def parse_scene_node(node: ET.Element, base_dir: str, env_loader=None) -> SceneD
             sd.meshes.append(MeshDesc(pos, idx, bsdf, nrm, rad, bbox))
         elif ch.tag == "emitter":
             et = ch.attrib["type"]
-            if et != "env":
-                raise SceneError(f"emitter type {et!r} is not supported by the CUDA pathMIS core")
-            if sd.env is not None:
-                raise SceneError("Only one environment emiiter is allowed for the entire scene")
             ep = _props(ch)
-            if env_loader is None:
-                raise SceneError("no environment-map loader given")
-            rgb = env_loader(os.path.join(base_dir, ep["filename"]))
-            sd.env = EnvDesc(rgb, ep.get("toWorld", np.eye(4, dtype=np.float32)), ep.get("scale", 1.0))
+            if et in ("point", "directional"):   # src/emitter/PointLight.cpp:8, DirectionalLight.cpp:8
+                try:
+                    color = ep["power" if et == "point" else "irradiance"]
+                    vec = ep["position" if et == "point" else "direction"]
+                except KeyError as e:
+                    raise SceneError(f"Property {e.args[0]!r} is missing!") from None
+                sd.lights.append(LightDesc(et, [float(c) for c in color], [float(c) for c in vec], n_emit))
+                n_emit += 1
+                continue
+            if et not in ("env", "constant"):
+                raise SceneError(f"emitter type {et!r} is not supported by the CUDA pathMIS core")
+            if sd.env is not None or sd.env_constant is not None:
+                raise SceneError("Only one environment emiiter is allowed for the entire scene")
+            if et == "constant":   # src/emitter/ConstantLight.cpp:8
+                if "radiance" not in ep:
+                    raise SceneError("Property 'radiance' is missing!")
+                sd.env_constant = [float(c) for c in ep["radiance"]]
+            else:
+                if env_loader is None:
+                    raise SceneError("no environment-map loader given")
+                rgb = env_loader(os.path.join(base_dir, ep["filename"]))
+                sd.env = EnvDesc(rgb, ep.get("toWorld", np.eye(4, dtype=np.float32)), ep.get("scale", 1.0))
             sd.env_emitter_index = n_emit
             n_emit += 1
         elif ch.tag == "accelerator" or ch.tag == "acceleration":

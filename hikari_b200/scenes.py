@@ -2,6 +2,7 @@
 
 * ``cornell_box``      -- plain-method small case: a Cornell box of OBJ quads
 * ``cornell_smooth``   -- the Cornell box with smooth (delta) and two-sided materials
+* ``lights_scene``     -- an open scene lit by every emitter kind (area, point, directional, constant)
 * ``icosphere``        -- subdivided icosahedron, optionally displaced by value noise
 * ``sky_envmap``       -- procedural lat-long sky (sun disk of radiance 2e4 + gradient)
 * ``mesh_heavy``       -- displaced level-8 icosphere on a ground quad under the sky
@@ -21,7 +22,7 @@ import numpy as np
 from .scenedesc import (AIR_IOR, BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR,
                         BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
                         BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX, BSDFDesc, CameraDesc, EnvDesc,
-                        FilterDesc, MeshDesc, SceneDesc)
+                        FilterDesc, LightDesc, MeshDesc, SceneDesc)
 
 # Per-channel complex IOR (n, k) of copper and gold at R, G, B ~ (650, 550, 450) nm,
 # rounded from Johnson & Christy (1972) optical constants.
@@ -154,6 +155,37 @@ def cornell_smooth(seed: int = 0, width: int = 256, height: int = 256, spp: int 
     # by BSDF sampling alone are found four times as often
     lp, li = quad((-0.5, 1.98, -0.5), (0.5, 1.98, -0.5), (0.5, 1.98, 0.5), (-0.5, 1.98, 0.5))
     light.positions, light.indices, light.radiance = lp, li, [4.25, 3.0, 1.0]
+    return sd
+
+
+def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 12, seed: int = 0) -> SceneDesc:
+    """A ground quad and five displaced icospheres (diffuse, roughDiffuse,
+    smooth plastic, rough conductor, smooth dielectric) lit, in emitter order,
+    by a point light, an emissive quad, a constant environment and a
+    directional light -- the emitter kinds interleaved as an XML scene lists
+    them."""
+    sd = SceneDesc()
+    gp, gi = quad((-6, 0, 6), (6, 0, 6), (6, 0, -6), (-6, 0, -6))
+    sd.meshes.append(MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5])))
+    mats = [BSDFDesc(type=BSDF_DIFFUSE, kd=[0.7, 0.3, 0.2]),
+            BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.3, 0.6, 0.3], alpha_u=0.6, alpha_v=0.6),
+            BSDFDesc(type=BSDF_PLASTIC, int_ior=1.5046, ext_ior=AIR_IOR, kd=[0.2, 0.3, 0.7]),
+            BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=1.0, ext_ior=1.0,
+                     eta=AU_ETA, k=AU_K),
+            BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.5046, ext_ior=AIR_IOR)]
+    for k, b in enumerate(mats):
+        P, F = displaced_icosphere(2, 0.8, (-3.2 + 1.6 * k, 0.85, 0.3 * ((k % 2) * 2 - 1)), 0.05, seed + k)
+        sd.meshes.append(MeshDesc(P.astype(np.float32), F.astype(np.uint32), b))
+    lp, li = quad((-1, 4, -1), (1, 4, -1), (1, 4, 1), (-1, 4, 1))   # faces down
+    sd.meshes.append(MeshDesc(lp, li, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.0, 0.0, 0.0]), radiance=[3.0, 3.0, 3.0]))
+    sd.lights.append(LightDesc("point", [40.0, 32.0, 24.0], [2.5, 3.0, 2.0], emitter_index=0))
+    sd.env_constant = [0.3, 0.35, 0.45]
+    sd.env_emitter_index = 2
+    sd.lights.append(LightDesc("directional", [1.2, 1.1, 0.9], [-0.4, -1.0, -0.3], emitter_index=3))
+    sd.camera = CameraDesc(width, height, look_at((0, 3.5, 8), (0, 0.6, 0), (0, 1, 0)), 45.0, 1e-4, 1e4)
+    sd.filter = FilterDesc(2, 2.0, 0.5)
+    sd.depth = depth
+    sd.spp = spp
     return sd
 
 

@@ -105,6 +105,14 @@ int hk_scene_add_mesh(hk_scene *s, const float *positions, uint32_t nv, const ui
  * rgb is H*W*3 floats, row 0 at theta = 0; to_world row-major 4x4. */
 int hk_scene_set_envmap(hk_scene *s, const float *rgb, uint32_t width, uint32_t height, const float *to_world16,
                         float scale);
+/* Constant environment emitter (ConstantLight, src/emitter/ConstantLight.cpp:8):
+ * radiance 3 floats.  One environment emitter per scene (map or constant). */
+int hk_scene_set_constant_light(hk_scene *s, const float *radiance);
+/* Point light (PointLight, src/emitter/PointLight.cpp:8): power and position, 3 floats each. */
+int hk_scene_add_point_light(hk_scene *s, const float *power, const float *position);
+/* Directional light (DirectionalLight, src/emitter/DirectionalLight.cpp:8):
+ * irradiance and direction of travel, 3 floats each. */
+int hk_scene_add_directional_light(hk_scene *s, const float *irradiance, const float *direction);
 /* PerspectiveCamera (src/camera/PerspectiveCamera.cpp:13): to_world row-major 4x4. */
 int hk_scene_set_camera(hk_scene *s, uint32_t width, uint32_t height, const float *to_world16, float fov_deg,
                         float near_clip, float far_clip);

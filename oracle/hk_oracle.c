@@ -425,6 +425,9 @@ struct ho_scene {
     int n_emit; int32_t emit_mesh[64]; int env_index;
     /* env */
     int has_env; uint32_t ew, eh; float *env; float env_scale; float to_world[9], to_local[9];
+    int env_const_on; v3 env_const;                   /* ConstantLight instead of the map */
+    /* point / directional lights: emit_mesh codes -2 - k */
+    int n_delta; struct { int directional; v3 vec, color; } delta[64];
     pdf1d *env_rows; pdf1d env_marg;
     /* camera */
     uint32_t W, H; float cam[16]; float fov, near_c, far_c;
@@ -558,6 +561,26 @@ int ho_scene_set_envmap(ho_scene *s, const float *rgb, uint32_t w, uint32_t h, c
     s->emit_mesh[s->n_emit++] = -1;
     return 0;
 }
+/* ConstantLight ctor  src/emitter/ConstantLight.cpp:8; Scene::AddChild :191 */
+int ho_scene_set_constant_light(ho_scene *s, const float *rgb) {
+    if (s->has_env) return fail("only one environment emitter");
+    if (s->n_emit >= 64) return fail("too many emitters");
+    s->has_env = 1; s->env_const_on = 1; s->env_const = vload(rgb);
+    s->env_index = s->n_emit;
+    s->emit_mesh[s->n_emit++] = -1;
+    return 0;
+}
+/* PointLight / DirectionalLight ctors  src/emitter/PointLight.cpp:8, DirectionalLight.cpp:8 */
+static int add_delta_light(ho_scene *s, int directional, const float *color, const float *vec) {
+    if (s->n_emit >= 64 || s->n_delta >= 64) return fail("too many emitters");
+    s->delta[s->n_delta].directional = directional;
+    s->delta[s->n_delta].color = vload(color);
+    s->delta[s->n_delta].vec = vload(vec);
+    s->emit_mesh[s->n_emit++] = -2 - s->n_delta++;
+    return 0;
+}
+int ho_scene_add_point_light(ho_scene *s, const float *power, const float *pos) { return add_delta_light(s, 0, power, pos); }
+int ho_scene_add_directional_light(ho_scene *s, const float *irr, const float *dir) { return add_delta_light(s, 1, irr, dir); }
 int ho_scene_set_camera(ho_scene *s, uint32_t w, uint32_t h, const float *tw16, float fov, float n, float f) {
     s->W = w; s->H = h; memcpy(s->cam, tw16, 64); s->fov = fov; s->near_c = n; s->far_c = f;
     return 0;
@@ -1649,8 +1672,47 @@ static void spherical_coords(v3 d, float *th, float *ph) {
     *th = acosf(d.z); *ph = atan2f(d.y, d.x);
     if (*ph < 0) *ph += 2.0f * PI_F;
 }
+/* ConstantLight::Sample  src/emitter/ConstantLight.cpp:15 */
+static v3 const_sample(const ho_scene *s, erec *r, float ux, float uy) {
+    float th = uy * PI_F;
+    float st = sinf(th);
+    if (st != 0.0f) r->pdf = 1.0f / (2.0f * (float)(M_PI * M_PI) * st);
+    else return V(0, 0, 0);
+    float ph = ux * (float)(2.0 * M_PI);
+    float ct = cosf(th), sp = sinf(ph), cp = cosf(ph);
+    r->wi = V(st * cp, st * sp, ct);                  /* SphericalDirection :467 */
+    r->n = scl(r->wi, -1.0f);
+    r->p = add(r->ref, scl(scl(r->wi, r->dist), 2.0f));
+    return divs(s->env_const, r->pdf);
+}
+/* ConstantLight::Pdf :36 */
+static float const_pdf(const erec *r) {
+    float th, ph;
+    spherical_coords(r->wi, &th, &ph);
+    float st = sinf(th);
+    if (st == 0.0f) return 0.0f;
+    return 1.0f / (2.0f * (float)(M_PI * M_PI) * st);
+}
+/* PointLight::Sample  src/emitter/PointLight.cpp:15; DirectionalLight::Sample  DirectionalLight.cpp:18 */
+static v3 delta_sample(const ho_scene *s, int k, erec *r) {
+    if (!s->delta[k].directional) {
+        r->p = s->delta[k].vec;
+        v3 wi = sub(r->p, r->ref);
+        r->dist = norm(wi);
+        r->wi = normalize(wi);
+        r->n = scl(r->wi, -1.0f);
+        r->pdf = 1.0f;
+        return scl(s->delta[k].color, 1.0f / ((4.0f * PI_F) * (r->dist * r->dist)));
+    }
+    r->wi = scl(normalize(s->delta[k].vec), -1.0f);
+    r->p = add(r->ref, scl(r->wi, 2.0f * r->dist));
+    r->n = scl(r->wi, -1.0f);
+    r->pdf = 1.0f;
+    return s->delta[k].color;
+}
 /* EnvironmentLight::Sample  src/emitter/EnvironmentLight.cpp:41 */
 static v3 env_sample(const ho_scene *s, erec *r, float ux, float uy) {
+    if (s->env_const_on) return const_sample(s, r, ux, uy);
     float py, px; int iy, ix;
     float dy = pdf1d_sample_cont(&s->env_marg, uy, &py, &iy);
     float dx = pdf1d_sample_cont(&s->env_rows[iy], ux, &px, &ix);
@@ -1671,6 +1733,7 @@ static v3 env_sample(const ho_scene *s, erec *r, float ux, float uy) {
 }
 /* EnvironmentLight::Pdf :78 and DiscretePDF2D::Pdf  src/core/DiscretePDF.cpp:127 */
 static float env_pdf(const ho_scene *s, const erec *r) {
+    if (s->env_const_on) return const_pdf(r);
     float th, ph;
     spherical_coords(mat3_mul(s->to_local, r->wi), &th, &ph);
     float st = sinf(th);
@@ -1682,6 +1745,7 @@ static float env_pdf(const ho_scene *s, const erec *r) {
 }
 /* EnvironmentLight::Eval :92 */
 static v3 env_eval(const ho_scene *s, v3 wi) {
+    if (s->env_const_on) return s->env_const;   /* ConstantLight::Eval :47 */
     float th, ph;
     spherical_coords(mat3_mul(s->to_local, wi), &th, &ph);
     if (isnan(th) || isnan(ph)) return V(0, 0, 0);
@@ -1714,7 +1778,8 @@ static void camera_ray(const ho_scene *s, float px, float py, v3 *o, v3 *d, floa
 typedef struct { uint64_t rays, shadow; } ctr_t;
 static inline v3 emitter_sample_any(const ho_scene *s, int e, erec *r, float ux, float uy, float u1) {
     int mi = s->emit_mesh[e];
-    if (mi < 0) return env_sample(s, r, ux, uy);
+    if (mi == -1) return env_sample(s, r, ux, uy);
+    if (mi < -1) return delta_sample(s, -2 - mi, r);
     return area_sample(s, &s->meshes[mi], r, ux, uy, u1);
 }
 
@@ -1935,6 +2000,7 @@ float ho_emitter_pdf(const ho_scene *s, int e, const float *ref, const float *p,
     erec r; r.ref = vload(ref); r.p = vload(p); r.n = vload(n);
     v3 wi = sub(r.p, r.ref); r.dist = norm(wi); r.wi = divs(wi, r.dist);
     int mi = s->emit_mesh[e];
+    if (mi < -1) return 0.0f;                                  /* point / directional: Pdf is 0 */
     if (mi < 0) { r.wi = vload(p); return env_pdf(s, &r); }   /* env: p carries the direction */
     return area_pdf(&s->meshes[mi], &r);
 }

@@ -82,6 +82,10 @@ int  ho_scene_add_mesh(ho_scene *s, const float *positions, uint32_t nv,
 /* rgb H*W*3 row-major (row 0 = theta 0); to_world row-major 4x4. */
 int  ho_scene_set_envmap(ho_scene *s, const float *rgb, uint32_t w, uint32_t h,
                          const float *to_world16, float scale);
+/* ConstantLight radiance (one environment emitter per scene); point / directional lights. */
+int  ho_scene_set_constant_light(ho_scene *s, const float *radiance);
+int  ho_scene_add_point_light(ho_scene *s, const float *power, const float *position);
+int  ho_scene_add_directional_light(ho_scene *s, const float *irradiance, const float *direction);
 /* camera: to_world row-major 4x4, horizontal fov degrees, clip planes. */
 int  ho_scene_set_camera(ho_scene *s, uint32_t width, uint32_t height, const float *to_world16,
                          float fov_deg, float near_clip, float far_clip);

@@ -54,6 +54,9 @@ def lib():
         L.ho_scene_add_bsdf.argtypes = [P, C.POINTER(BsdfDescC)]
         L.ho_scene_add_mesh.argtypes = [P, P, C.c_uint32, P, C.c_uint32, P, C.c_int32, P]
         L.ho_scene_set_envmap.argtypes = [P, P, C.c_uint32, C.c_uint32, P, C.c_float]
+        L.ho_scene_set_constant_light.argtypes = [P, P]
+        L.ho_scene_add_point_light.argtypes = [P, P, P]
+        L.ho_scene_add_directional_light.argtypes = [P, P, P]
         L.ho_scene_set_camera.argtypes = [P, C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
         L.ho_scene_set_filter.argtypes = [P, C.c_int, C.c_float, C.c_float, C.c_float]
         L.ho_scene_set_background.argtypes = [P, P, C.c_int]
@@ -124,26 +127,27 @@ class OracleScene:
         self.mesh_bsdf = []
         for m in desc.meshes:
             self.mesh_bsdf.append(self.add_bsdf(m.bsdf))
-        emitters = desc.emitter_order()
-        env_pos = emitters.index(-1) if -1 in emitters else -1
-        n_added = 0
-        for i, m in enumerate(desc.meshes):
-            if desc.env is not None and n_added == env_pos:
+        for kind, i in desc.build_steps():   # emitters in Scene::AddChild order
+            if kind == "env":
                 self._set_env()
-                n_added += 1
-            pos = _f32(m.positions)
-            idx = np.ascontiguousarray(m.indices, dtype=np.uint32)
-            nrm = _f32(m.normals) if m.normals is not None else None
-            rad = _f32(m.radiance) if m.radiance is not None else None
-            self._keep += [pos, idx, nrm, rad]
-            r = L.ho_scene_add_mesh(self.h, _p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm),
-                                    self.mesh_bsdf[i], _p(rad))
-            if r < 0:
-                raise RuntimeError(L.ho_last_error().decode())
-            if m.radiance is not None:
-                n_added += 1
-        if desc.env is not None and env_pos >= n_added:
-            self._set_env()
+            elif kind == "light":
+                l = desc.lights[i]
+                col, vec = _f32(l.color), _f32(l.vector)
+                self._keep += [col, vec]
+                add = L.ho_scene_add_point_light if l.kind == "point" else L.ho_scene_add_directional_light
+                if add(self.h, _p(col), _p(vec)) < 0:
+                    raise RuntimeError(L.ho_last_error().decode())
+            else:
+                m = desc.meshes[i]
+                pos = _f32(m.positions)
+                idx = np.ascontiguousarray(m.indices, dtype=np.uint32)
+                nrm = _f32(m.normals) if m.normals is not None else None
+                rad = _f32(m.radiance) if m.radiance is not None else None
+                self._keep += [pos, idx, nrm, rad]
+                r = L.ho_scene_add_mesh(self.h, _p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm),
+                                        self.mesh_bsdf[i], _p(rad))
+                if r < 0:
+                    raise RuntimeError(L.ho_last_error().decode())
         cam = desc.camera
         tw = _f32(cam.to_world)
         L.ho_scene_set_camera(self.h, cam.width, cam.height, _p(tw), cam.fov, cam.near_clip, cam.far_clip)
@@ -155,6 +159,12 @@ class OracleScene:
             raise RuntimeError(L.ho_last_error().decode())
 
     def _set_env(self):
+        if self.desc.env_constant is not None:
+            c = _f32(self.desc.env_constant)
+            self._keep.append(c)
+            if lib().ho_scene_set_constant_light(self.h, _p(c)) < 0:
+                raise RuntimeError(lib().ho_last_error().decode())
+            return
         e = self.desc.env
         rgb = _f32(e.rgb)
         tw = _f32(e.to_world)

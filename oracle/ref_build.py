@@ -1,6 +1,7 @@
-"""Build oracle/_ref/libhikari_ref_bsdf.so: the reference's own BSDF classes
-compiled from the reference sources where they lie, for record-wise parity
-tests of the oracle restatement.
+"""Build oracle/_ref/libhikari_ref_bsdf.so: the reference's own BSDF and
+point / directional / constant emitter classes compiled from the reference
+sources where they lie, for record-wise parity tests of the oracle
+restatement.
 
 Recipe (no reference build system is run):
   * a shim include tree (oracle/_ref/shim) of symlinks named like the
@@ -33,6 +34,7 @@ CORE = ["Object", "PropertyList", "BSDF", "Texture", "MicrofacetDistribution", "
 BSDFS = ["DiffuseBSDF", "RoughConductorBSDF", "RoughDielectricBSDF", "RoughPlasticBSDF", "RoughCoatingBSDF",
          "MirrorBSDF", "ConductorBSDF", "DielectricBSDF", "PlasticBSDF", "TwoSidedBSDF", "CoatingBSDF",
          "RoughDiffuseBSDF"]
+EMITTERS = ["PointLight", "DirectionalLight", "ConstantLight"]
 
 
 def _link(src, dst):
@@ -80,6 +82,7 @@ def build(ref: str = "/root/reference") -> str:
     objs = []
     srcs = [os.path.join(ref, "src", "core", c + ".cpp") for c in CORE] + \
            [os.path.join(ref, "src", "bsdf", b + ".cpp") for b in BSDFS] + \
+           [os.path.join(ref, "src", "emitter", e + ".cpp") for e in EMITTERS] + \
            [os.path.join(HERE, "ref_shim", "ref_bridge.cpp")]
     for s in srcs:
         o = os.path.join(objd, os.path.basename(s) + ".o")

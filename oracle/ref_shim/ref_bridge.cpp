@@ -9,6 +9,7 @@
 #include <core\Intersection.hpp>
 #include <core\Color.hpp>
 #include <core\Vector.hpp>
+#include <core\Emitter.hpp>
 
 using namespace Hikari;
 
@@ -106,6 +107,50 @@ float hr_bsdf_pdf(void *h, const float *wi, const float *wo, int measure) {
     BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), Vector3f(wo[0], wo[1], wo[2]), EMeasure(measure),
                       ETransportMode::ERadiance, &g_sampler, null_isect());
     return ((BSDF *)h)->Pdf(r);
+}
+
+/* kind: 0 point (power, position), 1 directional (irradiance, direction), 2 constant (radiance) */
+void *hr_emitter_create(int kind, const float *color, const float *vec) {
+    static const char *names[] = {"point", "directional", "constant"};
+    try {
+        PropertyList pl;
+        Color3f c(color[0], color[1], color[2]);
+        if (kind == 0) { pl.SetColor("power", c); pl.SetPoint("position", Point3f(vec[0], vec[1], vec[2])); }
+        if (kind == 1) { pl.SetColor("irradiance", c); pl.SetVector("direction", Vector3f(vec[0], vec[1], vec[2])); }
+        if (kind == 2) pl.SetColor("radiance", c);
+        Emitter *e = (Emitter *)ObjectFactory::CreateInstance(names[kind], pl);
+        e->Activate();
+        return e;
+    } catch (const std::exception &ex) {
+        fprintf(stderr, "hr_emitter_create: %s\n", ex.what());
+        return nullptr;
+    }
+}
+
+/* Emitter::Sample for n references: in ref(3) u2(2) u1 distance; out p(3) n(3) wi(3) pdf dist value(3) */
+void hr_emitter_sample(void *h, uint64_t n, const float *in, float *out) {
+    for (uint64_t i = 0; i < n; i++) {
+        const float *q = in + 7 * i;
+        EmitterQueryRecord r(Point3f(q[0], q[1], q[2]));
+        r.Distance = q[6];
+        r.Pdf = 0.0f;
+        Color3f v = ((Emitter *)h)->Sample(r, Point2f(q[3], q[4]), q[5]);
+        float *o = out + 14 * i;
+        o[0] = r.P.x(); o[1] = r.P.y(); o[2] = r.P.z(); o[3] = r.N.x(); o[4] = r.N.y(); o[5] = r.N.z();
+        o[6] = r.Wi.x(); o[7] = r.Wi.y(); o[8] = r.Wi.z(); o[9] = r.Pdf; o[10] = r.Distance;
+        o[11] = v[0]; o[12] = v[1]; o[13] = v[2];
+    }
+}
+
+/* Emitter::Eval / Pdf for world directions (the environment emitters): out value(3) pdf */
+void hr_emitter_eval_dir(void *h, uint64_t n, const float *wi, float *out) {
+    for (uint64_t i = 0; i < n; i++) {
+        EmitterQueryRecord r;
+        r.Wi = Vector3f(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        Color3f v = ((Emitter *)h)->Eval(r);
+        out[4 * i] = v[0]; out[4 * i + 1] = v[1]; out[4 * i + 2] = v[2];
+        out[4 * i + 3] = ((Emitter *)h)->Pdf(r);
+    }
 }
 
 /* batched over n AoS records (same layout as ho_bsdf_batch) */

@@ -83,12 +83,21 @@ def test_bsdf_batch_parity(bsdf_pair):
         bad = (dwo > 1e-5) & steep
         assert np.mean(~bad) >= 0.9998, f"{name}: sampled directions differ by > 1e-5 on {bad.sum()} steep records"
         assert dwo.max() <= 1e-3, f"{name}: sampled directions differ by {dwo.max()}"
+        # weights and pdfs: 1e-2 on every record whose sampled direction is not
+        # grazing; at grazing exits the Fresnel transmittance near the critical
+        # angle (a square-root edge) and the cosine map turn ulps into percents
+        idx = np.nonzero(keep)[0]
+        steep_all = np.abs(o["s_wo"][idx][:, 2]) >= 0.05
         for key in ("s_w", "s_pdf"):
-            ok = rel_close(g[key][keep], o[key][keep], RTOL).reshape(keep.sum(), -1).all(1)
-            loose = rel_close(g[key][keep], o[key][keep], 1e-2).reshape(keep.sum(), -1).all(1)
+            ok = rel_close(g[key][idx], o[key][idx], RTOL).reshape(len(idx), -1).all(1)
+            loose = rel_close(g[key][idx], o[key][idx], 1e-2).reshape(len(idx), -1).all(1)
             report.append((name, key, ok.mean()))
             assert ok.mean() >= 0.999, f"{name} {key}: {ok.mean():.6f} within {RTOL}"
-            assert loose.all(), f"{name} {key}: {np.sum(~loose)} records beyond 1e-2"
+            far = idx[~loose & steep_all]
+            assert len(far) == 0, (f"{name} {key}: {len(far)} steep records beyond 1e-2, first {far[0]}: wi {wi[far[0]]} "
+                                   f"u2 {u2[far[0]]} u1 {u1[far[0]]} gpu {g[key][far[0]]} oracle {o[key][far[0]]} "
+                                   f"wo {o['s_wo'][far[0]]}")
+            assert np.isfinite(g[key][idx]).all() == np.isfinite(o[key][idx]).all()
     worst = min(report, key=lambda r: r[2])
     print("worst BSDF agreement:", worst)
 
@@ -188,6 +197,32 @@ def test_area_emitter_sample_parity():
     g = gs.emitter_sample(0, _t(inp)).cpu().numpy()
     o = np.stack([os_.emitter_sample(0, r[:3], (r[3], r[4], r[5])) for r in inp])
     assert rel_close(g[:, :14], o[:, :14], 1e-5, atol=1e-6).mean() > 0.9999
+
+
+@pytest.mark.parametrize("emitter", [0, 1, 2, 3])
+def test_light_emitter_sample_parity(emitter):
+    """Point light, area light, constant environment and directional light
+    (the emitter order of the lights scene) sampled on the GPU and by the oracle."""
+    sd = scenes.lights_scene(width=16, height=16)
+    gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
+    assert gs.info.n_emitters == 4 and gs.info.env_index == 2
+    rng = np.random.default_rng(40 + emitter)
+    n = 4096
+    inp = np.zeros((n, 8), np.float32)
+    inp[:, 0:3] = rng.uniform(-3, 3, (n, 3)) + [0, 2, 0]
+    inp[:, 3:6] = rng.random((n, 3))
+    g = gs.emitter_sample(emitter, _t(inp)).cpu().numpy()
+    o = np.stack([os_.emitter_sample(emitter, r[:3], (r[3], r[4], r[5])) for r in inp])
+    ok = rel_close(g[:, :14], o[:, :14], 1e-5, atol=1e-5)
+    print("emitter", emitter, "records within 1e-5:", ok.all(1).mean())
+    assert ok.all(1).mean() > 0.999
+    if emitter == 2:   # the constant environment's Eval and Pdf
+        d = rng.normal(size=(n, 3)).astype(np.float32)
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        rgb, pdf = gs.env_eval(_t(d))
+        assert np.array_equal(rgb.cpu().numpy(), np.tile(np.float32(sd.env_constant), (n, 1)))
+        po = np.array([os_.emitter_pdf(2, np.zeros(3), x, np.zeros(3)) for x in d], np.float32)
+        assert rel_close(pdf.cpu().numpy(), po, 1e-5).mean() > 0.999
 
 
 def test_env_emitter_parity():

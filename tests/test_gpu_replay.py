@@ -40,6 +40,7 @@ SCENES = {
     "cornell": lambda: scenes.cornell_box(width=32, height=32),
     "smooth": lambda: scenes.cornell_smooth(width=32, height=32),
     "heterogeneous": lambda: scenes.heterogeneous(width=32, height=32, n_spheres=12, levels=(3,), level_p=(1.0,), env_res=(256, 128)),
+    "lights": lambda: scenes.lights_scene(width=32, height=32),
 }
 
 

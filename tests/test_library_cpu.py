@@ -222,3 +222,54 @@ def test_xml_two_sided_errors(L, tmp_path, body, needle):
         hk.parse_xml_info(path)
     with pytest.raises(SceneError, match=needle):
         parse_xml(path)
+
+
+LIGHTS_XML = """<?xml version="1.0"?>
+<scene>
+  <integrator type="pathMIS"><integer name="depth" value="8"/></integrator>
+  <camera type="perspective">
+    <transform name="toWorld"><lookat origin="0, 1, 4" target="0, 0.5, 0" up="0, 1, 0"/></transform>
+    <integer name="width" value="16"/><integer name="height" value="16"/>
+  </camera>
+  <emitter type="point"><color name="power" value="10, 10, 10"/><point name="position" value="0, 3, 0"/></emitter>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="coating"><float name="thickness" value="0.5"/><bsdf type="roughDiffuse"><float name="alpha" value="0.4"/></bsdf></bsdf>
+  </mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/><bsdf type="diffuse"/>
+    <emitter type="area"><color name="radiance" value="1, 1, 1"/></emitter></mesh>
+  <emitter type="constant"><color name="radiance" value="0.5, 0.6, 0.7"/></emitter>
+  <emitter type="directional"><color name="irradiance" value="1, 1, 1"/><vector name="direction" value="0, -1, 0"/></emitter>
+</scene>
+"""
+
+
+def test_xml_lights_and_layers(L, tmp_path):
+    """Point, area, constant and directional emitters keep the XML order in
+    both parsers; coating over roughDiffuse parses in both."""
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "lights.xml")
+    open(path, "w").write(LIGHTS_XML)
+    info, depth, spp = hk.parse_xml_info(path)
+    sd = parse_xml(path)[0]
+    assert info.n_emitters == 4 and info.env_index == 2
+    assert sd.emitter_order() == [-2, 1, -1, -3]
+    assert [l.kind for l in sd.lights] == ["point", "directional"] and sd.env_constant == pytest.approx([0.5, 0.6, 0.7])
+    assert info.n_bsdfs == 3
+    c = sd.meshes[0].bsdf
+    assert c.type == 10 and c.thickness == 0.5 and c.nested.type == 11 and c.nested.alpha_u == pytest.approx(0.4)
+
+
+def test_oracle_builds_every_light(tmp_path):
+    from oracle.oracle import OracleScene
+
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "lights.xml")
+    open(path, "w").write(LIGHTS_XML)
+    sd = parse_xml(path)[0]
+    o = OracleScene(sd)
+    from oracle import oracle as O
+    assert O.lib().ho_scene_num_emitters(o.h) == 4
+    p = o.emitter_sample(0, np.float32([0, 0, 0]), (0.5, 0.5, 0.5))   # point light at (0, 3, 0)
+    assert np.allclose(p[:3], [0, 3, 0]) and p[9] == 1.0 and np.allclose(p[11:], 10 / (4 * np.pi * 9), rtol=1e-6)
+    d = o.emitter_sample(3, np.float32([0, 0, 0]), (0.5, 0.5, 0.5))   # directional light travelling down
+    assert np.allclose(d[6:9], [0, 1, 0]) and np.allclose(d[11:], 1.0)

@@ -162,3 +162,56 @@ def test_oracle_bsdf_bit_exact_vs_reference(name):
 
 def _has_delta(d):
     return d is not None and (d.type in SMOOTH_BSDFS or _has_delta(d.nested) or _has_delta(d.nested2))
+
+
+LIGHTS = {   # kind (0 point, 1 directional, 2 constant), power / irradiance / radiance, position / direction
+    "point": (0, [10.0, 8.0, 6.0], [0.3, 1.5, -0.2]),
+    "directional": (1, [2.0, 1.5, 1.0], [0.3, -1.0, 0.2]),
+    "constant": (2, [1.28, 1.27, 1.25], [0.0, 0.0, 0.0]),
+}
+
+
+@pytest.mark.parametrize("name", list(LIGHTS))
+def test_oracle_lights_bit_exact_vs_reference(name):
+    """PointLight / DirectionalLight / ConstantLight::Sample (and the constant
+    light's Eval / Pdf) record by record against the reference classes."""
+    from hikari_b200.scenedesc import LightDesc, MeshDesc
+
+    R = _ref_lib()
+    R.hr_emitter_create.restype = C.c_void_p
+    R.hr_emitter_create.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+    R.hr_emitter_sample.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    R.hr_emitter_eval_dir.argtypes = [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]
+    kind, col, vec = LIGHTS[name]
+    sd = SceneDesc()
+    quad = np.array([[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], np.float32)
+    sd.meshes.append(MeshDesc(quad, np.array([[0, 1, 2], [3, 0, 2]], np.uint32), BSDFDesc()))
+    if kind == 2:
+        sd.env_constant = col
+    else:
+        sd.lights.append(LightDesc("point" if kind == 0 else "directional", col, vec))
+    o = O.OracleScene(sd)
+    bb = o.bbox()
+    ext = (bb[3:] - bb[:3]).astype(np.float32)
+    radius = np.float32(0.5) * np.sqrt(ext[0] * ext[0] + (ext[1] * ext[1] + ext[2] * ext[2]), dtype=np.float32)
+    rng = np.random.default_rng(5)
+    n = 4000
+    inp = np.concatenate([rng.uniform(-2, 2, (n, 3)), rng.random((n, 3)), np.full((n, 1), radius)], 1).astype(np.float32)
+    inp[:8, 4] = [0.0, 1.0, 0.5, 0.25, 1e-8, 1 - 1e-7, 0.0, 1.0]   # theta at the poles for the constant light
+    h = R.hr_emitter_create(kind, O._p(np.float32(col)), O._p(np.float32(vec)))
+    assert h
+    ref = np.zeros((n, 14), np.float32)
+    R.hr_emitter_sample(h, n, O._p(inp), O._p(ref))
+    got = np.stack([o.emitter_sample(0, inp[i, :3], inp[i, 3:6]) for i in range(n)])
+    valid = np.any(ref[:, 11:] != 0, 1)
+    np.testing.assert_array_equal(got[:, 11:], ref[:, 11:])          # value
+    np.testing.assert_array_equal(got[valid], ref[valid])             # p, n, wi, pdf, distance
+    if kind == 2:
+        d = rng.normal(size=(n, 3))
+        d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+        d[:2] = [[0, 0, 1], [0, 0, -1]]
+        ev = np.zeros((n, 4), np.float32)
+        R.hr_emitter_eval_dir(h, n, O._p(d), O._p(ev))
+        for i in range(n):
+            np.testing.assert_array_equal(o.env_eval(d[i]), ev[i, :3])
+            assert o.emitter_pdf(0, np.zeros(3, np.float32), d[i], np.zeros(3, np.float32)) == ev[i, 3]
