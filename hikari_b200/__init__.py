@@ -116,6 +116,8 @@ def lib():
         "hk_scene_add_mesh": ([P, P, C.c_uint32, P, C.c_uint32, P, I32, P, C.POINTER(I32)], C.c_int),
         "hk_scene_set_envmap": ([P, P, C.c_uint32, C.c_uint32, P, F], C.c_int),
         "hk_scene_set_constant_light": ([P, P], C.c_int),
+        "hk_obj_load": ([C.c_char_p, P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P, P, P, P, C.POINTER(I32)],
+                        C.c_int),
         "hk_scene_add_point_light": ([P, P, P], C.c_int),
         "hk_scene_add_directional_light": ([P, P, P], C.c_int),
         "hk_scene_set_camera": ([P, C.c_uint32, C.c_uint32, P, F, F, F], C.c_int),
@@ -481,6 +483,22 @@ def bvh_check(tris: np.ndarray):
     a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
     check(lib().hk_bvh_check(t.ctypes.data, t.shape[0], C.byref(a), C.byref(b), C.byref(c)))
     return a.value, b.value, c.value
+
+
+def obj_load(path: str, to_world=None):
+    """Load an OBJ through the library's parallel reader: (positions (nv, 3),
+    indices (nt, 3), normals (nv, 3) or None, uv (nv, 2) or None)."""
+    L = lib()
+    tw = None if to_world is None else np.ascontiguousarray(to_world, dtype=np.float32)
+    nv, nt, attrs = C.c_uint32(), C.c_uint32(), C.c_int32()
+    check(L.hk_obj_load(path.encode(), _p(tw), C.byref(nv), C.byref(nt), None, None, None, None, C.byref(attrs)))
+    pos = np.empty((nv.value, 3), np.float32)
+    nrm = np.empty((nv.value, 3), np.float32)
+    uv = np.empty((nv.value, 2), np.float32)
+    idx = np.empty((nt.value, 3), np.uint32)
+    check(L.hk_obj_load(path.encode(), _p(tw), C.byref(nv), C.byref(nt), _p(pos), _p(nrm), _p(uv), _p(idx),
+                        C.byref(attrs)))
+    return pos, idx, (nrm if attrs.value & 1 else None), (uv if attrs.value & 2 else None)
 
 
 def parse_xml_info(path: str):

@@ -16,9 +16,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libhikari_b200.so")
-SOURCES = ["hk_kernels.cu", "hk_wavefront.cu", "hk_host.cpp", "hk_engine.cpp", "hk_server.cpp", "hk_bvh.cpp", "hk_xml.cpp"]
+SOURCES = ["hk_kernels.cu", "hk_wavefront.cu", "hk_host.cpp", "hk_engine.cpp", "hk_server.cpp", "hk_bvh.cpp", "hk_xml.cpp",
+           "hk_obj.cpp"]
 HEADERS = ["hk_device.h", "hk_math.cuh", "hk_bsdf.cuh", "hk_traverse.cuh", "hk_shading.cuh", "hk_kernels.h",
-           "hk_bvh.h", "hk_xml.h", "hk_wavefront.h", "hk_engine.h", "hk_hostutil.h", "hk_internal.h"]
+           "hk_bvh.h", "hk_xml.h", "hk_wavefront.h", "hk_engine.h", "hk_hostutil.h", "hk_internal.h", "hk_obj.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-pthread",
                      "--expt-relaxed-constexpr"]

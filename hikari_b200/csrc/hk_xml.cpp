@@ -5,6 +5,7 @@
 // HikariException messages) and ends in the C ABI: a parsed Scene uploads
 // itself through hk_scene_* and builds (Integrator::Preprocess).
 #include "hk_xml.h"
+#include "hk_obj.h"
 
 #include <zlib.h>
 
@@ -829,75 +830,14 @@ public:
         Matrix4f M = p.GetTransform("toWorld", identity4());
         Matrix4f Minv;
         if (!inverse4(M, Minv)) throw HikariException("mesh toWorld is singular");
-        std::ifstream f(fn);
-        if (!f) throw HikariException("Unable to open OBJ file \"" + fn + "\"!");
-        std::vector<Color3f> P, N;
-        struct Key { int p, t, n; bool operator==(const Key &o) const { return p == o.p && t == o.t && n == o.n; } };
-        struct KH { size_t operator()(const Key &k) const { return ((size_t)k.p * 73856093u) ^ ((size_t)k.t * 19349663u) ^ ((size_t)k.n * 83492791u); } };
-        std::unordered_map<Key, uint32_t, KH> vmap;
-        std::vector<Key> verts;
-        std::string line;
-        auto parse_key = [&](const std::string &s) {
-            Key k{0, 0, 0};
-            auto parts = std::vector<std::string>();
-            size_t a = 0;
-            for (;;) {
-                size_t b = s.find('/', a);
-                parts.push_back(s.substr(a, b == std::string::npos ? std::string::npos : b - a));
-                if (b == std::string::npos) break;
-                a = b + 1;
-            }
-            if (parts.empty() || parts.size() > 3) throw HikariException("Invalid vertex data: \"" + s + "\"");
-            k.p = to_int(parts[0]);
-            if (parts.size() > 1 && !parts[1].empty()) k.t = to_int(parts[1]);
-            if (parts.size() > 2 && !parts[2].empty()) k.n = to_int(parts[2]);
-            return k;
-        };
-        while (std::getline(f, line)) {
-            std::istringstream ls(line);
-            std::string pre;
-            ls >> pre;
-            if (pre == "v") {
-                float x, y, z;
-                ls >> x >> y >> z;
-                float q[4];
-                for (int r = 0; r < 4; r++) q[r] = M[4 * r] * x + M[4 * r + 1] * y + M[4 * r + 2] * z + M[4 * r + 3];
-                P.push_back({q[0] / q[3], q[1] / q[3], q[2] / q[3]});
-            } else if (pre == "vn") {
-                float x, y, z;
-                ls >> x >> y >> z;
-                // normals by the inverse transpose, then normalised
-                Color3f n{Minv[0] * x + Minv[4] * y + Minv[8] * z, Minv[1] * x + Minv[5] * y + Minv[9] * z,
-                          Minv[2] * x + Minv[6] * y + Minv[10] * z};
-                N.push_back(normalized(n));
-            } else if (pre == "f") {
-                std::string v[4];
-                ls >> v[0] >> v[1] >> v[2] >> v[3];
-                Key k[4];
-                int nv = v[3].empty() ? 3 : 4;
-                for (int i = 0; i < nv; i++) k[i] = parse_key(v[i]);
-                Key tri[6] = {k[0], k[1], k[2], k[3], k[0], k[2]};
-                for (int i = 0; i < (nv == 4 ? 6 : 3); i++) {
-                    auto it = vmap.find(tri[i]);
-                    if (it == vmap.end()) {
-                        vmap[tri[i]] = (uint32_t)verts.size();
-                        idx.push_back((uint32_t)verts.size());
-                        verts.push_back(tri[i]);
-                    } else {
-                        idx.push_back(it->second);
-                    }
-                }
-            }
+        try {
+            ObjMesh m = load_obj(fn, M.data(), Minv.data());
+            pos.swap(m.pos);
+            nrm.swap(m.nrm);
+            idx.swap(m.idx);
+        } catch (const std::runtime_error &e) {
+            throw HikariException(e.what());
         }
-        for (auto &k : verts) {
-            if (k.p < 1 || k.p > (int)P.size()) throw HikariException("OBJ position index out of range");
-            for (int c = 0; c < 3; c++) pos.push_back(P[k.p - 1][c]);
-        }
-        if (!N.empty())
-            for (auto &k : verts) {
-                if (k.n < 1 || k.n > (int)N.size()) throw HikariException("OBJ normal index out of range");
-                for (int c = 0; c < 3; c++) nrm.push_back(N[k.n - 1][c]);
-            }
     }
     EClassType GetClassType() const override { return EClassType::EMesh; }
     void AddChild(Object *c, const std::string &name) override {
@@ -1224,3 +1164,13 @@ extern "C" int hk_exr_write_impl(const char *path, int w, int h, const float *rg
         return HK_ERR_IO;
     }
 }
+
+namespace hikari {
+bool invert4(const float *m, float *out) {
+    Matrix4f a, b;
+    std::memcpy(a.data(), m, sizeof a);
+    if (!inverse4(a, b)) return false;
+    std::memcpy(out, b.data(), sizeof b);
+    return true;
+}
+}  // namespace hikari

@@ -113,6 +113,14 @@ int hk_scene_add_point_light(hk_scene *s, const float *power, const float *posit
 /* Directional light (DirectionalLight, src/emitter/DirectionalLight.cpp:8):
  * irradiance and direction of travel, 3 floats each. */
 int hk_scene_add_directional_light(hk_scene *s, const float *irradiance, const float *direction);
+/* OBJ ingest (WavefrontObjMesh, src/mesh/WavefrontObjMesh.cpp:10-152), parsed
+ * in parallel: positions (3*nv) transformed by to_world16 (row-major 4x4, NULL =
+ * identity), normals (3*nv) by its inverse transpose, texture coordinates
+ * (2*nv), indices (3*nt), quads split and vertices de-duplicated in first-use
+ * order like the reference.  Call with positions == NULL to get nv / nt, then
+ * with arrays of that size; attrs bit 0: normals present, bit 1: uv present. */
+int hk_obj_load(const char *path, const float *to_world16, uint32_t *nv, uint32_t *nt, float *positions,
+                float *normals, float *uv, uint32_t *indices, int32_t *attrs);
 /* PerspectiveCamera (src/camera/PerspectiveCamera.cpp:13): to_world row-major 4x4. */
 int hk_scene_set_camera(hk_scene *s, uint32_t width, uint32_t height, const float *to_world16, float fov_deg,
                         float near_clip, float far_clip);

@@ -273,3 +273,62 @@ def test_oracle_builds_every_light(tmp_path):
     assert np.allclose(p[:3], [0, 3, 0]) and p[9] == 1.0 and np.allclose(p[11:], 10 / (4 * np.pi * 9), rtol=1e-6)
     d = o.emitter_sample(3, np.float32([0, 0, 0]), (0.5, 0.5, 0.5))   # directional light travelling down
     assert np.allclose(d[6:9], [0, 1, 0]) and np.allclose(d[11:], 1.0)
+
+
+def _mixed_obj(rng, style, n=3000):
+    """style: 0 "p", 1 "p/t", 2 "p//n", 3 "p/t/n" face keys (the reference
+    reads normals / texcoords of every vertex when the file has any)."""
+    lines = ["# OBJ with comments, quads, CRLF, signs and exponents", "o thing", "g group"]
+    P = rng.uniform(-5, 5, (n, 3))
+    for i, p in enumerate(P):
+        x, y, z = (f"{c:+.7e}" if i % 7 == 0 else f"{c:.6f}" for c in p)
+        lines.append(f"v {x} {y} {z}" + ("\r" if i % 5 == 0 else ""))
+    if style in (1, 3):
+        lines += [f"vt {rng.random():.5f} {rng.random():.5f}" for _ in range(n // 2)]
+    if style in (2, 3):
+        for _ in range(n // 3):
+            v = rng.normal(size=3)
+            lines.append(f"vn {v[0]:.6f} {v[1]:.6f} {v[2]:.6f}")
+    lines.append("s off")
+    for i in range(2 * n):
+        ids = rng.integers(1, n + 1, 4 if i % 3 == 0 else 3)
+        t = lambda: rng.integers(1, n // 2 + 1)
+        m = lambda: rng.integers(1, n // 3 + 1)
+        keys = [[f"{a}", f"{a}/{t()}", f"{a}//{m()}", f"{a}/{t()}/{m()}"][style] for a in ids]
+        lines.append("f " + " ".join(keys))
+    return "\n".join(lines) + "\n"
+
+
+def test_parallel_obj_reader_matches_reference_rules(L, tmp_path):
+    """The library's parallel OBJ reader against the line-by-line restatement
+    of WavefrontObjMesh: same vertex order and indices, positions and normals
+    to float rounding of the transform."""
+    from hikari_b200.scenedesc import load_obj
+
+    rng = np.random.default_rng(12)
+    M = np.array([[0.5, 0.1, 0, 1], [0, 2, 0.3, -1], [0.2, 0, 1.5, 3], [0, 0, 0, 1]], np.float32)
+    for style in range(4):
+        path = str(tmp_path / f"mixed{style}.obj")
+        open(path, "w", newline="").write(_mixed_obj(rng, style))
+        pos, idx, nrm, uv = hk.obj_load(path, M)
+        p2, i2, n2, bbox = load_obj(path, M)
+        assert idx.shape == i2.shape and np.array_equal(idx, i2)
+        assert pos.shape == p2.shape and np.allclose(pos, p2, rtol=1e-6, atol=1e-5)
+        assert (nrm is None) == (n2 is None) and (nrm is None or np.allclose(nrm, n2, atol=1e-5))
+        assert (uv is not None) == (style in (1, 3))
+    # positions-only fast path, with quads
+    path2 = str(tmp_path / "plain.obj")
+    open(path2, "w").write(QUAD_OBJ + "v 0 1 0\nf 1 2 5\n")
+    pos, idx, nrm, uv = hk.obj_load(path2)
+    # "f 1 4 3 2" -> (1,4,3) (2,1,3); ids in first-use order 1,4,3,2 then 5
+    assert idx.tolist() == [[0, 1, 2], [3, 0, 2], [0, 3, 4]] and nrm is None and uv is None
+    assert pos.tolist()[1] == [-1.0, 0.0, 1.0] and pos.tolist()[4] == [0.0, 1.0, 0.0]
+
+
+@pytest.mark.parametrize("text,needle", [("v 0 0 0\nf 1 2 3\n", "out of range"), ("v 0 0 0\nf 1 a 1\n", "Invalid vertex"),
+                                         ("v 0 0 0\nf 1/1/1/1 1 1\n", "Invalid vertex")])
+def test_obj_reader_errors(L, tmp_path, text, needle):
+    path = str(tmp_path / "bad.obj")
+    open(path, "w").write(text)
+    with pytest.raises(hk.HikariError, match=needle):
+        hk.obj_load(path)
