@@ -148,6 +148,7 @@ def lib():
         "hk_job_poll": ([P, U64, C.POINTER(JobStatus)], C.c_int),
         "hk_job_wait": ([P, U64, C.c_double, C.POINTER(JobStatus)], C.c_int),
         "hk_job_cancel": ([P, U64], C.c_int),
+        "hk_job_preview": ([P, U64, P, C.c_double, C.POINTER(C.c_double)], C.c_int),
         "hk_server_get_stats": ([P, C.POINTER(ServerStats)], C.c_int),
         "hk_trace": ([P, U64, P, P, P, P, P, C.c_int, P, P], C.c_int),
         "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P], C.c_int),

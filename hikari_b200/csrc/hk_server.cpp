@@ -60,6 +60,11 @@ struct Job {
     uint64_t bytes = 0;
     double t_submit = 0, t_admit = 0, t_done = 0;
     cudaEvent_t ev = nullptr;
+    // progressive preview (under the server mutex): a request names the host
+    // buffer; the server thread resolves the film between iterations
+    float *preview_dst = nullptr;
+    int preview_state = 0;       // 0 none, 1 requested, 2 written
+    double preview_fraction = 0.0;
 };
 
 struct SceneEntry {
@@ -129,7 +134,39 @@ struct hk_server {
     bool poll(const std::vector<SceneEntry *> &sc);
     void end_job(SceneEntry &e, Job *j, int state);
     void fail_all(const std::string &msg);
+    void serve_previews(SceneEntry &e);
 };
+
+// Progressive preview (the headless stand-in for the reference's preview
+// window, src/core/Screen.cpp): between iterations, when the scene's pool is
+// idle, resolve each requested job's film as accumulated so far
+// (ImageBlock::ToBitmap, src/core/Block.cpp:61) and copy it to the caller's
+// buffer.
+void hk_server::serve_previews(SceneEntry &e) {
+    std::vector<Job *> want;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (Job *j : e.jobs)
+            if (j->phase == 1 && j->preview_state == 1) want.push_back(j);
+    }
+    if (want.empty()) return;
+    cudaStream_t st = e.eng->stream();
+    const unsigned long long *fin = e.eng->finished();
+    for (Job *j : want) {
+        HK_CUDA(hk::launch_resolve((const float *)j->film, (float *)j->rgb, (int)j->size.width, (int)j->size.height,
+                                   e.view.dev->border, st));
+        HK_CUDA(cudaMemcpyAsync(j->preview_dst, j->rgb, j->size.rgb_bytes, cudaMemcpyDeviceToHost, st));
+    }
+    HK_CUDA(cudaStreamSynchronize(st));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (Job *j : want) {
+            j->preview_fraction = j->work ? (double)fin[j->slot] / (double)j->work : 1.0;
+            j->preview_state = 2;
+        }
+    }
+    cv_done.notify_all();
+}
 
 void hk_server::end_job(SceneEntry &e, Job *j, int state) {
     if (e.eng) {
@@ -288,6 +325,7 @@ bool hk_server::poll(const std::vector<SceneEntry *> &sc) {
     bool progress = false;
     for (SceneEntry *ep : sc) {
         SceneEntry &e = *ep;
+        if (!e.inflight && e.eng) serve_previews(e);
         if (e.inflight) {
             cudaError_t q = cudaEventQuery(e.eng->done_event());
             if (q == cudaErrorNotReady) continue;
@@ -338,6 +376,7 @@ bool hk_server::poll(const std::vector<SceneEntry *> &sc) {
                     j->phase = 2;
                 }
             }
+            serve_previews(e);   // the pool is idle until the next launch
         }
         std::vector<Job *> snapshot = e.jobs;
         for (Job *j : snapshot) {
@@ -570,6 +609,44 @@ int hk_job_cancel(hk_server *s, uint64_t id) {
             find_job(s, id)->cancel = true;
         }
         s->cv_work.notify_all();
+        return HK_OK;
+    });
+}
+
+int hk_job_preview(hk_server *s, uint64_t id, float *rgb, double timeout_s, double *fraction) {
+    return guarded([&] {
+        if (!s || !rgb) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        std::unique_lock<std::mutex> lk(s->mu);
+        Job *j = find_job(s, id);
+        const size_t bytes = (size_t)j->size.width * j->size.height * 12;
+        if (j->state == HK_JOB_QUEUED || j->state == HK_JOB_CANCELLED || j->state == HK_JOB_FAILED) {
+            std::memset(rgb, 0, bytes);
+            if (fraction) *fraction = 0.0;
+            return HK_OK;
+        }
+        if (j->state == HK_JOB_DONE) {
+            if (j->out) std::memcpy(rgb, j->out, bytes);
+            if (fraction) *fraction = 1.0;
+            return HK_OK;
+        }
+        j->preview_dst = rgb;
+        j->preview_state = 1;
+        s->cv_work.notify_all();
+        // the job may also end meanwhile: then its final image is the preview
+        auto ready = [&] { return j->preview_state == 2 || j->state >= HK_JOB_DONE; };
+        bool ok = timeout_s < 0 ? (s->cv_done.wait(lk, ready), true)
+                                : s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready);
+        const bool written = j->preview_state == 2;
+        j->preview_state = 0;
+        j->preview_dst = nullptr;
+        if (!ok) throw HkError{HK_ERR_TIMEOUT, "preview not ready within the timeout"};
+        if (!written) {
+            if (j->state == HK_JOB_DONE && j->out) std::memcpy(rgb, j->out, bytes);
+            else std::memset(rgb, 0, bytes);
+            if (fraction) *fraction = j->state == HK_JOB_DONE ? 1.0 : 0.0;
+            return HK_OK;
+        }
+        if (fraction) *fraction = j->preview_fraction;
         return HK_OK;
     });
 }

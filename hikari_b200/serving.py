@@ -102,6 +102,15 @@ class Server:
     def cancel(self, job_id: int) -> None:
         check(lib().hk_job_cancel(self.h, job_id))
 
+    def preview(self, job_id: int, timeout_s: float = 10.0):
+        """Progressive preview: (the image accumulated so far, H x W x 3, and
+        the fraction of the job's paths finished)."""
+        st = self.poll(job_id)
+        img = np.empty((st["height"], st["width"], 3), np.float32)
+        frac = C.c_double()
+        check(lib().hk_job_preview(self.h, job_id, img.ctypes.data, timeout_s, C.byref(frac)))
+        return img, frac.value
+
     def stats(self) -> dict:
         s = ServerStats()
         check(lib().hk_server_get_stats(self.h, C.byref(s)))

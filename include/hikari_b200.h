@@ -312,6 +312,13 @@ int hk_job_wait(hk_server *srv, uint64_t job_id, double timeout_s, hk_job_status
 /* A queued job is dropped; a running job stops dispatching and ends when its
  * paths in flight are done (its image is not written). */
 int hk_job_cancel(hk_server *srv, uint64_t job_id);
+/* Progressive preview (the headless replacement of the reference's preview
+ * window): the job's film accumulated so far, resolved into rgb_host
+ * (width*height*3 floats, row-major), and the fraction of its paths finished.
+ * A queued, cancelled or failed job gives zeros, a finished job its final image.
+ * Waits at most timeout_s (< 0: no limit) for the server to reach a point
+ * between iterations. */
+int hk_job_preview(hk_server *srv, uint64_t job_id, float *rgb_host, double timeout_s, double *fraction);
 int hk_server_get_stats(hk_server *srv, hk_server_stats *stats);
 
 /* Host-only check of the tree builder (no counterpart in the reference; used

@@ -164,3 +164,38 @@ def test_poisson_driver_reports_percentiles(resident):
         print(summ)
         assert summ["jobs"] == 24 and summ["p50_s"] <= summ["p95_s"] <= summ["p99_s"]
         assert summ["mpaths_per_s"] > 0 and np.all(res.latencies > 0)
+
+
+def test_progressive_preview(resident):
+    """The preview of a running job is its film so far: finite, its finished
+    fraction grows, it converges to the final image, and a finished job's
+    preview is the final image."""
+    sds, gss = resident
+    with serving.Server(capacity=1 << 14, iterations_per_poll=2) as srv:
+        srv.add_scene(gss[0])
+        jid, out = srv.submit(0, 2048, sds[0].depth, 21, 96, 96)
+        fracs, imgs = [], []
+        t_end = time.time() + 60
+        while time.time() < t_end:
+            img, frac = srv.preview(jid)
+            assert np.isfinite(img).all() and (img >= 0).all()
+            fracs.append(frac)
+            imgs.append(img)
+            if frac >= 1.0 or srv.poll(jid)["state"] == serving.DONE:
+                break
+            time.sleep(0.02)
+        st = srv.wait(jid, timeout_s=120)
+        assert st["state"] == serving.DONE
+        final, ff = srv.preview(jid)
+        assert ff == 1.0 and np.array_equal(final, out)
+        print("preview fractions", [round(f, 3) for f in fracs[:10]], "... of", len(fracs))
+        assert all(b >= a for a, b in zip(fracs, fracs[1:]))
+        mid = [i for i, f in enumerate(fracs) if 0.05 < f < 0.95]
+        assert mid, "no preview taken mid-render"
+        m = imgs[mid[len(mid) // 2]]
+        assert abs(m.mean() / out.mean() - 1) < 0.1   # a partial image is already close to the final one
+        victim, _ = srv.submit(0, 4096, sds[0].depth, 22, 96, 96)
+        srv.cancel(victim)
+        srv.wait(victim, timeout_s=120)
+        z, fz = srv.preview(victim)
+        assert fz == 0.0 and not z.any()
