@@ -331,6 +331,28 @@ class Scene:
     def resolve(self, film, rgb, stream=None) -> None:
         check(lib().hk_film_resolve(self.h, _p(film), _p(rgb), _stream(stream)))
 
+    def render_progressive(self, passes: int, spp_per_pass: int, depth: int, seed: int = 0, exr_path=None,
+                           capacity: int = 0):
+        """Progressive rendering into one film (the headless replacement of
+        the reference's preview window): pass k renders samples
+        [k * spp_per_pass, (k + 1) * spp_per_pass) of every pixel, so after n
+        passes the film equals an n * spp_per_pass render of the same seed up
+        to float addition order.  Yields (pass, H x W x 3 image) after each
+        pass; with exr_path the current image is also written there."""
+        import torch
+
+        cam = self.desc.camera
+        film = torch.zeros(self.film_shape(), dtype=torch.float32, device="cuda")
+        rgb = torch.empty((cam.height, cam.width, 3), dtype=torch.float32, device="cuda")
+        for k in range(passes):
+            self.render_batch([film], spp=spp_per_pass, depth=depth, seeds=[seed], image_indices=[0],
+                              sample_offset=k * spp_per_pass, capacity=capacity)
+            self.resolve(film, rgb)
+            img = rgb.cpu().numpy()
+            if exr_path is not None:
+                exr_write(exr_path, img)
+            yield k, img
+
     def render_image(self, spp: int, depth: int, seed: int = 0, rr_start: int = 0, out: Optional[np.ndarray] = None,
                      camera=None, image_index: int = 0, stream=None):
         """End-to-end: render, resolve and return the H x W x 3 float32 image on the host."""

@@ -130,3 +130,23 @@ def test_equal_rmse_wavefront_and_megakernel(accel):
     print(f"accel {accel}: MSE at 64 spp megakernel {m64:.3e} wavefront {w64:.3e}; wavefront 256 spp {w256:.3e}")
     assert 0.75 < w64 / m64 < 1.33           # equal RMSE at equal spp (16 images each; fireflies add spread)
     assert 2.8 < w64 / w256 < 5.5            # MSE ~ 1/spp (4x spp -> 1/4 MSE)
+
+
+def test_progressive_passes_equal_one_render(tmp_path):
+    """Passes over consecutive sample ranges accumulate to the single render of
+    all samples (each sample's stream depends only on seed, sample and pixel);
+    the preview written after each pass reads back as that pass's image."""
+    sd = scenes.cornell_box(width=48, height=40)
+    gs = hk.Scene.from_desc(sd)
+    path = str(tmp_path / "progress.exr")
+    imgs = [img for _, img in gs.render_progressive(4, 16, sd.depth, seed=5, exr_path=path, capacity=1 << 14)]
+    assert np.array_equal(hk.exr_read(path), imgs[-1])
+    film = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
+    gs.render_batch([film], spp=64, depth=sd.depth, seeds=[5], image_indices=[0], capacity=1 << 14)
+    one = _resolve(gs, film)
+    d = np.abs(imgs[-1].astype(np.float64) - one)
+    print("progressive vs one render: max abs", d.max(), "mean", one.mean())
+    assert np.all(d <= 2e-4 * np.abs(one) + 1e-5)
+    # earlier passes are noisier estimates of the same image
+    errs = [np.mean((i - one) ** 2) for i in imgs]
+    assert errs[0] > errs[-1]
