@@ -116,6 +116,7 @@ def lib():
         "hk_scene_add_mesh": ([P, P, C.c_uint32, P, C.c_uint32, P, I32, P, C.POINTER(I32)], C.c_int),
         "hk_scene_set_envmap": ([P, P, C.c_uint32, C.c_uint32, P, F], C.c_int),
         "hk_scene_set_constant_light": ([P, P], C.c_int),
+        "hk_scene_set_mesh_uv": ([P, I32, P], C.c_int),
         "hk_obj_load": ([C.c_char_p, P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P, P, P, P, C.POINTER(I32)],
                         C.c_int),
         "hk_scene_add_point_light": ([P, P, P], C.c_int),
@@ -266,8 +267,12 @@ class Scene:
                     idx = np.ascontiguousarray(m.indices, dtype=np.uint32)
                     nrm = _f32(m.normals) if m.normals is not None else None
                     rad = _f32(m.radiance) if m.radiance is not None else None
+                    mid = C.c_int32()
                     check(L.hk_scene_add_mesh(h, _p(pos), pos.shape[0], _p(idx), idx.shape[0], _p(nrm), mesh_bsdf[i],
-                                              _p(rad), None))
+                                              _p(rad), C.byref(mid)))
+                    if getattr(m, "uv", None) is not None:
+                        uv = _f32(m.uv)
+                        check(L.hk_scene_set_mesh_uv(h, mid.value, _p(uv)))
             cam = desc.camera
             tw = _f32(cam.to_world)
             check(L.hk_scene_set_camera(h, cam.width, cam.height, tw.ctypes.data, cam.fov, cam.near_clip, cam.far_clip))

@@ -44,7 +44,7 @@ struct alignas(16) DevMesh {
     int32_t bsdf;          // DevBsdf index
     int32_t emitter;       // emitter index or -1
     int32_t has_normals;   // vertex normals present -> interpolated shading frame
-    int32_t pad;
+    int32_t has_uv;        // texture coordinates present (with normals: the frame follows dP/du)
     float radiance[3];     // area emitter radiance
     float pad1;
 };
@@ -78,6 +78,7 @@ struct DevScene {
     const float4 *nodes;          // 4 float4 per BVH2 node
     const uint4 *wnodes;          // 5 uint4 per compressed 8-wide node (hk_bvh.h)
     const float4 *tri_normals;    // 3 float4 per ORIGINAL triangle (only if any mesh has normals)
+    const float2 *tri_uv;         // 3 float2 per ORIGINAL triangle (only if any mesh has texture coordinates)
     uint32_t ntris, nnodes, nwnodes;
     int32_t accel;                // kAccelBvh2 or kAccelBvh8: the tree the kernels traverse
     int32_t postpone;             // 8-wide traversal may postpone triangle tests (stack bound allows it)

@@ -190,7 +190,7 @@ struct RftTable {
 };
 
 struct MeshIn {
-    std::vector<float> pos, nrm;
+    std::vector<float> pos, nrm, uv;
     std::vector<uint32_t> idx;
     int32_t bsdf;
     bool emitter;
@@ -225,7 +225,7 @@ struct hk_scene {
     bool built = false;
     hk::DevScene dev{};
     int32_t accel = HK_ACCEL_BVH8;
-    DevBuf b_tris, b_nodes, b_wnodes, b_tri_normals, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
+    DevBuf b_tris, b_nodes, b_wnodes, b_tri_normals, b_tri_uv, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
         b_light_cdf, b_delta, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
     DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
     std::vector<std::unique_ptr<DevBuf>> batch_films;   // films of hk_render_batch_host
@@ -405,8 +405,14 @@ void build_scene(hk_scene *s) {
     P.reserve(ntris * 9);
     tmesh.reserve(ntris);
     std::vector<float> tri_normals;   // 12 floats per triangle (3 float4) if any normals
-    for (auto &m : s->meshes) any_normals |= !m.nrm.empty();
+    std::vector<float> tri_uv;        // 6 floats per triangle (3 float2) if any texture coordinates
+    bool any_uv = false;
+    for (auto &m : s->meshes) {
+        any_normals |= !m.nrm.empty();
+        any_uv |= !m.uv.empty();
+    }
     if (any_normals) tri_normals.resize(ntris * 12, 0.0f);
+    if (any_uv) tri_uv.resize(ntris * 6, 0.0f);
     float bb[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
     std::vector<int> mesh_emitter(s->meshes.size(), -1);
     for (size_t e = 0; e < s->emitter_mesh.size(); ++e)
@@ -420,6 +426,7 @@ void build_scene(hk_scene *s) {
         d.bsdf = m.bsdf;
         d.emitter = mesh_emitter[mi];
         d.has_normals = !m.nrm.empty();
+        d.has_uv = !m.uv.empty();
         for (int c = 0; c < 3; c++) d.radiance[c] = m.radiance[c];
         dm.push_back(d);
         size_t nv = m.pos.size() / 3;
@@ -434,6 +441,8 @@ void build_scene(hk_scene *s) {
                 for (int c = 0; c < 3; c++) P.push_back(m.pos[3 * vi + c]);
                 if (any_normals && !m.nrm.empty())
                     for (int c = 0; c < 3; c++) tri_normals[t * 12 + 4 * k + c] = m.nrm[3 * vi + c];
+                if (any_uv && !m.uv.empty())
+                    for (int c = 0; c < 2; c++) tri_uv[t * 6 + 2 * k + c] = m.uv[2 * vi + c];
             }
             tmesh.push_back((int32_t)mi);
         }
@@ -443,6 +452,8 @@ void build_scene(hk_scene *s) {
     D.nmeshes = (int)dm.size();
     if (any_normals) { s->b_tri_normals.upload(tri_normals); track(s->b_tri_normals); }
     D.tri_normals = s->b_tri_normals.as<float4>();
+    if (any_uv) { s->b_tri_uv.upload(tri_uv); track(s->b_tri_uv); }
+    D.tri_uv = s->b_tri_uv.as<float2>();
 
     // BVH: one binned-SAH build, packed as the binary tree and collapsed into
     // the compressed 8-wide tree over one triangle order
@@ -789,6 +800,15 @@ int hk_scene_add_mesh(hk_scene *s, const float *pos, uint32_t nv, const uint32_t
         s->meshes.push_back(std::move(m));
         if (rad) s->emitter_mesh.push_back((int)s->meshes.size() - 1);
         if (out_id) *out_id = (int32_t)s->meshes.size() - 1;
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_set_mesh_uv(hk_scene *s, int32_t mesh, const float *uv) {
+    return guarded([&] {
+        if (!s || !uv || mesh < 0 || mesh >= (int)s->meshes.size()) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        MeshIn &m = s->meshes[mesh];
+        m.uv.assign(uv, uv + m.pos.size() / 3 * 2);
         s->built = false;
         return HK_OK;
     });

@@ -13,11 +13,29 @@ struct Isect {
     V3 p;
     Frame sh;
     int mesh;
+    float u, v;   // texture coordinates (0 without them)
 };
 
-// Triangle::PostIntersect (src/core/Mesh.cpp:67): position from barycentrics,
-// geometric frame from the face normal, shading frame from interpolated
-// vertex normals when the mesh has them.
+// normalized() of an expression over MatrixXf columns (dynamic size): Eigen
+// reduces the squared norm left to right, ((x*x + y*y) + z*z), where a
+// fixed-size vector reduces x*x + (y*y + z*z)
+__device__ __forceinline__ V3 normalize_dyn(V3 a) {
+    float z = (a.x * a.x + a.y * a.y) + a.z * a.z;
+    return z > 0.0f ? a / sqrtf(z) : a;
+}
+// Frame(N, dPdU) (src/core/Frame.cpp:7): tangent by Gram-Schmidt against N
+__device__ __forceinline__ Frame frame_from_n_dpdu(V3 n, V3 dpdu) {
+    Frame f;
+    f.n = n;
+    f.s = normalize(dpdu - n * dot(n, dpdu));
+    f.t = cross(n, f.s);
+    return f;
+}
+
+// Triangle::PostIntersect (src/core/Mesh.cpp:67-172): position and texture
+// coordinates from barycentrics; the shading frame from the face normal, from
+// interpolated vertex normals, or -- with normals and texture coordinates --
+// from the interpolated normal and dP/du.
 __device__ __forceinline__ void post_intersect(const DevScene &S, const Hit &h, Isect &it) {
     const float4 *tp = S.tris + 3 * h.tri;
     float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
@@ -25,11 +43,38 @@ __device__ __forceinline__ void post_intersect(const DevScene &S, const Hit &h, 
     float b0 = 1 - (h.u + h.v), b1 = h.u, b2 = h.v;
     it.p = (p0 * b0 + p1 * b1) + p2 * b2;
     it.mesh = __float_as_int(q1.w);
+    it.u = it.v = 0.0f;
     const DevMesh &m = S.meshes[it.mesh];
+    const uint32_t orig = (uint32_t)__float_as_int(q0.w);
+    float2 t0, t1, t2;
+    if (m.has_uv) {
+        t0 = __ldg(S.tri_uv + 3 * orig);
+        t1 = __ldg(S.tri_uv + 3 * orig + 1);
+        t2 = __ldg(S.tri_uv + 3 * orig + 2);
+        it.u = (b0 * t0.x + b1 * t1.x) + b2 * t2.x;
+        it.v = (b0 * t0.y + b1 * t1.y) + b2 * t2.y;
+    }
     if (m.has_normals) {
-        const float4 *np = S.tri_normals + 3 * (uint32_t)__float_as_int(q0.w);
+        const float4 *np = S.tri_normals + 3 * orig;
         V3 n0 = xyz(__ldg(np)), n1 = xyz(__ldg(np + 1)), n2 = xyz(__ldg(np + 2));
-        it.sh = frame_from_n(normalize((n0 * b0 + n1 * b1) + n2 * b2));
+        if (m.has_uv) {
+            V3 dp1 = p1 - p0, dp2 = p2 - p0;
+            float du1 = t1.x - t0.x, dv1 = t1.y - t0.y, du2 = t2.x - t0.x, dv2 = t2.y - t0.y;
+            if (norm(cross(dp1, dp2)) == 0.0f) {
+                it.sh = frame_from_n(normalize(cross(dp1, dp2)));   // the geometric frame
+                return;
+            }
+            float det = du1 * dv2 - dv1 * du2;
+            if (det != 0.0f) {
+                float inv = 1.0f / det;
+                V3 dpdu = (dp1 * dv2 - dp2 * dv1) * inv;
+                V3 ns = (n0 * b0 + n1 * b1) + n2 * b2;
+                ns = ns * (1.0f / norm(ns));
+                it.sh = frame_from_n_dpdu(ns, dpdu);
+                return;
+            }
+        }
+        it.sh = frame_from_n(normalize_dyn((n0 * b0 + n1 * b1) + n2 * b2));
     } else {
         it.sh = frame_from_n(normalize(cross(p1 - p0, p2 - p0)));
     }

@@ -821,7 +821,7 @@ HK_REGISTER_CLASS(DirectionalLight, "directional")
 // WavefrontObjMesh (src/mesh/WavefrontObjMesh.cpp:10-152)
 class Mesh : public Object {
 public:
-    std::vector<float> pos, nrm;
+    std::vector<float> pos, nrm, uv;
     std::vector<uint32_t> idx;
     std::unique_ptr<BSDFPlugin> bsdf;
     std::unique_ptr<AreaLight> emitter;
@@ -834,6 +834,7 @@ public:
             ObjMesh m = load_obj(fn, M.data(), Minv.data());
             pos.swap(m.pos);
             nrm.swap(m.nrm);
+            uv.swap(m.uv);
             idx.swap(m.idx);
         } catch (const std::runtime_error &e) {
             throw HikariException(e.what());
@@ -1098,9 +1099,12 @@ int upload_scene(const Scene &sc, const std::string &data_dir, hk_scene *h) {
         add_pending(false);
         int32_t bid = add_bsdf(*m->bsdf);
         const float *rad = m->emitter ? m->emitter->radiance.data() : nullptr;
+        int32_t mid = -1;
         if ((rc = hk_scene_add_mesh(h, m->pos.data(), (uint32_t)(m->pos.size() / 3), m->idx.data(),
                                     (uint32_t)(m->idx.size() / 3), m->nrm.empty() ? nullptr : m->nrm.data(), bid, rad,
-                                    nullptr)) != HK_OK)
+                                    &mid)) != HK_OK)
+            throw HikariException(hk_last_error());
+        if (!m->uv.empty() && (rc = hk_scene_set_mesh_uv(h, mid, m->uv.data())) != HK_OK)
             throw HikariException(hk_last_error());
         if (rad) emitted++;
     }

@@ -88,6 +88,7 @@ class MeshDesc:
     normals: Optional[np.ndarray] = None  # (nv, 3) float32
     radiance: Optional[List[float]] = None  # area emitter
     bbox: Optional[np.ndarray] = None  # (2,3): includes unreferenced vertices
+    uv: Optional[np.ndarray] = None  # (nv, 2) float32 texture coordinates (OBJ "vt")
 
 
 @dataclass
@@ -288,9 +289,13 @@ def load_obj(path: str, to_world: Optional[np.ndarray] = None):
     if N:
         Narr = np.asarray(N, dtype=np.float32)
         normals = np.array([Narr[k[2] - 1] for k in verts], dtype=np.float32).reshape(-1, 3)
+    uvs = None
+    if UV:
+        UVarr = np.asarray(UV, dtype=np.float32)
+        uvs = np.array([UVarr[k[1] - 1] for k in verts], dtype=np.float32).reshape(-1, 2)
     indices = np.asarray(F, dtype=np.uint32).reshape(-1, 3)
     bbox = np.stack([Parr.min(0), Parr.max(0)]) if len(Parr) else None
-    return positions, indices, normals, bbox
+    return positions, indices, normals, bbox, uvs
 
 
 # ----------------------------------------------------------------------- XML
@@ -455,7 +460,7 @@ def parse_scene_node(node: ET.Element, base_dir: str, env_loader=None) -> SceneD
         elif ch.tag == "mesh":
             mp = _props(ch)
             fn = os.path.join(base_dir, mp["filename"])
-            pos, idx, nrm, bbox = load_obj(fn, mp.get("toWorld"))
+            pos, idx, nrm, bbox, uv = load_obj(fn, mp.get("toWorld"))
             bs = [c for c in ch if c.tag == "bsdf"]
             bsdf = _bsdf_from_xml(bs[0]) if bs else BSDFDesc()
             em = [c for c in ch if c.tag == "emitter"]
@@ -465,7 +470,7 @@ def parse_scene_node(node: ET.Element, base_dir: str, env_loader=None) -> SceneD
                     raise SceneError("only area emitters attach to meshes")
                 rad = _props(em[0])["radiance"]
                 n_emit += 1
-            sd.meshes.append(MeshDesc(pos, idx, bsdf, nrm, rad, bbox))
+            sd.meshes.append(MeshDesc(pos, idx, bsdf, nrm, rad, bbox, uv))
         elif ch.tag == "emitter":
             et = ch.attrib["type"]
             ep = _props(ch)

@@ -158,12 +158,33 @@ def cornell_smooth(seed: int = 0, width: int = 256, height: int = 256, spp: int 
     return sd
 
 
-def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 12, seed: int = 0) -> SceneDesc:
+def vertex_normals(P: np.ndarray, F: np.ndarray) -> np.ndarray:
+    """Area-weighted vertex normals of a triangle mesh (unit length, float32)."""
+    n = np.cross(P[F[:, 1]] - P[F[:, 0]], P[F[:, 2]] - P[F[:, 0]]).astype(np.float64)
+    acc = np.zeros((len(P), 3))
+    for k in range(3):
+        np.add.at(acc, F[:, k], n)
+    return (acc / np.linalg.norm(acc, axis=1, keepdims=True)).astype(np.float32)
+
+
+def spherical_uv(P: np.ndarray, center) -> np.ndarray:
+    """Latitude-longitude texture coordinates of points about a center."""
+    d = P - np.asarray(center, np.float32)
+    d = d / np.linalg.norm(d, axis=1, keepdims=True)
+    u = np.arctan2(d[:, 2], d[:, 0]) / (2 * np.pi) + 0.5
+    v = np.arccos(np.clip(d[:, 1], -1, 1)) / np.pi
+    return np.stack([u, v], 1).astype(np.float32)
+
+
+def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 12, seed: int = 0,
+                 shading_normals: bool = False) -> SceneDesc:
     """A ground quad and five displaced icospheres (diffuse, roughDiffuse,
     smooth plastic, rough conductor, smooth dielectric) lit, in emitter order,
     by a point light, an emissive quad, a constant environment and a
     directional light -- the emitter kinds interleaved as an XML scene lists
-    them."""
+    them.  With shading_normals the spheres carry vertex normals and
+    latitude-longitude texture coordinates (the shading frame then follows
+    dP/du) and the conductor is anisotropic (alpha 0.05 x 0.4)."""
     sd = SceneDesc()
     gp, gi = quad((-6, 0, 6), (6, 0, 6), (6, 0, -6), (-6, 0, -6))
     sd.meshes.append(MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5])))
@@ -173,9 +194,17 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
             BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=1.0, ext_ior=1.0,
                      eta=AU_ETA, k=AU_K),
             BSDFDesc(type=BSDF_DIELECTRIC, int_ior=1.5046, ext_ior=AIR_IOR)]
+    if shading_normals:
+        mats[3] = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, anisotropic=True, alpha_u=0.05, alpha_v=0.4,
+                           int_ior=1.0, ext_ior=1.0, eta=AU_ETA, k=AU_K)
     for k, b in enumerate(mats):
-        P, F = displaced_icosphere(2, 0.8, (-3.2 + 1.6 * k, 0.85, 0.3 * ((k % 2) * 2 - 1)), 0.05, seed + k)
-        sd.meshes.append(MeshDesc(P.astype(np.float32), F.astype(np.uint32), b))
+        c = (-3.2 + 1.6 * k, 0.85, 0.3 * ((k % 2) * 2 - 1))
+        P, F = displaced_icosphere(2, 0.8, c, 0.05, seed + k)
+        P, F = P.astype(np.float32), F.astype(np.uint32)
+        if shading_normals:
+            sd.meshes.append(MeshDesc(P, F, b, normals=vertex_normals(P, F), uv=spherical_uv(P, c)))
+        else:
+            sd.meshes.append(MeshDesc(P, F, b))
     lp, li = quad((-1, 4, -1), (1, 4, -1), (1, 4, 1), (-1, 4, 1))   # faces down
     sd.meshes.append(MeshDesc(lp, li, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.0, 0.0, 0.0]), radiance=[3.0, 3.0, 3.0]))
     sd.lights.append(LightDesc("point", [40.0, 32.0, 24.0], [2.5, 3.0, 2.0], emitter_index=0))

@@ -101,6 +101,10 @@ int hk_scene_add_bsdf(hk_scene *s, const hk_bsdf_desc *desc, int32_t *out_id);
  * for an attached area emitter (src/emitter/AreaLight.cpp:8) or NULL. */
 int hk_scene_add_mesh(hk_scene *s, const float *positions, uint32_t nv, const uint32_t *indices, uint32_t nt,
                       const float *normals, int32_t bsdf, const float *radiance, int32_t *out_id);
+/* Texture coordinates of a mesh (the OBJ "vt" of each vertex): 2*nv floats.
+ * With vertex normals they orient the shading frame along dP/du
+ * (Triangle::PostIntersect, src/core/Mesh.cpp:107-158). */
+int hk_scene_set_mesh_uv(hk_scene *s, int32_t mesh, const float *uv);
 /* Environment emitter (EnvironmentLight ctor, src/emitter/EnvironmentLight.cpp:8):
  * rgb is H*W*3 floats, row 0 at theta = 0; to_world row-major 4x4. */
 int hk_scene_set_envmap(hk_scene *s, const float *rgb, uint32_t width, uint32_t height, const float *to_world16,

@@ -404,6 +404,7 @@ typedef struct {
     uint32_t v0, nv, t0, nt;
     int32_t bsdf, emitter;
     int has_n;
+    int has_uv;        /* texture coordinates present (ho_scene_set_mesh_uv) */
     float *cdf;        /* nt+1 area CDF (DiscretePDF1D) */
     float *func;       /* nt areas */
     float func_int;    /* m_FuncIntegral */
@@ -418,7 +419,7 @@ typedef struct { float bmin[3], bmax[3]; int32_t left_or_first, count, axis, rig
 struct ho_scene {
     int nb, cap_b; bsdf_t *bsdfs;
     int nm, cap_m; mesh_t *meshes;
-    float *P; float *N; uint32_t nv, cap_v;          /* global vertices (world space) */
+    float *P; float *N; float *UV; uint32_t nv, cap_v;   /* global vertices (world space); UV 2 per vertex */
     uint32_t *F; int32_t *tri_mesh; uint32_t nt, cap_t;
     rft_table rft[2]; int has_rft[2];
     /* emitters in Scene::AddChild order: meshes (XML order), env appended */
@@ -450,7 +451,7 @@ ho_scene *ho_scene_create(void) {
 void ho_scene_destroy(ho_scene *s) {
     if (!s) return;
     for (int i = 0; i < s->nm; i++) { free(s->meshes[i].cdf); free(s->meshes[i].func); }
-    free(s->meshes); free(s->bsdfs); free(s->P); free(s->N); free(s->F); free(s->tri_mesh);
+    free(s->meshes); free(s->bsdfs); free(s->P); free(s->N); free(s->UV); free(s->F); free(s->tri_mesh);
     for (int i = 0; i < 2; i++) free(s->rft[i].owned);
     free(s->env);
     if (s->env_rows) { for (uint32_t i = 0; i < s->eh; i++) { free(s->env_rows[i].func); free(s->env_rows[i].cdf); } }
@@ -477,6 +478,7 @@ int ho_scene_add_mesh(ho_scene *s, const float *pos, uint32_t nv, const uint32_t
     if (s->nv + nv > s->cap_v) {
         while (s->nv + nv > s->cap_v) s->cap_v = s->cap_v ? 2 * s->cap_v : 1024;
         s->P = realloc(s->P, 3ull * s->cap_v * 4); s->N = realloc(s->N, 3ull * s->cap_v * 4);
+        s->UV = realloc(s->UV, 2ull * s->cap_v * 4);
     }
     if (s->nt + nt > s->cap_t) {
         while (s->nt + nt > s->cap_t) s->cap_t = s->cap_t ? 2 * s->cap_t : 1024;
@@ -498,8 +500,17 @@ int ho_scene_add_mesh(ho_scene *s, const float *pos, uint32_t nv, const uint32_t
         m->emitter = s->n_emit;
         s->emit_mesh[s->n_emit++] = s->nm;
     }
+    memset(s->UV + 2ull * s->nv, 0, 8ull * nv);
     s->nv += nv; s->nt += nt;
     return s->nm++;
+}
+/* Texture coordinates of a mesh (2 per vertex, the OBJ "vt" of each vertex). */
+int ho_scene_set_mesh_uv(ho_scene *s, int mesh, const float *uv) {
+    if (mesh < 0 || mesh >= s->nm || !uv) return fail("bad mesh id");
+    mesh_t *m = &s->meshes[mesh];
+    memcpy(s->UV + 2ull * m->v0, uv, 8ull * m->nv);
+    m->has_uv = 1;
+    return 0;
 }
 static void mat3_inverse(const float *m, float *o) {
     double a = m[0], b = m[1], c = m[2], d = m[3], e = m[4], f = m[5], g = m[6], h = m[7], i = m[8];
@@ -1612,22 +1623,71 @@ void ho_trace(const ho_scene *s, uint64_t n, const float *rays, float *th, float
     }
 }
 
-/* Triangle::PostIntersect  src/core/Mesh.cpp:67 (no UV partials: meshes here carry no vt) */
-typedef struct { v3 p; frame sh, geo; int mesh; float t; } isect_t;
+/* normalized() of an expression over MatrixXf columns (dynamic size): Eigen
+ * reduces the squared norm left to right, ((x*x + y*y) + z*z), where a
+ * fixed-size Vector3f reduces x*x + (y*y + z*z) */
+static inline v3 normalize_dyn(v3 a) {
+    float z = (a.x * a.x + a.y * a.y) + a.z * a.z;
+    return z > 0.0f ? divs(a, sqrtf(z)) : a;
+}
+/* Frame(N, dPdU)  src/core/Frame.cpp:7: tangent by Gram-Schmidt against N */
+static frame frame_from_n_dpdu(v3 n, v3 dpdu) {
+    frame f; f.n = n;
+    f.s = normalize(sub(dpdu, scl(n, dot(n, dpdu))));
+    f.t = cross(n, f.s);
+    return f;
+}
+/* Triangle::PostIntersect  src/core/Mesh.cpp:67-172 (the UV partials of :137-156
+ * are used only for the shading frame; dNdU / dNdV serve texture filtering) */
+typedef struct { v3 p; frame sh, geo; int mesh; float t; float uv[2]; } isect_t;
 static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
     const uint32_t *f = s->F + 3ull * h->tri;
     v3 p0 = vload(s->P + 3ull * f[0]), p1 = vload(s->P + 3ull * f[1]), p2 = vload(s->P + 3ull * f[2]);
     float b0 = 1 - (h->u + h->v), b1 = h->u, b2 = h->v;
+    const mesh_t *m = &s->meshes[s->tri_mesh[h->tri]];
     it->p = add(add(scl(p0, b0), scl(p1, b1)), scl(p2, b2));
+    it->uv[0] = it->uv[1] = 0.0f;
+    const float *u0 = s->UV + 2ull * f[0], *u1 = s->UV + 2ull * f[1], *u2 = s->UV + 2ull * f[2];
+    if (m->has_uv)
+        for (int c = 0; c < 2; c++) it->uv[c] = (b0 * u0[c] + b1 * u1[c]) + b2 * u2[c];
     it->geo = frame_from_n(normalize(cross(sub(p1, p0), sub(p2, p0))));
     it->mesh = s->tri_mesh[h->tri];
     it->t = h->t;
-    if (s->meshes[it->mesh].has_n) {
+    if (m->has_n && m->has_uv) {
+        v3 dp1 = sub(p1, p0), dp2 = sub(p2, p0);
+        float du1 = u1[0] - u0[0], dv1 = u1[1] - u0[1], du2 = u2[0] - u0[0], dv2 = u2[1] - u0[1];
+        float len = norm(cross(dp1, dp2));
         v3 n0 = vload(s->N + 3ull * f[0]), n1 = vload(s->N + 3ull * f[1]), n2 = vload(s->N + 3ull * f[2]);
-        it->sh = frame_from_n(normalize(add(add(scl(n0, b0), scl(n1, b1)), scl(n2, b2))));
+        if (len == 0.0f) {
+            it->sh = it->geo;
+        } else {
+            float det = du1 * dv2 - dv1 * du2;
+            if (det == 0.0f) {
+                it->sh = frame_from_n(normalize_dyn(add(add(scl(n0, b0), scl(n1, b1)), scl(n2, b2))));
+            } else {
+                float inv = 1.0f / det;
+                v3 dpdu = scl(sub(scl(dp1, dv2), scl(dp2, dv1)), inv);
+                v3 ns = add(add(scl(n0, b0), scl(n1, b1)), scl(n2, b2));
+                float ln = norm(ns);
+                ns = scl(ns, 1.0f / ln);
+                it->sh = frame_from_n_dpdu(ns, dpdu);
+            }
+        }
+    } else if (m->has_n) {
+        v3 n0 = vload(s->N + 3ull * f[0]), n1 = vload(s->N + 3ull * f[1]), n2 = vload(s->N + 3ull * f[2]);
+        it->sh = frame_from_n(normalize_dyn(add(add(scl(n0, b0), scl(n1, b1)), scl(n2, b2))));
     } else {
         it->sh = it->geo;
     }
+}
+/* Triangle::PostIntersect for (triangle, barycentric u, v): out p(3) s(3) t(3) n(3) uv(2) */
+void ho_post_intersect(const ho_scene *s, uint32_t tri, float u, float v, float *out) {
+    hit_t h; memset(&h, 0, sizeof h);
+    h.tri = tri; h.u = u; h.v = v;
+    isect_t it;
+    post_intersect(s, &h, &it);
+    vstore(out, it.p); vstore(out + 3, it.sh.s); vstore(out + 6, it.sh.t); vstore(out + 9, it.sh.n);
+    out[12] = it.uv[0]; out[13] = it.uv[1];
 }
 
 /* ------------------------------------------------------------ emitters */

@@ -82,6 +82,10 @@ int  ho_scene_add_mesh(ho_scene *s, const float *positions, uint32_t nv,
 /* rgb H*W*3 row-major (row 0 = theta 0); to_world row-major 4x4. */
 int  ho_scene_set_envmap(ho_scene *s, const float *rgb, uint32_t w, uint32_t h,
                          const float *to_world16, float scale);
+/* Texture coordinates of a mesh: 2 floats per vertex. */
+int  ho_scene_set_mesh_uv(ho_scene *s, int mesh, const float *uv);
+/* Triangle::PostIntersect of a finalized scene: out p(3) s(3) t(3) n(3) uv(2). */
+void ho_post_intersect(const ho_scene *s, uint32_t tri, float u, float v, float *out);
 /* ConstantLight radiance (one environment emitter per scene); point / directional lights. */
 int  ho_scene_set_constant_light(ho_scene *s, const float *radiance);
 int  ho_scene_add_point_light(ho_scene *s, const float *power, const float *position);

@@ -55,6 +55,8 @@ def lib():
         L.ho_scene_add_mesh.argtypes = [P, P, C.c_uint32, P, C.c_uint32, P, C.c_int32, P]
         L.ho_scene_set_envmap.argtypes = [P, P, C.c_uint32, C.c_uint32, P, C.c_float]
         L.ho_scene_set_constant_light.argtypes = [P, P]
+        L.ho_scene_set_mesh_uv.argtypes = [P, C.c_int, P]
+        L.ho_post_intersect.argtypes = [P, C.c_uint32, C.c_float, C.c_float, P]
         L.ho_scene_add_point_light.argtypes = [P, P, P]
         L.ho_scene_add_directional_light.argtypes = [P, P, P]
         L.ho_scene_set_camera.argtypes = [P, C.c_uint32, C.c_uint32, P, C.c_float, C.c_float, C.c_float]
@@ -148,6 +150,10 @@ class OracleScene:
                                         self.mesh_bsdf[i], _p(rad))
                 if r < 0:
                     raise RuntimeError(L.ho_last_error().decode())
+                if getattr(m, "uv", None) is not None:
+                    uv = _f32(m.uv)
+                    self._keep.append(uv)
+                    L.ho_scene_set_mesh_uv(self.h, r, _p(uv))
         cam = desc.camera
         tw = _f32(cam.to_world)
         L.ho_scene_set_camera(self.h, cam.width, cam.height, _p(tw), cam.fov, cam.near_clip, cam.far_clip)

@@ -10,6 +10,7 @@
 #include <core\Color.hpp>
 #include <core\Vector.hpp>
 #include <core\Emitter.hpp>
+#include <core\Mesh.hpp>
 
 using namespace Hikari;
 
@@ -107,6 +108,48 @@ float hr_bsdf_pdf(void *h, const float *wi, const float *wo, int measure) {
     BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), Vector3f(wo[0], wo[1], wo[2]), EMeasure(measure),
                       ETransportMode::ERadiance, &g_sampler, null_isect());
     return ((BSDF *)h)->Pdf(r);
+}
+
+namespace {
+/* A Mesh whose buffers are filled from arrays (the OBJ reader's result). */
+class ArrayMesh : public Mesh {
+public:
+    ArrayMesh(const float *P, uint32_t nv, const float *N, const float *UV, const uint32_t *F, uint32_t nt) {
+        m_V.resize(3, nv);
+        for (uint32_t i = 0; i < nv; i++) m_V.col(i) = Vector3f(P[3 * i], P[3 * i + 1], P[3 * i + 2]);
+        if (N) {
+            m_N.resize(3, nv);
+            for (uint32_t i = 0; i < nv; i++) m_N.col(i) = Vector3f(N[3 * i], N[3 * i + 1], N[3 * i + 2]);
+        }
+        if (UV) {
+            m_UV.resize(2, nv);
+            for (uint32_t i = 0; i < nv; i++) m_UV.col(i) = Vector2f(UV[2 * i], UV[2 * i + 1]);
+        }
+        m_F.resize(3, nt);
+        for (uint32_t i = 0; i < nt; i++)
+            for (int c = 0; c < 3; c++) m_F(c, i) = F[3 * i + c];
+    }
+    uint32_t *facet(uint32_t i) { return m_F.data() + 3 * i; }
+};
+}
+
+void *hr_mesh_create(const float *P, uint32_t nv, const float *N, const float *UV, const uint32_t *F, uint32_t nt) {
+    return new ArrayMesh(P, nv, N, UV, F, nt);
+}
+
+/* Triangle::PostIntersect at barycentric (u, v) of triangle tri: out p(3) s(3) t(3) n(3) uv(2) */
+void hr_post_intersect(void *h, uint32_t tri, float u, float v, float *out) {
+    ArrayMesh *m = (ArrayMesh *)h;
+    Triangle T(m, m->facet(tri), tri);
+    Intersection I;
+    I.pShape = &T;
+    I.UV = Point2f(u, v);
+    T.PostIntersect(I);
+    const Frame &F = I.ShadingFrame;
+    for (int c = 0; c < 3; c++) {
+        out[c] = I.P[c]; out[3 + c] = F.S[c]; out[6 + c] = F.T[c]; out[9 + c] = F.N[c];
+    }
+    out[12] = I.UV.x(); out[13] = I.UV.y();
 }
 
 /* kind: 0 point (power, position), 1 directional (irradiance, direction), 2 constant (radiance) */

@@ -41,6 +41,7 @@ SCENES = {
     "smooth": lambda: scenes.cornell_smooth(width=32, height=32),
     "heterogeneous": lambda: scenes.heterogeneous(width=32, height=32, n_spheres=12, levels=(3,), level_p=(1.0,), env_res=(256, 128)),
     "lights": lambda: scenes.lights_scene(width=32, height=32),
+    "shading_normals_uv": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True),
 }
 
 

@@ -311,11 +311,12 @@ def test_parallel_obj_reader_matches_reference_rules(L, tmp_path):
         path = str(tmp_path / f"mixed{style}.obj")
         open(path, "w", newline="").write(_mixed_obj(rng, style))
         pos, idx, nrm, uv = hk.obj_load(path, M)
-        p2, i2, n2, bbox = load_obj(path, M)
+        p2, i2, n2, bbox, uv2 = load_obj(path, M)
         assert idx.shape == i2.shape and np.array_equal(idx, i2)
         assert pos.shape == p2.shape and np.allclose(pos, p2, rtol=1e-6, atol=1e-5)
         assert (nrm is None) == (n2 is None) and (nrm is None or np.allclose(nrm, n2, atol=1e-5))
-        assert (uv is not None) == (style in (1, 3))
+        assert (uv is not None) == (style in (1, 3)) == (uv2 is not None)
+        assert uv is None or np.array_equal(uv, uv2)
     # positions-only fast path, with quads
     path2 = str(tmp_path / "plain.obj")
     open(path2, "w").write(QUAD_OBJ + "v 0 1 0\nf 1 2 5\n")

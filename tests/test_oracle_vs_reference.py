@@ -215,3 +215,40 @@ def test_oracle_lights_bit_exact_vs_reference(name):
         for i in range(n):
             np.testing.assert_array_equal(o.env_eval(d[i]), ev[i, :3])
             assert o.emitter_pdf(0, np.zeros(3, np.float32), d[i], np.zeros(3, np.float32)) == ev[i, 3]
+
+
+def test_oracle_post_intersect_bit_exact_vs_reference():
+    """Triangle::PostIntersect (src/core/Mesh.cpp:67-172) on a mesh with vertex
+    normals and texture coordinates: the shading frame follows dP/du, with the
+    degenerate-UV and zero-area fallbacks."""
+    from hikari_b200 import scenes
+    from hikari_b200.scenedesc import MeshDesc
+
+    R = _ref_lib()
+    R.hr_mesh_create.restype = C.c_void_p
+    R.hr_mesh_create.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+    R.hr_post_intersect.argtypes = [C.c_void_p, C.c_uint32, C.c_float, C.c_float, C.c_void_p]
+    rng = np.random.default_rng(17)
+    P, F = scenes.displaced_icosphere(2, 1.0, (0.3, -0.2, 0.1), 0.08, 4)
+    P = P.astype(np.float32)
+    F = F.astype(np.uint32)
+    N = (P + rng.normal(0, 0.05, P.shape)).astype(np.float32)   # unnormalised on purpose
+    UV = rng.random((len(P), 2)).astype(np.float32)
+    UV[F[0]] = UV[F[0][0]]                                # triangle 0: degenerate UVs (det == 0)
+    P[F[1][1]] = P[F[1][0]]                                 # triangle 1: zero area
+    cases = {"normals+uv": (N, UV), "normals": (N, None), "uv": (None, UV), "plain": (None, None)}
+    for name, (n, uv) in cases.items():
+        sd = SceneDesc()
+        sd.meshes.append(MeshDesc(P, F, BSDFDesc(), normals=n, uv=uv))
+        o = O.OracleScene(sd)
+        h = R.hr_mesh_create(O._p(P), len(P), O._p(n), O._p(uv), O._p(F), len(F))
+        tri = np.concatenate([[0, 0, 1, 1], rng.integers(0, len(F), 4000)]).astype(np.uint32)
+        u = rng.random(len(tri)).astype(np.float32)
+        v = (rng.random(len(tri)) * (1 - u)).astype(np.float32)
+        for k in range(len(tri)):
+            a = np.zeros(14, np.float32)
+            b = np.zeros(14, np.float32)
+            O.lib().ho_post_intersect(o.h, int(tri[k]), float(u[k]), float(v[k]), O._p(a))
+            R.hr_post_intersect(h, int(tri[k]), float(u[k]), float(v[k]), O._p(b))
+            assert np.array_equal(a, b) or (np.isnan(a) == np.isnan(b)).all() and np.array_equal(a[~np.isnan(a)], b[~np.isnan(b)]), \
+                f"{name}: triangle {tri[k]} ({u[k]}, {v[k]}): oracle {a} reference {b}"
