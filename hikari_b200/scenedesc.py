@@ -49,6 +49,28 @@ class SceneError(RuntimeError):
     """Raised for malformed scenes (the reference throws HikariException)."""
 
 
+# Procedural textures, matching hk_texture_kind in include/hikari_b200.h
+TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE = 1, 2, 3
+TEX_TYPE_NAMES = {"checkerboard": TEX_CHECKERBOARD, "grid": TEX_GRID, "scale": TEX_SCALE}
+# textured BSDF parameters, in the order of hk_bsdf_desc.tex
+TEX_SLOTS = ("kd", "ks", "ks_refract", "sigma_a", "alpha_u", "alpha_v")
+
+
+@dataclass
+class TextureDesc:
+    """A procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp);
+    defaults are the reference's (include/core/Common.hpp:436-458)."""
+    kind: int
+    count: int = 10                    # checkerboard "blocks", grid "lines"
+    width: float = 0.01                # grid "lineWidth"
+    scale: float = 1.0                 # scale "scale"
+    uv_scale: List[float] = field(default_factory=lambda: [1.0, 1.0])
+    uv_offset: List[float] = field(default_factory=lambda: [0.0, 0.0])
+    a: List[float] = field(default_factory=lambda: [0.4, 0.4, 0.4])   # colorA / lineColor
+    b: List[float] = field(default_factory=lambda: [0.2, 0.2, 0.2])   # colorB / backgroundColor
+    nested: Optional["TextureDesc"] = None                           # scale: the scaled texture
+
+
 @dataclass
 class BSDFDesc:
     """Properties of one BSDF; defaults are the reference's
@@ -72,6 +94,7 @@ class BSDFDesc:
     nested: Optional["BSDFDesc"] = None    # roughCoating's BSDF, twoSided's front BSDF
     nested2: Optional["BSDFDesc"] = None   # twoSided's back BSDF (None: the front one)
     fast_approx: bool = False              # roughDiffuse "fastApprox"
+    textures: Dict[str, "TextureDesc"] = field(default_factory=dict)   # slot (TEX_SLOTS) -> texture
 
     def conductor_eta(self) -> List[float]:
         if self.eta is not None:

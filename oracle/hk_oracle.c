@@ -389,9 +389,10 @@ typedef struct {
     float rft[RFT_MAX_THETA];          /* activated 1D transmittance table */
     int rft_n;
     float fdr_int;                     /* plastic: 1 - IntData.EvalDiffuse(alpha) */
+    const ho_texture_desc *textures;   /* the scene's textures (set when finalized) */
 } bsdf_t;
 
-typedef struct { v3 wi, wo; float eta; int measure; } brec;
+typedef struct { v3 wi, wo; float eta; int measure; float uv[2]; } brec;   /* uv: Record.Isect.UV */
 
 struct ho_scene;
 static v3 bsdf_eval(const struct ho_scene *s, int id, const brec *r);
@@ -418,6 +419,7 @@ typedef struct { float bmin[3], bmax[3]; int32_t left_or_first, count, axis, rig
 
 struct ho_scene {
     int nb, cap_b; bsdf_t *bsdfs;
+    int ntex, cap_tex; ho_texture_desc *tex;
     int nm, cap_m; mesh_t *meshes;
     float *P; float *N; float *UV; uint32_t nv, cap_v;   /* global vertices (world space); UV 2 per vertex */
     uint32_t *F; int32_t *tri_mesh; uint32_t nt, cap_t;
@@ -451,7 +453,7 @@ ho_scene *ho_scene_create(void) {
 void ho_scene_destroy(ho_scene *s) {
     if (!s) return;
     for (int i = 0; i < s->nm; i++) { free(s->meshes[i].cdf); free(s->meshes[i].func); }
-    free(s->meshes); free(s->bsdfs); free(s->P); free(s->N); free(s->UV); free(s->F); free(s->tri_mesh);
+    free(s->meshes); free(s->bsdfs); free(s->tex); free(s->P); free(s->N); free(s->UV); free(s->F); free(s->tri_mesh);
     for (int i = 0; i < 2; i++) free(s->rft[i].owned);
     free(s->env);
     if (s->env_rows) { for (uint32_t i = 0; i < s->eh; i++) { free(s->env_rows[i].func); free(s->env_rows[i].cdf); } }
@@ -465,6 +467,14 @@ int ho_scene_set_rft(ho_scene *s, int dist, const void *bytes, uint64_t n) {
     if (s->rft[dist].theta_n > RFT_MAX_THETA) return fail("rft theta too large");
     s->has_rft[dist] = 1;
     return 0;
+}
+int ho_scene_add_texture(ho_scene *s, const ho_texture_desc *d) {
+    if (d->kind < HO_TEX_CHECKERBOARD || d->kind > HO_TEX_SCALE) return fail("unknown texture kind");
+    if (d->kind == HO_TEX_SCALE && (d->nested < 0 || d->nested >= s->ntex)) return fail("scale texture needs a nested texture");
+    if (d->kind != HO_TEX_SCALE && d->count <= 0) return fail("texture block / line count must be positive");
+    if (s->ntex == s->cap_tex) { s->cap_tex = s->cap_tex ? 2 * s->cap_tex : 8; s->tex = realloc(s->tex, s->cap_tex * sizeof *s->tex); }
+    s->tex[s->ntex] = *d;
+    return s->ntex++;
 }
 int ho_scene_add_bsdf(ho_scene *s, const ho_bsdf_desc *d) {
     if (s->nb == s->cap_b) { s->cap_b = s->cap_b ? 2 * s->cap_b : 8; s->bsdfs = realloc(s->bsdfs, s->cap_b * sizeof(bsdf_t)); }
@@ -640,8 +650,18 @@ static int bsdf_transmits(const ho_scene *s, int id, int depth) {
 }
 
 /* BSDF activation: RoughPlasticBSDF::Activate :261, RoughCoatingBSDF::Activate :315 */
+static v3 tex_average(const ho_texture_desc *T, int id);
+/* Texture::GetAverage of a parameter: the texture's average or the constant */
+static v3 par_average(const ho_scene *s, const ho_bsdf_desc *d, int slot, const float *c) {
+    return d->tex[slot] ? tex_average(s->tex, d->tex[slot] - 1) : vload(c);
+}
 static int activate_bsdf(ho_scene *s, bsdf_t *b) {
     const ho_bsdf_desc *d = &b->d;
+    b->textures = s->tex;
+    for (int k = 0; k < 6; k++)
+        if (d->tex[k] < 0 || d->tex[k] > s->ntex) return fail("invalid texture id");
+    if ((d->type == HO_BSDF_ROUGH_PLASTIC || d->type == HO_BSDF_ROUGH_COATING) && d->tex[4])
+        return fail("textured alpha of roughPlastic / roughCoating is not supported");
     b->eta = d->int_ior / d->ext_ior;
     b->inv_eta = 1.0f / b->eta;
     b->inv_eta2 = b->inv_eta * b->inv_eta;
@@ -661,7 +681,7 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
         rft_set_alpha(t, t2d, d1d, alpha, b->rft, &dsc);
         b->rft_n = T;
         if (d->type == HO_BSDF_ROUGH_PLASTIC) {
-            float ksa = lum(vload(d->ks)), kda = lum(vload(d->kd));
+            float ksa = lum(par_average(s, d, 1, d->ks)), kda = lum(par_average(s, d, 0, d->kd));
             b->spec_w = ksa / (kda + ksa);
             /* m_pIntData: SetEta(1/eta) only; EvalDiffuse(alpha) is the 1D cubic over alpha */
             rft_set_eta(t, b->inv_eta, t2d, d1d);
@@ -670,8 +690,9 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
             b->fdr_int = 1.0f - ed;
         } else {
             float th = d->thickness;
-            float a0 = expf(d->sigma_a[0] * (-2.0f * th)), a1 = expf(d->sigma_a[1] * (-2.0f * th)),
-                  a2 = expf(d->sigma_a[2] * (-2.0f * th));
+            v3 sav = par_average(s, d, 3, d->sigma_a);
+            float a0 = expf(sav.x * (-2.0f * th)), a1 = expf(sav.y * (-2.0f * th)),
+                  a2 = expf(sav.z * (-2.0f * th));
             float avg = (a0 + a1 + a2) / 3.0f;
             b->spec_w = 1.0f / (avg + 1.0f);
             if (d->nested < 0 || d->nested >= s->nb) return fail("roughCoating needs a nested BSDF");
@@ -681,7 +702,7 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
     if (d->type == HO_BSDF_CONDUCTOR)   /* ConductorBSDF ctor :17: m_Eta = Color3f(intIOR / extIOR) */
         for (int c = 0; c < 3; c++) b->eta_c[c] = b->eta;
     if (d->type == HO_BSDF_PLASTIC) {   /* PlasticBSDF ctor :25 and Activate :170 */
-        float ksa = lum(vload(d->ks)), kda = lum(vload(d->kd));
+        float ksa = lum(par_average(s, d, 1, d->ks)), kda = lum(par_average(s, d, 0, d->kd));
         b->spec_w = ksa / (kda + ksa);
         b->fdr_int = approx_fresnel_diffuse(b->inv_eta);
     }
@@ -694,8 +715,9 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
     }
     if (d->type == HO_BSDF_COATING) {   /* CoatingBSDF::Activate :255 */
         float th = d->thickness;
-        float a0 = expf(d->sigma_a[0] * (-2.0f * th)), a1 = expf(d->sigma_a[1] * (-2.0f * th)),
-              a2 = expf(d->sigma_a[2] * (-2.0f * th));
+        v3 sav = par_average(s, d, 3, d->sigma_a);
+            float a0 = expf(sav.x * (-2.0f * th)), a1 = expf(sav.y * (-2.0f * th)),
+              a2 = expf(sav.z * (-2.0f * th));
         b->spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
         if (d->nested < 0 || d->nested >= s->nb) return fail("CoatingBSDF needs a nested BSDF!");
     }
@@ -738,9 +760,48 @@ int ho_scene_num_emitters(const ho_scene *s) { return s->n_emit; }
 int ho_film_border(const ho_scene *s) { return s->border; }
 
 /* ------------------------------------------------------------ BSDF impl */
-static inline float alpha_u_of(const bsdf_t *b) { return clampf(b->d.alpha_u, 5e-4f, 1.0f); }
-static inline float alpha_v_of(const bsdf_t *b) {
-    return b->d.anisotropic ? clampf(b->d.alpha_v, 5e-4f, 1.0f) : alpha_u_of(b);
+/* Texture2D::Eval(Isect) (src/core/Texture.cpp:211) of the procedural textures:
+ * UV scaled and offset, then CheckerboardTexture::Eval (src/texture/
+ * CheckerboardTexture.cpp:24) or GridTexture::Eval (src/texture/GridTexture.cpp:26);
+ * ScaleTexture::Eval (src/texture/ScaleTexture.cpp:17) scales its nested texture. */
+static inline int mod_positive(int a, int b) { int r = a % b; return r < 0 ? r + b : r; }
+static v3 tex_eval(const ho_texture_desc *T, int id, const float *uvi) {
+    const ho_texture_desc *t = &T[id];
+    if (t->kind == HO_TEX_SCALE) return scl(tex_eval(T, t->nested, uvi), t->scale);
+    float u = uvi[0] * t->uv_scale[0] + t->uv_offset[0], v = uvi[1] * t->uv_scale[1] + t->uv_offset[1];
+    if (t->kind == HO_TEX_CHECKERBOARD) {
+        int ex = mod_positive(mod_positive((int)(u * t->count), t->count), 2) == 0;
+        int ey = mod_positive(mod_positive((int)(v * t->count), t->count), 2) == 0;
+        return (ex ^ ey) ? vload(t->a) : vload(t->b);
+    }
+    float su = u * (float)(t->count - 1), sv = v * (float)(t->count - 1);
+    float dx = su - floorf(su), dy = sv - floorf(sv);
+    if (dx > 0.5f) dx -= 1.0f;
+    if (dy > 0.5f) dy -= 1.0f;
+    return (fabsf(dx) < t->width || fabsf(dy) < t->width) ? vload(t->a) : vload(t->b);
+}
+/* Texture::GetAverage of the procedural textures (used when BSDFs activate) */
+static v3 tex_average(const ho_texture_desc *T, int id) {
+    const ho_texture_desc *t = &T[id];
+    if (t->kind == HO_TEX_SCALE) return scl(tex_average(T, t->nested), t->scale);
+    if (t->kind == HO_TEX_CHECKERBOARD) return scl(add(vload(t->a), vload(t->b)), 0.5f);
+    float iw = fmaxf(0.0f, 1.0f - 2.0f * t->width);    /* GridTexture::GetAverage :40 */
+    float ia = iw * iw, la = 1.0f - ia;
+    return add(scl(vload(t->a), la), scl(vload(t->b), ia));
+}
+/* A BSDF parameter at the query's intersection: its texture or its constant.
+ * slot: 0 kd, 1 ks, 2 ksRefract, 3 sigmaA, 4 alpha(U), 5 alphaV */
+static inline v3 par_rgb(const bsdf_t *b, int slot, const float *c, const brec *r) {
+    int t = b->d.tex[slot];
+    return t ? tex_eval(b->textures, t - 1, r->uv) : vload(c);
+}
+static inline float par_alpha(const bsdf_t *b, int slot, float c, const brec *r) {
+    int t = b->d.tex[slot];
+    return t ? tex_eval(b->textures, t - 1, r->uv).x : c;
+}
+static inline float alpha_u_of(const bsdf_t *b, const brec *r) { return clampf(par_alpha(b, 4, b->d.alpha_u, r), 5e-4f, 1.0f); }
+static inline float alpha_v_of(const bsdf_t *b, const brec *r) {
+    return b->d.anisotropic ? clampf(par_alpha(b, 5, b->d.alpha_v, r), 5e-4f, 1.0f) : alpha_u_of(b, r);
 }
 
 /* DiffuseBSDF  src/bsdf/DiffuseBSDF.cpp:20-67 */
@@ -749,11 +810,11 @@ static v3 diffuse_sample(const bsdf_t *b, brec *r, float ux, float uy) {
     r->measure = HO_MEASURE_SOLID_ANGLE;
     r->wo = square_to_cos_hemi(ux, uy);
     r->eta = 1.0f;
-    return vload(b->d.kd);
+    return par_rgb(b, 0, b->d.kd, r);
 }
 static v3 diffuse_eval(const bsdf_t *b, const brec *r) {
     if (r->measure != HO_MEASURE_SOLID_ANGLE || r->wi.z <= 0 || r->wo.z <= 0) return V(0, 0, 0);
-    return scl(vload(b->d.kd), (float)INV_PI_D);
+    return scl(par_rgb(b, 0, b->d.kd, r), (float)INV_PI_D);
 }
 static float diffuse_pdf(const brec *r) {
     if (r->measure != HO_MEASURE_SOLID_ANGLE || r->wi.z <= 0 || r->wo.z <= 0) return 0.0f;
@@ -765,7 +826,7 @@ static v3 conductor_sample(const bsdf_t *b, brec *r, float ux, float uy) {
     r->measure = HO_MEASURE_SOLID_ANGLE;
     float ci = r->wi.z;
     if (ci <= 0.0f) return V(0, 0, 0);
-    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b, r), alpha_v_of(b, r));
     float pdf;
     v3 m = mfd_sample(&d, ux, uy, &pdf);
     if (pdf == 0.0f) return V(0, 0, 0);
@@ -776,7 +837,7 @@ static v3 conductor_sample(const bsdf_t *b, brec *r, float ux, float uy) {
     v3 F = fresnel_conductor(mdw, b->eta_c, b->k_c);
     float G = mfd_g(&d, r->wi, r->wo, m);
     float D = mfd_eval(&d, m);
-    v3 ks = vload(b->d.ks);
+    v3 ks = par_rgb(b, 1, b->d.ks, r);
     float den = pdf * r->wi.z;
     return V((((ks.x * F.x) * D) * G) * mdw / den, (((ks.y * F.y) * D) * G) * mdw / den,
              (((ks.z * F.z) * D) * G) * mdw / den);
@@ -785,10 +846,10 @@ static v3 conductor_eval(const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z;
     if (r->measure != HO_MEASURE_SOLID_ANGLE || ci <= 0.0f || co <= 0.0f) return V(0, 0, 0);
     v3 h = normalize(add(r->wi, r->wo));
-    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b, r), alpha_v_of(b, r));
     float D = mfd_eval(&d, h);
     if (D == 0.0f) return V(0, 0, 0);
-    v3 F = mul(fresnel_conductor(dot(h, r->wi), b->eta_c, b->k_c), vload(b->d.ks));
+    v3 F = mul(fresnel_conductor(dot(h, r->wi), b->eta_c, b->k_c), par_rgb(b, 1, b->d.ks, r));
     float G = mfd_g(&d, r->wi, r->wo, h);
     float dg = D * G, den = 4.0f * ci;
     return V(dg * F.x / den, dg * F.y / den, dg * F.z / den);
@@ -797,7 +858,7 @@ static float conductor_pdf(const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z;
     if (r->measure != HO_MEASURE_SOLID_ANGLE || ci <= 0.0f || co <= 0.0f) return 0.0f;
     v3 h = normalize(add(r->wi, r->wo));
-    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b, r), alpha_v_of(b, r));
     return mfd_pdf(&d, h) / (4.0f * fabsf(dot(h, r->wo)));
 }
 
@@ -806,7 +867,7 @@ static v3 dielectric_sample(const bsdf_t *b, brec *r, float ux, float uy, ho_pcg
     r->measure = HO_MEASURE_SOLID_ANGLE;
     float ci = r->wi.z;
     if (ci == 0.0f) return V(0, 0, 0);
-    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b, r), alpha_v_of(b, r));
     mfd sd = d;
     float s = 1.2f - 0.2f * sqrtf(fabsf(ci));
     sd.au *= s; sd.av *= s;                                    /* ScaleAlpha */
@@ -826,7 +887,7 @@ static v3 dielectric_sample(const bsdf_t *b, brec *r, float ux, float uy, ho_pcg
         r->eta = 1.0f;
         float co = r->wo.z;
         if (co * ci <= 0.0f) return V(0, 0, 0);
-        W = mul(W, vload(b->d.ks));
+        W = mul(W, par_rgb(b, 1, b->d.ks, r));
     } else {
         if (ct == 0.0f) return V(0, 0, 0);
         r->wo = refract_m(r->wi, m, ct, b->eta, b->inv_eta);
@@ -834,7 +895,7 @@ static v3 dielectric_sample(const bsdf_t *b, brec *r, float ux, float uy, ho_pcg
         float co = r->wo.z;
         if (co * ci >= 0.0f) return V(0, 0, 0);
         float fac = (ct < 0.0f ? b->inv_eta : b->eta);
-        W = mul(W, scl(vload(b->d.ks_refract), fac * fac));
+        W = mul(W, scl(par_rgb(b, 2, b->d.ks_refract, r), fac * fac));
     }
     float v = fabsf(mfd_eval(&d, m) * mfd_g(&d, r->wi, r->wo, m) * dot(r->wi, m) / (pdf * ci));
     return scl(W, v);
@@ -847,18 +908,18 @@ static v3 dielectric_eval(const bsdf_t *b, const brec *r) {
     if (refl) h = normalize(add(r->wi, r->wo));
     else { float e = ci > 0.0f ? b->eta : b->inv_eta; h = normalize(add(r->wi, scl(r->wo, e))); }
     h = scl(h, signum(h.z));
-    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b, r), alpha_v_of(b, r));
     float D = mfd_eval(&d, h);
     if (D == 0.0f) return V(0, 0, 0);
     float ct;
     float F = fresnel_dielectric(dot(r->wi, h), b->eta, b->inv_eta, &ct);
     float G = mfd_g(&d, r->wi, r->wo, h);
-    if (refl) return scl(vload(b->d.ks), F * D * G / (4.0f * fabsf(ci)));
+    if (refl) return scl(par_rgb(b, 1, b->d.ks, r), F * D * G / (4.0f * fabsf(ci)));
     float e = ci > 0.0f ? b->eta : b->inv_eta;
     float sd = dot(r->wi, h) + e * dot(r->wo, h);
     float val = ((1.0f - F) * D * G * e * e * dot(r->wi, h) * dot(r->wo, h)) / (ci * sd * sd);
     float fac = (ci < 0.0f ? b->inv_eta : b->eta);
-    return scl(vload(b->d.ks_refract), fabsf(val * fac * fac));
+    return scl(par_rgb(b, 2, b->d.ks_refract, r), fabsf(val * fac * fac));
 }
 static float dielectric_pdf(const bsdf_t *b, const brec *r) {
     if (r->measure != HO_MEASURE_SOLID_ANGLE) return 0.0f;
@@ -874,7 +935,7 @@ static float dielectric_pdf(const bsdf_t *b, const brec *r) {
         J = (e * e * dot(r->wo, h)) / (sd * sd);
     }
     h = scl(h, signum(h.z));
-    mfd d = mfd_make(b->d.distribution, alpha_u_of(b), alpha_v_of(b));
+    mfd d = mfd_make(b->d.distribution, alpha_u_of(b, r), alpha_v_of(b, r));
     float s = 1.2f - 0.2f * sqrtf(fabsf(ci));
     d.au *= s; d.av *= s;
     float ct;
@@ -887,7 +948,7 @@ static float dielectric_pdf(const bsdf_t *b, const brec *r) {
 static v3 plastic_eval(const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z;
     if (r->measure == HO_MEASURE_UNKNOWN || ci <= 0.0f || co <= 0.0f) return V(0, 0, 0);
-    float a = alpha_u_of(b);
+    float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     float ct;
     v3 h = normalize(add(r->wi, r->wo));
@@ -895,8 +956,8 @@ static v3 plastic_eval(const bsdf_t *b, const brec *r) {
     float F = fresnel_dielectric(dot(r->wi, h), b->eta, b->inv_eta, &ct);
     float G = mfd_g(&d, r->wi, r->wi, h);                     /* G(Wi, Wi, H) as in :146 */
     float val = F * D * G / (4.0f * ci);
-    v3 res = scl(vload(b->d.ks), val);
-    v3 dif = vload(b->d.kd);
+    v3 res = scl(par_rgb(b, 1, b->d.ks, r), val);
+    v3 dif = par_rgb(b, 0, b->d.kd, r);
     float t12 = rft_eval1d(b->rft, b->rft_n, ci);
     float t21 = rft_eval1d(b->rft, b->rft_n, co);
     float fdr = b->fdr_int;
@@ -912,7 +973,7 @@ static float plastic_spec_pdf(const bsdf_t *b, float ci) {
 static float plastic_pdf(const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z;
     if (r->measure == HO_MEASURE_UNKNOWN || ci <= 0.0f || co <= 0.0f) return 0.0f;
-    float a = alpha_u_of(b);
+    float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     v3 h = normalize(add(r->wi, r->wo));
     float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
@@ -924,7 +985,7 @@ static float plastic_pdf(const bsdf_t *b, const brec *r) {
 static v3 plastic_sample(const bsdf_t *b, brec *r, float ux, float uy) {
     float ci = r->wi.z;
     if (ci <= 0.0f) return V(0, 0, 0);
-    float a = alpha_u_of(b);
+    float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
     int spec;
@@ -959,14 +1020,14 @@ static v3 coat_refract(v3 wi, float inv_eta) {   /* RefractIn :347 (RefractOut :
 static v3 coating_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z;
     if (ci * co <= 0.0f) return V(0, 0, 0);
-    float a = alpha_u_of(b);
+    float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     v3 h = scl(normalize(add(r->wi, r->wo)), signum(r->wo.z));
     float ct;
     float D = mfd_eval(&d, h);
     float F = fresnel_dielectric(fabsf(dot(r->wi, h)), b->eta, b->inv_eta, &ct);
     float G = mfd_g(&d, r->wi, r->wo, h);
-    v3 ks = vload(b->d.ks);
+    v3 ks = par_rgb(b, 1, b->d.ks, r);
     float den = 4.0f * fabsf(ci);
     v3 res = V((((ks.x * F) * D) * G) / den, (((ks.y * F) * D) * G) / den, (((ks.z * F) * D) * G) / den);
     brec ri = *r;
@@ -975,7 +1036,7 @@ static v3 coating_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
     v3 nv = bsdf_eval(s, b->d.nested, &ri);
     float ti = rft_eval1d(b->rft, b->rft_n, fabsf(ci)), to = rft_eval1d(b->rft, b->rft_n, fabsf(co));
     nv = V(nv.x * ti * to, nv.y * ti * to, nv.z * ti * to);
-    v3 sa = scl(vload(b->d.sigma_a), b->d.thickness);
+    v3 sa = scl(par_rgb(b, 3, b->d.sigma_a, r), b->d.thickness);
     if (!is_zero(sa)) {
         float q = 1.0f / fabsf(ri.wi.z) + 1.0f / fabsf(ri.wo.z);
         nv = mul(nv, V(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q)));
@@ -985,7 +1046,7 @@ static v3 coating_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
 }
 static float coating_pdf(const ho_scene *s, const bsdf_t *b, const brec *r) {
     v3 h = scl(normalize(add(r->wi, r->wo)), signum(r->wo.z));
-    float a = alpha_u_of(b);
+    float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     float ci = r->wi.z, co = r->wo.z;
     float r12 = 1.0f - rft_eval1d(b->rft, b->rft_n, fabsf(ci));
@@ -1005,7 +1066,7 @@ static float coating_pdf(const ho_scene *s, const bsdf_t *b, const brec *r) {
 }
 static v3 coating_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux, float uy, ho_pcg32 *rng,
                          const float *u1f) {
-    float a = alpha_u_of(b);
+    float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     float aci = fabsf(r->wi.z);
     float r12 = 1.0f - rft_eval1d(b->rft, b->rft_n, aci);
@@ -1074,11 +1135,11 @@ static v3 sconductor_sample(const bsdf_t *b, brec *r) {
     v3 F = fresnel_conductor(ci, b->eta_c, b->k_c);
     r->wo = reflect_n(r->wi);
     r->eta = 1.0f;
-    return mul(vload(b->d.ks), F);
+    return mul(par_rgb(b, 1, b->d.ks, r), F);
 }
 static v3 sconductor_eval(const bsdf_t *b, const brec *r) {
     if (!mirror_match(r)) return V(0, 0, 0);
-    return mul(vload(b->d.ks), fresnel_conductor(r->wi.z, b->eta_c, b->k_c));
+    return mul(par_rgb(b, 1, b->d.ks, r), fresnel_conductor(r->wi.z, b->eta_c, b->k_c));
 }
 static float sconductor_pdf(const brec *r) { return mirror_match(r) ? 1.0f : 0.0f; }
 
@@ -1090,21 +1151,21 @@ static v3 sdielectric_sample(const bsdf_t *b, brec *r, float ux) {
     if (ux < F) {
         r->wo = reflect_n(r->wi);
         r->eta = 1.0f;
-        return vload(b->d.ks);
+        return par_rgb(b, 1, b->d.ks, r);
     }
     r->wo = refract_n(r->wi, ct, b->eta, b->inv_eta);
     r->eta = ct < 0.0f ? b->eta : b->inv_eta;
     float f = ct < 0.0f ? b->inv_eta : b->eta;   /* radiance transport */
-    return scl(vload(b->d.ks_refract), f * f);
+    return scl(par_rgb(b, 2, b->d.ks_refract, r), f * f);
 }
 static v3 sdielectric_eval(const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z, ct;
     float F = fresnel_dielectric(ci, b->eta, b->inv_eta, &ct);
     if (ci * co >= 0.0f) {
-        if (delta_match(reflect_n(r->wi), r->wo)) return scl(vload(b->d.ks), F);
+        if (delta_match(reflect_n(r->wi), r->wo)) return scl(par_rgb(b, 1, b->d.ks, r), F);
     } else if (delta_match(refract_n(r->wi, ct, b->eta, b->inv_eta), r->wo)) {
         float f = ct < 0.0f ? b->inv_eta : b->eta;
-        return scl(scl(vload(b->d.ks_refract), f * f), 1.0f - F);
+        return scl(scl(par_rgb(b, 2, b->d.ks_refract, r), f * f), 1.0f - F);
     }
     return V(0, 0, 0);
 }
@@ -1123,8 +1184,8 @@ static float sdielectric_pdf(const bsdf_t *b, const brec *r) {
 static float splastic_spec_pdf(const bsdf_t *b, float Fi) {
     return (Fi * b->spec_w) / (Fi * b->spec_w + (1.0f - Fi) * (1.0f - b->spec_w));
 }
-static v3 splastic_diffuse(const bsdf_t *b) {
-    v3 dif = vload(b->d.kd);
+static v3 splastic_diffuse(const bsdf_t *b, const brec *r) {
+    v3 dif = par_rgb(b, 0, b->d.kd, r);
     float fdr = b->fdr_int;
     if (b->d.nonlinear) return V(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
     return divs(dif, 1.0f - fdr);
@@ -1139,12 +1200,12 @@ static v3 splastic_sample(const bsdf_t *b, brec *r, float ux, float uy) {
     if (ux < sp) {
         r->measure = HO_MEASURE_DISCRETE;
         r->wo = reflect_n(r->wi);
-        return divs(scl(vload(b->d.ks), Fi), sp);
+        return divs(scl(par_rgb(b, 1, b->d.ks, r), Fi), sp);
     }
     r->measure = HO_MEASURE_SOLID_ANGLE;
     r->wo = square_to_cos_hemi((ux - sp) / (1.0f - sp), uy);
     float Fo = fresnel_dielectric(r->wo.z, b->eta, b->inv_eta, &ct);
-    return scl(splastic_diffuse(b), b->inv_eta2 * (1.0f - Fi) * (1.0f - Fo) / (1.0f - sp));
+    return scl(splastic_diffuse(b, r), b->inv_eta2 * (1.0f - Fi) * (1.0f - Fo) / (1.0f - sp));
 }
 static v3 splastic_eval(const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z;
@@ -1152,9 +1213,9 @@ static v3 splastic_eval(const bsdf_t *b, const brec *r) {
     float ct;
     float Fi = fresnel_dielectric(ci, b->eta, b->inv_eta, &ct);
     if (r->measure == HO_MEASURE_DISCRETE)
-        return delta_match(reflect_n(r->wi), r->wo) ? scl(vload(b->d.ks), Fi) : V(0, 0, 0);
+        return delta_match(reflect_n(r->wi), r->wo) ? scl(par_rgb(b, 1, b->d.ks, r), Fi) : V(0, 0, 0);
     float Fo = fresnel_dielectric(co, b->eta, b->inv_eta, &ct);
-    return scl(splastic_diffuse(b), cos_hemi_pdf(r->wo) * b->inv_eta2 * (1.0f - Fi) * (1.0f - Fo));
+    return scl(splastic_diffuse(b, r), cos_hemi_pdf(r->wo) * b->inv_eta2 * (1.0f - Fi) * (1.0f - Fo));
 }
 static float splastic_pdf(const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z;
@@ -1178,8 +1239,8 @@ static v3 scoat_refract_out(const bsdf_t *b, v3 wi, float *R) {   /* RefractOut 
     *R = fresnel_dielectric(fabsf(wi.z), b->inv_eta, b->eta, &ct);
     return V(b->eta * wi.x, b->eta * wi.y, -signum(wi.z) * ct);
 }
-static v3 scoat_absorb(const bsdf_t *b, v3 res, v3 wi_int, v3 wo_int) {
-    v3 sa = scl(vload(b->d.sigma_a), b->d.thickness);
+static v3 scoat_absorb(const bsdf_t *b, const brec *r, v3 res, v3 wi_int, v3 wo_int) {
+    v3 sa = scl(par_rgb(b, 3, b->d.sigma_a, r), b->d.thickness);
     if (is_zero(sa)) return res;
     float q = 1.0f / fabsf(wi_int.z) + 1.0f / fabsf(wo_int.z);
     return mul(res, V(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q)));
@@ -1196,7 +1257,7 @@ static v3 scoating_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux,
         r->wo = reflect_n(r->wi);
         r->eta = 1.0f;
         r->measure = HO_MEASURE_DISCRETE;
-        return scl(vload(b->d.ks), R12 / sp);
+        return scl(par_rgb(b, 1, b->d.ks, r), R12 / sp);
     }
     ux = (ux - sp) / (1.0f - sp);
     if (R12 == 1.0f) return V(0, 0, 0);
@@ -1206,7 +1267,7 @@ static v3 scoating_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux,
     r->wi = wib;
     if (is_zero(res)) return V(0, 0, 0);
     v3 wop = r->wo;
-    res = scoat_absorb(b, res, wip, wop);
+    res = scoat_absorb(b, r, res, wip, wop);
     float R21;
     r->wo = scoat_refract_out(b, wop, &R21);
     if (R21 == 1.0f) return V(0, 0, 0);
@@ -1217,7 +1278,7 @@ static v3 scoating_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
     if (r->measure == HO_MEASURE_DISCRETE) {
         if (!delta_match(reflect_n(r->wi), r->wo)) return V(0, 0, 0);
         float ct;
-        return scl(vload(b->d.ks), fresnel_dielectric(fabsf(r->wi.z), b->eta, b->inv_eta, &ct));
+        return scl(par_rgb(b, 1, b->d.ks, r), fresnel_dielectric(fabsf(r->wi.z), b->eta, b->inv_eta, &ct));
     }
     float R12, R21;
     brec ri = *r;
@@ -1225,7 +1286,7 @@ static v3 scoating_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
     ri.wo = scoat_refract_in(b, r->wo, &R21);
     if (R12 == 1.0f || R21 == 1.0f) return V(0, 0, 0);
     v3 res = scl(scl(bsdf_eval(s, b->d.nested, &ri), 1.0f - R12), 1.0f - R21);
-    res = scoat_absorb(b, res, ri.wi, ri.wo);
+    res = scoat_absorb(b, r, res, ri.wi, ri.wo);
     if (r->measure == HO_MEASURE_SOLID_ANGLE) res = scl(res, b->inv_eta * b->inv_eta * r->wo.z / ri.wo.z);
     return res;
 }
@@ -1264,7 +1325,7 @@ static inline float frame_cos_phi(v3 v) {   /* :78 */
 static v3 roughdiffuse_eval(const bsdf_t *b, const brec *r) {
     float ci = r->wi.z, co = r->wo.z;
     if (ci <= 0.0f || co <= 0.0f || r->measure != HO_MEASURE_SOLID_ANGLE) return V(0, 0, 0);
-    float sigma = clampf(b->d.alpha_u, 5e-4f, 1.0f) * 0.70710678118655f;
+    float sigma = clampf(par_alpha(b, 4, b->d.alpha_u, r), 5e-4f, 1.0f) * 0.70710678118655f;
     float s2 = sigma * sigma;
     float sti = frame_sin_theta(r->wi), sto = frame_sin_theta(r->wo);
     float cpd = 0.0f;
@@ -1280,7 +1341,7 @@ static v3 roughdiffuse_eval(const bsdf_t *b, const brec *r) {
         float sa, tb;
         if (ci > co) { sa = sto; tb = sti / ci; }
         else { sa = sti; tb = sto / co; }
-        return scl(vload(b->d.kd), inv_pi * co * (A + B * max_f(cpd, 0.0f) * sa * tb));
+        return scl(par_rgb(b, 0, b->d.kd, r), inv_pi * co * (A + B * max_f(cpd, 0.0f) * sa * tb));
     }
     float thi = safe_acos(ci), tho = safe_acos(co);
     float al = max_f(thi, tho), be = min_f(thi, tho);
@@ -1298,7 +1359,7 @@ static v3 roughdiffuse_eval(const bsdf_t *b, const brec *r) {
     else C2 *= sa - t3 * t3 * t3;
     float th = (sa + sb) / (safe_sqrt(1.0f - sa * sa) + safe_sqrt(1.0f - sb * sb));
     if (isinf(th) || isnan(th)) return V(0, 0, 0);
-    v3 rho = vload(b->d.kd);
+    v3 rho = par_rgb(b, 0, b->d.kd, r);
     v3 lr1 = scl(rho, C1 + cpd * C2 * tb + (1.0f - fabsf(cpd)) * C3 * th);
     v3 lr2 = scl(mul(rho, rho), C4 * (1.0f - cpd * t3 * t3));
     return scl(add(lr1, lr2), inv_pi * co);
@@ -1404,11 +1465,11 @@ void ho_bsdf_sample(const ho_scene *s, int id, const float *wi, const float *u2,
     vstore(owo, r.wo); vstore(ow, w); *om = r.measure; *oeta = r.eta;
 }
 void ho_bsdf_eval(const ho_scene *s, int id, const float *wi, const float *wo, int measure, float *o) {
-    brec r; r.wi = vload(wi); r.wo = vload(wo); r.measure = measure; r.eta = 0.0f;
+    brec r; memset(&r, 0, sizeof r); r.wi = vload(wi); r.wo = vload(wo); r.measure = measure; r.eta = 0.0f;
     vstore(o, bsdf_eval(s, id, &r));
 }
 float ho_bsdf_pdf(const ho_scene *s, int id, const float *wi, const float *wo, int measure) {
-    brec r; r.wi = vload(wi); r.wo = vload(wo); r.measure = measure; r.eta = 0.0f;
+    brec r; memset(&r, 0, sizeof r); r.wi = vload(wi); r.wo = vload(wo); r.measure = measure; r.eta = 0.0f;
     return bsdf_pdf(s, id, &r);
 }
 float ho_bsdf_rft_eval(const ho_scene *s, int id, float c) {
@@ -1416,8 +1477,8 @@ float ho_bsdf_rft_eval(const ho_scene *s, int id, float c) {
     return rft_eval1d(b->rft, b->rft_n, c);
 }
 void ho_bsdf_batch(const ho_scene *s, int id, uint64_t n, const float *wi, const float *u2, const float *u1,
-                   const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
-                   float *p_pdf, int nthreads) {
+                   const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m,
+                   float *e_rgb, float *p_pdf, int nthreads) {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(static)
@@ -1425,13 +1486,16 @@ void ho_bsdf_batch(const ho_scene *s, int id, uint64_t n, const float *wi, const
     for (int64_t i = 0; i < (int64_t)n; i++) {
         brec r; memset(&r, 0, sizeof r);
         r.wi = vload(wi + 3 * i); r.measure = HO_MEASURE_UNKNOWN;
+        if (uv) { r.uv[0] = uv[2 * i]; r.uv[1] = uv[2 * i + 1]; }
         float uu = u1 ? u1[i] : 0.0f;
         v3 w = bsdf_sample(s, id, &r, u2[2 * i], u2[2 * i + 1], NULL, &uu);
         if (s_wo) vstore(s_wo + 3 * i, r.wo);
         if (s_w) vstore(s_w + 3 * i, w);
         if (s_m) s_m[i] = r.measure;
         if (s_pdf) s_pdf[i] = is_zero(w) && w.x == 0 && w.y == 0 && w.z == 0 ? 0.0f : bsdf_pdf(s, id, &r);
-        brec q; q.wi = vload(wi + 3 * i); q.wo = vload(wo + 3 * i); q.measure = HO_MEASURE_SOLID_ANGLE; q.eta = 0;
+        brec q; memset(&q, 0, sizeof q);
+        q.wi = vload(wi + 3 * i); q.wo = vload(wo + 3 * i); q.measure = HO_MEASURE_SOLID_ANGLE; q.eta = 0;
+        if (uv) { q.uv[0] = uv[2 * i]; q.uv[1] = uv[2 * i + 1]; }
         if (e_rgb) vstore(e_rgb + 3 * i, bsdf_eval(s, id, &q));
         if (p_pdf) p_pdf[i] = bsdf_pdf(s, id, &q);
     }
@@ -1890,6 +1954,7 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
                 hit_t sh;
                 if (!trace(s, it.p, sd, EPS_RAY, 1.0f - EPS_RAY, 1, 1, &sh)) {
                     brec br; br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.wo = to_local(&it.sh, er.wi);
+                    br.uv[0] = it.uv[0]; br.uv[1] = it.uv[1];
                     br.measure = HO_MEASURE_SOLID_ANGLE; br.eta = 0;
                     float pb = bsdf_pdf(s, bsdf, &br);
                     if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
@@ -1901,6 +1966,7 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
             }
         }
         brec br; memset(&br, 0, sizeof br);
+        br.uv[0] = it.uv[0]; br.uv[1] = it.uv[1];
         br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.measure = HO_MEASURE_UNKNOWN;
         float sx = ho_pcg32_nextf(rng), sy = ho_pcg32_nextf(rng);
         v3 F = bsdf_sample(s, bsdf, &br, sx, sy, rng, NULL);

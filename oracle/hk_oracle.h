@@ -58,7 +58,22 @@ typedef struct {
     int32_t nested;        /* roughCoating / twoSided (front): index of the nested BSDF, else -1 */
     int32_t nested2;       /* twoSided (back): index of the second nested BSDF, -1 = the front one */
     int32_t fast_approx;   /* roughDiffuse "fastApprox" */
+    /* textures of kd, ks / ksReflect, ksRefract, sigmaA, alpha / alphaU, alphaV:
+     * 1 + texture id (ho_scene_add_texture), 0 = the constant value above */
+    int32_t tex[6];
 } ho_bsdf_desc;
+
+/* Procedural textures (src/texture/{Checkerboard,Grid,Scale}Texture.cpp). */
+enum { HO_TEX_CHECKERBOARD = 1, HO_TEX_GRID = 2, HO_TEX_SCALE = 3 };
+typedef struct {
+    int32_t kind;          /* HO_TEX_* */
+    int32_t nested;        /* scale: the scaled texture's id */
+    int32_t count;         /* checkerboard "blocks", grid "lines" */
+    float width;           /* grid "lineWidth" */
+    float scale;           /* scale "scale" */
+    float uv_scale[2], uv_offset[2];   /* "uScale" "vScale", "uOffset" "vOffset" */
+    float a[3], b[3];      /* checkerboard colorA / colorB; grid lineColor / backgroundColor */
+} ho_texture_desc;
 
 typedef struct ho_scene ho_scene;
 
@@ -74,6 +89,7 @@ void      ho_scene_destroy(ho_scene *s);
 /* Raw RFT table file bytes (data/{Beckmann,GGX}RFTData.bin), index = distribution. */
 int  ho_scene_set_rft(ho_scene *s, int distribution, const void *bytes, uint64_t nbytes);
 int  ho_scene_add_bsdf(ho_scene *s, const ho_bsdf_desc *d);   /* returns id or <0 */
+int  ho_scene_add_texture(ho_scene *s, const ho_texture_desc *d);   /* returns id or <0 */
 /* positions 3*nv, indices 3*nt (mesh-local), normals 3*nv or NULL,
  * radiance 3 or NULL (area light).  Returns mesh id or <0. */
 int  ho_scene_add_mesh(ho_scene *s, const float *positions, uint32_t nv,
@@ -111,8 +127,9 @@ void  ho_bsdf_eval(const ho_scene *s, int bsdf, const float *wi, const float *wo
 float ho_bsdf_pdf(const ho_scene *s, int bsdf, const float *wi, const float *wo, int measure);
 /* batched over n records, 2^k friendly; records are AoS float3 */
 void  ho_bsdf_batch(const ho_scene *s, int bsdf, uint64_t n, const float *wi, const float *u2,
-                    const float *u1, const float *wo, float *s_wo, float *s_w, float *s_pdf,
-                    int32_t *s_measure, float *e_rgb, float *p_pdf, int nthreads);
+                    const float *u1, const float *wo, const float *uv, float *s_wo, float *s_w,
+                    float *s_pdf, int32_t *s_measure, float *e_rgb, float *p_pdf, int nthreads);
+/* (uv: n x 2 texture coordinates of the records' intersections, or NULL) */
 /* RFT 1D eval after activation (for table parity tests). */
 float ho_bsdf_rft_eval(const ho_scene *s, int bsdf, float cos_theta);
 

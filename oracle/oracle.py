@@ -35,8 +35,23 @@ class BsdfDescC(C.Structure):
         ("alpha_u", C.c_float), ("alpha_v", C.c_float), ("int_ior", C.c_float), ("ext_ior", C.c_float),
         ("eta", C.c_float * 3), ("k", C.c_float * 3), ("ks", C.c_float * 3), ("ks_refract", C.c_float * 3),
         ("kd", C.c_float * 3), ("sigma_a", C.c_float * 3), ("thickness", C.c_float), ("nested", C.c_int32),
-        ("nested2", C.c_int32), ("fast_approx", C.c_int32),
+        ("nested2", C.c_int32), ("fast_approx", C.c_int32), ("tex", C.c_int32 * 6),
     ]
+
+
+class TextureDescC(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("nested", C.c_int32), ("count", C.c_int32), ("width", C.c_float),
+        ("scale", C.c_float), ("uv_scale", C.c_float * 2), ("uv_offset", C.c_float * 2), ("a", C.c_float * 3),
+        ("b", C.c_float * 3),
+    ]
+
+
+def texture_desc_c(t, nested_index=-1) -> TextureDescC:
+    c = TextureDescC()
+    c.kind, c.nested, c.count, c.width, c.scale = t.kind, nested_index, t.count, t.width, t.scale
+    c.uv_scale[:], c.uv_offset[:], c.a[:], c.b[:] = t.uv_scale, t.uv_offset, t.a, t.b
+    return c
 
 
 _lib = None
@@ -69,7 +84,8 @@ def lib():
         L.ho_bsdf_eval.argtypes = [P, C.c_int, P, P, C.c_int, P]
         L.ho_bsdf_pdf.argtypes = [P, C.c_int, P, P, C.c_int]
         L.ho_bsdf_pdf.restype = C.c_float
-        L.ho_bsdf_batch.argtypes = [P, C.c_int, C.c_uint64, P, P, P, P, P, P, P, P, P, P, C.c_int]
+        L.ho_bsdf_batch.argtypes = [P, C.c_int, C.c_uint64, P, P, P, P, P, P, P, P, P, P, P, C.c_int]
+        L.ho_scene_add_texture.argtypes = [P, C.POINTER(TextureDescC)]
         L.ho_bsdf_rft_eval.argtypes = [P, C.c_int, C.c_float]
         L.ho_bsdf_rft_eval.restype = C.c_float
         L.ho_trace.argtypes = [P, C.c_uint64, P, P, P, P, P, C.c_int, C.c_int, C.c_int]
@@ -96,7 +112,7 @@ def _f32(a):
     return np.ascontiguousarray(a, dtype=np.float32)
 
 
-def bsdf_desc_c(d, nested_index=-1, nested2_index=-1) -> BsdfDescC:
+def bsdf_desc_c(d, nested_index=-1, nested2_index=-1, tex_ids=None) -> BsdfDescC:
     c = BsdfDescC()
     c.type, c.distribution = d.type, d.distribution
     c.anisotropic, c.nonlinear = int(d.anisotropic), int(d.nonlinear)
@@ -105,6 +121,8 @@ def bsdf_desc_c(d, nested_index=-1, nested2_index=-1) -> BsdfDescC:
     c.k[:], c.ks[:], c.ks_refract[:], c.kd[:], c.sigma_a[:] = d.k, d.ks, d.ks_refract, d.kd, d.sigma_a
     c.thickness, c.nested, c.nested2 = d.thickness, nested_index, nested2_index
     c.fast_approx = int(getattr(d, "fast_approx", False))
+    for k, t in enumerate(tex_ids or [-1] * 6):
+        c.tex[k] = t + 1
     return c
 
 
@@ -184,10 +202,26 @@ class OracleScene:
             return self.bsdf_ids[key]
         nested = self.add_bsdf(d.nested) if d.nested is not None else -1
         nested2 = self.add_bsdf(d.nested2) if getattr(d, "nested2", None) is not None else -1
-        c = bsdf_desc_c(d, nested, nested2)
+        from hikari_b200.scenedesc import TEX_SLOTS
+        tex = getattr(d, "textures", {}) or {}
+        c = bsdf_desc_c(d, nested, nested2, [self.add_texture(tex[k]) if k in tex else -1 for k in TEX_SLOTS])
         self._keep.append(c)
         i = lib().ho_scene_add_bsdf(self.h, C.byref(c))
         self.bsdf_ids[key] = i
+        return i
+
+    def add_texture(self, t) -> int:
+        if not hasattr(self, "tex_ids"):
+            self.tex_ids = {}
+        if id(t) in self.tex_ids:
+            return self.tex_ids[id(t)]
+        nested = self.add_texture(t.nested) if t.nested is not None else -1
+        c = texture_desc_c(t, nested)
+        self._keep.append(c)
+        i = lib().ho_scene_add_texture(self.h, C.byref(c))
+        if i < 0:
+            raise RuntimeError(lib().ho_last_error().decode())
+        self.tex_ids[id(t)] = i
         return i
 
     def __del__(self):
@@ -202,15 +236,16 @@ class OracleScene:
         lib().ho_scene_bbox(self.h, _p(o))
         return o
 
-    def bsdf_batch(self, bsdf, wi, u2, u1, wo, nthreads=0):
+    def bsdf_batch(self, bsdf, wi, u2, u1, wo, nthreads=0, uv=None):
         n = wi.shape[0]
         wi, u2, wo = _f32(wi), _f32(u2), _f32(wo)
         u1 = _f32(u1) if u1 is not None else None
+        uv = _f32(uv) if uv is not None else None
         out = dict(
             s_wo=np.zeros((n, 3), np.float32), s_w=np.zeros((n, 3), np.float32), s_pdf=np.zeros(n, np.float32),
             s_measure=np.zeros(n, np.int32), e_rgb=np.zeros((n, 3), np.float32), p_pdf=np.zeros(n, np.float32),
         )
-        lib().ho_bsdf_batch(self.h, bsdf, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(out["s_wo"]), _p(out["s_w"]),
+        lib().ho_bsdf_batch(self.h, bsdf, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(uv), _p(out["s_wo"]), _p(out["s_w"]),
                             _p(out["s_pdf"]), _p(out["s_measure"]), _p(out["e_rgb"]), _p(out["p_pdf"]), nthreads)
         return out
 

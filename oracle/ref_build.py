@@ -35,6 +35,7 @@ BSDFS = ["DiffuseBSDF", "RoughConductorBSDF", "RoughDielectricBSDF", "RoughPlast
          "MirrorBSDF", "ConductorBSDF", "DielectricBSDF", "PlasticBSDF", "TwoSidedBSDF", "CoatingBSDF",
          "RoughDiffuseBSDF"]
 EMITTERS = ["PointLight", "DirectionalLight", "ConstantLight"]
+TEXTURES = ["CheckerboardTexture", "GridTexture", "ScaleTexture"]
 
 
 def _link(src, dst):
@@ -83,6 +84,7 @@ def build(ref: str = "/root/reference") -> str:
     srcs = [os.path.join(ref, "src", "core", c + ".cpp") for c in CORE] + \
            [os.path.join(ref, "src", "bsdf", b + ".cpp") for b in BSDFS] + \
            [os.path.join(ref, "src", "emitter", e + ".cpp") for e in EMITTERS] + \
+           [os.path.join(ref, "src", "texture", t + ".cpp") for t in TEXTURES] + \
            [os.path.join(HERE, "ref_shim", "ref_bridge.cpp")]
     for s in srcs:
         o = os.path.join(objd, os.path.basename(s) + ".o")

@@ -30,6 +30,9 @@ public:
 };
 thread_local FixedSampler g_sampler;
 const Intersection &null_isect() { static const Intersection I; return I; }
+/* the intersection of the current query: only its texture coordinates matter */
+thread_local Intersection g_isect;
+const Intersection &query_isect() { return g_isect; }
 }
 
 extern "C" {
@@ -41,7 +44,8 @@ void hr_init(const char *search_dir) { GetFileResolver()->prepend(filesystem::pa
  * 10 coating, 11 roughDiffuse */
 void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_ior, const float *k,
                      const float *ks, const float *kd, const float *sigma_a, float thickness, void *nested,
-                     void *nested2, const float *ks_refract, int nonlinear, int fast_approx) {
+                     void *nested2, const float *ks_refract, int nonlinear, int fast_approx, void **tex,
+                     int anisotropic) {
     static const char *names[] = {"diffuse", "roughConductor", "roughDielectric", "roughPlastic", "roughCoating",
                                   "mirror", "conductor", "dielectric", "plastic", "twoSided", "coating",
                                   "roughDiffuse"};
@@ -53,6 +57,11 @@ void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_io
         } else if (type <= 4) {
             pl.SetString("type", ggx ? "ggx" : "beckmann");
             pl.SetFloat("alpha", alpha);
+            if (anisotropic && (type == 1 || type == 2)) {
+                pl.SetBoolean("as", true);
+                pl.SetFloat("alphaU", alpha);
+                pl.SetFloat("alphaV", alpha);
+            }
             pl.SetFloat("intIOR", int_ior);
             pl.SetFloat("extIOR", ext_ior);
             if (type == 1) { pl.SetColor("k", col(k)); pl.SetColor("ks", col(ks)); }
@@ -79,6 +88,14 @@ void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_io
         BSDF *b = (BSDF *)ObjectFactory::CreateInstance(names[type], pl);
         if (nested) b->AddChild((Object *)nested, "");
         if (nested2) b->AddChild((Object *)nested2, "");
+        /* textures by their XML names: kd / albedo, ks / ksReflect, ksRefract, sigmaA, alpha(U), alphaV */
+        for (int k = 0; k < 6 && tex; k++) {
+            if (!tex[k]) continue;
+            const bool refl = type == 2 || type == 7, albedo = type == 0 || type == 11;
+            const char *names[6] = {albedo ? "albedo" : "kd", refl ? "ksReflect" : "ks", "ksRefract", "sigmaA",
+                                    anisotropic ? "alphaU" : "alpha", "alphaV"};
+            b->AddChild((Object *)tex[k], names[k]);
+        }
         b->Activate();
         return b;
     } catch (const std::exception &e) {
@@ -89,7 +106,7 @@ void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_io
 
 void hr_bsdf_sample(void *h, const float *wi, const float *u2, float u1, float *wo, float *w, int *measure, float *eta) {
     g_sampler.u1 = u1;
-    BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), ETransportMode::ERadiance, &g_sampler, null_isect());
+    BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), ETransportMode::ERadiance, &g_sampler, query_isect());
     r.Wo = Vector3f(0.0f); r.Eta = 0.0f;
     Color3f c = ((BSDF *)h)->Sample(r, Point2f(u2[0], u2[1]));
     wo[0] = r.Wo.x(); wo[1] = r.Wo.y(); wo[2] = r.Wo.z();
@@ -99,14 +116,14 @@ void hr_bsdf_sample(void *h, const float *wi, const float *u2, float u1, float *
 
 void hr_bsdf_eval(void *h, const float *wi, const float *wo, int measure, float *out) {
     BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), Vector3f(wo[0], wo[1], wo[2]), EMeasure(measure),
-                      ETransportMode::ERadiance, &g_sampler, null_isect());
+                      ETransportMode::ERadiance, &g_sampler, query_isect());
     Color3f c = ((BSDF *)h)->Eval(r);
     out[0] = c[0]; out[1] = c[1]; out[2] = c[2];
 }
 
 float hr_bsdf_pdf(void *h, const float *wi, const float *wo, int measure) {
     BSDFQueryRecord r(Vector3f(wi[0], wi[1], wi[2]), Vector3f(wo[0], wo[1], wo[2]), EMeasure(measure),
-                      ETransportMode::ERadiance, &g_sampler, null_isect());
+                      ETransportMode::ERadiance, &g_sampler, query_isect());
     return ((BSDF *)h)->Pdf(r);
 }
 
@@ -150,6 +167,38 @@ void hr_post_intersect(void *h, uint32_t tri, float u, float v, float *out) {
         out[c] = I.P[c]; out[3 + c] = F.S[c]; out[6 + c] = F.T[c]; out[9 + c] = F.N[c];
     }
     out[12] = I.UV.x(); out[13] = I.UV.y();
+}
+
+/* texture coordinates of the single-record queries (hr_bsdf_sample / eval / pdf) */
+void hr_set_uv(float u, float v) { g_isect.UV = Point2f(u, v); }
+
+/* kind 1 checkerboard, 2 grid, 3 scale (of nested) */
+void *hr_texture_create(int kind, int count, float width, float scale, const float *uv_scale, const float *uv_offset,
+                        const float *a, const float *b, void *nested) {
+    try {
+        PropertyList pl;
+        Color3f ca(a[0], a[1], a[2]), cb(b[0], b[1], b[2]);
+        const char *name = kind == 1 ? "checkerboard" : (kind == 2 ? "grid" : "scale");
+        if (kind == 1 || kind == 2) {
+            pl.SetInteger(kind == 1 ? "blocks" : "lines", count);
+            pl.SetColor(kind == 1 ? "colorA" : "lineColor", ca);
+            pl.SetColor(kind == 1 ? "colorB" : "backgroundColor", cb);
+            if (kind == 2) pl.SetFloat("lineWidth", width);
+            pl.SetFloat("uScale", uv_scale[0]);
+            pl.SetFloat("vScale", uv_scale[1]);
+            pl.SetFloat("uOffset", uv_offset[0]);
+            pl.SetFloat("vOffset", uv_offset[1]);
+        } else {
+            pl.SetFloat("scale", scale);
+        }
+        Object *t = ObjectFactory::CreateInstance(name, pl);
+        if (nested) t->AddChild((Object *)nested, "");
+        t->Activate();
+        return t;
+    } catch (const std::exception &e) {
+        fprintf(stderr, "hr_texture_create: %s\n", e.what());
+        return nullptr;
+    }
 }
 
 /* kind: 0 point (power, position), 1 directional (irradiance, direction), 2 constant (radiance) */
@@ -198,8 +247,10 @@ void hr_emitter_eval_dir(void *h, uint64_t n, const float *wi, float *out) {
 
 /* batched over n AoS records (same layout as ho_bsdf_batch) */
 void hr_bsdf_batch(void *h, uint64_t n, const float *wi, const float *u2, const float *u1, const float *wo,
+                   const float *uv,
                    float *s_wo, float *s_w, float *s_pdf, int *s_m, float *e_rgb, float *p_pdf) {
     for (uint64_t i = 0; i < n; i++) {
+        g_isect.UV = uv ? Point2f(uv[2 * i], uv[2 * i + 1]) : Point2f(0.0f, 0.0f);
         float eta; int m;
         hr_bsdf_sample(h, wi + 3 * i, u2 + 2 * i, u1 ? u1[i] : 0.0f, s_wo + 3 * i, s_w + 3 * i, &m, &eta);
         s_m[i] = m;

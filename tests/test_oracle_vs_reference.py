@@ -11,7 +11,8 @@ import pytest
 from hikari_b200.scenedesc import (BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE,
                                    BSDF_MIRROR, BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR,
                                    BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX,
-                                   SMOOTH_BSDFS, BSDFDesc, SceneDesc)
+                                   SMOOTH_BSDFS, TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE, TEX_SLOTS, BSDFDesc,
+                                   SceneDesc, TextureDesc)
 from oracle import oracle as O
 
 REF_LIB = os.path.join(os.path.dirname(O.HERE), "oracle", "_ref", "libhikari_ref_bsdf.so")
@@ -28,16 +29,24 @@ def _ref_lib():
     R.hr_init.argtypes = [C.c_char_p]
     R.hr_bsdf_create.restype = C.c_void_p
     R.hr_bsdf_create.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float, C.c_float] + [C.c_void_p] * 4 + [
-        C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int]
+    R.hr_texture_create.restype = C.c_void_p
+    R.hr_texture_create.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float] + [C.c_void_p] * 5
     R.hr_bsdf_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     R.hr_bsdf_pdf.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     R.hr_bsdf_pdf.restype = C.c_float
-    R.hr_bsdf_batch.argtypes = [C.c_void_p, C.c_uint64] + [C.c_void_p] * 10
+    R.hr_bsdf_batch.argtypes = [C.c_void_p, C.c_uint64] + [C.c_void_p] * 11
     R.hr_init(os.path.dirname(REF_LIB).encode())
     return R
 
 
 CU_K = [3.9, 2.4, 2.2]
+CHECKER = TextureDesc(kind=TEX_CHECKERBOARD, count=7, a=[0.9, 0.2, 0.1], b=[0.1, 0.3, 0.8], uv_scale=[1.5, 0.7],
+                      uv_offset=[0.25, -0.1])
+GRID = TextureDesc(kind=TEX_GRID, count=5, width=0.08, a=[0.05, 0.05, 0.05], b=[0.7, 0.6, 0.5])
+SCALED = TextureDesc(kind=TEX_SCALE, scale=0.6, nested=TextureDesc(kind=TEX_CHECKERBOARD, count=3))
+ALPHA_CHECKER = TextureDesc(kind=TEX_CHECKERBOARD, count=4, a=[0.05, 0.05, 0.05], b=[0.4, 0.4, 0.4])
+ALPHA_GRID = TextureDesc(kind=TEX_GRID, count=6, width=0.1, a=[0.6, 0.6, 0.6], b=[0.15, 0.15, 0.15])
 
 
 def _cases():
@@ -87,6 +96,28 @@ def _cases():
         "rough_diffuse_rough": BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.9, 0.9, 0.9], alpha_u=0.8, alpha_v=0.8),
         "rough_diffuse_fast": BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.7, 0.5, 0.3], alpha_u=0.4, alpha_v=0.4,
                                        fast_approx=True),
+        # textured parameters (Record.Isect.UV drives Texture2D::Eval)
+        "tex_diffuse_checker": BSDFDesc(type=BSDF_DIFFUSE, textures={"kd": CHECKER}),
+        "tex_plastic_grid": BSDFDesc(type=BSDF_PLASTIC, kd=[0.3, 0.3, 0.3], textures={"kd": GRID, "ks": SCALED}),
+        "tex_rough_conductor_alpha": BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2,
+                                              int_ior=0.2, ext_ior=1.0, k=CU_K,
+                                              textures={"alpha_u": ALPHA_CHECKER, "ks": CHECKER}),
+        "tex_rough_conductor_aniso": BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=BECKMANN, anisotropic=True,
+                                              alpha_u=0.1, alpha_v=0.3, int_ior=0.2, ext_ior=1.0, k=CU_K,
+                                              textures={"alpha_u": ALPHA_CHECKER, "alpha_v": ALPHA_GRID}),
+        "tex_rough_dielectric": BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=0.1, alpha_v=0.1,
+                                         int_ior=1.5, ext_ior=1.0,
+                                         textures={"alpha_u": ALPHA_GRID, "ks_refract": CHECKER}),
+        "tex_rough_plastic": BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=0.15, alpha_v=0.15,
+                                      textures={"kd": CHECKER, "ks": GRID}),
+        "tex_coating_sigma": BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2,
+                                      thickness=0.5, nested=BSDFDesc(type=BSDF_DIFFUSE, textures={"kd": GRID}),
+                                      textures={"sigma_a": SCALED, "ks": CHECKER}),
+        "tex_smooth_coating": BSDFDesc(type=BSDF_COATING, nested=BSDFDesc(type=BSDF_DIFFUSE, textures={"kd": CHECKER}),
+                                       textures={"sigma_a": SCALED}),
+        "tex_rough_diffuse": BSDFDesc(type=BSDF_ROUGH_DIFFUSE, textures={"kd": GRID, "alpha_u": ALPHA_CHECKER}),
+        "tex_dielectric": BSDFDesc(type=BSDF_DIELECTRIC, textures={"ks": GRID, "ks_refract": SCALED}),
+        "tex_conductor": BSDFDesc(type=BSDF_CONDUCTOR, int_ior=0.27, ext_ior=1.0, k=CU_K, textures={"ks": CHECKER}),
     }
 
 
@@ -117,16 +148,27 @@ def test_oracle_bsdf_bit_exact_vs_reference(name):
     bid = o.add_bsdf(d)
     assert O.lib().ho_scene_finalize(o.h) == 0
 
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+
+    def mk_tex(t):
+        arrs = [f(t.uv_scale), f(t.uv_offset), f(t.a), f(t.b)]
+        keep.append(arrs)
+        nested = mk_tex(t.nested) if t.nested is not None else None
+        h = R.hr_texture_create(t.kind, t.count, t.width, t.scale, *[O._p(a) for a in arrs], nested)
+        assert h
+        return h
+
     def mk(b):
         if b is None:
             return None
-        f = lambda a: np.ascontiguousarray(a, np.float32)
         arrs = [f(b.k), f(b.ks), f(b.kd), f(b.sigma_a), f(b.ks_refract)]
         keep.append(arrs)
         k, ks, kd, sa, kr = arrs
+        tex = (C.c_void_p * 6)(*[mk_tex(b.textures[s]) if s in b.textures else None for s in TEX_SLOTS])
+        keep.append(tex)
         h = R.hr_bsdf_create(b.type, b.distribution, b.alpha_u, b.int_ior, b.ext_ior, O._p(k), O._p(ks), O._p(kd),
                              O._p(sa), b.thickness, mk(b.nested), mk(b.nested2), O._p(kr), int(b.nonlinear),
-                             int(b.fast_approx))
+                             int(b.fast_approx), tex, int(b.anisotropic))
         assert h
         return h
 
@@ -138,9 +180,10 @@ def test_oracle_bsdf_bit_exact_vs_reference(name):
         t = wi[5::10] * [-0.6, -0.6, 1]
         t[:, 2] = -np.sign(t[:, 2]) * np.sqrt(np.maximum(0, 1 - t[:, 0] ** 2 - t[:, 1] ** 2))
         wo[5::10] = t.astype(np.float32)
-    a = o.bsdf_batch(bid, wi, u2, u1, wo)
+    uv = (np.random.default_rng(3).random((n, 2)) * 4 - 1).astype(np.float32)   # texture coordinates
+    a = o.bsdf_batch(bid, wi, u2, u1, wo, uv=uv)
     b = {k: np.zeros_like(v) for k, v in a.items()}
-    R.hr_bsdf_batch(h, n, O._p(wi), O._p(u2), O._p(u1), O._p(wo), O._p(b["s_wo"]), O._p(b["s_w"]),
+    R.hr_bsdf_batch(h, n, O._p(wi), O._p(u2), O._p(u1), O._p(wo), O._p(uv), O._p(b["s_wo"]), O._p(b["s_w"]),
                     O._p(b["s_pdf"]), O._p(b["s_measure"]), O._p(b["e_rgb"]), O._p(b["p_pdf"]))
     valid = np.any(a["s_w"] != 0, axis=1)
     np.testing.assert_array_equal(a["s_w"], b["s_w"])
@@ -150,7 +193,9 @@ def test_oracle_bsdf_bit_exact_vs_reference(name):
     np.testing.assert_array_equal(a["e_rgb"], b["e_rgb"])
     np.testing.assert_array_equal(a["p_pdf"], b["p_pdf"])
     if _has_delta(d):
-        # Eval / Pdf on the sampled direction with the sampled measure (the delta lobes)
+        # Eval / Pdf on the sampled direction with the sampled measure (the delta lobes),
+        # at texture coordinates (0, 0) like the oracle's single-record queries
+        R.hr_set_uv(C.c_float(0.0), C.c_float(0.0))
         for i in range(0, 3000):
             m = int(a["s_measure"][i])
             wi_i, wo_i = np.ascontiguousarray(wi[i]), np.ascontiguousarray(a["s_wo"][i])
