@@ -358,7 +358,7 @@ def run_bsdf(args):
     P = hk._p
 
     def batch(bid):
-        hk.check(L.hk_bsdf_batch(gs.h, bid, n, P(wi), P(u2), P(u1), P(wo), P(out["s_wo"]), P(out["s_w"]),
+        hk.check(L.hk_bsdf_batch(gs.h, bid, n, P(wi), P(u2), P(u1), P(wo), None, P(out["s_wo"]), P(out["s_w"]),
                                  P(out["s_pdf"]), P(out["s_m"]), P(out["e_rgb"]), P(out["p_pdf"]), stream.cuda_stream))
 
     for _ in range(args.warmup):

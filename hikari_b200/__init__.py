@@ -14,7 +14,7 @@ from typing import Optional
 import numpy as np
 
 from . import scenedesc
-from .scenedesc import BSDFDesc, SceneDesc
+from .scenedesc import TEX_SLOTS, BSDFDesc, SceneDesc
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libhikari_b200.so")
@@ -34,7 +34,15 @@ class BsdfDesc(C.Structure):
         ("alpha_u", C.c_float), ("alpha_v", C.c_float), ("int_ior", C.c_float), ("ext_ior", C.c_float),
         ("eta", C.c_float * 3), ("k", C.c_float * 3), ("ks", C.c_float * 3), ("ks_refract", C.c_float * 3),
         ("kd", C.c_float * 3), ("sigma_a", C.c_float * 3), ("thickness", C.c_float), ("nested", C.c_int32),
-        ("nested2", C.c_int32), ("fast_approx", C.c_int32),
+        ("nested2", C.c_int32), ("fast_approx", C.c_int32), ("tex", C.c_int32 * 6),
+    ]
+
+
+class TextureDesc(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("nested", C.c_int32), ("count", C.c_int32), ("width", C.c_float),
+        ("scale", C.c_float), ("uv_scale", C.c_float * 2), ("uv_offset", C.c_float * 2), ("a", C.c_float * 3),
+        ("b", C.c_float * 3),
     ]
 
 
@@ -116,6 +124,7 @@ def lib():
         "hk_scene_add_mesh": ([P, P, C.c_uint32, P, C.c_uint32, P, I32, P, C.POINTER(I32)], C.c_int),
         "hk_scene_set_envmap": ([P, P, C.c_uint32, C.c_uint32, P, F], C.c_int),
         "hk_scene_set_constant_light": ([P, P], C.c_int),
+        "hk_scene_add_texture": ([P, C.POINTER(TextureDesc), C.POINTER(I32)], C.c_int),
         "hk_scene_set_mesh_uv": ([P, I32, P], C.c_int),
         "hk_obj_load": ([C.c_char_p, P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P, P, P, P, C.POINTER(I32)],
                         C.c_int),
@@ -152,7 +161,7 @@ def lib():
         "hk_job_preview": ([P, U64, P, C.c_double, C.POINTER(C.c_double)], C.c_int),
         "hk_server_get_stats": ([P, C.POINTER(ServerStats)], C.c_int),
         "hk_trace": ([P, U64, P, P, P, P, P, C.c_int, P, P], C.c_int),
-        "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
+        "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
         "hk_emitter_sample": ([P, I32, U64, P, P, P], C.c_int),
         "hk_camera_rays": ([P, U64, P, P, P], C.c_int),
         "hk_env_eval": ([P, U64, P, P, P, P], C.c_int),
@@ -193,7 +202,14 @@ def _stream(stream) -> Optional[int]:
     return getattr(stream, "cuda_stream", stream)
 
 
-def bsdf_desc_c(d: BSDFDesc, nested_id: int = -1, nested2_id: int = -1) -> BsdfDesc:
+def texture_desc_c(t, nested_id: int = -1) -> TextureDesc:
+    c = TextureDesc()
+    c.kind, c.nested, c.count, c.width, c.scale = t.kind, nested_id, t.count, t.width, t.scale
+    c.uv_scale[:], c.uv_offset[:], c.a[:], c.b[:] = t.uv_scale, t.uv_offset, t.a, t.b
+    return c
+
+
+def bsdf_desc_c(d: BSDFDesc, nested_id: int = -1, nested2_id: int = -1, tex_ids=None) -> BsdfDesc:
     c = BsdfDesc()
     c.type, c.distribution = d.type, d.distribution
     c.anisotropic, c.nonlinear = int(d.anisotropic), int(d.nonlinear)
@@ -202,6 +218,8 @@ def bsdf_desc_c(d: BSDFDesc, nested_id: int = -1, nested2_id: int = -1) -> BsdfD
     c.k[:], c.ks[:], c.ks_refract[:], c.kd[:], c.sigma_a[:] = d.k, d.ks, d.ks_refract, d.kd, d.sigma_a
     c.thickness, c.nested, c.nested2 = d.thickness, nested_id, nested2_id
     c.fast_approx = int(getattr(d, "fast_approx", False))
+    for k, t in enumerate(tex_ids or [-1] * 6):
+        c.tex[k] = t + 1
     return c
 
 
@@ -235,12 +253,25 @@ class Scene:
                 check(L.hk_scene_set_rft(h, dist, b, len(b)))
             ids = {}
 
+            tids = {}
+
+            def add_texture(t) -> int:
+                if id(t) in tids:
+                    return tids[id(t)]
+                nested = add_texture(t.nested) if t.nested is not None else -1
+                c = texture_desc_c(t, nested)
+                out = C.c_int32()
+                check(L.hk_scene_add_texture(h, C.byref(c), C.byref(out)))
+                tids[id(t)] = out.value
+                return out.value
+
             def add_bsdf(d: BSDFDesc) -> int:
                 if id(d) in ids:
                     return ids[id(d)]
                 nested = add_bsdf(d.nested) if d.nested is not None else -1
                 nested2 = add_bsdf(d.nested2) if d.nested2 is not None else -1
-                c = bsdf_desc_c(d, nested, nested2)
+                tex = d.textures or {}
+                c = bsdf_desc_c(d, nested, nested2, [add_texture(tex[k]) if k in tex else -1 for k in TEX_SLOTS])
                 out = C.c_int32()
                 check(L.hk_scene_add_bsdf(h, C.byref(c), C.byref(out)))
                 ids[id(d)] = out.value
@@ -447,7 +478,7 @@ class Scene:
                              _stream(stream)))
         return tri, t, u, v, visits
 
-    def bsdf_batch(self, bsdf_id: int, wi, u2, u1, wo, stream=None):
+    def bsdf_batch(self, bsdf_id: int, wi, u2, u1, wo, stream=None, uv=None):
         import torch
 
         n = wi.shape[0]
@@ -460,7 +491,7 @@ class Scene:
             e_rgb=torch.empty((n, 3), dtype=torch.float32, device=dev),
             p_pdf=torch.empty(n, dtype=torch.float32, device=dev),
         )
-        check(lib().hk_bsdf_batch(self.h, bsdf_id, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(out["s_wo"]),
+        check(lib().hk_bsdf_batch(self.h, bsdf_id, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(uv), _p(out["s_wo"]),
                                   _p(out["s_w"]), _p(out["s_pdf"]), _p(out["s_measure"]), _p(out["e_rgb"]),
                                   _p(out["p_pdf"]), _stream(stream)))
         return out

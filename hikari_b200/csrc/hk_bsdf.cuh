@@ -18,6 +18,8 @@ struct BRec {
     V3 wi, wo;
     float eta;
     int measure;
+    float tu, tv;   // texture coordinates of the intersection (Record.Isect.UV)
+    bool tex;       // textures are looked up (false in kernels that shade untextured materials only)
 };
 
 // ------------------------------------------------------------ microfacet
@@ -152,6 +154,56 @@ __device__ __forceinline__ float rft_eval(const DevBsdf &b, float c) {
 
 __device__ __forceinline__ V3 ld_rgb(const float *p) { return v3(p[0], p[1], p[2]); }
 
+// ------------------------------------------------------------ textures
+// Texture2D::Eval(Isect) (src/core/Texture.cpp:211): UV scaled and offset, then
+// CheckerboardTexture::Eval (src/texture/CheckerboardTexture.cpp:24) or
+// GridTexture::Eval (src/texture/GridTexture.cpp:26); ScaleTexture::Eval
+// (src/texture/ScaleTexture.cpp:17) scales its nested texture, innermost first.
+__device__ __forceinline__ int mod_positive(int a, int b) {
+    int q = a % b;
+    return q < 0 ? q + b : q;
+}
+__device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, float tv) {
+    float sc[4];
+    int ns = 0;
+    while (T[id].kind == kTexScale && ns < 4) {
+        sc[ns++] = T[id].scale;
+        id = T[id].nested;
+    }
+    const DevTexture &t = T[id];
+    const float u = tu * t.uv_scale[0] + t.uv_offset[0], v = tv * t.uv_scale[1] + t.uv_offset[1];
+    V3 c;
+    if (t.kind == kTexCheckerboard) {
+        bool ex = mod_positive(mod_positive((int)(u * t.count), t.count), 2) == 0;
+        bool ey = mod_positive(mod_positive((int)(v * t.count), t.count), 2) == 0;
+        c = (ex ^ ey) ? ld_rgb(t.a) : ld_rgb(t.b);
+    } else {
+        float su = u * (float)(t.count - 1), sv = v * (float)(t.count - 1);
+        float dx = su - floorf(su), dy = sv - floorf(sv);
+        if (dx > 0.5f) dx -= 1.0f;
+        if (dy > 0.5f) dy -= 1.0f;
+        c = (fabsf(dx) < t.width || fabsf(dy) < t.width) ? ld_rgb(t.a) : ld_rgb(t.b);
+    }
+    while (ns > 0) c = c * sc[--ns];
+    return c;
+}
+// A BSDF parameter at the query's intersection: its texture or its constant.
+// slot: 0 kd, 1 ks, 2 ks_refract, 3 sigma_a, 4 alpha(U), 5 alphaV
+__device__ __forceinline__ V3 par_rgb(const DevBsdf &b, int slot, const float *c, const BRec &r) {
+    if (r.tex) {
+        const int t = b.tex[slot];
+        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv);
+    }
+    return ld_rgb(c);
+}
+__device__ __forceinline__ float par_alpha(const DevBsdf &b, int slot, float c, const BRec &r) {
+    if (r.tex) {
+        const int t = b.tex[slot];
+        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv).x;
+    }
+    return c;
+}
+
 // ------------------------------------------------------------ diffuse
 // src/bsdf/DiffuseBSDF.cpp:20-67
 __device__ __forceinline__ V3 diffuse_sample(const DevBsdf &b, BRec &r, float ux, float uy) {
@@ -159,11 +211,11 @@ __device__ __forceinline__ V3 diffuse_sample(const DevBsdf &b, BRec &r, float ux
     r.measure = kMeasureSolidAngle;
     r.wo = square_to_cos_hemi(ux, uy);
     r.eta = 1.0f;
-    return ld_rgb(b.kd);
+    return par_rgb(b, 0, b.kd, r);
 }
 __device__ __forceinline__ V3 diffuse_eval(const DevBsdf &b, const BRec &r) {
     if (r.measure != kMeasureSolidAngle || r.wi.z <= 0 || r.wo.z <= 0) return v3(0, 0, 0);
-    return ld_rgb(b.kd) * (float)kInvPiD;
+    return par_rgb(b, 0, b.kd, r) * (float)kInvPiD;
 }
 __device__ __forceinline__ float diffuse_pdf(const BRec &r) {
     if (r.measure != kMeasureSolidAngle || r.wi.z <= 0 || r.wo.z <= 0) return 0.0f;
@@ -172,8 +224,9 @@ __device__ __forceinline__ float diffuse_pdf(const BRec &r) {
 
 // ------------------------------------------------------------ roughConductor
 // src/bsdf/RoughConductorBSDF.cpp:54-154
-__device__ __forceinline__ Mfd bsdf_mfd(const DevBsdf &b) {
-    return mfd_make(b.distribution, b.alpha_u, b.anisotropic ? b.alpha_v : b.alpha_u);
+__device__ __forceinline__ Mfd bsdf_mfd(const DevBsdf &b, const BRec &r) {
+    const float au = par_alpha(b, 4, b.alpha_u, r);
+    return mfd_make(b.distribution, au, b.anisotropic ? par_alpha(b, 5, b.alpha_v, r) : au);
 }
 __device__ __forceinline__ V3 conductor_fresnel(const DevBsdf &b, float c) {
     return v3(fresnel_conductor1(c, b.eta_c[0], b.k_c[0]), fresnel_conductor1(c, b.eta_c[1], b.k_c[1]),
@@ -183,7 +236,7 @@ __device__ __forceinline__ V3 conductor_sample(const DevBsdf &b, BRec &r, float 
     r.measure = kMeasureSolidAngle;
     float ci = r.wi.z;
     if (ci <= 0.0f) return v3(0, 0, 0);
-    Mfd d = bsdf_mfd(b);
+    Mfd d = bsdf_mfd(b, r);
     float pdf;
     V3 m = mfd_sample(d, ux, uy, pdf);
     if (pdf == 0.0f) return v3(0, 0, 0);
@@ -195,17 +248,18 @@ __device__ __forceinline__ V3 conductor_sample(const DevBsdf &b, BRec &r, float 
     float G = mfd_g(d, r.wi, r.wo, m);
     float D = mfd_eval(d, m);
     float den = pdf * r.wi.z;
-    return v3((((b.ks[0] * F.x) * D) * G) * mdw / den, (((b.ks[1] * F.y) * D) * G) * mdw / den,
-              (((b.ks[2] * F.z) * D) * G) * mdw / den);
+    const V3 ks = par_rgb(b, 1, b.ks, r);
+    return v3((((ks.x * F.x) * D) * G) * mdw / den, (((ks.y * F.y) * D) * G) * mdw / den,
+              (((ks.z * F.z) * D) * G) * mdw / den);
 }
 __device__ __forceinline__ V3 conductor_eval(const DevBsdf &b, const BRec &r) {
     float ci = r.wi.z, co = r.wo.z;
     if (r.measure != kMeasureSolidAngle || ci <= 0.0f || co <= 0.0f) return v3(0, 0, 0);
     V3 h = normalize(r.wi + r.wo);
-    Mfd d = bsdf_mfd(b);
+    Mfd d = bsdf_mfd(b, r);
     float D = mfd_eval(d, h);
     if (D == 0.0f) return v3(0, 0, 0);
-    V3 F = conductor_fresnel(b, dot(h, r.wi)) * ld_rgb(b.ks);
+    V3 F = conductor_fresnel(b, dot(h, r.wi)) * par_rgb(b, 1, b.ks, r);
     float G = mfd_g(d, r.wi, r.wo, h);
     float dg = D * G, den = 4.0f * ci;
     return v3(dg * F.x / den, dg * F.y / den, dg * F.z / den);
@@ -214,7 +268,7 @@ __device__ __forceinline__ float conductor_pdf(const DevBsdf &b, const BRec &r) 
     float ci = r.wi.z, co = r.wo.z;
     if (r.measure != kMeasureSolidAngle || ci <= 0.0f || co <= 0.0f) return 0.0f;
     V3 h = normalize(r.wi + r.wo);
-    Mfd d = bsdf_mfd(b);
+    Mfd d = bsdf_mfd(b, r);
     return mfd_pdf(d, h) / (4.0f * fabsf(dot(h, r.wo)));
 }
 
@@ -225,7 +279,7 @@ __device__ __forceinline__ V3 dielectric_sample(const DevBsdf &b, BRec &r, float
     r.measure = kMeasureSolidAngle;
     float ci = r.wi.z;
     if (ci == 0.0f) return v3(0, 0, 0);
-    Mfd d = bsdf_mfd(b);
+    Mfd d = bsdf_mfd(b, r);
     Mfd sd = d;
     float s = 1.2f - 0.2f * sqrtf(fabsf(ci));
     sd.au *= s;
@@ -241,14 +295,14 @@ __device__ __forceinline__ V3 dielectric_sample(const DevBsdf &b, BRec &r, float
         r.wo = reflect_m(r.wi, m);
         r.eta = 1.0f;
         if (r.wo.z * ci <= 0.0f) return v3(0, 0, 0);
-        W = ld_rgb(b.ks);
+        W = par_rgb(b, 1, b.ks, r);
     } else {
         if (ct == 0.0f) return v3(0, 0, 0);
         r.wo = refract_m(r.wi, m, ct, b.eta, b.inv_eta);
         r.eta = (ct < 0.0f ? b.eta : b.inv_eta);
         if (r.wo.z * ci >= 0.0f) return v3(0, 0, 0);
         float fac = (ct < 0.0f ? b.inv_eta : b.eta);
-        W = ld_rgb(b.ks_refract) * (fac * fac);
+        W = par_rgb(b, 2, b.ks_refract, r) * (fac * fac);
     }
     float v = fabsf(mfd_eval(d, m) * mfd_g(d, r.wi, r.wo, m) * dot(r.wi, m) / (pdf * ci));
     return W * v;
@@ -260,17 +314,17 @@ __device__ __forceinline__ V3 dielectric_eval(const DevBsdf &b, const BRec &r) {
     float e = ci > 0.0f ? b.eta : b.inv_eta;
     V3 h = refl ? normalize(r.wi + r.wo) : normalize(r.wi + r.wo * e);
     h = h * signum(h.z);
-    Mfd d = bsdf_mfd(b);
+    Mfd d = bsdf_mfd(b, r);
     float D = mfd_eval(d, h);
     if (D == 0.0f) return v3(0, 0, 0);
     float ct;
     float F = fresnel_dielectric(dot(r.wi, h), b.eta, b.inv_eta, ct);
     float G = mfd_g(d, r.wi, r.wo, h);
-    if (refl) return ld_rgb(b.ks) * (F * D * G / (4.0f * fabsf(ci)));
+    if (refl) return par_rgb(b, 1, b.ks, r) * (F * D * G / (4.0f * fabsf(ci)));
     float sd = dot(r.wi, h) + e * dot(r.wo, h);
     float val = ((1.0f - F) * D * G * e * e * dot(r.wi, h) * dot(r.wo, h)) / (ci * sd * sd);
     float fac = (ci < 0.0f ? b.inv_eta : b.eta);
-    return ld_rgb(b.ks_refract) * fabsf(val * fac * fac);
+    return par_rgb(b, 2, b.ks_refract, r) * fabsf(val * fac * fac);
 }
 __device__ __forceinline__ float dielectric_pdf(const DevBsdf &b, const BRec &r) {
     if (r.measure != kMeasureSolidAngle) return 0.0f;
@@ -289,7 +343,7 @@ __device__ __forceinline__ float dielectric_pdf(const DevBsdf &b, const BRec &r)
         J = (e * e * dot(r.wo, h)) / (sd * sd);
     }
     h = h * signum(h.z);
-    Mfd d = bsdf_mfd(b);
+    Mfd d = bsdf_mfd(b, r);
     float s = 1.2f - 0.2f * sqrtf(fabsf(ci));
     d.au *= s;
     d.av *= s;
@@ -311,8 +365,8 @@ __device__ __forceinline__ V3 plastic_eval(const DevBsdf &b, const BRec &r) {
     float F = fresnel_dielectric(dot(r.wi, h), b.eta, b.inv_eta, ct);
     float G = mfd_g(d, r.wi, r.wi, h);   // G(Wi, Wi, H) as the reference does (:146)
     float val = F * D * G / (4.0f * ci);
-    V3 res = ld_rgb(b.ks) * val;
-    V3 dif = ld_rgb(b.kd);
+    V3 res = par_rgb(b, 1, b.ks, r) * val;
+    V3 dif = par_rgb(b, 0, b.kd, r);
     float t12 = rft_eval(b, ci), t21 = rft_eval(b, co);
     float fdr = b.fdr_int;
     if (b.nonlinear) dif = v3(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
@@ -395,11 +449,11 @@ __device__ __forceinline__ V3 sconductor_sample(const DevBsdf &b, BRec &r) {
     V3 F = conductor_fresnel(b, ci);
     r.wo = reflect_n(r.wi);
     r.eta = 1.0f;
-    return ld_rgb(b.ks) * F;
+    return par_rgb(b, 1, b.ks, r) * F;
 }
 __device__ __forceinline__ V3 sconductor_eval(const DevBsdf &b, const BRec &r) {
     if (!mirror_match(r)) return v3(0, 0, 0);
-    return ld_rgb(b.ks) * conductor_fresnel(b, r.wi.z);
+    return par_rgb(b, 1, b.ks, r) * conductor_fresnel(b, r.wi.z);
 }
 
 // src/bsdf/DielectricBSDF.cpp:33-110 (Eval and Pdf test no measure)
@@ -410,12 +464,12 @@ __device__ __forceinline__ V3 sdielectric_sample(const DevBsdf &b, BRec &r, floa
     if (ux < F) {
         r.wo = reflect_n(r.wi);
         r.eta = 1.0f;
-        return ld_rgb(b.ks);
+        return par_rgb(b, 1, b.ks, r);
     }
     r.wo = refract_n(r.wi, ct, b.eta, b.inv_eta);
     r.eta = ct < 0.0f ? b.eta : b.inv_eta;
     float f = ct < 0.0f ? b.inv_eta : b.eta;   // radiance transport
-    return ld_rgb(b.ks_refract) * (f * f);
+    return par_rgb(b, 2, b.ks_refract, r) * (f * f);
 }
 // Eval and Pdf share the lobe test: 0 none, 1 reflection, 2 refraction with
 // cos(theta_t) < 0 (entering), 3 refraction leaving
@@ -433,10 +487,10 @@ __device__ __forceinline__ float sdielectric_lobe(const DevBsdf &b, const BRec &
 __device__ __forceinline__ V3 sdielectric_eval(const DevBsdf &b, const BRec &r) {
     int lobe;
     float F = sdielectric_lobe(b, r, lobe);
-    if (lobe == 1) return ld_rgb(b.ks) * F;
+    if (lobe == 1) return par_rgb(b, 1, b.ks, r) * F;
     if (lobe == 0) return v3(0, 0, 0);
     float f = lobe == 2 ? b.inv_eta : b.eta;
-    return (ld_rgb(b.ks_refract) * (f * f)) * (1.0f - F);
+    return (par_rgb(b, 2, b.ks_refract, r) * (f * f)) * (1.0f - F);
 }
 __device__ __forceinline__ float sdielectric_pdf(const DevBsdf &b, const BRec &r) {
     int lobe;
@@ -448,8 +502,8 @@ __device__ __forceinline__ float sdielectric_pdf(const DevBsdf &b, const BRec &r
 __device__ __forceinline__ float splastic_spec_pdf(const DevBsdf &b, float Fi) {
     return (Fi * b.spec_w) / (Fi * b.spec_w + (1.0f - Fi) * (1.0f - b.spec_w));
 }
-__device__ __forceinline__ V3 splastic_diffuse(const DevBsdf &b) {
-    V3 dif = ld_rgb(b.kd);
+__device__ __forceinline__ V3 splastic_diffuse(const DevBsdf &b, const BRec &r) {
+    V3 dif = par_rgb(b, 0, b.kd, r);
     float fdr = b.fdr_int;
     if (b.nonlinear) return v3(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
     return dif / (1.0f - fdr);
@@ -464,21 +518,21 @@ __device__ __forceinline__ V3 splastic_sample(const DevBsdf &b, BRec &r, float u
     if (ux < sp) {
         r.measure = kMeasureDiscrete;
         r.wo = reflect_n(r.wi);
-        return (ld_rgb(b.ks) * Fi) / sp;
+        return (par_rgb(b, 1, b.ks, r) * Fi) / sp;
     }
     r.measure = kMeasureSolidAngle;
     r.wo = square_to_cos_hemi((ux - sp) / (1.0f - sp), uy);
     float Fo = fresnel_dielectric(r.wo.z, b.eta, b.inv_eta, ct);
-    return splastic_diffuse(b) * (b.inv_eta2 * (1.0f - Fi) * (1.0f - Fo) / (1.0f - sp));
+    return splastic_diffuse(b, r) * (b.inv_eta2 * (1.0f - Fi) * (1.0f - Fo) / (1.0f - sp));
 }
 __device__ __forceinline__ V3 splastic_eval(const DevBsdf &b, const BRec &r) {
     float ci = r.wi.z, co = r.wo.z;
     if (r.measure == kMeasureUnknown || ci <= 0.0f || co <= 0.0f) return v3(0, 0, 0);
     float ct;
     float Fi = fresnel_dielectric(ci, b.eta, b.inv_eta, ct);
-    if (r.measure == kMeasureDiscrete) return delta_match(reflect_n(r.wi), r.wo) ? ld_rgb(b.ks) * Fi : v3(0, 0, 0);
+    if (r.measure == kMeasureDiscrete) return delta_match(reflect_n(r.wi), r.wo) ? par_rgb(b, 1, b.ks, r) * Fi : v3(0, 0, 0);
     float Fo = fresnel_dielectric(co, b.eta, b.inv_eta, ct);
-    return splastic_diffuse(b) * (cos_hemi_pdf(r.wo) * b.inv_eta2 * (1.0f - Fi) * (1.0f - Fo));
+    return splastic_diffuse(b, r) * (cos_hemi_pdf(r.wo) * b.inv_eta2 * (1.0f - Fi) * (1.0f - Fo));
 }
 __device__ __forceinline__ float splastic_pdf(const DevBsdf &b, const BRec &r) {
     float ci = r.wi.z, co = r.wo.z;
@@ -513,7 +567,7 @@ __device__ __forceinline__ float frame_cos_phi(V3 v) {   // :78
 __device__ __forceinline__ V3 roughdiffuse_eval(const DevBsdf &b, const BRec &r) {
     float ci = r.wi.z, co = r.wo.z;
     if (ci <= 0.0f || co <= 0.0f || r.measure != kMeasureSolidAngle) return v3(0, 0, 0);
-    float sigma = clampf(b.alpha_u, 5e-4f, 1.0f) * 0.70710678118655f;
+    float sigma = clampf(par_alpha(b, 4, b.alpha_u, r), 5e-4f, 1.0f) * 0.70710678118655f;
     float s2 = sigma * sigma;
     float sti = frame_sin_theta(r.wi), sto = frame_sin_theta(r.wo);
     float cpd = 0.0f;
@@ -529,7 +583,7 @@ __device__ __forceinline__ V3 roughdiffuse_eval(const DevBsdf &b, const BRec &r)
         float sa, tb;
         if (ci > co) { sa = sto; tb = sti / ci; }
         else { sa = sti; tb = sto / co; }
-        return ld_rgb(b.kd) * (inv_pi * co * (A + B * max_f(cpd, 0.0f) * sa * tb));
+        return par_rgb(b, 0, b.kd, r) * (inv_pi * co * (A + B * max_f(cpd, 0.0f) * sa * tb));
     }
     float thi = safe_acos(ci), tho = safe_acos(co);
     float al = max_f(thi, tho), be = min_f(thi, tho);
@@ -547,7 +601,7 @@ __device__ __forceinline__ V3 roughdiffuse_eval(const DevBsdf &b, const BRec &r)
     else C2 *= sa - t3 * t3 * t3;
     float th = (sa + sb) / (safe_sqrt(1.0f - sa * sa) + safe_sqrt(1.0f - sb * sb));
     if (isinf(th) || isnan(th)) return v3(0, 0, 0);
-    V3 rho = ld_rgb(b.kd);
+    V3 rho = par_rgb(b, 0, b.kd, r);
     V3 lr1 = rho * (C1 + cpd * C2 * tb + (1.0f - fabsf(cpd)) * C3 * th);
     V3 lr2 = (rho * rho) * (C4 * (1.0f - cpd * t3 * t3));
     return (lr1 + lr2) * (inv_pi * co);
@@ -626,14 +680,15 @@ __device__ __forceinline__ V3 coating_eval(const DevBsdf &b, const DevBsdf &nb, 
     float F = fresnel_dielectric(fabsf(dot(r.wi, h)), b.eta, b.inv_eta, ct);
     float G = mfd_g(d, r.wi, r.wo, h);
     float den = 4.0f * fabsf(ci);
-    V3 res = v3((((b.ks[0] * F) * D) * G) / den, (((b.ks[1] * F) * D) * G) / den, (((b.ks[2] * F) * D) * G) / den);
+    const V3 ks = par_rgb(b, 1, b.ks, r);
+    V3 res = v3((((ks.x * F) * D) * G) / den, (((ks.y * F) * D) * G) / den, (((ks.z * F) * D) * G) / den);
     BRec ri = r;
     ri.wi = coat_refract(r.wi, b.inv_eta);
     ri.wo = coat_refract(r.wo, b.inv_eta);
     V3 nv = leaf_eval(nb, ri);
     float ti = rft_eval(b, fabsf(ci)), to = rft_eval(b, fabsf(co));
     nv = v3(nv.x * ti * to, nv.y * ti * to, nv.z * ti * to);
-    V3 sa = ld_rgb(b.sigma_a) * b.thickness;
+    V3 sa = par_rgb(b, 3, b.sigma_a, r) * b.thickness;
     if (!is_zero(sa)) {
         float q = 1.0f / fabsf(ri.wi.z) + 1.0f / fabsf(ri.wo.z);
         nv = nv * v3(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q));
@@ -701,8 +756,8 @@ __device__ __forceinline__ V3 scoat_refract_out(const DevBsdf &b, V3 wi, float &
     R = fresnel_dielectric(fabsf(wi.z), b.inv_eta, b.eta, ct);
     return v3(b.eta * wi.x, b.eta * wi.y, -signum(wi.z) * ct);
 }
-__device__ __forceinline__ V3 scoat_absorb(const DevBsdf &b, V3 res, V3 wi_int, V3 wo_int) {
-    V3 sa = ld_rgb(b.sigma_a) * b.thickness;
+__device__ __forceinline__ V3 scoat_absorb(const DevBsdf &b, const BRec &r, V3 res, V3 wi_int, V3 wo_int) {
+    V3 sa = par_rgb(b, 3, b.sigma_a, r) * b.thickness;
     if (is_zero(sa)) return res;
     float q = 1.0f / fabsf(wi_int.z) + 1.0f / fabsf(wo_int.z);
     return res * v3(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q));
@@ -718,7 +773,7 @@ __device__ __forceinline__ V3 scoating_sample(const DevBsdf &b, const DevBsdf &n
         r.wo = reflect_n(r.wi);
         r.eta = 1.0f;
         r.measure = kMeasureDiscrete;
-        return ld_rgb(b.ks) * (R12 / sp);
+        return par_rgb(b, 1, b.ks, r) * (R12 / sp);
     }
     ux = (ux - sp) / (1.0f - sp);
     if (R12 == 1.0f) return v3(0, 0, 0);
@@ -728,7 +783,7 @@ __device__ __forceinline__ V3 scoating_sample(const DevBsdf &b, const DevBsdf &n
     r.wi = wib;
     if (is_zero(res)) return v3(0, 0, 0);
     V3 wop = r.wo;
-    res = scoat_absorb(b, res, wip, wop);
+    res = scoat_absorb(b, r, res, wip, wop);
     float R21;
     r.wo = scoat_refract_out(b, wop, R21);
     if (R21 == 1.0f) return v3(0, 0, 0);
@@ -739,7 +794,7 @@ __device__ __forceinline__ V3 scoating_eval(const DevBsdf &b, const DevBsdf &nb,
     if (r.measure == kMeasureDiscrete) {
         if (!delta_match(reflect_n(r.wi), r.wo)) return v3(0, 0, 0);
         float ct;
-        return ld_rgb(b.ks) * fresnel_dielectric(fabsf(r.wi.z), b.eta, b.inv_eta, ct);
+        return par_rgb(b, 1, b.ks, r) * fresnel_dielectric(fabsf(r.wi.z), b.eta, b.inv_eta, ct);
     }
     float R12, R21;
     BRec ri = r;
@@ -747,7 +802,7 @@ __device__ __forceinline__ V3 scoating_eval(const DevBsdf &b, const DevBsdf &nb,
     ri.wo = scoat_refract_in(b, r.wo, R21);
     if (R12 == 1.0f || R21 == 1.0f) return v3(0, 0, 0);
     V3 res = (leaf_eval(nb, ri) * (1.0f - R12)) * (1.0f - R21);
-    res = scoat_absorb(b, res, ri.wi, ri.wo);
+    res = scoat_absorb(b, r, res, ri.wi, ri.wo);
     if (r.measure == kMeasureSolidAngle) res = res * (b.inv_eta * b.inv_eta * r.wo.z / ri.wo.z);
     return res;
 }

@@ -22,6 +22,7 @@ constexpr int kRftThetaMax = 100;   // data/*RFTData.bin hold 100 theta samples
 // One activated BSDF: constant-texture parameters plus the 1D rough
 // transmittance table reduced at activation (RoughTransmittance::SetEta then
 // SetAlpha, src/core/RoughTransmitance.cpp:170,237).
+struct DevTexture;
 struct alignas(16) DevBsdf {
     int32_t type, distribution, anisotropic, nonlinear;
     float alpha_u, alpha_v;          // clamped to [MIN_ALPHA, MAX_ALPHA]
@@ -36,7 +37,23 @@ struct alignas(16) DevBsdf {
     int32_t rft_n;                   // theta samples in rft[]
     int32_t nested2;                 // twoSided back BSDF index (the front one when only one is given)
     int32_t fast_approx;             // roughDiffuse: the fast Oren-Nayar approximation
+    // textures of kd, ks, ks_refract, sigma_a, alpha_u, alpha_v: 1 + index into
+    // textures, 0 = the constant above; textured: any slot here or in a nested BSDF
+    int32_t tex[6];
+    const DevTexture *textures;
+    int32_t textured;
+    int32_t pad2, pad3, pad4;
     float rft[kRftThetaMax];
+};
+
+// Procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp).
+enum TexKind : int32_t { kTexCheckerboard = 1, kTexGrid = 2, kTexScale = 3 };
+struct alignas(16) DevTexture {
+    int32_t kind, nested, count;     // nested: the scaled texture; count: blocks / lines
+    float width, scale;              // grid line width; scale factor
+    float uv_scale[2], uv_offset[2];
+    float a[3], b[3];                // colorA / lineColor, colorB / backgroundColor
+    float pad;
 };
 
 // Per-mesh shading data.

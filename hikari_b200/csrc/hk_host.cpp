@@ -202,6 +202,7 @@ struct MeshIn {
 struct hk_scene {
     // inputs
     std::vector<hk_bsdf_desc> bsdfs;
+    std::vector<hk_texture_desc> textures;
     std::vector<MeshIn> meshes;
     std::vector<int> emitter_mesh;   // Scene order: mesh id, -1 environment, -2 - k delta_lights[k]
     struct DeltaLight { int directional; float color[3], vec[3]; };
@@ -226,7 +227,7 @@ struct hk_scene {
     hk::DevScene dev{};
     int32_t accel = HK_ACCEL_BVH8;
     DevBuf b_tris, b_nodes, b_wnodes, b_tri_normals, b_tri_uv, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
-        b_light_cdf, b_delta, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
+        b_light_cdf, b_delta, b_textures, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
     DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
     std::vector<std::unique_ptr<DevBuf>> batch_films;   // films of hk_render_batch_host
     hk_scene_info info{};
@@ -293,10 +294,48 @@ bool bsdf_transmits(const hk_scene *s, int id, int depth) {
     }
 }
 
+// Texture::GetAverage of the procedural textures (CheckerboardTexture.cpp:30,
+// GridTexture.cpp:40, ScaleTexture.cpp:28), used when BSDFs activate
+F3 tex_average(const std::vector<hk_texture_desc> &T, int id) {
+    const hk_texture_desc &t = T[id];
+    if (t.kind == HK_TEX_SCALE) {
+        F3 c = tex_average(T, t.nested);
+        return {c.x * t.scale, c.y * t.scale, c.z * t.scale};
+    }
+    if (t.kind == HK_TEX_CHECKERBOARD)
+        return {(t.a[0] + t.b[0]) * 0.5f, (t.a[1] + t.b[1]) * 0.5f, (t.a[2] + t.b[2]) * 0.5f};
+    float iw = std::max(0.0f, 1.0f - 2.0f * t.width);
+    float ia = iw * iw, la = 1.0f - ia;
+    return {t.a[0] * la + t.b[0] * ia, t.a[1] * la + t.b[1] * ia, t.a[2] * la + t.b[2] * ia};
+}
+// A parameter's average: its texture's or the constant
+void par_average(const hk_scene *s, const hk_bsdf_desc &d, int slot, const float *c, float *out) {
+    if (!d.tex[slot]) {
+        for (int k = 0; k < 3; k++) out[k] = c[k];
+        return;
+    }
+    F3 a = tex_average(s->textures, d.tex[slot] - 1);
+    out[0] = a.x; out[1] = a.y; out[2] = a.z;
+}
+bool bsdf_textured(const hk_scene *s, int id, int depth) {
+    if (id < 0 || id >= (int)s->bsdfs.size() || depth > 8) return false;
+    const hk_bsdf_desc &d = s->bsdfs[id];
+    for (int k = 0; k < 6; k++)
+        if (d.tex[k]) return true;
+    return bsdf_textured(s, (d.type == hk::kRoughCoating || d.type == hk::kCoating || d.type == hk::kTwoSided) ? d.nested : -1, depth + 1) ||
+           bsdf_textured(s, d.type == hk::kTwoSided ? d.nested2 : -1, depth + 1);
+}
+
 hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs) {
     hk::DevBsdf b;
     std::memset(&b, 0, sizeof b);
     if (d.type < hk::kDiffuse || d.type > hk::kRoughDiffuse) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+    for (int k = 0; k < 6; k++) {
+        if (d.tex[k] < 0 || d.tex[k] > (int)s->textures.size()) throw HkError{HK_ERR_INVALID, "invalid texture id"};
+        b.tex[k] = d.tex[k];
+    }
+    if ((d.type == hk::kRoughPlastic || d.type == hk::kRoughCoating) && d.tex[4])
+        throw HkError{HK_ERR_INVALID, "textured alpha of roughPlastic / roughCoating is not supported"};
     if (d.distribution != 0 && d.distribution != 1) throw HkError{HK_ERR_INVALID, "Unexpected distribution type"};
     b.type = d.type;
     b.distribution = d.distribution;
@@ -332,15 +371,20 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
         t.set_alpha(t2d, d1d, alpha, b.rft, dsc);
         b.rft_n = (int)t.theta_n;
         if (d.type == hk::kRoughPlastic) {
-            float ksa = lum(d.ks), kda = lum(d.kd);
+            float ksv[3], kdv[3];
+            par_average(s, d, 1, d.ks, ksv);
+            par_average(s, d, 0, d.kd, kdv);
+            float ksa = lum(ksv), kda = lum(kdv);
             b.spec_w = ksa / (kda + ksa);
             t.set_eta(b.inv_eta, t2d, d1d);   // m_pIntData: SetEta(1/eta) only
             float wa = std::pow((alpha - t.alpha_min) / (t.alpha_max - t.alpha_min), 0.25f);
             b.fdr_int = 1.0f - clampf(cubic1d(wa, d1d.data(), (int)t.alpha_n, 0.0f, 1.0f), 0.0f, 1.0f);
         } else {
             float th = d.thickness;
-            float a0 = std::exp(d.sigma_a[0] * (-2.0f * th)), a1 = std::exp(d.sigma_a[1] * (-2.0f * th)),
-                  a2 = std::exp(d.sigma_a[2] * (-2.0f * th));
+            float sav[3];
+            par_average(s, d, 3, d.sigma_a, sav);
+            float a0 = std::exp(sav[0] * (-2.0f * th)), a1 = std::exp(sav[1] * (-2.0f * th)),
+                  a2 = std::exp(sav[2] * (-2.0f * th));
             b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
             if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
             const int nt = s->bsdfs[d.nested].type;
@@ -350,8 +394,10 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
     }
     if (d.type == hk::kCoating) {   // CoatingBSDF::Activate (:255)
         float th = d.thickness;
-        float a0 = std::exp(d.sigma_a[0] * (-2.0f * th)), a1 = std::exp(d.sigma_a[1] * (-2.0f * th)),
-              a2 = std::exp(d.sigma_a[2] * (-2.0f * th));
+        float sav[3];
+            par_average(s, d, 3, d.sigma_a, sav);
+            float a0 = std::exp(sav[0] * (-2.0f * th)), a1 = std::exp(sav[1] * (-2.0f * th)),
+              a2 = std::exp(sav[2] * (-2.0f * th));
         b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
         if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "CoatingBSDF needs a nested BSDF!"};
         const int nt = s->bsdfs[d.nested].type;
@@ -361,7 +407,10 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
     if (d.type == hk::kConductor)   // ConductorBSDF ctor (:17): m_Eta = Color3f(intIOR / extIOR)
         for (int c = 0; c < 3; c++) b.eta_c[c] = b.eta;
     if (d.type == hk::kPlastic) {   // PlasticBSDF ctor (:25) and Activate (:170)
-        float ksa = lum(d.ks), kda = lum(d.kd);
+        float ksv[3], kdv[3];
+        par_average(s, d, 1, d.ks, ksv);
+        par_average(s, d, 0, d.kd, kdv);
+        float ksa = lum(ksv), kda = lum(kdv);
         b.spec_w = ksa / (kda + ksa);
         b.fdr_int = approx_fresnel_diffuse(b.inv_eta);
     }
@@ -389,7 +438,21 @@ void build_scene(hk_scene *s) {
 
     // BSDFs
     std::vector<hk::DevBsdf> bs;
+    std::vector<hk::DevTexture> tex;
+    for (auto &t : s->textures) {
+        hk::DevTexture x;
+        std::memset(&x, 0, sizeof x);
+        x.kind = t.kind; x.nested = t.nested; x.count = t.count; x.width = t.width; x.scale = t.scale;
+        for (int k = 0; k < 2; k++) { x.uv_scale[k] = t.uv_scale[k]; x.uv_offset[k] = t.uv_offset[k]; }
+        for (int k = 0; k < 3; k++) { x.a[k] = t.a[k]; x.b[k] = t.b[k]; }
+        tex.push_back(x);
+    }
+    s->b_textures.upload(tex); track(s->b_textures);
     for (auto &d : s->bsdfs) bs.push_back(activate_bsdf(s, d, (int)s->bsdfs.size()));
+    for (size_t i = 0; i < bs.size(); ++i) {
+        bs[i].textures = s->b_textures.as<hk::DevTexture>();
+        bs[i].textured = bsdf_textured(s, (int)i, 0) ? 1 : 0;
+    }
     s->b_bsdfs.upload(bs); track(s->b_bsdfs);
     D.bsdfs = s->b_bsdfs.as<hk::DevBsdf>();
     D.nbsdfs = (int)bs.size();
@@ -763,6 +826,20 @@ int hk_scene_set_rft(hk_scene *s, int distribution, const void *bytes, uint64_t 
     return guarded([&] {
         if (!s || !bytes || (distribution != 0 && distribution != 1)) throw HkError{HK_ERR_INVALID, "bad arguments"};
         s->rft[distribution].parse(bytes, nbytes);
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_add_texture(hk_scene *s, const hk_texture_desc *d, int32_t *out_id) {
+    return guarded([&] {
+        if (!s || !d) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (d->kind < HK_TEX_CHECKERBOARD || d->kind > HK_TEX_SCALE) throw HkError{HK_ERR_INVALID, "unknown texture kind"};
+        if (d->kind == HK_TEX_SCALE && (d->nested < 0 || d->nested >= (int)s->textures.size()))
+            throw HkError{HK_ERR_INVALID, "scale texture needs a nested texture"};
+        if (d->kind != HK_TEX_SCALE && d->count <= 0)
+            throw HkError{HK_ERR_INVALID, "texture block / line count must be positive"};
+        s->textures.push_back(*d);
+        if (out_id) *out_id = (int32_t)s->textures.size() - 1;
         s->built = false;
         return HK_OK;
     });
@@ -1279,15 +1356,15 @@ int hk_trace(hk_scene *s, uint64_t n, const float *rays, int32_t *tri, float *t,
     });
 }
 int hk_bsdf_batch(hk_scene *s, int32_t bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
-                  const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb, float *p_pdf,
-                  void *stream) {
+                  const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
+                  float *p_pdf, void *stream) {
     return guarded([&] {
         require_built(s);
         if (bsdf < 0 || bsdf >= s->dev.nbsdfs) throw HkError{HK_ERR_INVALID, "invalid BSDF id"};
         if (n == 0) return HK_OK;
         if (!wi || !u2 || !wo) throw HkError{HK_ERR_INVALID, "bad arguments"};
-        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, s->bsdfs[bsdf].type, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf,
-                                      (cudaStream_t)stream));
+        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, s->bsdfs[bsdf].type, n, wi, u2, u1, wo, uv, s_wo, s_w, s_pdf, s_m,
+                                      e_rgb, p_pdf, (cudaStream_t)stream));
         return HK_OK;
     });
 }

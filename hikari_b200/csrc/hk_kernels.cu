@@ -80,6 +80,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
                     br.wo = to_local(it.sh, er.wi);
                     br.measure = kMeasureSolidAngle;
                     br.eta = 0.0f;
+                    br.tu = it.u; br.tv = it.v; br.tex = true;
                     float pb = bsdf_pdf(S.bsdfs, bsdf, br);
                     if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
                     V3 f = bsdf_eval(S.bsdfs, bsdf, br);
@@ -94,6 +95,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
         br.wo = v3(0, 0, 0);
         br.measure = kMeasureUnknown;
         br.eta = 0.0f;
+        br.tu = it.u; br.tv = it.v; br.tex = true;
         float sx = rng.nextf(), sy = rng.nextf();
         float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
         V3 F = bsdf_sample(S.bsdfs, bsdf, br, sx, sy, u1);
@@ -283,16 +285,19 @@ __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int
 // direction, measure), Eval and Pdf at the given wo with ESolidAngle.
 // One instantiation per top-level BSDF type (the host picks the id's type),
 // so a launch carries only that BSDF's code.
-template <int BT>
+template <int BT, bool kTex>
 __global__ void bsdf_batch_kernel(DevScene S, int bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
-                                  const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
-                                  float *p_pdf) {
+                                  const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf,
+                                  int32_t *s_m, float *e_rgb, float *p_pdf) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         BRec r;
         r.wi = v3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
         r.wo = v3(0, 0, 0);
         r.measure = kMeasureUnknown;
         r.eta = 0.0f;
+        r.tex = kTex;
+        r.tu = kTex ? uv[2 * i] : 0.0f;
+        r.tv = kTex ? uv[2 * i + 1] : 0.0f;
         V3 w = bsdf_sample_t<BT>(S.bsdfs, bsdf, r, u2[2 * i], u2[2 * i + 1], u1 ? u1[i] : 0.0f);
         if (s_wo) { s_wo[3 * i] = r.wo.x; s_wo[3 * i + 1] = r.wo.y; s_wo[3 * i + 2] = r.wo.z; }
         if (s_w) { s_w[3 * i] = w.x; s_w[3 * i + 1] = w.y; s_w[3 * i + 2] = w.z; }
@@ -303,6 +308,9 @@ __global__ void bsdf_batch_kernel(DevScene S, int bsdf, uint64_t n, const float 
         q.wo = v3(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
         q.measure = kMeasureSolidAngle;
         q.eta = 0.0f;
+        q.tex = kTex;
+        q.tu = r.tu;
+        q.tv = r.tv;
         if (e_rgb) {
             V3 e = bsdf_eval_t<BT>(S.bsdfs, bsdf, q);
             e_rgb[3 * i] = e.x; e_rgb[3 * i + 1] = e.y; e_rgb[3 * i + 2] = e.z;
@@ -401,11 +409,14 @@ cudaError_t launch_trace(const DevScene &S, uint64_t n, const float *rays, int32
     return cudaGetLastError();
 }
 cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, int type, uint64_t n, const float *wi, const float *u2, const float *u1,
-                              const float *wo, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
-                              float *p_pdf, cudaStream_t st) {
+                              const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m,
+                              float *e_rgb, float *p_pdf, cudaStream_t st) {
     const int g = grid_for(n, 256);
-#define HK_BSDF_BATCH(T) \
-    case T: bsdf_batch_kernel<T><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); break
+#define HK_BSDF_BATCH(T)                                                                                          \
+    case T:                                                                                                       \
+        if (uv) bsdf_batch_kernel<T, true><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, uv, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); \
+        else bsdf_batch_kernel<T, false><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, uv, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); \
+        break
     switch (type) {
         HK_BSDF_BATCH(kDiffuse);
         HK_BSDF_BATCH(kRoughConductor);

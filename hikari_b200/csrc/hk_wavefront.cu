@@ -269,7 +269,8 @@ __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, i
             int type = 0;
             if (w.found) {
                 const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
-                type = wf_queue_of(S.bsdfs[S.meshes[mesh].bsdf].type);
+                const DevBsdf &B = S.bsdfs[S.meshes[mesh].bsdf];
+                type = B.textured ? kWfGenericQueue : wf_queue_of(B.type);
             }
             W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
             W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
@@ -345,6 +346,13 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                         pb.wo = v3(pwo.x, pwo.y, pwo.z);
                         pb.measure = __float_as_int(pwo.w);
                         pb.eta = 0.0f;
+                        pb.tex = S.bsdfs[__float_as_int(pwi.w)].textured != 0;
+                        pb.tu = pb.tv = 0.0f;
+                        if (pb.tex) {
+                            const float2 puv = W.prev_uv[slot];
+                            pb.tu = puv.x;
+                            pb.tv = puv.y;
+                        }
                         float plm = area_pdf(AL, er);
                         float pbm = bsdf_pdf(S.bsdfs, __float_as_int(pwi.w), pb);
                         if (pbm + plm != 0.0f) w_mats = pbm / (pbm + plm);
@@ -369,6 +377,9 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                 br.wo = to_local(it.sh, er.wi);
                 br.measure = kMeasureSolidAngle;
                 br.eta = 0.0f;
+                br.tex = BT < 0;   // textured materials are shaded by the run-time-dispatched kernel
+                br.tu = it.u;
+                br.tv = it.v;
                 float pl = er.pdf;
                 float pb = bsdf_pdf_t<BT>(S.bsdfs, bsdf, br);
                 float w = (pl + pb != 0.0f) ? pl / (pl + pb) : 1.0f;
@@ -390,6 +401,9 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             br.wo = v3(0, 0, 0);
             br.measure = kMeasureUnknown;
             br.eta = 0.0f;
+            br.tex = BT < 0;
+            br.tu = it.u;
+            br.tv = it.v;
             float sx = rng.nextf(), sy = rng.nextf();
             float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
             V3 F = bsdf_sample_t<BT>(S.bsdfs, bsdf, br, sx, sy, u1);
@@ -416,6 +430,9 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             W.pix[slot] = make_float4(p4.x, p4.y, p4.z, __int_as_float((int)((flags << 16) | (uint32_t)depth)));
             W.prev_wi[slot] = f4(br.wi, __int_as_float(bsdf));
             W.prev_wo[slot] = f4(br.wo, __int_as_float(br.measure));
+            if constexpr (BT < 0) {
+                if (S.bsdfs[bsdf].textured) W.prev_uv[slot] = make_float2(it.u, it.v);
+            }
             W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
                                      (uint32_t)(rng.inc >> 32));
             W.eq[nxt][warp_append(&W.ctr->eq_count[nxt])] = slot;

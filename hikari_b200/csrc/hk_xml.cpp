@@ -38,6 +38,7 @@ const char *class_name(EClassType t) {
     case EClassType::EReconstructionFilter: return "rfilter";
     case EClassType::EAcceleration: return "acceleration";
     case EClassType::ETest: return "test";
+    case EClassType::ETexture: return "texture";
     }
     return "unknown";
 }
@@ -268,7 +269,7 @@ const std::map<std::string, EClassType> &object_tags() {
         {"scene", EClassType::EScene}, {"mesh", EClassType::EMesh}, {"bsdf", EClassType::EBSDF},
         {"emitter", EClassType::EEmitter}, {"camera", EClassType::ECamera}, {"integrator", EClassType::EIntegrator},
         {"sampler", EClassType::ESampler}, {"rfilter", EClassType::EReconstructionFilter},
-        {"acceleration", EClassType::EAcceleration}, {"test", EClassType::ETest}};
+        {"acceleration", EClassType::EAcceleration}, {"test", EClassType::ETest}, {"texture", EClassType::ETexture}};
     return m;
 }
 const std::map<std::string, Tag> &prop_tags() {
@@ -602,6 +603,76 @@ std::string resolve(const std::string &f) {
     return g_base_dir + "/" + f;
 }
 
+// Texture plugins (src/texture/{Checkerboard,Grid,Scale}Texture.cpp): the
+// procedural textures, defaults of include/core/Common.hpp:436-458
+class TexturePlugin : public Object {
+public:
+    hk_texture_desc d{};
+    std::unique_ptr<TexturePlugin> nested;
+    TexturePlugin(const PropertyList &p, int kind) {
+        std::memset(&d, 0, sizeof d);
+        d.kind = kind;
+        d.nested = -1;
+        d.uv_scale[0] = p.GetFloat("uScale", 1.0f);
+        d.uv_scale[1] = p.GetFloat("vScale", 1.0f);
+        d.uv_offset[0] = p.GetFloat("uOffset", 0.0f);
+        d.uv_offset[1] = p.GetFloat("vOffset", 0.0f);
+        auto setc = [](float *dst, const Color3f &c) { dst[0] = c[0]; dst[1] = c[1]; dst[2] = c[2]; };
+        if (kind == HK_TEX_CHECKERBOARD) {
+            d.count = p.GetInteger("blocks", 10);
+            setc(d.a, p.GetColor("colorA", {0.4f, 0.4f, 0.4f}));
+            setc(d.b, p.GetColor("colorB", {0.2f, 0.2f, 0.2f}));
+        } else if (kind == HK_TEX_GRID) {
+            d.count = p.GetInteger("lines", 10);
+            setc(d.a, p.GetColor("lineColor", {0.4f, 0.4f, 0.4f}));
+            setc(d.b, p.GetColor("backgroundColor", {0.2f, 0.2f, 0.2f}));
+            d.width = p.GetFloat("lineWidth", 0.01f);
+        } else {
+            d.scale = p.GetFloat("scale");
+        }
+        if (kind != HK_TEX_SCALE && d.count <= 0) throw HikariException("texture block / line count must be positive");
+    }
+    EClassType GetClassType() const override { return EClassType::ETexture; }
+    void AddChild(Object *c, const std::string &name) override {
+        if (d.kind == HK_TEX_SCALE && c->GetClassType() == EClassType::ETexture && !nested) {
+            nested.reset((TexturePlugin *)c);
+            return;
+        }
+        delete c;
+        throw HikariException("ScaleTexture: tried to specify multiple nested textures");
+    }
+    void Activate() override {
+        if (d.kind == HK_TEX_SCALE && !nested) throw HikariException("ScaleTexture needs a nested texture");
+    }
+};
+struct CheckerboardTexture : TexturePlugin { CheckerboardTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_CHECKERBOARD) {} };
+struct GridTexture : TexturePlugin { GridTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_GRID) {} };
+struct ScaleTexture : TexturePlugin { ScaleTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_SCALE) {} };
+HK_REGISTER_CLASS(CheckerboardTexture, "checkerboard")
+HK_REGISTER_CLASS(GridTexture, "grid")
+HK_REGISTER_CLASS(ScaleTexture, "scale")
+
+// The texture slot (hk_bsdf_desc.tex) of a named BSDF texture child, -1 if the
+// BSDF takes no texture of that name (the plugins' AddChild)
+int texture_slot(int type, const std::string &name) {
+    switch (type) {
+    case HK_BSDF_DIFFUSE: return name == "albedo" ? 0 : -1;
+    case HK_BSDF_ROUGH_DIFFUSE: return name == "albedo" ? 0 : (name == "alpha" ? 4 : -1);
+    case HK_BSDF_CONDUCTOR: return name == "ks" ? 1 : -1;
+    case HK_BSDF_DIELECTRIC: return name == "ksReflect" ? 1 : (name == "ksRefract" ? 2 : -1);
+    case HK_BSDF_PLASTIC:
+    case HK_BSDF_ROUGH_PLASTIC: return name == "kd" ? 0 : (name == "ks" ? 1 : -1);
+    case HK_BSDF_ROUGH_CONDUCTOR:
+        return name == "ks" ? 1 : (name == "alpha" || name == "alphaU" ? 4 : (name == "alphaV" ? 5 : -1));
+    case HK_BSDF_ROUGH_DIELECTRIC:
+        return name == "ksReflect" ? 1 : name == "ksRefract" ? 2 : (name == "alpha" || name == "alphaU") ? 4
+                                                                   : name == "alphaV" ? 5 : -1;
+    case HK_BSDF_ROUGH_COATING:
+    case HK_BSDF_COATING: return name == "ks" ? 1 : (name == "sigmaA" ? 3 : -1);
+    default: return -1;
+    }
+}
+
 // BSDF plugins: one class per reference type; properties and defaults of
 // include/core/Common.hpp:331-392 and the plugin constructors.
 class BSDFPlugin : public Object {
@@ -609,6 +680,7 @@ public:
     hk_bsdf_desc d{};
     std::unique_ptr<BSDFPlugin> nested;    // roughCoating's BSDF, twoSided's front BSDF
     std::unique_ptr<BSDFPlugin> nested2;   // twoSided's back BSDF
+    std::unique_ptr<TexturePlugin> tex[6]; // textured parameters by slot
     BSDFPlugin(const PropertyList &p, int type) {
         std::memset(&d, 0, sizeof d);
         d.type = type;
@@ -701,6 +773,15 @@ public:
     }
     EClassType GetClassType() const override { return EClassType::EBSDF; }
     void AddChild(Object *c, const std::string &name) override {
+        if (c->GetClassType() == EClassType::ETexture) {
+            const int slot = texture_slot(d.type, name);
+            if (slot < 0 || tex[slot]) {
+                delete c;
+                throw HikariException(type_name + ": a texture named \"" + name + "\" is not supported");
+            }
+            tex[slot].reset((TexturePlugin *)c);
+            return;
+        }
         if ((d.type == HK_BSDF_ROUGH_COATING || d.type == HK_BSDF_COATING) && c->GetClassType() == EClassType::EBSDF) {
             if (nested) {
                 delete c;
@@ -1058,10 +1139,19 @@ int upload_scene(const Scene &sc, const std::string &data_dir, hk_scene *h) {
         if ((rc = hk_scene_set_rft(h, dist, bytes.data(), bytes.size())) != HK_OK) return rc;
     }
     // nested BSDFs first, so that the parent can name their ids
+    std::function<int32_t(const TexturePlugin &)> add_texture = [&](const TexturePlugin &t) -> int32_t {
+        hk_texture_desc d = t.d;
+        if (t.nested) d.nested = add_texture(*t.nested);
+        int32_t id;
+        if ((rc = hk_scene_add_texture(h, &d, &id)) != HK_OK) throw HikariException(hk_last_error());
+        return id;
+    };
     std::function<int32_t(const BSDFPlugin &)> add_bsdf = [&](const BSDFPlugin &b) -> int32_t {
         hk_bsdf_desc d = b.d;
         if (b.nested) d.nested = add_bsdf(*b.nested);
         if (b.nested2) d.nested2 = add_bsdf(*b.nested2);
+        for (int k = 0; k < 6; k++)
+            if (b.tex[k]) d.tex[k] = 1 + add_texture(*b.tex[k]);
         int32_t id;
         if ((rc = hk_scene_add_bsdf(h, &d, &id)) != HK_OK) throw HikariException(hk_last_error());
         return id;

@@ -78,7 +78,7 @@ private:
 };
 
 enum class EClassType { EScene, EMesh, EBSDF, EEmitter, ECamera, EIntegrator, ESampler, EReconstructionFilter,
-                        EAcceleration, ETest };
+                        EAcceleration, ETest, ETexture };
 
 // Object (include/core/Object.hpp:26): lifecycle ctor -> AddChild -> SetParent -> Activate
 class Object {

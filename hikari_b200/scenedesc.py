@@ -351,6 +351,53 @@ def _transmits(d: Optional[BSDFDesc]) -> bool:
     return _transmits(d.nested) or _transmits(d.nested2)
 
 
+# XML names of the textured parameters each BSDF accepts (the plugins' AddChild)
+_TEX_NAMES = {
+    BSDF_DIFFUSE: {"albedo": "kd"},
+    BSDF_ROUGH_DIFFUSE: {"albedo": "kd", "alpha": "alpha_u"},
+    BSDF_CONDUCTOR: {"ks": "ks"},
+    BSDF_DIELECTRIC: {"ksReflect": "ks", "ksRefract": "ks_refract"},
+    BSDF_PLASTIC: {"kd": "kd", "ks": "ks"},
+    BSDF_ROUGH_CONDUCTOR: {"ks": "ks", "alpha": "alpha_u", "alphaU": "alpha_u", "alphaV": "alpha_v"},
+    BSDF_ROUGH_DIELECTRIC: {"ksReflect": "ks", "ksRefract": "ks_refract", "alpha": "alpha_u", "alphaU": "alpha_u",
+                            "alphaV": "alpha_v"},
+    BSDF_ROUGH_PLASTIC: {"kd": "kd", "ks": "ks"},
+    BSDF_ROUGH_COATING: {"ks": "ks", "sigmaA": "sigma_a"},
+    BSDF_COATING: {"ks": "ks", "sigmaA": "sigma_a"},
+}
+
+
+def _texture_from_xml(node: ET.Element) -> TextureDesc:
+    """CheckerboardTexture / GridTexture / ScaleTexture ctors (src/texture/*.cpp)."""
+    t = node.attrib["type"]
+    if t not in TEX_TYPE_NAMES:
+        raise SceneError(f"texture type {t!r} is not supported by the CUDA pathMIS core")
+    p = _props(node)
+    d = TextureDesc(kind=TEX_TYPE_NAMES[t])
+    d.uv_scale = [float(p.get("uScale", 1.0)), float(p.get("vScale", 1.0))]
+    d.uv_offset = [float(p.get("uOffset", 0.0)), float(p.get("vOffset", 0.0))]
+    if d.kind == TEX_CHECKERBOARD:
+        d.count = int(p.get("blocks", 10))
+        d.a = [float(c) for c in p.get("colorA", [0.4, 0.4, 0.4])]
+        d.b = [float(c) for c in p.get("colorB", [0.2, 0.2, 0.2])]
+    elif d.kind == TEX_GRID:
+        d.count = int(p.get("lines", 10))
+        d.a = [float(c) for c in p.get("lineColor", [0.4, 0.4, 0.4])]
+        d.b = [float(c) for c in p.get("backgroundColor", [0.2, 0.2, 0.2])]
+        d.width = float(p.get("lineWidth", 0.01))
+    else:
+        if "scale" not in p:
+            raise SceneError("Property 'scale' is missing!")
+        d.scale = float(p["scale"])
+        nested = [c for c in node if c.tag == "texture"]
+        if len(nested) != 1:
+            raise SceneError("ScaleTexture needs exactly one nested texture")
+        d.nested = _texture_from_xml(nested[0])
+    if d.kind != TEX_SCALE and d.count <= 0:
+        raise SceneError("texture block / line count must be positive")
+    return d
+
+
 def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
     t = node.attrib["type"]
     if t not in BSDF_TYPE_NAMES:
@@ -439,6 +486,16 @@ def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
         d.alpha_u = d.alpha_v = p.get("alpha", 0.2 if d.type == BSDF_ROUGH_DIFFUSE else 0.1)
     if d.type == BSDF_ROUGH_DIFFUSE:
         d.alpha_u = d.alpha_v = min(max(d.alpha_u, 5e-4), 1.0)   # Clamp(alpha, MIN_ALPHA, MAX_ALPHA)
+    for c in node:
+        if c.tag != "texture":
+            continue
+        name = c.attrib.get("name", "")
+        slot = _TEX_NAMES.get(d.type, {}).get(name)
+        if slot is None:
+            raise SceneError(f"{t}: a texture named {name!r} is not supported")
+        if slot in d.textures:
+            raise SceneError(f"{t}: tried to specify multiple {name} textures")
+        d.textures[slot] = _texture_from_xml(c)
     return d
 
 

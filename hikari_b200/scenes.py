@@ -21,8 +21,9 @@ import numpy as np
 
 from .scenedesc import (AIR_IOR, BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR,
                         BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
-                        BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX, BSDFDesc, CameraDesc, EnvDesc,
-                        FilterDesc, LightDesc, MeshDesc, SceneDesc)
+                        BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX, TEX_CHECKERBOARD, TEX_GRID,
+                        TEX_SCALE, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, LightDesc, MeshDesc, SceneDesc,
+                        TextureDesc)
 
 # Per-channel complex IOR (n, k) of copper and gold at R, G, B ~ (650, 550, 450) nm,
 # rounded from Johnson & Christy (1972) optical constants.
@@ -177,17 +178,26 @@ def spherical_uv(P: np.ndarray, center) -> np.ndarray:
 
 
 def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 12, seed: int = 0,
-                 shading_normals: bool = False) -> SceneDesc:
+                 shading_normals: bool = False, textured: bool = False) -> SceneDesc:
     """A ground quad and five displaced icospheres (diffuse, roughDiffuse,
     smooth plastic, rough conductor, smooth dielectric) lit, in emitter order,
     by a point light, an emissive quad, a constant environment and a
     directional light -- the emitter kinds interleaved as an XML scene lists
     them.  With shading_normals the spheres carry vertex normals and
     latitude-longitude texture coordinates (the shading frame then follows
-    dP/du) and the conductor is anisotropic (alpha 0.05 x 0.4)."""
+    dP/du) and the conductor is anisotropic (alpha 0.05 x 0.4).  textured (with
+    shading_normals) adds procedural textures: a checkerboard ground, a grid on
+    the diffuse sphere, checkerboard roughness on the roughDiffuse sphere, a
+    scaled checkerboard on the plastic's kd, textured alphaU / alphaV on the
+    conductor and a grid on the glass's refraction colour."""
     sd = SceneDesc()
     gp, gi = quad((-6, 0, 6), (6, 0, 6), (6, 0, -6), (-6, 0, -6))
-    sd.meshes.append(MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5])))
+    ground = MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5]))
+    if textured:
+        ground.uv = np.float32([[0, 0], [1, 0], [1, 1], [0, 1]])
+        ground.bsdf.textures["kd"] = TextureDesc(kind=TEX_CHECKERBOARD, count=12, a=[0.7, 0.7, 0.65],
+                                                 b=[0.15, 0.2, 0.3])
+    sd.meshes.append(ground)
     mats = [BSDFDesc(type=BSDF_DIFFUSE, kd=[0.7, 0.3, 0.2]),
             BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.3, 0.6, 0.3], alpha_u=0.6, alpha_v=0.6),
             BSDFDesc(type=BSDF_PLASTIC, int_ior=1.5046, ext_ior=AIR_IOR, kd=[0.2, 0.3, 0.7]),
@@ -197,6 +207,17 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
     if shading_normals:
         mats[3] = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, anisotropic=True, alpha_u=0.05, alpha_v=0.4,
                            int_ior=1.0, ext_ior=1.0, eta=AU_ETA, k=AU_K)
+    if textured:
+        checker = TextureDesc(kind=TEX_CHECKERBOARD, count=8, a=[0.9, 0.85, 0.8], b=[0.1, 0.1, 0.1])
+        mats[0].textures["kd"] = TextureDesc(kind=TEX_GRID, count=12, width=0.06, a=[0.05, 0.05, 0.05],
+                                             b=[0.8, 0.3, 0.2])
+        mats[1].textures["alpha_u"] = TextureDesc(kind=TEX_CHECKERBOARD, count=6, a=[0.05] * 3, b=[0.9] * 3)
+        mats[2].textures["kd"] = TextureDesc(kind=TEX_SCALE, scale=0.7, nested=checker)
+        mats[3].textures["alpha_u"] = TextureDesc(kind=TEX_GRID, count=8, width=0.1, a=[0.4] * 3, b=[0.02] * 3)
+        mats[3].textures["alpha_v"] = TextureDesc(kind=TEX_CHECKERBOARD, count=5, uv_scale=[2, 1], a=[0.3] * 3,
+                                                  b=[0.05] * 3)
+        mats[4].textures["ks_refract"] = TextureDesc(kind=TEX_GRID, count=6, width=0.05, a=[0.2, 0.2, 0.2],
+                                                     b=[1.0, 1.0, 1.0])
     for k, b in enumerate(mats):
         c = (-3.2 + 1.6 * k, 0.85, 0.3 * ((k % 2) * 2 - 1))
         P, F = displaced_icosphere(2, 0.8, c, 0.05, seed + k)
@@ -480,6 +501,41 @@ def smooth_materials():
         ("rough_diffuse_rough", BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.9, 0.9, 0.9], alpha_u=0.8, alpha_v=0.8)),
         ("rough_diffuse_fast", BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.7, 0.5, 0.3], alpha_u=0.4, alpha_v=0.4,
                                         fast_approx=True)),
+    ]
+
+
+def textured_materials():
+    """BSDFs with procedural textures on every textured parameter: diffuse and
+    roughDiffuse albedo / roughness, smooth and rough conductors (ks, alphaU /
+    alphaV), dielectrics (ksReflect / ksRefract / alpha), plastics (kd, ks),
+    and coatings (ks, sigmaA) over textured diffuse."""
+    chk = TextureDesc(kind=TEX_CHECKERBOARD, count=7, a=[0.9, 0.2, 0.1], b=[0.1, 0.3, 0.8], uv_scale=[1.5, 0.7],
+                      uv_offset=[0.25, -0.1])
+    grid = TextureDesc(kind=TEX_GRID, count=5, width=0.08, a=[0.05, 0.05, 0.05], b=[0.7, 0.6, 0.5])
+    scaled = TextureDesc(kind=TEX_SCALE, scale=0.6, nested=TextureDesc(kind=TEX_CHECKERBOARD, count=3))
+    a_chk = TextureDesc(kind=TEX_CHECKERBOARD, count=4, a=[0.05] * 3, b=[0.4] * 3)
+    a_grid = TextureDesc(kind=TEX_GRID, count=6, width=0.1, a=[0.6] * 3, b=[0.15] * 3)
+    return [
+        ("tex_diffuse", BSDFDesc(type=BSDF_DIFFUSE, textures={"kd": chk})),
+        ("tex_rough_diffuse", BSDFDesc(type=BSDF_ROUGH_DIFFUSE, textures={"kd": grid, "alpha_u": a_chk})),
+        ("tex_conductor", BSDFDesc(type=BSDF_CONDUCTOR, int_ior=0.27, ext_ior=1.0, k=CU_K, textures={"ks": chk})),
+        ("tex_rough_conductor", BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2,
+                                         int_ior=1.0, ext_ior=1.0, eta=CU_ETA, k=CU_K,
+                                         textures={"alpha_u": a_chk, "ks": chk})),
+        ("tex_rough_conductor_aniso", BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=BECKMANN, anisotropic=True,
+                                               alpha_u=0.1, alpha_v=0.3, int_ior=1.0, ext_ior=1.0, eta=AU_ETA, k=AU_K,
+                                               textures={"alpha_u": a_chk, "alpha_v": a_grid})),
+        ("tex_dielectric", BSDFDesc(type=BSDF_DIELECTRIC, textures={"ks": grid, "ks_refract": scaled})),
+        ("tex_rough_dielectric", BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=0.1, alpha_v=0.1,
+                                          int_ior=1.5, ext_ior=1.0, textures={"alpha_u": a_grid, "ks_refract": chk})),
+        ("tex_plastic", BSDFDesc(type=BSDF_PLASTIC, kd=[0.3, 0.3, 0.3], textures={"kd": grid, "ks": scaled})),
+        ("tex_rough_plastic", BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=0.15, alpha_v=0.15,
+                                       textures={"kd": chk, "ks": grid})),
+        ("tex_rough_coating", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2,
+                                       thickness=0.5, nested=BSDFDesc(type=BSDF_DIFFUSE, textures={"kd": grid}),
+                                       textures={"sigma_a": scaled, "ks": chk})),
+        ("tex_coating", BSDFDesc(type=BSDF_COATING, nested=BSDFDesc(type=BSDF_DIFFUSE, textures={"kd": chk}),
+                                 textures={"sigma_a": scaled})),
     ]
 
 

@@ -66,6 +66,9 @@ typedef struct {
     int32_t nested;        /* roughCoating / twoSided front: id of the nested BSDF (added first), else -1 */
     int32_t nested2;       /* twoSided back: id of the second nested BSDF, -1 = the front one */
     int32_t fast_approx;   /* roughDiffuse "fastApprox" */
+    /* textures of kd / albedo, ks / ksReflect, ksRefract, sigmaA, alpha / alphaU,
+     * alphaV: 1 + texture id (hk_scene_add_texture), 0 = the constant above */
+    int32_t tex[6];
 } hk_bsdf_desc;
 
 typedef struct {
@@ -92,6 +95,20 @@ int hk_version(void);
 /* ---- scene construction (Scene::AddChild src/core/Scene.cpp:167 order) ---- */
 int hk_scene_create(hk_scene **out);
 int hk_scene_destroy(hk_scene *s);
+/* Procedural textures (src/texture/{Checkerboard,Grid,Scale}Texture.cpp). */
+#define HK_TEX_CHECKERBOARD 1
+#define HK_TEX_GRID 2
+#define HK_TEX_SCALE 3
+typedef struct {
+    int32_t kind;          /* HK_TEX_* */
+    int32_t nested;        /* scale: id of the scaled texture (added first) */
+    int32_t count;         /* checkerboard "blocks", grid "lines" */
+    float width;           /* grid "lineWidth" */
+    float scale;           /* scale "scale" */
+    float uv_scale[2], uv_offset[2];   /* "uScale" "vScale", "uOffset" "vOffset" */
+    float a[3], b[3];      /* checkerboard colorA / colorB; grid lineColor / backgroundColor */
+} hk_texture_desc;
+int hk_scene_add_texture(hk_scene *s, const hk_texture_desc *desc, int32_t *out_id);
 /* Raw bytes of data/BeckmannRFTData.bin (distribution 0) or GGXRFTData.bin (1),
  * the RoughTransmittance table file (src/core/RoughTransmitance.cpp:9). */
 int hk_scene_set_rft(hk_scene *s, int distribution, const void *bytes, uint64_t nbytes);
@@ -342,11 +359,13 @@ int hk_trace(hk_scene *s, uint64_t n, const float *rays_dev, int32_t *tri_dev, f
              int any_hit, unsigned long long *node_visits_dev, void *stream);
 /* BSDF::Sample/Eval/Pdf (include/core/BSDF.hpp:67,78,94) over n records in
  * the local frame: inputs wi (n x 3), u2 (n x 2), u1 (n, roughDielectric's
- * Next1D draw, may be NULL), wo (n x 3); outputs (any may be NULL): sampled
- * wo, weight, pdf of the sample, measure; Eval and Pdf at wo (ESolidAngle). */
+ * Next1D draw, may be NULL), wo (n x 3), uv (n x 2 texture coordinates of the
+ * records' intersection, for textured parameters; NULL = (0, 0)); outputs (any
+ * may be NULL): sampled wo, weight, pdf of the sample, measure; Eval and Pdf at
+ * wo (ESolidAngle). */
 int hk_bsdf_batch(hk_scene *s, int32_t bsdf, uint64_t n, const float *wi_dev, const float *u2_dev, const float *u1_dev,
-                  const float *wo_dev, float *s_wo_dev, float *s_w_dev, float *s_pdf_dev, int32_t *s_measure_dev,
-                  float *e_rgb_dev, float *p_pdf_dev, void *stream);
+                  const float *wo_dev, const float *uv_dev, float *s_wo_dev, float *s_w_dev, float *s_pdf_dev,
+                  int32_t *s_measure_dev, float *e_rgb_dev, float *p_pdf_dev, void *stream);
 /* Emitter::Sample (include/core/Emitter.hpp:77) for emitter e: in n x 8
  * (ref xyz, u2, u1, -, -), out n x 16 (p, n, wi, pdf, distance, value, -). */
 int hk_emitter_sample(hk_scene *s, int32_t e, uint64_t n, const float *in_dev, float *out_dev, void *stream);

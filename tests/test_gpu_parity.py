@@ -33,11 +33,13 @@ DEV = "cuda:0"
 RTOL = 1e-5
 
 
-@pytest.fixture(scope="module", params=["rough", "smooth"])
+@pytest.fixture(scope="module", params=["rough", "smooth", "textured"])
 def bsdf_pair(request):
-    """The BSDF-batch material set (rough BSDFs and a coating) or the smooth
-    and two-sided set."""
-    mats = scenes.config2_materials() if request.param == "rough" else scenes.smooth_materials()
+    """The BSDF-batch material set (rough BSDFs and a coating), the smooth and
+    two-sided set, or the set with procedural textures (records carry texture
+    coordinates)."""
+    mats = {"rough": scenes.config2_materials, "smooth": scenes.smooth_materials,
+            "textured": scenes.textured_materials}[request.param]()
     sd = scenes.bsdf_scene(mats)
     return mats, hk.Scene.from_desc(sd), OracleScene(sd), request.param
 
@@ -50,15 +52,17 @@ def test_bsdf_batch_parity(bsdf_pair):
     mats, gs, os_, kind = bsdf_pair
     n = 1 << 17
     wi, u2, u1, wo = bsdf_records(n, 11)
-    if kind == "smooth":   # a tenth of the evaluation directions on the mirror direction
+    if kind != "rough":   # a tenth of the evaluation directions on the mirror direction
         wo[0::10] = wi[0::10] * np.float32([-1, -1, 1])
+    uv = (np.random.default_rng(5).random((n, 2)) * 4 - 1).astype(np.float32) if kind == "textured" else None
+    tuv = _t(uv) if uv is not None else None
     twi, tu2, tu1, two = _t(wi), _t(u2), _t(u1), _t(wo)
     report = []
     for i, (name, d) in enumerate(mats):
         gid = gs.bsdf_ids[id(d)]
         oid = os_.bsdf_ids[id(d)]
-        g = {k: v.cpu().numpy() for k, v in gs.bsdf_batch(gid, twi, tu2, tu1, two).items()}
-        o = os_.bsdf_batch(oid, wi, u2, u1, wo)
+        g = {k: v.cpu().numpy() for k, v in gs.bsdf_batch(gid, twi, tu2, tu1, two, uv=tuv).items()}
+        o = os_.bsdf_batch(oid, wi, u2, u1, wo, uv=uv)
         for key in ("e_rgb", "p_pdf"):
             ok = rel_close(g[key], o[key], RTOL).reshape(n, -1).all(1)
             loose = rel_close(g[key], o[key], 1e-3).reshape(n, -1).all(1)

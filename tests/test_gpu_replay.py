@@ -42,6 +42,7 @@ SCENES = {
     "heterogeneous": lambda: scenes.heterogeneous(width=32, height=32, n_spheres=12, levels=(3,), level_p=(1.0,), env_res=(256, 128)),
     "lights": lambda: scenes.lights_scene(width=32, height=32),
     "shading_normals_uv": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True),
+    "textured": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True, textured=True),
 }
 
 

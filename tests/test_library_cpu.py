@@ -333,3 +333,57 @@ def test_obj_reader_errors(L, tmp_path, text, needle):
     open(path, "w").write(text)
     with pytest.raises(hk.HikariError, match=needle):
         hk.obj_load(path)
+
+
+TEXTURE_XML = """<?xml version="1.0"?>
+<scene>
+  <integrator type="pathMIS"><integer name="depth" value="8"/></integrator>
+  <camera type="perspective"><integer name="width" value="16"/><integer name="height" value="16"/></camera>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="diffuse">
+      <texture type="checkerboard" name="albedo"><integer name="blocks" value="4"/>
+        <color name="colorA" value="0.9, 0.1, 0.1"/><float name="uScale" value="2"/></texture>
+    </bsdf>
+  </mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="roughConductor"><boolean name="as" value="true"/>
+      <texture type="grid" name="alphaU"><integer name="lines" value="6"/><float name="lineWidth" value="0.05"/></texture>
+      <texture type="scale" name="alphaV"><float name="scale" value="0.5"/><texture type="checkerboard"/></texture>
+    </bsdf>
+  </mesh>
+</scene>
+"""
+
+
+def test_xml_textures(L, tmp_path):
+    from hikari_b200.scenedesc import TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE
+
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "tex.xml")
+    open(path, "w").write(TEXTURE_XML)
+    info, depth, spp = hk.parse_xml_info(path)
+    sd = parse_xml(path)[0]
+    assert info.n_bsdfs == 2
+    t = sd.meshes[0].bsdf.textures["kd"]
+    assert t.kind == TEX_CHECKERBOARD and t.count == 4 and t.a == pytest.approx([0.9, 0.1, 0.1]) and t.uv_scale == [2.0, 1.0]
+    c = sd.meshes[1].bsdf.textures
+    assert c["alpha_u"].kind == TEX_GRID and c["alpha_u"].width == pytest.approx(0.05)
+    assert c["alpha_v"].kind == TEX_SCALE and c["alpha_v"].nested.kind == TEX_CHECKERBOARD
+
+
+@pytest.mark.parametrize("body,needle", [
+    ('<bsdf type="diffuse"><texture type="checkerboard" name="ks"/></bsdf>', "not supported"),
+    ('<bsdf type="roughPlastic"><texture type="checkerboard" name="alpha"/></bsdf>', "not supported"),
+    ('<bsdf type="diffuse"><texture type="scale" name="albedo"><float name="scale" value="2"/></texture></bsdf>',
+     "nested texture"),
+])
+def test_xml_texture_errors(L, tmp_path, body, needle):
+    from hikari_b200.scenedesc import SceneError
+
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "bad.xml")
+    open(path, "w").write(f'<scene><mesh type="obj"><string name="filename" value="quad.obj"/>{body}</mesh></scene>')
+    with pytest.raises(hk.HikariError, match=needle):
+        hk.parse_xml_info(path)
+    with pytest.raises(SceneError, match=needle):
+        parse_xml(path)
