@@ -99,6 +99,7 @@ struct DevScene {
     uint32_t ntris, nnodes, nwnodes;
     int32_t accel;                // kAccelBvh2 or kAccelBvh8: the tree the kernels traverse
     int32_t postpone;             // 8-wide traversal may postpone triangle tests (stack bound allows it)
+    int32_t textured;             // some material has textures (the megakernel compiles lookups in)
     const DevMesh *meshes;
     const DevBsdf *bsdfs;
     int32_t nmeshes, nbsdfs;

@@ -452,6 +452,7 @@ void build_scene(hk_scene *s) {
     for (size_t i = 0; i < bs.size(); ++i) {
         bs[i].textures = s->b_textures.as<hk::DevTexture>();
         bs[i].textured = bsdf_textured(s, (int)i, 0) ? 1 : 0;
+        D.textured |= bs[i].textured;
     }
     s->b_bsdfs.upload(bs); track(s->b_bsdfs);
     D.bsdfs = s->b_bsdfs.as<hk::DevBsdf>();
@@ -701,7 +702,7 @@ void build_scene(hk_scene *s) {
     int dev = 0;
     HK_CUDA(cudaGetDevice(&dev));
     HK_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, dev));
-    for (int a = 0; a < 2; ++a) s->occupancy_of[a] = std::max(1, hk::render_occupancy(s->margin_lo, s->margin_hi, a));
+    for (int a = 0; a < 2; ++a) s->occupancy_of[a] = std::max(1, hk::render_occupancy(s->margin_lo, s->margin_hi, a, D.textured != 0));
     s->occupancy = s->occupancy_of[D.accel];
     HK_CUDA(cudaGetLastError());
 

@@ -26,7 +26,8 @@ __device__ __forceinline__ uint32_t mesh_emitter(const DevScene &S, int mesh) { 
 // (reference: every bounce), NEE over all emitters, MIS state carried across
 // bounces, unweighted environment on BSDF-sampled misses, the EDiscrete
 // override and Eigen's |c| <= 1e-5 zero test on throughput and NEE values.
-template <int kAccel>
+// kTex: the scene has textured materials (texture lookups compiled in)
+template <int kAccel, bool kTex>
 __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, int rr_start, PathCounters &pc) {
     Hit hn;
     bool found_next = false;
@@ -80,7 +81,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
                     br.wo = to_local(it.sh, er.wi);
                     br.measure = kMeasureSolidAngle;
                     br.eta = 0.0f;
-                    br.tu = it.u; br.tv = it.v; br.tex = true;
+                    br.tu = it.u; br.tv = it.v; br.tex = kTex;
                     float pb = bsdf_pdf(S.bsdfs, bsdf, br);
                     if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
                     V3 f = bsdf_eval(S.bsdfs, bsdf, br);
@@ -95,7 +96,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
         br.wo = v3(0, 0, 0);
         br.measure = kMeasureUnknown;
         br.eta = 0.0f;
-        br.tu = it.u; br.tv = it.v; br.tex = true;
+        br.tu = it.u; br.tv = it.v; br.tex = kTex;
         float sx = rng.nextf(), sy = rng.nextf();
         float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
         V3 F = bsdf_sample(S.bsdfs, bsdf, br, sx, sy, u1);
@@ -163,7 +164,7 @@ __device__ __forceinline__ uint64_t mix_seed(uint64_t seed, uint64_t s0) {
     return z ^ (z >> 31);
 }
 
-template <int kAccel>
+template <int kAccel, bool kTex>
 __global__ void __launch_bounds__(kTileThreads) render_pathmis_kernel(DevScene S, RenderLaunch P) {
     extern __shared__ float tile[];
     __shared__ int s_item;
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(kTileThreads) render_pathmis_kernel(DevScene S
             for (int s = s0; s < s1; ++s) {
                 float px = (float)x + rng.nextf(), py = (float)y + rng.nextf();
                 Ray r = camera_ray(S, px, py);
-                V3 L = li_pathmis<kAccel>(S, rng, r, P.depth, P.rr_start, pc);
+                V3 L = li_pathmis<kAccel, kTex>(S, rng, r, P.depth, P.rr_start, pc);
                 if (!is_valid(L)) { ++dropped; continue; }
                 splat_shared(S, tile, tw, th, fx0, fy0, FW, FH, px, py, L);
             }
@@ -391,8 +392,13 @@ static int grid_for(uint64_t n, int threads) {
 cudaError_t launch_render(const DevScene &S, const RenderLaunch &P, int grid, cudaStream_t st) {
     const int tw = kTile + P.margin_hi - P.margin_lo;
     size_t smem = (size_t)tw * tw * 4 * sizeof(float);
-    if (S.accel == kAccelBvh8) render_pathmis_kernel<kAccelBvh8><<<grid, kTileThreads, smem, st>>>(S, P);
-    else render_pathmis_kernel<kAccelBvh2><<<grid, kTileThreads, smem, st>>>(S, P);
+    if (S.accel == kAccelBvh8) {
+        if (S.textured) render_pathmis_kernel<kAccelBvh8, true><<<grid, kTileThreads, smem, st>>>(S, P);
+        else render_pathmis_kernel<kAccelBvh8, false><<<grid, kTileThreads, smem, st>>>(S, P);
+    } else {
+        if (S.textured) render_pathmis_kernel<kAccelBvh2, true><<<grid, kTileThreads, smem, st>>>(S, P);
+        else render_pathmis_kernel<kAccelBvh2, false><<<grid, kTileThreads, smem, st>>>(S, P);
+    }
     return cudaGetLastError();
 }
 cudaError_t launch_resolve(const float *film, float *rgb, int W, int H, int B, cudaStream_t st) {
@@ -447,13 +453,16 @@ cudaError_t launch_env_eval(const DevScene &S, uint64_t n, const float *wi, floa
     env_eval_kernel<<<grid_for(n, 128), 128, 0, st>>>(S, n, wi, out, pdf);
     return cudaGetLastError();
 }
-int render_occupancy(int margin_lo, int margin_hi, int accel) {
+int render_occupancy(int margin_lo, int margin_hi, int accel, bool textured) {
     int n = 0;
-    const int tw = kTile + margin_hi - margin_lo;
-    if (accel == kAccelBvh8)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel<kAccelBvh8>, kTileThreads, (size_t)tw * tw * 16);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel<kAccelBvh2>, kTileThreads, (size_t)tw * tw * 16);
+    const size_t smem = (size_t)(kTile + margin_hi - margin_lo) * (kTile + margin_hi - margin_lo) * 16;
+    if (accel == kAccelBvh8) {
+        if (textured) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel<kAccelBvh8, true>, kTileThreads, smem);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel<kAccelBvh8, false>, kTileThreads, smem);
+    } else {
+        if (textured) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel<kAccelBvh2, true>, kTileThreads, smem);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, render_pathmis_kernel<kAccelBvh2, false>, kTileThreads, smem);
+    }
     return n;
 }
 

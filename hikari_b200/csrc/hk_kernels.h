@@ -46,6 +46,6 @@ cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, int type, uint64_t n,
 cudaError_t launch_emitter_sample(const DevScene &S, int e, uint64_t n, const float *in, float *out, cudaStream_t st);
 cudaError_t launch_camera_rays(const DevScene &S, uint64_t n, const float *pos, float *out, cudaStream_t st);
 cudaError_t launch_env_eval(const DevScene &S, uint64_t n, const float *wi, float *out, float *pdf, cudaStream_t st);
-int render_occupancy(int margin_lo, int margin_hi, int accel);
+int render_occupancy(int margin_lo, int margin_hi, int accel, bool textured);
 
 }  // namespace hk
