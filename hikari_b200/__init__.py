@@ -14,7 +14,7 @@ from typing import Optional
 import numpy as np
 
 from . import scenedesc
-from .scenedesc import TEX_SLOTS, BSDFDesc, SceneDesc
+from .scenedesc import TEX_BITMAP, TEX_SLOTS, BSDFDesc, SceneDesc
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libhikari_b200.so")
@@ -42,7 +42,8 @@ class TextureDesc(C.Structure):
     _fields_ = [
         ("kind", C.c_int32), ("nested", C.c_int32), ("count", C.c_int32), ("width", C.c_float),
         ("scale", C.c_float), ("uv_scale", C.c_float * 2), ("uv_offset", C.c_float * 2), ("a", C.c_float * 3),
-        ("b", C.c_float * 3),
+        ("b", C.c_float * 3), ("filter", C.c_int32), ("wrap_u", C.c_int32), ("wrap_v", C.c_int32),
+        ("channels", C.c_int32), ("gamma", C.c_float), ("max_anisotropy", C.c_float),
     ]
 
 
@@ -125,6 +126,11 @@ def lib():
         "hk_scene_set_envmap": ([P, P, C.c_uint32, C.c_uint32, P, F], C.c_int),
         "hk_scene_set_constant_light": ([P, P], C.c_int),
         "hk_scene_add_texture": ([P, C.POINTER(TextureDesc), C.POINTER(I32)], C.c_int),
+        "hk_scene_add_bitmap": ([P, C.POINTER(TextureDesc), P, I32, I32, C.POINTER(I32)], C.c_int),
+        "hk_image_load": ([C.c_char_p, I32, C.POINTER(I32), C.POINTER(I32), C.POINTER(C.POINTER(C.c_uint8))],
+                          C.c_int),
+        "hk_image_free": ([C.POINTER(C.c_uint8)], None),
+        "hk_texture_eval": ([P, I32, U64, P, P, P, P], C.c_int),
         "hk_scene_set_mesh_uv": ([P, I32, P], C.c_int),
         "hk_obj_load": ([C.c_char_p, P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), P, P, P, P, C.POINTER(I32)],
                         C.c_int),
@@ -161,7 +167,7 @@ def lib():
         "hk_job_preview": ([P, U64, P, C.c_double, C.POINTER(C.c_double)], C.c_int),
         "hk_server_get_stats": ([P, C.POINTER(ServerStats)], C.c_int),
         "hk_trace": ([P, U64, P, P, P, P, P, C.c_int, P, P], C.c_int),
-        "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
+        "hk_bsdf_batch": ([P, I32, U64, P, P, P, P, P, P, P, P, P, P, P, P, P], C.c_int),
         "hk_emitter_sample": ([P, I32, U64, P, P, P], C.c_int),
         "hk_camera_rays": ([P, U64, P, P, P], C.c_int),
         "hk_env_eval": ([P, U64, P, P, P, P], C.c_int),
@@ -206,7 +212,24 @@ def texture_desc_c(t, nested_id: int = -1) -> TextureDesc:
     c = TextureDesc()
     c.kind, c.nested, c.count, c.width, c.scale = t.kind, nested_id, t.count, t.width, t.scale
     c.uv_scale[:], c.uv_offset[:], c.a[:], c.b[:] = t.uv_scale, t.uv_offset, t.a, t.b
+    c.filter, c.wrap_u, c.wrap_v = t.filter, t.wrap_u, t.wrap_v
+    c.channels, c.gamma, c.max_anisotropy = t.channels, t.gamma, t.max_anisotropy
     return c
+
+
+def image_load(path: str, channels: int = 3) -> np.ndarray:
+    """Decode an 8-bit image file (PNG, PGM / PPM, baseline JPEG) like
+    stbi_load with `channels` (1 or 3): height x width x channels uint8, row 0
+    = the top row."""
+    L = lib()
+    w, h = C.c_int32(), C.c_int32()
+    buf = C.POINTER(C.c_uint8)()
+    check(L.hk_image_load(os.fsencode(path), channels, C.byref(w), C.byref(h), C.byref(buf)))
+    try:
+        a = np.ctypeslib.as_array(buf, shape=(h.value, w.value, channels)).copy()
+    finally:
+        L.hk_image_free(buf)
+    return a
 
 
 def bsdf_desc_c(d: BSDFDesc, nested_id: int = -1, nested2_id: int = -1, tex_ids=None) -> BsdfDesc:
@@ -261,7 +284,11 @@ class Scene:
                 nested = add_texture(t.nested) if t.nested is not None else -1
                 c = texture_desc_c(t, nested)
                 out = C.c_int32()
-                check(L.hk_scene_add_texture(h, C.byref(c), C.byref(out)))
+                if t.kind == TEX_BITMAP:
+                    px = np.ascontiguousarray(t.pixels, dtype=np.uint8)
+                    check(L.hk_scene_add_bitmap(h, C.byref(c), _p(px), px.shape[1], px.shape[0], C.byref(out)))
+                else:
+                    check(L.hk_scene_add_texture(h, C.byref(c), C.byref(out)))
                 tids[id(t)] = out.value
                 return out.value
 
@@ -315,7 +342,9 @@ class Scene:
         except Exception:
             L.hk_scene_destroy(h)
             raise
-        return cls(h, desc, ids)
+        sc = cls(h, desc, ids)
+        sc.tex_ids = tids
+        return sc
 
     @classmethod
     def from_xml(cls, path: str) -> "Scene":
@@ -478,7 +507,7 @@ class Scene:
                              _stream(stream)))
         return tri, t, u, v, visits
 
-    def bsdf_batch(self, bsdf_id: int, wi, u2, u1, wo, stream=None, uv=None):
+    def bsdf_batch(self, bsdf_id: int, wi, u2, u1, wo, stream=None, uv=None, duv=None):
         import torch
 
         n = wi.shape[0]
@@ -491,9 +520,18 @@ class Scene:
             e_rgb=torch.empty((n, 3), dtype=torch.float32, device=dev),
             p_pdf=torch.empty(n, dtype=torch.float32, device=dev),
         )
-        check(lib().hk_bsdf_batch(self.h, bsdf_id, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(uv), _p(out["s_wo"]),
+        check(lib().hk_bsdf_batch(self.h, bsdf_id, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(uv), _p(duv), _p(out["s_wo"]),
                                   _p(out["s_w"]), _p(out["s_pdf"]), _p(out["s_measure"]), _p(out["e_rgb"]),
                                   _p(out["p_pdf"]), _stream(stream)))
+        return out
+
+    def texture_eval(self, tex_id: int, uv, duv=None, stream=None):
+        """Texture2D::Eval(Isect, filter) of texture `tex_id` at device texture
+        coordinates uv (n x 2) with partials duv (n x 4, or None): n x 3."""
+        import torch
+
+        out = torch.empty((uv.shape[0], 3), dtype=torch.float32, device=uv.device)
+        check(lib().hk_texture_eval(self.h, tex_id, uv.shape[0], _p(uv), _p(duv), _p(out), _stream(stream)))
         return out
 
     def emitter_sample(self, e: int, inp, stream=None):

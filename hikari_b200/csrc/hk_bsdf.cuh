@@ -19,6 +19,7 @@ struct BRec {
     float eta;
     int measure;
     float tu, tv;   // texture coordinates of the intersection (Record.Isect.UV)
+    float4 duv;     // their screen-space partials (dUdX, dVdX, dUdY, dVdY): a camera ray's first hit, else 0
     bool tex;       // textures are looked up (false in kernels that shade untextured materials only)
 };
 
@@ -163,7 +164,114 @@ __device__ __forceinline__ int mod_positive(int a, int b) {
     int q = a % b;
     return q < 0 ? q + b : q;
 }
-__device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, float tv) {
+// ---- bitmaps: MipMap<T> (include/core/MipMap.hpp) over the pyramid built on
+// the host.  All arithmetic follows the reference's float order; the level of
+// detail uses the device log2f (the host's log2f may differ in the last place,
+// which moves the lerp between two levels by as much).
+// MipMap::Texel :244 -- outside the level, or everywhere with a "black" wrap mode, black.
+__device__ __forceinline__ V3 mip_texel(const DevTexture &t, int l, int x, int y) {
+    const int w = 1 << max(0, t.lw - l), h = 1 << max(0, t.lh - l);
+    if (t.black || x < 0 || x >= w || y < 0 || y >= h) return v3(0, 0, 0);
+    const uint32_t i = t.lvl_off[l] + (uint32_t)y * (uint32_t)w + (uint32_t)x;
+    if (t.channels == 1) {
+        const float r = __ldg(t.texels + i);
+        return v3(r, r, r);
+    }
+    const float4 c = __ldg(reinterpret_cast<const float4 *>(t.texels) + i);
+    return v3(c.x, c.y, c.z);
+}
+// MipMap::Triangle :412
+__device__ __forceinline__ V3 mip_triangle(const DevTexture &t, int l, float u, float v) {
+    l = clampi(l, 0, t.levels - 1);
+    const float U = u * (float)(1 << max(0, t.lw - l)) - 0.5f, Vv = v * (float)(1 << max(0, t.lh - l)) - 0.5f;
+    const int u0 = (int)floorf(U), v0 = (int)floorf(Vv);
+    const float du = U - (float)u0, dv = Vv - (float)v0;
+    const float a = (1.0f - du) * (1.0f - dv), b = (1.0f - du) * dv, c = du * (1.0f - dv), d = du * dv;
+    V3 r = mip_texel(t, l, u0, v0) * a;
+    r = r + mip_texel(t, l, u0, v0 + 1) * b;
+    r = r + mip_texel(t, l, u0 + 1, v0) * c;
+    return r + mip_texel(t, l, u0 + 1, v0 + 1) * d;
+}
+__device__ __forceinline__ V3 lerp3(float x, V3 a, V3 b) { return a * (1.0f - x) + b * x; }
+// MipMap::Lookup(UV, Width) :287 (bilinear with width 0, trilinear)
+__device__ __forceinline__ V3 mip_lookup_width(const DevTexture &t, float u, float v, float width) {
+    const float level = (float)t.levels - 1.0f + log2f(fmaxf(width, 1e-8f));
+    if (level < 0.0f) return mip_triangle(t, 0, u, v);
+    if (level >= (float)(t.levels - 1)) return mip_texel(t, t.levels - 1, 0, 0);
+    const int il = (int)floorf(level);
+    return lerp3(level - (float)il, mip_triangle(t, il, u, v), mip_triangle(t, il + 1, u, v));
+}
+// MipMap::EWA :427.  The scan is bounded to 4096 x 4096 texels (reached only
+// with a maxAnisotropy of the order of a thousand or more).
+static __device__ __noinline__ V3 mip_ewa(const DevTexture &t, int l, float u, float v, float d0x, float d0y, float d1x,
+                                   float d1y) {
+    if (l >= t.levels) return mip_texel(t, t.levels - 1, 0, 0);
+    const float W = (float)(1 << max(0, t.lw - l)), H = (float)(1 << max(0, t.lh - l));
+    u = u * W - 0.5f;
+    v = v * H - 0.5f;
+    d0x *= W; d0y *= H; d1x *= W; d1y *= H;
+    float A = (d0y * d0y + d1y * d1y) + 1.0f;
+    float B = -2.0f * (d0x * d0y + d1x * d1y);
+    float C = (d0x * d0x + d1x * d1x) + 1.0f;
+    const float invf = 1.0f / (A * C - (B * B) * 0.25f);
+    A *= invf; B *= invf; C *= invf;
+    const float det = (-B) * B + (4.0f * A) * C;
+    const float invdet = 1.0f / det;
+    const float usq = sqrtf(det * C), vsq = sqrtf(A * det);
+    const int u0 = (int)ceilf(u - (2.0f * invdet) * usq), v0 = (int)ceilf(v - (2.0f * invdet) * vsq);
+    const int u1 = min((int)floorf(u + (2.0f * invdet) * usq), u0 + 4095);
+    const int v1 = min((int)floorf(v + (2.0f * invdet) * vsq), v0 + 4095);
+    V3 sum = v3(0, 0, 0);
+    float sw = 0.0f;
+    for (int iv = v0; iv <= v1; ++iv) {
+        const float dv = (float)iv - v;
+        for (int iu = u0; iu <= u1; ++iu) {
+            const float du = (float)iu - u;
+            const float r2 = ((A * du) * du + (B * du) * dv) + (C * dv) * dv;
+            if (r2 < 1.0f) {
+                const float wt = __ldg(t.lut + min((int)(r2 * (float)kEwaLutSize), kEwaLutSize - 1));
+                sum = sum + mip_texel(t, l, iu, iv) * wt;
+                sw += wt;
+            }
+        }
+    }
+    return v3(sum.x / sw, sum.y / sw, sum.z / sw);
+}
+// MipMap::Lookup(UV, D0, D1) :309
+__device__ __forceinline__ V3 mip_lookup_diff(const DevTexture &t, float u, float v, float d0x, float d0y, float d1x,
+                                              float d1y) {
+    if (t.filter == kFilterTrilinear) {
+        const float w = fmaxf(fmaxf(fabsf(d0x), fabsf(d0y)), fmaxf(fabsf(d1x), fabsf(d1y)));
+        return mip_lookup_width(t, u, v, 2.0f * w);
+    }
+    if (d0x * d0x + d0y * d0y < d1x * d1x + d1y * d1y) {
+        float a = d0x, b = d0y;
+        d0x = d1x; d0y = d1y; d1x = a; d1y = b;
+    }
+    const float major = sqrtf(d0x * d0x + d0y * d0y);
+    float minor = sqrtf(d1x * d1x + d1y * d1y);
+    if (minor * t.max_aniso < major && minor > 0.0f) {
+        const float sc = major / (minor * t.max_aniso);
+        d1x *= sc; d1y *= sc;
+        minor *= sc;
+    }
+    if (minor == 0.0f) return mip_triangle(t, 0, u, v);
+    const float lod = fmaxf(0.0f, (float)t.levels - 1.0f + log2f(minor));
+    const float ilod = floorf(lod);
+    return lerp3(lod - ilod, mip_ewa(t, (int)ilod, u, v, d0x, d0y, d1x, d1y),
+                 mip_ewa(t, (int)(ilod + 1.0f), u, v, d0x, d0y, d1x, d1y));
+}
+// BitmapTexture::Eval(UV, D0, D1) (src/texture/BitmapTexture.cpp:101) after
+// Texture2D::Eval (src/core/Texture.cpp:211) scaled UV and the partials
+static __device__ __noinline__ V3 bitmap_eval(const DevTexture &t, float u, float v, float4 d) {
+    if (t.filter == kFilterNearest)
+        return mip_texel(t, 0, (int)floorf(u * (float)(1 << t.lw)), (int)floorf(v * (float)(1 << t.lh)));
+    if (t.filter == kFilterBilinear) return mip_lookup_width(t, u, v, 0.0f);
+    return mip_lookup_diff(t, u, v, d.x * t.uv_scale[0], d.y * t.uv_scale[1], d.z * t.uv_scale[0],
+                           d.w * t.uv_scale[1]);
+}
+
+__device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, float tv, float4 duv) {
     float sc[4];
     int ns = 0;
     while (T[id].kind == kTexScale && ns < 4) {
@@ -173,7 +281,9 @@ __device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, fl
     const DevTexture &t = T[id];
     const float u = tu * t.uv_scale[0] + t.uv_offset[0], v = tv * t.uv_scale[1] + t.uv_offset[1];
     V3 c;
-    if (t.kind == kTexCheckerboard) {
+    if (t.kind == kTexBitmap) {
+        c = bitmap_eval(t, u, v, duv);
+    } else if (t.kind == kTexCheckerboard) {
         bool ex = mod_positive(mod_positive((int)(u * t.count), t.count), 2) == 0;
         bool ey = mod_positive(mod_positive((int)(v * t.count), t.count), 2) == 0;
         c = (ex ^ ey) ? ld_rgb(t.a) : ld_rgb(t.b);
@@ -192,14 +302,14 @@ __device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, fl
 __device__ __forceinline__ V3 par_rgb(const DevBsdf &b, int slot, const float *c, const BRec &r) {
     if (r.tex) {
         const int t = b.tex[slot];
-        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv);
+        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv, r.duv);
     }
     return ld_rgb(c);
 }
 __device__ __forceinline__ float par_alpha(const DevBsdf &b, int slot, float c, const BRec &r) {
     if (r.tex) {
         const int t = b.tex[slot];
-        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv).x;
+        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv, r.duv).x;
     }
     return c;
 }

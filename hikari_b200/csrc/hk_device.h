@@ -46,14 +46,28 @@ struct alignas(16) DevBsdf {
     float rft[kRftThetaMax];
 };
 
-// Procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp).
-enum TexKind : int32_t { kTexCheckerboard = 1, kTexGrid = 2, kTexScale = 3 };
+// Procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp) or
+// bitmap (src/texture/BitmapTexture.cpp over include/core/MipMap.hpp).
+enum TexKind : int32_t { kTexCheckerboard = 1, kTexGrid = 2, kTexScale = 3, kTexBitmap = 4 };
+enum TexFilter : int32_t { kFilterNearest = 0, kFilterBilinear = 1, kFilterTrilinear = 2, kFilterEwa = 3 };
+constexpr int kMipMaxLevels = 16;   // level 0 up to 32768 texels a side
+constexpr int kEwaLutSize = 128;
 struct alignas(16) DevTexture {
     int32_t kind, nested, count;     // nested: the scaled texture; count: blocks / lines
     float width, scale;              // grid line width; scale factor
     float uv_scale[2], uv_offset[2];
     float a[3], b[3];                // colorA / lineColor, colorB / backgroundColor
-    float pad;
+    // bitmap: MIP levels of power-of-two sizes, level l is (1 << max(0, lw - l)) x
+    // (1 << max(0, lh - l)) texels, row-major from v = 0; rgb texels are float4
+    // (w unused), r texels one float
+    int32_t filter;                  // TexFilter
+    int32_t channels, levels, lw, lh;
+    int32_t black;                   // a wrap mode is "black": every texel reads black
+    float max_aniso;
+    int32_t pad0, pad1;
+    const float *texels;             // level 0 first
+    const float *lut;                // EWA weights (kEwaLutSize)
+    uint32_t lvl_off[kMipMaxLevels]; // first texel of each level
 };
 
 // Per-mesh shading data.
@@ -100,6 +114,7 @@ struct DevScene {
     int32_t accel;                // kAccelBvh2 or kAccelBvh8: the tree the kernels traverse
     int32_t postpone;             // 8-wide traversal may postpone triangle tests (stack bound allows it)
     int32_t textured;             // some material has textures (the megakernel compiles lookups in)
+    int32_t ray_diff;             // a bitmap filters with the camera ray's differentials (first hits)
     const DevMesh *meshes;
     const DevBsdf *bsdfs;
     int32_t nmeshes, nbsdfs;

@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -19,6 +20,7 @@
 #include "hk_engine.h"
 #include "hk_internal.h"
 #include "hk_kernels.h"
+#include "hk_mipmap.h"
 #include "hk_wavefront.h"
 
 extern "C" int hk_scene_load_xml_impl(const char *path, const char *data_dir, hk_scene **out, int32_t *depth,
@@ -203,6 +205,7 @@ struct hk_scene {
     // inputs
     std::vector<hk_bsdf_desc> bsdfs;
     std::vector<hk_texture_desc> textures;
+    std::vector<std::shared_ptr<hk::MipPyramid>> bitmaps;   // per texture: the MIP pyramid of a bitmap, else null
     std::vector<MeshIn> meshes;
     std::vector<int> emitter_mesh;   // Scene order: mesh id, -1 environment, -2 - k delta_lights[k]
     struct DeltaLight { int directional; float color[3], vec[3]; };
@@ -227,7 +230,7 @@ struct hk_scene {
     hk::DevScene dev{};
     int32_t accel = HK_ACCEL_BVH8;
     DevBuf b_tris, b_nodes, b_wnodes, b_tri_normals, b_tri_uv, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
-        b_light_cdf, b_delta, b_textures, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
+        b_light_cdf, b_delta, b_textures, b_texels, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
     DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
     std::vector<std::unique_ptr<DevBuf>> batch_films;   // films of hk_render_batch_host
     hk_scene_info info{};
@@ -296,11 +299,15 @@ bool bsdf_transmits(const hk_scene *s, int id, int depth) {
 
 // Texture::GetAverage of the procedural textures (CheckerboardTexture.cpp:30,
 // GridTexture.cpp:40, ScaleTexture.cpp:28), used when BSDFs activate
-F3 tex_average(const std::vector<hk_texture_desc> &T, int id) {
-    const hk_texture_desc &t = T[id];
+F3 tex_average(const hk_scene *s, int id) {
+    const hk_texture_desc &t = s->textures[id];
     if (t.kind == HK_TEX_SCALE) {
-        F3 c = tex_average(T, t.nested);
+        F3 c = tex_average(s, t.nested);
         return {c.x * t.scale, c.y * t.scale, c.z * t.scale};
+    }
+    if (t.kind == HK_TEX_BITMAP) {   // BitmapTexture::GetAverage (src/texture/BitmapTexture.cpp:176)
+        const float *a = s->bitmaps[id]->avg;
+        return {a[0], a[1], a[2]};
     }
     if (t.kind == HK_TEX_CHECKERBOARD)
         return {(t.a[0] + t.b[0]) * 0.5f, (t.a[1] + t.b[1]) * 0.5f, (t.a[2] + t.b[2]) * 0.5f};
@@ -314,7 +321,7 @@ void par_average(const hk_scene *s, const hk_bsdf_desc &d, int slot, const float
         for (int k = 0; k < 3; k++) out[k] = c[k];
         return;
     }
-    F3 a = tex_average(s->textures, d.tex[slot] - 1);
+    F3 a = tex_average(s, d.tex[slot] - 1);
     out[0] = a.x; out[1] = a.y; out[2] = a.z;
 }
 bool bsdf_textured(const hk_scene *s, int id, int depth) {
@@ -439,12 +446,50 @@ void build_scene(hk_scene *s) {
     // BSDFs
     std::vector<hk::DevBsdf> bs;
     std::vector<hk::DevTexture> tex;
-    for (auto &t : s->textures) {
+    // bitmap texels: one pool in HBM, the EWA weights first, then each
+    // texture's levels (rgb as float4, 16-byte aligned; r as float)
+    std::vector<float> pool(hk::kEwaLutSize);
+    hk::ewa_weight_lut(pool.data());
+    std::vector<size_t> base(s->textures.size(), 0);
+    D.ray_diff = 0;
+    for (size_t i = 0; i < s->textures.size(); ++i) {
+        const hk::MipPyramid *m = s->bitmaps[i].get();
+        if (!m) continue;
+        pool.resize((pool.size() + 3) & ~size_t(3));
+        base[i] = pool.size();
+        for (auto &L : m->lv) {
+            if (m->channels == 1) {
+                pool.insert(pool.end(), L.begin(), L.end());
+            } else {
+                for (size_t k = 0; k < L.size(); k += 3) pool.insert(pool.end(), {L[k], L[k + 1], L[k + 2], 0.0f});
+            }
+        }
+        if (pool.size() - base[i] >= (size_t)UINT32_MAX) throw HkError{HK_ERR_INVALID, "bitmap texture too large"};
+        if (s->textures[i].filter >= HK_FILTER_TRILINEAR) D.ray_diff = 1;
+    }
+    if (pool.size() > hk::kEwaLutSize) { s->b_texels.upload(pool); track(s->b_texels); }
+    const float *texels = s->b_texels.as<float>();
+    for (size_t i = 0; i < s->textures.size(); ++i) {
+        const hk_texture_desc &t = s->textures[i];
         hk::DevTexture x;
         std::memset(&x, 0, sizeof x);
         x.kind = t.kind; x.nested = t.nested; x.count = t.count; x.width = t.width; x.scale = t.scale;
         for (int k = 0; k < 2; k++) { x.uv_scale[k] = t.uv_scale[k]; x.uv_offset[k] = t.uv_offset[k]; }
         for (int k = 0; k < 3; k++) { x.a[k] = t.a[k]; x.b[k] = t.b[k]; }
+        if (const hk::MipPyramid *m = s->bitmaps[i].get()) {
+            x.filter = t.filter;
+            x.channels = m->channels;
+            x.levels = m->levels; x.lw = m->lw; x.lh = m->lh;
+            x.black = (t.wrap_u == HK_WRAP_BLACK || t.wrap_v == HK_WRAP_BLACK) ? 1 : 0;
+            x.max_aniso = t.max_anisotropy;
+            x.texels = texels + base[i];
+            x.lut = texels;
+            uint32_t off = 0;
+            for (int l = 0; l < m->levels; ++l) {
+                x.lvl_off[l] = off;
+                off += (uint32_t)(m->lv[(size_t)l].size() / (size_t)m->channels);
+            }
+        }
         tex.push_back(x);
     }
     s->b_textures.upload(tex); track(s->b_textures);
@@ -840,6 +885,25 @@ int hk_scene_add_texture(hk_scene *s, const hk_texture_desc *d, int32_t *out_id)
         if (d->kind != HK_TEX_SCALE && d->count <= 0)
             throw HkError{HK_ERR_INVALID, "texture block / line count must be positive"};
         s->textures.push_back(*d);
+        s->bitmaps.push_back(nullptr);
+        if (out_id) *out_id = (int32_t)s->textures.size() - 1;
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_add_bitmap(hk_scene *s, const hk_texture_desc *d, const uint8_t *pixels, int32_t width, int32_t height,
+                        int32_t *out_id) {
+    return guarded([&] {
+        if (!s || !d) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (d->kind != HK_TEX_BITMAP) throw HkError{HK_ERR_INVALID, "bitmap texture expected"};
+        std::shared_ptr<hk::MipPyramid> m;
+        try {
+            m = std::make_shared<hk::MipPyramid>(hk::build_bitmap(*d, pixels, width, height));
+        } catch (const std::invalid_argument &e) {
+            throw HkError{HK_ERR_INVALID, e.what()};
+        }
+        s->textures.push_back(*d);
+        s->bitmaps.push_back(std::move(m));
         if (out_id) *out_id = (int32_t)s->textures.size() - 1;
         s->built = false;
         return HK_OK;
@@ -1357,15 +1421,26 @@ int hk_trace(hk_scene *s, uint64_t n, const float *rays, int32_t *tri, float *t,
     });
 }
 int hk_bsdf_batch(hk_scene *s, int32_t bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
-                  const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb,
-                  float *p_pdf, void *stream) {
+                  const float *wo, const float *uv, const float *duv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m,
+                  float *e_rgb, float *p_pdf, void *stream) {
     return guarded([&] {
         require_built(s);
         if (bsdf < 0 || bsdf >= s->dev.nbsdfs) throw HkError{HK_ERR_INVALID, "invalid BSDF id"};
         if (n == 0) return HK_OK;
         if (!wi || !u2 || !wo) throw HkError{HK_ERR_INVALID, "bad arguments"};
-        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, s->bsdfs[bsdf].type, n, wi, u2, u1, wo, uv, s_wo, s_w, s_pdf, s_m,
-                                      e_rgb, p_pdf, (cudaStream_t)stream));
+        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, s->bsdfs[bsdf].type, n, wi, u2, u1, wo, uv, duv, s_wo, s_w, s_pdf,
+                                      s_m, e_rgb, p_pdf, (cudaStream_t)stream));
+        return HK_OK;
+    });
+}
+int hk_texture_eval(hk_scene *s, int32_t tex, uint64_t n, const float *uv, const float *duv, float *out, void *stream) {
+    return guarded([&] {
+        require_built(s);
+        if (tex < 0 || tex >= (int)s->textures.size()) throw HkError{HK_ERR_INVALID, "invalid texture id"};
+        if (n == 0) return HK_OK;
+        if (!uv || !out) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        HK_CUDA(hk::launch_texture_eval(s->dev, s->b_textures.as<hk::DevTexture>(), tex, n, uv, duv, out,
+                                        (cudaStream_t)stream));
         return HK_OK;
     });
 }

@@ -26,12 +26,17 @@ __device__ __forceinline__ uint32_t mesh_emitter(const DevScene &S, int mesh) { 
 // (reference: every bounce), NEE over all emitters, MIS state carried across
 // bounces, unweighted environment on BSDF-sampled misses, the EDiscrete
 // override and Eigen's |c| <= 1e-5 zero test on throughput and NEE values.
-// kTex: the scene has textured materials (texture lookups compiled in)
+// kTex: the scene has textured materials (texture lookups compiled in); the
+// first hit's texture lookups filter with the camera ray's differentials
+// through film position (px, py), later hits have none (src/core/
+// Intersection.cpp:35).
 template <int kAccel, bool kTex>
-__device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, int rr_start, PathCounters &pc) {
+__device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float py, int depth_max, int rr_start,
+                         PathCounters &pc) {
     Hit hn;
     bool found_next = false;
     Isect it, itn;
+    float4 duv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     V3 L = v3(0, 0, 0), beta = v3(1, 1, 1);
     int depth = 0;
     float w_ems = 1.0f, w_mats = 1.0f;
@@ -45,7 +50,13 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
                 return ld3(S.background);
             }
             post_intersect(S, h, it);
+            if (kTex && S.ray_diff) {
+                V3 rx, ry;
+                camera_diff(S, S.cam, S.width, S.height, S.cam_aspect, px, py, rx, ry);
+                duv = screen_partials(S, h, it, ray.o, rx, ry);
+            }
         } else {
+            if (kTex) duv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             if (found_next) it = itn;
             else {
                 if (has_env) L = L + beta * env_eval(S, ray.d);
@@ -81,7 +92,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
                     br.wo = to_local(it.sh, er.wi);
                     br.measure = kMeasureSolidAngle;
                     br.eta = 0.0f;
-                    br.tu = it.u; br.tv = it.v; br.tex = kTex;
+                    br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv;
                     float pb = bsdf_pdf(S.bsdfs, bsdf, br);
                     if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
                     V3 f = bsdf_eval(S.bsdfs, bsdf, br);
@@ -96,7 +107,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, int depth_max, 
         br.wo = v3(0, 0, 0);
         br.measure = kMeasureUnknown;
         br.eta = 0.0f;
-        br.tu = it.u; br.tv = it.v; br.tex = kTex;
+        br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv;
         float sx = rng.nextf(), sy = rng.nextf();
         float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
         V3 F = bsdf_sample(S.bsdfs, bsdf, br, sx, sy, u1);
@@ -195,7 +206,7 @@ __global__ void __launch_bounds__(kTileThreads) render_pathmis_kernel(DevScene S
             for (int s = s0; s < s1; ++s) {
                 float px = (float)x + rng.nextf(), py = (float)y + rng.nextf();
                 Ray r = camera_ray(S, px, py);
-                V3 L = li_pathmis<kAccel, kTex>(S, rng, r, P.depth, P.rr_start, pc);
+                V3 L = li_pathmis<kAccel, kTex>(S, rng, r, px, py, P.depth, P.rr_start, pc);
                 if (!is_valid(L)) { ++dropped; continue; }
                 splat_shared(S, tile, tw, th, fx0, fy0, FW, FH, px, py, L);
             }
@@ -288,8 +299,8 @@ __global__ void trace_rays_kernel(DevScene S, uint64_t n, const float *rays, int
 // so a launch carries only that BSDF's code.
 template <int BT, bool kTex>
 __global__ void bsdf_batch_kernel(DevScene S, int bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
-                                  const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf,
-                                  int32_t *s_m, float *e_rgb, float *p_pdf) {
+                                  const float *wo, const float *uv, const float *duv, float *s_wo, float *s_w,
+                                  float *s_pdf, int32_t *s_m, float *e_rgb, float *p_pdf) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         BRec r;
         r.wi = v3(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
@@ -299,6 +310,8 @@ __global__ void bsdf_batch_kernel(DevScene S, int bsdf, uint64_t n, const float 
         r.tex = kTex;
         r.tu = kTex ? uv[2 * i] : 0.0f;
         r.tv = kTex ? uv[2 * i + 1] : 0.0f;
+        r.duv = (kTex && duv) ? make_float4(duv[4 * i], duv[4 * i + 1], duv[4 * i + 2], duv[4 * i + 3])
+                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         V3 w = bsdf_sample_t<BT>(S.bsdfs, bsdf, r, u2[2 * i], u2[2 * i + 1], u1 ? u1[i] : 0.0f);
         if (s_wo) { s_wo[3 * i] = r.wo.x; s_wo[3 * i + 1] = r.wo.y; s_wo[3 * i + 2] = r.wo.z; }
         if (s_w) { s_w[3 * i] = w.x; s_w[3 * i + 1] = w.y; s_w[3 * i + 2] = w.z; }
@@ -312,12 +325,31 @@ __global__ void bsdf_batch_kernel(DevScene S, int bsdf, uint64_t n, const float 
         q.tex = kTex;
         q.tu = r.tu;
         q.tv = r.tv;
+        q.duv = r.duv;
         if (e_rgb) {
             V3 e = bsdf_eval_t<BT>(S.bsdfs, bsdf, q);
             e_rgb[3 * i] = e.x; e_rgb[3 * i + 1] = e.y; e_rgb[3 * i + 2] = e.z;
         }
         if (p_pdf) p_pdf[i] = bsdf_pdf_t<BT>(S.bsdfs, bsdf, q);
     }
+}
+
+// Texture2D::Eval(Isect, filter = true) of texture `tex` at n texture
+// coordinates uv (n x 2) with screen-space partials duv (n x 4, or null): out n x 3.
+__global__ void texture_eval_kernel(DevScene S, const DevTexture *T, int tex, uint64_t n, const float *uv,
+                                    const float *duv, float *out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 d = duv ? make_float4(duv[4 * i], duv[4 * i + 1], duv[4 * i + 2], duv[4 * i + 3])
+                             : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const V3 c = tex_eval(T, tex, uv[2 * i], uv[2 * i + 1], d);
+        out[3 * i] = c.x; out[3 * i + 1] = c.y; out[3 * i + 2] = c.z;
+    }
+}
+cudaError_t launch_texture_eval(const DevScene &S, const DevTexture *T, int tex, uint64_t n, const float *uv,
+                                const float *duv, float *out, cudaStream_t st) {
+    const int g = (int)(n / 128 + 1 < 148 * 64 ? n / 128 + 1 : 148 * 64);
+    texture_eval_kernel<<<g, 128, 0, st>>>(S, T, tex, n, uv, duv, out);
+    return cudaGetLastError();
 }
 
 // Emitter record queries (parity tests).  in: n x 8 (ref xyz, ux, uy, u1, -, -)
@@ -415,13 +447,13 @@ cudaError_t launch_trace(const DevScene &S, uint64_t n, const float *rays, int32
     return cudaGetLastError();
 }
 cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, int type, uint64_t n, const float *wi, const float *u2, const float *u1,
-                              const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m,
-                              float *e_rgb, float *p_pdf, cudaStream_t st) {
+                              const float *wo, const float *uv, const float *duv, float *s_wo, float *s_w, float *s_pdf,
+                              int32_t *s_m, float *e_rgb, float *p_pdf, cudaStream_t st) {
     const int g = grid_for(n, 256);
 #define HK_BSDF_BATCH(T)                                                                                          \
     case T:                                                                                                       \
-        if (uv) bsdf_batch_kernel<T, true><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, uv, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); \
-        else bsdf_batch_kernel<T, false><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, uv, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); \
+        if (uv) bsdf_batch_kernel<T, true><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, uv, duv, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); \
+        else bsdf_batch_kernel<T, false><<<g, 256, 0, st>>>(S, bsdf, n, wi, u2, u1, wo, uv, duv, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf); \
         break
     switch (type) {
         HK_BSDF_BATCH(kDiffuse);

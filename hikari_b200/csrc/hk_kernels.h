@@ -41,8 +41,10 @@ cudaError_t launch_trace(const DevScene &S, uint64_t n, const float *rays, int32
                          int any_hit, unsigned long long *visits, cudaStream_t st);
 // type: top-level BSDF type of id `bsdf` (HK_BSDF_*)
 cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, int type, uint64_t n, const float *wi, const float *u2,
-                              const float *u1, const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf,
-                              int32_t *s_m, float *e_rgb, float *p_pdf, cudaStream_t st);
+                              const float *u1, const float *wo, const float *uv, const float *duv, float *s_wo, float *s_w,
+                              float *s_pdf, int32_t *s_m, float *e_rgb, float *p_pdf, cudaStream_t st);
+cudaError_t launch_texture_eval(const DevScene &S, const DevTexture *T, int tex, uint64_t n, const float *uv,
+                                const float *duv, float *out, cudaStream_t st);
 cudaError_t launch_emitter_sample(const DevScene &S, int e, uint64_t n, const float *in, float *out, cudaStream_t st);
 cudaError_t launch_camera_rays(const DevScene &S, uint64_t n, const float *pos, float *out, cudaStream_t st);
 cudaError_t launch_env_eval(const DevScene &S, uint64_t n, const float *wi, float *out, float *pdf, cudaStream_t st);

@@ -80,6 +80,61 @@ __device__ __forceinline__ void post_intersect(const DevScene &S, const Hit &h, 
     }
 }
 
+// Intersection::ComputeScreenSpacePartial (src/core/Intersection.cpp:30) of
+// the first hit of a camera ray from o with differential directions rx, ry:
+// (dUdX, dVdX, dUdY, dVdY), zero where the hit has no UV partials (a mesh
+// without normals or texture coordinates, a zero-area triangle).  dP/du and
+// dP/dv are those of Triangle::PostIntersect (src/core/Mesh.cpp:116-156).
+__device__ __forceinline__ float4 screen_partials(const DevScene &S, const Hit &h, const Isect &it, V3 o, V3 rx, V3 ry) {
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const DevMesh &m = S.meshes[it.mesh];
+    if (!m.has_uv || !m.has_normals) return zero;
+    const float4 *tp = S.tris + 3 * h.tri;
+    const float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
+    const V3 p0 = xyz(q0), dp1 = xyz(q1) - p0, dp2 = xyz(q2) - p0;
+    const V3 c = cross(dp1, dp2);
+    if (norm(c) == 0.0f) return zero;
+    const uint32_t orig = (uint32_t)__float_as_int(q0.w);
+    const float2 t0 = __ldg(S.tri_uv + 3 * orig), t1 = __ldg(S.tri_uv + 3 * orig + 1), t2 = __ldg(S.tri_uv + 3 * orig + 2);
+    const float du1 = t1.x - t0.x, dv1 = t1.y - t0.y, du2 = t2.x - t0.x, dv2 = t2.y - t0.y;
+    const float det = du1 * dv2 - dv1 * du2;
+    V3 dpdu, dpdv;
+    if (det == 0.0f) {
+        dpdu = it.sh.s;
+        dpdv = it.sh.t;
+    } else {
+        const float inv = 1.0f / det;
+        dpdu = (dp1 * dv2 - dp2 * dv1) * inv;
+        dpdv = (dp1 * (-du2) + dp2 * du1) * inv;
+    }
+    if (is_zero(dpdu) && is_zero(dpdv)) return zero;
+    const V3 n = normalize(c);
+    const float pp = dot(n, it.p), po = dot(n, o);
+    const float prx = dot(n, rx), pry = dot(n, ry);
+    if (prx == 0.0f || pry == 0.0f) return zero;
+    const float tx = (pp - po) / prx, ty = (pp - po) / pry;
+    const float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+    int a0, a1;
+    if (ax > ay && ax > az) { a0 = 1; a1 = 2; }
+    else if (ay > az) { a0 = 0; a1 = 2; }
+    else { a0 = 0; a1 = 1; }
+    auto c_of = [](V3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); };
+    const float A00 = c_of(dpdu, a0), A01 = c_of(dpdv, a0), A10 = c_of(dpdu, a1), A11 = c_of(dpdv, a1);
+    const V3 px = o + rx * tx, py = o + ry * ty;
+    float4 r;
+    // SolveLinearSystem2x2 (include/core/Common.hpp:881), its failure defaults
+    const float d = A00 * A11 - A01 * A10;
+    const bool ok = fabsf(d) > 1.0f / 3.40282347e+38f;
+    const float id = ok ? 1.0f / d : 0.0f;
+    const float bx0 = c_of(px, a0) - c_of(it.p, a0), bx1 = c_of(px, a1) - c_of(it.p, a1);
+    const float by0 = c_of(py, a0) - c_of(it.p, a0), by1 = c_of(py, a1) - c_of(it.p, a1);
+    r.x = ok ? (A11 * bx0 - A01 * bx1) * id : 1.0f;
+    r.y = ok ? (A00 * bx1 - A10 * bx0) * id : 0.0f;
+    r.z = ok ? (A11 * by0 - A01 * by1) * id : 0.0f;
+    r.w = ok ? (A00 * by1 - A10 * by0) * id : 1.0f;
+    return r;
+}
+
 // ------------------------------------------------------------ emitters
 struct ERec {
     V3 ref, p, n, wi;
@@ -265,6 +320,25 @@ __device__ __forceinline__ Ray camera_ray(const DevScene &S, float px, float py)
     r.tmin = S.cam_near * invz;
     r.tmax = S.cam_far * invz;
     return r;
+}
+
+// The differential ray directions of PerspectiveCamera::SampleRay (:94-98):
+// through the near-plane point moved by m_dX / m_dY (:64), one pixel along x
+// / y, in the closed form of the near-plane map.  M: row-major 3x4
+// camera-to-world; width, height, aspect: the image's.
+__device__ __forceinline__ void camera_diff(const DevScene &S, const float *M, uint32_t width, uint32_t height,
+                                            float aspect, float px, float py, V3 &rx, V3 &ry) {
+    const float iw = 1.0f / (float)width, ih = 1.0f / (float)height;
+    const float u = px * iw, v = py * ih;
+    const V3 np = v3(S.cam_near * (1.0f - 2.0f * u) / S.cam_cot, S.cam_near * (1.0f - 2.0f * v) / (aspect * S.cam_cot),
+                     S.cam_near);
+    const float dx = S.cam_near * (1.0f - 2.0f * iw) / S.cam_cot - S.cam_near / S.cam_cot;
+    const float dy = S.cam_near * (1.0f - 2.0f * ih) / (aspect * S.cam_cot) - S.cam_near / (aspect * S.cam_cot);
+    const V3 a = normalize(v3(np.x + dx, np.y, np.z)), b = normalize(v3(np.x, np.y + dy, np.z));
+    rx = v3(M[0] * a.x + M[1] * a.y + M[2] * a.z, M[4] * a.x + M[5] * a.y + M[6] * a.z,
+            M[8] * a.x + M[9] * a.y + M[10] * a.z);
+    ry = v3(M[0] * b.x + M[1] * b.y + M[2] * b.z, M[4] * b.x + M[5] * b.y + M[6] * b.z,
+            M[8] * b.x + M[9] * b.y + M[10] * b.z);
 }
 
 }  // namespace hk

@@ -346,20 +346,28 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                         pb.wo = v3(pwo.x, pwo.y, pwo.z);
                         pb.measure = __float_as_int(pwo.w);
                         pb.eta = 0.0f;
-                        pb.tex = S.bsdfs[__float_as_int(pwi.w)].textured != 0;
+                        pb.tex = false;
                         pb.tu = pb.tv = 0.0f;
-                        if (pb.tex) {
-                            const float2 puv = W.prev_uv[slot];
-                            pb.tu = puv.x;
-                            pb.tv = puv.y;
-                        }
                         float plm = area_pdf(AL, er);
-                        float pbm = bsdf_pdf(S.bsdfs, __float_as_int(pwi.w), pb);
+                        // a textured BSDF's pdf was taken when it sampled (its
+                        // parameters depend on that vertex's texture lookups)
+                        float pbm = S.bsdfs[__float_as_int(pwi.w)].textured ? W.prev_pdf[slot]
+                                                                            : bsdf_pdf(S.bsdfs, __float_as_int(pwi.w), pb);
                         if (pbm + plm != 0.0f) w_mats = pbm / (pbm + plm);
                     }
                 }
                 const V3 Le = (beta * w_mats) * area_eval(AL, er);
                 if (!all_zero(Le)) red_add_v4(W.lacc + slot, Le.x, Le.y, Le.z, 0.0f);
+            }
+            // screen-space partials of a camera ray's first hit (textured
+            // materials only: Intersection::ComputeScreenSpacePartial)
+            float4 duv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if constexpr (BT < 0) {
+                if (depth == 0 && S.ray_diff) {
+                    V3 rx, ry;
+                    camera_diff(S, J.cam, J.width, J.height, J.cam_aspect, p4.x, p4.y, rx, ry);
+                    duv = screen_partials(S, h, it, ro, rx, ry);
+                }
             }
             // next-event estimation over every emitter (PathMISIntegrator.cpp:83-109)
             const V3 wi_local = to_local(it.sh, rd * -1.0f);
@@ -380,6 +388,7 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                 br.tex = BT < 0;   // textured materials are shaded by the run-time-dispatched kernel
                 br.tu = it.u;
                 br.tv = it.v;
+                if constexpr (BT < 0) br.duv = duv;   // unread where lookups are compiled out
                 float pl = er.pdf;
                 float pb = bsdf_pdf_t<BT>(S.bsdfs, bsdf, br);
                 float w = (pl + pb != 0.0f) ? pl / (pl + pb) : 1.0f;
@@ -404,6 +413,7 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             br.tex = BT < 0;
             br.tu = it.u;
             br.tv = it.v;
+            if constexpr (BT < 0) br.duv = duv;
             float sx = rng.nextf(), sy = rng.nextf();
             float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
             V3 F = bsdf_sample_t<BT>(S.bsdfs, bsdf, br, sx, sy, u1);
@@ -431,7 +441,13 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             W.prev_wi[slot] = f4(br.wi, __int_as_float(bsdf));
             W.prev_wo[slot] = f4(br.wo, __int_as_float(br.measure));
             if constexpr (BT < 0) {
-                if (S.bsdfs[bsdf].textured) W.prev_uv[slot] = make_float2(it.u, it.v);
+                // the MIS weight at an emitter hit next needs this BSDF's pdf of
+                // the sampled direction (PathMISIntegrator.cpp:128)
+                if (S.bsdfs[bsdf].textured && !(flags & kWfFlagForceMats)) {
+                    BRec pr = br;
+                    pr.eta = 0.0f;
+                    W.prev_pdf[slot] = bsdf_pdf_t<BT>(S.bsdfs, bsdf, pr);
+                }
             }
             W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
                                      (uint32_t)(rng.inc >> 32));

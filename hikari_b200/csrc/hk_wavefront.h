@@ -89,7 +89,7 @@ struct WfState {
     uint4 *rng;         // pcg32 state, increment
     float4 *prev_wi;    // previous vertex: BSDF record wi.xyz, bits(bsdf id)
     float4 *prev_wo;    // previous vertex: BSDF record wo.xyz, bits(measure)
-    float2 *prev_uv;    // previous vertex: texture coordinates (written for textured materials only)
+    float *prev_pdf;    // previous vertex: its BSDF's pdf of the sampled direction (textured materials only)
     float4 *hit;        // t, u, v, bits(tri in leaf order or -1)
     // queues
     int *eq[2];

@@ -50,16 +50,23 @@ class SceneError(RuntimeError):
 
 
 # Procedural textures, matching hk_texture_kind in include/hikari_b200.h
-TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE = 1, 2, 3
-TEX_TYPE_NAMES = {"checkerboard": TEX_CHECKERBOARD, "grid": TEX_GRID, "scale": TEX_SCALE}
+TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE, TEX_BITMAP = 1, 2, 3, 4
+TEX_TYPE_NAMES = {"checkerboard": TEX_CHECKERBOARD, "grid": TEX_GRID, "scale": TEX_SCALE, "bitmap": TEX_BITMAP}
+# bitmap "filterType" and "uWrapMode" / "vWrapMode" (src/texture/BitmapTexture.cpp:15-46)
+FILTER_NEAREST, FILTER_BILINEAR, FILTER_TRILINEAR, FILTER_EWA = 0, 1, 2, 3
+FILTER_NAMES = {"nearest": FILTER_NEAREST, "bilinear": FILTER_BILINEAR, "trilinear": FILTER_TRILINEAR,
+                "ewa": FILTER_EWA}
+WRAP_REPEAT, WRAP_CLAMP, WRAP_BLACK = 0, 1, 2
+WRAP_NAMES = {"repeat": WRAP_REPEAT, "clamp": WRAP_CLAMP, "black": WRAP_BLACK}
 # textured BSDF parameters, in the order of hk_bsdf_desc.tex
 TEX_SLOTS = ("kd", "ks", "ks_refract", "sigma_a", "alpha_u", "alpha_v")
 
 
 @dataclass
 class TextureDesc:
-    """A procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp);
-    defaults are the reference's (include/core/Common.hpp:436-458)."""
+    """A procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp)
+    or a bitmap (src/texture/BitmapTexture.cpp); defaults are the reference's
+    (include/core/Common.hpp:425-458)."""
     kind: int
     count: int = 10                    # checkerboard "blocks", grid "lines"
     width: float = 0.01                # grid "lineWidth"
@@ -69,6 +76,14 @@ class TextureDesc:
     a: List[float] = field(default_factory=lambda: [0.4, 0.4, 0.4])   # colorA / lineColor
     b: List[float] = field(default_factory=lambda: [0.2, 0.2, 0.2])   # colorB / backgroundColor
     nested: Optional["TextureDesc"] = None                           # scale: the scaled texture
+    # bitmap: 8-bit pixels as stbi_load returns them (height x width x channels, row 0 = top)
+    pixels: Optional[np.ndarray] = None
+    filter: int = FILTER_EWA
+    wrap_u: int = WRAP_REPEAT
+    wrap_v: int = WRAP_REPEAT
+    channels: int = 3                  # "channel": r (1) or rgb (3)
+    gamma: float = 1.0
+    max_anisotropy: float = 20.0
 
 
 @dataclass

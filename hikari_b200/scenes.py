@@ -21,8 +21,9 @@ import numpy as np
 
 from .scenedesc import (AIR_IOR, BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR,
                         BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
-                        BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX, TEX_CHECKERBOARD, TEX_GRID,
-                        TEX_SCALE, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, LightDesc, MeshDesc, SceneDesc,
+                        BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, FILTER_BILINEAR, FILTER_EWA,
+                        FILTER_NEAREST, FILTER_TRILINEAR, GGX, TEX_BITMAP, TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE,
+                        WRAP_CLAMP, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, LightDesc, MeshDesc, SceneDesc,
                         TextureDesc)
 
 # Per-channel complex IOR (n, k) of copper and gold at R, G, B ~ (650, 550, 450) nm,
@@ -177,8 +178,20 @@ def spherical_uv(P: np.ndarray, center) -> np.ndarray:
     return np.stack([u, v], 1).astype(np.float32)
 
 
+def synthetic_image(width: int, height: int, channels: int, seed: int) -> np.ndarray:
+    """8-bit test pixels (height x width x channels, row 0 = top): smooth
+    gradients, a fine stripe pattern and noise, so that every MIP level and
+    filter footprint sees structure."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:height, 0:width]
+    base = np.stack([x * 255 // max(width - 1, 1), y * 255 // max(height - 1, 1), ((x // 3 + y // 3) % 2) * 200 + 30],
+                    -1)
+    img = (0.7 * base + 0.3 * rng.integers(0, 256, (height, width, 3))).astype(np.uint8)
+    return np.ascontiguousarray(img[:, :, :channels])
+
+
 def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 12, seed: int = 0,
-                 shading_normals: bool = False, textured: bool = False) -> SceneDesc:
+                 shading_normals: bool = False, textured: bool = False, bitmap: bool = False) -> SceneDesc:
     """A ground quad and five displaced icospheres (diffuse, roughDiffuse,
     smooth plastic, rough conductor, smooth dielectric) lit, in emitter order,
     by a point light, an emissive quad, a constant environment and a
@@ -189,7 +202,12 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
     shading_normals) adds procedural textures: a checkerboard ground, a grid on
     the diffuse sphere, checkerboard roughness on the roughDiffuse sphere, a
     scaled checkerboard on the plastic's kd, textured alphaU / alphaV on the
-    conductor and a grid on the glass's refraction colour."""
+    conductor and a grid on the glass's refraction colour.  bitmap (with
+    textured) swaps in bitmap textures where they differ most: an EWA-filtered
+    ground (with vertex normals, so first hits carry screen-space partials), a
+    trilinear albedo on the diffuse sphere, a bilinear roughDiffuse albedo, a
+    scaled one-channel EWA roughness on the conductor and a nearest, clamped
+    refraction colour on the glass."""
     sd = SceneDesc()
     gp, gi = quad((-6, 0, 6), (6, 0, 6), (6, 0, -6), (-6, 0, -6))
     ground = MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5]))
@@ -197,6 +215,10 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
         ground.uv = np.float32([[0, 0], [1, 0], [1, 1], [0, 1]])
         ground.bsdf.textures["kd"] = TextureDesc(kind=TEX_CHECKERBOARD, count=12, a=[0.7, 0.7, 0.65],
                                                  b=[0.15, 0.2, 0.3])
+        if bitmap:
+            ground.normals = np.float32([[0, 1, 0]] * 4)
+            ground.bsdf.textures["kd"] = TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(96, 80, 3, seed + 1),
+                                                     filter=FILTER_EWA, gamma=2.2, uv_scale=[3.0, 3.0])
     sd.meshes.append(ground)
     mats = [BSDFDesc(type=BSDF_DIFFUSE, kd=[0.7, 0.3, 0.2]),
             BSDFDesc(type=BSDF_ROUGH_DIFFUSE, kd=[0.3, 0.6, 0.3], alpha_u=0.6, alpha_v=0.6),
@@ -218,6 +240,16 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
                                                   b=[0.05] * 3)
         mats[4].textures["ks_refract"] = TextureDesc(kind=TEX_GRID, count=6, width=0.05, a=[0.2, 0.2, 0.2],
                                                      b=[1.0, 1.0, 1.0])
+    if textured and bitmap:
+        mats[0].textures["kd"] = TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(64, 64, 3, seed + 2),
+                                             filter=FILTER_TRILINEAR)
+        mats[1].textures["kd"] = TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(40, 30, 3, seed + 3),
+                                             filter=FILTER_BILINEAR)
+        mats[3].textures["alpha_u"] = TextureDesc(
+            kind=TEX_SCALE, scale=0.5, nested=TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(50, 70, 1, seed + 4),
+                                                          channels=1, filter=FILTER_EWA, max_anisotropy=8.0))
+        mats[4].textures["ks_refract"] = TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(33, 17, 3, seed + 5),
+                                                     filter=FILTER_NEAREST, wrap_u=WRAP_CLAMP, wrap_v=WRAP_CLAMP)
     for k, b in enumerate(mats):
         c = (-3.2 + 1.6 * k, 0.85, 0.3 * ((k % 2) * 2 - 1))
         P, F = displaced_icosphere(2, 0.8, c, 0.05, seed + k)

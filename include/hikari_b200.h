@@ -95,10 +95,21 @@ int hk_version(void);
 /* ---- scene construction (Scene::AddChild src/core/Scene.cpp:167 order) ---- */
 int hk_scene_create(hk_scene **out);
 int hk_scene_destroy(hk_scene *s);
-/* Procedural textures (src/texture/{Checkerboard,Grid,Scale}Texture.cpp). */
+/* Procedural textures (src/texture/{Checkerboard,Grid,Scale}Texture.cpp) and
+ * bitmaps (src/texture/BitmapTexture.cpp over include/core/MipMap.hpp). */
 #define HK_TEX_CHECKERBOARD 1
 #define HK_TEX_GRID 2
 #define HK_TEX_SCALE 3
+#define HK_TEX_BITMAP 4
+/* bitmap "filterType" */
+#define HK_FILTER_NEAREST 0
+#define HK_FILTER_BILINEAR 1
+#define HK_FILTER_TRILINEAR 2
+#define HK_FILTER_EWA 3
+/* bitmap "uWrapMode" / "vWrapMode" */
+#define HK_WRAP_REPEAT 0
+#define HK_WRAP_CLAMP 1
+#define HK_WRAP_BLACK 2
 typedef struct {
     int32_t kind;          /* HK_TEX_* */
     int32_t nested;        /* scale: id of the scaled texture (added first) */
@@ -107,8 +118,25 @@ typedef struct {
     float scale;           /* scale "scale" */
     float uv_scale[2], uv_offset[2];   /* "uScale" "vScale", "uOffset" "vOffset" */
     float a[3], b[3];      /* checkerboard colorA / colorB; grid lineColor / backgroundColor */
+    /* bitmap: "filterType" (HK_FILTER_*), "uWrapMode" / "vWrapMode" (HK_WRAP_*),
+     * "channel" (1 = r, 3 = rgb), "gamma", "maxAnisotropy" */
+    int32_t filter, wrap_u, wrap_v, channels;
+    float gamma, max_anisotropy;
 } hk_texture_desc;
 int hk_scene_add_texture(hk_scene *s, const hk_texture_desc *desc, int32_t *out_id);
+/* A bitmap texture (desc->kind HK_TEX_BITMAP) from 8-bit pixels as stbi_load
+ * returns them to LoadImageFromFileR / RGB (src/core/Texture.cpp:12, :74):
+ * row 0 is the image's top row, desc->channels bytes per pixel.  The gamma
+ * correction, the resampling to power-of-two sizes and the MIP pyramid
+ * (include/core/MipMap.hpp:67) are built on the host when the scene is added
+ * to; the pyramid lives in HBM from hk_scene_build on. */
+int hk_scene_add_bitmap(hk_scene *s, const hk_texture_desc *desc, const uint8_t *pixels, int32_t width,
+                        int32_t height, int32_t *out_id);
+/* Decode an 8-bit image file (PNG, binary PGM / PPM, baseline JPEG) into
+ * `channels` (1 or 3) bytes per pixel, row 0 = top, like stbi_load with that
+ * request.  *out is allocated by the library (hk_image_free). */
+int hk_image_load(const char *path, int32_t channels, int32_t *width, int32_t *height, uint8_t **out);
+void hk_image_free(uint8_t *p);
 /* Raw bytes of data/BeckmannRFTData.bin (distribution 0) or GGXRFTData.bin (1),
  * the RoughTransmittance table file (src/core/RoughTransmitance.cpp:9). */
 int hk_scene_set_rft(hk_scene *s, int distribution, const void *bytes, uint64_t nbytes);
@@ -364,8 +392,15 @@ int hk_trace(hk_scene *s, uint64_t n, const float *rays_dev, int32_t *tri_dev, f
  * may be NULL): sampled wo, weight, pdf of the sample, measure; Eval and Pdf at
  * wo (ESolidAngle). */
 int hk_bsdf_batch(hk_scene *s, int32_t bsdf, uint64_t n, const float *wi_dev, const float *u2_dev, const float *u1_dev,
-                  const float *wo_dev, const float *uv_dev, float *s_wo_dev, float *s_w_dev, float *s_pdf_dev,
-                  int32_t *s_measure_dev, float *e_rgb_dev, float *p_pdf_dev, void *stream);
+                  const float *wo_dev, const float *uv_dev, const float *duv_dev, float *s_wo_dev, float *s_w_dev,
+                  float *s_pdf_dev, int32_t *s_measure_dev, float *e_rgb_dev, float *p_pdf_dev, void *stream);
+/* (duv: n x 4 screen-space partials of the texture coordinates, (dUdX, dVdX,
+ * dUdY, dVdY) per record, or NULL = 0; used by filtered bitmap lookups) */
+/* Texture2D::Eval(Isect, filter = true) (src/core/Texture.cpp:211) of texture
+ * `tex` at n texture coordinates uv (n x 2) with partials duv (n x 4 or NULL):
+ * out n x 3. */
+int hk_texture_eval(hk_scene *s, int32_t tex, uint64_t n, const float *uv_dev, const float *duv_dev, float *out_dev,
+                    void *stream);
 /* Emitter::Sample (include/core/Emitter.hpp:77) for emitter e: in n x 8
  * (ref xyz, u2, u1, -, -), out n x 16 (p, n, wi, pdf, distance, value, -). */
 int hk_emitter_sample(hk_scene *s, int32_t e, uint64_t n, const float *in_dev, float *out_dev, void *stream);

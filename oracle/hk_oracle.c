@@ -11,6 +11,7 @@
 #define _GNU_SOURCE
 #include "hk_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -390,9 +391,231 @@ typedef struct {
     int rft_n;
     float fdr_int;                     /* plastic: 1 - IntData.EvalDiffuse(alpha) */
     const ho_texture_desc *textures;   /* the scene's textures (set when finalized) */
+    struct mip_t *const *mips;         /* their MIP pyramids (bitmaps; NULL otherwise) */
 } bsdf_t;
 
-typedef struct { v3 wi, wo; float eta; int measure; float uv[2]; } brec;   /* uv: Record.Isect.UV */
+/* uv: Record.Isect.UV; duv: its screen-space partials (dUdX, dVdX, dUdY, dVdY) */
+typedef struct { v3 wi, wo; float eta; int measure; float uv[2]; float duv[4]; } brec;
+
+/* ------------------------------------------------------------ bitmap textures */
+/* LoadImageFromFileR / LoadImageFromFileRGB (src/core/Texture.cpp:12, :74):
+ * 8-bit pixels -> gamma-corrected floats, rows flipped (row 0 = v 0 = the
+ * image's bottom row), average over x-major order.  MipMap<T> (include/core/
+ * MipMap.hpp:67): Lanczos resampling to power-of-two sizes, then a 2x2 box
+ * pyramid; lookups Lookup(UV) :281 (nearest), Lookup(UV, width) :287
+ * (bilinear / trilinear), Lookup(UV, D0, D1) :309 (trilinear or EWA). */
+#define HO_MIP_MAX 32
+typedef struct mip_t {
+    int ch, levels, black, trilinear;
+    float max_aniso;
+    int w[HO_MIP_MAX], h[HO_MIP_MAX];
+    float *lv[HO_MIP_MAX];     /* 3 floats per texel (one channel: all three equal) */
+    float avg[3];
+} mip_t;
+
+static float ewa_lut[128];    /* MipMap::s_WeightLut: exp(-2 r^2) - exp(-2) at r^2 = i / 127 */
+static void ewa_lut_init(void) {
+    if (ewa_lut[0] != 0.0f) return;
+    for (int i = 0; i < 128; i++) {
+        float alpha = 2.0f, r2 = (float)i / (float)(128 - 1);
+        ewa_lut[i] = expf(-alpha * r2) - expf(-alpha);
+    }
+}
+static void mip_free(mip_t *m) {
+    if (!m) return;
+    for (int i = 0; i < m->levels; i++) free(m->lv[i]);
+    free(m);
+}
+static int is_pow2(int v) { return v && !(v & (v - 1)); }
+static int round_up_pow2(int v) {
+    v--; v |= v >> 1; v |= v >> 2; v |= v >> 4; v |= v >> 8; v |= v >> 16;
+    return v + 1;
+}
+static int log2_int(uint32_t v) { int r = 0; while (v >>= 1) r++; return r; }
+static int mod_int(int a, int b) { int r = a % b; return r < 0 ? r + b : r; }
+static int clamp_int(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+/* Lanczos (src/core/MipMap.cpp:5), as written there: sin(x tau)/(x tau) * sin(x)/x */
+static float lanczos(float x, float tau) {
+    x = fabsf(x);
+    float sa = sinf(x * tau) / (x * tau);
+    float lz = sinf(x) / x;
+    return sa * lz;
+}
+typedef struct { int first; float w[4]; } rs_weight;
+/* MipMap::GetResampleWeights :386 */
+static rs_weight *resample_weights(int old_n, int new_n) {
+    rs_weight *W = malloc(sizeof *W * (size_t)new_n);
+    const float fw = 2.0f;
+    for (int i = 0; i < new_n; i++) {
+        float center = ((float)i + 0.5f) * (float)old_n / (float)new_n;
+        W[i].first = (int)floorf((center - fw) + 0.5f);
+        for (int j = 0; j < 4; j++) {
+            float pos = (float)(W[i].first + j) + 0.5f;
+            W[i].w[j] = lanczos((pos - center) / fw, 2.0f);
+        }
+        float inv = 1.0f / (((W[i].w[0] + W[i].w[1]) + W[i].w[2]) + W[i].w[3]);
+        for (int j = 0; j < 4; j++) W[i].w[j] *= inv;
+    }
+    return W;
+}
+static int wrap_index(int x, int n, int wrap) {
+    if (wrap == HO_WRAP_REPEAT) return mod_int(x, n);
+    if (wrap == HO_WRAP_CLAMP) return clamp_int(x, 0, n - 1);
+    return x;
+}
+/* MipMap::Texel :244 -- any coordinate outside the level, and every texel
+ * when a wrap mode is "black", reads black (the wrap switch that follows is
+ * reached only for coordinates already inside). */
+static inline v3 mip_texel(const mip_t *m, int l, int x, int y) {
+    if (m->black || x < 0 || x >= m->w[l] || y < 0 || y >= m->h[l]) return V(0, 0, 0);
+    return vload(m->lv[l] + 3 * ((size_t)y * m->w[l] + x));
+}
+static float clamp_max(float v) { return v < 0.0f ? 0.0f : (v > FLT_MAX ? FLT_MAX : v); }
+/* texels: w * h * 3 floats (gamma-corrected, flipped); ch 1 stores x in all three. */
+static mip_t *mip_build(const float *texels, int w, int h, int ch, int wrap_u, int wrap_v, int trilinear,
+                        float max_aniso) {
+    ewa_lut_init();
+    mip_t *m = calloc(1, sizeof *m);
+    m->ch = ch; m->trilinear = trilinear; m->max_aniso = max_aniso;
+    m->black = wrap_u == HO_WRAP_BLACK || wrap_v == HO_WRAP_BLACK;
+    int W = w, H = h;
+    float *l0;
+    if (!is_pow2(w) || !is_pow2(h)) {
+        W = round_up_pow2(w); H = round_up_pow2(h);
+        rs_weight *uw = resample_weights(w, W);
+        l0 = malloc(sizeof(float) * 3 * (size_t)W * H);
+        for (int v = 0; v < h; v++)
+            for (int u = 0; u < W; u++) {
+                float acc[3] = {0, 0, 0};
+                for (int j = 0; j < 4; j++) {
+                    int ou = wrap_index(uw[u].first + j, w, wrap_u);
+                    if (ou >= 0 && ou < w)
+                        for (int c = 0; c < 3; c++) acc[c] += uw[u].w[j] * texels[3 * ((size_t)v * w + ou) + c];
+                }
+                for (int c = 0; c < 3; c++) l0[3 * ((size_t)v * W + u) + c] = acc[c];
+            }
+        free(uw);
+        rs_weight *vw = resample_weights(h, H);
+        float *col = malloc(sizeof(float) * 3 * (size_t)H);
+        for (int u = 0; u < W; u++) {
+            for (int v = 0; v < H; v++) {
+                float acc[3] = {0, 0, 0};
+                for (int j = 0; j < 4; j++) {
+                    int ov = wrap_index(vw[v].first + j, h, wrap_v);
+                    if (ov >= 0 && ov < h)
+                        for (int c = 0; c < 3; c++) acc[c] += vw[v].w[j] * l0[3 * ((size_t)ov * W + u) + c];
+                }
+                for (int c = 0; c < 3; c++) col[3 * v + c] = acc[c];
+            }
+            for (int v = 0; v < H; v++)
+                for (int c = 0; c < 3; c++) l0[3 * ((size_t)v * W + u) + c] = clamp_max(col[3 * v + c]);
+        }
+        free(col); free(vw);
+    } else {
+        l0 = malloc(sizeof(float) * 3 * (size_t)W * H);
+        memcpy(l0, texels, sizeof(float) * 3 * (size_t)W * H);
+    }
+    m->levels = 1 + log2_int((uint32_t)(W > H ? W : H));
+    m->w[0] = W; m->h[0] = H; m->lv[0] = l0;
+    for (int i = 1; i < m->levels; i++) {
+        int ur = m->w[i - 1] / 2 > 1 ? m->w[i - 1] / 2 : 1, vr = m->h[i - 1] / 2 > 1 ? m->h[i - 1] / 2 : 1;
+        m->w[i] = ur; m->h[i] = vr;
+        m->lv[i] = malloc(sizeof(float) * 3 * (size_t)ur * vr);
+        for (int v = 0; v < vr; v++)
+            for (int u = 0; u < ur; u++) {
+                v3 a = mip_texel(m, i - 1, 2 * u, 2 * v), b = mip_texel(m, i - 1, 2 * u + 1, 2 * v);
+                v3 c = mip_texel(m, i - 1, 2 * u, 2 * v + 1), d = mip_texel(m, i - 1, 2 * u + 1, 2 * v + 1);
+                vstore(m->lv[i] + 3 * ((size_t)v * ur + u), scl(add(add(add(a, b), c), d), 0.25f));
+            }
+    }
+    return m;
+}
+/* MipMap::Triangle :412 (bilinear at one level) */
+static v3 mip_triangle(const mip_t *m, int l, float u, float v) {
+    l = clamp_int(l, 0, m->levels - 1);
+    float U = u * (float)m->w[l] - 0.5f, Vv = v * (float)m->h[l] - 0.5f;
+    int u0 = (int)floorf(U), v0 = (int)floorf(Vv);
+    float du = U - (float)u0, dv = Vv - (float)v0;
+    v3 t00 = mip_texel(m, l, u0, v0), t01 = mip_texel(m, l, u0, v0 + 1);
+    v3 t10 = mip_texel(m, l, u0 + 1, v0), t11 = mip_texel(m, l, u0 + 1, v0 + 1);
+    float a = (1.0f - du) * (1.0f - dv), b = (1.0f - du) * dv, c = du * (1.0f - dv), d = du * dv;
+    return add(add(add(scl(t00, a), scl(t01, b)), scl(t10, c)), scl(t11, d));
+}
+static v3 lerp3(float t, v3 a, v3 b) { return add(scl(a, 1.0f - t), scl(b, t)); }
+/* MipMap::Lookup(UV, Width) :287 */
+static v3 mip_lookup_width(const mip_t *m, float u, float v, float width) {
+    float level = (float)m->levels - 1.0f + log2f(fmaxf(width, 1e-8f));
+    if (level < 0.0f) return mip_triangle(m, 0, u, v);
+    if (level >= (float)(m->levels - 1)) return mip_texel(m, m->levels - 1, 0, 0);
+    int il = (int)floorf(level);
+    float delta = level - (float)il;
+    return lerp3(delta, mip_triangle(m, il, u, v), mip_triangle(m, il + 1, u, v));
+}
+/* MipMap::EWA :427 */
+static v3 mip_ewa(const mip_t *m, int l, float u, float v, float d0x, float d0y, float d1x, float d1y) {
+    if (l >= m->levels) return mip_texel(m, m->levels - 1, 0, 0);
+    float W = (float)m->w[l], H = (float)m->h[l];
+    u = u * W - 0.5f; v = v * H - 0.5f;
+    d0x *= W; d0y *= H; d1x *= W; d1y *= H;
+    float A = (d0y * d0y + d1y * d1y) + 1.0f;
+    float B = -2.0f * (d0x * d0y + d1x * d1y);
+    float C = (d0x * d0x + d1x * d1x) + 1.0f;
+    float invf = 1.0f / (A * C - (B * B) * 0.25f);
+    A *= invf; B *= invf; C *= invf;
+    float det = (-B) * B + (4.0f * A) * C;
+    float invdet = 1.0f / det;
+    float usq = sqrtf(det * C), vsq = sqrtf(A * det);
+    int u0 = (int)ceilf(u - (2.0f * invdet) * usq), u1 = (int)floorf(u + (2.0f * invdet) * usq);
+    int v0 = (int)ceilf(v - (2.0f * invdet) * vsq), v1 = (int)floorf(v + (2.0f * invdet) * vsq);
+    v3 sum = V(0, 0, 0);
+    float sw = 0.0f;
+    for (int iv = v0; iv <= v1; ++iv) {
+        float dv = (float)iv - v;
+        for (int iu = u0; iu <= u1; ++iu) {
+            float du = (float)iu - u;
+            float r2 = ((A * du) * du + (B * du) * dv) + (C * dv) * dv;
+            if (r2 < 1.0f) {
+                int idx = (int)(r2 * 128.0f);
+                if (idx > 127) idx = 127;
+                float wt = ewa_lut[idx];
+                sum = add(sum, scl(mip_texel(m, l, iu, iv), wt));
+                sw += wt;
+            }
+        }
+    }
+    return divs(sum, sw);
+}
+/* MipMap::Lookup(UV, D0, D1) :309 */
+static v3 mip_lookup_diff(const mip_t *m, float u, float v, float d0x, float d0y, float d1x, float d1y) {
+    if (m->trilinear) {
+        float w = fmaxf(fmaxf(fabsf(d0x), fabsf(d0y)), fmaxf(fabsf(d1x), fabsf(d1y)));
+        return mip_lookup_width(m, u, v, 2.0f * w);
+    }
+    if (d0x * d0x + d0y * d0y < d1x * d1x + d1y * d1y) {
+        float tx = d0x, ty = d0y; d0x = d1x; d0y = d1y; d1x = tx; d1y = ty;
+    }
+    float major = sqrtf(d0x * d0x + d0y * d0y), minor = sqrtf(d1x * d1x + d1y * d1y);
+    if (minor * m->max_aniso < major && minor > 0.0f) {
+        float sc = major / (minor * m->max_aniso);
+        d1x *= sc; d1y *= sc;
+        minor *= sc;
+    }
+    if (minor == 0.0f) return mip_triangle(m, 0, u, v);
+    float lod = fmaxf(0.0f, (float)m->levels - 1.0f + log2f(minor));
+    float ilod = floorf(lod);
+    return lerp3(lod - ilod, mip_ewa(m, (int)ilod, u, v, d0x, d0y, d1x, d1y),
+                 mip_ewa(m, (int)(ilod + 1.0f), u, v, d0x, d0y, d1x, d1y));
+}
+/* BitmapTexture::Eval(UV, D0, D1) (src/texture/BitmapTexture.cpp:101) after
+ * Texture2D::Eval (src/core/Texture.cpp:211) scaled and offset UV and D. */
+static v3 bitmap_eval(const ho_texture_desc *t, const mip_t *m, const float *uvi, const float *duv) {
+    float u = uvi[0] * t->uv_scale[0] + t->uv_offset[0], v = uvi[1] * t->uv_scale[1] + t->uv_offset[1];
+    if (t->filter == HO_FILTER_NEAREST)
+        return mip_texel(m, 0, (int)floorf(u * (float)m->w[0]), (int)floorf(v * (float)m->h[0]));
+    if (t->filter == HO_FILTER_BILINEAR) return mip_lookup_width(m, u, v, 0.0f);
+    return mip_lookup_diff(m, u, v, duv[0] * t->uv_scale[0], duv[1] * t->uv_scale[1], duv[2] * t->uv_scale[0],
+                           duv[3] * t->uv_scale[1]);
+}
 
 struct ho_scene;
 static v3 bsdf_eval(const struct ho_scene *s, int id, const brec *r);
@@ -419,7 +642,8 @@ typedef struct { float bmin[3], bmax[3]; int32_t left_or_first, count, axis, rig
 
 struct ho_scene {
     int nb, cap_b; bsdf_t *bsdfs;
-    int ntex, cap_tex; ho_texture_desc *tex;
+    int ntex, cap_tex; ho_texture_desc *tex; struct mip_t **mips;
+    int ray_diff;                      /* a bitmap texture filters with the camera ray's differentials */
     int nm, cap_m; mesh_t *meshes;
     float *P; float *N; float *UV; uint32_t nv, cap_v;   /* global vertices (world space); UV 2 per vertex */
     uint32_t *F; int32_t *tri_mesh; uint32_t nt, cap_t;
@@ -453,6 +677,8 @@ ho_scene *ho_scene_create(void) {
 void ho_scene_destroy(ho_scene *s) {
     if (!s) return;
     for (int i = 0; i < s->nm; i++) { free(s->meshes[i].cdf); free(s->meshes[i].func); }
+    for (int i = 0; i < s->ntex; i++) mip_free(s->mips[i]);
+    free(s->mips);
     free(s->meshes); free(s->bsdfs); free(s->tex); free(s->P); free(s->N); free(s->UV); free(s->F); free(s->tri_mesh);
     for (int i = 0; i < 2; i++) free(s->rft[i].owned);
     free(s->env);
@@ -468,13 +694,50 @@ int ho_scene_set_rft(ho_scene *s, int dist, const void *bytes, uint64_t n) {
     s->has_rft[dist] = 1;
     return 0;
 }
+static int push_texture(ho_scene *s, const ho_texture_desc *d, mip_t *m) {
+    if (s->ntex == s->cap_tex) {
+        s->cap_tex = s->cap_tex ? 2 * s->cap_tex : 8;
+        s->tex = realloc(s->tex, s->cap_tex * sizeof *s->tex);
+        s->mips = realloc(s->mips, s->cap_tex * sizeof *s->mips);
+    }
+    s->tex[s->ntex] = *d;
+    s->mips[s->ntex] = m;
+    return s->ntex++;
+}
 int ho_scene_add_texture(ho_scene *s, const ho_texture_desc *d) {
     if (d->kind < HO_TEX_CHECKERBOARD || d->kind > HO_TEX_SCALE) return fail("unknown texture kind");
     if (d->kind == HO_TEX_SCALE && (d->nested < 0 || d->nested >= s->ntex)) return fail("scale texture needs a nested texture");
     if (d->kind != HO_TEX_SCALE && d->count <= 0) return fail("texture block / line count must be positive");
-    if (s->ntex == s->cap_tex) { s->cap_tex = s->cap_tex ? 2 * s->cap_tex : 8; s->tex = realloc(s->tex, s->cap_tex * sizeof *s->tex); }
-    s->tex[s->ntex] = *d;
-    return s->ntex++;
+    return push_texture(s, d, NULL);
+}
+/* BitmapTexture ctor (src/texture/BitmapTexture.cpp:7) over LoadImageFromFileR
+ * / LoadImageFromFileRGB (src/core/Texture.cpp:12, :74) and MipMap. */
+int ho_scene_add_bitmap(ho_scene *s, const ho_texture_desc *d, const uint8_t *pix, int w, int h) {
+    if (d->kind != HO_TEX_BITMAP) return fail("bitmap texture expected");
+    if (d->channels != 1 && d->channels != 3) return fail("bitmap channel must be r (1) or rgb (3)");
+    if (w <= 0 || h <= 0 || w > (1 << 15) || h > (1 << 15) || !pix) return fail("invalid bitmap size");
+    if (d->filter < HO_FILTER_NEAREST || d->filter > HO_FILTER_EWA) return fail("invalid filter type");
+    if (d->wrap_u < 0 || d->wrap_u > 2 || d->wrap_v < 0 || d->wrap_v > 2) return fail("invalid wrap mode");
+    const int ch = d->channels;
+    const float inv255 = 1.0f / 255.0f, inv_gamma = 1.0f / d->gamma;
+    float *t = malloc(sizeof(float) * 3 * (size_t)w * h);
+    float avg[3] = {0, 0, 0};
+    for (int x = 0; x < w; x++)
+        for (int y = 0; y < h; y++) {
+            size_t ld = (size_t)y * w + x, st = (size_t)(h - 1 - y) * w + x;
+            for (int c = 0; c < 3; c++) {
+                int cc = ch == 1 ? 0 : c;
+                float val = (float)pix[ld * ch + cc] * inv255;
+                val = inv_gamma == 1.0f ? val : powf(val, inv_gamma);   /* GammaCorrect (include/core/Common.hpp:982) */
+                t[3 * st + c] = val;
+                avg[c] += val;
+            }
+        }
+    mip_t *m = mip_build(t, w, h, ch, d->wrap_u, d->wrap_v, d->filter == HO_FILTER_TRILINEAR, d->max_anisotropy);
+    free(t);
+    for (int c = 0; c < 3; c++) m->avg[c] = avg[c] / (float)(w * h);
+    if (d->filter >= HO_FILTER_TRILINEAR) s->ray_diff = 1;
+    return push_texture(s, d, m);
 }
 int ho_scene_add_bsdf(ho_scene *s, const ho_bsdf_desc *d) {
     if (s->nb == s->cap_b) { s->cap_b = s->cap_b ? 2 * s->cap_b : 8; s->bsdfs = realloc(s->bsdfs, s->cap_b * sizeof(bsdf_t)); }
@@ -650,14 +913,15 @@ static int bsdf_transmits(const ho_scene *s, int id, int depth) {
 }
 
 /* BSDF activation: RoughPlasticBSDF::Activate :261, RoughCoatingBSDF::Activate :315 */
-static v3 tex_average(const ho_texture_desc *T, int id);
+static v3 tex_average(const ho_texture_desc *T, mip_t *const *M, int id);
 /* Texture::GetAverage of a parameter: the texture's average or the constant */
 static v3 par_average(const ho_scene *s, const ho_bsdf_desc *d, int slot, const float *c) {
-    return d->tex[slot] ? tex_average(s->tex, d->tex[slot] - 1) : vload(c);
+    return d->tex[slot] ? tex_average(s->tex, s->mips, d->tex[slot] - 1) : vload(c);
 }
 static int activate_bsdf(ho_scene *s, bsdf_t *b) {
     const ho_bsdf_desc *d = &b->d;
     b->textures = s->tex;
+    b->mips = s->mips;
     for (int k = 0; k < 6; k++)
         if (d->tex[k] < 0 || d->tex[k] > s->ntex) return fail("invalid texture id");
     if ((d->type == HO_BSDF_ROUGH_PLASTIC || d->type == HO_BSDF_ROUGH_COATING) && d->tex[4])
@@ -765,9 +1029,10 @@ int ho_film_border(const ho_scene *s) { return s->border; }
  * CheckerboardTexture.cpp:24) or GridTexture::Eval (src/texture/GridTexture.cpp:26);
  * ScaleTexture::Eval (src/texture/ScaleTexture.cpp:17) scales its nested texture. */
 static inline int mod_positive(int a, int b) { int r = a % b; return r < 0 ? r + b : r; }
-static v3 tex_eval(const ho_texture_desc *T, int id, const float *uvi) {
+static v3 tex_eval(const ho_texture_desc *T, mip_t *const *M, int id, const float *uvi, const float *duv) {
     const ho_texture_desc *t = &T[id];
-    if (t->kind == HO_TEX_SCALE) return scl(tex_eval(T, t->nested, uvi), t->scale);
+    if (t->kind == HO_TEX_SCALE) return scl(tex_eval(T, M, t->nested, uvi, duv), t->scale);
+    if (t->kind == HO_TEX_BITMAP) return bitmap_eval(t, M[id], uvi, duv);
     float u = uvi[0] * t->uv_scale[0] + t->uv_offset[0], v = uvi[1] * t->uv_scale[1] + t->uv_offset[1];
     if (t->kind == HO_TEX_CHECKERBOARD) {
         int ex = mod_positive(mod_positive((int)(u * t->count), t->count), 2) == 0;
@@ -781,9 +1046,10 @@ static v3 tex_eval(const ho_texture_desc *T, int id, const float *uvi) {
     return (fabsf(dx) < t->width || fabsf(dy) < t->width) ? vload(t->a) : vload(t->b);
 }
 /* Texture::GetAverage of the procedural textures (used when BSDFs activate) */
-static v3 tex_average(const ho_texture_desc *T, int id) {
+static v3 tex_average(const ho_texture_desc *T, mip_t *const *M, int id) {
     const ho_texture_desc *t = &T[id];
-    if (t->kind == HO_TEX_SCALE) return scl(tex_average(T, t->nested), t->scale);
+    if (t->kind == HO_TEX_SCALE) return scl(tex_average(T, M, t->nested), t->scale);
+    if (t->kind == HO_TEX_BITMAP) return vload(M[id]->avg);   /* BitmapTexture::GetAverage :176 */
     if (t->kind == HO_TEX_CHECKERBOARD) return scl(add(vload(t->a), vload(t->b)), 0.5f);
     float iw = fmaxf(0.0f, 1.0f - 2.0f * t->width);    /* GridTexture::GetAverage :40 */
     float ia = iw * iw, la = 1.0f - ia;
@@ -793,11 +1059,27 @@ static v3 tex_average(const ho_texture_desc *T, int id) {
  * slot: 0 kd, 1 ks, 2 ksRefract, 3 sigmaA, 4 alpha(U), 5 alphaV */
 static inline v3 par_rgb(const bsdf_t *b, int slot, const float *c, const brec *r) {
     int t = b->d.tex[slot];
-    return t ? tex_eval(b->textures, t - 1, r->uv) : vload(c);
+    return t ? tex_eval(b->textures, b->mips, t - 1, r->uv, r->duv) : vload(c);
 }
 static inline float par_alpha(const bsdf_t *b, int slot, float c, const brec *r) {
     int t = b->d.tex[slot];
-    return t ? tex_eval(b->textures, t - 1, r->uv).x : c;
+    return t ? tex_eval(b->textures, b->mips, t - 1, r->uv, r->duv).x : c;
+}
+void ho_texture_eval(const ho_scene *s, int id, const float *uv, const float *duv, float *out) {
+    static const float zero[4] = {0, 0, 0, 0};
+    vstore(out, tex_eval(s->tex, s->mips, id, uv, duv ? duv : zero));
+}
+int ho_texture_mip(const ho_scene *s, int id, int level, int *wh, float *texels) {
+    if (id < 0 || id >= s->ntex || !s->mips[id]) return fail("not a bitmap texture");
+    const mip_t *m = s->mips[id];
+    if (level < 0 || level >= m->levels) return m->levels;
+    wh[0] = m->w[level]; wh[1] = m->h[level];
+    if (texels) {
+        size_t n = (size_t)m->w[level] * m->h[level];
+        for (size_t i = 0; i < n; i++)
+            for (int c = 0; c < m->ch; c++) texels[i * m->ch + c] = m->lv[level][3 * i + c];
+    }
+    return m->levels;
 }
 static inline float alpha_u_of(const bsdf_t *b, const brec *r) { return clampf(par_alpha(b, 4, b->d.alpha_u, r), 5e-4f, 1.0f); }
 static inline float alpha_v_of(const bsdf_t *b, const brec *r) {
@@ -1477,7 +1759,7 @@ float ho_bsdf_rft_eval(const ho_scene *s, int id, float c) {
     return rft_eval1d(b->rft, b->rft_n, c);
 }
 void ho_bsdf_batch(const ho_scene *s, int id, uint64_t n, const float *wi, const float *u2, const float *u1,
-                   const float *wo, const float *uv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m,
+                   const float *wo, const float *uv, const float *duv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m,
                    float *e_rgb, float *p_pdf, int nthreads) {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -1487,6 +1769,7 @@ void ho_bsdf_batch(const ho_scene *s, int id, uint64_t n, const float *wi, const
         brec r; memset(&r, 0, sizeof r);
         r.wi = vload(wi + 3 * i); r.measure = HO_MEASURE_UNKNOWN;
         if (uv) { r.uv[0] = uv[2 * i]; r.uv[1] = uv[2 * i + 1]; }
+        if (duv) memcpy(r.duv, duv + 4 * i, 4 * sizeof(float));
         float uu = u1 ? u1[i] : 0.0f;
         v3 w = bsdf_sample(s, id, &r, u2[2 * i], u2[2 * i + 1], NULL, &uu);
         if (s_wo) vstore(s_wo + 3 * i, r.wo);
@@ -1496,6 +1779,7 @@ void ho_bsdf_batch(const ho_scene *s, int id, uint64_t n, const float *wi, const
         brec q; memset(&q, 0, sizeof q);
         q.wi = vload(wi + 3 * i); q.wo = vload(wo + 3 * i); q.measure = HO_MEASURE_SOLID_ANGLE; q.eta = 0;
         if (uv) { q.uv[0] = uv[2 * i]; q.uv[1] = uv[2 * i + 1]; }
+        if (duv) memcpy(q.duv, duv + 4 * i, 4 * sizeof(float));
         if (e_rgb) vstore(e_rgb + 3 * i, bsdf_eval(s, id, &q));
         if (p_pdf) p_pdf[i] = bsdf_pdf(s, id, &q);
     }
@@ -1703,7 +1987,8 @@ static frame frame_from_n_dpdu(v3 n, v3 dpdu) {
 }
 /* Triangle::PostIntersect  src/core/Mesh.cpp:67-172 (the UV partials of :137-156
  * are used only for the shading frame; dNdU / dNdV serve texture filtering) */
-typedef struct { v3 p; frame sh, geo; int mesh; float t; float uv[2]; } isect_t;
+/* dpdu / dpdv with has_uvp: Isect.dPdU / dPdV and bHasUVPartial (set with normals and texture coordinates) */
+typedef struct { v3 p; frame sh, geo; int mesh; float t; float uv[2]; v3 dpdu, dpdv; int has_uvp; } isect_t;
 static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
     const uint32_t *f = s->F + 3ull * h->tri;
     v3 p0 = vload(s->P + 3ull * f[0]), p1 = vload(s->P + 3ull * f[1]), p2 = vload(s->P + 3ull * f[2]);
@@ -1717,6 +2002,7 @@ static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
     it->geo = frame_from_n(normalize(cross(sub(p1, p0), sub(p2, p0))));
     it->mesh = s->tri_mesh[h->tri];
     it->t = h->t;
+    it->has_uvp = 0;
     if (m->has_n && m->has_uv) {
         v3 dp1 = sub(p1, p0), dp2 = sub(p2, p0);
         float du1 = u1[0] - u0[0], dv1 = u1[1] - u0[1], du2 = u2[0] - u0[0], dv2 = u2[1] - u0[1];
@@ -1726,11 +2012,15 @@ static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
             it->sh = it->geo;
         } else {
             float det = du1 * dv2 - dv1 * du2;
+            it->has_uvp = 1;
             if (det == 0.0f) {
                 it->sh = frame_from_n(normalize_dyn(add(add(scl(n0, b0), scl(n1, b1)), scl(n2, b2))));
+                it->dpdu = it->sh.s; it->dpdv = it->sh.t;
             } else {
                 float inv = 1.0f / det;
                 v3 dpdu = scl(sub(scl(dp1, dv2), scl(dp2, dv1)), inv);
+                it->dpdu = dpdu;
+                it->dpdv = scl(add(scl(dp1, -du2), scl(dp2, du1)), inv);
                 v3 ns = add(add(scl(n0, b0), scl(n1, b1)), scl(n2, b2));
                 float ln = norm(ns);
                 ns = scl(ns, 1.0f / ln);
@@ -1898,6 +2188,72 @@ static void camera_ray(const ho_scene *s, float px, float py, v3 *o, v3 *d, floa
     *maxt = s->far_c * invz;
 }
 
+/* The differential rays of PerspectiveCamera::SampleRay (:94-98): origins at
+ * the camera, directions through the near-plane point offset by m_dX / m_dY
+ * (:64, one pixel along x / y on the near plane; in closed form (near(1 - 2/W)
+ * / cot - near / cot, 0, 0) and (0, near(1 - 2/H) / (aspect cot) - near /
+ * (aspect cot), 0)). */
+static void camera_diff(const ho_scene *s, float px, float py, v3 *rx, v3 *ry) {
+    float iw = 1.0f / (float)s->W, ih = 1.0f / (float)s->H;
+    float u = px * iw, v = py * ih;
+    v3 np = V(s->near_c * (1.0f - 2.0f * u) / s->cot, s->near_c * (1.0f - 2.0f * v) / (s->aspect * s->cot), s->near_c);
+    float dx = s->near_c * (1.0f - 2.0f * iw) / s->cot - s->near_c / s->cot;
+    float dy = s->near_c * (1.0f - 2.0f * ih) / (s->aspect * s->cot) - s->near_c / (s->aspect * s->cot);
+    const float *M = s->cam;
+    v3 a = normalize(V(np.x + dx, np.y, np.z)), b = normalize(V(np.x, np.y + dy, np.z));
+    *rx = V(M[0] * a.x + M[1] * a.y + M[2] * a.z, M[4] * a.x + M[5] * a.y + M[6] * a.z,
+            M[8] * a.x + M[9] * a.y + M[10] * a.z);
+    *ry = V(M[0] * b.x + M[1] * b.y + M[2] * b.z, M[4] * b.x + M[5] * b.y + M[6] * b.z,
+            M[8] * b.x + M[9] * b.y + M[10] * b.z);
+}
+/* SolveLinearSystem2x2 (include/core/Common.hpp:881) */
+static int solve2x2(const float A[2][2], const float B[2], float X[2]) {
+    float det = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+    if (fabsf(det) <= 1.0f / FLT_MAX) return 0;
+    float inv = 1.0f / det;
+    X[0] = (A[1][1] * B[0] - A[0][1] * B[1]) * inv;
+    X[1] = (A[0][0] * B[1] - A[1][0] * B[0]) * inv;
+    return 1;
+}
+static inline float v3c(v3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+/* Intersection::ComputeScreenSpacePartial (src/core/Intersection.cpp:30) for
+ * a camera ray from o with differential directions rx, ry: out (dUdX, dVdX,
+ * dUdY, dVdY), zero without UV partials. */
+static void screen_partials(const isect_t *it, v3 o, v3 rx, v3 ry, float *out) {
+    out[0] = out[1] = out[2] = out[3] = 0.0f;
+    if (!it->has_uvp) return;
+    if (is_zero(it->dpdu) && is_zero(it->dpdv)) return;
+    v3 n = it->geo.n;
+    float pp = dot(n, it->p), pro = dot(n, o);
+    float prd = dot(n, rx), pyd = dot(n, ry);
+    if (prd == 0.0f || pyd == 0.0f) return;
+    float tx = (pp - pro) / prd, ty = (pp - pro) / pyd;
+    float ax = fabsf(n.x), ay = fabsf(n.y), az = fabsf(n.z);
+    int a0, a1;
+    if (ax > ay && ax > az) { a0 = 1; a1 = 2; }
+    else if (ay > az) { a0 = 0; a1 = 2; }
+    else { a0 = 0; a1 = 1; }
+    float A[2][2] = {{v3c(it->dpdu, a0), v3c(it->dpdv, a0)}, {v3c(it->dpdu, a1), v3c(it->dpdv, a1)}};
+    v3 px = add(o, scl(rx, tx)), py = add(o, scl(ry, ty));
+    float bx[2] = {v3c(px, a0) - v3c(it->p, a0), v3c(px, a1) - v3c(it->p, a1)};
+    float by[2] = {v3c(py, a0) - v3c(it->p, a0), v3c(py, a1) - v3c(it->p, a1)};
+    float X[2];
+    if (solve2x2(A, bx, X)) { out[0] = X[0]; out[1] = X[1]; }
+    else { out[0] = 1.0f; out[1] = 0.0f; }
+    if (solve2x2(A, by, X)) { out[2] = X[0]; out[3] = X[1]; }
+    else { out[2] = 0.0f; out[3] = 1.0f; }
+}
+void ho_screen_partials(const ho_scene *s, float px, float py, uint32_t tri, float u, float v, float *out4) {
+    hit_t h; memset(&h, 0, sizeof h);
+    h.tri = tri; h.u = u; h.v = v;
+    isect_t it;
+    post_intersect(s, &h, &it);
+    v3 o, d, rx, ry; float mn, mx;
+    camera_ray(s, px, py, &o, &d, &mn, &mx);
+    camera_diff(s, px, py, &rx, &ry);
+    screen_partials(&it, o, rx, ry, out4);
+}
+
 /* ------------------------------------------------------------ integrator */
 typedef struct { uint64_t rays, shadow; } ctr_t;
 static inline v3 emitter_sample_any(const ho_scene *s, int e, erec *r, float ux, float uy, float u1) {
@@ -1908,8 +2264,11 @@ static inline v3 emitter_sample_any(const ho_scene *s, int e, erec *r, float ux,
 }
 
 /* PathMISIntegrator::Li  src/integrator/PathMISIntegrator.cpp:16-157 */
+/* pxy: the camera sample's film position (its differential rays give the
+ * first hit's screen-space UV partials; later hits have none) */
 static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 rdir, float rmint, float rmaxt,
-                     ctr_t *ctr) {
+                     const float *pxy, ctr_t *ctr) {
+    float duv[4] = {0, 0, 0, 0};
     hit_t hn; int found_next = 0;
     isect_t it, itn;
     v3 L = V(0, 0, 0), beta = V(1, 1, 1);
@@ -1926,7 +2285,13 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
                 return s->background;
             }
             post_intersect(s, &h, &it);
+            if (s->ray_diff && pxy) {
+                v3 rx, ry;
+                camera_diff(s, pxy[0], pxy[1], &rx, &ry);
+                screen_partials(&it, ro, rx, ry, duv);
+            }
         } else {
+            duv[0] = duv[1] = duv[2] = duv[3] = 0.0f;
             if (found_next) it = itn;
             else {
                 if (has_env) L = add(L, mul(beta, env_eval(s, rdir)));
@@ -1955,6 +2320,7 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
                 if (!trace(s, it.p, sd, EPS_RAY, 1.0f - EPS_RAY, 1, 1, &sh)) {
                     brec br; br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.wo = to_local(&it.sh, er.wi);
                     br.uv[0] = it.uv[0]; br.uv[1] = it.uv[1];
+                    memcpy(br.duv, duv, sizeof duv);
                     br.measure = HO_MEASURE_SOLID_ANGLE; br.eta = 0;
                     float pb = bsdf_pdf(s, bsdf, &br);
                     if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
@@ -1967,6 +2333,7 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
         }
         brec br; memset(&br, 0, sizeof br);
         br.uv[0] = it.uv[0]; br.uv[1] = it.uv[1];
+        memcpy(br.duv, duv, sizeof duv);
         br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.measure = HO_MEASURE_UNKNOWN;
         float sx = ho_pcg32_nextf(rng), sy = ho_pcg32_nextf(rng);
         v3 F = bsdf_sample(s, bsdf, &br, sx, sy, rng, NULL);
@@ -2046,7 +2413,8 @@ int64_t ho_render(const ho_scene *s, int depth, int spp, const int32_t *blist, i
                         (void)ho_pcg32_nextf(&rng); (void)ho_pcg32_nextf(&rng);   /* aperture sample */
                         v3 o, d; float mn, mx;
                         camera_ray(s, px, py, &o, &d, &mn, &mx);
-                        v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, &c);
+                        float pxy[2] = {px, py};
+            v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, pxy, &c);
                         dropped += film_put(s, loc, px, py, L);
                     }
         }
@@ -2076,7 +2444,8 @@ void ho_pixel_stats(const ho_scene *s, int depth, int spp, uint64_t seed, int np
             float px = (float)x + ho_pcg32_nextf(&rng), py = (float)y + ho_pcg32_nextf(&rng);
             v3 o, d; float mn, mx;
             camera_ray(s, px, py, &o, &d, &mn, &mx);
-            v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, &c);
+            float pxy[2] = {px, py};
+            v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, pxy, &c);
             double r[3] = {L.x, L.y, L.z};
             for (int ch = 0; ch < 3; ch++) { double dl = r[ch] - m[ch]; m[ch] += dl / (i + 1); v[ch] += dl * (r[ch] - m[ch]); }
         }
@@ -2094,7 +2463,8 @@ void ho_ttest_scene(const ho_scene *s, int depth, int n, double *mean, double *v
         (void)ho_pcg32_nextf(&rng); (void)ho_pcg32_nextf(&rng);
         v3 o, d; float mn, mx;
         camera_ray(s, px, py, &o, &d, &mn, &mx);
-        v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, &c);
+        float pxy[2] = {px, py};
+            v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, pxy, &c);
         double r = lum(L);
         double dl = r - m; m += dl / (double)(k + 1); v += dl * (r - m);
     }

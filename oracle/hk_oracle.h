@@ -63,8 +63,11 @@ typedef struct {
     int32_t tex[6];
 } ho_bsdf_desc;
 
-/* Procedural textures (src/texture/{Checkerboard,Grid,Scale}Texture.cpp). */
-enum { HO_TEX_CHECKERBOARD = 1, HO_TEX_GRID = 2, HO_TEX_SCALE = 3 };
+/* Procedural textures (src/texture/{Checkerboard,Grid,Scale}Texture.cpp) and
+ * bitmap textures (src/texture/BitmapTexture.cpp over include/core/MipMap.hpp). */
+enum { HO_TEX_CHECKERBOARD = 1, HO_TEX_GRID = 2, HO_TEX_SCALE = 3, HO_TEX_BITMAP = 4 };
+enum { HO_FILTER_NEAREST = 0, HO_FILTER_BILINEAR = 1, HO_FILTER_TRILINEAR = 2, HO_FILTER_EWA = 3 };
+enum { HO_WRAP_REPEAT = 0, HO_WRAP_CLAMP = 1, HO_WRAP_BLACK = 2 };
 typedef struct {
     int32_t kind;          /* HO_TEX_* */
     int32_t nested;        /* scale: the scaled texture's id */
@@ -73,6 +76,10 @@ typedef struct {
     float scale;           /* scale "scale" */
     float uv_scale[2], uv_offset[2];   /* "uScale" "vScale", "uOffset" "vOffset" */
     float a[3], b[3];      /* checkerboard colorA / colorB; grid lineColor / backgroundColor */
+    /* bitmap: "filterType", "uWrapMode" / "vWrapMode", "channel" (1 = r, 3 = rgb),
+     * "gamma", "maxAnisotropy" */
+    int32_t filter, wrap_u, wrap_v, channels;
+    float gamma, max_anisotropy;
 } ho_texture_desc;
 
 typedef struct ho_scene ho_scene;
@@ -90,6 +97,16 @@ void      ho_scene_destroy(ho_scene *s);
 int  ho_scene_set_rft(ho_scene *s, int distribution, const void *bytes, uint64_t nbytes);
 int  ho_scene_add_bsdf(ho_scene *s, const ho_bsdf_desc *d);   /* returns id or <0 */
 int  ho_scene_add_texture(ho_scene *s, const ho_texture_desc *d);   /* returns id or <0 */
+/* Bitmap texture from 8-bit pixels as stbi_load returns them (row 0 = the top
+ * row, d->channels bytes per pixel).  Returns id or <0. */
+int  ho_scene_add_bitmap(ho_scene *s, const ho_texture_desc *d, const uint8_t *pixels, int width, int height);
+/* Texture2D::Eval(Isect, filter = true) at texture coordinates uv (2) with the
+ * screen-space partials duv = (dUdX, dVdX, dUdY, dVdY) or NULL (zero): out rgb (3). */
+void ho_texture_eval(const ho_scene *s, int id, const float *uv, const float *duv, float *out);
+/* The MIP pyramid of a bitmap texture: level count, or, for 0 <= level <
+ * levels, the level's size (out wh[2]) and texels (channels floats each,
+ * row-major, row 0 = v 0) when texels != NULL. */
+int  ho_texture_mip(const ho_scene *s, int id, int level, int *wh, float *texels);
 /* positions 3*nv, indices 3*nt (mesh-local), normals 3*nv or NULL,
  * radiance 3 or NULL (area light).  Returns mesh id or <0. */
 int  ho_scene_add_mesh(ho_scene *s, const float *positions, uint32_t nv,
@@ -127,9 +144,14 @@ void  ho_bsdf_eval(const ho_scene *s, int bsdf, const float *wi, const float *wo
 float ho_bsdf_pdf(const ho_scene *s, int bsdf, const float *wi, const float *wo, int measure);
 /* batched over n records, 2^k friendly; records are AoS float3 */
 void  ho_bsdf_batch(const ho_scene *s, int bsdf, uint64_t n, const float *wi, const float *u2,
-                    const float *u1, const float *wo, const float *uv, float *s_wo, float *s_w,
-                    float *s_pdf, int32_t *s_measure, float *e_rgb, float *p_pdf, int nthreads);
-/* (uv: n x 2 texture coordinates of the records' intersections, or NULL) */
+                    const float *u1, const float *wo, const float *uv, const float *duv, float *s_wo,
+                    float *s_w, float *s_pdf, int32_t *s_measure, float *e_rgb, float *p_pdf, int nthreads);
+/* (uv: n x 2 texture coordinates of the records' intersections, or NULL;
+ *  duv: n x 4 screen-space partials (dUdX, dVdX, dUdY, dVdY), or NULL) */
+/* Intersection::ComputeScreenSpacePartial (src/core/Intersection.cpp:30) of
+ * the camera ray through film position (px, py) hitting (tri, u, v):
+ * out duv (4) = (dUdX, dVdX, dUdY, dVdY). */
+void  ho_screen_partials(const ho_scene *s, float px, float py, uint32_t tri, float u, float v, float *out4);
 /* RFT 1D eval after activation (for table parity tests). */
 float ho_bsdf_rft_eval(const ho_scene *s, int bsdf, float cos_theta);
 

@@ -43,7 +43,8 @@ class TextureDescC(C.Structure):
     _fields_ = [
         ("kind", C.c_int32), ("nested", C.c_int32), ("count", C.c_int32), ("width", C.c_float),
         ("scale", C.c_float), ("uv_scale", C.c_float * 2), ("uv_offset", C.c_float * 2), ("a", C.c_float * 3),
-        ("b", C.c_float * 3),
+        ("b", C.c_float * 3), ("filter", C.c_int32), ("wrap_u", C.c_int32), ("wrap_v", C.c_int32),
+        ("channels", C.c_int32), ("gamma", C.c_float), ("max_anisotropy", C.c_float),
     ]
 
 
@@ -51,7 +52,19 @@ def texture_desc_c(t, nested_index=-1) -> TextureDescC:
     c = TextureDescC()
     c.kind, c.nested, c.count, c.width, c.scale = t.kind, nested_index, t.count, t.width, t.scale
     c.uv_scale[:], c.uv_offset[:], c.a[:], c.b[:] = t.uv_scale, t.uv_offset, t.a, t.b
+    c.filter, c.wrap_u, c.wrap_v = t.filter, t.wrap_u, t.wrap_v
+    c.channels, c.gamma, c.max_anisotropy = t.channels, t.gamma, t.max_anisotropy
     return c
+
+
+def bitmap_pixels(t) -> np.ndarray:
+    """The bitmap's 8-bit pixels as a contiguous height x width x channels array."""
+    px = np.ascontiguousarray(t.pixels, dtype=np.uint8)
+    if px.ndim == 2:
+        px = px[:, :, None]
+    if px.ndim != 3 or px.shape[2] != t.channels:
+        raise ValueError(f"bitmap pixels must be height x width x {t.channels}")
+    return px
 
 
 _lib = None
@@ -84,8 +97,12 @@ def lib():
         L.ho_bsdf_eval.argtypes = [P, C.c_int, P, P, C.c_int, P]
         L.ho_bsdf_pdf.argtypes = [P, C.c_int, P, P, C.c_int]
         L.ho_bsdf_pdf.restype = C.c_float
-        L.ho_bsdf_batch.argtypes = [P, C.c_int, C.c_uint64, P, P, P, P, P, P, P, P, P, P, P, C.c_int]
+        L.ho_bsdf_batch.argtypes = [P, C.c_int, C.c_uint64, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int]
         L.ho_scene_add_texture.argtypes = [P, C.POINTER(TextureDescC)]
+        L.ho_scene_add_bitmap.argtypes = [P, C.POINTER(TextureDescC), P, C.c_int, C.c_int]
+        L.ho_texture_eval.argtypes = [P, C.c_int, P, P, P]
+        L.ho_texture_mip.argtypes = [P, C.c_int, C.c_int, P, P]
+        L.ho_screen_partials.argtypes = [P, C.c_float, C.c_float, C.c_uint32, C.c_float, C.c_float, P]
         L.ho_bsdf_rft_eval.argtypes = [P, C.c_int, C.c_float]
         L.ho_bsdf_rft_eval.restype = C.c_float
         L.ho_trace.argtypes = [P, C.c_uint64, P, P, P, P, P, C.c_int, C.c_int, C.c_int]
@@ -218,10 +235,17 @@ class OracleScene:
         nested = self.add_texture(t.nested) if t.nested is not None else -1
         c = texture_desc_c(t, nested)
         self._keep.append(c)
-        i = lib().ho_scene_add_texture(self.h, C.byref(c))
+        if t.kind == 4:   # bitmap
+            px = bitmap_pixels(t)
+            i = lib().ho_scene_add_bitmap(self.h, C.byref(c), _p(px), px.shape[1], px.shape[0])
+        else:
+            i = lib().ho_scene_add_texture(self.h, C.byref(c))
         if i < 0:
             raise RuntimeError(lib().ho_last_error().decode())
         self.tex_ids[id(t)] = i
+        if not hasattr(self, "_tex_channels"):
+            self._tex_channels = {}
+        self._tex_channels[id(t)] = t.channels if t.kind == 4 else 3
         return i
 
     def __del__(self):
@@ -236,17 +260,56 @@ class OracleScene:
         lib().ho_scene_bbox(self.h, _p(o))
         return o
 
-    def bsdf_batch(self, bsdf, wi, u2, u1, wo, nthreads=0, uv=None):
+    def bsdf_batch(self, bsdf, wi, u2, u1, wo, nthreads=0, uv=None, duv=None):
         n = wi.shape[0]
         wi, u2, wo = _f32(wi), _f32(u2), _f32(wo)
         u1 = _f32(u1) if u1 is not None else None
         uv = _f32(uv) if uv is not None else None
+        duv = _f32(duv) if duv is not None else None
         out = dict(
             s_wo=np.zeros((n, 3), np.float32), s_w=np.zeros((n, 3), np.float32), s_pdf=np.zeros(n, np.float32),
             s_measure=np.zeros(n, np.int32), e_rgb=np.zeros((n, 3), np.float32), p_pdf=np.zeros(n, np.float32),
         )
-        lib().ho_bsdf_batch(self.h, bsdf, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(uv), _p(out["s_wo"]), _p(out["s_w"]),
+        lib().ho_bsdf_batch(self.h, bsdf, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(uv), _p(duv), _p(out["s_wo"]), _p(out["s_w"]),
                             _p(out["s_pdf"]), _p(out["s_measure"]), _p(out["e_rgb"]), _p(out["p_pdf"]), nthreads)
+        return out
+
+    def texture_eval(self, tex, uv, duv=None):
+        """Texture2D::Eval(Isect) of texture `tex` (an id or a TextureDesc added
+        with a BSDF) at n x 2 texture coordinates, n x 4 partials or None."""
+        tid = tex if isinstance(tex, int) else self.tex_ids[id(tex)]
+        uv = _f32(uv)
+        duv = _f32(duv) if duv is not None else None
+        out = np.zeros((uv.shape[0], 3), np.float32)
+        for k in range(uv.shape[0]):
+            lib().ho_texture_eval(self.h, tid, _p(uv[k]), _p(duv[k]) if duv is not None else None, _p(out[k]))
+        return out
+
+    def texture_mip(self, tex):
+        """The MIP pyramid of a bitmap texture: a list of height x width x channels float arrays."""
+        tid = tex if isinstance(tex, int) else self.tex_ids[id(tex)]
+        wh = np.zeros(2, np.int32)
+        n = lib().ho_texture_mip(self.h, tid, -1, _p(wh), None)
+        if n < 0:
+            raise RuntimeError(lib().ho_last_error().decode())
+        out = []
+        for l in range(n):
+            lib().ho_texture_mip(self.h, tid, l, _p(wh), None)
+            ch = self.desc_channels(tid)
+            a = np.zeros((wh[1], wh[0], ch), np.float32)
+            lib().ho_texture_mip(self.h, tid, l, _p(wh), _p(a))
+            out.append(a)
+        return out
+
+    def desc_channels(self, tid):
+        for key, i in self.tex_ids.items():
+            if i == tid:
+                return self._tex_channels[key]
+        return 3
+
+    def screen_partials(self, px, py, tri, u, v):
+        out = np.zeros(4, np.float32)
+        lib().ho_screen_partials(self.h, px, py, tri, u, v, _p(out))
         return out
 
     def bsdf_sample(self, bsdf, wi, u2, u1=0.0):

@@ -7,7 +7,7 @@ Recipe (no reference build system is run):
   * a shim include tree (oracle/_ref/shim) of symlinks named like the
     reference's backslash include paths ("core\\Common.hpp" -> include/core/
     Common.hpp, "Eigen\\Lu" -> ext/eigen/Eigen/LU), plus oracle/ref_shim/ for
-    glog and <windows.h>;
+    glog, <windows.h> and a serial stand-in for the TBB loops of MipMap;
   * -DWIN32 selects the reference's Windows branches (its non-Windows branch
     of Signum has a bare #elif that GCC rejects); oracle/ref_shim/prelude.h
     supplies the MSVC CRT helpers they use;
@@ -30,12 +30,13 @@ LIB = os.path.join(OUT, "libhikari_ref_bsdf.so")
 
 CORE = ["Object", "PropertyList", "BSDF", "Texture", "MicrofacetDistribution", "RoughTransmitance", "Frame",
         "Sampling", "Color", "Vector", "Transform", "Sampler", "Intersection", "Timer", "MemoryArena", "Shape",
-        "Mesh", "Emitter", "DiscretePDF", "BoundingBox", "Ray"]
+        "Mesh", "Emitter", "DiscretePDF", "BoundingBox", "Ray", "MipMap", "Camera", "ReconstructionFilter"]
 BSDFS = ["DiffuseBSDF", "RoughConductorBSDF", "RoughDielectricBSDF", "RoughPlasticBSDF", "RoughCoatingBSDF",
          "MirrorBSDF", "ConductorBSDF", "DielectricBSDF", "PlasticBSDF", "TwoSidedBSDF", "CoatingBSDF",
          "RoughDiffuseBSDF"]
 EMITTERS = ["PointLight", "DirectionalLight", "ConstantLight"]
-TEXTURES = ["CheckerboardTexture", "GridTexture", "ScaleTexture"]
+TEXTURES = ["CheckerboardTexture", "GridTexture", "ScaleTexture", "BitmapTexture"]
+OTHERS = [("camera", "PerspectiveCamera"), ("filter", "GaussianFilter")]
 
 
 def _link(src, dst):
@@ -69,6 +70,7 @@ def build(ref: str = "/root/reference") -> str:
     for name, real in [("Core", "Core"), ("Geometry", "Geometry"), ("Lu", "LU")]:
         _forward(os.path.join(ref, "ext", "eigen", "Eigen", real), os.path.join(shim, f"Eigen\\{name}"))
     _forward(os.path.join(HERE, "ref_shim", "glog_logging.h"), os.path.join(shim, "glog\\logging.h"))
+    _forward(os.path.join(HERE, "ref_shim", "tbb_serial.h"), os.path.join(shim, "tbb\\tbb.h"))
     _forward(os.path.join(ref, "ext", "filesystem", "filesystem", "resolver.h"), os.path.join(shim, "filesystem\\resolver.h"))
     data = os.path.join(os.path.dirname(HERE), "hikari_b200", "data")   # identical copies of ref data/
     for f in ("BeckmannRFTData.bin", "GGXRFTData.bin"):
@@ -85,6 +87,7 @@ def build(ref: str = "/root/reference") -> str:
            [os.path.join(ref, "src", "bsdf", b + ".cpp") for b in BSDFS] + \
            [os.path.join(ref, "src", "emitter", e + ".cpp") for e in EMITTERS] + \
            [os.path.join(ref, "src", "texture", t + ".cpp") for t in TEXTURES] + \
+           [os.path.join(ref, "src", d, f + ".cpp") for d, f in OTHERS] + \
            [os.path.join(HERE, "ref_shim", "ref_bridge.cpp")]
     for s in srcs:
         o = os.path.join(objd, os.path.basename(s) + ".o")

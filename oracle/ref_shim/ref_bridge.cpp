@@ -11,6 +11,10 @@
 #include <core\Vector.hpp>
 #include <core\Emitter.hpp>
 #include <core\Mesh.hpp>
+#include <core\Texture.hpp>
+#include <core\Camera.hpp>
+#include <core\Transform.hpp>
+#include <stb_image.h>
 
 using namespace Hikari;
 
@@ -245,12 +249,121 @@ void hr_emitter_eval_dir(void *h, uint64_t n, const float *wi, float *out) {
     }
 }
 
+/* BitmapTexture (src/texture/BitmapTexture.cpp) of `filename` found under
+ * search_dir: filter 0 nearest 1 bilinear 2 trilinear 3 ewa; wrap 0 repeat 1
+ * clamp 2 black; channels 1 (r) or 3 (rgb). */
+void *hr_bitmap_create(const char *search_dir, const char *filename, int filter, int wrap_u, int wrap_v,
+                       int channels, float gamma, float max_aniso, const float *uv_scale, const float *uv_offset) {
+    static const char *filters[] = {"nearest", "bilinear", "trilinear", "ewa"};
+    static const char *wraps[] = {"repeat", "clamp", "black"};
+    try {
+        GetFileResolver()->prepend(filesystem::path(search_dir));
+        PropertyList pl;
+        pl.SetString("filename", filename);
+        pl.SetString("filterType", filters[filter]);
+        pl.SetString("uWrapMode", wraps[wrap_u]);
+        pl.SetString("vWrapMode", wraps[wrap_v]);
+        pl.SetString("channel", channels == 1 ? "r" : "rgb");
+        pl.SetFloat("gamma", gamma);
+        pl.SetFloat("maxAnisotropy", max_aniso);
+        pl.SetFloat("uScale", uv_scale[0]);
+        pl.SetFloat("vScale", uv_scale[1]);
+        pl.SetFloat("uOffset", uv_offset[0]);
+        pl.SetFloat("vOffset", uv_offset[1]);
+        Object *t = ObjectFactory::CreateInstance("bitmap", pl);
+        t->Activate();
+        return t;
+    } catch (const std::exception &e) {
+        fprintf(stderr, "hr_bitmap_create: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+/* Texture::Eval(Isect, bFilter = true) at n texture coordinates uv (2 each)
+ * with screen-space partials duv (dUdX, dVdX, dUdY, dVdY each, or NULL): out rgb */
+void hr_texture_eval(void *t, uint64_t n, const float *uv, const float *duv, float *out) {
+    for (uint64_t i = 0; i < n; i++) {
+        Intersection I;
+        I.UV = Point2f(uv[2 * i], uv[2 * i + 1]);
+        if (duv) { I.dUdX = duv[4 * i]; I.dVdX = duv[4 * i + 1]; I.dUdY = duv[4 * i + 2]; I.dVdY = duv[4 * i + 3]; }
+        Color3f c = ((Texture *)t)->Eval(I, true);
+        out[3 * i] = c[0]; out[3 * i + 1] = c[1]; out[3 * i + 2] = c[2];
+    }
+}
+/* Texture::GetAverage: out rgb */
+void hr_texture_average(void *t, float *out) {
+    Color3f c = ((Texture *)t)->GetAverage();
+    out[0] = c[0]; out[1] = c[1]; out[2] = c[2];
+}
+
+/* stbi_load as LoadImageFromFileR / RGB (src/core/Texture.cpp:28, :90) call
+ * it: returns width * height * req bytes (copied to out when not NULL), 0 on failure. */
+uint64_t hr_image_load(const char *path, int req, int *w, int *h, unsigned char *out) {
+    int c = 0;
+    unsigned char *p = stbi_load(path, w, h, &c, req);
+    if (!p) return 0;
+    uint64_t n = (uint64_t)(*w) * (uint64_t)(*h) * (uint64_t)req;
+    if (out) memcpy(out, p, n);
+    stbi_image_free(p);
+    return n;
+}
+
+/* PerspectiveCamera (src/camera/PerspectiveCamera.cpp) with its default filter */
+void *hr_camera_create(int width, int height, const float *to_world16, float fov, float near_clip, float far_clip) {
+    try {
+        PropertyList pl;
+        pl.SetInteger("width", width);
+        pl.SetInteger("height", height);
+        Eigen::Matrix4f M;
+        for (int r = 0; r < 4; r++)
+            for (int c = 0; c < 4; c++) M(r, c) = to_world16[4 * r + c];
+        pl.SetTransform("toWorld", Transform(M));
+        pl.SetFloat("fov", fov);
+        pl.SetFloat("nearClip", near_clip);
+        pl.SetFloat("farClip", far_clip);
+        Object *c = ObjectFactory::CreateInstance("perspective", pl);
+        c->Activate();
+        return c;
+    } catch (const std::exception &e) {
+        fprintf(stderr, "hr_camera_create: %s\n", e.what());
+        return nullptr;
+    }
+}
+/* Camera::SampleRay at film position (px, py): out o(3) d(3) rx_o(3) rx_d(3) ry_o(3) ry_d(3) mint maxt */
+void hr_camera_ray(void *c, float px, float py, float *out) {
+    Ray3f R;
+    ((Camera *)c)->SampleRay(R, Point2f(px, py), Point2f(0.5f, 0.5f));
+    for (int k = 0; k < 3; k++) {
+        out[k] = R.Origin[k]; out[3 + k] = R.Direction[k]; out[6 + k] = R.RxOrigin[k];
+        out[9 + k] = R.RxDirection[k]; out[12 + k] = R.RyOrigin[k]; out[15 + k] = R.RyDirection[k];
+    }
+    out[18] = R.MinT; out[19] = R.MaxT;
+}
+/* Triangle::PostIntersect then Intersection::ComputeScreenSpacePartial for the
+ * camera ray through (px, py): out (dUdX, dVdX, dUdY, dVdY) */
+void hr_screen_partials(void *cam, void *mesh, uint32_t tri, float u, float v, float px, float py, float *out) {
+    Ray3f R;
+    ((Camera *)cam)->SampleRay(R, Point2f(px, py), Point2f(0.5f, 0.5f));
+    ArrayMesh *m = (ArrayMesh *)mesh;
+    Triangle T(m, m->facet(tri), tri);
+    Intersection I;
+    I.pShape = &T;
+    I.UV = Point2f(u, v);
+    T.PostIntersect(I);
+    I.ComputeScreenSpacePartial(R);
+    out[0] = I.dUdX; out[1] = I.dVdX; out[2] = I.dUdY; out[3] = I.dVdY;
+}
+
 /* batched over n AoS records (same layout as ho_bsdf_batch) */
 void hr_bsdf_batch(void *h, uint64_t n, const float *wi, const float *u2, const float *u1, const float *wo,
-                   const float *uv,
+                   const float *uv, const float *duv,
                    float *s_wo, float *s_w, float *s_pdf, int *s_m, float *e_rgb, float *p_pdf) {
     for (uint64_t i = 0; i < n; i++) {
         g_isect.UV = uv ? Point2f(uv[2 * i], uv[2 * i + 1]) : Point2f(0.0f, 0.0f);
+        g_isect.dUdX = duv ? duv[4 * i] : 0.0f;
+        g_isect.dVdX = duv ? duv[4 * i + 1] : 0.0f;
+        g_isect.dUdY = duv ? duv[4 * i + 2] : 0.0f;
+        g_isect.dVdY = duv ? duv[4 * i + 3] : 0.0f;
         float eta; int m;
         hr_bsdf_sample(h, wi + 3 * i, u2 + 2 * i, u1 ? u1[i] : 0.0f, s_wo + 3 * i, s_w + 3 * i, &m, &eta);
         s_m[i] = m;

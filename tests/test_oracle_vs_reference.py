@@ -35,7 +35,7 @@ def _ref_lib():
     R.hr_bsdf_eval.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
     R.hr_bsdf_pdf.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     R.hr_bsdf_pdf.restype = C.c_float
-    R.hr_bsdf_batch.argtypes = [C.c_void_p, C.c_uint64] + [C.c_void_p] * 11
+    R.hr_bsdf_batch.argtypes = [C.c_void_p, C.c_uint64] + [C.c_void_p] * 12
     R.hr_init(os.path.dirname(REF_LIB).encode())
     return R
 
@@ -183,7 +183,7 @@ def test_oracle_bsdf_bit_exact_vs_reference(name):
     uv = (np.random.default_rng(3).random((n, 2)) * 4 - 1).astype(np.float32)   # texture coordinates
     a = o.bsdf_batch(bid, wi, u2, u1, wo, uv=uv)
     b = {k: np.zeros_like(v) for k, v in a.items()}
-    R.hr_bsdf_batch(h, n, O._p(wi), O._p(u2), O._p(u1), O._p(wo), O._p(uv), O._p(b["s_wo"]), O._p(b["s_w"]),
+    R.hr_bsdf_batch(h, n, O._p(wi), O._p(u2), O._p(u1), O._p(wo), O._p(uv), None, O._p(b["s_wo"]), O._p(b["s_w"]),
                     O._p(b["s_pdf"]), O._p(b["s_measure"]), O._p(b["e_rgb"]), O._p(b["p_pdf"]))
     valid = np.any(a["s_w"] != 0, axis=1)
     np.testing.assert_array_equal(a["s_w"], b["s_w"])
