@@ -603,12 +603,14 @@ std::string resolve(const std::string &f) {
     return g_base_dir + "/" + f;
 }
 
-// Texture plugins (src/texture/{Checkerboard,Grid,Scale}Texture.cpp): the
-// procedural textures, defaults of include/core/Common.hpp:436-458
+// Texture plugins (src/texture/{Checkerboard,Grid,Scale,Bitmap}Texture.cpp),
+// defaults of include/core/Common.hpp:425-458
 class TexturePlugin : public Object {
 public:
     hk_texture_desc d{};
     std::unique_ptr<TexturePlugin> nested;
+    std::vector<uint8_t> pixels;   // bitmap: decoded 8-bit pixels (row 0 = top)
+    int32_t width = 0, height = 0;
     TexturePlugin(const PropertyList &p, int kind) {
         std::memset(&d, 0, sizeof d);
         d.kind = kind;
@@ -627,10 +629,48 @@ public:
             setc(d.a, p.GetColor("lineColor", {0.4f, 0.4f, 0.4f}));
             setc(d.b, p.GetColor("backgroundColor", {0.2f, 0.2f, 0.2f}));
             d.width = p.GetFloat("lineWidth", 0.01f);
+        } else if (kind == HK_TEX_BITMAP) {
+            load_bitmap(p);
+            return;
         } else {
             d.scale = p.GetFloat("scale");
         }
         if (kind != HK_TEX_SCALE && d.count <= 0) throw HikariException("texture block / line count must be positive");
+    }
+    // BitmapTexture ctor (src/texture/BitmapTexture.cpp:7): the image decoded
+    // like stbi_load (hk_image_load), wrap / filter / channel names as there
+    void load_bitmap(const PropertyList &p) {
+        const std::string fn = resolve(p.GetString("filename"));
+        d.gamma = p.GetFloat("gamma", 1.0f);
+        auto wrap_of = [](const std::string &w) {
+            if (w == "repeat") return HK_WRAP_REPEAT;
+            if (w == "clamp") return HK_WRAP_CLAMP;
+            if (w == "black") return HK_WRAP_BLACK;
+            throw HikariException("Illegal wrap mode [" + w + "].");
+        };
+        const std::string both = p.GetString("wrapMode", "");
+        if (!both.empty()) {
+            d.wrap_u = d.wrap_v = wrap_of(both);
+        } else {
+            d.wrap_u = wrap_of(p.GetString("uWrapMode", "repeat"));
+            d.wrap_v = wrap_of(p.GetString("vWrapMode", "repeat"));
+        }
+        const std::string ft = p.GetString("filterType", "ewa");
+        if (ft == "nearest") d.filter = HK_FILTER_NEAREST;
+        else if (ft == "bilinear") d.filter = HK_FILTER_BILINEAR;
+        else if (ft == "trilinear") d.filter = HK_FILTER_TRILINEAR;
+        else if (ft == "ewa") d.filter = HK_FILTER_EWA;
+        else throw HikariException("Illegal filter type [" + ft + "].");
+        d.max_anisotropy = p.GetFloat("maxAnisotropy", 20.0f);
+        const std::string chn = p.GetString("channel", "rgb");
+        if (chn == "r") d.channels = 1;
+        else if (chn == "rgb") d.channels = 3;
+        else throw HikariException("Illegal channel [" + chn + "].");
+        uint8_t *buf = nullptr;
+        if (hk_image_load(fn.c_str(), d.channels, &width, &height, &buf) != HK_OK)
+            throw HikariException(std::string("Load texture \"") + fn + "\" failed. Reason : [" + hk_last_error() + "]");
+        pixels.assign(buf, buf + (size_t)width * height * d.channels);
+        hk_image_free(buf);
     }
     EClassType GetClassType() const override { return EClassType::ETexture; }
     void AddChild(Object *c, const std::string &name) override {
@@ -648,9 +688,11 @@ public:
 struct CheckerboardTexture : TexturePlugin { CheckerboardTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_CHECKERBOARD) {} };
 struct GridTexture : TexturePlugin { GridTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_GRID) {} };
 struct ScaleTexture : TexturePlugin { ScaleTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_SCALE) {} };
+struct BitmapTexture : TexturePlugin { BitmapTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_BITMAP) {} };
 HK_REGISTER_CLASS(CheckerboardTexture, "checkerboard")
 HK_REGISTER_CLASS(GridTexture, "grid")
 HK_REGISTER_CLASS(ScaleTexture, "scale")
+HK_REGISTER_CLASS(BitmapTexture, "bitmap")
 
 // The texture slot (hk_bsdf_desc.tex) of a named BSDF texture child, -1 if the
 // BSDF takes no texture of that name (the plugins' AddChild)
@@ -1143,7 +1185,9 @@ int upload_scene(const Scene &sc, const std::string &data_dir, hk_scene *h) {
         hk_texture_desc d = t.d;
         if (t.nested) d.nested = add_texture(*t.nested);
         int32_t id;
-        if ((rc = hk_scene_add_texture(h, &d, &id)) != HK_OK) throw HikariException(hk_last_error());
+        rc = d.kind == HK_TEX_BITMAP ? hk_scene_add_bitmap(h, &d, t.pixels.data(), t.width, t.height, &id)
+                                     : hk_scene_add_texture(h, &d, &id);
+        if (rc != HK_OK) throw HikariException(hk_last_error());
         return id;
     };
     std::function<int32_t(const BSDFPlugin &)> add_bsdf = [&](const BSDFPlugin &b) -> int32_t {

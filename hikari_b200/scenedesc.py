@@ -382,8 +382,40 @@ _TEX_NAMES = {
 }
 
 
+_XML_BASE = ["."]   # directory of the scene file being parsed (bitmap file names resolve against it)
+
+
+def _bitmap_from_xml(d: TextureDesc, p: dict) -> TextureDesc:
+    """BitmapTexture ctor (src/texture/BitmapTexture.cpp:7): the image decoded
+    by the library like stbi_load (hikari_b200.image_load)."""
+    from hikari_b200 import image_load
+
+    d.gamma = float(p.get("gamma", 1.0))
+
+    def wrap(w):
+        if w not in WRAP_NAMES:
+            raise SceneError(f"Illegal wrap mode [{w}].")
+        return WRAP_NAMES[w]
+
+    if p.get("wrapMode", ""):
+        d.wrap_u = d.wrap_v = wrap(p["wrapMode"])
+    else:
+        d.wrap_u, d.wrap_v = wrap(p.get("uWrapMode", "repeat")), wrap(p.get("vWrapMode", "repeat"))
+    ft = p.get("filterType", "ewa")
+    if ft not in FILTER_NAMES:
+        raise SceneError(f"Illegal filter type [{ft}].")
+    d.filter = FILTER_NAMES[ft]
+    d.max_anisotropy = float(p.get("maxAnisotropy", 20.0))
+    ch = p.get("channel", "rgb")
+    if ch not in ("r", "rgb"):
+        raise SceneError(f"Illegal channel [{ch}].")
+    d.channels = 1 if ch == "r" else 3
+    d.pixels = image_load(os.path.join(_XML_BASE[-1], p["filename"]), d.channels)
+    return d
+
+
 def _texture_from_xml(node: ET.Element) -> TextureDesc:
-    """CheckerboardTexture / GridTexture / ScaleTexture ctors (src/texture/*.cpp)."""
+    """CheckerboardTexture / GridTexture / ScaleTexture / BitmapTexture ctors (src/texture/*.cpp)."""
     t = node.attrib["type"]
     if t not in TEX_TYPE_NAMES:
         raise SceneError(f"texture type {t!r} is not supported by the CUDA pathMIS core")
@@ -391,6 +423,8 @@ def _texture_from_xml(node: ET.Element) -> TextureDesc:
     d = TextureDesc(kind=TEX_TYPE_NAMES[t])
     d.uv_scale = [float(p.get("uScale", 1.0)), float(p.get("vScale", 1.0))]
     d.uv_offset = [float(p.get("uOffset", 0.0)), float(p.get("vOffset", 0.0))]
+    if d.kind == TEX_BITMAP:
+        return _bitmap_from_xml(d, p)
     if d.kind == TEX_CHECKERBOARD:
         d.count = int(p.get("blocks", 10))
         d.a = [float(c) for c in p.get("colorA", [0.4, 0.4, 0.4])]
@@ -515,6 +549,14 @@ def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
 
 
 def parse_scene_node(node: ET.Element, base_dir: str, env_loader=None) -> SceneDesc:
+    _XML_BASE.append(base_dir)
+    try:
+        return _parse_scene_node(node, base_dir, env_loader)
+    finally:
+        _XML_BASE.pop()
+
+
+def _parse_scene_node(node: ET.Element, base_dir: str, env_loader=None) -> SceneDesc:
     sd = SceneDesc()
     p = _props(node)
     sd.background = p.get("background", [0.0, 0.0, 0.0])

@@ -243,3 +243,98 @@ def test_camera_differentials_and_screen_partials_vs_reference():
         # the partials solve a 2x2 system on differences of nearby points: an
         # ulp in a direction shows up relative to the largest partial
         np.testing.assert_allclose(pa, pb, rtol=0, atol=5e-4 * np.abs(pb).max() + 1e-7)
+
+
+def _decode(path, ch):
+    import hikari_b200 as hk
+
+    return hk.image_load(str(path), ch)
+
+
+def _stb(R, path, ch):
+    w, h = C.c_int(0), C.c_int(0)
+    n = R.hr_image_load(str(path).encode(), ch, C.byref(w), C.byref(h), None)
+    assert n > 0, f"stb_image cannot read {path}"
+    out = np.zeros(n, np.uint8)
+    R.hr_image_load(str(path).encode(), ch, C.byref(w), C.byref(h), O._p(out))
+    return out.reshape(h.value, w.value, ch)
+
+
+@pytest.mark.parametrize("mode", ["RGB", "RGBA", "L", "LA", "P", "I;16", "1"])
+def test_png_decode_equals_stb(mode, tmp_path):
+    """hk_image_load of PNG files (every color type PIL writes, 16-bit, 1-bit,
+    palette) equals the reference's stbi_load byte for byte, for both channel
+    requests."""
+    R = _ref()
+    img = image(45, 31, 3, 7)
+    im = PIL.fromarray(img)
+    if mode == "RGBA":
+        im = im.convert("RGBA")
+    elif mode == "LA":
+        im = im.convert("LA")
+    elif mode == "P":
+        im = im.convert("P", palette=PIL.Palette.ADAPTIVE, colors=37) if hasattr(PIL, "Palette") else im.convert("P")
+    elif mode == "I;16":
+        im = PIL.fromarray((img[:, :, 0].astype(np.uint16) * 257 + 3).astype(np.uint16))
+    elif mode != "RGB":
+        im = im.convert(mode)
+    p = tmp_path / "t.png"
+    im.save(p)
+    for ch in (1, 3):
+        np.testing.assert_array_equal(_decode(p, ch), _stb(R, p, ch), err_msg=f"{mode} ch {ch}")
+
+
+def test_pnm_decode(tmp_path):
+    img = image(13, 9, 3, 8)
+    p = tmp_path / "t.ppm"
+    p.write_bytes(b"P6\n# comment\n13 9\n255\n" + img.tobytes())
+    np.testing.assert_array_equal(_decode(p, 3), img)
+    g = tmp_path / "t.pgm"
+    g.write_bytes(b"P5 13 9 255\n" + img[:, :, 0].tobytes())
+    np.testing.assert_array_equal(_decode(g, 1)[:, :, 0], img[:, :, 0])
+
+
+@pytest.mark.parametrize("kind", ["420", "444", "422", "gray", "restart"])
+def test_jpeg_decode_close_to_stb(kind, tmp_path):
+    """Baseline JPEG: the library's float IDCT / triangle upsampling / JFIF
+    colour conversion against stb_image's integer versions of the same steps
+    (the reference decode): a few levels apart at most, almost all within one."""
+    R = _ref()
+    img = image(123, 77, 3, 9)
+    im = PIL.fromarray(img)
+    p = tmp_path / "t.jpg"
+    if kind == "gray":
+        im.convert("L").save(p, quality=90)
+    else:
+        sub = {"420": 2, "444": 0, "422": 1, "restart": 2}[kind]
+        extra = {"restart_marker_blocks": 3} if kind == "restart" else {}
+        try:
+            im.save(p, quality=90, subsampling=sub, **extra)
+        except TypeError:
+            im.save(p, quality=90, subsampling=sub)
+    for ch in (1, 3):
+        a, b = _decode(p, ch).astype(int), _stb(R, p, ch).astype(int)
+        assert a.shape == b.shape
+        d = np.abs(a - b)
+        if kind == "422" and ch == 3:
+            # horizontal-only chroma upsampling: stb_image weights the image's
+            # last column differently from the edge-replicating triangle filter
+            d = d[:, :-1]
+        assert d.max() <= 6 and (d <= 1).mean() >= 0.97, f"{kind} ch {ch}: max {d.max()}, <=1: {(d <= 1).mean():.4f}"
+
+
+def test_reference_scene_jpegs_close_to_stb():
+    """The reference's own scene textures (when its checkout is present)."""
+    R = _ref()
+    import glob
+
+    files = sorted(glob.glob("/root/reference/scene/bsdf/*.jpg"))
+    if not files:
+        pytest.skip("reference scene images unavailable")
+    for f in files:
+        if os.path.getsize(f) > 3_000_000:
+            continue
+        a, b = _decode(f, 3).astype(int), _stb(R, f, 3).astype(int)
+        d = np.abs(a - b)
+        assert a.shape == b.shape and d.max() <= 8 and (d <= 1).mean() >= 0.95, \
+            f"{os.path.basename(f)}: max {d.max()}, <=1: {(d <= 1).mean():.4f}"

@@ -387,3 +387,86 @@ def test_xml_texture_errors(L, tmp_path, body, needle):
         hk.parse_xml_info(path)
     with pytest.raises(SceneError, match=needle):
         parse_xml(path)
+
+
+BITMAP_XML = """<?xml version="1.0"?>
+<scene>
+  <integrator type="pathMIS"><integer name="depth" value="8"/></integrator>
+  <camera type="perspective"><integer name="width" value="16"/><integer name="height" value="16"/></camera>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="diffuse"><texture type="bitmap" name="albedo">
+      <string name="filename" value="tex/a.png"/><float name="gamma" value="2.2"/>
+      <float name="uScale" value="2"/></texture></bsdf>
+  </mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="roughConductor"><string name="type" value="ggx"/>
+      <texture type="bitmap" name="alpha"><string name="filename" value="tex/b.ppm"/>
+        <string name="channel" value="r"/><string name="wrapMode" value="clamp"/>
+        <string name="filterType" value="trilinear"/><float name="maxAnisotropy" value="8"/></texture>
+    </bsdf>
+  </mesh>
+</scene>
+"""
+
+
+def test_xml_bitmap_textures(L, tmp_path):
+    """BitmapTexture in both parsers: file names resolve against the scene's
+    directory, the image is decoded like stbi_load, wrap / filter / channel /
+    gamma / anisotropy properties as the reference names them."""
+    from hikari_b200 import scenes
+    from hikari_b200.scenedesc import FILTER_EWA, FILTER_TRILINEAR, TEX_BITMAP, WRAP_CLAMP, WRAP_REPEAT
+
+    PIL = pytest.importorskip("PIL.Image")
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    (tmp_path / "tex").mkdir()
+    a = scenes.synthetic_image(20, 12, 3, 1)
+    PIL.fromarray(a).save(tmp_path / "tex" / "a.png")
+    b = scenes.synthetic_image(9, 7, 3, 2)
+    (tmp_path / "tex" / "b.ppm").write_bytes(b"P6 9 7 255\n" + b.tobytes())
+    path = str(tmp_path / "bitmap.xml")
+    open(path, "w").write(BITMAP_XML)
+    info, depth, spp = hk.parse_xml_info(path)
+    assert info.n_bsdfs == 2 and info.n_meshes == 2
+    sd = parse_xml(path)[0]
+    ta = sd.meshes[0].bsdf.textures["kd"]
+    assert ta.kind == TEX_BITMAP and ta.filter == FILTER_EWA and ta.wrap_u == ta.wrap_v == WRAP_REPEAT
+    assert ta.gamma == pytest.approx(2.2) and ta.uv_scale == [2.0, 1.0] and ta.channels == 3
+    np.testing.assert_array_equal(ta.pixels, a)
+    tb = sd.meshes[1].bsdf.textures["alpha_u"]
+    assert tb.channels == 1 and tb.filter == FILTER_TRILINEAR and tb.wrap_u == tb.wrap_v == WRAP_CLAMP
+    assert tb.max_anisotropy == 8.0
+    luma = (b[..., 0].astype(int) * 77 + b[..., 1].astype(int) * 150 + b[..., 2].astype(int) * 29) >> 8
+    np.testing.assert_array_equal(tb.pixels[:, :, 0], luma)
+
+
+@pytest.mark.parametrize("prop,needle", [
+    ('<string name="filterType" value="cubic"/>', "Illegal filter type"),
+    ('<string name="wrapMode" value="mirror"/>', "Illegal wrap mode"),
+    ('<string name="channel" value="rg"/>', "Illegal channel"),
+])
+def test_xml_bitmap_errors(L, tmp_path, prop, needle):
+    from hikari_b200 import scenes
+    from hikari_b200.scenedesc import SceneError
+
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    (tmp_path / "a.ppm").write_bytes(b"P6 4 4 255\n" + scenes.synthetic_image(4, 4, 3, 0).tobytes())
+    path = str(tmp_path / "bad.xml")
+    open(path, "w").write('<scene><mesh type="obj"><string name="filename" value="quad.obj"/><bsdf type="diffuse">'
+                          '<texture type="bitmap" name="albedo"><string name="filename" value="a.ppm"/>'
+                          f'{prop}</texture></bsdf></mesh></scene>')
+    with pytest.raises(hk.HikariError, match=needle):
+        hk.parse_xml_info(path)
+    with pytest.raises(SceneError, match=needle):
+        parse_xml(path)
+
+
+def test_image_load_errors(L, tmp_path):
+    p = tmp_path / "x.bin"
+    p.write_bytes(b"not an image")
+    with pytest.raises(hk.HikariError, match="unknown image format"):
+        hk.image_load(str(p), 3)
+    with pytest.raises(hk.HikariError, match="cannot open"):
+        hk.image_load(str(tmp_path / "missing.png"), 3)
+    (tmp_path / "p.jpg").write_bytes(b"\xff\xd8\xff\xc2\x00\x0b\x08\x00\x10\x00\x10\x01\x01\x11\x00\xff\xd9")
+    with pytest.raises(hk.HikariError, match="progressive"):
+        hk.image_load(str(tmp_path / "p.jpg"), 3)
