@@ -21,6 +21,8 @@ import numpy as np
 # BSDF kinds, matching hk_bsdf_type in include/hikari_b200.h
 BSDF_DIFFUSE, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_PLASTIC, BSDF_ROUGH_COATING = range(5)
 BSDF_MIRROR, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_PLASTIC, BSDF_TWO_SIDED, BSDF_COATING, BSDF_ROUGH_DIFFUSE = range(5, 12)
+# bumpMap / normalMap wrap one nested BSDF; their map texture is textures["kd"] (slot 0)
+BSDF_BUMP_MAP, BSDF_NORMAL_MAP = 12, 13
 BECKMANN, GGX = 0, 1
 BSDF_TYPE_NAMES = {
     "diffuse": BSDF_DIFFUSE,
@@ -35,6 +37,8 @@ BSDF_TYPE_NAMES = {
     "twoSided": BSDF_TWO_SIDED,
     "coating": BSDF_COATING,
     "roughDiffuse": BSDF_ROUGH_DIFFUSE,
+    "bumpMap": BSDF_BUMP_MAP,
+    "normalMap": BSDF_NORMAL_MAP,
 }
 # BSDFs with a delta (specular) lobe and no microfacet distribution
 SMOOTH_BSDFS = (BSDF_MIRROR, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_PLASTIC, BSDF_COATING)
@@ -526,6 +530,18 @@ def _bsdf_from_xml(node: ET.Element) -> BSDFDesc:
     elif d.type == BSDF_ROUGH_DIFFUSE:   # src/bsdf/RoughDiffuseBSDF.cpp:10-17
         d.kd = p.get("albedo", [0.5, 0.5, 0.5])
         d.fast_approx = bool(p.get("fastApprox", False))
+    elif d.type in (BSDF_BUMP_MAP, BSDF_NORMAL_MAP):   # src/bsdf/{BumpMap,NormalMap}BSDF.cpp AddChild / Activate
+        nested = [c for c in node if c.tag == "bsdf"]
+        maps = [c for c in node if c.tag == "texture"]
+        if len(nested) > 1:
+            raise SceneError(f"{t}: tried to specify multiple nested BSDF")
+        if len(maps) > 1:
+            raise SceneError(f"{t}: tried to specify multiple map textures")
+        if not nested or not maps:
+            raise SceneError(f"{t} needs a nested BSDF and a map texture")
+        d.nested = _bsdf_from_xml(nested[0])
+        d.textures["kd"] = _texture_from_xml(maps[0])
+        return d
     if d.type in (BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC):
         d.anisotropic = bool(p.get("as", False))
     if d.anisotropic:

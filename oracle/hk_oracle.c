@@ -394,8 +394,12 @@ typedef struct {
     struct mip_t *const *mips;         /* their MIP pyramids (bitmaps; NULL otherwise) */
 } bsdf_t;
 
-/* uv: Record.Isect.UV; duv: its screen-space partials (dUdX, dVdX, dUdY, dVdY) */
-typedef struct { v3 wi, wo; float eta; int measure; float uv[2]; float duv[4]; } brec;
+/* uv: Record.Isect.UV; duv: its screen-space partials (dUdX, dVdX, dUdY, dVdY);
+ * it: the record's intersection (frames and dP/du, dP/dv for bumpMap /
+ * normalMap), NULL in queries without one */
+/* dpdu / dpdv with has_uvp: Isect.dPdU / dPdV and bHasUVPartial (set with normals and texture coordinates) */
+typedef struct isect_s { v3 p; frame sh, geo; int mesh; float t; float uv[2]; v3 dpdu, dpdv; int has_uvp; } isect_t;
+typedef struct { v3 wi, wo; float eta; int measure; float uv[2]; float duv[4]; const isect_t *it; } brec;
 
 /* ------------------------------------------------------------ bitmap textures */
 /* LoadImageFromFileR / LoadImageFromFileRGB (src/core/Texture.cpp:12, :74):
@@ -542,6 +546,17 @@ static v3 mip_triangle(const mip_t *m, int l, float u, float v) {
     return add(add(add(scl(t00, a), scl(t01, b)), scl(t10, c)), scl(t11, d));
 }
 static v3 lerp3(float t, v3 a, v3 b) { return add(scl(a, 1.0f - t), scl(b, t)); }
+/* MipMap::EvalGradient :363 (bilinear slope at one level, unscaled UV) */
+static void mip_gradient(const mip_t *m, int l, float u, float v, v3 *g) {
+    float U = u * (float)m->w[l] - 0.5f, Vv = v * (float)m->h[l] - 0.5f;
+    int x = (int)floorf(U), y = (int)floorf(Vv);
+    float dx = U - (float)x, dy = Vv - (float)y;
+    v3 p00 = mip_texel(m, l, x, y), p10 = mip_texel(m, l, x + 1, y);
+    v3 p01 = mip_texel(m, l, x, y + 1), p11 = mip_texel(m, l, x + 1, y + 1);
+    v3 tmp = sub(add(p01, p10), p11);
+    g[0] = scl(sub(add(p10, scl(p00, dy - 1.0f)), scl(tmp, dy)), (float)m->w[l]);
+    g[1] = scl(sub(add(p01, scl(p00, dx - 1.0f)), scl(tmp, dx)), (float)m->h[l]);
+}
 /* MipMap::Lookup(UV, Width) :287 */
 static v3 mip_lookup_width(const mip_t *m, float u, float v, float width) {
     float level = (float)m->levels - 1.0f + log2f(fmaxf(width, 1e-8f));
@@ -610,7 +625,7 @@ static v3 mip_lookup_diff(const mip_t *m, float u, float v, float d0x, float d0y
  * Texture2D::Eval (src/core/Texture.cpp:211) scaled and offset UV and D. */
 static v3 bitmap_eval(const ho_texture_desc *t, const mip_t *m, const float *uvi, const float *duv) {
     float u = uvi[0] * t->uv_scale[0] + t->uv_offset[0], v = uvi[1] * t->uv_scale[1] + t->uv_offset[1];
-    if (t->filter == HO_FILTER_NEAREST)
+    if (t->filter == HO_FILTER_NEAREST || !duv)   /* Eval(UV): the unfiltered lookup (:134) */
         return mip_texel(m, 0, (int)floorf(u * (float)m->w[0]), (int)floorf(v * (float)m->h[0]));
     if (t->filter == HO_FILTER_BILINEAR) return mip_lookup_width(m, u, v, 0.0f);
     return mip_lookup_diff(m, u, v, duv[0] * t->uv_scale[0], duv[1] * t->uv_scale[1], duv[2] * t->uv_scale[0],
@@ -908,6 +923,7 @@ static int bsdf_transmits(const ho_scene *s, int id, int depth) {
     case HO_BSDF_COATING: return bsdf_transmits(s, d->nested, depth + 1);
     case HO_BSDF_TWO_SIDED:
         return bsdf_transmits(s, d->nested, depth + 1) || bsdf_transmits(s, d->nested2, depth + 1);
+    case HO_BSDF_BUMP_MAP: case HO_BSDF_NORMAL_MAP: return bsdf_transmits(s, d->nested, depth + 1);
     default: return 0;
     }
 }
@@ -985,7 +1001,11 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
         b->spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
         if (d->nested < 0 || d->nested >= s->nb) return fail("CoatingBSDF needs a nested BSDF!");
     }
-    if (d->type < HO_BSDF_DIFFUSE || d->type > HO_BSDF_ROUGH_DIFFUSE) return fail("unknown BSDF type");
+    if (d->type == HO_BSDF_BUMP_MAP || d->type == HO_BSDF_NORMAL_MAP) {   /* BumpMapBSDF::Activate :138 */
+        if (d->nested < 0 || d->nested >= s->nb) return fail("bumpMap / normalMap needs a nested BSDF");
+        if (d->tex[0] <= 0) return fail("bumpMap / normalMap needs a map texture");
+    }
+    if (d->type < HO_BSDF_DIFFUSE || d->type > HO_BSDF_NORMAL_MAP) return fail("unknown BSDF type");
     return 0;
 }
 
@@ -1029,11 +1049,16 @@ int ho_film_border(const ho_scene *s) { return s->border; }
  * CheckerboardTexture.cpp:24) or GridTexture::Eval (src/texture/GridTexture.cpp:26);
  * ScaleTexture::Eval (src/texture/ScaleTexture.cpp:17) scales its nested texture. */
 static inline int mod_positive(int a, int b) { int r = a % b; return r < 0 ? r + b : r; }
+static v3 pattern_eval(const ho_texture_desc *t, float u, float v);
+/* duv NULL: Texture::Eval(Isect, bFilter = false) */
 static v3 tex_eval(const ho_texture_desc *T, mip_t *const *M, int id, const float *uvi, const float *duv) {
     const ho_texture_desc *t = &T[id];
     if (t->kind == HO_TEX_SCALE) return scl(tex_eval(T, M, t->nested, uvi, duv), t->scale);
     if (t->kind == HO_TEX_BITMAP) return bitmap_eval(t, M[id], uvi, duv);
-    float u = uvi[0] * t->uv_scale[0] + t->uv_offset[0], v = uvi[1] * t->uv_scale[1] + t->uv_offset[1];
+    return pattern_eval(t, uvi[0] * t->uv_scale[0] + t->uv_offset[0], uvi[1] * t->uv_scale[1] + t->uv_offset[1]);
+}
+/* CheckerboardTexture / GridTexture::Eval(UV) at already scaled coordinates */
+static v3 pattern_eval(const ho_texture_desc *t, float u, float v) {
     if (t->kind == HO_TEX_CHECKERBOARD) {
         int ex = mod_positive(mod_positive((int)(u * t->count), t->count), 2) == 0;
         int ey = mod_positive(mod_positive((int)(v * t->count), t->count), 2) == 0;
@@ -1046,6 +1071,31 @@ static v3 tex_eval(const ho_texture_desc *T, mip_t *const *M, int id, const floa
     return (fabsf(dx) < t->width || fabsf(dy) < t->width) ? vload(t->a) : vload(t->b);
 }
 /* Texture::GetAverage of the procedural textures (used when BSDFs activate) */
+/* Texture::EvalGradient(Isect) (src/core/Texture.cpp:227): the gradient at the
+ * UNSCALED texture coordinates times the UV scale -- MipMap::EvalGradient at
+ * level 0 for bitmaps (zero with nearest filtering, BitmapTexture.cpp:145),
+ * forward differences of Eval(UV) with step Epsilon = 1e-4 for the
+ * procedural ones (:235); ScaleTexture scales its nested gradient (:24). */
+static void tex_gradient(const ho_texture_desc *T, mip_t *const *M, int id, const float *uv, v3 *g) {
+    const ho_texture_desc *t = &T[id];
+    if (t->kind == HO_TEX_SCALE) {
+        tex_gradient(T, M, t->nested, uv, g);
+        g[0] = scl(g[0], t->scale); g[1] = scl(g[1], t->scale);
+        return;
+    }
+    if (t->kind == HO_TEX_BITMAP) {
+        if (t->filter == HO_FILTER_NEAREST) g[0] = g[1] = V(0, 0, 0);
+        else mip_gradient(M[id], 0, uv[0], uv[1], g);
+    } else {
+        const float eps = 1e-4f;
+        v3 c = pattern_eval(t, uv[0], uv[1]), cu = pattern_eval(t, uv[0] + eps, uv[1]),
+           cv = pattern_eval(t, uv[0], uv[1] + eps);
+        g[0] = divs(sub(cu, c), eps);
+        g[1] = divs(sub(cv, c), eps);
+    }
+    g[0] = scl(g[0], t->uv_scale[0]);
+    g[1] = scl(g[1], t->uv_scale[1]);
+}
 static v3 tex_average(const ho_texture_desc *T, mip_t *const *M, int id) {
     const ho_texture_desc *t = &T[id];
     if (t->kind == HO_TEX_SCALE) return scl(tex_average(T, M, t->nested), t->scale);
@@ -1687,9 +1737,71 @@ static float twosided_pdf(const ho_scene *s, const bsdf_t *b, const brec *r) {
     return bsdf_pdf(s, b->d.nested2, &c);
 }
 
+/* BumpMapBSDF::GetPerturbebFrame (src/bsdf/BumpMapBSDF.cpp:172) and
+ * NormalMapBSDF::GetPerturbebFrame (src/bsdf/NormalMapBSDF.cpp:169) */
+static frame perturbed_frame(const ho_scene *s, const bsdf_t *b, const isect_t *it) {
+    frame f;
+    const int tid = b->d.tex[0] - 1;
+    if (b->d.type == HO_BSDF_BUMP_MAP) {
+        v3 g[2];
+        tex_gradient(s->tex, s->mips, tid, it->uv, g);
+        float ddu = lum(g[0]), ddv = lum(g[1]);
+        v3 n = it->sh.n;
+        v3 dpdu = add(it->dpdu, scl(n, ddu - dot(n, it->dpdu)));
+        v3 dpdv = add(it->dpdv, scl(n, ddv - dot(n, it->dpdv)));
+        f.n = normalize(cross(dpdu, dpdv));
+        f.s = normalize(sub(dpdu, scl(f.n, dot(f.n, dpdu))));
+        f.t = cross(f.n, f.s);
+        if (dot(f.n, it->geo.n) < 0.0f) f.n = scl(f.n, -1.0f);
+    } else {
+        v3 c = tex_eval(s->tex, s->mips, tid, it->uv, NULL);   /* Eval(Isect, false) */
+        v3 nn = V(2.0f * c.x - 1.0f, 2.0f * c.y - 1.0f, 2.0f * c.z - 1.0f);
+        f.n = normalize(to_world(&it->sh, nn));
+        f.s = normalize(sub(it->dpdu, scl(f.n, dot(f.n, it->dpdu))));
+        f.t = cross(f.n, f.s);
+    }
+    return f;
+}
+/* BumpMapBSDF / NormalMapBSDF Eval, Pdf (:56, :80): the record moved into the
+ * perturbed frame, zero where a direction changes side */
+static int perturb_record(const ho_scene *s, const bsdf_t *b, const brec *r, brec *q, frame *pf) {
+    *pf = perturbed_frame(s, b, r->it);
+    *q = *r;
+    q->wi = to_local(pf, to_world(&r->it->sh, r->wi));
+    q->wo = to_local(pf, to_world(&r->it->sh, r->wo));
+    return !(r->wo.z * q->wo.z <= 0.0f || r->wi.z * q->wi.z <= 0.0f);
+}
+static v3 bump_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
+    brec q; frame pf;
+    if (!perturb_record(s, b, r, &q, &pf)) return V(0, 0, 0);
+    return bsdf_eval(s, b->d.nested, &q);
+}
+static float bump_pdf(const ho_scene *s, const bsdf_t *b, const brec *r) {
+    brec q; frame pf;
+    if (!perturb_record(s, b, r, &q, &pf)) return 0.0f;
+    return bsdf_pdf(s, b->d.nested, &q);
+}
+/* BumpMapBSDF::Sample (:22) */
+static v3 bump_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux, float uy, ho_pcg32 *rng, const float *u1f) {
+    frame pf = perturbed_frame(s, b, r->it);
+    brec q = *r;
+    q.wi = to_local(&pf, to_world(&r->it->sh, r->wi));
+    q.wo = V(0, 0, 0);
+    q.measure = HO_MEASURE_UNKNOWN;
+    if (r->wi.z * q.wi.z <= 0.0f) return V(0, 0, 0);
+    v3 res = bsdf_sample(s, b->d.nested, &q, ux, uy, rng, u1f);
+    if (!is_zero(res)) {
+        r->wo = to_local(&r->it->sh, to_world(&pf, q.wo));
+        r->eta = q.eta;
+        r->measure = q.measure;
+        if (r->wo.z * q.wo.z <= 0.0f) return V(0, 0, 0);
+    }
+    return res;
+}
 static v3 bsdf_eval(const ho_scene *s, int id, const brec *r) {
     const bsdf_t *b = &s->bsdfs[id];
     switch (b->d.type) {
+    case HO_BSDF_BUMP_MAP: case HO_BSDF_NORMAL_MAP: return bump_eval(s, b, r);
     case HO_BSDF_DIFFUSE: return diffuse_eval(b, r);
     case HO_BSDF_ROUGH_CONDUCTOR: return conductor_eval(b, r);
     case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_eval(b, r);
@@ -1707,6 +1819,7 @@ static v3 bsdf_eval(const ho_scene *s, int id, const brec *r) {
 static float bsdf_pdf(const ho_scene *s, int id, const brec *r) {
     const bsdf_t *b = &s->bsdfs[id];
     switch (b->d.type) {
+    case HO_BSDF_BUMP_MAP: case HO_BSDF_NORMAL_MAP: return bump_pdf(s, b, r);
     case HO_BSDF_DIFFUSE: return diffuse_pdf(r);
     case HO_BSDF_ROUGH_CONDUCTOR: return conductor_pdf(b, r);
     case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_pdf(b, r);
@@ -1724,6 +1837,7 @@ static float bsdf_pdf(const ho_scene *s, int id, const brec *r) {
 static v3 bsdf_sample(const ho_scene *s, int id, brec *r, float ux, float uy, ho_pcg32 *rng, const float *u1f) {
     const bsdf_t *b = &s->bsdfs[id];
     switch (b->d.type) {
+    case HO_BSDF_BUMP_MAP: case HO_BSDF_NORMAL_MAP: return bump_sample(s, b, r, ux, uy, rng, u1f);
     case HO_BSDF_DIFFUSE: return diffuse_sample(b, r, ux, uy);
     case HO_BSDF_ROUGH_CONDUCTOR: return conductor_sample(b, r, ux, uy);
     case HO_BSDF_ROUGH_DIELECTRIC: return dielectric_sample(b, r, ux, uy, rng, u1f);
@@ -1758,15 +1872,37 @@ float ho_bsdf_rft_eval(const ho_scene *s, int id, float c) {
     const bsdf_t *b = &s->bsdfs[id];
     return rft_eval1d(b->rft, b->rft_n, c);
 }
+static void bsdf_batch_any(const ho_scene *s, int id, uint64_t n, const float *wi, const float *u2, const float *u1,
+                           const float *wo, const float *uv, const float *duv, const float *isect, float *s_wo,
+                           float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb, float *p_pdf, int nthreads);
 void ho_bsdf_batch(const ho_scene *s, int id, uint64_t n, const float *wi, const float *u2, const float *u1,
                    const float *wo, const float *uv, const float *duv, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m,
                    float *e_rgb, float *p_pdf, int nthreads) {
+    bsdf_batch_any(s, id, n, wi, u2, u1, wo, uv, duv, NULL, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf, nthreads);
+}
+void ho_bsdf_batch_isect(const ho_scene *s, int id, uint64_t n, const float *wi, const float *u2, const float *u1,
+                         const float *wo, const float *isect, float *s_wo, float *s_w, float *s_pdf, int32_t *s_m,
+                         float *e_rgb, float *p_pdf, int nthreads) {
+    bsdf_batch_any(s, id, n, wi, u2, u1, wo, NULL, NULL, isect, s_wo, s_w, s_pdf, s_m, e_rgb, p_pdf, nthreads);
+}
+static void bsdf_batch_any(const ho_scene *s, int id, uint64_t n, const float *wi, const float *u2, const float *u1,
+                           const float *wo, const float *uv, const float *duv, const float *isect, float *s_wo,
+                           float *s_w, float *s_pdf, int32_t *s_m, float *e_rgb, float *p_pdf, int nthreads) {
 #ifdef _OPENMP
     if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(static)
 #endif
     for (int64_t i = 0; i < (int64_t)n; i++) {
+        isect_t it; memset(&it, 0, sizeof it);
+        if (isect) {   /* S T N, geometric N, dPdU, dPdV, UV */
+            const float *q = isect + 20 * i;
+            it.sh.s = vload(q); it.sh.t = vload(q + 3); it.sh.n = vload(q + 6); it.geo.n = vload(q + 9);
+            it.dpdu = vload(q + 12); it.dpdv = vload(q + 15); it.uv[0] = q[18]; it.uv[1] = q[19];
+            it.has_uvp = 1;
+        }
         brec r; memset(&r, 0, sizeof r);
+        r.it = isect ? &it : NULL;
+        if (isect) { r.uv[0] = it.uv[0]; r.uv[1] = it.uv[1]; }
         r.wi = vload(wi + 3 * i); r.measure = HO_MEASURE_UNKNOWN;
         if (uv) { r.uv[0] = uv[2 * i]; r.uv[1] = uv[2 * i + 1]; }
         if (duv) memcpy(r.duv, duv + 4 * i, 4 * sizeof(float));
@@ -1777,6 +1913,8 @@ void ho_bsdf_batch(const ho_scene *s, int id, uint64_t n, const float *wi, const
         if (s_m) s_m[i] = r.measure;
         if (s_pdf) s_pdf[i] = is_zero(w) && w.x == 0 && w.y == 0 && w.z == 0 ? 0.0f : bsdf_pdf(s, id, &r);
         brec q; memset(&q, 0, sizeof q);
+        q.it = r.it;
+        q.uv[0] = r.uv[0]; q.uv[1] = r.uv[1];
         q.wi = vload(wi + 3 * i); q.wo = vload(wo + 3 * i); q.measure = HO_MEASURE_SOLID_ANGLE; q.eta = 0;
         if (uv) { q.uv[0] = uv[2 * i]; q.uv[1] = uv[2 * i + 1]; }
         if (duv) memcpy(q.duv, duv + 4 * i, 4 * sizeof(float));
@@ -1987,8 +2125,7 @@ static frame frame_from_n_dpdu(v3 n, v3 dpdu) {
 }
 /* Triangle::PostIntersect  src/core/Mesh.cpp:67-172 (the UV partials of :137-156
  * are used only for the shading frame; dNdU / dNdV serve texture filtering) */
-/* dpdu / dpdv with has_uvp: Isect.dPdU / dPdV and bHasUVPartial (set with normals and texture coordinates) */
-typedef struct { v3 p; frame sh, geo; int mesh; float t; float uv[2]; v3 dpdu, dpdv; int has_uvp; } isect_t;
+
 static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
     const uint32_t *f = s->F + 3ull * h->tri;
     v3 p0 = vload(s->P + 3ull * f[0]), p1 = vload(s->P + 3ull * f[1]), p2 = vload(s->P + 3ull * f[2]);
@@ -2321,6 +2458,7 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
                     brec br; br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.wo = to_local(&it.sh, er.wi);
                     br.uv[0] = it.uv[0]; br.uv[1] = it.uv[1];
                     memcpy(br.duv, duv, sizeof duv);
+                    br.it = &it;
                     br.measure = HO_MEASURE_SOLID_ANGLE; br.eta = 0;
                     float pb = bsdf_pdf(s, bsdf, &br);
                     if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
@@ -2334,6 +2472,7 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
         brec br; memset(&br, 0, sizeof br);
         br.uv[0] = it.uv[0]; br.uv[1] = it.uv[1];
         memcpy(br.duv, duv, sizeof duv);
+        br.it = &it;
         br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.measure = HO_MEASURE_UNKNOWN;
         float sx = ho_pcg32_nextf(rng), sy = ho_pcg32_nextf(rng);
         v3 F = bsdf_sample(s, bsdf, &br, sx, sy, rng, NULL);

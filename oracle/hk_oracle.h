@@ -35,7 +35,10 @@ enum {
     HO_BSDF_PLASTIC = 8,          /* "plastic"          src/bsdf/PlasticBSDF.cpp        */
     HO_BSDF_TWO_SIDED = 9,        /* "twoSided"         src/bsdf/TwoSidedBSDF.cpp       */
     HO_BSDF_COATING = 10,         /* "coating"          src/bsdf/CoatingBSDF.cpp        */
-    HO_BSDF_ROUGH_DIFFUSE = 11    /* "roughDiffuse"     src/bsdf/RoughDiffuseBSDF.cpp   */
+    HO_BSDF_ROUGH_DIFFUSE = 11,   /* "roughDiffuse"     src/bsdf/RoughDiffuseBSDF.cpp   */
+    HO_BSDF_BUMP_MAP = 12,        /* "bumpMap"          src/bsdf/BumpMapBSDF.cpp        */
+    HO_BSDF_NORMAL_MAP = 13       /* "normalMap"        src/bsdf/NormalMapBSDF.cpp      */
+    /* bumpMap / normalMap: the map texture in tex[0], the wrapped BSDF in nested */
 };
 enum { HO_BECKMANN = 0, HO_GGX = 1 };
 enum { HO_MEASURE_UNKNOWN = 0, HO_MEASURE_SOLID_ANGLE = 1, HO_MEASURE_DISCRETE = 2 };
@@ -151,6 +154,12 @@ void  ho_bsdf_batch(const ho_scene *s, int bsdf, uint64_t n, const float *wi, co
 /* Intersection::ComputeScreenSpacePartial (src/core/Intersection.cpp:30) of
  * the camera ray through film position (px, py) hitting (tri, u, v):
  * out duv (4) = (dUdX, dVdX, dUdY, dVdY). */
+/* ho_bsdf_batch with each record's intersection (n x 20 floats: shading
+ * frame S T N, geometric N, dPdU, dPdV, UV) -- the records of bumpMap /
+ * normalMap, whose frames perturb the shading frame. */
+void  ho_bsdf_batch_isect(const ho_scene *s, int bsdf, uint64_t n, const float *wi, const float *u2,
+                          const float *u1, const float *wo, const float *isect, float *s_wo, float *s_w,
+                          float *s_pdf, int32_t *s_measure, float *e_rgb, float *p_pdf, int nthreads);
 void  ho_screen_partials(const ho_scene *s, float px, float py, uint32_t tri, float u, float v, float *out4);
 /* RFT 1D eval after activation (for table parity tests). */
 float ho_bsdf_rft_eval(const ho_scene *s, int bsdf, float cos_theta);

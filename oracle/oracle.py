@@ -99,6 +99,7 @@ def lib():
         L.ho_bsdf_pdf.restype = C.c_float
         L.ho_bsdf_batch.argtypes = [P, C.c_int, C.c_uint64, P, P, P, P, P, P, P, P, P, P, P, P, C.c_int]
         L.ho_scene_add_texture.argtypes = [P, C.POINTER(TextureDescC)]
+        L.ho_bsdf_batch_isect.argtypes = [P, C.c_int, C.c_uint64, P, P, P, P, P, P, P, P, P, P, P, C.c_int]
         L.ho_scene_add_bitmap.argtypes = [P, C.POINTER(TextureDescC), P, C.c_int, C.c_int]
         L.ho_texture_eval.argtypes = [P, C.c_int, P, P, P]
         L.ho_texture_mip.argtypes = [P, C.c_int, C.c_int, P, P]
@@ -272,6 +273,21 @@ class OracleScene:
         )
         lib().ho_bsdf_batch(self.h, bsdf, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(uv), _p(duv), _p(out["s_wo"]), _p(out["s_w"]),
                             _p(out["s_pdf"]), _p(out["s_measure"]), _p(out["e_rgb"]), _p(out["p_pdf"]), nthreads)
+        return out
+
+    def bsdf_batch_isect(self, bsdf, wi, u2, u1, wo, isect, nthreads=0):
+        """bsdf_batch with each record's intersection: isect n x 20 (shading
+        frame S T N, geometric N, dPdU, dPdV, UV)."""
+        n = wi.shape[0]
+        wi, u2, wo, isect = _f32(wi), _f32(u2), _f32(wo), _f32(isect)
+        u1 = _f32(u1) if u1 is not None else None
+        out = dict(
+            s_wo=np.zeros((n, 3), np.float32), s_w=np.zeros((n, 3), np.float32), s_pdf=np.zeros(n, np.float32),
+            s_measure=np.zeros(n, np.int32), e_rgb=np.zeros((n, 3), np.float32), p_pdf=np.zeros(n, np.float32),
+        )
+        lib().ho_bsdf_batch_isect(self.h, bsdf, n, _p(wi), _p(u2), _p(u1), _p(wo), _p(isect), _p(out["s_wo"]),
+                                  _p(out["s_w"]), _p(out["s_pdf"]), _p(out["s_measure"]), _p(out["e_rgb"]),
+                                  _p(out["p_pdf"]), nthreads)
         return out
 
     def texture_eval(self, tex, uv, duv=None):

@@ -33,7 +33,7 @@ CORE = ["Object", "PropertyList", "BSDF", "Texture", "MicrofacetDistribution", "
         "Mesh", "Emitter", "DiscretePDF", "BoundingBox", "Ray", "MipMap", "Camera", "ReconstructionFilter"]
 BSDFS = ["DiffuseBSDF", "RoughConductorBSDF", "RoughDielectricBSDF", "RoughPlasticBSDF", "RoughCoatingBSDF",
          "MirrorBSDF", "ConductorBSDF", "DielectricBSDF", "PlasticBSDF", "TwoSidedBSDF", "CoatingBSDF",
-         "RoughDiffuseBSDF"]
+         "RoughDiffuseBSDF", "BumpMapBSDF", "NormalMapBSDF"]
 EMITTERS = ["PointLight", "DirectionalLight", "ConstantLight"]
 TEXTURES = ["CheckerboardTexture", "GridTexture", "ScaleTexture", "BitmapTexture"]
 OTHERS = [("camera", "PerspectiveCamera"), ("filter", "GaussianFilter")]

@@ -52,7 +52,7 @@ void *hr_bsdf_create(int type, int ggx, float alpha, float int_ior, float ext_io
                      int anisotropic) {
     static const char *names[] = {"diffuse", "roughConductor", "roughDielectric", "roughPlastic", "roughCoating",
                                   "mirror", "conductor", "dielectric", "plastic", "twoSided", "coating",
-                                  "roughDiffuse"};
+                                  "roughDiffuse", "bumpMap", "normalMap"};
     auto col = [](const float *c) { return Color3f(c[0], c[1], c[2]); };
     try {
         PropertyList pl;
@@ -352,6 +352,31 @@ void hr_screen_partials(void *cam, void *mesh, uint32_t tri, float u, float v, f
     T.PostIntersect(I);
     I.ComputeScreenSpacePartial(R);
     out[0] = I.dUdX; out[1] = I.dVdX; out[2] = I.dUdY; out[3] = I.dVdY;
+}
+
+/* hr_bsdf_batch with each record's intersection: n x 20 floats (shading frame
+ * S T N, geometric N, dPdU, dPdV, UV) -- for bumpMap / normalMap */
+void hr_bsdf_batch_isect(void *h, uint64_t n, const float *wi, const float *u2, const float *u1, const float *wo,
+                         const float *isect, float *s_wo, float *s_w, float *s_pdf, int *s_m, float *e_rgb,
+                         float *p_pdf) {
+    for (uint64_t i = 0; i < n; i++) {
+        const float *q = isect + 20 * i;
+        Intersection I;
+        I.ShadingFrame = Frame(Vector3f(q[0], q[1], q[2]), Vector3f(q[3], q[4], q[5]), Vector3f(q[6], q[7], q[8]));
+        I.GeometricFrame = Frame(Vector3f(q[9], q[10], q[11]));
+        I.dPdU = Vector3f(q[12], q[13], q[14]);
+        I.dPdV = Vector3f(q[15], q[16], q[17]);
+        I.UV = Point2f(q[18], q[19]);
+        I.bHasUVPartial = true;
+        g_isect = I;
+        float eta; int m;
+        hr_bsdf_sample(h, wi + 3 * i, u2 + 2 * i, u1 ? u1[i] : 0.0f, s_wo + 3 * i, s_w + 3 * i, &m, &eta);
+        s_m[i] = m;
+        bool zero = s_w[3 * i] == 0.0f && s_w[3 * i + 1] == 0.0f && s_w[3 * i + 2] == 0.0f;
+        s_pdf[i] = zero ? 0.0f : hr_bsdf_pdf(h, wi + 3 * i, s_wo + 3 * i, m);
+        hr_bsdf_eval(h, wi + 3 * i, wo + 3 * i, 1, e_rgb + 3 * i);
+        p_pdf[i] = hr_bsdf_pdf(h, wi + 3 * i, wo + 3 * i, 1);
+    }
 }
 
 /* batched over n AoS records (same layout as ho_bsdf_batch) */

@@ -338,3 +338,109 @@ def test_reference_scene_jpegs_close_to_stb():
         d = np.abs(a - b)
         assert a.shape == b.shape and d.max() <= 8 and (d <= 1).mean() >= 0.95, \
             f"{os.path.basename(f)}: max {d.max()}, <=1: {(d <= 1).mean():.4f}"
+
+
+def random_isects(n, seed):
+    """n x 20 intersection records: an orthonormal shading frame S T N, a
+    geometric normal near N (a tenth facing away), dP/du and dP/dv near S and
+    T with random lengths, texture coordinates in [0, 1)."""
+    rng = np.random.default_rng(seed)
+    N = rng.normal(size=(n, 3))
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    a = rng.normal(size=(n, 3))
+    S = a - N * np.sum(a * N, 1, keepdims=True)
+    S /= np.linalg.norm(S, axis=1, keepdims=True)
+    T = np.cross(N, S)
+    G = N + 0.2 * rng.normal(size=(n, 3))
+    G /= np.linalg.norm(G, axis=1, keepdims=True)
+    G[::10] *= -1
+    dpdu = S * rng.uniform(0.2, 3, (n, 1)) + 0.1 * rng.normal(size=(n, 3))
+    dpdv = T * rng.uniform(0.2, 3, (n, 1)) + 0.1 * rng.normal(size=(n, 3))
+    uv = rng.random((n, 2))
+    return np.concatenate([S, T, N, G, dpdu, dpdv, uv], 1).astype(np.float32)
+
+
+def _bump_cases(img3, img1):
+    from hikari_b200.scenedesc import (BSDF_BUMP_MAP, BSDF_NORMAL_MAP, BSDF_ROUGH_DIELECTRIC, TEX_CHECKERBOARD,
+                                       TEX_GRID)
+
+    ewa = TextureDesc(kind=TEX_BITMAP, pixels=img3, channels=3, filter=FILTER_EWA, uv_scale=[2.0, 0.5])
+    near = TextureDesc(kind=TEX_BITMAP, pixels=img3, channels=3, filter=FILTER_NEAREST)
+    r1 = TextureDesc(kind=TEX_BITMAP, pixels=img1, channels=1, filter=FILTER_TRILINEAR)
+    chk = TextureDesc(kind=TEX_CHECKERBOARD, count=9, a=[0.9, 0.7, 0.2], b=[0.1, 0.2, 0.3], uv_scale=[1.5, 1.0])
+    grid = TextureDesc(kind=TEX_SCALE, scale=0.3, nested=TextureDesc(kind=TEX_GRID, count=7, width=0.1))
+    cond = lambda: BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.15, alpha_v=0.15, int_ior=0.2,
+                            ext_ior=1.0, k=[3.9, 2.4, 2.2])
+    return {
+        "bump_bitmap_diffuse": BSDFDesc(type=BSDF_BUMP_MAP, nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.6, 0.5, 0.4]),
+                                        textures={"kd": ewa}),
+        "bump_r_conductor": BSDFDesc(type=BSDF_BUMP_MAP, nested=cond(), textures={"kd": r1}),
+        "bump_nearest_plastic": BSDFDesc(type=BSDF_BUMP_MAP, nested=BSDFDesc(type=BSDF_ROUGH_PLASTIC,
+                                                                             distribution=GGX, alpha_u=0.2,
+                                                                             alpha_v=0.2), textures={"kd": near}),
+        "bump_checker_dielectric": BSDFDesc(type=BSDF_BUMP_MAP, nested=BSDFDesc(
+            type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=1.5, ext_ior=1.0),
+            textures={"kd": chk}),
+        "bump_scaled_grid_conductor": BSDFDesc(type=BSDF_BUMP_MAP, nested=cond(), textures={"kd": grid}),
+        "normal_bitmap_plastic": BSDFDesc(type=BSDF_NORMAL_MAP, nested=BSDFDesc(type=BSDF_ROUGH_PLASTIC,
+                                                                              distribution=GGX, alpha_u=0.2,
+                                                                              alpha_v=0.2), textures={"kd": ewa}),
+        "normal_checker_diffuse": BSDFDesc(type=BSDF_NORMAL_MAP, nested=BSDFDesc(type=BSDF_DIFFUSE),
+                                           textures={"kd": chk}),
+    }
+
+
+BUMP_CASES = ["bump_bitmap_diffuse", "bump_r_conductor", "bump_nearest_plastic", "bump_checker_dielectric",
+              "bump_scaled_grid_conductor", "normal_bitmap_plastic", "normal_checker_diffuse"]
+
+
+@pytest.mark.parametrize("name", BUMP_CASES)
+def test_bump_normal_map_bit_exact_vs_reference(name, tmp_path):
+    """BumpMapBSDF / NormalMapBSDF (perturbed frames from texture gradients or
+    a normal map) record by record, each record with its own intersection."""
+    R = _ref()
+    R.hr_bsdf_batch_isect.argtypes = [C.c_void_p, C.c_uint64] + [C.c_void_p] * 11
+    img3, img1 = image(40, 24, 3, 21), image(33, 29, 1, 22)
+    d = _bump_cases(img3, img1)[name]
+    o = O.OracleScene(SceneDesc())
+    bid = o.add_bsdf(d)
+    assert O.lib().ho_scene_finalize(o.h) == 0
+    keep = []
+    f = lambda a: np.ascontiguousarray(a, np.float32)
+
+    def mk_tex(t):
+        if t.kind == TEX_BITMAP:
+            return ref_bitmap(R, tmp_path, f"t{len(keep)}.png", t.pixels, t)
+        arrs = [f(t.uv_scale), f(t.uv_offset), f(t.a), f(t.b)]
+        keep.append(arrs)
+        h = R.hr_texture_create(t.kind, t.count, t.width, t.scale, *[O._p(a) for a in arrs],
+                                mk_tex(t.nested) if t.nested is not None else None)
+        assert h
+        return h
+
+    def mk(b):
+        if b is None:
+            return None
+        arrs = [f(b.k), f(b.ks), f(b.kd), f(b.sigma_a), f(b.ks_refract)]
+        keep.append(arrs)
+        tex = (C.c_void_p * 6)(*[mk_tex(b.textures[s]) if s in b.textures else None for s in TEX_SLOTS])
+        keep.append(tex)
+        h = R.hr_bsdf_create(b.type, b.distribution, b.alpha_u, b.int_ior, b.ext_ior, *[O._p(a) for a in arrs[:4]],
+                             b.thickness, mk(b.nested), None, O._p(arrs[4]), int(b.nonlinear), int(b.fast_approx), tex,
+                             int(b.anisotropic))
+        assert h
+        return h
+
+    h = mk(d)
+    n = 20000
+    wi, u2, u1, wo = records(n, 31)
+    isect = random_isects(n, 32)
+    a = o.bsdf_batch_isect(bid, wi, u2, u1, wo, isect)
+    b = {k: np.zeros_like(v) for k, v in a.items()}
+    R.hr_bsdf_batch_isect(h, n, O._p(wi), O._p(u2), O._p(u1), O._p(wo), O._p(isect), O._p(b["s_wo"]),
+                          O._p(b["s_w"]), O._p(b["s_pdf"]), O._p(b["s_measure"]), O._p(b["e_rgb"]), O._p(b["p_pdf"]))
+    valid = np.any(a["s_w"] != 0, axis=1)
+    assert valid.mean() > 0.05 and (a["e_rgb"] != 0).any()
+    for k in ("s_w", "s_measure", "s_pdf", "e_rgb", "p_pdf"):
+        assert eq_nan(a[k], b[k]), f"{name}: {k}"
+    assert eq_nan(a["s_wo"][valid], b["s_wo"][valid]), f"{name}: s_wo"
