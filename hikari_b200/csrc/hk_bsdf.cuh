@@ -271,7 +271,21 @@ static __device__ __noinline__ V3 bitmap_eval(const DevTexture &t, float u, floa
                            d.w * t.uv_scale[1]);
 }
 
-__device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, float tv, float4 duv) {
+// MipMap::EvalGradient (include/core/MipMap.hpp:363) at level l, unscaled UV
+__device__ __forceinline__ void mip_gradient(const DevTexture &t, int l, float u, float v, V3 &gu, V3 &gv) {
+    const float W = (float)(1 << max(0, t.lw - l)), H = (float)(1 << max(0, t.lh - l));
+    const float U = u * W - 0.5f, Vv = v * H - 0.5f;
+    const int x = (int)floorf(U), y = (int)floorf(Vv);
+    const float dx = U - (float)x, dy = Vv - (float)y;
+    const V3 p00 = mip_texel(t, l, x, y), p10 = mip_texel(t, l, x + 1, y);
+    const V3 p01 = mip_texel(t, l, x, y + 1), p11 = mip_texel(t, l, x + 1, y + 1);
+    const V3 tmp = (p01 + p10) - p11;
+    gu = ((p10 + p00 * (dy - 1.0f)) - tmp * dy) * W;
+    gv = ((p01 + p00 * (dx - 1.0f)) - tmp * dx) * H;
+}
+__device__ __forceinline__ V3 pattern_eval(const DevTexture &t, float u, float v);
+// filter: Texture::Eval(Isect, bFilter) -- unfiltered bitmaps read the nearest texel (BitmapTexture::Eval(UV) :134)
+__device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, float tv, float4 duv, bool filter = true) {
     float sc[4];
     int ns = 0;
     while (T[id].kind == kTexScale && ns < 4) {
@@ -282,8 +296,47 @@ __device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, fl
     const float u = tu * t.uv_scale[0] + t.uv_offset[0], v = tv * t.uv_scale[1] + t.uv_offset[1];
     V3 c;
     if (t.kind == kTexBitmap) {
-        c = bitmap_eval(t, u, v, duv);
-    } else if (t.kind == kTexCheckerboard) {
+        c = filter ? bitmap_eval(t, u, v, duv)
+                   : mip_texel(t, 0, (int)floorf(u * (float)(1 << t.lw)), (int)floorf(v * (float)(1 << t.lh)));
+    } else {
+        c = pattern_eval(t, u, v);
+    }
+    while (ns > 0) c = c * sc[--ns];
+    return c;
+}
+// Texture::EvalGradient(Isect) (src/core/Texture.cpp:227): gradient at the
+// UNSCALED coordinates times the UV scale; bitmaps: MipMap::EvalGradient at
+// level 0 (zero with nearest filtering, BitmapTexture.cpp:145); procedural:
+// forward differences with step 1e-4 (:235); ScaleTexture scales (:24).
+__device__ __forceinline__ void tex_gradient(const DevTexture *T, int id, float tu, float tv, V3 &gu, V3 &gv) {
+    float sc[4];
+    int ns = 0;
+    while (T[id].kind == kTexScale && ns < 4) {
+        sc[ns++] = T[id].scale;
+        id = T[id].nested;
+    }
+    const DevTexture &t = T[id];
+    if (t.kind == kTexBitmap) {
+        if (t.filter == kFilterNearest) gu = gv = v3(0, 0, 0);
+        else mip_gradient(t, 0, tu, tv, gu, gv);
+    } else {
+        const float eps = 1e-4f;
+        const V3 c = pattern_eval(t, tu, tv), cu = pattern_eval(t, tu + eps, tv), cv = pattern_eval(t, tu, tv + eps);
+        gu = v3((cu.x - c.x) / eps, (cu.y - c.y) / eps, (cu.z - c.z) / eps);
+        gv = v3((cv.x - c.x) / eps, (cv.y - c.y) / eps, (cv.z - c.z) / eps);
+    }
+    gu = gu * t.uv_scale[0];
+    gv = gv * t.uv_scale[1];
+    while (ns > 0) {
+        --ns;
+        gu = gu * sc[ns];
+        gv = gv * sc[ns];
+    }
+}
+// CheckerboardTexture / GridTexture::Eval(UV) at scaled coordinates
+__device__ __forceinline__ V3 pattern_eval(const DevTexture &t, float u, float v) {
+    V3 c;
+    if (t.kind == kTexCheckerboard) {
         bool ex = mod_positive(mod_positive((int)(u * t.count), t.count), 2) == 0;
         bool ey = mod_positive(mod_positive((int)(v * t.count), t.count), 2) == 0;
         c = (ex ^ ey) ? ld_rgb(t.a) : ld_rgb(t.b);
@@ -294,7 +347,6 @@ __device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, fl
         if (dy > 0.5f) dy -= 1.0f;
         c = (fabsf(dx) < t.width || fabsf(dy) < t.width) ? ld_rgb(t.a) : ld_rgb(t.b);
     }
-    while (ns > 0) c = c * sc[--ns];
     return c;
 }
 // A BSDF parameter at the query's intersection: its texture or its constant.
@@ -988,6 +1040,7 @@ __device__ __forceinline__ float bsdf_pdf(const DevBsdf *bs, int id, const BRec 
 // caller draws it lazily through needs_u1().  A twoSided BSDF nests no
 // transmission, so it never draws one.
 __device__ __forceinline__ bool needs_u1(const DevBsdf *bs, int id) {
+    if (bs[id].type == kBumpMap || bs[id].type == kNormalMap) id = bs[id].nested;
     const DevBsdf &b = bs[id];
     if (b.type == kRoughDielectric) return true;
     return (b.type == kRoughCoating || b.type == kCoating) && bs[b.nested].type == kRoughDielectric;
@@ -996,6 +1049,61 @@ __device__ __forceinline__ V3 bsdf_sample(const DevBsdf *bs, int id, BRec &r, fl
     const DevBsdf &b = bs[id];
     if (b.type == kTwoSided) return twosided_sample(bs, b, r, ux, uy, u1);
     return layer_sample(bs, b, r, ux, uy, u1);
+}
+
+// ---- bumpMap / normalMap (src/bsdf/BumpMapBSDF.cpp, src/bsdf/NormalMapBSDF.cpp).
+// The perturbed frame depends on the intersection only, so the shading code
+// computes it once per vertex (perturbed_frames, hk_shading.cuh) and these
+// wrappers move each record between the shading frame and the perturbed one
+// through world space, as the reference does; other BSDFs pass through.
+struct BumpFrames {
+    Frame sh, pf;   // the intersection's shading frame and its perturbed frame
+};
+__device__ __forceinline__ bool is_bump(const DevBsdf &b) { return b.type == kBumpMap || b.type == kNormalMap; }
+// BumpMapBSDF::Eval / Pdf (:56, :80): zero where a direction changes side
+__device__ __forceinline__ bool bump_record(const BumpFrames &f, const BRec &r, BRec &q) {
+    q = r;
+    q.wi = to_local(f.pf, to_world(f.sh, r.wi));
+    q.wo = to_local(f.pf, to_world(f.sh, r.wo));
+    return !(r.wo.z * q.wo.z <= 0.0f || r.wi.z * q.wi.z <= 0.0f);
+}
+static __device__ __noinline__ V3 bump_eval(const DevBsdf *bs, int id, const BRec &r, const BumpFrames &f) {
+    BRec q;
+    if (!bump_record(f, r, q)) return v3(0, 0, 0);
+    return bsdf_eval(bs, bs[id].nested, q);
+}
+static __device__ __noinline__ float bump_pdf(const DevBsdf *bs, int id, const BRec &r, const BumpFrames &f) {
+    BRec q;
+    if (!bump_record(f, r, q)) return 0.0f;
+    return bsdf_pdf(bs, bs[id].nested, q);
+}
+// BumpMapBSDF::Sample (:22)
+static __device__ __noinline__ V3 bump_sample(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1,
+                                       const BumpFrames &f) {
+    BRec q = r;
+    q.wi = to_local(f.pf, to_world(f.sh, r.wi));
+    q.wo = v3(0, 0, 0);
+    q.measure = kMeasureUnknown;
+    if (r.wi.z * q.wi.z <= 0.0f) return v3(0, 0, 0);
+    const V3 res = bsdf_sample(bs, bs[id].nested, q, ux, uy, u1);
+    if (!is_zero(res)) {
+        r.wo = to_local(f.sh, to_world(f.pf, q.wo));
+        r.eta = q.eta;
+        r.measure = q.measure;
+        if (r.wo.z * q.wo.z <= 0.0f) return v3(0, 0, 0);
+    }
+    return res;
+}
+// run-time dispatch including the wrappers (f is read only for them)
+__device__ __forceinline__ V3 bsdf_eval_b(const DevBsdf *bs, int id, const BRec &r, const BumpFrames &f) {
+    return is_bump(bs[id]) ? bump_eval(bs, id, r, f) : bsdf_eval(bs, id, r);
+}
+__device__ __forceinline__ float bsdf_pdf_b(const DevBsdf *bs, int id, const BRec &r, const BumpFrames &f) {
+    return is_bump(bs[id]) ? bump_pdf(bs, id, r, f) : bsdf_pdf(bs, id, r);
+}
+__device__ __forceinline__ V3 bsdf_sample_b(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1,
+                                            const BumpFrames &f) {
+    return is_bump(bs[id]) ? bump_sample(bs, id, r, ux, uy, u1, f) : bsdf_sample(bs, id, r, ux, uy, u1);
 }
 
 }  // namespace hk

@@ -10,7 +10,8 @@ namespace hk {
 
 enum BsdfType : int32_t {
     kDiffuse = 0, kRoughConductor = 1, kRoughDielectric = 2, kRoughPlastic = 3, kRoughCoating = 4,
-    kMirror = 5, kConductor = 6, kDielectric = 7, kPlastic = 8, kTwoSided = 9, kCoating = 10, kRoughDiffuse = 11
+    kMirror = 5, kConductor = 6, kDielectric = 7, kPlastic = 8, kTwoSided = 9, kCoating = 10, kRoughDiffuse = 11,
+    kBumpMap = 12, kNormalMap = 13   // wrap `nested`; the map texture is tex[0]
 };
 enum Distribution : int32_t { kBeckmann = 0, kGGX = 1 };
 enum Measure : int32_t { kMeasureUnknown = 0, kMeasureSolidAngle = 1, kMeasureDiscrete = 2 };

@@ -293,6 +293,8 @@ bool bsdf_transmits(const hk_scene *s, int id, int depth) {
     case hk::kRoughCoating:
     case hk::kCoating: return bsdf_transmits(s, d.nested, depth + 1);
     case hk::kTwoSided: return bsdf_transmits(s, d.nested, depth + 1) || bsdf_transmits(s, d.nested2, depth + 1);
+    case hk::kBumpMap:
+    case hk::kNormalMap: return bsdf_transmits(s, d.nested, depth + 1);
     default: return false;
     }
 }
@@ -336,7 +338,7 @@ bool bsdf_textured(const hk_scene *s, int id, int depth) {
 hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs) {
     hk::DevBsdf b;
     std::memset(&b, 0, sizeof b);
-    if (d.type < hk::kDiffuse || d.type > hk::kRoughDiffuse) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+    if (d.type < hk::kDiffuse || d.type > hk::kNormalMap) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
     for (int k = 0; k < 6; k++) {
         if (d.tex[k] < 0 || d.tex[k] > (int)s->textures.size()) throw HkError{HK_ERR_INVALID, "invalid texture id"};
         b.tex[k] = d.tex[k];
@@ -395,8 +397,9 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
             b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
             if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
             const int nt = s->bsdfs[d.nested].type;
-            if (nt == hk::kRoughCoating || nt == hk::kCoating || nt == hk::kTwoSided)
-                throw HkError{HK_ERR_INVALID, "roughCoating over a coating or twoSided BSDF is not supported"};
+            if (nt == hk::kRoughCoating || nt == hk::kCoating || nt == hk::kTwoSided || nt == hk::kBumpMap ||
+                nt == hk::kNormalMap)
+                throw HkError{HK_ERR_INVALID, "roughCoating over a coating, twoSided, bumpMap or normalMap BSDF is not supported"};
         }
     }
     if (d.type == hk::kCoating) {   // CoatingBSDF::Activate (:255)
@@ -408,8 +411,9 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
         b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
         if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "CoatingBSDF needs a nested BSDF!"};
         const int nt = s->bsdfs[d.nested].type;
-        if (nt == hk::kRoughCoating || nt == hk::kCoating || nt == hk::kTwoSided)
-            throw HkError{HK_ERR_INVALID, "coating over a coating or twoSided BSDF is not supported"};
+        if (nt == hk::kRoughCoating || nt == hk::kCoating || nt == hk::kTwoSided || nt == hk::kBumpMap ||
+            nt == hk::kNormalMap)
+            throw HkError{HK_ERR_INVALID, "coating over a coating, twoSided, bumpMap or normalMap BSDF is not supported"};
     }
     if (d.type == hk::kConductor)   // ConductorBSDF ctor (:17): m_Eta = Color3f(intIOR / extIOR)
         for (int c = 0; c < 3; c++) b.eta_c[c] = b.eta;
@@ -426,10 +430,18 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
         if (d.nested2 >= n_bsdfs) throw HkError{HK_ERR_INVALID, "twoSided: invalid second nested BSDF"};
         if (d.nested2 < 0) b.nested2 = d.nested;
         for (int side : {b.nested, b.nested2}) {
-            if (s->bsdfs[side].type == hk::kTwoSided)
-                throw HkError{HK_ERR_INVALID, "twoSided nested in twoSided is not supported"};
+            const int st = s->bsdfs[side].type;
+            if (st == hk::kTwoSided || st == hk::kBumpMap || st == hk::kNormalMap)
+                throw HkError{HK_ERR_INVALID, "twoSided over a twoSided, bumpMap or normalMap BSDF is not supported"};
             if (bsdf_transmits(s, side, 0)) throw HkError{HK_ERR_INVALID, "Only BSDF without transmission can be nested!"};
         }
+    }
+    if (d.type == hk::kBumpMap || d.type == hk::kNormalMap) {   // BumpMapBSDF / NormalMapBSDF::Activate
+        if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "bumpMap / normalMap needs a nested BSDF"};
+        if (d.tex[0] <= 0) throw HkError{HK_ERR_INVALID, "bumpMap / normalMap needs a map texture"};
+        const int nt = s->bsdfs[d.nested].type;
+        if (nt == hk::kBumpMap || nt == hk::kNormalMap)
+            throw HkError{HK_ERR_INVALID, "bumpMap / normalMap over another bumpMap / normalMap is not supported"};
     }
     return b;
 }
@@ -437,6 +449,15 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
 void build_scene(hk_scene *s) {
     if (s->meshes.empty()) throw HkError{HK_ERR_INVALID, "scene has no meshes"};
     if (s->width == 0 || s->height == 0) throw HkError{HK_ERR_INVALID, "camera has an empty film"};
+    // the perturbed frames need dP/du, dP/dv, which Triangle::PostIntersect sets
+    // only with vertex normals and texture coordinates (the reference reads
+    // stale or unset values otherwise)
+    for (const MeshIn &m : s->meshes) {
+        if (m.bsdf < 0 || m.bsdf >= (int)s->bsdfs.size()) continue;
+        const int t = s->bsdfs[m.bsdf].type;
+        if ((t == hk::kBumpMap || t == hk::kNormalMap) && (m.nrm.empty() || m.uv.empty()))
+            throw HkError{HK_ERR_INVALID, "a mesh with a bumpMap / normalMap BSDF needs vertex normals and texture coordinates"};
+    }
     s->wf.reset();   // the engine holds a copy of the device description that is rebuilt here
     hk::DevScene &D = s->dev;
     std::memset(&D, 0, sizeof D);

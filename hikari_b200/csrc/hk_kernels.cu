@@ -33,10 +33,11 @@ __device__ __forceinline__ uint32_t mesh_emitter(const DevScene &S, int mesh) { 
 template <int kAccel, bool kTex>
 __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float py, int depth_max, int rr_start,
                          PathCounters &pc) {
-    Hit hn;
+    Hit hn, hc;   // the next hit; the current vertex's hit
     bool found_next = false;
     Isect it, itn;
     float4 duv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    BumpFrames bf;   // a bumpMap / normalMap vertex's frames (kTex only)
     V3 L = v3(0, 0, 0), beta = v3(1, 1, 1);
     int depth = 0;
     float w_ems = 1.0f, w_mats = 1.0f;
@@ -50,6 +51,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
                 return ld3(S.background);
             }
             post_intersect(S, h, it);
+            hc = h;
             if (kTex && S.ray_diff) {
                 V3 rx, ry;
                 camera_diff(S, S.cam, S.width, S.height, S.cam_aspect, px, py, rx, ry);
@@ -57,14 +59,19 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
             }
         } else {
             if (kTex) duv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (found_next) it = itn;
-            else {
+            if (found_next) {
+                it = itn;
+                hc = hn;
+            } else {
                 if (has_env) L = L + beta * env_eval(S, ray.d);
                 break;
             }
         }
         const DevMesh &m = S.meshes[it.mesh];
         const int bsdf = m.bsdf;
+        if constexpr (kTex) {
+            if (is_bump(S.bsdfs[bsdf])) bf = perturbed_frames(S, hc, it, S.bsdfs[bsdf]);
+        }
         if (m.emitter >= 0) {
             const DevAreaLight &AL = S.area_lights[__ldg(S.emitter_area + m.emitter)];
             ERec er;
@@ -93,9 +100,16 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
                     br.measure = kMeasureSolidAngle;
                     br.eta = 0.0f;
                     br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv;
-                    float pb = bsdf_pdf(S.bsdfs, bsdf, br);
+                    float pb;
+                    V3 f;
+                    if constexpr (kTex) {
+                        pb = bsdf_pdf_b(S.bsdfs, bsdf, br, bf);
+                        f = bsdf_eval_b(S.bsdfs, bsdf, br, bf);
+                    } else {
+                        pb = bsdf_pdf(S.bsdfs, bsdf, br);
+                        f = bsdf_eval(S.bsdfs, bsdf, br);
+                    }
                     if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
-                    V3 f = bsdf_eval(S.bsdfs, bsdf, br);
                     float c = fabsf(br.wo.z);
                     L = L + v3((((beta.x * f.x) * c) * ld.x) * w_ems, (((beta.y * f.y) * c) * ld.y) * w_ems,
                                (((beta.z * f.z) * c) * ld.z) * w_ems);
@@ -110,7 +124,9 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
         br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv;
         float sx = rng.nextf(), sy = rng.nextf();
         float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
-        V3 F = bsdf_sample(S.bsdfs, bsdf, br, sx, sy, u1);
+        V3 F;
+        if constexpr (kTex) F = bsdf_sample_b(S.bsdfs, bsdf, br, sx, sy, u1, bf);
+        else F = bsdf_sample(S.bsdfs, bsdf, br, sx, sy, u1);
         ray.o = it.p;
         ray.d = to_world(it.sh, br.wo);
         ray.tmin = kRayEps;
@@ -128,7 +144,9 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
                 er.ref = it.p; er.p = itn.p; er.n = itn.sh.n;
                 V3 wi = er.p - er.ref; er.dist = norm(wi); er.wi = wi / er.dist;
                 float plm = area_pdf(AL, er);
-                float pbm = bsdf_pdf(S.bsdfs, bsdf, br);
+                float pbm;
+                if constexpr (kTex) pbm = bsdf_pdf_b(S.bsdfs, bsdf, br, bf);
+                else pbm = bsdf_pdf(S.bsdfs, bsdf, br);
                 if (pbm + plm != 0.0f) w_mats = pbm / (pbm + plm);
             }
         }

@@ -80,25 +80,22 @@ __device__ __forceinline__ void post_intersect(const DevScene &S, const Hit &h, 
     }
 }
 
-// Intersection::ComputeScreenSpacePartial (src/core/Intersection.cpp:30) of
-// the first hit of a camera ray from o with differential directions rx, ry:
-// (dUdX, dVdX, dUdY, dVdY), zero where the hit has no UV partials (a mesh
-// without normals or texture coordinates, a zero-area triangle).  dP/du and
-// dP/dv are those of Triangle::PostIntersect (src/core/Mesh.cpp:116-156).
-__device__ __forceinline__ float4 screen_partials(const DevScene &S, const Hit &h, const Isect &it, V3 o, V3 rx, V3 ry) {
-    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+// dP/du, dP/dv and the geometric normal of a hit as Triangle::PostIntersect
+// leaves them (src/core/Mesh.cpp:106-156): false without UV partials (a mesh
+// without normals or texture coordinates, a zero-area triangle).
+__device__ __forceinline__ bool uv_tangents(const DevScene &S, const Hit &h, const Isect &it, V3 &dpdu, V3 &dpdv,
+                                            V3 &ng) {
     const DevMesh &m = S.meshes[it.mesh];
-    if (!m.has_uv || !m.has_normals) return zero;
+    if (!m.has_uv || !m.has_normals) return false;
     const float4 *tp = S.tris + 3 * h.tri;
     const float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
     const V3 p0 = xyz(q0), dp1 = xyz(q1) - p0, dp2 = xyz(q2) - p0;
     const V3 c = cross(dp1, dp2);
-    if (norm(c) == 0.0f) return zero;
+    if (norm(c) == 0.0f) return false;
     const uint32_t orig = (uint32_t)__float_as_int(q0.w);
     const float2 t0 = __ldg(S.tri_uv + 3 * orig), t1 = __ldg(S.tri_uv + 3 * orig + 1), t2 = __ldg(S.tri_uv + 3 * orig + 2);
     const float du1 = t1.x - t0.x, dv1 = t1.y - t0.y, du2 = t2.x - t0.x, dv2 = t2.y - t0.y;
     const float det = du1 * dv2 - dv1 * du2;
-    V3 dpdu, dpdv;
     if (det == 0.0f) {
         dpdu = it.sh.s;
         dpdv = it.sh.t;
@@ -107,8 +104,18 @@ __device__ __forceinline__ float4 screen_partials(const DevScene &S, const Hit &
         dpdu = (dp1 * dv2 - dp2 * dv1) * inv;
         dpdv = (dp1 * (-du2) + dp2 * du1) * inv;
     }
+    ng = normalize(c);
+    return true;
+}
+
+// Intersection::ComputeScreenSpacePartial (src/core/Intersection.cpp:30) of
+// the first hit of a camera ray from o with differential directions rx, ry:
+// (dUdX, dVdX, dUdY, dVdY), zero where the hit has no UV partials.
+__device__ __forceinline__ float4 screen_partials(const DevScene &S, const Hit &h, const Isect &it, V3 o, V3 rx, V3 ry) {
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    V3 dpdu, dpdv, n;
+    if (!uv_tangents(S, h, it, dpdu, dpdv, n)) return zero;
     if (is_zero(dpdu) && is_zero(dpdv)) return zero;
-    const V3 n = normalize(c);
     const float pp = dot(n, it.p), po = dot(n, o);
     const float prx = dot(n, rx), pry = dot(n, ry);
     if (prx == 0.0f || pry == 0.0f) return zero;
@@ -133,6 +140,36 @@ __device__ __forceinline__ float4 screen_partials(const DevScene &S, const Hit &
     r.z = ok ? (A11 * by0 - A01 * by1) * id : 0.0f;
     r.w = ok ? (A00 * by1 - A10 * by0) * id : 1.0f;
     return r;
+}
+
+// BumpMapBSDF::GetPerturbebFrame (src/bsdf/BumpMapBSDF.cpp:172) and
+// NormalMapBSDF::GetPerturbebFrame (src/bsdf/NormalMapBSDF.cpp:169) for the
+// hit's BSDF b (a bumpMap or normalMap); the host admits these BSDFs only on
+// meshes with normals and texture coordinates.
+__device__ __forceinline__ BumpFrames perturbed_frames(const DevScene &S, const Hit &h, const Isect &it,
+                                                       const DevBsdf &b) {
+    BumpFrames f;
+    f.sh = it.sh;
+    V3 dpdu = v3(0, 0, 0), dpdv = v3(0, 0, 0), ng = it.sh.n;
+    uv_tangents(S, h, it, dpdu, dpdv, ng);
+    Frame &p = f.pf;
+    if (b.type == kBumpMap) {
+        V3 gu, gv;
+        tex_gradient(b.textures, b.tex[0] - 1, it.u, it.v, gu, gv);
+        const float ddu = luminance(gu), ddv = luminance(gv);
+        const V3 n = it.sh.n;
+        const V3 pu = dpdu + n * (ddu - dot(n, dpdu)), pv = dpdv + n * (ddv - dot(n, dpdv));
+        p.n = normalize(cross(pu, pv));
+        p.s = normalize(pu - p.n * dot(p.n, pu));
+        p.t = cross(p.n, p.s);
+        if (dot(p.n, ng) < 0.0f) p.n = p.n * -1.0f;
+    } else {
+        const V3 c = tex_eval(b.textures, b.tex[0] - 1, it.u, it.v, make_float4(0.0f, 0.0f, 0.0f, 0.0f), false);
+        p.n = normalize(to_world(it.sh, v3(2.0f * c.x - 1.0f, 2.0f * c.y - 1.0f, 2.0f * c.z - 1.0f)));
+        p.s = normalize(dpdu - p.n * dot(p.n, dpdu));
+        p.t = cross(p.n, p.s);
+    }
+    return f;
 }
 
 // ------------------------------------------------------------ emitters

@@ -362,7 +362,9 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             // screen-space partials of a camera ray's first hit (textured
             // materials only: Intersection::ComputeScreenSpacePartial)
             float4 duv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            BumpFrames bf;   // a bumpMap / normalMap vertex's frames (this kernel only)
             if constexpr (BT < 0) {
+                if (is_bump(S.bsdfs[bsdf])) bf = perturbed_frames(S, h, it, S.bsdfs[bsdf]);
                 if (depth == 0 && S.ray_diff) {
                     V3 rx, ry;
                     camera_diff(S, J.cam, J.width, J.height, J.cam_aspect, p4.x, p4.y, rx, ry);
@@ -390,9 +392,16 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                 br.tv = it.v;
                 if constexpr (BT < 0) br.duv = duv;   // unread where lookups are compiled out
                 float pl = er.pdf;
-                float pb = bsdf_pdf_t<BT>(S.bsdfs, bsdf, br);
+                float pb;
+                V3 f;
+                if constexpr (BT < 0) {
+                    pb = bsdf_pdf_b(S.bsdfs, bsdf, br, bf);
+                    f = bsdf_eval_b(S.bsdfs, bsdf, br, bf);
+                } else {
+                    pb = bsdf_pdf_t<BT>(S.bsdfs, bsdf, br);
+                    f = bsdf_eval_t<BT>(S.bsdfs, bsdf, br);
+                }
                 float w = (pl + pb != 0.0f) ? pl / (pl + pb) : 1.0f;
-                V3 f = bsdf_eval_t<BT>(S.bsdfs, bsdf, br);
                 float c = fabsf(br.wo.z);
                 V3 contrib = v3((((beta.x * f.x) * c) * ld.x) * w, (((beta.y * f.y) * c) * ld.y) * w,
                                 (((beta.z * f.z) * c) * ld.z) * w);
@@ -416,7 +425,9 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             if constexpr (BT < 0) br.duv = duv;
             float sx = rng.nextf(), sy = rng.nextf();
             float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
-            V3 F = bsdf_sample_t<BT>(S.bsdfs, bsdf, br, sx, sy, u1);
+            V3 F;
+            if constexpr (BT < 0) F = bsdf_sample_b(S.bsdfs, bsdf, br, sx, sy, u1, bf);
+            else F = bsdf_sample_t<BT>(S.bsdfs, bsdf, br, sx, sy, u1);
             beta = beta * F;
             bool alive = !is_zero(beta);
             if (alive) {
@@ -446,7 +457,7 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                 if (S.bsdfs[bsdf].textured && !(flags & kWfFlagForceMats)) {
                     BRec pr = br;
                     pr.eta = 0.0f;
-                    W.prev_pdf[slot] = bsdf_pdf_t<BT>(S.bsdfs, bsdf, pr);
+                    W.prev_pdf[slot] = bsdf_pdf_b(S.bsdfs, bsdf, pr, bf);
                 }
             }
             W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,

@@ -815,6 +815,18 @@ public:
     }
     EClassType GetClassType() const override { return EClassType::EBSDF; }
     void AddChild(Object *c, const std::string &name) override {
+        const bool wrap = d.type == HK_BSDF_BUMP_MAP || d.type == HK_BSDF_NORMAL_MAP;
+        if (wrap) {   // BumpMapBSDF / NormalMapBSDF::AddChild: one BSDF, one map texture (any name)
+            const bool is_tex = c->GetClassType() == EClassType::ETexture;
+            if (is_tex ? (bool)tex[0] : (bool)nested || c->GetClassType() != EClassType::EBSDF) {
+                delete c;
+                throw HikariException(type_name + (is_tex ? ": tried to specify multiple map textures"
+                                                          : ": tried to specify multiple nested BSDF"));
+            }
+            if (is_tex) tex[0].reset((TexturePlugin *)c);
+            else nested.reset((BSDFPlugin *)c);
+            return;
+        }
         if (c->GetClassType() == EClassType::ETexture) {
             const int slot = texture_slot(d.type, name);
             if (slot < 0 || tex[slot]) {
@@ -849,6 +861,8 @@ public:
     void Activate() override {
         if (d.type == HK_BSDF_ROUGH_COATING && !nested) throw HikariException("RoughCoatingBSDF needs a nested BSDF!");
         if (d.type == HK_BSDF_COATING && !nested) throw HikariException("CoatingBSDF needs a nested BSDF!");
+        if ((d.type == HK_BSDF_BUMP_MAP || d.type == HK_BSDF_NORMAL_MAP) && (!nested || !tex[0]))
+            throw HikariException(type_name + " needs a nested BSDF and a map texture");
         if (d.type == HK_BSDF_TWO_SIDED) {   // TwoSidedBSDF::Activate :98
             if (!nested) throw HikariException("TwoSidedBSDF needs at least one nested BSDF!");
             if (nested->transmits() || (nested2 && nested2->transmits()))
@@ -875,6 +889,10 @@ struct ConductorBSDF : BSDFPlugin { ConductorBSDF(const PropertyList &p) : BSDFP
 struct DielectricBSDF : BSDFPlugin { DielectricBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_DIELECTRIC) {} };
 struct PlasticBSDF : BSDFPlugin { PlasticBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_PLASTIC) {} };
 struct TwoSidedBSDF : BSDFPlugin { TwoSidedBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_TWO_SIDED) {} };
+struct BumpMapBSDF : BSDFPlugin { BumpMapBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_BUMP_MAP) {} };
+struct NormalMapBSDF : BSDFPlugin { NormalMapBSDF(const PropertyList &p) : BSDFPlugin(p, HK_BSDF_NORMAL_MAP) {} };
+HK_REGISTER_CLASS(BumpMapBSDF, "bumpMap")
+HK_REGISTER_CLASS(NormalMapBSDF, "normalMap")
 HK_REGISTER_CLASS(MirrorBSDF, "mirror")
 HK_REGISTER_CLASS(ConductorBSDF, "conductor")
 HK_REGISTER_CLASS(DielectricBSDF, "dielectric")

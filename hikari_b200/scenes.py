@@ -21,7 +21,8 @@ import numpy as np
 
 from .scenedesc import (AIR_IOR, BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_DIELECTRIC, BSDF_DIFFUSE, BSDF_MIRROR,
                         BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
-                        BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, FILTER_BILINEAR, FILTER_EWA,
+                        BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, BSDF_BUMP_MAP, BSDF_NORMAL_MAP,
+                        FILTER_BILINEAR, FILTER_EWA,
                         FILTER_NEAREST, FILTER_TRILINEAR, GGX, TEX_BITMAP, TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE,
                         WRAP_CLAMP, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, LightDesc, MeshDesc, SceneDesc,
                         TextureDesc)
@@ -191,7 +192,8 @@ def synthetic_image(width: int, height: int, channels: int, seed: int) -> np.nda
 
 
 def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 12, seed: int = 0,
-                 shading_normals: bool = False, textured: bool = False, bitmap: bool = False) -> SceneDesc:
+                 shading_normals: bool = False, textured: bool = False, bitmap: bool = False,
+                 bump: bool = False) -> SceneDesc:
     """A ground quad and five displaced icospheres (diffuse, roughDiffuse,
     smooth plastic, rough conductor, smooth dielectric) lit, in emitter order,
     by a point light, an emissive quad, a constant environment and a
@@ -207,7 +209,9 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
     ground (with vertex normals, so first hits carry screen-space partials), a
     trilinear albedo on the diffuse sphere, a bilinear roughDiffuse albedo, a
     scaled one-channel EWA roughness on the conductor and a nearest, clamped
-    refraction colour on the glass."""
+    refraction colour on the glass.  bump (with bitmap) wraps the ground in a
+    bumpMap over an EWA bitmap, the roughDiffuse sphere in a normalMap and the
+    conductor in a bumpMap over a checkerboard."""
     sd = SceneDesc()
     gp, gi = quad((-6, 0, 6), (6, 0, 6), (6, 0, -6), (-6, 0, -6))
     ground = MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5]))
@@ -250,6 +254,15 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
                                                           channels=1, filter=FILTER_EWA, max_anisotropy=8.0))
         mats[4].textures["ks_refract"] = TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(33, 17, 3, seed + 5),
                                                      filter=FILTER_NEAREST, wrap_u=WRAP_CLAMP, wrap_v=WRAP_CLAMP)
+    if textured and bitmap and bump:
+        ground.bsdf = BSDFDesc(type=BSDF_BUMP_MAP, nested=ground.bsdf, textures={"kd": TextureDesc(
+            kind=TEX_SCALE, scale=0.02, nested=TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(60, 44, 3, seed + 6),
+                                                           filter=FILTER_EWA, uv_scale=[4.0, 4.0]))})
+        mats[1] = BSDFDesc(type=BSDF_NORMAL_MAP, nested=mats[1], textures={"kd": TextureDesc(
+            kind=TEX_BITMAP, pixels=np.clip(synthetic_image(32, 32, 3, seed + 7) // 4 + [96, 96, 190], 0, 255)
+            .astype(np.uint8), filter=FILTER_BILINEAR)})
+        mats[3] = BSDFDesc(type=BSDF_BUMP_MAP, nested=mats[3], textures={"kd": TextureDesc(
+            kind=TEX_CHECKERBOARD, count=6, a=[0.01] * 3, b=[0.0] * 3)})
     for k, b in enumerate(mats):
         c = (-3.2 + 1.6 * k, 0.85, 0.3 * ((k % 2) * 2 - 1))
         P, F = displaced_icosphere(2, 0.8, c, 0.05, seed + k)

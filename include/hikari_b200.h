@@ -43,6 +43,9 @@ typedef struct hk_scene hk_scene;
 #define HK_BSDF_TWO_SIDED 9        /* "twoSided"        src/bsdf/TwoSidedBSDF.cpp       */
 #define HK_BSDF_COATING 10         /* "coating"         src/bsdf/CoatingBSDF.cpp        */
 #define HK_BSDF_ROUGH_DIFFUSE 11   /* "roughDiffuse"    src/bsdf/RoughDiffuseBSDF.cpp   */
+#define HK_BSDF_BUMP_MAP 12        /* "bumpMap"         src/bsdf/BumpMapBSDF.cpp        */
+#define HK_BSDF_NORMAL_MAP 13      /* "normalMap"       src/bsdf/NormalMapBSDF.cpp      */
+/* bumpMap / normalMap wrap the BSDF `nested`; their map texture is tex[0] */
 #define HK_BECKMANN 0
 #define HK_GGX 1
 

@@ -44,6 +44,8 @@ SCENES = {
     "shading_normals_uv": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True),
     "textured": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True, textured=True),
     "bitmap": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True, textured=True, bitmap=True),
+    "bump": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True, textured=True, bitmap=True,
+                                        bump=True),
 }
 
 
