@@ -934,7 +934,7 @@ int hk_scene_add_bsdf(hk_scene *s, const hk_bsdf_desc *d, int32_t *out_id) {
     return guarded([&] {
         if (!s || !d) throw HkError{HK_ERR_INVALID, "bad arguments"};
         const int nb = (int)s->bsdfs.size();
-        if (d->type < HK_BSDF_DIFFUSE || d->type > HK_BSDF_ROUGH_DIFFUSE) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
+        if (d->type < HK_BSDF_DIFFUSE || d->type > HK_BSDF_NORMAL_MAP) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
         if (d->type == HK_BSDF_ROUGH_COATING && (d->nested < 0 || d->nested >= nb))
             throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
         if (d->type == HK_BSDF_COATING && (d->nested < 0 || d->nested >= nb))
