@@ -470,3 +470,52 @@ def test_image_load_errors(L, tmp_path):
     (tmp_path / "p.jpg").write_bytes(b"\xff\xd8\xff\xc2\x00\x0b\x08\x00\x10\x00\x10\x01\x01\x11\x00\xff\xd9")
     with pytest.raises(hk.HikariError, match="progressive"):
         hk.image_load(str(tmp_path / "p.jpg"), 3)
+
+
+BUMP_XML = """<?xml version="1.0"?>
+<scene>
+  <integrator type="pathMIS"><integer name="depth" value="8"/></integrator>
+  <camera type="perspective"><integer name="width" value="16"/><integer name="height" value="16"/></camera>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="bumpMap">
+      <texture type="scale"><float name="scale" value="0.1"/>
+        <texture type="checkerboard"><integer name="blocks" value="5"/></texture></texture>
+      <bsdf type="roughConductor"><string name="type" value="ggx"/></bsdf>
+    </bsdf>
+  </mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="normalMap">
+      <bsdf type="diffuse"/>
+      <texture type="grid"/>
+    </bsdf>
+  </mesh>
+</scene>
+"""
+
+
+def test_xml_bump_and_normal_maps(L, tmp_path):
+    """bumpMap / normalMap in both parsers: one nested BSDF and one map
+    texture of any name, in either order."""
+    from hikari_b200.scenedesc import (BSDF_BUMP_MAP, BSDF_DIFFUSE, BSDF_NORMAL_MAP, BSDF_ROUGH_CONDUCTOR, TEX_GRID,
+                                       TEX_SCALE)
+
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "bump.xml")
+    open(path, "w").write(BUMP_XML)
+    info, depth, spp = hk.parse_xml_info(path)
+    assert info.n_bsdfs == 4
+    sd = parse_xml(path)[0]
+    b, n = sd.meshes[0].bsdf, sd.meshes[1].bsdf
+    assert b.type == BSDF_BUMP_MAP and b.nested.type == BSDF_ROUGH_CONDUCTOR and b.textures["kd"].kind == TEX_SCALE
+    assert n.type == BSDF_NORMAL_MAP and n.nested.type == BSDF_DIFFUSE and n.textures["kd"].kind == TEX_GRID
+
+
+def test_bump_map_needs_normals_and_uv(L, tmp_path):
+    """The quad has neither vertex normals nor texture coordinates: a
+    bump-mapped mesh is rejected when the scene is built."""
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "bump.xml")
+    open(path, "w").write(BUMP_XML)
+    sd = parse_xml(path)[0]
+    with pytest.raises(hk.HikariError, match="vertex normals and texture coordinates"):
+        hk.Scene.from_desc(sd)
