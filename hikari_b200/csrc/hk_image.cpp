@@ -25,11 +25,28 @@
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "hk_hostutil.h"
 
 namespace {
+
+// rows [0, n) spread over the host's threads (each row written by one thread)
+template <class F>
+void parallel_rows(int n, F f) {
+    const int nt = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), n / 16));
+    if (nt <= 1) {
+        for (int i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < nt; ++t)
+        th.emplace_back([&, t] {
+            for (int i = t; i < n; i += nt) f(i);
+        });
+    for (auto &x : th) x.join();
+}
 
 struct Image {
     int w = 0, h = 0, ch = 0;   // ch: 1 gray, 2 gray+alpha, 3 rgb, 4 rgba
@@ -450,9 +467,10 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
     for (auto &c : comps) {
         const int pw = c.bw * 8;
         c.plane.assign((size_t)pw * c.bh * 8, 0);
-        for (int by = 0; by < c.bh; ++by)
+        parallel_rows(c.bh, [&](int by) {
             for (int bx = 0; bx < c.bw; ++bx)
                 idct8x8(&c.coef[((size_t)by * c.bw + bx) * 64], &c.plane[(size_t)by * 8 * pw + bx * 8], pw, cosk);
+        });
     }
     // upsample each plane to full resolution: triangle filter for 2x factors
     // (3/4 nearer sample, 1/4 farther), replication otherwise
@@ -467,7 +485,7 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
         };
         const int cw = (w * c.hs + hmax - 1) / hmax, chh = (h * c.vs + vmax - 1) / vmax;   // meaningful samples
         auto atc = [&](int x, int y) { return at(std::min(x, cw - 1), std::min(y, chh - 1)); };
-        for (int y = 0; y < h; ++y)
+        parallel_rows(h, [&](int y) {
             for (int x = 0; x < w; ++x) {
                 int v;
                 if (fx == 1 && fy == 1) {
@@ -485,6 +503,7 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
                 }
                 full[(size_t)y * w + x] = (uint8_t)v;
             }
+        });
     };
     Image im;
     im.w = w;
@@ -505,7 +524,8 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
     sample(comps[2], Cr);
     im.ch = 3;
     im.px.resize((size_t)w * h * 3);
-    for (size_t i = 0; i < (size_t)w * h; ++i) {
+    parallel_rows(h, [&](int row) {
+      for (size_t i = (size_t)row * w; i < (size_t)(row + 1) * w; ++i) {
         int r, g, b;
         if (adobe_rgb) {
             r = Y[i]; g = Cb[i]; b = Cr[i];
@@ -518,7 +538,8 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
         im.px[3 * i] = (uint8_t)std::min(255, std::max(0, r));
         im.px[3 * i + 1] = (uint8_t)std::min(255, std::max(0, g));
         im.px[3 * i + 2] = (uint8_t)std::min(255, std::max(0, b));
-    }
+      }
+    });
     return im;
 }
 
