@@ -9,7 +9,7 @@ timed region, as the reference's render timer excludes scene load
 (src/Main.cpp:72-123).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload heterogeneous|mesh_heavy|cornell] [--spp S] [--views V]
+                  [--workload heterogeneous|mesh_heavy|cornell|textured] [--spp S] [--views V]
 
 N > 1 runs under torch.distributed (one process per GPU, replicas: every
 rank renders its own 8 views, "scaling": "weak").  Rank 0 prints one JSON
@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="heterogeneous",
-                    choices=["heterogeneous", "mesh_heavy", "cornell", "serving", "bsdf"])
+                    choices=["heterogeneous", "mesh_heavy", "cornell", "textured", "serving", "bsdf"])
     ap.add_argument("--records", type=int, default=1 << 26, help="bsdf: records per material")
     ap.add_argument("--accel", default="bvh8", choices=["bvh8", "bvh2"],
                     help="tree the kernels traverse: compressed 8-wide (80-byte nodes) or binary (64-byte nodes)")
@@ -80,6 +80,15 @@ def make_workload(name, spp=0, views=0, res=0):
         sd = scenes.mesh_heavy("conductor", width=r, height=r, spp=spp or 256, depth=16)
         cams = [None] * (views or 1)
         desc = f"mesh_heavy: displaced level-8 icosphere (1.31M tris), GGX conductor, sky; {r}x{r} x {sd.spp} spp"
+    elif name == "textured":
+        r = res or 1024
+        sd = scenes.lights_scene(width=r, height=r, spp=spp or 64, depth=12, shading_normals=True, textured=True,
+                                 bitmap=True, bump=True)
+        cams = [None] * (views or 4)
+        desc = (f"textured: ground and five spheres under point, area, constant and directional lights; bitmap "
+                f"textures under every filter (EWA with first-hit ray differentials, trilinear, bilinear, nearest), "
+                f"procedural textures, a bump-mapped ground, a normal-mapped and a bump-mapped sphere; "
+                f"{len(cams)} views x {r}x{r} x {sd.spp} spp, pathMIS depth 12")
     else:
         r = res or 256
         sd = scenes.cornell_box(width=r, height=r, spp=spp or 64)
