@@ -120,8 +120,8 @@ def test_argument_checks_without_device(L):
         assert L.hk_scene_build(h) == -1                       # no meshes
         assert b"no meshes" in L.hk_last_error()
         d = hk.BsdfDesc()
-        d.type = 12
-        assert L.hk_scene_add_bsdf(h, C.byref(d), None) == -1  # unknown BSDF type
+        d.type = 14
+        assert L.hk_scene_add_bsdf(h, C.byref(d), None) == -1  # unknown BSDF type (13 = normalMap is the last)
         d.type = 4
         d.nested = 3
         assert L.hk_scene_add_bsdf(h, C.byref(d), None) == -1  # coating without a nested BSDF
