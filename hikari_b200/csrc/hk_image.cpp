@@ -354,10 +354,15 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
         if (len < 2 || p + len > f.size()) bad("truncated JPEG segment");
         const uint8_t *d = &f[p + 2];
         const size_t n = len - 2;
+        // every read below stays inside the segment
+        auto need = [&](size_t k) {
+            if (k > n) bad("truncated JPEG segment");
+        };
         if (m == 0xdb) {   // DQT
             for (size_t i = 0; i < n;) {
                 const int pq = d[i] >> 4, tq = d[i] & 15;
-                if (tq > 3) bad("bad JPEG quantisation table");
+                if (tq > 3 || pq > 1) bad("bad JPEG quantisation table");
+                need(i + 1 + 64 * (pq ? 2 : 1));
                 ++i;
                 for (int k = 0; k < 64; ++k) {
                     qt[tq][kZigzag[k]] = pq ? (uint16_t)(d[i] << 8 | d[i + 1]) : d[i];
@@ -368,20 +373,25 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
             for (size_t i = 0; i < n;) {
                 const int tc = d[i] >> 4, th = d[i] & 15;
                 if (th > 3 || tc > 1) bad("bad JPEG Huffman table");
+                need(i + 17);
                 Huff &hf = tc ? hac[th] : hdc[th];
                 int total = 0;
                 for (int l = 1; l <= 16; ++l) total += (hf.bits[l] = d[i + l]);
                 if (total > 256) bad("bad JPEG Huffman table");
+                need(i + 17 + (size_t)total);
                 std::memcpy(hf.vals, d + i + 17, (size_t)total);
                 hf.build();
                 i += 17 + (size_t)total;
             }
         } else if (m == 0xc0 || m == 0xc1) {   // SOF0 / SOF1
+            need(6);
             if (d[0] != 8) bad("only 8-bit JPEG is supported");
             h = d[1] << 8 | d[2];
             w = d[3] << 8 | d[4];
             const int nc = d[5];
             if (w <= 0 || h <= 0 || w > 32768 || h > 32768 || (nc != 1 && nc != 3)) bad("unsupported JPEG frame");
+            need(6 + 3 * (size_t)nc);
+            if (frame) bad("JPEG with two frames");
             for (int c = 0; c < nc; ++c) {
                 JComp jc;
                 jc.id = d[6 + 3 * c];
@@ -397,17 +407,20 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
         } else if (m >= 0xc2 && m <= 0xcf && m != 0xc4 && m != 0xc8 && m != 0xcc) {
             bad("progressive / lossless / arithmetic JPEG is not supported");
         } else if (m == 0xdd) {   // DRI
+            need(2);
             restart_interval = d[0] << 8 | d[1];
         } else if (m == 0xee && n >= 12 && std::memcmp(d, "Adobe", 5) == 0) {
             adobe_rgb = d[11] == 0 && comps.size() == 3;
         } else if (m == 0xda) {   // SOS: baseline has one scan holding every component
             if (!frame) bad("JPEG scan before frame");
+            need(1);
             const int ns = d[0];
+            need(1 + 2 * (size_t)ns);
             if (ns != (int)comps.size()) bad("multi-scan JPEG is not supported");
             for (int s = 0; s < ns; ++s) {
                 const int cid = d[1 + 2 * s];
                 for (auto &c : comps)
-                    if (c.id == cid) { c.td = d[2 + 2 * s] >> 4; c.ta = d[2 + 2 * s] & 15; }
+                    if (c.id == cid) { c.td = (d[2 + 2 * s] >> 4) & 3; c.ta = d[2 + 2 * s] & 3; }
             }
             p += len;
             break;
