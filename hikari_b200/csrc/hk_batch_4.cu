@@ -1,0 +1,6 @@
+// BSDF batch instantiations: TwoSided.
+#include "hk_batch.cuh"
+
+namespace hk {
+template cudaError_t launch_bsdf_batch_t<kTwoSided>(const DevScene &, int, uint64_t, const float *, const float *, const float *, const float *, const float *, const float *, float *, float *, float *, int32_t *, float *, float *, int, cudaStream_t);
+}  // namespace hk

@@ -50,4 +50,15 @@ cudaError_t launch_camera_rays(const DevScene &S, uint64_t n, const float *pos, 
 cudaError_t launch_env_eval(const DevScene &S, uint64_t n, const float *wi, float *out, float *pdf, cudaStream_t st);
 int render_occupancy(int margin_lo, int margin_hi, int accel, bool textured);
 
+// Per-instantiation launchers behind the functions above, each compiled in its
+// own translation unit (megakernel: hk_render_*.cu; BSDF batch: hk_batch_*.cu).
+template <int kAccel, bool kTex>
+cudaError_t launch_render_t(const DevScene &S, const RenderLaunch &P, int grid, cudaStream_t st);
+template <int kAccel, bool kTex>
+int render_occupancy_t(int margin_lo, int margin_hi);
+template <int BT>
+cudaError_t launch_bsdf_batch_t(const DevScene &S, int bsdf, uint64_t n, const float *wi, const float *u2, const float *u1,
+                                const float *wo, const float *uv, const float *duv, float *s_wo, float *s_w, float *s_pdf,
+                                int32_t *s_m, float *e_rgb, float *p_pdf, int grid, cudaStream_t st);
+
 }  // namespace hk

@@ -1,0 +1,7 @@
+// Megakernel instantiation: 8-wide tree, texture lookups compiled in.
+#include "hk_megakernel.cuh"
+
+namespace hk {
+template cudaError_t launch_render_t<kAccelBvh8, true>(const DevScene &, const RenderLaunch &, int, cudaStream_t);
+template int render_occupancy_t<kAccelBvh8, true>(int, int);
+}  // namespace hk

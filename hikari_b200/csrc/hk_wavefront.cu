@@ -14,6 +14,9 @@
 //   shadow  any-hit of every queued shadow ray; unoccluded contributions are
 //           added to their path's radiance
 //
+// This file holds regen and the launch sequence; the queue helpers and the
+// extend / shade / shadow kernels are in hk_wf_kernels.cuh.
+//
 // The estimator is the reference's: the next-event MIS weight of an
 // unoccluded emitter is its own pl / (pl + pb) (the reference updates its
 // carried weight exactly when the shadow ray is unoccluded, and uses it right
@@ -21,94 +24,30 @@
 // record and forced to 1 after an EDiscrete sample; Russian roulette runs
 // before the continuation ray is traced (the reference traces first and
 // discards the hit of a terminated path, which changes nothing).
-#include "hk_shading.cuh"
-#include "hk_wavefront.h"
+#include "hk_wf_kernels.cuh"
 
 namespace hk {
 
-// ------------------------------------------------------------ helpers
-__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
-
-// Warp-aggregated append to a queue counter: one atomic per warp.
-__device__ __forceinline__ unsigned warp_append(unsigned *counter) {
-    unsigned mask = __activemask();
-    int leader = __ffs(mask) - 1;
-    unsigned rank = __popc(mask & ((1u << lane_id()) - 1u));
-    unsigned base = 0;
-    if ((int)lane_id() == leader) base = atomicAdd(counter, (unsigned)__popc(mask));
-    base = __shfl_sync(mask, base, leader);
-    return base + rank;
-}
-// Append grouped by key (lanes with equal keys share one atomic).
-__device__ __forceinline__ unsigned warp_append_keyed(unsigned *counters, int key) {
-    unsigned mask = __activemask();
-    unsigned peers = __match_any_sync(mask, key);
-    int leader = __ffs(peers) - 1;
-    unsigned rank = __popc(peers & ((1u << lane_id()) - 1u));
-    unsigned base = 0;
-    if ((int)lane_id() == leader) base = atomicAdd(counters + key, (unsigned)__popc(peers));
-    base = __shfl_sync(peers, base, leader);
-    return base + rank;
-}
-__device__ __forceinline__ void red_add_v4(float4 *addr, float a, float b, float c, float d) {
-    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(addr), "f"(a), "f"(b), "f"(c), "f"(d)
-                 : "memory");
-}
-__device__ __forceinline__ float4 f4(V3 v, float w) { return make_float4(v.x, v.y, v.z, w); }
-
-// PerspectiveCamera::SampleRay (src/camera/PerspectiveCamera.cpp:71) at the
-// job's resolution and pose; field of view and clip planes are the scene's.
-__device__ __forceinline__ Ray camera_ray_job(const DevScene &S, const WfJob &J, float px, float py) {
-    const float *M = J.cam;
-    float u = px * (1.0f / (float)J.width), v = py * (1.0f / (float)J.height);
-    V3 np = v3(S.cam_near * (1.0f - 2.0f * u) / S.cam_cot, S.cam_near * (1.0f - 2.0f * v) / (J.cam_aspect * S.cam_cot),
-               S.cam_near);
-    V3 dir = normalize(np);
-    float invz = 1.0f / dir.z;
-    Ray r;
-    r.o = v3(M[3], M[7], M[11]);
-    r.d = v3(M[0] * dir.x + M[1] * dir.y + M[2] * dir.z, M[4] * dir.x + M[5] * dir.y + M[6] * dir.z,
-             M[8] * dir.x + M[9] * dir.y + M[10] * dir.z);
-    r.tmin = S.cam_near * invz;
-    r.tmax = S.cam_far * invz;
-    return r;
-}
-
-__device__ __forceinline__ uint64_t wf_mix_seed(uint64_t seed, uint64_t s) {
-    uint64_t z = seed + 0x9E3779B97F4A7C15ULL * (s + 1);
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
-    return z ^ (z >> 31);
-}
-
-// Piece of the current plan that holds plan item w (pieces are sorted by plan_begin).
-__device__ __forceinline__ int find_seg(const WfState &W, uint64_t w, int nseg) {
-    int lo = 0, hi = nseg - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (W.segs[mid].plan_begin <= w) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
-// ImageBlock::Put into the job's global film with vector reductions.
-__device__ __forceinline__ void splat_global(const DevScene &S, const WfJob &J, float px, float py, V3 val) {
-    const int B = S.border, FW = (int)J.width + 2 * B, FH = (int)J.height + 2 * B;
-    float *film = J.film;
-    float cx = px - 0.5f - (0 - B), cy = py - 0.5f - (0 - B);
-    int x0 = max((int)ceilf(cx - S.filt_radius), 0), y0 = max((int)ceilf(cy - S.filt_radius), 0);
-    int x1 = min((int)floorf(cx + S.filt_radius), FW - 1), y1 = min((int)floorf(cy + S.filt_radius), FH - 1);
-    float4 *F = reinterpret_cast<float4 *>(film);
-    for (int y = y0; y <= y1; ++y) {
-        float wy = __ldg(S.ftab + (int)(fabsf((float)y - cy) * S.filt_lookup));
-        for (int x = x0; x <= x1; ++x) {
-            float wx = __ldg(S.ftab + (int)(fabsf((float)x - cx) * S.filt_lookup));
-            float w = wx * wy;
-            if (w == 0.0f) continue;
-            red_add_v4(F + (size_t)y * FW + x, (val.x * wx) * wy, (val.y * wx) * wy, (val.z * wx) * wy, w);
-        }
-    }
-}
+// The traversal and shade kernels are instantiated in hk_wf_trace_*.cu and
+// hk_wf_shade_*.cu; this file only calls their launchers.
+extern template cudaError_t wf_launch_extend_t<kAccelBvh8>(const DevScene &, const WfState &, const WfLaunchConfig &, int, cudaStream_t);
+extern template cudaError_t wf_launch_extend_t<kAccelBvh2>(const DevScene &, const WfState &, const WfLaunchConfig &, int, cudaStream_t);
+extern template cudaError_t wf_launch_shadow_t<kAccelBvh8>(const DevScene &, const WfState &, const WfLaunchConfig &, cudaStream_t);
+extern template cudaError_t wf_launch_shadow_t<kAccelBvh2>(const DevScene &, const WfState &, const WfLaunchConfig &, cudaStream_t);
+extern template int wf_trace_occupancy_t<kAccelBvh8>(int, int);
+extern template int wf_trace_occupancy_t<kAccelBvh2>(int, int);
+#define HK_WF_SHADE_EXTERN(K)                                                                                           \
+    extern template cudaError_t wf_launch_shade_t<K>(const DevScene &, const WfState &, const WfLaunchConfig &, int, \
+                                                     cudaStream_t);                                                 \
+    extern template int wf_shade_occupancy_t<K>(int)
+HK_WF_SHADE_EXTERN(0);
+HK_WF_SHADE_EXTERN(1);
+HK_WF_SHADE_EXTERN(2);
+HK_WF_SHADE_EXTERN(3);
+HK_WF_SHADE_EXTERN(4);
+HK_WF_SHADE_EXTERN(5);
+HK_WF_SHADE_EXTERN(6);
+#undef HK_WF_SHADE_EXTERN
 
 // ------------------------------------------------------------ regen
 // Splat and retire the finished paths, then give every finished or idle slot
@@ -229,289 +168,6 @@ __global__ void wf_init_kernel(WfState W) {
     }
 }
 
-// ------------------------------------------------------------ extend
-// Shared memory of the traversal short stacks: kShStack entries per thread.
-__device__ __forceinline__ SharedStack make_stack() {
-    extern __shared__ uint2 wf_stack_smem[];
-    SharedStack s;
-    s.sh = wf_stack_smem + threadIdx.x;
-    s.stride = (int)blockDim.x;
-    s.spill = nullptr;
-    return s;
-}
-
-template <int kAccel>
-__global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, int cur, int steps, int min_idle) {
-    const unsigned n = W.ctr->eq_count[cur];
-    TravStats ts;
-    WalkerOf<kAccel, SharedStack> wk;
-    std::conditional_t<kAccel == kAccelBvh8, uint2, int> stack_mem[kAccel == kAccelBvh8 ? kStackSize - kShStack : kStackSize];
-    if constexpr (kAccel == kAccelBvh8) {
-        wk.stk = make_stack();
-        wk.stk.spill = stack_mem;
-    } else {
-        wk.stack = stack_mem;
-    }
-    int slot = -1;
-    trace_queue<false>(
-        S, wk, &W.ctr->ext_fetch, n, steps, min_idle,
-        [&](int i) {
-            slot = W.eq[cur][i];
-            const float4 o = W.ray_o[slot], d = W.ray_d[slot];
-            Ray r;
-            r.o = v3(o.x, o.y, o.z);
-            r.d = v3(d.x, d.y, d.z);
-            r.tmin = o.w;
-            r.tmax = d.w;
-            return r;
-        },
-        [&](int, const auto &w) {
-            int type = 0;
-            if (w.found) {
-                const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
-                const DevBsdf &B = S.bsdfs[S.meshes[mesh].bsdf];
-                type = B.textured ? kWfGenericQueue : wf_queue_of(B.type);
-            }
-            W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
-            W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
-        },
-        ts);
-    unsigned long long nv = ts.nodes, nt = ts.tris;
-    for (int o = 16; o > 0; o >>= 1) {
-        nv += __shfl_down_sync(0xffffffffu, nv, o);
-        nt += __shfl_down_sync(0xffffffffu, nt, o);
-    }
-    if (lane_id() == 0 && (nv || nt)) {
-        atomicAdd(&W.ctr->node_visits, nv);
-        atomicAdd(&W.ctr->tri_tests, nt);
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&W.ctr->rays, (unsigned long long)n);
-}
-
-// ------------------------------------------------------------ shade
-__device__ __forceinline__ void finish(const WfState &W, int slot) { W.fq[warp_append(&W.ctr->fq_count)] = slot; }
-
-template <int kType>
-__global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, int nxt) {
-    const int n = (int)W.ctr->sq_count[kType];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = W.sq[kType][i];
-        const float4 o4 = W.ray_o[slot], d4 = W.ray_d[slot];
-        const V3 ro = v3(o4.x, o4.y, o4.z), rd = v3(d4.x, d4.y, d4.z);
-        float4 b4 = W.beta[slot];
-        V3 beta = v3(b4.x, b4.y, b4.z);
-        float w_mats = b4.w;
-        float4 p4 = W.pix[slot];
-        const uint32_t dflags = (uint32_t)__float_as_int(p4.w);
-        int depth = (int)(dflags & 0xffffu);
-        uint32_t flags = dflags >> 16;
-        const WfJob &J = W.jobs[__float_as_int(p4.z)];
-        // radiance terms go to the path's accumulator with vector reductions
-        // (as the unoccluded next-event terms do): shade neither reads nor
-        // rewrites it
-        if constexpr (kType == 0) {
-            // miss (PathMISIntegrator.cpp:35-66); a new path's accumulator is zero
-            V3 Le = v3(0, 0, 0);
-            if (S.env_index >= 0 && (depth > 0 || !S.force_background)) Le = beta * env_eval(S, rd);
-            else if (depth == 0) Le = ld3(S.background);
-            if (!all_zero(Le)) red_add_v4(W.lacc + slot, Le.x, Le.y, Le.z, 0.0f);
-            finish(W, slot);
-            continue;
-        } else {
-            constexpr int BT = kType == kWfGenericQueue ? -1 : kType - 1;
-            uint4 rs = W.rng[slot];
-            Pcg32 rng;
-            rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
-            rng.inc = (uint64_t)rs.z | ((uint64_t)rs.w << 32);
-            float4 h4 = W.hit[slot];
-            Hit h;
-            h.t = h4.x; h.u = h4.y; h.v = h4.z; h.tri = __float_as_int(h4.w);
-            Isect it;
-            post_intersect(S, h, it);
-            const DevMesh &m = S.meshes[it.mesh];
-            const int bsdf = m.bsdf;
-            if (m.emitter >= 0) {
-                const DevAreaLight &AL = S.area_lights[__ldg(S.emitter_area + m.emitter)];
-                ERec er;
-                er.ref = ro; er.p = it.p; er.n = it.sh.n;
-                V3 wi = er.p - er.ref; er.dist = norm(wi); er.wi = wi / er.dist;
-                if (depth > 0) {
-                    // MIS weight of the BSDF-sampled hit (PathMISIntegrator.cpp:122-140)
-                    if (flags & kWfFlagForceMats) {
-                        w_mats = 1.0f;
-                    } else {
-                        float4 pwi = W.prev_wi[slot], pwo = W.prev_wo[slot];
-                        BRec pb;
-                        pb.wi = v3(pwi.x, pwi.y, pwi.z);
-                        pb.wo = v3(pwo.x, pwo.y, pwo.z);
-                        pb.measure = __float_as_int(pwo.w);
-                        pb.eta = 0.0f;
-                        pb.tex = false;
-                        pb.tu = pb.tv = 0.0f;
-                        float plm = area_pdf(AL, er);
-                        // a textured BSDF's pdf was taken when it sampled (its
-                        // parameters depend on that vertex's texture lookups)
-                        float pbm = S.bsdfs[__float_as_int(pwi.w)].textured ? W.prev_pdf[slot]
-                                                                            : bsdf_pdf(S.bsdfs, __float_as_int(pwi.w), pb);
-                        if (pbm + plm != 0.0f) w_mats = pbm / (pbm + plm);
-                    }
-                }
-                const V3 Le = (beta * w_mats) * area_eval(AL, er);
-                if (!all_zero(Le)) red_add_v4(W.lacc + slot, Le.x, Le.y, Le.z, 0.0f);
-            }
-            // screen-space partials of a camera ray's first hit (textured
-            // materials only: Intersection::ComputeScreenSpacePartial)
-            float4 duv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            BumpFrames bf;   // a bumpMap / normalMap vertex's frames (this kernel only)
-            if constexpr (BT < 0) {
-                if (is_bump(S.bsdfs[bsdf])) bf = perturbed_frames(S, h, it, S.bsdfs[bsdf]);
-                if (depth == 0 && S.ray_diff) {
-                    V3 rx, ry;
-                    camera_diff(S, J.cam, J.width, J.height, J.cam_aspect, p4.x, p4.y, rx, ry);
-                    duv = screen_partials(S, h, it, ro, rx, ry);
-                }
-            }
-            // next-event estimation over every emitter (PathMISIntegrator.cpp:83-109)
-            const V3 wi_local = to_local(it.sh, rd * -1.0f);
-            for (int e = 0; e < S.nemitters; ++e) {
-                ERec er;
-                er.ref = it.p;
-                er.dist = 0.0f;
-                er.pdf = 0.0f;
-                float u1 = rng.nextf();
-                float ux = rng.nextf(), uy = rng.nextf();
-                V3 ld = emitter_sample(S, e, er, ux, uy, u1);
-                if (is_zero(ld)) continue;
-                BRec br;
-                br.wi = wi_local;
-                br.wo = to_local(it.sh, er.wi);
-                br.measure = kMeasureSolidAngle;
-                br.eta = 0.0f;
-                br.tex = BT < 0;   // textured materials are shaded by the run-time-dispatched kernel
-                br.tu = it.u;
-                br.tv = it.v;
-                if constexpr (BT < 0) br.duv = duv;   // unread where lookups are compiled out
-                float pl = er.pdf;
-                float pb;
-                V3 f;
-                if constexpr (BT < 0) {
-                    pb = bsdf_pdf_b(S.bsdfs, bsdf, br, bf);
-                    f = bsdf_eval_b(S.bsdfs, bsdf, br, bf);
-                } else {
-                    pb = bsdf_pdf_t<BT>(S.bsdfs, bsdf, br);
-                    f = bsdf_eval_t<BT>(S.bsdfs, bsdf, br);
-                }
-                float w = (pl + pb != 0.0f) ? pl / (pl + pb) : 1.0f;
-                float c = fabsf(br.wo.z);
-                V3 contrib = v3((((beta.x * f.x) * c) * ld.x) * w, (((beta.y * f.y) * c) * ld.y) * w,
-                                (((beta.z * f.z) * c) * ld.z) * w);
-                if (all_zero(contrib)) continue;   // adds nothing whether occluded or not
-                unsigned q = warp_append(&W.ctr->shadow_count);
-                if (q < (unsigned)W.max_shadow) {
-                    W.sh_o[q] = f4(it.p, __int_as_float(slot));
-                    W.sh_d[q] = f4(er.p - it.p, 0.0f);
-                    W.sh_c[q] = f4(contrib, 0.0f);
-                }
-            }
-            // BSDF sampling (PathMISIntegrator.cpp:111-120)
-            BRec br;
-            br.wi = wi_local;
-            br.wo = v3(0, 0, 0);
-            br.measure = kMeasureUnknown;
-            br.eta = 0.0f;
-            br.tex = BT < 0;
-            br.tu = it.u;
-            br.tv = it.v;
-            if constexpr (BT < 0) br.duv = duv;
-            float sx = rng.nextf(), sy = rng.nextf();
-            float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
-            V3 F;
-            if constexpr (BT < 0) F = bsdf_sample_b(S.bsdfs, bsdf, br, sx, sy, u1, bf);
-            else F = bsdf_sample_t<BT>(S.bsdfs, bsdf, br, sx, sy, u1);
-            beta = beta * F;
-            bool alive = !is_zero(beta);
-            if (alive) {
-                flags = (br.measure == kMeasureDiscrete) ? kWfFlagForceMats : 0u;
-                if (flags) w_mats = 1.0f;
-                // Russian roulette (PathMISIntegrator.cpp:142-151)
-                if (depth >= J.rr_start) {
-                    if (rng.nextf() < 0.95f) beta = beta * (1.0f / 0.95f);
-                    else alive = false;
-                }
-                ++depth;
-                if (depth >= J.depth) alive = false;   // the next hit would not be shaded
-            }
-            if (!alive) {
-                finish(W, slot);
-                continue;
-            }
-            W.ray_o[slot] = f4(it.p, kRayEps);
-            W.ray_d[slot] = f4(to_world(it.sh, br.wo), __int_as_float(0x7f800000));
-            W.beta[slot] = f4(beta, w_mats);
-            W.pix[slot] = make_float4(p4.x, p4.y, p4.z, __int_as_float((int)((flags << 16) | (uint32_t)depth)));
-            W.prev_wi[slot] = f4(br.wi, __int_as_float(bsdf));
-            W.prev_wo[slot] = f4(br.wo, __int_as_float(br.measure));
-            if constexpr (BT < 0) {
-                // the MIS weight at an emitter hit next needs this BSDF's pdf of
-                // the sampled direction (PathMISIntegrator.cpp:128)
-                if (S.bsdfs[bsdf].textured && !(flags & kWfFlagForceMats)) {
-                    BRec pr = br;
-                    pr.eta = 0.0f;
-                    W.prev_pdf[slot] = bsdf_pdf_b(S.bsdfs, bsdf, pr, bf);
-                }
-            }
-            W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
-                                     (uint32_t)(rng.inc >> 32));
-            W.eq[nxt][warp_append(&W.ctr->eq_count[nxt])] = slot;
-        }
-    }
-}
-
-// ------------------------------------------------------------ shadow
-template <int kAccel>
-__global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W, int steps, int min_idle) {
-    const unsigned n = min(W.ctr->shadow_count, (unsigned)W.max_shadow);
-    TravStats ts;
-    WalkerOf<kAccel, SharedStack> wk;
-    std::conditional_t<kAccel == kAccelBvh8, uint2, int> stack_mem[kAccel == kAccelBvh8 ? kStackSize - kShStack : kStackSize];
-    if constexpr (kAccel == kAccelBvh8) {
-        wk.stk = make_stack();
-        wk.stk.spill = stack_mem;
-    } else {
-        wk.stack = stack_mem;
-    }
-    int slot = -1;
-    trace_queue<true>(
-        S, wk, &W.ctr->sh_fetch, n, steps, min_idle,
-        [&](int i) {
-            const float4 o = W.sh_o[i], d = W.sh_d[i];
-            slot = __float_as_int(o.w);
-            Ray r;
-            r.o = v3(o.x, o.y, o.z);
-            r.d = v3(d.x, d.y, d.z);
-            r.tmin = kRayEps;
-            r.tmax = 1.0f - kRayEps;
-            return r;
-        },
-        [&](int i, const auto &w) {
-            if (!w.found) {
-                const float4 c = W.sh_c[i];
-                red_add_v4(W.lacc + slot, c.x, c.y, c.z, 0.0f);
-            }
-        },
-        ts);
-    unsigned long long nv = ts.nodes, nt = ts.tris;
-    for (int o = 16; o > 0; o >>= 1) {
-        nv += __shfl_down_sync(0xffffffffu, nv, o);
-        nt += __shfl_down_sync(0xffffffffu, nt, o);
-    }
-    if (lane_id() == 0 && (nv || nt)) {
-        atomicAdd(&W.ctr->node_visits_shadow, nv);
-        atomicAdd(&W.ctr->tri_tests_shadow, nt);
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&W.ctr->shadow_rays, (unsigned long long)n);
-}
-
 // Add the engine's statistics to a caller's 7-slot u64 array.
 __global__ void wf_counters_add_kernel(const WfCounters *c, unsigned long long *out) {
     if (threadIdx.x != 0) return;
@@ -525,23 +181,20 @@ __global__ void wf_counters_add_kernel(const WfCounters *c, unsigned long long *
 }
 
 // ------------------------------------------------------------ launchers
-static size_t stack_smem(int threads) { return (size_t)threads * kShStack * sizeof(uint2); }
-
-static void launch_extend(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
-    if (S.accel == kAccelBvh8)
-        wf_extend_kernel<kAccelBvh8><<<C.blocks_extend, C.threads_extend, stack_smem(C.threads_extend), st>>>(
-            S, W, cur, C.fetch_steps, C.fetch_min_idle);
-    else
-        wf_extend_kernel<kAccelBvh2><<<C.blocks_extend, C.threads_extend, 0, st>>>(S, W, cur, C.fetch_steps,
-                                                                               C.fetch_min_idle);
+static cudaError_t launch_extend(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
+    return S.accel == kAccelBvh8 ? wf_launch_extend_t<kAccelBvh8>(S, W, C, cur, st) : wf_launch_extend_t<kAccelBvh2>(S, W, C, cur, st);
 }
-static void launch_shadow(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
-    if (S.accel == kAccelBvh8)
-        wf_shadow_kernel<kAccelBvh8><<<C.blocks_shadow, C.threads_shadow, stack_smem(C.threads_shadow), st>>>(
-            S, W, C.fetch_steps, C.fetch_min_idle);
-    else
-        wf_shadow_kernel<kAccelBvh2><<<C.blocks_shadow, C.threads_shadow, 0, st>>>(S, W, C.fetch_steps,
-                                                                              C.fetch_min_idle);
+static cudaError_t launch_shadow(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
+    return S.accel == kAccelBvh8 ? wf_launch_shadow_t<kAccelBvh8>(S, W, C, st) : wf_launch_shadow_t<kAccelBvh2>(S, W, C, st);
+}
+static cudaError_t launch_shade_all(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int nxt, cudaStream_t st) {
+    wf_launch_shade_t<0>(S, W, C, nxt, st);
+    wf_launch_shade_t<1>(S, W, C, nxt, st);
+    wf_launch_shade_t<2>(S, W, C, nxt, st);
+    wf_launch_shade_t<3>(S, W, C, nxt, st);
+    wf_launch_shade_t<4>(S, W, C, nxt, st);
+    wf_launch_shade_t<5>(S, W, C, nxt, st);
+    return wf_launch_shade_t<6>(S, W, C, nxt, st);
 }
 
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st) {
@@ -559,13 +212,7 @@ cudaError_t wf_launch_iteration(const DevScene &S, const WfState &W, const WfLau
     wf_regen_kernel<<<C.blocks_regen, C.threads_regen, 0, st>>>(S, W, cur);
     wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
     launch_extend(S, W, C, cur, st);
-    wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-    wf_shade_kernel<1><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-    wf_shade_kernel<2><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-    wf_shade_kernel<3><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-    wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-    wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-    wf_shade_kernel<6><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+    launch_shade_all(S, W, C, nxt, st);
     launch_shadow(S, W, C, st);
     return cudaGetLastError();
 }
@@ -579,15 +226,7 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
         wf_reset_kernel<<<1, 32, 0, st>>>(W, cur);
         break;
     case 1: launch_extend(S, W, C, cur, st); break;
-    case 2:
-        wf_shade_kernel<0><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-        wf_shade_kernel<1><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-        wf_shade_kernel<2><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-        wf_shade_kernel<3><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-        wf_shade_kernel<4><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-        wf_shade_kernel<5><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-        wf_shade_kernel<6><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
-        break;
+    case 2: launch_shade_all(S, W, C, nxt, st); break;
     default: launch_shadow(S, W, C, st); break;
     }
     return cudaGetLastError();
@@ -598,14 +237,8 @@ int wf_occupancy(int which, int threads, int accel) {
     const bool w8 = accel == kAccelBvh8;
     switch (which) {
     case 0:
-        if (w8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccelBvh8>, threads, stack_smem(threads));
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccelBvh2>, threads, 0);
-        break;
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade_kernel<5>, threads, 0); break;
-    case 2:
-        if (w8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccelBvh8>, threads, stack_smem(threads));
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccelBvh2>, threads, 0);
-        break;
+    case 2: return w8 ? wf_trace_occupancy_t<kAccelBvh8>(which, threads) : wf_trace_occupancy_t<kAccelBvh2>(which, threads);
+    case 1: return wf_shade_occupancy_t<5>(threads);
     default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_regen_kernel, threads, 0); break;
     }
     return n;
