@@ -488,7 +488,34 @@ class Scene:
                             camera=None, image_index: int = 0, stream=None) -> None:
         """Render into the device tensor `out` (H x W x 3 float32) through the
         entry point that allocates no device memory (static scratch; films up
-        to 520 x 520 including the filter border)."""
+        to 520 x 520 including the filter border).
+
+        The C side cannot check the buffers it is given, so they are checked
+        here: `out` a contiguous float32 CUDA tensor of shape (H, W, 3),
+        `counters` (optional) a contiguous 8-byte integer CUDA tensor of at
+        least 5 elements, both on the current device."""
+        import torch
+
+        cam = self.desc.camera if self.desc is not None else None
+        dev = torch.cuda.current_device()
+
+        def on_device(t, what):
+            if not isinstance(t, torch.Tensor) or not t.is_cuda:
+                raise TypeError(f"{what} must be a CUDA tensor")
+            if t.device.index != dev:
+                raise ValueError(f"{what} is on cuda:{t.device.index}, the current device is cuda:{dev}")
+            if not t.is_contiguous():
+                raise ValueError(f"{what} must be contiguous")
+
+        on_device(out, "out")
+        if out.dtype != torch.float32 or out.dim() != 3 or out.shape[2] != 3:
+            raise ValueError(f"out must be float32 of shape (H, W, 3), got {out.dtype} {tuple(out.shape)}")
+        if cam is not None and (out.shape[0], out.shape[1]) != (cam.height, cam.width):
+            raise ValueError(f"out is {tuple(out.shape[:2])}, the image is ({cam.height}, {cam.width})")
+        if counters is not None:
+            on_device(counters, "counters")
+            if counters.element_size() != 8 or counters.dtype.is_floating_point or counters.numel() < 5:
+                raise ValueError("counters must hold at least 5 64-bit integers")
         d = render_desc(spp, depth, seed, 0, rr_start, image_index, 0, camera)
         check(lib().hk_render_image_static(self.h, C.byref(d), _p(out), _p(counters), _stream(stream)))
 

@@ -236,6 +236,7 @@ struct hk_scene {
     hk_scene_info info{};
     int margin_lo = 0, margin_hi = 0;
     int sm_count = 148;
+    int device = 0;   // CUDA device the scene was built on
     int occupancy = 1;        // resident megakernel CTAs per SM for the traversed tree
     int occupancy_of[2] = {1, 1};
     std::unique_ptr<hk::WfEngine> wf;   // wavefront engine (allocated on first use)
@@ -767,6 +768,7 @@ void build_scene(hk_scene *s) {
 
     int dev = 0;
     HK_CUDA(cudaGetDevice(&dev));
+    s->device = dev;
     HK_CUDA(cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, dev));
     for (int a = 0; a < 2; ++a) s->occupancy_of[a] = std::max(1, hk::render_occupancy(s->margin_lo, s->margin_hi, a, D.textured != 0));
     s->occupancy = s->occupancy_of[D.accel];
@@ -1213,6 +1215,12 @@ int hk_render_image_static(hk_scene *s, const hk_render_desc *d, float *rgb_dev,
                                               std::to_string(film_floats) + " film floats; the static scratch holds " +
                                               std::to_string(hk::kStaticFilmFloats) +
                                               " (up to 512x512 pixels at border 4); use hk_render"};
+        // the scratch address is per device: the scene's device must be current
+        int cur = 0;
+        HK_CUDA(cudaGetDevice(&cur));
+        if (cur != s->device)
+            throw HkError{HK_ERR_INVALID, "the scene was built on device " + std::to_string(s->device) +
+                                              " but device " + std::to_string(cur) + " is current"};
         void *scratch = nullptr;
         HK_CUDA(hk::static_render_scratch(&scratch));
         cudaStream_t st = (cudaStream_t)stream;

@@ -21,12 +21,17 @@ struct HkError {
 // Records msg as the calling thread's hk_last_error() and returns code.
 int set_error(int code, const std::string &msg);
 
+// A failing call's error is reported to the caller and then cleared from the
+// runtime's last-error slot (a failed cudaMalloc would otherwise surface again
+// at the next launch check of an unrelated call on this thread).
 #define HK_CUDA(call)                                                                                   \
     do {                                                                                                \
         cudaError_t e_ = (call);                                                                        \
-        if (e_ != cudaSuccess)                                                                          \
+        if (e_ != cudaSuccess) {                                                                        \
+            (void)cudaGetLastError();                                                                   \
             throw ::hk::HkError{e_ == cudaErrorMemoryAllocation ? HK_ERR_NOMEM : HK_ERR_CUDA,           \
                                 std::string(#call) + ": " + cudaGetErrorString(e_)};                    \
+        }                                                                                               \
     } while (0)
 
 // Runs f and turns every exception into an HK_ERR_* status: nothing throws

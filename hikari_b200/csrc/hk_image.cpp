@@ -217,14 +217,18 @@ Image decode_pnm(const std::vector<uint8_t> &f) {
 struct Huff {
     uint8_t bits[17] = {};
     uint8_t vals[256] = {};
-    int mincode[17], maxcode[18], valptr[17];
-    uint16_t fast[512];   // 9-bit lookahead: (length << 8) | value, 0 = slow path
+    int mincode[17] = {}, maxcode[18] = {}, valptr[17] = {};
+    uint16_t fast[512] = {};   // 9-bit lookahead: (length << 8) | value, 0 = slow path
+    bool defined = false;      // set by a DHT segment
     void build() {
         int code = 0, k = 0;
         for (int l = 1; l <= 16; ++l) {
             valptr[l] = k;
             mincode[l] = code;
             code += bits[l];
+            // a prefix code has at most 2^l codes of length <= l: more would
+            // run the fast table below past its 512 entries
+            if (code > (1 << l)) bad("bad JPEG Huffman table");
             k += bits[l];
             maxcode[l] = bits[l] ? code - 1 : -1;
             code <<= 1;
@@ -240,6 +244,7 @@ struct Huff {
             }
             code <<= 1;
         }
+        defined = true;
     }
 };
 
@@ -336,7 +341,8 @@ void idct8x8(const int16_t *in, uint8_t *out, int stride, const float *cosk) {
 }
 
 Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
-    uint16_t qt[4][64];
+    uint16_t qt[4][64] = {};
+    bool qt_defined[4] = {};
     Huff hdc[4], hac[4];
     std::vector<JComp> comps;
     int w = 0, h = 0, hmax = 1, vmax = 1, restart_interval = 0;
@@ -368,6 +374,7 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
                     qt[tq][kZigzag[k]] = pq ? (uint16_t)(d[i] << 8 | d[i + 1]) : d[i];
                     i += pq ? 2 : 1;
                 }
+                qt_defined[tq] = true;
             }
         } else if (m == 0xc4) {   // DHT
             for (size_t i = 0; i < n;) {
@@ -422,6 +429,10 @@ Image decode_jpeg(const std::vector<uint8_t> &f, int req) {
                 for (auto &c : comps)
                     if (c.id == cid) { c.td = (d[2 + 2 * s] >> 4) & 3; c.ta = d[2 + 2 * s] & 3; }
             }
+            // every table the scan decodes with must have been defined
+            for (const auto &c : comps)
+                if (!hdc[c.td].defined || !hac[c.ta].defined || !qt_defined[c.tq])
+                    bad("JPEG scan names an undefined table");
             p += len;
             break;
         }

@@ -287,9 +287,13 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
  * holds until exit; films are limited to (W+2B)*(H+2B) <= 520*520 pixels
  * (512x512 at a filter border of 4) and larger images are rejected with
  * HK_ERR_INVALID.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) and caches it; make that first call before
- * any stream capture.  All calls share the array and each call clears it:
- * calls that overlap on the GPU (other streams, other threads) race.
+ * address (cudaGetSymbolAddress) and caches it for the life of the process;
+ * make that first call before any stream capture.  The scene's device must be
+ * the current device (HK_ERR_INVALID otherwise).  A device reset
+ * (cudaDeviceReset, or a reset of the primary context) while the library is
+ * loaded is not supported: the cached address would be stale.  All calls share
+ * the array and each call clears it: calls that overlap on the GPU (other
+ * streams, other threads) race, and the caller must serialise them.
  * rgb_dev: H*W*3 floats; counters_dev (optional): 5 x u64 as hk_render. */
 int hk_render_image_static(hk_scene *s, const hk_render_desc *desc, float *rgb_dev, unsigned long long *counters_dev,
                            void *stream);

@@ -8,9 +8,10 @@ accumulator) in a static device array and writes into an image the caller
 supplies.  This test checks, through the C ABI, that two calls in a row give
 the image of the allocating entry point (hk_render_image) within the
 tolerance of the other GPU tests -- the same sample streams, summed in a
-different atomic order -- and that a film beyond the array's limit is
-rejected.  The file sorts last so a stop-at-first-failure run has already run
-every other test."""
+different atomic order -- that the second call still succeeds with the
+device's free memory taken up (where the allocating entry point then fails),
+and that a film beyond the array's limit is rejected.  The file sorts last so
+a stop-at-first-failure run has already run every other test."""
 import numpy as np
 import pytest
 
@@ -23,16 +24,44 @@ from tests.gpu_helpers import rel_close  # noqa: E402
 RTOL = 1e-5
 
 
+def _take_free_memory(keep_bytes: int):
+    """Hold device memory until less than keep_bytes is free (a cudaMalloc of
+    the film the allocating path needs cannot succeed then)."""
+    torch.cuda.empty_cache()
+    held = []
+    chunk = 8 << 30
+    while chunk >= (2 << 20):
+        free, _ = torch.cuda.mem_get_info()
+        if free <= keep_bytes:
+            break
+        try:
+            held.append(torch.empty(min(chunk, free - keep_bytes // 2), dtype=torch.uint8, device="cuda"))
+        except torch.OutOfMemoryError:
+            chunk //= 2
+    return held
+
+
 @pytest.mark.gpu
 def test_static_scratch_render_matches_allocating_entry_point():
-    sd = scenes.cornell_box(width=64, height=48)
+    w, h = 256, 192
+    sd = scenes.cornell_box(width=w, height=h)
     gs = hk.Scene.from_desc(sd)
-    ref, ref_ctr = gs.render_image(256, sd.depth, seed=11)
+    ref, ref_ctr = gs.render_image(64, sd.depth, seed=11)
+    film_bytes = (w + 4) * (h + 4) * 16
     for call in range(2):
-        out = torch.full((48, 64, 3), -1.0, dtype=torch.float32, device="cuda")
+        out = torch.full((h, w, 3), -1.0, dtype=torch.float32, device="cuda")
         ctr = torch.zeros(5, dtype=torch.int64, device="cuda")
-        gs.render_image_static(out, 256, sd.depth, seed=11, counters=ctr)
+        held = []
+        if call == 1:
+            # the second call runs with the device's free memory taken: an
+            # allocation of the film would fail (checked on the allocating path)
+            held = _take_free_memory(film_bytes // 2)
+            with pytest.raises(hk.HikariError):
+                gs.render_image(1, sd.depth, seed=11)
+        gs.render_image_static(out, 64, sd.depth, seed=11, counters=ctr)
         torch.cuda.synchronize()
+        del held
+        torch.cuda.empty_cache()
         img = out.cpu().numpy()
         ok = rel_close(img, ref, RTOL, atol=1e-6 * float(np.abs(ref).max()))
         assert ok.all(), f"call {call}: {np.sum(~ok)} pixels differ beyond {RTOL}"
@@ -47,3 +76,21 @@ def test_static_scratch_rejects_films_beyond_its_size():
     out = torch.empty((600, 600, 3), dtype=torch.float32, device="cuda")
     with pytest.raises(hk.HikariError, match="static scratch"):
         gs.render_image_static(out, 1, sd.depth)
+
+
+@pytest.mark.gpu
+def test_static_scratch_checks_its_buffers():
+    sd = scenes.cornell_box(width=32, height=32)
+    gs = hk.Scene.from_desc(sd)
+    with pytest.raises(TypeError):
+        gs.render_image_static(np.zeros((32, 32, 3), np.float32), 1, sd.depth)
+    with pytest.raises(ValueError):
+        gs.render_image_static(torch.zeros((32, 32, 3), dtype=torch.float64, device="cuda"), 1, sd.depth)
+    with pytest.raises(ValueError):
+        gs.render_image_static(torch.zeros((16, 32, 3), dtype=torch.float32, device="cuda"), 1, sd.depth)
+    with pytest.raises(ValueError):
+        gs.render_image_static(torch.zeros((32, 3, 32), dtype=torch.float32, device="cuda").transpose(1, 2), 1,
+                               sd.depth)
+    with pytest.raises(ValueError):
+        gs.render_image_static(torch.zeros((32, 32, 3), dtype=torch.float32, device="cuda"), 1, sd.depth,
+                               counters=torch.zeros(4, dtype=torch.int64, device="cuda"))
