@@ -33,6 +33,12 @@ CU_ETA = [0.27, 0.98, 1.16]
 CU_K = [3.41, 2.58, 2.40]
 AU_ETA = [0.17, 0.42, 1.37]
 AU_K = [3.57, 2.39, 1.79]
+# Scalar-IOR versions (the mean eta of the three channels with the per-channel
+# k): the reference's conductors take one intIOR / extIOR for every channel
+# (src/bsdf/RoughConductorBSDF.cpp:43), so scenes that the reference renderer
+# must read use these.
+CU_IOR = 0.80
+AU_IOR = 0.65
 
 
 def look_at(origin, target, up) -> np.ndarray:
@@ -389,8 +395,8 @@ def mesh_heavy(material: str = "conductor", width: int = 1024, height: int = 102
     0.1), 'plastic' (alpha 0.15)."""
     sd = SceneDesc()
     if material == "conductor":
-        b = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=1.0, ext_ior=1.0,
-                     eta=CU_ETA, k=CU_K)
+        b = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=CU_IOR,
+                     ext_ior=1.0, k=CU_K)
     elif material == "dielectric":
         b = BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=0.1, alpha_v=0.1, int_ior=1.5, ext_ior=1.0)
     elif material == "plastic":
@@ -421,14 +427,13 @@ def random_material(rng, kind: Optional[str] = None) -> BSDFDesc:
     if kind in ("ggx_conductor", "beckmann_conductor"):
         cu = rng.random() < 0.5
         return BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX if kind == "ggx_conductor" else BECKMANN,
-                        alpha_u=a, alpha_v=a, int_ior=1.0, ext_ior=1.0, eta=CU_ETA if cu else AU_ETA,
-                        k=CU_K if cu else AU_K)
+                        alpha_u=a, alpha_v=a, int_ior=CU_IOR if cu else AU_IOR, ext_ior=1.0, k=CU_K if cu else AU_K)
     if kind == "dielectric":
         return BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=a, alpha_v=a, int_ior=1.5, ext_ior=1.0)
     if kind == "plastic":
         return BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=a, alpha_v=a, kd=col)
-    nested = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=a, alpha_v=a, int_ior=1.0, ext_ior=1.0,
-                      eta=AU_ETA, k=AU_K)
+    nested = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=a, alpha_v=a, int_ior=AU_IOR, ext_ior=1.0,
+                      k=AU_K)
     return BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2, nested=nested)
 
 

@@ -656,6 +656,11 @@ typedef struct { int n; float *func; float *cdf; float integral; } pdf1d;
 typedef struct { float bmin[3], bmax[3]; int32_t left_or_first, count, axis, right; } bnode;
 
 struct ho_scene {
+    /* 1: Sampler::Next2D returns (second draw, first draw), the order the
+     * reference's Point2f(nextFloat(), nextFloat()) takes when its arguments
+     * are evaluated right to left (GCC; the order is unspecified in C++).
+     * 0 (default): (first, second), the order the CUDA kernels use. */
+    int swap2d;
     int nb, cap_b; bsdf_t *bsdfs;
     int ntex, cap_tex; ho_texture_desc *tex; struct mip_t **mips;
     int ray_diff;                      /* a bitmap texture filters with the camera ray's differentials */
@@ -2448,6 +2453,7 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
             if (s->emit_mesh[e] < 0) er.dist = radius;
             float u1 = ho_pcg32_nextf(rng);
             float ux = ho_pcg32_nextf(rng), uy = ho_pcg32_nextf(rng);
+            if (s->swap2d) { float t_ = ux; ux = uy; uy = t_; }
             v3 ld = emitter_sample_any(s, e, &er, ux, uy, u1);
             float pl = er.pdf;
             if (!is_zero(ld)) {
@@ -2475,6 +2481,7 @@ static v3 li_pathmis(const ho_scene *s, int depth_max, ho_pcg32 *rng, v3 ro, v3 
         br.it = &it;
         br.wi = to_local(&it.sh, scl(rdir, -1.0f)); br.measure = HO_MEASURE_UNKNOWN;
         float sx = ho_pcg32_nextf(rng), sy = ho_pcg32_nextf(rng);
+        if (s->swap2d) { float t_ = sx; sx = sy; sy = t_; }
         v3 F = bsdf_sample(s, bsdf, &br, sx, sy, rng, NULL);
         ro = it.p; rdir = to_world(&it.sh, br.wo);
         beta = mul(beta, F);
@@ -2511,16 +2518,31 @@ static int film_put(const ho_scene *s, double *film, float px, float py, v3 val)
     float wx[16], wy[16];
     for (int x = x0, i = 0; x <= x1; ++x) wx[i++] = s->ftab[(int)(fabsf((float)x - cx) * s->lookup)];
     for (int y = y0, i = 0; y <= y1; ++y) wy[i++] = s->ftab[(int)(fabsf((float)y - cy) * s->lookup)];
+    /* Color4f(Value) * WeightX * WeightY: each channel (v * wx) * wy in float,
+     * the weight channel (1 * wx) * wy (Block.cpp:129-132) */
     for (int y = y0, yr = 0; y <= y1; ++y, ++yr)
         for (int x = x0, xr = 0; x <= x1; ++x, ++xr) {
-            float w = wx[xr] * wy[yr];
             double *p = film + 4ull * ((uint64_t)y * FW + x);
-            p[0] += (double)(val.x * w); p[1] += (double)(val.y * w); p[2] += (double)(val.z * w); p[3] += (double)w;
+            p[0] += (double)((val.x * wx[xr]) * wy[yr]);
+            p[1] += (double)((val.y * wx[xr]) * wy[yr]);
+            p[2] += (double)((val.z * wx[xr]) * wy[yr]);
+            p[3] += (double)(wx[xr] * wy[yr]);
         }
     return 0;
 }
 
+int64_t ho_film_put_samples(const ho_scene *s, uint64_t n, const float *pos, const float *val, double *film) {
+    int64_t dropped = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        v3 c = {val[3 * i], val[3 * i + 1], val[3 * i + 2]};
+        dropped += film_put(s, film, pos[2 * i], pos[2 * i + 1], c);
+    }
+    return dropped;
+}
+
 /* Render / RenderBlock  src/Main.cpp:11-44, 46-147 */
+void ho_scene_set_reference_draw_order(ho_scene *s, int swap2d) { s->swap2d = swap2d != 0; }
+
 int64_t ho_render(const ho_scene *s, int depth, int spp, const int32_t *blist, int nblk, double *film, int nthreads,
                   uint64_t *counters) {
     int BS = 32;
@@ -2548,6 +2570,7 @@ int64_t ho_render(const ho_scene *s, int depth, int spp, const int32_t *blist, i
                 for (int x = 0; x < sx; ++x)
                     for (int i = 0; i < spp; ++i) {
                         float jx = ho_pcg32_nextf(&rng), jy = ho_pcg32_nextf(&rng);
+                        if (s->swap2d) { float t_ = jx; jx = jy; jy = t_; }
                         float px = (float)(x + ox) + jx, py = (float)(y + oy) + jy;
                         (void)ho_pcg32_nextf(&rng); (void)ho_pcg32_nextf(&rng);   /* aperture sample */
                         v3 o, d; float mn, mx;
@@ -2598,6 +2621,7 @@ void ho_ttest_scene(const ho_scene *s, int depth, int n, double *mean, double *v
     ctr_t c = {0, 0};
     for (int k = 0; k < n; k++) {
         float a = ho_pcg32_nextf(&rng), b = ho_pcg32_nextf(&rng);
+        if (s->swap2d) { float t_ = a; a = b; b = t_; }
         float px = a * (float)s->W, py = b * (float)s->H;
         (void)ho_pcg32_nextf(&rng); (void)ho_pcg32_nextf(&rng);
         v3 o, d; float mn, mx;

@@ -178,6 +178,12 @@ void ho_trace(const ho_scene *s, uint64_t n, const float *rays, float *thit, flo
  * (H+2B)*(W+2B)*4 doubles where B = ceil(radius-0.5).  If block_list is
  * non-NULL only those block indices (row-major over the block grid) render.
  * depth: the integrator's "depth".  Returns number of dropped samples. */
+/* swap2d != 0: every two-dimensional draw (pixel jitter, emitter and BSDF
+ * sample pairs) takes (second, first) uniform, as the reference's Next2D does
+ * when built with right-to-left argument evaluation (GCC); default (first,
+ * second), the CUDA kernels' order.  Only path-level comparisons against the
+ * compiled reference need it. */
+void ho_scene_set_reference_draw_order(ho_scene *s, int swap2d);
 int64_t ho_render(const ho_scene *s, int depth, int spp, const int32_t *block_list, int nblocks,
                   double *film_rgbw, int nthreads, uint64_t *counters /* 4: paths, rays, shadow, 0 */);
 /* Per-pixel per-sample statistics: sample 'spp' paths per pixel of the listed
@@ -191,6 +197,10 @@ void ho_ttest_scene(const ho_scene *s, int depth, int n, double *mean, double *v
 /* Resolve the bordered film to an H*W*3 float image (Block.cpp:61). */
 void ho_film_resolve(const ho_scene *s, const double *film_rgbw, float *out_rgb);
 int  ho_film_border(const ho_scene *s);
+/* ImageBlock::Put (src/core/Block.cpp:95-134) of n samples (film positions
+ * n x 2, values n x 3) into a bordered film of doubles; returns the number
+ * dropped as invalid. */
+int64_t ho_film_put_samples(const ho_scene *s, uint64_t n, const float *pos, const float *val, double *film);
 
 /* --- emitter / camera / filter record queries -------------------------- */
 void  ho_emitter_sample(const ho_scene *s, int e, const float *ref, float ux, float uy, float u1, float *out14);

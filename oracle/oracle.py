@@ -109,6 +109,9 @@ def lib():
         L.ho_trace.argtypes = [P, C.c_uint64, P, P, P, P, P, C.c_int, C.c_int, C.c_int]
         L.ho_render.argtypes = [P, C.c_int, C.c_int, P, C.c_int, P, C.c_int, P]
         L.ho_render.restype = C.c_int64
+        L.ho_scene_set_reference_draw_order.argtypes = [P, C.c_int]
+        L.ho_film_put_samples.argtypes = [P, C.c_uint64, P, P, P]
+        L.ho_film_put_samples.restype = C.c_int64
         L.ho_pixel_stats.argtypes = [P, C.c_int, C.c_int, C.c_uint64, C.c_int, P, P, C.c_int]
         L.ho_ttest_scene.argtypes = [P, C.c_int, C.c_int, P, P]
         L.ho_film_resolve.argtypes = [P, P, P]
@@ -351,6 +354,11 @@ class OracleScene:
         lib().ho_trace(self.h, n, _p(rays), _p(t), _p(u), _p(v), _p(tri), int(any_hit), int(use_bvh), nthreads)
         return tri, t, u, v
 
+    def set_reference_draw_order(self, on: bool = True):
+        """Two-dimensional draws as the compiled reference's Next2D takes them
+        (second uniform first); for path-level comparisons with the reference."""
+        lib().ho_scene_set_reference_draw_order(self.h, int(on))
+
     def render(self, spp, depth=None, blocks=None, nthreads=0):
         L = lib()
         B = L.ho_film_border(self.h)
@@ -361,6 +369,15 @@ class OracleScene:
         dropped = L.ho_render(self.h, depth or self.desc.depth, spp, _p(bl), 0 if bl is None else len(bl),
                               _p(film), nthreads, _p(ctr))
         return film, int(dropped), ctr
+
+    def film_put(self, pos, val):
+        """ImageBlock::Put of samples into an empty bordered film (double)."""
+        B = lib().ho_film_border(self.h)
+        W, H = self.desc.camera.width, self.desc.camera.height
+        film = np.zeros((H + 2 * B, W + 2 * B, 4), np.float64)
+        pos, val = _f32(pos), _f32(val)
+        dropped = lib().ho_film_put_samples(self.h, pos.shape[0], _p(pos), _p(val), _p(film))
+        return film, int(dropped)
 
     def resolve(self, film):
         W, H = self.desc.camera.width, self.desc.camera.height

@@ -1,13 +1,23 @@
-"""Build oracle/_ref/libhikari_ref_bsdf.so: the reference's own BSDF and
-point / directional / constant emitter classes compiled from the reference
-sources where they lie, for record-wise parity tests of the oracle
-restatement.
+"""Build oracle/_ref/libhikari_ref.so: the reference renderer's own sources
+compiled where they lie, for the parity tests of the oracle restatement and
+as the timed CPU baseline (the reference's own pathMIS renderer).
+
+Every file of src/ is compiled except three:
+  * src/Main.cpp and src/core/Screen.cpp (the OpenGL preview window and the
+    program's main): oracle/ref_shim/ref_render.cpp is the headless driver
+    that runs Render's block loop (src/Main.cpp:46-147) without the window;
+  * src/core/Bitmap.cpp (OpenEXR I/O through the OpenEXR library, which needs
+    its own CMake build): oracle/ref_shim/ref_bitmap.cpp implements the same
+    Bitmap members over a small uncompressed-EXR codec.
+ext/pugixml/src/pugixml.cpp (the parser's XML library) is compiled from its
+source too.
 
 Recipe (no reference build system is run):
-  * a shim include tree (oracle/_ref/shim) of symlinks named like the
-    reference's backslash include paths ("core\\Common.hpp" -> include/core/
+  * a shim include tree (oracle/_ref/shim) of forwarding headers named like
+    the reference's backslash include paths ("core\\Common.hpp" -> include/core/
     Common.hpp, "Eigen\\Lu" -> ext/eigen/Eigen/LU), plus oracle/ref_shim/ for
-    glog, <windows.h> and a serial stand-in for the TBB loops of MipMap;
+    glog, <windows.h> and a stand-in for the TBB pieces used (blocked_range,
+    parallel_for on the calling thread, mutex);
   * -DWIN32 selects the reference's Windows branches (its non-Windows branch
     of Signum has a bare #elif that GCC rejects); oracle/ref_shim/prelude.h
     supplies the MSVC CRT helpers they use;
@@ -19,6 +29,7 @@ Recipe (no reference build system is run):
 
 usage: python oracle/ref_build.py [reference-root]   (needs the reference checkout)
 """
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -26,17 +37,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-LIB = os.path.join(OUT, "libhikari_ref_bsdf.so")
-
-CORE = ["Object", "PropertyList", "BSDF", "Texture", "MicrofacetDistribution", "RoughTransmitance", "Frame",
-        "Sampling", "Color", "Vector", "Transform", "Sampler", "Intersection", "Timer", "MemoryArena", "Shape",
-        "Mesh", "Emitter", "DiscretePDF", "BoundingBox", "Ray", "MipMap", "Camera", "ReconstructionFilter"]
-BSDFS = ["DiffuseBSDF", "RoughConductorBSDF", "RoughDielectricBSDF", "RoughPlasticBSDF", "RoughCoatingBSDF",
-         "MirrorBSDF", "ConductorBSDF", "DielectricBSDF", "PlasticBSDF", "TwoSidedBSDF", "CoatingBSDF",
-         "RoughDiffuseBSDF", "BumpMapBSDF", "NormalMapBSDF"]
-EMITTERS = ["PointLight", "DirectionalLight", "ConstantLight"]
-TEXTURES = ["CheckerboardTexture", "GridTexture", "ScaleTexture", "BitmapTexture"]
-OTHERS = [("camera", "PerspectiveCamera"), ("filter", "GaussianFilter")]
+LIB = os.path.join(OUT, "libhikari_ref.so")
+SHIM_SOURCES = ["ref_bridge.cpp", "ref_bitmap.cpp", "ref_render.cpp"]
+SKIP = {"Main.cpp", "Screen.cpp", "Bitmap.cpp"}
 
 
 def _link(src, dst):
@@ -48,13 +51,22 @@ def _link(src, dst):
 def _forward(src, dst):
     """One-line forwarding header, so that quoted includes inside src resolve
     relative to its real directory."""
+    text = f'#include "{src}"\n'
+    if os.path.exists(dst) and not os.path.islink(dst):
+        with open(dst) as f:
+            if f.read() == text:
+                return
     if os.path.lexists(dst):
         os.remove(dst)
     with open(dst, "w") as f:
-        f.write(f'#include "{src}"\n')
+        f.write(text)
 
 
-def build(ref: str = "/root/reference") -> str:
+def _newer(obj, *deps):
+    return not os.path.exists(obj) or any(os.path.getmtime(d) > os.path.getmtime(obj) for d in deps)
+
+
+def build(ref: str = "/root/reference", jobs: int = 0) -> str:
     if not os.path.isdir(ref):
         raise FileNotFoundError(f"reference checkout not found at {ref}")
     shim = os.path.join(OUT, "shim")
@@ -71,6 +83,7 @@ def build(ref: str = "/root/reference") -> str:
         _forward(os.path.join(ref, "ext", "eigen", "Eigen", real), os.path.join(shim, f"Eigen\\{name}"))
     _forward(os.path.join(HERE, "ref_shim", "glog_logging.h"), os.path.join(shim, "glog\\logging.h"))
     _forward(os.path.join(HERE, "ref_shim", "tbb_serial.h"), os.path.join(shim, "tbb\\tbb.h"))
+    _forward(os.path.join(HERE, "ref_shim", "tbb_serial.h"), os.path.join(shim, "tbb\\mutex.h"))
     _forward(os.path.join(ref, "ext", "filesystem", "filesystem", "resolver.h"), os.path.join(shim, "filesystem\\resolver.h"))
     data = os.path.join(os.path.dirname(HERE), "hikari_b200", "data")   # identical copies of ref data/
     for f in ("BeckmannRFTData.bin", "GGXRFTData.bin"):
@@ -81,25 +94,36 @@ def build(ref: str = "/root/reference") -> str:
              "-I", os.path.join(ref, "ext", "eigen"), "-I", os.path.join(ref, "ext", "tinyformat"),
              "-I", os.path.join(ref, "ext", "pcg32"), "-I", os.path.join(ref, "ext", "filesystem"),
              "-I", os.path.join(ref, "ext", "stb"), "-I", os.path.join(ref, "ext", "openexr", "IlmBase", "Imath"),
-             "-I", os.path.join(ref, "ext", "hypothesis")]
-    objs = []
-    srcs = [os.path.join(ref, "src", "core", c + ".cpp") for c in CORE] + \
-           [os.path.join(ref, "src", "bsdf", b + ".cpp") for b in BSDFS] + \
-           [os.path.join(ref, "src", "emitter", e + ".cpp") for e in EMITTERS] + \
-           [os.path.join(ref, "src", "texture", t + ".cpp") for t in TEXTURES] + \
-           [os.path.join(ref, "src", d, f + ".cpp") for d, f in OTHERS] + \
-           [os.path.join(HERE, "ref_shim", "ref_bridge.cpp")]
-    for s in srcs:
-        o = os.path.join(objd, os.path.basename(s) + ".o")
-        subprocess.check_call(flags + ["-c", s, "-o", o])
-        objs.append(o)
+             "-I", os.path.join(ref, "ext", "hypothesis"), "-I", os.path.join(ref, "ext", "pugixml", "src")]
+    shim_hdrs = [os.path.join(HERE, "ref_shim", h) for h in ("prelude.h", "tbb_serial.h", "glog_logging.h")]
+    srcs = sorted(p for p in glob.glob(os.path.join(ref, "src", "**", "*.cpp"), recursive=True)
+                  if os.path.basename(p) not in SKIP)
+    srcs += [os.path.join(ref, "ext", "pugixml", "src", "pugixml.cpp")]
+    srcs += [os.path.join(HERE, "ref_shim", s) for s in SHIM_SOURCES]
     common = os.path.join(ref, "src", "core", "Common.cpp")
-    o = os.path.join(objd, "Common.cpp.o")
-    sed = subprocess.run(["sed", "s/unsigned int(strtoul/(unsigned int)(strtoul/", common], check=True,
-                         capture_output=True)
-    subprocess.run(flags + ["-x", "c++", "-c", "-", "-o", o], input=sed.stdout, check=True)
-    objs.append(o)
-    subprocess.check_call(["g++", "-shared", "-o", LIB] + objs + ["-lpthread"])
+    tasks, objs = [], []
+    for s in srcs:
+        o = os.path.join(objd, os.path.relpath(s, ref if s.startswith(ref) else HERE).replace(os.sep, "_") + ".o")
+        objs.append(o)
+        if not _newer(o, s, *shim_hdrs):
+            continue
+        if s == common:
+            sed = subprocess.run(["sed", "s/unsigned int(strtoul/(unsigned int)(strtoul/", common], check=True,
+                                 capture_output=True)
+            tasks.append((flags + ["-x", "c++", "-c", "-", "-o", o], sed.stdout))
+        else:
+            tasks.append((flags + ["-c", s, "-o", o], None))
+
+    def run(t):
+        subprocess.run(t[0], input=t[1], check=True)
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
+        for f in [ex.submit(run, t) for t in tasks]:
+            f.result()
+    if tasks or not os.path.exists(LIB):
+        tmp = LIB + ".tmp"
+        subprocess.check_call(["g++", "-shared", "-o", tmp] + objs + ["-lpthread"])
+        os.replace(tmp, LIB)
     return LIB
 
 

@@ -14,7 +14,12 @@
 #include <core\Texture.hpp>
 #include <core\Camera.hpp>
 #include <core\Transform.hpp>
+#include <core\Acceleration.hpp>
+#include <core\ReconstructionFilter.hpp>
+#include <core\Block.hpp>
 #include <stb_image.h>
+
+#include <vector>
 
 using namespace Hikari;
 
@@ -149,6 +154,8 @@ public:
         m_F.resize(3, nt);
         for (uint32_t i = 0; i < nt; i++)
             for (int c = 0; c < 3; c++) m_F(c, i) = F[3 * i + c];
+        /* the mesh box over every vertex, as WavefrontObjMesh computes it */
+        for (uint32_t i = 0; i < nv; i++) m_BBox.ExpandBy(Point3f(m_V.col(i)));
     }
     uint32_t *facet(uint32_t i) { return m_F.data() + 3 * i; }
 };
@@ -397,5 +404,156 @@ void hr_bsdf_batch(void *h, uint64_t n, const float *wi, const float *u2, const 
         hr_bsdf_eval(h, wi + 3 * i, wo + 3 * i, 1, e_rgb + 3 * i);
         p_pdf[i] = hr_bsdf_pdf(h, wi + 3 * i, wo + 3 * i, 1);
     }
+}
+
+/* ---- acceleration structures (src/core/Acceleration.cpp, src/acceleration/*.cpp) ---- */
+namespace {
+struct RefAccel {
+    Acceleration *accel = nullptr;
+    std::vector<Mesh *> meshes;
+    std::vector<uint32_t> base;   /* global index of each mesh's first triangle */
+};
+}
+
+/* kind 0 "bruto" (the reference's brute-force loop), 1 "bvh", 2 "hlbvh" over
+ * the meshes (hr_mesh_create handles, in order); triangle ids are global in
+ * that order. */
+void *hr_accel_create(int kind, int leaf_size, void *const *meshes, int n) {
+    static const char *names[] = {"bruto", "bvh", "hlbvh"};
+    try {
+        PropertyList pl;
+        if (kind > 0) pl.SetInteger("leafSize", leaf_size);
+        RefAccel *r = new RefAccel;
+        r->accel = (Acceleration *)ObjectFactory::CreateInstance(names[kind], pl);
+        uint32_t b = 0;
+        for (int i = 0; i < n; i++) {
+            Mesh *m = (Mesh *)meshes[i];
+            r->meshes.push_back(m);
+            r->base.push_back(b);
+            b += m->GetTriangleCount();
+            r->accel->AddMesh(m);
+        }
+        r->accel->Build();
+        return r;
+    } catch (const std::exception &e) {
+        fprintf(stderr, "hr_accel_create: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+/* Acceleration::RayIntersect for n rays of 8 floats (o, d, minT, maxT).
+ * any_hit: tri[i] = 1 / 0.  Otherwise tri[i] = global triangle id or -1 and
+ * t, u, v of the hit; u, v are the barycentrics Mesh::RayIntersect returns for
+ * the hit triangle (PostIntersect replaces Isect.UV by texture coordinates). */
+void hr_accel_trace(void *h, uint64_t n, const float *rays, int any_hit, int32_t *tri, float *t, float *u, float *v) {
+    RefAccel *r = (RefAccel *)h;
+    for (uint64_t i = 0; i < n; i++) {
+        const float *q = rays + 8 * i;
+        Ray3f R(Point3f(q[0], q[1], q[2]), Vector3f(q[3], q[4], q[5]), q[6], q[7]);
+        Intersection I;
+        const bool f = r->accel->RayIntersect(R, I, any_hit != 0);
+        if (any_hit) { tri[i] = f ? 1 : 0; continue; }
+        if (!f) { tri[i] = -1; t[i] = u[i] = v[i] = 0.0f; continue; }
+        const Mesh *m = I.pShape->GetMesh();
+        const uint32_t facet = I.pShape->GetFacetIndex();
+        size_t k = 0;
+        while (k < r->meshes.size() && r->meshes[k] != m) k++;
+        tri[i] = (int32_t)(r->base[k] + facet);
+        float U = 0.0f, V = 0.0f, T = 0.0f;
+        m->RayIntersect(facet, R, U, V, T);
+        t[i] = I.T; u[i] = U; v[i] = V;
+    }
+}
+
+void hr_accel_free(void *h) {
+    RefAccel *r = (RefAccel *)h;
+    delete r->accel;
+    delete r;
+}
+
+/* ---- EnvironmentLight (src/emitter/EnvironmentLight.cpp) ---- */
+/* The "env" emitter of an EXR file (read through the oracle's Bitmap
+ * stand-in), toWorld a row-major 4x4.  Sample / Eval / Pdf go through
+ * hr_emitter_sample and hr_emitter_eval_dir. */
+void *hr_env_create(const char *exr_path, const float *to_world16, float scale) {
+    try {
+        PropertyList pl;
+        pl.SetString("filename", exr_path);
+        Eigen::Matrix4f M;
+        for (int r = 0; r < 4; r++)
+            for (int c = 0; c < 4; c++) M(r, c) = to_world16[4 * r + c];
+        pl.SetTransform("toWorld", Transform(M));
+        pl.SetFloat("scale", scale);
+        Emitter *e = (Emitter *)ObjectFactory::CreateInstance("env", pl);
+        e->Activate();
+        return e;
+    } catch (const std::exception &ex) {
+        fprintf(stderr, "hr_env_create: %s\n", ex.what());
+        return nullptr;
+    }
+}
+
+void hr_object_free(void *o) { delete (Object *)o; }
+
+/* ---- reconstruction filters and ImageBlock::Put (src/filter/*.cpp, src/core/Block.cpp) ---- */
+/* kind 0 box, 1 tent, 2 gaussian (radius, stddev = p0), 3 mitchell (radius, B = p0, C = p1) */
+void *hr_filter_create(int kind, float radius, float p0, float p1) {
+    static const char *names[] = {"box", "tent", "gaussian", "mitchell"};
+    try {
+        PropertyList pl;
+        if (kind == 2) { pl.SetFloat("radius", radius); pl.SetFloat("stddev", p0); }
+        if (kind == 3) { pl.SetFloat("radius", radius); pl.SetFloat("B", p0); pl.SetFloat("C", p1); }
+        Object *f = ObjectFactory::CreateInstance(names[kind], pl);
+        f->Activate();
+        return f;
+    } catch (const std::exception &e) {
+        fprintf(stderr, "hr_filter_create: %s\n", e.what());
+        return nullptr;
+    }
+}
+
+/* ReconstructionFilter::Eval at n offsets; returns the filter radius */
+float hr_filter_eval(void *f, uint64_t n, const float *x, float *out) {
+    const ReconstructionFilter *F = (const ReconstructionFilter *)f;
+    for (uint64_t i = 0; i < n; i++) out[i] = F->Eval(x[i]);
+    return F->GetRadius();
+}
+
+/* ImageBlock(W x H, filter) with offset (0, 0): Clear, then Put every sample
+ * (pos n x 2 film coordinates, val n x 3) in order; film_rgbw receives the
+ * (H+2B) x (W+2B) x 4 result.  Returns the border B. */
+int hr_block_put(void *f, int W, int H, uint64_t n, const float *pos, const float *val, float *film_rgbw) {
+    ImageBlock B(Vector2i(W, H), (const ReconstructionFilter *)f);
+    B.Clear();
+    for (uint64_t i = 0; i < n; i++)
+        B.Put(Point2f(pos[2 * i], pos[2 * i + 1]), Color3f(val[3 * i], val[3 * i + 1], val[3 * i + 2]));
+    if (film_rgbw) {
+        const int rows = (int)B.rows(), cols = (int)B.cols();
+        for (int y = 0; y < rows; y++)
+            for (int x = 0; x < cols; x++)
+                for (int c = 0; c < 4; c++) film_rgbw[4 * ((size_t)y * cols + x) + c] = B.coeff(y, x)(c);
+    }
+    return B.GetBorderSize();
+}
+}
+
+extern "C" {
+/* The reference IndependentSampler prepared for a block at (ox, oy): n calls
+ * of Next2D (out 2n floats), then n of Next1D (out n floats) -- shows the
+ * order in which this build's Next2D consumes its two draws (the argument
+ * evaluation order of Point2f(nextFloat(), nextFloat()) is unspecified in C++). */
+void hr_sampler_draws(int ox, int oy, int n, float *out2d, float *out1d) {
+    PropertyList pl;
+    pl.SetInteger("sampleCount", 1);
+    std::unique_ptr<Sampler> S((Sampler *)ObjectFactory::CreateInstance("independent", pl));
+    ImageBlock B(Vector2i(1, 1), nullptr);
+    B.SetOffset(Point2i(ox, oy));
+    S->Prepare(B);
+    for (int i = 0; i < n; i++) {
+        Point2f p = S->Next2D();
+        out2d[2 * i] = p.x();
+        out2d[2 * i + 1] = p.y();
+    }
+    for (int i = 0; i < n; i++) out1d[i] = S->Next1D();
 }
 }

@@ -15,16 +15,18 @@ from hikari_b200.scenedesc import (BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_
                                    SceneDesc, TextureDesc)
 from oracle import oracle as O
 
-REF_LIB = os.path.join(os.path.dirname(O.HERE), "oracle", "_ref", "libhikari_ref_bsdf.so")
+from oracle import ref_build  # noqa: E402
+
+REF_LIB = ref_build.LIB
 
 
 def _ref_lib():
-    if not os.path.exists(REF_LIB):
-        try:
-            from oracle import ref_build
-            ref_build.build()
-        except Exception as e:  # reference checkout absent (e.g. on the GPU box)
-            pytest.skip(f"reference BSDF library unavailable: {e}")
+    try:
+        ref_build.build()   # incremental; needs the reference checkout
+    except FileNotFoundError:
+        pass
+    if not os.path.exists(REF_LIB):   # no checkout and nothing prebuilt
+        pytest.skip("reference library unavailable")
     R = C.CDLL(REF_LIB)
     R.hr_init.argtypes = [C.c_char_p]
     R.hr_bsdf_create.restype = C.c_void_p
