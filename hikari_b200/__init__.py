@@ -22,6 +22,8 @@ DATA_DIR = os.path.join(HERE, "data")
 
 HK_OK = 0
 ACCEL_BVH2, ACCEL_BVH8 = 0, 1
+# forms of Scene.render_image (HK_FORM_*)
+FORM_AUTO, FORM_MEGAKERNEL, FORM_WAVEFRONT = 0, 1, 2
 
 
 class HikariError(RuntimeError):
@@ -141,6 +143,8 @@ def lib():
         "hk_scene_set_background": ([P, P, C.c_int], C.c_int),
         "hk_scene_build": ([P], C.c_int),
         "hk_scene_set_accel": ([P, I32], C.c_int),
+        "hk_scene_set_image_form": ([P, I32], C.c_int),
+        "hk_scene_set_wavefront_config": ([P, C.POINTER(WavefrontConfig)], C.c_int),
         "hk_bvh_check": ([P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
                          C.c_int),
         "hk_scene_get_info": ([P, C.POINTER(SceneInfo)], C.c_int),
@@ -372,6 +376,23 @@ class Scene:
     @property
     def width(self):
         return self.desc.camera.width if self.desc else None
+
+    def set_image_form(self, form: int) -> None:
+        """The form render_image renders with: FORM_AUTO (the wavefront for
+        images of at least 256 x 256 pixels and 2^22 paths), FORM_MEGAKERNEL
+        or FORM_WAVEFRONT."""
+        check(lib().hk_scene_set_image_form(self.h, form))
+
+    def set_wavefront_config(self, cfg: Optional[dict]) -> None:
+        """The wavefront configuration of render_image's wavefront calls (a dict
+        as autotune returns; None: the defaults).  autotune sets it too."""
+        if cfg is None:
+            check(lib().hk_scene_set_wavefront_config(self.h, None))
+            return
+        c = WavefrontConfig(cfg.get("capacity", 0), cfg.get("threads_extend", 0), cfg.get("threads_shade", 0),
+                            cfg.get("iterations_per_check", 0), 0, None, None, cfg.get("fetch_steps", 0),
+                            cfg.get("fetch_min_idle", 0))
+        check(lib().hk_scene_set_wavefront_config(self.h, C.byref(c)))
 
     def set_accel(self, accel: int) -> None:
         """Traverse the binary tree (ACCEL_BVH2) or the compressed 8-wide tree (ACCEL_BVH8)."""

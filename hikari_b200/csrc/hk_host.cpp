@@ -237,6 +237,9 @@ struct hk_scene {
     int margin_lo = 0, margin_hi = 0;
     int sm_count = 148;
     int device = 0;   // CUDA device the scene was built on
+    int image_form = HK_FORM_AUTO;             // form hk_render_image renders with
+    bool has_wf_cfg = false;                   // wf_cfg was set (autotuner or caller)
+    hk_wavefront_config wf_cfg{};              // wavefront configuration of hk_render_image
     int occupancy = 1;        // resident megakernel CTAs per SM for the traversed tree
     int occupancy_of[2] = {1, 1};
     std::unique_ptr<hk::WfEngine> wf;   // wavefront engine (allocated on first use)
@@ -1175,25 +1178,80 @@ int hk_film_resolve(hk_scene *s, const float *film, float *rgb, void *stream) {
         return HK_OK;
     });
 }
+// Whether hk_render_image renders this call with the wavefront: always for
+// HK_FORM_WAVEFRONT; for HK_FORM_AUTO once the image has at least 256 x 256
+// pixels and 2^22 paths (below that a pool of path slots cannot fill the GPU
+// better than the megakernel's persistent tiles).
+static bool image_uses_wavefront(const hk_scene *s, const hk_render_desc &d) {
+    if (s->image_form == HK_FORM_WAVEFRONT) return true;
+    if (s->image_form == HK_FORM_MEGAKERNEL) return false;
+    const uint64_t px = (uint64_t)s->width * s->height;
+    return px >= 65536 && px * (uint64_t)std::max(d.spp, 0) >= (1ull << 22);
+}
 int hk_render_image(hk_scene *s, const hk_render_desc *d, float *rgb_host, unsigned long long *counters, void *stream) {
     return guarded([&] {
         require_built(s);
-        if (!rgb_host) throw HkError{HK_ERR_INVALID, "null output"};
+        if (!d || !rgb_host) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (d->spp <= 0 || d->depth < 0) throw HkError{HK_ERR_INVALID, "spp must be > 0 and depth >= 0"};
+        require_scene_size(s, *d);
         cudaStream_t st = (cudaStream_t)stream;
         size_t FW = s->width + 2 * s->dev.border, FH = s->height + 2 * s->dev.border;
         size_t film_bytes = FW * FH * 4 * sizeof(float), rgb_bytes = (size_t)s->width * s->height * 3 * sizeof(float);
         if (s->b_film.bytes < film_bytes) s->b_film.alloc(film_bytes);
         if (s->b_rgb.bytes < rgb_bytes) s->b_rgb.alloc(rgb_bytes);
+        // counters: [1..5] the megakernel's, [8..14] the wavefront's 7
         unsigned long long *ctr = (unsigned long long *)s->b_scratch.p + 1;
+        unsigned long long *ctr7 = (unsigned long long *)s->b_scratch.p + 8;
         HK_CUDA(cudaMemsetAsync(s->b_film.p, 0, film_bytes, st));
-        HK_CUDA(cudaMemsetAsync(ctr, 0, 5 * sizeof(unsigned long long), st));
-        int rc = hk_render(s, d, s->b_film.as<float>(), ctr, stream);
+        const bool wave = image_uses_wavefront(s, *d);
+        int rc;
+        if (wave) {
+            HK_CUDA(cudaMemsetAsync(ctr7, 0, 7 * sizeof(unsigned long long), st));
+            hk_render_job job;
+            job.film_dev = s->b_film.as<float>();
+            job.desc = *d;
+            job.desc.width = job.desc.height = 0;
+            rc = hk_render_batch(s, &job, 1, s->has_wf_cfg ? &s->wf_cfg : nullptr, ctr7, stream);
+        } else {
+            HK_CUDA(cudaMemsetAsync(ctr, 0, 5 * sizeof(unsigned long long), st));
+            rc = hk_render(s, d, s->b_film.as<float>(), ctr, stream);
+        }
         if (rc != HK_OK) return rc;
         HK_CUDA(hk::launch_resolve(s->b_film.as<float>(), s->b_rgb.as<float>(), (int)s->width, (int)s->height,
                                    s->dev.border, st));
         HK_CUDA(cudaMemcpyAsync(rgb_host, s->b_rgb.p, rgb_bytes, cudaMemcpyDeviceToHost, st));
-        if (counters) HK_CUDA(cudaMemcpyAsync(counters, ctr, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        unsigned long long c7[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (counters) {
+            if (wave) HK_CUDA(cudaMemcpyAsync(c7, ctr7, sizeof c7, cudaMemcpyDeviceToHost, st));
+            else HK_CUDA(cudaMemcpyAsync(counters, ctr, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+        }
         HK_CUDA(cudaStreamSynchronize(st));
+        if (counters && wave) {   // the megakernel's five: traversal totals over both ray kinds
+            counters[0] = c7[0];
+            counters[1] = c7[1];
+            counters[2] = c7[2];
+            counters[3] = c7[3] + c7[5];
+            counters[4] = c7[4] + c7[6];
+        }
+        return HK_OK;
+    });
+}
+int hk_scene_set_image_form(hk_scene *s, int32_t form) {
+    return guarded([&] {
+        if (!s || form < HK_FORM_AUTO || form > HK_FORM_WAVEFRONT) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        s->image_form = form;
+        return HK_OK;
+    });
+}
+int hk_scene_set_wavefront_config(hk_scene *s, const hk_wavefront_config *cfg) {
+    return guarded([&] {
+        if (!s) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        s->has_wf_cfg = cfg != nullptr;
+        if (cfg) {
+            s->wf_cfg = *cfg;
+            s->wf_cfg.kernel_ms = nullptr;
+            s->wf_cfg.kernel_launches = nullptr;
+        }
         return HK_OK;
     });
 }
@@ -1436,6 +1494,8 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
         cudaEventDestroy(e1);
         *best = bc;
         if (best_ms) *best_ms = best_t;
+        s->wf_cfg = bc;   // hk_render_image renders its wavefront calls with it
+        s->has_wf_cfg = true;
         return HK_OK;
     });
 }

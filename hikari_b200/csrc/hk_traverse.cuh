@@ -2,11 +2,13 @@
 //
 // Nodes are 64-byte BVH2 records (both child boxes in one node, fetched with
 // four 128-bit read-only loads); triangles are pre-gathered 48-byte records
-// in leaf order.  The ray-triangle test is the watertight test of Woop,
-// Benthin and Wald (JCGT 2013), accepting both windings like the reference's
-// Moller-Trumbore (src/core/Mesh.cpp:340) and the reference's closest-hit
-// rule: a hit with t in [tmin, tmax] replaces the current one, tmax shrinks
-// to its t (src/acceleration/HLBVHAcceleration.cpp:229-240).
+// in leaf order.  Closest-hit rays test triangles with the watertight test
+// of Woop, Benthin and Wald (JCGT 2013), accepting both windings like the
+// reference's Moller-Trumbore (src/core/Mesh.cpp:340) and the reference's
+// closest-hit rule: a hit with t in [tmin, tmax] replaces the current one,
+// tmax shrinks to its t (src/acceleration/HLBVHAcceleration.cpp:229-240).
+// Any-hit (shadow) rays test with the reference's Moller-Trumbore itself, the
+// test its shadow query applies, and stop at the first triangle it accepts.
 #pragma once
 #include "hk_device.h"
 #include "hk_math.cuh"
@@ -105,6 +107,26 @@ __device__ __forceinline__ bool refine_mt(V3 o, V3 d, V3 p0, V3 p1, V3 p2, float
     u = uu;
     v = vv;
     return true;
+}
+
+// Any-hit test of a shadow ray: Mesh::RayIntersect (src/core/Mesh.cpp:340-384)
+// as the reference's shadow query runs it (HLBVHAcceleration::RayIntersect
+// returns on the first triangle it accepts), so the occlusion decision is the
+// reference's own.  No barycentrics or t leave the function.
+__device__ __forceinline__ bool occludes_mt(V3 o, V3 d, V3 p0, V3 p1, V3 p2, float tmin, float tmax) {
+    const V3 e1 = p1 - p0, e2 = p2 - p0;
+    const V3 pv = cross(d, e2);
+    const float det = dot(e1, pv);
+    if (det > -1e-8f && det < 1e-8f) return false;
+    const float inv = 1.0f / det;
+    const V3 tv = o - p0;
+    const float uu = dot(tv, pv) * inv;
+    if (uu < 0.0f || uu > 1.0f) return false;
+    const V3 qv = cross(tv, e1);
+    const float vv = dot(d, qv) * inv;
+    if (vv < 0.0f || uu + vv > 1.0f) return false;
+    const float tt = dot(e2, qv) * inv;
+    return tt >= tmin && tt <= tmax;
 }
 
 // Three-input min / max (PTX min.f32 / max.f32 with three sources, sm_100a).
@@ -206,12 +228,19 @@ struct Bvh2Walker {
             for (uint32_t i = 0; i < cnt; ++i) {
                 const float4 *tp = S.tris + 3 * (start + i);
                 const float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
-                float tt, uu, vv;
-                if (intersect_watertight(w, o, xyz(p0), xyz(p1), xyz(p2), tmin, tmax, tt, uu, vv)) {
-                    found = true;
-                    hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)(start + i);
-                    if (kAnyHit) return true;
-                    tmax = tt;
+                if constexpr (kAnyHit) {
+                    if (occludes_mt(o, d, xyz(p0), xyz(p1), xyz(p2), tmin, tmax)) {
+                        found = true;
+                        hit.tri = (int)(start + i);
+                        return true;
+                    }
+                } else {
+                    float tt, uu, vv;
+                    if (intersect_watertight(w, o, xyz(p0), xyz(p1), xyz(p2), tmin, tmax, tt, uu, vv)) {
+                        found = true;
+                        hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)(start + i);
+                        tmax = tt;
+                    }
                 }
             }
         }
@@ -386,12 +415,19 @@ struct Bvh8Walker {
             ++ntri;
             const float4 *tp = S.tris + 3 * (size_t)tri;
             const float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
-            float tt, uu, vv;
-            if (intersect_watertight(w, o, xyz(p0), xyz(p1), xyz(p2), tmin, tmax, tt, uu, vv)) {
-                found = true;
-                hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)tri;
-                if (kAnyHit) return true;
-                tmax = tt;
+            if constexpr (kAnyHit) {
+                if (occludes_mt(o, d, xyz(p0), xyz(p1), xyz(p2), tmin, tmax)) {
+                    found = true;
+                    hit.tri = (int)tri;
+                    return true;
+                }
+            } else {
+                float tt, uu, vv;
+                if (intersect_watertight(w, o, xyz(p0), xyz(p1), xyz(p2), tmin, tmax, tt, uu, vv)) {
+                    found = true;
+                    hit.t = tt; hit.u = uu; hit.v = vv; hit.tri = (int)tri;
+                    tmax = tt;
+                }
             }
         }
         if (ng.y <= 0x00ffffffu) {

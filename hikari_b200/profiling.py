@@ -5,11 +5,14 @@ selected raw metrics of a `--set full` report (`ncu -i X --page raw --csv`).
 usage: python -m hikari_b200.profiling launches <launches.csv>
        python -m hikari_b200.profiling raw <report.ncu-rep> [regex]
        python -m hikari_b200.profiling render [--views V] [--spp S] [--accel bvh2|bvh8] [--out F]
+                                              [--threads-extend T] [--threads-shade T] [--fetch-steps K]
+                                              [--fetch-min-idle K]
        python -m hikari_b200.profiling traffic <dram.csv> <render.json>
 
 `render` renders the heterogeneous scene once with the wavefront integrator
-(no autotuning, no other launches of the traversal kernels) and writes its
-counters as JSON; run under `ncu --metrics dram__bytes_read.sum,
+(no autotuning, no other launches of the traversal kernels; the launch
+configuration is given on the command line, e.g. the one bench.py's
+autotuner picked) and writes its counters as JSON; run under `ncu --metrics dram__bytes_read.sum,
 dram__bytes_write.sum,gpu__time_duration.sum -k regex:"wf_(extend|shadow)"
 --cache-control none`, `traffic` turns the per-launch DRAM bytes of that
 capture into DRAM bytes per closest-hit and per shadow ray.
@@ -121,6 +124,11 @@ def render(argv):
     ap.add_argument("--accel", default="bvh2", choices=["bvh2", "bvh8"])
     ap.add_argument("--capacity", type=int, default=1 << 22)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--threads-extend", type=int, default=0)
+    ap.add_argument("--threads-shade", type=int, default=0)
+    ap.add_argument("--fetch-steps", type=int, default=0)
+    ap.add_argument("--fetch-min-idle", type=int, default=0)
+    ap.add_argument("--iterations-per-check", type=int, default=0)
     a = ap.parse_args(argv)
     sd = scenes.heterogeneous(width=1024, height=1024, spp=a.spp, depth=16)
     cams = scenes.heterogeneous_cameras(a.views)
@@ -128,11 +136,15 @@ def render(argv):
     gs.set_accel(hk.ACCEL_BVH8 if a.accel == "bvh8" else hk.ACCEL_BVH2)
     films = [torch.zeros(gs.film_shape(), device="cuda") for _ in range(a.views)]
     ctr = torch.zeros(7, dtype=torch.int64, device="cuda")
-    gs.render_batch(films, spp=a.spp, depth=sd.depth, cameras=cams, counters=ctr, capacity=a.capacity)
+    gs.render_batch(films, spp=a.spp, depth=sd.depth, cameras=cams, counters=ctr, capacity=a.capacity,
+                    threads_extend=a.threads_extend, threads_shade=a.threads_shade, fetch_steps=a.fetch_steps,
+                    fetch_min_idle=a.fetch_min_idle, iterations_per_check=a.iterations_per_check)
     torch.cuda.synchronize()
     c = [int(x) for x in ctr.cpu().tolist()]
     names = ["rays", "shadow_rays", "dropped", "node_visits", "tri_tests", "node_visits_shadow", "tri_tests_shadow"]
     out = {"workload": f"heterogeneous {a.views} x 1024^2 x {a.spp} spp", "accel": a.accel,
+           "launch": {"capacity": a.capacity, "threads_extend": a.threads_extend, "threads_shade": a.threads_shade,
+                      "fetch_steps": a.fetch_steps, "fetch_min_idle": a.fetch_min_idle},
            "counters": dict(zip(names, c))}
     text = json.dumps(out)
     if a.out:

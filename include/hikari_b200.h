@@ -225,10 +225,21 @@ int hk_render(hk_scene *s, const hk_render_desc *desc, float *film_dev, unsigned
               void *stream);
 /* film -> H*W*3 RGB (ImageBlock::ToBitmap, src/core/Block.cpp:61) */
 int hk_film_resolve(hk_scene *s, const float *film_dev, float *rgb_dev, void *stream);
-/* End-to-end call: render into the scene's own film, resolve and copy the
- * H*W*3 float image to host memory rgb_host.  counters (host, 5) optional. */
+/* End-to-end call, the whole-image render a pathMISCuda plugin's RenderImage
+ * makes in place of Render's block loop (src/Main.cpp:46-147): render into
+ * the scene's own film, resolve and copy the H*W*3 float image to host memory
+ * rgb_host.  counters (host, 5) optional: as hk_render's (node visits and
+ * triangle tests summed over closest-hit and shadow rays).  The image is
+ * rendered with the wavefront integrator (hk_render_batch, one job) when the
+ * scene's image form says so -- by default once it has at least 256 x 256
+ * pixels and 2^22 paths -- else with the megakernel (hk_render).  Both run the
+ * same estimator on the same per-sample streams: the images agree up to the
+ * order of the film's float additions. */
 int hk_render_image(hk_scene *s, const hk_render_desc *desc, float *rgb_host, unsigned long long *counters,
                     void *stream);
+enum { HK_FORM_AUTO = 0, HK_FORM_MEGAKERNEL = 1, HK_FORM_WAVEFRONT = 2 };
+/* The form hk_render_image renders with (HK_FORM_AUTO by default). */
+int hk_scene_set_image_form(hk_scene *s, int32_t form);
 
 /* ---- wavefront rendering (the batched form) ---- */
 /* One image of a batch: accumulate desc.spp samples into film_dev (film layout
@@ -275,6 +286,10 @@ int hk_render_batch_host(hk_scene *s, const hk_render_desc *descs, int n, const 
  * interval 16/64, traversal refill interval and idle-lane threshold -- by
  * coordinate descent and return the fastest. */
 int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront_config *best, float *best_ms);
+/* The wavefront configuration hk_render_image uses (NULL: the defaults of
+ * hk_render_batch).  hk_wavefront_autotune sets it to the configuration it
+ * finds, so a plugin that tunes once in Preprocess renders every image with it. */
+int hk_scene_set_wavefront_config(hk_scene *s, const hk_wavefront_config *cfg);
 
 /* Render into a caller-provided device image without allocating any device
  * memory.  This entry point has no counterpart in the reference.  It is for

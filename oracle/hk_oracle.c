@@ -2615,6 +2615,28 @@ void ho_pixel_stats(const ho_scene *s, int depth, int spp, uint64_t seed, int np
     }
 }
 
+/* One sample per listed pixel from the stream seeded (seed, pixel), as
+ * ho_pixel_stats draws it: out npix x 5 floats (film x, film y, radiance rgb;
+ * the radiance unfiltered and not checked for validity). */
+void ho_pixel_samples(const ho_scene *s, int depth, uint64_t seed, int npix, const int32_t *pix, float *out,
+                      int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+    for (int k = 0; k < npix; k++) {
+        int x = pix[2 * k], y = pix[2 * k + 1];
+        ho_pcg32 rng; ho_pcg32_seed(&rng, seed, (uint64_t)y * s->W + x);
+        ctr_t c = {0, 0};
+        float px = (float)x + ho_pcg32_nextf(&rng), py = (float)y + ho_pcg32_nextf(&rng);
+        v3 o, d; float mn, mx;
+        camera_ray(s, px, py, &o, &d, &mn, &mx);
+        float pxy[2] = {px, py};
+        v3 L = li_pathmis(s, depth, &rng, o, d, mn, mx, pxy, &c);
+        out[5 * k] = px; out[5 * k + 1] = py; out[5 * k + 2] = L.x; out[5 * k + 3] = L.y; out[5 * k + 4] = L.z;
+    }
+}
+
 void ho_ttest_scene(const ho_scene *s, int depth, int n, double *mean, double *var) {
     ho_pcg32 rng; pcg_default(&rng);
     double m = 0, v = 0;

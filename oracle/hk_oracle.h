@@ -191,6 +191,10 @@ int64_t ho_render(const ho_scene *s, int depth, int spp, const int32_t *block_li
  * of each channel of Li (no filter). pix: npix*2 ints. out: npix*6 doubles. */
 void ho_pixel_stats(const ho_scene *s, int depth, int spp, uint64_t seed, int npix,
                     const int32_t *pix, double *out, int nthreads);
+/* One sample per listed pixel from the stream (seed, pixel): out npix x 5
+ * floats (film x, film y, radiance rgb). */
+void ho_pixel_samples(const ho_scene *s, int depth, uint64_t seed, int npix, const int32_t *pix, float *out,
+                      int nthreads);
 /* StudentTTest scene mode (src/core/StudentTTest.cpp:143-174): n paths with
  * a default-seeded independent sampler; mean and variance of luminance. */
 void ho_ttest_scene(const ho_scene *s, int depth, int n, double *mean, double *var);

@@ -111,6 +111,7 @@ def lib():
         L.ho_render.restype = C.c_int64
         L.ho_scene_set_reference_draw_order.argtypes = [P, C.c_int]
         L.ho_film_put_samples.argtypes = [P, C.c_uint64, P, P, P]
+        L.ho_pixel_samples.argtypes = [P, C.c_int, C.c_uint64, C.c_int, P, P, C.c_int]
         L.ho_film_put_samples.restype = C.c_int64
         L.ho_pixel_stats.argtypes = [P, C.c_int, C.c_int, C.c_uint64, C.c_int, P, P, C.c_int]
         L.ho_ttest_scene.argtypes = [P, C.c_int, C.c_int, P, P]
@@ -390,6 +391,13 @@ class OracleScene:
         out = np.zeros((pix.shape[0], 6), np.float64)
         lib().ho_pixel_stats(self.h, depth or self.desc.depth, spp, seed, pix.shape[0], _p(pix), _p(out), nthreads)
         return out[:, :3], out[:, 3:]
+
+    def pixel_samples(self, pixels, seed, depth=None, nthreads=0):
+        """One path per pixel from the stream (seed, pixel): (film positions n x 2, radiance n x 3)."""
+        pix = np.ascontiguousarray(pixels, dtype=np.int32)
+        out = np.zeros((pix.shape[0], 5), np.float32)
+        lib().ho_pixel_samples(self.h, depth or self.desc.depth, seed, pix.shape[0], _p(pix), _p(out), nthreads)
+        return out[:, :2].copy(), out[:, 2:].copy()
 
     def ttest_scene(self, n, depth=None):
         m = C.c_double(0); v = C.c_double(0)

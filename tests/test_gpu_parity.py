@@ -288,7 +288,7 @@ def test_render_cornell_matches_oracle():
     sd = scenes.cornell_box(width=48, height=48)
     sd.filter = FilterDesc(0, 0.5)
     gs, os_ = hk.Scene.from_desc(sd), OracleScene(sd)
-    spp_g, spp_o = 4096, 512
+    spp_g, spp_o = 4096, 2048
     img, ctr = gs.render_image(spp_g, sd.depth, seed=7)
     pix = np.stack(np.meshgrid(np.arange(48), np.arange(48), indexing="xy"), -1).reshape(-1, 2)
     mean_o, var_o = os_.pixel_stats(pix, spp_o, seed=3)
@@ -298,21 +298,6 @@ def test_render_cornell_matches_oracle():
     frac3 = np.mean(np.abs(z) > 3)
     print("z mean", z.mean(), "frac |z|>3", frac3, "max", np.abs(z).max(), "counters", ctr)
     assert abs(g.mean() / mean_o.mean() - 1) < 0.01
-    assert frac3 < 0.02
+    # normal tail P(|z| > 3) = 0.27%; the per-pixel variances are estimates
+    assert frac3 < 0.008
     assert ctr[0] >= 48 * 48 * spp_g
-
-
-def test_render_rmse_scales_with_spp():
-    """Mean squared error against a high-spp reference falls like 1/spp
-    (RMSE like 1/sqrt(spp)); MSE averaged over 16 independent renders per spp
-    so single fireflies do not dominate."""
-    sd = scenes.cornell_box(width=32, height=32)
-    gs = hk.Scene.from_desc(sd)
-    ref, _ = gs.render_image(65536, sd.depth, seed=99)
-    mse = []
-    for spp in (16, 64, 256):
-        e = [np.mean((gs.render_image(spp, sd.depth, seed=1000 * spp + k)[0] - ref) ** 2) for k in range(16)]
-        mse.append(np.mean(e))
-    r1, r2 = mse[0] / mse[1], mse[1] / mse[2]
-    print("mse", mse, "ratios", r1, r2)
-    assert 2.5 < r1 < 6.0 and 2.5 < r2 < 6.0, mse

@@ -50,13 +50,14 @@ def test_wavefront_cornell_matches_oracle():
     gs.render_batch([film], spp=4096, depth=sd.depth, seeds=[7], counters=ctr, capacity=1 << 18)
     g = _resolve(gs, film).reshape(-1, 3).astype(np.float64)
     pix = np.stack(np.meshgrid(np.arange(48), np.arange(48), indexing="xy"), -1).reshape(-1, 2)
-    mean_o, var_o = os_.pixel_stats(pix, 512, seed=3)
-    z = (g - mean_o) / (np.sqrt(var_o / 4096 + var_o / 512) + 1e-6)
+    mean_o, var_o = os_.pixel_stats(pix, 2048, seed=3)
+    z = (g - mean_o) / (np.sqrt(var_o / 4096 + var_o / 2048) + 1e-6)
     frac3 = np.mean(np.abs(z) > 3)
     c = ctr.cpu().numpy()
     print("z mean", z.mean(), "frac |z|>3", frac3, "max", np.abs(z).max(), "counters", c)
     assert abs(g.mean() / mean_o.mean() - 1) < 0.01
-    assert frac3 < 0.02
+    # normal tail P(|z| > 3) = 0.27%; the per-pixel variances are estimates
+    assert frac3 < 0.008
     assert c[0] >= 48 * 48 * 4096
 
 
@@ -100,38 +101,6 @@ def test_wavefront_batch_of_images_equals_separate_images():
         assert np.allclose(a, b, rtol=1e-5, atol=1e-6), np.abs(a - b).max()
 
 
-@pytest.mark.parametrize("accel", [hk.ACCEL_BVH8, hk.ACCEL_BVH2])
-def test_equal_rmse_wavefront_and_megakernel(accel):
-    """At equal spp the wavefront and the megakernel have equal RMSE against a
-    high-spp reference (they run the same estimator), and both halve their MSE
-    when spp doubles.  The reference is a 65536-spp image of the Cornell box
-    whose per-pixel means match the CPU oracle (test_wavefront_cornell_matches_oracle)."""
-    sd = scenes.cornell_box(width=48, height=48)
-    sd.filter = FilterDesc(0, 0.5)
-    gs = hk.Scene.from_desc(sd)
-    gs.set_accel(accel)
-    ref_film = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
-    gs.render(ref_film, spp=65536, depth=sd.depth, seed=424242)
-    ref = _resolve(gs, ref_film).astype(np.float64)
-
-    def mse(form, spp, k):
-        out = []
-        for s in range(k):
-            f = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
-            if form == "mega":
-                gs.render(f, spp=spp, depth=sd.depth, seed=9000 + s)
-            else:
-                gs.render_batch([f], spp=spp, depth=sd.depth, seeds=[7000 + s], capacity=1 << 16)
-            out.append(np.mean((_resolve(gs, f).astype(np.float64) - ref) ** 2))
-        return float(np.mean(out))
-
-    m64, w64 = mse("mega", 64, 16), mse("wave", 64, 16)
-    w256 = mse("wave", 256, 16)
-    print(f"accel {accel}: MSE at 64 spp megakernel {m64:.3e} wavefront {w64:.3e}; wavefront 256 spp {w256:.3e}")
-    assert 0.75 < w64 / m64 < 1.33           # equal RMSE at equal spp (16 images each; fireflies add spread)
-    assert 2.8 < w64 / w256 < 5.5            # MSE ~ 1/spp (4x spp -> 1/4 MSE)
-
-
 def test_progressive_passes_equal_one_render(tmp_path):
     """Passes over consecutive sample ranges accumulate to the single render of
     all samples (each sample's stream depends only on seed, sample and pixel);
@@ -150,3 +119,29 @@ def test_progressive_passes_equal_one_render(tmp_path):
     # earlier passes are noisier estimates of the same image
     errs = [np.mean((i - one) ** 2) for i in imgs]
     assert errs[0] > errs[-1]
+
+
+def test_render_image_forms_agree():
+    """hk_render_image, the call a pathMISCuda plugin's RenderImage makes,
+    renders large images with the wavefront: both forms draw the same
+    per-sample streams, so the images agree up to the order of the film's
+    float additions, and so do the ray counters."""
+    sd = scenes.cornell_box(width=256, height=256)
+    gs = hk.Scene.from_desc(sd)
+    imgs, ctrs = {}, {}
+    for form in (hk.FORM_MEGAKERNEL, hk.FORM_WAVEFRONT, hk.FORM_AUTO):
+        gs.set_image_form(form)
+        imgs[form], ctrs[form] = gs.render_image(64, sd.depth, seed=31)
+    a, b, c = imgs[hk.FORM_MEGAKERNEL], imgs[hk.FORM_WAVEFRONT], imgs[hk.FORM_AUTO]
+    scale = float(np.abs(a).max())
+    close = np.abs(a.astype(np.float64) - b) <= 1e-4 * np.abs(a) + 1e-6 * scale
+    print("megakernel vs wavefront: max abs", np.abs(a - b).max(), "close", close.mean())
+    assert close.mean() > 0.999
+    assert np.allclose(b, c, rtol=1e-5, atol=1e-6 * scale)   # auto picks the wavefront at this size
+    m, w = ctrs[hk.FORM_MEGAKERNEL], ctrs[hk.FORM_WAVEFRONT]
+    assert abs(int(m[0]) - int(w[0])) <= 2e-3 * m[0] and abs(int(m[1]) - int(w[1])) <= 2e-3 * m[1]
+    # an autotuned configuration is kept for render_image
+    gs.autotune(4, sd.depth)
+    gs.set_image_form(hk.FORM_AUTO)
+    d, _ = gs.render_image(64, sd.depth, seed=31)
+    assert np.allclose(d, b, rtol=1e-4, atol=1e-6 * scale)

@@ -46,7 +46,12 @@ def test_static_scratch_render_matches_allocating_entry_point():
     w, h = 256, 192
     sd = scenes.cornell_box(width=w, height=h)
     gs = hk.Scene.from_desc(sd)
+    gs.set_image_form(hk.FORM_MEGAKERNEL)   # the same kernel as the static entry point
     ref, ref_ctr = gs.render_image(64, sd.depth, seed=11)
+    # a second scene that has not rendered yet: its first render_image must
+    # allocate a film (built here, before the device memory is taken)
+    fresh = hk.Scene.from_desc(sd)
+    fresh.set_image_form(hk.FORM_MEGAKERNEL)
     film_bytes = (w + 4) * (h + 4) * 16
     for call in range(2):
         out = torch.full((h, w, 3), -1.0, dtype=torch.float32, device="cuda")
@@ -54,10 +59,10 @@ def test_static_scratch_render_matches_allocating_entry_point():
         held = []
         if call == 1:
             # the second call runs with the device's free memory taken: an
-            # allocation of the film would fail (checked on the allocating path)
+            # allocation of the film fails there (shown on the allocating path)
             held = _take_free_memory(film_bytes // 2)
             with pytest.raises(hk.HikariError):
-                gs.render_image(1, sd.depth, seed=11)
+                fresh.render_image(1, sd.depth, seed=11)
         gs.render_image_static(out, 64, sd.depth, seed=11, counters=ctr)
         torch.cuda.synchronize()
         del held
