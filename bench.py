@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--records", type=int, default=1 << 26, help="bsdf: records per material")
     ap.add_argument("--accel", default="bvh8", choices=["bvh8", "bvh2"],
                     help="tree the kernels traverse: compressed 8-wide (80-byte nodes) or binary (64-byte nodes)")
-    ap.add_argument("--jobs", type=int, default=40, help="serving: jobs of the Poisson run")
+    ap.add_argument("--jobs", type=int, default=400, help="serving: jobs of the Poisson run")
     ap.add_argument("--load", type=float, default=0.8, help="serving: arrival rate as a fraction of the peak")
     ap.add_argument("--capacity", type=int, default=1 << 19, help="serving: path slots of each scene's pool")
     ap.add_argument("--spp", type=int, default=0)
@@ -311,15 +311,19 @@ def run_reference(args, rank, world):
 
 
 def serving_scenes():
-    """The serving set: Cornell box, the mesh-heavy icosphere, the heterogeneous
-    scene and five seeded variants of it from about 20k to 3M triangles."""
+    """The serving set of config 5: the Cornell box (config 1), the mesh-heavy
+    icosphere (config 3, 1.31M triangles), the heterogeneous scene (config 4,
+    4.75M) and five seeded variants of it spanning about 10k to 3M triangles."""
     from hikari_b200 import scenes
 
     sds = [scenes.cornell_box(width=256, height=256, spp=64),
            scenes.mesh_heavy("conductor", width=1024, height=1024, spp=256, depth=16),
            scenes.heterogeneous(width=1024, height=1024, spp=128, depth=16)]
-    for k, n in enumerate((1, 4, 12, 24, 40)):
-        sds.append(scenes.heterogeneous(width=1024, height=1024, spp=128, depth=16, n_spheres=n, seed=k + 1))
+    variants = [(2, (4,), (1.0,)), (4, (5,), (1.0,)), (12, (5, 6), (0.5, 0.5)), (24, (6, 7), (0.5, 0.5)),
+                (40, (5, 6, 7), (0.55, 0.30, 0.15))]
+    for k, (n, lv, lp) in enumerate(variants):
+        sds.append(scenes.heterogeneous(width=1024, height=1024, spp=128, depth=16, n_spheres=n, levels=lv,
+                                        level_p=lp, seed=k + 1))
     return sds
 
 
@@ -360,9 +364,26 @@ def run_serving(args):
         peak_rate = peak_mpaths * 1e6 / mean_paths
         iso = serving.isolated_latencies(srv, jobs)
         rate = args.load * peak_rate
-        res = serving.run_poisson(srv, jobs, rate, seed=11, isolated=iso)
+        res = serving.run_poisson(srv, jobs, rate, seed=11, isolated=iso, keep=lambda j: j.width == 256)
         summ = res.summary()
         st = srv.stats()
+    # RMSE of the 256 x 256 jobs rendered in the mix against each scene's
+    # reference image (the same scene and view at 256 x 256, 4096 spp)
+    rmse = {}
+    refs = {}
+    for k, img in res.images.items():
+        j = jobs[k]
+        if j.scene not in refs:
+            f = torch.zeros(gss[j.scene].film_shape(256, 256), dtype=torch.float32, device="cuda")
+            gss[j.scene].render_batch([f], spp=4096, depth=j.depth, seeds=[424242], image_indices=[0],
+                                      sizes=[(256, 256)])
+            B = int(gss[j.scene].info.film_border)
+            c = f.cpu().numpy().astype(np.float64)[B:B + 256, B:B + 256]
+            refs[j.scene] = np.where(c[..., 3:] != 0, c[..., :3] / np.where(c[..., 3:] != 0, c[..., 3:], 1), 0)
+        ref = refs[j.scene]
+        rel = float(np.sqrt(np.mean((img.astype(np.float64) - ref) ** 2)) / max(np.mean(np.abs(ref)), 1e-12))
+        rmse.setdefault(j.spp, []).append(rel)
+    rmse_summary = {str(sp): {"jobs": len(v), "relative_rmse_mean": float(np.mean(v))} for sp, v in sorted(rmse.items())}
     line = {
         "metric": "Mpaths/s", "value": summ["mpaths_per_s"], "unit": "Mpaths/s", "n_gpus": 1, "steps": 1,
         "warmup": 1, "ms_per_step": summ["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -381,6 +402,7 @@ def run_serving(args):
                                    "p99": float(np.percentile(iso, 99))},
             "p99_over_isolated_p99": summ["p99_s"] / float(np.percentile(iso, 99)),
             "slowdown": {"p50": summ["slowdown_p50"], "p95": summ["slowdown_p95"], "p99": summ["slowdown_p99"]},
+            "rmse_256px_jobs_vs_4096spp_reference": rmse_summary,
             "rays": int(st["rays"]), "shadow_rays": int(st["shadow_rays"]),
         },
     }

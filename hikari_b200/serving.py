@@ -175,26 +175,31 @@ def isolated_latencies(server: Server, jobs: Sequence[JobSpec]) -> np.ndarray:
 
 
 def run_poisson(server: Server, jobs: Sequence[JobSpec], rate_hz: float, seed: int = 0,
-                isolated: Optional[np.ndarray] = None) -> LoadResult:
+                isolated: Optional[np.ndarray] = None, keep=None) -> LoadResult:
     """Submit `jobs` with exponential inter-arrival gaps of mean 1/rate_hz and
     wait for all; the latency of a job runs from its submission to its image
-    being in host memory."""
+    being in host memory.  keep(job) -> bool selects the jobs whose images are
+    returned (LoadResult.images: job index -> image)."""
     rng = np.random.default_rng(seed)
     gaps = rng.exponential(1.0 / rate_hz, len(jobs))
-    ids = []
+    ids, imgs = [], {}
     t0 = time.perf_counter()
     t_next = t0
-    for j, g in zip(jobs, gaps):
+    for k, (j, g) in enumerate(zip(jobs, gaps)):
         t_next += g
         while True:
             dt = t_next - time.perf_counter()
             if dt <= 0:
                 break
             time.sleep(min(dt, 0.002))
-        jid, _ = server.submit(j.scene, j.spp, j.depth, j.seed, j.width, j.height, j.camera)
+        jid, img = server.submit(j.scene, j.spp, j.depth, j.seed, j.width, j.height, j.camera)
         ids.append(jid)
+        if keep is not None and keep(j):
+            imgs[k] = img
     lat = np.array([server.wait(i)["latency_s"] for i in ids])
     wall = time.perf_counter() - t0
     paths = sum(j.paths for j in jobs)
     sd = lat / isolated if isolated is not None else None
-    return LoadResult(rate_hz, lat, sd, paths, wall, server.stats())
+    res = LoadResult(rate_hz, lat, sd, paths, wall, server.stats())
+    res.images = imgs
+    return res

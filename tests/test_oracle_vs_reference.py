@@ -299,3 +299,65 @@ def test_oracle_post_intersect_bit_exact_vs_reference():
             R.hr_post_intersect(h, int(tri[k]), float(u[k]), float(v[k]), O._p(b))
             assert np.array_equal(a, b) or (np.isnan(a) == np.isnan(b)).all() and np.array_equal(a[~np.isnan(a)], b[~np.isnan(b)]), \
                 f"{name}: triangle {tri[k]} ({u[k]}, {v[k]}): oracle {a} reference {b}"
+
+
+def _config2_complex_ior():
+    """The config-2 materials with a per-channel complex IOR (Cu, Au) and the
+    coated conductor, whose nested conductor has one too."""
+    from hikari_b200 import scenes
+
+    return [(name, d) for name, d in scenes.config2_materials()
+            if d.eta is not None or (d.nested is not None and d.nested.eta is not None)]
+
+
+@pytest.mark.parametrize("case", range(len(_config2_complex_ior())))
+def test_per_channel_ior_pinned_channel_by_channel(case):
+    """The reference's conductors take one IOR for every channel
+    (m_Eta = Color3f(intIOR / extIOR), src/bsdf/RoughConductorBSDF.cpp:43), so a
+    per-channel eta is pinned one channel at a time: the reference built with
+    intIOR = eta_c (extIOR 1) gives channel c of the oracle's per-channel
+    material bit for bit.  D and G do not depend on eta and the conductor
+    Fresnel term is channel-wise (src/core/Common.cpp:529), so the sampled
+    directions, measures and pdfs agree on every channel too."""
+    import copy
+
+    R = _ref_lib()
+    name, d = _config2_complex_ior()[case]
+    n = 20000
+    wi, u2, u1, wo = records(n, 11)
+    o = O.OracleScene(SceneDesc())
+    bid = o.add_bsdf(d)
+    assert O.lib().ho_scene_finalize(o.h) == 0
+    a = o.bsdf_batch(bid, wi, u2, u1, wo)
+    f = lambda x: np.ascontiguousarray(x, np.float32)
+    keep = []
+
+    def mk(b):
+        if b is None:
+            return None
+        arrs = [f(b.k), f(b.ks), f(b.kd), f(b.sigma_a), f(b.ks_refract)]
+        keep.append(arrs)
+        k, ks, kd, sa, kr = arrs
+        tex = (C.c_void_p * 6)()
+        keep.append(tex)
+        h = R.hr_bsdf_create(b.type, b.distribution, b.alpha_u, b.int_ior, b.ext_ior, O._p(k), O._p(ks), O._p(kd),
+                             O._p(sa), b.thickness, mk(b.nested), mk(b.nested2), O._p(kr), int(b.nonlinear),
+                             int(b.fast_approx), tex, int(b.anisotropic))
+        assert h
+        return h
+
+    for c in range(3):
+        dc = copy.deepcopy(d)
+        target = dc if dc.eta is not None else dc.nested
+        target.int_ior, target.ext_ior, target.eta = float(np.float32(d.eta[c] if d.eta is not None
+                                                                       else d.nested.eta[c])), 1.0, None
+        h = mk(dc)
+        b = {k: np.zeros_like(v) for k, v in a.items()}
+        R.hr_bsdf_batch(h, n, O._p(wi), O._p(u2), O._p(u1), O._p(wo), None, None, O._p(b["s_wo"]), O._p(b["s_w"]),
+                        O._p(b["s_pdf"]), O._p(b["s_measure"]), O._p(b["e_rgb"]), O._p(b["p_pdf"]))
+        np.testing.assert_array_equal(a["s_w"][:, c], b["s_w"][:, c], err_msg=f"{name} channel {c}")
+        np.testing.assert_array_equal(a["e_rgb"][:, c], b["e_rgb"][:, c], err_msg=f"{name} channel {c}")
+        valid = np.any(a["s_w"] != 0, axis=1)
+        np.testing.assert_array_equal(a["s_wo"][valid], b["s_wo"][valid])
+        np.testing.assert_array_equal(a["s_pdf"], b["s_pdf"])
+        np.testing.assert_array_equal(a["p_pdf"], b["p_pdf"])
