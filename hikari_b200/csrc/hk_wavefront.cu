@@ -47,7 +47,13 @@ HK_WF_SHADE_EXTERN(3);
 HK_WF_SHADE_EXTERN(4);
 HK_WF_SHADE_EXTERN(5);
 HK_WF_SHADE_EXTERN(6);
+HK_WF_SHADE_EXTERN(7);
+HK_WF_SHADE_EXTERN(8);
+HK_WF_SHADE_EXTERN(9);
+HK_WF_SHADE_EXTERN(10);
+HK_WF_SHADE_EXTERN(11);
 #undef HK_WF_SHADE_EXTERN
+static_assert(kWfTypes == 12, "launch_shade_all launches one kernel per shade queue");
 
 // ------------------------------------------------------------ regen
 // Splat and retire the finished paths, then give every finished or idle slot
@@ -194,7 +200,12 @@ static cudaError_t launch_shade_all(const DevScene &S, const WfState &W, const W
     wf_launch_shade_t<3>(S, W, C, nxt, st);
     wf_launch_shade_t<4>(S, W, C, nxt, st);
     wf_launch_shade_t<5>(S, W, C, nxt, st);
-    return wf_launch_shade_t<6>(S, W, C, nxt, st);
+    wf_launch_shade_t<6>(S, W, C, nxt, st);
+    wf_launch_shade_t<7>(S, W, C, nxt, st);
+    wf_launch_shade_t<8>(S, W, C, nxt, st);
+    wf_launch_shade_t<9>(S, W, C, nxt, st);
+    wf_launch_shade_t<10>(S, W, C, nxt, st);
+    return wf_launch_shade_t<11>(S, W, C, nxt, st);
 }
 
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st) {

@@ -18,13 +18,17 @@
 
 namespace hk {
 
-// Shade queues: 0 miss, 1..5 the rough BSDF types (type + 1), each shaded by a
-// kernel compiled for that type; 6 the smooth and twoSided BSDFs, shaded by one
-// kernel that dispatches at run time.
-constexpr int kWfTypes = 7;
-constexpr int kWfGenericQueue = kWfTypes - 1;
-__host__ __device__ constexpr int wf_queue_of(int bsdf_type) {
-    return bsdf_type <= kRoughCoating ? bsdf_type + 1 : kWfGenericQueue;
+// Shade queues: 0 miss; 1..5 the rough BSDF types without textures (type +
+// 1), each shaded by a kernel compiled for that type with texture lookups
+// compiled out; 6 the smooth, twoSided, bump- and normal-mapped BSDFs, shaded
+// by one kernel that dispatches at run time; 7..11 the rough BSDF types with
+// textured parameters (type + 7), each shaded by a kernel compiled for that
+// type with texture lookups.
+constexpr int kWfGenericQueue = 6;
+constexpr int kWfTexturedQueue0 = 7;
+constexpr int kWfTypes = kWfTexturedQueue0 + kRoughCoating + 1;
+__host__ __device__ constexpr int wf_queue_of(int bsdf_type, bool textured = false) {
+    return bsdf_type <= kRoughCoating ? (textured ? kWfTexturedQueue0 + bsdf_type : bsdf_type + 1) : kWfGenericQueue;
 }
 constexpr int kWfMaxJobs = 1024;   // job table entries of one engine
 constexpr int kWfMaxSegs = 4096;   // pieces of one dispatch plan

@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, i
             if (w.found) {
                 const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
                 const DevBsdf &B = S.bsdfs[S.meshes[mesh].bsdf];
-                type = B.textured ? kWfGenericQueue : wf_queue_of(B.type);
+                type = wf_queue_of(B.type, B.textured != 0);
             }
             W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
             W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
@@ -181,7 +181,11 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             finish(W, slot);
             continue;
         } else {
-            constexpr int BT = kType == kWfGenericQueue ? -1 : kType - 1;
+            // queue -> top-level BSDF type (run-time dispatch for the generic
+            // queue) and whether texture lookups are compiled in
+            constexpr int BT = kType == kWfGenericQueue ? -1
+                                                        : (kType >= kWfTexturedQueue0 ? kType - kWfTexturedQueue0 : kType - 1);
+            constexpr bool kTexQ = kType >= kWfGenericQueue;
             uint4 rs = W.rng[slot];
             Pcg32 rng;
             rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
@@ -225,9 +229,11 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             // screen-space partials of a camera ray's first hit (textured
             // materials only: Intersection::ComputeScreenSpacePartial)
             float4 duv = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            BumpFrames bf;   // a bumpMap / normalMap vertex's frames (this kernel only)
+            BumpFrames bf;   // a bumpMap / normalMap vertex's frames (the generic queue only)
             if constexpr (BT < 0) {
                 if (is_bump(S.bsdfs[bsdf])) bf = perturbed_frames(S, h, it, S.bsdfs[bsdf]);
+            }
+            if constexpr (kTexQ) {
                 if (depth == 0 && S.ray_diff) {
                     V3 rx, ry;
                     camera_diff(S, J.cam, J.width, J.height, J.cam_aspect, p4.x, p4.y, rx, ry);
@@ -250,10 +256,10 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
                 br.wo = to_local(it.sh, er.wi);
                 br.measure = kMeasureSolidAngle;
                 br.eta = 0.0f;
-                br.tex = BT < 0;   // textured materials are shaded by the run-time-dispatched kernel
+                br.tex = kTexQ;   // lookups only in the kernels of textured materials
                 br.tu = it.u;
                 br.tv = it.v;
-                if constexpr (BT < 0) br.duv = duv;   // unread where lookups are compiled out
+                if constexpr (kTexQ) br.duv = duv;   // unread where lookups are compiled out
                 float pl = er.pdf;
                 float pb;
                 V3 f;
@@ -282,10 +288,10 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             br.wo = v3(0, 0, 0);
             br.measure = kMeasureUnknown;
             br.eta = 0.0f;
-            br.tex = BT < 0;
+            br.tex = kTexQ;
             br.tu = it.u;
             br.tv = it.v;
-            if constexpr (BT < 0) br.duv = duv;
+            if constexpr (kTexQ) br.duv = duv;
             float sx = rng.nextf(), sy = rng.nextf();
             float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
             V3 F;
@@ -314,13 +320,14 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
             W.pix[slot] = make_float4(p4.x, p4.y, p4.z, __int_as_float((int)((flags << 16) | (uint32_t)depth)));
             W.prev_wi[slot] = f4(br.wi, __int_as_float(bsdf));
             W.prev_wo[slot] = f4(br.wo, __int_as_float(br.measure));
-            if constexpr (BT < 0) {
+            if constexpr (kTexQ) {
                 // the MIS weight at an emitter hit next needs this BSDF's pdf of
                 // the sampled direction (PathMISIntegrator.cpp:128)
                 if (S.bsdfs[bsdf].textured && !(flags & kWfFlagForceMats)) {
                     BRec pr = br;
                     pr.eta = 0.0f;
-                    W.prev_pdf[slot] = bsdf_pdf_b(S.bsdfs, bsdf, pr, bf);
+                    if constexpr (BT < 0) W.prev_pdf[slot] = bsdf_pdf_b(S.bsdfs, bsdf, pr, bf);
+                    else W.prev_pdf[slot] = bsdf_pdf_t<BT>(S.bsdfs, bsdf, pr);
                 }
             }
             W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
