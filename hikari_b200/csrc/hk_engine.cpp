@@ -70,8 +70,11 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     L_.threads_shade = cfg_.threads_shade;
     L_.threads_shadow = cfg_.threads_extend;
     L_.threads_regen = 256;
+    L_.lean_extend = cfg_.reg_lean & 1;
+    L_.lean_shadow = (cfg_.reg_lean >> 1) & 1;
     auto grid = [&](int which, int threads) {
-        return std::max(1, sm_count * std::max(1, wf_occupancy(which, threads, S.accel)));
+        const bool lean = which == 0 ? L_.lean_extend : (which == 2 ? L_.lean_shadow : false);
+        return std::max(1, sm_count * std::max(1, wf_occupancy(which, threads, S.accel, lean)));
     };
     L_.blocks_extend = grid(0, L_.threads_extend);
     L_.blocks_shade = grid(1, L_.threads_shade);
@@ -79,6 +82,9 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     L_.blocks_regen = grid(3, L_.threads_regen);
     L_.fetch_steps = cfg_.fetch_steps > 0 ? cfg_.fetch_steps : (S.accel == kAccelBvh8 ? 3 : 8);
     L_.fetch_min_idle = std::max(1, std::min(32, cfg_.fetch_min_idle));
+    L_.fetch_steps_shadow = cfg_.fetch_steps_shadow > 0 ? cfg_.fetch_steps_shadow : L_.fetch_steps;
+    L_.fetch_min_idle_shadow = cfg_.fetch_min_idle_shadow > 0 ? std::min(32, cfg_.fetch_min_idle_shadow)
+                                                              : L_.fetch_min_idle;
     HK_CUDA(cudaGetLastError());
     reset();
 }

@@ -21,6 +21,9 @@ struct WfEngineConfig {
     int threads_shade = 128;
     int fetch_steps = 0;      // node visits between traversal refills (0: per-tree default)
     int fetch_min_idle = 1;   // idle lanes before a warp refills while others traverse
+    int fetch_steps_shadow = 0;      // the same for the shadow rays (0: the closest-hit value)
+    int fetch_min_idle_shadow = 0;
+    int reg_lean = 0;   // bit 0: extend, bit 1: shadow kernel with the smaller register budget
 };
 
 class WfEngine {

@@ -810,7 +810,9 @@ hk::WfEngine &wf_ensure(hk_scene *s, const hk::WfEngineConfig &c) {
     if (s->wf) {
         const hk::WfEngineConfig &o = s->wf->config();
         if (o.capacity == c.capacity && o.threads_extend == c.threads_extend && o.threads_shade == c.threads_shade &&
-            o.fetch_steps == c.fetch_steps && o.fetch_min_idle == c.fetch_min_idle)
+            o.fetch_steps == c.fetch_steps && o.fetch_min_idle == c.fetch_min_idle &&
+            o.fetch_steps_shadow == c.fetch_steps_shadow && o.fetch_min_idle_shadow == c.fetch_min_idle_shadow &&
+            o.reg_lean == c.reg_lean)
             return *s->wf;
         s->wf.reset();
     }
@@ -1342,6 +1344,9 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         ec.threads_shade = c.threads_shade > 0 ? c.threads_shade : 128;
         ec.fetch_steps = std::max(0, std::min(1024, c.fetch_steps));
         ec.fetch_min_idle = c.fetch_min_idle > 0 ? std::min(32, c.fetch_min_idle) : 1;
+        ec.fetch_steps_shadow = std::max(0, std::min(1024, c.fetch_steps_shadow));
+        ec.fetch_min_idle_shadow = c.fetch_min_idle_shadow > 0 ? std::min(32, c.fetch_min_idle_shadow) : 0;
+        ec.reg_lean = c.reg_lean & 3;
         hk::WfEngine &E = wf_ensure(s, ec);
         cudaStream_t user = (cudaStream_t)stream, st = E.stream();
         // order after the caller's stream (the films may have been cleared there)
@@ -1487,6 +1492,26 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
         c = bc;
         for (int k : min_idle) {
             c.fetch_min_idle = k;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        // register budgets of the extend and shadow kernels
+        c = bc;
+        for (int k : {1, 2, 3}) {
+            c.reg_lean = k;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        // the shadow rays' own refill interval and idle-lane threshold
+        c = bc;
+        for (int k : (s->dev.accel == hk::kAccelBvh8 ? steps8 : steps2)) {
+            c.fetch_steps_shadow = k;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        c = bc;
+        for (int k : min_idle) {
+            c.fetch_min_idle_shadow = k;
             float ms = run(c);
             if (ms < best_t) { best_t = ms; bc = c; }
         }

@@ -215,9 +215,12 @@ __global__ void __launch_bounds__(kTileThreads) render_pathmis_kernel(DevScene S
         if (x < (int)S.width && y < (int)S.height) {
             const int s0 = P.sample_offset + chunk * P.spp_per_item;
             const int s1 = min(s0 + P.spp_per_item, P.sample_offset + P.spp);
-            Pcg32 rng;
-            rng.seed(mix_seed(P.seed, (uint64_t)s0), (uint64_t)y * S.width + x + (uint64_t)P.image_index * S.width * S.height);
+            const uint64_t stream = (uint64_t)y * S.width + x + (uint64_t)P.image_index * S.width * S.height;
             for (int s = s0; s < s1; ++s) {
+                // one stream per (seed, sample, pixel, image), as the wavefront
+                // draws it: the image does not depend on the work split or the form
+                Pcg32 rng;
+                rng.seed(mix_seed(P.seed, (uint64_t)s), stream);
                 float px = (float)x + rng.nextf(), py = (float)y + rng.nextf();
                 Ray r = camera_ray(S, px, py);
                 V3 L = li_pathmis<kAccel, kTex>(S, rng, r, px, py, P.depth, P.rr_start, pc);

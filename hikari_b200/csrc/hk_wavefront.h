@@ -116,7 +116,9 @@ struct WfLaunchConfig {
     int blocks_shade, threads_shade;
     int blocks_shadow, threads_shadow;
     int blocks_regen, threads_regen;
-    int fetch_steps, fetch_min_idle;   // dynamic ray fetch of the extend and shadow kernels
+    int fetch_steps, fetch_min_idle;                 // dynamic ray fetch of the extend kernel
+    int fetch_steps_shadow, fetch_min_idle_shadow;   // and of the shadow kernel
+    int lean_extend, lean_shadow;                    // traversal kernels with the smaller register budget
 };
 
 // empty pool: every slot idle, queues and statistics zero (the dispatch head is the host's)
@@ -128,6 +130,8 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
                             cudaStream_t st);
 // out[0..6] += rays, shadow rays, dropped, node visits, triangle tests, shadow node visits, shadow tests
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st);
-int wf_occupancy(int which, int threads, int accel);
+// resident blocks per SM of a kernel (which: 0 extend, 1 shade, 2 shadow, 3
+// regen); lean: the traversal kernels' smaller register budget
+int wf_occupancy(int which, int threads, int accel, bool lean = false);
 
 }  // namespace hk

@@ -103,8 +103,15 @@ __device__ __forceinline__ SharedStack make_stack() {
     return s;
 }
 
-template <int kAccel>
-__global__ void __launch_bounds__(256) wf_extend_kernel(DevScene S, WfState W, int cur, int steps, int min_idle) {
+// The traversal kernels come in two register budgets: kMinBlocks = 0 leaves
+// the budget to the compiler; kLeanBlocks asks for five resident blocks of
+// 256 threads (at most 48 registers), more warps to hide the latency of the
+// node and triangle fetches at the price of some spilling.  The autotuner
+// picks per kernel (hk_wavefront_config.reg_lean).
+constexpr int kLeanBlocks = 5;
+
+template <int kAccel, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) wf_extend_kernel(DevScene S, WfState W, int cur, int steps, int min_idle) {
     const unsigned n = W.ctr->eq_count[cur];
     TravStats ts;
     WalkerOf<kAccel, SharedStack> wk;
@@ -338,8 +345,8 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
 }
 
 // ------------------------------------------------------------ shadow
-template <int kAccel>
-__global__ void __launch_bounds__(256) wf_shadow_kernel(DevScene S, WfState W, int steps, int min_idle) {
+template <int kAccel, int kMinBlocks>
+__global__ void __launch_bounds__(256, kMinBlocks) wf_shadow_kernel(DevScene S, WfState W, int steps, int min_idle) {
     const unsigned n = min(W.ctr->shadow_count, (unsigned)W.max_shadow);
     TravStats ts;
     WalkerOf<kAccel, SharedStack> wk;
@@ -388,22 +395,37 @@ __host__ inline size_t wf_stack_bytes(int threads) { return (size_t)threads * kS
 template <int kAccel>
 cudaError_t wf_launch_extend_t(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
     const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(C.threads_extend) : 0;
-    wf_extend_kernel<kAccel><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, C.fetch_steps, C.fetch_min_idle);
+    if (C.lean_extend)
+        wf_extend_kernel<kAccel, kLeanBlocks><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, C.fetch_steps,
+                                                                                          C.fetch_min_idle);
+    else
+        wf_extend_kernel<kAccel, 0><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, C.fetch_steps,
+                                                                                C.fetch_min_idle);
     return cudaGetLastError();
 }
 template <int kAccel>
 cudaError_t wf_launch_shadow_t(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
     const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(C.threads_shadow) : 0;
-    wf_shadow_kernel<kAccel><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(S, W, C.fetch_steps, C.fetch_min_idle);
+    if (C.lean_shadow)
+        wf_shadow_kernel<kAccel, kLeanBlocks><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(
+            S, W, C.fetch_steps_shadow, C.fetch_min_idle_shadow);
+    else
+        wf_shadow_kernel<kAccel, 0><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(S, W, C.fetch_steps_shadow,
+                                                                                C.fetch_min_idle_shadow);
     return cudaGetLastError();
 }
-// which: 0 extend, 2 shadow
+// which: 0 extend, 2 shadow; lean: the kLeanBlocks register budget
 template <int kAccel>
-int wf_trace_occupancy_t(int which, int threads) {
+int wf_trace_occupancy_t(int which, int threads, bool lean) {
     int n = 0;
     const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(threads) : 0;
-    if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel>, threads, smem);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel>, threads, smem);
+    if (which == 0) {
+        if (lean) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, kLeanBlocks>, threads, smem);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, 0>, threads, smem);
+    } else {
+        if (lean) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel, kLeanBlocks>, threads, smem);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel, 0>, threads, smem);
+    }
     return n;
 }
 template <int kType>

@@ -129,6 +129,9 @@ def render(argv):
     ap.add_argument("--fetch-steps", type=int, default=0)
     ap.add_argument("--fetch-min-idle", type=int, default=0)
     ap.add_argument("--iterations-per-check", type=int, default=0)
+    ap.add_argument("--fetch-steps-shadow", type=int, default=0)
+    ap.add_argument("--fetch-min-idle-shadow", type=int, default=0)
+    ap.add_argument("--reg-lean", type=int, default=0)
     a = ap.parse_args(argv)
     sd = scenes.heterogeneous(width=1024, height=1024, spp=a.spp, depth=16)
     cams = scenes.heterogeneous_cameras(a.views)
@@ -138,7 +141,9 @@ def render(argv):
     ctr = torch.zeros(7, dtype=torch.int64, device="cuda")
     gs.render_batch(films, spp=a.spp, depth=sd.depth, cameras=cams, counters=ctr, capacity=a.capacity,
                     threads_extend=a.threads_extend, threads_shade=a.threads_shade, fetch_steps=a.fetch_steps,
-                    fetch_min_idle=a.fetch_min_idle, iterations_per_check=a.iterations_per_check)
+                    fetch_min_idle=a.fetch_min_idle, iterations_per_check=a.iterations_per_check,
+                    fetch_steps_shadow=a.fetch_steps_shadow, fetch_min_idle_shadow=a.fetch_min_idle_shadow,
+                    reg_lean=a.reg_lean)
     torch.cuda.synchronize()
     c = [int(x) for x in ctr.cpu().tolist()]
     names = ["rays", "shadow_rays", "dropped", "node_visits", "tri_tests", "node_visits_shadow", "tri_tests_shadow"]

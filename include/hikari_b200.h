@@ -262,6 +262,10 @@ typedef struct {
                                       (0 = 8 for the binary tree, 3 for the 8-wide tree) */
     int32_t fetch_min_idle;        /* idle lanes of a warp before it refills while others still
                                       traverse (0 = 1: refill at once) */
+    int32_t fetch_steps_shadow;    /* the same two for the shadow (any-hit) rays; 0 = the closest-hit */
+    int32_t fetch_min_idle_shadow; /*   rays' values */
+    int32_t reg_lean;              /* bit 0 / bit 1: the extend / shadow kernel with a register budget of
+                                      48 (five resident blocks of 256 threads) instead of the compiler's */
 } hk_wavefront_config;
 
 /* Render every job of the batch with the wavefront integrator: a pool of path

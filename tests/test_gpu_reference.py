@@ -10,7 +10,7 @@ The device tests closest-hit triangles watertight (Woop et al.) and
 re-evaluates the winner with the reference's Moller-Trumbore arithmetic, so t,
 u and v are the reference's own where the triangle agrees; mismatches are
 allowed only where the reference's answer itself depends on the visit order
-(exact t ties of coplanar triangles) or on an edge (a barycentric within 1e-5
+(t ties of coplanar triangles, within 1e-6 relative) or on an edge (a barycentric within 1e-5
 of 0), where the watertight test and Moller-Trumbore may disagree on inside /
 outside.  Shadow rays test with the reference's Moller-Trumbore itself.
 """
@@ -70,7 +70,10 @@ def test_trace_matches_reference_hlbvh(R, scene, accel):
     same = tri_g == tri_r
     bad = ~same
     edge = np.minimum(np.minimum(u_r, v_r), 1 - u_r - v_r) < 1e-5
-    tie = (tri_g >= 0) & (tri_r >= 0) & (t_g == t_r)
+    # a tie: both hit at the same distance within 1e-6 relative (coplanar
+    # triangles -- the Cornell boxes stand on the floor -- give their plane's
+    # t rounded through different vertices)
+    tie = (tri_g >= 0) & (tri_r >= 0) & (np.abs(t_g - t_r) <= 1e-6 * np.abs(t_r))
     assert np.all(tie[bad] | edge[bad]), f"{np.sum(bad & ~tie & ~edge)} mismatches that are neither ties nor edges"
     rate = same.mean()
     print(f"{scene} accel {accel}: triangle ids equal to the reference HLBVH on {rate:.5f} of {len(rays)} rays "

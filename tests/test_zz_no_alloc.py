@@ -25,19 +25,16 @@ RTOL = 1e-5
 
 
 def _take_free_memory(keep_bytes: int):
-    """Hold device memory until less than keep_bytes is free (a cudaMalloc of
-    the film the allocating path needs cannot succeed then)."""
+    """Hold device memory in shrinking chunks until less than 2 * keep_bytes
+    is free: an allocation of more than that cannot succeed then."""
     torch.cuda.empty_cache()
     held = []
-    chunk = 8 << 30
-    while chunk >= (2 << 20):
-        free, _ = torch.cuda.mem_get_info()
-        if free <= keep_bytes:
-            break
-        try:
-            held.append(torch.empty(min(chunk, free - keep_bytes // 2), dtype=torch.uint8, device="cuda"))
-        except torch.OutOfMemoryError:
-            chunk //= 2
+    for chunk in (8 << 30, 1 << 30, 128 << 20, 16 << 20, 2 << 20):
+        while torch.cuda.mem_get_info()[0] - chunk >= keep_bytes:
+            try:
+                held.append(torch.empty(chunk, dtype=torch.uint8, device="cuda"))
+            except torch.OutOfMemoryError:
+                break
     return held
 
 
@@ -48,25 +45,29 @@ def test_static_scratch_render_matches_allocating_entry_point():
     gs = hk.Scene.from_desc(sd)
     gs.set_image_form(hk.FORM_MEGAKERNEL)   # the same kernel as the static entry point
     ref, ref_ctr = gs.render_image(64, sd.depth, seed=11)
-    # a second scene that has not rendered yet: its first render_image must
-    # allocate a film (built here, before the device memory is taken)
-    fresh = hk.Scene.from_desc(sd)
+    # a second scene, 1024 x 1024, that has not rendered yet: its first
+    # render_image must allocate a 17 MB film (built here, before the device
+    # memory is taken)
+    big = scenes.cornell_box(width=1024, height=1024)
+    fresh = hk.Scene.from_desc(big)
     fresh.set_image_form(hk.FORM_MEGAKERNEL)
-    film_bytes = (w + 4) * (h + 4) * 16
     for call in range(2):
         out = torch.full((h, w, 3), -1.0, dtype=torch.float32, device="cuda")
         ctr = torch.zeros(5, dtype=torch.int64, device="cuda")
         held = []
-        if call == 1:
-            # the second call runs with the device's free memory taken: an
-            # allocation of the film fails there (shown on the allocating path)
-            held = _take_free_memory(film_bytes // 2)
-            with pytest.raises(hk.HikariError):
-                fresh.render_image(1, sd.depth, seed=11)
-        gs.render_image_static(out, 64, sd.depth, seed=11, counters=ctr)
-        torch.cuda.synchronize()
-        del held
-        torch.cuda.empty_cache()
+        try:
+            if call == 1:
+                # the second call runs with the device's free memory taken (less
+                # than 8 MB left): the allocating path fails there
+                held = _take_free_memory(4 << 20)
+                assert torch.cuda.mem_get_info()[0] < (8 << 20)
+                with pytest.raises(hk.HikariError):
+                    fresh.render_image(1, big.depth, seed=11)
+            gs.render_image_static(out, 64, sd.depth, seed=11, counters=ctr)
+            torch.cuda.synchronize()
+        finally:
+            del held
+            torch.cuda.empty_cache()
         img = out.cpu().numpy()
         ok = rel_close(img, ref, RTOL, atol=1e-6 * float(np.abs(ref).max()))
         assert ok.all(), f"call {call}: {np.sum(~ok)} pixels differ beyond {RTOL}"
