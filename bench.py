@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--jobs", type=int, default=400, help="serving: jobs of the Poisson run")
     ap.add_argument("--load", type=float, default=0.8, help="serving: arrival rate as a fraction of the peak")
     ap.add_argument("--capacity", type=int, default=1 << 19, help="serving: path slots of each scene's pool")
+    ap.add_argument("--policy", default="srpt_across", choices=["srpt", "fifo", "srpt_across"],
+                    help="serving: dispatch policy (SRPT within a scene; srpt_across also gates scenes)")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--res", type=int, default=0)
@@ -346,7 +348,8 @@ def run_serving(args):
     tris = [int(g.info.n_triangles) for g in gss]
     rng = np.random.default_rng(7)
     depths = [sd.depth for sd in sds]
-    with serving.Server(capacity=args.capacity, iterations_per_poll=4) as srv:
+    policy = {"srpt": serving.SRPT, "fifo": serving.FIFO, "srpt_across": serving.SRPT_ACROSS}[args.policy]
+    with serving.Server(capacity=args.capacity, iterations_per_poll=4, policy=policy) as srv:
         for g in gss:
             srv.add_scene(g)
         for k in range(len(gss)):   # engines and graphs of every scene (untimed)
@@ -391,7 +394,7 @@ def run_serving(args):
         "config": {"workload": "serving: Poisson arrivals over 8 resident scenes (Cornell box, mesh-heavy 1.31M tris, "
                                "heterogeneous 4.75M tris, 5 heterogeneous variants); jobs of 256/512/1024 px "
                                "square at 16/64/256 spp",
-                   "form": "wavefront serving loop (continuous batching, SRPT dispatch)", "triangles": tris,
+                   "form": f"wavefront serving loop (continuous batching, {args.policy} dispatch)", "triangles": tris,
                    "scene_build_s": round(build_s, 2), "capacity": args.capacity, "jobs": args.jobs,
                    "load": args.load},
         "serving": {

@@ -51,6 +51,7 @@ struct Job {
     bool out_pinned = false;
     hk::JobSize size{};
     uint64_t work = 0, dispensed = 0, paths = 0;
+    uint64_t finished_seen = 0;  // work items finished at the last poll of its engine
     int state = HK_JOB_QUEUED;   // published state (under the server mutex)
     int phase = 0;               // server thread: 0 queued, 1 rendering, 2 copying out, 3 ended
     bool cancel = false;         // under the server mutex
@@ -272,19 +273,30 @@ void hk_server::launch(const std::vector<SceneEntry *> &sc) {
     const SceneEntry *urgent = nullptr;
     uint64_t least = UINT64_MAX;
     int busy = 0;
-    for (SceneEntry *ep : sc) {
+    // remaining work of each scene's least job: undispensed plus in flight
+    // (work - finished), for the across-scenes gate
+    std::vector<uint64_t> scene_least(sc.size(), UINT64_MAX);
+    uint64_t global_least = UINT64_MAX;
+    for (size_t k = 0; k < sc.size(); ++k) {
+        SceneEntry *ep = sc[k];
         bool any = false;
         for (Job *j : ep->jobs)
             if (j->phase == 1) {
                 any = true;
                 const uint64_t rem = j->work - j->dispensed;
                 if (rem < least) { least = rem; urgent = ep; }
+                const uint64_t left = j->work - std::min<uint64_t>(j->finished_seen, j->work);
+                scene_least[k] = std::min(scene_least[k], left);
             }
         busy += any ? 1 : 0;
+        global_least = std::min(global_least, scene_least[k]);
     }
-    for (SceneEntry *ep : sc) {
-        SceneEntry &e = *ep;
+    for (size_t k = 0; k < sc.size(); ++k) {
+        SceneEntry &e = *sc[k];
         if (!e.eng || e.inflight) continue;
+        if (cfg.policy == HK_SERVE_SRPT_ACROSS && scene_least[k] != UINT64_MAX &&
+            scene_least[k] > (uint64_t)HK_SERVE_GATE * global_least)
+            continue;   // waits while a much smaller job of another scene renders
         std::vector<Job *> rendering;
         for (Job *j : e.jobs)
             if (j->phase == 1) rendering.push_back(j);
@@ -351,6 +363,7 @@ bool hk_server::poll(const std::vector<SceneEntry *> &sc) {
             for (Job *j : snapshot) {
                 if (j->phase != 1) continue;
                 const uint64_t f = fin[j->slot];
+                j->finished_seen = f;
                 bool cancel;
                 {
                     std::lock_guard<std::mutex> lk(mu);
@@ -483,7 +496,8 @@ int hk_server_create(const hk_server_config *cfg, hk_server **out) {
         if (c.iterations_per_poll <= 0) c.iterations_per_poll = 4;
         if (c.max_jobs <= 0) c.max_jobs = 256;
         if (c.max_jobs > hk::kWfMaxJobs) throw HkError{HK_ERR_INVALID, "max_jobs above 1024"};
-        if (c.policy != HK_SERVE_SRPT && c.policy != HK_SERVE_FIFO) throw HkError{HK_ERR_INVALID, "unknown policy"};
+        if (c.policy != HK_SERVE_SRPT && c.policy != HK_SERVE_FIFO && c.policy != HK_SERVE_SRPT_ACROSS)
+            throw HkError{HK_ERR_INVALID, "unknown policy"};
         if (c.capacity < 1024 || c.capacity > (1 << 26)) throw HkError{HK_ERR_INVALID, "capacity outside [1024, 2^26]"};
         s->ec.capacity = c.capacity;
         s->ec.threads_extend = c.threads_extend;

@@ -336,6 +336,12 @@ typedef struct hk_server hk_server;
 
 #define HK_SERVE_SRPT 0   /* dispatch the job with the least undispensed work first */
 #define HK_SERVE_FIFO 1   /* dispatch jobs in arrival order */
+/* SRPT within and across scenes: a scene's engine runs only while its job
+ * with the least remaining work (undispensed plus in flight) has at most
+ * HK_SERVE_GATE times the remaining work of the least job of any scene, so a
+ * small job is not slowed by large jobs of other scenes sharing the GPU. */
+#define HK_SERVE_SRPT_ACROSS 2
+#define HK_SERVE_GATE 4
 
 #define HK_JOB_QUEUED 0
 #define HK_JOB_RUNNING 1
@@ -348,7 +354,7 @@ typedef struct {
     int32_t threads_extend;       /* 0 = 128 */
     int32_t threads_shade;        /* 0 = 128 */
     int32_t iterations_per_poll;  /* wavefront iterations between host polls (0 = 4) */
-    int32_t policy;               /* HK_SERVE_SRPT or HK_SERVE_FIFO */
+    int32_t policy;               /* HK_SERVE_SRPT, HK_SERVE_FIFO or HK_SERVE_SRPT_ACROSS */
     int32_t max_jobs;             /* jobs admitted at once per scene (0 = 256, max 1024) */
     uint64_t hbm_budget;          /* device bytes for pools, films and images (0 = 90% of free at create) */
 } hk_server_config;

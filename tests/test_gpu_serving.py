@@ -49,10 +49,11 @@ def _requests(sds):
             (2, 80, 80, 48, 15), (1, 128, 96, 16, 16)]
 
 
-def test_same_alone_and_in_mix(resident):
+@pytest.mark.parametrize("policy", [serving.SRPT, serving.SRPT_ACROSS])
+def test_same_alone_and_in_mix(resident, policy):
     sds, gss = resident
     reqs = _requests(sds)
-    with serving.Server(capacity=1 << 16, iterations_per_poll=4) as srv:
+    with serving.Server(capacity=1 << 16, iterations_per_poll=4, policy=policy) as srv:
         ids = [srv.add_scene(g) for g in gss]
         assert ids == [0, 1, 2]
         alone = []
