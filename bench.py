@@ -702,6 +702,19 @@ def main():
         torch.cuda.synchronize()
         plain = {"mpaths_per_s": W * H * ps / (e0.elapsed_time(e1) / 1e3) / 1e6,
                  "sample": f"view 0, {W}x{H} x {ps} spp, render_pathmis_kernel"}
+    # the drop-in call a pathMISCuda plugin's RenderImage makes (hk_render_image:
+    # host image out, the wavefront at this size with the autotuned configuration)
+    drop_in = None
+    if wave and rank == 0:
+        gs.set_wavefront_config(tuned)
+        img = np.empty((H, W, 3), np.float32)
+        gs.render_image(spp, depth, seed=6, out=img, camera=cams[0])   # untimed: first call allocates the film
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        gs.render_image(spp, depth, seed=7, out=img, camera=cams[0])
+        dt = time.perf_counter() - t0
+        drop_in = {"mpaths_per_s": W * H * spp / dt / 1e6,
+                   "sample": f"hk_render_image, view 0, {W}x{H} x {spp} spp, host image out, wall clock"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -744,6 +757,7 @@ def main():
         "phase_share": phase_share,
         "traversal": traversal,
         "plain_megakernel": plain,
+        "drop_in_render_image": drop_in,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "peak_kind": peak_kind, "basis": basis,
                      "traffic_basis": ("DRAM bytes per ray from one ncu capture of the 1-view 4-spp case, scaled by "

@@ -129,6 +129,16 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
         ray.tmax = __int_as_float(0x7f800000);
         beta = beta * F;
         if (is_zero(beta)) break;
+        // Russian roulette (PathMISIntegrator.cpp:142-151) and the depth bound
+        // before the continuation ray is traced: the reference traces first and
+        // ends the path afterwards, discarding the hit; the trace draws no
+        // random numbers, so the stream is consumed in the same order
+        if (depth >= rr_start) {
+            if (rng.nextf() < 0.95f) beta = beta * (1.0f / 0.95f);
+            else break;
+        }
+        ++depth;
+        if (depth >= depth_max) break;   // the next hit would not be shaded
         pc.rays++;
         found_next = trace<kAccel, false>(S, ray, hn, pc.trav);
         if (found_next) {
@@ -147,11 +157,6 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
             }
         }
         if (br.measure == kMeasureDiscrete) { w_ems = 0.0f; w_mats = 1.0f; }
-        if (depth >= rr_start) {
-            if (rng.nextf() < 0.95f) beta = beta * (1.0f / 0.95f);
-            else break;
-        }
-        ++depth;
     }
     return L;
 }

@@ -143,7 +143,9 @@ def test_render_image_forms_agree():
     assert abs(a.sum() / b.sum() - 1) < 1e-4
     assert np.allclose(b, c, rtol=1e-5, atol=1e-6 * scale)   # auto picks the wavefront at this size
     m, w = ctrs[hk.FORM_MEGAKERNEL], ctrs[hk.FORM_WAVEFRONT]
-    assert abs(int(m[0]) - int(w[0])) <= 2e-3 * m[0] and abs(int(m[1]) - int(w[1])) <= 2e-3 * m[1]
+    print("counters megakernel", m, "wavefront", w)
+    # both end a path by Russian roulette before tracing its continuation ray
+    assert abs(int(m[0]) - int(w[0])) <= 1e-3 * m[0] and abs(int(m[1]) - int(w[1])) <= 1e-3 * m[1]
     # an autotuned configuration is kept for render_image
     gs.autotune(4, sd.depth)
     gs.set_image_form(hk.FORM_AUTO)
