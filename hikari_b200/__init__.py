@@ -22,6 +22,8 @@ DATA_DIR = os.path.join(HERE, "data")
 
 HK_OK = 0
 ACCEL_BVH2, ACCEL_BVH8 = 0, 1
+# where Scene.from_desc builds the trees (HK_BUILDER_*)
+BUILDER_HOST, BUILDER_GPU = 0, 1
 # forms of Scene.render_image (HK_FORM_*)
 FORM_AUTO, FORM_MEGAKERNEL, FORM_WAVEFRONT = 0, 1, 2
 
@@ -146,6 +148,9 @@ def lib():
         "hk_scene_set_accel": ([P, I32], C.c_int),
         "hk_scene_set_image_form": ([P, I32], C.c_int),
         "hk_scene_set_wavefront_config": ([P, C.POINTER(WavefrontConfig)], C.c_int),
+        "hk_scene_set_builder": ([P, I32], C.c_int),
+        "hk_scene_tree_build_seconds": ([P, C.POINTER(C.c_double)], C.c_int),
+        "hk_bvh_check_gpu": ([P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)], C.c_int),
         "hk_bvh_check": ([P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
                          C.c_int),
         "hk_scene_get_info": ([P, C.POINTER(SceneInfo)], C.c_int),
@@ -271,7 +276,7 @@ class Scene:
 
     # ------------------------------------------------------------ construction
     @classmethod
-    def from_desc(cls, desc: SceneDesc) -> "Scene":
+    def from_desc(cls, desc: SceneDesc, builder: int = BUILDER_HOST) -> "Scene":
         L = lib()
         h = C.c_void_p()
         check(L.hk_scene_create(C.byref(h)))
@@ -343,6 +348,7 @@ class Scene:
             check(L.hk_scene_set_filter(h, f.kind, f.radius, f.p0, f.p1))
             bg = _f32(desc.background)
             check(L.hk_scene_set_background(h, bg.ctypes.data, int(desc.force_background)))
+            check(L.hk_scene_set_builder(h, builder))
             check(L.hk_scene_build(h))
         except Exception:
             L.hk_scene_destroy(h)
@@ -395,6 +401,12 @@ class Scene:
                             cfg.get("fetch_min_idle", 0), cfg.get("fetch_steps_shadow", 0),
                             cfg.get("fetch_min_idle_shadow", 0), cfg.get("reg_lean", 0))
         check(lib().hk_scene_set_wavefront_config(self.h, C.byref(c)))
+
+    def tree_build_seconds(self) -> float:
+        """Seconds the scene's last build spent on its trees."""
+        s = C.c_double()
+        check(lib().hk_scene_tree_build_seconds(self.h, C.byref(s)))
+        return s.value
 
     def set_accel(self, accel: int) -> None:
         """Traverse the binary tree (ACCEL_BVH2) or the compressed 8-wide tree (ACCEL_BVH8)."""
@@ -634,6 +646,15 @@ def bvh_check(tris: np.ndarray):
     a, b, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
     check(lib().hk_bvh_check(t.ctypes.data, t.shape[0], C.byref(a), C.byref(b), C.byref(c)))
     return a.value, b.value, c.value
+
+
+def bvh_check_gpu(tris: np.ndarray):
+    """Build the 8-wide tree over tris (n x 3 x 3 float32) on the device and
+    check it; returns (8-wide nodes, 8-wide depth)."""
+    t = np.ascontiguousarray(tris, np.float32).reshape(-1, 9)
+    a, b = C.c_uint32(), C.c_uint32()
+    check(lib().hk_bvh_check_gpu(t.ctypes.data, t.shape[0], C.byref(a), C.byref(b)))
+    return a.value, b.value
 
 
 def obj_load(path: str, to_world=None):

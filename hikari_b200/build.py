@@ -20,7 +20,7 @@ LIB = os.path.join(OUT_DIR, "libhikari_b200.so")
 SOURCES = ["hk_render_b8.cu", "hk_render_b8t.cu", "hk_render_b2.cu", "hk_render_b2t.cu", "hk_wf_shade_3.cu",
            "hk_wf_shade_2.cu", "hk_wf_shade_1.cu", "hk_wf_shade_0.cu", "hk_wf_shade_4.cu", "hk_wf_shade_5.cu", "hk_wf_trace_8.cu", "hk_wf_trace_2.cu",
            "hk_batch_0.cu", "hk_batch_1.cu", "hk_batch_2.cu", "hk_batch_3.cu", "hk_batch_4.cu",
-           "hk_kernels.cu", "hk_wavefront.cu", "hk_host.cpp", "hk_engine.cpp", "hk_server.cpp", "hk_bvh.cpp", "hk_xml.cpp",
+           "hk_kernels.cu", "hk_wavefront.cu", "hk_lbvh.cu", "hk_host.cpp", "hk_engine.cpp", "hk_server.cpp", "hk_bvh.cpp", "hk_xml.cpp",
            "hk_obj.cpp", "hk_mipmap.cpp", "hk_image.cpp"]
 HEADERS = ["hk_megakernel.cuh", "hk_batch.cuh", "hk_wf_kernels.cuh", "hk_device.h", "hk_math.cuh", "hk_bsdf.cuh", "hk_traverse.cuh", "hk_shading.cuh", "hk_kernels.h",
            "hk_bvh.h", "hk_xml.h", "hk_wavefront.h", "hk_engine.h", "hk_hostutil.h", "hk_internal.h", "hk_obj.h", "hk_mipmap.h"]

@@ -596,17 +596,16 @@ BvhPair build_bvh_pair(const float *tris, uint32_t n) {
     return P;
 }
 
-std::string check_bvh_pair(const BvhPair &P, const float *tris, uint32_t n) {
-    const std::vector<uint32_t> &order = P.bvh2.tri_order;
+std::string check_bvh8(const std::vector<uint32_t> &W, const std::vector<uint32_t> &order, const float *tris,
+                       uint32_t n) {
     if (order.size() != n) return "triangle order has the wrong size";
     std::vector<uint8_t> seen(n, 0);
     for (uint32_t o : order) {
         if (o >= n || seen[o]) return "triangle order is not a permutation";
         seen[o] = 1;
     }
-    // ---- 8-wide tree
-    const std::vector<uint32_t> &W = P.bvh8.nodes;
     const uint32_t nw = (uint32_t)(W.size() / 20);
+    if (nw == 0) return "8-wide tree is empty";
     std::vector<uint8_t> tri_ref(n, 0), node_ref(nw, 0);
     struct Item {
         uint32_t node;
@@ -670,6 +669,12 @@ std::string check_bvh_pair(const BvhPair &P, const float *tris, uint32_t n) {
         if (!tri_ref[i]) return "8-wide tree misses a triangle";
     for (uint32_t i = 0; i < nw; i++)
         if (!node_ref[i]) return "8-wide tree has an unreachable node";
+    return std::string();
+}
+
+std::string check_bvh_pair(const BvhPair &P, const float *tris, uint32_t n) {
+    const std::string e8 = check_bvh8(P.bvh8.nodes, P.bvh2.tri_order, tris, n);
+    if (!e8.empty()) return e8;
     // ---- binary tree: leaves cover the order once
     std::vector<uint8_t> tri2(n, 0);
     const std::vector<float> &B = P.bvh2.nodes;

@@ -50,5 +50,8 @@ BvhPair build_bvh_pair(const float *tris, uint32_t ntris);
 // contains its subtree's triangles, child indices are in range.  Returns an
 // empty string when the trees are consistent, else the first problem found.
 std::string check_bvh_pair(const BvhPair &P, const float *tris, uint32_t ntris);
+// The 8-wide part of that check for nodes over the triangle order `order`.
+std::string check_bvh8(const std::vector<uint32_t> &nodes, const std::vector<uint32_t> &order, const float *tris,
+                       uint32_t ntris);
 
 }  // namespace hk

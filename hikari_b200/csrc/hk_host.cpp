@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,7 @@
 #include "hk_engine.h"
 #include "hk_internal.h"
 #include "hk_kernels.h"
+#include "hk_lbvh.h"
 #include "hk_mipmap.h"
 #include "hk_wavefront.h"
 
@@ -238,6 +240,8 @@ struct hk_scene {
     int sm_count = 148;
     int device = 0;   // CUDA device the scene was built on
     int image_form = HK_FORM_AUTO;             // form hk_render_image renders with
+    int builder = HK_BUILDER_HOST;             // where hk_scene_build builds the trees
+    double tree_build_s = 0.0;                 // seconds of the last tree build
     bool has_wf_cfg = false;                   // wf_cfg was set (autotuner or caller)
     hk_wavefront_config wf_cfg{};              // wavefront configuration of hk_render_image
     int occupancy = 1;        // resident megakernel CTAs per SM for the traversed tree
@@ -589,6 +593,36 @@ void build_scene(hk_scene *s) {
     if (any_uv) { s->b_tri_uv.upload(tri_uv); track(s->b_tri_uv); }
     D.tri_uv = s->b_tri_uv.as<float2>();
 
+    const auto t_tree = std::chrono::steady_clock::now();
+    uint32_t tree_depth2 = 0, tree_depth8 = 0;
+    if (s->builder == HK_BUILDER_GPU) {
+        // the 8-wide tree built on the device (no binary tree)
+        if (s->accel != HK_ACCEL_BVH8) throw HkError{HK_ERR_INVALID, "the device builder makes the 8-wide tree only"};
+        DevBuf dP, dmesh;
+        dP.upload(P);
+        dmesh.upload(tmesh);
+        hk::GpuBvh8 G;
+        hk::build_bvh8_gpu(dP.as<float>(), (uint32_t)ntris, nullptr, G);
+        s->b_tris.alloc((size_t)ntris * 48);
+        hk::gather_tri_records(dP.as<float>(), dmesh.as<int32_t>(), G.order.as<uint32_t>(), (uint32_t)ntris,
+                               s->b_tris.as<float>(), nullptr);
+        HK_CUDA(cudaDeviceSynchronize());
+        track(s->b_tris);
+        s->b_nodes.release();
+        s->b_wnodes.take(G.nodes);
+        track(s->b_wnodes);
+        D.tris = s->b_tris.as<float4>();
+        D.nodes = nullptr;
+        D.nnodes = 0;
+        D.ntris = (uint32_t)ntris;
+        D.wnodes = s->b_wnodes.as<uint4>();
+        D.nwnodes = G.nnodes;
+        tree_depth8 = G.depth;
+        D.postpone = 2 * (int)G.depth + 2 <= hk::kStackSize ? 1 : 0;
+        if ((int)G.depth + 1 > hk::kStackSize) throw HkError{HK_ERR_INVALID, "8-wide BVH too deep"};
+        D.accel = s->accel;
+        s->tree_build_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_tree).count();
+    } else {
     // BVH: one binned-SAH build, packed as the binary tree and collapsed into
     // the compressed 8-wide tree over one triangle order
     hk::BvhPair pair = hk::build_bvh_pair(P.data(), (uint32_t)ntris);
@@ -615,9 +649,13 @@ void build_scene(hk_scene *s) {
     D.nwnodes = (uint32_t)(pair.bvh8.nodes.size() / 20);
     // the traversal stack holds at most one node group and one postponed
     // triangle group per level (plus the root)
+    tree_depth2 = bvh.depth;
+    tree_depth8 = pair.bvh8.depth;
     D.postpone = 2 * (int)pair.bvh8.depth + 2 <= hk::kStackSize ? 1 : 0;
     if ((int)pair.bvh8.depth + 1 > hk::kStackSize) throw HkError{HK_ERR_INVALID, "8-wide BVH too deep"};
     D.accel = s->accel;
+    s->tree_build_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_tree).count();
+    }
 
     // emitters (Scene order)
     std::vector<int32_t> emitter_area;
@@ -783,9 +821,9 @@ void build_scene(hk_scene *s) {
     I.n_bsdfs = (uint32_t)bs.size();
     I.n_emitters = (uint32_t)emitter_area.size();
     I.n_bvh_nodes = D.nnodes;
-    I.bvh_depth = bvh.depth;
+    I.bvh_depth = tree_depth2;
     I.n_wide_nodes = D.nwnodes;
-    I.wide_depth = pair.bvh8.depth;
+    I.wide_depth = tree_depth8;
     I.accel = D.accel;
     I.postpone = D.postpone;
     I.env_index = D.env_index;
@@ -1080,9 +1118,44 @@ int hk_bvh_check(const float *tris, uint32_t n, uint32_t *n_bvh_nodes, uint32_t 
         return HK_OK;
     });
 }
+int hk_scene_set_builder(hk_scene *s, int32_t builder) {
+    return guarded([&] {
+        if (!s || (builder != HK_BUILDER_HOST && builder != HK_BUILDER_GPU)) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        s->builder = builder;
+        s->built = false;
+        return HK_OK;
+    });
+}
+int hk_scene_tree_build_seconds(const hk_scene *s, double *seconds) {
+    return guarded([&] {
+        if (!s || !seconds) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        *seconds = s->tree_build_s;
+        return HK_OK;
+    });
+}
+int hk_bvh_check_gpu(const float *tris, uint32_t n, uint32_t *n_wide_nodes, uint32_t *wide_depth) {
+    return guarded([&] {
+        if (!tris || n == 0) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        DevBuf dP;
+        dP.alloc((size_t)n * 9 * sizeof(float));
+        HK_CUDA(cudaMemcpy(dP.p, tris, dP.bytes, cudaMemcpyHostToDevice));
+        hk::GpuBvh8 G;
+        hk::build_bvh8_gpu(dP.as<float>(), n, nullptr, G);
+        std::vector<uint32_t> nodes((size_t)G.nnodes * 20), order(n);
+        HK_CUDA(cudaMemcpy(nodes.data(), G.nodes.p, nodes.size() * 4, cudaMemcpyDeviceToHost));
+        HK_CUDA(cudaMemcpy(order.data(), G.order.p, order.size() * 4, cudaMemcpyDeviceToHost));
+        const std::string err = hk::check_bvh8(nodes, order, tris, n);
+        if (!err.empty()) throw HkError{HK_ERR_INVALID, err};
+        if (n_wide_nodes) *n_wide_nodes = G.nnodes;
+        if (wide_depth) *wide_depth = G.depth;
+        return HK_OK;
+    });
+}
 int hk_scene_set_accel(hk_scene *s, int32_t accel) {
     return guarded([&] {
         if (!s || (accel != HK_ACCEL_BVH2 && accel != HK_ACCEL_BVH8)) throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (accel == HK_ACCEL_BVH2 && s->built && s->dev.nnodes == 0)
+            throw HkError{HK_ERR_INVALID, "the scene was built on the device: it has the 8-wide tree only"};
         s->accel = accel;
         s->dev.accel = accel;
         s->info.accel = accel;

@@ -75,6 +75,14 @@ struct DevBuf {
     }
     template <class T>
     T *as() const { return (T *)p; }
+    // take over o's allocation (o ends empty)
+    void take(DevBuf &o) {
+        release();
+        p = o.p;
+        bytes = o.bytes;
+        o.p = nullptr;
+        o.bytes = 0;
+    }
 };
 
 // Owning pinned host allocation.

@@ -183,8 +183,25 @@ int hk_scene_set_background(hk_scene *s, const float *rgb3, int force_background
 /* Activate every object and upload (Scene::Activate src/core/Scene.cpp:128 +
  * Integrator::Preprocess): BSDF tables, light CDFs, the BVH, device buffers. */
 int hk_scene_build(hk_scene *s);
+/* Where hk_scene_build builds the trees.  HK_BUILDER_HOST (default): the
+ * binned-SAH binary tree and its SAH-optimal 8-wide collapse on the host
+ * threads (the reference builds its HLBVH on the host too,
+ * src/acceleration/HLBVHAcceleration.cpp:81).  HK_BUILDER_GPU: the 8-wide tree
+ * only, built on the device from Morton-ordered triangles (a linear BVH
+ * collapsed greedily): milliseconds instead of seconds for millions of
+ * triangles, for scenes that must become renderable fast, at some cost in
+ * traversal work; the scene then traverses the 8-wide tree only. */
+enum { HK_BUILDER_HOST = 0, HK_BUILDER_GPU = 1 };
+int hk_scene_set_builder(hk_scene *s, int32_t builder);
+/* Seconds the last hk_scene_build spent building (and uploading) its trees. */
+int hk_scene_tree_build_seconds(const hk_scene *s, double *seconds);
+/* Build the device 8-wide tree over n triangles (9 floats each, host) and run
+ * hk_bvh_check's structural check of the 8-wide tree on it (HK_ERR_INVALID
+ * with the first problem found). */
+int hk_bvh_check_gpu(const float *tris, uint32_t n, uint32_t *n_wide_nodes, uint32_t *wide_depth);
 /* Select the tree the render and trace kernels traverse (takes effect
- * immediately on a built scene; both trees share one triangle order). */
+ * immediately on a built scene; both trees share one triangle order; a scene
+ * built with HK_BUILDER_GPU has the 8-wide tree only). */
 int hk_scene_set_accel(hk_scene *s, int32_t accel);
 /* Counts and bbox; before hk_scene_build the BVH and device fields are 0. */
 int hk_scene_get_info(const hk_scene *s, hk_scene_info *info);
