@@ -559,6 +559,14 @@ def main():
     t0 = time.perf_counter()
     gs = hk.Scene.from_desc(sd)
     build_s = time.perf_counter() - t0
+    tree_s = {"host": round(gs.tree_build_seconds(), 4)}
+    if rank == 0:   # the device builder on the same scene (untimed set-up; the second build is reported)
+        for _ in range(2):
+            g2 = hk.Scene.from_desc(sd, builder=hk.BUILDER_GPU)
+            tree_s["device"] = round(g2.tree_build_seconds(), 4)
+            tree_s["device_wide_nodes"] = int(g2.info.n_wide_nodes)
+            del g2
+        torch.cuda.synchronize()
     gs.set_accel(hk.ACCEL_BVH8 if args.accel == "bvh8" else hk.ACCEL_BVH2)
     accel_name = args.accel
     node_b = 80.0 if args.accel == "bvh8" else 64.0
@@ -748,7 +756,7 @@ def main():
                    "triangles": int(gs.info.n_triangles), "accel": args.accel,
                    "bvh_nodes": int(gs.info.n_bvh_nodes), "wide_nodes": int(gs.info.n_wide_nodes),
                    "wide_depth": int(gs.info.wide_depth),
-                   "scene_build_s": round(build_s, 2), "wavefront": tuned or None,
+                   "scene_build_s": round(build_s, 2), "tree_build_s": tree_s, "wavefront": tuned or None,
                    "autotune_probe_ms": tune_ms,
                    "l2": "256 MiB buffer written between timed steps (outside the step events)",
                    "rr": "reference rule: p=0.95 at every bounce"},
