@@ -85,30 +85,39 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
             V3 ld = emitter_sample(S, e, er, ux, uy, u1);
             float pl = er.pdf;
             if (!is_zero(ld)) {
-                Ray sr;
-                sr.o = it.p; sr.d = er.p - it.p; sr.tmin = kRayEps; sr.tmax = 1.0f - kRayEps;
-                Hit sh;
-                pc.shadow++;
-                if (!trace<kAccel, true>(S, sr, sh, pc.trav)) {
-                    BRec br;
-                    br.wi = to_local(it.sh, ray.d * -1.0f);
-                    br.wo = to_local(it.sh, er.wi);
-                    br.measure = kMeasureSolidAngle;
-                    br.eta = 0.0f;
-                    br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv;
-                    float pb;
-                    V3 f;
-                    if constexpr (kTex) {
-                        pb = bsdf_pdf_b(S.bsdfs, bsdf, br, bf);
-                        f = bsdf_eval_b(S.bsdfs, bsdf, br, bf);
-                    } else {
-                        pb = bsdf_pdf(S.bsdfs, bsdf, br);
-                        f = bsdf_eval(S.bsdfs, bsdf, br);
+                // the BSDF term first, the shadow ray only for a non-zero
+                // contribution (an occluded ray adds nothing either way; the
+                // reference updates WeightEMS only for an unoccluded ray, and
+                // every use recomputes it, as the emitter pdf of a non-zero
+                // sample is positive)
+                BRec br;
+                br.wi = to_local(it.sh, ray.d * -1.0f);
+                br.wo = to_local(it.sh, er.wi);
+                br.measure = kMeasureSolidAngle;
+                br.eta = 0.0f;
+                br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv;
+                float pb;
+                V3 f;
+                if constexpr (kTex) {
+                    pb = bsdf_pdf_b(S.bsdfs, bsdf, br, bf);
+                    f = bsdf_eval_b(S.bsdfs, bsdf, br, bf);
+                } else {
+                    pb = bsdf_pdf(S.bsdfs, bsdf, br);
+                    f = bsdf_eval(S.bsdfs, bsdf, br);
+                }
+                const float w = (pl + pb != 0.0f) ? pl / (pl + pb) : w_ems;
+                const float c = fabsf(br.wo.z);
+                const V3 contrib = v3((((beta.x * f.x) * c) * ld.x) * w, (((beta.y * f.y) * c) * ld.y) * w,
+                                      (((beta.z * f.z) * c) * ld.z) * w);
+                if (!all_zero(contrib)) {
+                    Ray sr;
+                    sr.o = it.p; sr.d = er.p - it.p; sr.tmin = kRayEps; sr.tmax = 1.0f - kRayEps;
+                    Hit sh;
+                    pc.shadow++;
+                    if (!trace<kAccel, true>(S, sr, sh, pc.trav)) {
+                        w_ems = w;
+                        L = L + contrib;
                     }
-                    if (pl + pb != 0.0f) w_ems = pl / (pl + pb);
-                    float c = fabsf(br.wo.z);
-                    L = L + v3((((beta.x * f.x) * c) * ld.x) * w_ems, (((beta.y * f.y) * c) * ld.y) * w_ems,
-                               (((beta.z * f.z) * c) * ld.z) * w_ems);
                 }
             }
         }

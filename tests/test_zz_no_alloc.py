@@ -45,10 +45,10 @@ def test_static_scratch_render_matches_allocating_entry_point():
     gs = hk.Scene.from_desc(sd)
     gs.set_image_form(hk.FORM_MEGAKERNEL)   # the same kernel as the static entry point
     ref, ref_ctr = gs.render_image(64, sd.depth, seed=11)
-    # a second scene, 1024 x 1024, that has not rendered yet: its first
-    # render_image must allocate a 17 MB film (built here, before the device
+    # a second scene, 2048 x 2048, that has not rendered yet: its first
+    # render_image must allocate a 67 MB film (built here, before the device
     # memory is taken)
-    big = scenes.cornell_box(width=1024, height=1024)
+    big = scenes.cornell_box(width=2048, height=2048)
     fresh = hk.Scene.from_desc(big)
     fresh.set_image_form(hk.FORM_MEGAKERNEL)
     for call in range(2):
@@ -58,9 +58,9 @@ def test_static_scratch_render_matches_allocating_entry_point():
         try:
             if call == 1:
                 # the second call runs with the device's free memory taken (less
-                # than 8 MB left): the allocating path fails there
+                # than 32 MB left): the allocating path fails there
                 held = _take_free_memory(4 << 20)
-                assert torch.cuda.mem_get_info()[0] < (8 << 20)
+                assert torch.cuda.mem_get_info()[0] < (32 << 20)
                 with pytest.raises(hk.HikariError):
                     fresh.render_image(1, big.depth, seed=11)
             gs.render_image_static(out, 64, sd.depth, seed=11, counters=ctr)
