@@ -36,12 +36,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per ray of the
-# 8-wide traversal kernels, from one ncu capture of every extend / shadow launch
-# of `python -m hikari_b200.profiling render --views 1 --spp 4 --accel bvh8`
-# (the heterogeneous scene, pool of 2^22 slots) divided by the rays the render
-# traced; the bench scales them by the rays of its own launches.
-DRAM_BYTES_PER_RAY = {"bvh8": {"extend": 178.0, "shadow": 117.7}}
+# Per-ray figures of the 8-wide traversal kernels from one ncu capture of every
+# extend / shadow launch of `python -m hikari_b200.profiling render --views 1
+# --spp 4 --accel bvh8` with the bench's tuned launch configuration (the
+# heterogeneous scene, pool of 2^22 slots), summed per kernel and divided by the
+# rays the render traced: DRAM bytes (dram__bytes_read.sum +
+# dram__bytes_write.sum), L2 bytes (lts__t_bytes.sum) and warp instructions
+# issued (smsp__inst_executed.sum).  The bench scales them by the rays of its
+# own launches.
+TRAVERSAL_PER_RAY = {"bvh8": {"extend": {"dram": 190.75, "l2": 725.7, "inst": 297.9},
+                              "shadow": {"dram": 125.01, "l2": 744.0, "inst": 264.4}}}
+SMS, SCHEDULERS_PER_SM = 148, 4
+MEASURED_SM_MAX_MHZ = 1965.0
 
 
 def parse():
@@ -58,7 +64,7 @@ def parse():
     ap.add_argument("--jobs", type=int, default=400, help="serving: jobs of the Poisson run")
     ap.add_argument("--load", type=float, default=0.8, help="serving: arrival rate as a fraction of the peak")
     ap.add_argument("--capacity", type=int, default=1 << 19, help="serving: path slots of each scene's pool")
-    ap.add_argument("--policy", default="srpt_across", choices=["srpt", "fifo", "srpt_across"],
+    ap.add_argument("--policy", default="srpt", choices=["srpt", "fifo", "srpt_across"],
                     help="serving: dispatch policy (SRPT within a scene; srpt_across also gates scenes)")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--views", type=int, default=0)
@@ -169,6 +175,27 @@ def slowest_rank_seconds(seconds, device="cuda"):
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def l2_copy_gbs():
+    """L2 bandwidth as a plain copy sees it: a 16 MiB float buffer copied into
+    another (both L2-resident after the first pass), read + write bytes over
+    the best of 20 timed copies."""
+    import torch
+
+    a = torch.ones(4 << 20, device="cuda")
+    b = torch.empty_like(a)
+    for _ in range(5):
+        b.copy_(a)
+    best = float("inf")
+    for _ in range(20):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        b.copy_(a)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    return 2 * a.numel() * 4 / best / 1e9
 
 
 def measured_peaks():
@@ -633,11 +660,10 @@ def main():
         dom = int(np.argmax(kms))
         trav_bytes = {1: pcn[3] * node_b + pcn[4] * 48.0, 3: pcn[5] * node_b + pcn[6] * 48.0}
         traffic = None
-        per_ray = DRAM_BYTES_PER_RAY.get(args.accel, {})
-        if dom == 1 and "extend" in per_ray:
-            traffic = per_ray["extend"] * pcn[0] / max(1, kl[dom])
-        elif dom == 3 and "shadow" in per_ray:
-            traffic = per_ray["shadow"] * pcn[1] / max(1, kl[dom])
+        per_ray = TRAVERSAL_PER_RAY.get(args.accel, {}).get({1: "extend", 3: "shadow"}.get(dom, ""), {})
+        dom_rays = pcn[0] if dom == 1 else pcn[1]
+        if per_ray.get("dram") is not None:
+            traffic = per_ray["dram"] * dom_rays / max(1, kl[dom])
         if dom in trav_bytes:
             bytes_per_launch = trav_bytes[dom] / max(1, kl[dom])
             avg_s = float(kms[dom]) / max(1, kl[dom]) / 1e3
@@ -650,6 +676,27 @@ def main():
             avg_s = float(kms[dom]) / max(1, kl[dom]) / 1e3
             basis = f"{phases[dom]} kernels: path-state bytes (144 B per shaded vertex) per launch"
         achieved = bytes_per_launch / max(avg_s, 1e-12) / 1e9
+        # the traversal kernels are bound by instruction issue and SIMT
+        # divergence, not by DRAM: their issue rate against one warp
+        # instruction per scheduler per cycle, and their L2 bytes against an
+        # L2-resident copy measured here
+        l2_peak = l2_copy_gbs()
+        limiter = {"bound": "hbm"}
+        if per_ray.get("inst") is not None:
+            dom_s = float(kms[dom]) / 1e3
+            issue_rate = per_ray["inst"] * dom_rays / max(dom_s, 1e-12)
+            limiter = {"bound": "issue", "issue": {"achieved_ginst_per_s": issue_rate / 1e9,
+                                                   "inst_per_ray": per_ray["inst"], "sms": SMS,
+                                                   "schedulers_per_sm": SCHEDULERS_PER_SM}}
+        if per_ray.get("l2") is not None:
+            l2_ach = per_ray["l2"] * dom_rays / max(float(kms[dom]) / 1e3, 1e-12) / 1e9
+            limiter["l2"] = {"achieved": l2_ach, "peak": l2_peak, "unit": "GB/s", "frac": l2_ach / l2_peak,
+                             "peak_kind": "measured here: L2-resident copy, 2 x 16 MiB, read + write bytes"}
+        sm_mhz = clk.summary().get("sm_mhz") or MEASURED_SM_MAX_MHZ
+        if "issue" in limiter:
+            peak_ginst = SMS * SCHEDULERS_PER_SM * sm_mhz * 1e6 / 1e9
+            limiter["issue"].update({"peak_ginst_per_s": peak_ginst, "sm_mhz": sm_mhz,
+                                     "frac": limiter["issue"]["achieved_ginst_per_s"] / peak_ginst})
         launches_per_step = int(kl.sum()) + 1
         rays_c, rays_s = max(pcn[0], 1.0), max(pcn[1], 1.0)
         traversal = {"closest": {"node_visits_per_ray": pcn[3] / rays_c, "tri_tests_per_ray": pcn[4] / rays_c,
@@ -668,6 +715,7 @@ def main():
         phase_share = None
         traversal = None
         traffic = None
+        limiter = {"bound": "hbm"}
 
     # end to end through the C ABI: host images out, per-view camera pose in
     e2e_value = None
@@ -766,10 +814,11 @@ def main():
         "traversal": traversal,
         "plain_megakernel": plain,
         "drop_in_render_image": drop_in,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "peak_kind": peak_kind, "basis": basis,
+        "roofline": {"bound": limiter["bound"], "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind, "basis": basis,
                      "traffic_basis": ("DRAM bytes per ray from one ncu capture of the 1-view 4-spp case, scaled by "
-                                       "the rays per launch" if traffic is not None else None)},
+                                       "the rays per launch" if traffic is not None else None),
+                     **{k: v for k, v in limiter.items() if k != "bound"}},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": V * int(hk.C.sizeof(hk.RenderDesc)),
                 "d2h_bytes_per_step": V * W * H * 3 * 4},

@@ -114,6 +114,7 @@ struct DevScene {
     uint32_t ntris, nnodes, nwnodes;
     int32_t accel;                // kAccelBvh2 or kAccelBvh8: the tree the kernels traverse
     int32_t postpone;             // 8-wide traversal may postpone triangle tests (stack bound allows it)
+    int32_t postpone_any;         // ... and does so for any-hit rays too (set per launch, 0 in the scene)
     int32_t textured;             // some material has textures (the megakernel compiles lookups in)
     int32_t ray_diff;             // a bitmap filters with the camera ray's differentials (first hits)
     const DevMesh *meshes;

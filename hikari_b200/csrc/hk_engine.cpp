@@ -72,6 +72,7 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     L_.threads_regen = 256;
     L_.lean_extend = cfg_.reg_lean & 1;
     L_.lean_shadow = (cfg_.reg_lean >> 1) & 1;
+    L_.postpone_shadow = cfg_.postpone_shadow ? 1 : 0;
     auto grid = [&](int which, int threads) {
         const bool lean = which == 0 ? L_.lean_extend : (which == 2 ? L_.lean_shadow : false);
         return std::max(1, sm_count * std::max(1, wf_occupancy(which, threads, S.accel, lean)));

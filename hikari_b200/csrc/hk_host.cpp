@@ -850,7 +850,7 @@ hk::WfEngine &wf_ensure(hk_scene *s, const hk::WfEngineConfig &c) {
         if (o.capacity == c.capacity && o.threads_extend == c.threads_extend && o.threads_shade == c.threads_shade &&
             o.fetch_steps == c.fetch_steps && o.fetch_min_idle == c.fetch_min_idle &&
             o.fetch_steps_shadow == c.fetch_steps_shadow && o.fetch_min_idle_shadow == c.fetch_min_idle_shadow &&
-            o.reg_lean == c.reg_lean)
+            o.reg_lean == c.reg_lean && o.postpone_shadow == c.postpone_shadow)
             return *s->wf;
         s->wf.reset();
     }
@@ -1420,6 +1420,7 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         ec.fetch_steps_shadow = std::max(0, std::min(1024, c.fetch_steps_shadow));
         ec.fetch_min_idle_shadow = c.fetch_min_idle_shadow > 0 ? std::min(32, c.fetch_min_idle_shadow) : 0;
         ec.reg_lean = c.reg_lean & 3;
+        ec.postpone_shadow = c.postpone_shadow ? 1 : 0;
         hk::WfEngine &E = wf_ensure(s, ec);
         cudaStream_t user = (cudaStream_t)stream, st = E.stream();
         // order after the caller's stream (the films may have been cleared there)
@@ -1585,6 +1586,13 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
         c = bc;
         for (int k : min_idle) {
             c.fetch_min_idle_shadow = k;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        // shadow rays postponing their triangle tests (8-wide tree only)
+        if (s->dev.accel == hk::kAccelBvh8 && s->dev.postpone) {
+            c = bc;
+            c.postpone_shadow = 1;
             float ms = run(c);
             if (ms < best_t) { best_t = ms; bc = c; }
         }

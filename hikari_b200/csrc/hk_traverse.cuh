@@ -401,7 +401,7 @@ struct Bvh8Walker {
             tg = ng;   // a postponed triangle group from the stack (or nothing)
             ng = make_uint2(0u, 0u);
         }
-        if (!kAnyHit && S.postpone) {   // a shadow ray wants any hit soon: it never postpones
+        if (kAnyHit ? S.postpone_any : S.postpone) {   // any-hit rays only where the launch asks
             const unsigned act = __activemask();
             const unsigned want = __ballot_sync(act, tg.y != 0u);
             if (tg.y != 0u && ng.y > 0x00ffffffu && __popc(want) * 5 < __popc(act)) {

@@ -119,6 +119,7 @@ struct WfLaunchConfig {
     int fetch_steps, fetch_min_idle;                 // dynamic ray fetch of the extend kernel
     int fetch_steps_shadow, fetch_min_idle_shadow;   // and of the shadow kernel
     int lean_extend, lean_shadow;                    // traversal kernels with the smaller register budget
+    int postpone_shadow;                             // shadow rays postpone triangle tests
 };
 
 // empty pool: every slot idle, queues and statistics zero (the dispatch head is the host's)

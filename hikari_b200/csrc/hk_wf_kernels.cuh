@@ -406,12 +406,14 @@ cudaError_t wf_launch_extend_t(const DevScene &S, const WfState &W, const WfLaun
 template <int kAccel>
 cudaError_t wf_launch_shadow_t(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
     const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(C.threads_shadow) : 0;
+    DevScene SS = S;
+    SS.postpone_any = S.postpone && C.postpone_shadow ? 1 : 0;
     if (C.lean_shadow)
         wf_shadow_kernel<kAccel, kLeanBlocks><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(
-            S, W, C.fetch_steps_shadow, C.fetch_min_idle_shadow);
+            SS, W, C.fetch_steps_shadow, C.fetch_min_idle_shadow);
     else
-        wf_shadow_kernel<kAccel, 0><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(S, W, C.fetch_steps_shadow,
-                                                                                C.fetch_min_idle_shadow);
+        wf_shadow_kernel<kAccel, 0><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(SS, W, C.fetch_steps_shadow,
+                                                                                 C.fetch_min_idle_shadow);
     return cudaGetLastError();
 }
 // which: 0 extend, 2 shadow; lean: the kLeanBlocks register budget

@@ -13,9 +13,11 @@ usage: python -m hikari_b200.profiling launches <launches.csv>
 (no autotuning, no other launches of the traversal kernels; the launch
 configuration is given on the command line, e.g. the one bench.py's
 autotuner picked) and writes its counters as JSON; run under `ncu --metrics dram__bytes_read.sum,
-dram__bytes_write.sum,gpu__time_duration.sum -k regex:"wf_(extend|shadow)"
---cache-control none`, `traffic` turns the per-launch DRAM bytes of that
-capture into DRAM bytes per closest-hit and per shadow ray.
+dram__bytes_write.sum,lts__t_bytes.sum,smsp__inst_executed.sum,
+smsp__thread_inst_executed.sum,gpu__time_duration.sum
+-k regex:"wf_(extend|shadow)" --cache-control none`, `traffic` turns the
+per-launch sums of that capture into DRAM bytes, L2 bytes and warp
+instructions per closest-hit and per shadow ray.
 """
 import csv
 import io
@@ -88,24 +90,43 @@ def _metric_rows(path):
     return [(r[ii], r[ki].split("(")[0], r[ni], float(r[vi].replace(",", "")), r[ui]) for r in data]
 
 
-BYTE_UNIT = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9}
+BYTE_UNIT = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "Tbyte": 1e12}
+INST_UNIT = {"inst": 1.0, "Kinst": 1e3, "Minst": 1e6, "Ginst": 1e9}
 
 
 def traffic(csv_path, render_json):
+    """Per-ray figures of the traversal kernels from a capture of every
+    extend / shadow launch: DRAM bytes (dram__bytes_read.sum +
+    dram__bytes_write.sum), L2 bytes (lts__t_bytes.sum), warp instructions
+    issued (smsp__inst_executed.sum) and active lanes per warp instruction
+    (smsp__thread_inst_executed.sum / smsp__inst_executed.sum), each divided
+    by the rays the render traced (closest-hit rays for extend, shadow rays for
+    shadow)."""
     import json
 
     ctr = json.load(open(render_json))["counters"]
     agg = {}
-    for _, kern, metric, val, unit in _metric_rows(csv_path):
-        a = agg.setdefault(kern, {"launches": set(), "bytes": 0.0, "ms": 0.0})
+    for lid, kern, metric, val, unit in _metric_rows(csv_path):
+        a = agg.setdefault(kern, {"launches": set(), "dram": 0.0, "l2": 0.0, "inst": 0.0, "thread_inst": 0.0,
+                                  "ms": 0.0})
+        a["launches"].add(lid)
         if metric.startswith("dram__bytes"):
-            a["bytes"] += val * BYTE_UNIT[unit]
+            a["dram"] += val * BYTE_UNIT[unit]
+        elif metric == "lts__t_bytes.sum":
+            a["l2"] += val * BYTE_UNIT[unit]
+        elif metric == "smsp__inst_executed.sum":
+            a["inst"] += val * INST_UNIT.get(unit, 1.0)
+        elif metric == "smsp__thread_inst_executed.sum":
+            a["thread_inst"] += val * INST_UNIT.get(unit, 1.0)
         elif metric == "gpu__time_duration.sum":
             a["ms"] += val * UNIT_MS[unit]
-    rows = ["| kernel | DRAM bytes | rays | DRAM bytes per ray | device ms (ncu) |", "|---|---|---|---|---|"]
+    rows = ["| kernel | launches | rays | DRAM bytes per ray | L2 bytes per ray | warp instructions per ray "
+            "| lanes per instruction | device ms (ncu) |", "|---|---|---|---|---|---|---|---|"]
     for kern, a in sorted(agg.items()):
-        rays = ctr["shadow_rays"] if "shadow" in kern else ctr["rays"]
-        rows.append(f"| {kern} | {a['bytes']:.4g} | {rays} | {a['bytes'] / max(rays, 1):.2f} | {a['ms']:.2f} |")
+        rays = max(ctr["shadow_rays"] if "shadow" in kern else ctr["rays"], 1)
+        lanes = a["thread_inst"] / a["inst"] if a["inst"] else float("nan")
+        rows.append(f"| {kern} | {len(a['launches'])} | {rays} | {a['dram'] / rays:.2f} | {a['l2'] / rays:.1f} "
+                    f"| {a['inst'] / rays:.1f} | {lanes:.2f} | {a['ms']:.2f} |")
     return "\n".join(rows)
 
 
@@ -132,6 +153,7 @@ def render(argv):
     ap.add_argument("--fetch-steps-shadow", type=int, default=0)
     ap.add_argument("--fetch-min-idle-shadow", type=int, default=0)
     ap.add_argument("--reg-lean", type=int, default=0)
+    ap.add_argument("--postpone-shadow", type=int, default=0)
     a = ap.parse_args(argv)
     sd = scenes.heterogeneous(width=1024, height=1024, spp=a.spp, depth=16)
     cams = scenes.heterogeneous_cameras(a.views)
@@ -143,7 +165,7 @@ def render(argv):
                     threads_extend=a.threads_extend, threads_shade=a.threads_shade, fetch_steps=a.fetch_steps,
                     fetch_min_idle=a.fetch_min_idle, iterations_per_check=a.iterations_per_check,
                     fetch_steps_shadow=a.fetch_steps_shadow, fetch_min_idle_shadow=a.fetch_min_idle_shadow,
-                    reg_lean=a.reg_lean)
+                    reg_lean=a.reg_lean, postpone_shadow=a.postpone_shadow)
     torch.cuda.synchronize()
     c = [int(x) for x in ctr.cpu().tolist()]
     names = ["rays", "shadow_rays", "dropped", "node_visits", "tri_tests", "node_visits_shadow", "tri_tests_shadow"]

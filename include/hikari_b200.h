@@ -283,6 +283,8 @@ typedef struct {
     int32_t fetch_min_idle_shadow; /*   rays' values */
     int32_t reg_lean;              /* bit 0 / bit 1: the extend / shadow kernel with a register budget of
                                       48 (five resident blocks of 256 threads) instead of the compiler's */
+    int32_t postpone_shadow;       /* 1: shadow rays postpone triangle tests like closest-hit rays (a lane
+                                      keeps visiting nodes while few lanes of its warp have triangles) */
 } hk_wavefront_config;
 
 /* Render every job of the batch with the wavefront integrator: a pool of path
