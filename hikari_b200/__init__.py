@@ -77,7 +77,7 @@ class WavefrontConfig(C.Structure):
                 ("iterations_per_check", C.c_int32), ("no_graph", C.c_int32), ("kernel_ms", C.c_void_p),
                 ("kernel_launches", C.c_void_p), ("fetch_steps", C.c_int32), ("fetch_min_idle", C.c_int32),
                 ("fetch_steps_shadow", C.c_int32), ("fetch_min_idle_shadow", C.c_int32), ("reg_lean", C.c_int32),
-                ("postpone_shadow", C.c_int32)]
+                ("shadow_tests", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -401,7 +401,7 @@ class Scene:
                             cfg.get("iterations_per_check", 0), 0, None, None, cfg.get("fetch_steps", 0),
                             cfg.get("fetch_min_idle", 0), cfg.get("fetch_steps_shadow", 0),
                             cfg.get("fetch_min_idle_shadow", 0), cfg.get("reg_lean", 0),
-                            cfg.get("postpone_shadow", 0))
+                            cfg.get("shadow_tests", 0))
         check(lib().hk_scene_set_wavefront_config(self.h, C.byref(c)))
 
     def tree_build_seconds(self) -> float:
@@ -471,7 +471,7 @@ class Scene:
                      threads_extend: int = 0, threads_shade: int = 0, iterations_per_check: int = 0,
                      no_graph: bool = False, kernel_ms=None, kernel_launches=None, sizes=None,
                      fetch_steps: int = 0, fetch_min_idle: int = 0, fetch_steps_shadow: int = 0,
-                     fetch_min_idle_shadow: int = 0, reg_lean: int = 0, postpone_shadow: int = 0,
+                     fetch_min_idle_shadow: int = 0, reg_lean: int = 0, shadow_tests: int = 0,
                      stream=None) -> None:
         """Wavefront render of several images at once: films[i] (device
         tensors of film_shape(), or of film_shape(*sizes[i]) with per-image
@@ -491,14 +491,14 @@ class Scene:
             jobs[i].desc = render_desc(spp, depth, seed, sample_offset, rr_start, idx, 0, cam, w, h)
         cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, int(no_graph),
                               _p(kernel_ms), _p(kernel_launches), fetch_steps, fetch_min_idle, fetch_steps_shadow,
-                              fetch_min_idle_shadow, reg_lean, postpone_shadow)
+                              fetch_min_idle_shadow, reg_lean, shadow_tests)
         check(lib().hk_render_batch(self.h, jobs, n, C.byref(cfg), _p(counters), _stream(stream)))
 
     def render_batch_host(self, outs, spp: int, depth: int, seeds=None, cameras=None, image_indices=None,
                           rr_start: int = 0, capacity: int = 0, threads_extend: int = 0, threads_shade: int = 0,
                           iterations_per_check: int = 0, fetch_steps: int = 0, fetch_min_idle: int = 0,
                           fetch_steps_shadow: int = 0, fetch_min_idle_shadow: int = 0, reg_lean: int = 0,
-                          postpone_shadow: int = 0, stream=None):
+                          shadow_tests: int = 0, stream=None):
         """End-to-end wavefront batch into host images outs[i] (H x W x 3 float32)."""
         n = len(outs)
         descs = (RenderDesc * n)()
@@ -511,7 +511,7 @@ class Scene:
         ctr = np.zeros(7, np.uint64)
         cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, 0, None, None,
                               fetch_steps, fetch_min_idle, fetch_steps_shadow, fetch_min_idle_shadow, reg_lean,
-                              postpone_shadow)
+                              shadow_tests)
         check(lib().hk_render_batch_host(self.h, descs, n, C.byref(cfg), ptrs, ctr.ctypes.data, _stream(stream)))
         return ctr
 
@@ -526,7 +526,7 @@ class Scene:
                     iterations_per_check=cfg.iterations_per_check, fetch_steps=cfg.fetch_steps,
                     fetch_min_idle=cfg.fetch_min_idle, fetch_steps_shadow=cfg.fetch_steps_shadow,
                     fetch_min_idle_shadow=cfg.fetch_min_idle_shadow, reg_lean=cfg.reg_lean,
-                    postpone_shadow=cfg.postpone_shadow), ms.value
+                    shadow_tests=cfg.shadow_tests), ms.value
 
     def render_image_static(self, out, spp: int, depth: int, seed: int = 0, rr_start: int = 0, counters=None,
                             camera=None, image_index: int = 0, stream=None) -> None:

@@ -850,7 +850,7 @@ hk::WfEngine &wf_ensure(hk_scene *s, const hk::WfEngineConfig &c) {
         if (o.capacity == c.capacity && o.threads_extend == c.threads_extend && o.threads_shade == c.threads_shade &&
             o.fetch_steps == c.fetch_steps && o.fetch_min_idle == c.fetch_min_idle &&
             o.fetch_steps_shadow == c.fetch_steps_shadow && o.fetch_min_idle_shadow == c.fetch_min_idle_shadow &&
-            o.reg_lean == c.reg_lean && o.postpone_shadow == c.postpone_shadow)
+            o.reg_lean == c.reg_lean && o.shadow_tests == c.shadow_tests)
             return *s->wf;
         s->wf.reset();
     }
@@ -1420,7 +1420,7 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         ec.fetch_steps_shadow = std::max(0, std::min(1024, c.fetch_steps_shadow));
         ec.fetch_min_idle_shadow = c.fetch_min_idle_shadow > 0 ? std::min(32, c.fetch_min_idle_shadow) : 0;
         ec.reg_lean = c.reg_lean & 3;
-        ec.postpone_shadow = c.postpone_shadow ? 1 : 0;
+        ec.shadow_tests = c.shadow_tests >= 0 && c.shadow_tests <= 2 ? c.shadow_tests : 0;
         hk::WfEngine &E = wf_ensure(s, ec);
         cudaStream_t user = (cudaStream_t)stream, st = E.stream();
         // order after the caller's stream (the films may have been cleared there)
@@ -1589,12 +1589,15 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
             float ms = run(c);
             if (ms < best_t) { best_t = ms; bc = c; }
         }
-        // shadow rays postponing their triangle tests (8-wide tree only)
-        if (s->dev.accel == hk::kAccelBvh8 && s->dev.postpone) {
+        // the shadow rays' triangle tests postponed or shared out over the warp (8-wide tree only)
+        if (s->dev.accel == hk::kAccelBvh8) {
             c = bc;
-            c.postpone_shadow = 1;
-            float ms = run(c);
-            if (ms < best_t) { best_t = ms; bc = c; }
+            for (int k : {1, 2}) {
+                if (k == 1 && !s->dev.postpone) continue;
+                c.shadow_tests = k;
+                float ms = run(c);
+                if (ms < best_t) { best_t = ms; bc = c; }
+            }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

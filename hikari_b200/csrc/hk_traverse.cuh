@@ -437,6 +437,85 @@ struct Bvh8Walker {
         return false;
     }
 
+    // One step of an any-hit ray with the warp's triangle tests shared out:
+    // every lane of the warp calls it (alive: the lane holds a ray).  Alive
+    // lanes visit a node (or pop a triangle group); the triangles of all
+    // lanes' groups are then numbered in lane order and tested 32 at a time,
+    // lane j taking triangle r + j of the numbering against its owner's ray
+    // (rays: the warp's rays in shared memory, origin + tmin then direction +
+    // tmax per lane), and a lane is occluded when any of its triangles is.
+    // The serial loop of step() runs as many rounds as the warp's largest
+    // group, with the other lanes idle; this runs ceil(sum / 32).
+    __device__ __forceinline__ bool step_any_shared(const DevScene &S, bool alive, const float4 *rays) {
+        const unsigned lane = threadIdx.x & 31u;
+        uint2 grp = make_uint2(0u, 0u);
+        if (alive) {
+            if (ng.y > 0x00ffffffu) {
+                const uint32_t b = __ffs(ng.y >> 24) - 1;
+                ng.y &= ~(1u << (24 + b));
+                const uint32_t slot = b ^ ko;
+                const uint32_t child = ng.x + __popc(ng.y & 0xffu & ((1u << slot) - 1u));
+                if (ng.y > 0x00ffffffu) stk.push(ng);
+                visit(S, child);
+                grp = tg;
+            } else {
+                grp = ng;   // a postponed triangle group from the stack (or nothing)
+                ng = make_uint2(0u, 0u);
+            }
+            tg = make_uint2(0u, 0u);
+        }
+        const uint32_t cnt = __popc(grp.y);
+        uint32_t incl = cnt;   // inclusive prefix of the counts in lane order
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t excl = incl - cnt;
+        ntri += cnt;
+        bool occluded = false;
+        for (uint32_t r = 0; r < total; r += 32) {   // warp-uniform
+            const uint32_t w = r + lane;
+            // owner: the number of lanes whose inclusive prefix is <= w
+            // (binary lifting; every index read stays within 0..31)
+            uint32_t own = 0;
+#pragma unroll
+            for (uint32_t b = 16; b > 0; b >>= 1) {
+                const uint32_t v = __shfl_sync(0xffffffffu, incl, own + b - 1);
+                if (v <= w) own += b;
+            }
+            const uint32_t obase = __shfl_sync(0xffffffffu, grp.x, own);
+            const uint32_t omask = __shfl_sync(0xffffffffu, grp.y, own);
+            const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, own);
+            bool hit = false;
+            if (w < total) {
+                const uint32_t tri = obase + __fns(omask, 0u, (int)(w - oexcl) + 1);
+                const float4 *tp = S.tris + 3 * (size_t)tri;
+                const float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
+                const float4 ro = rays[2 * own], rd = rays[2 * own + 1];
+                hit = occludes_mt(xyz(ro), xyz(rd), xyz(p0), xyz(p1), xyz(p2), ro.w, rd.w);
+            }
+            const uint32_t hb = __ballot_sync(0xffffffffu, hit);
+            // the lanes that tested this lane's triangles in round r
+            const int lo = max((int)excl - (int)r, 0), hi = min((int)incl - (int)r, 32);
+            if (lo < hi) {
+                const uint32_t upto = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
+                if (hb & upto & ~((1u << lo) - 1u)) occluded = true;
+            }
+        }
+        if (!alive) return false;
+        if (occluded) {
+            found = true;
+            return true;
+        }
+        if (ng.y <= 0x00ffffffu) {
+            if (stk.sp == 0) return true;
+            ng = stk.pop();
+        }
+        return false;
+    }
+
     // Intersect the 8 children of node `child`: ng / tg become its groups.
     __device__ __forceinline__ void visit(const DevScene &S, uint32_t child) {
         const uint4 *np = S.wnodes + 5 * (size_t)child;
@@ -580,6 +659,64 @@ __device__ __forceinline__ void trace_queue(const DevScene &S, Walker &wk, unsig
                 }
             }
         }
+    }
+}
+
+// trace_queue for any-hit rays with the warp's triangle tests shared out
+// (Bvh8Walker::step_any_shared): the same refills, but every lane takes every
+// step, lanes without a ray as idle partners.  rays: 2 float4 per thread of
+// the block (shared memory), written here when a lane takes a ray.
+template <class Walker, class Load, class Store>
+__device__ __forceinline__ void trace_queue_any_shared(const DevScene &S, Walker &wk, unsigned *fetch, unsigned n,
+                                                       int steps, int min_idle, float4 *rays, Load load, Store store,
+                                                       TravStats &st) {
+    const unsigned lane = threadIdx.x & 31u;
+    float4 *mine = rays + 2 * threadIdx.x;
+    const float4 *warp_rays = rays + 2 * (threadIdx.x & ~31u);
+    int item = -1;
+    bool exhausted = false;
+    unsigned chunk_next = 0, chunk_end = 0;
+    for (;;) {
+        const unsigned want = __ballot_sync(0xffffffffu, item < 0 && !exhausted);
+        const unsigned busy = __ballot_sync(0xffffffffu, item >= 0);
+        if (want && (busy == 0u || __popc(want) >= min_idle)) {
+            const unsigned k = __popc(want), rank = __popc(want & ((1u << lane) - 1u));
+            const unsigned avail = chunk_end - chunk_next;
+            unsigned idx = chunk_next + rank;
+            if (k > avail) {
+                unsigned base = 0;
+                if ((int)lane == __ffs(want) - 1) base = atomicAdd(fetch, kFetchChunk);
+                base = __shfl_sync(0xffffffffu, base, __ffs(want) - 1);
+                if (rank >= avail) idx = base + (rank - avail);
+                chunk_next = base + (k - avail);
+                chunk_end = base + kFetchChunk;
+            } else {
+                chunk_next += k;
+            }
+            if (want >> lane & 1u) {
+                if (idx < n) {
+                    item = (int)idx;
+                    const Ray r = load(item);
+                    wk.begin(S, r);
+                    mine[0] = make_float4(r.o.x, r.o.y, r.o.z, r.tmin);
+                    mine[1] = make_float4(r.d.x, r.d.y, r.d.z, r.tmax);
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, item >= 0)) break;
+        __syncwarp();   // the new rays are visible to the warp's other lanes
+        for (int k = 0; k < steps; ++k) {
+            const bool done = wk.step_any_shared(S, item >= 0, warp_rays);
+            if (item >= 0 && done) {
+                wk.template end<true>(S, st);
+                store(item, wk);
+                item = -1;
+            }
+            if (!__any_sync(0xffffffffu, item >= 0)) break;
+        }
+        __syncwarp();   // every read of a lane's ray precedes its replacement
     }
 }
 

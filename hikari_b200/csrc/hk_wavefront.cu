@@ -34,8 +34,8 @@ extern template cudaError_t wf_launch_extend_t<kAccelBvh8>(const DevScene &, con
 extern template cudaError_t wf_launch_extend_t<kAccelBvh2>(const DevScene &, const WfState &, const WfLaunchConfig &, int, cudaStream_t);
 extern template cudaError_t wf_launch_shadow_t<kAccelBvh8>(const DevScene &, const WfState &, const WfLaunchConfig &, cudaStream_t);
 extern template cudaError_t wf_launch_shadow_t<kAccelBvh2>(const DevScene &, const WfState &, const WfLaunchConfig &, cudaStream_t);
-extern template int wf_trace_occupancy_t<kAccelBvh8>(int, int, bool);
-extern template int wf_trace_occupancy_t<kAccelBvh2>(int, int, bool);
+extern template int wf_trace_occupancy_t<kAccelBvh8>(int, int, bool, bool);
+extern template int wf_trace_occupancy_t<kAccelBvh2>(int, int, bool, bool);
 #define HK_WF_SHADE_EXTERN(K)                                                                                           \
     extern template cudaError_t wf_launch_shade_t<K>(const DevScene &, const WfState &, const WfLaunchConfig &, int, \
                                                      cudaStream_t);                                                 \
@@ -243,14 +243,14 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
     return cudaGetLastError();
 }
 
-int wf_occupancy(int which, int threads, int accel, bool lean) {
+int wf_occupancy(int which, int threads, int accel, bool lean, bool shared) {
     int n = 0;
     const bool w8 = accel == kAccelBvh8;
     switch (which) {
     case 0:
     case 2:
-        return w8 ? wf_trace_occupancy_t<kAccelBvh8>(which, threads, lean)
-                  : wf_trace_occupancy_t<kAccelBvh2>(which, threads, lean);
+        return w8 ? wf_trace_occupancy_t<kAccelBvh8>(which, threads, lean, shared)
+                  : wf_trace_occupancy_t<kAccelBvh2>(which, threads, lean, shared);
     case 1: return wf_shade_occupancy_t<5>(threads);
     default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_regen_kernel, threads, 0); break;
     }

@@ -119,7 +119,7 @@ struct WfLaunchConfig {
     int fetch_steps, fetch_min_idle;                 // dynamic ray fetch of the extend kernel
     int fetch_steps_shadow, fetch_min_idle_shadow;   // and of the shadow kernel
     int lean_extend, lean_shadow;                    // traversal kernels with the smaller register budget
-    int postpone_shadow;                             // shadow rays postpone triangle tests
+    int shadow_tests;   // shadow rays' triangle tests: 0 per lane, 1 postponed, 2 shared over the warp
 };
 
 // empty pool: every slot idle, queues and statistics zero (the dispatch head is the host's)
@@ -133,6 +133,6 @@ cudaError_t wf_launch_phase(const DevScene &S, const WfState &W, const WfLaunchC
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st);
 // resident blocks per SM of a kernel (which: 0 extend, 1 shade, 2 shadow, 3
 // regen); lean: the traversal kernels' smaller register budget
-int wf_occupancy(int which, int threads, int accel, bool lean = false);
+int wf_occupancy(int which, int threads, int accel, bool lean = false, bool shared = false);
 
 }  // namespace hk

@@ -345,7 +345,9 @@ __global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, in
 }
 
 // ------------------------------------------------------------ shadow
-template <int kAccel, int kMinBlocks>
+// kShared: the warp's triangle tests shared out over its lanes (8-wide tree;
+// the block's rays in dynamic shared memory after the stacks).
+template <int kAccel, int kMinBlocks, bool kShared>
 __global__ void __launch_bounds__(256, kMinBlocks) wf_shadow_kernel(DevScene S, WfState W, int steps, int min_idle) {
     const unsigned n = min(W.ctr->shadow_count, (unsigned)W.max_shadow);
     TravStats ts;
@@ -358,25 +360,29 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_shadow_kernel(DevScene S, 
         wk.stack = stack_mem;
     }
     int slot = -1;
-    trace_queue<true>(
-        S, wk, &W.ctr->sh_fetch, n, steps, min_idle,
-        [&](int i) {
-            const float4 o = W.sh_o[i], d = W.sh_d[i];
-            slot = __float_as_int(o.w);
-            Ray r;
-            r.o = v3(o.x, o.y, o.z);
-            r.d = v3(d.x, d.y, d.z);
-            r.tmin = kRayEps;
-            r.tmax = 1.0f - kRayEps;
-            return r;
-        },
-        [&](int i, const auto &w) {
-            if (!w.found) {
-                const float4 c = W.sh_c[i];
-                red_add_v4(W.lacc + slot, c.x, c.y, c.z, 0.0f);
-            }
-        },
-        ts);
+    auto load = [&](int i) {
+        const float4 o = W.sh_o[i], d = W.sh_d[i];
+        slot = __float_as_int(o.w);
+        Ray r;
+        r.o = v3(o.x, o.y, o.z);
+        r.d = v3(d.x, d.y, d.z);
+        r.tmin = kRayEps;
+        r.tmax = 1.0f - kRayEps;
+        return r;
+    };
+    auto store = [&](int i, const auto &w) {
+        if (!w.found) {
+            const float4 c = W.sh_c[i];
+            red_add_v4(W.lacc + slot, c.x, c.y, c.z, 0.0f);
+        }
+    };
+    if constexpr (kShared && kAccel == kAccelBvh8) {
+        extern __shared__ uint2 wf_stack_smem[];
+        float4 *rays = reinterpret_cast<float4 *>(wf_stack_smem + (size_t)blockDim.x * kShStack);
+        trace_queue_any_shared(S, wk, &W.ctr->sh_fetch, n, steps, min_idle, rays, load, store, ts);
+    } else {
+        trace_queue<true>(S, wk, &W.ctr->sh_fetch, n, steps, min_idle, load, store, ts);
+    }
     unsigned long long nv = ts.nodes, nt = ts.tris;
     for (int o = 16; o > 0; o >>= 1) {
         nv += __shfl_down_sync(0xffffffffu, nv, o);
@@ -403,30 +409,54 @@ cudaError_t wf_launch_extend_t(const DevScene &S, const WfState &W, const WfLaun
                                                                                 C.fetch_min_idle);
     return cudaGetLastError();
 }
+// dynamic shared memory of a shadow launch: the short stacks, and the rays
+// where the triangle tests are shared out
+__host__ inline size_t wf_shadow_smem(int threads, bool shared) {
+    return wf_stack_bytes(threads) + (shared ? (size_t)threads * 2 * sizeof(float4) : 0);
+}
 template <int kAccel>
 cudaError_t wf_launch_shadow_t(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
-    const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(C.threads_shadow) : 0;
+    const bool shared = kAccel == kAccelBvh8 && C.shadow_tests == 2;
+    const size_t smem = kAccel == kAccelBvh8 ? wf_shadow_smem(C.threads_shadow, shared) : 0;
     DevScene SS = S;
-    SS.postpone_any = S.postpone && C.postpone_shadow ? 1 : 0;
-    if (C.lean_shadow)
-        wf_shadow_kernel<kAccel, kLeanBlocks><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(
-            SS, W, C.fetch_steps_shadow, C.fetch_min_idle_shadow);
-    else
-        wf_shadow_kernel<kAccel, 0><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(SS, W, C.fetch_steps_shadow,
-                                                                                 C.fetch_min_idle_shadow);
+    SS.postpone_any = S.postpone && C.shadow_tests == 1 ? 1 : 0;
+    const int a = C.fetch_steps_shadow, b = C.fetch_min_idle_shadow;
+    if (shared) {
+        if (C.lean_shadow)
+            wf_shadow_kernel<kAccel, kLeanBlocks, true><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(SS, W, a, b);
+        else
+            wf_shadow_kernel<kAccel, 0, true><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(SS, W, a, b);
+    } else {
+        if (C.lean_shadow)
+            wf_shadow_kernel<kAccel, kLeanBlocks, false><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(SS, W, a, b);
+        else
+            wf_shadow_kernel<kAccel, 0, false><<<C.blocks_shadow, C.threads_shadow, smem, st>>>(SS, W, a, b);
+    }
     return cudaGetLastError();
 }
-// which: 0 extend, 2 shadow; lean: the kLeanBlocks register budget
+// which: 0 extend, 2 shadow; lean: the kLeanBlocks register budget; shared:
+// the shadow kernel with shared triangle tests
 template <int kAccel>
-int wf_trace_occupancy_t(int which, int threads, bool lean) {
+int wf_trace_occupancy_t(int which, int threads, bool lean, bool shared) {
     int n = 0;
-    const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(threads) : 0;
+    shared = shared && kAccel == kAccelBvh8;
     if (which == 0) {
+        const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(threads) : 0;
         if (lean) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, kLeanBlocks>, threads, smem);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, 0>, threads, smem);
     } else {
-        if (lean) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel, kLeanBlocks>, threads, smem);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel, 0>, threads, smem);
+        const size_t smem = kAccel == kAccelBvh8 ? wf_shadow_smem(threads, shared) : 0;
+        if (shared) {
+            if (lean)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel, kLeanBlocks, true>, threads,
+                                                              smem);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel, 0, true>, threads, smem);
+        } else {
+            if (lean)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel, kLeanBlocks, false>, threads,
+                                                              smem);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shadow_kernel<kAccel, 0, false>, threads, smem);
+        }
     }
     return n;
 }

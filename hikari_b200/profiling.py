@@ -153,7 +153,7 @@ def render(argv):
     ap.add_argument("--fetch-steps-shadow", type=int, default=0)
     ap.add_argument("--fetch-min-idle-shadow", type=int, default=0)
     ap.add_argument("--reg-lean", type=int, default=0)
-    ap.add_argument("--postpone-shadow", type=int, default=0)
+    ap.add_argument("--shadow-tests", type=int, default=0)
     a = ap.parse_args(argv)
     sd = scenes.heterogeneous(width=1024, height=1024, spp=a.spp, depth=16)
     cams = scenes.heterogeneous_cameras(a.views)
@@ -165,7 +165,7 @@ def render(argv):
                     threads_extend=a.threads_extend, threads_shade=a.threads_shade, fetch_steps=a.fetch_steps,
                     fetch_min_idle=a.fetch_min_idle, iterations_per_check=a.iterations_per_check,
                     fetch_steps_shadow=a.fetch_steps_shadow, fetch_min_idle_shadow=a.fetch_min_idle_shadow,
-                    reg_lean=a.reg_lean, postpone_shadow=a.postpone_shadow)
+                    reg_lean=a.reg_lean, shadow_tests=a.shadow_tests)
     torch.cuda.synchronize()
     c = [int(x) for x in ctr.cpu().tolist()]
     names = ["rays", "shadow_rays", "dropped", "node_visits", "tri_tests", "node_visits_shadow", "tri_tests_shadow"]

@@ -283,8 +283,10 @@ typedef struct {
     int32_t fetch_min_idle_shadow; /*   rays' values */
     int32_t reg_lean;              /* bit 0 / bit 1: the extend / shadow kernel with a register budget of
                                       48 (five resident blocks of 256 threads) instead of the compiler's */
-    int32_t postpone_shadow;       /* 1: shadow rays postpone triangle tests like closest-hit rays (a lane
-                                      keeps visiting nodes while few lanes of its warp have triangles) */
+    int32_t shadow_tests;          /* triangle tests of the shadow rays (8-wide tree): 0 each lane tests
+                                      its own; 1 the same, postponed like closest-hit rays' while few
+                                      lanes of the warp have triangles; 2 shared out over the warp, 32
+                                      at a time */
 } hk_wavefront_config;
 
 /* Render every job of the batch with the wavefront integrator: a pool of path

@@ -151,3 +151,30 @@ def test_render_image_forms_agree():
     gs.set_image_form(hk.FORM_AUTO)
     d, _ = gs.render_image(64, sd.depth, seed=31)
     assert np.allclose(d, b, rtol=1e-4, atol=1e-6 * scale)
+
+
+@pytest.mark.parametrize("lean", [0, 2])
+def test_shadow_test_modes_agree(lean):
+    """The shadow rays' triangle tests -- each lane its own, postponed, or
+    shared out over the warp (hk_wavefront_config.shadow_tests 0 / 1 / 2) --
+    decide occlusion by the same Moller-Trumbore test on the same triangles,
+    and an any-hit decision does not depend on the order of the tests: the
+    images agree up to the order of the film's float additions, the ray
+    counts exactly."""
+    sd = scenes.heterogeneous(width=128, height=128, spp=8, depth=8, n_spheres=12, levels=(3, 4),
+                              level_p=(0.5, 0.5), env_res=(256, 128))
+    gs = hk.Scene.from_desc(sd)
+    gs.set_accel(hk.ACCEL_BVH8)
+    imgs, ctrs = [], []
+    for mode in (0, 1, 2):
+        f = torch.zeros(gs.film_shape(), dtype=torch.float32, device="cuda")
+        ctr = torch.zeros(7, dtype=torch.int64, device="cuda")
+        gs.render_batch([f], spp=8, depth=8, seeds=[3], counters=ctr, capacity=1 << 16, threads_extend=64,
+                        shadow_tests=mode, reg_lean=lean)
+        imgs.append(f.cpu().numpy().astype(np.float64))
+        ctrs.append(ctr.cpu().numpy())
+    scale = float(np.abs(imgs[0]).max())
+    for mode in (1, 2):
+        print(f"mode {mode}: counters {ctrs[mode]} vs {ctrs[0]}, max abs diff {np.abs(imgs[mode] - imgs[0]).max():.3e}")
+        assert ctrs[mode][0] == ctrs[0][0] and ctrs[mode][1] == ctrs[0][1]
+        assert np.allclose(imgs[mode], imgs[0], rtol=1e-5, atol=1e-6 * scale)
