@@ -36,16 +36,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
-# Per-ray figures of the 8-wide traversal kernels from one ncu capture of every
-# extend / shadow launch of `python -m hikari_b200.profiling render --views 1
-# --spp 4 --accel bvh8` with the bench's tuned launch configuration (the
-# heterogeneous scene, pool of 2^22 slots), summed per kernel and divided by the
-# rays the render traced: DRAM bytes (dram__bytes_read.sum +
-# dram__bytes_write.sum), L2 bytes (lts__t_bytes.sum) and warp instructions
-# issued (smsp__inst_executed.sum).  The bench scales them by the rays of its
-# own launches.
-TRAVERSAL_PER_RAY = {"bvh8": {"extend": {"dram": 190.75, "l2": 725.7, "inst": 297.9},
-                              "shadow": {"dram": 125.01, "l2": 744.0, "inst": 264.4}}}
+# Per-ray figures of the 8-wide traversal kernels from ncu captures of launches
+# 2-4 of each kernel (the steady state, a full pool of 2^22 slots) in
+# `python -m hikari_b200.profiling render --views 1 --spp 16 --accel bvh8
+# --config-json <the tuned configuration>` (the heterogeneous scene), divided by
+# the rays those launches traced (hk_wavefront_launch_log): DRAM bytes
+# (dram__bytes_read.sum + dram__bytes_write.sum), L2 bytes (lts__t_bytes.sum)
+# and warp instructions issued (smsp__inst_executed.sum).  The bench scales them
+# by the rays of its own launches.
+TRAVERSAL_PER_RAY = {"bvh8": {"extend": {"dram": 231.40, "l2": 964.0, "inst": 343.9},
+                              "shadow": {"dram": 114.43, "l2": 798.4, "inst": 241.9}}}
 SMS, SCHEDULERS_PER_SM = 148, 4
 MEASURED_SM_MAX_MHZ = 1965.0
 
@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end pass (profiling runs)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-megakernel comparison sample")
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                    help="override one entry of the autotuned wavefront configuration (e.g. sample_major=1)")
     ap.add_argument("--form", default="wavefront", choices=["wavefront", "megakernel"],
                     help="wavefront (the batched form) or the plain one-thread-per-path megakernel")
     return ap.parse_args()
@@ -372,6 +374,11 @@ def run_serving(args):
     sds = serving_scenes()
     gss = [hk.Scene.from_desc(sd) for sd in sds]
     build_s = time.perf_counter() - t0
+    # each scene's traversal settings, which the server's engines take (untimed)
+    t1 = time.perf_counter()
+    for g, sd in zip(gss, sds):
+        g.autotune(4, sd.depth)
+    tune_s = time.perf_counter() - t1
     tris = [int(g.info.n_triangles) for g in gss]
     rng = np.random.default_rng(7)
     depths = [sd.depth for sd in sds]
@@ -422,7 +429,9 @@ def run_serving(args):
                                "heterogeneous 4.75M tris, 5 heterogeneous variants); jobs of 256/512/1024 px "
                                "square at 16/64/256 spp",
                    "form": f"wavefront serving loop (continuous batching, {args.policy} dispatch)", "triangles": tris,
-                   "scene_build_s": round(build_s, 2), "capacity": args.capacity, "jobs": args.jobs,
+                   "scene_build_s": round(build_s, 2), "autotune_s": round(tune_s, 2),
+                   "traversal": "each scene's autotuned fetch intervals, register budgets and triangle-test modes",
+                   "capacity": args.capacity, "jobs": args.jobs,
                    "load": args.load},
         "serving": {
             "peak_mpaths_per_s": peak_mpaths, "peak_rate_hz": peak_rate, "arrival_rate_hz": rate,
@@ -610,6 +619,11 @@ def main():
     tuned, tune_ms = {}, None
     if wave:
         tuned, tune_ms = gs.autotune(min(16, spp), depth, camera=cams[0])   # untimed set-up
+        for kv in args.set:
+            k, v = kv.split("=", 1)
+            if k not in tuned:
+                raise SystemExit(f"--set: unknown configuration key {k}")
+            tuned[k] = int(v)
 
     def step(it, ctr=None, **extra):
         for f in films:
@@ -816,8 +830,9 @@ def main():
         "drop_in_render_image": drop_in,
         "roofline": {"bound": limiter["bound"], "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind, "basis": basis,
-                     "traffic_basis": ("DRAM bytes per ray from one ncu capture of the 1-view 4-spp case, scaled by "
-                                       "the rays per launch" if traffic is not None else None),
+                     "traffic_basis": ("DRAM bytes per ray from an ncu capture of three steady-state launches of the "
+                                       "1-view 16-spp case, scaled by the rays per launch"
+                                       if traffic is not None else None),
                      **{k: v for k, v in limiter.items() if k != "bound"}},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "Mpaths/s", "h2d_bytes_per_step": V * int(hk.C.sizeof(hk.RenderDesc)),

@@ -77,7 +77,7 @@ class WavefrontConfig(C.Structure):
                 ("iterations_per_check", C.c_int32), ("no_graph", C.c_int32), ("kernel_ms", C.c_void_p),
                 ("kernel_launches", C.c_void_p), ("fetch_steps", C.c_int32), ("fetch_min_idle", C.c_int32),
                 ("fetch_steps_shadow", C.c_int32), ("fetch_min_idle_shadow", C.c_int32), ("reg_lean", C.c_int32),
-                ("shadow_tests", C.c_int32)]
+                ("shadow_tests", C.c_int32), ("closest_tests", C.c_int32), ("sample_major", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -151,6 +151,7 @@ def lib():
         "hk_scene_set_wavefront_config": ([P, C.POINTER(WavefrontConfig)], C.c_int),
         "hk_scene_set_builder": ([P, I32], C.c_int),
         "hk_scene_tree_build_seconds": ([P, C.POINTER(C.c_double)], C.c_int),
+        "hk_wavefront_launch_log": ([P, I32, P, I32, C.POINTER(I32)], C.c_int),
         "hk_bvh_check_gpu": ([P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)], C.c_int),
         "hk_bvh_check": ([P, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
                          C.c_int),
@@ -401,7 +402,7 @@ class Scene:
                             cfg.get("iterations_per_check", 0), 0, None, None, cfg.get("fetch_steps", 0),
                             cfg.get("fetch_min_idle", 0), cfg.get("fetch_steps_shadow", 0),
                             cfg.get("fetch_min_idle_shadow", 0), cfg.get("reg_lean", 0),
-                            cfg.get("shadow_tests", 0))
+                            cfg.get("shadow_tests", 0), cfg.get("closest_tests", 0), cfg.get("sample_major", 0))
         check(lib().hk_scene_set_wavefront_config(self.h, C.byref(c)))
 
     def tree_build_seconds(self) -> float:
@@ -409,6 +410,14 @@ class Scene:
         s = C.c_double()
         check(lib().hk_scene_tree_build_seconds(self.h, C.byref(s)))
         return s.value
+
+    def wavefront_launch_log(self, which: int) -> np.ndarray:
+        """Rays of each launch of the closest-hit (which 0) or shadow (which 1)
+        traversal kernel in the scene's last render_batch, in launch order."""
+        buf = np.zeros(1024, np.uint32)
+        n = C.c_int32()
+        check(lib().hk_wavefront_launch_log(self.h, which, buf.ctypes.data, len(buf), C.byref(n)))
+        return buf[:min(n.value, len(buf))].copy()
 
     def set_accel(self, accel: int) -> None:
         """Traverse the binary tree (ACCEL_BVH2) or the compressed 8-wide tree (ACCEL_BVH8)."""
@@ -472,7 +481,7 @@ class Scene:
                      no_graph: bool = False, kernel_ms=None, kernel_launches=None, sizes=None,
                      fetch_steps: int = 0, fetch_min_idle: int = 0, fetch_steps_shadow: int = 0,
                      fetch_min_idle_shadow: int = 0, reg_lean: int = 0, shadow_tests: int = 0,
-                     stream=None) -> None:
+                     closest_tests: int = 0, sample_major: int = 0, stream=None) -> None:
         """Wavefront render of several images at once: films[i] (device
         tensors of film_shape(), or of film_shape(*sizes[i]) with per-image
         sizes (width, height)) accumulate spp samples of view cameras[i].
@@ -491,14 +500,14 @@ class Scene:
             jobs[i].desc = render_desc(spp, depth, seed, sample_offset, rr_start, idx, 0, cam, w, h)
         cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, int(no_graph),
                               _p(kernel_ms), _p(kernel_launches), fetch_steps, fetch_min_idle, fetch_steps_shadow,
-                              fetch_min_idle_shadow, reg_lean, shadow_tests)
+                              fetch_min_idle_shadow, reg_lean, shadow_tests, closest_tests, sample_major)
         check(lib().hk_render_batch(self.h, jobs, n, C.byref(cfg), _p(counters), _stream(stream)))
 
     def render_batch_host(self, outs, spp: int, depth: int, seeds=None, cameras=None, image_indices=None,
                           rr_start: int = 0, capacity: int = 0, threads_extend: int = 0, threads_shade: int = 0,
                           iterations_per_check: int = 0, fetch_steps: int = 0, fetch_min_idle: int = 0,
                           fetch_steps_shadow: int = 0, fetch_min_idle_shadow: int = 0, reg_lean: int = 0,
-                          shadow_tests: int = 0, stream=None):
+                          shadow_tests: int = 0, closest_tests: int = 0, sample_major: int = 0, stream=None):
         """End-to-end wavefront batch into host images outs[i] (H x W x 3 float32)."""
         n = len(outs)
         descs = (RenderDesc * n)()
@@ -511,7 +520,7 @@ class Scene:
         ctr = np.zeros(7, np.uint64)
         cfg = WavefrontConfig(capacity, threads_extend, threads_shade, iterations_per_check, 0, None, None,
                               fetch_steps, fetch_min_idle, fetch_steps_shadow, fetch_min_idle_shadow, reg_lean,
-                              shadow_tests)
+                              shadow_tests, closest_tests, sample_major)
         check(lib().hk_render_batch_host(self.h, descs, n, C.byref(cfg), ptrs, ctr.ctypes.data, _stream(stream)))
         return ctr
 
@@ -526,7 +535,8 @@ class Scene:
                     iterations_per_check=cfg.iterations_per_check, fetch_steps=cfg.fetch_steps,
                     fetch_min_idle=cfg.fetch_min_idle, fetch_steps_shadow=cfg.fetch_steps_shadow,
                     fetch_min_idle_shadow=cfg.fetch_min_idle_shadow, reg_lean=cfg.reg_lean,
-                    shadow_tests=cfg.shadow_tests), ms.value
+                    shadow_tests=cfg.shadow_tests, closest_tests=cfg.closest_tests,
+                    sample_major=cfg.sample_major), ms.value
 
     def render_image_static(self, out, spp: int, depth: int, seed: int = 0, rr_start: int = 0, counters=None,
                             camera=None, image_index: int = 0, stream=None) -> None:

@@ -49,6 +49,8 @@ struct alignas(16) DevBsdf {
 
 // Procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp) or
 // bitmap (src/texture/BitmapTexture.cpp over include/core/MipMap.hpp).
+// cutpoints per CDF in the environment map's guide tables (a power of two)
+constexpr int kEnvGuide = 1024;
 enum TexKind : int32_t { kTexCheckerboard = 1, kTexGrid = 2, kTexScale = 3, kTexBitmap = 4 };
 enum TexFilter : int32_t { kFilterNearest = 0, kFilterBilinear = 1, kFilterTrilinear = 2, kFilterEwa = 3 };
 constexpr int kMipMaxLevels = 16;   // level 0 up to 32768 texels a side
@@ -139,6 +141,8 @@ struct DevScene {
     const float *env_cond_cdf;    // H*(W+1)
     const float *env_cond_func;   // H*W
     const float *env_cond_int;    // H row integrals
+    const int32_t *env_marg_guide;   // kEnvGuide + 1 cutpoints of the marginal CDF
+    const int32_t *env_cond_guide;   // H * (kEnvGuide + 1) cutpoints of the row CDFs
     float env_marg_int;
     uint32_t env_w, env_h;
     float env_scale;

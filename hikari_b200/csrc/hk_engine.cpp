@@ -73,9 +73,10 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     L_.lean_extend = cfg_.reg_lean & 1;
     L_.lean_shadow = (cfg_.reg_lean >> 1) & 1;
     L_.shadow_tests = cfg_.shadow_tests >= 0 && cfg_.shadow_tests <= 2 ? cfg_.shadow_tests : 0;
+    L_.closest_tests = cfg_.closest_tests == 2 ? 2 : 0;
     auto grid = [&](int which, int threads) {
         const bool lean = which == 0 ? L_.lean_extend : (which == 2 ? L_.lean_shadow : false);
-        const bool shared = which == 2 && L_.shadow_tests == 2;
+        const bool shared = (which == 2 && L_.shadow_tests == 2) || (which == 0 && L_.closest_tests == 2);
         return std::max(1, sm_count * std::max(1, wf_occupancy(which, threads, S.accel, lean, shared)));
     };
     L_.blocks_extend = grid(0, L_.threads_extend);
@@ -185,12 +186,25 @@ void WfEngine::run(int iterations, bool use_graph, float *kernel_ms, int32_t *ke
 }
 
 void WfEngine::fetch_status() {
-    HK_CUDA(cudaMemcpyAsync(h_ctr_.p, W_.ctr, sizeof(WfCounters), cudaMemcpyDeviceToHost, stream_));
+    HK_CUDA(cudaMemcpyAsync(h_ctr_.p, W_.ctr, offsetof(WfCounters, log_n), cudaMemcpyDeviceToHost, stream_));
     HK_CUDA(cudaMemcpyAsync(h_fin_.p, finished_.p, sizeof(unsigned long long) * kWfMaxJobs, cudaMemcpyDeviceToHost,
                             stream_));
     HK_CUDA(cudaEventRecord(ev_done_, stream_));
 }
 
 void WfEngine::add_counters(unsigned long long *out_dev) { HK_CUDA(wf_launch_counters_add(W_, out_dev, stream_)); }
+
+int WfEngine::launch_log(int which, uint32_t *rays, int max) {
+    unsigned n = 0;
+    HK_CUDA(cudaMemcpyAsync(&n, &W_.ctr->log_n[which], sizeof n, cudaMemcpyDeviceToHost, stream_));
+    HK_CUDA(cudaStreamSynchronize(stream_));
+    const int k = (int)std::min<unsigned>(n, (unsigned)std::min(max, kWfLaunchLog));
+    if (k > 0) {
+        HK_CUDA(cudaMemcpyAsync(rays, &W_.ctr->log_rays[which][0], sizeof(uint32_t) * k, cudaMemcpyDeviceToHost,
+                                stream_));
+        HK_CUDA(cudaStreamSynchronize(stream_));
+    }
+    return (int)n;
+}
 
 }  // namespace hk

@@ -25,6 +25,7 @@ struct WfEngineConfig {
     int fetch_min_idle_shadow = 0;
     int reg_lean = 0;   // bit 0: extend, bit 1: shadow kernel with the smaller register budget
     int shadow_tests = 0;   // shadow rays' triangle tests: 0 per lane, 1 postponed, 2 shared over the warp
+    int closest_tests = 0;  // closest-hit rays' triangle tests: 0 per lane, 2 shared over the warp
 };
 
 class WfEngine {
@@ -64,6 +65,10 @@ public:
     const unsigned long long *finished() const { return h_fin_.p; }
     // Add the statistics to a caller's 7-slot device array.  Async.
     void add_counters(unsigned long long *out_dev);
+    // Rays of each extend (which 0) / shadow (which 1) launch since the last
+    // reset, in launch order: up to max of them into rays (host); returns the
+    // number of launches.  Synchronises the engine's stream.
+    int launch_log(int which, uint32_t *rays, int max);
     const WfState &state() const { return W_; }
 
 private:

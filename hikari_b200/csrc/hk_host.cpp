@@ -58,6 +58,17 @@ inline float lum(const float *c) { return c[0] * 0.212671f + c[1] * 0.715160f + 
 inline float clampf(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
 // DiscretePDF1D ctor (src/core/DiscretePDF.cpp:5): cdf in float, normalised.
+// Guide table of a CDF c[0..n] (the cutpoint method): g[k], k = 0..G, is the
+// first index i with c[i] >= k / G (n + 1 if none).  A u in [k / G, (k+1) / G)
+// has its lower bound in [g[k], g[k+1]], so a search there returns the index
+// the search over the whole CDF returns.  G is a power of two, so k / G and
+// u * G are exact in float.
+constexpr int kCdfGuide = hk::kEnvGuide;
+void cdf_guide(const float *c, int n, int32_t *g) {
+    for (int k = 0; k <= kCdfGuide; ++k)
+        g[k] = (int32_t)(std::lower_bound(c, c + n + 1, (float)k / (float)kCdfGuide) - c);
+}
+
 struct Pdf1D {
     std::vector<float> func, cdf;
     float integral = 0.0f;
@@ -232,7 +243,8 @@ struct hk_scene {
     hk::DevScene dev{};
     int32_t accel = HK_ACCEL_BVH8;
     DevBuf b_tris, b_nodes, b_wnodes, b_tri_normals, b_tri_uv, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
-        b_light_cdf, b_delta, b_textures, b_texels, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab;
+        b_light_cdf, b_delta, b_textures, b_texels, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab,
+        b_env_marg_guide, b_env_cond_guide;
     DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
     std::vector<std::unique_ptr<DevBuf>> batch_films;   // films of hk_render_batch_host
     hk_scene_info info{};
@@ -741,6 +753,7 @@ void build_scene(hk_scene *s) {
             }
         }
         std::vector<float> ccdf((size_t)H * (W + 1)), cfunc((size_t)H * W), cint(H), marg(H);
+        std::vector<int32_t> cguide((size_t)H * (kCdfGuide + 1)), mguide(kCdfGuide + 1);
         for (uint32_t y = 0; y < H; y++) {
             Pdf1D r;
             r.build(&lumv[(size_t)y * W], (int)W);
@@ -748,9 +761,15 @@ void build_scene(hk_scene *s) {
             std::copy(r.func.begin(), r.func.end(), cfunc.begin() + (size_t)y * W);
             cint[y] = r.integral;
             marg[y] = r.integral;
+            cdf_guide(r.cdf.data(), (int)W, &cguide[(size_t)y * (kCdfGuide + 1)]);
         }
         Pdf1D mp;
         mp.build(marg.data(), (int)H);
+        cdf_guide(mp.cdf.data(), (int)H, mguide.data());
+        s->b_env_marg_guide.upload(mguide); track(s->b_env_marg_guide);
+        s->b_env_cond_guide.upload(cguide); track(s->b_env_cond_guide);
+        D.env_marg_guide = s->b_env_marg_guide.as<int32_t>();
+        D.env_cond_guide = s->b_env_cond_guide.as<int32_t>();
         s->b_env_rgb.upload(rgb4); track(s->b_env_rgb);
         s->b_env_marg_cdf.upload(mp.cdf); track(s->b_env_marg_cdf);
         s->b_env_marg_func.upload(mp.func); track(s->b_env_marg_func);
@@ -850,7 +869,7 @@ hk::WfEngine &wf_ensure(hk_scene *s, const hk::WfEngineConfig &c) {
         if (o.capacity == c.capacity && o.threads_extend == c.threads_extend && o.threads_shade == c.threads_shade &&
             o.fetch_steps == c.fetch_steps && o.fetch_min_idle == c.fetch_min_idle &&
             o.fetch_steps_shadow == c.fetch_steps_shadow && o.fetch_min_idle_shadow == c.fetch_min_idle_shadow &&
-            o.reg_lean == c.reg_lean && o.shadow_tests == c.shadow_tests)
+            o.reg_lean == c.reg_lean && o.shadow_tests == c.shadow_tests && o.closest_tests == c.closest_tests)
             return *s->wf;
         s->wf.reset();
     }
@@ -869,6 +888,8 @@ SceneView scene_view(hk_scene *s) {
     v.sm_count = s->sm_count;
     v.width = s->width;
     v.height = s->height;
+    v.cfg = &s->wf_cfg;
+    v.has_cfg = &s->has_wf_cfg;
     return v;
 }
 
@@ -1130,6 +1151,16 @@ int hk_scene_tree_build_seconds(const hk_scene *s, double *seconds) {
     return guarded([&] {
         if (!s || !seconds) throw HkError{HK_ERR_INVALID, "bad arguments"};
         *seconds = s->tree_build_s;
+        return HK_OK;
+    });
+}
+int hk_wavefront_launch_log(hk_scene *s, int32_t which, uint32_t *rays_host, int32_t max, int32_t *launches) {
+    return guarded([&] {
+        require_built(s);
+        if ((which != 0 && which != 1) || max < 0 || (max > 0 && !rays_host) || !launches)
+            throw HkError{HK_ERR_INVALID, "bad arguments"};
+        if (!s->wf) throw HkError{HK_ERR_INVALID, "the scene has not rendered with the wavefront integrator"};
+        *launches = s->wf->launch_log(which, rays_host, max);
         return HK_OK;
     });
 }
@@ -1421,6 +1452,7 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         ec.fetch_min_idle_shadow = c.fetch_min_idle_shadow > 0 ? std::min(32, c.fetch_min_idle_shadow) : 0;
         ec.reg_lean = c.reg_lean & 3;
         ec.shadow_tests = c.shadow_tests >= 0 && c.shadow_tests <= 2 ? c.shadow_tests : 0;
+        ec.closest_tests = c.closest_tests == 2 ? 2 : 0;
         hk::WfEngine &E = wf_ensure(s, ec);
         cudaStream_t user = (cudaStream_t)stream, st = E.stream();
         // order after the caller's stream (the films may have been cleared there)
@@ -1438,6 +1470,7 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         for (int j = 0; j < njobs; ++j) {
             if (!jobs[j].film_dev) throw HkError{HK_ERR_INVALID, "bad job: null film"};
             hk::WfJob J = hk::make_wf_job(s, jobs[j].desc);
+            J.sample_major = c.sample_major ? 1 : 0;
             J.film = jobs[j].film_dev;
             E.set_job(j, J);
             plan[j] = hk::WfSeg{total, 0, j, 0};
@@ -1522,18 +1555,24 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
         const int checks[] = {16, 64};
         const int steps8[] = {2, 3, 6}, steps2[] = {4, 8, 16};
         const int min_idle[] = {1, 8, 16};
+        // a configuration's time: the better of two timed renders after a warm one
+        // (one timed render lets run-to-run noise of a few percent pick the configuration)
         auto run = [&](const hk_wavefront_config &c) {
             HK_CUDA(cudaMemset(film.p, 0, film.bytes));
             int rc = hk_render_batch(s, &job, 1, &c, nullptr, nullptr);   // warm (allocation, graph)
             if (rc != HK_OK) throw HkError{rc, hk_last_error()};
-            HK_CUDA(cudaEventRecord(e0, nullptr));
-            rc = hk_render_batch(s, &job, 1, &c, nullptr, nullptr);
-            if (rc != HK_OK) throw HkError{rc, hk_last_error()};
-            HK_CUDA(cudaEventRecord(e1, nullptr));
-            HK_CUDA(cudaEventSynchronize(e1));
-            float ms = 0;
-            HK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            return ms;
+            float best_ms = INFINITY;
+            for (int rep = 0; rep < 2; ++rep) {
+                HK_CUDA(cudaEventRecord(e0, nullptr));
+                rc = hk_render_batch(s, &job, 1, &c, nullptr, nullptr);
+                if (rc != HK_OK) throw HkError{rc, hk_last_error()};
+                HK_CUDA(cudaEventRecord(e1, nullptr));
+                HK_CUDA(cudaEventSynchronize(e1));
+                float ms = 0;
+                HK_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                best_ms = std::min(best_ms, ms);
+            }
+            return best_ms;
         };
         // coordinate descent: capacity, then block sizes, then the check interval
         hk_wavefront_config c{};
@@ -1598,6 +1637,18 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
                 float ms = run(c);
                 if (ms < best_t) { best_t = ms; bc = c; }
             }
+            // and the closest-hit rays' shared out
+            c = bc;
+            c.closest_tests = 2;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        // work items sample by sample
+        c = bc;
+        c.sample_major = 1;
+        {
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

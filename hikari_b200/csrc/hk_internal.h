@@ -13,6 +13,10 @@ struct SceneView {
     const DevScene *dev;   // device description; valid while the scene lives and is not rebuilt
     int sm_count;
     uint32_t width, height;   // scene camera's image size
+    // the scene's wavefront configuration (autotuner or caller) when *has_cfg;
+    // both point into the scene and stay valid while it lives
+    const hk_wavefront_config *cfg;
+    const bool *has_cfg;
 };
 // Throws HkError when the scene is null or not built.
 SceneView scene_view(hk_scene *s);

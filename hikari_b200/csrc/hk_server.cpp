@@ -230,7 +230,20 @@ void hk_server::admit(const std::vector<SceneEntry *> &sc) {
         }
         if ((int)e.jobs.size() >= cfg.max_jobs || used + need + pool > budget) break;   // arrival order: wait
         if (!e.eng) {
-            e.eng.reset(new hk::WfEngine(*e.view.dev, e.view.sm_count, ec));
+            // the server's pool size and block sizes; the traversal knobs of
+            // the scene's own configuration where it has one (autotuned)
+            hk::WfEngineConfig sec = ec;
+            if (*e.view.has_cfg) {
+                const hk_wavefront_config &t = *e.view.cfg;
+                sec.fetch_steps = std::max(0, std::min(1024, t.fetch_steps));
+                sec.fetch_min_idle = t.fetch_min_idle > 0 ? std::min(32, t.fetch_min_idle) : 1;
+                sec.fetch_steps_shadow = std::max(0, std::min(1024, t.fetch_steps_shadow));
+                sec.fetch_min_idle_shadow = t.fetch_min_idle_shadow > 0 ? std::min(32, t.fetch_min_idle_shadow) : 0;
+                sec.reg_lean = t.reg_lean & 3;
+                sec.shadow_tests = t.shadow_tests >= 0 && t.shadow_tests <= 2 ? t.shadow_tests : 0;
+                sec.closest_tests = t.closest_tests == 2 ? 2 : 0;
+            }
+            e.eng.reset(new hk::WfEngine(*e.view.dev, e.view.sm_count, sec));
             e.free_slots.clear();
             for (int k = cfg.max_jobs - 1; k >= 0; --k) e.free_slots.push_back(k);
             std::lock_guard<std::mutex> lk(mu);

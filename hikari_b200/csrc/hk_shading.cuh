@@ -188,6 +188,19 @@ __device__ __forceinline__ int cdf_find(const float *cdf, int n, float u) {
     return clampi(lo - 1, 0, n - 1);
 }
 
+// cdf_find through a guide table (cutpoint method): g[k] is the first index
+// with cdf >= k / kEnvGuide, so the lower bound of u lies in [g[k], g[k+1]]
+// for k = floor(u * kEnvGuide) and the search there returns cdf_find's index.
+__device__ __forceinline__ int cdf_find_guided(const float *cdf, int n, float u, const int32_t *g) {
+    const int k = min((int)(u * (float)kEnvGuide), kEnvGuide - 1);
+    int lo = __ldg(g + k), hi = __ldg(g + k + 1);
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(cdf + mid) < u) lo = mid + 1; else hi = mid;
+    }
+    return clampi(lo - 1, 0, n - 1);
+}
+
 // AreaLight::Pdf / Eval (src/emitter/AreaLight.cpp:38,59)
 __device__ __forceinline__ float area_pdf(const DevAreaLight &L, const ERec &r) {
     float gd = fabsf(dot(r.wi * -1.0f, r.n));
@@ -235,10 +248,11 @@ __device__ __forceinline__ void spherical_coords(V3 d, float &th, float &ph) {
 __device__ __forceinline__ V3 env_texel(const DevScene &S, int y, int x) {
     return xyz(__ldg(S.env_rgb + (uint64_t)y * S.env_w + x));
 }
-// DiscretePDF1D::SampleContinuous (src/core/DiscretePDF.cpp:39)
+// DiscretePDF1D::SampleContinuous (src/core/DiscretePDF.cpp:39), the index
+// found through the CDF's guide table
 __device__ __forceinline__ float sample_cont(const float *cdf, const float *func, float integral, int n, float u,
-                                             float &pdf, int &idx) {
-    idx = cdf_find(cdf, n, u);
+                                             float &pdf, int &idx, const int32_t *guide) {
+    idx = cdf_find_guided(cdf, n, u, guide);
     float c0 = __ldg(cdf + idx), c1 = __ldg(cdf + idx + 1);
     float du = u - c0;
     if (c1 - c0 > 0.0f) du /= (c1 - c0);
@@ -281,9 +295,10 @@ __device__ __forceinline__ V3 env_sample(const DevScene &S, ERec &r, float ux, f
     if (S.env_kind == kEnvConstant) return const_sample(S, r, ux, uy);
     float py, px;
     int iy, ix;
-    float dy = sample_cont(S.env_marg_cdf, S.env_marg_func, S.env_marg_int, (int)S.env_h, uy, py, iy);
+    float dy = sample_cont(S.env_marg_cdf, S.env_marg_func, S.env_marg_int, (int)S.env_h, uy, py, iy, S.env_marg_guide);
     float dx = sample_cont(S.env_cond_cdf + (uint64_t)iy * (S.env_w + 1), S.env_cond_func + (uint64_t)iy * S.env_w,
-                           __ldg(S.env_cond_int + iy), (int)S.env_w, ux, px, ix);
+                           __ldg(S.env_cond_int + iy), (int)S.env_w, ux, px, ix,
+                           S.env_cond_guide + (uint64_t)iy * (kEnvGuide + 1));
     float mp = px * py;
     float th = dy * kPi, st = sinf(th);
     if (mp == 0.0f) return v3(0, 0, 0);

@@ -516,6 +516,113 @@ struct Bvh8Walker {
         return false;
     }
 
+    // One step of a closest-hit ray with the warp's triangle tests shared out,
+    // numbered and dealt as in step_any_shared: lane j of round r tests
+    // triangle r + j with the watertight test against its owner's ray (rays:
+    // origin + tmin and the packed watertight constants per lane; the owner's
+    // current tmax by shuffle).  Per owner the hit of least t wins and, on
+    // equal t, the one later in the owner's test order: the hit that the
+    // serial loop of step() keeps, since it accepts t <= tmax and then shrinks
+    // tmax to t.  A group that spans two rounds sees the first round's tmax in
+    // the second, as the serial loop would.
+    __device__ __forceinline__ bool step_closest_shared(const DevScene &S, bool alive, const float4 *rays) {
+        const unsigned lane = threadIdx.x & 31u;
+        uint2 grp = make_uint2(0u, 0u);
+        if (alive) {
+            if (ng.y > 0x00ffffffu) {
+                const uint32_t b = __ffs(ng.y >> 24) - 1;
+                ng.y &= ~(1u << (24 + b));
+                const uint32_t slot = b ^ ko;
+                const uint32_t child = ng.x + __popc(ng.y & 0xffu & ((1u << slot) - 1u));
+                if (ng.y > 0x00ffffffu) stk.push(ng);
+                visit(S, child);
+                grp = tg;
+            } else {
+                grp = ng;
+                ng = make_uint2(0u, 0u);
+            }
+            tg = make_uint2(0u, 0u);
+        }
+        const uint32_t cnt = __popc(grp.y);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t excl = incl - cnt;
+        ntri += cnt;
+        for (uint32_t r = 0; r < total; r += 32) {   // warp-uniform
+            const uint32_t w = r + lane;
+            uint32_t own = 0;
+#pragma unroll
+            for (uint32_t b = 16; b > 0; b >>= 1) {
+                const uint32_t v = __shfl_sync(0xffffffffu, incl, own + b - 1);
+                if (v <= w) own += b;
+            }
+            const uint32_t obase = __shfl_sync(0xffffffffu, grp.x, own);
+            const uint32_t omask = __shfl_sync(0xffffffffu, grp.y, own);
+            const uint32_t oexcl = __shfl_sync(0xffffffffu, excl, own);
+            const float otmax = __shfl_sync(0xffffffffu, tmax, own);
+            // (t, 31 - lane): the least key is the least t, then the latest lane
+            unsigned long long key = ~0ull;
+            float tt = 0.0f, uu = 0.0f, vv = 0.0f;
+            uint32_t tri = 0u;
+            if (w < total) {
+                tri = obase + __fns(omask, 0u, (int)(w - oexcl) + 1);
+                const float4 *tp = S.tris + 3 * (size_t)tri;
+                const float4 p0 = ldg4(tp), p1 = ldg4(tp + 1), p2 = ldg4(tp + 2);
+                const float4 ro = rays[2 * own], rw = rays[2 * own + 1];
+                const uint32_t kp = __float_as_uint(rw.w);
+                WatertightRay wr;
+                wr.kx = (int)(kp & 3u);
+                wr.ky = (int)((kp >> 2) & 3u);
+                wr.kz = (int)((kp >> 4) & 3u);
+                wr.sx = rw.x;
+                wr.sy = rw.y;
+                wr.sz = rw.z;
+                if (intersect_watertight(wr, xyz(ro), xyz(p0), xyz(p1), xyz(p2), ro.w, otmax, tt, uu, vv)) {
+                    const uint32_t tb = __float_as_uint(tt);
+                    const uint32_t ord = (tb & 0x80000000u) ? ~tb : (tb | 0x80000000u);   // order of the floats
+                    key = ((unsigned long long)ord << 32) | (31u - lane);
+                }
+            }
+            // least key within each owner's run of lanes (runs are contiguous)
+#pragma unroll
+            for (int s = 1; s < 32; s <<= 1) {
+                const unsigned long long k2 = __shfl_down_sync(0xffffffffu, key, s);
+                const uint32_t o2 = __shfl_down_sync(0xffffffffu, own, s);
+                if (lane + (unsigned)s < 32u && o2 == own && k2 < key) key = k2;
+            }
+            // this lane's run in round r starts at lane lo
+            const int lo = max((int)excl - (int)r, 0), hi = min((int)incl - (int)r, 32);
+            const unsigned long long mk = __shfl_sync(0xffffffffu, key, lo < hi ? lo : 0);
+            const uint32_t wl = 31u - (uint32_t)(mk & 31u);
+            const float wt = __shfl_sync(0xffffffffu, tt, wl), wu = __shfl_sync(0xffffffffu, uu, wl),
+                        wv = __shfl_sync(0xffffffffu, vv, wl);
+            const uint32_t wtri = __shfl_sync(0xffffffffu, tri, wl);
+            if (lo < hi && mk != ~0ull) {
+                found = true;
+                hit.t = wt; hit.u = wu; hit.v = wv; hit.tri = (int)wtri;
+                tmax = wt;
+            }
+        }
+        if (!alive) return false;
+        if (ng.y <= 0x00ffffffu) {
+            if (stk.sp == 0) return true;
+            ng = stk.pop();
+        }
+        return false;
+    }
+
+    // The per-lane record step_closest_shared reads: origin + tmin, and the
+    // watertight constants with kx | ky << 2 | kz << 4 in the last word.
+    __device__ __forceinline__ void closest_record(float4 *dst) const {
+        dst[0] = make_float4(o.x, o.y, o.z, tmin);
+        dst[1] = make_float4(w.sx, w.sy, w.sz, __uint_as_float((uint32_t)w.kx | ((uint32_t)w.ky << 2) | ((uint32_t)w.kz << 4)));
+    }
+
     // Intersect the 8 children of node `child`: ng / tg become its groups.
     __device__ __forceinline__ void visit(const DevScene &S, uint32_t child) {
         const uint4 *np = S.wnodes + 5 * (size_t)child;
@@ -662,14 +769,15 @@ __device__ __forceinline__ void trace_queue(const DevScene &S, Walker &wk, unsig
     }
 }
 
-// trace_queue for any-hit rays with the warp's triangle tests shared out
-// (Bvh8Walker::step_any_shared): the same refills, but every lane takes every
-// step, lanes without a ray as idle partners.  rays: 2 float4 per thread of
-// the block (shared memory), written here when a lane takes a ray.
-template <class Walker, class Load, class Store>
-__device__ __forceinline__ void trace_queue_any_shared(const DevScene &S, Walker &wk, unsigned *fetch, unsigned n,
-                                                       int steps, int min_idle, float4 *rays, Load load, Store store,
-                                                       TravStats &st) {
+// trace_queue with the warp's triangle tests shared out
+// (Bvh8Walker::step_any_shared for any-hit rays, step_closest_shared for
+// closest-hit rays): the same refills, but every lane takes every step, lanes
+// without a ray as idle partners.  rays: 2 float4 per thread of the block
+// (shared memory), written here when a lane takes a ray.
+template <bool kAnyHit, class Walker, class Load, class Store>
+__device__ __forceinline__ void trace_queue_shared(const DevScene &S, Walker &wk, unsigned *fetch, unsigned n,
+                                                   int steps, int min_idle, float4 *rays, Load load, Store store,
+                                                   TravStats &st) {
     const unsigned lane = threadIdx.x & 31u;
     float4 *mine = rays + 2 * threadIdx.x;
     const float4 *warp_rays = rays + 2 * (threadIdx.x & ~31u);
@@ -698,8 +806,12 @@ __device__ __forceinline__ void trace_queue_any_shared(const DevScene &S, Walker
                     item = (int)idx;
                     const Ray r = load(item);
                     wk.begin(S, r);
-                    mine[0] = make_float4(r.o.x, r.o.y, r.o.z, r.tmin);
-                    mine[1] = make_float4(r.d.x, r.d.y, r.d.z, r.tmax);
+                    if constexpr (kAnyHit) {
+                        mine[0] = make_float4(r.o.x, r.o.y, r.o.z, r.tmin);
+                        mine[1] = make_float4(r.d.x, r.d.y, r.d.z, r.tmax);
+                    } else {
+                        wk.closest_record(mine);
+                    }
                 } else {
                     exhausted = true;
                 }
@@ -708,9 +820,11 @@ __device__ __forceinline__ void trace_queue_any_shared(const DevScene &S, Walker
         if (!__any_sync(0xffffffffu, item >= 0)) break;
         __syncwarp();   // the new rays are visible to the warp's other lanes
         for (int k = 0; k < steps; ++k) {
-            const bool done = wk.step_any_shared(S, item >= 0, warp_rays);
+            bool done;
+            if constexpr (kAnyHit) done = wk.step_any_shared(S, item >= 0, warp_rays);
+            else done = wk.step_closest_shared(S, item >= 0, warp_rays);
             if (item >= 0 && done) {
-                wk.template end<true>(S, st);
+                wk.template end<kAnyHit>(S, st);
                 store(item, wk);
                 item = -1;
             }

@@ -59,85 +59,117 @@ static_assert(kWfTypes == 12, "launch_shade_all launches one kernel per shade qu
 // Splat and retire the finished paths, then give every finished or idle slot
 // new work from the dispatch plan; slots that find none wait in the next idle
 // list.  Queues read here: fq, idle[cur]; written: eq[cur], idle[cur ^ 1].
-// The per-job finished counts and the change of the in-flight count are
-// gathered per block in shared memory and added once per block: a global
-// atomic per path on a handful of addresses would serialise at the L2.
-__global__ void wf_regen_kernel(DevScene S, WfState W, int cur) {
+// Slot i of the n slots that want work (finished paths first, then idle
+// slots) takes plan item next_work + i: the items are dealt without an
+// atomic, and wf_reset_kernel advances next_work by n afterwards.  An item
+// whose pixel lies outside its image (the partial tiles at the right and
+// bottom edges) counts as work done and leaves its slot idle until the next
+// iteration.  Appends to the extend and idle lists, the per-job finished
+// counts and the change of the in-flight count are gathered per block in
+// shared memory and added once per block and round: a global atomic per warp
+// on a handful of addresses serialises at the L2.
+__global__ void __launch_bounds__(256) wf_regen_kernel(DevScene S, WfState W, int cur) {
     __shared__ unsigned s_finished[kWfMaxJobs];
     __shared__ int s_active;
+    __shared__ unsigned s_warp[2][8];   // per-warp counts, then offsets, of the extend / idle appends
+    __shared__ unsigned s_base[2];
     for (int k = threadIdx.x; k < kWfMaxJobs; k += blockDim.x) s_finished[k] = 0u;
     if (threadIdx.x == 0) s_active = 0;
     __syncthreads();
     const int nf = (int)W.ctr->fq_count;
     const int n = nf + (int)W.ctr->idle_count[cur];
     const uint64_t total = W.ctr->total_work;
+    const uint64_t first = W.ctr->next_work;
     const int nseg = (int)W.ctr->seg_count;
+    const unsigned lane = lane_id(), warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     unsigned long long dropped = 0;
     int active_delta = 0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        int slot;
-        if (i < nf) {
-            slot = W.fq[i];
-            float4 p = W.pix[slot];
-            float4 L = W.lacc[slot];
-            const int pj = __float_as_int(p.z);
-            const WfJob &J = W.jobs[pj];
-            V3 val = v3(L.x, L.y, L.z);
-            if (is_valid(val)) splat_global(S, J, p.x, p.y, val);
-            else ++dropped;
-            atomicAdd(&s_finished[pj], 1u);
-            --active_delta;
-        } else {
-            slot = W.idle[cur][i - nf];
-        }
-        // claim plan items until a pixel inside its image or the plan runs dry
+    for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {   // block-uniform rounds
+        const int i = i0 + (int)threadIdx.x;
+        int slot = -1;
         bool started = false;
-        while (W.ctr->next_work < total) {
-            unsigned mask = __activemask();
-            int leader = __ffs(mask) - 1;
-            unsigned rank = __popc(mask & ((1u << lane_id()) - 1u));
-            unsigned long long base = 0;
-            if ((int)lane_id() == leader) base = atomicAdd(&W.ctr->next_work, (unsigned long long)__popc(mask));
-            base = __shfl_sync(mask, base, leader);
-            const uint64_t w = base + rank;
-            if (w >= total) break;
-            const WfSeg &G = W.segs[find_seg(W, w, nseg)];
-            const int j = G.job;
-            const WfJob &J = W.jobs[j];
-            const uint64_t l = G.job_begin + (w - G.plan_begin);
-            const uint32_t p = (uint32_t)(l % kWfTilePixels);
-            const uint64_t ts = l / kWfTilePixels;
-            const uint32_t s = (uint32_t)(ts % J.spp);
-            const uint32_t t = (uint32_t)(ts / J.spp);
-            const uint32_t x = (t % J.tiles_x) * kWfTileSide + p % kWfTileSide;
-            const uint32_t y = (t / J.tiles_x) * kWfTileSide + p / kWfTileSide;
-            if (x >= J.width || y >= J.height) {
-                atomicAdd(&s_finished[j], 1u);   // counted as work done: no path
-                continue;
+        if (i < n) {
+            if (i < nf) {
+                slot = W.fq[i];
+                float4 p = W.pix[slot];
+                float4 L = W.lacc[slot];
+                const int pj = __float_as_int(p.z);
+                const WfJob &J = W.jobs[pj];
+                V3 val = v3(L.x, L.y, L.z);
+                if (is_valid(val)) splat_global(S, J, p.x, p.y, val);
+                else ++dropped;
+                atomicAdd(&s_finished[pj], 1u);
+                --active_delta;
+            } else {
+                slot = W.idle[cur][i - nf];
             }
-            Pcg32 rng;
-            rng.seed(wf_mix_seed(J.seed, (uint64_t)J.sample_offset + s),
-                     (uint64_t)y * J.width + x + (uint64_t)J.image_index * J.width * J.height);
-            float px = (float)x + rng.nextf(), py = (float)y + rng.nextf();
-            Ray r = camera_ray_job(S, J, px, py);
-            W.ray_o[slot] = f4(r.o, r.tmin);
-            W.ray_d[slot] = f4(r.d, r.tmax);
-            W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-            W.lacc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            W.pix[slot] = make_float4(px, py, __int_as_float(j), __int_as_float(0));
-            W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
-                                     (uint32_t)(rng.inc >> 32));
-            W.eq[cur][warp_append(&W.ctr->eq_count[cur])] = slot;
-            ++active_delta;
-            started = true;
-            break;
+            const uint64_t w = first + (uint64_t)i;
+            if (w < total) {
+                const WfSeg &G = W.segs[find_seg(W, w, nseg)];
+                const int j = G.job;
+                const WfJob &J = W.jobs[j];
+                const uint64_t l = G.job_begin + (w - G.plan_begin);
+                const uint32_t p = (uint32_t)(l % kWfTilePixels);
+                const uint64_t ts = l / kWfTilePixels;
+                uint32_t s, t;
+                if (J.sample_major) {
+                    const uint64_t ntiles = J.work_count / ((uint64_t)J.spp * kWfTilePixels);
+                    t = (uint32_t)(ts % ntiles);
+                    s = (uint32_t)(ts / ntiles);
+                } else {
+                    s = (uint32_t)(ts % J.spp);
+                    t = (uint32_t)(ts / J.spp);
+                }
+                const uint32_t x = (t % J.tiles_x) * kWfTileSide + p % kWfTileSide;
+                const uint32_t y = (t / J.tiles_x) * kWfTileSide + p / kWfTileSide;
+                if (x >= J.width || y >= J.height) {
+                    atomicAdd(&s_finished[j], 1u);   // counted as work done: no path
+                } else {
+                    Pcg32 rng;
+                    rng.seed(wf_mix_seed(J.seed, (uint64_t)J.sample_offset + s),
+                             (uint64_t)y * J.width + x + (uint64_t)J.image_index * J.width * J.height);
+                    float px = (float)x + rng.nextf(), py = (float)y + rng.nextf();
+                    Ray r = camera_ray_job(S, J, px, py);
+                    W.ray_o[slot] = f4(r.o, r.tmin);
+                    W.ray_d[slot] = f4(r.d, r.tmax);
+                    W.beta[slot] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+                    W.lacc[slot] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    W.pix[slot] = make_float4(px, py, __int_as_float(j), __int_as_float(0));
+                    W.rng[slot] = make_uint4((uint32_t)rng.state, (uint32_t)(rng.state >> 32), (uint32_t)rng.inc,
+                                             (uint32_t)(rng.inc >> 32));
+                    ++active_delta;
+                    started = true;
+                }
+            }
         }
-        if (!started) W.idle[cur ^ 1][warp_append(&W.ctr->idle_count[cur ^ 1])] = slot;
+        // block-aggregated appends: one atomic per list per block and round
+        const bool to_idle = i < n && !started;
+        const unsigned be = __ballot_sync(0xffffffffu, started), bi = __ballot_sync(0xffffffffu, to_idle);
+        if (lane == 0) {
+            s_warp[0][warp] = __popc(be);
+            s_warp[1][warp] = __popc(bi);
+        }
+        __syncthreads();
+        if (threadIdx.x < 2) {
+            unsigned sum = 0;
+            for (unsigned k = 0; k < nwarps; ++k) {
+                const unsigned c = s_warp[threadIdx.x][k];
+                s_warp[threadIdx.x][k] = sum;
+                sum += c;
+            }
+            unsigned *ctr = threadIdx.x == 0 ? &W.ctr->eq_count[cur] : &W.ctr->idle_count[cur ^ 1];
+            s_base[threadIdx.x] = sum ? atomicAdd(ctr, sum) : 0u;
+        }
+        __syncthreads();
+        const unsigned below = (1u << lane) - 1u;
+        if (started) W.eq[cur][s_base[0] + s_warp[0][warp] + __popc(be & below)] = slot;
+        if (to_idle) W.idle[cur ^ 1][s_base[1] + s_warp[1][warp] + __popc(bi & below)] = slot;
+        __syncthreads();   // s_warp and s_base are rewritten by the next round
     }
     if (dropped) atomicAdd(&W.ctr->dropped, dropped);
     // one atomic per warp into the block, one per block and job into HBM
     for (int o = 16; o > 0; o >>= 1) active_delta += __shfl_down_sync(0xffffffffu, active_delta, o);
-    if (lane_id() == 0 && active_delta) atomicAdd(&s_active, active_delta);
+    if (lane == 0 && active_delta) atomicAdd(&s_active, active_delta);
     __syncthreads();
     for (int k = threadIdx.x; k < kWfMaxJobs; k += blockDim.x)
         if (s_finished[k]) atomicAdd(W.jobs[k].finished, (unsigned long long)s_finished[k]);
@@ -148,6 +180,9 @@ __global__ void wf_regen_kernel(DevScene S, WfState W, int cur) {
 // phases fill.
 __global__ void wf_reset_kernel(WfState W, int cur) {
     if (threadIdx.x == 0) {
+        // regen dealt plan items next_work .. next_work + n - 1 to its n slots
+        const unsigned long long dealt = W.ctr->next_work + W.ctr->fq_count + W.ctr->idle_count[cur];
+        W.ctr->next_work = dealt < W.ctr->total_work ? dealt : W.ctr->total_work;
         W.ctr->fq_count = 0;
         W.ctr->idle_count[cur] = 0;
         W.ctr->eq_count[cur ^ 1] = 0;
@@ -171,6 +206,7 @@ __global__ void wf_init_kernel(WfState W) {
         c->ext_fetch = c->sh_fetch = 0;
         c->rays = c->shadow_rays = c->dropped = 0;
         c->node_visits = c->tri_tests = c->node_visits_shadow = c->tri_tests_shadow = 0;
+        c->log_n[0] = c->log_n[1] = 0;
     }
 }
 

@@ -48,7 +48,11 @@ struct WfJob {
     uint32_t width, height;
     float cam_aspect;               // width / height (PerspectiveCamera::Activate)
     int32_t depth, rr_start;
-    int32_t pad;
+    // order of the job's work items: 0 tile by tile (all samples of a tile,
+    // then the next tile: partial images show finished tiles); 1 sample by
+    // sample (every tile's sample s, then s + 1: the paths in flight splat
+    // over the whole image rather than over a few tiles)
+    int32_t sample_major;
 };
 
 // One piece of the dispatch plan: work items [plan_begin, next piece's
@@ -63,6 +67,8 @@ struct WfSeg {
 
 // Device-wide counters of the engine (one struct in HBM).  The first three
 // fields are the dispatch head, rewritten by the host with each plan.
+constexpr int kWfLaunchLog = 1024;   // launches whose ray counts the counters keep
+
 struct WfCounters {
     unsigned long long next_work;      // next plan item to hand out
     unsigned long long total_work;     // plan items in the current plan
@@ -79,6 +85,10 @@ struct WfCounters {
     unsigned long long rays, shadow_rays, dropped;
     unsigned long long node_visits, tri_tests;                 // closest-hit traversal (extend)
     unsigned long long node_visits_shadow, tri_tests_shadow;   // any-hit traversal (shadow)
+    // rays of each extend (0) / shadow (1) launch since the last reset, in
+    // launch order (profiling; the host's status copies stop before it)
+    unsigned int log_n[2];
+    unsigned int log_rays[2][kWfLaunchLog];
 };
 
 struct WfState {
@@ -120,6 +130,7 @@ struct WfLaunchConfig {
     int fetch_steps_shadow, fetch_min_idle_shadow;   // and of the shadow kernel
     int lean_extend, lean_shadow;                    // traversal kernels with the smaller register budget
     int shadow_tests;   // shadow rays' triangle tests: 0 per lane, 1 postponed, 2 shared over the warp
+    int closest_tests;  // closest-hit rays' triangle tests: 0 per lane (postponed where the tree allows), 2 shared
 };
 
 // empty pool: every slot idle, queues and statistics zero (the dispatch head is the host's)

@@ -110,7 +110,9 @@ __device__ __forceinline__ SharedStack make_stack() {
 // picks per kernel (hk_wavefront_config.reg_lean).
 constexpr int kLeanBlocks = 5;
 
-template <int kAccel, int kMinBlocks>
+// kShared: the warp's triangle tests shared out over its lanes (8-wide tree;
+// the block's ray records in dynamic shared memory after the stacks).
+template <int kAccel, int kMinBlocks, bool kShared>
 __global__ void __launch_bounds__(256, kMinBlocks) wf_extend_kernel(DevScene S, WfState W, int cur, int steps, int min_idle) {
     const unsigned n = W.ctr->eq_count[cur];
     TravStats ts;
@@ -123,29 +125,33 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_extend_kernel(DevScene S, 
         wk.stack = stack_mem;
     }
     int slot = -1;
-    trace_queue<false>(
-        S, wk, &W.ctr->ext_fetch, n, steps, min_idle,
-        [&](int i) {
-            slot = W.eq[cur][i];
-            const float4 o = W.ray_o[slot], d = W.ray_d[slot];
-            Ray r;
-            r.o = v3(o.x, o.y, o.z);
-            r.d = v3(d.x, d.y, d.z);
-            r.tmin = o.w;
-            r.tmax = d.w;
-            return r;
-        },
-        [&](int, const auto &w) {
-            int type = 0;
-            if (w.found) {
-                const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
-                const DevBsdf &B = S.bsdfs[S.meshes[mesh].bsdf];
-                type = wf_queue_of(B.type, B.textured != 0);
-            }
-            W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
-            W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
-        },
-        ts);
+    auto load = [&](int i) {
+        slot = W.eq[cur][i];
+        const float4 o = W.ray_o[slot], d = W.ray_d[slot];
+        Ray r;
+        r.o = v3(o.x, o.y, o.z);
+        r.d = v3(d.x, d.y, d.z);
+        r.tmin = o.w;
+        r.tmax = d.w;
+        return r;
+    };
+    auto store = [&](int, const auto &w) {
+        int type = 0;
+        if (w.found) {
+            const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
+            const DevBsdf &B = S.bsdfs[S.meshes[mesh].bsdf];
+            type = wf_queue_of(B.type, B.textured != 0);
+        }
+        W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
+        W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
+    };
+    if constexpr (kShared && kAccel == kAccelBvh8) {
+        extern __shared__ uint2 wf_stack_smem[];
+        float4 *rays = reinterpret_cast<float4 *>(wf_stack_smem + (size_t)blockDim.x * kShStack);
+        trace_queue_shared<false>(S, wk, &W.ctr->ext_fetch, n, steps, min_idle, rays, load, store, ts);
+    } else {
+        trace_queue<false>(S, wk, &W.ctr->ext_fetch, n, steps, min_idle, load, store, ts);
+    }
     unsigned long long nv = ts.nodes, nt = ts.tris;
     for (int o = 16; o > 0; o >>= 1) {
         nv += __shfl_down_sync(0xffffffffu, nv, o);
@@ -155,7 +161,12 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_extend_kernel(DevScene S, 
         atomicAdd(&W.ctr->node_visits, nv);
         atomicAdd(&W.ctr->tri_tests, nt);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&W.ctr->rays, (unsigned long long)n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&W.ctr->rays, (unsigned long long)n);
+        const unsigned k = W.ctr->log_n[0];   // one thread per launch; launches are stream-ordered
+        if (k < (unsigned)kWfLaunchLog) W.ctr->log_rays[0][k] = n;
+        W.ctr->log_n[0] = k + 1;
+    }
 }
 
 // ------------------------------------------------------------ shade
@@ -379,7 +390,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_shadow_kernel(DevScene S, 
     if constexpr (kShared && kAccel == kAccelBvh8) {
         extern __shared__ uint2 wf_stack_smem[];
         float4 *rays = reinterpret_cast<float4 *>(wf_stack_smem + (size_t)blockDim.x * kShStack);
-        trace_queue_any_shared(S, wk, &W.ctr->sh_fetch, n, steps, min_idle, rays, load, store, ts);
+        trace_queue_shared<true>(S, wk, &W.ctr->sh_fetch, n, steps, min_idle, rays, load, store, ts);
     } else {
         trace_queue<true>(S, wk, &W.ctr->sh_fetch, n, steps, min_idle, load, store, ts);
     }
@@ -392,27 +403,39 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_shadow_kernel(DevScene S, 
         atomicAdd(&W.ctr->node_visits_shadow, nv);
         atomicAdd(&W.ctr->tri_tests_shadow, nt);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&W.ctr->shadow_rays, (unsigned long long)n);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        atomicAdd(&W.ctr->shadow_rays, (unsigned long long)n);
+        const unsigned k = W.ctr->log_n[1];
+        if (k < (unsigned)kWfLaunchLog) W.ctr->log_rays[1][k] = n;
+        W.ctr->log_n[1] = k + 1;
+    }
 }
 
 // ------------------------------------------------------------ launchers
 __host__ inline size_t wf_stack_bytes(int threads) { return (size_t)threads * kShStack * sizeof(uint2); }
 
-template <int kAccel>
-cudaError_t wf_launch_extend_t(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
-    const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(C.threads_extend) : 0;
-    if (C.lean_extend)
-        wf_extend_kernel<kAccel, kLeanBlocks><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, C.fetch_steps,
-                                                                                          C.fetch_min_idle);
-    else
-        wf_extend_kernel<kAccel, 0><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, C.fetch_steps,
-                                                                                C.fetch_min_idle);
-    return cudaGetLastError();
-}
-// dynamic shared memory of a shadow launch: the short stacks, and the rays
-// where the triangle tests are shared out
+// dynamic shared memory of a traversal launch: the short stacks, and the ray
+// records where the triangle tests are shared out
 __host__ inline size_t wf_shadow_smem(int threads, bool shared) {
     return wf_stack_bytes(threads) + (shared ? (size_t)threads * 2 * sizeof(float4) : 0);
+}
+template <int kAccel>
+cudaError_t wf_launch_extend_t(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int cur, cudaStream_t st) {
+    const bool shared = kAccel == kAccelBvh8 && C.closest_tests == 2;
+    const size_t smem = kAccel == kAccelBvh8 ? wf_shadow_smem(C.threads_extend, shared) : 0;
+    const int a = C.fetch_steps, b = C.fetch_min_idle;
+    if (shared) {
+        if (C.lean_extend)
+            wf_extend_kernel<kAccel, kLeanBlocks, true><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, a, b);
+        else
+            wf_extend_kernel<kAccel, 0, true><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, a, b);
+    } else {
+        if (C.lean_extend)
+            wf_extend_kernel<kAccel, kLeanBlocks, false><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, a, b);
+        else
+            wf_extend_kernel<kAccel, 0, false><<<C.blocks_extend, C.threads_extend, smem, st>>>(S, W, cur, a, b);
+    }
+    return cudaGetLastError();
 }
 template <int kAccel>
 cudaError_t wf_launch_shadow_t(const DevScene &S, const WfState &W, const WfLaunchConfig &C, cudaStream_t st) {
@@ -435,15 +458,24 @@ cudaError_t wf_launch_shadow_t(const DevScene &S, const WfState &W, const WfLaun
     return cudaGetLastError();
 }
 // which: 0 extend, 2 shadow; lean: the kLeanBlocks register budget; shared:
-// the shadow kernel with shared triangle tests
+// the kernel with shared triangle tests
 template <int kAccel>
 int wf_trace_occupancy_t(int which, int threads, bool lean, bool shared) {
     int n = 0;
     shared = shared && kAccel == kAccelBvh8;
     if (which == 0) {
-        const size_t smem = kAccel == kAccelBvh8 ? wf_stack_bytes(threads) : 0;
-        if (lean) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, kLeanBlocks>, threads, smem);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, 0>, threads, smem);
+        const size_t smem = kAccel == kAccelBvh8 ? wf_shadow_smem(threads, shared) : 0;
+        if (shared) {
+            if (lean)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, kLeanBlocks, true>, threads,
+                                                              smem);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, 0, true>, threads, smem);
+        } else {
+            if (lean)
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, kLeanBlocks, false>, threads,
+                                                              smem);
+            else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_extend_kernel<kAccel, 0, false>, threads, smem);
+        }
     } else {
         const size_t smem = kAccel == kAccelBvh8 ? wf_shadow_smem(threads, shared) : 0;
         if (shared) {

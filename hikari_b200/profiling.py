@@ -6,18 +6,18 @@ usage: python -m hikari_b200.profiling launches <launches.csv>
        python -m hikari_b200.profiling raw <report.ncu-rep> [regex]
        python -m hikari_b200.profiling render [--views V] [--spp S] [--accel bvh2|bvh8] [--out F]
                                               [--threads-extend T] [--threads-shade T] [--fetch-steps K]
-                                              [--fetch-min-idle K]
-       python -m hikari_b200.profiling traffic <dram.csv> <render.json>
+                                              [--fetch-min-idle K] [--shadow-tests M] [--closest-tests M]
+       python -m hikari_b200.profiling traffic <metrics.csv> <render.json> [skip]
 
 `render` renders the heterogeneous scene once with the wavefront integrator
 (no autotuning, no other launches of the traversal kernels; the launch
 configuration is given on the command line, e.g. the one bench.py's
-autotuner picked) and writes its counters as JSON; run under `ncu --metrics dram__bytes_read.sum,
+autotuner picked) and writes its counters and the rays of every traversal
+launch as JSON; run under `ncu --metrics dram__bytes_read.sum,
 dram__bytes_write.sum,lts__t_bytes.sum,smsp__inst_executed.sum,
-smsp__thread_inst_executed.sum,gpu__time_duration.sum
--k regex:"wf_(extend|shadow)" --cache-control none`, `traffic` turns the
-per-launch sums of that capture into DRAM bytes, L2 bytes and warp
-instructions per closest-hit and per shadow ray.
+smsp__thread_inst_executed.sum,gpu__time_duration.sum -k regex:wf_shadow
+-s <skip> -c 3 --cache-control none`, `traffic` turns the captured launches'
+sums into DRAM bytes, L2 bytes and warp instructions per ray of that kernel.
 """
 import csv
 import io
@@ -94,22 +94,23 @@ BYTE_UNIT = {"byte": 1.0, "Kbyte": 1e3, "Mbyte": 1e6, "Gbyte": 1e9, "Tbyte": 1e1
 INST_UNIT = {"inst": 1.0, "Kinst": 1e3, "Minst": 1e6, "Ginst": 1e9}
 
 
-def traffic(csv_path, render_json):
-    """Per-ray figures of the traversal kernels from a capture of every
-    extend / shadow launch: DRAM bytes (dram__bytes_read.sum +
-    dram__bytes_write.sum), L2 bytes (lts__t_bytes.sum), warp instructions
-    issued (smsp__inst_executed.sum) and active lanes per warp instruction
+def traffic(csv_path, render_json, skip=0):
+    """Per-ray figures of a traversal kernel from a capture of its launches
+    skip, skip + 1, ... (`ncu -k regex:<kernel> -s <skip> -c <n>`, one kernel
+    per capture): DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum),
+    L2 bytes (lts__t_bytes.sum), warp instructions issued
+    (smsp__inst_executed.sum) and active lanes per warp instruction
     (smsp__thread_inst_executed.sum / smsp__inst_executed.sum), each divided
-    by the rays the render traced (closest-hit rays for extend, shadow rays for
-    shadow)."""
+    by the rays those launches traced (the render's per-launch log; closest-
+    hit rays for extend, shadow rays for shadow)."""
     import json
 
-    ctr = json.load(open(render_json))["counters"]
+    log = json.load(open(render_json))["launch_rays"]
     agg = {}
     for lid, kern, metric, val, unit in _metric_rows(csv_path):
         a = agg.setdefault(kern, {"launches": set(), "dram": 0.0, "l2": 0.0, "inst": 0.0, "thread_inst": 0.0,
                                   "ms": 0.0})
-        a["launches"].add(lid)
+        a["launches"].add(int(lid))
         if metric.startswith("dram__bytes"):
             a["dram"] += val * BYTE_UNIT[unit]
         elif metric == "lts__t_bytes.sum":
@@ -123,10 +124,12 @@ def traffic(csv_path, render_json):
     rows = ["| kernel | launches | rays | DRAM bytes per ray | L2 bytes per ray | warp instructions per ray "
             "| lanes per instruction | device ms (ncu) |", "|---|---|---|---|---|---|---|---|"]
     for kern, a in sorted(agg.items()):
-        rays = max(ctr["shadow_rays"] if "shadow" in kern else ctr["rays"], 1)
+        kind = "shadow" if "shadow" in kern else "extend"
+        n = len(a["launches"])
+        rays = max(sum(log[kind][skip + k] for k in range(n) if skip + k < len(log[kind])), 1)
         lanes = a["thread_inst"] / a["inst"] if a["inst"] else float("nan")
-        rows.append(f"| {kern} | {len(a['launches'])} | {rays} | {a['dram'] / rays:.2f} | {a['l2'] / rays:.1f} "
-                    f"| {a['inst'] / rays:.1f} | {lanes:.2f} | {a['ms']:.2f} |")
+        rows.append(f"| {kern} | {skip}..{skip + n - 1} | {rays} | {a['dram'] / rays:.2f} | {a['l2'] / rays:.1f} "
+                    f"| {a['inst'] / rays:.1f} | {lanes:.2f} | {a['ms']:.3f} |")
     return "\n".join(rows)
 
 
@@ -154,7 +157,16 @@ def render(argv):
     ap.add_argument("--fetch-min-idle-shadow", type=int, default=0)
     ap.add_argument("--reg-lean", type=int, default=0)
     ap.add_argument("--shadow-tests", type=int, default=0)
+    ap.add_argument("--closest-tests", type=int, default=0)
+    ap.add_argument("--sample-major", type=int, default=0)
+    ap.add_argument("--config-json", default=None,
+                    help="a JSON file with a wavefront configuration (bench.py's config.wavefront); its keys set "
+                         "the options above")
     a = ap.parse_args(argv)
+    if a.config_json:
+        for k, v in json.load(open(a.config_json)).items():
+            if hasattr(a, k) and v is not None:
+                setattr(a, k, int(v))
     sd = scenes.heterogeneous(width=1024, height=1024, spp=a.spp, depth=16)
     cams = scenes.heterogeneous_cameras(a.views)
     gs = hk.Scene.from_desc(sd)
@@ -165,14 +177,21 @@ def render(argv):
                     threads_extend=a.threads_extend, threads_shade=a.threads_shade, fetch_steps=a.fetch_steps,
                     fetch_min_idle=a.fetch_min_idle, iterations_per_check=a.iterations_per_check,
                     fetch_steps_shadow=a.fetch_steps_shadow, fetch_min_idle_shadow=a.fetch_min_idle_shadow,
-                    reg_lean=a.reg_lean, shadow_tests=a.shadow_tests)
+                    reg_lean=a.reg_lean, shadow_tests=a.shadow_tests, closest_tests=a.closest_tests,
+                    sample_major=a.sample_major)
     torch.cuda.synchronize()
     c = [int(x) for x in ctr.cpu().tolist()]
     names = ["rays", "shadow_rays", "dropped", "node_visits", "tri_tests", "node_visits_shadow", "tri_tests_shadow"]
     out = {"workload": f"heterogeneous {a.views} x 1024^2 x {a.spp} spp", "accel": a.accel,
            "launch": {"capacity": a.capacity, "threads_extend": a.threads_extend, "threads_shade": a.threads_shade,
-                      "fetch_steps": a.fetch_steps, "fetch_min_idle": a.fetch_min_idle},
-           "counters": dict(zip(names, c))}
+                      "fetch_steps": a.fetch_steps, "fetch_min_idle": a.fetch_min_idle,
+                      "fetch_steps_shadow": a.fetch_steps_shadow, "fetch_min_idle_shadow": a.fetch_min_idle_shadow,
+                      "reg_lean": a.reg_lean, "shadow_tests": a.shadow_tests, "closest_tests": a.closest_tests,
+                      "sample_major": a.sample_major},
+           "counters": dict(zip(names, c)),
+           # rays of each traversal launch, in launch order (ncu -k <kernel> -s i -c k captures launches i..i+k-1)
+           "launch_rays": {"extend": [int(x) for x in gs.wavefront_launch_log(0)],
+                           "shadow": [int(x) for x in gs.wavefront_launch_log(1)]}}
     text = json.dumps(out)
     if a.out:
         open(a.out, "w").write(text + "\n")
@@ -185,6 +204,6 @@ if __name__ == "__main__":
     elif sys.argv[1] == "render":
         render(sys.argv[2:])
     elif sys.argv[1] == "traffic":
-        print(traffic(sys.argv[2], sys.argv[3]))
+        print(traffic(sys.argv[2], sys.argv[3], int(sys.argv[4]) if len(sys.argv) > 4 else 0))
     else:
         print(raw(sys.argv[2], sys.argv[3] if len(sys.argv) > 3 else None))

@@ -195,6 +195,12 @@ enum { HK_BUILDER_HOST = 0, HK_BUILDER_GPU = 1 };
 int hk_scene_set_builder(hk_scene *s, int32_t builder);
 /* Seconds the last hk_scene_build spent building (and uploading) its trees. */
 int hk_scene_tree_build_seconds(const hk_scene *s, double *seconds);
+/* Profiling aid, no counterpart in the reference: the rays each launch of the
+ * closest-hit (which 0) or shadow (which 1) traversal kernel traced in the
+ * scene's last hk_render_batch, in launch order.  Up to max counts go to
+ * rays_host (the first 1024 launches are kept); *launches gets the number of
+ * launches.  Waits for the scene's wavefront work to finish. */
+int hk_wavefront_launch_log(hk_scene *s, int32_t which, uint32_t *rays_host, int32_t max, int32_t *launches);
 /* Build the device 8-wide tree over n triangles (9 floats each, host) and run
  * hk_bvh_check's structural check of the 8-wide tree on it (HK_ERR_INVALID
  * with the first problem found). */
@@ -287,6 +293,13 @@ typedef struct {
                                       its own; 1 the same, postponed like closest-hit rays' while few
                                       lanes of the warp have triangles; 2 shared out over the warp, 32
                                       at a time */
+    int32_t closest_tests;         /* triangle tests of the closest-hit rays (8-wide tree): 0 each lane
+                                      tests its own, postponed while few lanes of the warp have
+                                      triangles; 2 shared out over the warp, 32 at a time, the least t
+                                      of each ray kept (the later test on equal t, as the serial loop) */
+    int32_t sample_major;          /* 0: each image's work is dealt tile by tile (all samples of a 16 x 16
+                                      tile, then the next); 1: sample by sample over the whole image.
+                                      Images agree up to the order of the film's float additions */
 } hk_wavefront_config;
 
 /* Render every job of the batch with the wavefront integrator: a pool of path
@@ -402,7 +415,11 @@ typedef struct {
 int hk_server_create(const hk_server_config *cfg, hk_server **out);
 /* Cancels queued jobs, finishes the running ones and frees everything. */
 int hk_server_destroy(hk_server *srv);
-/* Register a built scene (not owned; keep it alive and unchanged while the server lives). */
+/* Register a built scene (not owned; keep it alive and unchanged while the server lives).
+ * The scene's pool is sized by the server's configuration; its traversal
+ * settings (ray-fetch intervals, register budgets, triangle-test modes) come
+ * from the scene's wavefront configuration (hk_wavefront_autotune or
+ * hk_scene_set_wavefront_config) when the scene has one at its first job. */
 int hk_server_add_scene(hk_server *srv, hk_scene *scene, int32_t *scene_id);
 /* Queue a job.  rgb_host receives height*width*3 floats (pinned memory is
  * copied into directly, other memory through a pinned staging buffer); it

@@ -178,3 +178,48 @@ def test_shadow_test_modes_agree(lean):
         print(f"mode {mode}: counters {ctrs[mode]} vs {ctrs[0]}, max abs diff {np.abs(imgs[mode] - imgs[0]).max():.3e}")
         assert ctrs[mode][0] == ctrs[0][0] and ctrs[mode][1] == ctrs[0][1]
         assert np.allclose(imgs[mode], imgs[0], rtol=1e-5, atol=1e-6 * scale)
+
+
+@pytest.mark.parametrize("lean", [0, 1])
+def test_closest_test_modes_agree(lean):
+    """The closest-hit rays' triangle tests each lane its own or shared out
+    over the warp (hk_wavefront_config.closest_tests 0 / 2) keep the same hit:
+    the least t of the triangles a ray reaches, the later test on equal t.
+    Paths then follow the same vertices, so the ray counts agree exactly and
+    the images up to the order of the film's float additions."""
+    sd = scenes.heterogeneous(width=128, height=128, spp=8, depth=8, n_spheres=12, levels=(3, 4),
+                              level_p=(0.5, 0.5), env_res=(256, 128))
+    gs = hk.Scene.from_desc(sd)
+    gs.set_accel(hk.ACCEL_BVH8)
+    imgs, ctrs = [], []
+    for mode in (0, 2):
+        f = torch.zeros(gs.film_shape(), dtype=torch.float32, device="cuda")
+        ctr = torch.zeros(7, dtype=torch.int64, device="cuda")
+        gs.render_batch([f], spp=8, depth=8, seeds=[3], counters=ctr, capacity=1 << 16, threads_extend=64,
+                        closest_tests=mode, reg_lean=lean)
+        imgs.append(f.cpu().numpy().astype(np.float64))
+        ctrs.append(ctr.cpu().numpy())
+    scale = float(np.abs(imgs[0]).max())
+    print(f"counters {ctrs[1]} vs {ctrs[0]}, max abs diff {np.abs(imgs[1] - imgs[0]).max():.3e}")
+    assert ctrs[1][0] == ctrs[0][0] and ctrs[1][1] == ctrs[0][1]
+    assert np.allclose(imgs[1], imgs[0], rtol=1e-5, atol=1e-6 * scale)
+
+
+def test_sample_major_dispatch_renders_the_same_image():
+    """Dealing a job's work sample by sample over the whole image instead of
+    tile by tile (hk_wavefront_config.sample_major) changes which paths are in
+    flight together, not the paths: each sample's stream depends on (seed,
+    sample, pixel, image) only, so ray counts agree exactly and images up to
+    the order of the film's float additions."""
+    sd = scenes.cornell_box(width=80, height=56)   # 5 x 4 tiles, the last row partial
+    gs = hk.Scene.from_desc(sd)
+    imgs, ctrs = [], []
+    for order in (0, 1):
+        f = torch.zeros(gs.film_shape(), dtype=torch.float32, device=DEV)
+        ctr = torch.zeros(7, dtype=torch.int64, device=DEV)
+        gs.render_batch([f], spp=32, depth=sd.depth, seeds=[9], counters=ctr, capacity=1 << 14, sample_major=order)
+        imgs.append(_resolve(gs, f).astype(np.float64))
+        ctrs.append(ctr.cpu().numpy())
+    print("counters", ctrs, "max abs diff", np.abs(imgs[1] - imgs[0]).max())
+    assert ctrs[1][0] == ctrs[0][0] and ctrs[1][1] == ctrs[0][1] and ctrs[1][2] == ctrs[0][2]
+    assert np.allclose(imgs[1], imgs[0], rtol=1e-5, atol=1e-6 * float(np.abs(imgs[0]).max()))
