@@ -9,13 +9,12 @@ namespace hk {
 
 namespace {
 constexpr int kQueueArrays = 2 /*eq*/ + 2 /*idle*/ + kWfTypes /*sq*/ + 1 /*fq*/;
-constexpr int kStateArrays = 9;   // float4-sized arrays per slot
 }  // namespace
 
 size_t WfEngine::bytes_for(int capacity, int nemitters) {
     const size_t N = (size_t)capacity;
     const size_t shadow = N * (size_t)std::max(1, nemitters);
-    return N * 16 * kStateArrays + N * sizeof(float) + N * sizeof(int) * kQueueArrays + shadow * 16 * 3 + sizeof(WfCounters) +
+    return N * kSlotBytes + N * sizeof(int) * kQueueArrays + shadow * 16 * 3 + sizeof(WfCounters) +
            (sizeof(WfJob) + sizeof(unsigned long long)) * kWfMaxJobs + sizeof(WfSeg) * kWfMaxSegs;
 }
 
@@ -28,7 +27,7 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     const size_t N = (size_t)cfg_.capacity;
     W_.capacity = cfg_.capacity;
     W_.max_shadow = cfg_.capacity * std::max(1, S.nemitters);
-    state_.alloc(N * 16 * kStateArrays + N * sizeof(float));
+    state_.alloc(N * kSlotBytes);
     queues_.alloc(N * sizeof(int) * kQueueArrays);
     shadow_.alloc((size_t)W_.max_shadow * 16 * 3);
     counters_.alloc(sizeof(WfCounters));
@@ -36,10 +35,17 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     finished_.alloc(sizeof(unsigned long long) * kWfMaxJobs);
     segs_.alloc(sizeof(WfSeg) * kWfMaxSegs);
     bytes_ = bytes_for(cfg_.capacity, S.nemitters);
-    float4 *st = state_.as<float4>();
-    W_.ray_o = st; W_.ray_d = st + N; W_.beta = st + 2 * N; W_.lacc = st + 3 * N; W_.pix = st + 4 * N;
-    W_.rng = (uint4 *)(st + 5 * N); W_.prev_wi = st + 6 * N; W_.prev_wo = st + 7 * N; W_.hit = st + 8 * N;
-    W_.prev_pdf = (float *)(st + 9 * N);
+    char *rec = state_.as<char>();   // slot records (kSlotBytes each, 256-byte aligned base)
+    W_.ray_o.p = (float4 *)(rec + 0);
+    W_.ray_d.p = (float4 *)(rec + 16);
+    W_.beta.p = (float4 *)(rec + 32);
+    W_.pix.p = (float4 *)(rec + 48);
+    W_.rng.p = (uint4 *)(rec + 64);
+    W_.hit.p = (float4 *)(rec + 80);
+    W_.prev_wi.p = (float4 *)(rec + 96);
+    W_.prev_wo.p = (float4 *)(rec + 112);
+    W_.lacc.p = (float4 *)(rec + 128);
+    W_.prev_pdf.p = (float *)(rec + 144);
     int *q = queues_.as<int>();
     W_.eq[0] = q; W_.eq[1] = q + N;
     W_.idle[0] = q + 2 * N; W_.idle[1] = q + 3 * N;

@@ -91,20 +91,38 @@ struct WfCounters {
     unsigned int log_rays[2][kWfLaunchLog];
 };
 
+// Path state: one 160-byte record per slot, five 32-byte sectors, the fields
+// a kernel reads together in one sector: (ray o, ray d) extend and shade;
+// (throughput, pixel) shade and regen; (rng, hit) shade; (previous BSDF record
+// wi, wo) shade at emitter hits; (radiance, previous pdf) regen and the
+// next-event reductions.  Slots are visited in queue order, i.e. scattered, so
+// a separate array per field would fetch a whole sector for each 16-byte field.
+constexpr size_t kSlotBytes = 160;
+// One field of every slot's record: f[slot] is the field of that slot.
+template <class T>
+struct SlotField {
+    T *p;   // the field in slot 0's record
+    __host__ __device__ __forceinline__ T &operator[](size_t slot) const {
+        return *reinterpret_cast<T *>(reinterpret_cast<char *>(p) + slot * kSlotBytes);
+    }
+    __host__ __device__ __forceinline__ T *operator+(size_t slot) const { return &(*this)[slot]; }
+};
+
 struct WfState {
     int capacity;
     int max_shadow;                    // shadow queue capacity
-    // per-slot path state
-    float4 *ray_o;      // o.xyz, tmin
-    float4 *ray_d;      // d.xyz, tmax
-    float4 *beta;       // throughput.xyz, w_mats
-    float4 *lacc;       // radiance.xyz (next-event terms added atomically), -
-    float4 *pix;        // film x, film y, bits(job), bits(depth | flags << 16)
-    uint4 *rng;         // pcg32 state, increment
-    float4 *prev_wi;    // previous vertex: BSDF record wi.xyz, bits(bsdf id)
-    float4 *prev_wo;    // previous vertex: BSDF record wo.xyz, bits(measure)
-    float *prev_pdf;    // previous vertex: its BSDF's pdf of the sampled direction (textured materials only)
-    float4 *hit;        // t, u, v, bits(tri in leaf order or -1)
+    // per-slot path state (byte offset in the slot's record)
+    SlotField<float4> ray_o;      //   0: o.xyz, tmin
+    SlotField<float4> ray_d;      //  16: d.xyz, tmax
+    SlotField<float4> beta;       //  32: throughput.xyz, w_mats
+    SlotField<float4> pix;        //  48: film x, film y, bits(job), bits(depth | flags << 16)
+    SlotField<uint4> rng;         //  64: pcg32 state, increment
+    SlotField<float4> hit;        //  80: t, u, v, bits(tri in leaf order or -1)
+    SlotField<float4> prev_wi;    //  96: previous vertex: BSDF record wi.xyz, bits(bsdf id)
+    SlotField<float4> prev_wo;    // 112: previous vertex: BSDF record wo.xyz, bits(measure)
+    SlotField<float4> lacc;       // 128: radiance.xyz (next-event terms added atomically), -
+    SlotField<float> prev_pdf;    // 144: previous vertex: its BSDF's pdf of the sampled direction (textured
+                                  //      materials only)
     // queues
     int *eq[2];
     int *idle[2];
