@@ -498,7 +498,8 @@ def run_bsdf(args):
     P = hk._p
 
     def batch(bid):
-        hk.check(L.hk_bsdf_batch(gs.h, bid, n, P(wi), P(u2), P(u1), P(wo), None, P(out["s_wo"]), P(out["s_w"]),
+        # uv, duv: no texture coordinates (the config-2 materials are untextured)
+        hk.check(L.hk_bsdf_batch(gs.h, bid, n, P(wi), P(u2), P(u1), P(wo), None, None, P(out["s_wo"]), P(out["s_w"]),
                                  P(out["s_pdf"]), P(out["s_m"]), P(out["e_rgb"]), P(out["p_pdf"]), stream.cuda_stream))
 
     for _ in range(args.warmup):
@@ -618,7 +619,7 @@ def main():
     cam_list = [c for c in cams] if cams[0] is not None else None
     tuned, tune_ms = {}, None
     if wave:
-        tuned, tune_ms = gs.autotune(min(16, spp), depth, camera=cams[0])   # untimed set-up
+        tuned, tune_ms = gs.autotune(min(32, spp), depth, camera=cams[0])   # untimed set-up
         for kv in args.set:
             k, v = kv.split("=", 1)
             if k not in tuned:

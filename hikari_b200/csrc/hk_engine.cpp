@@ -78,10 +78,11 @@ WfEngine::WfEngine(const DevScene &S, int sm_count, const WfEngineConfig &cfg) :
     L_.threads_regen = 256;
     L_.lean_extend = cfg_.reg_lean & 1;
     L_.lean_shadow = (cfg_.reg_lean >> 1) & 1;
+    L_.lean_shade = (cfg_.reg_lean >> 2) & 1;
     L_.shadow_tests = cfg_.shadow_tests >= 0 && cfg_.shadow_tests <= 2 ? cfg_.shadow_tests : 0;
     L_.closest_tests = cfg_.closest_tests == 2 ? 2 : 0;
     auto grid = [&](int which, int threads) {
-        const bool lean = which == 0 ? L_.lean_extend : (which == 2 ? L_.lean_shadow : false);
+        const bool lean = which == 0 ? L_.lean_extend : (which == 2 ? L_.lean_shadow : (which == 1 ? L_.lean_shade : false));
         const bool shared = (which == 2 && L_.shadow_tests == 2) || (which == 0 && L_.closest_tests == 2);
         return std::max(1, sm_count * std::max(1, wf_occupancy(which, threads, S.accel, lean, shared)));
     };

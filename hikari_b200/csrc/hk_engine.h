@@ -23,7 +23,7 @@ struct WfEngineConfig {
     int fetch_min_idle = 1;   // idle lanes before a warp refills while others traverse
     int fetch_steps_shadow = 0;      // the same for the shadow rays (0: the closest-hit value)
     int fetch_min_idle_shadow = 0;
-    int reg_lean = 0;   // bit 0: extend, bit 1: shadow kernel with the smaller register budget
+    int reg_lean = 0;   // bit 0: extend, bit 1: shadow, bit 2: untextured shade kernels with the smaller register budget
     int shadow_tests = 0;   // shadow rays' triangle tests: 0 per lane, 1 postponed, 2 shared over the warp
     int closest_tests = 0;  // closest-hit rays' triangle tests: 0 per lane, 2 shared over the warp
 };

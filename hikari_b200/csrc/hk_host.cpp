@@ -1450,7 +1450,7 @@ int hk_render_batch(hk_scene *s, const hk_render_job *jobs, int njobs, const hk_
         ec.fetch_min_idle = c.fetch_min_idle > 0 ? std::min(32, c.fetch_min_idle) : 1;
         ec.fetch_steps_shadow = std::max(0, std::min(1024, c.fetch_steps_shadow));
         ec.fetch_min_idle_shadow = c.fetch_min_idle_shadow > 0 ? std::min(32, c.fetch_min_idle_shadow) : 0;
-        ec.reg_lean = c.reg_lean & 3;
+        ec.reg_lean = c.reg_lean & 7;
         ec.shadow_tests = c.shadow_tests >= 0 && c.shadow_tests <= 2 ? c.shadow_tests : 0;
         ec.closest_tests = c.closest_tests == 2 ? 2 : 0;
         hk::WfEngine &E = wf_ensure(s, ec);
@@ -1608,10 +1608,16 @@ int hk_wavefront_autotune(hk_scene *s, const hk_render_desc *probe, hk_wavefront
             float ms = run(c);
             if (ms < best_t) { best_t = ms; bc = c; }
         }
-        // register budgets of the extend and shadow kernels
+        // register budgets of the extend and shadow kernels, then of the shade kernels
         c = bc;
         for (int k : {1, 2, 3}) {
             c.reg_lean = k;
+            float ms = run(c);
+            if (ms < best_t) { best_t = ms; bc = c; }
+        }
+        c = bc;
+        c.reg_lean |= 4;
+        {
             float ms = run(c);
             if (ms < best_t) { best_t = ms; bc = c; }
         }

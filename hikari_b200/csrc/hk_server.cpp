@@ -239,7 +239,7 @@ void hk_server::admit(const std::vector<SceneEntry *> &sc) {
                 sec.fetch_min_idle = t.fetch_min_idle > 0 ? std::min(32, t.fetch_min_idle) : 1;
                 sec.fetch_steps_shadow = std::max(0, std::min(1024, t.fetch_steps_shadow));
                 sec.fetch_min_idle_shadow = t.fetch_min_idle_shadow > 0 ? std::min(32, t.fetch_min_idle_shadow) : 0;
-                sec.reg_lean = t.reg_lean & 3;
+                sec.reg_lean = t.reg_lean & 7;
                 sec.shadow_tests = t.shadow_tests >= 0 && t.shadow_tests <= 2 ? t.shadow_tests : 0;
                 sec.closest_tests = t.closest_tests == 2 ? 2 : 0;
             }

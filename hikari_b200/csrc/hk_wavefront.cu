@@ -39,7 +39,7 @@ extern template int wf_trace_occupancy_t<kAccelBvh2>(int, int, bool, bool);
 #define HK_WF_SHADE_EXTERN(K)                                                                                           \
     extern template cudaError_t wf_launch_shade_t<K>(const DevScene &, const WfState &, const WfLaunchConfig &, int, \
                                                      cudaStream_t);                                                 \
-    extern template int wf_shade_occupancy_t<K>(int)
+    extern template int wf_shade_occupancy_t<K>(int, bool)
 HK_WF_SHADE_EXTERN(0);
 HK_WF_SHADE_EXTERN(1);
 HK_WF_SHADE_EXTERN(2);
@@ -287,7 +287,7 @@ int wf_occupancy(int which, int threads, int accel, bool lean, bool shared) {
     case 2:
         return w8 ? wf_trace_occupancy_t<kAccelBvh8>(which, threads, lean, shared)
                   : wf_trace_occupancy_t<kAccelBvh2>(which, threads, lean, shared);
-    case 1: return wf_shade_occupancy_t<5>(threads);
+    case 1: return wf_shade_occupancy_t<5>(threads, lean);
     default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_regen_kernel, threads, 0); break;
     }
     return n;

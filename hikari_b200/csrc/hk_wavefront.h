@@ -147,6 +147,7 @@ struct WfLaunchConfig {
     int fetch_steps, fetch_min_idle;                 // dynamic ray fetch of the extend kernel
     int fetch_steps_shadow, fetch_min_idle_shadow;   // and of the shadow kernel
     int lean_extend, lean_shadow;                    // traversal kernels with the smaller register budget
+    int lean_shade;                                  // untextured shade kernels with the smaller register budget
     int shadow_tests;   // shadow rays' triangle tests: 0 per lane, 1 postponed, 2 shared over the warp
     int closest_tests;  // closest-hit rays' triangle tests: 0 per lane (postponed where the tree allows), 2 shared
 };

@@ -172,8 +172,13 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_extend_kernel(DevScene S, 
 // ------------------------------------------------------------ shade
 __device__ __forceinline__ void finish(const WfState &W, int slot) { W.fq[warp_append(&W.ctr->fq_count)] = slot; }
 
-template <int kType>
-__global__ void __launch_bounds__(256) wf_shade_kernel(DevScene S, WfState W, int nxt) {
+// kMinBlocks = 0 leaves the register budget to the compiler; kLeanShade asks
+// for four resident blocks of 256 threads (at most 64 registers): more warps
+// to hide the latency of the path-state and scene gathers, at the price of
+// some spilling.  Only the untextured queues (0-5) come in both budgets.
+constexpr int kLeanShade = 4;
+template <int kType, int kMinBlocks = 0>
+__global__ void __launch_bounds__(256, kMinBlocks) wf_shade_kernel(DevScene S, WfState W, int nxt) {
     const int n = (int)W.ctr->sq_count[kType];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int slot = W.sq[kType][i];
@@ -494,12 +499,24 @@ int wf_trace_occupancy_t(int which, int threads, bool lean, bool shared) {
 }
 template <int kType>
 cudaError_t wf_launch_shade_t(const DevScene &S, const WfState &W, const WfLaunchConfig &C, int nxt, cudaStream_t st) {
+    if constexpr (kType <= 5) {
+        if (C.lean_shade) {
+            wf_shade_kernel<kType, kLeanShade><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
+            return cudaGetLastError();
+        }
+    }
     wf_shade_kernel<kType><<<C.blocks_shade, C.threads_shade, 0, st>>>(S, W, nxt);
     return cudaGetLastError();
 }
 template <int kType>
-int wf_shade_occupancy_t(int threads) {
+int wf_shade_occupancy_t(int threads, bool lean) {
     int n = 0;
+    if constexpr (kType <= 5) {
+        if (lean) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade_kernel<kType, kLeanShade>, threads, 0);
+            return n;
+        }
+    }
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wf_shade_kernel<kType>, threads, 0);
     return n;
 }

@@ -3,5 +3,5 @@
 
 namespace hk {
 template cudaError_t wf_launch_shade_t<5>(const DevScene &, const WfState &, const WfLaunchConfig &, int, cudaStream_t);
-template int wf_shade_occupancy_t<5>(int);
+template int wf_shade_occupancy_t<5>(int, bool);
 }  // namespace hk

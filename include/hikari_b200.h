@@ -288,7 +288,9 @@ typedef struct {
     int32_t fetch_steps_shadow;    /* the same two for the shadow (any-hit) rays; 0 = the closest-hit */
     int32_t fetch_min_idle_shadow; /*   rays' values */
     int32_t reg_lean;              /* bit 0 / bit 1: the extend / shadow kernel with a register budget of
-                                      48 (five resident blocks of 256 threads) instead of the compiler's */
+                                      48 (five resident blocks of 256 threads) instead of the compiler's;
+                                      bit 2: the shade kernels of untextured materials with 64 (four
+                                      resident blocks of 256 threads) */
     int32_t shadow_tests;          /* triangle tests of the shadow rays (8-wide tree): 0 each lane tests
                                       its own; 1 the same, postponed like closest-hit rays' while few
                                       lanes of the warp have triangles; 2 shared out over the warp, 32
