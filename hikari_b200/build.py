@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libhikari_b200.so")
 SOURCES = ["hk_render_b8.cu", "hk_render_b8t.cu", "hk_render_b2.cu", "hk_render_b2t.cu", "hk_wf_shade_3.cu",
-           "hk_wf_shade_2.cu", "hk_wf_shade_1.cu", "hk_wf_shade_0.cu", "hk_wf_shade_4.cu", "hk_wf_shade_5.cu", "hk_wf_trace_8.cu", "hk_wf_trace_2.cu",
+           "hk_wf_shade_2.cu", "hk_wf_shade_1.cu", "hk_wf_shade_0.cu", "hk_wf_shade_4.cu", "hk_wf_shade_5.cu", "hk_wf_shade_6.cu", "hk_wf_shade_7.cu", "hk_wf_trace_8.cu", "hk_wf_trace_2.cu",
            "hk_batch_0.cu", "hk_batch_1.cu", "hk_batch_2.cu", "hk_batch_3.cu", "hk_batch_4.cu",
            "hk_kernels.cu", "hk_wavefront.cu", "hk_lbvh.cu", "hk_host.cpp", "hk_engine.cpp", "hk_server.cpp", "hk_bvh.cpp", "hk_xml.cpp",
            "hk_obj.cpp", "hk_mipmap.cpp", "hk_image.cpp"]

@@ -21,6 +21,11 @@ struct BRec {
     float tu, tv;   // texture coordinates of the intersection (Record.Isect.UV)
     float4 duv;     // their screen-space partials (dUdX, dVdX, dUdY, dVdY): a camera ray's first hit, else 0
     bool tex;       // textures are looked up (false in kernels that shade untextured materials only)
+    // what the wireframe and curvature textures read at the intersection: the
+    // distance from P to the nearest edge line of the hit triangle, the mean
+    // and the Gaussian curvature (tex_geometry); without an intersection the
+    // wireframe reads its interior colour and the curvature black
+    float3 geo = make_float3(INFINITY, 0.0f, 0.0f);
 };
 
 // ------------------------------------------------------------ microfacet
@@ -284,8 +289,35 @@ __device__ __forceinline__ void mip_gradient(const DevTexture &t, int l, float u
     gv = ((p01 + p00 * (dx - 1.0f)) - tmp * dx) * H;
 }
 __device__ __forceinline__ V3 pattern_eval(const DevTexture &t, float u, float v);
+// SmoothStep (include/core/Common.hpp:994) with Clamp (:752)
+__device__ __forceinline__ float smooth_step(float lo, float hi, float x) {
+    float v = (x - lo) / (hi - lo);
+    v = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+    return v * v * (-2.0f * v + 3.0f);
+}
+// WireframeTexture::Eval (src/texture/WireframeTexture.cpp:22) and
+// CurvatureTexture::Eval (src/texture/CurvatureTexture.cpp:34) from the hit's
+// edge distance and curvatures (geo, see BRec)
+__device__ __forceinline__ V3 geo_tex_eval(const DevTexture &t, float3 geo) {
+    if (t.kind == kTexWireframe) {
+        const float w = t.width;
+        const float al = smooth_step(w * (1.0f - t.scale), w, geo.x);
+        return ld_rgb(t.b) * (1.0f - al) + ld_rgb(t.a) * al;
+    }
+    const float val = t.count ? geo.z : geo.y;
+    if (val < 0.0f) {
+        const float x = -val * t.scale;
+        return ld_rgb(t.b) * (1.0f < x ? 1.0f : x);   // std::min(x, 1)
+    }
+    if (val > 0.0f) {
+        const float x = val * t.scale;
+        return ld_rgb(t.a) * (1.0f < x ? 1.0f : x);
+    }
+    return v3(0, 0, 0);
+}
 // filter: Texture::Eval(Isect, bFilter) -- unfiltered bitmaps read the nearest texel (BitmapTexture::Eval(UV) :134)
-__device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, float tv, float4 duv, bool filter = true) {
+__device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, float tv, float4 duv, bool filter = true,
+                                       float3 geo = make_float3(INFINITY, 0.0f, 0.0f)) {
     float sc[4];
     int ns = 0;
     while (T[id].kind == kTexScale && ns < 4) {
@@ -298,6 +330,8 @@ __device__ __forceinline__ V3 tex_eval(const DevTexture *T, int id, float tu, fl
     if (t.kind == kTexBitmap) {
         c = filter ? bitmap_eval(t, u, v, duv)
                    : mip_texel(t, 0, (int)floorf(u * (float)(1 << t.lw)), (int)floorf(v * (float)(1 << t.lh)));
+    } else if (t.kind == kTexWireframe || t.kind == kTexCurvature) {
+        c = geo_tex_eval(t, geo);
     } else {
         c = pattern_eval(t, u, v);
     }
@@ -354,14 +388,14 @@ __device__ __forceinline__ V3 pattern_eval(const DevTexture &t, float u, float v
 __device__ __forceinline__ V3 par_rgb(const DevBsdf &b, int slot, const float *c, const BRec &r) {
     if (r.tex) {
         const int t = b.tex[slot];
-        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv, r.duv);
+        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv, r.duv, true, r.geo);
     }
     return ld_rgb(c);
 }
 __device__ __forceinline__ float par_alpha(const DevBsdf &b, int slot, float c, const BRec &r) {
     if (r.tex) {
         const int t = b.tex[slot];
-        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv, r.duv).x;
+        if (t) return tex_eval(b.textures, t - 1, r.tu, r.tv, r.duv, true, r.geo).x;
     }
     return c;
 }
@@ -1161,5 +1195,37 @@ __device__ __forceinline__ V3 bsdf_sample_t(const DevBsdf *bs, int id, BRec &r, 
     else if constexpr (BT == kCoating) return scoating_sample(b, bs[b.nested], r, ux, uy, u1);
     else if constexpr (BT == kRoughDiffuse) return roughdiffuse_sample(b, r, ux, uy);
     else return twosided_sample(bs, b, r, ux, uy, u1);
+}
+
+// bumpMap / normalMap id wrapping a BSDF of type BT known at compile time:
+// the wrappers above with the nested call dispatched statically
+template <int BT>
+__device__ __forceinline__ V3 bump_eval_t(const DevBsdf *bs, int id, const BRec &r, const BumpFrames &f) {
+    BRec q;
+    if (!bump_record(f, r, q)) return v3(0, 0, 0);
+    return bsdf_eval_t<BT>(bs, bs[id].nested, q);
+}
+template <int BT>
+__device__ __forceinline__ float bump_pdf_t(const DevBsdf *bs, int id, const BRec &r, const BumpFrames &f) {
+    BRec q;
+    if (!bump_record(f, r, q)) return 0.0f;
+    return bsdf_pdf_t<BT>(bs, bs[id].nested, q);
+}
+template <int BT>
+__device__ __forceinline__ V3 bump_sample_t(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1,
+                                            const BumpFrames &f) {
+    BRec q = r;
+    q.wi = to_local(f.pf, to_world(f.sh, r.wi));
+    q.wo = v3(0, 0, 0);
+    q.measure = kMeasureUnknown;
+    if (r.wi.z * q.wi.z <= 0.0f) return v3(0, 0, 0);
+    const V3 res = bsdf_sample_t<BT>(bs, bs[id].nested, q, ux, uy, u1);
+    if (!is_zero(res)) {
+        r.wo = to_local(f.sh, to_world(f.pf, q.wo));
+        r.eta = q.eta;
+        r.measure = q.measure;
+        if (r.wo.z * q.wo.z <= 0.0f) return v3(0, 0, 0);
+    }
+    return res;
 }
 }  // namespace hk

@@ -43,15 +43,21 @@ struct alignas(16) DevBsdf {
     int32_t tex[6];
     const DevTexture *textures;
     int32_t textured;
-    int32_t pad2, pad3, pad4;
+    int32_t geo_tex;                 // a wireframe or curvature texture in a slot here or in a nested BSDF
+    int32_t pad3, pad4;
     float rft[kRftThetaMax];
 };
 
-// Procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp) or
-// bitmap (src/texture/BitmapTexture.cpp over include/core/MipMap.hpp).
 // cutpoints per CDF in the environment map's guide tables (a power of two)
 constexpr int kEnvGuide = 1024;
-enum TexKind : int32_t { kTexCheckerboard = 1, kTexGrid = 2, kTexScale = 3, kTexBitmap = 4 };
+// Procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp),
+// bitmap (src/texture/BitmapTexture.cpp over include/core/MipMap.hpp) or a
+// texture of the hit's geometry (src/texture/{Wireframe,Curvature}Texture.cpp:
+// a interior / positive colour, b edge / negative colour, width the edge
+// width, scale the transition width / curvature scale, count 1 for Gaussian
+// curvature, 0 for mean curvature).
+enum TexKind : int32_t { kTexCheckerboard = 1, kTexGrid = 2, kTexScale = 3, kTexBitmap = 4, kTexWireframe = 5,
+                         kTexCurvature = 6 };
 enum TexFilter : int32_t { kFilterNearest = 0, kFilterBilinear = 1, kFilterTrilinear = 2, kFilterEwa = 3 };
 constexpr int kMipMaxLevels = 16;   // level 0 up to 32768 texels a side
 constexpr int kEwaLutSize = 128;

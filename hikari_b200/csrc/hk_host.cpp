@@ -333,6 +333,9 @@ F3 tex_average(const hk_scene *s, int id) {
     }
     if (t.kind == HK_TEX_CHECKERBOARD)
         return {(t.a[0] + t.b[0]) * 0.5f, (t.a[1] + t.b[1]) * 0.5f, (t.a[2] + t.b[2]) * 0.5f};
+    if (t.kind == HK_TEX_WIREFRAME)   // (edge + interior) / 2 (src/texture/WireframeTexture.cpp:80)
+        return {(t.b[0] + t.a[0]) * 0.5f, (t.b[1] + t.a[1]) * 0.5f, (t.b[2] + t.a[2]) * 0.5f};
+    if (t.kind == HK_TEX_CURVATURE) return {0.5f, 0.5f, 0.5f};   // src/texture/CurvatureTexture.cpp:61
     float iw = std::max(0.0f, 1.0f - 2.0f * t.width);
     float ia = iw * iw, la = 1.0f - ia;
     return {t.a[0] * la + t.b[0] * ia, t.a[1] * la + t.b[1] * ia, t.a[2] * la + t.b[2] * ia};
@@ -345,6 +348,29 @@ void par_average(const hk_scene *s, const hk_bsdf_desc &d, int slot, const float
     }
     F3 a = tex_average(s, d.tex[slot] - 1);
     out[0] = a.x; out[1] = a.y; out[2] = a.z;
+}
+// Whether texture id is (or scales) a wireframe or curvature texture
+bool tex_geo(const hk_scene *s, int id) {
+    while (s->textures[id].kind == HK_TEX_SCALE) id = s->textures[id].nested;
+    return s->textures[id].kind == HK_TEX_WIREFRAME || s->textures[id].kind == HK_TEX_CURVATURE;
+}
+// The wireframe / curvature textures BSDF id reaches (its slots, nested BSDFs and
+// maps), each once, through scale textures
+void bsdf_geo_textures(const hk_scene *s, int id, int depth, std::vector<int> &out) {
+    if (id < 0 || id >= (int)s->bsdfs.size() || depth > 8) return;
+    const hk_bsdf_desc &d = s->bsdfs[id];
+    for (int k = 0; k < 6; k++) {
+        if (!d.tex[k]) continue;
+        int t = d.tex[k] - 1;
+        while (s->textures[t].kind == HK_TEX_SCALE) t = s->textures[t].nested;
+        if ((s->textures[t].kind == HK_TEX_WIREFRAME || s->textures[t].kind == HK_TEX_CURVATURE) &&
+            std::find(out.begin(), out.end(), t) == out.end())
+            out.push_back(t);
+    }
+    const bool nests = d.type == hk::kRoughCoating || d.type == hk::kCoating || d.type == hk::kTwoSided ||
+                       d.type == hk::kBumpMap || d.type == hk::kNormalMap;
+    if (nests) bsdf_geo_textures(s, d.nested, depth + 1, out);
+    if (d.type == hk::kTwoSided) bsdf_geo_textures(s, d.nested2, depth + 1, out);
 }
 bool bsdf_textured(const hk_scene *s, int id, int depth) {
     if (id < 0 || id >= (int)s->bsdfs.size() || depth > 8) return false;
@@ -459,6 +485,8 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
     if (d.type == hk::kBumpMap || d.type == hk::kNormalMap) {   // BumpMapBSDF / NormalMapBSDF::Activate
         if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "bumpMap / normalMap needs a nested BSDF"};
         if (d.tex[0] <= 0) throw HkError{HK_ERR_INVALID, "bumpMap / normalMap needs a map texture"};
+        if (tex_geo(s, d.tex[0] - 1))
+            throw HkError{HK_ERR_INVALID, "a wireframe or curvature texture as a bump / normal map is not supported"};
         const int nt = s->bsdfs[d.nested].type;
         if (nt == hk::kBumpMap || nt == hk::kNormalMap)
             throw HkError{HK_ERR_INVALID, "bumpMap / normalMap over another bumpMap / normalMap is not supported"};
@@ -510,11 +538,36 @@ void build_scene(hk_scene *s) {
     }
     if (pool.size() > hk::kEwaLutSize) { s->b_texels.upload(pool); track(s->b_texels); }
     const float *texels = s->b_texels.as<float>();
+    // a wireframe texture's automatic edge width: a tenth of the mean edge
+    // length of the first mesh (scene order) whose BSDF uses it (the reference
+    // takes the first mesh that evaluates it, src/texture/WireframeTexture.cpp:37-53)
+    std::vector<float> tex_width(s->textures.size());
+    for (size_t i = 0; i < s->textures.size(); ++i) tex_width[i] = s->textures[i].width;
+    std::vector<char> width_set(s->textures.size(), 0);
+    for (const MeshIn &m : s->meshes) {
+        std::vector<int> used;
+        bsdf_geo_textures(s, m.bsdf, 0, used);
+        for (int t : used) {
+            if (s->textures[t].kind != HK_TEX_WIREFRAME || s->textures[t].width != 0.0f || width_set[t]) continue;
+            float ew = 0.0f;
+            const size_t nt = m.idx.size() / 3;
+            for (size_t f = 0; f < nt; ++f) {
+                const float *p0 = &m.pos[3 * (size_t)m.idx[3 * f]], *p1 = &m.pos[3 * (size_t)m.idx[3 * f + 1]],
+                            *p2 = &m.pos[3 * (size_t)m.idx[3 * f + 2]];
+                const float l0 = f3norm(F3{p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]});
+                const float l1 = f3norm(F3{p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]});
+                const float l2 = f3norm(F3{p0[0] - p2[0], p0[1] - p2[1], p0[2] - p2[2]});
+                ew += (l0 + l1) + l2;
+            }
+            tex_width[t] = 0.1f * ew / (float)(3u * (uint32_t)nt);
+            width_set[t] = 1;
+        }
+    }
     for (size_t i = 0; i < s->textures.size(); ++i) {
         const hk_texture_desc &t = s->textures[i];
         hk::DevTexture x;
         std::memset(&x, 0, sizeof x);
-        x.kind = t.kind; x.nested = t.nested; x.count = t.count; x.width = t.width; x.scale = t.scale;
+        x.kind = t.kind; x.nested = t.nested; x.count = t.count; x.width = tex_width[i]; x.scale = t.scale;
         for (int k = 0; k < 2; k++) { x.uv_scale[k] = t.uv_scale[k]; x.uv_offset[k] = t.uv_offset[k]; }
         for (int k = 0; k < 3; k++) { x.a[k] = t.a[k]; x.b[k] = t.b[k]; }
         if (const hk::MipPyramid *m = s->bitmaps[i].get()) {
@@ -538,6 +591,9 @@ void build_scene(hk_scene *s) {
     for (size_t i = 0; i < bs.size(); ++i) {
         bs[i].textures = s->b_textures.as<hk::DevTexture>();
         bs[i].textured = bsdf_textured(s, (int)i, 0) ? 1 : 0;
+        std::vector<int> geo;
+        bsdf_geo_textures(s, (int)i, 0, geo);
+        bs[i].geo_tex = geo.empty() ? 0 : 1;
         D.textured |= bs[i].textured;
     }
     s->b_bsdfs.upload(bs); track(s->b_bsdfs);
@@ -966,10 +1022,12 @@ int hk_scene_set_rft(hk_scene *s, int distribution, const void *bytes, uint64_t 
 int hk_scene_add_texture(hk_scene *s, const hk_texture_desc *d, int32_t *out_id) {
     return guarded([&] {
         if (!s || !d) throw HkError{HK_ERR_INVALID, "bad arguments"};
-        if (d->kind < HK_TEX_CHECKERBOARD || d->kind > HK_TEX_SCALE) throw HkError{HK_ERR_INVALID, "unknown texture kind"};
+        const bool geo = d->kind == HK_TEX_WIREFRAME || d->kind == HK_TEX_CURVATURE;
+        if ((d->kind < HK_TEX_CHECKERBOARD || d->kind > HK_TEX_SCALE) && !geo)
+            throw HkError{HK_ERR_INVALID, "unknown texture kind"};
         if (d->kind == HK_TEX_SCALE && (d->nested < 0 || d->nested >= (int)s->textures.size()))
             throw HkError{HK_ERR_INVALID, "scale texture needs a nested texture"};
-        if (d->kind != HK_TEX_SCALE && d->count <= 0)
+        if (d->kind != HK_TEX_SCALE && !geo && d->count <= 0)
             throw HkError{HK_ERR_INVALID, "texture block / line count must be positive"};
         s->textures.push_back(*d);
         s->bitmaps.push_back(nullptr);

@@ -65,8 +65,10 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
         }
         const DevMesh &m = S.meshes[it.mesh];
         const int bsdf = m.bsdf;
+        float3 geo = make_float3(INFINITY, 0.0f, 0.0f);
         if constexpr (kTex) {
             if (is_bump(S.bsdfs[bsdf])) bf = perturbed_frames(S, hc, it, S.bsdfs[bsdf]);
+            if (S.bsdfs[bsdf].geo_tex) geo = tex_geometry(S, hc, it);
         }
         if (m.emitter >= 0) {
             const DevAreaLight &AL = S.area_lights[__ldg(S.emitter_area + m.emitter)];
@@ -95,7 +97,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
                 br.wo = to_local(it.sh, er.wi);
                 br.measure = kMeasureSolidAngle;
                 br.eta = 0.0f;
-                br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv;
+                br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv; br.geo = geo;
                 float pb;
                 V3 f;
                 if constexpr (kTex) {
@@ -126,7 +128,7 @@ __device__ V3 li_pathmis(const DevScene &S, Pcg32 &rng, Ray ray, float px, float
         br.wo = v3(0, 0, 0);
         br.measure = kMeasureUnknown;
         br.eta = 0.0f;
-        br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv;
+        br.tu = it.u; br.tv = it.v; br.tex = kTex; br.duv = duv; br.geo = geo;
         float sx = rng.nextf(), sy = rng.nextf();
         float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
         V3 F;

@@ -108,6 +108,64 @@ __device__ __forceinline__ bool uv_tangents(const DevScene &S, const Hit &h, con
     return true;
 }
 
+// What the wireframe and curvature textures read at a hit (BRec::geo): the
+// distance from P to the nearest of the hit triangle's edge lines
+// (WireframeTexture::Eval, src/texture/WireframeTexture.cpp:60-72), and the
+// mean and Gaussian curvature from the first and second fundamental forms
+// (Shape::ComputeCurvature, src/core/Shape.cpp:30-51) with dN/du, dN/dv as
+// Triangle::PostIntersect forms them (src/core/Mesh.cpp:137-156); 0 without
+// UV partials.
+__device__ __forceinline__ float3 tex_geometry(const DevScene &S, const Hit &h, const Isect &it) {
+    const float4 *tp = S.tris + 3 * h.tri;
+    const float4 q0 = __ldg(tp), q1 = __ldg(tp + 1), q2 = __ldg(tp + 2);
+    const V3 ps[3] = {xyz(q0), xyz(q1), xyz(q2)};
+    float min_d2 = 3.402823466e38f;   // std::numeric_limits<float>::max()
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const V3 cur = ps[i], nxt = ps[(i + 1) % 3];
+        const V3 d1 = normalize(nxt - cur), d2 = it.p - cur;
+        const V3 e = (cur + d1 * dot(d1, d2)) - it.p;
+        const float d2e = dot(e, e);
+        min_d2 = d2e < min_d2 ? d2e : min_d2;   // std::min
+    }
+    float3 g = make_float3(sqrtf(min_d2), 0.0f, 0.0f);
+    const DevMesh &m = S.meshes[it.mesh];
+    if (!m.has_uv || !m.has_normals) return g;
+    const V3 p0 = ps[0], dp1 = ps[1] - p0, dp2 = ps[2] - p0;
+    if (norm(cross(dp1, dp2)) == 0.0f) return g;   // no UV partials
+    const uint32_t orig = (uint32_t)__float_as_int(q0.w);
+    const float2 t0 = __ldg(S.tri_uv + 3 * orig), t1 = __ldg(S.tri_uv + 3 * orig + 1), t2 = __ldg(S.tri_uv + 3 * orig + 2);
+    const float du1 = t1.x - t0.x, dv1 = t1.y - t0.y, du2 = t2.x - t0.x, dv2 = t2.y - t0.y;
+    const float det = du1 * dv2 - dv1 * du2;
+    V3 dpdu, dpdv, dndu = v3(0, 0, 0), dndv = v3(0, 0, 0);
+    if (det == 0.0f) {
+        dpdu = it.sh.s;
+        dpdv = it.sh.t;
+    } else {
+        const float inv = 1.0f / det;
+        dpdu = (dp1 * dv2 - dp2 * dv1) * inv;
+        dpdv = (dp1 * (-du2) + dp2 * du1) * inv;
+        const float4 *np = S.tri_normals + 3 * orig;
+        const V3 n0 = xyz(__ldg(np)), n1 = xyz(__ldg(np + 1)), n2 = xyz(__ldg(np + 2));
+        const float b0 = 1 - (h.u + h.v), b1 = h.u, b2 = h.v;
+        V3 ns = (n0 * b0 + n1 * b1) + n2 * b2;
+        const float inv_ln = 1.0f / norm(ns);
+        ns = ns * inv_ln;
+        V3 dnu = (n1 - n0) * inv_ln;
+        dnu = dnu - ns * dot(ns, dnu);
+        V3 dnv = (n2 - n0) * inv_ln;
+        dnv = dnv - ns * dot(ns, dnv);
+        dndu = (dnu * dv2 - dnv * dv1) * inv;
+        dndv = (dnu * (-du2) + dnv * du1) * inv;
+    }
+    const float E = dot(dpdu, dpdu), F = dot(dpdu, dpdv), G = dot(dpdv, dpdv);
+    const float L = -dot(dpdu, dndu), M = -dot(dpdv, dndu), N = -dot(dpdv, dndv);
+    const float inv_denom = 1.0f / (E * G - F * F);
+    g.z = (L * N - M * M) * inv_denom;
+    g.y = 0.5f * ((L * G - 2.0f * M * F) + N * E) * inv_denom;
+    return g;
+}
+
 // Intersection::ComputeScreenSpacePartial (src/core/Intersection.cpp:30) of
 // the first hit of a camera ray from o with differential directions rx, ry:
 // (dUdX, dVdX, dUdY, dVdY), zero where the hit has no UV partials.

@@ -52,8 +52,13 @@ HK_WF_SHADE_EXTERN(8);
 HK_WF_SHADE_EXTERN(9);
 HK_WF_SHADE_EXTERN(10);
 HK_WF_SHADE_EXTERN(11);
+HK_WF_SHADE_EXTERN(12);
+HK_WF_SHADE_EXTERN(13);
+HK_WF_SHADE_EXTERN(14);
+HK_WF_SHADE_EXTERN(15);
+HK_WF_SHADE_EXTERN(16);
 #undef HK_WF_SHADE_EXTERN
-static_assert(kWfTypes == 12, "launch_shade_all launches one kernel per shade queue");
+static_assert(kWfTypes == 17, "launch_shade_all launches one kernel per shade queue");
 
 // ------------------------------------------------------------ regen
 // Splat and retire the finished paths, then give every finished or idle slot
@@ -241,7 +246,12 @@ static cudaError_t launch_shade_all(const DevScene &S, const WfState &W, const W
     wf_launch_shade_t<8>(S, W, C, nxt, st);
     wf_launch_shade_t<9>(S, W, C, nxt, st);
     wf_launch_shade_t<10>(S, W, C, nxt, st);
-    return wf_launch_shade_t<11>(S, W, C, nxt, st);
+    wf_launch_shade_t<11>(S, W, C, nxt, st);
+    wf_launch_shade_t<12>(S, W, C, nxt, st);
+    wf_launch_shade_t<13>(S, W, C, nxt, st);
+    wf_launch_shade_t<14>(S, W, C, nxt, st);
+    wf_launch_shade_t<15>(S, W, C, nxt, st);
+    return wf_launch_shade_t<16>(S, W, C, nxt, st);
 }
 
 cudaError_t wf_launch_counters_add(const WfState &W, unsigned long long *out, cudaStream_t st) {

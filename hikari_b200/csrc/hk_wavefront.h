@@ -26,9 +26,18 @@ namespace hk {
 // type with texture lookups.
 constexpr int kWfGenericQueue = 6;
 constexpr int kWfTexturedQueue0 = 7;
-constexpr int kWfTypes = kWfTexturedQueue0 + kRoughCoating + 1;
-__host__ __device__ constexpr int wf_queue_of(int bsdf_type, bool textured = false) {
-    return bsdf_type <= kRoughCoating ? (textured ? kWfTexturedQueue0 + bsdf_type : bsdf_type + 1) : kWfGenericQueue;
+constexpr int kWfBumpQueue0 = kWfTexturedQueue0 + kRoughCoating + 1;   // bumpMap / normalMap over a rough type
+constexpr int kWfTypes = kWfBumpQueue0 + kRoughCoating + 1;
+// Shade queue of a hit's top-level BSDF: 0 the miss queue; 1-5 the rough types
+// without textures; 7-11 the same with textures; 12-16 bumpMap / normalMap
+// wrapping a rough type (nested_type); 6 everything else (smooth BSDFs,
+// twoSided, maps over them), dispatched at run time.
+__host__ __device__ constexpr int wf_queue_of(int bsdf_type, bool textured = false, int nested_type = -1) {
+    return bsdf_type <= kRoughCoating
+               ? (textured ? kWfTexturedQueue0 + bsdf_type : bsdf_type + 1)
+               : ((bsdf_type == kBumpMap || bsdf_type == kNormalMap) && nested_type >= 0 && nested_type <= kRoughCoating
+                      ? kWfBumpQueue0 + nested_type
+                      : kWfGenericQueue);
 }
 constexpr int kWfMaxJobs = 1024;   // job table entries of one engine
 constexpr int kWfMaxSegs = 4096;   // pieces of one dispatch plan

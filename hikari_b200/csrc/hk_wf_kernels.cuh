@@ -140,7 +140,8 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_extend_kernel(DevScene S, 
         if (w.found) {
             const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
             const DevBsdf &B = S.bsdfs[S.meshes[mesh].bsdf];
-            type = wf_queue_of(B.type, B.textured != 0);
+            const bool map = B.type == kBumpMap || B.type == kNormalMap;
+            type = wf_queue_of(B.type, B.textured != 0, map ? S.bsdfs[B.nested].type : -1);
         }
         W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
         W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;
@@ -206,8 +207,14 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_shade_kernel(DevScene S, W
         } else {
             // queue -> top-level BSDF type (run-time dispatch for the generic
             // queue) and whether texture lookups are compiled in
-            constexpr int BT = kType == kWfGenericQueue ? -1
-                                                        : (kType >= kWfTexturedQueue0 ? kType - kWfTexturedQueue0 : kType - 1);
+            // kBumpQ: a bumpMap / normalMap over the rough type BT (the
+            // records move through the perturbed frame, the nested BSDF is
+            // evaluated with its type compiled in)
+            constexpr bool kBumpQ = kType >= kWfBumpQueue0;
+            constexpr int BT = kType == kWfGenericQueue
+                                   ? -1
+                                   : (kBumpQ ? kType - kWfBumpQueue0
+                                             : (kType >= kWfTexturedQueue0 ? kType - kWfTexturedQueue0 : kType - 1));
             constexpr bool kTexQ = kType >= kWfGenericQueue;
             uint4 rs = W.rng[slot];
             Pcg32 rng;
@@ -255,13 +262,18 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_shade_kernel(DevScene S, W
             BumpFrames bf;   // a bumpMap / normalMap vertex's frames (the generic queue only)
             if constexpr (BT < 0) {
                 if (is_bump(S.bsdfs[bsdf])) bf = perturbed_frames(S, h, it, S.bsdfs[bsdf]);
+            } else if constexpr (kBumpQ) {
+                bf = perturbed_frames(S, h, it, S.bsdfs[bsdf]);
             }
+            // what wireframe / curvature textures read at this vertex
+            float3 geo = make_float3(INFINITY, 0.0f, 0.0f);
             if constexpr (kTexQ) {
                 if (depth == 0 && S.ray_diff) {
                     V3 rx, ry;
                     camera_diff(S, J.cam, J.width, J.height, J.cam_aspect, p4.x, p4.y, rx, ry);
                     duv = screen_partials(S, h, it, ro, rx, ry);
                 }
+                if (S.bsdfs[bsdf].geo_tex) geo = tex_geometry(S, h, it);
             }
             // next-event estimation over every emitter (PathMISIntegrator.cpp:83-109)
             const V3 wi_local = to_local(it.sh, rd * -1.0f);
@@ -282,13 +294,19 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_shade_kernel(DevScene S, W
                 br.tex = kTexQ;   // lookups only in the kernels of textured materials
                 br.tu = it.u;
                 br.tv = it.v;
-                if constexpr (kTexQ) br.duv = duv;   // unread where lookups are compiled out
+                if constexpr (kTexQ) {   // unread where lookups are compiled out
+                    br.duv = duv;
+                    br.geo = geo;
+                }
                 float pl = er.pdf;
                 float pb;
                 V3 f;
                 if constexpr (BT < 0) {
                     pb = bsdf_pdf_b(S.bsdfs, bsdf, br, bf);
                     f = bsdf_eval_b(S.bsdfs, bsdf, br, bf);
+                } else if constexpr (kBumpQ) {
+                    pb = bump_pdf_t<BT>(S.bsdfs, bsdf, br, bf);
+                    f = bump_eval_t<BT>(S.bsdfs, bsdf, br, bf);
                 } else {
                     pb = bsdf_pdf_t<BT>(S.bsdfs, bsdf, br);
                     f = bsdf_eval_t<BT>(S.bsdfs, bsdf, br);
@@ -314,11 +332,15 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_shade_kernel(DevScene S, W
             br.tex = kTexQ;
             br.tu = it.u;
             br.tv = it.v;
-            if constexpr (kTexQ) br.duv = duv;
+            if constexpr (kTexQ) {
+                br.duv = duv;
+                br.geo = geo;
+            }
             float sx = rng.nextf(), sy = rng.nextf();
             float u1 = needs_u1(S.bsdfs, bsdf) ? rng.nextf() : 0.0f;
             V3 F;
             if constexpr (BT < 0) F = bsdf_sample_b(S.bsdfs, bsdf, br, sx, sy, u1, bf);
+            else if constexpr (kBumpQ) F = bump_sample_t<BT>(S.bsdfs, bsdf, br, sx, sy, u1, bf);
             else F = bsdf_sample_t<BT>(S.bsdfs, bsdf, br, sx, sy, u1);
             beta = beta * F;
             bool alive = !is_zero(beta);
@@ -350,6 +372,7 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_shade_kernel(DevScene S, W
                     BRec pr = br;
                     pr.eta = 0.0f;
                     if constexpr (BT < 0) W.prev_pdf[slot] = bsdf_pdf_b(S.bsdfs, bsdf, pr, bf);
+                    else if constexpr (kBumpQ) W.prev_pdf[slot] = bump_pdf_t<BT>(S.bsdfs, bsdf, pr, bf);
                     else W.prev_pdf[slot] = bsdf_pdf_t<BT>(S.bsdfs, bsdf, pr);
                 }
             }

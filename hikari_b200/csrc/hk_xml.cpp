@@ -603,8 +603,8 @@ std::string resolve(const std::string &f) {
     return g_base_dir + "/" + f;
 }
 
-// Texture plugins (src/texture/{Checkerboard,Grid,Scale,Bitmap}Texture.cpp),
-// defaults of include/core/Common.hpp:425-458
+// Texture plugins (src/texture/{Checkerboard,Grid,Scale,Bitmap,Wireframe,Curvature}Texture.cpp),
+// defaults of include/core/Common.hpp:425-462
 class TexturePlugin : public Object {
 public:
     hk_texture_desc d{};
@@ -631,6 +631,21 @@ public:
             d.width = p.GetFloat("lineWidth", 0.01f);
         } else if (kind == HK_TEX_BITMAP) {
             load_bitmap(p);
+            return;
+        } else if (kind == HK_TEX_WIREFRAME) {   // WireframeTexture ctor (src/texture/WireframeTexture.cpp:10)
+            setc(d.a, p.GetColor("interiorColor", {0.5f, 0.5f, 0.5f}));
+            setc(d.b, p.GetColor("edgeColor", {0.1f, 0.1f, 0.1f}));
+            d.width = p.GetFloat("edgeWidth", 0.0f);
+            d.scale = p.GetFloat("transitionWidth", 0.5f);
+            return;
+        } else if (kind == HK_TEX_CURVATURE) {   // CurvatureTexture ctor (src/texture/CurvatureTexture.cpp:9)
+            setc(d.a, p.GetColor("positiveColor", {1.0f, 0.0f, 0.0f}));
+            setc(d.b, p.GetColor("negativeColor", {0.0f, 0.0f, 1.0f}));
+            d.scale = p.GetFloat("scale", 1.0f);
+            const std::string ct = p.GetString("curvatureType");
+            if (ct == "gaussian") d.count = 1;
+            else if (ct == "mean") d.count = 0;
+            else throw HikariException("Unexpected curvature type <" + ct + ">.");
             return;
         } else {
             d.scale = p.GetFloat("scale");
@@ -689,10 +704,14 @@ struct CheckerboardTexture : TexturePlugin { CheckerboardTexture(const PropertyL
 struct GridTexture : TexturePlugin { GridTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_GRID) {} };
 struct ScaleTexture : TexturePlugin { ScaleTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_SCALE) {} };
 struct BitmapTexture : TexturePlugin { BitmapTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_BITMAP) {} };
+struct WireframeTexture : TexturePlugin { WireframeTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_WIREFRAME) {} };
+struct CurvatureTexture : TexturePlugin { CurvatureTexture(const PropertyList &p) : TexturePlugin(p, HK_TEX_CURVATURE) {} };
 HK_REGISTER_CLASS(CheckerboardTexture, "checkerboard")
 HK_REGISTER_CLASS(GridTexture, "grid")
 HK_REGISTER_CLASS(ScaleTexture, "scale")
 HK_REGISTER_CLASS(BitmapTexture, "bitmap")
+HK_REGISTER_CLASS(WireframeTexture, "wireframe")
+HK_REGISTER_CLASS(CurvatureTexture, "curvature")
 
 // The texture slot (hk_bsdf_desc.tex) of a named BSDF texture child, -1 if the
 // BSDF takes no texture of that name (the plugins' AddChild)

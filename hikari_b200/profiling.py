@@ -4,7 +4,7 @@ selected raw metrics of a `--set full` report (`ncu -i X --page raw --csv`).
 
 usage: python -m hikari_b200.profiling launches <launches.csv>
        python -m hikari_b200.profiling raw <report.ncu-rep> [regex]
-       python -m hikari_b200.profiling render [--views V] [--spp S] [--accel bvh2|bvh8] [--out F]
+       python -m hikari_b200.profiling render [--workload heterogeneous|textured] [--views V] [--spp S] [--accel bvh2|bvh8] [--out F]
                                               [--threads-extend T] [--threads-shade T] [--fetch-steps K]
                                               [--fetch-min-idle K] [--shadow-tests M] [--closest-tests M]
        python -m hikari_b200.profiling traffic <metrics.csv> <render.json> [skip]
@@ -143,6 +143,9 @@ def render(argv):
     from hikari_b200 import scenes
 
     ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="heterogeneous", choices=["heterogeneous", "textured"],
+                    help="heterogeneous: 64 displaced icospheres (bench's default workload); textured: the "
+                         "bitmap / bump / normal-mapped light scene of bench.py --workload textured")
     ap.add_argument("--views", type=int, default=1)
     ap.add_argument("--spp", type=int, default=16)
     ap.add_argument("--accel", default="bvh2", choices=["bvh2", "bvh8"])
@@ -167,8 +170,13 @@ def render(argv):
         for k, v in json.load(open(a.config_json)).items():
             if hasattr(a, k) and v is not None:
                 setattr(a, k, int(v))
-    sd = scenes.heterogeneous(width=1024, height=1024, spp=a.spp, depth=16)
-    cams = scenes.heterogeneous_cameras(a.views)
+    if a.workload == "textured":
+        sd = scenes.lights_scene(width=1024, height=1024, spp=a.spp, depth=12, shading_normals=True, textured=True,
+                                 bitmap=True, bump=True)
+        cams = None
+    else:
+        sd = scenes.heterogeneous(width=1024, height=1024, spp=a.spp, depth=16)
+        cams = scenes.heterogeneous_cameras(a.views)
     gs = hk.Scene.from_desc(sd)
     gs.set_accel(hk.ACCEL_BVH8 if a.accel == "bvh8" else hk.ACCEL_BVH2)
     films = [torch.zeros(gs.film_shape(), device="cuda") for _ in range(a.views)]
@@ -182,7 +190,7 @@ def render(argv):
     torch.cuda.synchronize()
     c = [int(x) for x in ctr.cpu().tolist()]
     names = ["rays", "shadow_rays", "dropped", "node_visits", "tri_tests", "node_visits_shadow", "tri_tests_shadow"]
-    out = {"workload": f"heterogeneous {a.views} x 1024^2 x {a.spp} spp", "accel": a.accel,
+    out = {"workload": f"{a.workload} {a.views} x 1024^2 x {a.spp} spp", "accel": a.accel,
            "launch": {"capacity": a.capacity, "threads_extend": a.threads_extend, "threads_shade": a.threads_shade,
                       "fetch_steps": a.fetch_steps, "fetch_min_idle": a.fetch_min_idle,
                       "fetch_steps_shadow": a.fetch_steps_shadow, "fetch_min_idle_shadow": a.fetch_min_idle_shadow,

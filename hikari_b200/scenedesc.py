@@ -54,8 +54,9 @@ class SceneError(RuntimeError):
 
 
 # Procedural textures, matching hk_texture_kind in include/hikari_b200.h
-TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE, TEX_BITMAP = 1, 2, 3, 4
-TEX_TYPE_NAMES = {"checkerboard": TEX_CHECKERBOARD, "grid": TEX_GRID, "scale": TEX_SCALE, "bitmap": TEX_BITMAP}
+TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE, TEX_BITMAP, TEX_WIREFRAME, TEX_CURVATURE = 1, 2, 3, 4, 5, 6
+TEX_TYPE_NAMES = {"checkerboard": TEX_CHECKERBOARD, "grid": TEX_GRID, "scale": TEX_SCALE, "bitmap": TEX_BITMAP,
+                  "wireframe": TEX_WIREFRAME, "curvature": TEX_CURVATURE}
 # bitmap "filterType" and "uWrapMode" / "vWrapMode" (src/texture/BitmapTexture.cpp:15-46)
 FILTER_NEAREST, FILTER_BILINEAR, FILTER_TRILINEAR, FILTER_EWA = 0, 1, 2, 3
 FILTER_NAMES = {"nearest": FILTER_NEAREST, "bilinear": FILTER_BILINEAR, "trilinear": FILTER_TRILINEAR,
@@ -68,9 +69,13 @@ TEX_SLOTS = ("kd", "ks", "ks_refract", "sigma_a", "alpha_u", "alpha_v")
 
 @dataclass
 class TextureDesc:
-    """A procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp)
-    or a bitmap (src/texture/BitmapTexture.cpp); defaults are the reference's
-    (include/core/Common.hpp:425-458)."""
+    """A procedural texture (src/texture/{Checkerboard,Grid,Scale}Texture.cpp),
+    a bitmap (src/texture/BitmapTexture.cpp) or a texture of the hit's geometry
+    (src/texture/{Wireframe,Curvature}Texture.cpp); defaults are the reference's
+    (include/core/Common.hpp:425-462).  Wireframe: a interiorColor, b edgeColor,
+    width edgeWidth (0: a tenth of the mean edge length of the first mesh that
+    uses it), scale transitionWidth.  Curvature: a positiveColor, b
+    negativeColor, scale, count 1 "gaussian" / 0 "mean"."""
     kind: int
     count: int = 10                    # checkerboard "blocks", grid "lines"
     width: float = 0.01                # grid "lineWidth"
@@ -429,6 +434,21 @@ def _texture_from_xml(node: ET.Element) -> TextureDesc:
     d.uv_offset = [float(p.get("uOffset", 0.0)), float(p.get("vOffset", 0.0))]
     if d.kind == TEX_BITMAP:
         return _bitmap_from_xml(d, p)
+    if d.kind == TEX_WIREFRAME:   # WireframeTexture ctor (src/texture/WireframeTexture.cpp:10)
+        d.a = [float(c) for c in p.get("interiorColor", [0.5, 0.5, 0.5])]
+        d.b = [float(c) for c in p.get("edgeColor", [0.1, 0.1, 0.1])]
+        d.width = float(p.get("edgeWidth", 0.0))
+        d.scale = float(p.get("transitionWidth", 0.5))
+        return d
+    if d.kind == TEX_CURVATURE:   # CurvatureTexture ctor (src/texture/CurvatureTexture.cpp:9)
+        d.a = [float(c) for c in p.get("positiveColor", [1.0, 0.0, 0.0])]
+        d.b = [float(c) for c in p.get("negativeColor", [0.0, 0.0, 1.0])]
+        d.scale = float(p.get("scale", 1.0))
+        ct = p.get("curvatureType", "")
+        if ct not in ("gaussian", "mean"):
+            raise SceneError(f"Unexpected curvature type <{ct}>.")
+        d.count = 1 if ct == "gaussian" else 0
+        return d
     if d.kind == TEX_CHECKERBOARD:
         d.count = int(p.get("blocks", 10))
         d.a = [float(c) for c in p.get("colorA", [0.4, 0.4, 0.4])]

@@ -23,7 +23,8 @@ from .scenedesc import (AIR_IOR, BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_DI
                         BSDF_PLASTIC, BSDF_ROUGH_COATING, BSDF_ROUGH_CONDUCTOR, BSDF_ROUGH_DIELECTRIC,
                         BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, BSDF_BUMP_MAP, BSDF_NORMAL_MAP,
                         FILTER_BILINEAR, FILTER_EWA,
-                        FILTER_NEAREST, FILTER_TRILINEAR, GGX, TEX_BITMAP, TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE,
+                        FILTER_NEAREST, FILTER_TRILINEAR, GGX, TEX_BITMAP, TEX_CHECKERBOARD, TEX_CURVATURE, TEX_GRID, TEX_SCALE,
+                        TEX_WIREFRAME,
                         WRAP_CLAMP, BSDFDesc, CameraDesc, EnvDesc, FilterDesc, LightDesc, MeshDesc, SceneDesc,
                         TextureDesc)
 
@@ -199,7 +200,7 @@ def synthetic_image(width: int, height: int, channels: int, seed: int) -> np.nda
 
 def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 12, seed: int = 0,
                  shading_normals: bool = False, textured: bool = False, bitmap: bool = False,
-                 bump: bool = False) -> SceneDesc:
+                 bump: bool = False, geometric: bool = False) -> SceneDesc:
     """A ground quad and five displaced icospheres (diffuse, roughDiffuse,
     smooth plastic, rough conductor, smooth dielectric) lit, in emitter order,
     by a point light, an emissive quad, a constant environment and a
@@ -217,7 +218,11 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
     scaled one-channel EWA roughness on the conductor and a nearest, clamped
     refraction colour on the glass.  bump (with bitmap) wraps the ground in a
     bumpMap over an EWA bitmap, the roughDiffuse sphere in a normalMap and the
-    conductor in a bumpMap over a checkerboard."""
+    conductor in a bumpMap over a checkerboard.  geometric (with textured)
+    gives the textures of the hit's geometry: a wireframe albedo with the
+    automatic edge width on the diffuse sphere, a wireframe with a fixed edge
+    width on the ground, mean curvature on the plastic's kd and scaled
+    Gaussian curvature on the conductor's ks."""
     sd = SceneDesc()
     gp, gi = quad((-6, 0, 6), (6, 0, 6), (6, 0, -6), (-6, 0, -6))
     ground = MeshDesc(gp, gi, BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5]))
@@ -260,6 +265,15 @@ def lights_scene(width: int = 64, height: int = 64, spp: int = 16, depth: int = 
                                                           channels=1, filter=FILTER_EWA, max_anisotropy=8.0))
         mats[4].textures["ks_refract"] = TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(33, 17, 3, seed + 5),
                                                      filter=FILTER_NEAREST, wrap_u=WRAP_CLAMP, wrap_v=WRAP_CLAMP)
+    if textured and geometric:
+        ground.bsdf.textures["kd"] = TextureDesc(kind=TEX_WIREFRAME, a=[0.6, 0.6, 0.55], b=[0.05, 0.05, 0.2],
+                                                 width=0.4, scale=0.5)
+        mats[0].textures["kd"] = TextureDesc(kind=TEX_WIREFRAME, a=[0.8, 0.4, 0.2], b=[0.1, 0.1, 0.1], width=0.0,
+                                             scale=0.6)
+        mats[2].textures["kd"] = TextureDesc(kind=TEX_CURVATURE, a=[0.9, 0.3, 0.1], b=[0.1, 0.4, 0.9], scale=0.8,
+                                             count=0)
+        mats[3].textures["ks"] = TextureDesc(kind=TEX_SCALE, scale=0.9, nested=TextureDesc(
+            kind=TEX_CURVATURE, a=[1.0, 0.8, 0.3], b=[0.3, 0.8, 1.0], scale=2.0, count=1))
     if textured and bitmap and bump:
         ground.bsdf = BSDFDesc(type=BSDF_BUMP_MAP, nested=ground.bsdf, textures={"kd": TextureDesc(
             kind=TEX_SCALE, scale=0.02, nested=TextureDesc(kind=TEX_BITMAP, pixels=synthetic_image(60, 44, 3, seed + 6),

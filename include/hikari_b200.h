@@ -104,6 +104,14 @@ int hk_scene_destroy(hk_scene *s);
 #define HK_TEX_GRID 2
 #define HK_TEX_SCALE 3
 #define HK_TEX_BITMAP 4
+/* Textures of the hit's geometry (src/texture/{Wireframe,Curvature}Texture.cpp):
+ * wireframe: a interiorColor, b edgeColor, width edgeWidth (0: a tenth of the
+ * mean edge length of the first mesh, in scene order, whose BSDF uses it),
+ * scale transitionWidth; curvature: a positiveColor, b negativeColor, scale,
+ * count 1 "gaussian" / 0 "mean" curvatureType.  Neither may be the map of a
+ * bumpMap or normalMap. */
+#define HK_TEX_WIREFRAME 5
+#define HK_TEX_CURVATURE 6
 /* bitmap "filterType" */
 #define HK_FILTER_NEAREST 0
 #define HK_FILTER_BILINEAR 1

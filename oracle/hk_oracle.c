@@ -398,7 +398,14 @@ typedef struct {
  * it: the record's intersection (frames and dP/du, dP/dv for bumpMap /
  * normalMap), NULL in queries without one */
 /* dpdu / dpdv with has_uvp: Isect.dPdU / dPdV and bHasUVPartial (set with normals and texture coordinates) */
-typedef struct isect_s { v3 p; frame sh, geo; int mesh; float t; float uv[2]; v3 dpdu, dpdv; int has_uvp; } isect_t;
+/* edge_d, curv_h, curv_k: what the wireframe and curvature textures read (the
+ * distance from p to the nearest edge line of the hit triangle, the mean and
+ * Gaussian curvature from the UV partials), set only for meshes whose BSDF
+ * uses one of them */
+typedef struct isect_s {
+    v3 p; frame sh, geo; int mesh; float t; float uv[2]; v3 dpdu, dpdv; int has_uvp;
+    v3 dndu, dndv; float edge_d, curv_h, curv_k;
+} isect_t;
 typedef struct { v3 wi, wo; float eta; int measure; float uv[2]; float duv[4]; const isect_t *it; } brec;
 
 /* ------------------------------------------------------------ bitmap textures */
@@ -649,6 +656,7 @@ typedef struct {
     float func_int;    /* m_FuncIntegral */
     float inv_area;    /* Mesh::m_InvMeshArea */
     v3 radiance;
+    int geo_tex;       /* its BSDF uses a wireframe or curvature texture: hits compute their inputs */
 } mesh_t;
 
 typedef struct { int n; float *func; float *cdf; float integral; } pdf1d;
@@ -725,9 +733,10 @@ static int push_texture(ho_scene *s, const ho_texture_desc *d, mip_t *m) {
     return s->ntex++;
 }
 int ho_scene_add_texture(ho_scene *s, const ho_texture_desc *d) {
-    if (d->kind < HO_TEX_CHECKERBOARD || d->kind > HO_TEX_SCALE) return fail("unknown texture kind");
+    const int geo = d->kind == HO_TEX_WIREFRAME || d->kind == HO_TEX_CURVATURE;
+    if ((d->kind < HO_TEX_CHECKERBOARD || d->kind > HO_TEX_SCALE) && !geo) return fail("unknown texture kind");
     if (d->kind == HO_TEX_SCALE && (d->nested < 0 || d->nested >= s->ntex)) return fail("scale texture needs a nested texture");
-    if (d->kind != HO_TEX_SCALE && d->count <= 0) return fail("texture block / line count must be positive");
+    if (d->kind != HO_TEX_SCALE && !geo && d->count <= 0) return fail("texture block / line count must be positive");
     return push_texture(s, d, NULL);
 }
 /* BitmapTexture ctor (src/texture/BitmapTexture.cpp:7) over LoadImageFromFileR
@@ -1009,13 +1018,51 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
     if (d->type == HO_BSDF_BUMP_MAP || d->type == HO_BSDF_NORMAL_MAP) {   /* BumpMapBSDF::Activate :138 */
         if (d->nested < 0 || d->nested >= s->nb) return fail("bumpMap / normalMap needs a nested BSDF");
         if (d->tex[0] <= 0) return fail("bumpMap / normalMap needs a map texture");
+        int t = d->tex[0] - 1;
+        while (s->tex[t].kind == HO_TEX_SCALE) t = s->tex[t].nested;
+        if (s->tex[t].kind == HO_TEX_WIREFRAME || s->tex[t].kind == HO_TEX_CURVATURE)
+            return fail("a wireframe or curvature texture as a bump / normal map is not supported");
     }
     if (d->type < HO_BSDF_DIFFUSE || d->type > HO_BSDF_NORMAL_MAP) return fail("unknown BSDF type");
     return 0;
 }
 
+/* Whether texture tid is (or scales) a wireframe or curvature texture; a
+ * wireframe texture whose edgeWidth is 0 takes a tenth of the mean edge length
+ * of mesh mi (WireframeTexture::Eval, src/texture/WireframeTexture.cpp:37-53:
+ * the first mesh that evaluates it). */
+static int tex_geo(ho_scene *s, int tid, int mi) {
+    ho_texture_desc *t = &s->tex[tid];
+    if (t->kind == HO_TEX_SCALE) return tex_geo(s, t->nested, mi);
+    if (t->kind == HO_TEX_WIREFRAME && t->width == 0.0f) {
+        const mesh_t *m = &s->meshes[mi];
+        float ew = 0.0f;
+        for (uint32_t i = 0; i < m->nt; i++) {
+            const uint32_t *f = s->F + 3ull * (m->t0 + i);
+            const v3 p0 = vload(s->P + 3ull * f[0]), p1 = vload(s->P + 3ull * f[1]), p2 = vload(s->P + 3ull * f[2]);
+            const float l0 = norm(sub(p1, p0)), l1 = norm(sub(p2, p1)), l2 = norm(sub(p0, p2));
+            ew += (l0 + l1) + l2;
+        }
+        t->width = 0.1f * ew / (float)(3u * m->nt);
+    }
+    return t->kind == HO_TEX_WIREFRAME || t->kind == HO_TEX_CURVATURE;
+}
+static int bsdf_geo(ho_scene *s, int bid, int mi, int depth) {
+    if (bid < 0 || bid >= s->nb || depth > 4) return 0;
+    const ho_bsdf_desc *d = &s->bsdfs[bid].d;
+    int g = 0;
+    for (int k = 0; k < 6; k++)
+        if (d->tex[k] > 0) g |= tex_geo(s, d->tex[k] - 1, mi);
+    if (d->type == HO_BSDF_ROUGH_COATING || d->type == HO_BSDF_COATING || d->type == HO_BSDF_TWO_SIDED ||
+        d->type == HO_BSDF_BUMP_MAP || d->type == HO_BSDF_NORMAL_MAP)
+        g |= bsdf_geo(s, d->nested, mi, depth + 1);
+    if (d->type == HO_BSDF_TWO_SIDED) g |= bsdf_geo(s, d->nested2, mi, depth + 1);
+    return g;
+}
+
 int ho_scene_finalize(ho_scene *s) {
     for (int i = 0; i < s->nb; i++) if (activate_bsdf(s, &s->bsdfs[i])) return -1;
+    for (int i = 0; i < s->nm; i++) s->meshes[i].geo_tex = bsdf_geo(s, s->meshes[i].bsdf, i, 0);
     /* Mesh::Activate  src/core/Mesh.cpp:233 (area CDF) */
     for (int i = 0; i < s->nm; i++) {
         mesh_t *m = &s->meshes[i];
@@ -1055,11 +1102,41 @@ int ho_film_border(const ho_scene *s) { return s->border; }
  * ScaleTexture::Eval (src/texture/ScaleTexture.cpp:17) scales its nested texture. */
 static inline int mod_positive(int a, int b) { int r = a % b; return r < 0 ? r + b : r; }
 static v3 pattern_eval(const ho_texture_desc *t, float u, float v);
-/* duv NULL: Texture::Eval(Isect, bFilter = false) */
-static v3 tex_eval(const ho_texture_desc *T, mip_t *const *M, int id, const float *uvi, const float *duv) {
+static float smooth_step(float lo, float hi, float x) {   /* SmoothStep (include/core/Common.hpp:994) */
+    float v = (x - lo) / (hi - lo);
+    v = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);   /* Clamp (:752) */
+    return v * v * (-2.0f * v + 3.0f);
+}
+/* WireframeTexture::Eval (src/texture/WireframeTexture.cpp:22) and
+ * CurvatureTexture::Eval (src/texture/CurvatureTexture.cpp:34) from the hit's
+ * edge distance and curvatures; without an intersection (record-level
+ * queries) the interior colour and black */
+static v3 geo_tex_eval(const ho_texture_desc *t, const isect_t *it) {
+    if (t->kind == HO_TEX_WIREFRAME) {
+        if (!it) return vload(t->a);
+        const float w = t->width;
+        const float al = smooth_step(w * (1.0f - t->scale), w, it->edge_d);
+        return add(scl(vload(t->b), 1.0f - al), scl(vload(t->a), al));
+    }
+    const float val = !it ? 0.0f : (t->count ? it->curv_k : it->curv_h);
+    if (val < 0.0f) {
+        const float x = -val * t->scale;
+        return scl(vload(t->b), 1.0f < x ? 1.0f : x);   /* std::min(x, 1) */
+    }
+    if (val > 0.0f) {
+        const float x = val * t->scale;
+        return scl(vload(t->a), 1.0f < x ? 1.0f : x);
+    }
+    return V(0, 0, 0);
+}
+/* duv NULL: Texture::Eval(Isect, bFilter = false); it: the record's
+ * intersection (NULL in queries without one) */
+static v3 tex_eval(const ho_texture_desc *T, mip_t *const *M, int id, const float *uvi, const float *duv,
+                   const isect_t *it) {
     const ho_texture_desc *t = &T[id];
-    if (t->kind == HO_TEX_SCALE) return scl(tex_eval(T, M, t->nested, uvi, duv), t->scale);
+    if (t->kind == HO_TEX_SCALE) return scl(tex_eval(T, M, t->nested, uvi, duv, it), t->scale);
     if (t->kind == HO_TEX_BITMAP) return bitmap_eval(t, M[id], uvi, duv);
+    if (t->kind == HO_TEX_WIREFRAME || t->kind == HO_TEX_CURVATURE) return geo_tex_eval(t, it);
     return pattern_eval(t, uvi[0] * t->uv_scale[0] + t->uv_offset[0], uvi[1] * t->uv_scale[1] + t->uv_offset[1]);
 }
 /* CheckerboardTexture / GridTexture::Eval(UV) at already scaled coordinates */
@@ -1106,6 +1183,8 @@ static v3 tex_average(const ho_texture_desc *T, mip_t *const *M, int id) {
     if (t->kind == HO_TEX_SCALE) return scl(tex_average(T, M, t->nested), t->scale);
     if (t->kind == HO_TEX_BITMAP) return vload(M[id]->avg);   /* BitmapTexture::GetAverage :176 */
     if (t->kind == HO_TEX_CHECKERBOARD) return scl(add(vload(t->a), vload(t->b)), 0.5f);
+    if (t->kind == HO_TEX_WIREFRAME) return scl(add(vload(t->b), vload(t->a)), 0.5f);   /* :80 */
+    if (t->kind == HO_TEX_CURVATURE) return V(0.5f, 0.5f, 0.5f);                       /* :61 */
     float iw = fmaxf(0.0f, 1.0f - 2.0f * t->width);    /* GridTexture::GetAverage :40 */
     float ia = iw * iw, la = 1.0f - ia;
     return add(scl(vload(t->a), la), scl(vload(t->b), ia));
@@ -1114,15 +1193,15 @@ static v3 tex_average(const ho_texture_desc *T, mip_t *const *M, int id) {
  * slot: 0 kd, 1 ks, 2 ksRefract, 3 sigmaA, 4 alpha(U), 5 alphaV */
 static inline v3 par_rgb(const bsdf_t *b, int slot, const float *c, const brec *r) {
     int t = b->d.tex[slot];
-    return t ? tex_eval(b->textures, b->mips, t - 1, r->uv, r->duv) : vload(c);
+    return t ? tex_eval(b->textures, b->mips, t - 1, r->uv, r->duv, r->it) : vload(c);
 }
 static inline float par_alpha(const bsdf_t *b, int slot, float c, const brec *r) {
     int t = b->d.tex[slot];
-    return t ? tex_eval(b->textures, b->mips, t - 1, r->uv, r->duv).x : c;
+    return t ? tex_eval(b->textures, b->mips, t - 1, r->uv, r->duv, r->it).x : c;
 }
 void ho_texture_eval(const ho_scene *s, int id, const float *uv, const float *duv, float *out) {
     static const float zero[4] = {0, 0, 0, 0};
-    vstore(out, tex_eval(s->tex, s->mips, id, uv, duv ? duv : zero));
+    vstore(out, tex_eval(s->tex, s->mips, id, uv, duv ? duv : zero, NULL));
 }
 int ho_texture_mip(const ho_scene *s, int id, int level, int *wh, float *texels) {
     if (id < 0 || id >= s->ntex || !s->mips[id]) return fail("not a bitmap texture");
@@ -1759,7 +1838,7 @@ static frame perturbed_frame(const ho_scene *s, const bsdf_t *b, const isect_t *
         f.t = cross(f.n, f.s);
         if (dot(f.n, it->geo.n) < 0.0f) f.n = scl(f.n, -1.0f);
     } else {
-        v3 c = tex_eval(s->tex, s->mips, tid, it->uv, NULL);   /* Eval(Isect, false) */
+        v3 c = tex_eval(s->tex, s->mips, tid, it->uv, NULL, it);   /* Eval(Isect, false) */
         v3 nn = V(2.0f * c.x - 1.0f, 2.0f * c.y - 1.0f, 2.0f * c.z - 1.0f);
         f.n = normalize(to_world(&it->sh, nn));
         f.s = normalize(sub(it->dpdu, scl(f.n, dot(f.n, it->dpdu))));
@@ -2145,6 +2224,9 @@ static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
     it->mesh = s->tri_mesh[h->tri];
     it->t = h->t;
     it->has_uvp = 0;
+    it->dndu = it->dndv = V(0, 0, 0);
+    it->edge_d = INFINITY;
+    it->curv_h = it->curv_k = 0.0f;
     if (m->has_n && m->has_uv) {
         v3 dp1 = sub(p1, p0), dp2 = sub(p2, p0);
         float du1 = u1[0] - u0[0], dv1 = u1[1] - u0[1], du2 = u2[0] - u0[0], dv2 = u2[1] - u0[1];
@@ -2165,8 +2247,16 @@ static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
                 it->dpdv = scl(add(scl(dp1, -du2), scl(dp2, du1)), inv);
                 v3 ns = add(add(scl(n0, b0), scl(n1, b1)), scl(n2, b2));
                 float ln = norm(ns);
-                ns = scl(ns, 1.0f / ln);
+                float inv_ln = 1.0f / ln;
+                ns = scl(ns, inv_ln);
                 it->sh = frame_from_n_dpdu(ns, dpdu);
+                /* dN/du, dN/dv (:146-153) */
+                v3 dnu = scl(sub(n1, n0), inv_ln);
+                dnu = sub(dnu, scl(ns, dot(ns, dnu)));
+                v3 dnv = scl(sub(n2, n0), inv_ln);
+                dnv = sub(dnv, scl(ns, dot(ns, dnv)));
+                it->dndu = scl(sub(scl(dnu, dv2), scl(dnv, dv1)), inv);
+                it->dndv = scl(add(scl(dnu, -du2), scl(dnv, du1)), inv);
             }
         }
     } else if (m->has_n) {
@@ -2175,6 +2265,37 @@ static void post_intersect(const ho_scene *s, const hit_t *h, isect_t *it) {
     } else {
         it->sh = it->geo;
     }
+    if (m->geo_tex) {
+        /* WireframeTexture::Eval (src/texture/WireframeTexture.cpp:22-77): the
+         * distance from P to the nearest of the three edge lines */
+        const v3 ps[3] = {p0, p1, p2};
+        float min_d2 = FLT_MAX;
+        for (int i = 0; i < 3; i++) {
+            const v3 cur = ps[i], nxt = ps[(i + 1) % 3];
+            const v3 d1 = normalize(sub(nxt, cur)), d2 = sub(it->p, cur);
+            const v3 e = sub(add(cur, scl(d1, dot(d1, d2))), it->p);
+            const float d2x = dot(e, e);
+            min_d2 = d2x < min_d2 ? d2x : min_d2;   /* std::min */
+        }
+        it->edge_d = sqrtf(min_d2);
+        /* Shape::ComputeCurvature (src/core/Shape.cpp:30-51) */
+        if (it->has_uvp) {
+            const float E = dot(it->dpdu, it->dpdu), F = dot(it->dpdu, it->dpdv), G = dot(it->dpdv, it->dpdv);
+            const float L = -dot(it->dpdu, it->dndu), M = -dot(it->dpdv, it->dndu), N = -dot(it->dpdv, it->dndv);
+            const float inv_denom = 1.0f / (E * G - F * F);
+            it->curv_k = (L * N - M * M) * inv_denom;
+            it->curv_h = 0.5f * ((L * G - 2.0f * M * F) + N * E) * inv_denom;
+        }
+    }
+}
+/* Texture::Eval(Isect, true) at the intersection of (triangle, barycentric u, v) */
+void ho_texture_eval_hit(const ho_scene *s, int id, uint32_t tri, float u, float v, float *out) {
+    static const float zero[4] = {0, 0, 0, 0};
+    hit_t h; memset(&h, 0, sizeof h);
+    h.tri = tri; h.u = u; h.v = v;
+    isect_t it;
+    post_intersect(s, &h, &it);
+    vstore(out, tex_eval(s->tex, s->mips, id, it.uv, zero, &it));
 }
 /* Triangle::PostIntersect for (triangle, barycentric u, v): out p(3) s(3) t(3) n(3) uv(2) */
 void ho_post_intersect(const ho_scene *s, uint32_t tri, float u, float v, float *out) {

@@ -68,7 +68,8 @@ typedef struct {
 
 /* Procedural textures (src/texture/{Checkerboard,Grid,Scale}Texture.cpp) and
  * bitmap textures (src/texture/BitmapTexture.cpp over include/core/MipMap.hpp). */
-enum { HO_TEX_CHECKERBOARD = 1, HO_TEX_GRID = 2, HO_TEX_SCALE = 3, HO_TEX_BITMAP = 4 };
+enum { HO_TEX_CHECKERBOARD = 1, HO_TEX_GRID = 2, HO_TEX_SCALE = 3, HO_TEX_BITMAP = 4, HO_TEX_WIREFRAME = 5,
+       HO_TEX_CURVATURE = 6 };
 enum { HO_FILTER_NEAREST = 0, HO_FILTER_BILINEAR = 1, HO_FILTER_TRILINEAR = 2, HO_FILTER_EWA = 3 };
 enum { HO_WRAP_REPEAT = 0, HO_WRAP_CLAMP = 1, HO_WRAP_BLACK = 2 };
 typedef struct {
@@ -78,7 +79,11 @@ typedef struct {
     float width;           /* grid "lineWidth" */
     float scale;           /* scale "scale" */
     float uv_scale[2], uv_offset[2];   /* "uScale" "vScale", "uOffset" "vOffset" */
-    float a[3], b[3];      /* checkerboard colorA / colorB; grid lineColor / backgroundColor */
+    float a[3], b[3];      /* checkerboard colorA / colorB; grid lineColor / backgroundColor;
+                              wireframe interiorColor / edgeColor; curvature positiveColor / negativeColor */
+    /* wireframe: width "edgeWidth" (0: a tenth of the mean edge length of the
+     * first mesh whose BSDF uses it), scale "transitionWidth"; curvature:
+     * scale "scale", count 1 "gaussian" / 0 "mean" ("curvatureType") */
     /* bitmap: "filterType", "uWrapMode" / "vWrapMode", "channel" (1 = r, 3 = rgb),
      * "gamma", "maxAnisotropy" */
     int32_t filter, wrap_u, wrap_v, channels;
@@ -110,6 +115,11 @@ void ho_texture_eval(const ho_scene *s, int id, const float *uv, const float *du
  * levels, the level's size (out wh[2]) and texels (channels floats each,
  * row-major, row 0 = v 0) when texels != NULL. */
 int  ho_texture_mip(const ho_scene *s, int id, int level, int *wh, float *texels);
+/* Texture::Eval(Isect, true) at the intersection Triangle::PostIntersect makes
+ * of barycentric (u, v) on triangle tri (scene order): out rgb (3).  The form
+ * the wireframe and curvature textures need (they read the hit's triangle,
+ * position and UV partials). */
+void ho_texture_eval_hit(const ho_scene *s, int id, uint32_t tri, float u, float v, float *out);
 /* positions 3*nv, indices 3*nt (mesh-local), normals 3*nv or NULL,
  * radiance 3 or NULL (area light).  Returns mesh id or <0. */
 int  ho_scene_add_mesh(ho_scene *s, const float *positions, uint32_t nv,

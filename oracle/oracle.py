@@ -102,6 +102,7 @@ def lib():
         L.ho_bsdf_batch_isect.argtypes = [P, C.c_int, C.c_uint64, P, P, P, P, P, P, P, P, P, P, P, C.c_int]
         L.ho_scene_add_bitmap.argtypes = [P, C.POINTER(TextureDescC), P, C.c_int, C.c_int]
         L.ho_texture_eval.argtypes = [P, C.c_int, P, P, P]
+        L.ho_texture_eval_hit.argtypes = [P, C.c_int, C.c_uint32, C.c_float, C.c_float, P]
         L.ho_texture_mip.argtypes = [P, C.c_int, C.c_int, P, P]
         L.ho_screen_partials.argtypes = [P, C.c_float, C.c_float, C.c_uint32, C.c_float, C.c_float, P]
         L.ho_bsdf_rft_eval.argtypes = [P, C.c_int, C.c_float]
@@ -303,6 +304,15 @@ class OracleScene:
         out = np.zeros((uv.shape[0], 3), np.float32)
         for k in range(uv.shape[0]):
             lib().ho_texture_eval(self.h, tid, _p(uv[k]), _p(duv[k]) if duv is not None else None, _p(out[k]))
+        return out
+
+    def texture_eval_hit(self, tex, tri, u, v):
+        """Texture::Eval(Isect, true) of texture `tex` at the intersections of
+        triangles tri (scene order) at barycentric (u, v): n x 3."""
+        tid = tex if isinstance(tex, int) else self.tex_ids[id(tex)]
+        out = np.zeros((len(tri), 3), np.float32)
+        for k in range(len(tri)):
+            lib().ho_texture_eval_hit(self.h, tid, int(tri[k]), float(u[k]), float(v[k]), _p(out[k]))
         return out
 
     def texture_mip(self, tex):

@@ -183,14 +183,27 @@ void hr_post_intersect(void *h, uint32_t tri, float u, float v, float *out) {
 /* texture coordinates of the single-record queries (hr_bsdf_sample / eval / pdf) */
 void hr_set_uv(float u, float v) { g_isect.UV = Point2f(u, v); }
 
-/* kind 1 checkerboard, 2 grid, 3 scale (of nested) */
+/* kind 1 checkerboard, 2 grid, 3 scale (of nested), 5 wireframe (a interiorColor,
+ * b edgeColor, width edgeWidth, scale transitionWidth), 6 curvature (a
+ * positiveColor, b negativeColor, scale, count 1 gaussian / 0 mean) */
 void *hr_texture_create(int kind, int count, float width, float scale, const float *uv_scale, const float *uv_offset,
                         const float *a, const float *b, void *nested) {
     try {
         PropertyList pl;
         Color3f ca(a[0], a[1], a[2]), cb(b[0], b[1], b[2]);
-        const char *name = kind == 1 ? "checkerboard" : (kind == 2 ? "grid" : "scale");
-        if (kind == 1 || kind == 2) {
+        const char *name = kind == 1 ? "checkerboard"
+                                     : (kind == 2 ? "grid" : (kind == 5 ? "wireframe" : (kind == 6 ? "curvature" : "scale")));
+        if (kind == 5) {
+            pl.SetColor("interiorColor", ca);
+            pl.SetColor("edgeColor", cb);
+            pl.SetFloat("edgeWidth", width);
+            pl.SetFloat("transitionWidth", scale);
+        } else if (kind == 6) {
+            pl.SetColor("positiveColor", ca);
+            pl.SetColor("negativeColor", cb);
+            pl.SetFloat("scale", scale);
+            pl.SetString("curvatureType", count ? "gaussian" : "mean");
+        } else if (kind == 1 || kind == 2) {
             pl.SetInteger(kind == 1 ? "blocks" : "lines", count);
             pl.SetColor(kind == 1 ? "colorA" : "lineColor", ca);
             pl.SetColor(kind == 1 ? "colorB" : "backgroundColor", cb);
@@ -293,6 +306,20 @@ void hr_texture_eval(void *t, uint64_t n, const float *uv, const float *duv, flo
         Intersection I;
         I.UV = Point2f(uv[2 * i], uv[2 * i + 1]);
         if (duv) { I.dUdX = duv[4 * i]; I.dVdX = duv[4 * i + 1]; I.dUdY = duv[4 * i + 2]; I.dVdY = duv[4 * i + 3]; }
+        Color3f c = ((Texture *)t)->Eval(I, true);
+        out[3 * i] = c[0]; out[3 * i + 1] = c[1]; out[3 * i + 2] = c[2];
+    }
+}
+/* Texture::Eval(Isect, true) at the intersection Triangle::PostIntersect
+ * makes of barycentric (u, v) on triangle tri[i] of mesh: out rgb per record */
+void hr_texture_eval_hit(void *t, void *mesh, uint64_t n, const uint32_t *tri, const float *uv, float *out) {
+    ArrayMesh *m = (ArrayMesh *)mesh;
+    for (uint64_t i = 0; i < n; i++) {
+        Triangle T(m, m->facet(tri[i]), tri[i]);
+        Intersection I;
+        I.pShape = &T;
+        I.UV = Point2f(uv[2 * i], uv[2 * i + 1]);
+        T.PostIntersect(I);
         Color3f c = ((Texture *)t)->Eval(I, true);
         out[3 * i] = c[0]; out[3 * i + 1] = c[1]; out[3 * i + 2] = c[2];
     }

@@ -46,6 +46,10 @@ SCENES = {
     "bitmap": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True, textured=True, bitmap=True),
     "bump": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True, textured=True, bitmap=True,
                                         bump=True),
+    # wireframe and curvature textures: the edge distance and the curvatures of
+    # each hit computed on the device and by the oracle (pinned to the reference)
+    "geometric": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True, textured=True,
+                                             geometric=True),
 }
 
 

@@ -371,6 +371,49 @@ def test_xml_textures(L, tmp_path):
     assert c["alpha_v"].kind == TEX_SCALE and c["alpha_v"].nested.kind == TEX_CHECKERBOARD
 
 
+GEOMETRIC_XML = """<?xml version="1.0"?>
+<scene>
+  <integrator type="pathMIS"><integer name="depth" value="8"/></integrator>
+  <camera type="perspective"><integer name="width" value="16"/><integer name="height" value="16"/></camera>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="diffuse">
+      <texture type="wireframe" name="albedo"><color name="edgeColor" value="0.9, 0.1, 0.1"/>
+        <float name="transitionWidth" value="0.25"/></texture>
+    </bsdf>
+  </mesh>
+  <mesh type="obj"><string name="filename" value="quad.obj"/>
+    <bsdf type="roughConductor">
+      <texture type="curvature" name="ks"><string name="curvatureType" value="gaussian"/>
+        <float name="scale" value="3"/></texture>
+    </bsdf>
+  </mesh>
+</scene>
+"""
+
+
+def test_xml_wireframe_and_curvature_textures(L, tmp_path):
+    """The wireframe and curvature plugins (src/texture/{Wireframe,Curvature}Texture.cpp
+    ctors) in both parsers, with the reference's defaults."""
+    from hikari_b200.scenedesc import TEX_CURVATURE, TEX_WIREFRAME
+
+    (tmp_path / "quad.obj").write_text(QUAD_OBJ)
+    path = str(tmp_path / "geo.xml")
+    open(path, "w").write(GEOMETRIC_XML)
+    info, depth, spp = hk.parse_xml_info(path)
+    assert info.n_bsdfs == 2
+    sd = parse_xml(path)[0]
+    w = sd.meshes[0].bsdf.textures["kd"]
+    assert w.kind == TEX_WIREFRAME and w.b == pytest.approx([0.9, 0.1, 0.1]) and w.a == pytest.approx([0.5] * 3)
+    assert w.width == 0.0 and w.scale == pytest.approx(0.25)
+    c = sd.meshes[1].bsdf.textures["ks"]
+    assert c.kind == TEX_CURVATURE and c.count == 1 and c.scale == pytest.approx(3.0)
+    assert c.a == pytest.approx([1, 0, 0]) and c.b == pytest.approx([0, 0, 1])
+    bad = GEOMETRIC_XML.replace('value="gaussian"', 'value="total"')
+    open(path, "w").write(bad)
+    with pytest.raises(hk.HikariError, match="curvature type"):
+        hk.parse_xml_info(path)
+
+
 @pytest.mark.parametrize("body,needle", [
     ('<bsdf type="diffuse"><texture type="checkerboard" name="ks"/></bsdf>', "not supported"),
     ('<bsdf type="roughPlastic"><texture type="checkerboard" name="alpha"/></bsdf>', "not supported"),

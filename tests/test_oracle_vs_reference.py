@@ -361,3 +361,86 @@ def test_per_channel_ior_pinned_channel_by_channel(case):
         np.testing.assert_array_equal(a["s_wo"][valid], b["s_wo"][valid])
         np.testing.assert_array_equal(a["s_pdf"], b["s_pdf"])
         np.testing.assert_array_equal(a["p_pdf"], b["p_pdf"])
+
+
+_GEO_TEX = {}
+
+
+def _geo_textures(R):
+    """The reference's wireframe and curvature textures for the pin, made once
+    per process and kept: CurvatureTexture::Eval (src/texture/CurvatureTexture.cpp:39)
+    keeps its colour lookup in a function-local static lambda that captures the
+    first evaluated instance, so every curvature texture of a process colours
+    with that instance's scale and colours -- the pin gives both of its
+    curvature textures the same ones."""
+    from hikari_b200.scenedesc import TEX_CURVATURE, TEX_WIREFRAME
+
+    if not _GEO_TEX:
+        descs = {
+            "wire_auto": TextureDesc(kind=TEX_WIREFRAME, a=[0.8, 0.7, 0.6], b=[0.05, 0.1, 0.2], width=0.0, scale=0.5),
+            "wire_fixed": TextureDesc(kind=TEX_WIREFRAME, a=[0.9, 0.9, 0.9], b=[0.3, 0.0, 0.0], width=0.02,
+                                      scale=0.25),
+            "curv_mean": TextureDesc(kind=TEX_CURVATURE, a=[1.0, 0.2, 0.0], b=[0.0, 0.3, 1.0], scale=0.7, count=0),
+            "curv_gauss": TextureDesc(kind=TEX_CURVATURE, a=[1.0, 0.2, 0.0], b=[0.0, 0.3, 1.0], scale=0.7, count=1),
+        }
+        for name, t in descs.items():
+            arrs = [np.array(x, np.float32) for x in (t.uv_scale, t.uv_offset, t.a, t.b)]
+            h = R.hr_texture_create(t.kind, t.count, t.width, t.scale, *[O._p(a) for a in arrs], None)
+            assert h, name
+            _GEO_TEX[name] = (t, h, arrs)
+    return _GEO_TEX
+
+
+def test_oracle_wireframe_and_curvature_bit_exact_vs_reference():
+    """WireframeTexture::Eval (src/texture/WireframeTexture.cpp:22: distance to
+    the nearest edge line, the automatic edge width of a tenth of the mean edge
+    length) and CurvatureTexture::Eval over Shape::ComputeCurvature
+    (src/core/Shape.cpp:30, from the dP/du, dN/du partials of
+    Triangle::PostIntersect) at hits of a displaced icosphere with vertex
+    normals and texture coordinates, bit for bit."""
+    from hikari_b200 import scenes
+    from hikari_b200.scenedesc import MeshDesc
+
+    R = _ref_lib()
+    R.hr_mesh_create.restype = C.c_void_p
+    R.hr_mesh_create.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+    R.hr_texture_eval_hit.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]
+    R.hr_object_free.argtypes = [C.c_void_p]
+    tex = _geo_textures(R)
+    rng = np.random.default_rng(23)
+    P, F = scenes.displaced_icosphere(2, 1.0, (0.1, 0.2, -0.3), 0.1, 4)
+    P = P.astype(np.float32)
+    F = F.astype(np.uint32)
+    N = (P + rng.normal(0, 0.05, P.shape)).astype(np.float32)
+    # texture coordinates from the sphere's longitude and latitude, so the UV
+    # partials (and the curvatures) are smooth over most triangles
+    c = P - P.mean(0)
+    UV = np.stack([np.arctan2(c[:, 1], c[:, 0]) / (2 * np.pi) + 0.5,
+                   np.arccos(np.clip(c[:, 2] / np.linalg.norm(c, axis=1), -1, 1)) / np.pi], 1).astype(np.float32)
+    UV[F[0]] = UV[F[0][0]]                                # triangle 0: degenerate UVs (det == 0)
+    bsdf = BSDFDesc(type=BSDF_ROUGH_DIELECTRIC, distribution=GGX, alpha_u=0.3, alpha_v=0.3)
+    bsdf.textures = {"ks": tex["wire_auto"][0], "ks_refract": tex["wire_fixed"][0],
+                     "alpha_u": tex["curv_mean"][0], "alpha_v": tex["curv_gauss"][0]}
+    for name, (n_, uv_) in {"normals+uv": (N, UV), "plain": (None, None)}.items():
+        sd = SceneDesc()
+        sd.meshes.append(MeshDesc(P, F, bsdf, normals=n_, uv=uv_))
+        o = O.OracleScene(sd)
+        h = R.hr_mesh_create(O._p(P), len(P), O._p(n_), O._p(uv_), O._p(F), len(F))
+        tri = np.concatenate([[0, 0], rng.integers(0, len(F), 3000)]).astype(np.uint32)
+        u = rng.random(len(tri)).astype(np.float32)
+        v = (rng.random(len(tri)) * (1 - u)).astype(np.float32)
+        # barycentrics on and near the edges, where the wireframe's transition lies
+        u[2:200:3] = 0.0
+        v[3:200:3] = (1.0 - u[3:200:3]).astype(np.float32)
+        buv = np.stack([u, v], 1).astype(np.float32)
+        nz = 0
+        for key, (t, ht, _) in tex.items():
+            got = o.texture_eval_hit(t, tri, u, v)
+            ref = np.zeros((len(tri), 3), np.float32)
+            R.hr_texture_eval_hit(ht, h, len(tri), O._p(tri), O._p(buv), O._p(ref))
+            same = (got == ref) | (np.isnan(got) & np.isnan(ref))
+            assert same.all(), f"{name} {key}: {np.sum(~same.all(1))} hits differ, e.g. {got[~same.all(1)][:2]} vs " \
+                               f"{ref[~same.all(1)][:2]}"
+            nz += int(np.any(got != got[0], axis=1).sum())
+        assert nz > 0   # the textures vary over the hits
+        R.hr_object_free(h)
