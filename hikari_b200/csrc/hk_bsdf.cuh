@@ -151,11 +151,59 @@ __device__ __forceinline__ float cubic1d01(float x, const float *val, int size) 
     return (2.0f * t3 - 3.0f * t2 + 1) * f0 + (-2.0f * t3 + 3.0f * t2) * f1 + (t3 - 2.0f * t2 + t) * d0 +
            (t3 - t2) * d1;
 }
-// RoughTransmittance::Eval with eta and alpha fixed (src/core/RoughTransmitance.cpp:48-70)
-__device__ __forceinline__ float rft_eval(const DevBsdf &b, float c) {
+// EvalCubicInterpolate2D over [0,1]^2 (src/core/Common.cpp:285) of a
+// [y][x] table with sx x samples and sy y samples
+__device__ __forceinline__ bool cubic_knot_weights(float p, int size, float *w, int &knot) {
+    if (!(p >= 0.0f && p <= 1.0f)) return false;
+    float t = ((p - 0.0f) * (float)(size - 1)) / (1.0f - 0.0f);
+    knot = min((int)t, size - 2);
+    t = t - (float)knot;
+    const float t2 = t * t, t3 = t2 * t;
+    w[0] = 0.0f;
+    w[1] = 2.0f * t3 - 3.0f * t2 + 1;
+    w[2] = -2.0f * t3 + 3.0f * t2;
+    w[3] = 0.0f;
+    const float d0 = t3 - 2.0f * t2 + t, d1 = t3 - t2;
+    if (knot > 0) { w[2] += 0.5f * d0; w[0] -= 0.5f * d0; }
+    else { w[2] += d0; w[1] -= d0; }
+    if (knot + 2 < size) { w[3] += 0.5f * d1; w[1] -= 0.5f * d1; }
+    else { w[2] += d1; w[1] -= d1; }
+    return true;
+}
+__device__ __forceinline__ float cubic2d01(float px, float py, const float *val, int sx, int sy) {
+    float wx[4], wy[4];
+    int kx, ky;
+    if (!cubic_knot_weights(px, sx, wx, kx) || !cubic_knot_weights(py, sy, wy, ky)) return 0.0f;
+    float r = 0.0f;
+#pragma unroll
+    for (int y = -1; y <= 2; y++) {
+        const float w_y = wy[y + 1];
+#pragma unroll
+        for (int x = -1; x <= 2; x++) {
+            const float wxy = wx[x + 1] * w_y;
+            if (wxy == 0) continue;
+            r += __ldg(val + (ky + y) * sx + kx + x) * wxy;
+        }
+    }
+    return r;
+}
+// RoughTransmittance::Eval (src/core/RoughTransmitance.cpp:48-87): eta fixed,
+// alpha fixed (the activated 1D table) or, under a textured alpha, per query
+// (the 2D table over warped cos and warped alpha)
+__device__ __forceinline__ float rft_eval(const DevBsdf &b, float c, float alpha) {
     float wc = powf(fabsf(c), 0.25f);
     if (c < 0.0f) return 0.0f;
+    if (b.alpha_tex) {
+        const float wa = powf((alpha - b.rft_amin) / (b.rft_amax - b.rft_amin), 0.25f);
+        return clampf(cubic2d01(wc, wa, b.rft2d, b.rft_n, b.rft_an), 0.0f, 1.0f);
+    }
     return clampf(cubic1d01(wc, b.rft, b.rft_n), 0.0f, 1.0f);
+}
+// roughPlastic's 1 - IntData.EvalDiffuse(alpha) (:119-132): activated, or per query
+__device__ __forceinline__ float plastic_fdr(const DevBsdf &b, float alpha) {
+    if (!b.alpha_tex) return b.fdr_int;
+    const float wa = powf((alpha - b.rft_amin) / (b.rft_amax - b.rft_amin), 0.25f);
+    return 1.0f - clampf(cubic1d01(wa, b.rft_diff, b.rft_an), 0.0f, 1.0f);
 }
 
 __device__ __forceinline__ V3 ld_rgb(const float *p) { return v3(p[0], p[1], p[2]); }
@@ -550,11 +598,17 @@ __device__ __forceinline__ float dielectric_pdf(const DevBsdf &b, const BRec &r)
 }
 
 // ------------------------------------------------------------ roughPlastic
+// The roughness of roughPlastic / roughCoating: the activated constant, or the
+// texture's first channel clamped to [5e-4, 1] (RoughPlasticBSDF.cpp:77)
+__device__ __forceinline__ float coat_alpha(const DevBsdf &b, const BRec &r) {
+    return b.alpha_tex ? clampf(par_alpha(b, 4, b.alpha_u, r), 5e-4f, 1.0f) : b.alpha_u;
+}
 // src/bsdf/RoughPlasticBSDF.cpp:66-192
 __device__ __forceinline__ V3 plastic_eval(const DevBsdf &b, const BRec &r) {
     float ci = r.wi.z, co = r.wo.z;
     if (r.measure == kMeasureUnknown || ci <= 0.0f || co <= 0.0f) return v3(0, 0, 0);
-    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    const float a = coat_alpha(b, r);
+    Mfd d = mfd_make(b.distribution, a, a);
     float ct;
     V3 h = normalize(r.wi + r.wo);
     float D = mfd_eval(d, h);
@@ -563,24 +617,25 @@ __device__ __forceinline__ V3 plastic_eval(const DevBsdf &b, const BRec &r) {
     float val = F * D * G / (4.0f * ci);
     V3 res = par_rgb(b, 1, b.ks, r) * val;
     V3 dif = par_rgb(b, 0, b.kd, r);
-    float t12 = rft_eval(b, ci), t21 = rft_eval(b, co);
-    float fdr = b.fdr_int;
+    float t12 = rft_eval(b, ci, d.au), t21 = rft_eval(b, co, d.au);
+    float fdr = plastic_fdr(b, d.au);
     if (b.nonlinear) dif = v3(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
     else dif = dif / (1.0f - fdr);
     // INV_PI is a double literal in the reference: the scalar is formed in double
     float k = (float)(kInvPiD * co * t12 * t21 * b.inv_eta2);
     return res + dif * k;
 }
-__device__ __forceinline__ float plastic_spec_pdf(const DevBsdf &b, float ci) {
-    float sp = 1.0f - rft_eval(b, ci);
+__device__ __forceinline__ float plastic_spec_pdf(const DevBsdf &b, float ci, float alpha) {
+    float sp = 1.0f - rft_eval(b, ci, alpha);
     return (sp * b.spec_w) / (sp * b.spec_w + (1.0f - sp) * (1.0f - b.spec_w));
 }
 __device__ __forceinline__ float plastic_pdf(const DevBsdf &b, const BRec &r) {
     float ci = r.wi.z, co = r.wo.z;
     if (r.measure == kMeasureUnknown || ci <= 0.0f || co <= 0.0f) return 0.0f;
-    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    const float a = coat_alpha(b, r);
+    Mfd d = mfd_make(b.distribution, a, a);
     V3 h = normalize(r.wi + r.wo);
-    float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
+    float sp = plastic_spec_pdf(b, ci, d.au), dp = 1.0f - sp;
     float J = 1.0f / (4.0f * dot(r.wo, h));
     float res = mfd_pdf(d, h) * J * sp;
     res += dp * cos_hemi_pdf(r.wo);
@@ -589,8 +644,9 @@ __device__ __forceinline__ float plastic_pdf(const DevBsdf &b, const BRec &r) {
 __device__ __forceinline__ V3 plastic_sample(const DevBsdf &b, BRec &r, float ux, float uy) {
     float ci = r.wi.z;
     if (ci <= 0.0f) return v3(0, 0, 0);
-    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
-    float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
+    const float a = coat_alpha(b, r);
+    Mfd d = mfd_make(b.distribution, a, a);
+    float sp = plastic_spec_pdf(b, ci, d.au), dp = 1.0f - sp;
     bool spec;
     if (uy < sp) { uy /= sp; spec = true; }
     else { uy = (uy - sp) / (1.0f - sp); spec = false; }
@@ -869,7 +925,8 @@ __device__ __forceinline__ V3 coat_refract(V3 wi, float inv_eta) {   // RefractI
 __device__ __forceinline__ V3 coating_eval(const DevBsdf &b, const DevBsdf &nb, const BRec &r) {
     float ci = r.wi.z, co = r.wo.z;
     if (ci * co <= 0.0f) return v3(0, 0, 0);
-    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    const float a = coat_alpha(b, r);
+    Mfd d = mfd_make(b.distribution, a, a);
     V3 h = normalize(r.wi + r.wo) * signum(r.wo.z);
     float ct;
     float D = mfd_eval(d, h);
@@ -882,7 +939,7 @@ __device__ __forceinline__ V3 coating_eval(const DevBsdf &b, const DevBsdf &nb, 
     ri.wi = coat_refract(r.wi, b.inv_eta);
     ri.wo = coat_refract(r.wo, b.inv_eta);
     V3 nv = leaf_eval(nb, ri);
-    float ti = rft_eval(b, fabsf(ci)), to = rft_eval(b, fabsf(co));
+    float ti = rft_eval(b, fabsf(ci), d.au), to = rft_eval(b, fabsf(co), d.au);
     nv = v3(nv.x * ti * to, nv.y * ti * to, nv.z * ti * to);
     V3 sa = par_rgb(b, 3, b.sigma_a, r) * b.thickness;
     if (!is_zero(sa)) {
@@ -894,9 +951,10 @@ __device__ __forceinline__ V3 coating_eval(const DevBsdf &b, const DevBsdf &nb, 
 }
 __device__ __forceinline__ float coating_pdf(const DevBsdf &b, const DevBsdf &nb, const BRec &r) {
     V3 h = normalize(r.wi + r.wo) * signum(r.wo.z);
-    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    const float a = coat_alpha(b, r);
+    Mfd d = mfd_make(b.distribution, a, a);
     float ci = r.wi.z, co = r.wo.z;
-    float r12 = 1.0f - rft_eval(b, fabsf(ci));
+    float r12 = 1.0f - rft_eval(b, fabsf(ci), d.au);
     float sp = (r12 * b.spec_w) / (r12 * b.spec_w + (1.0f - r12) * (1.0f - b.spec_w));
     float np = 1.0f - sp;
     float res = 0.0f;
@@ -912,9 +970,10 @@ __device__ __forceinline__ float coating_pdf(const DevBsdf &b, const DevBsdf &nb
     return res + p * np;
 }
 __device__ __forceinline__ V3 coating_sample(const DevBsdf &b, const DevBsdf &nb, BRec &r, float ux, float uy, float u1) {
-    Mfd d = mfd_make(b.distribution, b.alpha_u, b.alpha_u);
+    const float a = coat_alpha(b, r);
+    Mfd d = mfd_make(b.distribution, a, a);
     float aci = fabsf(r.wi.z);
-    float r12 = 1.0f - rft_eval(b, aci);
+    float r12 = 1.0f - rft_eval(b, aci, d.au);
     float sp = (r12 * b.spec_w) / (r12 * b.spec_w + (1.0f - r12) * (1.0f - b.spec_w));
     bool spec;
     if (ux < sp) { spec = true; ux /= sp; }

@@ -44,8 +44,15 @@ struct alignas(16) DevBsdf {
     const DevTexture *textures;
     int32_t textured;
     int32_t geo_tex;                 // a wireframe or curvature texture in a slot here or in a nested BSDF
-    int32_t pad3, pad4;
+    int32_t alpha_tex;               // roughPlastic / roughCoating with a textured alpha: rft2d / rft_diff below
+    int32_t rft_an;                  // alpha samples of rft2d / rft_diff
     float rft[kRftThetaMax];
+    // a textured alpha: the transmittance left 2D by SetEta ([alpha][theta],
+    // rft_an x rft_n) and roughPlastic's diffuse one over alpha (rft_an)
+    const float *rft2d;
+    const float *rft_diff;
+    float rft_amin, rft_amax;
+    int32_t pad5, pad6;
 };
 
 // cutpoints per CDF in the environment map's guide tables (a power of two)

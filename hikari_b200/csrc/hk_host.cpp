@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -244,7 +245,7 @@ struct hk_scene {
     int32_t accel = HK_ACCEL_BVH8;
     DevBuf b_tris, b_nodes, b_wnodes, b_tri_normals, b_tri_uv, b_meshes, b_bsdfs, b_emitter_area, b_area, b_light_tris, b_light_normals,
         b_light_cdf, b_delta, b_textures, b_texels, b_env_rgb, b_env_marg_cdf, b_env_marg_func, b_env_cond_cdf, b_env_cond_func, b_env_cond_int, b_ftab,
-        b_env_marg_guide, b_env_cond_guide;
+        b_env_marg_guide, b_env_cond_guide, b_rft2d;
     DevBuf b_film, b_rgb, b_scratch;   // scratch: work counter + counters
     std::vector<std::unique_ptr<DevBuf>> batch_films;   // films of hk_render_batch_host
     hk_scene_info info{};
@@ -381,7 +382,37 @@ bool bsdf_textured(const hk_scene *s, int id, int depth) {
            bsdf_textured(s, d.type == hk::kTwoSided ? d.nested2 : -1, depth + 1);
 }
 
-hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs) {
+// Channel 0 of Texture::GetMinimum / GetMaximum, for the roughness range
+// check of a textured alpha: checkerboard / grid / wireframe the smaller and
+// larger colour, scale the nested range scaled, bitmaps their level-0
+// texels, curvature [0, 1]
+void tex_range0(const hk_scene *s, int id, float &lo, float &hi) {
+    const hk_texture_desc &t = s->textures[id];
+    if (t.kind == HK_TEX_SCALE) {
+        tex_range0(s, t.nested, lo, hi);
+        lo *= t.scale;
+        hi *= t.scale;
+        return;
+    }
+    if (t.kind == HK_TEX_CURVATURE) { lo = 0.0f; hi = 1.0f; return; }
+    if (t.kind == HK_TEX_BITMAP) {
+        const hk::MipPyramid &m = *s->bitmaps[id];
+        lo = FLT_MAX;
+        hi = -FLT_MAX;
+        const std::vector<float> &L = m.lv[0];
+        for (size_t i = 0; i < L.size(); i += (size_t)m.channels) {
+            lo = std::min(lo, L[i]);
+            hi = std::max(hi, L[i]);
+        }
+        return;
+    }
+    lo = std::min(t.a[0], t.b[0]);
+    hi = std::max(t.a[0], t.b[0]);
+}
+
+// rft_pool: where a textured alpha's 2D transmittance tables go (their
+// offsets are kept in rft2d / rft_diff until the pool is on the device)
+hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs, std::vector<float> &rft_pool) {
     hk::DevBsdf b;
     std::memset(&b, 0, sizeof b);
     if (d.type < hk::kDiffuse || d.type > hk::kNormalMap) throw HkError{HK_ERR_INVALID, "unknown BSDF type"};
@@ -389,8 +420,6 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
         if (d.tex[k] < 0 || d.tex[k] > (int)s->textures.size()) throw HkError{HK_ERR_INVALID, "invalid texture id"};
         b.tex[k] = d.tex[k];
     }
-    if ((d.type == hk::kRoughPlastic || d.type == hk::kRoughCoating) && d.tex[4])
-        throw HkError{HK_ERR_INVALID, "textured alpha of roughPlastic / roughCoating is not supported"};
     if (d.distribution != 0 && d.distribution != 1) throw HkError{HK_ERR_INVALID, "Unexpected distribution type"};
     b.type = d.type;
     b.distribution = d.distribution;
@@ -419,12 +448,29 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
         float alpha = b.alpha_u;
         float e = b.eta < 1.0f ? 1.0f / b.eta : b.eta;   // CheckEta / CheckAlpha (:315-345)
         if (e < t.eta_min || e > t.eta_max) throw HkError{HK_ERR_INVALID, "relative IOR outside the RFT table range"};
-        if (alpha < t.alpha_min || alpha > t.alpha_max) throw HkError{HK_ERR_INVALID, "alpha outside the RFT range"};
+        b.alpha_tex = d.tex[4] ? 1 : 0;
+        if (b.alpha_tex) {   // CheckAlpha(GetMinimum / GetMaximum) (RoughPlasticBSDF.cpp:268)
+            float lo, hi;
+            tex_range0(s, d.tex[4] - 1, lo, hi);
+            if (lo < t.alpha_min || lo > t.alpha_max || hi < t.alpha_min || hi > t.alpha_max)
+                throw HkError{HK_ERR_INVALID, "alpha texture outside the RFT range"};
+        } else if (alpha < t.alpha_min || alpha > t.alpha_max) {
+            throw HkError{HK_ERR_INVALID, "alpha outside the RFT range"};
+        }
         std::vector<float> t2d, d1d;
         float dsc;
         t.set_eta(b.eta, t2d, d1d);
-        t.set_alpha(t2d, d1d, alpha, b.rft, dsc);
         b.rft_n = (int)t.theta_n;
+        b.rft_an = (int)t.alpha_n;
+        b.rft_amin = t.alpha_min;
+        b.rft_amax = t.alpha_max;
+        if (b.alpha_tex) {   // no SetAlpha: the 2D table is interpolated per query
+            rft_pool.resize((rft_pool.size() + 3) & ~size_t(3));
+            b.rft2d = reinterpret_cast<const float *>(rft_pool.size());
+            rft_pool.insert(rft_pool.end(), t2d.begin(), t2d.end());
+        } else {
+            t.set_alpha(t2d, d1d, alpha, b.rft, dsc);
+        }
         if (d.type == hk::kRoughPlastic) {
             float ksv[3], kdv[3];
             par_average(s, d, 1, d.ks, ksv);
@@ -434,6 +480,11 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs)
             t.set_eta(b.inv_eta, t2d, d1d);   // m_pIntData: SetEta(1/eta) only
             float wa = std::pow((alpha - t.alpha_min) / (t.alpha_max - t.alpha_min), 0.25f);
             b.fdr_int = 1.0f - clampf(cubic1d(wa, d1d.data(), (int)t.alpha_n, 0.0f, 1.0f), 0.0f, 1.0f);
+            if (b.alpha_tex) {   // EvalDiffuse(alpha) per query
+                rft_pool.resize((rft_pool.size() + 3) & ~size_t(3));
+                b.rft_diff = reinterpret_cast<const float *>(rft_pool.size());
+                rft_pool.insert(rft_pool.end(), d1d.begin(), d1d.end());
+            }
         } else {
             float th = d.thickness;
             float sav[3];
@@ -587,8 +638,15 @@ void build_scene(hk_scene *s) {
         tex.push_back(x);
     }
     s->b_textures.upload(tex); track(s->b_textures);
-    for (auto &d : s->bsdfs) bs.push_back(activate_bsdf(s, d, (int)s->bsdfs.size()));
+    std::vector<float> rft_pool;
+    for (auto &d : s->bsdfs) bs.push_back(activate_bsdf(s, d, (int)s->bsdfs.size(), rft_pool));
+    if (!rft_pool.empty()) { s->b_rft2d.upload(rft_pool); track(s->b_rft2d); }
     for (size_t i = 0; i < bs.size(); ++i) {
+        if (bs[i].alpha_tex) {   // pool offsets -> device pointers
+            const float *base = s->b_rft2d.as<float>();
+            bs[i].rft2d = base + reinterpret_cast<size_t>(bs[i].rft2d);
+            if (bs[i].type == hk::kRoughPlastic) bs[i].rft_diff = base + reinterpret_cast<size_t>(bs[i].rft_diff);
+        }
         bs[i].textures = s->b_textures.as<hk::DevTexture>();
         bs[i].textured = bsdf_textured(s, (int)i, 0) ? 1 : 0;
         std::vector<int> geo;

@@ -721,14 +721,14 @@ int texture_slot(int type, const std::string &name) {
     case HK_BSDF_ROUGH_DIFFUSE: return name == "albedo" ? 0 : (name == "alpha" ? 4 : -1);
     case HK_BSDF_CONDUCTOR: return name == "ks" ? 1 : -1;
     case HK_BSDF_DIELECTRIC: return name == "ksReflect" ? 1 : (name == "ksRefract" ? 2 : -1);
-    case HK_BSDF_PLASTIC:
-    case HK_BSDF_ROUGH_PLASTIC: return name == "kd" ? 0 : (name == "ks" ? 1 : -1);
+    case HK_BSDF_PLASTIC: return name == "kd" ? 0 : (name == "ks" ? 1 : -1);
+    case HK_BSDF_ROUGH_PLASTIC: return name == "kd" ? 0 : (name == "ks" ? 1 : (name == "alpha" ? 4 : -1));
     case HK_BSDF_ROUGH_CONDUCTOR:
         return name == "ks" ? 1 : (name == "alpha" || name == "alphaU" ? 4 : (name == "alphaV" ? 5 : -1));
     case HK_BSDF_ROUGH_DIELECTRIC:
         return name == "ksReflect" ? 1 : name == "ksRefract" ? 2 : (name == "alpha" || name == "alphaU") ? 4
                                                                    : name == "alphaV" ? 5 : -1;
-    case HK_BSDF_ROUGH_COATING:
+    case HK_BSDF_ROUGH_COATING: return name == "ks" ? 1 : (name == "sigmaA" ? 3 : (name == "alpha" ? 4 : -1));
     case HK_BSDF_COATING: return name == "ks" ? 1 : (name == "sigmaA" ? 3 : -1);
     default: return -1;
     }

@@ -385,8 +385,8 @@ _TEX_NAMES = {
     BSDF_ROUGH_CONDUCTOR: {"ks": "ks", "alpha": "alpha_u", "alphaU": "alpha_u", "alphaV": "alpha_v"},
     BSDF_ROUGH_DIELECTRIC: {"ksReflect": "ks", "ksRefract": "ks_refract", "alpha": "alpha_u", "alphaU": "alpha_u",
                             "alphaV": "alpha_v"},
-    BSDF_ROUGH_PLASTIC: {"kd": "kd", "ks": "ks"},
-    BSDF_ROUGH_COATING: {"ks": "ks", "sigmaA": "sigma_a"},
+    BSDF_ROUGH_PLASTIC: {"kd": "kd", "ks": "ks", "alpha": "alpha_u"},
+    BSDF_ROUGH_COATING: {"ks": "ks", "sigmaA": "sigma_a", "alpha": "alpha_u"},
     BSDF_COATING: {"ks": "ks", "sigmaA": "sigma_a"},
 }
 

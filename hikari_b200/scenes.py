@@ -571,8 +571,9 @@ def smooth_materials():
 def textured_materials():
     """BSDFs with procedural textures on every textured parameter: diffuse and
     roughDiffuse albedo / roughness, smooth and rough conductors (ks, alphaU /
-    alphaV), dielectrics (ksReflect / ksRefract / alpha), plastics (kd, ks),
-    and coatings (ks, sigmaA) over textured diffuse."""
+    alphaV), dielectrics (ksReflect / ksRefract / alpha), plastics (kd, ks,
+    roughPlastic alpha), and coatings (ks, sigmaA, roughCoating alpha) over
+    diffuse."""
     chk = TextureDesc(kind=TEX_CHECKERBOARD, count=7, a=[0.9, 0.2, 0.1], b=[0.1, 0.3, 0.8], uv_scale=[1.5, 0.7],
                       uv_offset=[0.25, -0.1])
     grid = TextureDesc(kind=TEX_GRID, count=5, width=0.08, a=[0.05, 0.05, 0.05], b=[0.7, 0.6, 0.5])
@@ -600,6 +601,13 @@ def textured_materials():
                                        textures={"sigma_a": scaled, "ks": chk})),
         ("tex_coating", BSDFDesc(type=BSDF_COATING, nested=BSDFDesc(type=BSDF_DIFFUSE, textures={"kd": chk}),
                                  textures={"sigma_a": scaled})),
+        # textured roughness of the transmittance-table BSDFs (2D table per query)
+        ("tex_rough_plastic_alpha", BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=0.15,
+                                             alpha_v=0.15, textures={"alpha_u": a_grid, "kd": chk})),
+        ("tex_rough_coating_alpha", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=BECKMANN, alpha_u=0.2,
+                                             alpha_v=0.2, thickness=0.3, sigma_a=[0.2, 0.4, 0.8],
+                                             nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.6, 0.5, 0.4]),
+                                             textures={"alpha_u": a_chk})),
     ]
 
 

@@ -379,6 +379,13 @@ static float rft_eval1d(const float *t1d, int T, float c) {
     if (c < 0.0f) return 0.0f;
     return clampf(cubic1d(wc, t1d, T, 0.0f, 1.0f), 0.0f, 1.0f);
 }
+/* Eval with eta fixed, alpha per query (:71-87): the 2D cubic over warped cos, alpha */
+static float rft_eval2d(const float *t2d, int T, int A, float amin, float amax, float c, float alpha) {
+    float wc = powf(fabsf(c), 0.25f);
+    if (c < 0.0f) return 0.0f;
+    float wa = powf((alpha - amin) / (amax - amin), 0.25f);
+    return clampf(cubic2d(wc, wa, t2d, T, A), 0.0f, 1.0f);
+}
 
 /* ------------------------------------------------------------------ BSDF */
 #define RFT_MAX_THETA 128
@@ -390,6 +397,11 @@ typedef struct {
     float rft[RFT_MAX_THETA];          /* activated 1D transmittance table */
     int rft_n;
     float fdr_int;                     /* plastic: 1 - IntData.EvalDiffuse(alpha) */
+    /* a textured alpha of roughPlastic / roughCoating: the transmittance left
+     * 2D after SetEta ([alpha][theta]) and the plastic's diffuse one over alpha */
+    int alpha_tex, rft_an;
+    float rft_amin, rft_amax;
+    float *rft2d, *rft_diff;
     const ho_texture_desc *textures;   /* the scene's textures (set when finalized) */
     struct mip_t *const *mips;         /* their MIP pyramids (bitmaps; NULL otherwise) */
 } bsdf_t;
@@ -948,14 +960,37 @@ static v3 tex_average(const ho_texture_desc *T, mip_t *const *M, int id);
 static v3 par_average(const ho_scene *s, const ho_bsdf_desc *d, int slot, const float *c) {
     return d->tex[slot] ? tex_average(s->tex, s->mips, d->tex[slot] - 1) : vload(c);
 }
+/* channel 0 of Texture::GetMinimum / GetMaximum, for the roughness range
+ * check of a textured alpha (checkerboard / grid / wireframe: the smaller and
+ * larger colour; scale: the nested range scaled; bitmap: the level-0 texels;
+ * curvature: [0, 1]) */
+static void tex_range0(const ho_scene *s, int id, float *lo, float *hi) {
+    const ho_texture_desc *t = &s->tex[id];
+    if (t->kind == HO_TEX_SCALE) {
+        tex_range0(s, t->nested, lo, hi);
+        *lo *= t->scale; *hi *= t->scale;
+        return;
+    }
+    if (t->kind == HO_TEX_CURVATURE) { *lo = 0.0f; *hi = 1.0f; return; }
+    if (t->kind == HO_TEX_BITMAP) {
+        const mip_t *m = s->mips[id];
+        float mn = FLT_MAX, mx = -FLT_MAX;
+        for (int64_t i = 0; i < (int64_t)m->w[0] * m->h[0]; i++) {
+            mn = fminf(mn, m->lv[0][3 * i]);
+            mx = fmaxf(mx, m->lv[0][3 * i]);
+        }
+        *lo = mn; *hi = mx;
+        return;
+    }
+    *lo = fminf(t->a[0], t->b[0]);
+    *hi = fmaxf(t->a[0], t->b[0]);
+}
 static int activate_bsdf(ho_scene *s, bsdf_t *b) {
     const ho_bsdf_desc *d = &b->d;
     b->textures = s->tex;
     b->mips = s->mips;
     for (int k = 0; k < 6; k++)
         if (d->tex[k] < 0 || d->tex[k] > s->ntex) return fail("invalid texture id");
-    if ((d->type == HO_BSDF_ROUGH_PLASTIC || d->type == HO_BSDF_ROUGH_COATING) && d->tex[4])
-        return fail("textured alpha of roughPlastic / roughCoating is not supported");
     b->eta = d->int_ior / d->ext_ior;
     b->inv_eta = 1.0f / b->eta;
     b->inv_eta2 = b->inv_eta * b->inv_eta;
@@ -967,13 +1002,29 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
         float alpha = clampf(d->alpha_u, 5e-4f, 1.0f);
         float e = b->eta < 1.0f ? 1.0f / b->eta : b->eta;        /* CheckEta :315 */
         if (e < t->eta_min || e > t->eta_max) return fail("eta outside RFT range");
-        if (alpha < t->alpha_min || alpha > t->alpha_max) return fail("alpha outside RFT range");
         int A = (int)t->alpha_n, T = (int)t->theta_n;
         float *t2d = malloc(4ull * A * T), *d1d = malloc(4ull * A);
         float dsc;
+        b->alpha_tex = d->tex[4] != 0;
+        if (b->alpha_tex) {   /* CheckAlpha(GetMinimum / GetMaximum) (RoughPlasticBSDF.cpp:268) */
+            float lo, hi;
+            tex_range0(s, d->tex[4] - 1, &lo, &hi);
+            if (lo < t->alpha_min || lo > t->alpha_max || hi < t->alpha_min || hi > t->alpha_max)
+                return fail("alpha outside RFT range");
+        } else if (alpha < t->alpha_min || alpha > t->alpha_max) {
+            return fail("alpha outside RFT range");
+        }
         rft_set_eta(t, b->eta, t2d, d1d);
-        rft_set_alpha(t, t2d, d1d, alpha, b->rft, &dsc);
         b->rft_n = T;
+        b->rft_an = A;
+        b->rft_amin = t->alpha_min;
+        b->rft_amax = t->alpha_max;
+        if (b->alpha_tex) {   /* no SetAlpha: Eval interpolates in alpha per query */
+            b->rft2d = t2d;
+            t2d = malloc(4ull * A * T);
+        } else {
+            rft_set_alpha(t, t2d, d1d, alpha, b->rft, &dsc);
+        }
         if (d->type == HO_BSDF_ROUGH_PLASTIC) {
             float ksa = lum(par_average(s, d, 1, d->ks)), kda = lum(par_average(s, d, 0, d->kd));
             b->spec_w = ksa / (kda + ksa);
@@ -982,6 +1033,10 @@ static int activate_bsdf(ho_scene *s, bsdf_t *b) {
             float wa = powf((alpha - t->alpha_min) / (t->alpha_max - t->alpha_min), 0.25f);
             float ed = clampf(cubic1d(wa, d1d, A, 0.0f, 1.0f), 0.0f, 1.0f);
             b->fdr_int = 1.0f - ed;
+            if (b->alpha_tex) {
+                b->rft_diff = d1d;
+                d1d = malloc(4ull * A);
+            }
         } else {
             float th = d->thickness;
             v3 sav = par_average(s, d, 3, d->sigma_a);
@@ -1216,6 +1271,18 @@ int ho_texture_mip(const ho_scene *s, int id, int level, int *wh, float *texels)
     return m->levels;
 }
 static inline float alpha_u_of(const bsdf_t *b, const brec *r) { return clampf(par_alpha(b, 4, b->d.alpha_u, r), 5e-4f, 1.0f); }
+/* the rough BSDFs' RoughTransmittance::Eval(c, Distribution.GetAlpha()) and
+ * 1 - EvalDiffuse(alpha): the activated 1D table, or the 2D one per query
+ * under a textured alpha (src/core/RoughTransmitance.cpp:48-87, :119-132) */
+static inline float rft_b(const bsdf_t *b, float c, float alpha) {
+    return b->alpha_tex ? rft_eval2d(b->rft2d, b->rft_n, b->rft_an, b->rft_amin, b->rft_amax, c, alpha)
+                        : rft_eval1d(b->rft, b->rft_n, c);
+}
+static inline float fdr_b(const bsdf_t *b, float alpha) {
+    if (!b->alpha_tex) return b->fdr_int;
+    float wa = powf((alpha - b->rft_amin) / (b->rft_amax - b->rft_amin), 0.25f);
+    return 1.0f - clampf(cubic1d(wa, b->rft_diff, b->rft_an, 0.0f, 1.0f), 0.0f, 1.0f);
+}
 static inline float alpha_v_of(const bsdf_t *b, const brec *r) {
     return b->d.anisotropic ? clampf(par_alpha(b, 5, b->d.alpha_v, r), 5e-4f, 1.0f) : alpha_u_of(b, r);
 }
@@ -1374,16 +1441,16 @@ static v3 plastic_eval(const bsdf_t *b, const brec *r) {
     float val = F * D * G / (4.0f * ci);
     v3 res = scl(par_rgb(b, 1, b->d.ks, r), val);
     v3 dif = par_rgb(b, 0, b->d.kd, r);
-    float t12 = rft_eval1d(b->rft, b->rft_n, ci);
-    float t21 = rft_eval1d(b->rft, b->rft_n, co);
-    float fdr = b->fdr_int;
+    float t12 = rft_b(b, ci, d.au);
+    float t21 = rft_b(b, co, d.au);
+    float fdr = fdr_b(b, d.au);
     if (b->d.nonlinear) dif = V(dif.x / (1.0f - dif.x * fdr), dif.y / (1.0f - dif.y * fdr), dif.z / (1.0f - dif.z * fdr));
     else dif = divs(dif, 1.0f - fdr);
     float k = (float)(INV_PI_D * co * t12 * t21 * b->inv_eta2);
     return add(res, scl(dif, k));
 }
-static float plastic_spec_pdf(const bsdf_t *b, float ci) {
-    float sp = 1.0f - rft_eval1d(b->rft, b->rft_n, ci);
+static float plastic_spec_pdf(const bsdf_t *b, float ci, float alpha) {
+    float sp = 1.0f - rft_b(b, ci, alpha);
     return (sp * b->spec_w) / (sp * b->spec_w + (1.0f - sp) * (1.0f - b->spec_w));
 }
 static float plastic_pdf(const bsdf_t *b, const brec *r) {
@@ -1392,7 +1459,7 @@ static float plastic_pdf(const bsdf_t *b, const brec *r) {
     float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     v3 h = normalize(add(r->wi, r->wo));
-    float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
+    float sp = plastic_spec_pdf(b, ci, d.au), dp = 1.0f - sp;
     float J = 1.0f / (4.0f * dot(r->wo, h));
     float res = mfd_pdf(&d, h) * J * sp;
     res += dp * cos_hemi_pdf(r->wo);
@@ -1403,7 +1470,7 @@ static v3 plastic_sample(const bsdf_t *b, brec *r, float ux, float uy) {
     if (ci <= 0.0f) return V(0, 0, 0);
     float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
-    float sp = plastic_spec_pdf(b, ci), dp = 1.0f - sp;
+    float sp = plastic_spec_pdf(b, ci, d.au), dp = 1.0f - sp;
     int spec;
     if (uy < sp) { uy /= sp; spec = 1; }
     else { uy = (uy - sp) / (1.0f - sp); spec = 0; }
@@ -1450,7 +1517,7 @@ static v3 coating_eval(const ho_scene *s, const bsdf_t *b, const brec *r) {
     ri.wi = coat_refract(r->wi, b->inv_eta);
     ri.wo = coat_refract(r->wo, b->inv_eta);
     v3 nv = bsdf_eval(s, b->d.nested, &ri);
-    float ti = rft_eval1d(b->rft, b->rft_n, fabsf(ci)), to = rft_eval1d(b->rft, b->rft_n, fabsf(co));
+    float ti = rft_b(b, fabsf(ci), d.au), to = rft_b(b, fabsf(co), d.au);
     nv = V(nv.x * ti * to, nv.y * ti * to, nv.z * ti * to);
     v3 sa = scl(par_rgb(b, 3, b->d.sigma_a, r), b->d.thickness);
     if (!is_zero(sa)) {
@@ -1465,7 +1532,7 @@ static float coating_pdf(const ho_scene *s, const bsdf_t *b, const brec *r) {
     float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     float ci = r->wi.z, co = r->wo.z;
-    float r12 = 1.0f - rft_eval1d(b->rft, b->rft_n, fabsf(ci));
+    float r12 = 1.0f - rft_b(b, fabsf(ci), d.au);
     float sp = (r12 * b->spec_w) / (r12 * b->spec_w + (1.0f - r12) * (1.0f - b->spec_w));
     float np = 1.0f - sp;
     float res = 0.0f;
@@ -1485,7 +1552,7 @@ static v3 coating_sample(const ho_scene *s, const bsdf_t *b, brec *r, float ux, 
     float a = alpha_u_of(b, r);
     mfd d = mfd_make(b->d.distribution, a, a);
     float aci = fabsf(r->wi.z);
-    float r12 = 1.0f - rft_eval1d(b->rft, b->rft_n, aci);
+    float r12 = 1.0f - rft_b(b, aci, d.au);
     float sp = (r12 * b->spec_w) / (r12 * b->spec_w + (1.0f - r12) * (1.0f - b->spec_w));
     int spec;
     if (ux < sp) { spec = 1; ux /= sp; }

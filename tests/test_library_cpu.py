@@ -416,7 +416,7 @@ def test_xml_wireframe_and_curvature_textures(L, tmp_path):
 
 @pytest.mark.parametrize("body,needle", [
     ('<bsdf type="diffuse"><texture type="checkerboard" name="ks"/></bsdf>', "not supported"),
-    ('<bsdf type="roughPlastic"><texture type="checkerboard" name="alpha"/></bsdf>', "not supported"),
+    ('<bsdf type="roughPlastic"><texture type="checkerboard" name="sigmaA"/></bsdf>', "not supported"),
     ('<bsdf type="diffuse"><texture type="scale" name="albedo"><float name="scale" value="2"/></texture></bsdf>',
      "nested texture"),
 ])

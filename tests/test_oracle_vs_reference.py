@@ -120,6 +120,19 @@ def _cases():
         "tex_rough_diffuse": BSDFDesc(type=BSDF_ROUGH_DIFFUSE, textures={"kd": GRID, "alpha_u": ALPHA_CHECKER}),
         "tex_dielectric": BSDFDesc(type=BSDF_DIELECTRIC, textures={"ks": GRID, "ks_refract": SCALED}),
         "tex_conductor": BSDFDesc(type=BSDF_CONDUCTOR, int_ior=0.27, ext_ior=1.0, k=CU_K, textures={"ks": CHECKER}),
+        # textured roughness of the transmittance-table BSDFs: RoughTransmittance::Eval
+        # in 2D per query, EvalDiffuse over alpha (src/core/RoughTransmitance.cpp:71-132)
+        "tex_rough_plastic_alpha": BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=GGX, alpha_u=0.15, alpha_v=0.15,
+                                            textures={"alpha_u": ALPHA_GRID, "kd": CHECKER}),
+        "tex_rough_plastic_alpha_nonlinear": BSDFDesc(type=BSDF_ROUGH_PLASTIC, distribution=BECKMANN, alpha_u=0.3,
+                                                      alpha_v=0.3, kd=[0.8, 0.4, 0.1], nonlinear=True,
+                                                      textures={"alpha_u": ALPHA_CHECKER}),
+        "tex_coating_alpha": BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2,
+                                      nested=nested, textures={"alpha_u": ALPHA_CHECKER}),
+        "tex_coating_alpha_beckmann": BSDFDesc(type=BSDF_ROUGH_COATING, distribution=BECKMANN, alpha_u=0.2,
+                                               alpha_v=0.2, thickness=0.3, sigma_a=[0.2, 0.4, 0.8],
+                                               nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.6, 0.5, 0.4]),
+                                               textures={"alpha_u": ALPHA_GRID}),
     }
 
 
