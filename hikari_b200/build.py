@@ -12,6 +12,7 @@ import os
 import re
 import subprocess
 import sys
+import threading
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -70,6 +71,23 @@ def needs_build() -> bool:
                for s in SOURCES)
 
 
+def _host_gb() -> float:
+    try:
+        return os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 1e9
+    except (ValueError, OSError):
+        return 64.0
+
+
+def _unit_gb(cmd) -> float:
+    """Peak host memory (GB) the unit's compile is expected to take."""
+    name = next((os.path.basename(a) for a in cmd if a.endswith((".cu", ".cpp"))), "")
+    if name in ("hk_render_b8t.cu", "hk_render_b2t.cu", "hk_wf_shade_3.cu"):
+        return 22.0
+    if name.startswith("hk_render_"):
+        return 10.0
+    return 3.0
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
@@ -88,9 +106,28 @@ def build(force: bool = False, verbose: bool = False) -> str:
             print(" ".join(cmd))
         cmds.append(cmd)
     # translation units compile in parallel (SOURCES lists the slowest first)
+    # within a host-memory budget: ptxas takes about 20 GB for the textured
+    # megakernels and the run-time-dispatched shade kernel, 9 GB for the other
+    # megakernels and a few GB for the rest
+    total = max(16.0, _host_gb() * 0.75)
+    budget = [total]
+    cv = threading.Condition()
+
+    def run(cmd):
+        need = min(total, _unit_gb(cmd))
+        with cv:
+            cv.wait_for(lambda: budget[0] >= need)
+            budget[0] -= need
+        try:
+            return subprocess.check_call(cmd)
+        finally:
+            with cv:
+                budget[0] += need
+                cv.notify_all()
+
     if cmds:
         with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
-            for f in [ex.submit(subprocess.check_call, c) for c in cmds]:
+            for f in [ex.submit(run, c) for c in cmds]:
                 f.result()
     tmp = LIB + ".tmp"
     subprocess.check_call([_nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lpthread", "-lz"])

@@ -568,6 +568,74 @@ def smooth_materials():
     ]
 
 
+def nested_materials():
+    """Layered BSDFs nested deeper than one coating over a leaf: a rough
+    coating over a smooth coating over a rough conductor, a smooth coating
+    over a rough coating over diffuse, three layers (rough over smooth over
+    rough) over a plastic, a coating over a two-sided BSDF, a two-sided BSDF
+    inside a two-sided one, a two-sided BSDF over a doubly coated conductor,
+    and a coating stack over a rough dielectric (the innermost layer still
+    transmits)."""
+    rc = BSDFDesc(type=BSDF_ROUGH_CONDUCTOR, distribution=GGX, alpha_u=0.2, alpha_v=0.2, int_ior=0.27, ext_ior=1.0,
+                  k=CU_K)
+    dif = BSDFDesc(type=BSDF_DIFFUSE, kd=[0.7, 0.5, 0.3])
+    return [
+        ("rough_over_smooth_conductor", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.15,
+                                                 alpha_v=0.15, int_ior=1.4, ext_ior=1.0,
+                                                 nested=BSDFDesc(type=BSDF_COATING, int_ior=1.6, ext_ior=1.0,
+                                                                 sigma_a=[0.3, 0.2, 0.1], thickness=0.4,
+                                                                 nested=rc))),
+        ("smooth_over_rough_diffuse", BSDFDesc(type=BSDF_COATING, int_ior=1.5, ext_ior=1.0, ks=[0.9, 0.9, 0.8],
+                                               nested=BSDFDesc(type=BSDF_ROUGH_COATING, distribution=BECKMANN,
+                                                               alpha_u=0.3, alpha_v=0.3, thickness=0.5,
+                                                               sigma_a=[0.4, 0.8, 1.2], nested=dif))),
+        ("three_layers_plastic", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=BECKMANN, alpha_u=0.25, alpha_v=0.25,
+                                          nested=BSDFDesc(type=BSDF_COATING, int_ior=1.3, ext_ior=1.0,
+                                                          nested=BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX,
+                                                                          alpha_u=0.1, alpha_v=0.1, int_ior=1.7,
+                                                                          ext_ior=1.0,
+                                                                          nested=BSDFDesc(type=BSDF_PLASTIC,
+                                                                                          kd=[0.2, 0.5, 0.7]))))),
+        ("coating_over_twosided", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2, alpha_v=0.2,
+                                           nested=BSDFDesc(type=BSDF_TWO_SIDED, nested=dif, nested2=rc))),
+        ("twosided_in_twosided", BSDFDesc(type=BSDF_TWO_SIDED,
+                                          nested=BSDFDesc(type=BSDF_TWO_SIDED, nested=rc, nested2=dif),
+                                          nested2=BSDFDesc(type=BSDF_MIRROR))),
+        ("twosided_double_coated", BSDFDesc(type=BSDF_TWO_SIDED,
+                                            nested=BSDFDesc(type=BSDF_COATING, int_ior=1.5, ext_ior=1.0,
+                                                            nested=BSDFDesc(type=BSDF_ROUGH_COATING,
+                                                                            distribution=GGX, alpha_u=0.3,
+                                                                            alpha_v=0.3, nested=rc)),
+                                            nested2=dif)),
+        ("coatings_over_rough_dielectric", BSDFDesc(type=BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.1,
+                                                    alpha_v=0.1, int_ior=1.3, ext_ior=1.0,
+                                                    nested=BSDFDesc(type=BSDF_COATING, int_ior=1.4, ext_ior=1.0,
+                                                                    nested=BSDFDesc(type=BSDF_ROUGH_DIELECTRIC,
+                                                                                    distribution=GGX, alpha_u=0.2,
+                                                                                    alpha_v=0.2, int_ior=1.5,
+                                                                                    ext_ior=1.0)))),
+    ]
+
+
+def cornell_nested(seed: int = 0, width: int = 256, height: int = 256, spp: int = 64, depth: int = 64) -> SceneDesc:
+    """The Cornell box with deeply nested layered BSDFs on its walls and boxes
+    (the set of nested_materials: coatings over coatings, coatings over
+    two-sided BSDFs, two-sided BSDFs inside two-sided ones; the coating stack
+    over a rough dielectric is left out, so that no path draws the random
+    number of a transmission lobe it may not reach)."""
+    sd = cornell_box(seed, width, height, spp, depth)
+    mats = dict(nested_materials())
+    floor, ceil, back, left, right, tall, short, light = sd.meshes
+    floor.bsdf = mats["three_layers_plastic"]
+    back.bsdf = mats["twosided_in_twosided"]
+    left.bsdf = mats["smooth_over_rough_diffuse"]
+    right.bsdf = mats["coating_over_twosided"]
+    ceil.bsdf = mats["twosided_double_coated"]
+    tall.bsdf = mats["rough_over_smooth_conductor"]
+    short.bsdf = BSDFDesc(type=BSDF_COATING, int_ior=1.45, ext_ior=1.0, nested=mats["twosided_in_twosided"])
+    return sd
+
+
 def textured_materials():
     """BSDFs with procedural textures on every textured parameter: diffuse and
     roughDiffuse albedo / roughness, smooth and rough conductors (ks, alphaU /

@@ -13,6 +13,7 @@ from hikari_b200.scenedesc import (BECKMANN, BSDF_COATING, BSDF_CONDUCTOR, BSDF_
                                    BSDF_ROUGH_DIELECTRIC, BSDF_ROUGH_DIFFUSE, BSDF_ROUGH_PLASTIC, BSDF_TWO_SIDED, GGX,
                                    SMOOTH_BSDFS, TEX_CHECKERBOARD, TEX_GRID, TEX_SCALE, TEX_SLOTS, BSDFDesc,
                                    SceneDesc, TextureDesc)
+from hikari_b200 import scenes
 from oracle import oracle as O
 
 from oracle import ref_build  # noqa: E402
@@ -133,6 +134,8 @@ def _cases():
                                                alpha_v=0.2, thickness=0.3, sigma_a=[0.2, 0.4, 0.8],
                                                nested=BSDFDesc(type=BSDF_DIFFUSE, kd=[0.6, 0.5, 0.4]),
                                                textures={"alpha_u": ALPHA_GRID}),
+        # layered BSDFs nested deeper than one coating over a leaf
+        **{"nested_" + k: v for k, v in scenes.nested_materials()},
     }
 
 
