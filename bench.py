@@ -64,8 +64,9 @@ def parse():
     ap.add_argument("--jobs", type=int, default=400, help="serving: jobs of the Poisson run")
     ap.add_argument("--load", type=float, default=0.8, help="serving: arrival rate as a fraction of the peak")
     ap.add_argument("--capacity", type=int, default=1 << 19, help="serving: path slots of each scene's pool")
-    ap.add_argument("--policy", default="srpt", choices=["srpt", "fifo", "srpt_across"],
-                    help="serving: dispatch policy (SRPT within a scene; srpt_across also gates scenes)")
+    ap.add_argument("--policy", default="srpt", choices=["srpt", "fifo", "srpt_across", "srpt_small"],
+                    help="serving: dispatch policy (SRPT within a scene; srpt_across also gates scenes; srpt_small "
+                         "gates them only while a small job renders)")
     ap.add_argument("--spp", type=int, default=0)
     ap.add_argument("--views", type=int, default=0)
     ap.add_argument("--res", type=int, default=0)
@@ -382,7 +383,8 @@ def run_serving(args):
     tris = [int(g.info.n_triangles) for g in gss]
     rng = np.random.default_rng(7)
     depths = [sd.depth for sd in sds]
-    policy = {"srpt": serving.SRPT, "fifo": serving.FIFO, "srpt_across": serving.SRPT_ACROSS}[args.policy]
+    policy = {"srpt": serving.SRPT, "fifo": serving.FIFO, "srpt_across": serving.SRPT_ACROSS,
+              "srpt_small": serving.SRPT_SMALL}[args.policy]
     with serving.Server(capacity=args.capacity, iterations_per_poll=4, policy=policy) as srv:
         for g in gss:
             srv.add_scene(g)

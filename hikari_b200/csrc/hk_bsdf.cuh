@@ -1,7 +1,8 @@
 // Device BSDFs of the pathMIS core: diffuse, roughConductor, roughDielectric,
-// roughPlastic, roughCoating and coating (over one leaf BSDF), roughDiffuse,
-// the smooth mirror, conductor, dielectric and plastic, and twoSided (over one
-// layer per side),
+// roughPlastic, roughCoating and coating, roughDiffuse, the smooth mirror,
+// conductor, dielectric and plastic, and twoSided; layers (coatings, twoSided)
+// stack up to kNestLevels deep (one level inline, deeper stacks through the
+// deep_* functions),
 // with the Beckmann/GGX microfacet distribution and the 1D rough-transmittance
 // lookups.
 //
@@ -1079,7 +1080,7 @@ __device__ __forceinline__ float scoating_pdf(const DevBsdf &b, const DevBsdf &n
 // ------------------------------------------------------------ full dispatch
 // A layer is a leaf BSDF or a (rough) coating over a leaf; a twoSided BSDF picks
 // one layer per side (src/bsdf/TwoSidedBSDF.cpp:19-67), mirroring z for the
-// back side.  The host rejects deeper nestings.
+// back side.  Deeper stacks go through deep_* below.
 __device__ __forceinline__ V3 layer_eval(const DevBsdf *bs, const DevBsdf &b, const BRec &r) {
     if (b.type == kRoughCoating) return coating_eval(b, bs[b.nested], r);
     if (b.type == kCoating) return scoating_eval(b, bs[b.nested], r);
@@ -1119,13 +1120,297 @@ __device__ __forceinline__ V3 twosided_sample(const DevBsdf *bs, const DevBsdf &
     }
     return res;
 }
+// ---- stacks deeper than one layer (a coating over a coating or a twoSided, a
+// twoSided over a twoSided or over a coated coating; the host flags them `deep`
+// and bounds them to kNestLevels layers).  The reference evaluates a stack by
+// recursion (each coating calls its nested BSDF, src/bsdf/RoughCoatingBSDF.cpp,
+// src/bsdf/CoatingBSDF.cpp, src/bsdf/TwoSidedBSDF.cpp); here one loop walks
+// down the stack, recording what each layer adds and multiplies, evaluates the
+// leaf once, and applies the layers on the way back up in the reference's
+// operation order -- the same arithmetic as coating_* / scoating_* above, in
+// three compact out-of-line functions.
+static __device__ __noinline__ V3 deep_leaf_eval(const DevBsdf &b, const BRec &r) { return leaf_eval(b, r); }
+static __device__ __noinline__ float deep_leaf_pdf(const DevBsdf &b, const BRec &r) { return leaf_pdf(b, r); }
+static __device__ __noinline__ V3 deep_leaf_sample(const DevBsdf &b, BRec &r, float ux, float uy, float u1) {
+    return leaf_sample(b, r, ux, uy, u1);
+}
+struct DeepLayer {
+    int kind;        // 0 roughCoating, 1 coating, 2 twoSided (no arithmetic on the way up)
+    bool has_e, has_s;
+    V3 add, e;       // eval: the layer's own lobe; its absorption factor
+    float m1, m2;    // eval: rft in and out (roughCoating), 1 - R12 and 1 - R21 (coating); pdf: the nested weight
+    float s;         // the solid-angle factor of the refraction
+};
+static __device__ __noinline__ V3 deep_eval(const DevBsdf *bs, int id, const BRec &r0) {
+    DeepLayer L[kNestLevels];
+    int n = 0;
+    BRec c = r0;
+    V3 v = v3(0, 0, 0);
+    bool stop = false;
+    for (;;) {
+        const DevBsdf &b = bs[id];
+        if (n == kNestLevels || !(b.type == kRoughCoating || b.type == kCoating || b.type == kTwoSided)) {
+            v = deep_leaf_eval(b, c);
+            break;
+        }
+        DeepLayer &l = L[n++];
+        l.kind = b.type == kRoughCoating ? 0 : b.type == kCoating ? 1 : 2;
+        l.has_e = l.has_s = false;
+        if (l.kind == 2) {   // TwoSidedBSDF::Eval (:46)
+            if (c.wi.z > 0.0f) {
+                id = b.nested;
+            } else {
+                c.wi.z *= -1.0f;
+                c.wo.z *= -1.0f;
+                id = b.nested2;
+            }
+            continue;
+        }
+        BRec ri = c;
+        if (l.kind == 0) {   // RoughCoatingBSDF::Eval (coating_eval)
+            const float ci = c.wi.z, co = c.wo.z;
+            if (ci * co <= 0.0f) { stop = true; break; }
+            const float a = coat_alpha(b, c);
+            Mfd d = mfd_make(b.distribution, a, a);
+            V3 h = normalize(c.wi + c.wo) * signum(c.wo.z);
+            float ct;
+            float D = mfd_eval(d, h);
+            float F = fresnel_dielectric(fabsf(dot(c.wi, h)), b.eta, b.inv_eta, ct);
+            float G = mfd_g(d, c.wi, c.wo, h);
+            float den = 4.0f * fabsf(ci);
+            const V3 ks = par_rgb(b, 1, b.ks, c);
+            l.add = v3((((ks.x * F) * D) * G) / den, (((ks.y * F) * D) * G) / den, (((ks.z * F) * D) * G) / den);
+            ri.wi = coat_refract(c.wi, b.inv_eta);
+            ri.wo = coat_refract(c.wo, b.inv_eta);
+            l.m1 = rft_eval(b, fabsf(ci), d.au);
+            l.m2 = rft_eval(b, fabsf(co), d.au);
+            V3 sa = par_rgb(b, 3, b.sigma_a, c) * b.thickness;
+            if (!is_zero(sa)) {
+                float q = 1.0f / fabsf(ri.wi.z) + 1.0f / fabsf(ri.wo.z);
+                l.e = v3(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q));
+                l.has_e = true;
+            }
+        } else {             // CoatingBSDF::Eval (scoating_eval)
+            if (c.measure == kMeasureDiscrete) {
+                float ct;
+                v = delta_match(reflect_n(c.wi), c.wo)
+                        ? par_rgb(b, 1, b.ks, c) * fresnel_dielectric(fabsf(c.wi.z), b.eta, b.inv_eta, ct)
+                        : v3(0, 0, 0);
+                --n;
+                break;
+            }
+            float R12, R21;
+            ri.wi = scoat_refract_in(b, c.wi, R12);
+            ri.wo = scoat_refract_in(b, c.wo, R21);
+            if (R12 == 1.0f || R21 == 1.0f) { stop = true; break; }
+            l.m1 = 1.0f - R12;
+            l.m2 = 1.0f - R21;
+            V3 sa = par_rgb(b, 3, b.sigma_a, c) * b.thickness;
+            if (!is_zero(sa)) {
+                float q = 1.0f / fabsf(ri.wi.z) + 1.0f / fabsf(ri.wo.z);
+                l.e = v3(expf(-sa.x * q), expf(-sa.y * q), expf(-sa.z * q));
+                l.has_e = true;
+            }
+        }
+        if (c.measure == kMeasureSolidAngle) { l.s = b.inv_eta * b.inv_eta * c.wo.z / ri.wo.z; l.has_s = true; }
+        c = ri;
+        id = b.nested;
+    }
+    if (stop) { v = v3(0, 0, 0); --n; }   // the layer that stopped contributes zero
+    for (int k = n - 1; k >= 0; --k) {
+        const DeepLayer &l = L[k];
+        if (l.kind == 2) continue;
+        if (l.kind == 0) {
+            V3 nv = v3(v.x * l.m1 * l.m2, v.y * l.m1 * l.m2, v.z * l.m1 * l.m2);
+            if (l.has_e) nv = nv * l.e;
+            if (l.has_s) nv = nv * l.s;
+            v = l.add + nv;
+        } else {
+            V3 res = (v * l.m1) * l.m2;
+            if (l.has_e) res = res * l.e;
+            if (l.has_s) res = res * l.s;
+            v = res;
+        }
+    }
+    return v;
+}
+static __device__ __noinline__ float deep_pdf(const DevBsdf *bs, int id, const BRec &r0) {
+    DeepLayer L[kNestLevels];
+    int n = 0;
+    BRec c = r0;
+    float p = 0.0f;
+    for (;;) {
+        const DevBsdf &b = bs[id];
+        if (n == kNestLevels || !(b.type == kRoughCoating || b.type == kCoating || b.type == kTwoSided)) {
+            p = deep_leaf_pdf(b, c);
+            break;
+        }
+        DeepLayer &l = L[n++];
+        l.kind = b.type == kRoughCoating ? 0 : b.type == kCoating ? 1 : 2;
+        l.has_s = false;
+        if (l.kind == 2) {   // TwoSidedBSDF::Pdf (:61)
+            if (c.wi.z > 0.0f) {
+                id = b.nested;
+            } else {
+                c.wi.z *= -1.0f;
+                c.wo.z *= -1.0f;
+                id = b.nested2;
+            }
+            continue;
+        }
+        BRec ri = c;
+        if (l.kind == 0) {   // RoughCoatingBSDF::Pdf (coating_pdf)
+            V3 h = normalize(c.wi + c.wo) * signum(c.wo.z);
+            const float a = coat_alpha(b, c);
+            Mfd d = mfd_make(b.distribution, a, a);
+            const float ci = c.wi.z, co = c.wo.z;
+            float r12 = 1.0f - rft_eval(b, fabsf(ci), d.au);
+            float sp = (r12 * b.spec_w) / (r12 * b.spec_w + (1.0f - r12) * (1.0f - b.spec_w));
+            l.m1 = 1.0f - sp;
+            l.add.x = 0.0f;
+            if (ci * co > 0.0f) {
+                float J = 1.0f / (4.0f * fabsf(dot(c.wo, h)));
+                l.add.x = mfd_pdf(d, h) * J * sp;
+            }
+            ri.wi = coat_refract(c.wi, b.inv_eta);
+            ri.wo = coat_refract(c.wo, b.inv_eta);
+            if (ri.measure == kMeasureSolidAngle) { l.s = b.inv_eta * b.inv_eta * co / ri.wo.z; l.has_s = true; }
+        } else {             // CoatingBSDF::Pdf (scoating_pdf)
+            float R12, R21;
+            V3 wip = scoat_refract_in(b, c.wi, R12);
+            float sp = scoat_spec_pdf(b, R12);
+            if (c.measure == kMeasureDiscrete) {
+                p = delta_match(reflect_n(c.wi), c.wo) ? sp : 0.0f;
+                --n;
+                break;
+            }
+            ri.wi = wip;
+            ri.wo = scoat_refract_in(b, c.wo, R21);
+            if (R12 == 1.0f || R21 == 1.0f) { p = 0.0f; --n; break; }
+            l.m1 = 1.0f - sp;
+            if (c.measure == kMeasureSolidAngle) { l.s = b.inv_eta * b.inv_eta * c.wo.z / ri.wo.z; l.has_s = true; }
+        }
+        c = ri;
+        id = b.nested;
+    }
+    for (int k = n - 1; k >= 0; --k) {
+        const DeepLayer &l = L[k];
+        if (l.kind == 2) continue;
+        if (l.has_s) p *= l.s;
+        p = l.kind == 0 ? l.add.x + p * l.m1 : p * l.m1;
+    }
+    return p;
+}
+static __device__ __noinline__ V3 deep_sample(const DevBsdf *bs, int id0, BRec &r, float ux, float uy, float u1) {
+    struct Down {
+        int id, kind;   // kind: 0 roughCoating, 1 coating, 2 twoSided
+        bool spec;      // roughCoating: the layer's own lobe was sampled (the walk ended here)
+        V3 wi, wip;     // wi on entering the layer; coating: wi refracted into it
+        float r12, sp;  // coating: the entering Fresnel reflectance and the specular probability
+    } L[kNestLevels];
+    int n = 0, id = id0;
+    V3 res = v3(0, 0, 0);
+    for (;;) {   // down: each layer picks its lobe and passes the refracted wi on
+        const DevBsdf &b = bs[id];
+        if (n == kNestLevels || !(b.type == kRoughCoating || b.type == kCoating || b.type == kTwoSided)) {
+            res = deep_leaf_sample(b, r, ux, uy, u1);
+            break;
+        }
+        Down &l = L[n++];
+        l.id = id;
+        l.kind = b.type == kRoughCoating ? 0 : b.type == kCoating ? 1 : 2;
+        l.spec = false;
+        l.wi = r.wi;
+        if (l.kind == 2) {   // TwoSidedBSDF::Sample (:21)
+            const bool flip = r.wi.z < 0.0f;
+            if (flip) r.wi.z *= -1.0f;
+            l.spec = flip;   // twoSided: whether the back side was taken
+            id = flip ? b.nested2 : b.nested;
+            continue;
+        }
+        if (l.kind == 0) {   // RoughCoatingBSDF::Sample (coating_sample)
+            const float a = coat_alpha(b, r);
+            Mfd d = mfd_make(b.distribution, a, a);
+            float aci = fabsf(r.wi.z);
+            float r12 = 1.0f - rft_eval(b, aci, d.au);
+            float sp = (r12 * b.spec_w) / (r12 * b.spec_w + (1.0f - r12) * (1.0f - b.spec_w));
+            if (ux < sp) {
+                ux /= sp;
+                l.spec = true;
+                float pdf;
+                V3 m = mfd_sample(d, ux, uy, pdf);
+                r.wo = reflect_m(r.wi, m);
+                r.measure = kMeasureDiscrete;
+                r.eta = 1.0f;
+                res = r.wo.z * r.wo.z <= 0.0f ? v3(0, 0, 0) : v3(1, 1, 1);
+                break;
+            }
+            ux = (ux - sp) / (1.0f - sp);
+            r.wi = coat_refract(r.wi, b.inv_eta);
+        } else {             // CoatingBSDF::Sample (scoating_sample)
+            float R12;
+            l.wip = scoat_refract_in(b, r.wi, R12);
+            l.r12 = R12;
+            l.sp = scoat_spec_pdf(b, R12);
+            if (ux < l.sp) {
+                r.wo = reflect_n(r.wi);
+                r.eta = 1.0f;
+                r.measure = kMeasureDiscrete;
+                res = par_rgb(b, 1, b.ks, r) * (R12 / l.sp);
+                --n;
+                break;
+            }
+            ux = (ux - l.sp) / (1.0f - l.sp);
+            if (R12 == 1.0f) { res = v3(0, 0, 0); --n; break; }
+            r.wi = l.wip;
+        }
+        id = b.nested;
+    }
+    for (int k = n - 1; k >= 0; --k) {   // up: each layer refracts wo out and weighs the sample
+        const Down &l = L[k];
+        const DevBsdf &b = bs[l.id];
+        if (l.kind == 2) {
+            if (l.spec) {
+                r.wi.z *= -1.0f;
+                if (!is_zero(res)) r.wo.z *= -1.0f;
+            }
+            continue;
+        }
+        if (l.kind == 0) {
+            if (!l.spec) {
+                r.wi = l.wi;
+                if (is_zero(res)) continue;
+                r.wo = coat_refract(r.wo, b.eta);
+                if (is_zero(r.wo)) { res = v3(0, 0, 0); continue; }
+            } else if (is_zero(res)) {
+                continue;
+            }
+            float P = deep_pdf(bs, l.id, r);
+            res = P == 0.0f ? v3(0, 0, 0) : deep_eval(bs, l.id, r) / P;
+            continue;
+        }
+        r.wi = l.wi;
+        if (is_zero(res)) continue;
+        V3 wop = r.wo;
+        res = scoat_absorb(b, r, res, l.wip, wop);
+        float R21;
+        r.wo = scoat_refract_out(b, wop, R21);
+        if (R21 == 1.0f) { res = v3(0, 0, 0); continue; }
+        res = res / (1.0f - l.sp);
+        res = res * ((1.0f - l.r12) * (1.0f - R21));
+    }
+    return res;
+}
+
 __device__ __forceinline__ V3 bsdf_eval(const DevBsdf *bs, int id, const BRec &r) {
     const DevBsdf &b = bs[id];
+    if (b.deep) return deep_eval(bs, id, r);
     if (b.type == kTwoSided) return twosided_eval(bs, b, r);
     return layer_eval(bs, b, r);
 }
 __device__ __forceinline__ float bsdf_pdf(const DevBsdf *bs, int id, const BRec &r) {
     const DevBsdf &b = bs[id];
+    if (b.deep) return deep_pdf(bs, id, r);
     if (b.type == kTwoSided) return twosided_pdf(bs, b, r);
     return layer_pdf(bs, b, r);
 }
@@ -1136,10 +1421,17 @@ __device__ __forceinline__ bool needs_u1(const DevBsdf *bs, int id) {
     if (bs[id].type == kBumpMap || bs[id].type == kNormalMap) id = bs[id].nested;
     const DevBsdf &b = bs[id];
     if (b.type == kRoughDielectric) return true;
+    if (b.deep) {   // a stack of coatings over a rough dielectric
+        if (b.type == kTwoSided) return false;
+        int k = b.nested;
+        for (int l = 1; l < kNestLevels && (bs[k].type == kRoughCoating || bs[k].type == kCoating); ++l) k = bs[k].nested;
+        return bs[k].type == kRoughDielectric;
+    }
     return (b.type == kRoughCoating || b.type == kCoating) && bs[b.nested].type == kRoughDielectric;
 }
 __device__ __forceinline__ V3 bsdf_sample(const DevBsdf *bs, int id, BRec &r, float ux, float uy, float u1) {
     const DevBsdf &b = bs[id];
+    if (b.deep) return deep_sample(bs, id, r, ux, uy, u1);
     if (b.type == kTwoSided) return twosided_sample(bs, b, r, ux, uy, u1);
     return layer_sample(bs, b, r, ux, uy, u1);
 }

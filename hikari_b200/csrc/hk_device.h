@@ -24,6 +24,9 @@ constexpr int kRftThetaMax = 100;   // data/*RFTData.bin hold 100 theta samples
 // transmittance table reduced at activation (RoughTransmittance::SetEta then
 // SetAlpha, src/core/RoughTransmitance.cpp:170,237).
 struct DevTexture;
+// Layers (coatings, twoSided) a BSDF may stack above its leaf BSDFs: the
+// device's deep layer dispatch is unrolled to this depth
+constexpr int kNestLevels = 4;
 struct alignas(16) DevBsdf {
     int32_t type, distribution, anisotropic, nonlinear;
     float alpha_u, alpha_v;          // clamped to [MIN_ALPHA, MAX_ALPHA]
@@ -37,6 +40,10 @@ struct alignas(16) DevBsdf {
     int32_t nested;                  // (rough)coating nested BSDF / twoSided front BSDF index, -1 otherwise
     int32_t rft_n;                   // theta samples in rft[]
     int32_t nested2;                 // twoSided back BSDF index (the front one when only one is given)
+    // a layered BSDF nested deeper than one (rough) coating over a leaf, or a
+    // twoSided over such a layer or over a twoSided: dispatched through the
+    // bounded-depth layer dispatch (hk_bsdf.cuh deep_*), never by per-type kernels
+    int32_t deep;
     int32_t fast_approx;             // roughDiffuse: the fast Oren-Nayar approximation
     // textures of kd, ks, ks_refract, sigma_a, alpha_u, alpha_v: 1 + index into
     // textures, 0 = the constant above; textured: any slot here or in a nested BSDF
@@ -52,7 +59,6 @@ struct alignas(16) DevBsdf {
     const float *rft2d;
     const float *rft_diff;
     float rft_amin, rft_amax;
-    int32_t pad5, pad6;
 };
 
 // cutpoints per CDF in the environment map's guide tables (a power of two)

@@ -218,6 +218,7 @@ struct MeshIn {
 struct hk_scene {
     // inputs
     std::vector<hk_bsdf_desc> bsdfs;
+    std::vector<int> bsdf_deep;   // per BSDF: dispatched through the deep layer dispatch (set by the build)
     std::vector<hk_texture_desc> textures;
     std::vector<std::shared_ptr<hk::MipPyramid>> bitmaps;   // per texture: the MIP pyramid of a bitmap, else null
     std::vector<MeshIn> meshes;
@@ -410,6 +411,32 @@ void tex_range0(const hk_scene *s, int id, float &lo, float &hi) {
     hi = std::max(t.a[0], t.b[0]);
 }
 
+bool is_layer(int type) { return type == hk::kRoughCoating || type == hk::kCoating || type == hk::kTwoSided; }
+
+// Layers above the leaf BSDFs: 0 for a leaf, one more than the nested BSDF for
+// a (rough) coating, one more than the deeper side for a twoSided; a cycle or
+// an invalid index counts as too deep.
+int layer_depth(const hk_scene *s, int id, int guard) {
+    if (id < 0 || id >= (int)s->bsdfs.size() || guard > 2 * hk::kNestLevels) return 1 << 20;
+    const hk_bsdf_desc &d = s->bsdfs[id];
+    if (d.type == hk::kRoughCoating || d.type == hk::kCoating) return 1 + layer_depth(s, d.nested, guard + 1);
+    if (d.type == hk::kTwoSided)
+        return 1 + std::max(layer_depth(s, d.nested, guard + 1),
+                            layer_depth(s, d.nested2 < 0 ? d.nested : d.nested2, guard + 1));
+    return 0;
+}
+
+// Whether the one-level dispatch (a coating over a leaf; a twoSided over leaves
+// or coatings over leaves) cannot evaluate the BSDF, so that it goes through
+// the bounded-depth layer dispatch.
+bool layer_deep(const hk_scene *s, const hk_bsdf_desc &d) {
+    if (d.type == hk::kRoughCoating || d.type == hk::kCoating) return is_layer(s->bsdfs[d.nested].type);
+    if (d.type != hk::kTwoSided) return false;
+    for (int side : {d.nested, d.nested2 < 0 ? d.nested : d.nested2})
+        if (s->bsdfs[side].type == hk::kTwoSided || layer_depth(s, side, 0) >= 2) return true;
+    return false;
+}
+
 // rft_pool: where a textured alpha's 2D transmittance tables go (their
 // offsets are kept in rft2d / rft_diff until the pool is on the device)
 hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs, std::vector<float> &rft_pool) {
@@ -494,9 +521,8 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs,
             b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
             if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "RoughCoatingBSDF needs a nested BSDF!"};
             const int nt = s->bsdfs[d.nested].type;
-            if (nt == hk::kRoughCoating || nt == hk::kCoating || nt == hk::kTwoSided || nt == hk::kBumpMap ||
-                nt == hk::kNormalMap)
-                throw HkError{HK_ERR_INVALID, "roughCoating over a coating, twoSided, bumpMap or normalMap BSDF is not supported"};
+            if (nt == hk::kBumpMap || nt == hk::kNormalMap)
+                throw HkError{HK_ERR_INVALID, "roughCoating over a bumpMap or normalMap BSDF is not supported"};
         }
     }
     if (d.type == hk::kCoating) {   // CoatingBSDF::Activate (:255)
@@ -508,9 +534,8 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs,
         b.spec_w = 1.0f / ((a0 + a1 + a2) / 3.0f + 1.0f);
         if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "CoatingBSDF needs a nested BSDF!"};
         const int nt = s->bsdfs[d.nested].type;
-        if (nt == hk::kRoughCoating || nt == hk::kCoating || nt == hk::kTwoSided || nt == hk::kBumpMap ||
-            nt == hk::kNormalMap)
-            throw HkError{HK_ERR_INVALID, "coating over a coating, twoSided, bumpMap or normalMap BSDF is not supported"};
+        if (nt == hk::kBumpMap || nt == hk::kNormalMap)
+            throw HkError{HK_ERR_INVALID, "coating over a bumpMap or normalMap BSDF is not supported"};
     }
     if (d.type == hk::kConductor)   // ConductorBSDF ctor (:17): m_Eta = Color3f(intIOR / extIOR)
         for (int c = 0; c < 3; c++) b.eta_c[c] = b.eta;
@@ -528,10 +553,15 @@ hk::DevBsdf activate_bsdf(const hk_scene *s, const hk_bsdf_desc &d, int n_bsdfs,
         if (d.nested2 < 0) b.nested2 = d.nested;
         for (int side : {b.nested, b.nested2}) {
             const int st = s->bsdfs[side].type;
-            if (st == hk::kTwoSided || st == hk::kBumpMap || st == hk::kNormalMap)
-                throw HkError{HK_ERR_INVALID, "twoSided over a twoSided, bumpMap or normalMap BSDF is not supported"};
+            if (st == hk::kBumpMap || st == hk::kNormalMap)
+                throw HkError{HK_ERR_INVALID, "twoSided over a bumpMap or normalMap BSDF is not supported"};
             if (bsdf_transmits(s, side, 0)) throw HkError{HK_ERR_INVALID, "Only BSDF without transmission can be nested!"};
         }
+    }
+    if (is_layer(d.type)) {
+        if (layer_depth(s, (int)(&d - s->bsdfs.data()), 0) > hk::kNestLevels)
+            throw HkError{HK_ERR_INVALID, "BSDF layers nested deeper than 4 (or in a cycle) are not supported"};
+        b.deep = layer_deep(s, d) ? 1 : 0;
     }
     if (d.type == hk::kBumpMap || d.type == hk::kNormalMap) {   // BumpMapBSDF / NormalMapBSDF::Activate
         if (d.nested < 0 || d.nested >= n_bsdfs) throw HkError{HK_ERR_INVALID, "bumpMap / normalMap needs a nested BSDF"};
@@ -640,6 +670,8 @@ void build_scene(hk_scene *s) {
     s->b_textures.upload(tex); track(s->b_textures);
     std::vector<float> rft_pool;
     for (auto &d : s->bsdfs) bs.push_back(activate_bsdf(s, d, (int)s->bsdfs.size(), rft_pool));
+    s->bsdf_deep.clear();
+    for (const hk::DevBsdf &b : bs) s->bsdf_deep.push_back(b.deep);
     if (!rft_pool.empty()) { s->b_rft2d.upload(rft_pool); track(s->b_rft2d); }
     for (size_t i = 0; i < bs.size(); ++i) {
         if (bs[i].alpha_tex) {   // pool offsets -> device pointers
@@ -1799,7 +1831,7 @@ int hk_bsdf_batch(hk_scene *s, int32_t bsdf, uint64_t n, const float *wi, const 
         if (bsdf < 0 || bsdf >= s->dev.nbsdfs) throw HkError{HK_ERR_INVALID, "invalid BSDF id"};
         if (n == 0) return HK_OK;
         if (!wi || !u2 || !wo) throw HkError{HK_ERR_INVALID, "bad arguments"};
-        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, s->bsdfs[bsdf].type, n, wi, u2, u1, wo, uv, duv, s_wo, s_w, s_pdf,
+        HK_CUDA(hk::launch_bsdf_batch(s->dev, bsdf, s->bsdf_deep[bsdf] ? -1 : s->bsdfs[bsdf].type, n, wi, u2, u1, wo, uv, duv, s_wo, s_w, s_pdf,
                                       s_m, e_rgb, p_pdf, (cudaStream_t)stream));
         return HK_OK;
     });

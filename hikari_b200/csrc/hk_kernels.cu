@@ -182,6 +182,7 @@ cudaError_t launch_bsdf_batch(const DevScene &S, int bsdf, int type, uint64_t n,
         HK_BSDF_BATCH(kTwoSided);
         HK_BSDF_BATCH(kCoating);
         HK_BSDF_BATCH(kRoughDiffuse);
+        HK_BSDF_BATCH(-1);   // layers nested deeper than one level: run-time dispatch
     default: return cudaErrorInvalidValue;
     }
 #undef HK_BSDF_BATCH

@@ -307,8 +307,9 @@ void hk_server::launch(const std::vector<SceneEntry *> &sc) {
     for (size_t k = 0; k < sc.size(); ++k) {
         SceneEntry &e = *sc[k];
         if (!e.eng || e.inflight) continue;
-        if (cfg.policy == HK_SERVE_SRPT_ACROSS && scene_least[k] != UINT64_MAX &&
-            scene_least[k] > (uint64_t)HK_SERVE_GATE * global_least)
+        const bool gated = cfg.policy == HK_SERVE_SRPT_ACROSS ||
+                           (cfg.policy == HK_SERVE_SRPT_SMALL && global_least <= HK_SERVE_SMALL_WORK);
+        if (gated && scene_least[k] != UINT64_MAX && scene_least[k] > (uint64_t)HK_SERVE_GATE * global_least)
             continue;   // waits while a much smaller job of another scene renders
         std::vector<Job *> rendering;
         for (Job *j : e.jobs)
@@ -509,7 +510,8 @@ int hk_server_create(const hk_server_config *cfg, hk_server **out) {
         if (c.iterations_per_poll <= 0) c.iterations_per_poll = 4;
         if (c.max_jobs <= 0) c.max_jobs = 256;
         if (c.max_jobs > hk::kWfMaxJobs) throw HkError{HK_ERR_INVALID, "max_jobs above 1024"};
-        if (c.policy != HK_SERVE_SRPT && c.policy != HK_SERVE_FIFO && c.policy != HK_SERVE_SRPT_ACROSS)
+        if (c.policy != HK_SERVE_SRPT && c.policy != HK_SERVE_FIFO && c.policy != HK_SERVE_SRPT_ACROSS &&
+            c.policy != HK_SERVE_SRPT_SMALL)
             throw HkError{HK_ERR_INVALID, "unknown policy"};
         if (c.capacity < 1024 || c.capacity > (1 << 26)) throw HkError{HK_ERR_INVALID, "capacity outside [1024, 2^26]"};
         s->ec.capacity = c.capacity;

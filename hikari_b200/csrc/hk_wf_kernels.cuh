@@ -141,7 +141,8 @@ __global__ void __launch_bounds__(256, kMinBlocks) wf_extend_kernel(DevScene S, 
             const int mesh = __float_as_int(__ldg(S.tris + 3 * w.hit.tri + 1).w);
             const DevBsdf &B = S.bsdfs[S.meshes[mesh].bsdf];
             const bool map = B.type == kBumpMap || B.type == kNormalMap;
-            type = wf_queue_of(B.type, B.textured != 0, map ? S.bsdfs[B.nested].type : -1);
+            type = B.deep ? kWfGenericQueue : wf_queue_of(B.type, B.textured != 0, map ? S.bsdfs[B.nested].type : -1);
+            if (map && S.bsdfs[B.nested].deep) type = kWfGenericQueue;   // a map over a deep stack of layers
         }
         W.hit[slot] = make_float4(w.hit.t, w.hit.u, w.hit.v, __int_as_float(w.found ? w.hit.tri : -1));
         W.sq[type][warp_append_keyed(W.ctr->sq_count, type)] = slot;

@@ -22,7 +22,7 @@ import numpy as np
 
 from . import HikariError, JobStatus, Scene, ServerConfig, ServerStats, check, lib, render_desc
 
-SRPT, FIFO, SRPT_ACROSS = 0, 1, 2
+SRPT, FIFO, SRPT_ACROSS, SRPT_SMALL = 0, 1, 2, 3
 QUEUED, RUNNING, DONE, CANCELLED, FAILED = 0, 1, 2, 3, 4
 HK_ERR_TIMEOUT = -5
 

@@ -66,7 +66,10 @@ typedef struct {
     float kd[3];           /* roughPlastic "kd", diffuse "albedo" */
     float sigma_a[3];      /* roughCoating "sigmaA" */
     float thickness;       /* roughCoating "thickness" */
-    int32_t nested;        /* roughCoating / twoSided front: id of the nested BSDF (added first), else -1 */
+    int32_t nested;        /* roughCoating / twoSided front: id of the nested BSDF (added first), else -1;
+                              coatings and twoSided stack up to four layers above a leaf BSDF (deeper
+                              stacks fail hk_scene_build); a bumpMap / normalMap may wrap a stack but
+                              not sit inside one */
     int32_t nested2;       /* twoSided back: id of the second nested BSDF, -1 = the front one */
     int32_t fast_approx;   /* roughDiffuse "fastApprox" */
     /* textures of kd / albedo, ks / ksReflect, ksRefract, sigmaA, alpha / alphaU,
@@ -386,6 +389,12 @@ typedef struct hk_server hk_server;
  * small job is not slowed by large jobs of other scenes sharing the GPU. */
 #define HK_SERVE_SRPT_ACROSS 2
 #define HK_SERVE_GATE 4
+/* SRPT within a scene; across scenes the gate of HK_SERVE_SRPT_ACROSS holds
+ * only while the least job of any scene has at most HK_SERVE_SMALL_WORK paths
+ * left: a small job gets the GPU nearly to itself for the few milliseconds it
+ * needs, while large jobs of different scenes keep overlapping. */
+#define HK_SERVE_SRPT_SMALL 3
+#define HK_SERVE_SMALL_WORK (1ull << 22)
 
 #define HK_JOB_QUEUED 0
 #define HK_JOB_RUNNING 1

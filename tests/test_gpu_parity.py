@@ -33,13 +33,13 @@ DEV = "cuda:0"
 RTOL = 1e-5
 
 
-@pytest.fixture(scope="module", params=["rough", "smooth", "textured"])
+@pytest.fixture(scope="module", params=["rough", "smooth", "textured", "nested"])
 def bsdf_pair(request):
     """The BSDF-batch material set (rough BSDFs and a coating), the smooth and
-    two-sided set, or the set with procedural textures (records carry texture
-    coordinates)."""
+    two-sided set, the set with procedural textures (records carry texture
+    coordinates), or layers nested deeper than one coating over a leaf."""
     mats = {"rough": scenes.config2_materials, "smooth": scenes.smooth_materials,
-            "textured": scenes.textured_materials}[request.param]()
+            "textured": scenes.textured_materials, "nested": scenes.nested_materials}[request.param]()
     sd = scenes.bsdf_scene(mats)
     return mats, hk.Scene.from_desc(sd), OracleScene(sd), request.param
 
@@ -301,3 +301,26 @@ def test_render_cornell_matches_oracle():
     # normal tail P(|z| > 3) = 0.27%; the per-pixel variances are estimates
     assert frac3 < 0.008
     assert ctr[0] >= 48 * 48 * spp_g
+
+
+def test_layer_nesting_depth_limit():
+    """Coatings stack up to four layers over a leaf BSDF on the device; a fifth
+    is rejected when the scene is built, with the limit in the message."""
+    from hikari_b200.scenedesc import BSDF_COATING, BSDF_DIFFUSE, BSDF_ROUGH_COATING, GGX, BSDFDesc
+
+    def stack(n):
+        d = BSDFDesc(type=BSDF_DIFFUSE, kd=[0.5, 0.5, 0.5])
+        for k in range(n):
+            d = BSDFDesc(type=BSDF_COATING if k % 2 else BSDF_ROUGH_COATING, distribution=GGX, alpha_u=0.2,
+                         alpha_v=0.2, nested=d)
+        return d
+
+    four = scenes.bsdf_scene([("four", stack(4))])
+    gs, os_ = hk.Scene.from_desc(four), OracleScene(four)
+    wi, u2, u1, wo = bsdf_records(1 << 12, 3)
+    d = four.meshes[0].bsdf
+    g = gs.bsdf_batch(gs.bsdf_ids[id(d)], _t(wi), _t(u2), _t(u1), _t(wo))
+    o = os_.bsdf_batch(os_.bsdf_ids[id(d)], wi, u2, u1, wo)
+    assert rel_close(g["e_rgb"].cpu().numpy(), o["e_rgb"], 1e-4).all(1).mean() >= 0.999
+    with pytest.raises(hk.HikariError, match="deeper than 4"):
+        hk.Scene.from_desc(scenes.bsdf_scene([("five", stack(5))]))

@@ -50,6 +50,9 @@ SCENES = {
     # each hit computed on the device and by the oracle (pinned to the reference)
     "geometric": lambda: scenes.lights_scene(width=32, height=32, shading_normals=True, textured=True,
                                              geometric=True),
+    # coatings over coatings and over two-sided BSDFs, two-sided BSDFs inside
+    # two-sided ones (the device's bounded-depth layer dispatch)
+    "nested": lambda: scenes.cornell_nested(width=32, height=32),
 }
 
 

@@ -49,7 +49,7 @@ def _requests(sds):
             (2, 80, 80, 48, 15), (1, 128, 96, 16, 16)]
 
 
-@pytest.mark.parametrize("policy", [serving.SRPT, serving.SRPT_ACROSS])
+@pytest.mark.parametrize("policy", [serving.SRPT, serving.SRPT_ACROSS, serving.SRPT_SMALL])
 def test_same_alone_and_in_mix(resident, policy):
     sds, gss = resident
     reqs = _requests(sds)
