@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--workload", default="heterogeneous",
                     choices=["heterogeneous", "mesh_heavy", "cornell", "textured", "serving", "bsdf"])
     ap.add_argument("--records", type=int, default=1 << 26, help="bsdf: records per material")
+    ap.add_argument("--material", default="conductor", choices=["conductor", "dielectric", "plastic"],
+                    help="mesh_heavy: the icosphere's material (the three runs of the mesh-heavy workload)")
     ap.add_argument("--accel", default="bvh8", choices=["bvh8", "bvh2"],
                     help="tree the kernels traverse: compressed 8-wide (80-byte nodes) or binary (64-byte nodes)")
     ap.add_argument("--jobs", type=int, default=400, help="serving: jobs of the Poisson run")
@@ -81,7 +83,7 @@ def parse():
     return ap.parse_args()
 
 
-def make_workload(name, spp=0, views=0, res=0):
+def make_workload(name, spp=0, views=0, res=0, material="conductor"):
     from hikari_b200 import scenes
 
     if name == "heterogeneous":
@@ -92,9 +94,11 @@ def make_workload(name, spp=0, views=0, res=0):
                 f"2048x1024 sky; {len(cams)} views x {r}x{r} x {sd.spp} spp, pathMIS depth 16")
     elif name == "mesh_heavy":
         r = res or 1024
-        sd = scenes.mesh_heavy("conductor", width=r, height=r, spp=spp or 256, depth=16)
+        sd = scenes.mesh_heavy(material, width=r, height=r, spp=spp or 256, depth=16)
         cams = [None] * (views or 1)
-        desc = f"mesh_heavy: displaced level-8 icosphere (1.31M tris), GGX conductor, sky; {r}x{r} x {sd.spp} spp"
+        mat = {"conductor": "GGX rough conductor alpha 0.2", "dielectric": "rough dielectric IOR 1.5 alpha 0.1",
+               "plastic": "rough plastic alpha 0.15"}[material]
+        desc = f"mesh_heavy: displaced level-8 icosphere (1.31M tris), {mat}, sky; {r}x{r} x {sd.spp} spp"
     elif name == "textured":
         r = res or 1024
         sd = scenes.lights_scene(width=r, height=r, spp=spp or 64, depth=12, shading_normals=True, textured=True,
@@ -322,7 +326,7 @@ def cpu_baseline(sd, cams, depth):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    sd, cams, desc = make_workload(args.workload, args.spp, args.views, args.res)
+    sd, cams, desc = make_workload(args.workload, args.spp, args.views, args.res, args.material)
     cb = cpu_baseline(sd, cams, sd.depth)
     vals = [cb.sample(max(3.0, args.cpu_seconds / 3)) for _ in range(args.warmup + args.steps)]
     v = vals[args.warmup:]
@@ -594,7 +598,7 @@ def main():
         if world > 1:
             dist.barrier()
 
-    sd, cams, desc = make_workload(args.workload, args.spp, args.views, args.res)
+    sd, cams, desc = make_workload(args.workload, args.spp, args.views, args.res, args.material)
     t0 = time.perf_counter()
     gs = hk.Scene.from_desc(sd)
     build_s = time.perf_counter() - t0

@@ -25,7 +25,7 @@ constexpr int kRftThetaMax = 100;   // data/*RFTData.bin hold 100 theta samples
 // SetAlpha, src/core/RoughTransmitance.cpp:170,237).
 struct DevTexture;
 // Layers (coatings, twoSided) a BSDF may stack above its leaf BSDFs: the
-// device's deep layer dispatch is unrolled to this depth
+// device walks at most this many layers of a stack (deep_* in hk_bsdf.cuh)
 constexpr int kNestLevels = 4;
 struct alignas(16) DevBsdf {
     int32_t type, distribution, anisotropic, nonlinear;
