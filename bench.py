@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--workload", default="heterogeneous",
                     choices=["heterogeneous", "mesh_heavy", "cornell", "textured", "serving", "bsdf"])
     ap.add_argument("--records", type=int, default=1 << 26, help="bsdf: records per material")
+    ap.add_argument("--small-work", type=int, default=0,
+                    help="serving, srpt_small: paths left below which a job gates the other scenes (0 = 2^22)")
     ap.add_argument("--material", default="conductor", choices=["conductor", "dielectric", "plastic"],
                     help="mesh_heavy: the icosphere's material (the three runs of the mesh-heavy workload)")
     ap.add_argument("--accel", default="bvh8", choices=["bvh8", "bvh2"],
@@ -389,7 +391,7 @@ def run_serving(args):
     depths = [sd.depth for sd in sds]
     policy = {"srpt": serving.SRPT, "fifo": serving.FIFO, "srpt_across": serving.SRPT_ACROSS,
               "srpt_small": serving.SRPT_SMALL}[args.policy]
-    with serving.Server(capacity=args.capacity, iterations_per_poll=4, policy=policy) as srv:
+    with serving.Server(capacity=args.capacity, iterations_per_poll=4, policy=policy, small_work=args.small_work) as srv:
         for g in gss:
             srv.add_scene(g)
         for k in range(len(gss)):   # engines and graphs of every scene (untimed)
@@ -437,7 +439,7 @@ def run_serving(args):
                    "form": f"wavefront serving loop (continuous batching, {args.policy} dispatch)", "triangles": tris,
                    "scene_build_s": round(build_s, 2), "autotune_s": round(tune_s, 2),
                    "traversal": "each scene's autotuned fetch intervals, register budgets and triangle-test modes",
-                   "capacity": args.capacity, "jobs": args.jobs,
+                   "capacity": args.capacity, "jobs": args.jobs, "small_work": args.small_work or (1 << 22),
                    "load": args.load},
         "serving": {
             "peak_mpaths_per_s": peak_mpaths, "peak_rate_hz": peak_rate, "arrival_rate_hz": rate,

@@ -83,7 +83,7 @@ class WavefrontConfig(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("capacity", C.c_int32), ("threads_extend", C.c_int32), ("threads_shade", C.c_int32),
                 ("iterations_per_poll", C.c_int32), ("policy", C.c_int32), ("max_jobs", C.c_int32),
-                ("hbm_budget", C.c_uint64)]
+                ("hbm_budget", C.c_uint64), ("small_work", C.c_uint64)]
 
 
 class JobStatus(C.Structure):

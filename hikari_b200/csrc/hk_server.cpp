@@ -308,7 +308,7 @@ void hk_server::launch(const std::vector<SceneEntry *> &sc) {
         SceneEntry &e = *sc[k];
         if (!e.eng || e.inflight) continue;
         const bool gated = cfg.policy == HK_SERVE_SRPT_ACROSS ||
-                           (cfg.policy == HK_SERVE_SRPT_SMALL && global_least <= HK_SERVE_SMALL_WORK);
+                           (cfg.policy == HK_SERVE_SRPT_SMALL && global_least <= cfg.small_work);
         if (gated && scene_least[k] != UINT64_MAX && scene_least[k] > (uint64_t)HK_SERVE_GATE * global_least)
             continue;   // waits while a much smaller job of another scene renders
         std::vector<Job *> rendering;
@@ -509,6 +509,7 @@ int hk_server_create(const hk_server_config *cfg, hk_server **out) {
         if (c.threads_shade <= 0) c.threads_shade = 128;
         if (c.iterations_per_poll <= 0) c.iterations_per_poll = 4;
         if (c.max_jobs <= 0) c.max_jobs = 256;
+        if (c.small_work == 0) c.small_work = HK_SERVE_SMALL_WORK;
         if (c.max_jobs > hk::kWfMaxJobs) throw HkError{HK_ERR_INVALID, "max_jobs above 1024"};
         if (c.policy != HK_SERVE_SRPT && c.policy != HK_SERVE_FIFO && c.policy != HK_SERVE_SRPT_ACROSS &&
             c.policy != HK_SERVE_SRPT_SMALL)

@@ -39,8 +39,10 @@ class Server:
     staging copy."""
 
     def __init__(self, capacity: int = 0, threads_extend: int = 0, threads_shade: int = 0,
-                 iterations_per_poll: int = 0, policy: int = SRPT, max_jobs: int = 0, hbm_budget: int = 0):
-        cfg = ServerConfig(capacity, threads_extend, threads_shade, iterations_per_poll, policy, max_jobs, hbm_budget)
+                 iterations_per_poll: int = 0, policy: int = SRPT, max_jobs: int = 0, hbm_budget: int = 0,
+                 small_work: int = 0):
+        cfg = ServerConfig(capacity, threads_extend, threads_shade, iterations_per_poll, policy, max_jobs, hbm_budget,
+                           small_work)
         h = C.c_void_p()
         check(lib().hk_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

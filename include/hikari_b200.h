@@ -390,9 +390,10 @@ typedef struct hk_server hk_server;
 #define HK_SERVE_SRPT_ACROSS 2
 #define HK_SERVE_GATE 4
 /* SRPT within a scene; across scenes the gate of HK_SERVE_SRPT_ACROSS holds
- * only while the least job of any scene has at most HK_SERVE_SMALL_WORK paths
- * left: a small job gets the GPU nearly to itself for the few milliseconds it
- * needs, while large jobs of different scenes keep overlapping. */
+ * only while the least job of any scene has at most `small_work` paths left
+ * (hk_server_config; default HK_SERVE_SMALL_WORK): a small job gets the GPU
+ * nearly to itself for the few milliseconds it needs, while large jobs of
+ * different scenes keep overlapping. */
 #define HK_SERVE_SRPT_SMALL 3
 #define HK_SERVE_SMALL_WORK (1ull << 22)
 
@@ -410,6 +411,8 @@ typedef struct {
     int32_t policy;               /* HK_SERVE_SRPT, HK_SERVE_FIFO or HK_SERVE_SRPT_ACROSS */
     int32_t max_jobs;             /* jobs admitted at once per scene (0 = 256, max 1024) */
     uint64_t hbm_budget;          /* device bytes for pools, films and images (0 = 90% of free at create) */
+    uint64_t small_work;          /* HK_SERVE_SRPT_SMALL: paths left below which a job gates the other
+                                     scenes (0 = HK_SERVE_SMALL_WORK) */
 } hk_server_config;
 
 typedef struct {
