@@ -109,7 +109,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     # within a host-memory budget: ptxas takes about 20 GB for the textured
     # megakernels and the run-time-dispatched shade kernel, 9 GB for the other
     # megakernels and a few GB for the rest
-    total = max(16.0, _host_gb() * 0.75)
+    total = max(16.0, _host_gb() * 0.8)
     budget = [total]
     cv = threading.Condition()
 

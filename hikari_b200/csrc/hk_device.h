@@ -40,10 +40,6 @@ struct alignas(16) DevBsdf {
     int32_t nested;                  // (rough)coating nested BSDF / twoSided front BSDF index, -1 otherwise
     int32_t rft_n;                   // theta samples in rft[]
     int32_t nested2;                 // twoSided back BSDF index (the front one when only one is given)
-    // a layered BSDF nested deeper than one (rough) coating over a leaf, or a
-    // twoSided over such a layer or over a twoSided: dispatched through the
-    // bounded-depth layer dispatch (hk_bsdf.cuh deep_*), never by per-type kernels
-    int32_t deep;
     int32_t fast_approx;             // roughDiffuse: the fast Oren-Nayar approximation
     // textures of kd, ks, ks_refract, sigma_a, alpha_u, alpha_v: 1 + index into
     // textures, 0 = the constant above; textured: any slot here or in a nested BSDF
@@ -59,6 +55,12 @@ struct alignas(16) DevBsdf {
     const float *rft2d;
     const float *rft_diff;
     float rft_amin, rft_amax;
+    // a layered BSDF nested deeper than one (rough) coating over a leaf, or a
+    // twoSided over such a layer or over a twoSided: dispatched through the
+    // deep_* functions of hk_bsdf.cuh, never by per-type kernels (kept at the
+    // end so that the fields above keep their offsets and vector loads)
+    int32_t deep;
+    int32_t pad6;
 };
 
 // cutpoints per CDF in the environment map's guide tables (a power of two)
